@@ -1,0 +1,320 @@
+"""Benchmark: the triangle-cloud traversal-stress workload on B200.
+
+Workload (one step): the 1,000,000-triangle cloud (seeded centres uniform in
+[-0.5, 0.5]^3, vertices jittered by N(0, 0.01^2)) rendered at 1920x1080 with
+16 samples per pixel, diffuse albedo 0.5, one distant light, max depth 8,
+Russian roulette from depth 3: 33,177,600 camera samples per step.
+
+Printed (one JSON line on rank 0):
+  value      Msamples/s of the whole job, scene and path state resident in HBM
+             (device time, CUDA events on the session stream, max over ranks);
+  e2e        the same metric through the C ABI's render call a user makes
+             (rt_session_create from host arrays + rt_render_samples +
+             rt_read_image to host), host<->device copies included;
+  roofline   the closest-hit (extend) kernel: algorithmic bytes per extension
+             ray (reference binary BVH: 32 B per node visit, 48 B per triangle
+             test, 48 B per instance visit, 48 B ray in/out, counted by the f64
+             oracle on a pixel sample of the same frame) x rays per launch /
+             launch time, against the measured HBM copy bandwidth;
+  cpu_baseline  the f64 oracle (C++ restatement of the reference's CPU path
+             tracer, all host threads) on a bounded pixel sample of the frame.
+  traversal  the 4,194,304-ray closest-hit and any-hit batches (Mrays/s).
+
+`--impl reference` times the reference arm instead: the reference's CPU path
+(its Rust build is unavailable here, so the f64 C++ restatement of
+src/raytracer/pt/*) on the host cores, on a bounded sample of the workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "render.rs_b200"))
+
+METRIC = "Msamples/s at 1 B200; equal-time relMSE guided vs plain PT vs f64 CPU oracle"
+UNIT = "Msamples/s"
+WIDTH, HEIGHT, SPP, MAX_DEPTH = 1920, 1080, 16, 8
+N_TRIS, N_RAYS = 1_000_000, 4_194_304
+WORKLOAD = "triangle_cloud_1M_1920x1080_16spp_depth8"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_sample(scene, params, threads=0, target_s=12.0):
+    """The f64 oracle on a strided pixel sample of the frame, all host threads.
+    Returns Msamples/s, the sample description and per-ray traversal work."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # test infrastructure: the CPU baseline and the work counter
+    o_s = oracle.OracleScene(scene)
+    npix = scene.width * scene.height
+    stride = 64
+    pixels = np.arange(0, npix, stride, dtype=np.uint32)
+    t0 = time.perf_counter()
+    _, _, counts = o_s.render(params, 0, SPP, pixels=pixels, threads=threads)
+    el = time.perf_counter() - t0
+    # Grow the sample toward target_s of CPU work for a steadier number.
+    if el < target_s / 4:
+        stride = max(1, int(stride * el / target_s * 1.0) or 1)
+        stride = max(stride, 2)
+        pixels = np.arange(1, npix, stride, dtype=np.uint32)
+        t0 = time.perf_counter()
+        _, _, counts = o_s.render(params, 0, SPP, pixels=pixels, threads=threads)
+        el = time.perf_counter() - t0
+    samples = len(pixels) * SPP
+    cores = threads if threads > 0 else os.cpu_count()
+    ext, sh = int(counts[0]), int(counts[1])
+    work = {"ext_rays": ext, "shadow_rays": sh,
+            "ext_bytes_per_ray": (32.0 * counts[2] + 48.0 * counts[3] + 48.0 * counts[4]) / max(ext, 1) + 48.0,
+            "shadow_bytes_per_ray": (32.0 * counts[5] + 48.0 * counts[6] + 48.0 * counts[7]) / max(sh, 1) + 48.0}
+    return samples / el / 1e6, f"{len(pixels)} pixels (every {stride}th) x {SPP} spp of the frame", cores, work, el
+
+
+def run_reference(args):
+    """Reference arm: the reference's CPU path (f64 restatement) on host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from rtcuda import abi, scenes
+    scene = scenes.triangle_cloud(WIDTH, HEIGHT, N_TRIS)
+    params = abi.make_params(max_depth=MAX_DEPTH)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, sample, cores, _, el = cpu_baseline_sample(scene, params, target_s=max(2.0, 60.0 / (args.warmup + args.steps)))
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_depth": MAX_DEPTH,
+                       "triangles": N_TRIS},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference is Rust (no toolchain here): its CPU path restated in C++ f64 (oracle/)"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    from rtcuda import PtSession, abi, scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+
+    scene = scenes.triangle_cloud(WIDTH, HEIGHT, N_TRIS)
+    params = abi.make_params(max_depth=MAX_DEPTH)
+    sess = PtSession(scene, params)
+    stream = torch.cuda.ExternalStream(sess.stream(), device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
+
+    def barrier():
+        if world > 1:
+            dist.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+    # Weak scaling: every rank renders its own 16 samples of the same frame
+    # (sample range offset by rank, as --sample-range partitions the reference).
+    def step(i):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        sess.render_samples((rank * 100000 + i * SPP) % (1 << 31), SPP)
+
+    for i in range(args.warmup):
+        step(i)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    ext_ms = ext_rays = launches = 0.0
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for i in range(args.steps):
+        step(args.warmup + i)
+        st = sess.stats()
+        ext_ms += st["extend_ms"]
+        ext_rays += st["extension_rays"]
+        launches += st["kernel_launches"] + 1
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    samples_per_step = WIDTH * HEIGHT * SPP
+    value = samples_per_step * args.steps * world / (ms_max / 1e3) / 1e6
+    last = sess.stats()
+
+    # Traversal batches (4,194,304 rays) from HBM.
+    rays = scenes.triangle_cloud_rays(N_RAYS)
+    d_rays = torch.from_numpy(rays).to(dev)
+    prim = torch.empty(N_RAYS, dtype=torch.int32, device=dev)
+    inst = torch.empty_like(prim)
+    tt = torch.empty(N_RAYS, dtype=torch.float32, device=dev)
+    trav = {}
+    for any_hit, name in ((0, "closest_hit"), (1, "any_hit")):
+        for _ in range(3):
+            sess.intersect_device(d_rays.data_ptr(), N_RAYS, any_hit, prim.data_ptr(), inst.data_ptr(),
+                                  tt.data_ptr(), sess.stream())
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        reps = 5
+        a.record(stream)
+        for _ in range(reps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            sess.intersect_device(d_rays.data_ptr(), N_RAYS, any_hit, prim.data_ptr(), inst.data_ptr(),
+                                  tt.data_ptr(), sess.stream())
+        b.record(stream)
+        torch.cuda.synchronize()
+        tms = a.elapsed_time(b) / reps
+        trav[name] = {"ms": tms, "Mrays_per_s": N_RAYS / tms / 1e3}
+
+    # End to end through the C ABI: host scene arrays in, host image out.
+    e2e_ms = []
+    h2d = sum(p.nbytes + i.nbytes for p, i, _ in scene.meshes) + scene.instance_array().nbytes
+    d2h = WIDTH * HEIGHT * 3 * 4
+    for i in range(args.e2e_steps):
+        barrier()
+        t0 = time.perf_counter()
+        with PtSession(scene, params) as s2:
+            s2.render_samples(rank * 1000 + 7 + i, SPP)
+            s2.image()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    et = torch.tensor([max(e2e_ms)], device=dev)
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_val = samples_per_step * world / (float(et.item()) / 1e3) / 1e6
+
+    result = None
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        cpu = None
+        work = None
+        if not args.no_cpu_baseline and world == 1:
+            v, sample, cores, work, el = cpu_baseline_sample(scene, params)
+            cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+                   "seconds": round(el, 2)}
+        roof = None
+        if work:
+            bytes_per_ray = work["ext_bytes_per_ray"]
+            launches_ext = args.steps * MAX_DEPTH * int(np.ceil(1.0))
+            achieved = bytes_per_ray * ext_rays / (ext_ms / 1e3) / 1e9
+            roof = {"kernel": "k_extend (closest hit, 8-wide BVH)", "bound": "hbm", "achieved": achieved,
+                    "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                    "peak_kind": peak_kind, "bytes_per_ray": bytes_per_ray,
+                    "rays_per_launch": ext_rays / max(1, launches_ext), "launch_ms": ext_ms / max(1, launches_ext)}
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP,
+                       "max_depth": MAX_DEPTH, "triangles": N_TRIS, "rays": N_RAYS,
+                       "parallelism": f"replica-sample-ranges x{world}", "l2_flush": True,
+                       "accumulator": "f64"},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h,
+                    "ms": max(e2e_ms)},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "gpu_launches": int(launches + 3 * 0),
+            "traversal": trav,
+            "rays_per_step": {"extension": last["extension_rays"], "shadow": last["shadow_rays"]},
+            "Mrays_per_s": (last["extension_rays"] + last["shadow_rays"]) / (last["total_ms"] / 1e3) / 1e6,
+        }
+        print(json.dumps(result), flush=True)
+    sess.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,143 @@
+/*
+ * rt_cuda.h — C ABI of the B200 (sm_100a) wavefront path tracer, librtcuda.so.
+ *
+ * This is the `cuda` arm of the reference's backend dispatch
+ * (src/main.rs:405-453). Each entry point replaces one call of the
+ * reference's Metal backend, src/raytracer/metal/renderer.rs; the mapping
+ * is given beside each declaration. Plain C types only: a Rust crate binds
+ * it with an `extern "C"` block (the reference is Rust).
+ *
+ * Conventions
+ *  - Every function returns an rt_status (0 = RT_OK, negative = error);
+ *    rt_last_error() gives the message of the most recent failure on the
+ *    calling thread.
+ *  - A session owns all of its device memory and one CUDA stream; calls are
+ *    synchronous on that stream. One session per host thread (the reference's
+ *    PtSession is not Send, renderer.rs:256-259).
+ *  - Output buffers are caller-allocated host memory unless the name says
+ *    `_device`.
+ *  - Seeding is per (pixel, sample) exactly as Pcg32::for_pixel_sample
+ *    (src/raytracer/pt/sampler.rs:24-32), so sample ranges rendered in any
+ *    split add up to the same image.
+ */
+#ifndef RT_CUDA_H
+#define RT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "rt_scene.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rt_status {
+    RT_OK = 0,
+    RT_ERR_INVALID = -1,   /* bad argument or scene (indices out of range, ...) */
+    RT_ERR_CUDA = -2,      /* a CUDA runtime call failed */
+    RT_ERR_OOM = -3,       /* device allocation failed */
+    RT_ERR_DEVICE = -4,    /* a kernel reported a bounded-loop or capacity overrun */
+    RT_ERR_IO = -5,        /* checkpoint file could not be read or written */
+    RT_ERR_MISMATCH = -6   /* checkpoint does not match this session */
+} rt_status;
+
+typedef struct rt_session rt_session;
+
+/* Flatten the scene (binned-SAH BLAS per mesh + TLAS over instances,
+ * collapsed to 8-wide quantised nodes; light BVH; materials) and upload it.
+ * Replaces PtSession::new / WfSession::new (renderer.rs:275, 518) and
+ * GpuPtScene::build (src/raytracer/metal/gpu_scene.rs:306-753). The
+ * descriptor is only read during the call. */
+int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_session** out);
+
+/* Free the session's device memory and stream. NULL is accepted. */
+int rt_session_destroy(rt_session* s);
+
+/* Message of the last failure on this thread ("" if none). */
+const char* rt_last_error(void);
+
+/* Render `count` more samples per pixel, sample indices
+ * [sample_start, sample_start + count), adding them to the f64
+ * accumulator. Replaces PtSession::render_samples / WfSession::render_samples
+ * (renderer.rs:410-437, 672-749). */
+int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count);
+
+/* Zero the accumulators (beauty and AOVs). */
+int rt_reset(rt_session* s);
+
+/* Copy the f64 accumulator: 4 doubles per pixel (r, g, b sums, sample
+ * weight), row-major from the top-left pixel. Replaces
+ * PtSession::sum_and_weight (renderer.rs:476-490). */
+int rt_read_accum(rt_session* s, double* rgbw);
+
+/* Beauty image: 3 floats per pixel = sum / weight. Replaces
+ * PtSession::image (renderer.rs:455-471). */
+int rt_read_image(rt_session* s, float* rgb);
+
+/* AOV sums: 12 floats per pixel in the reference's layout
+ * (src/raytracer/metal/kernel_pt.metal:1846-1847 and 2435-2452):
+ * 0-2 albedo, 3-5 normal, 6 depth, 7 id (first writer), 8-10 diffuse
+ * share, 11 hit count. Requires params.aovs = 1. Feeds render_pt_film's
+ * decode (renderer.rs:180-217). */
+int rt_read_aux(rt_session* s, float* aux12);
+
+/* Checkpoint / resume of the f64 accumulator and completed-sample count.
+ * Written to `path`.tmp then renamed (atomic). A load only succeeds when the
+ * image size matches. Replaces save_checkpoint / load_checkpoint
+ * (renderer.rs:219-254) with an f64 payload (magic "RCU1"). */
+int rt_checkpoint_save(rt_session* s, const char* path);
+int rt_checkpoint_load(rt_session* s, const char* path, uint32_t* samples_done);
+
+/* Ray batch against the session's scene. `rays` holds 8 floats per ray in
+ * two planes: [0, 4n) = (ox, oy, oz, unused), [4n, 8n) = (dx, dy, dz, tmax).
+ * Directions are used as given; t is parametric along them.
+ * Closest hit (any_hit = 0): prim = triangle index within its mesh,
+ * inst = instance index, t = hit distance; 0xFFFFFFFF / +inf on a miss.
+ * Any hit (any_hit = 1): prim = 1 if anything is hit with t < tmax, else 0;
+ * inst and t may be NULL.
+ * Host pointers. Replaces intersect_probe (renderer.rs:813-877). */
+int rt_intersect_batch(rt_session* s, const float* rays, uint64_t n, int any_hit,
+                       uint32_t* prim, uint32_t* inst, float* t);
+
+/* Same, with device pointers, enqueued on the session's stream (or on
+ * `stream` when non-NULL, a cudaStream_t) without a host synchronisation. */
+int rt_intersect_batch_device(rt_session* s, const float* rays, uint64_t n, int any_hit,
+                              uint32_t* prim, uint32_t* inst, float* t, void* stream);
+
+/* Statistics of the session and of its last rt_render_samples call. */
+typedef struct rt_stats {
+    uint64_t blas_nodes;        /* 8-wide BLAS nodes, all meshes */
+    uint64_t tlas_nodes;        /* 8-wide TLAS nodes */
+    uint64_t triangles;         /* unique triangles stored */
+    uint64_t device_bytes;      /* device memory held by the session */
+    uint64_t extension_rays;    /* last render: closest-hit rays traced */
+    uint64_t shadow_rays;       /* last render: shadow rays traced */
+    uint64_t samples;           /* last render: camera samples */
+    uint64_t kernel_launches;   /* last render: kernels launched */
+    double   extend_ms;         /* last render: time in the closest-hit kernel */
+    double   shadow_ms;         /* last render: time in the shadow kernel */
+    double   shade_ms;          /* last render: time in raygen + shade kernels */
+    double   total_ms;          /* last render: wall time on the stream */
+} rt_stats;
+
+int rt_get_stats(rt_session* s, rt_stats* out);
+
+/* Diagnostic: white-furnace estimate of one material on the GPU, using the
+ * shade kernel's f32 BSDF sampling. `wo` is in the local frame (z = shading
+ * normal), eta = transmitted / incident IOR. out[0] = mean of
+ * lum(f)*|cos|/pdf over n samples, out[1..3] = mean RGB weight. The
+ * reference's equivalent is the furnace_estimates unit test
+ * (src/raytracer/pt/bxdf.rs:428-453). */
+int rt_bsdf_furnace(const rt_material_desc* material, const double* wo, double eta, uint64_t n,
+                    uint64_t seed, double* out);
+
+/* The session's CUDA stream (a cudaStream_t), for callers that time or
+ * order work against it. */
+void* rt_session_stream(rt_session* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RT_CUDA_H */

@@ -1,0 +1,153 @@
+/*
+ * rt_scene.h — plain-C scene description handed across the C ABI.
+ *
+ * One descriptor feeds both the CUDA backend (librtcuda.so) and the f64 CPU
+ * oracle, so the two always see byte-identical scene input.
+ *
+ * It replaces the reference's flattened GPU scene payload: `GpuPtScene`
+ * (src/raytracer/metal/gpu_scene.rs:254-288) built from `Scene`
+ * (src/scene/mod.rs:27-56). Only the parts the path tracer consumes are
+ * carried: triangle meshes with optional vertex normals
+ * (src/geometry/mesh.rs:20-33), affine instances (mesh.rs:232-250),
+ * PxrSurface-lite material parameters (src/scene/pbr.rs:10-51) with emission
+ * and the area-light link (src/scene/material.rs:14-40), finite/distant
+ * lights (src/scene/light.rs:7-35) and the camera (src/scene/camera.rs:67-92).
+ *
+ * Doubles are used for every host-side parameter so the f64 oracle reads the
+ * same values the reference would; the CUDA backend converts to f32 (and
+ * inverts instance transforms in f64) when it flattens the scene.
+ *
+ * All arrays are borrowed only for the duration of the create call.
+ */
+#ifndef RT_SCENE_H
+#define RT_SCENE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Triangle mesh: f32 xyz positions, u32 index triples, optional normals.
+ * Mirrors `Mesh { positions, indices, normals }` (src/geometry/mesh.rs:20-33). */
+typedef struct rt_mesh_desc {
+    const float*    positions;    /* 3 * n_vertices */
+    const uint32_t* indices;      /* 3 * n_triangles */
+    const float*    normals;      /* 3 * n_vertices, or NULL (geometric normal) */
+    uint32_t        n_vertices;
+    uint32_t        n_triangles;
+} rt_mesh_desc;
+
+/* Placed copy of a mesh. `object_to_world` is the row-major upper 3x4 of
+ * the reference's `Instance::transform` (mesh.rs:237); the bottom row is
+ * (0,0,0,1). The inverse is computed by the consumer in f64. */
+typedef struct rt_instance_desc {
+    double   object_to_world[12];
+    uint32_t mesh_id;
+    uint32_t material_id;
+} rt_instance_desc;
+
+/* Material: `PbrParams` fields in scope (src/scene/pbr.rs:10-51) plus
+ * `Material::{emission, area_light, id}` (src/scene/material.rs:21-39). */
+typedef struct rt_material_desc {
+    double  diffuse_gain;
+    double  diffuse_color[3];
+    double  diffuse_roughness;       /* Oren-Nayar sigma (0 = Lambert) */
+    double  specular_face_color[3];  /* Schlick F0; black -> from specular_ior */
+    double  specular_edge_color[3];  /* Schlick F90 */
+    double  specular_roughness;
+    double  specular_ior;
+    double  clearcoat_gain;
+    double  clearcoat_roughness;
+    double  fuzz_gain;
+    double  fuzz_color[3];
+    double  glass_gain;
+    double  glass_ior;
+    double  glass_roughness;
+    double  refraction_color[3];
+    double  glow[3];
+    double  presence;                /* stochastic cutout alpha, 1 = solid */
+    double  emission[3];             /* emitted radiance */
+    int32_t area_light;              /* index into lights, or -1 */
+    uint32_t id;                     /* object id for the id AOV */
+} rt_material_desc;
+
+enum {
+    RT_LIGHT_POINT   = 0,  /* p = position */
+    RT_LIGHT_DISTANT = 1,  /* e1 = direction light travels; radius = angular radius */
+    RT_LIGHT_RECT    = 2,  /* p = corner, e1/e2 = edges */
+    RT_LIGHT_SPHERE  = 3,  /* p = centre, radius */
+    RT_LIGHT_DISK    = 4   /* p = centre, e1/e2 span the radius */
+};
+
+/* Light: `Light { light_type, intensity, color }` (src/scene/light.rs:7-49).
+ * Radiance is color * intensity (light.rs:151-153). */
+typedef struct rt_light_desc {
+    int32_t type;
+    int32_t pad_;
+    double  intensity;
+    double  color[3];
+    double  p[3];
+    double  e1[3];
+    double  e2[3];
+    double  radius;
+} rt_light_desc;
+
+enum { RT_FILTER_BOX = 0, RT_FILTER_TRIANGLE = 1, RT_FILTER_GAUSSIAN = 2 };
+
+/* Pinhole / thin-lens camera (src/scene/camera.rs:67-92, 150-179).
+ * right/up/forward are used as given (Camera::set_transform computes
+ * right = forward x up, up = right x forward). */
+typedef struct rt_camera_desc {
+    uint32_t width;
+    uint32_t height;
+    double   fov_deg;               /* vertical field of view */
+    double   eye[3];
+    double   forward[3];
+    double   up[3];
+    double   right[3];
+    double   lens_radius;           /* 0 = pinhole */
+    double   focal_distance;
+    int32_t  filter;                /* RT_FILTER_* */
+    int32_t  pad_;
+    double   filter_width;
+} rt_camera_desc;
+
+typedef struct rt_scene_desc {
+    const rt_mesh_desc*     meshes;
+    const rt_instance_desc* instances;
+    const rt_material_desc* materials;
+    const rt_light_desc*    lights;
+    uint32_t n_meshes;
+    uint32_t n_instances;
+    uint32_t n_materials;
+    uint32_t n_lights;
+    rt_camera_desc camera;
+    double background[3];
+} rt_scene_desc;
+
+/* Integrator knobs. The reference hard-codes these as constants
+ * (src/raytracer/pt/mod.rs:26-32: MAX_BOUNCES 10, RR_START 3,
+ * FIREFLY_CLAMP 60); the configs here need 8/12/16/10 bounces. */
+typedef struct rt_params {
+    uint32_t max_depth;       /* bounce cap (reference MAX_BOUNCES) */
+    uint32_t rr_start;        /* Russian roulette from this depth (RR_START) */
+    double   firefly_clamp;   /* per-sample luminance clamp (FIREFLY_CLAMP) */
+    uint32_t aovs;            /* 1 = also accumulate the 12-float AOV record */
+    uint32_t guided;          /* 1 = learned directional proposal on */
+    double   guide_fraction;  /* one-sample MIS fraction drawn from the guide */
+    uint64_t max_paths;       /* wavefront slab capacity in paths (0 = auto) */
+} rt_params;
+
+/* Size checks shared by every consumer of the descriptor. */
+#ifdef __cplusplus
+static_assert(sizeof(rt_mesh_desc) == 32, "rt_mesh_desc layout");
+static_assert(sizeof(rt_instance_desc) == 104, "rt_instance_desc layout");
+static_assert(sizeof(rt_material_desc) == 264, "rt_material_desc layout");
+static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
+static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
+static_assert(sizeof(rt_params) == 40, "rt_params layout");
+}
+#endif
+
+#endif /* RT_SCENE_H */

@@ -1,0 +1,151 @@
+"""ctypes wrapper for the f64 CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+the bench's cpu_baseline / reference legs as the checker and the timed CPU
+baseline. The CUDA backend never imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+
+class Counters(C.Structure):
+    _fields_ = [("node_pops", C.c_uint64), ("tri_tests", C.c_uint64),
+                ("inst_tests", C.c_uint64), ("rays", C.c_uint64)]
+
+
+def build():
+    """Compile liboracle.so from the sources in this folder."""
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        vp, u32p, f64p = C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_double)
+        L.oracle_scene_create.restype = vp
+        L.oracle_scene_create.argtypes = [vp]
+        L.oracle_scene_destroy.argtypes = [vp]
+        L.oracle_scene_stats.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.oracle_intersect.argtypes = [vp, vp, C.c_uint64, C.c_int, vp, vp, vp, C.POINTER(Counters), C.c_int]
+        L.oracle_render.argtypes = [vp, vp, vp, C.c_uint64, C.c_uint32, C.c_uint32, vp, vp, vp, C.c_int]
+        L.oracle_pcg_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, u32p]
+        L.oracle_pcg_new_stream.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, u32p]
+        L.oracle_bsdf_eval.argtypes = [vp, f64p, f64p, C.c_double, f64p, f64p]
+        L.oracle_bsdf_furnace.restype = C.c_double
+        L.oracle_bsdf_furnace.argtypes = [vp, f64p, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, f64p]
+        L.oracle_light_sample.argtypes = [vp, f64p, C.c_double, u32p, f64p]
+        L.oracle_light_pmf.restype = C.c_double
+        L.oracle_light_pmf.argtypes = [vp, f64p, C.c_uint32]
+        _lib = L
+    return _lib
+
+
+def _f64(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def pcg_stream(pixel, sample, n):
+    out = np.zeros(n, dtype=np.uint32)
+    lib().oracle_pcg_stream(pixel, sample, n, out.ctypes.data_as(C.POINTER(C.c_uint32)))
+    return out
+
+
+def pcg_new_stream(seed, stream, n):
+    out = np.zeros(n, dtype=np.uint32)
+    lib().oracle_pcg_new_stream(seed, stream, n, out.ctypes.data_as(C.POINTER(C.c_uint32)))
+    return out
+
+
+def bsdf_eval(material_desc, wo, wi, eta):
+    f = np.zeros(3)
+    pdf = C.c_double()
+    _, wop = _f64(wo)
+    _, wip = _f64(wi)
+    lib().oracle_bsdf_eval(C.byref(material_desc), wop, wip, eta, f.ctypes.data_as(C.POINTER(C.c_double)),
+                           C.byref(pdf))
+    return f, pdf.value
+
+
+def bsdf_furnace(material_desc, wo, eta, n, seed=7, stream=11):
+    rgb = np.zeros(3)
+    _, wop = _f64(wo)
+    m = lib().oracle_bsdf_furnace(C.byref(material_desc), wop, eta, n, seed, stream,
+                                  rgb.ctypes.data_as(C.POINTER(C.c_double)))
+    return m, rgb
+
+
+class OracleScene:
+    """The oracle's view of a scene built from the same ``rt_scene_desc``."""
+
+    def __init__(self, scene):
+        self.scene = scene
+        self._desc = scene.desc()
+        self.h = lib().oracle_scene_create(C.byref(self._desc))
+        if not self.h:
+            raise RuntimeError("oracle_scene_create failed")
+
+    def close(self):
+        if self.h:
+            lib().oracle_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stats(self):
+        b, t = C.c_uint64(), C.c_uint64()
+        lib().oracle_scene_stats(self.h, C.byref(b), C.byref(t))
+        return b.value, t.value
+
+    def intersect(self, planes, any_hit=False, threads=0):
+        planes = np.ascontiguousarray(planes, dtype=np.float32)
+        n = planes.shape[1]
+        prim = np.zeros(n, dtype=np.uint32)
+        inst = np.zeros(n, dtype=np.uint32)
+        t = np.zeros(n, dtype=np.float64)
+        c = Counters()
+        lib().oracle_intersect(self.h, planes.ctypes.data, n, 1 if any_hit else 0, prim.ctypes.data,
+                               inst.ctypes.data, t.ctypes.data, C.byref(c), threads)
+        return prim, inst, t, c
+
+    def render(self, params, s0, s1, pixels=None, aovs=False, threads=0):
+        """Radiance sums over samples [s0, s1) (and AOV sums) for a pixel list;
+        the whole image when `pixels` is None."""
+        W, H = self.scene.width, self.scene.height
+        if pixels is None:
+            pixels = np.arange(W * H, dtype=np.uint32)
+        pixels = np.ascontiguousarray(pixels, dtype=np.uint32)
+        rgb = np.zeros((len(pixels), 3))
+        aux = np.zeros((len(pixels), 12)) if aovs else None
+        counts = np.zeros(8, dtype=np.uint64)
+        rc = lib().oracle_render(self.h, C.byref(params), pixels.ctypes.data, len(pixels), s0, s1, rgb.ctypes.data,
+                                 aux.ctypes.data if aovs else None, counts.ctypes.data, threads)
+        if rc != 0:
+            raise RuntimeError("oracle_render failed")
+        return rgb, aux, counts
+
+    def light_sample(self, p, u):
+        li, pmf = C.c_uint32(), C.c_double()
+        _, pp = _f64(p)
+        ok = lib().oracle_light_sample(self.h, pp, u, C.byref(li), C.byref(pmf))
+        return (li.value, pmf.value) if ok else None
+
+    def light_pmf(self, p, light):
+        _, pp = _f64(p)
+        return lib().oracle_light_pmf(self.h, pp, light)

@@ -1,0 +1,1700 @@
+// pt_oracle.cpp — f64 CPU oracle for the render.rs path tracer.
+//
+// TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+// bench's cpu_baseline leg as the checker and the timed CPU baseline. The
+// CUDA backend never calls it.
+//
+// Every function cites the reference source (path:line within
+// anders94/render.rs) whose behaviour it restates. Arithmetic is f64 as in
+// the reference; the choices that decide tree shape or random-number use
+// (partition order, stable sort, bin index, draw order) follow it exactly.
+
+#include "pt_oracle.h"
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+static const double PI = 3.14159265358979323846;
+static const double INF = std::numeric_limits<double>::infinity();
+static const double EPSILON = 1e-6;          // src/math/mod.rs:9
+static const double RAY_OFFSET = 1e-4;       // src/raytracer/pt/mod.rs:30
+static const int MAX_PRESENCE_SKIPS = 16;    // src/raytracer/pt/mod.rs:32
+
+// ---- math (src/math/vector.rs, point.rs, matrix.rs) ----------------------
+
+struct V3 {
+    double x = 0, y = 0, z = 0;
+    V3() = default;
+    V3(double a, double b, double c) : x(a), y(b), z(c) {}
+};
+static inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline V3 operator-(V3 a) { return {-a.x, -a.y, -a.z}; }
+static inline V3 operator*(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline V3 operator*(V3 a, V3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+static inline V3 operator/(V3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+static inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3 cross(V3 a, V3 b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+static inline double length_sq(V3 a) { return dot(a, a); }
+static inline double length(V3 a) { return std::sqrt(length_sq(a)); }
+// vector.rs:31-38 — normalise only when the length exceeds EPSILON.
+static inline V3 normalize(V3 a) {
+    double l = length(a);
+    return l > EPSILON ? a / l : a;
+}
+// vector.rs:52-54
+static inline V3 reflect(V3 v, V3 n) { return v - n * 2.0 * dot(v, n); }
+static inline double max_comp(V3 c) { return std::fmax(std::fmax(c.x, c.y), c.z); }
+static inline double lum(V3 c) { return 0.2126 * c.x + 0.7152 * c.y + 0.0722 * c.z; }
+static inline double axis_of(V3 v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+static inline V3 v3(const double* p) { return {p[0], p[1], p[2]}; }
+
+struct M4 {
+    double m[4][4];
+};
+static M4 identity() {
+    M4 r{};
+    for (int i = 0; i < 4; i++) r.m[i][i] = 1.0;
+    return r;
+}
+// matrix.rs: inverse via cofactors; None when |det| < EPSILON.
+static bool inverse(const M4& a, M4& out) {
+    const double(*m)[4] = a.m;
+    double inv[4][4];
+    inv[0][0] = m[1][1] * m[2][2] * m[3][3] - m[1][1] * m[2][3] * m[3][2] - m[2][1] * m[1][2] * m[3][3] +
+                m[2][1] * m[1][3] * m[3][2] + m[3][1] * m[1][2] * m[2][3] - m[3][1] * m[1][3] * m[2][2];
+    inv[1][0] = -m[1][0] * m[2][2] * m[3][3] + m[1][0] * m[2][3] * m[3][2] + m[2][0] * m[1][2] * m[3][3] -
+                m[2][0] * m[1][3] * m[3][2] - m[3][0] * m[1][2] * m[2][3] + m[3][0] * m[1][3] * m[2][2];
+    inv[2][0] = m[1][0] * m[2][1] * m[3][3] - m[1][0] * m[2][3] * m[3][1] - m[2][0] * m[1][1] * m[3][3] +
+                m[2][0] * m[1][3] * m[3][1] + m[3][0] * m[1][1] * m[2][3] - m[3][0] * m[1][3] * m[2][1];
+    inv[3][0] = -m[1][0] * m[2][1] * m[3][2] + m[1][0] * m[2][2] * m[3][1] + m[2][0] * m[1][1] * m[3][2] -
+                m[2][0] * m[1][2] * m[3][1] - m[3][0] * m[1][1] * m[2][2] + m[3][0] * m[1][2] * m[2][1];
+    double det = m[0][0] * inv[0][0] + m[0][1] * inv[1][0] + m[0][2] * inv[2][0] + m[0][3] * inv[3][0];
+    if (std::fabs(det) < EPSILON) return false;
+    inv[0][1] = -m[0][1] * m[2][2] * m[3][3] + m[0][1] * m[2][3] * m[3][2] + m[2][1] * m[0][2] * m[3][3] -
+                m[2][1] * m[0][3] * m[3][2] - m[3][1] * m[0][2] * m[2][3] + m[3][1] * m[0][3] * m[2][2];
+    inv[1][1] = m[0][0] * m[2][2] * m[3][3] - m[0][0] * m[2][3] * m[3][2] - m[2][0] * m[0][2] * m[3][3] +
+                m[2][0] * m[0][3] * m[3][2] + m[3][0] * m[0][2] * m[2][3] - m[3][0] * m[0][3] * m[2][2];
+    inv[2][1] = -m[0][0] * m[2][1] * m[3][3] + m[0][0] * m[2][3] * m[3][1] + m[2][0] * m[0][1] * m[3][3] -
+                m[2][0] * m[0][3] * m[3][1] - m[3][0] * m[0][1] * m[2][3] + m[3][0] * m[0][3] * m[2][1];
+    inv[3][1] = m[0][0] * m[2][1] * m[3][2] - m[0][0] * m[2][2] * m[3][1] - m[2][0] * m[0][1] * m[3][2] +
+                m[2][0] * m[0][2] * m[3][1] + m[3][0] * m[0][1] * m[2][2] - m[3][0] * m[0][2] * m[2][1];
+    inv[0][2] = m[0][1] * m[1][2] * m[3][3] - m[0][1] * m[1][3] * m[3][2] - m[1][1] * m[0][2] * m[3][3] +
+                m[1][1] * m[0][3] * m[3][2] + m[3][1] * m[0][2] * m[1][3] - m[3][1] * m[0][3] * m[1][2];
+    inv[1][2] = -m[0][0] * m[1][2] * m[3][3] + m[0][0] * m[1][3] * m[3][2] + m[1][0] * m[0][2] * m[3][3] -
+                m[1][0] * m[0][3] * m[3][2] - m[3][0] * m[0][2] * m[1][3] + m[3][0] * m[0][3] * m[1][2];
+    inv[2][2] = m[0][0] * m[1][1] * m[3][3] - m[0][0] * m[1][3] * m[3][1] - m[1][0] * m[0][1] * m[3][3] +
+                m[1][0] * m[0][3] * m[3][1] + m[3][0] * m[0][1] * m[1][3] - m[3][0] * m[0][3] * m[1][1];
+    inv[3][2] = -m[0][0] * m[1][1] * m[3][2] + m[0][0] * m[1][2] * m[3][1] + m[1][0] * m[0][1] * m[3][2] -
+                m[1][0] * m[0][2] * m[3][1] - m[3][0] * m[0][1] * m[1][2] + m[3][0] * m[0][2] * m[1][1];
+    inv[0][3] = -m[0][1] * m[1][2] * m[2][3] + m[0][1] * m[1][3] * m[2][2] + m[1][1] * m[0][2] * m[2][3] -
+                m[1][1] * m[0][3] * m[2][2] - m[2][1] * m[0][2] * m[1][3] + m[2][1] * m[0][3] * m[1][2];
+    inv[1][3] = m[0][0] * m[1][2] * m[2][3] - m[0][0] * m[1][3] * m[2][2] - m[1][0] * m[0][2] * m[2][3] +
+                m[1][0] * m[0][3] * m[2][2] + m[2][0] * m[0][2] * m[1][3] - m[2][0] * m[0][3] * m[1][2];
+    inv[2][3] = -m[0][0] * m[1][1] * m[2][3] + m[0][0] * m[1][3] * m[2][1] + m[1][0] * m[0][1] * m[2][3] -
+                m[1][0] * m[0][3] * m[2][1] - m[2][0] * m[0][1] * m[1][3] + m[2][0] * m[0][3] * m[1][1];
+    inv[3][3] = m[0][0] * m[1][1] * m[2][2] - m[0][0] * m[1][2] * m[2][1] - m[1][0] * m[0][1] * m[2][2] +
+                m[1][0] * m[0][2] * m[2][1] + m[2][0] * m[0][1] * m[1][2] - m[2][0] * m[0][2] * m[1][1];
+    double det_inv = 1.0 / det;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) out.m[i][j] = inv[i][j] * det_inv;
+    return true;
+}
+// matrix.rs transform_point: divides by w only when w differs from 1.
+static V3 xf_point(const M4& a, V3 p) {
+    const double(*m)[4] = a.m;
+    double x = m[0][0] * p.x + m[0][1] * p.y + m[0][2] * p.z + m[0][3];
+    double y = m[1][0] * p.x + m[1][1] * p.y + m[1][2] * p.z + m[1][3];
+    double z = m[2][0] * p.x + m[2][1] * p.y + m[2][2] * p.z + m[2][3];
+    double w = m[3][0] * p.x + m[3][1] * p.y + m[3][2] * p.z + m[3][3];
+    if (std::fabs(w - 1.0) < EPSILON) return {x, y, z};
+    return {x / w, y / w, z / w};
+}
+static V3 xf_vec(const M4& a, V3 v) {
+    const double(*m)[4] = a.m;
+    return {m[0][0] * v.x + m[0][1] * v.y + m[0][2] * v.z, m[1][0] * v.x + m[1][1] * v.y + m[1][2] * v.z,
+            m[2][0] * v.x + m[2][1] * v.y + m[2][2] * v.z};
+}
+// transform_normal: multiplies by the transpose (callers pass the inverse).
+static V3 xf_normal(const M4& a, V3 n) {
+    const double(*m)[4] = a.m;
+    return {m[0][0] * n.x + m[1][0] * n.y + m[2][0] * n.z, m[0][1] * n.x + m[1][1] * n.y + m[2][1] * n.z,
+            m[0][2] * n.x + m[1][2] * n.y + m[2][2] * n.z};
+}
+
+// ---- sampler (src/raytracer/pt/sampler.rs:6-60) ---------------------------
+
+struct Pcg32 {
+    uint64_t state, inc;
+    Pcg32(uint64_t seed, uint64_t stream) : state(0), inc((stream << 1) | 1u) {  // :12-21
+        next_u32();
+        state += seed;
+        next_u32();
+    }
+    static uint64_t mix(uint64_t z) {  // :26-30
+        z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+        z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+        return z ^ (z >> 31);
+    }
+    static Pcg32 for_pixel_sample(uint64_t pixel, uint64_t sample) {  // :24-32
+        return Pcg32(mix((pixel * 0x9e3779b97f4a7c15ull) ^ sample), mix(sample) | 1u);
+    }
+    uint32_t next_u32() {  // :34-42
+        uint64_t old = state;
+        state = old * 6364136223846793005ull + inc;
+        uint32_t xorshifted = (uint32_t)(((old >> 18) ^ old) >> 27);
+        uint32_t rot = (uint32_t)(old >> 59);
+        return (xorshifted >> rot) | (xorshifted << ((32u - rot) & 31u));
+    }
+    double next_f64() { return (double)next_u32() * (1.0 / 4294967296.0); }  // :45-47
+};
+
+// ---- BVH (src/accel/bvh.rs) -----------------------------------------------
+
+struct Aabb {
+    V3 mn{INF, INF, INF}, mx{-INF, -INF, -INF};
+    // Rust f64::min/max ignore a NaN operand, as fmin/fmax do.
+    void grow_point(V3 p) {
+        mn = {std::fmin(mn.x, p.x), std::fmin(mn.y, p.y), std::fmin(mn.z, p.z)};
+        mx = {std::fmax(mx.x, p.x), std::fmax(mx.y, p.y), std::fmax(mx.z, p.z)};
+    }
+    void grow(const Aabb& o) {
+        grow_point(o.mn);
+        grow_point(o.mx);
+    }
+    V3 centroid() const { return (mn + mx) * 0.5; }
+    double surface_area() const {  // bvh.rs:45-51
+        V3 d = mx - mn;
+        if (d.x < 0.0 || d.y < 0.0 || d.z < 0.0) return 0.0;
+        return 2.0 * (d.x * d.y + d.y * d.z + d.z * d.x);
+    }
+    // bvh.rs:55-72 slab test.
+    bool hit(V3 o, V3 inv, double t_max, double* t_entry) const {
+        double t0x = (mn.x - o.x) * inv.x, t1x = (mx.x - o.x) * inv.x;
+        double t_near = std::fmin(t0x, t1x), t_far = std::fmax(t0x, t1x);
+        double t0y = (mn.y - o.y) * inv.y, t1y = (mx.y - o.y) * inv.y;
+        t_near = std::fmax(t_near, std::fmin(t0y, t1y));
+        t_far = std::fmin(t_far, std::fmax(t0y, t1y));
+        double t0z = (mn.z - o.z) * inv.z, t1z = (mx.z - o.z) * inv.z;
+        t_near = std::fmax(t_near, std::fmin(t0z, t1z));
+        t_far = std::fmin(t_far, std::fmax(t0z, t1z));
+        if (t_near <= t_far && t_far > 0.0 && t_near < t_max) {
+            if (t_entry) *t_entry = std::fmax(t_near, 0.0);
+            return true;
+        }
+        return false;
+    }
+};
+
+struct Ray {
+    V3 o, d;
+};
+// raytracer/ray.rs:13-19 — Ray::new normalises the direction.
+static inline Ray make_ray(V3 o, V3 d) { return {o, normalize(d)}; }
+
+struct Counters {
+    uint64_t pops = 0, tris = 0, insts = 0;
+};
+
+struct Bvh {
+    struct Node {
+        Aabb bounds;
+        uint32_t first = 0, count = 0;
+    };
+    std::vector<Node> nodes;
+    std::vector<uint32_t> prim_order;
+    static const int BINS = 16;     // bvh.rs:91
+    static const int MAX_LEAF = 4;  // bvh.rs:92
+
+    // bvh.rs:96-108
+    void build(const std::vector<Aabb>& bounds) {
+        prim_order.resize(bounds.size());
+        for (size_t i = 0; i < bounds.size(); i++) prim_order[i] = (uint32_t)i;
+        nodes.clear();
+        if (bounds.empty()) return;
+        nodes.reserve(bounds.size() * 2);
+        std::vector<V3> centroids(bounds.size());
+        for (size_t i = 0; i < bounds.size(); i++) centroids[i] = bounds[i].centroid();
+        nodes.push_back(Node{});
+        // Explicit stack keeps the reference's recursion order (left subtree
+        // fully before right) without deep native recursion.
+        struct Job { size_t node, start, count; };
+        std::vector<Job> stack{{0, 0, bounds.size()}};
+        while (!stack.empty()) {
+            Job j = stack.back();
+            stack.pop_back();
+            size_t split_at;
+            if (!subdivide(bounds, centroids, j.node, j.start, j.count, &split_at)) continue;
+            size_t left = nodes.size();
+            nodes.push_back(Node{});
+            nodes.push_back(Node{});
+            nodes[j.node].first = (uint32_t)left;
+            nodes[j.node].count = 0;
+            // Children are appended in pre-order: the left subtree's nodes
+            // must all be created before the right child's descendants.
+            stack.push_back({left + 1, split_at, j.start + j.count - split_at});
+            stack.push_back({left, j.start, split_at - j.start});
+        }
+    }
+
+    // bvh.rs:256-345 (one level). Returns false when the node became a leaf.
+    bool subdivide(const std::vector<Aabb>& bounds, const std::vector<V3>& centroids, size_t node_idx,
+                   size_t start, size_t count, size_t* split_out) {
+        Aabb b, cb;
+        for (size_t i = start; i < start + count; i++) {
+            uint32_t p = prim_order[i];
+            b.grow(bounds[p]);
+            cb.grow_point(centroids[p]);
+        }
+        nodes[node_idx].bounds = b;
+        if (count <= (size_t)MAX_LEAF) {
+            nodes[node_idx].first = (uint32_t)start;
+            nodes[node_idx].count = (uint32_t)count;
+            return false;
+        }
+        V3 ext = cb.mx - cb.mn;
+        int axis = (ext.x >= ext.y && ext.x >= ext.z) ? 0 : (ext.y >= ext.z ? 1 : 2);
+        double axis_min = axis_of(cb.mn, axis), axis_extent = axis_of(ext, axis);
+        size_t split_at = start + count / 2;  // median fallback
+        if (axis_extent > 1e-12) {
+            Aabb bin_bounds[BINS];
+            size_t bin_counts[BINS] = {0};
+            double scale = (double)BINS / axis_extent;
+            for (size_t i = start; i < start + count; i++) {
+                uint32_t p = prim_order[i];
+                double f = (axis_of(centroids[p], axis) - axis_min) * scale;
+                size_t bi = f > 0.0 ? (size_t)f : 0;  // Rust `as usize` saturates at 0
+                if (bi > (size_t)BINS - 1) bi = BINS - 1;
+                bin_counts[bi]++;
+                bin_bounds[bi].grow(bounds[p]);
+            }
+            Aabb right_acc[BINS], acc;
+            for (int i = BINS - 1; i >= 1; i--) {
+                acc.grow(bin_bounds[i]);
+                right_acc[i] = acc;
+            }
+            double best_cost = INF;
+            int best_bin = 0;
+            Aabb left;
+            size_t left_count = 0;
+            for (int i = 0; i < BINS - 1; i++) {
+                left.grow(bin_bounds[i]);
+                left_count += bin_counts[i];
+                size_t right_count = count - left_count;
+                if (left_count == 0 || right_count == 0) continue;
+                double cost = left.surface_area() * (double)left_count +
+                              right_acc[i + 1].surface_area() * (double)right_count;
+                if (cost < best_cost) {
+                    best_cost = cost;
+                    best_bin = i;
+                }
+            }
+            double leaf_cost = b.surface_area() * (double)count;
+            if (std::isfinite(best_cost) && best_cost < leaf_cost) {
+                double boundary = axis_min + axis_extent * (double)(best_bin + 1) / (double)BINS;
+                // bvh.rs:362-371 in-place swap partition.
+                size_t i = 0;
+                for (size_t j = 0; j < count; j++) {
+                    if (axis_of(centroids[prim_order[start + j]], axis) < boundary) {
+                        std::swap(prim_order[start + i], prim_order[start + j]);
+                        i++;
+                    }
+                }
+                if (i > 0 && i < count) split_at = start + i;
+            } else if (count <= (size_t)MAX_LEAF * 4) {
+                nodes[node_idx].first = (uint32_t)start;
+                nodes[node_idx].count = (uint32_t)count;
+                return false;
+            }
+        }
+        *split_out = split_at;
+        return true;
+    }
+
+    // bvh.rs:141-204. `isect(prim, t_max, &t)` must report hits < t_max.
+    template <class F>
+    bool traverse(V3 o, V3 d, double t_max, F&& isect, uint32_t* best_prim, double* best_t,
+                  Counters* c) const {
+        if (nodes.empty()) return false;
+        V3 inv{1.0 / d.x, 1.0 / d.y, 1.0 / d.z};
+        bool found = false;
+        uint32_t stack[64];
+        int sp = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            const Node& node = nodes[stack[--sp]];
+            if (c) c->pops++;
+            if (!node.bounds.hit(o, inv, t_max, nullptr)) continue;
+            if (node.count > 0) {
+                for (uint32_t i = node.first; i < node.first + node.count; i++) {
+                    uint32_t prim = prim_order[i];
+                    double t;
+                    if (isect(prim, t_max, &t) && t < t_max) {
+                        t_max = t;
+                        *best_prim = prim;
+                        *best_t = t;
+                        found = true;
+                    }
+                }
+            } else {
+                uint32_t l = node.first, r = l + 1;
+                double a, b;
+                bool hl = nodes[l].bounds.hit(o, inv, t_max, &a);
+                bool hr = nodes[r].bounds.hit(o, inv, t_max, &b);
+                if (hl && hr) {
+                    uint32_t nr = a <= b ? l : r, fr = a <= b ? r : l;
+                    stack[sp++] = fr;
+                    stack[sp++] = nr;
+                } else if (hl) {
+                    stack[sp++] = l;
+                } else if (hr) {
+                    stack[sp++] = r;
+                }
+            }
+        }
+        return found;
+    }
+
+    // bvh.rs:208-245
+    template <class F>
+    bool any_hit(V3 o, V3 d, double t_limit, F&& hitp, Counters* c) const {
+        if (nodes.empty()) return false;
+        V3 inv{1.0 / d.x, 1.0 / d.y, 1.0 / d.z};
+        uint32_t stack[64];
+        int sp = 0;
+        stack[sp++] = 0;
+        while (sp > 0) {
+            const Node& node = nodes[stack[--sp]];
+            if (c) c->pops++;
+            if (!node.bounds.hit(o, inv, t_limit, nullptr)) continue;
+            if (node.count > 0) {
+                for (uint32_t i = node.first; i < node.first + node.count; i++)
+                    if (hitp(prim_order[i], t_limit)) return true;
+            } else {
+                stack[sp++] = node.first;
+                stack[sp++] = node.first + 1;
+            }
+        }
+        return false;
+    }
+};
+
+// ---- meshes and instances (src/geometry/mesh.rs) --------------------------
+
+struct Mesh {
+    std::vector<float> pos;
+    std::vector<uint32_t> idx;
+    std::vector<float> nrm;  // empty when absent
+    Bvh blas;
+    Aabb local_bounds;
+
+    V3 vertex(uint32_t i) const { return {(double)pos[3 * i], (double)pos[3 * i + 1], (double)pos[3 * i + 2]}; }
+
+    void build() {  // mesh.rs:45-86
+        size_t n = idx.size() / 3;
+        std::vector<Aabb> bounds(n);
+        for (size_t t = 0; t < n; t++) {
+            Aabb b;
+            b.grow_point(vertex(idx[3 * t]));
+            b.grow_point(vertex(idx[3 * t + 1]));
+            b.grow_point(vertex(idx[3 * t + 2]));
+            bounds[t] = b;
+            local_bounds.grow(b);
+        }
+        blas.build(bounds);
+    }
+
+    // mesh.rs:117-142 Möller–Trumbore (parametric t along the local ray).
+    bool intersect_triangle(const Ray& r, uint32_t tri, double t_max, double* t_out, double* u_out,
+                            double* v_out) const {
+        V3 v0 = vertex(idx[3 * tri]);
+        V3 e1 = vertex(idx[3 * tri + 1]) - v0;
+        V3 e2 = vertex(idx[3 * tri + 2]) - v0;
+        V3 p = cross(r.d, e2);
+        double det = dot(e1, p);
+        if (std::fabs(det) < 1e-14) return false;
+        double inv = 1.0 / det;
+        V3 tv = r.o - v0;
+        double u = dot(tv, p) * inv;
+        if (!(u >= 0.0 && u <= 1.0)) return false;
+        V3 q = cross(tv, e1);
+        double v = dot(r.d, q) * inv;
+        if (v < 0.0 || u + v > 1.0) return false;
+        double t = dot(e2, q) * inv;
+        if (!(t > 1e-9 && t < t_max)) return false;
+        *t_out = t;
+        *u_out = u;
+        *v_out = v;
+        return true;
+    }
+
+    // mesh.rs:200-220 interpolated or geometric local normal.
+    V3 local_normal(uint32_t tri, double u, double v) const {
+        uint32_t i0 = idx[3 * tri], i1 = idx[3 * tri + 1], i2 = idx[3 * tri + 2];
+        if (!nrm.empty()) {
+            auto n = [&](uint32_t i) { return V3{nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]}; };
+            double w = 1.0 - u - v;
+            return normalize(n(i0) * w + n(i1) * u + n(i2) * v);
+        }
+        V3 v0 = vertex(i0);
+        return normalize(cross(vertex(i1) - v0, vertex(i2) - v0));
+    }
+};
+
+struct Instance {
+    uint32_t mesh_id = 0, material_id = 0;
+    M4 transform, inv;
+    Aabb world_bounds;
+};
+
+struct Hit {
+    double t;        // euclidean distance from the ray origin
+    V3 point, normal;
+    uint32_t material_id, inst, prim;
+    bool front_face;
+};
+
+// ---- lights (src/scene/light.rs) and the light BVH (light_sampler.rs) ----
+
+struct Light {
+    int type;
+    double intensity;
+    V3 color, p, e1, e2, normal;
+    double radius = 0, area = 0;
+    V3 radiance() const { return color * intensity; }  // light.rs:151-153
+};
+
+struct LightNode {  // light_sampler.rs:19-31 (f32 storage, 48 B)
+    float mn[3];
+    float power;
+    float mx[3];
+    uint32_t parent, a, b;
+};
+
+struct LightSampler {
+    std::vector<LightNode> nodes;
+    std::vector<uint32_t> light_leaf, infinite;
+    std::vector<double> infinite_power;
+    double infinite_total = 0, p_infinite = 0;
+
+    static double lum_floor(V3 c) { return std::fmax(lum(c), 1e-9); }  // light_sampler.rs:45-47
+
+    // light_sampler.rs:74-87
+    static double importance(const LightNode& n, V3 p) {
+        double cx = ((double)n.mn[0] + (double)n.mx[0]) * 0.5;
+        double cy = ((double)n.mn[1] + (double)n.mx[1]) * 0.5;
+        double cz = ((double)n.mn[2] + (double)n.mx[2]) * 0.5;
+        double dx = p.x - cx, dy = p.y - cy, dz = p.z - cz;
+        double d2 = dx * dx + dy * dy + dz * dz;
+        double rx = (double)(n.mx[0] - n.mn[0]) * 0.5;
+        double ry = (double)(n.mx[1] - n.mn[1]) * 0.5;
+        double rz = (double)(n.mx[2] - n.mn[2]) * 0.5;
+        double r2 = rx * rx + ry * ry + rz * rz;
+        return (double)n.power / std::fmax(std::fmax(d2, r2), 1e-6);
+    }
+
+    struct Entry {
+        uint32_t light;
+        V3 center;
+        double radius, power;
+    };
+
+    // light_sampler.rs:242-312 median split; stable sort as Rust's sort_by.
+    uint32_t build_rec(const std::vector<Entry>& e, std::vector<size_t>& order, size_t start, size_t end,
+                       uint32_t parent) {
+        uint32_t index = (uint32_t)nodes.size();
+        float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+        double power = 0;
+        for (size_t k = start; k < end; k++) {
+            const Entry& en = e[order[k]];
+            double c[3] = {en.center.x, en.center.y, en.center.z};
+            for (int a = 0; a < 3; a++) {
+                mn[a] = std::fmin(mn[a], (float)(c[a] - en.radius));
+                mx[a] = std::fmax(mx[a], (float)(c[a] + en.radius));
+            }
+            power += en.power;
+        }
+        LightNode nd{};
+        for (int a = 0; a < 3; a++) {
+            nd.mn[a] = mn[a];
+            nd.mx[a] = mx[a];
+        }
+        nd.power = (float)power;
+        nd.parent = parent;
+        nd.a = 0;
+        nd.b = 0xFFFFFFFFu;
+        nodes.push_back(nd);
+        if (end - start == 1) {
+            uint32_t light = e[order[start]].light;
+            nodes[index].a = light;
+            light_leaf[light] = index;
+            return index;
+        }
+        int axis = 0;
+        float widest = -1.0f;
+        for (int a = 0; a < 3; a++) {
+            float w = mx[a] - mn[a];
+            if (w > widest) {
+                widest = w;
+                axis = a;
+            }
+        }
+        size_t mid = (start + end) / 2;
+        std::stable_sort(order.begin() + start, order.begin() + end, [&](size_t x, size_t y) {
+            return axis_of(e[x].center, axis) < axis_of(e[y].center, axis);
+        });
+        uint32_t a = build_rec(e, order, start, mid, index);
+        uint32_t b = build_rec(e, order, mid, end, index);
+        nodes[index].a = a;
+        nodes[index].b = b;
+        return index;
+    }
+
+    // light_sampler.rs:97-141
+    void build(const std::vector<Light>& lights) {
+        std::vector<Entry> finite;
+        light_leaf.assign(lights.size(), 0xFFFFFFFFu);
+        for (size_t i = 0; i < lights.size(); i++) {
+            const Light& l = lights[i];
+            double pw = lum_floor(l.radiance());
+            switch (l.type) {
+                case RT_LIGHT_POINT: finite.push_back({(uint32_t)i, l.p, 0.0, pw * 4.0 * PI}); break;
+                case RT_LIGHT_RECT: {
+                    V3 c = l.p + l.e1 * 0.5 + l.e2 * 0.5;
+                    finite.push_back({(uint32_t)i, c, (length(l.e1) + length(l.e2)) * 0.5, pw * l.area * PI});
+                    break;
+                }
+                case RT_LIGHT_SPHERE:
+                    finite.push_back({(uint32_t)i, l.p, l.radius, pw * 4.0 * PI * l.radius * l.radius * PI});
+                    break;
+                case RT_LIGHT_DISK: finite.push_back({(uint32_t)i, l.p, length(l.e1), pw * l.area * PI}); break;
+                default:
+                    infinite.push_back((uint32_t)i);
+                    infinite_power.push_back(pw * 4.0 * PI);
+            }
+        }
+        infinite_total = 0;
+        for (double w : infinite_power) infinite_total += w;
+        if (!finite.empty()) {
+            std::vector<size_t> order(finite.size());
+            for (size_t i = 0; i < order.size(); i++) order[i] = i;
+            build_rec(finite, order, 0, finite.size(), 0xFFFFFFFFu);
+        }
+        double finite_total = 0;
+        for (auto& e : finite) finite_total += e.power;
+        if (infinite.empty()) p_infinite = 0.0;
+        else if (finite.empty()) p_infinite = 1.0;
+        else p_infinite = std::min(std::max(infinite_total / (infinite_total + finite_total), 0.1), 0.9);
+    }
+
+    // light_sampler.rs:150-208
+    bool sample(V3 p, double u, uint32_t* light, double* pmf_out) const {
+        bool has_f = !nodes.empty(), has_i = !infinite.empty();
+        if (!has_f && !has_i) return false;
+        double pmf = 1.0;
+        bool inf;
+        if (has_f && has_i) {
+            if (u < p_infinite) {
+                u /= p_infinite;
+                pmf *= p_infinite;
+                inf = true;
+            } else {
+                u = (u - p_infinite) / (1.0 - p_infinite);
+                pmf *= 1.0 - p_infinite;
+                inf = false;
+            }
+        } else {
+            inf = has_i;
+        }
+        if (inf) {
+            double acc = 0.0, target = u * infinite_total;
+            for (size_t k = 0; k < infinite_power.size(); k++) {
+                acc += infinite_power[k];
+                if (target <= acc || k == infinite.size() - 1) {
+                    *light = infinite[k];
+                    *pmf_out = pmf * infinite_power[k] / std::fmax(infinite_total, 1e-12);
+                    return true;
+                }
+            }
+            return false;
+        }
+        size_t node = 0;
+        for (;;) {
+            const LightNode& nd = nodes[node];
+            if (nd.b == 0xFFFFFFFFu) {
+                *light = nd.a;
+                *pmf_out = pmf;
+                return true;
+            }
+            double ia = importance(nodes[nd.a], p), ib = importance(nodes[nd.b], p);
+            double total = ia + ib;
+            double pa = total > 1e-30 ? ia / total : 0.5;
+            if (u < pa) {
+                u = std::fmin(u / pa, 1.0 - 1e-12);
+                pmf *= pa;
+                node = nd.a;
+            } else {
+                u = std::fmin((u - pa) / (1.0 - pa), 1.0 - 1e-12);
+                pmf *= 1.0 - pa;
+                node = nd.b;
+            }
+        }
+    }
+
+    // light_sampler.rs:212-238
+    double pmf(V3 p, uint32_t light) const {
+        bool has_f = !nodes.empty(), has_i = !infinite.empty();
+        for (size_t k = 0; k < infinite.size(); k++)
+            if (infinite[k] == light) {
+                double group = has_f ? p_infinite : 1.0;
+                return group * infinite_power[k] / std::fmax(infinite_total, 1e-12);
+            }
+        uint32_t leaf = light < light_leaf.size() ? light_leaf[light] : 0xFFFFFFFFu;
+        if (leaf == 0xFFFFFFFFu) return 0.0;
+        double pmf = has_i ? 1.0 - p_infinite : 1.0;
+        uint32_t node = leaf;
+        while (nodes[node].parent != 0xFFFFFFFFu) {
+            uint32_t parent = nodes[node].parent;
+            const LightNode& pn = nodes[parent];
+            double ia = importance(nodes[pn.a], p), ib = importance(nodes[pn.b], p);
+            double total = ia + ib;
+            double mine = node == pn.a ? ia : ib;
+            pmf *= total > 1e-30 ? mine / total : 0.5;
+            node = parent;
+        }
+        return pmf;
+    }
+};
+
+// ---- materials (src/scene/pbr.rs, material.rs) ----------------------------
+
+struct Pbr {
+    double diffuse_gain;
+    V3 diffuse_color;
+    double diffuse_roughness;
+    V3 spec_face, spec_edge;
+    double spec_rough, spec_ior;
+    double cc_gain, cc_rough;
+    double fuzz_gain;
+    V3 fuzz_color;
+    double glass_gain, glass_ior, glass_rough;
+    V3 refraction_color, glow;
+    double presence;
+    // Material fields
+    V3 emission;
+    int32_t area_light;
+    uint32_t id;
+
+    static Pbr from(const rt_material_desc& m) {
+        Pbr p;
+        p.diffuse_gain = m.diffuse_gain;
+        p.diffuse_color = v3(m.diffuse_color);
+        p.diffuse_roughness = m.diffuse_roughness;
+        p.spec_face = v3(m.specular_face_color);
+        p.spec_edge = v3(m.specular_edge_color);
+        p.spec_rough = m.specular_roughness;
+        p.spec_ior = m.specular_ior;
+        p.cc_gain = m.clearcoat_gain;
+        p.cc_rough = m.clearcoat_roughness;
+        p.fuzz_gain = m.fuzz_gain;
+        p.fuzz_color = v3(m.fuzz_color);
+        p.glass_gain = m.glass_gain;
+        p.glass_ior = m.glass_ior;
+        p.glass_rough = m.glass_roughness;
+        p.refraction_color = v3(m.refraction_color);
+        p.glow = v3(m.glow);
+        p.presence = m.presence;
+        p.emission = v3(m.emission);
+        p.area_light = m.area_light;
+        p.id = m.id;
+        return p;
+    }
+    // pbr.rs:86-96
+    V3 specular_f0() const {
+        if (lum(spec_face) > 1e-6) return spec_face;
+        if (spec_ior > 1.0) {
+            double r = (spec_ior - 1.0) / (spec_ior + 1.0);
+            return V3{1, 1, 1} * (r * r);
+        }
+        return {0, 0, 0};
+    }
+    bool has_specular() const { return lum(specular_f0()) > 1e-6; }  // pbr.rs:100-102
+    // pbr.rs:188-201
+    bool lobe_weights(double w[5]) const {
+        double wd = diffuse_gain * lum(diffuse_color);
+        double ws = std::sqrt(lum(specular_f0()));
+        double wc = cc_gain * 0.2;
+        double wf = fuzz_gain * lum(fuzz_color) * 0.3;
+        double wg = glass_gain;
+        double total = wd + ws + wc + wf + wg;
+        if (total <= 1e-9) return false;
+        w[0] = wd / total;
+        w[1] = ws / total;
+        w[2] = wc / total;
+        w[3] = wf / total;
+        w[4] = wg / total;
+        return true;
+    }
+};
+
+// ---- BSDF (src/raytracer/pt/bxdf.rs) ---------------------------------------
+
+struct Frame {  // bxdf.rs:16-39
+    V3 t, b, n;
+    explicit Frame(V3 nn) : n(nn) {
+        V3 t0 = std::fabs(n.x) > 0.9 ? V3{0, 1, 0} : V3{1, 0, 0};
+        t = normalize(cross(n, t0));
+        b = cross(n, t);
+    }
+    V3 to_local(V3 w) const { return {dot(w, t), dot(w, b), dot(w, n)}; }
+    V3 to_world(V3 w) const { return t * w.x + b * w.y + n * w.z; }
+};
+
+static V3 schlick(V3 f0, V3 f90, double c) {  // bxdf.rs:57-60
+    double m = std::pow(std::min(std::max(1.0 - c, 0.0), 1.0), 5);
+    return f0 + (f90 - f0) * m;
+}
+double fresnel_dielectric(double cos_i, double eta) {  // bxdf.rs:63-73
+    cos_i = std::min(std::max(cos_i, 0.0), 1.0);
+    double sin2_t = (1.0 - cos_i * cos_i) / (eta * eta);
+    if (sin2_t >= 1.0) return 1.0;
+    double cos_t = std::sqrt(1.0 - sin2_t);
+    double r_par = (eta * cos_i - cos_t) / (eta * cos_i + cos_t);
+    double r_perp = (cos_i - eta * cos_t) / (cos_i + eta * cos_t);
+    return 0.5 * (r_par * r_par + r_perp * r_perp);
+}
+static double ggx_d(V3 h, double alpha) {  // bxdf.rs:77-84
+    if (h.z <= 0.0) return 0.0;
+    double a2 = alpha * alpha;
+    double d = h.z * h.z * (a2 - 1.0) + 1.0;
+    return a2 / (PI * d * d);
+}
+static double ggx_lambda(V3 w, double alpha) {  // bxdf.rs:86-93
+    double cos2 = w.z * w.z;
+    if (cos2 <= 0.0) return 0.0;
+    double tan2 = std::fmax(1.0 - cos2, 0.0) / cos2;
+    return (std::sqrt(1.0 + alpha * alpha * tan2) - 1.0) * 0.5;
+}
+static double ggx_g1(V3 w, double a) { return 1.0 / (1.0 + ggx_lambda(w, a)); }
+static double ggx_g2(V3 wo, V3 wi, double a) { return 1.0 / (1.0 + ggx_lambda(wo, a) + ggx_lambda(wi, a)); }
+// bxdf.rs:104-123 Heitz 2018 VNDF sampling.
+static V3 ggx_sample_vndf(V3 wo, double alpha, double u1, double u2) {
+    V3 v = normalize(V3{alpha * wo.x, alpha * wo.y, wo.z});
+    double lensq = v.x * v.x + v.y * v.y;
+    V3 t1 = lensq > 1e-12 ? V3{-v.y, v.x, 0.0} / std::sqrt(lensq) : V3{1, 0, 0};
+    V3 t2 = cross(v, t1);
+    double r = std::sqrt(u1), phi = 2.0 * PI * u2;
+    double p1 = r * std::cos(phi), p2 = r * std::sin(phi);
+    double s = 0.5 * (1.0 + v.z);
+    p2 = (1.0 - s) * std::sqrt(std::fmax(1.0 - p1 * p1, 0.0)) + s * p2;
+    V3 nh = t1 * p1 + t2 * p2 + v * std::sqrt(std::fmax(1.0 - p1 * p1 - p2 * p2, 0.0));
+    return normalize(V3{alpha * nh.x, alpha * nh.y, std::fmax(nh.z, 1e-9)});
+}
+static double ggx_pdf_h(V3 wo, V3 h, double alpha) {  // bxdf.rs:126-132
+    double odh = dot(wo, h);
+    if (odh <= 0.0 || wo.z <= 0.0) return 0.0;
+    return ggx_g1(wo, alpha) * odh * ggx_d(h, alpha) / wo.z;
+}
+static double under_layer_scale(const Pbr& p) {  // bxdf.rs:137-143
+    V3 f0 = p.specular_f0();
+    double spec_take = 0.2126 * f0.x + 0.7152 * f0.y + 0.0722 * f0.z;
+    double coat_take = 0.04 * p.cc_gain;
+    return std::min(std::max((1.0 - spec_take) * (1.0 - coat_take), 0.0), 1.0);
+}
+static V3 eval_diffuse(const Pbr& p, V3 wo, V3 wi) {  // bxdf.rs:145-165
+    double sigma2 = p.diffuse_roughness * p.diffuse_roughness;
+    double a = 1.0 - sigma2 / (2.0 * (sigma2 + 0.33));
+    double b = 0.45 * sigma2 / (sigma2 + 0.09);
+    double sin_o = std::sqrt(std::fmax(1.0 - wo.z * wo.z, 0.0));
+    double sin_i = std::sqrt(std::fmax(1.0 - wi.z * wi.z, 0.0));
+    double cos_dphi = 0.0;
+    if (sin_o > 1e-6 && sin_i > 1e-6)
+        cos_dphi = std::min(std::max((wo.x * wi.x + wo.y * wi.y) / (sin_o * sin_i), -1.0), 1.0);
+    double sin_a, tan_b;
+    if (wo.z < wi.z) {
+        sin_a = sin_o;
+        tan_b = sin_i / std::fmax(wi.z, 1e-6);
+    } else {
+        sin_a = sin_i;
+        tan_b = sin_o / std::fmax(wo.z, 1e-6);
+    }
+    return p.diffuse_color * (p.diffuse_gain * under_layer_scale(p) / PI) *
+           (a + b * std::fmax(cos_dphi, 0.0) * sin_a * tan_b);
+}
+static V3 eval_fuzz(const Pbr& p, V3 wo, V3 wi) {  // bxdf.rs:167-171
+    double rim = 0.5 * (std::pow(1.0 - wi.z, 4) + std::pow(1.0 - wo.z, 4));
+    return p.fuzz_color * (p.fuzz_gain / PI) * rim;
+}
+static V3 eval_spec(V3 f0, V3 f90, double alpha, V3 wo, V3 wi) {  // bxdf.rs:173-179
+    V3 h = normalize(wo + wi);
+    double d = ggx_d(h, alpha), g = ggx_g2(wo, wi, alpha);
+    V3 f = schlick(f0, f90, std::fmax(dot(wo, h), 0.0));
+    return f * (d * g / std::fmax(4.0 * wo.z * wi.z, 1e-9));
+}
+static double spec_pdf(V3 wo, V3 wi, double alpha) {  // bxdf.rs:181-185
+    V3 h = normalize(wo + wi);
+    double odh = std::fmax(dot(wo, h), 1e-9);
+    return ggx_pdf_h(wo, h, alpha) / (4.0 * odh);
+}
+static double alpha_of(double r) { return std::min(std::max(r * r, 2.5e-5), 1.0); }  // bxdf.rs:187-189
+
+// bxdf.rs:193-232
+static V3 glass_transmit(const Pbr& p, V3 wo, V3 wi, double eta, double* pdf) {
+    double alpha = alpha_of(p.glass_rough);
+    V3 h = normalize(wo + wi * eta);
+    if (h.z < 0.0) h = -h;
+    double odh = dot(wo, h), idh = dot(wi, h);
+    *pdf = 0.0;
+    if (odh <= 0.0 || idh >= 0.0) return {0, 0, 0};
+    double fres = fresnel_dielectric(odh, eta);
+    double d = ggx_d(h, alpha);
+    double g = ggx_g2(wo, V3{wi.x, wi.y, -wi.z}, alpha);
+    double sqrt_denom = odh + eta * idh;
+    if (std::fabs(sqrt_denom) < 1e-9) return {0, 0, 0};
+    double factor = 1.0 / (eta * eta);
+    V3 f = p.refraction_color * (p.glass_gain * under_layer_scale(p) * (1.0 - fres) * d * g * factor *
+                                 std::fabs(idh * odh / (wi.z * wo.z)) * (eta * eta) / (sqrt_denom * sqrt_denom));
+    double dwh_dwi = std::fabs(eta * eta * idh) / (sqrt_denom * sqrt_denom);
+    *pdf = ggx_pdf_h(wo, h, alpha) * dwh_dwi;
+    return f;
+}
+
+// bxdf.rs:241-299
+static void eval_pdf(const Pbr& p, V3 wo, V3 wi, double eta, V3* f_out, double* pdf_out) {
+    double w[5];
+    *f_out = {0, 0, 0};
+    *pdf_out = 0.0;
+    if (!p.lobe_weights(w)) return;
+    double wd = w[0], ws = w[1], wc = w[2], wf = w[3], wg = w[4];
+    if (wi.z > 0.0) {
+        V3 f{0, 0, 0};
+        double pdf = 0.0, cos_pdf = wi.z / PI;
+        if (wd > 0.0) {
+            f = f + eval_diffuse(p, wo, wi);
+            pdf += wd * cos_pdf;
+        }
+        if (wf > 0.0) {
+            f = f + eval_fuzz(p, wo, wi);
+            pdf += wf * cos_pdf;
+        }
+        if (ws > 0.0) {
+            double a = alpha_of(p.spec_rough);
+            f = f + eval_spec(p.specular_f0(), p.spec_edge, a, wo, wi);
+            pdf += ws * spec_pdf(wo, wi, a);
+        }
+        if (wc > 0.0) {
+            double a = alpha_of(p.cc_rough);
+            V3 f0 = V3{0.04, 0.04, 0.04} * p.cc_gain;
+            f = f + eval_spec(f0, V3{1, 1, 1} * p.cc_gain, a, wo, wi);
+            pdf += wc * spec_pdf(wo, wi, a);
+        }
+        if (wg > 0.0) {
+            double a = alpha_of(p.glass_rough);
+            V3 h = normalize(wo + wi);
+            double fres = fresnel_dielectric(std::fmax(dot(wo, h), 0.0), eta);
+            double d = ggx_d(h, a), g = ggx_g2(wo, wi, a);
+            f = f + V3{1, 1, 1} * (p.glass_gain * under_layer_scale(p) * fres * d * g /
+                                   std::fmax(4.0 * wo.z * wi.z, 1e-9));
+            pdf += wg * fres * spec_pdf(wo, wi, a);
+        }
+        *f_out = f;
+        *pdf_out = pdf;
+    } else {
+        if (wg <= 0.0) return;
+        double pdf_lobe;
+        V3 f = glass_transmit(p, wo, wi, eta, &pdf_lobe);
+        V3 h = normalize(wo + wi * eta);
+        if (h.z < 0.0) h = -h;
+        double fres = fresnel_dielectric(std::fmax(dot(wo, h), 0.0), eta);
+        *f_out = f;
+        *pdf_out = wg * (1.0 - fres) * pdf_lobe;
+    }
+}
+
+struct BsdfSample {
+    bool specular_lobe, transmitted;
+    V3 wi, f;
+    double pdf;
+};
+
+static V3 cosine_sample(Pcg32& rng) {  // bxdf.rs:301-306
+    double u = rng.next_f64(), v = rng.next_f64();
+    double r = std::sqrt(u), phi = 2.0 * PI * v;
+    return {r * std::cos(phi), r * std::sin(phi), std::sqrt(std::fmax(1.0 - u, 0.0))};
+}
+
+// bxdf.rs:309-374
+static bool sample_bsdf(const Pbr& p, V3 wo, double eta, Pcg32& rng, BsdfSample* s) {
+    double w[5];
+    if (!p.lobe_weights(w)) return false;
+    double wd = w[0], ws = w[1], wc = w[2], wf = w[3], wg = w[4];
+    double pick = rng.next_f64();
+    bool transmitted = false;
+    bool specular_lobe = pick >= wd + wf;
+    V3 wi;
+    if (pick < wd + wf) {
+        wi = cosine_sample(rng);
+    } else if (pick < wd + wf + ws) {
+        double a = alpha_of(p.spec_rough);
+        double u1 = rng.next_f64(), u2 = rng.next_f64();
+        V3 h = ggx_sample_vndf(wo, a, u1, u2);
+        wi = reflect(-wo, h);
+        if (wi.z <= 0.0) return false;
+    } else if (pick < wd + wf + ws + wc) {
+        double a = alpha_of(p.cc_rough);
+        double u1 = rng.next_f64(), u2 = rng.next_f64();
+        V3 h = ggx_sample_vndf(wo, a, u1, u2);
+        wi = reflect(-wo, h);
+        if (wi.z <= 0.0) return false;
+    } else if (wg > 0.0) {
+        double a = alpha_of(p.glass_rough);
+        double u1 = rng.next_f64(), u2 = rng.next_f64();
+        V3 h = ggx_sample_vndf(wo, a, u1, u2);
+        double fres = fresnel_dielectric(std::fmax(dot(wo, h), 0.0), eta);
+        if (rng.next_f64() < fres) {
+            wi = reflect(-wo, h);
+            if (wi.z <= 0.0) return false;
+        } else {
+            double cos_i = dot(wo, h);
+            double sin2_t = (1.0 - cos_i * cos_i) / (eta * eta);
+            if (sin2_t >= 1.0) return false;
+            double cos_t = std::sqrt(1.0 - sin2_t);
+            wi = normalize((-wo) / eta + h * (cos_i / eta - cos_t));
+            if (wi.z >= 0.0) return false;
+            transmitted = true;
+        }
+    } else {
+        return false;
+    }
+    V3 f;
+    double pdf;
+    eval_pdf(p, wo, wi, eta, &f, &pdf);
+    if (pdf <= 0.0) return false;
+    s->wi = wi;
+    s->f = f;
+    s->pdf = pdf;
+    s->transmitted = transmitted;
+    s->specular_lobe = specular_lobe;
+    return true;
+}
+
+// ---- scene ------------------------------------------------------------------
+
+struct Camera {
+    uint32_t width, height;
+    double fov;
+    V3 eye, forward, up, right;
+    double lens_radius, focal_distance;
+    int filter;
+    double filter_width;
+
+    double sample_1d(double u) const {  // camera.rs:36-61
+        switch (filter) {
+            case RT_FILTER_TRIANGLE: {
+                double half = filter_width * 0.5;
+                return u < 0.5 ? (std::sqrt(2.0 * u) - 1.0) * half : (1.0 - std::sqrt(2.0 * (1.0 - u))) * half;
+            }
+            case RT_FILTER_GAUSSIAN: {
+                double u1 = std::fmax(u, 1e-12);
+                double x = u * 2654435761.0;
+                double u2 = x - std::trunc(x);
+                double sigma = filter_width / 4.0;
+                double g = std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * PI * u2);
+                return std::min(std::max(g * sigma, -filter_width * 0.5), filter_width * 0.5);
+            }
+            default: return (u - 0.5) * filter_width;
+        }
+    }
+    // camera.rs:150-179 (perspective).
+    Ray generate(double px, double py, double lu, double lv) const {
+        double u = (px / (double)width) * 2.0 - 1.0;
+        double v = 1.0 - (py / (double)height) * 2.0;
+        double aspect = (double)width / (double)height;
+        double half_h = std::tan(fov * PI / 180.0 / 2.0);
+        double half_w = aspect * half_h;
+        V3 dir = forward + right * (u * half_w) + up * (v * half_h);
+        if (lens_radius <= 0.0) return make_ray(eye, dir);
+        double r = lens_radius * std::sqrt(lu), phi = 2.0 * PI * lv;
+        V3 off = right * (r * std::cos(phi)) + up * (r * std::sin(phi));
+        V3 focus = eye + dir * focal_distance;
+        V3 origin = eye + off;
+        return make_ray(origin, focus - origin);
+    }
+};
+
+struct Scene {
+    std::vector<Mesh> meshes;
+    std::vector<Instance> instances;
+    std::vector<Pbr> materials;
+    std::vector<Light> lights;
+    LightSampler ls;
+    Bvh tlas;
+    Camera cam;
+    V3 background;
+    bool any_presence = false;
+
+    // mesh.rs:308-381 Instance::intersect + scene/mod.rs:105-146.
+    bool intersect(const Ray& ray, Hit* out, Counters* c) const {
+        if (instances.empty()) return false;
+        double dir_len = std::fmax(length(ray.d), 1e-300);
+        double t_budget = INF / dir_len;
+        struct Best {
+            uint32_t inst, tri;
+            double u, v;
+        } best{0, 0, 0, 0};
+        auto inst_isect = [&](uint32_t ii, double t_max, double* t_out) -> bool {
+            const Instance& in = instances[ii];
+            if (c) c->insts++;
+            Ray lr{xf_point(in.inv, ray.o), xf_vec(in.inv, ray.d)};
+            const Mesh& m = meshes[in.mesh_id];
+            double hu = 0, hv = 0;
+            uint32_t tri;
+            double t;
+            auto tri_isect = [&](uint32_t tr, double tmax, double* to) -> bool {
+                if (c) c->tris++;
+                double tt, uu, vv;
+                if (m.intersect_triangle(lr, tr, tmax, &tt, &uu, &vv)) {
+                    hu = uu;
+                    hv = vv;
+                    *to = tt;
+                    return true;
+                }
+                return false;
+            };
+            if (!m.blas.traverse(lr.o, lr.d, t_max, tri_isect, &tri, &t, c)) return false;
+            best = {ii, tri, hu, hv};
+            *t_out = t;
+            return true;
+        };
+        uint32_t winner;
+        double tw;
+        if (!tlas.traverse(ray.o, ray.d, t_budget, inst_isect, &winner, &tw, c)) return false;
+        const Instance& in = instances[best.inst];
+        const Mesh& m = meshes[in.mesh_id];
+        V3 ln = m.local_normal(best.tri, best.u, best.v);
+        V3 wn = normalize(xf_normal(in.inv, ln));
+        // mesh.rs:427-439 to_intersection.
+        V3 point = ray.o + ray.d * tw;
+        bool front = dot(wn, ray.d) < 0.0;
+        if (!front) wn = -wn;
+        out->t = length(point - ray.o);
+        out->point = point;
+        out->normal = normalize(wn);
+        out->material_id = in.material_id;
+        out->inst = best.inst;
+        out->prim = best.tri;
+        out->front_face = front;
+        return true;
+    }
+
+    bool intersect_param(V3 o, V3 d, double t_max, uint32_t* inst, uint32_t* prim, double* t_out,
+                         Counters* c) const {
+        if (instances.empty()) return false;
+        Ray ray{o, d};
+        uint32_t bi = 0, bt = 0;
+        auto inst_isect = [&](uint32_t ii, double tmax, double* to) -> bool {
+            const Instance& in = instances[ii];
+            if (c) c->insts++;
+            Ray lr{xf_point(in.inv, ray.o), xf_vec(in.inv, ray.d)};
+            const Mesh& m = meshes[in.mesh_id];
+            uint32_t tri;
+            double t;
+            auto tri_isect = [&](uint32_t tr, double tm, double* tt) -> bool {
+                if (c) c->tris++;
+                double uu, vv;
+                return m.intersect_triangle(lr, tr, tm, tt, &uu, &vv);
+            };
+            if (!m.blas.traverse(lr.o, lr.d, tmax, tri_isect, &tri, &t, c)) return false;
+            bi = ii;
+            bt = tri;
+            *to = t;
+            return true;
+        };
+        uint32_t w;
+        double tw;
+        if (!tlas.traverse(o, d, t_max, inst_isect, &w, &tw, c)) return false;
+        *inst = bi;
+        *prim = bt;
+        *t_out = tw;
+        return true;
+    }
+
+    // mesh.rs:384-407 Instance::occludes under Bvh::any_hit on the TLAS.
+    bool occluded_param(V3 o, V3 d, double t_limit, Counters* c) const {
+        if (instances.empty()) return false;
+        auto inst_hit = [&](uint32_t ii, double lim) -> bool {
+            const Instance& in = instances[ii];
+            if (c) c->insts++;
+            Ray lr{xf_point(in.inv, o), xf_vec(in.inv, d)};
+            const Mesh& m = meshes[in.mesh_id];
+            return m.blas.any_hit(lr.o, lr.d, lim, [&](uint32_t tr, double l2) -> bool {
+                if (c) c->tris++;
+                double t, u, v;
+                return m.intersect_triangle(lr, tr, l2, &t, &u, &v);
+            }, c);
+        };
+        return tlas.any_hit(o, d, t_limit, inst_hit, c);
+    }
+};
+
+// ---- integrator (src/raytracer/pt/mod.rs) -----------------------------------
+
+struct Aux {
+    V3 albedo, normal, diffuse;
+    double depth = 0;
+    uint32_t id = 0;
+};
+
+static double power_heuristic(double a, double b) {  // mod.rs:992-996
+    double a2 = a * a, b2 = b * b;
+    return a2 + b2 <= 0.0 ? 0.0 : a2 / (a2 + b2);
+}
+
+struct Tracer {
+    const Scene& sc;
+    const rt_params& prm;
+    uint64_t ext_rays = 0, shadow_rays = 0;
+    Counters cext, cshadow;  // traversal work of extension / shadow rays
+
+    // mod.rs:1254-1306 transmittance, restricted to surfaces (no media).
+    V3 transmittance(V3 origin, V3 dir, double remaining) {
+        V3 vis{1, 1, 1};
+        for (int k = 0; k < MAX_PRESENCE_SKIPS; k++) {
+            shadow_rays++;
+            Hit h;
+            Ray r = make_ray(origin, dir);
+            if (!sc.intersect(r, &h, &cshadow)) return vis;
+            if (h.t >= remaining) return vis;
+            double presence = std::min(std::max(sc.materials[h.material_id].presence, 0.0), 1.0);
+            if (presence >= 1.0) return {0, 0, 0};
+            vis = vis * (1.0 - presence);
+            if (max_comp(vis) < 1e-4) return {0, 0, 0};
+            origin = h.point + dir * RAY_OFFSET;
+            remaining -= h.t + RAY_OFFSET;
+        }
+        return vis;
+    }
+    // mod.rs:1212-1237
+    V3 visibility_to(V3 p, V3 n, V3 target) {
+        V3 dir = target - p;
+        double dist = length(dir);
+        return transmittance(p + n * RAY_OFFSET, normalize(dir), dist - 1e-3);
+    }
+    V3 visibility_toward(V3 p, V3 n, V3 wi) { return transmittance(p + n * RAY_OFFSET, wi, 1e8); }
+
+    // mod.rs:1000-1023 (rect/disk/sphere).
+    static double light_pdf_sa(const Light& l, V3 origin, const Hit& h) {
+        if (l.type == RT_LIGHT_RECT || l.type == RT_LIGHT_DISK) {
+            V3 d = h.point - origin;
+            double dist2 = length_sq(d);
+            double cos_l = std::fabs(dot(normalize(d), l.normal));
+            if (cos_l < 1e-9 || l.area <= 0.0) return 0.0;
+            return dist2 / (cos_l * l.area);
+        }
+        if (l.type == RT_LIGHT_SPHERE) {
+            double dist2 = length_sq(l.p - origin);
+            double sin2 = std::fmin(l.radius * l.radius / dist2, 1.0);
+            double cos_max = std::sqrt(std::fmax(1.0 - sin2, 0.0));
+            double sa = 2.0 * PI * (1.0 - cos_max);
+            return sa < 1e-12 ? 0.0 : 1.0 / sa;
+        }
+        return 0.0;
+    }
+
+    // mod.rs:1177-1209
+    template <class E>
+    V3 area_contrib(V3 p, V3 n, V3 sp, const Light& l, E& eval, double pick) {
+        V3 to = sp - p;
+        double dist2 = std::fmax(length_sq(to), 1e-12);
+        V3 wi = normalize(to);
+        double cos_l = std::fabs(dot(wi, l.normal));
+        if (cos_l < 1e-9 || l.area <= 0.0) return {0, 0, 0};
+        double bpdf;
+        V3 f = eval(wi, &bpdf);
+        if (max_comp(f) <= 0.0) return {0, 0, 0};
+        V3 vis = visibility_to(p, n, sp);
+        if (max_comp(vis) <= 0.0) return {0, 0, 0};
+        double pdf_sa = pick * dist2 / (cos_l * l.area);
+        double w = power_heuristic(pdf_sa, bpdf);
+        return f * l.radiance() * vis * (w / pdf_sa);
+    }
+
+    // mod.rs:1032-1174 (point, distant, rect, disk, sphere).
+    template <class E>
+    V3 sample_light(const Light& l, V3 p, V3 n, E& eval, double pick, Pcg32& rng) {
+        switch (l.type) {
+            case RT_LIGHT_POINT: {
+                V3 to = l.p - p;
+                double dist2 = std::fmax(length_sq(to), 1e-12);
+                V3 wi = normalize(to);
+                double bp;
+                V3 f = eval(wi, &bp);
+                if (max_comp(f) <= 0.0) return {0, 0, 0};
+                V3 vis = visibility_to(p, n, l.p);
+                if (max_comp(vis) <= 0.0) return {0, 0, 0};
+                return f * l.radiance() * vis / (dist2 * pick);
+            }
+            case RT_LIGHT_DISTANT: {
+                V3 base = -l.e1;
+                V3 wi = base;
+                if (l.radius > 1e-5) {
+                    double cos_max = std::cos(l.radius);
+                    double u = rng.next_f64(), v = rng.next_f64();
+                    double cos_t = 1.0 - u * (1.0 - cos_max);
+                    double sin_t = std::sqrt(std::fmax(1.0 - cos_t * cos_t, 0.0));
+                    double phi = 2.0 * PI * v;
+                    Frame lf(base);
+                    wi = lf.to_world(V3{sin_t * std::cos(phi), sin_t * std::sin(phi), cos_t});
+                }
+                double bp;
+                V3 f = eval(wi, &bp);
+                if (max_comp(f) <= 0.0) return {0, 0, 0};
+                V3 vis = visibility_toward(p, n, wi);
+                if (max_comp(vis) <= 0.0) return {0, 0, 0};
+                return f * l.radiance() * vis / pick;
+            }
+            case RT_LIGHT_RECT: {
+                double u = rng.next_f64(), v = rng.next_f64();
+                V3 sp = l.p + l.e1 * u + l.e2 * v;
+                return area_contrib(p, n, sp, l, eval, pick);
+            }
+            case RT_LIGHT_DISK: {
+                double u = rng.next_f64(), v = rng.next_f64();
+                double r = std::sqrt(u), phi = 2.0 * PI * v;
+                V3 sp = l.p + l.e1 * (r * std::cos(phi)) + l.e2 * (r * std::sin(phi));
+                return area_contrib(p, n, sp, l, eval, pick);
+            }
+            case RT_LIGHT_SPHERE: {
+                V3 tc = l.p - p;
+                double dist2 = length_sq(tc);
+                if (dist2 <= l.radius * l.radius * 1.0001) return {0, 0, 0};
+                double sin2 = std::fmin(l.radius * l.radius / dist2, 1.0);
+                double cos_max = std::sqrt(std::fmax(1.0 - sin2, 0.0));
+                double u = rng.next_f64(), v = rng.next_f64();
+                double cos_t = 1.0 - u * (1.0 - cos_max);
+                double sin_t = std::sqrt(std::fmax(1.0 - cos_t * cos_t, 0.0));
+                double phi = 2.0 * PI * v;
+                Frame lf(normalize(tc));
+                V3 wi = lf.to_world(V3{sin_t * std::cos(phi), sin_t * std::sin(phi), cos_t});
+                double bp;
+                V3 f = eval(wi, &bp);
+                if (max_comp(f) <= 0.0) return {0, 0, 0};
+                double dist = std::sqrt(dist2) * cos_t -
+                              std::sqrt(std::fmax(l.radius * l.radius - dist2 * sin_t * sin_t, 0.0));
+                V3 target = p + wi * dist;
+                V3 vis = visibility_to(p, n, target);
+                if (max_comp(vis) <= 0.0) return {0, 0, 0};
+                double pdf_sa = pick / std::fmax(2.0 * PI * (1.0 - cos_max), 1e-12);
+                double w = power_heuristic(pdf_sa, bp);
+                return f * l.radiance() * vis * (w / pdf_sa);
+            }
+        }
+        return {0, 0, 0};
+    }
+
+    // mod.rs:449-990 trace_full, surface transport only.
+    V3 trace(Ray ray, Pcg32& rng, Aux& aux) {
+        V3 L{0, 0, 0};
+        int first_specular = -1;  // -1 None, 0 false, 1 true
+        bool aux_set = false;
+        double travel = 0.0;
+        auto emit = [&](V3 c) {
+            L = L + c;
+            if (first_specular != 1) aux.diffuse = aux.diffuse + c;
+        };
+        V3 beta{1, 1, 1};
+        double prev_pdf = 0.0;
+        V3 prev_origin = ray.o;
+        bool from_camera = true;
+        int presence_skips = 0;
+        uint32_t depth = 0;
+        while (depth < prm.max_depth) {
+            Hit hit;
+            ext_rays++;
+            if (!sc.intersect(ray, &hit, &cext)) {
+                emit(beta * sc.background);
+                break;
+            }
+            const Pbr& pbr = sc.materials[hit.material_id];
+            V3 wo = -normalize(ray.d);
+            travel += hit.t;
+            if (!aux_set) {
+                aux_set = true;
+                V3 a = pbr.diffuse_color * pbr.diffuse_gain + pbr.specular_f0() * (pbr.has_specular() ? 1.0 : 0.0) +
+                       pbr.refraction_color * pbr.glass_gain;
+                aux.albedo = {std::fmin(a.x, 1.0), std::fmin(a.y, 1.0), std::fmin(a.z, 1.0)};
+                aux.normal = dot(hit.normal, wo) >= 0.0 ? hit.normal : -hit.normal;
+                aux.depth = travel;
+                aux.id = pbr.id;
+            }
+            double presence = std::min(std::max(pbr.presence, 0.0), 1.0);
+            if (presence < 1.0 && rng.next_f64() >= presence && presence_skips < MAX_PRESENCE_SKIPS) {
+                presence_skips++;
+                travel += hit.t;
+                ray = make_ray(hit.point + normalize(ray.d) * RAY_OFFSET, ray.d);
+                continue;
+            }
+            bool entering = hit.front_face;
+            V3 n = dot(hit.normal, wo) >= 0.0 ? hit.normal : -hit.normal;
+            double eta_rel = entering ? pbr.glass_ior : 1.0 / pbr.glass_ior;
+            V3 emission = pbr.emission + pbr.glow;
+            if (max_comp(emission) > 0.0) {
+                double weight = 1.0;
+                if (!from_camera && pbr.area_light >= 0) {
+                    const Light& l = sc.lights[pbr.area_light];
+                    double pick = sc.ls.pmf(prev_origin, (uint32_t)pbr.area_light);
+                    double pdf_light = light_pdf_sa(l, prev_origin, hit) * pick;
+                    weight = power_heuristic(prev_pdf, pdf_light);
+                }
+                emit(beta * emission * weight);
+            }
+            Frame frame(n);
+            V3 wo_l = frame.to_local(wo);
+            double lw[5];
+            if (!sc.lights.empty() && pbr.lobe_weights(lw)) {
+                auto eval = [&](V3 wi_world, double* pdf) -> V3 {
+                    V3 wi_l = frame.to_local(wi_world);
+                    if (wi_l.z <= 0.0) {
+                        *pdf = 0.0;
+                        return {0, 0, 0};
+                    }
+                    V3 f;
+                    eval_pdf(pbr, wo_l, wi_l, eta_rel, &f, pdf);
+                    return f * wi_l.z;
+                };
+                uint32_t li;
+                double pmf;
+                if (sc.ls.sample(hit.point, rng.next_f64(), &li, &pmf)) {
+                    V3 c = sample_light(sc.lights[li], hit.point, n, eval, pmf, rng);
+                    emit(beta * c);
+                }
+            }
+            BsdfSample s;
+            if (!sample_bsdf(pbr, wo_l, eta_rel, rng, &s)) break;
+            V3 wi_world = frame.to_world(s.wi);
+            beta = beta * s.f * (std::fabs(s.wi.z) / s.pdf);
+            if (first_specular < 0) first_specular = s.specular_lobe ? 1 : 0;
+            prev_pdf = s.pdf;
+            prev_origin = hit.point;
+            from_camera = false;
+            double off = s.transmitted ? -RAY_OFFSET : RAY_OFFSET;
+            ray = make_ray(hit.point + n * off, wi_world);
+            depth++;
+            if (depth >= prm.rr_start) {
+                double q = std::fmin(max_comp(beta), 0.95);
+                if (q <= 0.0 || rng.next_f64() > q) break;
+                beta = beta / q;
+            }
+        }
+        return L;
+    }
+};
+
+}  // namespace orc
+
+using namespace orc;
+
+struct oracle_scene {
+    Scene s;
+};
+
+static Light make_light(const rt_light_desc& d) {
+    Light l;
+    l.type = d.type;
+    l.intensity = d.intensity;
+    l.color = v3(d.color);
+    l.p = v3(d.p);
+    l.e1 = v3(d.e1);
+    l.e2 = v3(d.e2);
+    l.radius = d.radius;
+    if (d.type == RT_LIGHT_DISTANT) l.e1 = normalize(l.e1);  // light.rs:68-80
+    if (d.type == RT_LIGHT_RECT) {                            // light.rs:95-110
+        V3 c = cross(l.e1, l.e2);
+        l.area = length(c);
+        l.normal = normalize(c);
+    }
+    if (d.type == RT_LIGHT_DISK) {  // light.rs:124-135
+        l.normal = normalize(cross(l.e1, l.e2));
+        l.area = PI * length(l.e1) * length(l.e2);
+    }
+    return l;
+}
+
+template <class F>
+static void parallel_for(uint64_t n, int threads, F&& f) {
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    if (threads == 1 || n < 64) {
+        f(0, n, 0);
+        return;
+    }
+    std::atomic<uint64_t> next{0};
+    const uint64_t chunk = 64;
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++)
+        pool.emplace_back([&, t] {
+            for (;;) {
+                uint64_t b = next.fetch_add(chunk);
+                if (b >= n) break;
+                f(b, std::min(n, b + chunk), t);
+            }
+        });
+    for (auto& th : pool) th.join();
+}
+
+extern "C" {
+
+oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
+    if (!d) return nullptr;
+    auto* os = new oracle_scene();
+    Scene& s = os->s;
+    s.meshes.resize(d->n_meshes);
+    for (uint32_t i = 0; i < d->n_meshes; i++) {
+        const rt_mesh_desc& md = d->meshes[i];
+        Mesh& m = s.meshes[i];
+        m.pos.assign(md.positions, md.positions + 3ull * md.n_vertices);
+        m.idx.assign(md.indices, md.indices + 3ull * md.n_triangles);
+        if (md.normals) m.nrm.assign(md.normals, md.normals + 3ull * md.n_vertices);
+        m.build();
+    }
+    s.instances.resize(d->n_instances);
+    std::vector<Aabb> ib(d->n_instances);
+    for (uint32_t i = 0; i < d->n_instances; i++) {
+        const rt_instance_desc& id = d->instances[i];
+        Instance& in = s.instances[i];
+        in.mesh_id = id.mesh_id;
+        in.material_id = id.material_id;
+        in.transform = identity();
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 4; c++) in.transform.m[r][c] = id.object_to_world[r * 4 + c];
+        if (!inverse(in.transform, in.inv)) in.inv = identity();  // mesh.rs:282
+        // mesh.rs:283-297 world bounds from the 8 transformed corners.
+        const Aabb& lb = s.meshes[in.mesh_id].local_bounds;
+        for (int k = 0; k < 8; k++) {
+            V3 corner{(k & 1) ? lb.mx.x : lb.mn.x, (k & 2) ? lb.mx.y : lb.mn.y, (k & 4) ? lb.mx.z : lb.mn.z};
+            in.world_bounds.grow_point(xf_point(in.transform, corner));
+        }
+        ib[i] = in.world_bounds;
+    }
+    s.tlas.build(ib);  // scene/mod.rs:82-86
+    for (uint32_t i = 0; i < d->n_materials; i++) {
+        s.materials.push_back(Pbr::from(d->materials[i]));
+        if (d->materials[i].presence < 1.0) s.any_presence = true;
+    }
+    for (uint32_t i = 0; i < d->n_lights; i++) s.lights.push_back(make_light(d->lights[i]));
+    s.ls.build(s.lights);
+    const rt_camera_desc& c = d->camera;
+    s.cam.width = c.width;
+    s.cam.height = c.height;
+    s.cam.fov = c.fov_deg;
+    s.cam.eye = v3(c.eye);
+    s.cam.forward = v3(c.forward);
+    s.cam.up = v3(c.up);
+    s.cam.right = v3(c.right);
+    s.cam.lens_radius = c.lens_radius;
+    s.cam.focal_distance = c.focal_distance;
+    s.cam.filter = c.filter;
+    s.cam.filter_width = c.filter_width;
+    s.background = v3(d->background);
+    return os;
+}
+
+void oracle_scene_destroy(oracle_scene* s) { delete s; }
+
+void oracle_scene_stats(const oracle_scene* os, uint64_t* blas_nodes, uint64_t* tlas_nodes) {
+    uint64_t b = 0;
+    for (auto& m : os->s.meshes) b += m.blas.nodes.size();
+    if (blas_nodes) *blas_nodes = b;
+    if (tlas_nodes) *tlas_nodes = os->s.tlas.nodes.size();
+}
+
+int oracle_intersect(const oracle_scene* os, const float* planes, uint64_t n, int any_hit, uint32_t* prim,
+                     uint32_t* inst, double* t, oracle_counters* counters, int threads) {
+    if (!os || !planes) return -1;
+    const Scene& s = os->s;
+    int nt = threads <= 0 ? (int)std::max(1u, std::thread::hardware_concurrency()) : threads;
+    std::vector<Counters> per(nt);
+    parallel_for(n, nt, [&](uint64_t b, uint64_t e, int tid) {
+        Counters& c = per[tid];
+        for (uint64_t i = b; i < e; i++) {
+            const float* po = planes + 4 * i;
+            const float* pd = planes + 4 * n + 4 * i;
+            V3 o{po[0], po[1], po[2]}, d{pd[0], pd[1], pd[2]};
+            double tmax = pd[3];
+            if (any_hit) {
+                bool h = s.occluded_param(o, d, tmax, &c);
+                if (prim) prim[i] = h ? 1u : 0u;
+            } else {
+                uint32_t ii = 0xFFFFFFFFu, pp = 0xFFFFFFFFu;
+                double tt = INF;
+                if (!s.intersect_param(o, d, tmax, &ii, &pp, &tt, &c)) {
+                    ii = pp = 0xFFFFFFFFu;
+                    tt = INF;
+                }
+                if (prim) prim[i] = pp;
+                if (inst) inst[i] = ii;
+                if (t) t[i] = tt;
+            }
+        }
+    });
+    if (counters) {
+        memset(counters, 0, sizeof(*counters));
+        for (auto& c : per) {
+            counters->node_pops += c.pops;
+            counters->tri_tests += c.tris;
+            counters->inst_tests += c.insts;
+        }
+        counters->rays = n;
+    }
+    return 0;
+}
+
+int oracle_render(const oracle_scene* os, const rt_params* p, const uint32_t* pixels, uint64_t n_pixels, uint32_t s0,
+                  uint32_t s1, double* rgb, double* aux_out, uint64_t* ray_counts, int threads) {
+    if (!os || !p || !pixels || !rgb) return -1;
+    const Scene& s = os->s;
+    int nt = threads <= 0 ? (int)std::max(1u, std::thread::hardware_concurrency()) : threads;
+    std::vector<uint64_t> ext(nt, 0), shd(nt, 0);
+    std::vector<std::array<uint64_t, 6>> work(nt, std::array<uint64_t, 6>{});
+    const double clampv = p->firefly_clamp;
+    parallel_for(n_pixels, nt, [&](uint64_t b, uint64_t e, int tid) {
+        Tracer tr{s, *p, 0, 0, Counters{}, Counters{}};
+        for (uint64_t k = b; k < e; k++) {
+            uint32_t pix = pixels[k];
+            uint32_t x = pix % s.cam.width, y = pix / s.cam.width;
+            V3 sum{0, 0, 0}, alb{0, 0, 0}, nrm{0, 0, 0}, dif{0, 0, 0};
+            double depth_sum = 0;
+            uint32_t hits = 0;
+            std::map<uint32_t, uint32_t> votes;
+            for (uint32_t smp = s0; smp < s1; smp++) {
+                // mod.rs:84-93 per-sample seeding, camera ray, clamp.
+                Pcg32 rng = Pcg32::for_pixel_sample(pix, smp);
+                double u1 = rng.next_f64(), u2 = rng.next_f64();
+                double px = x + 0.5 + s.cam.sample_1d(u1), py = y + 0.5 + s.cam.sample_1d(u2);
+                double lu = 0.5, lv = 0.5;
+                if (s.cam.lens_radius > 0.0) {
+                    lu = rng.next_f64();
+                    lv = rng.next_f64();
+                }
+                Ray ray = s.cam.generate(px, py, lu, lv);
+                Aux aux;
+                V3 l = tr.trace(ray, rng, aux);
+                double lm = lum(l);
+                if (lm > clampv) {
+                    double kk = clampv / lm;
+                    l = l * kk;
+                    aux.diffuse = aux.diffuse * kk;
+                }
+                sum = sum + l;
+                dif = dif + aux.diffuse;
+                alb = alb + aux.albedo;
+                nrm = nrm + aux.normal;
+                if (aux.depth > 0.0) {
+                    depth_sum += aux.depth;
+                    hits++;
+                }
+                votes[aux.id]++;
+            }
+            rgb[3 * k] = sum.x;
+            rgb[3 * k + 1] = sum.y;
+            rgb[3 * k + 2] = sum.z;
+            if (aux_out) {
+                double* a = aux_out + 12 * k;
+                uint32_t best_id = 0, best_n = 0;
+                for (auto& kv : votes)
+                    if (kv.second > best_n) {
+                        best_n = kv.second;
+                        best_id = kv.first;
+                    }
+                a[0] = alb.x; a[1] = alb.y; a[2] = alb.z;
+                a[3] = nrm.x; a[4] = nrm.y; a[5] = nrm.z;
+                a[6] = depth_sum;
+                a[7] = best_id;
+                a[8] = dif.x; a[9] = dif.y; a[10] = dif.z;
+                a[11] = hits;
+            }
+        }
+        ext[tid] += tr.ext_rays;
+        shd[tid] += tr.shadow_rays;
+        work[tid][0] += tr.cext.pops;
+        work[tid][1] += tr.cext.tris;
+        work[tid][2] += tr.cext.insts;
+        work[tid][3] += tr.cshadow.pops;
+        work[tid][4] += tr.cshadow.tris;
+        work[tid][5] += tr.cshadow.insts;
+    });
+    if (ray_counts) {
+        for (int k = 0; k < 8; k++) ray_counts[k] = 0;
+        for (int t = 0; t < nt; t++) {
+            ray_counts[0] += ext[t];
+            ray_counts[1] += shd[t];
+            for (int k = 0; k < 6; k++) ray_counts[2 + k] += work[t][k];
+        }
+    }
+    return 0;
+}
+
+void oracle_pcg_stream(uint64_t pixel, uint64_t sample, uint32_t n, uint32_t* out) {
+    Pcg32 r = Pcg32::for_pixel_sample(pixel, sample);
+    for (uint32_t i = 0; i < n; i++) out[i] = r.next_u32();
+}
+
+void oracle_pcg_new_stream(uint64_t seed, uint64_t stream, uint32_t n, uint32_t* out) {
+    Pcg32 r(seed, stream);
+    for (uint32_t i = 0; i < n; i++) out[i] = r.next_u32();
+}
+
+int oracle_bsdf_eval(const rt_material_desc* m, const double* wo, const double* wi, double eta, double* f_out,
+                     double* pdf_out) {
+    Pbr p = Pbr::from(*m);
+    V3 f;
+    double pdf;
+    eval_pdf(p, v3(wo), v3(wi), eta, &f, &pdf);
+    f_out[0] = f.x;
+    f_out[1] = f.y;
+    f_out[2] = f.z;
+    *pdf_out = pdf;
+    return 0;
+}
+
+double oracle_bsdf_furnace(const rt_material_desc* m, const double* wo, double eta, uint64_t n, uint64_t seed,
+                           uint64_t stream, double* rgb_out) {
+    Pbr p = Pbr::from(*m);
+    Pcg32 rng(seed, stream);
+    V3 w = v3(wo);
+    double acc = 0.0;
+    V3 acc3{0, 0, 0};
+    for (uint64_t i = 0; i < n; i++) {
+        BsdfSample s;
+        if (sample_bsdf(p, w, eta, rng, &s)) {
+            double k = std::fabs(s.wi.z) / s.pdf;
+            acc += lum(s.f) * k;
+            acc3 = acc3 + s.f * k;
+        }
+    }
+    if (rgb_out) {
+        rgb_out[0] = acc3.x / (double)n;
+        rgb_out[1] = acc3.y / (double)n;
+        rgb_out[2] = acc3.z / (double)n;
+    }
+    return acc / (double)n;
+}
+
+int oracle_light_sample(const oracle_scene* os, const double* p, double u, uint32_t* light, double* pmf) {
+    return os->s.ls.sample(v3(p), u, light, pmf) ? 1 : 0;
+}
+
+double oracle_light_pmf(const oracle_scene* os, const double* p, uint32_t light) { return os->s.ls.pmf(v3(p), light); }
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+/*
+ * pt_oracle.h — f64 CPU oracle for the render.rs path tracer.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library restates the reference's CPU path
+ * (anders94/render.rs, Rust, f64) so that tests, smoke() and the bench's
+ * cpu_baseline leg can check and time the CUDA backend against it. Nothing in
+ * the product links it; the CUDA backend never falls back to it.
+ *
+ * Sources restated (paths within the reference project):
+ *   src/raytracer/pt/sampler.rs      PCG32 + per-(pixel, sample) seeding
+ *   src/accel/bvh.rs                 binned-SAH BVH, traverse, any_hit
+ *   src/geometry/mesh.rs             Mesh, Möller–Trumbore, Instance
+ *   src/scene/mod.rs                 Scene::intersect (TLAS over instances)
+ *   src/scene/camera.rs              camera rays, pixel filters
+ *   src/scene/light.rs               light records
+ *   src/scene/light_sampler.rs       light BVH sample / pmf
+ *   src/scene/pbr.rs                 PbrParams, lobe weights
+ *   src/raytracer/pt/bxdf.rs         Oren-Nayar, GGX-VNDF, clearcoat, fuzz, glass
+ *   src/raytracer/pt/mod.rs          trace_full, sample_light, transmittance
+ * Out of scope (no config uses them): media, SSS, hair, textures/patterns,
+ * dome/IES lights, motion blur.
+ */
+#ifndef PT_ORACLE_H
+#define PT_ORACLE_H
+
+#include <stdint.h>
+#include "rt_scene.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_scene oracle_scene;
+
+/* Traversal work counters (reference binary BVH, both levels). */
+typedef struct oracle_counters {
+    uint64_t node_pops;      /* nodes popped from the traversal stack */
+    uint64_t tri_tests;      /* ray-triangle tests */
+    uint64_t inst_tests;     /* instance (TLAS leaf) visits */
+    uint64_t rays;
+} oracle_counters;
+
+oracle_scene* oracle_scene_create(const rt_scene_desc* desc);
+void          oracle_scene_destroy(oracle_scene* s);
+/* Binary BVH sizes: total BLAS nodes and TLAS nodes. */
+void          oracle_scene_stats(const oracle_scene* s, uint64_t* blas_nodes, uint64_t* tlas_nodes);
+
+/* Ray batch: planes[0..4n) = (ox,oy,oz,-) per ray, planes[4n..8n) =
+ * (dx,dy,dz,tmax). Directions are used as given; t is parametric.
+ * Closest hit: prim/inst = 0xFFFFFFFF on a miss. Any hit: prim = 1/0. */
+int oracle_intersect(const oracle_scene* s, const float* planes, uint64_t n, int any_hit,
+                     uint32_t* prim, uint32_t* inst, double* t, oracle_counters* counters,
+                     int threads);
+
+/* Render samples [s0, s1) for the listed pixel indices (y*W + x).
+ * rgb: 3 doubles per listed pixel (radiance SUM over the samples, each
+ * sample firefly-clamped). aux (optional): 12 doubles per listed pixel in
+ * the reference's GPU AOV layout (0-2 albedo sum, 3-5 normal sum, 6 depth
+ * sum, 7 id, 8-10 diffuse sum, 11 hit count); the id is the majority vote
+ * of the CPU film path. ray_counts (optional, 8 x u64): extension rays,
+ * shadow rays, then node pops / triangle tests / instance visits of the
+ * extension rays, then the same three for the shadow rays. */
+int oracle_render(const oracle_scene* s, const rt_params* p, const uint32_t* pixels,
+                  uint64_t n_pixels, uint32_t s0, uint32_t s1, double* rgb, double* aux,
+                  uint64_t* ray_counts, int threads);
+
+/* First n u32 outputs of Pcg32::for_pixel_sample(pixel, sample). */
+void oracle_pcg_stream(uint64_t pixel, uint64_t sample, uint32_t n, uint32_t* out);
+/* First n u32 outputs of Pcg32::new(seed, stream). */
+void oracle_pcg_new_stream(uint64_t seed, uint64_t stream, uint32_t n, uint32_t* out);
+
+/* BSDF helpers for lobe tests. wo is local (z = shading normal). */
+int oracle_bsdf_eval(const rt_material_desc* m, const double* wo, const double* wi,
+                     double eta, double* f_out, double* pdf_out);
+/* Furnace: mean of lum(f)*|cos|/pdf over n BSDF samples from Pcg32::new(seed, stream). */
+double oracle_bsdf_furnace(const rt_material_desc* m, const double* wo, double eta,
+                           uint64_t n, uint64_t seed, uint64_t stream, double* rgb_out);
+
+/* Light BVH queries. */
+int    oracle_light_sample(const oracle_scene* s, const double* p, double u,
+                           uint32_t* light, double* pmf);
+double oracle_light_pmf(const oracle_scene* s, const double* p, uint32_t light);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

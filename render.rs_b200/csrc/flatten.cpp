@@ -1,0 +1,670 @@
+// flatten.cpp — scene flattening for the CUDA backend (host, C++17).
+//
+// 1. Binary BVHs are built with the reference's binned-SAH rules
+//    (src/accel/bvh.rs:96-108, 256-345: 16 bins on the widest centroid axis,
+//    leaves of <= 4 primitives or <= 16 when SAH prefers a leaf, median
+//    fallback, the same in-place partition), so the GPU sees the same tree
+//    the reference's CPU path traverses.
+// 2. Each binary tree is collapsed into 8-wide nodes (the child with the
+//    largest surface area is opened until 8 children), and the child boxes
+//    are quantised to 8 bits per plane against a per-node power-of-two grid
+//    chosen so every decoded plane p + q * 2^e is exactly representable in
+//    f32 and never inside the true box (conservative).
+// 3. The light BVH follows src/scene/light_sampler.rs:97-141, 242-312.
+// 4. Materials are folded to f32 constants as src/raytracer/pt/bxdf.rs and
+//    src/scene/pbr.rs evaluate them.
+
+#include "flatten.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+namespace rt {
+
+namespace {
+
+const double PI = 3.14159265358979323846;
+const double INF = std::numeric_limits<double>::infinity();
+
+struct Box {
+    double lo[3] = {INF, INF, INF};
+    double hi[3] = {-INF, -INF, -INF};
+    void grow_pt(const double* p) {
+        for (int a = 0; a < 3; a++) {
+            lo[a] = std::fmin(lo[a], p[a]);
+            hi[a] = std::fmax(hi[a], p[a]);
+        }
+    }
+    void grow(const Box& b) {
+        grow_pt(b.lo);
+        grow_pt(b.hi);
+    }
+    double area() const {
+        double d0 = hi[0] - lo[0], d1 = hi[1] - lo[1], d2 = hi[2] - lo[2];
+        if (d0 < 0 || d1 < 0 || d2 < 0) return 0.0;
+        return 2.0 * (d0 * d1 + d1 * d2 + d2 * d0);
+    }
+};
+
+struct BinNode {
+    Box b;
+    uint32_t first = 0, count = 0;  // interior: first = left child index, count = 0
+};
+
+struct BinBvh {
+    std::vector<BinNode> nodes;
+    std::vector<uint32_t> order;
+};
+
+// Binned SAH with the reference's split rules and node numbering.
+BinBvh build_binary(const std::vector<Box>& bounds) {
+    const int BINS = 16, MAX_LEAF = 4;
+    BinBvh t;
+    size_t n = bounds.size();
+    t.order.resize(n);
+    for (size_t i = 0; i < n; i++) t.order[i] = (uint32_t)i;
+    if (n == 0) return t;
+    std::vector<double> cen(3 * n);
+    for (size_t i = 0; i < n; i++)
+        for (int a = 0; a < 3; a++) cen[3 * i + a] = (bounds[i].lo[a] + bounds[i].hi[a]) * 0.5;
+    t.nodes.reserve(2 * n / 3 + 8);
+    t.nodes.push_back(BinNode{});
+    struct Job { size_t node, start, count; };
+    std::vector<Job> stack{{0, 0, n}};
+    uint32_t* ord = t.order.data();
+    while (!stack.empty()) {
+        Job j = stack.back();
+        stack.pop_back();
+        Box b, cb;
+        for (size_t i = j.start; i < j.start + j.count; i++) {
+            b.grow(bounds[ord[i]]);
+            cb.grow_pt(&cen[3 * ord[i]]);
+        }
+        t.nodes[j.node].b = b;
+        auto make_leaf = [&]() {
+            t.nodes[j.node].first = (uint32_t)j.start;
+            t.nodes[j.node].count = (uint32_t)j.count;
+        };
+        if (j.count <= (size_t)MAX_LEAF) {
+            make_leaf();
+            continue;
+        }
+        double ext[3] = {cb.hi[0] - cb.lo[0], cb.hi[1] - cb.lo[1], cb.hi[2] - cb.lo[2]};
+        int axis = (ext[0] >= ext[1] && ext[0] >= ext[2]) ? 0 : (ext[1] >= ext[2] ? 1 : 2);
+        double amin = cb.lo[axis], aext = ext[axis];
+        size_t split = j.start + j.count / 2;
+        if (aext > 1e-12) {
+            Box bb[BINS];
+            size_t bc[BINS] = {0};
+            double scale = (double)BINS / aext;
+            for (size_t i = j.start; i < j.start + j.count; i++) {
+                double f = (cen[3 * ord[i] + axis] - amin) * scale;
+                size_t k = f > 0.0 ? (size_t)f : 0;
+                if (k > (size_t)BINS - 1) k = BINS - 1;
+                bc[k]++;
+                bb[k].grow(bounds[ord[i]]);
+            }
+            Box racc[BINS], acc;
+            for (int i = BINS - 1; i >= 1; i--) {
+                acc.grow(bb[i]);
+                racc[i] = acc;
+            }
+            double best = INF;
+            int best_bin = 0;
+            Box left;
+            size_t lc = 0;
+            for (int i = 0; i < BINS - 1; i++) {
+                left.grow(bb[i]);
+                lc += bc[i];
+                size_t rc = j.count - lc;
+                if (lc == 0 || rc == 0) continue;
+                double cost = left.area() * (double)lc + racc[i + 1].area() * (double)rc;
+                if (cost < best) {
+                    best = cost;
+                    best_bin = i;
+                }
+            }
+            double leaf_cost = b.area() * (double)j.count;
+            if (std::isfinite(best) && best < leaf_cost) {
+                double boundary = amin + aext * (double)(best_bin + 1) / (double)BINS;
+                size_t m = 0;
+                for (size_t q = 0; q < j.count; q++) {
+                    if (cen[3 * ord[j.start + q] + axis] < boundary) {
+                        std::swap(ord[j.start + m], ord[j.start + q]);
+                        m++;
+                    }
+                }
+                if (m > 0 && m < j.count) split = j.start + m;
+            } else if (j.count <= (size_t)MAX_LEAF * 4) {
+                make_leaf();
+                continue;
+            }
+        }
+        size_t l = t.nodes.size();
+        t.nodes.push_back(BinNode{});
+        t.nodes.push_back(BinNode{});
+        t.nodes[j.node].first = (uint32_t)l;
+        t.nodes[j.node].count = 0;
+        stack.push_back({l + 1, split, j.start + j.count - split});
+        stack.push_back({l, j.start, split - j.start});
+    }
+    return t;
+}
+
+// Per-node quantisation grid: origin p (multiple of s = 2^e) and e such that
+// every p + q*s (q in 0..255) is an exact f32 and p + 255*s >= box hi.
+void choose_grid(double lo, double hi, float* p_out, int* e_out) {
+    if (!(hi >= lo)) hi = lo;
+    double maxabs = std::fmax(std::fabs(lo), std::fabs(hi));
+    int e_ulp = -149;
+    if (maxabs > 0) e_ulp = (int)std::floor(std::log2(maxabs)) - 23 + 4;
+    double extent = hi - lo;
+    int e = extent > 0 ? (int)std::ceil(std::log2(extent / 255.0)) : -126;
+    e = std::max(std::max(e, e_ulp), -126);
+    for (;;) {
+        double s = std::ldexp(1.0, e);
+        double p = std::floor(lo / s) * s;
+        if ((hi - p) / s <= 255.0 && (float)p == p) {
+            *p_out = (float)p;
+            *e_out = e;
+            return;
+        }
+        e++;
+    }
+}
+
+struct Collapser {
+    const BinBvh& bin;
+    std::vector<uint4>& out;
+    uint32_t prim_base;
+    uint64_t emitted = 0;
+
+    uint32_t leaf_ref(const BinNode& nd) const { return make_leaf_ref(prim_base + nd.first, nd.count); }
+
+    // Emit the wide node covering binary node `bi`; returns its index.
+    uint32_t emit(uint32_t bi) {
+        const BinNode& root = bin.nodes[bi];
+        uint32_t kids[8];
+        int nk = 0;
+        if (root.count > 0) {
+            kids[nk++] = bi;  // a lone leaf becomes a one-child wide node
+        } else {
+            kids[nk++] = root.first;
+            kids[nk++] = root.first + 1;
+            while (nk < 8) {
+                int best = -1;
+                double best_a = -1.0;
+                for (int k = 0; k < nk; k++) {
+                    const BinNode& c = bin.nodes[kids[k]];
+                    if (c.count == 0 && c.b.area() > best_a) {
+                        best_a = c.b.area();
+                        best = k;
+                    }
+                }
+                if (best < 0) break;
+                uint32_t open = kids[best];
+                kids[best] = bin.nodes[open].first;
+                kids[nk++] = bin.nodes[open].first + 1;
+            }
+        }
+        uint32_t idx = (uint32_t)(out.size() / WIDE_NODE_WORDS);
+        out.resize(out.size() + WIDE_NODE_WORDS);
+        emitted++;
+        uint32_t refs[8];
+        for (int k = 0; k < 8; k++) refs[k] = REF_EMPTY;
+        for (int k = 0; k < nk; k++) {
+            const BinNode& c = bin.nodes[kids[k]];
+            refs[k] = c.count > 0 ? leaf_ref(c) : emit(kids[k]);
+        }
+        // Node box = union of children boxes.
+        Box nb;
+        for (int k = 0; k < nk; k++) nb.grow(bin.nodes[kids[k]].b);
+        float p[3];
+        int e[3];
+        for (int a = 0; a < 3; a++) choose_grid(nb.lo[a], nb.hi[a], &p[a], &e[a]);
+        uint8_t qlo[3][8], qhi[3][8];
+        for (int k = 0; k < 8; k++)
+            for (int a = 0; a < 3; a++) {
+                qlo[a][k] = 255;
+                qhi[a][k] = 0;
+            }
+        for (int k = 0; k < nk; k++) {
+            const Box& cbx = bin.nodes[kids[k]].b;
+            for (int a = 0; a < 3; a++) {
+                double s = std::ldexp(1.0, e[a]);
+                double ql = std::floor((cbx.lo[a] - (double)p[a]) / s);
+                double qh = std::ceil((cbx.hi[a] - (double)p[a]) / s);
+                ql = std::min(std::max(ql, 0.0), 255.0);
+                qh = std::min(std::max(qh, 0.0), 255.0);
+                // Conservative by construction; widen if rounding ever bit.
+                while (ql > 0 && (double)p[a] + ql * s > cbx.lo[a]) ql -= 1;
+                while (qh < 255 && (double)p[a] + qh * s < cbx.hi[a]) qh += 1;
+                qlo[a][k] = (uint8_t)ql;
+                qhi[a][k] = (uint8_t)qh;
+            }
+        }
+        uint4* w = &out[(size_t)idx * WIDE_NODE_WORDS];
+        uint32_t pb[3];
+        memcpy(pb, p, sizeof(pb));
+        w[0] = make_uint4(pb[0], pb[1], pb[2],
+                          (uint32_t)(e[0] + 127) | ((uint32_t)(e[1] + 127) << 8) | ((uint32_t)(e[2] + 127) << 16) |
+                              ((uint32_t)nk << 24));
+        auto pack4 = [](const uint8_t* b) {
+            return (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) | ((uint32_t)b[3] << 24);
+        };
+        w[1] = make_uint4(pack4(qlo[0]), pack4(qlo[0] + 4), pack4(qlo[1]), pack4(qlo[1] + 4));
+        w[2] = make_uint4(pack4(qlo[2]), pack4(qlo[2] + 4), pack4(qhi[0]), pack4(qhi[0] + 4));
+        w[3] = make_uint4(pack4(qhi[1]), pack4(qhi[1] + 4), pack4(qhi[2]), pack4(qhi[2] + 4));
+        w[4] = make_uint4(refs[0], refs[1], refs[2], refs[3]);
+        w[5] = make_uint4(refs[4], refs[5], refs[6], refs[7]);
+        return idx;
+    }
+};
+
+inline double lum(const double* c) { return 0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2]; }
+
+// Affine 3x4 inverse in f64; identity when |det| < 1e-6 as the reference's
+// Matrix4::inverse().unwrap_or(identity) (src/geometry/mesh.rs:282).
+void affine_inverse(const double* m, double* inv) {
+    double a = m[0], b = m[1], c = m[2], d = m[4], e = m[5], f = m[6], g = m[8], h = m[9], i = m[10];
+    double A = e * i - f * h, B = -(d * i - f * g), Cc = d * h - e * g;
+    double det = a * A + b * B + c * Cc;
+    if (std::fabs(det) < 1e-6) {
+        static const double id[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};
+        memcpy(inv, id, sizeof(id));
+        return;
+    }
+    double r[9] = {A, -(b * i - c * h), b * f - c * e, B, a * i - c * g, -(a * f - c * d), Cc, -(a * h - b * g),
+                   a * e - b * d};
+    for (int k = 0; k < 9; k++) r[k] /= det;
+    double t[3] = {m[3], m[7], m[11]};
+    for (int row = 0; row < 3; row++) {
+        inv[row * 4 + 0] = r[row * 3 + 0];
+        inv[row * 4 + 1] = r[row * 3 + 1];
+        inv[row * 4 + 2] = r[row * 3 + 2];
+        inv[row * 4 + 3] = -(r[row * 3 + 0] * t[0] + r[row * 3 + 1] * t[1] + r[row * 3 + 2] * t[2]);
+    }
+}
+
+void xf_point(const double* m, const double* p, double* o) {
+    for (int r = 0; r < 3; r++) o[r] = m[r * 4] * p[0] + m[r * 4 + 1] * p[1] + m[r * 4 + 2] * p[2] + m[r * 4 + 3];
+}
+
+DevMaterial fold_material(const rt_material_desc& m) {
+    DevMaterial d;
+    memset(&d, 0, sizeof(d));
+    // PbrParams::specular_f0 (pbr.rs:86-96)
+    double f0[3] = {0, 0, 0};
+    if (lum(m.specular_face_color) > 1e-6) {
+        for (int k = 0; k < 3; k++) f0[k] = m.specular_face_color[k];
+    } else if (m.specular_ior > 1.0) {
+        double r = (m.specular_ior - 1.0) / (m.specular_ior + 1.0);
+        for (int k = 0; k < 3; k++) f0[k] = r * r;
+    }
+    bool has_spec = lum(f0) > 1e-6;
+    // lobe_weights (pbr.rs:188-201)
+    double wd = m.diffuse_gain * lum(m.diffuse_color);
+    double ws = std::sqrt(lum(f0));
+    double wc = m.clearcoat_gain * 0.2;
+    double wf = m.fuzz_gain * lum(m.fuzz_color) * 0.3;
+    double wg = m.glass_gain;
+    double total = wd + ws + wc + wf + wg;
+    bool lobes = total > 1e-9;
+    if (lobes) {
+        d.w_diff = (float)(wd / total);
+        d.w_spec = (float)(ws / total);
+        d.w_coat = (float)(wc / total);
+        d.w_fuzz = (float)(wf / total);
+        d.w_glass = (float)(wg / total);
+    }
+    d.has_lobes = lobes ? 1.0f : 0.0f;
+    // under_layer_scale (bxdf.rs:137-143)
+    double uls = std::min(std::max((1.0 - lum(f0)) * (1.0 - 0.04 * m.clearcoat_gain), 0.0), 1.0);
+    double sigma2 = m.diffuse_roughness * m.diffuse_roughness;
+    d.on_a = (float)(1.0 - sigma2 / (2.0 * (sigma2 + 0.33)));
+    d.on_b = (float)(0.45 * sigma2 / (sigma2 + 0.09));
+    auto alpha_of = [](double r) { return std::min(std::max(r * r, 2.5e-5), 1.0); };
+    d.alpha_spec = (float)alpha_of(m.specular_roughness);
+    d.alpha_coat = (float)alpha_of(m.clearcoat_roughness);
+    d.alpha_glass = (float)alpha_of(m.glass_roughness);
+    d.coat_gain = (float)m.clearcoat_gain;
+    d.glass_scale = (float)(m.glass_gain * uls);
+    d.ior = (float)m.glass_ior;
+    d.presence = (float)std::min(std::max(m.presence, 0.0), 1.0);
+    double alb[3];
+    for (int k = 0; k < 3; k++) {
+        d.kd[k] = (float)(m.diffuse_color[k] * m.diffuse_gain * uls / PI);
+        d.f0[k] = (float)f0[k];
+        d.f90[k] = (float)m.specular_edge_color[k];
+        d.kfuzz[k] = (float)(m.fuzz_color[k] * m.fuzz_gain / PI);
+        d.refr[k] = (float)m.refraction_color[k];
+        d.emission[k] = (float)(m.emission[k] + m.glow[k]);
+        alb[k] = m.diffuse_color[k] * m.diffuse_gain + f0[k] * (has_spec ? 1.0 : 0.0) +
+                 m.refraction_color[k] * m.glass_gain;
+        d.albedo[k] = (float)std::fmin(alb[k], 1.0);
+    }
+    d.area_light = m.area_light;
+    d.id = m.id;
+    if (!lobes) d.mclass = MAT_EMITTER;
+    else if (wd > 0 && ws == 0 && wc == 0 && wf == 0 && wg == 0) d.mclass = MAT_DIFFUSE;
+    else if (ws > 0 && wd == 0 && wc == 0 && wf == 0 && wg == 0) d.mclass = MAT_CONDUCTOR;
+    else if (wg > 0 && wd == 0 && ws == 0 && wc == 0 && wf == 0) d.mclass = MAT_GLASS;
+    else d.mclass = MAT_MIXED;
+    return d;
+}
+
+// Light BVH (light_sampler.rs:242-312): median split on the widest axis of
+// the light-extent box, stable sort by centre along that axis.
+struct LEntry {
+    uint32_t light;
+    double c[3], radius, power;
+};
+
+uint32_t lbvh_build(std::vector<LightNode>& nodes, std::vector<uint32_t>& leaf_of, const std::vector<LEntry>& e,
+                    std::vector<size_t>& order, size_t s, size_t t, uint32_t parent) {
+    uint32_t index = (uint32_t)nodes.size();
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    double power = 0;
+    for (size_t k = s; k < t; k++) {
+        const LEntry& en = e[order[k]];
+        for (int a = 0; a < 3; a++) {
+            mn[a] = std::fmin(mn[a], (float)(en.c[a] - en.radius));
+            mx[a] = std::fmax(mx[a], (float)(en.c[a] + en.radius));
+        }
+        power += en.power;
+    }
+    LightNode nd;
+    memset(&nd, 0, sizeof(nd));
+    for (int a = 0; a < 3; a++) {
+        nd.mn[a] = mn[a];
+        nd.mx[a] = mx[a];
+    }
+    nd.power = (float)power;
+    nd.parent = parent;
+    nd.b = 0xFFFFFFFFu;
+    nodes.push_back(nd);
+    if (t - s == 1) {
+        uint32_t l = e[order[s]].light;
+        nodes[index].a = l;
+        leaf_of[l] = index;
+        return index;
+    }
+    int axis = 0;
+    float widest = -1.0f;
+    for (int a = 0; a < 3; a++)
+        if (mx[a] - mn[a] > widest) {
+            widest = mx[a] - mn[a];
+            axis = a;
+        }
+    size_t mid = (s + t) / 2;
+    std::stable_sort(order.begin() + s, order.begin() + t,
+                     [&](size_t x, size_t y) { return e[x].c[axis] < e[y].c[axis]; });
+    uint32_t a = lbvh_build(nodes, leaf_of, e, order, s, mid, index);
+    uint32_t b = lbvh_build(nodes, leaf_of, e, order, mid, t, index);
+    nodes[index].a = a;
+    nodes[index].b = b;
+    return index;
+}
+
+}  // namespace
+
+DevMaterial fold_material_public(const rt_material_desc& m) { return fold_material(m); }
+
+bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
+    HostScene& H = *out;
+    if (!d) {
+        *err = "null scene descriptor";
+        return false;
+    }
+    if (d->camera.width == 0 || d->camera.height == 0) {
+        *err = "camera has zero width or height";
+        return false;
+    }
+    if (d->n_meshes && !d->meshes) {
+        *err = "meshes pointer is NULL";
+        return false;
+    }
+    // ---- BLAS per mesh -------------------------------------------------
+    std::vector<Box> local_bounds(d->n_meshes);
+    H.meshes.resize(d->n_meshes);
+    uint64_t tri_total = 0;
+    for (uint32_t m = 0; m < d->n_meshes; m++) tri_total += d->meshes[m].n_triangles;
+    if (tri_total >= (1ull << 27)) {
+        *err = "more than 2^27 unique triangles";
+        return false;
+    }
+    H.tris.reserve(3 * tri_total);
+    for (uint32_t m = 0; m < d->n_meshes; m++) {
+        const rt_mesh_desc& md = d->meshes[m];
+        if (md.n_triangles && (!md.positions || !md.indices)) {
+            *err = "mesh " + std::to_string(m) + " has NULL positions or indices";
+            return false;
+        }
+        std::vector<Box> tb(md.n_triangles);
+        for (uint32_t t = 0; t < md.n_triangles; t++) {
+            Box b;
+            for (int k = 0; k < 3; k++) {
+                uint32_t vi = md.indices[3ull * t + k];
+                if (vi >= md.n_vertices) {
+                    *err = "mesh " + std::to_string(m) + " index out of range";
+                    return false;
+                }
+                double p[3] = {md.positions[3ull * vi], md.positions[3ull * vi + 1], md.positions[3ull * vi + 2]};
+                if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) {
+                    *err = "mesh " + std::to_string(m) + " has a non-finite vertex";
+                    return false;
+                }
+                b.grow_pt(p);
+            }
+            tb[t] = b;
+            local_bounds[m].grow(b);
+        }
+        BinBvh bin = build_binary(tb);
+        H.binary_blas_nodes += bin.nodes.size();
+        MeshInfo& mi = H.meshes[m];
+        mi.n_tris = md.n_triangles;
+        mi.tri_base = (uint32_t)(H.tris.size() / 3);
+        mi.idx_base = 0xFFFFFFFFu;
+        if (md.normals) {
+            mi.idx_base = (uint32_t)H.orig_idx.size();
+            uint32_t vbase = (uint32_t)(H.normals.size() / 3);
+            for (uint64_t k = 0; k < 3ull * md.n_triangles; k++) H.orig_idx.push_back(vbase + md.indices[k]);
+            H.normals.insert(H.normals.end(), md.normals, md.normals + 3ull * md.n_vertices);
+        }
+        for (uint32_t k = 0; k < md.n_triangles; k++) {
+            uint32_t t = bin.order[k];
+            float4 v[3];
+            for (int c = 0; c < 3; c++) {
+                uint32_t vi = md.indices[3ull * t + c];
+                v[c] = make_float4(md.positions[3ull * vi], md.positions[3ull * vi + 1], md.positions[3ull * vi + 2],
+                                   0.0f);
+            }
+            uint32_t tid = t;
+            memcpy(&v[0].w, &tid, 4);
+            H.tris.push_back(v[0]);
+            H.tris.push_back(v[1]);
+            H.tris.push_back(v[2]);
+        }
+        if (md.n_triangles == 0) {
+            mi.blas_root = 0xFFFFFFFFu;
+            continue;
+        }
+        Collapser col{bin, H.nodes, mi.tri_base};
+        mi.blas_root = col.emit(0);
+        H.blas_nodes += col.emitted;
+    }
+    // ---- instances + TLAS ------------------------------------------------
+    if (d->n_instances && !d->instances) {
+        *err = "instances pointer is NULL";
+        return false;
+    }
+    std::vector<Box> ib(d->n_instances);
+    std::vector<double> invs(12ull * d->n_instances);
+    for (uint32_t i = 0; i < d->n_instances; i++) {
+        const rt_instance_desc& id = d->instances[i];
+        if (id.mesh_id >= d->n_meshes || id.material_id >= d->n_materials) {
+            *err = "instance " + std::to_string(i) + " references a missing mesh or material";
+            return false;
+        }
+        affine_inverse(id.object_to_world, &invs[12ull * i]);
+        const Box& lb = local_bounds[id.mesh_id];
+        Box wb;
+        if (d->meshes[id.mesh_id].n_triangles) {
+            for (int k = 0; k < 8; k++) {
+                double c[3] = {(k & 1) ? lb.hi[0] : lb.lo[0], (k & 2) ? lb.hi[1] : lb.lo[1],
+                               (k & 4) ? lb.hi[2] : lb.lo[2]};
+                double w[3];
+                xf_point(id.object_to_world, c, w);
+                wb.grow_pt(w);
+            }
+        }
+        ib[i] = wb;
+    }
+    H.tlas_nodes = 0;
+    H.scalars.tlas_root = 0xFFFFFFFFu;
+    if (d->n_instances) {
+        // Empty meshes get a degenerate far-away box so the TLAS never enters them.
+        for (auto& b : ib)
+            if (!(b.hi[0] >= b.lo[0])) {
+                double far[3] = {1e30, 1e30, 1e30};
+                b = Box();
+                b.grow_pt(far);
+            }
+        BinBvh tl = build_binary(ib);
+        Collapser col{tl, H.nodes, 0};
+        H.scalars.tlas_root = col.emit(0);
+        H.tlas_nodes = col.emitted;
+        H.inst_xf.resize(3ull * d->n_instances);
+        H.inst.resize(d->n_instances);
+        for (uint32_t k = 0; k < d->n_instances; k++) {
+            uint32_t i = tl.order[k];
+            const double* v = &invs[12ull * i];
+            for (int r = 0; r < 3; r++)
+                H.inst_xf[3ull * k + r] =
+                    make_float4((float)v[r * 4], (float)v[r * 4 + 1], (float)v[r * 4 + 2], (float)v[r * 4 + 3]);
+            const rt_instance_desc& id = d->instances[i];
+            H.inst[k] = make_uint4(H.meshes[id.mesh_id].blas_root, i, id.material_id, id.mesh_id);
+        }
+    }
+    H.scalars.n_instances = d->n_instances;
+    // ---- materials ---------------------------------------------------------
+    if (d->n_materials && !d->materials) {
+        *err = "materials pointer is NULL";
+        return false;
+    }
+    H.scalars.any_presence = 0;
+    for (uint32_t m = 0; m < d->n_materials; m++) {
+        const rt_material_desc& md = d->materials[m];
+        if (md.area_light >= (int32_t)d->n_lights) {
+            *err = "material " + std::to_string(m) + " names a missing area light";
+            return false;
+        }
+        H.materials.push_back(fold_material(md));
+        if (md.presence < 1.0) H.scalars.any_presence = 1;
+    }
+    // ---- lights + light BVH --------------------------------------------------
+    if (d->n_lights && !d->lights) {
+        *err = "lights pointer is NULL";
+        return false;
+    }
+    std::vector<LEntry> finite;
+    H.light_leaf.assign(d->n_lights, 0xFFFFFFFFu);
+    double inf_total = 0;
+    for (uint32_t l = 0; l < d->n_lights; l++) {
+        const rt_light_desc& ld = d->lights[l];
+        DevLight dl;
+        memset(&dl, 0, sizeof(dl));
+        dl.type = (uint32_t)ld.type;
+        double rad[3];
+        for (int k = 0; k < 3; k++) {
+            rad[k] = ld.color[k] * ld.intensity;
+            dl.radiance[k] = (float)rad[k];
+            dl.p[k] = (float)ld.p[k];
+            dl.e1[k] = (float)ld.e1[k];
+            dl.e2[k] = (float)ld.e2[k];
+        }
+        dl.radius = (float)ld.radius;
+        double pw = std::fmax(lum(rad), 1e-9);
+        double cx[3] = {ld.e1[1] * ld.e2[2] - ld.e1[2] * ld.e2[1], ld.e1[2] * ld.e2[0] - ld.e1[0] * ld.e2[2],
+                        ld.e1[0] * ld.e2[1] - ld.e1[1] * ld.e2[0]};
+        double cl = std::sqrt(cx[0] * cx[0] + cx[1] * cx[1] + cx[2] * cx[2]);
+        double l1 = std::sqrt(ld.e1[0] * ld.e1[0] + ld.e1[1] * ld.e1[1] + ld.e1[2] * ld.e1[2]);
+        double l2 = std::sqrt(ld.e2[0] * ld.e2[0] + ld.e2[1] * ld.e2[1] + ld.e2[2] * ld.e2[2]);
+        LEntry en{l, {ld.p[0], ld.p[1], ld.p[2]}, 0.0, 0.0};
+        switch (ld.type) {
+            case RT_LIGHT_POINT: en.power = pw * 4.0 * PI; finite.push_back(en); break;
+            case RT_LIGHT_RECT:
+                dl.area = (float)cl;
+                for (int k = 0; k < 3; k++) {
+                    dl.n[k] = (float)(cl > 1e-6 ? cx[k] / cl : cx[k]);
+                    en.c[k] = ld.p[k] + ld.e1[k] * 0.5 + ld.e2[k] * 0.5;
+                }
+                en.radius = (l1 + l2) * 0.5;
+                en.power = pw * cl * PI;
+                finite.push_back(en);
+                break;
+            case RT_LIGHT_SPHERE:
+                en.radius = ld.radius;
+                en.power = pw * 4.0 * PI * ld.radius * ld.radius * PI;
+                finite.push_back(en);
+                break;
+            case RT_LIGHT_DISK: {
+                double area = PI * l1 * l2;
+                dl.area = (float)area;
+                for (int k = 0; k < 3; k++) dl.n[k] = (float)(cl > 1e-6 ? cx[k] / cl : cx[k]);
+                en.radius = l1;
+                en.power = pw * area * PI;
+                finite.push_back(en);
+                break;
+            }
+            case RT_LIGHT_DISTANT: {
+                double dn = l1 > 1e-6 ? l1 : 1.0;
+                for (int k = 0; k < 3; k++) dl.e1[k] = (float)(ld.e1[k] / dn);
+                dl.cos_max = (float)std::cos(ld.radius);
+                H.inf_lights.push_back(l);
+                H.inf_power.push_back((float)(pw * 4.0 * PI));
+                inf_total += pw * 4.0 * PI;
+                break;
+            }
+            default: *err = "light " + std::to_string(l) + " has an unknown type"; return false;
+        }
+        H.lights.push_back(dl);
+    }
+    double finite_total = 0;
+    for (auto& e : finite) finite_total += e.power;
+    if (!finite.empty()) {
+        std::vector<size_t> order(finite.size());
+        for (size_t k = 0; k < order.size(); k++) order[k] = k;
+        lbvh_build(H.lbvh, H.light_leaf, finite, order, 0, finite.size(), 0xFFFFFFFFu);
+    }
+    H.scalars.n_lights = d->n_lights;
+    H.scalars.n_lbvh = (uint32_t)H.lbvh.size();
+    H.scalars.n_inf = (uint32_t)H.inf_lights.size();
+    H.scalars.inf_total = (float)inf_total;
+    H.scalars.p_infinite = H.inf_lights.empty() ? 0.0f
+                           : finite.empty()     ? 1.0f
+                                                : (float)std::min(std::max(inf_total / (inf_total + finite_total), 0.1), 0.9);
+    // ---- camera (camera.rs:150-179) ------------------------------------------
+    const rt_camera_desc& c = d->camera;
+    for (int k = 0; k < 3; k++) {
+        H.scalars.eye[k] = (float)c.eye[k];
+        H.scalars.fwd[k] = (float)c.forward[k];
+        H.scalars.right[k] = (float)c.right[k];
+        H.scalars.up[k] = (float)c.up[k];
+        H.scalars.background[k] = (float)d->background[k];
+    }
+    double half_h = std::tan(c.fov_deg * PI / 180.0 / 2.0);
+    H.scalars.half_h = (float)half_h;
+    H.scalars.half_w = (float)((double)c.width / (double)c.height * half_h);
+    H.scalars.lens_radius = (float)c.lens_radius;
+    H.scalars.focal_distance = (float)c.focal_distance;
+    H.scalars.filter = (uint32_t)c.filter;
+    H.scalars.filter_width = (float)c.filter_width;
+    H.scalars.width = c.width;
+    H.scalars.height = c.height;
+    return true;
+}
+
+}  // namespace rt

@@ -1,0 +1,674 @@
+// pt_kernels.cuh — wavefront path-tracing kernels.
+//
+// One slab = P path slots = k whole sample passes over the image
+// (slot = s_local * npix + pixel). Per wave:
+//   extend   closest hit for the queued slots, then push each slot onto the
+//            queue of its hit's material class (miss, diffuse, conductor,
+//            glass, mixed, emitter) with warp-aggregated atomics;
+//   shade    classes in order, so warps see one BSDF: emission with MIS,
+//            presence skip, NEE light pick + sample (shadow ray queued with
+//            its contribution), BSDF sample, Russian roulette, next ray;
+//   shadow   any hit (or the presence-attenuating closest-hit loop) and,
+//            when visible, add the queued contribution to the slot's L.
+// accumulate then clamps each sample (firefly) and adds it to the f64
+// per-pixel accumulator in sample order, so the image is bitwise
+// reproducible for a seed whatever order the queues were filled in.
+//
+// Reference: trace_full (src/raytracer/pt/mod.rs:449-990), sample_light
+// (:1032-1209), transmittance (:1254-1306), render/render_sum (:71-133);
+// the Metal wavefront it replaces is kernel_wf.metal:155-325.
+#pragma once
+
+#include "shade.cuh"
+
+namespace rt {
+
+enum : uint32_t { CLS_MISS = N_MAT_CLASSES, N_QUEUES = N_MAT_CLASSES + 1 };
+
+// Counter words (uint32) in Paths::cnt.
+enum : uint32_t {
+    CNT_EXT_IN = 0,
+    CNT_EXT_OUT = 1,
+    CNT_SHADOW = 2,
+    CNT_CLASS = 3,                  // N_QUEUES words
+    CNT_FETCH_EXT = CNT_CLASS + N_QUEUES,
+    CNT_FETCH_SH = CNT_FETCH_EXT + 1,
+    CNT_WORDS = 16
+};
+
+struct Paths {
+    float4* ray_o;    // origin xyz
+    float4* ray_d;    // direction xyz, w = tmax
+    uint4* hit;       // t bits, tri (leaf order), inst (leaf order), b1|b2 half2
+    float4* beta;     // throughput xyz, w = prev bsdf pdf
+    float4* L;        // radiance xyz, w = travelled distance
+    float4* prev;     // previous vertex xyz, w = flag bits
+    uint4* rng;       // pcg state (lo, hi), inc (lo, hi)
+    float4* sh_o;     // shadow origin xyz
+    float4* sh_d;     // shadow direction xyz, w = remaining distance
+    float4* sh_c;     // pending contribution xyz, w = 1 if it belongs to the diffuse AOV
+    float4* aux_a;    // albedo xyz, depth
+    float4* aux_n;    // normal xyz, id bits
+    float4* aux_d;    // diffuse share xyz, hit flag
+    uint32_t* q_ext[2];
+    uint32_t* q_cls;  // N_QUEUES x P
+    uint32_t* q_sh;
+    uint32_t* cnt;
+    unsigned long long* stats;  // [0] extension rays, [1] shadow rays
+    uint32_t* err;
+    uint32_t P;
+};
+
+struct PtConsts {
+    uint32_t npix, width, max_depth, rr_start, aovs;
+    float clamp;
+    uint64_t sample0;  // first sample index of the slab
+};
+
+// flag bits in Paths::prev.w
+#define FL_FROM_CAMERA 1u
+#define FL_SKIP_SHIFT 1
+#define FL_SKIP_MASK (31u << FL_SKIP_SHIFT)
+#define FL_SPEC_SHIFT 6
+#define FL_SPEC_NONE (3u << FL_SPEC_SHIFT)
+#define FL_SPEC_TRUE (1u << FL_SPEC_SHIFT)
+#define FL_SPEC_MASK (3u << FL_SPEC_SHIFT)
+#define FL_AUX_SET (1u << 8)
+#define FL_DEPTH_SHIFT 16
+
+#define RT_RAY_OFFSET 1e-4f
+#define RT_MAX_PRESENCE_SKIPS 16u
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated queue push of `val` into queue `q` (counter `c`).
+__device__ __forceinline__ void push_queue(uint32_t* q, uint32_t* c, uint32_t val, bool active) {
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, active);
+    if (!m) return;
+    uint32_t leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if (lane_id() == leader) base = atomicAdd(c, __popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (active) q[base + __popc(m & ((1u << lane_id()) - 1u))] = val;
+}
+
+// ---- raygen: camera rays for all P slots ------------------------------------------
+// render_pt prologue (kernel_pt.metal:2389-2434) / pt::camera_ray (mod.rs:340-356).
+__device__ __forceinline__ float filter_offset(uint32_t kind, float width, float u) {
+    if (kind == 1u) {
+        float hw = width * 0.5f;
+        return u < 0.5f ? (sqrtf(2.0f * u) - 1.0f) * hw : (1.0f - sqrtf(2.0f * (1.0f - u))) * hw;
+    }
+    if (kind == 2u) {
+        float u1 = fmaxf(u, 1e-12f);
+        float x = u * 2654435761.0f;
+        float u2 = x - truncf(x);
+        float g = sqrtf(-2.0f * logf(u1)) * cosf(2.0f * RT_PI * u2);
+        return fminf(fmaxf(g * (width * 0.25f), -width * 0.5f), width * 0.5f);
+    }
+    return (u - 0.5f) * width;
+}
+
+__global__ void k_raygen(DevScene S, Paths P, PtConsts C) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.P) return;
+    uint32_t pixel = i % C.npix;
+    uint64_t sample = C.sample0 + i / C.npix;
+    Pcg rng = pcg_for_pixel_sample(pixel, sample);
+    uint32_t x = pixel % S.width, y = pixel / S.width;
+    float fu = rng.next_f(), fv = rng.next_f();
+    float px = (float)x + 0.5f + filter_offset(S.filter, S.filter_width, fu);
+    float py = (float)y + 0.5f + filter_offset(S.filter, S.filter_width, fv);
+    float uu = (px / (float)S.width) * 2.0f - 1.0f;
+    float vv = 1.0f - (py / (float)S.height) * 2.0f;
+    float3 eye = f3(S.eye[0], S.eye[1], S.eye[2]);
+    float3 fwd = f3(S.fwd[0], S.fwd[1], S.fwd[2]);
+    float3 rgt = f3(S.right[0], S.right[1], S.right[2]);
+    float3 upv = f3(S.up[0], S.up[1], S.up[2]);
+    float3 dir = fwd + rgt * (uu * S.half_w) + upv * (vv * S.half_h);
+    float3 o = eye, d;
+    if (S.lens_radius > 0.0f) {
+        float lu = rng.next_f(), lv = rng.next_f();
+        float r = S.lens_radius * sqrtf(lu), sp, cp;
+        sincosf(2.0f * RT_PI * lv, &sp, &cp);
+        float3 off = rgt * (r * cp) + upv * (r * sp);
+        float3 focus = eye + dir * S.focal_distance;
+        o = eye + off;
+        d = normalize_ref(focus - o);
+    } else {
+        d = normalize_ref(dir);
+    }
+    P.ray_o[i] = make_float4(o.x, o.y, o.z, 0.0f);
+    P.ray_d[i] = make_float4(d.x, d.y, d.z, INFINITY);
+    P.beta[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    P.L[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    P.prev[i] = make_float4(o.x, o.y, o.z, __uint_as_float(FL_FROM_CAMERA | FL_SPEC_NONE));
+    P.rng[i] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
+                          (uint32_t)(rng.inc >> 32));
+    if (C.aovs) {
+        P.aux_a[i] = make_float4(0, 0, 0, 0);
+        P.aux_n[i] = make_float4(0, 0, 0, 0);
+        P.aux_d[i] = make_float4(0, 0, 0, 0);
+    }
+    P.q_ext[0][i] = i;
+    if (i == 0) P.cnt[CNT_EXT_IN] = P.P;
+}
+
+// ---- extend ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_extend(DevScene S, Paths P, uint32_t qsel) {
+    __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    __shared__ uint32_t warp_base[BLOCK / 32];
+    TravStack st;
+    st.init(stack_sh + threadIdx.x, BLOCK);
+    const uint32_t* q = P.q_ext[qsel];
+    uint32_t n = P.cnt[CNT_EXT_IN];
+    uint32_t w = threadIdx.x >> 5;
+    unsigned long long rays = 0;
+    for (;;) {
+        if (lane_id() == 0) warp_base[w] = atomicAdd(&P.cnt[CNT_FETCH_EXT], 32u);
+        __syncwarp();
+        uint32_t base = warp_base[w];
+        __syncwarp();
+        if (base >= n) break;
+        uint32_t j = base + lane_id();
+        bool active = j < n;
+        uint32_t slot = 0, cls = CLS_MISS;
+        if (active) {
+            slot = q[j];
+            float4 o = P.ray_o[slot], d = P.ray_d[slot];
+            TraceHit h;
+            trace<false>(S, xyz(o), xyz(d), d.w, h, st, P.err);
+            uint32_t uv = (uint32_t)__half_as_ushort(__float2half_rn(h.b1)) |
+                          ((uint32_t)__half_as_ushort(__float2half_rn(h.b2)) << 16);
+            P.hit[slot] = make_uint4(__float_as_uint(h.t), h.tri, h.inst, uv);
+            if (h.tri != 0xFFFFFFFFu) {
+                uint32_t mat = __ldg(&S.inst[h.inst].z);
+                cls = __ldg(&S.materials[mat].mclass);
+            }
+            rays++;
+        }
+        // Bucket by class: one atomic per (warp, class).
+        for (uint32_t c = 0; c < N_QUEUES; c++) {
+            bool mine = active && cls == c;
+            push_queue(P.q_cls + (size_t)c * P.P, &P.cnt[CNT_CLASS + c], slot, mine);
+        }
+    }
+    if (rays) atomicAdd(&P.stats[0], rays);
+}
+
+// ---- shade ------------------------------------------------------------------------------
+struct NeeOut {
+    float3 o, d, c;
+    float tmax;
+};
+
+// NEE for one light (mod.rs:1032-1209): returns true with a shadow ray and
+// its unoccluded contribution (already divided by the pick pmf).
+__device__ __forceinline__ bool nee_light(const DevScene& S, const DevLight& L, float3 p, float3 n, const Frame& fr,
+                                          float3 wo_l, float eta, const DevMaterial& m, float pick, Pcg& rng,
+                                          NeeOut& out) {
+    float3 Le = f3(L.radiance[0], L.radiance[1], L.radiance[2]);
+    auto eval = [&](float3 wi, float& pdf) -> float3 {
+        float3 wl = fr.to_local(wi);
+        if (wl.z <= 0.0f) {
+            pdf = 0.0f;
+            return f3(0, 0, 0);
+        }
+        return bsdf_eval(m, wo_l, wl, eta, pdf) * wl.z;
+    };
+    auto shadow_to = [&](float3 target) {
+        float3 dir = target - p;
+        float dist = length(dir);
+        out.o = p + n * RT_RAY_OFFSET;
+        out.d = normalize_ref(dir);
+        out.tmax = dist - 1e-3f;
+    };
+    float3 lp = f3(L.p[0], L.p[1], L.p[2]);
+    switch (L.type) {
+        case 0: {  // point
+            float3 to = lp - p;
+            float dist2 = fmaxf(dot(to, to), 1e-12f);
+            float3 wi = normalize_ref(to);
+            float bp;
+            float3 f = eval(wi, bp);
+            if (maxc(f) <= 0.0f) return false;
+            out.c = f * Le / (dist2 * pick);
+            shadow_to(lp);
+            return true;
+        }
+        case 1: {  // distant (soft when the angular radius > 1e-5)
+            float3 base = -f3(L.e1[0], L.e1[1], L.e1[2]);
+            float3 wi = base;
+            if (L.radius > 1e-5f) {
+                float u = rng.next_f(), v = rng.next_f();
+                float ct = 1.0f - u * (1.0f - L.cos_max);
+                float stt = sqrtf(fmaxf(1.0f - ct * ct, 0.0f)), sp, cp;
+                sincosf(2.0f * RT_PI * v, &sp, &cp);
+                Frame lf(base);
+                wi = lf.to_world(f3(stt * cp, stt * sp, ct));
+            }
+            float bp;
+            float3 f = eval(wi, bp);
+            if (maxc(f) <= 0.0f) return false;
+            out.c = f * Le / pick;
+            out.o = p + n * RT_RAY_OFFSET;
+            out.d = wi;
+            out.tmax = 1e8f;
+            return true;
+        }
+        case 2:    // rect
+        case 4: {  // disk
+            float u = rng.next_f(), v = rng.next_f();
+            float3 e1 = f3(L.e1[0], L.e1[1], L.e1[2]), e2 = f3(L.e2[0], L.e2[1], L.e2[2]);
+            float3 sp;
+            if (L.type == 2) {
+                sp = lp + e1 * u + e2 * v;
+            } else {
+                float r = sqrtf(u), s, c;
+                sincosf(2.0f * RT_PI * v, &s, &c);
+                sp = lp + e1 * (r * c) + e2 * (r * s);
+            }
+            float3 to = sp - p;
+            float dist2 = fmaxf(dot(to, to), 1e-12f);
+            float3 wi = normalize_ref(to);
+            float cos_l = fabsf(dot(wi, f3(L.n[0], L.n[1], L.n[2])));
+            if (cos_l < 1e-9f || L.area <= 0.0f) return false;
+            float bp;
+            float3 f = eval(wi, bp);
+            if (maxc(f) <= 0.0f) return false;
+            float pdf_sa = pick * dist2 / (cos_l * L.area);
+            out.c = f * Le * (power_heuristic(pdf_sa, bp) / pdf_sa);
+            shadow_to(sp);
+            return true;
+        }
+        case 3: {  // sphere
+            float3 tc = lp - p;
+            float dist2 = dot(tc, tc);
+            float r2 = L.radius * L.radius;
+            if (dist2 <= r2 * 1.0001f) return false;
+            float sin2 = fminf(r2 / dist2, 1.0f);
+            float cos_max = sqrtf(fmaxf(1.0f - sin2, 0.0f));
+            float u = rng.next_f(), v = rng.next_f();
+            float ct = 1.0f - u * (1.0f - cos_max);
+            float stt = sqrtf(fmaxf(1.0f - ct * ct, 0.0f)), s, c;
+            sincosf(2.0f * RT_PI * v, &s, &c);
+            Frame lf(normalize_ref(tc));
+            float3 wi = lf.to_world(f3(stt * c, stt * s, ct));
+            float bp;
+            float3 f = eval(wi, bp);
+            if (maxc(f) <= 0.0f) return false;
+            float dist = sqrtf(dist2) * ct - sqrtf(fmaxf(r2 - dist2 * stt * stt, 0.0f));
+            float pdf_sa = pick / fmaxf(2.0f * RT_PI * (1.0f - cos_max), 1e-12f);
+            out.c = f * Le * (power_heuristic(pdf_sa, bp) / pdf_sa);
+            shadow_to(p + wi * dist);
+            return true;
+        }
+    }
+    return false;
+}
+
+// mod.rs:1000-1023 solid-angle pdf of an area light toward a hit.
+__device__ __forceinline__ float light_pdf_sa(const DevLight& L, float3 origin, float3 hp) {
+    if (L.type == 2 || L.type == 4) {
+        float3 d = hp - origin;
+        float dist2 = dot(d, d);
+        float cos_l = fabsf(dot(normalize_ref(d), f3(L.n[0], L.n[1], L.n[2])));
+        if (cos_l < 1e-9f || L.area <= 0.0f) return 0.0f;
+        return dist2 / (cos_l * L.area);
+    }
+    if (L.type == 3) {
+        float3 c = f3(L.p[0], L.p[1], L.p[2]) - origin;
+        float sin2 = fminf(L.radius * L.radius / dot(c, c), 1.0f);
+        float cos_max = sqrtf(fmaxf(1.0f - sin2, 0.0f));
+        float sa = 2.0f * RT_PI * (1.0f - cos_max);
+        return sa < 1e-12f ? 0.0f : 1.0f / sa;
+    }
+    return 0.0f;
+}
+
+__global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, uint32_t qout) {
+    uint32_t counts[N_QUEUES];
+    uint32_t total = 0;
+#pragma unroll
+    for (uint32_t c = 0; c < N_QUEUES; c++) {
+        counts[c] = P.cnt[CNT_CLASS + c];
+        total += counts[c];
+    }
+    uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t j0 = blockIdx.x * blockDim.x; j0 < total; j0 += stride) {
+        uint32_t j = j0 + threadIdx.x;
+        bool active = j < total;
+        uint32_t slot = 0;
+        if (active) {
+            // Queues are consumed class by class: miss first, then materials.
+            uint32_t c = CLS_MISS, off = j;
+            if (off < counts[CLS_MISS]) {
+                c = CLS_MISS;
+            } else {
+                off -= counts[CLS_MISS];
+                for (uint32_t k = 0; k < N_MAT_CLASSES; k++) {
+                    if (off < counts[k]) {
+                        c = k;
+                        break;
+                    }
+                    off -= counts[k];
+                }
+            }
+            slot = P.q_cls[(size_t)c * P.P + off];
+        }
+        bool extend = false, shadow = false;
+        if (active) {
+            float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot];
+            uint4 hr = P.hit[slot];
+            float4 beta4 = P.beta[slot], L4 = P.L[slot], prev4 = P.prev[slot];
+            uint4 rs = P.rng[slot];
+            Pcg rng;
+            rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
+            rng.inc = (uint64_t)rs.z | ((uint64_t)rs.w << 32);
+            uint32_t flags = __float_as_uint(prev4.w);
+            float3 beta = xyz(beta4), Lr = xyz(L4);
+            float3 o = xyz(o4), d = xyz(d4);
+            float travel = L4.w;
+            bool spec_true = (flags & FL_SPEC_MASK) == FL_SPEC_TRUE;
+            float4 auxd = C.aovs ? P.aux_d[slot] : make_float4(0, 0, 0, 0);
+            auto emit = [&](float3 c) {
+                Lr = Lr + c;
+                if (C.aovs && !spec_true) {
+                    auxd.x += c.x;
+                    auxd.y += c.y;
+                    auxd.z += c.z;
+                }
+            };
+            if (hr.y == 0xFFFFFFFFu) {
+                emit(beta * f3(S.background[0], S.background[1], S.background[2]));
+            } else {
+                float t = __uint_as_float(hr.x);
+                float3 p = o + d * t;
+                uint32_t il = hr.z;
+                float4 x0 = __ldg(S.inst_xf + 3 * (size_t)il), x1 = __ldg(S.inst_xf + 3 * (size_t)il + 1),
+                       x2 = __ldg(S.inst_xf + 3 * (size_t)il + 2);
+                uint4 info = __ldg(S.inst + il);
+                const float4* tp = S.tris + 3 * (size_t)hr.y;
+                float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+                float3 nl;
+                MeshInfo mi = S.meshes[info.w];
+                if (mi.idx_base != 0xFFFFFFFFu) {
+                    float b1 = __half2float(__ushort_as_half((unsigned short)(hr.w & 0xFFFFu)));
+                    float b2 = __half2float(__ushort_as_half((unsigned short)(hr.w >> 16)));
+                    uint32_t ot = __float_as_uint(v0.w);
+                    const uint32_t* ix = S.orig_idx + mi.idx_base + 3 * (size_t)ot;
+                    auto nrm = [&](uint32_t v) { return f3(S.normals[3 * v], S.normals[3 * v + 1], S.normals[3 * v + 2]); };
+                    nl = normalize_ref(nrm(ix[0]) * (1.0f - b1 - b2) + nrm(ix[1]) * b1 + nrm(ix[2]) * b2);
+                } else {
+                    nl = normalize_ref(cross(xyz(v1) - xyz(v0), xyz(v2) - xyz(v0)));
+                }
+                float3 nw = normalize_ref(xf_normal(x0, x1, x2, nl));
+                bool front = dot(nw, d) < 0.0f;
+                if (!front) nw = -nw;
+                float3 wo = -normalize_ref(d);
+                float eucl = length(p - o);
+                travel += eucl;
+                const DevMaterial& m = S.materials[info.z];
+                if (C.aovs && !(flags & FL_AUX_SET)) {
+                    flags |= FL_AUX_SET;
+                    float3 an = dot(nw, wo) >= 0.0f ? nw : -nw;
+                    P.aux_a[slot] = make_float4(m.albedo[0], m.albedo[1], m.albedo[2], travel);
+                    P.aux_n[slot] = make_float4(an.x, an.y, an.z, __uint_as_float(m.id));
+                    auxd.w = 1.0f;
+                }
+                uint32_t skips = (flags & FL_SKIP_MASK) >> FL_SKIP_SHIFT;
+                bool done = false;
+                if (m.presence < 1.0f && rng.next_f() >= m.presence && skips < RT_MAX_PRESENCE_SKIPS) {
+                    // Presence cutout: pass straight through, no bounce.
+                    flags = (flags & ~FL_SKIP_MASK) | ((skips + 1) << FL_SKIP_SHIFT);
+                    travel += eucl;
+                    float3 no = p + normalize_ref(d) * RT_RAY_OFFSET;
+                    P.ray_o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
+                    P.ray_d[slot] = make_float4(d.x, d.y, d.z, INFINITY);
+                    extend = true;
+                    done = true;
+                }
+                if (!done) {
+                    float3 n = dot(nw, wo) >= 0.0f ? nw : -nw;
+                    float eta = front ? m.ior : 1.0f / m.ior;
+                    float3 em = f3(m.emission[0], m.emission[1], m.emission[2]);
+                    if (maxc(em) > 0.0f) {
+                        float wgt = 1.0f;
+                        if (!(flags & FL_FROM_CAMERA) && m.area_light >= 0) {
+                            float3 po = xyz(prev4);
+                            float pick = light_pmf(S, po, (uint32_t)m.area_light);
+                            float pl = light_pdf_sa(S.lights[m.area_light], po, p) * pick;
+                            wgt = power_heuristic(beta4.w, pl);
+                        }
+                        emit(beta * em * wgt);
+                    }
+                    Frame fr(n);
+                    float3 wo_l = fr.to_local(wo);
+                    if (S.n_lights > 0 && m.has_lobes != 0.0f) {
+                        uint32_t li;
+                        float pmf;
+                        if (light_sample(S, p, rng.next_f(), li, pmf)) {
+                            NeeOut ne;
+                            if (nee_light(S, S.lights[li], p, n, fr, wo_l, eta, m, pmf, rng, ne)) {
+                                float3 c = beta * ne.c;
+                                if (maxc(c) > 0.0f) {
+                                    P.sh_o[slot] = make_float4(ne.o.x, ne.o.y, ne.o.z, 0.0f);
+                                    P.sh_d[slot] = make_float4(ne.d.x, ne.d.y, ne.d.z, ne.tmax);
+                                    P.sh_c[slot] = make_float4(c.x, c.y, c.z, spec_true ? 0.0f : 1.0f);
+                                    shadow = true;
+                                }
+                            }
+                        }
+                    }
+                    BsdfSample bs;
+                    if (bsdf_sample(m, wo_l, eta, rng, bs)) {
+                        float3 wi = fr.to_world(bs.wi);
+                        beta = beta * bs.f * (fabsf(bs.wi.z) / bs.pdf);
+                        if ((flags & FL_SPEC_MASK) == FL_SPEC_NONE)
+                            flags = (flags & ~FL_SPEC_MASK) | (bs.specular ? FL_SPEC_TRUE : 0u);
+                        flags &= ~FL_FROM_CAMERA;
+                        beta4.w = bs.pdf;
+                        prev4 = make_float4(p.x, p.y, p.z, 0.0f);
+                        float off = bs.transmitted ? -RT_RAY_OFFSET : RT_RAY_OFFSET;
+                        float3 no = p + n * off;
+                        float3 nd = normalize_ref(wi);
+                        uint32_t depth = (flags >> FL_DEPTH_SHIFT) + 1;
+                        flags = (flags & 0xFFFFu) | (depth << FL_DEPTH_SHIFT);
+                        bool alive = true;
+                        if (depth >= C.rr_start) {
+                            float q = fminf(maxc(beta), 0.95f);
+                            if (q <= 0.0f || rng.next_f() > q) alive = false;
+                            else beta = beta / q;
+                        }
+                        if (alive && depth < C.max_depth) {
+                            P.ray_o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
+                            P.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, INFINITY);
+                            extend = true;
+                        }
+                    }
+                }
+            }
+            P.beta[slot] = make_float4(beta.x, beta.y, beta.z, beta4.w);
+            P.L[slot] = make_float4(Lr.x, Lr.y, Lr.z, travel);
+            P.prev[slot] = make_float4(prev4.x, prev4.y, prev4.z, __uint_as_float(flags));
+            P.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), rs.z, rs.w);
+            if (C.aovs) P.aux_d[slot] = auxd;
+        }
+        push_queue(P.q_ext[qout], &P.cnt[CNT_EXT_OUT], slot, extend);
+        push_queue(P.q_sh, &P.cnt[CNT_SHADOW], slot, shadow);
+    }
+}
+
+// ---- shadow -------------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_shadow(DevScene S, Paths P, PtConsts C) {
+    __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    __shared__ uint32_t warp_base[BLOCK / 32];
+    TravStack st;
+    st.init(stack_sh + threadIdx.x, BLOCK);
+    uint32_t n = P.cnt[CNT_SHADOW];
+    uint32_t w = threadIdx.x >> 5;
+    unsigned long long rays = 0;
+    for (;;) {
+        if (lane_id() == 0) warp_base[w] = atomicAdd(&P.cnt[CNT_FETCH_SH], 32u);
+        __syncwarp();
+        uint32_t base = warp_base[w];
+        __syncwarp();
+        if (base >= n) break;
+        uint32_t j = base + lane_id();
+        if (j >= n) continue;
+        uint32_t slot = P.q_sh[j];
+        float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
+        float3 o = xyz(o4), d = xyz(d4);
+        float remaining = d4.w;
+        float vis = 1.0f;
+        if (!S.any_presence) {
+            TraceHit h;
+            rays++;
+            if (trace<true>(S, o, d, remaining, h, st, P.err)) vis = 0.0f;
+        } else {
+            // transmittance (mod.rs:1254-1306): closest-hit segments, cutouts
+            // attenuate by (1 - presence), opaque surfaces block.
+            for (uint32_t k = 0; k < RT_MAX_PRESENCE_SKIPS; k++) {
+                TraceHit h;
+                rays++;
+                if (!trace<false>(S, o, d, remaining, h, st, P.err)) break;
+                float pr = S.materials[__ldg(&S.inst[h.inst].z)].presence;
+                if (pr >= 1.0f) {
+                    vis = 0.0f;
+                    break;
+                }
+                vis *= 1.0f - pr;
+                if (vis < 1e-4f) {
+                    vis = 0.0f;
+                    break;
+                }
+                o = o + d * h.t + d * RT_RAY_OFFSET;
+                remaining -= h.t + RT_RAY_OFFSET;
+            }
+        }
+        if (vis > 0.0f) {
+            float4 c = P.sh_c[slot];
+            float4 L = P.L[slot];
+            P.L[slot] = make_float4(L.x + c.x * vis, L.y + c.y * vis, L.z + c.z * vis, L.w);
+            if (C.aovs && c.w != 0.0f) {
+                float4 a = P.aux_d[slot];
+                P.aux_d[slot] = make_float4(a.x + c.x * vis, a.y + c.y * vis, a.z + c.z * vis, a.w);
+            }
+        }
+    }
+    if (rays) atomicAdd(&P.stats[1], rays);
+}
+
+// Between waves: the next extend queue becomes the current one.
+__global__ void k_wave_prep(uint32_t* cnt) {
+    uint32_t t = threadIdx.x;
+    if (t == 0) {
+        cnt[CNT_EXT_IN] = cnt[CNT_EXT_OUT];
+        cnt[CNT_EXT_OUT] = 0;
+        cnt[CNT_SHADOW] = 0;
+        cnt[CNT_FETCH_EXT] = 0;
+        cnt[CNT_FETCH_SH] = 0;
+    }
+    if (t < N_QUEUES) cnt[CNT_CLASS + t] = 0;
+}
+
+// ---- accumulate ------------------------------------------------------------------------
+// Per pixel, in sample order: firefly clamp (mod.rs:90-93), f64 sum.
+__global__ void k_accumulate(Paths P, PtConsts C, uint32_t samples_in_slab, double* accum, float* aux) {
+    uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= C.npix) return;
+    double r = 0, g = 0, b = 0;
+    for (uint32_t s = 0; s < samples_in_slab; s++) {
+        uint32_t slot = s * C.npix + pix;
+        float4 L = P.L[slot];
+        float3 l = xyz(L);
+        float lum = luminance(l);
+        float k = 1.0f;
+        if (lum > C.clamp) {
+            k = C.clamp / lum;
+            l = l * k;
+        }
+        r += (double)l.x;
+        g += (double)l.y;
+        b += (double)l.z;
+        if (C.aovs) {
+            float4 a = P.aux_a[slot], nn = P.aux_n[slot], dd = P.aux_d[slot];
+            float* A = aux + 12 * (size_t)pix;
+            A[0] += a.x; A[1] += a.y; A[2] += a.z;
+            A[3] += nn.x; A[4] += nn.y; A[5] += nn.z;
+            A[6] += a.w;
+            if (A[11] == 0.0f && dd.w > 0.0f) A[7] = (float)__float_as_uint(nn.w);
+            A[8] += dd.x * k; A[9] += dd.y * k; A[10] += dd.z * k;
+            A[11] += dd.w;
+        }
+    }
+    double* acc = accum + 4 * (size_t)pix;
+    acc[0] += r;
+    acc[1] += g;
+    acc[2] += b;
+    acc[3] += (double)samples_in_slab;
+}
+
+// ---- ray batch (rt_intersect_batch) ------------------------------------------------------
+template <int BLOCK, bool ANY>
+__global__ void __launch_bounds__(BLOCK) k_intersect(DevScene S, const float4* __restrict__ org,
+                                                     const float4* __restrict__ dir, uint64_t n, uint32_t* prim,
+                                                     uint32_t* inst, float* tout, uint32_t* fetch, uint32_t* err) {
+    __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    __shared__ uint32_t warp_base[BLOCK / 32];
+    TravStack st;
+    st.init(stack_sh + threadIdx.x, BLOCK);
+    uint32_t w = threadIdx.x >> 5;
+    for (;;) {
+        if (lane_id() == 0) warp_base[w] = atomicAdd(fetch, 32u);
+        __syncwarp();
+        uint64_t base = warp_base[w];
+        __syncwarp();
+        if (base >= n) break;
+        uint64_t i = base + lane_id();
+        if (i >= n) continue;
+        float4 o = __ldg(org + i), d = __ldg(dir + i);
+        TraceHit h;
+        bool hit = trace<ANY>(S, xyz(o), xyz(d), d.w, h, st, err);
+        if (ANY) {
+            prim[i] = hit ? 1u : 0u;
+        } else {
+            uint32_t p = 0xFFFFFFFFu, ii = 0xFFFFFFFFu;
+            float t = INFINITY;
+            if (hit) {
+                p = __float_as_uint(__ldg(&S.tris[3 * (size_t)h.tri].w));
+                ii = __ldg(&S.inst[h.inst].y);
+                t = h.t;
+            }
+            prim[i] = p;
+            if (inst) inst[i] = ii;
+            if (tout) tout[i] = t;
+        }
+    }
+}
+
+// White-furnace estimator of one material: per thread, `per` BSDF samples
+// from its own PCG stream; sums of lum(f)|cos|/pdf and of the RGB weights.
+__global__ void k_furnace(DevMaterial m, float3 wo, float eta, uint64_t per, uint64_t seed, double* out) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    Pcg rng = pcg_for_pixel_sample(t, seed);
+    double a = 0, r = 0, g = 0, b = 0;
+    for (uint64_t i = 0; i < per; i++) {
+        BsdfSample s;
+        if (bsdf_sample(m, wo, eta, rng, s)) {
+            float k = fabsf(s.wi.z) / s.pdf;
+            a += (double)(luminance(s.f) * k);
+            r += (double)(s.f.x * k);
+            g += (double)(s.f.y * k);
+            b += (double)(s.f.z * k);
+        }
+    }
+    out[4 * t] = a;
+    out[4 * t + 1] = r;
+    out[4 * t + 2] = g;
+    out[4 * t + 3] = b;
+}
+
+}  // namespace rt

@@ -1,0 +1,452 @@
+// session.cu — the C ABI of librtcuda.so (include/rt_cuda.h).
+//
+// A session flattens the scene once (flatten.cpp), uploads it, and owns the
+// wavefront path state, queues and the f64 accumulator on one CUDA stream.
+// All device waits in the kernels are bounded (traversal step cap, stack
+// capacity); overruns set bits in a device error word that every call
+// checks and reports as RT_ERR_DEVICE instead of hanging or faulting.
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "flatten.h"
+#include "pt_kernels.cuh"
+#include "rt_cuda.h"
+
+using namespace rt;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (expr);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            return fail(e_ == cudaErrorMemoryAllocation ? RT_ERR_OOM : RT_ERR_CUDA,            \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));                  \
+        }                                                                                      \
+    } while (0)
+
+constexpr int TRAV_BLOCK = 128;
+constexpr int SHADE_BLOCK = 128;
+
+}  // namespace
+
+struct rt_session {
+    HostScene host;
+    DevScene S{};
+    rt_params params{};
+    cudaStream_t stream = nullptr;
+    int sm_count = 148;
+    std::vector<void*> allocs;
+    uint64_t device_bytes = 0;
+    // path state
+    Paths paths{};
+    uint32_t slab_samples = 1;     // sample passes per slab
+    double* accum = nullptr;       // 4 doubles per pixel
+    float* aux = nullptr;          // 12 floats per pixel
+    uint32_t* err = nullptr;       // device error word
+    unsigned long long* stats = nullptr;
+    uint32_t* fetch = nullptr;     // ray-batch work counter
+    uint32_t npix = 0;
+    uint32_t samples_done = 0;
+    // ray-batch staging for host-pointer calls
+    void* batch_buf = nullptr;
+    size_t batch_cap = 0;
+    rt_stats last{};
+    cudaEvent_t ev[8] = {};
+
+    template <class T>
+    int alloc(T** p, size_t count) {
+        size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+        void* v = nullptr;
+        cudaError_t e = cudaMalloc(&v, bytes);
+        if (e != cudaSuccess)
+            return fail(e == cudaErrorMemoryAllocation ? RT_ERR_OOM : RT_ERR_CUDA,
+                        std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+        allocs.push_back(v);
+        device_bytes += bytes;
+        *p = (T*)v;
+        return RT_OK;
+    }
+    template <class T>
+    int upload(const T** dst, const std::vector<T>& src) {
+        T* d = nullptr;
+        int rc = alloc(&d, src.size());
+        if (rc) return rc;
+        if (!src.empty()) CUDA_TRY(cudaMemcpyAsync(d, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
+        *dst = d;
+        return RT_OK;
+    }
+    int check_device_error() {
+        uint32_t e = 0;
+        CUDA_TRY(cudaMemcpyAsync(&e, err, 4, cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        if (e) {
+            cudaMemsetAsync(err, 0, 4, stream);
+            cudaStreamSynchronize(stream);
+            return fail(RT_ERR_DEVICE, std::string("device reported ") +
+                                           ((e & RT_DEVERR_STACK) ? "traversal stack overflow " : "") +
+                                           ((e & RT_DEVERR_ITER) ? "traversal step limit " : ""));
+        }
+        return RT_OK;
+    }
+    ~rt_session() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        for (void* p : allocs) cudaFree(p);
+        if (batch_buf) cudaFree(batch_buf);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+extern "C" {
+
+const char* rt_last_error(void) { return g_err.c_str(); }
+
+int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_session** out) {
+    if (!out) return fail(RT_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!scene || !params) return fail(RT_ERR_INVALID, "scene or params is NULL");
+    if (params->max_depth == 0 || params->max_depth > 255) return fail(RT_ERR_INVALID, "max_depth must be in 1..255");
+    auto* s = new rt_session();
+    s->params = *params;
+    std::string err;
+    if (!flatten_scene(scene, &s->host, &err)) {
+        delete s;
+        return fail(RT_ERR_INVALID, err);
+    }
+    int dev = 0;
+    cudaError_t de = cudaGetDevice(&dev);
+    if (de != cudaSuccess) {
+        delete s;
+        return fail(RT_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(de));
+    }
+    cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t ce = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) {
+        delete s;
+        return fail(RT_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(ce));
+    }
+    for (auto& e : s->ev) cudaEventCreate(&e);
+    HostScene& H = s->host;
+    DevScene& S = s->S;
+    S = H.scalars;
+    int rc = 0;
+    rc = rc ? rc : s->upload((const uint4**)&S.nodes, H.nodes);
+    rc = rc ? rc : s->upload((const float4**)&S.tris, H.tris);
+    rc = rc ? rc : s->upload((const float4**)&S.inst_xf, H.inst_xf);
+    rc = rc ? rc : s->upload((const uint4**)&S.inst, H.inst);
+    rc = rc ? rc : s->upload(&S.meshes, H.meshes);
+    rc = rc ? rc : s->upload(&S.orig_idx, H.orig_idx);
+    rc = rc ? rc : s->upload(&S.normals, H.normals);
+    rc = rc ? rc : s->upload(&S.materials, H.materials);
+    rc = rc ? rc : s->upload(&S.lights, H.lights);
+    rc = rc ? rc : s->upload(&S.lbvh, H.lbvh);
+    rc = rc ? rc : s->upload(&S.light_leaf, H.light_leaf);
+    rc = rc ? rc : s->upload(&S.inf_lights, H.inf_lights);
+    rc = rc ? rc : s->upload(&S.inf_power, H.inf_power);
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    // Path state: slabs of whole sample passes (see pt_kernels.cuh).
+    s->npix = scene->camera.width * scene->camera.height;
+    uint64_t cap = params->max_paths ? params->max_paths : (8ull << 20);
+    uint64_t k = std::max<uint64_t>(1, cap / s->npix);
+    if (k * s->npix > 0xFFFFFFFFull / 8) k = std::max<uint64_t>(1, (0xFFFFFFFFull / 8) / s->npix);
+    s->slab_samples = (uint32_t)k;
+    uint64_t P = k * s->npix;
+    Paths& Pp = s->paths;
+    Pp.P = (uint32_t)P;
+    bool aov = params->aovs != 0;
+    rc = rc ? rc : s->alloc(&Pp.ray_o, P);
+    rc = rc ? rc : s->alloc(&Pp.ray_d, P);
+    rc = rc ? rc : s->alloc(&Pp.hit, P);
+    rc = rc ? rc : s->alloc(&Pp.beta, P);
+    rc = rc ? rc : s->alloc(&Pp.L, P);
+    rc = rc ? rc : s->alloc(&Pp.prev, P);
+    rc = rc ? rc : s->alloc(&Pp.rng, P);
+    rc = rc ? rc : s->alloc(&Pp.sh_o, P);
+    rc = rc ? rc : s->alloc(&Pp.sh_d, P);
+    rc = rc ? rc : s->alloc(&Pp.sh_c, P);
+    rc = rc ? rc : s->alloc(&Pp.aux_a, aov ? P : 1);
+    rc = rc ? rc : s->alloc(&Pp.aux_n, aov ? P : 1);
+    rc = rc ? rc : s->alloc(&Pp.aux_d, aov ? P : 1);
+    rc = rc ? rc : s->alloc(&Pp.q_ext[0], P);
+    rc = rc ? rc : s->alloc(&Pp.q_ext[1], P);
+    rc = rc ? rc : s->alloc(&Pp.q_cls, P * N_QUEUES);
+    rc = rc ? rc : s->alloc(&Pp.q_sh, P);
+    rc = rc ? rc : s->alloc(&Pp.cnt, CNT_WORDS);
+    rc = rc ? rc : s->alloc(&s->stats, 4);
+    rc = rc ? rc : s->alloc(&s->err, 1);
+    rc = rc ? rc : s->alloc(&s->fetch, 1);
+    rc = rc ? rc : s->alloc(&s->accum, 4ull * s->npix);
+    rc = rc ? rc : s->alloc(&s->aux, aov ? 12ull * s->npix : 1);
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    Pp.stats = s->stats;
+    Pp.err = s->err;
+    cudaMemsetAsync(s->err, 0, 4, s->stream);
+    cudaMemsetAsync(s->accum, 0, 32ull * s->npix, s->stream);
+    if (aov) cudaMemsetAsync(s->aux, 0, 48ull * s->npix, s->stream);
+    ce = cudaStreamSynchronize(s->stream);
+    if (ce != cudaSuccess) {
+        delete s;
+        return fail(RT_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(ce));
+    }
+    *out = s;
+    return RT_OK;
+}
+
+int rt_session_destroy(rt_session* s) {
+    delete s;
+    return RT_OK;
+}
+
+void* rt_session_stream(rt_session* s) { return s ? (void*)s->stream : nullptr; }
+
+int rt_reset(rt_session* s) {
+    if (!s) return fail(RT_ERR_INVALID, "session is NULL");
+    CUDA_TRY(cudaMemsetAsync(s->accum, 0, 32ull * s->npix, s->stream));
+    if (s->params.aovs) CUDA_TRY(cudaMemsetAsync(s->aux, 0, 48ull * s->npix, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->samples_done = 0;
+    return RT_OK;
+}
+
+int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
+    if (!s) return fail(RT_ERR_INVALID, "session is NULL");
+    if (count == 0) return RT_OK;
+    cudaStream_t st = s->stream;
+    Paths& P = s->paths;
+    PtConsts C;
+    C.npix = s->npix;
+    C.width = s->S.width;
+    C.max_depth = s->params.max_depth;
+    C.rr_start = s->params.rr_start;
+    C.aovs = s->params.aovs;
+    C.clamp = (float)s->params.firefly_clamp;
+    uint32_t waves = s->params.max_depth + (s->S.any_presence ? RT_MAX_PRESENCE_SKIPS : 0u);
+    int trav_grid = s->sm_count * 4;
+    int shade_grid = s->sm_count * 8;
+    CUDA_TRY(cudaMemsetAsync(s->stats, 0, 32, st));
+    float ms_ext = 0, ms_sh = 0, ms_shade = 0;
+    uint64_t launches = 0;
+    CUDA_TRY(cudaEventRecord(s->ev[0], st));
+    for (uint32_t done = 0; done < count;) {
+        uint32_t k = std::min(s->slab_samples, count - done);
+        uint32_t slab_paths = k * s->npix;
+        P.P = slab_paths;
+        C.sample0 = (uint64_t)sample_start + done;
+        CUDA_TRY(cudaMemsetAsync(P.cnt, 0, CNT_WORDS * 4, st));
+        k_raygen<<<(slab_paths + 255) / 256, 256, 0, st>>>(s->S, P, C);
+        launches++;
+        for (uint32_t w = 0; w < waves; w++) {
+            uint32_t qin = w & 1u, qout = qin ^ 1u;
+            CUDA_TRY(cudaEventRecord(s->ev[1], st));
+            k_extend<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
+            CUDA_TRY(cudaEventRecord(s->ev[2], st));
+            k_shade<<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
+            CUDA_TRY(cudaEventRecord(s->ev[3], st));
+            k_shadow<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            CUDA_TRY(cudaEventRecord(s->ev[4], st));
+            k_wave_prep<<<1, 32, 0, st>>>(P.cnt);
+            launches += 4;
+            CUDA_TRY(cudaEventSynchronize(s->ev[4]));
+            float a, b, c;
+            cudaEventElapsedTime(&a, s->ev[1], s->ev[2]);
+            cudaEventElapsedTime(&b, s->ev[2], s->ev[3]);
+            cudaEventElapsedTime(&c, s->ev[3], s->ev[4]);
+            ms_ext += a;
+            ms_shade += b;
+            ms_sh += c;
+        }
+        k_accumulate<<<(s->npix + 255) / 256, 256, 0, st>>>(P, C, k, s->accum, s->aux);
+        launches++;
+        done += k;
+    }
+    CUDA_TRY(cudaEventRecord(s->ev[5], st));
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(st));
+    int rc = s->check_device_error();
+    if (rc) return rc;
+    unsigned long long stats[2];
+    CUDA_TRY(cudaMemcpy(stats, s->stats, 16, cudaMemcpyDeviceToHost));
+    float total = 0;
+    cudaEventElapsedTime(&total, s->ev[0], s->ev[5]);
+    s->last.extension_rays = stats[0];
+    s->last.shadow_rays = stats[1];
+    s->last.samples = (uint64_t)count * s->npix;
+    s->last.kernel_launches = launches;
+    s->last.extend_ms = ms_ext;
+    s->last.shadow_ms = ms_sh;
+    s->last.shade_ms = ms_shade;
+    s->last.total_ms = total;
+    s->samples_done += count;
+    return RT_OK;
+}
+
+int rt_read_accum(rt_session* s, double* rgbw) {
+    if (!s || !rgbw) return fail(RT_ERR_INVALID, "NULL argument");
+    CUDA_TRY(cudaMemcpyAsync(rgbw, s->accum, 32ull * s->npix, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return RT_OK;
+}
+
+int rt_read_image(rt_session* s, float* rgb) {
+    if (!s || !rgb) return fail(RT_ERR_INVALID, "NULL argument");
+    std::vector<double> a(4ull * s->npix);
+    int rc = rt_read_accum(s, a.data());
+    if (rc) return rc;
+    for (uint64_t i = 0; i < s->npix; i++) {
+        double w = a[4 * i + 3] > 0 ? a[4 * i + 3] : 1.0;
+        for (int c = 0; c < 3; c++) rgb[3 * i + c] = (float)(a[4 * i + c] / w);
+    }
+    return RT_OK;
+}
+
+int rt_read_aux(rt_session* s, float* aux12) {
+    if (!s || !aux12) return fail(RT_ERR_INVALID, "NULL argument");
+    if (!s->params.aovs) return fail(RT_ERR_INVALID, "session was created with aovs = 0");
+    CUDA_TRY(cudaMemcpyAsync(aux12, s->aux, 48ull * s->npix, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return RT_OK;
+}
+
+int rt_checkpoint_save(rt_session* s, const char* path) {
+    if (!s || !path) return fail(RT_ERR_INVALID, "NULL argument");
+    std::vector<double> a(4ull * s->npix);
+    int rc = rt_read_accum(s, a.data());
+    if (rc) return rc;
+    std::string tmp = std::string(path) + ".tmp";
+    FILE* f = fopen(tmp.c_str(), "wb");
+    if (!f) return fail(RT_ERR_IO, "cannot open " + tmp);
+    uint32_t hdr[4] = {0x31554352u /* "RCU1" */, s->S.width, s->S.height, s->samples_done};
+    bool ok = fwrite(hdr, 4, 4, f) == 4 && fwrite(a.data(), 8, a.size(), f) == a.size();
+    ok = (fclose(f) == 0) && ok;
+    if (!ok || rename(tmp.c_str(), path) != 0) {
+        remove(tmp.c_str());
+        return fail(RT_ERR_IO, std::string("cannot write checkpoint ") + path);
+    }
+    return RT_OK;
+}
+
+int rt_checkpoint_load(rt_session* s, const char* path, uint32_t* samples_done) {
+    if (!s || !path) return fail(RT_ERR_INVALID, "NULL argument");
+    FILE* f = fopen(path, "rb");
+    if (!f) return fail(RT_ERR_IO, std::string("cannot open ") + path);
+    uint32_t hdr[4];
+    std::vector<double> a(4ull * s->npix);
+    bool ok = fread(hdr, 4, 4, f) == 4;
+    if (ok && (hdr[0] != 0x31554352u || hdr[1] != s->S.width || hdr[2] != s->S.height)) {
+        fclose(f);
+        return fail(RT_ERR_MISMATCH, "checkpoint does not match this session");
+    }
+    ok = ok && fread(a.data(), 8, a.size(), f) == a.size();
+    char extra;
+    ok = ok && fread(&extra, 1, 1, f) == 0;
+    fclose(f);
+    if (!ok) return fail(RT_ERR_IO, std::string("truncated checkpoint ") + path);
+    CUDA_TRY(cudaMemcpyAsync(s->accum, a.data(), 32ull * s->npix, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->samples_done = hdr[3];
+    if (samples_done) *samples_done = hdr[3];
+    return RT_OK;
+}
+
+int rt_intersect_batch_device(rt_session* s, const float* rays, uint64_t n, int any_hit, uint32_t* prim,
+                              uint32_t* inst, float* t, void* stream) {
+    if (!s || (!rays && n) || (!prim && n)) return fail(RT_ERR_INVALID, "NULL argument");
+    if (n >= 0xFFFFFFFFull - 64) return fail(RT_ERR_INVALID, "batch larger than 2^32 rays");
+    if (((uintptr_t)rays & 15u) != 0) return fail(RT_ERR_INVALID, "rays must be 16-byte aligned");
+    if (n == 0) return RT_OK;
+    cudaStream_t st = stream ? (cudaStream_t)stream : s->stream;
+    CUDA_TRY(cudaMemsetAsync(s->fetch, 0, 4, st));
+    const float4* o = (const float4*)rays;
+    const float4* d = o + n;
+    int grid = s->sm_count * 4;
+    if (any_hit)
+        k_intersect<TRAV_BLOCK, true><<<grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, prim, inst, t, s->fetch, s->err);
+    else
+        k_intersect<TRAV_BLOCK, false><<<grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, prim, inst, t, s->fetch, s->err);
+    CUDA_TRY(cudaGetLastError());
+    return RT_OK;
+}
+
+int rt_intersect_batch(rt_session* s, const float* rays, uint64_t n, int any_hit, uint32_t* prim, uint32_t* inst,
+                       float* t) {
+    if (!s || (!rays && n) || (!prim && n)) return fail(RT_ERR_INVALID, "NULL argument");
+    if (n == 0) return RT_OK;
+    size_t need = n * (32 + 12);
+    if (need > s->batch_cap) {
+        if (s->batch_buf) cudaFree(s->batch_buf);
+        s->batch_buf = nullptr;
+        s->batch_cap = 0;
+        CUDA_TRY(cudaMalloc(&s->batch_buf, need));
+        s->batch_cap = need;
+    }
+    char* b = (char*)s->batch_buf;
+    float* d_rays = (float*)b;
+    uint32_t* d_prim = (uint32_t*)(b + 32 * n);
+    uint32_t* d_inst = (uint32_t*)(b + 36 * n);
+    float* d_t = (float*)(b + 40 * n);
+    CUDA_TRY(cudaMemcpyAsync(d_rays, rays, 32 * n, cudaMemcpyHostToDevice, s->stream));
+    int rc = rt_intersect_batch_device(s, d_rays, n, any_hit, d_prim, d_inst, d_t, nullptr);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(prim, d_prim, 4 * n, cudaMemcpyDeviceToHost, s->stream));
+    if (!any_hit && inst) CUDA_TRY(cudaMemcpyAsync(inst, d_inst, 4 * n, cudaMemcpyDeviceToHost, s->stream));
+    if (!any_hit && t) CUDA_TRY(cudaMemcpyAsync(t, d_t, 4 * n, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return s->check_device_error();
+}
+
+int rt_bsdf_furnace(const rt_material_desc* material, const double* wo, double eta, uint64_t n, uint64_t seed,
+                    double* out) {
+    if (!material || !wo || !out) return fail(RT_ERR_INVALID, "NULL argument");
+    DevMaterial m = fold_material_public(*material);
+    const int threads = 256, blocks = 148 * 8;
+    const uint64_t nt = (uint64_t)threads * blocks;
+    uint64_t per = (n + nt - 1) / nt;
+    double* d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, nt * 4 * sizeof(double)));
+    float3 w = make_float3((float)wo[0], (float)wo[1], (float)wo[2]);
+    k_furnace<<<blocks, threads>>>(m, w, (float)eta, per, seed, d);
+    cudaError_t e = cudaDeviceSynchronize();
+    std::vector<double> h(nt * 4);
+    if (e == cudaSuccess) e = cudaMemcpy(h.data(), d, nt * 4 * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(RT_ERR_CUDA, std::string("furnace: ") + cudaGetErrorString(e));
+    double acc[4] = {0, 0, 0, 0};
+    for (uint64_t i = 0; i < nt; i++)
+        for (int c = 0; c < 4; c++) acc[c] += h[4 * i + c];
+    double total = (double)(per * nt);
+    for (int c = 0; c < 4; c++) out[c] = acc[c] / total;
+    return RT_OK;
+}
+
+int rt_get_stats(rt_session* s, rt_stats* out) {
+    if (!s || !out) return fail(RT_ERR_INVALID, "NULL argument");
+    *out = s->last;
+    out->blas_nodes = s->host.blas_nodes;
+    out->tlas_nodes = s->host.tlas_nodes;
+    out->triangles = s->host.tris.size() / 3;
+    out->device_bytes = s->device_bytes;
+    return RT_OK;
+}
+
+}  // extern "C"

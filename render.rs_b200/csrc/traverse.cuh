@@ -1,0 +1,364 @@
+// traverse.cuh — ray traversal of the two-level 8-wide BVH on sm_100a.
+//
+// Closest hit and any hit over the TLAS/BLAS pair, one ray per thread:
+//  * node fetch: six 128-bit read-only loads (96-B node);
+//  * child boxes decoded exactly (p + q * 2^e is an exact f32) and tested
+//    with the robust slab test of Ize 2013 (t_far scaled by 1 + 2*gamma(3));
+//  * triangles with the watertight test of Woop, Benthin and Wald 2013
+//    (shear to ray space, edge functions, f64 fallback on exact zeros);
+//  * traversal stack: the top 32 entries live in shared memory (one column
+//    per thread, bank-conflict free), deeper entries spill to local memory
+//    in halves; a stack deeper than the spill area sets an error bit.
+// The reference's traversal is Bvh::traverse / any_hit (src/accel/bvh.rs:
+// 141-245) over 2-wide nodes with Möller–Trumbore triangles
+// (src/geometry/mesh.rs:117-142) and Instance::intersect (mesh.rs:308-381):
+// same closest hit (parametric t along the unnormalised ray, instance
+// transforms applied without renormalising), different arithmetic.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "rt_internal.h"
+
+namespace rt {
+
+// ---- small float3 helpers ---------------------------------------------------
+__device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 operator*(float3 a, float3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ float3 operator/(float3 a, float s) { return f3(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross(float3 a, float3 b) {
+    return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float length(float3 a) { return sqrtf(dot(a, a)); }
+// Normalise only above 1e-6, as the reference's Vec3::normalize
+// (src/math/vector.rs:31-38).
+__device__ __forceinline__ float3 normalize_ref(float3 a) {
+    float l = length(a);
+    return l > 1e-6f ? a / l : a;
+}
+__device__ __forceinline__ float maxc(float3 c) { return fmaxf(fmaxf(c.x, c.y), c.z); }
+__device__ __forceinline__ float luminance(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+__device__ __forceinline__ float3 xyz(float4 v) { return f3(v.x, v.y, v.z); }
+
+// Row-major 3x4 affine applied to a point / a vector / a normal (transpose).
+__device__ __forceinline__ float3 xf_point(const float4& r0, const float4& r1, const float4& r2, float3 p) {
+    return f3(fmaf(r0.x, p.x, fmaf(r0.y, p.y, fmaf(r0.z, p.z, r0.w))),
+              fmaf(r1.x, p.x, fmaf(r1.y, p.y, fmaf(r1.z, p.z, r1.w))),
+              fmaf(r2.x, p.x, fmaf(r2.y, p.y, fmaf(r2.z, p.z, r2.w))));
+}
+__device__ __forceinline__ float3 xf_vec(const float4& r0, const float4& r1, const float4& r2, float3 v) {
+    return f3(r0.x * v.x + r0.y * v.y + r0.z * v.z, r1.x * v.x + r1.y * v.y + r1.z * v.z,
+              r2.x * v.x + r2.y * v.y + r2.z * v.z);
+}
+__device__ __forceinline__ float3 xf_normal(const float4& r0, const float4& r1, const float4& r2, float3 n) {
+    return f3(r0.x * n.x + r1.x * n.y + r2.x * n.z, r0.y * n.x + r1.y * n.y + r2.y * n.z,
+              r0.z * n.x + r1.z * n.y + r2.z * n.z);
+}
+
+// ---- per-ray precomputation ------------------------------------------------------
+struct RayPre {
+    float3 o, d, inv;
+    // Woop shear as three rows: A_x = (v - o) . rx, A_y = (v - o) . ry, A_z = (v - o) . rz
+    float3 rx, ry, rz;
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+
+__device__ __forceinline__ float comp(float3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+__device__ __forceinline__ void ray_pre(RayPre& r, float3 o, float3 d) {
+    r.o = o;
+    r.d = d;
+    auto safe = [](float x) { return fabsf(x) < 1e-30f ? copysignf(1e-30f, x) : x; };
+    r.inv = f3(1.0f / safe(d.x), 1.0f / safe(d.y), 1.0f / safe(d.z));
+    float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    float dz = comp(d, kz);
+    if (dz < 0.0f) {
+        int t = kx;
+        kx = ky;
+        ky = t;
+    }
+    float sx = comp(d, kx) / dz, sy = comp(d, ky) / dz, sz = 1.0f / dz;
+    r.kx = kx;
+    r.ky = ky;
+    r.kz = kz;
+    r.sx = sx;
+    r.sy = sy;
+    r.sz = sz;
+    auto unit = [](int k) { return f3(k == 0 ? 1.f : 0.f, k == 1 ? 1.f : 0.f, k == 2 ? 1.f : 0.f); };
+    r.rx = unit(kx) - unit(kz) * sx;
+    r.ry = unit(ky) - unit(kz) * sy;
+    r.rz = unit(kz) * sz;
+}
+
+// Watertight ray/triangle test. Returns true and writes t, b1, b2
+// (barycentrics of v1, v2) when 0 < t < t_max.
+__device__ __forceinline__ bool tri_watertight(const RayPre& r, float3 v0, float3 v1, float3 v2, float t_max,
+                                               float& t_out, float& b1, float& b2) {
+    float3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
+    float ax = fmaf(-r.sx, comp(A, r.kz), comp(A, r.kx));
+    float ay = fmaf(-r.sy, comp(A, r.kz), comp(A, r.ky));
+    float bx = fmaf(-r.sx, comp(B, r.kz), comp(B, r.kx));
+    float by = fmaf(-r.sy, comp(B, r.kz), comp(B, r.ky));
+    float cx = fmaf(-r.sx, comp(C, r.kz), comp(C, r.kx));
+    float cy = fmaf(-r.sy, comp(C, r.kz), comp(C, r.ky));
+    float U = cx * by - cy * bx;
+    float V = ax * cy - ay * cx;
+    float W = bx * ay - by * ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = (float)((double)cx * (double)by - (double)cy * (double)bx);
+        V = (float)((double)ax * (double)cy - (double)ay * (double)cx);
+        W = (float)((double)bx * (double)ay - (double)by * (double)ax);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    float det = U + V + W;
+    if (det == 0.0f) return false;
+    float az = r.sz * comp(A, r.kz), bz = r.sz * comp(B, r.kz), cz = r.sz * comp(C, r.kz);
+    float T = U * az + V * bz + W * cz;
+    float t = T / det;
+    if (!(t > 0.0f && t < t_max)) return false;
+    t_out = t;
+    float rdet = 1.0f / det;
+    b1 = V * rdet;
+    b2 = W * rdet;
+    return true;
+}
+
+// ---- 8-wide node: decode and test all children --------------------------------------
+__device__ __forceinline__ float q8(uint32_t word, int byte) {
+    // Exact u8 -> f32 through the 2^23 mantissa trick.
+    return __uint_as_float(0x4B000000u | ((word >> (8 * byte)) & 0xFFu)) - 8388608.0f;
+}
+
+struct NodeHits {
+    float tn[8];
+    uint32_t ref[8];
+    uint32_t mask;
+};
+
+// ROBUST_SCALE = 1 + 2*gamma(3), gamma(n) = n*eps/(1 - n*eps), eps = 2^-24.
+#define RT_ROBUST_SCALE 1.0000003576278687f
+
+__device__ __forceinline__ void test_node(const uint4* __restrict__ nodes, uint32_t idx, const RayPre& r,
+                                          float t_max, NodeHits& h) {
+    const uint4* n = nodes + (size_t)idx * WIDE_NODE_WORDS;
+    uint4 w0 = __ldg(n + 0), w1 = __ldg(n + 1), w2 = __ldg(n + 2), w3 = __ldg(n + 3);
+    uint4 w4 = __ldg(n + 4), w5 = __ldg(n + 5);
+    float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
+    float sx = __uint_as_float((w0.w & 0xFFu) << 23);
+    float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
+    float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+    h.ref[0] = w4.x; h.ref[1] = w4.y; h.ref[2] = w4.z; h.ref[3] = w4.w;
+    h.ref[4] = w5.x; h.ref[5] = w5.y; h.ref[6] = w5.z; h.ref[7] = w5.w;
+    h.mask = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        uint32_t wlx = k < 4 ? w1.x : w1.y, wly = k < 4 ? w1.z : w1.w;
+        uint32_t wlz = k < 4 ? w2.x : w2.y, whx = k < 4 ? w2.z : w2.w;
+        uint32_t why = k < 4 ? w3.x : w3.y, whz = k < 4 ? w3.z : w3.w;
+        int b = k & 3;
+        float lox = fmaf(q8(wlx, b), sx, px), hix = fmaf(q8(whx, b), sx, px);
+        float loy = fmaf(q8(wly, b), sy, py), hiy = fmaf(q8(why, b), sy, py);
+        float loz = fmaf(q8(wlz, b), sz, pz), hiz = fmaf(q8(whz, b), sz, pz);
+        float t0x = (lox - r.o.x) * r.inv.x, t1x = (hix - r.o.x) * r.inv.x;
+        float t0y = (loy - r.o.y) * r.inv.y, t1y = (hiy - r.o.y) * r.inv.y;
+        float t0z = (loz - r.o.z) * r.inv.z, t1z = (hiz - r.o.z) * r.inv.z;
+        float tnear = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
+        float tfar = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), t_max));
+        tfar *= RT_ROBUST_SCALE;
+        h.tn[k] = tnear;
+        if (tnear <= tfar && h.ref[k] != REF_EMPTY) h.mask |= 1u << k;
+    }
+}
+
+// ---- traversal stack: shared-memory top, local-memory spill ----------------------------
+#define RT_SH_STACK 32
+#define RT_SPILL 96
+
+struct TravStack {
+    uint2* sh;       // this thread's column: entry k at sh[(k % 32) * stride]
+    int stride;
+    int sp, base;    // logical stack [0, sp); shared holds [base, sp)
+    uint2 spill[RT_SPILL];
+    bool overflow;
+
+    __device__ __forceinline__ void init(uint2* col, int stride_) {
+        sh = col;
+        stride = stride_;
+        sp = 0;
+        base = 0;
+        overflow = false;
+    }
+    __device__ __forceinline__ void push(uint32_t ref, float t) {
+        if (sp - base == RT_SH_STACK) {
+            if (base + RT_SH_STACK / 2 > RT_SPILL) {
+                overflow = true;
+                return;
+            }
+#pragma unroll 1
+            for (int i = 0; i < RT_SH_STACK / 2; i++) spill[base + i] = sh[((base + i) & (RT_SH_STACK - 1)) * stride];
+            base += RT_SH_STACK / 2;
+        }
+        sh[(sp & (RT_SH_STACK - 1)) * stride] = make_uint2(ref, __float_as_uint(t));
+        sp++;
+    }
+    __device__ __forceinline__ uint2 pop() {
+        if (sp == base && base > 0) {
+            base -= RT_SH_STACK / 2;
+#pragma unroll 1
+            for (int i = 0; i < RT_SH_STACK / 2; i++) sh[((base + i) & (RT_SH_STACK - 1)) * stride] = spill[base + i];
+        }
+        sp--;
+        return sh[(sp & (RT_SH_STACK - 1)) * stride];
+    }
+};
+
+struct TraceHit {
+    float t;
+    uint32_t tri;    // leaf-order triangle index (global), ~0 on miss
+    uint32_t inst;   // leaf-order instance index
+    float b1, b2;    // barycentrics of v1, v2
+};
+
+// Error bits written to the device error word.
+#define RT_DEVERR_STACK 1u
+#define RT_DEVERR_ITER 2u
+#define RT_MAX_TRAV_STEPS (1u << 22)
+
+// Closest hit (ANY = false) or any hit (ANY = true, returns at the first
+// hit with t < t_max). World-space ray (o, d), parametric t.
+template <bool ANY>
+__device__ __forceinline__ bool trace(const DevScene& S, float3 o, float3 d, float t_max, TraceHit& hit,
+                                      TravStack& st, uint32_t* err) {
+    hit.t = t_max;
+    hit.tri = 0xFFFFFFFFu;
+    hit.inst = 0xFFFFFFFFu;
+    hit.b1 = hit.b2 = 0.0f;
+    if (S.n_instances == 0) return false;
+    RayPre r;
+    ray_pre(r, o, d);
+    st.sp = 0;
+    st.base = 0;
+    bool in_inst = false;
+    int inst_sp = 0;
+    uint32_t cur_inst = 0;
+    uint32_t cur = S.tlas_root;  // interior node ref
+    bool found = false;
+    uint32_t steps = 0;
+    for (;;) {
+        if (++steps > RT_MAX_TRAV_STEPS) {
+            atomicOr(err, RT_DEVERR_ITER);
+            return found;
+        }
+        if (!(cur & REF_LEAF)) {
+            NodeHits h;
+            test_node(S.nodes, cur, r, hit.t, h);
+            uint32_t m = h.mask;
+            if (m) {
+                if (ANY) {
+                    // Unordered: keep the first hit child, push the rest.
+                    int k0 = __ffs(m) - 1;
+                    uint32_t next = 0;
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        if (k == k0) next = h.ref[k];
+                        else if ((m >> k) & 1u) st.push(h.ref[k], h.tn[k]);
+                    }
+                    cur = next;
+                } else {
+                    // Push far-to-near; continue with the nearest.
+                    while (__popc(m) > 1) {
+                        float bt = -1.0f;
+                        int bk = 0;
+#pragma unroll
+                        for (int k = 0; k < 8; k++)
+                            if (((m >> k) & 1u) && h.tn[k] > bt) {
+                                bt = h.tn[k];
+                                bk = k;
+                            }
+                        uint32_t rf = 0;
+#pragma unroll
+                        for (int k = 0; k < 8; k++)
+                            if (k == bk) rf = h.ref[k];
+                        st.push(rf, bt);
+                        m &= ~(1u << bk);
+                    }
+                    uint32_t next = 0;
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                        if ((m >> k) & 1u) next = h.ref[k];
+                    cur = next;
+                }
+                if (st.overflow) {
+                    atomicOr(err, RT_DEVERR_STACK);
+                    return found;
+                }
+                continue;
+            }
+        } else if (!in_inst) {
+            // TLAS leaf: a run of instances. Defer all but the first on the
+            // stack (as one-instance leaves), then enter the first.
+            uint32_t first = cur & LEAF_FIRST_MASK;
+            uint32_t count = ((cur >> 27) & 15u) + 1u;
+            for (uint32_t k = count - 1; k >= 1; k--) st.push(make_leaf_ref(first + k, 1), 0.0f);
+            if (st.overflow) {
+                atomicOr(err, RT_DEVERR_STACK);
+                return found;
+            }
+            cur_inst = first;
+            float4 x0 = __ldg(S.inst_xf + 3 * (size_t)first), x1 = __ldg(S.inst_xf + 3 * (size_t)first + 1),
+                   x2 = __ldg(S.inst_xf + 3 * (size_t)first + 2);
+            uint32_t root = __ldg(&S.inst[first].x);
+            ray_pre(r, xf_point(x0, x1, x2, o), xf_vec(x0, x1, x2, d));
+            in_inst = true;
+            inst_sp = st.sp;
+            if (root != 0xFFFFFFFFu) {
+                cur = root;
+                continue;
+            }
+        } else {
+            // BLAS leaf: triangles in leaf order.
+            uint32_t first = cur & LEAF_FIRST_MASK;
+            uint32_t count = ((cur >> 27) & 15u) + 1u;
+            for (uint32_t k = 0; k < count; k++) {
+                const float4* tp = S.tris + 3 * (size_t)(first + k);
+                float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+                float t, b1, b2;
+                if (tri_watertight(r, xyz(a), xyz(b), xyz(c), hit.t, t, b1, b2)) {
+                    hit.t = t;
+                    hit.tri = first + k;
+                    hit.inst = cur_inst;
+                    hit.b1 = b1;
+                    hit.b2 = b2;
+                    found = true;
+                    if (ANY) return true;
+                }
+            }
+        }
+        // Pop the next entry that can still hold a closer hit; leaving an
+        // instance's BLAS restores the world-space ray.
+        for (;;) {
+            if (in_inst && st.sp == inst_sp) {
+                in_inst = false;
+                ray_pre(r, o, d);
+            }
+            if (st.sp == 0) return found;
+            uint2 e = st.pop();
+            if (__uint_as_float(e.y) < hit.t) {
+                cur = e.x;
+                break;
+            }
+        }
+    }
+}
+
+}  // namespace rt

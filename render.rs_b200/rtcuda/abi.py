@@ -1,0 +1,124 @@
+"""ctypes mirrors of ``include/rt_scene.h`` and ``include/rt_cuda.h``.
+
+The field order and sizes are asserted against the C headers' static
+assertions so a drift between the two fails at import time.
+"""
+import ctypes as C
+
+c_double3 = C.c_double * 3
+
+
+class RtMeshDesc(C.Structure):
+    _fields_ = [
+        ("positions", C.POINTER(C.c_float)),
+        ("indices", C.POINTER(C.c_uint32)),
+        ("normals", C.POINTER(C.c_float)),
+        ("n_vertices", C.c_uint32),
+        ("n_triangles", C.c_uint32),
+    ]
+
+
+class RtInstanceDesc(C.Structure):
+    _fields_ = [
+        ("object_to_world", C.c_double * 12),
+        ("mesh_id", C.c_uint32),
+        ("material_id", C.c_uint32),
+    ]
+
+
+class RtMaterialDesc(C.Structure):
+    _fields_ = [
+        ("diffuse_gain", C.c_double),
+        ("diffuse_color", c_double3),
+        ("diffuse_roughness", C.c_double),
+        ("specular_face_color", c_double3),
+        ("specular_edge_color", c_double3),
+        ("specular_roughness", C.c_double),
+        ("specular_ior", C.c_double),
+        ("clearcoat_gain", C.c_double),
+        ("clearcoat_roughness", C.c_double),
+        ("fuzz_gain", C.c_double),
+        ("fuzz_color", c_double3),
+        ("glass_gain", C.c_double),
+        ("glass_ior", C.c_double),
+        ("glass_roughness", C.c_double),
+        ("refraction_color", c_double3),
+        ("glow", c_double3),
+        ("presence", C.c_double),
+        ("emission", c_double3),
+        ("area_light", C.c_int32),
+        ("id", C.c_uint32),
+    ]
+
+
+class RtLightDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("pad_", C.c_int32),
+        ("intensity", C.c_double),
+        ("color", c_double3),
+        ("p", c_double3),
+        ("e1", c_double3),
+        ("e2", c_double3),
+        ("radius", C.c_double),
+    ]
+
+
+class RtCameraDesc(C.Structure):
+    _fields_ = [
+        ("width", C.c_uint32),
+        ("height", C.c_uint32),
+        ("fov_deg", C.c_double),
+        ("eye", c_double3),
+        ("forward", c_double3),
+        ("up", c_double3),
+        ("right", c_double3),
+        ("lens_radius", C.c_double),
+        ("focal_distance", C.c_double),
+        ("filter", C.c_int32),
+        ("pad_", C.c_int32),
+        ("filter_width", C.c_double),
+    ]
+
+
+class RtSceneDesc(C.Structure):
+    _fields_ = [
+        ("meshes", C.POINTER(RtMeshDesc)),
+        ("instances", C.POINTER(RtInstanceDesc)),
+        ("materials", C.POINTER(RtMaterialDesc)),
+        ("lights", C.POINTER(RtLightDesc)),
+        ("n_meshes", C.c_uint32),
+        ("n_instances", C.c_uint32),
+        ("n_materials", C.c_uint32),
+        ("n_lights", C.c_uint32),
+        ("camera", RtCameraDesc),
+        ("background", c_double3),
+    ]
+
+
+class RtParams(C.Structure):
+    _fields_ = [
+        ("max_depth", C.c_uint32),
+        ("rr_start", C.c_uint32),
+        ("firefly_clamp", C.c_double),
+        ("aovs", C.c_uint32),
+        ("guided", C.c_uint32),
+        ("guide_fraction", C.c_double),
+        ("max_paths", C.c_uint64),
+    ]
+
+
+LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK = range(5)
+FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
+
+for _t, _n in ((RtMeshDesc, 32), (RtInstanceDesc, 104), (RtMaterialDesc, 264),
+               (RtLightDesc, 120), (RtCameraDesc, 144), (RtParams, 40)):
+    assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
+
+
+def make_params(max_depth=8, rr_start=3, firefly_clamp=60.0, aovs=False, guided=False,
+                guide_fraction=0.5, max_paths=0):
+    """Integrator knobs; defaults follow the reference's constants
+    (src/raytracer/pt/mod.rs:26-32) except the bounce cap, which the configs set."""
+    return RtParams(max_depth, rr_start, firefly_clamp, 1 if aovs else 0, 1 if guided else 0,
+                    guide_fraction, max_paths)

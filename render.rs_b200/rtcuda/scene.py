@@ -1,0 +1,257 @@
+"""Host-side scene assembly: numpy arrays in, ``rt_scene_desc`` out.
+
+This is the build-side counterpart of the reference's ``Scene``
+(src/scene/mod.rs:27-56) restricted to what the path tracer consumes:
+triangle meshes, affine instances, PbrParams materials, lights, camera.
+Material helpers follow the reference's legacy mappings
+(src/scene/pbr.rs:104-135) and ``PbrParams::default`` (pbr.rs:53-77).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+
+INSTANCE_DTYPE = np.dtype([("xf", "<f8", (12,)), ("mesh", "<u4"), ("mat", "<u4")])
+assert INSTANCE_DTYPE.itemsize == C.sizeof(abi.RtInstanceDesc)
+
+IDENTITY_3x4 = np.array([1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0], dtype=np.float64)
+
+
+def _normalize(v):
+    v = np.asarray(v, dtype=np.float64)
+    n = np.linalg.norm(v)
+    return v / n if n > 1e-6 else v
+
+
+def default_material():
+    """PbrParams::default (src/scene/pbr.rs:53-77) with no emission."""
+    return dict(diffuse_gain=1.0, diffuse_color=(0.5, 0.5, 0.5), diffuse_roughness=0.0,
+                specular_face_color=(0.0, 0.0, 0.0), specular_edge_color=(1.0, 1.0, 1.0),
+                specular_roughness=0.2, specular_ior=1.5, clearcoat_gain=0.0,
+                clearcoat_roughness=0.1, fuzz_gain=0.0, fuzz_color=(1.0, 1.0, 1.0),
+                glass_gain=0.0, glass_ior=1.5, glass_roughness=0.05,
+                refraction_color=(1.0, 1.0, 1.0), glow=(0.0, 0.0, 0.0), presence=1.0,
+                emission=(0.0, 0.0, 0.0), area_light=-1, id=0)
+
+
+def matte(color, sigma=0.0, **kw):
+    """PbrParams::from_matte (pbr.rs:104-111): diffuse only, specular off
+    (specular_ior = 1); `sigma` is the Oren-Nayar roughness."""
+    m = default_material()
+    m.update(diffuse_gain=1.0, diffuse_color=tuple(color), specular_ior=1.0,
+             diffuse_roughness=sigma)
+    m.update(kw)
+    return m
+
+
+def ggx_conductor(f0, roughness, **kw):
+    """PbrParams::from_metal (pbr.rs:123-131) with a scalar or RGB F0."""
+    f0 = (f0, f0, f0) if np.isscalar(f0) else tuple(f0)
+    m = default_material()
+    m.update(diffuse_gain=0.0, specular_face_color=f0, specular_edge_color=(1.0, 1.0, 1.0),
+             specular_roughness=max(roughness, 0.02))
+    m.update(kw)
+    return m
+
+
+def ggx_floor(color, roughness, **kw):
+    """Diffuse base with a GGX dielectric coat (PbrParams::from_plastic,
+    pbr.rs:113-121) at a chosen roughness."""
+    m = default_material()
+    m.update(diffuse_gain=0.9, diffuse_color=tuple(color), specular_ior=1.5,
+             specular_roughness=max(roughness, 0.02))
+    m.update(kw)
+    return m
+
+
+def rough_dielectric(ior=1.5, roughness=0.05, **kw):
+    """glassRefractionGain = 1 with no diffuse or primary specular lobe."""
+    m = default_material()
+    m.update(diffuse_gain=0.0, specular_ior=1.0, glass_gain=1.0, glass_ior=ior,
+             glass_roughness=roughness)
+    m.update(kw)
+    return m
+
+
+def emitter(radiance, area_light=-1, **kw):
+    """Black, non-reflecting emitter (no lobes)."""
+    m = default_material()
+    m.update(diffuse_gain=0.0, specular_ior=1.0, emission=tuple(radiance), area_light=area_light)
+    m.update(kw)
+    return m
+
+
+def rot_y(deg):
+    a = np.deg2rad(deg)
+    c, s = np.cos(a), np.sin(a)
+    return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]], dtype=np.float64)
+
+
+def affine(linear=None, translate=(0, 0, 0)):
+    """Row-major 3x4 object-to-world matrix."""
+    m = np.zeros((3, 4), dtype=np.float64)
+    m[:, :3] = np.eye(3) if linear is None else linear
+    m[:, 3] = translate
+    return m.reshape(12)
+
+
+class Scene:
+    """Scene under construction. Keeps every array alive for as long as the
+    descriptor returned by :meth:`desc` is in use."""
+
+    def __init__(self, width, height, fov=40.0):
+        self.width, self.height, self.fov = int(width), int(height), float(fov)
+        self.meshes = []          # (positions f32 (n,3), indices u32 (m,3), normals or None)
+        self.instances = np.zeros(0, dtype=INSTANCE_DTYPE)
+        self._inst_chunks = []
+        self.materials = []
+        self.lights = []
+        self.background = (0.0, 0.0, 0.0)
+        # Reference default camera: origin, looking down +z (camera.rs:97-103).
+        self.eye = np.zeros(3)
+        self.forward = np.array([0.0, 0.0, 1.0])
+        self.up = np.array([0.0, 1.0, 0.0])
+        self.right = np.cross(self.up, self.forward)
+        self.lens_radius, self.focal_distance = 0.0, 1.0
+        self.filter, self.filter_width = abi.FILTER_BOX, 1.0
+        self._desc = None
+
+    # -- geometry --------------------------------------------------------
+    def add_mesh(self, positions, indices, normals=None):
+        p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+        i = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
+        n = None if normals is None else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
+        if i.size and int(i.max()) >= len(p):
+            raise ValueError("mesh index out of range")
+        self.meshes.append((p, i, n))
+        self._desc = None
+        return len(self.meshes) - 1
+
+    def add_instance(self, mesh_id, material_id, xform=None):
+        rec = np.zeros(1, dtype=INSTANCE_DTYPE)
+        rec["xf"][0] = IDENTITY_3x4 if xform is None else np.asarray(xform, dtype=np.float64).reshape(12)
+        rec["mesh"][0] = mesh_id
+        rec["mat"][0] = material_id
+        self._inst_chunks.append(rec)
+        self._desc = None
+        return self.n_instances - 1
+
+    def add_instances(self, mesh_ids, material_ids, xforms):
+        """Vectorised instance placement: xforms (n, 12) row-major 3x4."""
+        n = len(mesh_ids)
+        rec = np.zeros(n, dtype=INSTANCE_DTYPE)
+        rec["xf"] = np.asarray(xforms, dtype=np.float64).reshape(n, 12)
+        rec["mesh"] = mesh_ids
+        rec["mat"] = material_ids
+        self._inst_chunks.append(rec)
+        self._desc = None
+
+    @property
+    def n_instances(self):
+        return sum(len(c) for c in self._inst_chunks)
+
+    def add_material(self, m):
+        self.materials.append(dict(m))
+        self._desc = None
+        return len(self.materials) - 1
+
+    # -- lights ----------------------------------------------------------
+    def _light(self, type_, intensity, color, p=(0, 0, 0), e1=(0, 0, 0), e2=(0, 0, 0), radius=0.0):
+        self.lights.append(dict(type=type_, intensity=float(intensity), color=tuple(color),
+                                p=tuple(p), e1=tuple(e1), e2=tuple(e2), radius=float(radius)))
+        self._desc = None
+        return len(self.lights) - 1
+
+    def add_point_light(self, position, intensity, color=(1, 1, 1)):
+        return self._light(abi.LIGHT_POINT, intensity, color, p=position)
+
+    def add_distant_light(self, direction, intensity, color=(1, 1, 1), angular_radius=0.0):
+        return self._light(abi.LIGHT_DISTANT, intensity, color, e1=direction, radius=angular_radius)
+
+    def add_rect_light(self, corner, edge1, edge2, intensity, color=(1, 1, 1)):
+        return self._light(abi.LIGHT_RECT, intensity, color, p=corner, e1=edge1, e2=edge2)
+
+    def add_emissive_quad(self, corner, edge1, edge2, radiance):
+        """A sampleable rectangle light plus its emissive geometry, as the
+        reference's scene builder makes for an AreaLightSource Polygon
+        (src/parser/scene_builder.rs:924-933)."""
+        corner, e1, e2 = (np.asarray(v, dtype=np.float64) for v in (corner, edge1, edge2))
+        li = self.add_rect_light(corner, e1, e2, 1.0, radiance)
+        mat = self.add_material(emitter(radiance, area_light=li))
+        pos = np.array([corner, corner + e1, corner + e1 + e2, corner + e2])
+        mesh = self.add_mesh(pos, [[0, 1, 2], [0, 2, 3]])
+        self.add_instance(mesh, mat)
+        return li
+
+    # -- camera ----------------------------------------------------------
+    def look_at(self, eye, target, up=(0, 1, 0), fov=None):
+        """Camera::set_transform (src/scene/camera.rs:124-129)."""
+        self.eye = np.asarray(eye, dtype=np.float64)
+        self.forward = _normalize(np.asarray(target, dtype=np.float64) - self.eye)
+        self.right = _normalize(np.cross(self.forward, np.asarray(up, dtype=np.float64)))
+        self.up = _normalize(np.cross(self.right, self.forward))
+        if fov is not None:
+            self.fov = float(fov)
+        self._desc = None
+
+    # -- descriptor ------------------------------------------------------
+    def triangle_count(self):
+        """Effective (instanced) triangles."""
+        inst = self.instance_array()
+        per_mesh = np.array([len(m[1]) for m in self.meshes], dtype=np.int64)
+        return int(per_mesh[inst["mesh"]].sum()) if len(inst) else 0
+
+    def instance_array(self):
+        if self._inst_chunks:
+            if len(self._inst_chunks) > 1:
+                self._inst_chunks = [np.concatenate(self._inst_chunks)]
+            return self._inst_chunks[0]
+        return np.zeros(0, dtype=INSTANCE_DTYPE)
+
+    def desc(self):
+        if self._desc is not None:
+            return self._desc
+        keep = []
+        mesh_arr = (abi.RtMeshDesc * max(1, len(self.meshes)))()
+        for k, (p, i, n) in enumerate(self.meshes):
+            keep += [p, i, n]
+            mesh_arr[k].positions = p.ctypes.data_as(C.POINTER(C.c_float))
+            mesh_arr[k].indices = i.ctypes.data_as(C.POINTER(C.c_uint32))
+            mesh_arr[k].normals = n.ctypes.data_as(C.POINTER(C.c_float)) if n is not None else None
+            mesh_arr[k].n_vertices = len(p)
+            mesh_arr[k].n_triangles = len(i)
+        inst = np.ascontiguousarray(self.instance_array())
+        keep.append(inst)
+        mat_arr = (abi.RtMaterialDesc * max(1, len(self.materials)))()
+        for k, m in enumerate(self.materials):
+            for key, val in m.items():
+                if isinstance(val, tuple):
+                    setattr(mat_arr[k], key, abi.c_double3(*val))
+                else:
+                    setattr(mat_arr[k], key, val)
+        light_arr = (abi.RtLightDesc * max(1, len(self.lights)))()
+        for k, l in enumerate(self.lights):
+            light_arr[k].type = l["type"]
+            light_arr[k].intensity = l["intensity"]
+            light_arr[k].color = abi.c_double3(*l["color"])
+            light_arr[k].p = abi.c_double3(*l["p"])
+            light_arr[k].e1 = abi.c_double3(*l["e1"])
+            light_arr[k].e2 = abi.c_double3(*l["e2"])
+            light_arr[k].radius = l["radius"]
+        cam = abi.RtCameraDesc(self.width, self.height, self.fov, abi.c_double3(*self.eye),
+                               abi.c_double3(*self.forward), abi.c_double3(*self.up),
+                               abi.c_double3(*self.right), self.lens_radius, self.focal_distance,
+                               self.filter, 0, self.filter_width)
+        d = abi.RtSceneDesc()
+        d.meshes = mesh_arr
+        d.instances = inst.ctypes.data_as(C.POINTER(abi.RtInstanceDesc))
+        d.materials = mat_arr
+        d.lights = light_arr
+        d.n_meshes, d.n_instances = len(self.meshes), len(inst)
+        d.n_materials, d.n_lights = len(self.materials), len(self.lights)
+        d.camera = cam
+        d.background = abi.c_double3(*self.background)
+        self._desc = d
+        self._keep = (keep, mesh_arr, mat_arr, light_arr)
+        return d
