@@ -161,6 +161,42 @@ def run_reference(args):
     return 0
 
 
+def run_traversal(args):
+    """Closest-hit then any-hit batches over the triangle cloud, `args.rays`
+    rays each, device-resident; one JSON line with per-launch times."""
+    import torch
+    from rtcuda import PtSession, abi, scenes
+    from rtcuda.scene import Scene, matte
+    s = Scene(8, 8)
+    s.add_instance(s.add_mesh(*scenes.triangle_cloud_mesh(N_TRIS)), s.add_material(matte((0.5, 0.5, 0.5))))
+    sess = PtSession(s, abi.make_params(max_depth=MAX_DEPTH, max_paths=64))
+    stream = torch.cuda.ExternalStream(sess.stream())
+    rays = torch.from_numpy(scenes.triangle_cloud_rays(args.rays)).cuda()
+    n = args.rays
+    prim = torch.empty(n, dtype=torch.int32, device="cuda")
+    inst = torch.empty_like(prim)
+    tt = torch.empty(n, dtype=torch.float32, device="cuda")
+    out = {"mode": "traversal", "rays": n}
+    for any_hit, name in ((0, "closest_hit"), (1, "any_hit")):
+        for _ in range(args.warmup):
+            sess.intersect_device(rays.data_ptr(), n, any_hit, prim.data_ptr(), inst.data_ptr(), tt.data_ptr(),
+                                  sess.stream())
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            sess.intersect_device(rays.data_ptr(), n, any_hit, prim.data_ptr(), inst.data_ptr(), tt.data_ptr(),
+                                  sess.stream())
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / max(args.steps, 1)
+        out[name] = {"ms": ms, "Mrays_per_s": n / ms / 1e3}
+    print(json.dumps(out), flush=True)
+    sess.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -169,9 +205,14 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--mode", default="full", choices=["full", "traversal"],
+                    help="traversal: only the closest/any-hit ray batches (for profiler captures)")
+    ap.add_argument("--rays", type=int, default=N_RAYS)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "traversal":
+        return run_traversal(args)
 
     import torch
     import torch.distributed as dist

@@ -149,3 +149,28 @@ class OracleScene:
     def light_pmf(self, p, light):
         _, pp = _f64(p)
         return lib().oracle_light_pmf(self.h, pp, light)
+
+
+def guide_eval(mlp, table16, res, lo, inv_ext, records, grads=True):
+    """f64 network oracle: raw outputs, loss and (optionally) gradients for
+    the MLP parameters and the hash table."""
+    L = lib()
+    if not hasattr(L, "_guide_ready"):
+        vp = C.c_void_p
+        L.oracle_guide_eval.argtypes = [vp, vp, vp, vp, vp, vp, C.c_uint32, vp, vp, vp, vp]
+        L._guide_ready = True
+    mlp = np.ascontiguousarray(mlp, dtype=np.float32)
+    table16 = np.ascontiguousarray(table16, dtype=np.uint16)
+    res = np.ascontiguousarray(res, dtype=np.float32)
+    lo = np.ascontiguousarray(lo, dtype=np.float32)
+    inv_ext = np.ascontiguousarray(inv_ext, dtype=np.float32)
+    rec = np.ascontiguousarray(records, dtype=np.float32)
+    n = rec.shape[0]
+    raw = np.zeros((n, 48))
+    g_mlp = np.zeros(mlp.size) if grads else None
+    g_tab = np.zeros(table16.size, dtype=np.float32) if grads else None
+    loss = C.c_double()
+    L.oracle_guide_eval(mlp.ctypes.data, table16.ctypes.data, res.ctypes.data, lo.ctypes.data, inv_ext.ctypes.data,
+                        rec.ctypes.data, n, raw.ctypes.data, g_mlp.ctypes.data if grads else None,
+                        g_tab.ctypes.data if grads else None, C.byref(loss))
+    return raw, loss.value, g_mlp, g_tab

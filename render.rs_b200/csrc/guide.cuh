@@ -1,0 +1,203 @@
+// guide.cuh — the learned directional proposal (device side).
+//
+// Network: multiresolution hash-grid encoding of the shading position
+// (16 levels x 2 features, 2^19 entries per level, FP16 table; Müller et al.
+// 2022, "Instant neural graphics primitives") plus the shading normal and the
+// outgoing direction, into an MLP of three hidden layers of 64 (BF16 weights,
+// FP32 accumulate, ReLU) whose 40 outputs parameterise a mixture of 8
+// von Mises-Fisher lobes (mean direction, concentration, weight).
+//
+// The reference has no counterpart (path guiding is an unimplemented stretch
+// goal in its ROADMAP.md:34); this proposal is MIS-combined with the
+// reference's BSDF sampling (one-sample MIS) so the estimator stays
+// unbiased whatever the network outputs.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "shade.cuh"
+
+namespace rt {
+
+static const int G_LEVELS = 16;
+static const int G_FEAT = 2;
+static const int G_LOG2_T = 19;
+static const uint32_t G_T = 1u << G_LOG2_T;
+static const int G_IN = 48;     // 32 hash features + normal(3) + wo(3) + zero pad
+static const int G_HID = 64;
+static const int G_OUT = 48;    // 40 used: 8 lobes x (mean xyz, kappa, weight)
+static const int G_LOBES = 8;
+static const int G_NW0 = G_HID * G_IN, G_NW1 = G_HID * G_HID, G_NW2 = G_HID * G_HID, G_NW3 = G_OUT * G_HID;
+static const int G_NWEIGHTS = G_NW0 + G_NW1 + G_NW2 + G_NW3;
+static const int G_NBIAS = G_HID * 3 + G_OUT;
+static const int G_NPARAMS = G_NWEIGHTS + G_NBIAS;  // MLP parameters (table separate)
+
+struct GuideDev {
+    const __half2* table;     // [levels][T] feature pairs (FP16)
+    const __nv_bfloat16* w;   // MLP weights, row-major [out][in], layers concatenated
+    const float* b;           // biases
+    float res[G_LEVELS];      // grid resolution per level
+    float lo[3], inv_ext[3];  // scene bounds -> [0,1]^3
+};
+
+// Spatial hash of a grid vertex (Teschner et al. 2003 primes, as used by
+// instant-ngp); coarse levels whose grid fits the table index densely.
+__device__ __forceinline__ uint32_t grid_index(uint32_t x, uint32_t y, uint32_t z, uint32_t res1, bool dense) {
+    if (dense) return x + y * res1 + z * res1 * res1;
+    return (x * 1u ^ y * 2654435761u ^ z * 805459861u) & (G_T - 1u);
+}
+
+// Encode one position: 32 features (16 levels x 2), trilinear in each level.
+__device__ __forceinline__ void hash_encode(const GuideDev& G, float3 pn, float* feat) {
+#pragma unroll 4
+    for (int l = 0; l < G_LEVELS; l++) {
+        float r = G.res[l];
+        uint32_t res1 = (uint32_t)r + 2u;
+        bool dense = (uint64_t)res1 * res1 * res1 <= G_T;
+        float fx = pn.x * r, fy = pn.y * r, fz = pn.z * r;
+        float ix = floorf(fx), iy = floorf(fy), iz = floorf(fz);
+        float tx = fx - ix, ty = fy - iy, tz = fz - iz;
+        uint32_t x0 = (uint32_t)ix, y0 = (uint32_t)iy, z0 = (uint32_t)iz;
+        float a0 = 0.f, a1 = 0.f;
+        const __half2* T = G.table + (size_t)l * G_T;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            uint32_t dx = c & 1, dy = (c >> 1) & 1, dz = (c >> 2) & 1;
+            float w = (dx ? tx : 1.f - tx) * (dy ? ty : 1.f - ty) * (dz ? tz : 1.f - tz);
+            float2 v = __half22float2(T[grid_index(x0 + dx, y0 + dy, z0 + dz, res1, dense)]);
+            a0 += w * v.x;
+            a1 += w * v.y;
+        }
+        feat[2 * l] = a0;
+        feat[2 * l + 1] = a1;
+    }
+}
+
+__device__ __forceinline__ float3 guide_normalize_pos(const GuideDev& G, float3 p) {
+    float3 q = f3((p.x - G.lo[0]) * G.inv_ext[0], (p.y - G.lo[1]) * G.inv_ext[1], (p.z - G.lo[2]) * G.inv_ext[2]);
+    return f3(fminf(fmaxf(q.x, 0.f), 1.f), fminf(fmaxf(q.y, 0.f), 1.f), fminf(fmaxf(q.z, 0.f), 1.f));
+}
+
+// ---- von Mises-Fisher mixture ----------------------------------------------------
+// Raw outputs per lobe j: o[5j..5j+2] mean (unnormalised), o[5j+3] log kappa,
+// o[5j+4] weight logit. kappa = exp(clamp(., -4, 9)); weights = softmax.
+struct Mixture {
+    float3 mu[G_LOBES];
+    float kappa[G_LOBES];
+    float w[G_LOBES];
+};
+
+__device__ __forceinline__ void mixture_decode(const float* o, Mixture& m) {
+    float mx = -1e30f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) mx = fmaxf(mx, o[5 * j + 4]);
+    float sw = 0.f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) {
+        float3 v = f3(o[5 * j], o[5 * j + 1], o[5 * j + 2]);
+        float len = length(v);
+        m.mu[j] = len > 1e-8f ? v / len : f3(0.f, 0.f, 1.f);
+        m.kappa[j] = __expf(fminf(fmaxf(o[5 * j + 3], -4.f), 9.f));
+        m.w[j] = __expf(o[5 * j + 4] - mx);
+        sw += m.w[j];
+    }
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) m.w[j] /= sw;
+}
+
+// log of the vMF density kappa / (2 pi (1 - e^{-2 kappa})) exp(kappa (mu.w - 1)).
+__device__ __forceinline__ float vmf_log_pdf(float3 mu, float kappa, float3 w) {
+    float norm = logf(kappa) - logf(2.f * RT_PI) - log1pf(-__expf(-2.f * kappa));
+    return norm + kappa * (dot(mu, w) - 1.f);
+}
+
+__device__ __forceinline__ float mixture_pdf(const Mixture& m, float3 w) {
+    float p = 0.f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) p += m.w[j] * __expf(vmf_log_pdf(m.mu[j], m.kappa[j], w));
+    return p;
+}
+
+// Sample: pick a lobe by weight, then a direction around its mean
+// (W. Jakob, "Numerically stable sampling of the von Mises-Fisher
+// distribution on S^2", 2012).
+__device__ __forceinline__ float3 mixture_sample(const Mixture& m, float u0, float u1, float u2) {
+    int j = G_LOBES - 1;
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < G_LOBES; k++) {
+        acc += m.w[k];
+        if (u0 < acc) {
+            j = k;
+            break;
+        }
+    }
+    float kappa = 0.f;
+    float3 mu = f3(0, 0, 1);
+#pragma unroll
+    for (int k = 0; k < G_LOBES; k++)
+        if (k == j) {
+            kappa = m.kappa[k];
+            mu = m.mu[k];
+        }
+    float wz = 1.f + logf(u1 + (1.f - u1) * __expf(-2.f * kappa)) / kappa;
+    wz = fminf(fmaxf(wz, -1.f), 1.f);
+    float sr = sqrtf(fmaxf(1.f - wz * wz, 0.f)), s, c;
+    sincosf(2.f * RT_PI * u2, &s, &c);
+    float3 t = fabsf(mu.x) > 0.9f ? f3(0, 1, 0) : f3(1, 0, 0);
+    float3 a = normalize_ref(cross(mu, t)), b = cross(mu, a);
+    return normalize_ref(a * (sr * c) + b * (sr * s) + mu * wz);
+}
+
+// Loss -weight * log q(w) for raw outputs o; writes d loss / d o into g (40 used).
+__device__ __forceinline__ float mixture_loss_grad(const float* o, float3 w, float weight, float* g) {
+    float mx = -1e30f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) mx = fmaxf(mx, o[5 * j + 4]);
+    float pi[G_LOBES], lv[G_LOBES], kap[G_LOBES], len[G_LOBES], dmw[G_LOBES];
+    float3 mu[G_LOBES];
+    float sw = 0.f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) {
+        float3 v = f3(o[5 * j], o[5 * j + 1], o[5 * j + 2]);
+        len[j] = fmaxf(length(v), 1e-8f);
+        mu[j] = v / len[j];
+        float lk = fminf(fmaxf(o[5 * j + 3], -4.f), 9.f);
+        kap[j] = __expf(lk);
+        pi[j] = __expf(o[5 * j + 4] - mx);
+        sw += pi[j];
+        dmw[j] = dot(mu[j], w);
+    }
+    float lmax = -1e30f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) {
+        pi[j] /= sw;
+        lv[j] = logf(fmaxf(pi[j], 1e-30f)) + vmf_log_pdf(mu[j], kap[j], w);
+        lmax = fmaxf(lmax, lv[j]);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) s += __expf(lv[j] - lmax);
+    float logq = lmax + logf(s);
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) {
+        float r = __expf(lv[j] - logq);   // responsibility
+        float k = kap[j];
+        // d log vmf / d kappa = 1/kappa + (mu.w - 1) - 2 / (e^{2 kappa} - 1)
+        float dlk = 1.f / k + (dmw[j] - 1.f) - 2.f / fmaxf(__expf(2.f * k) - 1.f, 1e-30f);
+        float lk = o[5 * j + 3];
+        float dk = (lk > -4.f && lk < 9.f) ? -weight * r * dlk * k : 0.f;
+        float3 gm = (w - mu[j] * dmw[j]) * (-weight * r * k / len[j]);
+        g[5 * j] = gm.x;
+        g[5 * j + 1] = gm.y;
+        g[5 * j + 2] = gm.z;
+        g[5 * j + 3] = dk;
+        g[5 * j + 4] = -weight * (r - pi[j]);
+    }
+#pragma unroll
+    for (int j = 5 * G_LOBES; j < G_OUT; j++) g[j] = 0.f;
+    return -weight * logq;
+}
+
+}  // namespace rt

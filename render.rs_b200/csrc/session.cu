@@ -66,6 +66,8 @@ struct rt_session {
     size_t batch_cap = 0;
     rt_stats last{};
     cudaEvent_t ev[8] = {};
+    std::vector<cudaEvent_t> evpool;
+    int trav_grid = 148 * 4;      // resident blocks of the traversal kernels
 
     template <class T>
     int alloc(T** p, size_t count) {
@@ -106,6 +108,7 @@ struct rt_session {
         if (stream) cudaStreamSynchronize(stream);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        for (auto& e : evpool) cudaEventDestroy(e);
         for (void* p : allocs) cudaFree(p);
         if (batch_buf) cudaFree(batch_buf);
         if (stream) cudaStreamDestroy(stream);
@@ -135,6 +138,12 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
         return fail(RT_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(de));
     }
     cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, dev);
+    {
+        // Persistent traversal grids: every resident block slot on every SM.
+        int nb = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<TRAV_BLOCK>, TRAV_BLOCK, 0);
+        s->trav_grid = s->sm_count * std::max(nb, 1);
+    }
     cudaError_t ce = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (ce != cudaSuccess) {
         delete s;
@@ -242,12 +251,21 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     C.aovs = s->params.aovs;
     C.clamp = (float)s->params.firefly_clamp;
     uint32_t waves = s->params.max_depth + (s->S.any_presence ? RT_MAX_PRESENCE_SKIPS : 0u);
-    int trav_grid = s->sm_count * 4;
-    int shade_grid = s->sm_count * 8;
+    const int trav_grid = s->trav_grid, shade_grid = s->sm_count * 8;
     CUDA_TRY(cudaMemsetAsync(s->stats, 0, 32, st));
     float ms_ext = 0, ms_sh = 0, ms_shade = 0;
     uint64_t launches = 0;
-    CUDA_TRY(cudaEventRecord(s->ev[0], st));
+    // Per-wave timing events are recorded without host waits and read once
+    // at the end, so the waves of a slab run back to back.
+    size_t nslabs = (count + s->slab_samples - 1) / s->slab_samples;
+    size_t need = 2 + nslabs * waves * 4;
+    while (s->evpool.size() < need) {
+        cudaEvent_t e;
+        CUDA_TRY(cudaEventCreate(&e));
+        s->evpool.push_back(e);
+    }
+    size_t ei = 2;
+    CUDA_TRY(cudaEventRecord(s->evpool[0], st));
     for (uint32_t done = 0; done < count;) {
         uint32_t k = std::min(s->slab_samples, count - done);
         uint32_t slab_paths = k * s->npix;
@@ -258,37 +276,39 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
         launches++;
         for (uint32_t w = 0; w < waves; w++) {
             uint32_t qin = w & 1u, qout = qin ^ 1u;
-            CUDA_TRY(cudaEventRecord(s->ev[1], st));
+            CUDA_TRY(cudaEventRecord(s->evpool[ei], st));
             k_extend<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
-            CUDA_TRY(cudaEventRecord(s->ev[2], st));
+            CUDA_TRY(cudaEventRecord(s->evpool[ei + 1], st));
             k_shade<<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
-            CUDA_TRY(cudaEventRecord(s->ev[3], st));
+            CUDA_TRY(cudaEventRecord(s->evpool[ei + 2], st));
             k_shadow<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
-            CUDA_TRY(cudaEventRecord(s->ev[4], st));
+            CUDA_TRY(cudaEventRecord(s->evpool[ei + 3], st));
             k_wave_prep<<<1, 32, 0, st>>>(P.cnt);
             launches += 4;
-            CUDA_TRY(cudaEventSynchronize(s->ev[4]));
-            float a, b, c;
-            cudaEventElapsedTime(&a, s->ev[1], s->ev[2]);
-            cudaEventElapsedTime(&b, s->ev[2], s->ev[3]);
-            cudaEventElapsedTime(&c, s->ev[3], s->ev[4]);
-            ms_ext += a;
-            ms_shade += b;
-            ms_sh += c;
+            ei += 4;
         }
         k_accumulate<<<(s->npix + 255) / 256, 256, 0, st>>>(P, C, k, s->accum, s->aux);
         launches++;
         done += k;
     }
-    CUDA_TRY(cudaEventRecord(s->ev[5], st));
+    CUDA_TRY(cudaEventRecord(s->evpool[1], st));
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(st));
+    for (size_t e = 2; e < ei; e += 4) {
+        float a, b, c;
+        cudaEventElapsedTime(&a, s->evpool[e], s->evpool[e + 1]);
+        cudaEventElapsedTime(&b, s->evpool[e + 1], s->evpool[e + 2]);
+        cudaEventElapsedTime(&c, s->evpool[e + 2], s->evpool[e + 3]);
+        ms_ext += a;
+        ms_shade += b;
+        ms_sh += c;
+    }
     int rc = s->check_device_error();
     if (rc) return rc;
     unsigned long long stats[2];
     CUDA_TRY(cudaMemcpy(stats, s->stats, 16, cudaMemcpyDeviceToHost));
     float total = 0;
-    cudaEventElapsedTime(&total, s->ev[0], s->ev[5]);
+    cudaEventElapsedTime(&total, s->evpool[0], s->evpool[1]);
     s->last.extension_rays = stats[0];
     s->last.shadow_rays = stats[1];
     s->last.samples = (uint64_t)count * s->npix;
@@ -379,7 +399,7 @@ int rt_intersect_batch_device(rt_session* s, const float* rays, uint64_t n, int 
     CUDA_TRY(cudaMemsetAsync(s->fetch, 0, 4, st));
     const float4* o = (const float4*)rays;
     const float4* d = o + n;
-    int grid = s->sm_count * 4;
+    int grid = s->trav_grid;
     if (any_hit)
         k_intersect<TRAV_BLOCK, true><<<grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, prim, inst, t, s->fetch, s->err);
     else

@@ -123,3 +123,270 @@ def triangle_cloud(width=1920, height=1080, n_tris=1_000_000, seed=2024):
 
 
 TRIANGLE_CLOUD = dict(spp=16, max_depth=8, rr_start=3)
+
+
+# ---------------------------------------------------------------------------
+# C3: instanced materials
+def icosphere(subdivisions=5):
+    """Unit icosphere: 20 * 4^s triangles, smooth vertex normals (= positions)."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(p, dtype=np.float64) / np.linalg.norm(p) for p in v]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5),
+             (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdivisions):
+        cache = {}
+
+        def mid(a, b):
+            key = (a, b) if a < b else (b, a)
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    p = np.array(verts)
+    return p, np.array(faces, dtype=np.uint32), p.copy()
+
+
+def value_noise_fbm(x, y, rng_seed, octaves=5, base=4.0):
+    """Seeded fBm of bilinear-smoothstep value noise on a lattice (sum of
+    octaves with frequency x2 and amplitude x0.5)."""
+    rng = np.random.default_rng(rng_seed)
+    out = np.zeros_like(x)
+    amp, freq = 1.0, base
+    for _ in range(octaves):
+        n = int(np.ceil(freq)) + 2
+        lat = rng.uniform(-1, 1, size=(n + 1, n + 1))
+        fx, fy = x * freq, y * freq
+        ix, iy = np.floor(fx).astype(int), np.floor(fy).astype(int)
+        tx, ty = fx - ix, fy - iy
+        sx, sy = tx * tx * (3 - 2 * tx), ty * ty * (3 - 2 * ty)
+        ix, iy = np.clip(ix, 0, n - 1), np.clip(iy, 0, n - 1)
+        a = lat[ix, iy] * (1 - sx) + lat[ix + 1, iy] * sx
+        b = lat[ix, iy + 1] * (1 - sx) + lat[ix + 1, iy + 1] * sx
+        out += amp * (a * (1 - sy) + b * sy)
+        amp *= 0.5
+        freq *= 2.0
+    return out
+
+
+def fbm_grid(n=128, seed=0, amplitude=0.15, size=1.0):
+    """n x n quads (2 n^2 triangles) over [-size/2, size/2]^2 in xz with an
+    fBm height field in y."""
+    u = np.linspace(0.0, 1.0, n + 1)
+    X, Z = np.meshgrid(u, u, indexing="ij")
+    H = value_noise_fbm(X, Z, seed) * amplitude
+    pos = np.stack([(X - 0.5) * size, H, (Z - 0.5) * size], axis=-1).reshape(-1, 3)
+    i = np.arange(n)
+    a = (i[:, None] * (n + 1) + i[None, :]).reshape(-1)
+    b, c, d = a + 1, a + n + 2, a + n + 1
+    idx = np.concatenate([np.stack([a, b, c], 1), np.stack([a, c, d], 1)])
+    return pos, idx.astype(np.uint32)
+
+
+def random_rotations(rng, n):
+    """Uniform random rotations from unit quaternions."""
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)], -1),
+        np.stack([2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)], -1),
+        np.stack([2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], -1)], 1)
+
+
+def instanced_materials(width=1920, height=1080, n_instances=1000, n_lights=64, seed=7, subdivisions=5,
+                        grid=128):
+    """1,000 instances of 4 base meshes (an icosphere subdivided 5 times =
+    20,480 triangles; three fBm-displaced 128x128 grid patches = 32,768
+    triangles each) under seeded uniform rotation, uniform scale in [0.2, 1]
+    and translation in a 20 x 5 x 20 box (y up). Per-instance materials: 60%
+    GGX conductor (roughness U[0.05, 0.8], F0 U[0.02, 0.9]), 30% Oren-Nayar
+    (sigma U[0, 0.5], albedo U[0.3, 0.9]^3), 10% rough dielectric (IOR 1.5,
+    roughness 0.05). 64 point lights of log-uniform power P in [1, 100];
+    a point light's intensity is P / (4 pi) so that its light-BVH power
+    (luminance * 4 pi, src/scene/light_sampler.rs:54) equals P."""
+    rng = np.random.default_rng(seed)
+    s = Scene(width, height, fov=40.0)
+    s.look_at((0.0, 9.0, -23.0), (0.0, 1.5, 0.0))
+    s.background = (0.02, 0.02, 0.03)
+    meshes = [s.add_mesh(*icosphere(subdivisions)[:2], normals=icosphere(subdivisions)[2])]
+    for k in range(3):
+        meshes.append(s.add_mesh(*fbm_grid(grid, seed=seed * 10 + k)))
+    kind = rng.uniform(size=n_instances)
+    for i in range(n_instances):
+        if kind[i] < 0.6:
+            m = ggx_conductor(rng.uniform(0.02, 0.9), rng.uniform(0.05, 0.8), id=i + 1)
+        elif kind[i] < 0.9:
+            m = matte(tuple(rng.uniform(0.3, 0.9, 3)), sigma=rng.uniform(0.0, 0.5), id=i + 1)
+        else:
+            m = rough_dielectric(1.5, 0.05, id=i + 1)
+        s.add_material(m)
+    mesh_ids = rng.integers(0, 4, size=n_instances)
+    R = random_rotations(rng, n_instances)
+    scale = rng.uniform(0.2, 1.0, size=n_instances)
+    t = np.stack([rng.uniform(-10, 10, n_instances), rng.uniform(0, 5, n_instances),
+                  rng.uniform(-10, 10, n_instances)], 1)
+    xf = np.zeros((n_instances, 3, 4))
+    xf[:, :, :3] = R * scale[:, None, None]
+    xf[:, :, 3] = t
+    s.add_instances(mesh_ids, np.arange(n_instances), xf.reshape(n_instances, 12))
+    power = np.exp(rng.uniform(np.log(1.0), np.log(100.0), size=n_lights))
+    lp = np.stack([rng.uniform(-11, 11, n_lights), rng.uniform(0.5, 7, n_lights), rng.uniform(-11, 11, n_lights)], 1)
+    for k in range(n_lights):
+        s.add_point_light(tuple(lp[k]), power[k] / (4 * np.pi))
+    return s
+
+
+INSTANCED_MATERIALS = dict(spp=64, max_depth=12, rr_start=3)
+
+
+# ---------------------------------------------------------------------------
+# C4: two rooms, light in the unseen one
+def two_rooms(width=1280, height=720):
+    """Two 4 x 3 x 3 rooms (x in [0,4] and [4,8], y up, z in [0,3]) joined by a
+    partition at x = 4 with one 0.2 (z) x 2.0 (y) opening at z in [1.4, 1.6].
+    A single 1 x 1 area light of radiance 50 hangs on the partition's far side
+    (x = 4.01, facing +x, z in [1.8, 2.8], y in [1.6, 2.6]) so nothing in the
+    camera's room sees it directly. Walls and ceiling: Oren-Nayar albedo 0.7,
+    sigma 0.3; floor: GGX-coated diffuse, roughness 0.3. The camera sits in the
+    first room looking at the partition."""
+    s = Scene(width, height, fov=60.0)
+    s.look_at((0.35, 1.4, 1.2), (4.0, 1.1, 1.5))
+    wall = s.add_material(matte((0.7, 0.7, 0.7), sigma=0.3, id=1))
+    floor = s.add_material(ggx_floor((0.7, 0.7, 0.7), 0.3, id=2))
+    walls = merge([
+        quad((0, 3, 0), (8, 0, 0), (0, 0, 3)),        # ceiling
+        quad((0, 0, 0), (0, 3, 0), (8, 0, 0)),        # z = 0 wall
+        quad((0, 0, 3), (8, 0, 0), (0, 3, 0)),        # z = 3 wall
+        quad((0, 0, 0), (0, 0, 3), (0, 3, 0)),        # x = 0 wall
+        quad((8, 0, 0), (0, 3, 0), (0, 0, 3)),        # x = 8 wall
+        # partition x = 4 with the opening z in [1.4, 1.6], y in [0, 2]
+        quad((4, 0, 0), (0, 3, 0), (0, 0, 1.4)),
+        quad((4, 0, 1.6), (0, 3, 0), (0, 0, 1.4)),
+        quad((4, 2, 1.4), (0, 1, 0), (0, 0, 0.2)),
+    ])
+    s.add_instance(s.add_mesh(*walls), wall)
+    s.add_instance(s.add_mesh(*quad((0, 0, 0), (0, 0, 3), (8, 0, 0))), floor)
+    # Light on the far side of the partition, facing +x (normal = e1 x e2).
+    s.add_emissive_quad((4.01, 1.6, 2.8), (0, 1, 0), (0, 0, -1), (50.0, 50.0, 50.0))
+    s.materials[-1]["id"] = 3
+    return s
+
+
+TWO_ROOMS = dict(max_depth=16, rr_start=3)
+
+
+# ---------------------------------------------------------------------------
+# C5: forest
+def _cylinder(p0, p1, r0, r1, sides=8):
+    axis = p1 - p0
+    L = np.linalg.norm(axis)
+    a = axis / max(L, 1e-9)
+    t = np.cross(a, [1.0, 0.0, 0.0] if abs(a[0]) < 0.9 else [0.0, 1.0, 0.0])
+    t /= np.linalg.norm(t)
+    b = np.cross(a, t)
+    ang = np.linspace(0, 2 * np.pi, sides, endpoint=False)
+    ring = np.cos(ang)[:, None] * t + np.sin(ang)[:, None] * b
+    pos = np.concatenate([p0 + r0 * ring, p1 + r1 * ring])
+    k = np.arange(sides)
+    k1 = (k + 1) % sides
+    idx = np.concatenate([np.stack([k, k1, k1 + sides], 1), np.stack([k, k1 + sides, k + sides], 1)])
+    return pos, idx
+
+
+def tree(seed, levels=7, children=3, leaves_per_tip=20, sides=8):
+    """Seeded L-system-like tree: a trunk that branches `children` ways per
+    level (random tilt and twist, tapering radius), 8-sided branch prisms,
+    and `leaves_per_tip` leaf quads around every tip. Returns (bark, leaves)
+    meshes; with the defaults about 17k bark + 29k leaf triangles."""
+    rng = np.random.default_rng(seed)
+    bark, leaves = [], []
+    stack = [(np.zeros(3), np.array([0.0, 1.0, 0.0]), 4.0, 0.35, 0)]
+    while stack:
+        p, d, L, r, lvl = stack.pop()
+        q = p + d * L
+        bark.append(_cylinder(p, q, r, r * 0.7, sides))
+        if lvl + 1 >= levels:
+            for _ in range(leaves_per_tip):
+                c = q + rng.normal(scale=0.6, size=3)
+                e1 = rng.normal(size=3)
+                e1 = e1 / np.linalg.norm(e1) * 0.35
+                e2 = np.cross(e1, rng.normal(size=3))
+                e2 = e2 / max(np.linalg.norm(e2), 1e-9) * 0.25
+                leaves.append(quad(c - 0.5 * (e1 + e2), e1, e2))
+            continue
+        for k in range(children):
+            tilt = rng.uniform(0.35, 0.8)
+            phi = rng.uniform(0, 2 * np.pi) + k * 2 * np.pi / children
+            t = np.cross(d, [1.0, 0.0, 0.0] if abs(d[0]) < 0.9 else [0.0, 0.0, 1.0])
+            t /= np.linalg.norm(t)
+            b = np.cross(d, t)
+            nd = np.cos(tilt) * d + np.sin(tilt) * (np.cos(phi) * t + np.sin(phi) * b)
+            nd /= np.linalg.norm(nd)
+            stack.append((q, nd, L * rng.uniform(0.6, 0.8), r * 0.7, lvl + 1))
+    return merge(bark), merge(leaves)
+
+
+def forest(width=3840, height=2160, n_trees=20, n_placements=386_000, n_lights=1200, seed=11, terrain=512,
+           tree_levels=7, extent=1000.0):
+    """20 seeded trees (bark + leaf meshes, ~45k triangles per tree; leaves
+    use a constant presence cutout of 0.5) placed 386,000 times with jitter on
+    a 1 km^2 fBm terrain (512 x 512 grid): every placement is two instances
+    (bark, leaves), 772,000 instances in all. 1,200 point lights with colour
+    U[0,1]^3 and log-uniform power in [0.1, 1000] (intensity = P / 4pi)."""
+    rng = np.random.default_rng(seed)
+    s = Scene(width, height, fov=45.0)
+    half = extent / 2
+    s.background = (0.01, 0.01, 0.02)
+    bark_m = s.add_material(matte((0.30, 0.20, 0.12), sigma=0.4, id=1))
+    leaf_m = s.add_material(matte((0.15, 0.45, 0.12), sigma=0.2, presence=0.5, id=2))
+    ground_m = s.add_material(matte((0.35, 0.30, 0.22), sigma=0.5, id=3))
+    tpos, tidx = fbm_grid(terrain, seed=seed, amplitude=40.0 / extent, size=1.0)
+    tpos = tpos * extent
+    s.add_instance(s.add_mesh(tpos, tidx), ground_m)
+    ids = []
+    for k in range(n_trees):
+        bark, leaves = tree(seed * 100 + k, levels=tree_levels)
+        ids.append((s.add_mesh(*bark), s.add_mesh(*leaves)))
+    # Jittered placements on the terrain (height looked up from the grid).
+    g = int(np.ceil(np.sqrt(n_placements)))
+    cell = extent / g
+    k = np.arange(n_placements)
+    xz = np.stack([(k % g + rng.uniform(0.1, 0.9, n_placements)) * cell - half,
+                   (k // g + rng.uniform(0.1, 0.9, n_placements)) * cell - half], 1)
+    hgrid = tpos[:, 1].reshape(terrain + 1, terrain + 1)
+    gi = np.clip(((xz + half) / extent * terrain).astype(int), 0, terrain)
+    y = hgrid[gi[:, 0], gi[:, 1]] - 0.2
+    which = rng.integers(0, n_trees, n_placements)
+    ang = rng.uniform(0, 2 * np.pi, n_placements)
+    sc = rng.uniform(0.7, 1.3, n_placements)
+    c, si = np.cos(ang) * sc, np.sin(ang) * sc
+    xf = np.zeros((n_placements, 3, 4))
+    xf[:, 0, 0], xf[:, 0, 2], xf[:, 1, 1], xf[:, 2, 0], xf[:, 2, 2] = c, si, sc, -si, c
+    xf[:, :, 3] = np.stack([xz[:, 0], y, xz[:, 1]], 1)
+    xf = xf.reshape(n_placements, 12)
+    bark_ids = np.array([ids[w][0] for w in which])
+    leaf_ids = np.array([ids[w][1] for w in which])
+    s.add_instances(bark_ids, np.full(n_placements, bark_m), xf)
+    s.add_instances(leaf_ids, np.full(n_placements, leaf_m), xf)
+    power = np.exp(rng.uniform(np.log(0.1), np.log(1000.0), size=n_lights))
+    col = rng.uniform(0, 1, size=(n_lights, 3))
+    lx = rng.uniform(-half, half, size=(n_lights, 2))
+    lgi = np.clip(((lx + half) / extent * terrain).astype(int), 0, terrain)
+    ly = hgrid[lgi[:, 0], lgi[:, 1]] + rng.uniform(2.0, 12.0, n_lights)
+    for j in range(n_lights):
+        s.add_point_light((lx[j, 0], ly[j], lx[j, 1]), power[j] / (4 * np.pi), tuple(col[j]))
+    cy = hgrid[terrain // 2, terrain // 2]
+    s.look_at((0.0, cy + 35.0, -half * 0.35), (0.0, cy, 0.0))
+    return s
+
+
+FOREST = dict(spp=32, max_depth=10, rr_start=3)

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = set()
-    for h in ("rt_cuda.h",):
+    for h in ("rt_cuda.h", "rt_guide.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names |= set(re.findall(r"\b(rt_[a-z_0-9]+)\s*\(", text))
@@ -27,7 +27,8 @@ def test_library_exports_every_declared_symbol():
     assert declared, "no declarations parsed"
     missing = [n for n in declared if not hasattr(lib, n)]
     assert not missing, missing
-    assert declared == set(backend.EXPORTS)
+    from rtcuda import guide
+    assert declared == set(backend.EXPORTS) | set(guide.EXPORTS)
 
 
 def test_descriptor_layouts_match_headers():

@@ -103,13 +103,14 @@ def test_checkpoint_resume(cornell, tmp_path):
 def test_aov_film(cornell):
     s, _, _ = cornell
     film = render_pt_film(s, 8, max_depth=8)
-    # Back wall centre: white albedo, normal +z, depth ~ distance to z = -1.
-    c = film["albedo"][30, 32]
+    # Back wall above the boxes (row 20, column 40): white albedo, normal +z,
+    # depth = distance from the eye to about (0.47, 0.64, -1), i.e. ~4.96.
+    c = film["albedo"][20, 40]
     assert np.allclose(c, 0.73, atol=1e-5)
-    n = film["normal"][30, 32]
-    assert n[2] > 0.99
-    assert 4.85 < film["depth"][30, 32, 0] < 5.0
-    assert (film["id"][30, 32, 0] == 1)
+    n = film["normal"][20, 40]
+    assert n[2] > 0.999
+    assert 4.9 < film["depth"][20, 40, 0] < 5.05
+    assert film["id"][20, 40, 0] == 1 and film["id"][20, 40, 1] == 1.0
     # Left wall: red albedo; diffuse AOV equals beauty for all-diffuse scenes.
     assert np.allclose(film["albedo"][32, 8], (0.63, 0.065, 0.05), atol=1e-5)
     assert np.allclose(film["diffuse"], film["beauty"], rtol=1e-4, atol=1e-5)
