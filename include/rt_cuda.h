@@ -119,6 +119,9 @@ typedef struct rt_stats {
     double   shadow_ms;         /* last render: time in the shadow kernel */
     double   shade_ms;          /* last render: time in raygen + shade kernels */
     double   total_ms;          /* last render: wall time on the stream */
+    uint64_t guide_steps;       /* last render: training iterations of the learned proposal */
+    uint64_t guide_records;     /* last render: records in the final training batch */
+    double   guide_loss;        /* last render: summed loss of the final training batch */
 } rt_stats;
 
 int rt_get_stats(rt_session* s, rt_stats* out);

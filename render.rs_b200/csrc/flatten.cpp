@@ -180,6 +180,7 @@ struct Collapser {
     std::vector<uint4>& out;
     uint32_t prim_base;
     uint64_t emitted = 0;
+    uint64_t decode_errors = 0;
 
     uint32_t leaf_ref(const BinNode& nd) const { return make_leaf_ref(prim_base + nd.first, nd.count); }
 
@@ -243,6 +244,14 @@ struct Collapser {
                 while (qh < 255 && (double)p[a] + qh * s < cbx.hi[a]) qh += 1;
                 qlo[a][k] = (uint8_t)ql;
                 qhi[a][k] = (uint8_t)qh;
+                // The traversal decodes fma(2^23 + q, s, p - 2^23 s) in f32;
+                // it must reproduce p + q s exactly and enclose the child.
+                float sf = (float)s, p2 = p[a] - 8388608.0f * sf;
+                float dlo = std::fmaf(8388608.0f + (float)ql, sf, p2);
+                float dhi = std::fmaf(8388608.0f + (float)qh, sf, p2);
+                if ((double)dlo != (double)p[a] + ql * s || (double)dhi != (double)p[a] + qh * s ||
+                    (double)dlo > cbx.lo[a] || (double)dhi < cbx.hi[a])
+                    decode_errors++;
             }
         }
         uint4* w = &out[(size_t)idx * WIDE_NODE_WORDS];
@@ -494,6 +503,10 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
         Collapser col{bin, H.nodes, mi.tri_base};
         mi.blas_root = col.emit(0);
         H.blas_nodes += col.emitted;
+        if (col.decode_errors) {
+            *err = "internal: quantised BLAS boxes not conservative";
+            return false;
+        }
     }
     // ---- instances + TLAS ------------------------------------------------
     if (d->n_instances && !d->instances) {
@@ -532,10 +545,21 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
                 b = Box();
                 b.grow_pt(far);
             }
+        Box world;
+        for (const auto& b : ib)
+            if (b.hi[0] < 1e29) world.grow(b);
+        for (int a = 0; a < 3; a++) {
+            H.world_lo[a] = world.lo[a] <= world.hi[a] ? world.lo[a] : 0.0;
+            H.world_hi[a] = world.lo[a] <= world.hi[a] ? world.hi[a] : 0.0;
+        }
         BinBvh tl = build_binary(ib);
         Collapser col{tl, H.nodes, 0};
         H.scalars.tlas_root = col.emit(0);
         H.tlas_nodes = col.emitted;
+        if (col.decode_errors) {
+            *err = "internal: quantised TLAS boxes not conservative";
+            return false;
+        }
         H.inst_xf.resize(3ull * d->n_instances);
         H.inst.resize(d->n_instances);
         for (uint32_t k = 0; k < d->n_instances; k++) {

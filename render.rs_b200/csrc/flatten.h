@@ -26,6 +26,7 @@ struct HostScene {
     std::vector<uint32_t> inf_lights;
     std::vector<float> inf_power;
     uint64_t blas_nodes = 0, tlas_nodes = 0, binary_blas_nodes = 0;
+    double world_lo[3] = {0, 0, 0}, world_hi[3] = {0, 0, 0};  // union of instance bounds
     DevScene scalars{};              // pointer fields unset; scalar fields filled
 };
 

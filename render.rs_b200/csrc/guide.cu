@@ -84,8 +84,10 @@ __device__ void stage_transpose(uint8_t* dst, const __nv_bfloat16* src, int R, i
 
 // ---- encode -------------------------------------------------------------------
 // rec: 16 floats per record (pos xyz, normal xyz, wo xyz, wi xyz, weight, -).
-__global__ void k_guide_encode(GuideDev G, const float* __restrict__ rec, uint32_t n, __nv_bfloat16* X0) {
+__global__ void k_guide_encode(GuideDev G, const float* __restrict__ rec, uint32_t n, const uint32_t* n_dev,
+                               __nv_bfloat16* X0) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n_dev) n = min(n, *n_dev);
     if (i >= n) return;
     const float* r = rec + 16 * (size_t)i;
     float feat[G_IN];
@@ -109,7 +111,9 @@ constexpr int F_W0 = 0, F_W1 = 6144, F_W2 = F_W1 + 8192, F_W3 = F_W2 + 8192, F_X
 
 template <bool TRAIN>
 __global__ void __launch_bounds__(TILE) k_guide_fwd(GuideDev G, const __nv_bfloat16* __restrict__ X0, uint32_t n,
-                                                    __nv_bfloat16* acts, float* out, uint32_t* err) {
+                                                    const uint32_t* n_dev, __nv_bfloat16* acts, float* out,
+                                                    uint32_t* err) {
+    if (n_dev) n = min(n, *n_dev);
     extern __shared__ __align__(1024) uint8_t sm[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
@@ -199,8 +203,9 @@ constexpr int B_WT0 = 0, B_WT1 = 6144, B_WT2 = B_WT1 + 8192, B_WT3 = B_WT2 + 819
 __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloat16* __restrict__ X0,
                                                     const __nv_bfloat16* __restrict__ acts,
                                                     const float* __restrict__ out, const float* __restrict__ rec,
-                                                    uint32_t n, float* gW, float* gb, float* dX0, float* loss_sum,
-                                                    uint32_t* err) {
+                                                    uint32_t n, const uint32_t* n_dev, float* gW, float* gb,
+                                                    float* dX0, float* loss_sum, uint32_t* err) {
+    if (n_dev) n = min(n, *n_dev);
     extern __shared__ __align__(1024) uint8_t sm[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
@@ -360,8 +365,9 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
 
 // ---- hash-grid backward ---------------------------------------------------------
 __global__ void k_guide_hash_bwd(GuideDev G, const float* __restrict__ rec, const float* __restrict__ dX0, uint32_t n,
-                                 float* gtable) {
+                                 const uint32_t* n_dev, float* gtable) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n_dev) n = min(n, *n_dev);
     if (i >= n) return;
     const float* r = rec + 16 * (size_t)i;
     float3 pn = guide_normalize_pos(G, f3(r[0], r[1], r[2]));
@@ -519,31 +525,69 @@ struct rt_guide {
     }
 };
 
-static int launch_forward(rt_guide* g, const float* rec, uint32_t n, bool train, cudaStream_t st) {
+static int launch_forward(rt_guide* g, const float* rec, uint32_t n, bool train, cudaStream_t st,
+                          const uint32_t* n_dev = nullptr) {
     if (n == 0) return 0;
     int rc = g->ensure(n);
     if (rc) return rc;
-    k_guide_encode<<<(n + 127) / 128, 128, 0, st>>>(g->G, rec, n, g->X0);
+    k_guide_encode<<<(n + 127) / 128, 128, 0, st>>>(g->G, rec, n, n_dev, g->X0);
     uint32_t tiles = (n + TILE - 1) / TILE;
     int grid = (int)std::min<uint32_t>(tiles, (uint32_t)g->sms * 2);
     if (train)
-        k_guide_fwd<true><<<grid, TILE, F_BYTES, st>>>(g->G, g->X0, n, g->acts, g->out, g->err);
+        k_guide_fwd<true><<<grid, TILE, F_BYTES, st>>>(g->G, g->X0, n, n_dev, g->acts, g->out, g->err);
     else
-        k_guide_fwd<false><<<grid, TILE, F_BYTES, st>>>(g->G, g->X0, n, g->acts, g->out, g->err);
+        k_guide_fwd<false><<<grid, TILE, F_BYTES, st>>>(g->G, g->X0, n, n_dev, g->acts, g->out, g->err);
     G_TRY(cudaGetLastError());
     return 0;
 }
 
-static int launch_backward(rt_guide* g, const float* rec, uint32_t n, cudaStream_t st) {
+static int launch_backward(rt_guide* g, const float* rec, uint32_t n, cudaStream_t st,
+                           const uint32_t* n_dev = nullptr) {
     uint32_t tiles = (n + TILE - 1) / TILE;
     int grid = (int)std::min<uint32_t>(tiles, (uint32_t)g->sms * 2);
     G_TRY(cudaMemsetAsync(g->loss, 0, 4, st));
-    k_guide_bwd<<<grid, TILE, B_BYTES, st>>>(g->G, g->X0, g->acts, g->out, rec, n, g->gw, g->gw + G_NWEIGHTS, g->dX0,
-                                             g->loss, g->err);
-    k_guide_hash_bwd<<<(n + 127) / 128, 128, 0, st>>>(g->G, rec, g->dX0, n, g->gt);
+    k_guide_bwd<<<grid, TILE, B_BYTES, st>>>(g->G, g->X0, g->acts, g->out, rec, n, n_dev, g->gw, g->gw + G_NWEIGHTS,
+                                             g->dX0, g->loss, g->err);
+    k_guide_hash_bwd<<<(n + 127) / 128, 128, 0, st>>>(g->G, rec, g->dX0, n, n_dev, g->gt);
     G_TRY(cudaGetLastError());
     return 0;
 }
+
+static void launch_adam(rt_guide* g, cudaStream_t st) {
+    g->step++;
+    AdamArgs A{g->lr, 0.9f, 0.99f, 1e-8f, 0, 0};
+    A.c1 = 1.f / (1.f - std::pow(A.b1, (float)g->step));
+    A.c2 = 1.f / (1.f - std::pow(A.b2, (float)g->step));
+    k_guide_adam_mlp<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(A, g->w32, g->gw, g->mw, g->vw, g->w16, G_NWEIGHTS,
+                                                             G_NPARAMS);
+    uint32_t tn = (uint32_t)(G_LEVELS * G_T * 2);
+    k_guide_adam_table<<<(tn + 255) / 256, 256, 0, st>>>(A, g->t32, g->gt, g->mt, g->vt, g->t16, tn);
+}
+
+// ---- entry points for the renderer (guide_internal.h) ------------------------------
+namespace rt {
+
+int guide_infer_counted(rt_guide* g, const float* rec, const uint32_t* n_dev, uint32_t cap, float** raw_out,
+                        cudaStream_t st) {
+    int rc = launch_forward(g, rec, cap, false, st, n_dev);
+    *raw_out = g->out;
+    return rc;
+}
+
+int guide_train_counted(rt_guide* g, const float* rec, const uint32_t* n_dev, uint32_t cap, cudaStream_t st) {
+    int rc = launch_forward(g, rec, cap, true, st, n_dev);
+    rc = rc ? rc : launch_backward(g, rec, cap, st, n_dev);
+    if (rc) return rc;
+    launch_adam(g, st);
+    G_TRY(cudaGetLastError());
+    return 0;
+}
+
+const float* guide_loss_ptr(rt_guide* g) { return g->loss; }
+const uint32_t* guide_err_ptr(rt_guide* g) { return g->err; }
+GuideDev guide_dev(rt_guide* g) { return g->G; }
+
+}  // namespace rt
 
 static int check_err(rt_guide* g, cudaStream_t st) {
     uint32_t e = 0;
@@ -708,14 +752,7 @@ int rt_guide_train_step_device(rt_guide* g, const float* rec, uint32_t n, float*
     int rc = launch_forward(g, rec, n, true, st);
     rc = rc ? rc : launch_backward(g, rec, n, st);
     if (rc) return rc;
-    g->step++;
-    AdamArgs A{g->lr, 0.9f, 0.99f, 1e-8f, 0, 0};
-    A.c1 = 1.f / (1.f - std::pow(A.b1, (float)g->step));
-    A.c2 = 1.f / (1.f - std::pow(A.b2, (float)g->step));
-    k_guide_adam_mlp<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(A, g->w32, g->gw, g->mw, g->vw, g->w16, G_NWEIGHTS,
-                                                             G_NPARAMS);
-    uint32_t tn = (uint32_t)(G_LEVELS * G_T * 2);
-    k_guide_adam_table<<<(tn + 255) / 256, 256, 0, st>>>(A, g->t32, g->gt, g->mt, g->vt, g->t16, tn);
+    launch_adam(g, st);
     G_TRY(cudaGetLastError());
     if (loss_out) {
         G_TRY(cudaMemcpyAsync(loss_out, g->loss, 4, cudaMemcpyDeviceToHost, st));

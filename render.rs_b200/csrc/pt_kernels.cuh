@@ -19,7 +19,7 @@
 // the Metal wavefront it replaces is kernel_wf.metal:155-325.
 #pragma once
 
-#include "shade.cuh"
+#include "guide.cuh"
 
 namespace rt {
 
@@ -57,12 +57,27 @@ struct Paths {
     unsigned long long* stats;  // [0] extension rays, [1] shadow rays
     uint32_t* err;
     uint32_t P;
+    // learned proposal (guided mode)
+    float* g_rec;          // inference records, 16 floats (position, normal, wo)
+    uint32_t* g_idx;       // slot -> inference record (~0 when not guided)
+    uint32_t* g_cnt;       // number of inference records this wave
+    const float* g_raw;    // network outputs, 48 floats per inference record
+    float* tr_rec;         // training vertices: [T][max_depth] x TR_FLOATS
+    float* tb_rec;         // training batch, 16 floats per record
+    uint32_t* tb_cnt;
+    uint32_t tr_stride, tr_phase, tr_T, tb_cap;
 };
+
+// Training vertex: p(3) n(3) wo(3) wi(3) beta(3) L at the next vertex(3), sampled flag, L-set flag.
+#define TR_FLOATS 20
 
 struct PtConsts {
     uint32_t npix, width, max_depth, rr_start, aovs;
     float clamp;
     uint64_t sample0;  // first sample index of the slab
+    uint32_t guided;
+    float alpha;       // one-sample MIS probability of sampling the guide
+    GuideDev G;
 };
 
 // flag bits in Paths::prev.w
@@ -90,6 +105,46 @@ __device__ __forceinline__ void push_queue(uint32_t* q, uint32_t* c, uint32_t va
     if (lane_id() == leader) base = atomicAdd(c, __popc(m));
     base = __shfl_sync(0xFFFFFFFFu, base, leader);
     if (active) q[base + __popc(m & ((1u << lane_id()) - 1u))] = val;
+}
+
+// Hit point, world normal flipped against the ray (to_intersection,
+// src/geometry/mesh.rs:427-439: front face from the unflipped normal),
+// outgoing direction and material of a closest-hit record.
+struct HitGeo {
+    float3 p, nw, wo;
+    float eucl;
+    uint32_t mat;
+    bool front;
+};
+
+__device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3 d, uint4 hr, HitGeo& g) {
+    float t = __uint_as_float(hr.x);
+    g.p = o + d * t;
+    uint32_t il = hr.z;
+    float4 x0 = __ldg(S.inst_xf + 3 * (size_t)il), x1 = __ldg(S.inst_xf + 3 * (size_t)il + 1),
+           x2 = __ldg(S.inst_xf + 3 * (size_t)il + 2);
+    uint4 info = __ldg(S.inst + il);
+    const float4* tp = S.tris + 3 * (size_t)hr.y;
+    float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+    float3 nl;
+    MeshInfo mi = S.meshes[info.w];
+    if (mi.idx_base != 0xFFFFFFFFu) {
+        // Interpolated vertex normals (Mesh::local_normal, mesh.rs:200-220).
+        float b1 = __half2float(__ushort_as_half((unsigned short)(hr.w & 0xFFFFu)));
+        float b2 = __half2float(__ushort_as_half((unsigned short)(hr.w >> 16)));
+        uint32_t ot = __float_as_uint(v0.w);
+        const uint32_t* ix = S.orig_idx + mi.idx_base + 3 * (size_t)ot;
+        auto nrm = [&](uint32_t v) { return f3(S.normals[3 * v], S.normals[3 * v + 1], S.normals[3 * v + 2]); };
+        nl = normalize_ref(nrm(ix[0]) * (1.0f - b1 - b2) + nrm(ix[1]) * b1 + nrm(ix[2]) * b2);
+    } else {
+        nl = normalize_ref(cross(xyz(v1) - xyz(v0), xyz(v2) - xyz(v0)));
+    }
+    float3 nw = normalize_ref(xf_normal(x0, x1, x2, nl));
+    g.front = dot(nw, d) < 0.0f;
+    g.nw = g.front ? nw : -nw;
+    g.wo = -normalize_ref(d);
+    g.eucl = length(g.p - o);
+    g.mat = info.z;
 }
 
 // ---- raygen: camera rays for all P slots ------------------------------------------
@@ -152,48 +207,215 @@ __global__ void k_raygen(DevScene S, Paths P, PtConsts C) {
     }
     P.q_ext[0][i] = i;
     if (i == 0) P.cnt[CNT_EXT_IN] = P.P;
+    if (C.guided && i % P.tr_stride == P.tr_phase && i / P.tr_stride < P.tr_T) {
+        float* r = P.tr_rec + (size_t)(i / P.tr_stride) * C.max_depth * TR_FLOATS;
+        for (uint32_t d = 0; d < C.max_depth; d++) r[d * TR_FLOATS + 18] = r[d * TR_FLOATS + 19] = 0.0f;
+    }
+}
+
+// ---- learned proposal: network inputs for this wave's guided vertices ------------------
+// Vertices of diffuse, conductor and mixed materials get a record (position,
+// shading normal facing wo, wo); the shade kernel reads the network output
+// through g_idx. Glass, emitters and misses keep plain BSDF sampling.
+__global__ void __launch_bounds__(128) k_guide_gather(DevScene S, Paths P) {
+    uint32_t counts[N_QUEUES];
+    uint32_t total = 0;
+#pragma unroll
+    for (uint32_t c = 0; c < N_QUEUES; c++) {
+        counts[c] = P.cnt[CNT_CLASS + c];
+        total += counts[c];
+    }
+    uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t j0 = blockIdx.x * blockDim.x; j0 < total; j0 += stride) {
+        uint32_t j = j0 + threadIdx.x;
+        bool active = j < total, want = false;
+        uint32_t slot = 0;
+        float rec[9];
+        if (active) {
+            uint32_t c = CLS_MISS, off = j;
+            if (off >= counts[CLS_MISS]) {
+                off -= counts[CLS_MISS];
+                for (uint32_t k = 0; k < N_MAT_CLASSES; k++) {
+                    if (off < counts[k]) {
+                        c = k;
+                        break;
+                    }
+                    off -= counts[k];
+                }
+            }
+            slot = P.q_cls[(size_t)c * P.P + off];
+            want = c == MAT_DIFFUSE || c == MAT_CONDUCTOR || c == MAT_MIXED;
+            if (want) {
+                HitGeo hg;
+                hit_geometry(S, xyz(P.ray_o[slot]), xyz(P.ray_d[slot]), P.hit[slot], hg);
+                float3 n = dot(hg.nw, hg.wo) >= 0.0f ? hg.nw : -hg.nw;
+                rec[0] = hg.p.x; rec[1] = hg.p.y; rec[2] = hg.p.z;
+                rec[3] = n.x; rec[4] = n.y; rec[5] = n.z;
+                rec[6] = hg.wo.x; rec[7] = hg.wo.y; rec[8] = hg.wo.z;
+            } else {
+                P.g_idx[slot] = 0xFFFFFFFFu;
+            }
+        }
+        uint32_t m = __ballot_sync(0xFFFFFFFFu, want);
+        if (m) {
+            uint32_t leader = __ffs(m) - 1, base = 0;
+            if (lane_id() == leader) base = atomicAdd(P.g_cnt, __popc(m));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (want) {
+                uint32_t idx = base + __popc(m & ((1u << lane_id()) - 1u));
+                P.g_idx[slot] = idx;
+                float4* r = reinterpret_cast<float4*>(P.g_rec + (size_t)idx * 16);
+                r[0] = make_float4(rec[0], rec[1], rec[2], rec[3]);
+                r[1] = make_float4(rec[4], rec[5], rec[6], rec[7]);
+                r[2] = make_float4(rec[8], 0.f, 0.f, 0.f);
+                r[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+    }
+}
+
+// ---- learned proposal: training batch from the slab's closed vertices -------------------
+// weight = lum(L_end - L_vertex) / lum(beta_vertex) estimates
+// lum(f cos Li) / pdf for the direction the path actually took (capped at 50).
+__global__ void k_guide_collect(Paths P, PtConsts C) {
+    uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t t = id / C.max_depth, d = id % C.max_depth;
+    bool ok = false;
+    float w = 0.f;
+    const float* r = nullptr;
+    if (t < P.tr_T) {
+        uint32_t slot = t * P.tr_stride + P.tr_phase;
+        r = P.tr_rec + ((size_t)t * C.max_depth + d) * TR_FLOATS;
+        if (slot < P.P && r[18] != 0.0f && r[19] != 0.0f) {
+            float4 Le = P.L[slot];
+            float3 dl = f3(Le.x - r[15], Le.y - r[16], Le.z - r[17]);
+            w = luminance(dl) / fmaxf(luminance(f3(r[12], r[13], r[14])), 1e-8f);
+            ok = w > 0.0f && isfinite(w);
+        }
+    }
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, ok);
+    if (!m) return;
+    uint32_t leader = __ffs(m) - 1, base = 0;
+    if (lane_id() == leader) base = atomicAdd(P.tb_cnt, __popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (!ok) return;
+    uint32_t idx = base + __popc(m & ((1u << lane_id()) - 1u));
+    if (idx >= P.tb_cap) return;
+    float* o = P.tb_rec + (size_t)idx * 16;
+    for (int k = 0; k < 12; k++) o[k] = r[k];
+    o[12] = fminf(w, 50.0f);
+    o[13] = o[14] = o[15] = 0.0f;
+}
+
+// ---- persistent ray pump ----------------------------------------------------------------
+// Each warp keeps 32 rays in flight. A lane whose ray finishes is refilled
+// from the global work counter as soon as half the warp is idle (one
+// warp-aggregated atomic per refill), so a few long rays no longer hold a
+// warp's other lanes hostage (Aila & Laine 2009, "persistent while-while").
+// load(j, o, d, tmax) reads work item j; finish(done, j, ts) is called by
+// the whole warp whenever some lane finished, with `done` true on those lanes.
+// Within a warp the work alternates between a node phase (every lane that
+// has no parked leaf tests nodes until it parks one or finishes) and a leaf
+// phase (every lane with a parked leaf processes it), so lanes mostly run
+// the same code path.
+template <bool ANY, class Load, class Finish>
+__device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
+                                         TravStack& st, Load load, Finish finish) {
+    PhaseState ps;
+    bool active = false, exhausted = false;
+    uint32_t item = 0, steps = 0;
+    const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
+    for (;;) {
+        uint32_t act = __ballot_sync(0xFFFFFFFFu, active);
+        if (!exhausted && __popc(act) <= 16) {
+            uint32_t idle = ~act;
+            uint32_t leader = __ffs(idle) - 1, base = 0;
+            if (lane == leader) base = atomicAdd(fetch, __popc(idle));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (base >= n || n - base <= (uint32_t)__popc(idle)) exhausted = true;
+            bool fresh = false;
+            if (!active) {
+                uint32_t j = base + __popc(idle & lt);
+                if (base < n && j < n) {
+                    item = j;
+                    float3 o, d;
+                    float tmax;
+                    load(j, o, d, tmax);
+                    active = trav_begin(S, ps.ts, st, o, d, tmax);
+                    if (active) {
+                        phase_begin(ps);
+                        steps = 0;
+                    } else {
+                        fresh = true;  // empty scene: a miss, finished at once
+                    }
+                }
+            }
+            if (__any_sync(0xFFFFFFFFu, fresh)) finish(fresh, item, ps.ts);
+            act = __ballot_sync(0xFFFFFFFFu, active);
+        }
+        if (act == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        // Node phase.
+        for (;;) {
+            bool want = active && ps.pending == 0;
+            if (!__any_sync(0xFFFFFFFFu, want)) break;
+            bool done_now = false;
+            if (want) {
+                if (++steps > RT_MAX_TRAV_STEPS) {
+                    atomicOr(err, RT_DEVERR_ITER);
+                    done_now = true;
+                } else if (ps.need_pop) {
+                    done_now = !op_pop(ps, st);
+                } else {
+                    done_now = op_node<ANY>(S, ps, st, err);
+                }
+            }
+            if (__any_sync(0xFFFFFFFFu, done_now)) finish(done_now, item, ps.ts);
+            if (done_now) active = false;
+        }
+        // Leaf phase.
+        bool done_now = false;
+        if (active && ps.pending) done_now = op_leaf<ANY>(S, ps, st, err);
+        if (__any_sync(0xFFFFFFFFu, done_now)) finish(done_now, item, ps.ts);
+        if (done_now) active = false;
+    }
 }
 
 // ---- extend ---------------------------------------------------------------------------
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_extend(DevScene S, Paths P, uint32_t qsel) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
-    __shared__ uint32_t warp_base[BLOCK / 32];
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
     const uint32_t* q = P.q_ext[qsel];
-    uint32_t n = P.cnt[CNT_EXT_IN];
-    uint32_t w = threadIdx.x >> 5;
+    const uint32_t n = P.cnt[CNT_EXT_IN];
     unsigned long long rays = 0;
-    for (;;) {
-        if (lane_id() == 0) warp_base[w] = atomicAdd(&P.cnt[CNT_FETCH_EXT], 32u);
-        __syncwarp();
-        uint32_t base = warp_base[w];
-        __syncwarp();
-        if (base >= n) break;
-        uint32_t j = base + lane_id();
-        bool active = j < n;
-        uint32_t slot = 0, cls = CLS_MISS;
-        if (active) {
-            slot = q[j];
-            float4 o = P.ray_o[slot], d = P.ray_d[slot];
-            TraceHit h;
-            trace<false>(S, xyz(o), xyz(d), d.w, h, st, P.err);
+    uint32_t slot = 0;
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
+        slot = q[j];
+        float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot];
+        o = xyz(o4);
+        d = xyz(d4);
+        tmax = d4.w;
+    };
+    auto finish = [&](bool done, uint32_t, const TravState& ts) {
+        uint32_t cls = CLS_MISS;
+        if (done) {
+            const TraceHit& h = ts.hit;
             uint32_t uv = (uint32_t)__half_as_ushort(__float2half_rn(h.b1)) |
                           ((uint32_t)__half_as_ushort(__float2half_rn(h.b2)) << 16);
-            P.hit[slot] = make_uint4(__float_as_uint(h.t), h.tri, h.inst, uv);
-            if (h.tri != 0xFFFFFFFFu) {
-                uint32_t mat = __ldg(&S.inst[h.inst].z);
-                cls = __ldg(&S.materials[mat].mclass);
-            }
+            uint32_t tri = ts.found ? h.tri : 0xFFFFFFFFu;
+            P.hit[slot] = make_uint4(__float_as_uint(h.t), tri, h.inst, uv);
+            if (ts.found) cls = __ldg(&S.materials[__ldg(&S.inst[h.inst].z)].mclass);
             rays++;
         }
-        // Bucket by class: one atomic per (warp, class).
-        for (uint32_t c = 0; c < N_QUEUES; c++) {
-            bool mine = active && cls == c;
-            push_queue(P.q_cls + (size_t)c * P.P, &P.cnt[CNT_CLASS + c], slot, mine);
-        }
-    }
+        // Bucket by material class: one atomic per (warp, class).
+        for (uint32_t c = 0; c < N_QUEUES; c++)
+            push_queue(P.q_cls + (size_t)c * P.P, &P.cnt[CNT_CLASS + c], slot, done && cls == c);
+    };
+    ray_pump<false>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, st, load, finish);
     if (rays) atomicAdd(&P.stats[0], rays);
 }
 
@@ -207,15 +429,20 @@ struct NeeOut {
 // its unoccluded contribution (already divided by the pick pmf).
 __device__ __forceinline__ bool nee_light(const DevScene& S, const DevLight& L, float3 p, float3 n, const Frame& fr,
                                           float3 wo_l, float eta, const DevMaterial& m, float pick, Pcg& rng,
-                                          NeeOut& out) {
+                                          NeeOut& out, const Mixture* mix = nullptr, float alpha = 0.0f) {
     float3 Le = f3(L.radiance[0], L.radiance[1], L.radiance[2]);
+    // BSDF value with cosine, and the pdf of the direction-sampling strategy
+    // it is MIS-weighted against: the BSDF pdf, or under guiding the one-sample
+    // mixture alpha * q + (1 - alpha) * p_bsdf.
     auto eval = [&](float3 wi, float& pdf) -> float3 {
         float3 wl = fr.to_local(wi);
         if (wl.z <= 0.0f) {
             pdf = 0.0f;
             return f3(0, 0, 0);
         }
-        return bsdf_eval(m, wo_l, wl, eta, pdf) * wl.z;
+        float3 f = bsdf_eval(m, wo_l, wl, eta, pdf) * wl.z;
+        if (mix) pdf = alpha * mixture_pdf(*mix, wi) + (1.0f - alpha) * pdf;
+        return f;
     };
     auto shadow_to = [&](float3 target) {
         float3 dir = target - p;
@@ -380,36 +607,32 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
                     auxd.z += c.z;
                 }
             };
+            // Training: close the previous vertex's record with the radiance
+            // gathered so far (its own emission and NEE included).
+            auto tr_close = [&]() {
+                if (!C.guided || slot % P.tr_stride != P.tr_phase) return;
+                uint32_t d0 = flags >> FL_DEPTH_SHIFT, t = slot / P.tr_stride;
+                if (d0 == 0 || t >= P.tr_T) return;
+                float* r = P.tr_rec + ((size_t)t * C.max_depth + (d0 - 1)) * TR_FLOATS;
+                if (r[18] != 0.0f && r[19] == 0.0f) {
+                    r[15] = Lr.x;
+                    r[16] = Lr.y;
+                    r[17] = Lr.z;
+                    r[19] = 1.0f;
+                }
+            };
             if (hr.y == 0xFFFFFFFFu) {
+                tr_close();
                 emit(beta * f3(S.background[0], S.background[1], S.background[2]));
             } else {
-                float t = __uint_as_float(hr.x);
-                float3 p = o + d * t;
-                uint32_t il = hr.z;
-                float4 x0 = __ldg(S.inst_xf + 3 * (size_t)il), x1 = __ldg(S.inst_xf + 3 * (size_t)il + 1),
-                       x2 = __ldg(S.inst_xf + 3 * (size_t)il + 2);
-                uint4 info = __ldg(S.inst + il);
-                const float4* tp = S.tris + 3 * (size_t)hr.y;
-                float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
-                float3 nl;
-                MeshInfo mi = S.meshes[info.w];
-                if (mi.idx_base != 0xFFFFFFFFu) {
-                    float b1 = __half2float(__ushort_as_half((unsigned short)(hr.w & 0xFFFFu)));
-                    float b2 = __half2float(__ushort_as_half((unsigned short)(hr.w >> 16)));
-                    uint32_t ot = __float_as_uint(v0.w);
-                    const uint32_t* ix = S.orig_idx + mi.idx_base + 3 * (size_t)ot;
-                    auto nrm = [&](uint32_t v) { return f3(S.normals[3 * v], S.normals[3 * v + 1], S.normals[3 * v + 2]); };
-                    nl = normalize_ref(nrm(ix[0]) * (1.0f - b1 - b2) + nrm(ix[1]) * b1 + nrm(ix[2]) * b2);
-                } else {
-                    nl = normalize_ref(cross(xyz(v1) - xyz(v0), xyz(v2) - xyz(v0)));
-                }
-                float3 nw = normalize_ref(xf_normal(x0, x1, x2, nl));
-                bool front = dot(nw, d) < 0.0f;
-                if (!front) nw = -nw;
-                float3 wo = -normalize_ref(d);
-                float eucl = length(p - o);
+                HitGeo hg;
+                hit_geometry(S, o, d, hr, hg);
+                const float3 p = hg.p, wo = hg.wo;
+                float3 nw = hg.nw;
+                const bool front = hg.front;
+                const float eucl = hg.eucl;
                 travel += eucl;
-                const DevMaterial& m = S.materials[info.z];
+                const DevMaterial& m = S.materials[hg.mat];
                 if (C.aovs && !(flags & FL_AUX_SET)) {
                     flags |= FL_AUX_SET;
                     float3 an = dot(nw, wo) >= 0.0f ? nw : -nw;
@@ -430,6 +653,7 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
                     done = true;
                 }
                 if (!done) {
+                    tr_close();
                     float3 n = dot(nw, wo) >= 0.0f ? nw : -nw;
                     float eta = front ? m.ior : 1.0f / m.ior;
                     float3 em = f3(m.emission[0], m.emission[1], m.emission[2]);
@@ -445,12 +669,23 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
                     }
                     Frame fr(n);
                     float3 wo_l = fr.to_local(wo);
+                    // Learned proposal at this vertex (guided mode only).
+                    Mixture mix;
+                    bool guided = false;
+                    if (C.guided) {
+                        uint32_t gi = P.g_idx[slot];
+                        if (gi != 0xFFFFFFFFu) {
+                            mixture_decode(P.g_raw + (size_t)gi * G_OUT, mix);
+                            guided = true;
+                        }
+                    }
                     if (S.n_lights > 0 && m.has_lobes != 0.0f) {
                         uint32_t li;
                         float pmf;
                         if (light_sample(S, p, rng.next_f(), li, pmf)) {
                             NeeOut ne;
-                            if (nee_light(S, S.lights[li], p, n, fr, wo_l, eta, m, pmf, rng, ne)) {
+                            if (nee_light(S, S.lights[li], p, n, fr, wo_l, eta, m, pmf, rng, ne,
+                                          guided ? &mix : nullptr, C.alpha)) {
                                 float3 c = beta * ne.c;
                                 if (maxc(c) > 0.0f) {
                                     P.sh_o[slot] = make_float4(ne.o.x, ne.o.y, ne.o.z, 0.0f);
@@ -462,13 +697,52 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
                         }
                     }
                     BsdfSample bs;
-                    if (bsdf_sample(m, wo_l, eta, rng, bs)) {
+                    bool sampled;
+                    float pdf_path = 0.0f;
+                    if (guided) {
+                        // One-sample MIS: the guide with probability alpha, else the
+                        // BSDF; the path pdf is the mixture of both full pdfs.
+                        if (rng.next_f() < C.alpha) {
+                            float u0 = rng.next_f(), u1 = rng.next_f(), u2 = rng.next_f();
+                            bs.wi = fr.to_local(mixture_sample(mix, u0, u1, u2));
+                            bs.f = bsdf_eval(m, wo_l, bs.wi, eta, bs.pdf);
+                            bs.transmitted = bs.wi.z < 0.0f;
+                            bs.specular = false;
+                            sampled = maxc(bs.f) > 0.0f;
+                        } else {
+                            sampled = bsdf_sample(m, wo_l, eta, rng, bs);
+                        }
+                        if (sampled) {
+                            pdf_path = C.alpha * mixture_pdf(mix, fr.to_world(bs.wi)) + (1.0f - C.alpha) * bs.pdf;
+                            sampled = pdf_path > 0.0f;
+                        }
+                    } else {
+                        sampled = bsdf_sample(m, wo_l, eta, rng, bs);
+                        pdf_path = bs.pdf;
+                    }
+                    if (sampled) {
                         float3 wi = fr.to_world(bs.wi);
-                        beta = beta * bs.f * (fabsf(bs.wi.z) / bs.pdf);
+                        const float3 beta_in = beta;
+                        beta = beta * bs.f * (fabsf(bs.wi.z) / pdf_path);
+                        if (C.guided && slot % P.tr_stride == P.tr_phase) {
+                            // Training vertex: closed with the radiance at the next vertex.
+                            uint32_t t = slot / P.tr_stride, d0 = flags >> FL_DEPTH_SHIFT;
+                            if (t < P.tr_T && d0 < C.max_depth) {
+                                float* r = P.tr_rec + ((size_t)t * C.max_depth + d0) * TR_FLOATS;
+                                float3 wn = normalize_ref(wi);
+                                r[0] = p.x; r[1] = p.y; r[2] = p.z;
+                                r[3] = n.x; r[4] = n.y; r[5] = n.z;
+                                r[6] = wo.x; r[7] = wo.y; r[8] = wo.z;
+                                r[9] = wn.x; r[10] = wn.y; r[11] = wn.z;
+                                r[12] = beta_in.x; r[13] = beta_in.y; r[14] = beta_in.z;
+                                r[18] = 1.0f;
+                                r[19] = 0.0f;
+                            }
+                        }
                         if ((flags & FL_SPEC_MASK) == FL_SPEC_NONE)
                             flags = (flags & ~FL_SPEC_MASK) | (bs.specular ? FL_SPEC_TRUE : 0u);
                         flags &= ~FL_FROM_CAMERA;
-                        beta4.w = bs.pdf;
+                        beta4.w = pdf_path;
                         prev4 = make_float4(p.x, p.y, p.z, 0.0f);
                         float off = bs.transmitted ? -RT_RAY_OFFSET : RT_RAY_OFFSET;
                         float3 no = p + n * off;
@@ -510,6 +784,34 @@ __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene S, Paths P, PtConsts 
     uint32_t n = P.cnt[CNT_SHADOW];
     uint32_t w = threadIdx.x >> 5;
     unsigned long long rays = 0;
+    auto add = [&](uint32_t slot, float vis) {
+        float4 c = P.sh_c[slot];
+        float4 L = P.L[slot];
+        P.L[slot] = make_float4(L.x + c.x * vis, L.y + c.y * vis, L.z + c.z * vis, L.w);
+        if (C.aovs && c.w != 0.0f) {
+            float4 a = P.aux_d[slot];
+            P.aux_d[slot] = make_float4(a.x + c.x * vis, a.y + c.y * vis, a.z + c.z * vis, a.w);
+        }
+    };
+    if (!S.any_presence) {
+        // Opaque scenes: one any-hit query per shadow ray, through the pump.
+        uint32_t slot = 0;
+        auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
+            slot = P.q_sh[j];
+            float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
+            o = xyz(o4);
+            d = xyz(d4);
+            tmax = d4.w;
+        };
+        auto finish = [&](bool done, uint32_t, const TravState& ts) {
+            if (!done) return;
+            rays++;
+            if (!ts.found) add(slot, 1.0f);
+        };
+        ray_pump<true>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, load, finish);
+        if (rays) atomicAdd(&P.stats[1], rays);
+        return;
+    }
     for (;;) {
         if (lane_id() == 0) warp_base[w] = atomicAdd(&P.cnt[CNT_FETCH_SH], 32u);
         __syncwarp();
@@ -617,36 +919,32 @@ __global__ void __launch_bounds__(BLOCK) k_intersect(DevScene S, const float4* _
                                                      const float4* __restrict__ dir, uint64_t n, uint32_t* prim,
                                                      uint32_t* inst, float* tout, uint32_t* fetch, uint32_t* err) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
-    __shared__ uint32_t warp_base[BLOCK / 32];
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
-    uint32_t w = threadIdx.x >> 5;
-    for (;;) {
-        if (lane_id() == 0) warp_base[w] = atomicAdd(fetch, 32u);
-        __syncwarp();
-        uint64_t base = warp_base[w];
-        __syncwarp();
-        if (base >= n) break;
-        uint64_t i = base + lane_id();
-        if (i >= n) continue;
-        float4 o = __ldg(org + i), d = __ldg(dir + i);
-        TraceHit h;
-        bool hit = trace<ANY>(S, xyz(o), xyz(d), d.w, h, st, err);
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
+        float4 o4 = __ldg(org + j), d4 = __ldg(dir + j);
+        o = xyz(o4);
+        d = xyz(d4);
+        tmax = d4.w;
+    };
+    auto finish = [&](bool done, uint32_t i, const TravState& ts) {
+        if (!done) return;
         if (ANY) {
-            prim[i] = hit ? 1u : 0u;
+            prim[i] = ts.found ? 1u : 0u;
         } else {
             uint32_t p = 0xFFFFFFFFu, ii = 0xFFFFFFFFu;
             float t = INFINITY;
-            if (hit) {
-                p = __float_as_uint(__ldg(&S.tris[3 * (size_t)h.tri].w));
-                ii = __ldg(&S.inst[h.inst].y);
-                t = h.t;
+            if (ts.found) {
+                p = __float_as_uint(__ldg(&S.tris[3 * (size_t)ts.hit.tri].w));
+                ii = __ldg(&S.inst[ts.hit.inst].y);
+                t = ts.hit.t;
             }
             prim[i] = p;
             if (inst) inst[i] = ii;
             if (tout) tout[i] = t;
         }
-    }
+    };
+    ray_pump<ANY>(S, (uint32_t)n, fetch, err, st, load, finish);
 }
 
 // White-furnace estimator of one material: per thread, `per` BSDF samples

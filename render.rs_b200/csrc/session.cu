@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "flatten.h"
+#include "guide_internal.h"
 #include "pt_kernels.cuh"
 #include "rt_cuda.h"
 
@@ -61,6 +62,10 @@ struct rt_session {
     uint32_t* fetch = nullptr;     // ray-batch work counter
     uint32_t npix = 0;
     uint32_t samples_done = 0;
+    // learned proposal (params.guided)
+    rt_guide* guide = nullptr;
+    uint64_t guide_records = 0;
+    double guide_loss = 0.0;
     // ray-batch staging for host-pointer calls
     void* batch_buf = nullptr;
     size_t batch_cap = 0;
@@ -111,6 +116,7 @@ struct rt_session {
         for (auto& e : evpool) cudaEventDestroy(e);
         for (void* p : allocs) cudaFree(p);
         if (batch_buf) cudaFree(batch_buf);
+        if (guide) rt_guide_destroy(guide);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -173,7 +179,10 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     }
     // Path state: slabs of whole sample passes (see pt_kernels.cuh).
     s->npix = scene->camera.width * scene->camera.height;
-    uint64_t cap = params->max_paths ? params->max_paths : (8ull << 20);
+    // Guided renders train between slabs, so they default to one sample pass
+    // per slab (one network update per sample per pixel).
+    const bool guided = params->guided != 0;
+    uint64_t cap = params->max_paths ? params->max_paths : guided ? (uint64_t)s->npix : (8ull << 20);
     uint64_t k = std::max<uint64_t>(1, cap / s->npix);
     if (k * s->npix > 0xFFFFFFFFull / 8) k = std::max<uint64_t>(1, (0xFFFFFFFFull / 8) / s->npix);
     s->slab_samples = (uint32_t)k;
@@ -204,6 +213,28 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     rc = rc ? rc : s->alloc(&s->fetch, 1);
     rc = rc ? rc : s->alloc(&s->accum, 4ull * s->npix);
     rc = rc ? rc : s->alloc(&s->aux, aov ? 12ull * s->npix : 1);
+    // Guiding: inference records per slot, training vertices for a strided
+    // subset of ~16k paths per slab, and a 2^16-record training batch.
+    const uint32_t tr_paths = 16384;
+    Pp.tr_stride = guided ? (uint32_t)std::max<uint64_t>(1, P / tr_paths) : 1u;
+    Pp.tr_T = guided ? (uint32_t)((P + Pp.tr_stride - 1) / Pp.tr_stride) : 0u;
+    Pp.tr_phase = 0;
+    Pp.tb_cap = guided ? (1u << 16) : 0u;
+    rc = rc ? rc : s->alloc(&Pp.g_rec, guided ? P * 16 : 1);
+    rc = rc ? rc : s->alloc(&Pp.g_idx, guided ? P : 1);
+    rc = rc ? rc : s->alloc(&Pp.g_cnt, 1);
+    rc = rc ? rc : s->alloc(&Pp.tr_rec, guided ? (size_t)Pp.tr_T * params->max_depth * TR_FLOATS : 1);
+    rc = rc ? rc : s->alloc(&Pp.tb_rec, guided ? (size_t)Pp.tb_cap * 16 : 1);
+    rc = rc ? rc : s->alloc(&Pp.tb_cnt, 1);
+    if (!rc && guided) {
+        float lo[3], hi[3];
+        for (int a = 0; a < 3; a++) {
+            double pad = 1e-3 * (s->host.world_hi[a] - s->host.world_lo[a]) + 1e-6;
+            lo[a] = (float)(s->host.world_lo[a] - pad);
+            hi[a] = (float)(s->host.world_hi[a] + pad);
+        }
+        if (rt_guide_create(lo, hi, 0x5eed, 1e-2f, &s->guide) != 0) rc = fail(RT_ERR_CUDA, rt_guide_last_error());
+    }
     if (rc) {
         delete s;
         return rc;
@@ -250,6 +281,11 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     C.rr_start = s->params.rr_start;
     C.aovs = s->params.aovs;
     C.clamp = (float)s->params.firefly_clamp;
+    C.guided = s->guide ? 1u : 0u;
+    C.alpha = (float)std::min(std::max(s->params.guide_fraction, 0.0), 1.0);
+    if (s->guide) C.G = guide_dev(s->guide);
+    uint64_t guide_records = 0;
+    int guide_trainings = 0;
     uint32_t waves = s->params.max_depth + (s->S.any_presence ? RT_MAX_PRESENCE_SKIPS : 0u);
     const int trav_grid = s->trav_grid, shade_grid = s->sm_count * 8;
     CUDA_TRY(cudaMemsetAsync(s->stats, 0, 32, st));
@@ -279,6 +315,16 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
             CUDA_TRY(cudaEventRecord(s->evpool[ei], st));
             k_extend<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 1], st));
+            if (s->guide) {
+                // Network inputs for this wave's guided vertices, then inference.
+                CUDA_TRY(cudaMemsetAsync(P.g_cnt, 0, 4, st));
+                k_guide_gather<<<shade_grid, 128, 0, st>>>(s->S, P);
+                float* raw = nullptr;
+                int grc = guide_infer_counted(s->guide, P.g_rec, P.g_cnt, P.P, &raw, st);
+                if (grc) return fail(grc, rt_guide_last_error());
+                P.g_raw = raw;
+                launches += 3;
+            }
             k_shade<<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 2], st));
             k_shadow<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
@@ -289,6 +335,18 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
         }
         k_accumulate<<<(s->npix + 255) / 256, 256, 0, st>>>(P, C, k, s->accum, s->aux);
         launches++;
+        if (s->guide) {
+            // One Adam step on the vertices this slab closed, then a new
+            // training subset for the next slab.
+            CUDA_TRY(cudaMemsetAsync(P.tb_cnt, 0, 4, st));
+            uint32_t nthreads = P.tr_T * C.max_depth;
+            k_guide_collect<<<(nthreads + 127) / 128, 128, 0, st>>>(P, C);
+            int grc = guide_train_counted(s->guide, P.tb_rec, P.tb_cnt, P.tb_cap, st);
+            if (grc) return fail(grc, rt_guide_last_error());
+            guide_trainings++;
+            launches += 7;
+            P.tr_phase = (P.tr_phase + 1) % P.tr_stride;
+        }
         done += k;
     }
     CUDA_TRY(cudaEventRecord(s->evpool[1], st));
@@ -317,6 +375,19 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     s->last.shadow_ms = ms_sh;
     s->last.shade_ms = ms_shade;
     s->last.total_ms = total;
+    s->last.guide_steps = (uint64_t)guide_trainings;
+    s->last.guide_records = 0;
+    s->last.guide_loss = 0.0;
+    if (s->guide) {
+        uint32_t gerr = 0, nrec = 0;
+        float loss = 0.f;
+        CUDA_TRY(cudaMemcpy(&gerr, guide_err_ptr(s->guide), 4, cudaMemcpyDeviceToHost));
+        if (gerr) return fail(RT_ERR_DEVICE, "guide network: tensor-core pipeline wait timed out");
+        CUDA_TRY(cudaMemcpy(&nrec, P.tb_cnt, 4, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(&loss, guide_loss_ptr(s->guide), 4, cudaMemcpyDeviceToHost));
+        s->last.guide_records = std::min(nrec, P.tb_cap);
+        s->last.guide_loss = loss;
+    }
     s->samples_done += count;
     return RT_OK;
 }

@@ -153,22 +153,31 @@ __device__ __forceinline__ void test_node(const uint4* __restrict__ nodes, uint3
     const uint4* n = nodes + (size_t)idx * WIDE_NODE_WORDS;
     uint4 w0 = __ldg(n + 0), w1 = __ldg(n + 1), w2 = __ldg(n + 2), w3 = __ldg(n + 3);
     uint4 w4 = __ldg(n + 4), w5 = __ldg(n + 5);
-    float px = __uint_as_float(w0.x), py = __uint_as_float(w0.y), pz = __uint_as_float(w0.z);
     float sx = __uint_as_float((w0.w & 0xFFu) << 23);
     float sy = __uint_as_float(((w0.w >> 8) & 0xFFu) << 23);
     float sz = __uint_as_float(((w0.w >> 16) & 0xFFu) << 23);
+    // Planes decode as fma(2^23 + q, s, p - 2^23 s): the byte q is spliced
+    // into the mantissa of 2^23 with one byte permute. p = k s with
+    // |k| <= 2^20 (the build keeps s >= 16 ulp of the node's coordinates), so
+    // p - 2^23 s and the plane p + q s are exact f32 values.
+    float px = __uint_as_float(w0.x) - 8388608.0f * sx;
+    float py = __uint_as_float(w0.y) - 8388608.0f * sy;
+    float pz = __uint_as_float(w0.z) - 8388608.0f * sz;
+    const uint32_t nc = w0.w >> 24;
     h.ref[0] = w4.x; h.ref[1] = w4.y; h.ref[2] = w4.z; h.ref[3] = w4.w;
     h.ref[4] = w5.x; h.ref[5] = w5.y; h.ref[6] = w5.z; h.ref[7] = w5.w;
     h.mask = 0;
 #pragma unroll
     for (int k = 0; k < 8; k++) {
+        if (k >= (int)nc) break;
         uint32_t wlx = k < 4 ? w1.x : w1.y, wly = k < 4 ? w1.z : w1.w;
         uint32_t wlz = k < 4 ? w2.x : w2.y, whx = k < 4 ? w2.z : w2.w;
         uint32_t why = k < 4 ? w3.x : w3.y, whz = k < 4 ? w3.z : w3.w;
-        int b = k & 3;
-        float lox = fmaf(q8(wlx, b), sx, px), hix = fmaf(q8(whx, b), sx, px);
-        float loy = fmaf(q8(wly, b), sy, py), hiy = fmaf(q8(why, b), sy, py);
-        float loz = fmaf(q8(wlz, b), sz, pz), hiz = fmaf(q8(whz, b), sz, pz);
+        const uint32_t sel = 0x7440u | (uint32_t)(k & 3);
+        auto qf = [&](uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B000000u, sel)); };
+        float lox = fmaf(qf(wlx), sx, px), hix = fmaf(qf(whx), sx, px);
+        float loy = fmaf(qf(wly), sy, py), hiy = fmaf(qf(why), sy, py);
+        float loz = fmaf(qf(wlz), sz, pz), hiz = fmaf(qf(whz), sz, pz);
         float t0x = (lox - r.o.x) * r.inv.x, t1x = (hix - r.o.x) * r.inv.x;
         float t0y = (loy - r.o.y) * r.inv.y, t1y = (hiy - r.o.y) * r.inv.y;
         float t0z = (loz - r.o.z) * r.inv.z, t1z = (hiz - r.o.z) * r.inv.z;
@@ -233,132 +242,310 @@ struct TraceHit {
 #define RT_DEVERR_STACK 1u
 #define RT_DEVERR_ITER 2u
 #define RT_MAX_TRAV_STEPS (1u << 22)
+// Error bits written to the device error word.
+#define RT_DEVERR_STACK 1u
+#define RT_DEVERR_ITER 2u
+#define RT_MAX_TRAV_STEPS (1u << 22)
 
-// Closest hit (ANY = false) or any hit (ANY = true, returns at the first
-// hit with t < t_max). World-space ray (o, d), parametric t.
-template <bool ANY>
-__device__ __forceinline__ bool trace(const DevScene& S, float3 o, float3 d, float t_max, TraceHit& hit,
-                                      TravStack& st, uint32_t* err) {
-    hit.t = t_max;
-    hit.tri = 0xFFFFFFFFu;
-    hit.inst = 0xFFFFFFFFu;
-    hit.b1 = hit.b2 = 0.0f;
-    if (S.n_instances == 0) return false;
-    RayPre r;
-    ray_pre(r, o, d);
+// Resumable traversal state of one ray (registers), so persistent warps can
+// advance rays a few steps at a time and refill lanes whose ray finished.
+struct TravState {
+    RayPre r;          // current ray (world, or the instance's object space)
+    float3 o, d;       // world ray
+    TraceHit hit;
+    uint32_t cur;      // node / leaf reference being processed
+    uint32_t cur_inst;
+    uint32_t steps;
+    int inst_sp;
+    bool in_inst, found;
+};
+
+// Start a closest-hit / any-hit query; false when the scene is empty.
+__device__ __forceinline__ bool trav_begin(const DevScene& S, TravState& ts, TravStack& st, float3 o, float3 d,
+                                           float t_max) {
+    ts.hit.t = t_max;
+    ts.hit.tri = 0xFFFFFFFFu;
+    ts.hit.inst = 0xFFFFFFFFu;
+    ts.hit.b1 = ts.hit.b2 = 0.0f;
+    ts.o = o;
+    ts.d = d;
+    ts.in_inst = false;
+    ts.found = false;
+    ts.inst_sp = 0;
+    ts.cur_inst = 0;
+    ts.steps = 0;
     st.sp = 0;
     st.base = 0;
-    bool in_inst = false;
-    int inst_sp = 0;
-    uint32_t cur_inst = 0;
-    uint32_t cur = S.tlas_root;  // interior node ref
-    bool found = false;
-    uint32_t steps = 0;
-    for (;;) {
-        if (++steps > RT_MAX_TRAV_STEPS) {
-            atomicOr(err, RT_DEVERR_ITER);
-            return found;
-        }
-        if (!(cur & REF_LEAF)) {
-            NodeHits h;
-            test_node(S.nodes, cur, r, hit.t, h);
-            uint32_t m = h.mask;
-            if (m) {
-                if (ANY) {
-                    // Unordered: keep the first hit child, push the rest.
-                    int k0 = __ffs(m) - 1;
-                    uint32_t next = 0;
+    st.overflow = false;
+    if (S.n_instances == 0) return false;
+    ray_pre(ts.r, o, d);
+    ts.cur = S.tlas_root;
+    return true;
+}
+
+// Process the current reference (test a node's 8 children, enter an
+// instance, or test a leaf's triangles), then pick the next one. Returns
+// true when the query is finished (ts.found / ts.hit hold the answer).
+template <bool ANY>
+__device__ __forceinline__ bool trav_step(const DevScene& S, TravState& ts, TravStack& st, uint32_t* err) {
+    if (++ts.steps > RT_MAX_TRAV_STEPS) {
+        atomicOr(err, RT_DEVERR_ITER);
+        return true;
+    }
+    const uint32_t cur = ts.cur;
+    if (!(cur & REF_LEAF)) {
+        NodeHits h;
+        test_node(S.nodes, cur, ts.r, ts.hit.t, h);
+        uint32_t m = h.mask;
+        if (m) {
+            if (ANY) {
+                int k0 = __ffs(m) - 1;
+                uint32_t next = 0;
 #pragma unroll
-                    for (int k = 0; k < 8; k++) {
-                        if (k == k0) next = h.ref[k];
-                        else if ((m >> k) & 1u) st.push(h.ref[k], h.tn[k]);
-                    }
-                    cur = next;
-                } else {
-                    // Push far-to-near; continue with the nearest.
-                    while (__popc(m) > 1) {
-                        float bt = -1.0f;
-                        int bk = 0;
-#pragma unroll
-                        for (int k = 0; k < 8; k++)
-                            if (((m >> k) & 1u) && h.tn[k] > bt) {
-                                bt = h.tn[k];
-                                bk = k;
-                            }
-                        uint32_t rf = 0;
-#pragma unroll
-                        for (int k = 0; k < 8; k++)
-                            if (k == bk) rf = h.ref[k];
-                        st.push(rf, bt);
-                        m &= ~(1u << bk);
-                    }
-                    uint32_t next = 0;
+                for (int k = 0; k < 8; k++) {
+                    if (k == k0) next = h.ref[k];
+                    else if ((m >> k) & 1u) st.push(h.ref[k], h.tn[k]);
+                }
+                ts.cur = next;
+            } else {
+                // Push far-to-near; continue with the nearest.
+                while (__popc(m) > 1) {
+                    float bt = -1.0f;
+                    int bk = 0;
 #pragma unroll
                     for (int k = 0; k < 8; k++)
-                        if ((m >> k) & 1u) next = h.ref[k];
-                    cur = next;
+                        if (((m >> k) & 1u) && h.tn[k] > bt) {
+                            bt = h.tn[k];
+                            bk = k;
+                        }
+                    uint32_t rf = 0;
+#pragma unroll
+                    for (int k = 0; k < 8; k++)
+                        if (k == bk) rf = h.ref[k];
+                    st.push(rf, bt);
+                    m &= ~(1u << bk);
                 }
-                if (st.overflow) {
-                    atomicOr(err, RT_DEVERR_STACK);
-                    return found;
-                }
-                continue;
+                uint32_t next = 0;
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                    if ((m >> k) & 1u) next = h.ref[k];
+                ts.cur = next;
             }
-        } else if (!in_inst) {
-            // TLAS leaf: a run of instances. Defer all but the first on the
-            // stack (as one-instance leaves), then enter the first.
-            uint32_t first = cur & LEAF_FIRST_MASK;
-            uint32_t count = ((cur >> 27) & 15u) + 1u;
-            for (uint32_t k = count - 1; k >= 1; k--) st.push(make_leaf_ref(first + k, 1), 0.0f);
             if (st.overflow) {
                 atomicOr(err, RT_DEVERR_STACK);
-                return found;
+                return true;
             }
-            cur_inst = first;
-            float4 x0 = __ldg(S.inst_xf + 3 * (size_t)first), x1 = __ldg(S.inst_xf + 3 * (size_t)first + 1),
-                   x2 = __ldg(S.inst_xf + 3 * (size_t)first + 2);
-            uint32_t root = __ldg(&S.inst[first].x);
-            ray_pre(r, xf_point(x0, x1, x2, o), xf_vec(x0, x1, x2, d));
-            in_inst = true;
-            inst_sp = st.sp;
-            if (root != 0xFFFFFFFFu) {
-                cur = root;
-                continue;
-            }
-        } else {
-            // BLAS leaf: triangles in leaf order.
-            uint32_t first = cur & LEAF_FIRST_MASK;
-            uint32_t count = ((cur >> 27) & 15u) + 1u;
-            for (uint32_t k = 0; k < count; k++) {
-                const float4* tp = S.tris + 3 * (size_t)(first + k);
-                float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-                float t, b1, b2;
-                if (tri_watertight(r, xyz(a), xyz(b), xyz(c), hit.t, t, b1, b2)) {
-                    hit.t = t;
-                    hit.tri = first + k;
-                    hit.inst = cur_inst;
-                    hit.b1 = b1;
-                    hit.b2 = b2;
-                    found = true;
-                    if (ANY) return true;
-                }
-            }
+            return false;
         }
-        // Pop the next entry that can still hold a closer hit; leaving an
-        // instance's BLAS restores the world-space ray.
-        for (;;) {
-            if (in_inst && st.sp == inst_sp) {
-                in_inst = false;
-                ray_pre(r, o, d);
-            }
-            if (st.sp == 0) return found;
-            uint2 e = st.pop();
-            if (__uint_as_float(e.y) < hit.t) {
-                cur = e.x;
-                break;
+    } else if (!ts.in_inst) {
+        // TLAS leaf: a run of instances. Defer all but the first on the
+        // stack (as one-instance leaves), then enter the first.
+        uint32_t first = cur & LEAF_FIRST_MASK;
+        uint32_t count = ((cur >> 27) & 15u) + 1u;
+        for (uint32_t k = count - 1; k >= 1; k--) st.push(make_leaf_ref(first + k, 1), 0.0f);
+        if (st.overflow) {
+            atomicOr(err, RT_DEVERR_STACK);
+            return true;
+        }
+        ts.cur_inst = first;
+        float4 x0 = __ldg(S.inst_xf + 3 * (size_t)first), x1 = __ldg(S.inst_xf + 3 * (size_t)first + 1),
+               x2 = __ldg(S.inst_xf + 3 * (size_t)first + 2);
+        uint32_t root = __ldg(&S.inst[first].x);
+        ray_pre(ts.r, xf_point(x0, x1, x2, ts.o), xf_vec(x0, x1, x2, ts.d));
+        ts.in_inst = true;
+        ts.inst_sp = st.sp;
+        if (root != 0xFFFFFFFFu) {
+            ts.cur = root;
+            return false;
+        }
+    } else {
+        // BLAS leaf: triangles in leaf order.
+        uint32_t first = cur & LEAF_FIRST_MASK;
+        uint32_t count = ((cur >> 27) & 15u) + 1u;
+        for (uint32_t k = 0; k < count; k++) {
+            const float4* tp = S.tris + 3 * (size_t)(first + k);
+            float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            float t, b1, b2;
+            if (tri_watertight(ts.r, xyz(a), xyz(b), xyz(c), ts.hit.t, t, b1, b2)) {
+                ts.hit.t = t;
+                ts.hit.tri = first + k;
+                ts.hit.inst = ts.cur_inst;
+                ts.hit.b1 = b1;
+                ts.hit.b2 = b2;
+                ts.found = true;
+                if (ANY) return true;
             }
         }
     }
+    // Pop the next entry that can still hold a closer hit; leaving an
+    // instance's BLAS restores the world-space ray.
+    for (;;) {
+        if (ts.in_inst && st.sp == ts.inst_sp) {
+            ts.in_inst = false;
+            ray_pre(ts.r, ts.o, ts.d);
+        }
+        if (st.sp == 0) return true;
+        uint2 e = st.pop();
+        if (__uint_as_float(e.y) < ts.hit.t) {
+            ts.cur = e.x;
+            return false;
+        }
+    }
+}
+
+// ---- phased traversal: node operations and leaf operations ---------------------------
+// A lane's work splits into three operations so a warp can run all of its
+// node tests together and then all of its leaf tests together (Aila & Laine
+// 2009, "while-while"): lanes are then mostly in the same code.
+//   op_node: test the 8 children of ts.cur, continue with the nearest, push
+//            the rest; a leaf found is parked in `pending`.
+//   op_pop:  next stack entry that can still hold a closer hit (leaving an
+//            instance restores the world ray); false when the stack is empty.
+//   op_leaf: the parked leaf — enter an instance (TLAS) or test triangles (BLAS).
+struct PhaseState {
+    TravState ts;
+    uint32_t pending;  // parked leaf reference (bit 31 set), 0 = none
+    bool need_pop;
+};
+
+__device__ __forceinline__ void phase_begin(PhaseState& ps) {
+    ps.pending = 0;
+    ps.need_pop = false;
+    if (ps.ts.cur & REF_LEAF) {
+        ps.pending = ps.ts.cur;
+        ps.need_pop = true;
+    }
+}
+
+// Returns false when the query is over (stack exhausted).
+__device__ __forceinline__ bool op_pop(PhaseState& ps, TravStack& st) {
+    TravState& ts = ps.ts;
+    for (;;) {
+        if (ts.in_inst && st.sp == ts.inst_sp) {
+            ts.in_inst = false;
+            ray_pre(ts.r, ts.o, ts.d);
+        }
+        if (st.sp == 0) return false;
+        uint2 e = st.pop();
+        if (__uint_as_float(e.y) < ts.hit.t) {
+            ts.cur = e.x;
+            ps.need_pop = false;
+            if (e.x & REF_LEAF) {
+                ps.pending = e.x;
+                ps.need_pop = true;
+            }
+            return true;
+        }
+    }
+}
+
+// Returns true on a fatal condition (stack overflow): the query is over.
+template <bool ANY>
+__device__ __forceinline__ bool op_node(const DevScene& S, PhaseState& ps, TravStack& st, uint32_t* err) {
+    TravState& ts = ps.ts;
+    NodeHits h;
+    test_node(S.nodes, ts.cur, ts.r, ts.hit.t, h);
+    uint32_t m = h.mask;
+    if (!m) {
+        ps.need_pop = true;
+        return false;
+    }
+    uint32_t next = 0;
+    if (ANY) {
+        int k0 = __ffs(m) - 1;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            if (k == k0) next = h.ref[k];
+            else if ((m >> k) & 1u) st.push(h.ref[k], h.tn[k]);
+        }
+    } else {
+        while (__popc(m) > 1) {
+            float bt = -1.0f;
+            int bk = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (((m >> k) & 1u) && h.tn[k] > bt) {
+                    bt = h.tn[k];
+                    bk = k;
+                }
+            uint32_t rf = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (k == bk) rf = h.ref[k];
+            st.push(rf, bt);
+            m &= ~(1u << bk);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if ((m >> k) & 1u) next = h.ref[k];
+    }
+    if (st.overflow) {
+        atomicOr(err, RT_DEVERR_STACK);
+        return true;
+    }
+    ts.cur = next;
+    if (next & REF_LEAF) {
+        ps.pending = next;
+        ps.need_pop = true;
+    }
+    return false;
+}
+
+// Returns true when the query is over (any-hit found, or a fatal condition).
+template <bool ANY>
+__device__ __forceinline__ bool op_leaf(const DevScene& S, PhaseState& ps, TravStack& st, uint32_t* err) {
+    TravState& ts = ps.ts;
+    const uint32_t leaf = ps.pending;
+    ps.pending = 0;
+    uint32_t first = leaf & LEAF_FIRST_MASK;
+    uint32_t count = ((leaf >> 27) & 15u) + 1u;
+    if (!ts.in_inst) {
+        for (uint32_t k = count - 1; k >= 1; k--) st.push(make_leaf_ref(first + k, 1), 0.0f);
+        if (st.overflow) {
+            atomicOr(err, RT_DEVERR_STACK);
+            return true;
+        }
+        ts.cur_inst = first;
+        float4 x0 = __ldg(S.inst_xf + 3 * (size_t)first), x1 = __ldg(S.inst_xf + 3 * (size_t)first + 1),
+               x2 = __ldg(S.inst_xf + 3 * (size_t)first + 2);
+        uint32_t root = __ldg(&S.inst[first].x);
+        ray_pre(ts.r, xf_point(x0, x1, x2, ts.o), xf_vec(x0, x1, x2, ts.d));
+        ts.in_inst = true;
+        ts.inst_sp = st.sp;
+        ts.cur = root;
+        ps.need_pop = root == 0xFFFFFFFFu;
+        return false;
+    }
+    for (uint32_t k = 0; k < count; k++) {
+        const float4* tp = S.tris + 3 * (size_t)(first + k);
+        float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float t, b1, b2;
+        if (tri_watertight(ts.r, xyz(a), xyz(b), xyz(c), ts.hit.t, t, b1, b2)) {
+            ts.hit.t = t;
+            ts.hit.tri = first + k;
+            ts.hit.inst = ts.cur_inst;
+            ts.hit.b1 = b1;
+            ts.hit.b2 = b2;
+            ts.found = true;
+            if (ANY) return true;
+        }
+    }
+    ps.need_pop = true;
+    return false;
+}
+
+// Closest hit (ANY = false) or any hit (ANY = true, returns at the first
+// hit with t < t_max) of one ray, to completion. World-space ray (o, d),
+// parametric t.
+template <bool ANY>
+__device__ __forceinline__ bool trace(const DevScene& S, float3 o, float3 d, float t_max, TraceHit& hit,
+                                      TravStack& st, uint32_t* err) {
+    TravState ts;
+    if (trav_begin(S, ts, st, o, d, t_max))
+        while (!trav_step<ANY>(S, ts, st, err)) {
+        }
+    hit = ts.hit;
+    return ts.found;
 }
 
 }  // namespace rt

@@ -68,7 +68,12 @@ def test_forward_matches_oracle(guide):
     res, lo, inv = guide.info()
     raw_o, _, _, _ = oracle.guide_eval(m, t, res, lo, inv, rec, grads=False)
     raw_g = guide.infer(rec)
-    assert np.allclose(raw_g[:, :40], raw_o[:, :40], rtol=2e-3, atol=2e-3), np.abs(raw_g - raw_o).max()
+    diff = np.abs(raw_g[:, :40] - raw_o[:, :40])
+    # An activation that lands on a bf16 rounding boundary may round the other
+    # way under f32 vs f64 accumulation and move its outputs by ~1 bf16 ulp;
+    # everything else agrees to accumulation order.
+    assert (diff < 1e-4).mean() > 0.999, (diff < 1e-4).mean()
+    assert diff.max() < 2e-2, diff.max()
 
 
 def test_gradients_match_oracle(guide):

@@ -40,8 +40,9 @@ def _check_closest(s, planes, gp, gi, gt, op, oi, ot, tri_of):
     bad = []
     agree = (gp == op) & (gi == oi)
     hit = agree & (op != 0xFFFFFFFF)
-    rel = np.abs(gt[hit].astype(np.float64) - ot[hit]) / np.maximum(ot[hit], 1e-30)
-    assert rel.max(initial=0) < 1e-5, rel.max()
+    # f32 t vs f64 t: relative 1e-5, absolute for hits close to the origin.
+    err = np.abs(gt[hit].astype(np.float64) - ot[hit]) / np.maximum(ot[hit], 1.0)
+    assert err.max(initial=0) < 1e-5, err.max()
     for k in np.nonzero(~agree)[0]:
         tg = np.inf if gp[k] == 0xFFFFFFFF else float(gt[k])
         to = float(ot[k])
