@@ -19,7 +19,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <atomic>
+#include <functional>
 #include <limits>
+#include <thread>
 
 namespace rt {
 
@@ -58,7 +61,10 @@ struct BinBvh {
     std::vector<uint32_t> order;
 };
 
-// Binned SAH with the reference's split rules and node numbering.
+// Binned SAH with the reference's split rules. Subtrees are independent
+// (each partitions only its own primitive range), so large ones are built on
+// their own threads; the tree is the same as a sequential build, only the
+// node numbering differs, and nothing downstream depends on it.
 BinBvh build_binary(const std::vector<Box>& bounds) {
     const int BINS = 16, MAX_LEAF = 4;
     BinBvh t;
@@ -69,27 +75,30 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
     std::vector<double> cen(3 * n);
     for (size_t i = 0; i < n; i++)
         for (int a = 0; a < 3; a++) cen[3 * i + a] = (bounds[i].lo[a] + bounds[i].hi[a]) * 0.5;
-    t.nodes.reserve(2 * n / 3 + 8);
-    t.nodes.push_back(BinNode{});
-    struct Job { size_t node, start, count; };
-    std::vector<Job> stack{{0, 0, n}};
+    t.nodes.resize(2 * n + 1);
+    std::atomic<size_t> next{1};
     uint32_t* ord = t.order.data();
-    while (!stack.empty()) {
-        Job j = stack.back();
-        stack.pop_back();
+    BinNode* nodes = t.nodes.data();
+    struct Job { size_t node, start, count; };
+    const size_t PAR_MIN = 32768;
+    const int max_threads = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::atomic<int> threads_live{1};
+
+    // One level: bounds, split choice, partition. Returns false for a leaf.
+    auto split_node = [&](const Job& j, size_t* split_out) -> bool {
         Box b, cb;
         for (size_t i = j.start; i < j.start + j.count; i++) {
             b.grow(bounds[ord[i]]);
             cb.grow_pt(&cen[3 * ord[i]]);
         }
-        t.nodes[j.node].b = b;
+        nodes[j.node].b = b;
         auto make_leaf = [&]() {
-            t.nodes[j.node].first = (uint32_t)j.start;
-            t.nodes[j.node].count = (uint32_t)j.count;
+            nodes[j.node].first = (uint32_t)j.start;
+            nodes[j.node].count = (uint32_t)j.count;
         };
         if (j.count <= (size_t)MAX_LEAF) {
             make_leaf();
-            continue;
+            return false;
         }
         double ext[3] = {cb.hi[0] - cb.lo[0], cb.hi[1] - cb.lo[1], cb.hi[2] - cb.lo[2]};
         int axis = (ext[0] >= ext[1] && ext[0] >= ext[2]) ? 0 : (ext[1] >= ext[2] ? 1 : 2);
@@ -139,17 +148,41 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
                 if (m > 0 && m < j.count) split = j.start + m;
             } else if (j.count <= (size_t)MAX_LEAF * 4) {
                 make_leaf();
-                continue;
+                return false;
             }
         }
-        size_t l = t.nodes.size();
-        t.nodes.push_back(BinNode{});
-        t.nodes.push_back(BinNode{});
-        t.nodes[j.node].first = (uint32_t)l;
-        t.nodes[j.node].count = 0;
-        stack.push_back({l + 1, split, j.start + j.count - split});
-        stack.push_back({l, j.start, split - j.start});
-    }
+        *split_out = split;
+        return true;
+    };
+
+    std::function<void(Job)> build_subtree = [&](Job root) {
+        std::vector<Job> stack{root};
+        std::vector<std::thread> spawned;
+        while (!stack.empty()) {
+            Job j = stack.back();
+            stack.pop_back();
+            size_t split;
+            if (!split_node(j, &split)) continue;
+            size_t l = next.fetch_add(2);
+            nodes[j.node].first = (uint32_t)l;
+            nodes[j.node].count = 0;
+            Job left{l, j.start, split - j.start}, right{l + 1, split, j.start + j.count - split};
+            if (left.count >= PAR_MIN && threads_live.load() < max_threads) {
+                threads_live++;
+                spawned.emplace_back([&, left] {
+                    build_subtree(left);
+                    threads_live--;
+                });
+                stack.push_back(right);
+            } else {
+                stack.push_back(right);
+                stack.push_back(left);
+            }
+        }
+        for (auto& th : spawned) th.join();
+    };
+    build_subtree({0, 0, n});
+    t.nodes.resize(next.load());
     return t;
 }
 

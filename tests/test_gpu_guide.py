@@ -70,9 +70,10 @@ def test_forward_matches_oracle(guide):
     raw_g = guide.infer(rec)
     diff = np.abs(raw_g[:, :40] - raw_o[:, :40])
     # An activation that lands on a bf16 rounding boundary may round the other
-    # way under f32 vs f64 accumulation and move its outputs by ~1 bf16 ulp;
-    # everything else agrees to accumulation order.
-    assert (diff < 1e-4).mean() > 0.999, (diff < 1e-4).mean()
+    # way under f32 vs f64 accumulation and move that sample's outputs by ~1
+    # bf16 ulp; every other sample agrees to accumulation order.
+    exact = (diff < 1e-4).all(axis=1)
+    assert exact.mean() > 0.99, exact.mean()
     assert diff.max() < 2e-2, diff.max()
 
 
