@@ -20,7 +20,6 @@
 #pragma once
 
 #include "guide.cuh"
-#include "traverse8.cuh"
 
 namespace rt {
 
@@ -306,6 +305,118 @@ __global__ void k_guide_collect(Paths P, PtConsts C) {
     for (int k = 0; k < 12; k++) o[k] = r[k];
     o[12] = fminf(w, 50.0f);
     o[13] = o[14] = o[15] = 0.0f;
+}
+
+// ---- persistent ray pump ----------------------------------------------------------------
+// Each warp keeps 32 rays in flight. A lane whose ray finishes is refilled
+// from the global work counter as soon as half the warp is idle (one
+// warp-aggregated atomic per refill), so a few long rays no longer hold a
+// warp's other lanes hostage (Aila & Laine 2009, "persistent while-while").
+// load(j, o, d, tmax) reads work item j; finish(done, j, ts) is called by
+// the whole warp whenever some lane finished, with `done` true on those lanes.
+// Within a warp the work alternates between a node phase (every lane that
+// has no parked leaf tests nodes until it parks one or finishes) and a leaf
+// phase (every lane with a parked leaf processes it), so lanes mostly run
+// the same code path.
+template <bool ANY, class Load, class Finish>
+__device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
+                                         TravStack& st, Load load, Finish finish) {
+    PhaseState ps;
+    bool active = false, exhausted = false;
+    uint32_t item = 0, steps = 0;
+    const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
+    for (;;) {
+        uint32_t act = __ballot_sync(0xFFFFFFFFu, active);
+        if (!exhausted && __popc(act) <= 16) {
+            uint32_t idle = ~act;
+            uint32_t leader = __ffs(idle) - 1, base = 0;
+            if (lane == leader) base = atomicAdd(fetch, __popc(idle));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (base >= n || n - base <= (uint32_t)__popc(idle)) exhausted = true;
+            bool fresh = false;
+            if (!active) {
+                uint32_t j = base + __popc(idle & lt);
+                if (base < n && j < n) {
+                    item = j;
+                    float3 o, d;
+                    float tmax;
+                    load(j, o, d, tmax);
+                    active = trav_begin(S, ps.ts, st, o, d, tmax);
+                    if (active) {
+                        phase_begin(ps);
+                        steps = 0;
+                    } else {
+                        fresh = true;  // empty scene: a miss, finished at once
+                    }
+                }
+            }
+            if (__any_sync(0xFFFFFFFFu, fresh)) finish(fresh, item, ps.ts);
+            act = __ballot_sync(0xFFFFFFFFu, active);
+        }
+        if (act == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        // Node phase.
+        for (;;) {
+            bool want = active && ps.pending == 0;
+            if (!__any_sync(0xFFFFFFFFu, want)) break;
+            bool done_now = false;
+            if (want) {
+                if (++steps > RT_MAX_TRAV_STEPS) {
+                    atomicOr(err, RT_DEVERR_ITER);
+                    done_now = true;
+                } else if (ps.need_pop) {
+                    done_now = !op_pop(ps, st);
+                } else {
+                    done_now = op_node<ANY>(S, ps, st, err);
+                }
+            }
+            if (__any_sync(0xFFFFFFFFu, done_now)) finish(done_now, item, ps.ts);
+            if (done_now) active = false;
+        }
+        // Leaf phase.
+        bool done_now = false;
+        if (active && ps.pending) done_now = op_leaf<ANY>(S, ps, st, err);
+        if (__any_sync(0xFFFFFFFFu, done_now)) finish(done_now, item, ps.ts);
+        if (done_now) active = false;
+    }
+}
+
+// ---- extend ---------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_extend(DevScene S, Paths P, uint32_t qsel) {
+    __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    TravStack st;
+    st.init(stack_sh + threadIdx.x, BLOCK);
+    const uint32_t* q = P.q_ext[qsel];
+    const uint32_t n = P.cnt[CNT_EXT_IN];
+    unsigned long long rays = 0;
+    uint32_t slot = 0;
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
+        slot = q[j];
+        float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot];
+        o = xyz(o4);
+        d = xyz(d4);
+        tmax = d4.w;
+    };
+    auto finish = [&](bool done, uint32_t, const TravState& ts) {
+        uint32_t cls = CLS_MISS;
+        if (done) {
+            const TraceHit& h = ts.hit;
+            uint32_t uv = (uint32_t)__half_as_ushort(__float2half_rn(h.b1)) |
+                          ((uint32_t)__half_as_ushort(__float2half_rn(h.b2)) << 16);
+            uint32_t tri = ts.found ? h.tri : 0xFFFFFFFFu;
+            P.hit[slot] = make_uint4(__float_as_uint(h.t), tri, h.inst, uv);
+            if (ts.found) cls = __ldg(&S.materials[__ldg(&S.inst[h.inst].z)].mclass);
+            rays++;
+        }
+        // Bucket by material class: one atomic per (warp, class).
+        for (uint32_t c = 0; c < N_QUEUES; c++)
+            push_queue(P.q_cls + (size_t)c * P.P, &P.cnt[CNT_CLASS + c], slot, done && cls == c);
+    };
+    ray_pump<false>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, st, load, finish);
+    if (rays) atomicAdd(&P.stats[0], rays);
 }
 
 // ---- shade ------------------------------------------------------------------------------
@@ -665,20 +776,9 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
 
 // ---- shadow -------------------------------------------------------------------------------
 template <int BLOCK>
-__device__ __forceinline__ void shadow_opaque(const DevScene& S, Paths& P, const PtConsts& C, uint2* stk);
-
-// Shadow rays. Opaque scenes: group any-hit (shadow_opaque). Scenes with
-// presence cutouts: the reference's transmittance loop (mod.rs:1254-1306),
-// closest-hit segments per lane; cutouts attenuate by (1 - presence).
-template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene S, Paths P, PtConsts C) {
-    constexpr int WORDS = RT_SH_STACK * BLOCK > (BLOCK / 8) * G8_STACK ? RT_SH_STACK * BLOCK : (BLOCK / 8) * G8_STACK;
-    __shared__ uint2 stack_sh[WORDS];
+    __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
     __shared__ uint32_t warp_base[BLOCK / 32];
-    if (!S.any_presence) {
-        shadow_opaque<BLOCK>(S, P, C, stack_sh + (threadIdx.x >> 3) * G8_STACK);
-        return;
-    }
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
     uint32_t n = P.cnt[CNT_SHADOW];
@@ -693,6 +793,25 @@ __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene S, Paths P, PtConsts 
             P.aux_d[slot] = make_float4(a.x + c.x * vis, a.y + c.y * vis, a.z + c.z * vis, a.w);
         }
     };
+    if (!S.any_presence) {
+        // Opaque scenes: one any-hit query per shadow ray, through the pump.
+        uint32_t slot = 0;
+        auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
+            slot = P.q_sh[j];
+            float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
+            o = xyz(o4);
+            d = xyz(d4);
+            tmax = d4.w;
+        };
+        auto finish = [&](bool done, uint32_t, const TravState& ts) {
+            if (!done) return;
+            rays++;
+            if (!ts.found) add(slot, 1.0f);
+        };
+        ray_pump<true>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, load, finish);
+        if (rays) atomicAdd(&P.stats[1], rays);
+        return;
+    }
     for (;;) {
         if (lane_id() == 0) warp_base[w] = atomicAdd(&P.cnt[CNT_FETCH_SH], 32u);
         __syncwarp();
@@ -794,100 +913,38 @@ __global__ void k_accumulate(Paths P, PtConsts C, uint32_t samples_in_slab, doub
     acc[3] += (double)samples_in_slab;
 }
 
-
-// ---- group traversal kernels (one ray per 8 lanes, traverse8.cuh) ------------------------
+// ---- ray batch (rt_intersect_batch) ------------------------------------------------------
 template <int BLOCK, bool ANY>
 __global__ void __launch_bounds__(BLOCK) k_intersect(DevScene S, const float4* __restrict__ org,
-                                                      const float4* __restrict__ dir, uint64_t n, uint32_t* prim,
-                                                      uint32_t* inst, float* tout, uint32_t* fetch, uint32_t* err) {
-    __shared__ uint2 gstack[BLOCK / 8][G8_STACK];
-    uint2* stk = gstack[threadIdx.x >> 3];
+                                                     const float4* __restrict__ dir, uint64_t n, uint32_t* prim,
+                                                     uint32_t* inst, float* tout, uint32_t* fetch, uint32_t* err) {
+    __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    TravStack st;
+    st.init(stack_sh + threadIdx.x, BLOCK);
     auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
         float4 o4 = __ldg(org + j), d4 = __ldg(dir + j);
         o = xyz(o4);
         d = xyz(d4);
         tmax = d4.w;
     };
-    auto finish = [&](bool done, uint32_t i, const GroupRay& g) {
+    auto finish = [&](bool done, uint32_t i, const TravState& ts) {
         if (!done) return;
         if (ANY) {
-            prim[i] = g.found ? 1u : 0u;
+            prim[i] = ts.found ? 1u : 0u;
         } else {
             uint32_t p = 0xFFFFFFFFu, ii = 0xFFFFFFFFu;
             float t = INFINITY;
-            if (g.found) {
-                p = __float_as_uint(__ldg(&S.tris[3 * (size_t)g.hit.tri].w));
-                ii = __ldg(&S.inst[g.hit.inst].y);
-                t = g.hit.t;
+            if (ts.found) {
+                p = __float_as_uint(__ldg(&S.tris[3 * (size_t)ts.hit.tri].w));
+                ii = __ldg(&S.inst[ts.hit.inst].y);
+                t = ts.hit.t;
             }
             prim[i] = p;
             if (inst) inst[i] = ii;
             if (tout) tout[i] = t;
         }
     };
-    g8_pump<ANY>(S, (uint32_t)n, fetch, err, stk, load, finish);
-}
-
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_extend(DevScene S, Paths P, uint32_t qsel) {
-    __shared__ uint2 gstack[BLOCK / 8][G8_STACK];
-    uint2* stk = gstack[threadIdx.x >> 3];
-    const uint32_t* q = P.q_ext[qsel];
-    const uint32_t n = P.cnt[CNT_EXT_IN];
-    unsigned long long rays = 0;
-    uint32_t slot = 0;
-    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
-        slot = q[j];
-        float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot];
-        o = xyz(o4);
-        d = xyz(d4);
-        tmax = d4.w;
-    };
-    auto finish = [&](bool done, uint32_t, const GroupRay& g) {
-        uint32_t cls = CLS_MISS;
-        if (done) {
-            const TraceHit& h = g.hit;
-            uint32_t uv = (uint32_t)__half_as_ushort(__float2half_rn(h.b1)) |
-                          ((uint32_t)__half_as_ushort(__float2half_rn(h.b2)) << 16);
-            uint32_t tri = g.found ? h.tri : 0xFFFFFFFFu;
-            P.hit[slot] = make_uint4(__float_as_uint(h.t), tri, h.inst, uv);
-            if (g.found) cls = __ldg(&S.materials[__ldg(&S.inst[h.inst].z)].mclass);
-            rays++;
-        }
-        for (uint32_t c = 0; c < N_QUEUES; c++)
-            push_queue(P.q_cls + (size_t)c * P.P, &P.cnt[CNT_CLASS + c], slot, done && cls == c);
-    };
-    g8_pump<false>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, stk, load, finish);
-    if (rays) atomicAdd(&P.stats[0], rays);
-}
-
-// Opaque scenes: one any-hit query per shadow ray, one ray per 8 lanes.
-template <int BLOCK>
-__device__ __forceinline__ void shadow_opaque(const DevScene& S, Paths& P, const PtConsts& C, uint2* stk) {
-    const uint32_t n = P.cnt[CNT_SHADOW];
-    unsigned long long rays = 0;
-    uint32_t slot = 0;
-    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
-        slot = P.q_sh[j];
-        float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
-        o = xyz(o4);
-        d = xyz(d4);
-        tmax = d4.w;
-    };
-    auto finish = [&](bool done, uint32_t, const GroupRay& g) {
-        if (!done) return;
-        rays++;
-        if (g.found) return;
-        float4 c = P.sh_c[slot];
-        float4 L = P.L[slot];
-        P.L[slot] = make_float4(L.x + c.x, L.y + c.y, L.z + c.z, L.w);
-        if (C.aovs && c.w != 0.0f) {
-            float4 a = P.aux_d[slot];
-            P.aux_d[slot] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, a.w);
-        }
-    };
-    g8_pump<true>(S, n, &P.cnt[CNT_FETCH_SH], P.err, stk, load, finish);
-    if (rays) atomicAdd(&P.stats[1], rays);
+    ray_pump<ANY>(S, (uint32_t)n, fetch, err, st, load, finish);
 }
 
 // White-furnace estimator of one material: per thread, `per` BSDF samples

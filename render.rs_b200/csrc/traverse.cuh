@@ -393,6 +393,147 @@ __device__ __forceinline__ bool trav_step(const DevScene& S, TravState& ts, Trav
     }
 }
 
+// ---- phased traversal: node operations and leaf operations ---------------------------
+// A lane's work splits into three operations so a warp can run all of its
+// node tests together and then all of its leaf tests together (Aila & Laine
+// 2009, "while-while"): lanes are then mostly in the same code.
+//   op_node: test the 8 children of ts.cur, continue with the nearest, push
+//            the rest; a leaf found is parked in `pending`.
+//   op_pop:  next stack entry that can still hold a closer hit (leaving an
+//            instance restores the world ray); false when the stack is empty.
+//   op_leaf: the parked leaf — enter an instance (TLAS) or test triangles (BLAS).
+struct PhaseState {
+    TravState ts;
+    uint32_t pending;  // parked leaf reference (bit 31 set), 0 = none
+    bool need_pop;
+};
+
+__device__ __forceinline__ void phase_begin(PhaseState& ps) {
+    ps.pending = 0;
+    ps.need_pop = false;
+    if (ps.ts.cur & REF_LEAF) {
+        ps.pending = ps.ts.cur;
+        ps.need_pop = true;
+    }
+}
+
+// Returns false when the query is over (stack exhausted).
+__device__ __forceinline__ bool op_pop(PhaseState& ps, TravStack& st) {
+    TravState& ts = ps.ts;
+    for (;;) {
+        if (ts.in_inst && st.sp == ts.inst_sp) {
+            ts.in_inst = false;
+            ray_pre(ts.r, ts.o, ts.d);
+        }
+        if (st.sp == 0) return false;
+        uint2 e = st.pop();
+        if (__uint_as_float(e.y) < ts.hit.t) {
+            ts.cur = e.x;
+            ps.need_pop = false;
+            if (e.x & REF_LEAF) {
+                ps.pending = e.x;
+                ps.need_pop = true;
+            }
+            return true;
+        }
+    }
+}
+
+// Returns true on a fatal condition (stack overflow): the query is over.
+template <bool ANY>
+__device__ __forceinline__ bool op_node(const DevScene& S, PhaseState& ps, TravStack& st, uint32_t* err) {
+    TravState& ts = ps.ts;
+    NodeHits h;
+    test_node(S.nodes, ts.cur, ts.r, ts.hit.t, h);
+    uint32_t m = h.mask;
+    if (!m) {
+        ps.need_pop = true;
+        return false;
+    }
+    uint32_t next = 0;
+    if (ANY) {
+        int k0 = __ffs(m) - 1;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+            if (k == k0) next = h.ref[k];
+            else if ((m >> k) & 1u) st.push(h.ref[k], h.tn[k]);
+        }
+    } else {
+        while (__popc(m) > 1) {
+            float bt = -1.0f;
+            int bk = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (((m >> k) & 1u) && h.tn[k] > bt) {
+                    bt = h.tn[k];
+                    bk = k;
+                }
+            uint32_t rf = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (k == bk) rf = h.ref[k];
+            st.push(rf, bt);
+            m &= ~(1u << bk);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            if ((m >> k) & 1u) next = h.ref[k];
+    }
+    if (st.overflow) {
+        atomicOr(err, RT_DEVERR_STACK);
+        return true;
+    }
+    ts.cur = next;
+    if (next & REF_LEAF) {
+        ps.pending = next;
+        ps.need_pop = true;
+    }
+    return false;
+}
+
+// Returns true when the query is over (any-hit found, or a fatal condition).
+template <bool ANY>
+__device__ __forceinline__ bool op_leaf(const DevScene& S, PhaseState& ps, TravStack& st, uint32_t* err) {
+    TravState& ts = ps.ts;
+    const uint32_t leaf = ps.pending;
+    ps.pending = 0;
+    uint32_t first = leaf & LEAF_FIRST_MASK;
+    uint32_t count = ((leaf >> 27) & 15u) + 1u;
+    if (!ts.in_inst) {
+        for (uint32_t k = count - 1; k >= 1; k--) st.push(make_leaf_ref(first + k, 1), 0.0f);
+        if (st.overflow) {
+            atomicOr(err, RT_DEVERR_STACK);
+            return true;
+        }
+        ts.cur_inst = first;
+        float4 x0 = __ldg(S.inst_xf + 3 * (size_t)first), x1 = __ldg(S.inst_xf + 3 * (size_t)first + 1),
+               x2 = __ldg(S.inst_xf + 3 * (size_t)first + 2);
+        uint32_t root = __ldg(&S.inst[first].x);
+        ray_pre(ts.r, xf_point(x0, x1, x2, ts.o), xf_vec(x0, x1, x2, ts.d));
+        ts.in_inst = true;
+        ts.inst_sp = st.sp;
+        ts.cur = root;
+        ps.need_pop = root == 0xFFFFFFFFu;
+        return false;
+    }
+    for (uint32_t k = 0; k < count; k++) {
+        const float4* tp = S.tris + 3 * (size_t)(first + k);
+        float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float t, b1, b2;
+        if (tri_watertight(ts.r, xyz(a), xyz(b), xyz(c), ts.hit.t, t, b1, b2)) {
+            ts.hit.t = t;
+            ts.hit.tri = first + k;
+            ts.hit.inst = ts.cur_inst;
+            ts.hit.b1 = b1;
+            ts.hit.b2 = b2;
+            ts.found = true;
+            if (ANY) return true;
+        }
+    }
+    ps.need_pop = true;
+    return false;
+}
+
 // Closest hit (ANY = false) or any hit (ANY = true, returns at the first
 // hit with t < t_max) of one ray, to completion. World-space ray (o, d),
 // parametric t.
