@@ -105,6 +105,27 @@ int rt_intersect_batch(rt_session* s, const float* rays, uint64_t n, int any_hit
 int rt_intersect_batch_device(rt_session* s, const float* rays, uint64_t n, int any_hit,
                               uint32_t* prim, uint32_t* inst, float* t, void* stream);
 
+/* Allocation-free ray batch, for callers that must not allocate GPU memory
+ * once set up: code that owns a fixed device-memory budget reserved at
+ * start-up (a real-time renderer's frame loop, an embedding host that routes
+ * all GPU memory through its own allocator and forbids cudaMalloc/cudaFree
+ * mid-frame because they synchronise the device and fragment its budget).
+ * Same inputs, outputs and semantics as rt_intersect_batch (host pointers),
+ * but the device staging for the rays, the results, the work counter and the
+ * error word live in a fixed static device array of RT_NOALLOC_MAX_RAYS rays
+ * (about 2.9 MB), reserved on every GPU that loads the library until the
+ * process exits; nothing is allocated or freed per call. n beyond
+ * RT_NOALLOC_MAX_RAYS is rejected with RT_ERR_INVALID. The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current, so make that first call before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (from several
+ * threads or sessions on the same device) race on it and must be serialised
+ * by the caller. No counterpart in the reference: its Metal backend has no
+ * allocation-free entry point. */
+#define RT_NOALLOC_MAX_RAYS 65536u
+int rt_intersect_batch_noalloc(rt_session* s, const float* rays, uint64_t n, int any_hit,
+                               uint32_t* prim, uint32_t* inst, float* t);
+
 /* Statistics of the session and of its last rt_render_samples call. */
 typedef struct rt_stats {
     uint64_t blas_nodes;        /* 8-wide BLAS nodes, all meshes */

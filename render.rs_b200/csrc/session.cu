@@ -506,6 +506,85 @@ int rt_intersect_batch(rt_session* s, const float* rays, uint64_t n, int any_hit
     return s->check_device_error();
 }
 
+}  // extern "C"
+
+// ---- ray batch without allocation ------------------------------------------------------
+// rt_intersect_batch stages the caller's host rays and results in a device
+// buffer it grows with cudaMalloc, plus a work counter and an error word.
+// rt_intersect_batch_noalloc keeps all of that in this file-scope array
+// instead: RT_NOALLOC_MAX_RAYS rays of staging (32 B in, 12 B out each) and
+// two counter words, 2,883,648 bytes in all, held by every GPU that loads the
+// library until the process exits.
+namespace {
+constexpr uint64_t NOALLOC_IN = 8ull * RT_NOALLOC_MAX_RAYS;       // floats: two planes of float4
+constexpr uint64_t NOALLOC_OUT = 3ull * RT_NOALLOC_MAX_RAYS;      // prim, inst, t (32-bit each)
+constexpr uint64_t NOALLOC_WORDS = NOALLOC_IN + NOALLOC_OUT + 64; // + fetch counter, error word (padded)
+}  // namespace
+static __device__ __align__(256) uint32_t g_noalloc_scratch[NOALLOC_WORDS];
+
+namespace {
+// Device address of g_noalloc_scratch per device. Host code cannot use the
+// array's name as a device address; cudaGetSymbolAddress gives it, once per
+// device, with that device current.
+constexpr int NOALLOC_MAX_DEVICES = 64;
+uint32_t* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+int noalloc_scratch(uint32_t** out) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(RT_ERR_INVALID, "device index beyond the no-alloc table");
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = (uint32_t*)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return RT_OK;
+}
+}  // namespace
+
+extern "C" int rt_intersect_batch_noalloc(rt_session* s, const float* rays, uint64_t n, int any_hit, uint32_t* prim,
+                                          uint32_t* inst, float* t) {
+    if (!s || (!rays && n) || (!prim && n)) return fail(RT_ERR_INVALID, "NULL argument");
+    if (n > RT_NOALLOC_MAX_RAYS)
+        return fail(RT_ERR_INVALID, "rt_intersect_batch_noalloc: " + std::to_string(n) + " rays exceed its fixed " +
+                                        std::to_string(RT_NOALLOC_MAX_RAYS) + "-ray staging area");
+    if (n == 0) return RT_OK;
+    uint32_t* base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    float* d_rays = (float*)base;                          // two planes, 16-byte aligned
+    uint32_t* d_prim = base + NOALLOC_IN;
+    uint32_t* d_inst = d_prim + RT_NOALLOC_MAX_RAYS;
+    float* d_t = (float*)(d_inst + RT_NOALLOC_MAX_RAYS);
+    uint32_t* d_fetch = base + NOALLOC_IN + NOALLOC_OUT;   // must start at zero
+    uint32_t* d_err = d_fetch + 32;                        // must start at zero
+    cudaStream_t st = s->stream;
+    // The planes are packed for n rays: origins [0, 4n), directions [4n, 8n).
+    CUDA_TRY(cudaMemcpyAsync(d_rays, rays, 32 * n, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemsetAsync(d_fetch, 0, 4, st));
+    CUDA_TRY(cudaMemsetAsync(d_err, 0, 4, st));
+    const float4* o = (const float4*)d_rays;
+    const float4* d = o + n;
+    if (any_hit)
+        k_intersect<TRAV_BLOCK, true><<<s->trav_grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, d_prim, d_inst, d_t,
+                                                                           d_fetch, d_err);
+    else
+        k_intersect<TRAV_BLOCK, false><<<s->trav_grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, d_prim, d_inst, d_t,
+                                                                            d_fetch, d_err);
+    CUDA_TRY(cudaGetLastError());
+    uint32_t e = 0;
+    CUDA_TRY(cudaMemcpyAsync(prim, d_prim, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (!any_hit && inst) CUDA_TRY(cudaMemcpyAsync(inst, d_inst, 4 * n, cudaMemcpyDeviceToHost, st));
+    if (!any_hit && t) CUDA_TRY(cudaMemcpyAsync(t, d_t, 4 * n, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(&e, d_err, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (e) return fail(RT_ERR_DEVICE, "device reported a traversal overrun");
+    return RT_OK;
+}
+
+extern "C" {
+
 int rt_bsdf_furnace(const rt_material_desc* material, const double* wo, double eta, uint64_t n, uint64_t seed,
                     double* out) {
     if (!material || !wo || !out) return fail(RT_ERR_INVALID, "NULL argument");

@@ -29,7 +29,7 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", 
 EXPORTS = ("rt_session_create", "rt_session_destroy", "rt_last_error", "rt_render_samples", "rt_reset",
            "rt_read_accum", "rt_read_image", "rt_read_aux", "rt_checkpoint_save", "rt_checkpoint_load",
            "rt_intersect_batch", "rt_intersect_batch_device", "rt_get_stats", "rt_session_stream",
-           "rt_bsdf_furnace")
+           "rt_bsdf_furnace", "rt_intersect_batch_noalloc")
 
 
 class RtError(RuntimeError):
