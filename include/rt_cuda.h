@@ -160,6 +160,13 @@ int rt_bsdf_furnace(const rt_material_desc* material, const double* wo, double e
  * order work against it. */
 void* rt_session_stream(rt_session* s);
 
+/* The session's learned directional proposal (rt_guide.h) when it renders
+ * guided, else NULL. The session owns the handle: callers may pass it to
+ * rt_guide_infer / rt_guide_get_params to inspect what the network has
+ * learned, and must not destroy it. No counterpart in the reference (path
+ * guiding is an unimplemented stretch goal there, ROADMAP.md:34). */
+struct rt_guide* rt_session_guide(rt_session* s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -260,6 +260,8 @@ int rt_session_destroy(rt_session* s) {
 
 void* rt_session_stream(rt_session* s) { return s ? (void*)s->stream : nullptr; }
 
+rt_guide* rt_session_guide(rt_session* s) { return s ? s->guide : nullptr; }
+
 int rt_reset(rt_session* s) {
     if (!s) return fail(RT_ERR_INVALID, "session is NULL");
     CUDA_TRY(cudaMemsetAsync(s->accum, 0, 32ull * s->npix, s->stream));

@@ -29,7 +29,7 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", 
 EXPORTS = ("rt_session_create", "rt_session_destroy", "rt_last_error", "rt_render_samples", "rt_reset",
            "rt_read_accum", "rt_read_image", "rt_read_aux", "rt_checkpoint_save", "rt_checkpoint_load",
            "rt_intersect_batch", "rt_intersect_batch_device", "rt_get_stats", "rt_session_stream",
-           "rt_bsdf_furnace", "rt_intersect_batch_noalloc")
+           "rt_bsdf_furnace", "rt_intersect_batch_noalloc", "rt_session_guide")
 
 
 class RtError(RuntimeError):
@@ -79,6 +79,8 @@ def lib():
         L.rt_bsdf_furnace.argtypes = [vp, vp, C.c_double, u64, u64, vp]
         L.rt_session_stream.restype = vp
         L.rt_session_stream.argtypes = [vp]
+        L.rt_session_guide.restype = vp
+        L.rt_session_guide.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -175,6 +177,13 @@ class PtSession:
 
     def stream(self):
         return lib().rt_session_stream(self.h)
+
+    def guide(self):
+        """The session's trained proposal network (rtcuda.guide.Guide view,
+        owned by the session), or None when the session is not guided."""
+        from .guide import Guide
+        h = lib().rt_session_guide(self.h)
+        return Guide.borrow(h) if h else None
 
 
 def bsdf_furnace(material, wo, eta, n, seed=1):

@@ -62,9 +62,18 @@ class Guide:
         _check(_g().rt_guide_create(lo.ctypes.data, hi.ctypes.data, seed, lr, C.byref(h)))
         self.h = h
 
+    @classmethod
+    def borrow(cls, handle):
+        """A view of a network owned elsewhere (a guided session's)."""
+        g = cls.__new__(cls)
+        g.h = C.c_void_p(handle)
+        g._borrowed = True
+        return g
+
     def close(self):
         if getattr(self, "h", None):
-            _g().rt_guide_destroy(self.h)
+            if not getattr(self, "_borrowed", False):
+                _g().rt_guide_destroy(self.h)
             self.h = None
 
     def __del__(self):
