@@ -137,6 +137,9 @@ typedef struct rt_params {
     uint32_t guided;          /* 1 = learned directional proposal on */
     double   guide_fraction;  /* one-sample MIS fraction drawn from the guide */
     uint64_t max_paths;       /* wavefront slab capacity in paths (0 = auto) */
+    double   guide_lr;        /* Adam learning rate of the proposal (0 = 1e-2) */
+    uint32_t guide_steps;     /* Adam steps per sample pass when guided (0 = 1) */
+    uint32_t guide_depth;     /* guide only vertices of depth < this (0 = all) */
 } rt_params;
 
 /* Size checks shared by every consumer of the descriptor. */
@@ -146,7 +149,7 @@ static_assert(sizeof(rt_instance_desc) == 104, "rt_instance_desc layout");
 static_assert(sizeof(rt_material_desc) == 264, "rt_material_desc layout");
 static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
 static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
-static_assert(sizeof(rt_params) == 40, "rt_params layout");
+static_assert(sizeof(rt_params) == 56, "rt_params layout");
 }
 #endif
 

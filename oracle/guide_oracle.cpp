@@ -4,8 +4,9 @@
 //
 // The reference has no counterpart (path guiding is unimplemented there,
 // ROADMAP.md:34), so this oracle restates the network as specified: the
-// hash-grid encoding (16 levels x 2 features, spatial hash with the
-// instant-ngp primes, dense indexing for coarse levels), a 48-64-64-64-48
+// hash-grid encoding (16 levels x 2 features; 2x2x2 vertex blocks placed by
+// a spatial hash with the instant-ngp primes, densely on coarse levels), a
+// 48-64-64-64-48
 // ReLU MLP, and the loss -w log q(wi) of an 8-lobe von Mises-Fisher
 // mixture. Arithmetic is f64; the values the GPU stores in bf16 (layer
 // inputs, activations and the back-propagated dZ fed to the tensor cores)
@@ -47,8 +48,12 @@ double half_to_double(uint16_t h) {
 }
 
 uint32_t grid_index(uint32_t x, uint32_t y, uint32_t z, uint32_t res1, bool dense) {
-    if (dense) return x + y * res1 + z * res1 * res1;
-    return (x * 1u ^ y * 2654435761u ^ z * 805459861u) & (T - 1u);
+    // 2x2x2 vertex blocks of 8 consecutive entries; blocks placed densely or by
+    // the Teschner et al. spatial hash (as render.rs_b200/csrc/guide.cuh)
+    const uint32_t intra = (x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2);
+    const uint32_t bx = x >> 1, by = y >> 1, bz = z >> 1, nb = (res1 + 1u) >> 1;
+    const uint32_t block = dense ? bx + (by + bz * nb) * nb : (bx * 1u ^ by * 2654435761u ^ bz * 805459861u);
+    return (block * 8u + intra) & (T - 1u);
 }
 
 struct Corner {
@@ -66,7 +71,8 @@ void encode(const double* table, const float* res, const float* lo, const float*
     for (int l = 0; l < L; l++) {
         float r = res[l];
         uint32_t res1 = (uint32_t)r + 2u;
-        bool dense = (uint64_t)res1 * res1 * res1 <= T;
+        const uint64_t nb = (res1 + 1u) >> 1;
+        bool dense = nb * nb * nb * 8u <= T;
         float fx = (float)pn[0] * r, fy = (float)pn[1] * r, fz = (float)pn[2] * r;
         float ix = std::floor(fx), iy = std::floor(fy), iz = std::floor(fz);
         double tx = fx - ix, ty = fy - iy, tz = fz - iz;

@@ -3,14 +3,16 @@
 // Kernels (one training iteration = encode -> forward -> backward -> hash
 // backward -> Adam; inference = encode -> forward):
 //   k_guide_encode    hash-grid features (+ normal, wo) -> X0 rows, bf16
-//   k_guide_fwd       tcgen05 MLP forward, 128-row tiles, weights resident in
-//                     shared memory, accumulators in TMEM; stores activations
-//                     (training) and the 48 raw outputs (f32)
+//   k_guide_fwd       tcgen05 MLP forward, 128-row tiles in two independent
+//                     pipelines per CTA, weights resident in shared memory,
+//                     accumulators in TMEM; stores activations (training) and
+//                     the 48 raw outputs, or the decoded mixture when rendering
 //   k_guide_bwd       vMF-mixture loss gradient in registers, then per layer
 //                     two tcgen05 GEMMs: dW = dZ^T H (batch is the K dimension)
 //                     and dH = dZ W; dW/db reduced into f32 gradients
 //   k_guide_hash_bwd  scatter-add of d loss / d features into the table gradient
 //   k_guide_adam      Adam on the f32 masters, refreshing the bf16 / fp16 copies
+//                     (lazy on the hash table: entries without gradient skip)
 // Loss: -w * log q(wi | x) with w = lum(f cos Li) / p_sample, the
 // importance-weighted KL objective of neural importance sampling
 // (Müller et al. 2019), estimated from the path tracer's own vertices.
@@ -84,86 +86,117 @@ __device__ void stage_transpose(uint8_t* dst, const __nv_bfloat16* src, int R, i
 
 // ---- encode -------------------------------------------------------------------
 // rec: 16 floats per record (pos xyz, normal xyz, wo xyz, wi xyz, weight, -).
-__global__ void k_guide_encode(GuideDev G, const float* __restrict__ rec, uint32_t n, const uint32_t* n_dev,
-                               __nv_bfloat16* X0) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n_dev) n = min(n, *n_dev);
-    if (i >= n) return;
-    const float* r = rec + 16 * (size_t)i;
-    float feat[G_IN];
+// One record -> 48 network inputs (32 hash-grid features, normal, wo, zeros).
+__device__ __forceinline__ void encode_record(const GuideDev& G, const float* r, float* feat) {
     hash_encode(G, guide_normalize_pos(G, f3(r[0], r[1], r[2])), feat);
 #pragma unroll
     for (int k = 0; k < 6; k++) feat[32 + k] = r[3 + k];
 #pragma unroll
     for (int k = 38; k < G_IN; k++) feat[k] = 0.f;
+}
+
+// Encoding runs as its own kernel at full occupancy: its cost is the 128
+// scattered table reads per record, which need many threads in flight (inside
+// the 128-thread forward CTAs they ran 1.7x slower than here).
+__global__ void __launch_bounds__(256) k_guide_encode(GuideDev G, const float* __restrict__ rec, uint32_t n,
+                                                      BatchSel B, __nv_bfloat16* X0) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, begin;
+    n = batch_slice(B, n, begin);
+    rec += 16 * (size_t)begin;
+    if (i >= n) return;
+    float feat[G_IN];
+    encode_record(G, rec + 16 * (size_t)i, feat);
     uint4* out = reinterpret_cast<uint4*>(X0 + (size_t)i * G_IN);
 #pragma unroll
-    for (int c = 0; c < G_IN / 8; c++) {
+    for (int c = 0; c < G_IN / 8; c++)
         out[c] = make_uint4(pack_bf16(feat[8 * c], feat[8 * c + 1]), pack_bf16(feat[8 * c + 2], feat[8 * c + 3]),
                             pack_bf16(feat[8 * c + 4], feat[8 * c + 5]), pack_bf16(feat[8 * c + 6], feat[8 * c + 7]));
-    }
 }
 
 // ---- forward ------------------------------------------------------------------
-// Shared memory: W0 6144 | W1 8192 | W2 8192 | W3 6144 | X 12288 | HA 16384 | HB 16384
-constexpr int F_W0 = 0, F_W1 = 6144, F_W2 = F_W1 + 8192, F_W3 = F_W2 + 8192, F_X = F_W3 + 6144,
-              F_HA = F_X + 12288, F_HB = F_HA + 16384, F_BYTES = F_HB + 16384;
+// Each CTA runs FWD_GROUPS independent 128-row tile pipelines (one per 128
+// threads) that share the weights in shared memory; a pipeline's layers are
+// latency-bound (MMA -> commit -> TMEM load -> epilogue), so several tiles in
+// flight per SM hide each other's waits. A tile keeps one activation buffer:
+// X (K = 48), then H1, H2, H3 (K = 64) overwrite it in turn, which is safe
+// because a layer's MMA has finished reading its input when the epilogue runs.
+// Shared memory: W0 6144 | W1 8192 | W2 8192 | W3 6144 | ACT 16384 per group.
+constexpr int FWD_GROUPS = 2, FWD_THREADS = FWD_GROUPS * TILE;
+constexpr int F_W0 = 0, F_W1 = 6144, F_W2 = F_W1 + 8192, F_W3 = F_W2 + 8192, F_ACT = F_W3 + 6144,
+              F_BYTES = F_ACT + FWD_GROUPS * 16384;
 
-template <bool TRAIN>
-__global__ void __launch_bounds__(TILE) k_guide_fwd(GuideDev G, const __nv_bfloat16* __restrict__ X0, uint32_t n,
-                                                    const uint32_t* n_dev, __nv_bfloat16* acts, float* out,
-                                                    uint32_t* err) {
-    if (n_dev) n = min(n, *n_dev);
+// Modes: raw outputs (inference API), training (raw outputs + the hidden
+// activations the backward pass reads), rendering (the decoded mixture of
+// guide.cuh, 48 floats).
+enum { FWD_RAW = 0, FWD_TRAIN = 1, FWD_RENDER = 2 };
+
+template <int MODE>
+__global__ void __launch_bounds__(FWD_THREADS, 3) k_guide_fwd(GuideDev G, const __nv_bfloat16* __restrict__ X0,
+                                                              uint32_t n, BatchSel B, __nv_bfloat16* acts,
+                                                              float* out, uint32_t* err) {
+    constexpr bool TRAIN = MODE == FWD_TRAIN;
+    uint32_t begin;
+    n = batch_slice(B, n, begin);
+    if ((uint64_t)blockIdx.x * FWD_GROUPS * TILE >= n) return;  // no tile for this CTA: skip the weight staging
     extern __shared__ __align__(1024) uint8_t sm[];
-    __shared__ uint64_t mbar;
+    __shared__ uint64_t mbar[FWD_GROUPS];
     __shared__ uint32_t tmem_base;
+    __shared__ uint32_t group_failed[FWD_GROUPS];
     __shared__ float bias[G_NBIAS];
-    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, grp = tid / TILE, gt = tid % TILE;
     stage_matrix(sm + F_W0, G.w + w_off(0), G_HID, G_IN);
     stage_matrix(sm + F_W1, G.w + w_off(1), G_HID, G_HID);
     stage_matrix(sm + F_W2, G.w + w_off(2), G_HID, G_HID);
     stage_matrix(sm + F_W3, G.w + w_off(3), G_OUT, G_HID);
-    for (int i = tid; i < G_NBIAS; i += TILE) bias[i] = G.b[i];
-    if (warp == 0) tmem_alloc(&tmem_base, 64);
-    if (tid == 0) mbar_init(&mbar, 1);
+    for (int i = tid; i < G_NBIAS; i += FWD_THREADS) bias[i] = G.b[i];
+    if (warp == 0) tmem_alloc(&tmem_base, 64 * FWD_GROUPS);
+    if (tid < FWD_GROUPS) {
+        mbar_init(&mbar[tid], 1);
+        group_failed[tid] = 0;
+    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    const uint32_t tb = tmem_base;
-    const uint32_t lane_addr = tb + ((uint32_t)(warp * 32) << 16);
-    uint32_t phase = 0;
+    // Group grp owns TMEM columns [64 grp, 64 grp + 64); warp w reads lanes 32 (w % 4) ...
+    const uint32_t acc = tmem_base + 64u * grp;
+    const uint32_t lane_addr = acc + ((uint32_t)((warp & 3) * 32) << 16);
     const uint32_t s0 = smem_u32(sm);
-    bool failed = false;
-    for (uint32_t tile = blockIdx.x; tile * TILE < n && !failed; tile += gridDim.x) {
-        uint32_t row = tile * TILE + tid;
+    const uint32_t act = F_ACT + 16384u * grp;
+    uint32_t phase = 0;
+    for (uint32_t tile = blockIdx.x * FWD_GROUPS + grp; tile * TILE < n; tile += gridDim.x * FWD_GROUPS) {
+        uint32_t row = tile * TILE + gt;
         bool valid = row < n;
         const uint4* xr = reinterpret_cast<const uint4*>(X0 + (size_t)row * G_IN);
 #pragma unroll
         for (int c = 0; c < G_IN / 8; c++)
-            *reinterpret_cast<uint4*>(sm + F_X + core_offset(tid, 8 * c, G_IN)) = valid ? xr[c] : make_uint4(0, 0, 0, 0);
-        for (int l = 0; l < 4 && !failed; l++) {
+            *reinterpret_cast<uint4*>(sm + act + core_offset(gt, 8 * c, G_IN)) = valid ? xr[c] : make_uint4(0, 0, 0, 0);
+        bool failed = false;
+        for (int l = 0; l < 4; l++) {
             const int K = l_in(l), N = l_out(l);
-            const uint32_t a_off = l == 0 ? F_X : (l & 1) ? F_HA : F_HB;
             const uint32_t w_sm = l == 0 ? F_W0 : l == 1 ? F_W1 : l == 2 ? F_W2 : F_W3;
-            const uint32_t o_off = (l & 1) ? F_HB : F_HA;
             fence_proxy_async_smem();
-            __syncthreads();
-            if (tid == 0) {
+            group_sync(grp);
+            if (gt == 0) {
                 tc_fence_after();
-                tc_gemm_issue(tb, s0 + a_off, s0 + w_sm, N, K, false);
-                tc_commit(&mbar);
+                tc_gemm_issue(acc, s0 + act, s0 + w_sm, N, K, false);
+                tc_commit(&mbar[grp]);
             }
-            bool ok = mbar_wait_bounded(&mbar, phase);
+            if (!mbar_wait_bounded(&mbar[grp], phase)) group_failed[grp] = 1;
             phase ^= 1u;
-            if (__syncthreads_or(!ok)) {
+            group_sync(grp);
+            if (group_failed[grp]) {
                 failed = true;
                 break;
             }
             tc_fence_after();
-            float v[64];
+            uint32_t r[64];
 #pragma unroll
             for (int c = 0; c < 4; c++)
-                if (c * 16 < N) tmem_ld16(lane_addr + c * 16, v + 16 * c);
+                if (c * 16 < N) tmem_ld16_nowait(lane_addr + c * 16, r + 16 * c);
+            tmem_ld_wait();
+            float v[64];
+#pragma unroll
+            for (int k = 0; k < 64; k++) v[k] = __uint_as_float(r[k]);
             if (l < 3) {
 #pragma unroll
                 for (int k = 0; k < 64; k++) v[k] = fmaxf(v[k] + bias[b_off(l) + k], 0.f);
@@ -171,25 +204,34 @@ __global__ void __launch_bounds__(TILE) k_guide_fwd(GuideDev G, const __nv_bfloa
                 for (int c = 0; c < 8; c++) {
                     uint4 q = make_uint4(pack_bf16(v[8 * c], v[8 * c + 1]), pack_bf16(v[8 * c + 2], v[8 * c + 3]),
                                          pack_bf16(v[8 * c + 4], v[8 * c + 5]), pack_bf16(v[8 * c + 6], v[8 * c + 7]));
-                    *reinterpret_cast<uint4*>(sm + o_off + core_offset(tid, 8 * c, G_HID)) = q;
+                    *reinterpret_cast<uint4*>(sm + act + core_offset(gt, 8 * c, G_HID)) = q;
                     if (TRAIN && valid)
                         reinterpret_cast<uint4*>(acts + ((size_t)row * 3 + l) * G_HID)[c] = q;
                 }
             } else if (valid) {
-                float4* o = reinterpret_cast<float4*>(out + (size_t)row * G_OUT);
 #pragma unroll
-                for (int c = 0; c < G_OUT / 4; c++)
-                    o[c] = make_float4(v[4 * c] + bias[b_off(3) + 4 * c], v[4 * c + 1] + bias[b_off(3) + 4 * c + 1],
-                                       v[4 * c + 2] + bias[b_off(3) + 4 * c + 2],
-                                       v[4 * c + 3] + bias[b_off(3) + 4 * c + 3]);
+                for (int k = 0; k < G_OUT; k++) v[k] += bias[b_off(3) + k];
+                if (MODE == FWD_RENDER) {
+                    Mixture mx;
+                    mixture_decode(v, mx);
+                    mixture_store(mx, out + (size_t)row * G_OUT);
+                } else {
+                    float4* o = reinterpret_cast<float4*>(out + (size_t)row * G_OUT);
+#pragma unroll
+                    for (int c = 0; c < G_OUT / 4; c++) o[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+                }
             }
             tc_fence_before();
         }
+        if (failed) {
+            if (gt == 0) atomicOr(err, GERR_WAIT);
+            break;
+        }
     }
-    if (failed && tid == 0) atomicOr(err, GERR_WAIT);
     __syncthreads();
     if (warp == 0) {
-        tmem_dealloc(tb, 64);
+        tc_fence_after();
+        tmem_dealloc(tmem_base, 64 * FWD_GROUPS);
         tmem_relinquish();
     }
 }
@@ -203,9 +245,12 @@ constexpr int B_WT0 = 0, B_WT1 = 6144, B_WT2 = B_WT1 + 8192, B_WT3 = B_WT2 + 819
 __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloat16* __restrict__ X0,
                                                     const __nv_bfloat16* __restrict__ acts,
                                                     const float* __restrict__ out, const float* __restrict__ rec,
-                                                    uint32_t n, const uint32_t* n_dev, float* gW, float* gb,
+                                                    uint32_t n, BatchSel B, float* gW, float* gb,
                                                     float* dX0, float* loss_sum, uint32_t* err) {
-    if (n_dev) n = min(n, *n_dev);
+    uint32_t begin;
+    n = batch_slice(B, n, begin);
+    rec += 16 * (size_t)begin;
+    if ((uint64_t)blockIdx.x * TILE >= n) return;
     extern __shared__ __align__(1024) uint8_t sm[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
@@ -365,9 +410,10 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
 
 // ---- hash-grid backward ---------------------------------------------------------
 __global__ void k_guide_hash_bwd(GuideDev G, const float* __restrict__ rec, const float* __restrict__ dX0, uint32_t n,
-                                 const uint32_t* n_dev, float* gtable) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n_dev) n = min(n, *n_dev);
+                                 BatchSel B, float* gtable) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, begin;
+    n = batch_slice(B, n, begin);
+    rec += 16 * (size_t)begin;
     if (i >= n) return;
     const float* r = rec + 16 * (size_t)i;
     float3 pn = guide_normalize_pos(G, f3(r[0], r[1], r[2]));
@@ -375,7 +421,7 @@ __global__ void k_guide_hash_bwd(GuideDev G, const float* __restrict__ rec, cons
     for (int l = 0; l < G_LEVELS; l++) {
         float rs = G.res[l];
         uint32_t res1 = (uint32_t)rs + 2u;
-        bool dense = (uint64_t)res1 * res1 * res1 <= G_T;
+        bool dense = grid_dense(res1);
         float fx = pn.x * rs, fy = pn.y * rs, fz = pn.z * rs;
         float ix = floorf(fx), iy = floorf(fy), iz = floorf(fz);
         float tx = fx - ix, ty = fy - iy, tz = fz - iz;
@@ -386,27 +432,43 @@ __global__ void k_guide_hash_bwd(GuideDev G, const float* __restrict__ rec, cons
             uint32_t ddx = c & 1, ddy = (c >> 1) & 1, ddz = (c >> 2) & 1;
             float w = (ddx ? tx : 1.f - tx) * (ddy ? ty : 1.f - ty) * (ddz ? tz : 1.f - tz);
             uint32_t idx = grid_index(x0 + ddx, y0 + ddy, z0 + ddz, res1, dense);
-            atomicAdd(T + 2 * idx, w * g0);
-            atomicAdd(T + 2 * idx + 1, w * g1);
+            atomicAdd(reinterpret_cast<float2*>(T) + idx, make_float2(w * g0, w * g1));
         }
     }
 }
 
 // ---- Adam -----------------------------------------------------------------------------
 struct AdamArgs {
-    float lr, b1, b2, eps, c1, c2;  // c1 = 1/(1-b1^t), c2 = 1/(1-b2^t)
+    float lr, b1, b2, eps;
+    const float* c;  // device: c[0] = 1/(1-b1^t), c[1] = 1/(1-b2^t), c[2] = 1 when the step runs
 };
+
+// Step counter and bias corrections on the device: a step whose batch slice is
+// empty is skipped (no update, no count).
+__global__ void k_guide_adam_tick(BatchSel B, uint32_t cap, AdamArgs A, uint32_t* step, float* c) {
+    uint32_t begin;
+    uint32_t n = batch_slice(B, cap, begin);
+    if (n == 0) {
+        c[2] = 0.f;
+        return;
+    }
+    uint32_t t = ++*step;
+    c[0] = 1.f / (1.f - powf(A.b1, (float)t));
+    c[1] = 1.f / (1.f - powf(A.b2, (float)t));
+    c[2] = 1.f;
+}
 
 __global__ void k_guide_adam_mlp(AdamArgs A, float* p, float* g, float* m, float* v, __nv_bfloat16* w16, int n_weights,
                                  int n_total) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_total) return;
+    if (i >= n_total || A.c[2] == 0.f) return;
+    const float c1 = A.c[0], c2 = A.c[1];
     float gi = g[i];
     float mi = A.b1 * m[i] + (1.f - A.b1) * gi;
     float vi = A.b2 * v[i] + (1.f - A.b2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
-    float pi = p[i] - A.lr * (mi * A.c1) / (sqrtf(vi * A.c2) + A.eps);
+    float pi = p[i] - A.lr * (mi * c1) / (sqrtf(vi * c2) + A.eps);
     p[i] = pi;
     g[i] = 0.f;
     if (i < n_weights) w16[i] = __float2bfloat16_rn(pi);
@@ -414,14 +476,18 @@ __global__ void k_guide_adam_mlp(AdamArgs A, float* p, float* g, float* m, float
 
 __global__ void k_guide_adam_table(AdamArgs A, float* p, float* g, float* m, float* v, __half* t16, uint32_t n) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || A.c[2] == 0.f) return;
+    const float c1 = A.c[0], c2 = A.c[1];
+    // Lazy (sparse) Adam: a table entry no record touched this step keeps its
+    // parameter and moments. A batch touches a few percent of the 16M
+    // entries, so the step reads the gradient table and updates only those.
     float gi = g[i];
-    if (gi == 0.f && m[i] == 0.f) return;  // untouched entries stay put
+    if (gi == 0.f) return;
     float mi = A.b1 * m[i] + (1.f - A.b1) * gi;
     float vi = A.b2 * v[i] + (1.f - A.b2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
-    float pi = p[i] - A.lr * (mi * A.c1) / (sqrtf(vi * A.c2) + A.eps);
+    float pi = p[i] - A.lr * (mi * c1) / (sqrtf(vi * c2) + A.eps);
     p[i] = pi;
     g[i] = 0.f;
     t16[i] = __float2half_rn(pi);
@@ -480,8 +546,9 @@ struct rt_guide {
     float* mt = nullptr;
     float* vt = nullptr;
     __half* t16 = nullptr;
-    // scratch for a batch
-    uint32_t cap = 0;
+    // scratch for a batch: inputs and outputs for `cap` records, activations
+    // and input gradients for `train_cap` (training batches only)
+    uint32_t cap = 0, train_cap = 0;
     __nv_bfloat16* X0 = nullptr;
     __nv_bfloat16* acts = nullptr;
     float* out = nullptr;
@@ -491,7 +558,8 @@ struct rt_guide {
     float* rec_dev = nullptr;  // staging for host-pointer calls
     uint32_t rec_cap = 0;
     int sms = 148;
-    uint64_t step = 0;
+    uint32_t* step = nullptr;  // device: Adam steps taken
+    float* adam_c = nullptr;   // device: bias corrections of the current step
     float lr = 1e-2f;
     std::vector<void*> allocs;
 
@@ -504,19 +572,27 @@ struct rt_guide {
         *p = (T*)v;
         return 0;
     }
-    int ensure(uint32_t n) {
-        if (n <= cap) return 0;
-        for (void* q : {(void*)X0, (void*)acts, (void*)out, (void*)dX0}) {
-            if (q) {
-                cudaFree(q);
-                allocs.erase(std::remove(allocs.begin(), allocs.end(), q), allocs.end());
-            }
+    void release(void* q) {
+        if (!q) return;
+        cudaFree(q);
+        allocs.erase(std::remove(allocs.begin(), allocs.end(), q), allocs.end());
+    }
+    int ensure(uint32_t n, bool train) {
+        int rc = 0;
+        if (n > cap) {
+            release(X0);
+            release(out);
+            cap = std::max(n, 1u << 16);
+            rc = rc ? rc : alloc(&X0, (size_t)cap * G_IN);
+            rc = rc ? rc : alloc(&out, (size_t)cap * G_OUT);
         }
-        cap = std::max(n, 1u << 16);
-        int rc = alloc(&X0, (size_t)cap * G_IN);
-        rc = rc ? rc : alloc(&acts, (size_t)cap * 3 * G_HID);
-        rc = rc ? rc : alloc(&out, (size_t)cap * G_OUT);
-        rc = rc ? rc : alloc(&dX0, (size_t)cap * 32);
+        if (train && n > train_cap) {
+            release(acts);
+            release(dX0);
+            train_cap = std::max(n, 1u << 16);
+            rc = rc ? rc : alloc(&acts, (size_t)train_cap * 3 * G_HID);
+            rc = rc ? rc : alloc(&dX0, (size_t)train_cap * 32);
+        }
         return rc;
     }
     ~rt_guide() {
@@ -525,39 +601,39 @@ struct rt_guide {
     }
 };
 
-static int launch_forward(rt_guide* g, const float* rec, uint32_t n, bool train, cudaStream_t st,
-                          const uint32_t* n_dev = nullptr) {
+static int launch_forward(rt_guide* g, const float* rec, uint32_t n, int mode, cudaStream_t st,
+                          BatchSel B = BatchSel{nullptr, 0, 1}) {
     if (n == 0) return 0;
-    int rc = g->ensure(n);
+    int rc = g->ensure(n, mode == FWD_TRAIN);
     if (rc) return rc;
-    k_guide_encode<<<(n + 127) / 128, 128, 0, st>>>(g->G, rec, n, n_dev, g->X0);
+    k_guide_encode<<<(n + 255) / 256, 256, 0, st>>>(g->G, rec, n, B, g->X0);
     uint32_t tiles = (n + TILE - 1) / TILE;
-    int grid = (int)std::min<uint32_t>(tiles, (uint32_t)g->sms * 2);
-    if (train)
-        k_guide_fwd<true><<<grid, TILE, F_BYTES, st>>>(g->G, g->X0, n, n_dev, g->acts, g->out, g->err);
+    int grid = (int)std::min<uint32_t>((tiles + FWD_GROUPS - 1) / FWD_GROUPS, (uint32_t)g->sms * 3);
+    if (mode == FWD_TRAIN)
+        k_guide_fwd<FWD_TRAIN><<<grid, FWD_THREADS, F_BYTES, st>>>(g->G, g->X0, n, B, g->acts, g->out, g->err);
+    else if (mode == FWD_RENDER)
+        k_guide_fwd<FWD_RENDER><<<grid, FWD_THREADS, F_BYTES, st>>>(g->G, g->X0, n, B, g->acts, g->out, g->err);
     else
-        k_guide_fwd<false><<<grid, TILE, F_BYTES, st>>>(g->G, g->X0, n, n_dev, g->acts, g->out, g->err);
+        k_guide_fwd<FWD_RAW><<<grid, FWD_THREADS, F_BYTES, st>>>(g->G, g->X0, n, B, g->acts, g->out, g->err);
     G_TRY(cudaGetLastError());
     return 0;
 }
 
 static int launch_backward(rt_guide* g, const float* rec, uint32_t n, cudaStream_t st,
-                           const uint32_t* n_dev = nullptr) {
+                           BatchSel B = BatchSel{nullptr, 0, 1}) {
     uint32_t tiles = (n + TILE - 1) / TILE;
     int grid = (int)std::min<uint32_t>(tiles, (uint32_t)g->sms * 2);
     G_TRY(cudaMemsetAsync(g->loss, 0, 4, st));
-    k_guide_bwd<<<grid, TILE, B_BYTES, st>>>(g->G, g->X0, g->acts, g->out, rec, n, n_dev, g->gw, g->gw + G_NWEIGHTS,
+    k_guide_bwd<<<grid, TILE, B_BYTES, st>>>(g->G, g->X0, g->acts, g->out, rec, n, B, g->gw, g->gw + G_NWEIGHTS,
                                              g->dX0, g->loss, g->err);
-    k_guide_hash_bwd<<<(n + 127) / 128, 128, 0, st>>>(g->G, rec, g->dX0, n, n_dev, g->gt);
+    k_guide_hash_bwd<<<(n + 127) / 128, 128, 0, st>>>(g->G, rec, g->dX0, n, B, g->gt);
     G_TRY(cudaGetLastError());
     return 0;
 }
 
-static void launch_adam(rt_guide* g, cudaStream_t st) {
-    g->step++;
-    AdamArgs A{g->lr, 0.9f, 0.99f, 1e-8f, 0, 0};
-    A.c1 = 1.f / (1.f - std::pow(A.b1, (float)g->step));
-    A.c2 = 1.f / (1.f - std::pow(A.b2, (float)g->step));
+static void launch_adam(rt_guide* g, uint32_t n, cudaStream_t st, BatchSel B = BatchSel{nullptr, 0, 1}) {
+    AdamArgs A{g->lr, 0.9f, 0.99f, 1e-8f, g->adam_c};
+    k_guide_adam_tick<<<1, 1, 0, st>>>(B, n, A, g->step, g->adam_c);
     k_guide_adam_mlp<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(A, g->w32, g->gw, g->mw, g->vw, g->w16, G_NWEIGHTS,
                                                              G_NPARAMS);
     uint32_t tn = (uint32_t)(G_LEVELS * G_T * 2);
@@ -569,19 +645,25 @@ namespace rt {
 
 int guide_infer_counted(rt_guide* g, const float* rec, const uint32_t* n_dev, uint32_t cap, float** raw_out,
                         cudaStream_t st) {
-    int rc = launch_forward(g, rec, cap, false, st, n_dev);
+    int rc = launch_forward(g, rec, cap, FWD_RENDER, st, BatchSel{n_dev, 0, 1});
     *raw_out = g->out;
     return rc;
 }
 
-int guide_train_counted(rt_guide* g, const float* rec, const uint32_t* n_dev, uint32_t cap, cudaStream_t st) {
-    int rc = launch_forward(g, rec, cap, true, st, n_dev);
-    rc = rc ? rc : launch_backward(g, rec, cap, st, n_dev);
-    if (rc) return rc;
-    launch_adam(g, st);
+int guide_train_slices(rt_guide* g, const float* rec, const uint32_t* total_dev, uint32_t cap, uint32_t steps,
+                       cudaStream_t st) {
+    for (uint32_t s = 0; s < steps; s++) {
+        const BatchSel B{total_dev, s, steps};
+        int rc = launch_forward(g, rec, cap, FWD_TRAIN, st, B);
+        rc = rc ? rc : launch_backward(g, rec, cap, st, B);
+        if (rc) return rc;
+        launch_adam(g, cap, st, B);
+    }
     G_TRY(cudaGetLastError());
     return 0;
 }
+
+int guide_reserve(rt_guide* g, uint32_t n) { return g->ensure(n, false); }
 
 const float* guide_loss_ptr(rt_guide* g) { return g->loss; }
 const uint32_t* guide_err_ptr(rt_guide* g) { return g->err; }
@@ -629,13 +711,16 @@ int rt_guide_create(const float* lo, const float* hi, uint64_t seed, float lr, r
     rc = rc ? rc : g->alloc(&g->t16, tn);
     rc = rc ? rc : g->alloc(&g->loss, 1);
     rc = rc ? rc : g->alloc(&g->err, 1);
-    rc = rc ? rc : g->ensure(1u << 16);
+    rc = rc ? rc : g->alloc(&g->step, 1);
+    rc = rc ? rc : g->alloc(&g->adam_c, 4);
+    rc = rc ? rc : g->ensure(1u << 16, true);
     if (rc) {
         delete g;
         return rc;
     }
-    cudaFuncSetAttribute(k_guide_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, F_BYTES);
-    cudaFuncSetAttribute(k_guide_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, F_BYTES);
+    cudaFuncSetAttribute(k_guide_fwd<FWD_RAW>, cudaFuncAttributeMaxDynamicSharedMemorySize, F_BYTES);
+    cudaFuncSetAttribute(k_guide_fwd<FWD_TRAIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, F_BYTES);
+    cudaFuncSetAttribute(k_guide_fwd<FWD_RENDER>, cudaFuncAttributeMaxDynamicSharedMemorySize, F_BYTES);
     cudaFuncSetAttribute(k_guide_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, B_BYTES);
     cudaFuncSetAttribute(k_tc_selftest, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024);
     // Init: He-uniform weights, zero biases; table U(-1e-4, 1e-4) (instant-ngp).
@@ -668,6 +753,7 @@ int rt_guide_create(const float* lo, const float* hi, uint64_t seed, float lr, r
     cudaMemset(g->mt, 0, tn * 4);
     cudaMemset(g->vt, 0, tn * 4);
     cudaMemset(g->err, 0, 4);
+    cudaMemset(g->step, 0, 4);
     g->G.table = reinterpret_cast<const __half2*>(g->t16);
     g->G.w = g->w16;
     g->G.b = g->w32 + G_NWEIGHTS;
@@ -739,7 +825,7 @@ int rt_guide_info(rt_guide* g, float* res_out, float* lo_out, float* inv_ext_out
 int rt_guide_infer_device(rt_guide* g, const float* rec, uint32_t n, float* raw_out, void* stream) {
     if (!g || (n && (!rec || !raw_out))) return gfail(-1, "NULL argument");
     cudaStream_t st = (cudaStream_t)stream;
-    int rc = launch_forward(g, rec, n, false, st);
+    int rc = launch_forward(g, rec, n, FWD_RAW, st);
     if (rc) return rc;
     if (n) G_TRY(cudaMemcpyAsync(raw_out, g->out, (size_t)n * G_OUT * 4, cudaMemcpyDeviceToDevice, st));
     return 0;
@@ -749,10 +835,10 @@ int rt_guide_train_step_device(rt_guide* g, const float* rec, uint32_t n, float*
     if (!g || (n && !rec)) return gfail(-1, "NULL argument");
     cudaStream_t st = (cudaStream_t)stream;
     if (n == 0) return 0;
-    int rc = launch_forward(g, rec, n, true, st);
+    int rc = launch_forward(g, rec, n, FWD_TRAIN, st);
     rc = rc ? rc : launch_backward(g, rec, n, st);
     if (rc) return rc;
-    launch_adam(g, st);
+    launch_adam(g, n, st);
     G_TRY(cudaGetLastError());
     if (loss_out) {
         G_TRY(cudaMemcpyAsync(loss_out, g->loss, 4, cudaMemcpyDeviceToHost, st));
@@ -771,7 +857,7 @@ int rt_guide_grads(rt_guide* g, const float* rec_host, uint32_t n, float* g_mlp,
     size_t tn = (size_t)G_LEVELS * G_T * 2;
     cudaMemset(g->gw, 0, G_NPARAMS * 4);
     cudaMemset(g->gt, 0, tn * 4);
-    int rc = launch_forward(g, rec, n, true, 0);
+    int rc = launch_forward(g, rec, n, FWD_TRAIN, 0);
     rc = rc ? rc : launch_backward(g, rec, n, 0);
     if (!rc) rc = check_err(g, 0);
     if (!rc && g_mlp) G_TRY(cudaMemcpy(g_mlp, g->gw, G_NPARAMS * 4, cudaMemcpyDeviceToHost));
@@ -803,7 +889,7 @@ int rt_guide_infer(rt_guide* g, const float* rec_host, uint32_t n, float* raw_ho
     float* rec = nullptr;
     G_TRY(cudaMalloc(&rec, (size_t)n * 64));
     G_TRY(cudaMemcpy(rec, rec_host, (size_t)n * 64, cudaMemcpyHostToDevice));
-    int rc = launch_forward(g, rec, n, false, 0);
+    int rc = launch_forward(g, rec, n, FWD_RAW, 0);
     if (!rc) rc = check_err(g, 0);
     if (!rc) G_TRY(cudaMemcpy(raw_host, g->out, (size_t)n * G_OUT * 4, cudaMemcpyDeviceToHost));
     cudaFree(rec);

@@ -33,6 +33,24 @@ static const int G_NWEIGHTS = G_NW0 + G_NW1 + G_NW2 + G_NW3;
 static const int G_NBIAS = G_HID * 3 + G_OUT;
 static const int G_NPARAMS = G_NWEIGHTS + G_NBIAS;  // MLP parameters (table separate)
 
+// Which records of a buffer a training or inference launch processes. With
+// `total` null: the launch's own count. Otherwise the count lives in device
+// memory and the launch takes slice s of `steps` equal slices of
+// min(*total, steps * cap), so a slab's training batches are chosen on the
+// device without a host round trip.
+struct BatchSel {
+    const uint32_t* total;
+    uint32_t s, steps;
+};
+
+__device__ __forceinline__ uint32_t batch_slice(const BatchSel& b, uint32_t cap, uint32_t& begin) {
+    begin = 0;
+    if (!b.total) return cap;
+    uint64_t t = min((uint64_t)*b.total, (uint64_t)cap * b.steps);
+    begin = (uint32_t)(t * b.s / b.steps);
+    return (uint32_t)(t * (b.s + 1) / b.steps) - begin;
+}
+
 struct GuideDev {
     const __half2* table;     // [levels][T] feature pairs (FP16)
     const __nv_bfloat16* w;   // MLP weights, row-major [out][in], layers concatenated
@@ -41,20 +59,30 @@ struct GuideDev {
     float lo[3], inv_ext[3];  // scene bounds -> [0,1]^3
 };
 
-// Spatial hash of a grid vertex (Teschner et al. 2003 primes, as used by
-// instant-ngp); coarse levels whose grid fits the table index densely.
+// Table slot of a grid vertex. Vertices are stored in 2x2x2 blocks of 8
+// consecutive entries (32 bytes, one memory sector), so the 8 corners of a
+// cell touch 1 to 8 sectors, 3.4 on average, instead of 8. Blocks are placed
+// by the spatial hash of Teschner et al. 2003 (the primes instant-ngp uses),
+// or densely on coarse levels whose blocks all fit in the table.
+__host__ __device__ __forceinline__ uint32_t grid_blocks(uint32_t res1) { return (res1 + 1u) >> 1; }
+__host__ __device__ __forceinline__ bool grid_dense(uint32_t res1) {
+    const uint64_t nb = grid_blocks(res1);
+    return nb * nb * nb * 8u <= G_T;
+}
 __device__ __forceinline__ uint32_t grid_index(uint32_t x, uint32_t y, uint32_t z, uint32_t res1, bool dense) {
-    if (dense) return x + y * res1 + z * res1 * res1;
-    return (x * 1u ^ y * 2654435761u ^ z * 805459861u) & (G_T - 1u);
+    const uint32_t intra = (x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2);
+    const uint32_t bx = x >> 1, by = y >> 1, bz = z >> 1, nb = grid_blocks(res1);
+    const uint32_t block = dense ? bx + (by + bz * nb) * nb : (bx * 1u ^ by * 2654435761u ^ bz * 805459861u);
+    return (block * 8u + intra) & (G_T - 1u);
 }
 
 // Encode one position: 32 features (16 levels x 2), trilinear in each level.
 __device__ __forceinline__ void hash_encode(const GuideDev& G, float3 pn, float* feat) {
-#pragma unroll 4
+#pragma unroll
     for (int l = 0; l < G_LEVELS; l++) {
         float r = G.res[l];
         uint32_t res1 = (uint32_t)r + 2u;
-        bool dense = (uint64_t)res1 * res1 * res1 <= G_T;
+        bool dense = grid_dense(res1);
         float fx = pn.x * r, fy = pn.y * r, fz = pn.z * r;
         float ix = floorf(fx), iy = floorf(fy), iz = floorf(fz);
         float tx = fx - ix, ty = fy - iy, tz = fz - iz;
@@ -82,10 +110,16 @@ __device__ __forceinline__ float3 guide_normalize_pos(const GuideDev& G, float3 
 // ---- von Mises-Fisher mixture ----------------------------------------------------
 // Raw outputs per lobe j: o[5j..5j+2] mean (unnormalised), o[5j+3] log kappa,
 // o[5j+4] weight logit. kappa = exp(clamp(., -4, 9)); weights = softmax.
+// The renderer reads the mixture in decoded form (48 floats, written by the
+// forward pass): lobe j's (mu.xyz, kappa) at [4j, 4j+4), its weight at
+// [32 + j] and at [40 + j] the log of its weighted density at mu.w = 0,
+// A_j = log w_j + log(kappa_j / (2 pi (1 - e^{-2 kappa_j}))) - kappa_j, so that
+// q(w) = sum_j exp(A_j + kappa_j mu_j.w).
 struct Mixture {
     float3 mu[G_LOBES];
     float kappa[G_LOBES];
     float w[G_LOBES];
+    float A[G_LOBES];
 };
 
 __device__ __forceinline__ void mixture_decode(const float* o, Mixture& m) {
@@ -103,7 +137,37 @@ __device__ __forceinline__ void mixture_decode(const float* o, Mixture& m) {
         sw += m.w[j];
     }
 #pragma unroll
-    for (int j = 0; j < G_LOBES; j++) m.w[j] /= sw;
+    for (int j = 0; j < G_LOBES; j++) {
+        m.w[j] /= sw;
+        const float k = m.kappa[j];
+        m.A[j] = logf(fmaxf(m.w[j], 1e-30f)) + logf(k) - logf(2.f * RT_PI) - log1pf(-__expf(-2.f * k)) - k;
+    }
+}
+
+// Decoded record <-> Mixture.
+__device__ __forceinline__ void mixture_store(const Mixture& m, float* dst) {
+    float4* d4 = reinterpret_cast<float4*>(dst);
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) d4[j] = make_float4(m.mu[j].x, m.mu[j].y, m.mu[j].z, m.kappa[j]);
+    d4[8] = make_float4(m.w[0], m.w[1], m.w[2], m.w[3]);
+    d4[9] = make_float4(m.w[4], m.w[5], m.w[6], m.w[7]);
+    d4[10] = make_float4(m.A[0], m.A[1], m.A[2], m.A[3]);
+    d4[11] = make_float4(m.A[4], m.A[5], m.A[6], m.A[7]);
+}
+
+__device__ __forceinline__ void mixture_load(const float* src, Mixture& m) {
+    const float4* s4 = reinterpret_cast<const float4*>(src);
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) {
+        float4 v = s4[j];
+        m.mu[j] = f3(v.x, v.y, v.z);
+        m.kappa[j] = v.w;
+    }
+    float4 a = s4[8], b = s4[9], c = s4[10], d = s4[11];
+    m.w[0] = a.x; m.w[1] = a.y; m.w[2] = a.z; m.w[3] = a.w;
+    m.w[4] = b.x; m.w[5] = b.y; m.w[6] = b.z; m.w[7] = b.w;
+    m.A[0] = c.x; m.A[1] = c.y; m.A[2] = c.z; m.A[3] = c.w;
+    m.A[4] = d.x; m.A[5] = d.y; m.A[6] = d.z; m.A[7] = d.w;
 }
 
 // log of the vMF density kappa / (2 pi (1 - e^{-2 kappa})) exp(kappa (mu.w - 1)).
@@ -115,7 +179,7 @@ __device__ __forceinline__ float vmf_log_pdf(float3 mu, float kappa, float3 w) {
 __device__ __forceinline__ float mixture_pdf(const Mixture& m, float3 w) {
     float p = 0.f;
 #pragma unroll
-    for (int j = 0; j < G_LOBES; j++) p += m.w[j] * __expf(vmf_log_pdf(m.mu[j], m.kappa[j], w));
+    for (int j = 0; j < G_LOBES; j++) p += __expf(m.A[j] + m.kappa[j] * dot(m.mu[j], w));
     return p;
 }
 

@@ -8,13 +8,18 @@
 
 namespace rt {
 
-// Inference / one training iteration on records whose count lives in device
-// memory (*n_dev <= cap), so a render wave needs no host round trip.
-// guide_infer_counted returns the raw-output buffer (48 floats per record),
-// valid until the next guide call.
+// Inference on records whose count lives in device memory (min(*n_dev, cap)
+// records), so a render wave needs no host round trip. Returns the buffer of
+// decoded mixtures (48 floats per record, guide.cuh), valid until the next
+// guide call.
 int guide_infer_counted(rt_guide* g, const float* rec, const uint32_t* n_dev, uint32_t cap, float** raw_out,
                         cudaStream_t st);
-int guide_train_counted(rt_guide* g, const float* rec, const uint32_t* n_dev, uint32_t cap, cudaStream_t st);
+// `steps` training iterations over the min(*total_dev, steps * cap) records
+// of `rec`, split into equal consecutive slices (at most cap records each).
+int guide_train_slices(rt_guide* g, const float* rec, const uint32_t* total_dev, uint32_t cap, uint32_t steps,
+                       cudaStream_t st);
+// Size the inference buffers for n records up front (no allocation mid-render).
+int guide_reserve(rt_guide* g, uint32_t n);
 const float* guide_loss_ptr(rt_guide* g);
 const uint32_t* guide_err_ptr(rt_guide* g);
 GuideDev guide_dev(rt_guide* g);

@@ -37,7 +37,7 @@ enum : uint32_t {
 };
 
 struct Paths {
-    float4* ray_o;    // origin xyz
+    float4* ray_o;    // origin xyz, w = roulette gain (see k_shade)
     float4* ray_d;    // direction xyz, w = tmax
     uint4* hit;       // t bits, tri (leaf order), inst (leaf order), b1|b2 half2
     float4* beta;     // throughput xyz, w = prev bsdf pdf
@@ -61,14 +61,18 @@ struct Paths {
     float* g_rec;          // inference records, 16 floats (position, normal, wo)
     uint32_t* g_idx;       // slot -> inference record (~0 when not guided)
     uint32_t* g_cnt;       // number of inference records this wave
-    const float* g_raw;    // network outputs, 48 floats per inference record
-    float* tr_rec;         // training vertices: [T][max_depth] x TR_FLOATS
+    const float* g_raw;    // decoded mixtures, 48 floats per inference record (guide.cuh)
+    float* tr_rec;         // training vertices: [P][max_depth] x TR_FLOATS
     float* tb_rec;         // training batch, 16 floats per record
-    uint32_t* tb_cnt;
-    uint32_t tr_stride, tr_phase, tr_T, tb_cap;
+    uint32_t* tb_cnt;      // [0] records kept, [1] candidate records
+    float* tr_keep;        // probability of keeping a candidate (device word)
+    uint32_t tr_tag, tb_cap;
 };
 
-// Training vertex: p(3) n(3) wo(3) wi(3) beta(3) L at the next vertex(3), sampled flag, L-set flag.
+// Training vertex: p(3) n(3) wo(3) wi(3) beta(3) L at the next vertex(3),
+// then the slab tag of its opening and of its closing (as uint bits). A
+// record belongs to the current slab when both tags equal Paths::tr_tag,
+// so stale records of earlier slabs never need clearing.
 #define TR_FLOATS 20
 
 struct PtConsts {
@@ -193,7 +197,7 @@ __global__ void k_raygen(DevScene S, Paths P, PtConsts C) {
     } else {
         d = normalize_ref(dir);
     }
-    P.ray_o[i] = make_float4(o.x, o.y, o.z, 0.0f);
+    P.ray_o[i] = make_float4(o.x, o.y, o.z, 1.0f);
     P.ray_d[i] = make_float4(d.x, d.y, d.z, INFINITY);
     P.beta[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     P.L[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -207,17 +211,14 @@ __global__ void k_raygen(DevScene S, Paths P, PtConsts C) {
     }
     P.q_ext[0][i] = i;
     if (i == 0) P.cnt[CNT_EXT_IN] = P.P;
-    if (C.guided && i % P.tr_stride == P.tr_phase && i / P.tr_stride < P.tr_T) {
-        float* r = P.tr_rec + (size_t)(i / P.tr_stride) * C.max_depth * TR_FLOATS;
-        for (uint32_t d = 0; d < C.max_depth; d++) r[d * TR_FLOATS + 18] = r[d * TR_FLOATS + 19] = 0.0f;
-    }
 }
 
 // ---- learned proposal: network inputs for this wave's guided vertices ------------------
-// Vertices of diffuse, conductor and mixed materials get a record (position,
-// shading normal facing wo, wo); the shade kernel reads the network output
-// through g_idx. Glass, emitters and misses keep plain BSDF sampling.
-__global__ void __launch_bounds__(128) k_guide_gather(DevScene S, Paths P) {
+// Vertices of diffuse, conductor and mixed materials (below guide_depth when
+// it is set) get a record (position, shading normal facing wo, wo); the shade
+// kernel reads the network output through g_idx. Glass, emitters, misses and
+// deeper vertices keep plain BSDF sampling.
+__global__ void __launch_bounds__(128) k_guide_gather(DevScene S, Paths P, uint32_t guide_depth) {
     uint32_t counts[N_QUEUES];
     uint32_t total = 0;
 #pragma unroll
@@ -245,6 +246,7 @@ __global__ void __launch_bounds__(128) k_guide_gather(DevScene S, Paths P) {
             }
             slot = P.q_cls[(size_t)c * P.P + off];
             want = c == MAT_DIFFUSE || c == MAT_CONDUCTOR || c == MAT_MIXED;
+            if (want && guide_depth) want = (__float_as_uint(P.prev[slot].w) >> FL_DEPTH_SHIFT) < guide_depth;
             if (want) {
                 HitGeo hg;
                 hit_geometry(S, xyz(P.ray_o[slot]), xyz(P.ray_d[slot]), P.hit[slot], hg);
@@ -277,34 +279,58 @@ __global__ void __launch_bounds__(128) k_guide_gather(DevScene S, Paths P) {
 // ---- learned proposal: training batch from the slab's closed vertices -------------------
 // weight = lum(L_end - L_vertex) / lum(beta_vertex) estimates
 // lum(f cos Li) / pdf for the direction the path actually took (capped at 50).
+// Every path of the slab recorded its vertices; a candidate (a closed record
+// of positive weight) is kept with probability *tr_keep, decided by a hash of
+// (slot, depth, slab tag), so the batch is a spatially uniform subsample.
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+    // integer finaliser ("lowbias32", C. Wellons, hash-prospector)
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
+}
+
 __global__ void k_guide_collect(Paths P, PtConsts C) {
-    uint32_t id = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t t = id / C.max_depth, d = id % C.max_depth;
-    bool ok = false;
-    float w = 0.f;
-    const float* r = nullptr;
-    if (t < P.tr_T) {
-        uint32_t slot = t * P.tr_stride + P.tr_phase;
-        r = P.tr_rec + ((size_t)t * C.max_depth + d) * TR_FLOATS;
-        if (slot < P.P && r[18] != 0.0f && r[19] != 0.0f) {
-            float4 Le = P.L[slot];
+    // One thread per (slot, depth): the records of a path are consecutive, so
+    // the threads of a warp read neighbouring records of a few paths.
+    const float keep = *P.tr_keep;
+    const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t slot = (uint32_t)(id / C.max_depth), d = (uint32_t)(id % C.max_depth);
+    bool cand = false;
+    if (slot < P.P) {
+        const float* r = P.tr_rec + ((size_t)slot * C.max_depth + d) * TR_FLOATS;
+        float2 tags = *reinterpret_cast<const float2*>(r + 18);
+        if (__float_as_uint(tags.x) == P.tr_tag && __float_as_uint(tags.y) == P.tr_tag) {
+            const float4 Le = P.L[slot];
             float3 dl = f3(Le.x - r[15], Le.y - r[16], Le.z - r[17]);
-            w = luminance(dl) / fmaxf(luminance(f3(r[12], r[13], r[14])), 1e-8f);
-            ok = w > 0.0f && isfinite(w);
+            float w = luminance(dl) / fmaxf(luminance(f3(r[12], r[13], r[14])), 1e-8f);
+            cand = w > 0.0f && isfinite(w);
+            uint32_t h = hash32((slot * C.max_depth + d) ^ hash32(P.tr_tag));
+            if (cand && (float)(h >> 8) * (1.0f / 16777216.0f) < keep) {
+                uint32_t idx = atomicAdd(P.tb_cnt, 1u);
+                if (idx < P.tb_cap) {
+                    float4* o = reinterpret_cast<float4*>(P.tb_rec + (size_t)idx * 16);
+                    const float4* ri = reinterpret_cast<const float4*>(r);
+                    o[0] = ri[0];
+                    o[1] = ri[1];
+                    o[2] = ri[2];
+                    o[3] = make_float4(fminf(w, 50.0f), 0.0f, 0.0f, 0.0f);
+                }
+            }
         }
     }
-    uint32_t m = __ballot_sync(0xFFFFFFFFu, ok);
-    if (!m) return;
-    uint32_t leader = __ffs(m) - 1, base = 0;
-    if (lane_id() == leader) base = atomicAdd(P.tb_cnt, __popc(m));
-    base = __shfl_sync(0xFFFFFFFFu, base, leader);
-    if (!ok) return;
-    uint32_t idx = base + __popc(m & ((1u << lane_id()) - 1u));
-    if (idx >= P.tb_cap) return;
-    float* o = P.tb_rec + (size_t)idx * 16;
-    for (int k = 0; k < 12; k++) o[k] = r[k];
-    o[12] = fminf(w, 50.0f);
-    o[13] = o[14] = o[15] = 0.0f;
+    uint32_t m = __ballot_sync(0xFFFFFFFFu, cand);
+    if (lane_id() == 0 && m) atomicAdd(P.tb_cnt + 1, (uint32_t)__popc(m));
+}
+
+// Keep probability for this slab's collection: aim the expected batch at 95%
+// of the training capacity, given the previous slab's number of candidates
+// (scaled by the ratio of the slabs' sample passes).
+__global__ void k_guide_keep(const uint32_t* tb_cnt, float scale, uint32_t cap, float* keep) {
+    float cand = (float)tb_cnt[1] * scale;
+    *keep = cand > 0.0f ? fminf(1.0f, 0.95f * (float)cap / cand) : 1.0f;
 }
 
 // ---- persistent ray pump ----------------------------------------------------------------
@@ -610,15 +636,15 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
             // Training: close the previous vertex's record with the radiance
             // gathered so far (its own emission and NEE included).
             auto tr_close = [&]() {
-                if (!C.guided || slot % P.tr_stride != P.tr_phase) return;
-                uint32_t d0 = flags >> FL_DEPTH_SHIFT, t = slot / P.tr_stride;
-                if (d0 == 0 || t >= P.tr_T) return;
-                float* r = P.tr_rec + ((size_t)t * C.max_depth + (d0 - 1)) * TR_FLOATS;
-                if (r[18] != 0.0f && r[19] == 0.0f) {
+                if (!C.guided) return;
+                uint32_t d0 = flags >> FL_DEPTH_SHIFT;
+                if (d0 == 0 || d0 > C.max_depth) return;
+                float* r = P.tr_rec + ((size_t)slot * C.max_depth + (d0 - 1)) * TR_FLOATS;
+                if (__float_as_uint(r[18]) == P.tr_tag && __float_as_uint(r[19]) != P.tr_tag) {
                     r[15] = Lr.x;
                     r[16] = Lr.y;
                     r[17] = Lr.z;
-                    r[19] = 1.0f;
+                    r[19] = __uint_as_float(P.tr_tag);
                 }
             };
             if (hr.y == 0xFFFFFFFFu) {
@@ -647,7 +673,7 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
                     flags = (flags & ~FL_SKIP_MASK) | ((skips + 1) << FL_SKIP_SHIFT);
                     travel += eucl;
                     float3 no = p + normalize_ref(d) * RT_RAY_OFFSET;
-                    P.ray_o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
+                    P.ray_o[slot] = make_float4(no.x, no.y, no.z, o4.w);
                     P.ray_d[slot] = make_float4(d.x, d.y, d.z, INFINITY);
                     extend = true;
                     done = true;
@@ -675,7 +701,7 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
                     if (C.guided) {
                         uint32_t gi = P.g_idx[slot];
                         if (gi != 0xFFFFFFFFu) {
-                            mixture_decode(P.g_raw + (size_t)gi * G_OUT, mix);
+                            mixture_load(P.g_raw + (size_t)gi * G_OUT, mix);
                             guided = true;
                         }
                     }
@@ -720,22 +746,33 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
                         sampled = bsdf_sample(m, wo_l, eta, rng, bs);
                         pdf_path = bs.pdf;
                     }
+                    // Roulette gain: Russian roulette acts on the throughput the
+                    // path would carry had every bounce been BSDF-sampled,
+                    // beta * prod(pdf_path / p_bsdf). Guiding concentrates paths
+                    // on directions of high incident radiance and gives them a
+                    // low beta for it; roulette on beta alone would kill those
+                    // paths at the next bounce and cancel the gain. Without
+                    // guiding the gain stays exactly 1 (the reference's rule,
+                    // pt/mod.rs:980-987).
+                    float rr_gain = o4.w;
+                    if (guided && sampled)
+                        rr_gain = fminf(fmaxf(rr_gain * (pdf_path / fmaxf(bs.pdf, 1e-20f)), 1e-20f), 1e20f);
                     if (sampled) {
                         float3 wi = fr.to_world(bs.wi);
                         const float3 beta_in = beta;
                         beta = beta * bs.f * (fabsf(bs.wi.z) / pdf_path);
-                        if (C.guided && slot % P.tr_stride == P.tr_phase) {
+                        if (C.guided) {
                             // Training vertex: closed with the radiance at the next vertex.
-                            uint32_t t = slot / P.tr_stride, d0 = flags >> FL_DEPTH_SHIFT;
-                            if (t < P.tr_T && d0 < C.max_depth) {
-                                float* r = P.tr_rec + ((size_t)t * C.max_depth + d0) * TR_FLOATS;
+                            uint32_t d0 = flags >> FL_DEPTH_SHIFT;
+                            if (d0 < C.max_depth) {
+                                float* r = P.tr_rec + ((size_t)slot * C.max_depth + d0) * TR_FLOATS;
                                 float3 wn = normalize_ref(wi);
                                 r[0] = p.x; r[1] = p.y; r[2] = p.z;
                                 r[3] = n.x; r[4] = n.y; r[5] = n.z;
                                 r[6] = wo.x; r[7] = wo.y; r[8] = wo.z;
                                 r[9] = wn.x; r[10] = wn.y; r[11] = wn.z;
                                 r[12] = beta_in.x; r[13] = beta_in.y; r[14] = beta_in.z;
-                                r[18] = 1.0f;
+                                r[18] = __uint_as_float(P.tr_tag);
                                 r[19] = 0.0f;
                             }
                         }
@@ -751,12 +788,12 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
                         flags = (flags & 0xFFFFu) | (depth << FL_DEPTH_SHIFT);
                         bool alive = true;
                         if (depth >= C.rr_start) {
-                            float q = fminf(maxc(beta), 0.95f);
+                            float q = fminf(maxc(beta) * rr_gain, 0.95f);
                             if (q <= 0.0f || rng.next_f() > q) alive = false;
                             else beta = beta / q;
                         }
                         if (alive && depth < C.max_depth) {
-                            P.ray_o[slot] = make_float4(no.x, no.y, no.z, 0.0f);
+                            P.ray_o[slot] = make_float4(no.x, no.y, no.z, rr_gain);
                             P.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, INFINITY);
                             extend = true;
                         }

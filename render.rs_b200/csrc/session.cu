@@ -64,6 +64,8 @@ struct rt_session {
     uint32_t samples_done = 0;
     // learned proposal (params.guided)
     rt_guide* guide = nullptr;
+    uint64_t guide_slabs = 0;    // slabs rendered with the guide (drives the slab growth)
+    uint32_t guide_prev_k = 0;   // sample passes of the previous guided slab
     uint64_t guide_records = 0;
     double guide_loss = 0.0;
     // ray-batch staging for host-pointer calls
@@ -179,10 +181,12 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     }
     // Path state: slabs of whole sample passes (see pt_kernels.cuh).
     s->npix = scene->camera.width * scene->camera.height;
-    // Guided renders train between slabs, so they default to one sample pass
-    // per slab (one network update per sample per pixel).
+    // Guided renders train between slabs: their slabs grow 1, 2, 4, ... sample
+    // passes up to about 4M paths (16 passes at most), with guide_steps
+    // network updates per sample pass.
     const bool guided = params->guided != 0;
-    uint64_t cap = params->max_paths ? params->max_paths : guided ? (uint64_t)s->npix : (8ull << 20);
+    uint64_t guided_k = std::max<uint64_t>(1, std::min<uint64_t>(16, (4ull << 20) / s->npix));
+    uint64_t cap = params->max_paths ? params->max_paths : guided ? guided_k * s->npix : (8ull << 20);
     uint64_t k = std::max<uint64_t>(1, cap / s->npix);
     if (k * s->npix > 0xFFFFFFFFull / 8) k = std::max<uint64_t>(1, (0xFFFFFFFFull / 8) / s->npix);
     s->slab_samples = (uint32_t)k;
@@ -213,19 +217,30 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     rc = rc ? rc : s->alloc(&s->fetch, 1);
     rc = rc ? rc : s->alloc(&s->accum, 4ull * s->npix);
     rc = rc ? rc : s->alloc(&s->aux, aov ? 12ull * s->npix : 1);
-    // Guiding: inference records per slot, training vertices for a strided
-    // subset of ~16k paths per slab, and a 2^16-record training batch.
-    const uint32_t tr_paths = 16384;
-    Pp.tr_stride = guided ? (uint32_t)std::max<uint64_t>(1, P / tr_paths) : 1u;
-    Pp.tr_T = guided ? (uint32_t)((P + Pp.tr_stride - 1) / Pp.tr_stride) : 0u;
-    Pp.tr_phase = 0;
-    Pp.tb_cap = guided ? (1u << 16) : 0u;
+    // Guiding: inference records per slot, training vertices of every path
+    // of the slab, and the slab's training batches (2^16 records per Adam
+    // step) subsampled from them.
+    const uint32_t steps_per_pass = std::max(1u, std::min(16u, params->guide_steps));
+    Pp.tr_tag = 0;
+    Pp.tb_cap = guided ? (1u << 16) * (uint32_t)k * steps_per_pass : 0u;
+    const size_t tr_floats = guided ? P * params->max_depth * TR_FLOATS : 1;
+    float* keep = nullptr;
     rc = rc ? rc : s->alloc(&Pp.g_rec, guided ? P * 16 : 1);
     rc = rc ? rc : s->alloc(&Pp.g_idx, guided ? P : 1);
     rc = rc ? rc : s->alloc(&Pp.g_cnt, 1);
-    rc = rc ? rc : s->alloc(&Pp.tr_rec, guided ? (size_t)Pp.tr_T * params->max_depth * TR_FLOATS : 1);
+    rc = rc ? rc : s->alloc(&Pp.tr_rec, tr_floats);
     rc = rc ? rc : s->alloc(&Pp.tb_rec, guided ? (size_t)Pp.tb_cap * 16 : 1);
-    rc = rc ? rc : s->alloc(&Pp.tb_cnt, 1);
+    rc = rc ? rc : s->alloc(&Pp.tb_cnt, 4);
+    rc = rc ? rc : s->alloc(&keep, 1);
+    if (!rc) {
+        const float one = 1.0f;
+        Pp.tr_keep = keep;
+        if (cudaMemsetAsync(Pp.tr_rec, 0, tr_floats * 4, s->stream) != cudaSuccess ||
+            cudaMemsetAsync(Pp.tb_cnt, 0, 16, s->stream) != cudaSuccess ||
+            cudaMemcpyAsync(keep, &one, 4, cudaMemcpyHostToDevice, s->stream) != cudaSuccess ||
+            cudaStreamSynchronize(s->stream) != cudaSuccess)
+            rc = fail(RT_ERR_CUDA, "guide buffers: initialisation failed");
+    }
     if (!rc && guided) {
         float lo[3], hi[3];
         for (int a = 0; a < 3; a++) {
@@ -233,7 +248,9 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
             lo[a] = (float)(s->host.world_lo[a] - pad);
             hi[a] = (float)(s->host.world_hi[a] + pad);
         }
-        if (rt_guide_create(lo, hi, 0x5eed, 1e-2f, &s->guide) != 0) rc = fail(RT_ERR_CUDA, rt_guide_last_error());
+        const float lr = params->guide_lr > 0.0 ? (float)params->guide_lr : 1e-2f;
+        if (rt_guide_create(lo, hi, 0x5eed, lr, &s->guide) != 0 || guide_reserve(s->guide, (uint32_t)P) != 0)
+            rc = fail(RT_ERR_CUDA, rt_guide_last_error());
     }
     if (rc) {
         delete s;
@@ -290,25 +307,37 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     int guide_trainings = 0;
     uint32_t waves = s->params.max_depth + (s->S.any_presence ? RT_MAX_PRESENCE_SKIPS : 0u);
     const int trav_grid = s->trav_grid, shade_grid = s->sm_count * 8;
+    const uint32_t batch = 1u << 16;  // training records per Adam step
     CUDA_TRY(cudaMemsetAsync(s->stats, 0, 32, st));
     float ms_ext = 0, ms_sh = 0, ms_shade = 0;
     uint64_t launches = 0;
+    uint32_t last_records_slab = 0;
     // Per-wave timing events are recorded without host waits and read once
     // at the end, so the waves of a slab run back to back.
-    size_t nslabs = (count + s->slab_samples - 1) / s->slab_samples;
-    size_t need = 2 + nslabs * waves * 4;
-    while (s->evpool.size() < need) {
-        cudaEvent_t e;
-        CUDA_TRY(cudaEventCreate(&e));
-        s->evpool.push_back(e);
-    }
+    auto events = [&](size_t need) -> int {
+        while (s->evpool.size() < need) {
+            cudaEvent_t e;
+            CUDA_TRY(cudaEventCreate(&e));
+            s->evpool.push_back(e);
+        }
+        return RT_OK;
+    };
+    int erc = events(2);
+    if (erc) return erc;
     size_t ei = 2;
     CUDA_TRY(cudaEventRecord(s->evpool[0], st));
     for (uint32_t done = 0; done < count;) {
         uint32_t k = std::min(s->slab_samples, count - done);
+        if (s->guide) {
+            // Slabs grow while the network is young, so it is updated often early on.
+            k = std::min(k, 1u << std::min<uint64_t>(s->guide_slabs, 31));
+        }
+        erc = events(ei + 4 * (size_t)waves);
+        if (erc) return erc;
         uint32_t slab_paths = k * s->npix;
         P.P = slab_paths;
         C.sample0 = (uint64_t)sample_start + done;
+        if (s->guide) P.tr_tag++;  // new tag: the training records of this slab
         CUDA_TRY(cudaMemsetAsync(P.cnt, 0, CNT_WORDS * 4, st));
         k_raygen<<<(slab_paths + 255) / 256, 256, 0, st>>>(s->S, P, C);
         launches++;
@@ -320,7 +349,7 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
             if (s->guide) {
                 // Network inputs for this wave's guided vertices, then inference.
                 CUDA_TRY(cudaMemsetAsync(P.g_cnt, 0, 4, st));
-                k_guide_gather<<<shade_grid, 128, 0, st>>>(s->S, P);
+                k_guide_gather<<<shade_grid, 128, 0, st>>>(s->S, P, s->params.guide_depth);
                 float* raw = nullptr;
                 int grc = guide_infer_counted(s->guide, P.g_rec, P.g_cnt, P.P, &raw, st);
                 if (grc) return fail(grc, rt_guide_last_error());
@@ -338,16 +367,25 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
         k_accumulate<<<(s->npix + 255) / 256, 256, 0, st>>>(P, C, k, s->accum, s->aux);
         launches++;
         if (s->guide) {
-            // One Adam step on the vertices this slab closed, then a new
-            // training subset for the next slab.
-            CUDA_TRY(cudaMemsetAsync(P.tb_cnt, 0, 4, st));
-            uint32_t nthreads = P.tr_T * C.max_depth;
-            k_guide_collect<<<(nthreads + 127) / 128, 128, 0, st>>>(P, C);
-            int grc = guide_train_counted(s->guide, P.tb_rec, P.tb_cnt, P.tb_cap, st);
+            // Adam steps (guide_steps per sample pass) on this slab's closed
+            // vertices: a subsample of about steps * 2^16 records (keep
+            // probability from the previous slab's candidate count), split
+            // into consecutive batches.
+            const uint32_t steps = k * std::max(1u, std::min(16u, s->params.guide_steps));
+            const float scale = s->guide_prev_k ? (float)k / (float)s->guide_prev_k : 1.0f;
+            k_guide_keep<<<1, 1, 0, st>>>(P.tb_cnt, scale, steps * batch, P.tr_keep);
+            CUDA_TRY(cudaMemsetAsync(P.tb_cnt, 0, 8, st));
+            Paths Pc = P;
+            Pc.tb_cap = steps * batch;
+            const uint64_t collect_threads = (uint64_t)P.P * C.max_depth;
+            k_guide_collect<<<(unsigned)((collect_threads + 255) / 256), 256, 0, st>>>(Pc, C);
+            int grc = guide_train_slices(s->guide, P.tb_rec, P.tb_cnt, batch, steps, st);
             if (grc) return fail(grc, rt_guide_last_error());
-            guide_trainings++;
-            launches += 7;
-            P.tr_phase = (P.tr_phase + 1) % P.tr_stride;
+            guide_trainings += (int)steps;
+            launches += 3 + 7 * (uint64_t)steps;
+            s->guide_prev_k = k;
+            s->guide_slabs++;
+            last_records_slab = steps * batch;
         }
         done += k;
     }
@@ -387,7 +425,7 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
         if (gerr) return fail(RT_ERR_DEVICE, "guide network: tensor-core pipeline wait timed out");
         CUDA_TRY(cudaMemcpy(&nrec, P.tb_cnt, 4, cudaMemcpyDeviceToHost));
         CUDA_TRY(cudaMemcpy(&loss, guide_loss_ptr(s->guide), 4, cudaMemcpyDeviceToHost));
-        s->last.guide_records = std::min(nrec, P.tb_cap);
+        s->last.guide_records = std::min(nrec, last_records_slab);
         s->last.guide_loss = loss;
     }
     s->samples_done += count;

@@ -105,6 +105,29 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// The same without the wait, so several loads share one tcgen05.wait::ld.
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t* r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Barrier over the 128 threads of tile group `grp` (named barrier 1 + grp;
+// immediate ids, so the kernel reserves only the barriers it uses).
+__device__ __forceinline__ void group_sync(uint32_t grp) {
+    if (grp == 0)
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+    else if (grp == 1)
+        asm volatile("bar.sync 2, 128;" ::: "memory");
+    else if (grp == 2)
+        asm volatile("bar.sync 3, 128;" ::: "memory");
+    else
+        asm volatile("bar.sync 4, 128;" ::: "memory");
+}
+
 // Issue D = A * B^T for a 128-row tile (thread 0 of the CTA issues).
 // a_saddr / b_saddr: shared addresses of the operands in the core layout.
 __device__ __forceinline__ void tc_gemm_issue(uint32_t d_tmem, uint32_t a_saddr, uint32_t b_saddr, int N, int K,

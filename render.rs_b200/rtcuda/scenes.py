@@ -253,11 +253,17 @@ INSTANCED_MATERIALS = dict(spp=64, max_depth=12, rr_start=3)
 def two_rooms(width=1280, height=720):
     """Two 4 x 3 x 3 rooms (x in [0,4] and [4,8], y up, z in [0,3]) joined by a
     partition at x = 4 with one 0.2 (z) x 2.0 (y) opening at z in [1.4, 1.6].
-    A single 1 x 1 area light of radiance 50 hangs on the partition's far side
-    (x = 4.01, facing +x, z in [1.8, 2.8], y in [1.6, 2.6]) so nothing in the
-    camera's room sees it directly. Walls and ceiling: Oren-Nayar albedo 0.7,
-    sigma 0.3; floor: GGX-coated diffuse, roughness 0.3. The camera sits in the
-    first room looking at the partition."""
+    A single 1 x 1 area light of radiance 50 hangs horizontally 0.4 below the
+    second room's ceiling (y = 2.6, x in [6, 7], z in [1, 2]); the camera
+    cannot see it, and of the first room only a small patch of its back wall
+    sees it through the opening, so nearly all light in the camera's room is
+    indirect. The panel emits from both faces (rect lights are double-sided),
+    so it is kept well away from every surface: a panel a centimetre from a
+    wall lights a thin band of that wall with near-singular NEE weights,
+    whose fireflies would swamp any comparison of estimators. Walls and
+    ceiling: Oren-Nayar albedo 0.7, sigma 0.3; floor: GGX-coated diffuse,
+    roughness 0.3. The camera sits in the first room looking at the
+    partition."""
     s = Scene(width, height, fov=60.0)
     s.look_at((0.35, 1.4, 1.2), (4.0, 1.1, 1.5))
     wall = s.add_material(matte((0.7, 0.7, 0.7), sigma=0.3, id=1))
@@ -275,8 +281,8 @@ def two_rooms(width=1280, height=720):
     ])
     s.add_instance(s.add_mesh(*walls), wall)
     s.add_instance(s.add_mesh(*quad((0, 0, 0), (0, 0, 3), (8, 0, 0))), floor)
-    # Light on the far side of the partition, facing +x (normal = e1 x e2).
-    s.add_emissive_quad((4.01, 1.6, 2.8), (0, 1, 0), (0, 0, -1), (50.0, 50.0, 50.0))
+    # Light panel hanging in the second room, facing down (normal = e1 x e2).
+    s.add_emissive_quad((6.0, 2.6, 1.0), (1, 0, 0), (0, 0, 1), (50.0, 50.0, 50.0))
     s.materials[-1]["id"] = 3
     return s
 
