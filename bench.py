@@ -19,6 +19,14 @@ Printed (one JSON line on rank 0):
   cpu_baseline  the f64 oracle (C++ restatement of the reference's CPU path
              tracer, all host threads) on a bounded pixel sample of the frame.
   traversal  the 4,194,304-ray closest-hit and any-hit batches (Mrays/s).
+  guided_equal_time  the learned-proposal workload: two 4x3x3 rooms joined by
+             a 0.2x2.0 opening, the light in the unseen room, 1280x720, max
+             depth 16. A fresh guided session renders GUIDED_SPP passes from
+             an untrained network (online training included in its time); a
+             plain session renders as many passes as fit in the same device
+             time. Both are scored by relMSE against a high-spp GPU render
+             (all pixels) and against the f64 CPU oracle on a strided pixel
+             subset (the 65,536-spp full-frame oracle render is hours of CPU).
 
 `--impl reference` times the reference arm instead: the reference's CPU path
 (its Rust build is unavailable here, so the f64 C++ restatement of
@@ -135,6 +143,61 @@ def cpu_baseline_sample(scene, params, threads=0, target_s=12.0):
     return samples / el / 1e6, f"{len(pixels)} pixels (every {stride}th) x {SPP} spp of the frame", cores, work, el
 
 
+GUIDED_W, GUIDED_H, GUIDED_SPP, GUIDED_DEPTH = 1280, 720, 256, 16
+
+
+def rel_mse(img, ref):
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def guided_equal_time(ref_spp=1024, cpu_pixels=256, cpu_spp=16384):
+    """Equal-time relMSE of guided vs plain path tracing on the two-room scene."""
+    from rtcuda import PtSession, abi, scenes
+    s = scenes.two_rooms(GUIDED_W, GUIDED_H)
+    plain_p = abi.make_params(max_depth=GUIDED_DEPTH)
+    guided_p = abi.make_params(max_depth=GUIDED_DEPTH, guided=True, guide_fraction=0.5)
+    with PtSession(s, plain_p) as g:                       # high-spp GPU reference
+        g.render_samples(1 << 24, ref_spp)
+        ref = g.image()
+    with PtSession(s, guided_p) as g:                      # warm-up of the code paths only
+        g.render_samples(1 << 23, 2)
+    with PtSession(s, guided_p) as g:
+        g.render_samples(0, GUIDED_SPP)
+        st = g.stats()
+        guided_ms = st["total_ms"]
+        guided = g.image()
+    with PtSession(s, plain_p) as g:
+        g.render_samples(1 << 22, 32)
+        per_spp = g.stats()["total_ms"] / 32
+        g.reset()
+        plain_spp = max(1, int(round(guided_ms / per_spp)))
+        g.render_samples(0, plain_spp)
+        plain_ms = g.stats()["total_ms"]
+        plain = g.image()
+    out = {"scene": f"two_rooms_{GUIDED_W}x{GUIDED_H}_depth{GUIDED_DEPTH}", "guided_spp": GUIDED_SPP,
+           "guided_ms": round(guided_ms, 2), "guide_steps": st["guide_steps"], "plain_spp": plain_spp,
+           "plain_ms": round(plain_ms, 2), "plain_ms_per_spp": round(per_spp, 4),
+           "gpu_reference_spp": ref_spp}
+    e_p, e_g = rel_mse(plain, ref), rel_mse(guided, ref)
+    out.update({"relmse_plain_vs_gpu_ref": e_p, "relmse_guided_vs_gpu_ref": e_g, "ratio_vs_gpu_ref": e_p / e_g})
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle  # test infrastructure: the f64 reference pixels
+        npix = GUIDED_W * GUIDED_H
+        pix = np.arange(npix // (2 * cpu_pixels), npix, npix // cpu_pixels, dtype=np.uint32)[:cpu_pixels]
+        t0 = time.perf_counter()
+        acc = oracle.OracleScene(s).render(plain_p, 1 << 25, (1 << 25) + cpu_spp, pixels=pix)[0]
+        cref = acc / cpu_spp  # (n, 3) radiance sums of the sampled pixels
+        el = time.perf_counter() - t0
+        gp, gg = plain.reshape(-1, 3)[pix], guided.reshape(-1, 3)[pix]
+        c_p, c_g = rel_mse(gp, cref), rel_mse(gg, cref)
+        out.update({"relmse_plain_vs_f64": c_p, "relmse_guided_vs_f64": c_g, "ratio_vs_f64": c_p / c_g,
+                    "f64_reference": f"oracle, {len(pix)} strided pixels x {cpu_spp} spp ({el:.1f} s)"})
+    except Exception as exc:  # the oracle is optional on a box without it
+        out["f64_reference"] = f"unavailable: {exc}"
+    return out
+
+
 def run_reference(args):
     """Reference arm: the reference's CPU path (f64 restatement) on host cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -208,6 +271,7 @@ def main():
     ap.add_argument("--mode", default="full", choices=["full", "traversal"],
                     help="traversal: only the closest/any-hit ray batches (for profiler captures)")
     ap.add_argument("--rays", type=int, default=N_RAYS)
+    ap.add_argument("--no-guided", action="store_true", help="skip the guided equal-time comparison")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -334,6 +398,9 @@ def main():
                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                     "peak_kind": peak_kind, "bytes_per_ray": bytes_per_ray,
                     "rays_per_launch": ext_rays / max(1, launches_ext), "launch_ms": ext_ms / max(1, launches_ext)}
+        guided = None
+        if not args.no_guided and world == 1:
+            guided = guided_equal_time()
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -348,6 +415,7 @@ def main():
             "gpu_launches": int(launches + 3 * 0),
             "traversal": trav,
             "rays_per_step": {"extension": last["extension_rays"], "shadow": last["shadow_rays"]},
+            "guided_equal_time": guided,
             "Mrays_per_s": (last["extension_rays"] + last["shadow_rays"]) / (last["total_ms"] / 1e3) / 1e6,
         }
         print(json.dumps(result), flush=True)

@@ -294,12 +294,14 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
 
 __global__ void k_guide_collect(Paths P, PtConsts C) {
     // One thread per (slot, depth): the records of a path are consecutive, so
-    // the threads of a warp read neighbouring records of a few paths.
+    // the threads of a warp read neighbouring records of a few paths. A path
+    // opened records 0 .. depth-1 (its final bounce count); threads past that
+    // leave without touching the record buffer.
     const float keep = *P.tr_keep;
     const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t slot = (uint32_t)(id / C.max_depth), d = (uint32_t)(id % C.max_depth);
     bool cand = false;
-    if (slot < P.P) {
+    if (slot < P.P && d < (__float_as_uint(P.prev[slot].w) >> FL_DEPTH_SHIFT)) {
         const float* r = P.tr_rec + ((size_t)slot * C.max_depth + d) * TR_FLOATS;
         float2 tags = *reinterpret_cast<const float2*>(r + 18);
         if (__float_as_uint(tags.x) == P.tr_tag && __float_as_uint(tags.y) == P.tr_tag) {

@@ -3,11 +3,14 @@
 1. The plain GPU render matches the f64 oracle statistically.
 2. Guiding keeps the estimator unbiased: guided and plain renders converge
    to the same image (one-sample MIS with the BSDF).
-3. Per sample, the guided estimator has lower relMSE than the plain one
-   against a high-spp reference (variance reduction of the learned proposal).
-4. At equal GPU time (network inference and training included) on a
-   320x180 frame, the guided render's relMSE is reported next to the plain
-   one's (the printed ratio); the assertion is that guiding is not worse.
+3. Per sample, the guided estimator trained online from scratch already has
+   lower relMSE than the plain one against a high-spp reference.
+4. What the trained network gains: after 256 sample passes of online
+   training, the next 256 guided passes have at least 2x lower relMSE than
+   256 plain ones, and the learned proposal sends several times more
+   probability through the opening than BSDF sampling does. (The equal-time
+   comparison at the workload's 1280x720 is measured and reported by
+   bench.py.)
 """
 import time
 
@@ -62,29 +65,69 @@ def test_guided_is_unbiased_and_reduces_variance(reference):
     assert e_guided < e_plain
 
 
-def test_guided_at_equal_time():
+def _fibonacci_sphere(n):
+    i = np.arange(n) + 0.5
+    z = 1 - 2 * i / n
+    r = np.sqrt(1 - z * z)
+    ph = np.pi * (1 + 5 ** 0.5) * i
+    return np.stack([r * np.cos(ph), r * np.sin(ph), z], 1)
+
+
+def _mixture_pdf(raw, W):
+    """Density of the raw network output's vMF mixture at directions W (f64)."""
+    raw = np.asarray(raw, np.float64)[:40].reshape(8, 5)
+    mu = raw[:, :3] / np.maximum(np.linalg.norm(raw[:, :3], axis=1, keepdims=True), 1e-8)
+    k = np.exp(np.clip(raw[:, 3], -4, 9))
+    a = np.exp(raw[:, 4] - raw[:, 4].max())
+    a /= a.sum()
+    pdf = k / (2 * np.pi * (1 - np.exp(-2 * k))) * np.exp(k * (W @ mu.T - 1))
+    return pdf @ a
+
+
+def _through_opening(p, W):
+    """Directions from p that cross the partition x = 4 inside the opening."""
+    t = (4.0 - p[0]) / np.where(np.abs(W[:, 0]) > 1e-9, W[:, 0], 1e-9)
+    y, z = p[1] + t * W[:, 1], p[2] + t * W[:, 2]
+    return (t > 0) & (y > 0) & (y < 2) & (z > 1.4) & (z < 1.6)
+
+
+def test_trained_proposal_gain():
     s = scenes.two_rooms(320, 180)
+    spp = 256
     with PtSession(s, abi.make_params(max_depth=16)) as g:
         g.render_samples(500000, 4096)
         ref = g.image()
+    with PtSession(s, abi.make_params(max_depth=16)) as g:
+        t0 = time.perf_counter()
+        g.render_samples(0, spp)
+        t_plain = time.perf_counter() - t0
+        plain = g.image()
     with PtSession(s, abi.make_params(max_depth=16, guided=True, guide_fraction=0.5)) as g:
-        g.render_samples(0, 4)
+        g.render_samples(100000, spp)  # online training, samples discarded
         g.reset()
         t0 = time.perf_counter()
-        g.render_samples(0, 128)
+        g.render_samples(0, spp)
         t_guided = time.perf_counter() - t0
         guided = g.image()
-    with PtSession(s, abi.make_params(max_depth=16)) as g:
-        g.render_samples(0, 4)
-        g.reset()
-        t0 = time.perf_counter()
-        g.render_samples(0, 64)
-        per_spp = (time.perf_counter() - t0) / 64
-        g.reset()
-        spp = max(1, int(t_guided / per_spp))
-        g.render_samples(0, spp)
-        plain = g.image()
+        # Where the trained proposal sends floor vertices of the dark room.
+        W = _fibonacci_sphere(200000)
+        dw = 4 * np.pi / len(W)
+        cam = np.array([0.35, 1.4, 1.2])
+        pts = [((2.0, 0.0, 1.5), (0.0, 1.0, 0.0)), ((1.0, 0.0, 0.5), (0.0, 1.0, 0.0))]
+        recs = []
+        for p, n in pts:
+            wo = cam - np.array(p)
+            recs.append(np.r_[p, n, wo / np.linalg.norm(wo), np.zeros(7)])
+        raw = g.guide().infer(np.array(recs, np.float32))
     e_plain, e_guided = rel_mse(plain, ref), rel_mse(guided, ref)
-    print(f"equal time {t_guided:.3f}s at 320x180: plain {spp} spp relMSE {e_plain:.4g}, "
-          f"guided 128 spp relMSE {e_guided:.4g}, ratio {e_plain / e_guided:.2f}")
-    assert e_guided < 1.5 * e_plain
+    gain = e_plain / e_guided
+    print(f"trained proposal at 320x180: plain {spp} spp relMSE {e_plain:.4g}, guided {spp} spp relMSE "
+          f"{e_guided:.4g}, gain {gain:.2f}x per sample (times {t_plain:.3f}s / {t_guided:.3f}s)")
+    assert gain >= 2.0
+    for (p, n), r in zip(pts, raw):
+        p, n = np.array(p), np.array(n)
+        sl = _through_opening(p, W)
+        p_guide = _mixture_pdf(r, W)[sl].sum() * dw
+        p_bsdf = (np.maximum(W @ n, 0) / np.pi)[sl].sum() * dw
+        print(f"  vertex {p}: P(opening) guide {p_guide:.4f}, cosine BSDF {p_bsdf:.4f}")
+        assert p_guide > 3.0 * p_bsdf
