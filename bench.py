@@ -150,7 +150,7 @@ def rel_mse(img, ref):
     return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
 
 
-def guided_equal_time(ref_spp=1024, cpu_pixels=256, cpu_spp=16384):
+def guided_equal_time(ref_spp=4096, cpu_pixels=256, cpu_spp=16384):
     """Equal-time relMSE of guided vs plain path tracing on the two-room scene."""
     from rtcuda import PtSession, abi, scenes
     s = scenes.two_rooms(GUIDED_W, GUIDED_H)
@@ -260,6 +260,26 @@ def run_traversal(args):
     return 0
 
 
+def run_guided(args):
+    """The learned-proposal workload alone (for profiler captures): a fresh
+    guided session on the 1280x720 two-room scene renders `args.steps` sample
+    passes (slabs grow 1, 2, 4 passes), after `args.warmup` passes in a
+    throwaway session; one JSON line with device times from the session."""
+    from rtcuda import PtSession, abi, scenes
+    s = scenes.two_rooms(GUIDED_W, GUIDED_H)
+    p = abi.make_params(max_depth=GUIDED_DEPTH, guided=True, guide_fraction=0.5)
+    if args.warmup:
+        with PtSession(s, p) as g:
+            g.render_samples(1 << 23, args.warmup)
+    with PtSession(s, p) as g:
+        g.render_samples(0, args.steps)
+        st = g.stats()
+    print(json.dumps({"mode": "guided", "scene": f"two_rooms_{GUIDED_W}x{GUIDED_H}_depth{GUIDED_DEPTH}",
+                      "spp": args.steps, "ms": st["total_ms"], "ms_per_spp": st["total_ms"] / max(args.steps, 1),
+                      "guide_steps": st["guide_steps"], "kernel_launches": st["kernel_launches"]}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -268,8 +288,9 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--mode", default="full", choices=["full", "traversal"],
-                    help="traversal: only the closest/any-hit ray batches (for profiler captures)")
+    ap.add_argument("--mode", default="full", choices=["full", "traversal", "guided"],
+                    help="traversal: only the closest/any-hit ray batches; guided: only the learned-proposal "
+                         "workload (both for profiler captures)")
     ap.add_argument("--rays", type=int, default=N_RAYS)
     ap.add_argument("--no-guided", action="store_true", help="skip the guided equal-time comparison")
     args = ap.parse_args()
@@ -277,6 +298,8 @@ def main():
         return run_reference(args)
     if args.mode == "traversal":
         return run_traversal(args)
+    if args.mode == "guided":
+        return run_guided(args)
 
     import torch
     import torch.distributed as dist
