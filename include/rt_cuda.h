@@ -160,6 +160,18 @@ int rt_bsdf_furnace(const rt_material_desc* material, const double* wo, double e
  * order work against it. */
 void* rt_session_stream(rt_session* s);
 
+/* Adaptive sampling (WfSession::set_adaptive, src/raytracer/metal/renderer.rs:
+ * 580-584; rule of kernel_wf.metal:173-183): with tol > 0, from sample 32 on
+ * a pixel with at least 16 samples receives no further samples once the 95%
+ * confidence interval of its luminance, 1.96 sqrt(var / n), is below
+ * tol * max(mean, 0.05). tol = 0 turns it off (the default). The weight
+ * channel of the accumulator counts the samples each pixel actually took. */
+int rt_set_adaptive(rt_session* s, double tol);
+
+/* Average samples per pixel actually taken (WfSession::average_spp,
+ * renderer.rs:586-591): the mean of the accumulator's weight channel. */
+int rt_average_spp(rt_session* s, double* out);
+
 /* The session's learned directional proposal (rt_guide.h) when it renders
  * guided, else NULL. The session owns the handle: callers may pass it to
  * rt_guide_infer / rt_guide_get_params to inspect what the network has

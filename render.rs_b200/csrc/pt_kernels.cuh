@@ -82,6 +82,10 @@ struct PtConsts {
     uint32_t guided;
     float alpha;       // one-sample MIS probability of sampling the guide
     GuideDev G;
+    // Adaptive sampling (tol > 0): per pixel (luminance sum, luminance^2 sum,
+    // samples counted), updated by k_accumulate, read by k_raygen.
+    float adaptive_tol;
+    double* lum_stats;
 };
 
 // flag bits in Paths::prev.w
@@ -93,6 +97,7 @@ struct PtConsts {
 #define FL_SPEC_TRUE (1u << FL_SPEC_SHIFT)
 #define FL_SPEC_MASK (3u << FL_SPEC_SHIFT)
 #define FL_AUX_SET (1u << 8)
+#define FL_INACTIVE (1u << 9)   // adaptive sampling: the pixel had converged, no path was spawned
 #define FL_DEPTH_SHIFT 16
 
 #define RT_RAY_OFFSET 1e-4f
@@ -168,11 +173,37 @@ __device__ __forceinline__ float filter_offset(uint32_t kind, float width, float
     return (u - 0.5f) * width;
 }
 
+// Adaptive sampling, as the reference's wavefront raygen
+// (kernel_wf.metal:173-183): from sample 32 on, a pixel with at least 16
+// samples stops spawning paths once the 95% confidence interval of its
+// luminance, 1.96 sqrt(var / n), is below tol * max(mean, 0.05).
+__device__ __forceinline__ bool pixel_converged(const PtConsts& C, uint32_t pixel, uint64_t sample) {
+    if (sample < 32) return false;
+    const double* st = C.lum_stats + 4 * (size_t)pixel;
+    const double n = st[2];
+    if (n < 16.0) return false;
+    const double mean = st[0] / n;
+    const double var = fmax(st[1] / n - mean * mean, 0.0);
+    return 1.96 * sqrt(var / n) < (double)C.adaptive_tol * fmax(mean, 0.05);
+}
+
 __global__ void k_raygen(DevScene S, Paths P, PtConsts C) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.P) return;
+    const bool adaptive = C.adaptive_tol > 0.0f;
     uint32_t pixel = i % C.npix;
     uint64_t sample = C.sample0 + i / C.npix;
+    if (adaptive) {
+        // Converged pixels get no path; live ones are compacted into the queue.
+        const bool live = i < P.P && !pixel_converged(C, pixel, sample);
+        push_queue(P.q_ext[0], &P.cnt[CNT_EXT_IN], i, live);
+        if (i >= P.P) return;
+        if (!live) {
+            P.L[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            P.prev[i] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(FL_INACTIVE));
+            return;
+        }
+    }
+    if (i >= P.P) return;
     Pcg rng = pcg_for_pixel_sample(pixel, sample);
     uint32_t x = pixel % S.width, y = pixel / S.width;
     float fu = rng.next_f(), fv = rng.next_f();
@@ -209,8 +240,10 @@ __global__ void k_raygen(DevScene S, Paths P, PtConsts C) {
         P.aux_n[i] = make_float4(0, 0, 0, 0);
         P.aux_d[i] = make_float4(0, 0, 0, 0);
     }
-    P.q_ext[0][i] = i;
-    if (i == 0) P.cnt[CNT_EXT_IN] = P.P;
+    if (!adaptive) {
+        P.q_ext[0][i] = i;
+        if (i == 0) P.cnt[CNT_EXT_IN] = P.P;
+    }
 }
 
 // ---- learned proposal: network inputs for this wave's guided vertices ------------------
@@ -920,9 +953,12 @@ __global__ void k_wave_prep(uint32_t* cnt) {
 __global__ void k_accumulate(Paths P, PtConsts C, uint32_t samples_in_slab, double* accum, float* aux) {
     uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
     if (pix >= C.npix) return;
-    double r = 0, g = 0, b = 0;
+    double r = 0, g = 0, b = 0, l1 = 0, l2 = 0;
+    uint32_t taken = 0;
     for (uint32_t s = 0; s < samples_in_slab; s++) {
         uint32_t slot = s * C.npix + pix;
+        if (C.adaptive_tol > 0.0f && (__float_as_uint(P.prev[slot].w) & FL_INACTIVE)) continue;
+        taken++;
         float4 L = P.L[slot];
         float3 l = xyz(L);
         float lum = luminance(l);
@@ -934,6 +970,9 @@ __global__ void k_accumulate(Paths P, PtConsts C, uint32_t samples_in_slab, doub
         r += (double)l.x;
         g += (double)l.y;
         b += (double)l.z;
+        const double lc = (double)luminance(l);
+        l1 += lc;
+        l2 += lc * lc;
         if (C.aovs) {
             float4 a = P.aux_a[slot], nn = P.aux_n[slot], dd = P.aux_d[slot];
             float* A = aux + 12 * (size_t)pix;
@@ -949,7 +988,11 @@ __global__ void k_accumulate(Paths P, PtConsts C, uint32_t samples_in_slab, doub
     acc[0] += r;
     acc[1] += g;
     acc[2] += b;
-    acc[3] += (double)samples_in_slab;
+    acc[3] += (double)taken;
+    double* st = C.lum_stats + 4 * (size_t)pix;
+    st[0] += l1;
+    st[1] += l2;
+    st[2] += (double)taken;
 }
 
 // ---- ray batch (rt_intersect_batch) ------------------------------------------------------

@@ -55,6 +55,8 @@ struct rt_session {
     // path state
     Paths paths{};
     uint32_t slab_samples = 1;     // sample passes per slab
+    double* lum_stats = nullptr;   // per pixel: luminance sum, sum of squares, count, pad
+    float adaptive_tol = 0.0f;     // rt_set_adaptive
     double* accum = nullptr;       // 4 doubles per pixel
     float* aux = nullptr;          // 12 floats per pixel
     uint32_t* err = nullptr;       // device error word
@@ -216,6 +218,7 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     rc = rc ? rc : s->alloc(&s->err, 1);
     rc = rc ? rc : s->alloc(&s->fetch, 1);
     rc = rc ? rc : s->alloc(&s->accum, 4ull * s->npix);
+    rc = rc ? rc : s->alloc(&s->lum_stats, 4ull * s->npix);
     rc = rc ? rc : s->alloc(&s->aux, aov ? 12ull * s->npix : 1);
     // Guiding: inference records per slot, training vertices of every path
     // of the slab, and the slab's training batches (2^16 records per Adam
@@ -260,6 +263,7 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     Pp.err = s->err;
     cudaMemsetAsync(s->err, 0, 4, s->stream);
     cudaMemsetAsync(s->accum, 0, 32ull * s->npix, s->stream);
+    cudaMemsetAsync(s->lum_stats, 0, 32ull * s->npix, s->stream);
     if (aov) cudaMemsetAsync(s->aux, 0, 48ull * s->npix, s->stream);
     ce = cudaStreamSynchronize(s->stream);
     if (ce != cudaSuccess) {
@@ -279,9 +283,28 @@ void* rt_session_stream(rt_session* s) { return s ? (void*)s->stream : nullptr; 
 
 rt_guide* rt_session_guide(rt_session* s) { return s ? s->guide : nullptr; }
 
+int rt_set_adaptive(rt_session* s, double tol) {
+    if (!s) return fail(RT_ERR_INVALID, "session is NULL");
+    if (!(tol >= 0.0) || tol > 1e30) return fail(RT_ERR_INVALID, "adaptive tolerance must be >= 0");
+    s->adaptive_tol = (float)tol;
+    return RT_OK;
+}
+
+int rt_average_spp(rt_session* s, double* out) {
+    if (!s || !out) return fail(RT_ERR_INVALID, "NULL argument");
+    std::vector<double> a(4ull * s->npix);
+    int rc = rt_read_accum(s, a.data());
+    if (rc) return rc;
+    double sum = 0.0;
+    for (size_t p = 0; p < s->npix; p++) sum += a[4 * p + 3];
+    *out = sum / (double)s->npix;
+    return RT_OK;
+}
+
 int rt_reset(rt_session* s) {
     if (!s) return fail(RT_ERR_INVALID, "session is NULL");
     CUDA_TRY(cudaMemsetAsync(s->accum, 0, 32ull * s->npix, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->lum_stats, 0, 32ull * s->npix, s->stream));
     if (s->params.aovs) CUDA_TRY(cudaMemsetAsync(s->aux, 0, 48ull * s->npix, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->samples_done = 0;
@@ -303,6 +326,8 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     C.guided = s->guide ? 1u : 0u;
     C.alpha = (float)std::min(std::max(s->params.guide_fraction, 0.0), 1.0);
     if (s->guide) C.G = guide_dev(s->guide);
+    C.adaptive_tol = s->adaptive_tol;
+    C.lum_stats = s->lum_stats;
     uint64_t guide_records = 0;
     int guide_trainings = 0;
     uint32_t waves = s->params.max_depth + (s->S.any_presence ? RT_MAX_PRESENCE_SKIPS : 0u);
@@ -328,6 +353,10 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     CUDA_TRY(cudaEventRecord(s->evpool[0], st));
     for (uint32_t done = 0; done < count;) {
         uint32_t k = std::min(s->slab_samples, count - done);
+        // Adaptive sampling decides per sample pass, so every decision sees
+        // all earlier samples of the pixel (as the reference's per-sample
+        // dispatches do): one pass per slab.
+        if (s->adaptive_tol > 0.0f) k = 1;
         if (s->guide) {
             // Slabs grow while the network is young, so it is updated often early on.
             k = std::min(k, 1u << std::min<uint64_t>(s->guide_slabs, 31));
@@ -494,6 +523,9 @@ int rt_checkpoint_load(rt_session* s, const char* path, uint32_t* samples_done) 
     fclose(f);
     if (!ok) return fail(RT_ERR_IO, std::string("truncated checkpoint ") + path);
     CUDA_TRY(cudaMemcpyAsync(s->accum, a.data(), 32ull * s->npix, cudaMemcpyHostToDevice, s->stream));
+    // The file holds no luminance statistics: adaptive stopping restarts its
+    // count from the samples rendered after the load.
+    CUDA_TRY(cudaMemsetAsync(s->lum_stats, 0, 32ull * s->npix, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->samples_done = hdr[3];
     if (samples_done) *samples_done = hdr[3];

@@ -29,7 +29,8 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", 
 EXPORTS = ("rt_session_create", "rt_session_destroy", "rt_last_error", "rt_render_samples", "rt_reset",
            "rt_read_accum", "rt_read_image", "rt_read_aux", "rt_checkpoint_save", "rt_checkpoint_load",
            "rt_intersect_batch", "rt_intersect_batch_device", "rt_get_stats", "rt_session_stream",
-           "rt_bsdf_furnace", "rt_intersect_batch_noalloc", "rt_session_guide")
+           "rt_bsdf_furnace", "rt_intersect_batch_noalloc", "rt_session_guide", "rt_set_adaptive",
+           "rt_average_spp")
 
 
 class RtError(RuntimeError):
@@ -81,6 +82,8 @@ def lib():
         L.rt_session_stream.argtypes = [vp]
         L.rt_session_guide.restype = vp
         L.rt_session_guide.argtypes = [vp]
+        L.rt_set_adaptive.argtypes = [vp, C.c_double]
+        L.rt_average_spp.argtypes = [vp, C.POINTER(C.c_double)]
         _lib = L
     return _lib
 
@@ -128,6 +131,16 @@ class PtSession:
     def reset(self):
         _check(lib().rt_reset(self.h))
         self.samples_done = 0
+
+    def set_adaptive(self, tol):
+        """Adaptive stopping (WfSession::set_adaptive): 0 turns it off."""
+        _check(lib().rt_set_adaptive(self.h, float(tol)))
+
+    def average_spp(self):
+        """Samples per pixel actually taken (WfSession::average_spp)."""
+        v = C.c_double()
+        _check(lib().rt_average_spp(self.h, C.byref(v)))
+        return v.value
 
     def sum_and_weight(self):
         """(H, W, 4) f64: radiance sums and the sample weight."""
