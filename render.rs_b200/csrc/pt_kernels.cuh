@@ -381,7 +381,7 @@ __global__ void k_guide_keep(const uint32_t* tb_cnt, float scale, uint32_t cap, 
 // the same code path.
 template <bool ANY, class Load, class Finish>
 __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
-                                         TravStack& st, Load load, Finish finish) {
+                                         TravStack& st, LeafShared& leaf, Load load, Finish finish) {
     PhaseState ps;
     bool active = false, exhausted = false;
     uint32_t item = 0, steps = 0;
@@ -436,9 +436,12 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
             if (__any_sync(0xFFFFFFFFu, done_now)) finish(done_now, item, ps.ts);
             if (done_now) active = false;
         }
-        // Leaf phase.
+        // Leaf phase: instance leaves (TLAS) per lane, then the warp's
+        // triangle leaves together (leaf_coop).
         bool done_now = false;
-        if (active && ps.pending) done_now = op_leaf<ANY>(S, ps, st, err);
+        if (active && ps.pending && !ps.ts.in_inst) done_now = op_leaf<ANY>(S, ps, st, err);
+        const bool tri_leaf = active && !done_now && ps.pending && ps.ts.in_inst;
+        if (__any_sync(0xFFFFFFFFu, tri_leaf)) done_now |= leaf_coop<ANY>(S, ps, tri_leaf, leaf);
         if (__any_sync(0xFFFFFFFFu, done_now)) finish(done_now, item, ps.ts);
         if (done_now) active = false;
     }
@@ -448,6 +451,7 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_extend(DevScene S, Paths P, uint32_t qsel) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    __shared__ LeafShared leaf_sh[BLOCK / 32];
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
     const uint32_t* q = P.q_ext[qsel];
@@ -476,7 +480,7 @@ __global__ void __launch_bounds__(BLOCK) k_extend(DevScene S, Paths P, uint32_t 
         for (uint32_t c = 0; c < N_QUEUES; c++)
             push_queue(P.q_cls + (size_t)c * P.P, &P.cnt[CNT_CLASS + c], slot, done && cls == c);
     };
-    ray_pump<false>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, st, load, finish);
+    ray_pump<false>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
     if (rays) atomicAdd(&P.stats[0], rays);
 }
 
@@ -850,6 +854,7 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene S, Paths P, PtConsts C) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    __shared__ LeafShared leaf_sh[BLOCK / 32];
     __shared__ uint32_t warp_base[BLOCK / 32];
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
@@ -880,7 +885,7 @@ __global__ void __launch_bounds__(BLOCK) k_shadow(DevScene S, Paths P, PtConsts 
             rays++;
             if (!ts.found) add(slot, 1.0f);
         };
-        ray_pump<true>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, load, finish);
+        ray_pump<true>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
         if (rays) atomicAdd(&P.stats[1], rays);
         return;
     }
@@ -1001,6 +1006,7 @@ __global__ void __launch_bounds__(BLOCK) k_intersect(DevScene S, const float4* _
                                                      const float4* __restrict__ dir, uint64_t n, uint32_t* prim,
                                                      uint32_t* inst, float* tout, uint32_t* fetch, uint32_t* err) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    __shared__ LeafShared leaf_sh[BLOCK / 32];
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
     auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
@@ -1026,7 +1032,7 @@ __global__ void __launch_bounds__(BLOCK) k_intersect(DevScene S, const float4* _
             if (tout) tout[i] = t;
         }
     };
-    ray_pump<ANY>(S, (uint32_t)n, fetch, err, st, load, finish);
+    ray_pump<ANY>(S, (uint32_t)n, fetch, err, st, leaf_sh[threadIdx.x >> 5], load, finish);
 }
 
 // White-furnace estimator of one material: per thread, `per` BSDF samples

@@ -534,6 +534,103 @@ __device__ __forceinline__ bool op_leaf(const DevScene& S, PhaseState& ps, TravS
     return false;
 }
 
+// ---- warp-cooperative triangle leaves --------------------------------------------------
+// In the leaf phase the lanes of a warp hold parked BLAS leaves of 1 to 16
+// triangles each. Testing its own leaf, a lane idles while the warp's largest
+// leaf finishes; instead the warp pools all parked triangles (at most
+// 32 x 16) and tests them 32 at a time, each lane taking the next triangle
+// of the pool with its owner's (object-space) ray fetched by shuffles. A
+// ray's closest hit in its leaf is the minimum of the 64-bit key
+// (t bits, triangle index) over its triangles, kept with a shared-memory
+// atomicMin: the smallest t, and among equal t the first triangle in leaf
+// order, which is the answer of the sequential loop.
+struct LeafShared {
+    unsigned long long key[32];  // best (t bits << 32 | triangle) per owner lane
+    float2 bary[32];             // barycentrics of that triangle
+    uint16_t item[512];          // pool item -> (owner lane << 4) | index in its leaf
+};
+
+// `mine`: this lane's parked leaf is a triangle leaf to test. Returns true
+// when an any-hit query found a hit (the query is over).
+template <bool ANY>
+__device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, bool mine, LeafShared& L) {
+    const uint32_t lane = threadIdx.x & 31u;
+    TravState& ts = ps.ts;
+    uint32_t first = 0, count = 0;
+    if (mine) {
+        first = ps.pending & LEAF_FIRST_MASK;
+        count = ((ps.pending >> 27) & 15u) + 1u;
+        ps.pending = 0;
+        ps.need_pop = true;
+    }
+    uint32_t incl = count;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, off);
+        if (lane >= (uint32_t)off) incl += v;
+    }
+    const uint32_t excl = incl - count, total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    for (uint32_t k = 0; k < count; k++) L.item[excl + k] = (uint16_t)((lane << 4) | k);
+    L.key[lane] = ~0ull;
+    __syncwarp();
+    // This lane's ray, as the owners of pool items read it.
+    const float tmax_own = ts.hit.t;
+    const uint32_t kpack = (uint32_t)ts.r.kx | ((uint32_t)ts.r.ky << 2) | ((uint32_t)ts.r.kz << 4);
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t idx = base + lane;
+        const bool has = idx < total;
+        const uint32_t it = has ? L.item[idx] : 0u;
+        const uint32_t owner = it >> 4;
+        RayPre r;
+        r.o.x = __shfl_sync(0xFFFFFFFFu, ts.r.o.x, owner);
+        r.o.y = __shfl_sync(0xFFFFFFFFu, ts.r.o.y, owner);
+        r.o.z = __shfl_sync(0xFFFFFFFFu, ts.r.o.z, owner);
+        r.sx = __shfl_sync(0xFFFFFFFFu, ts.r.sx, owner);
+        r.sy = __shfl_sync(0xFFFFFFFFu, ts.r.sy, owner);
+        r.sz = __shfl_sync(0xFFFFFFFFu, ts.r.sz, owner);
+        const uint32_t kp = __shfl_sync(0xFFFFFFFFu, kpack, owner);
+        const uint32_t f = __shfl_sync(0xFFFFFFFFu, first, owner);
+        float tmax = __shfl_sync(0xFFFFFFFFu, tmax_own, owner);
+        r.kx = (int)(kp & 3u);
+        r.ky = (int)((kp >> 2) & 3u);
+        r.kz = (int)((kp >> 4) & 3u);
+        float t = 0.0f, b1 = 0.0f, b2 = 0.0f;
+        unsigned long long key = ~0ull;
+        if (has) {
+            const unsigned long long best = L.key[owner];
+            // Cull with the best hit so far, keeping hits at equal t (they
+            // compete on the triangle index).
+            if (best != ~0ull) tmax = fminf(tmax, nextafterf(__uint_as_float((uint32_t)(best >> 32)), INFINITY));
+            const uint32_t tri = f + (it & 15u);
+            const float4* tp = S.tris + 3 * (size_t)tri;
+            float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            if (tri_watertight(r, xyz(a), xyz(b), xyz(c), tmax, t, b1, b2)) {
+                key = ((unsigned long long)__float_as_uint(t) << 32) | tri;
+                atomicMin(&L.key[owner], key);
+            }
+        }
+        __syncwarp();
+        if (key != ~0ull && L.key[owner] == key) L.bary[owner] = make_float2(b1, b2);
+        __syncwarp();
+    }
+    bool hit_now = false;
+    if (mine) {
+        const unsigned long long best = L.key[lane];
+        if (best != ~0ull) {
+            const float2 bb = L.bary[lane];
+            ts.hit.t = __uint_as_float((uint32_t)(best >> 32));
+            ts.hit.tri = (uint32_t)best;
+            ts.hit.inst = ts.cur_inst;
+            ts.hit.b1 = bb.x;
+            ts.hit.b2 = bb.y;
+            ts.found = true;
+            hit_now = true;
+        }
+    }
+    __syncwarp();
+    return ANY && hit_now;
+}
+
 // Closest hit (ANY = false) or any hit (ANY = true, returns at the first
 // hit with t < t_max) of one ray, to completion. World-space ray (o, d),
 // parametric t.

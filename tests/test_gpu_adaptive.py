@@ -39,17 +39,22 @@ def test_adaptive_spends_samples_where_noise_is():
     p = abi.make_params(max_depth=8)
     spp = 256
     with PtSession(s, p) as g:
-        g.set_adaptive(0.05)
+        g.set_adaptive(0.2)
         g.render_samples(0, spp)
         avg = g.average_spp()
         acc = g.sum_and_weight()
         img = g.image()
     n = acc[..., 3]
+    # A pixel whose samples have a coefficient of variation c stops near
+    # (1.96 c / 0.2)^2 samples: the noisy ones take many more than the flat.
     assert 32 <= n.min() and n.max() == spp
-    assert 32 < avg < 0.9 * spp
-    # The light's pixels (constant radiance) stop at the first check.
+    assert 32 < avg < 0.8 * spp
+    print(f"adaptive tol 0.2: {avg:.1f} spp on average of {spp}")
+    # Pixels wholly inside the light see its radiance (17, 12, 4), luminance
+    # 12.5, in every sample: zero variance, so they stop at the first check.
     lum = img @ np.array([0.2126, 0.7152, 0.0722])
-    assert n[lum > 5.0].max() == 32
+    inside = np.abs(lum - 12.5) < 0.05
+    assert inside.sum() > 4 and n[inside].max() == 32
     cpu = oracle.OracleScene(s).render(p, 0, 64)[0].reshape(64, 64, 3) / 64
     mc, mg = cpu.reshape(-1, 3).mean(0), img.reshape(-1, 3).mean(0)
     assert np.all(np.abs(mc - mg) / mc < 0.03), (mc, mg)
