@@ -190,7 +190,9 @@ __device__ __forceinline__ void test_node(const uint4* __restrict__ nodes, uint3
 }
 
 // ---- traversal stack: shared-memory top, local-memory spill ----------------------------
-#define RT_SH_STACK 32
+#ifndef RT_SH_STACK
+#define RT_SH_STACK 32   // traversal stack entries kept in shared memory per thread (power of two)
+#endif
 #define RT_SPILL 96
 
 struct TravStack {
