@@ -145,6 +145,14 @@ def cpu_baseline_sample(scene, params, threads=0, target_s=12.0):
 
 GUIDED_W, GUIDED_H, GUIDED_SPP, GUIDED_DEPTH = 1280, 720, 256, 16
 
+# DRAM bytes (read + write) per k_extend launch, averaged over the 32 launches
+# of one render step, from one ncu capture of this command (1 pass):
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#       --clock-control none -k regex:k_extend -s 32 -c 32
+#       python bench.py --steps 1 --warmup 1 --e2e-steps 0 --no-cpu-baseline --no-guided
+EXTEND_DRAM_BYTES_PER_LAUNCH = 135.8e6  # 106.0 MB read + 29.8 MB written
+EXTEND_DRAM_SOURCE = "ncu, dram__bytes_read.sum + dram__bytes_write.sum, mean of one step's 32 k_extend launches"
+
 
 def rel_mse(img, ref):
     return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
@@ -338,7 +346,7 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    ext_ms = ext_rays = launches = 0.0
+    ext_ms = ext_rays = launches = ext_launches = 0.0
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     barrier()
@@ -348,6 +356,7 @@ def main():
         st = sess.stats()
         ext_ms += st["extend_ms"]
         ext_rays += st["extension_rays"]
+        ext_launches += st["slabs"] * st["waves"]
         launches += st["kernel_launches"] + 1
     e1.record(stream)
     barrier()
@@ -415,12 +424,14 @@ def main():
         roof = None
         if work:
             bytes_per_ray = work["ext_bytes_per_ray"]
-            launches_ext = args.steps * MAX_DEPTH * int(np.ceil(1.0))
+            launches_ext = max(1.0, ext_launches)
             achieved = bytes_per_ray * ext_rays / (ext_ms / 1e3) / 1e9
             roof = {"kernel": "k_extend (closest hit, 8-wide BVH)", "bound": "hbm", "achieved": achieved,
-                    "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
-                    "peak_kind": peak_kind, "bytes_per_ray": bytes_per_ray,
-                    "rays_per_launch": ext_rays / max(1, launches_ext), "launch_ms": ext_ms / max(1, launches_ext)}
+                    "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": EXTEND_DRAM_BYTES_PER_LAUNCH,
+                    "traffic_source": EXTEND_DRAM_SOURCE, "peak_kind": peak_kind, "bytes_per_ray": bytes_per_ray,
+                    "algorithmic_bytes_per_launch": bytes_per_ray * ext_rays / launches_ext,
+                    "rays_per_launch": ext_rays / launches_ext, "launch_ms": ext_ms / launches_ext,
+                    "launches": int(launches_ext)}
         guided = None
         if not args.no_guided and world == 1:
             guided = guided_equal_time()

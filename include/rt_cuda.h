@@ -143,6 +143,8 @@ typedef struct rt_stats {
     uint64_t guide_steps;       /* last render: training iterations of the learned proposal */
     uint64_t guide_records;     /* last render: records in the final training batch */
     double   guide_loss;        /* last render: summed loss of the final training batch */
+    uint64_t slabs;             /* last render: wavefront slabs (each: raygen, waves, accumulate) */
+    uint64_t waves;             /* last render: waves per slab (extend/shade/shadow launches each) */
 } rt_stats;
 
 int rt_get_stats(rt_session* s, rt_stats* out);

@@ -337,6 +337,7 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     float ms_ext = 0, ms_sh = 0, ms_shade = 0;
     uint64_t launches = 0;
     uint32_t last_records_slab = 0;
+    uint64_t slabs = 0;
     // Per-wave timing events are recorded without host waits and read once
     // at the end, so the waves of a slab run back to back.
     auto events = [&](size_t need) -> int {
@@ -417,6 +418,7 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
             last_records_slab = steps * batch;
         }
         done += k;
+        slabs++;
     }
     CUDA_TRY(cudaEventRecord(s->evpool[1], st));
     CUDA_TRY(cudaGetLastError());
@@ -445,6 +447,8 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     s->last.shade_ms = ms_shade;
     s->last.total_ms = total;
     s->last.guide_steps = (uint64_t)guide_trainings;
+    s->last.slabs = slabs;
+    s->last.waves = waves;
     s->last.guide_records = 0;
     s->last.guide_loss = 0.0;
     if (s->guide) {

@@ -44,7 +44,8 @@ class RtStats(C.Structure):
                 ("device_bytes", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("samples", C.c_uint64), ("kernel_launches", C.c_uint64), ("extend_ms", C.c_double),
                 ("shadow_ms", C.c_double), ("shade_ms", C.c_double), ("total_ms", C.c_double),
-                ("guide_steps", C.c_uint64), ("guide_records", C.c_uint64), ("guide_loss", C.c_double)]
+                ("guide_steps", C.c_uint64), ("guide_records", C.c_uint64), ("guide_loss", C.c_double),
+                ("slabs", C.c_uint64), ("waves", C.c_uint64)]
 
 
 _lib = None
