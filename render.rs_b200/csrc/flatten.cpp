@@ -22,6 +22,8 @@
 #include <atomic>
 #include <functional>
 #include <limits>
+#include <condition_variable>
+#include <mutex>
 #include <thread>
 
 namespace rt {
@@ -34,15 +36,23 @@ const double INF = std::numeric_limits<double>::infinity();
 struct Box {
     double lo[3] = {INF, INF, INF};
     double hi[3] = {-INF, -INF, -INF};
+    // Plain comparisons (inputs are finite: flatten_scene rejects NaN/inf
+    // vertices), which compile to minsd / maxsd. grow() takes the union of
+    // two boxes, so an empty box leaves the other unchanged; the reference's
+    // Aabb::grow (src/accel/bvh.rs:36-39) grows by the other's corner points,
+    // which makes a union with an empty SAH bin infinite and rules out every
+    // split with an empty bin on either side. Here those splits stay open.
     void grow_pt(const double* p) {
         for (int a = 0; a < 3; a++) {
-            lo[a] = std::fmin(lo[a], p[a]);
-            hi[a] = std::fmax(hi[a], p[a]);
+            lo[a] = p[a] < lo[a] ? p[a] : lo[a];
+            hi[a] = p[a] > hi[a] ? p[a] : hi[a];
         }
     }
     void grow(const Box& b) {
-        grow_pt(b.lo);
-        grow_pt(b.hi);
+        for (int a = 0; a < 3; a++) {
+            lo[a] = b.lo[a] < lo[a] ? b.lo[a] : lo[a];
+            hi[a] = b.hi[a] > hi[a] ? b.hi[a] : hi[a];
+        }
     }
     double area() const {
         double d0 = hi[0] - lo[0], d1 = hi[1] - lo[1], d2 = hi[2] - lo[2];
@@ -50,6 +60,22 @@ struct Box {
         return 2.0 * (d0 * d1 + d1 * d2 + d2 * d0);
     }
 };
+
+// Run fn(begin, end) over [0, n) in contiguous chunks on all host threads
+// (one thread for small n).
+void parallel_for(size_t n, const std::function<void(size_t, size_t)>& fn) {
+    const size_t min_chunk = 65536;
+    size_t threads = std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency()));
+    threads = std::min(threads, std::max<size_t>(1, n / min_chunk));
+    if (threads <= 1) {
+        fn(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < threads; t++)
+        pool.emplace_back([&, t] { fn(n * t / threads, n * (t + 1) / threads); });
+    for (auto& th : pool) th.join();
+}
 
 struct BinNode {
     Box b;
@@ -64,32 +90,42 @@ struct BinBvh {
 // Binned SAH with the reference's split rules. Subtrees are independent
 // (each partitions only its own primitive range), so large ones are built on
 // their own threads; the tree is the same as a sequential build, only the
-// node numbering differs, and nothing downstream depends on it.
+// node numbering differs, and nothing downstream depends on it. The
+// primitives' boxes and centroids are partitioned in place with their
+// indices (the reference's swap partition, same order), so every pass over a
+// node's range reads memory sequentially.
 BinBvh build_binary(const std::vector<Box>& bounds) {
     const int BINS = 16, MAX_LEAF = 4;
     BinBvh t;
     size_t n = bounds.size();
     t.order.resize(n);
-    for (size_t i = 0; i < n; i++) t.order[i] = (uint32_t)i;
     if (n == 0) return t;
-    std::vector<double> cen(3 * n);
-    for (size_t i = 0; i < n; i++)
-        for (int a = 0; a < 3; a++) cen[3 * i + a] = (bounds[i].lo[a] + bounds[i].hi[a]) * 0.5;
+    struct Prim {
+        Box b;
+        uint32_t idx;
+        double c(int a) const { return (b.lo[a] + b.hi[a]) * 0.5; }  // centroid, as the reference
+    };
+    std::vector<Prim> prims(n);
+    for (size_t i = 0; i < n; i++) {
+        prims[i].b = bounds[i];
+        prims[i].idx = (uint32_t)i;
+    }
     t.nodes.resize(2 * n + 1);
     std::atomic<size_t> next{1};
-    uint32_t* ord = t.order.data();
+    Prim* P = prims.data();
     BinNode* nodes = t.nodes.data();
     struct Job { size_t node, start, count; };
     const size_t PAR_MIN = 32768;
     const int max_threads = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    std::atomic<int> threads_live{1};
 
     // One level: bounds, split choice, partition. Returns false for a leaf.
     auto split_node = [&](const Job& j, size_t* split_out) -> bool {
+        Prim* r = P + j.start;
         Box b, cb;
-        for (size_t i = j.start; i < j.start + j.count; i++) {
-            b.grow(bounds[ord[i]]);
-            cb.grow_pt(&cen[3 * ord[i]]);
+        for (size_t i = 0; i < j.count; i++) {
+            b.grow(r[i].b);
+            const double c[3] = {r[i].c(0), r[i].c(1), r[i].c(2)};
+            cb.grow_pt(c);
         }
         nodes[j.node].b = b;
         auto make_leaf = [&]() {
@@ -108,12 +144,12 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
             Box bb[BINS];
             size_t bc[BINS] = {0};
             double scale = (double)BINS / aext;
-            for (size_t i = j.start; i < j.start + j.count; i++) {
-                double f = (cen[3 * ord[i] + axis] - amin) * scale;
+            for (size_t i = 0; i < j.count; i++) {
+                double f = (r[i].c(axis) - amin) * scale;
                 size_t k = f > 0.0 ? (size_t)f : 0;
                 if (k > (size_t)BINS - 1) k = BINS - 1;
                 bc[k]++;
-                bb[k].grow(bounds[ord[i]]);
+                bb[k].grow(r[i].b);
             }
             Box racc[BINS], acc;
             for (int i = BINS - 1; i >= 1; i--) {
@@ -140,8 +176,8 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
                 double boundary = amin + aext * (double)(best_bin + 1) / (double)BINS;
                 size_t m = 0;
                 for (size_t q = 0; q < j.count; q++) {
-                    if (cen[3 * ord[j.start + q] + axis] < boundary) {
-                        std::swap(ord[j.start + m], ord[j.start + q]);
+                    if (r[q].c(axis) < boundary) {
+                        if (q != m) std::swap(r[m], r[q]);
                         m++;
                     }
                 }
@@ -155,34 +191,60 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
         return true;
     };
 
-    std::function<void(Job)> build_subtree = [&](Job root) {
-        std::vector<Job> stack{root};
-        std::vector<std::thread> spawned;
-        while (!stack.empty()) {
-            Job j = stack.back();
-            stack.pop_back();
-            size_t split;
-            if (!split_node(j, &split)) continue;
-            size_t l = next.fetch_add(2);
-            nodes[j.node].first = (uint32_t)l;
-            nodes[j.node].count = 0;
-            Job left{l, j.start, split - j.start}, right{l + 1, split, j.start + j.count - split};
-            if (left.count >= PAR_MIN && threads_live.load() < max_threads) {
-                threads_live++;
-                spawned.emplace_back([&, left] {
-                    build_subtree(left);
-                    threads_live--;
-                });
-                stack.push_back(right);
-            } else {
-                stack.push_back(right);
-                stack.push_back(left);
+    // Worker pool: subtrees of at least PAR_MIN primitives go to a shared
+    // queue that idle workers take from; smaller ones are finished by the
+    // worker that split them.
+    std::mutex mu;
+    std::condition_variable cv;
+    std::vector<Job> shared{Job{0, 0, n}};
+    int busy = 0;
+    auto worker = [&]() {
+        for (;;) {
+            Job root;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv.wait(lk, [&] { return !shared.empty() || busy == 0; });
+                if (shared.empty()) return;  // nothing queued and nobody can add more
+                root = shared.back();
+                shared.pop_back();
+                busy++;
             }
+            std::vector<Job> stack{root};
+            while (!stack.empty()) {
+                Job j = stack.back();
+                stack.pop_back();
+                size_t split;
+                if (!split_node(j, &split)) continue;
+                size_t l = next.fetch_add(2);
+                nodes[j.node].first = (uint32_t)l;
+                nodes[j.node].count = 0;
+                Job left{l, j.start, split - j.start}, right{l + 1, split, j.start + j.count - split};
+                if (left.count >= PAR_MIN) {
+                    {
+                        std::lock_guard<std::mutex> lk(mu);
+                        shared.push_back(left);
+                    }
+                    cv.notify_one();
+                    stack.push_back(right);
+                } else {
+                    stack.push_back(right);
+                    stack.push_back(left);
+                }
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                busy--;
+            }
+            cv.notify_all();
         }
-        for (auto& th : spawned) th.join();
     };
-    build_subtree({0, 0, n});
+    const int workers = n >= PAR_MIN ? max_threads : 1;
+    std::vector<std::thread> pool;
+    for (int w = 1; w < workers; w++) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
     t.nodes.resize(next.load());
+    for (size_t i = 0; i < n; i++) t.order[i] = P[i].idx;
     return t;
 }
 
@@ -257,7 +319,11 @@ struct Collapser {
         for (int k = 0; k < nk; k++) nb.grow(bin.nodes[kids[k]].b);
         float p[3];
         int e[3];
-        for (int a = 0; a < 3; a++) choose_grid(nb.lo[a], nb.hi[a], &p[a], &e[a]);
+        double sc[3];
+        for (int a = 0; a < 3; a++) {
+            choose_grid(nb.lo[a], nb.hi[a], &p[a], &e[a]);
+            sc[a] = std::ldexp(1.0, e[a]);
+        }
         uint8_t qlo[3][8], qhi[3][8];
         for (int k = 0; k < 8; k++)
             for (int a = 0; a < 3; a++) {
@@ -267,7 +333,7 @@ struct Collapser {
         for (int k = 0; k < nk; k++) {
             const Box& cbx = bin.nodes[kids[k]].b;
             for (int a = 0; a < 3; a++) {
-                double s = std::ldexp(1.0, e[a]);
+                const double s = sc[a];
                 double ql = std::floor((cbx.lo[a] - (double)p[a]) / s);
                 double qh = std::ceil((cbx.hi[a] - (double)p[a]) / s);
                 ql = std::min(std::max(ql, 0.0), 255.0);
@@ -485,23 +551,38 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
             return false;
         }
         std::vector<Box> tb(md.n_triangles);
-        for (uint32_t t = 0; t < md.n_triangles; t++) {
-            Box b;
-            for (int k = 0; k < 3; k++) {
-                uint32_t vi = md.indices[3ull * t + k];
-                if (vi >= md.n_vertices) {
-                    *err = "mesh " + std::to_string(m) + " index out of range";
-                    return false;
+        std::atomic<int> bad_index{0}, bad_vertex{0};
+        std::mutex bounds_mu;
+        parallel_for(md.n_triangles, [&](size_t t0, size_t t1) {
+            Box local;
+            for (size_t t = t0; t < t1; t++) {
+                Box b;
+                for (int k = 0; k < 3; k++) {
+                    uint32_t vi = md.indices[3ull * t + k];
+                    if (vi >= md.n_vertices) {
+                        bad_index = 1;
+                        continue;
+                    }
+                    double p[3] = {md.positions[3ull * vi], md.positions[3ull * vi + 1], md.positions[3ull * vi + 2]};
+                    if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) {
+                        bad_vertex = 1;
+                        continue;
+                    }
+                    b.grow_pt(p);
                 }
-                double p[3] = {md.positions[3ull * vi], md.positions[3ull * vi + 1], md.positions[3ull * vi + 2]};
-                if (!std::isfinite(p[0]) || !std::isfinite(p[1]) || !std::isfinite(p[2])) {
-                    *err = "mesh " + std::to_string(m) + " has a non-finite vertex";
-                    return false;
-                }
-                b.grow_pt(p);
+                tb[t] = b;
+                local.grow(b);
             }
-            tb[t] = b;
-            local_bounds[m].grow(b);
+            std::lock_guard<std::mutex> lk(bounds_mu);
+            local_bounds[m].grow(local);
+        });
+        if (bad_index) {
+            *err = "mesh " + std::to_string(m) + " index out of range";
+            return false;
+        }
+        if (bad_vertex) {
+            *err = "mesh " + std::to_string(m) + " has a non-finite vertex";
+            return false;
         }
         BinBvh bin = build_binary(tb);
         H.binary_blas_nodes += bin.nodes.size();
@@ -515,25 +596,31 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
             for (uint64_t k = 0; k < 3ull * md.n_triangles; k++) H.orig_idx.push_back(vbase + md.indices[k]);
             H.normals.insert(H.normals.end(), md.normals, md.normals + 3ull * md.n_vertices);
         }
-        for (uint32_t k = 0; k < md.n_triangles; k++) {
-            uint32_t t = bin.order[k];
-            float4 v[3];
-            for (int c = 0; c < 3; c++) {
-                uint32_t vi = md.indices[3ull * t + c];
-                v[c] = make_float4(md.positions[3ull * vi], md.positions[3ull * vi + 1], md.positions[3ull * vi + 2],
-                                   0.0f);
+        const size_t tri_off = H.tris.size();
+        H.tris.resize(tri_off + 3ull * md.n_triangles);
+        float4* dst = H.tris.data() + tri_off;
+        parallel_for(md.n_triangles, [&](size_t k0, size_t k1) {
+            for (size_t k = k0; k < k1; k++) {
+                uint32_t t = bin.order[k];
+                float4 v[3];
+                for (int c = 0; c < 3; c++) {
+                    uint32_t vi = md.indices[3ull * t + c];
+                    v[c] = make_float4(md.positions[3ull * vi], md.positions[3ull * vi + 1],
+                                       md.positions[3ull * vi + 2], 0.0f);
+                }
+                uint32_t tid = t;
+                memcpy(&v[0].w, &tid, 4);
+                dst[3 * k] = v[0];
+                dst[3 * k + 1] = v[1];
+                dst[3 * k + 2] = v[2];
             }
-            uint32_t tid = t;
-            memcpy(&v[0].w, &tid, 4);
-            H.tris.push_back(v[0]);
-            H.tris.push_back(v[1]);
-            H.tris.push_back(v[2]);
-        }
+        });
         if (md.n_triangles == 0) {
             mi.blas_root = 0xFFFFFFFFu;
             continue;
         }
         Collapser col{bin, H.nodes, mi.tri_base};
+        H.nodes.reserve(H.nodes.size() + WIDE_NODE_WORDS * (bin.nodes.size() / 4 + 1));
         mi.blas_root = col.emit(0);
         H.blas_nodes += col.emitted;
         if (col.decode_errors) {
