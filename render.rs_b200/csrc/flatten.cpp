@@ -62,9 +62,8 @@ struct Box {
 };
 
 // Run fn(begin, end) over [0, n) in contiguous chunks on all host threads
-// (one thread for small n).
-void parallel_for(size_t n, const std::function<void(size_t, size_t)>& fn) {
-    const size_t min_chunk = 65536;
+// (one thread when n is below two chunks of min_chunk items).
+void parallel_for(size_t n, const std::function<void(size_t, size_t)>& fn, size_t min_chunk = 65536) {
     size_t threads = std::max<size_t>(1, std::min<size_t>(16, std::thread::hardware_concurrency()));
     threads = std::min(threads, std::max<size_t>(1, n / min_chunk));
     if (threads <= 1) {
@@ -100,14 +99,33 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
     size_t n = bounds.size();
     t.order.resize(n);
     if (n == 0) return t;
+    // Primitive boxes are kept in f32 (28-byte records: the passes are
+    // memory-bound). Triangle bounds come from f32 vertices, so they are
+    // exact and every SAH decision (made in f64 from these values) is the
+    // one an f64 record would give; other boxes (instances) are rounded
+    // outward, which keeps them conservative.
     struct Prim {
-        Box b;
+        float lo[3], hi[3];
         uint32_t idx;
-        double c(int a) const { return (b.lo[a] + b.hi[a]) * 0.5; }  // centroid, as the reference
+        double c(int a) const { return ((double)lo[a] + (double)hi[a]) * 0.5; }  // centroid, as the reference
+        Box box() const {
+            Box b;
+            for (int a = 0; a < 3; a++) {
+                b.lo[a] = lo[a];
+                b.hi[a] = hi[a];
+            }
+            return b;
+        }
     };
     std::vector<Prim> prims(n);
     for (size_t i = 0; i < n; i++) {
-        prims[i].b = bounds[i];
+        for (int a = 0; a < 3; a++) {
+            float l = (float)bounds[i].lo[a], h = (float)bounds[i].hi[a];
+            if ((double)l > bounds[i].lo[a]) l = std::nextafter(l, -INFINITY);
+            if ((double)h < bounds[i].hi[a]) h = std::nextafter(h, INFINITY);
+            prims[i].lo[a] = l;
+            prims[i].hi[a] = h;
+        }
         prims[i].idx = (uint32_t)i;
     }
     t.nodes.resize(2 * n + 1);
@@ -118,14 +136,45 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
     const size_t PAR_MIN = 32768;
     const int max_threads = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
 
+    // Nodes of at least PAR_SPLIT primitives (the top levels, which are the
+    // build's critical path) run their passes on all threads: chunked bounds
+    // and bins merged afterwards, and a stable two-pass partition through a
+    // scratch buffer (same left / right sets as the swap partition; the order
+    // within each side differs, which only permutes leaf contents).
+    const size_t PAR_SPLIT = 262144;
+    const size_t CHUNKS = (size_t)max_threads;
+    auto chunked = [&](size_t count, const std::function<void(size_t, size_t, size_t)>& fn) {
+        std::vector<std::thread> pool;
+        for (size_t c = 1; c < CHUNKS; c++) pool.emplace_back([&, c] { fn(c, count * c / CHUNKS, count * (c + 1) / CHUNKS); });
+        fn(0, 0, count / CHUNKS);
+        for (auto& th : pool) th.join();
+    };
+    std::vector<Prim> scratch;
+
     // One level: bounds, split choice, partition. Returns false for a leaf.
     auto split_node = [&](const Job& j, size_t* split_out) -> bool {
         Prim* r = P + j.start;
+        const bool wide_node = j.count >= PAR_SPLIT && CHUNKS > 1;
         Box b, cb;
-        for (size_t i = 0; i < j.count; i++) {
-            b.grow(r[i].b);
-            const double c[3] = {r[i].c(0), r[i].c(1), r[i].c(2)};
-            cb.grow_pt(c);
+        if (wide_node) {
+            std::vector<Box> pb(CHUNKS), pcb(CHUNKS);
+            chunked(j.count, [&](size_t c, size_t i0, size_t i1) {
+                for (size_t i = i0; i < i1; i++) {
+                    pb[c].grow(r[i].box());
+                    const double cc[3] = {r[i].c(0), r[i].c(1), r[i].c(2)};
+                    pcb[c].grow_pt(cc);
+                }
+            });
+            for (size_t c = 0; c < CHUNKS; c++) {
+                b.grow(pb[c]);
+                cb.grow(pcb[c]);
+            }
+        } else {
+            for (size_t i = 0; i < j.count; i++) {
+                b.grow(r[i].box());
+                const double c[3] = {r[i].c(0), r[i].c(1), r[i].c(2)};
+                cb.grow_pt(c);
+            }
         }
         nodes[j.node].b = b;
         auto make_leaf = [&]() {
@@ -144,12 +193,26 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
             Box bb[BINS];
             size_t bc[BINS] = {0};
             double scale = (double)BINS / aext;
-            for (size_t i = 0; i < j.count; i++) {
-                double f = (r[i].c(axis) - amin) * scale;
-                size_t k = f > 0.0 ? (size_t)f : 0;
-                if (k > (size_t)BINS - 1) k = BINS - 1;
-                bc[k]++;
-                bb[k].grow(r[i].b);
+            auto bin_range = [&](size_t i0, size_t i1, Box* obb, size_t* obc) {
+                for (size_t i = i0; i < i1; i++) {
+                    double f = (r[i].c(axis) - amin) * scale;
+                    size_t k = f > 0.0 ? (size_t)f : 0;
+                    if (k > (size_t)BINS - 1) k = BINS - 1;
+                    obc[k]++;
+                    obb[k].grow(r[i].box());
+                }
+            };
+            if (wide_node) {
+                std::vector<Box> pbb(CHUNKS * BINS);
+                std::vector<size_t> pbc(CHUNKS * BINS, 0);
+                chunked(j.count, [&](size_t c, size_t i0, size_t i1) { bin_range(i0, i1, &pbb[c * BINS], &pbc[c * BINS]); });
+                for (size_t c = 0; c < CHUNKS; c++)
+                    for (int k = 0; k < BINS; k++) {
+                        bb[k].grow(pbb[c * BINS + k]);
+                        bc[k] += pbc[c * BINS + k];
+                    }
+            } else {
+                bin_range(0, j.count, bb, bc);
             }
             Box racc[BINS], acc;
             for (int i = BINS - 1; i >= 1; i--) {
@@ -175,10 +238,40 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
             if (std::isfinite(best) && best < leaf_cost) {
                 double boundary = amin + aext * (double)(best_bin + 1) / (double)BINS;
                 size_t m = 0;
-                for (size_t q = 0; q < j.count; q++) {
-                    if (r[q].c(axis) < boundary) {
-                        if (q != m) std::swap(r[m], r[q]);
-                        m++;
+                if (wide_node) {
+                    std::vector<size_t> nleft(CHUNKS, 0);
+                    chunked(j.count, [&](size_t c, size_t i0, size_t i1) {
+                        size_t cnt = 0;
+                        for (size_t i = i0; i < i1; i++) cnt += r[i].c(axis) < boundary;
+                        nleft[c] = cnt;
+                    });
+                    for (size_t c = 0; c < CHUNKS; c++) m += nleft[c];
+                    std::vector<size_t> lo_at(CHUNKS), hi_at(CHUNKS);
+                    size_t lacc = 0, racc_n = m;
+                    for (size_t c = 0; c < CHUNKS; c++) {
+                        lo_at[c] = lacc;
+                        hi_at[c] = racc_n;
+                        size_t len = j.count * (c + 1) / CHUNKS - j.count * c / CHUNKS;
+                        lacc += nleft[c];
+                        racc_n += len - nleft[c];
+                    }
+                    Prim* tmp = scratch.data() + j.start;  // this node's own range of the scratch buffer
+                    chunked(j.count, [&](size_t c, size_t i0, size_t i1) {
+                        size_t lw = lo_at[c], rw = hi_at[c];
+                        for (size_t i = i0; i < i1; i++) {
+                            if (r[i].c(axis) < boundary) tmp[lw++] = r[i];
+                            else tmp[rw++] = r[i];
+                        }
+                    });
+                    chunked(j.count, [&](size_t, size_t i0, size_t i1) {
+                        std::copy(tmp + i0, tmp + i1, r + i0);
+                    });
+                } else {
+                    for (size_t q = 0; q < j.count; q++) {
+                        if (r[q].c(axis) < boundary) {
+                            if (q != m) std::swap(r[m], r[q]);
+                            m++;
+                        }
                     }
                 }
                 if (m > 0 && m < j.count) split = j.start + m;
@@ -238,6 +331,7 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
             cv.notify_all();
         }
     };
+    if (n >= PAR_SPLIT && CHUNKS > 1) scratch.resize(n);
     const int workers = n >= PAR_MIN ? max_threads : 1;
     std::vector<std::thread> pool;
     for (int w = 1; w < workers; w++) pool.emplace_back(worker);
@@ -276,47 +370,77 @@ struct Collapser {
     uint32_t prim_base;
     uint64_t emitted = 0;
     uint64_t decode_errors = 0;
+    // Structure first (sequential recursion: which binary nodes become the
+    // children of each wide node), then quantisation of all wide nodes in
+    // parallel (finish()).
+    struct Wide {
+        uint32_t idx, nk;
+        uint32_t kids[8], refs[8];
+    };
+    std::vector<Wide> wide;
 
     uint32_t leaf_ref(const BinNode& nd) const { return make_leaf_ref(prim_base + nd.first, nd.count); }
 
-    // Emit the wide node covering binary node `bi`; returns its index.
+    // Reserve the wide node covering binary node `bi` (and, recursively, its
+    // descendants); returns its index. finish() writes the words.
     uint32_t emit(uint32_t bi) {
         const BinNode& root = bin.nodes[bi];
-        uint32_t kids[8];
-        int nk = 0;
+        Wide w{};
+        uint32_t nk = 0;
         if (root.count > 0) {
-            kids[nk++] = bi;  // a lone leaf becomes a one-child wide node
+            w.kids[nk++] = bi;  // a lone leaf becomes a one-child wide node
         } else {
-            kids[nk++] = root.first;
-            kids[nk++] = root.first + 1;
+            w.kids[nk++] = root.first;
+            w.kids[nk++] = root.first + 1;
             while (nk < 8) {
                 int best = -1;
                 double best_a = -1.0;
-                for (int k = 0; k < nk; k++) {
-                    const BinNode& c = bin.nodes[kids[k]];
+                for (uint32_t k = 0; k < nk; k++) {
+                    const BinNode& c = bin.nodes[w.kids[k]];
                     if (c.count == 0 && c.b.area() > best_a) {
                         best_a = c.b.area();
-                        best = k;
+                        best = (int)k;
                     }
                 }
                 if (best < 0) break;
-                uint32_t open = kids[best];
-                kids[best] = bin.nodes[open].first;
-                kids[nk++] = bin.nodes[open].first + 1;
+                uint32_t open = w.kids[best];
+                w.kids[best] = bin.nodes[open].first;
+                w.kids[nk++] = bin.nodes[open].first + 1;
             }
         }
-        uint32_t idx = (uint32_t)(out.size() / WIDE_NODE_WORDS);
+        w.nk = nk;
+        w.idx = (uint32_t)(out.size() / WIDE_NODE_WORDS);
         out.resize(out.size() + WIDE_NODE_WORDS);
         emitted++;
-        uint32_t refs[8];
-        for (int k = 0; k < 8; k++) refs[k] = REF_EMPTY;
-        for (int k = 0; k < nk; k++) {
-            const BinNode& c = bin.nodes[kids[k]];
-            refs[k] = c.count > 0 ? leaf_ref(c) : emit(kids[k]);
+        const size_t slot = wide.size();
+        wide.push_back(w);
+        for (int k = 0; k < 8; k++) wide[slot].refs[k] = REF_EMPTY;
+        for (uint32_t k = 0; k < nk; k++) {
+            const BinNode& c = bin.nodes[wide[slot].kids[k]];
+            uint32_t r = c.count > 0 ? leaf_ref(c) : emit(wide[slot].kids[k]);
+            wide[slot].refs[k] = r;
         }
+        return w.idx;
+    }
+
+    void finish() {
+        std::atomic<uint64_t> errors{0};
+        parallel_for(wide.size(), [&](size_t w0, size_t w1) {
+            uint64_t local_errors = 0;
+            for (size_t wi = w0; wi < w1; wi++) local_errors += write(wide[wi]);
+            errors += local_errors;
+        }, 2048);
+        decode_errors += errors.load();
+    }
+
+    // Quantise one wide node's child boxes and write its 6 words; returns the
+    // number of decode checks that failed.
+    uint64_t write(const Wide& wn) {
+        const uint32_t nk = wn.nk;
+        uint64_t errors = 0;
         // Node box = union of children boxes.
         Box nb;
-        for (int k = 0; k < nk; k++) nb.grow(bin.nodes[kids[k]].b);
+        for (uint32_t k = 0; k < nk; k++) nb.grow(bin.nodes[wn.kids[k]].b);
         float p[3];
         int e[3];
         double sc[3];
@@ -330,8 +454,8 @@ struct Collapser {
                 qlo[a][k] = 255;
                 qhi[a][k] = 0;
             }
-        for (int k = 0; k < nk; k++) {
-            const Box& cbx = bin.nodes[kids[k]].b;
+        for (uint32_t k = 0; k < nk; k++) {
+            const Box& cbx = bin.nodes[wn.kids[k]].b;
             for (int a = 0; a < 3; a++) {
                 const double s = sc[a];
                 double ql = std::floor((cbx.lo[a] - (double)p[a]) / s);
@@ -350,10 +474,10 @@ struct Collapser {
                 float dhi = std::fmaf(8388608.0f + (float)qh, sf, p2);
                 if ((double)dlo != (double)p[a] + ql * s || (double)dhi != (double)p[a] + qh * s ||
                     (double)dlo > cbx.lo[a] || (double)dhi < cbx.hi[a])
-                    decode_errors++;
+                    errors++;
             }
         }
-        uint4* w = &out[(size_t)idx * WIDE_NODE_WORDS];
+        uint4* w = &out[(size_t)wn.idx * WIDE_NODE_WORDS];
         uint32_t pb[3];
         memcpy(pb, p, sizeof(pb));
         w[0] = make_uint4(pb[0], pb[1], pb[2],
@@ -365,9 +489,9 @@ struct Collapser {
         w[1] = make_uint4(pack4(qlo[0]), pack4(qlo[0] + 4), pack4(qlo[1]), pack4(qlo[1] + 4));
         w[2] = make_uint4(pack4(qlo[2]), pack4(qlo[2] + 4), pack4(qhi[0]), pack4(qhi[0] + 4));
         w[3] = make_uint4(pack4(qhi[1]), pack4(qhi[1] + 4), pack4(qhi[2]), pack4(qhi[2] + 4));
-        w[4] = make_uint4(refs[0], refs[1], refs[2], refs[3]);
-        w[5] = make_uint4(refs[4], refs[5], refs[6], refs[7]);
-        return idx;
+        w[4] = make_uint4(wn.refs[0], wn.refs[1], wn.refs[2], wn.refs[3]);
+        w[5] = make_uint4(wn.refs[4], wn.refs[5], wn.refs[6], wn.refs[7]);
+        return errors;
     }
 };
 
@@ -622,6 +746,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
         Collapser col{bin, H.nodes, mi.tri_base};
         H.nodes.reserve(H.nodes.size() + WIDE_NODE_WORDS * (bin.nodes.size() / 4 + 1));
         mi.blas_root = col.emit(0);
+        col.finish();
         H.blas_nodes += col.emitted;
         if (col.decode_errors) {
             *err = "internal: quantised BLAS boxes not conservative";
@@ -675,6 +800,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
         BinBvh tl = build_binary(ib);
         Collapser col{tl, H.nodes, 0};
         H.scalars.tlas_root = col.emit(0);
+        col.finish();
         H.tlas_nodes = col.emitted;
         if (col.decode_errors) {
             *err = "internal: quantised TLAS boxes not conservative";

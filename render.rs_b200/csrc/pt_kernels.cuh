@@ -1008,6 +1008,17 @@ __global__ void k_accumulate(Paths P, PtConsts C, uint32_t samples_in_slab, doub
     st[2] += (double)taken;
 }
 
+// ---- image: radiance sums / sample weight, f64 division rounded to f32 -------------------
+__global__ void k_resolve(const double* __restrict__ accum, float* __restrict__ rgb, uint32_t npix) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    const double4 a = reinterpret_cast<const double4*>(accum)[i];
+    const double w = a.w > 0.0 ? a.w : 1.0;
+    rgb[3 * (size_t)i] = (float)(a.x / w);
+    rgb[3 * (size_t)i + 1] = (float)(a.y / w);
+    rgb[3 * (size_t)i + 2] = (float)(a.z / w);
+}
+
 // ---- ray batch (rt_intersect_batch) ------------------------------------------------------
 template <int BLOCK, bool ANY>
 __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_intersect(DevScene S, const float4* __restrict__ org,

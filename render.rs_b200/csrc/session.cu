@@ -474,13 +474,13 @@ int rt_read_accum(rt_session* s, double* rgbw) {
 
 int rt_read_image(rt_session* s, float* rgb) {
     if (!s || !rgb) return fail(RT_ERR_INVALID, "NULL argument");
-    std::vector<double> a(4ull * s->npix);
-    int rc = rt_read_accum(s, a.data());
-    if (rc) return rc;
-    for (uint64_t i = 0; i < s->npix; i++) {
-        double w = a[4 * i + 3] > 0 ? a[4 * i + 3] : 1.0;
-        for (int c = 0; c < 3; c++) rgb[3 * i + c] = (float)(a[4 * i + c] / w);
-    }
+    // Resolve on the device into the shadow-ray origin buffer (free between
+    // renders; at least 16 B per pixel), then copy 12 B per pixel.
+    float* img = reinterpret_cast<float*>(s->paths.sh_o);
+    k_resolve<<<(s->npix + 255) / 256, 256, 0, s->stream>>>(s->accum, img, s->npix);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(rgb, img, 12ull * s->npix, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
     return RT_OK;
 }
 
