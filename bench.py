@@ -19,6 +19,8 @@ Printed (one JSON line on rank 0):
   cpu_baseline  the f64 oracle (C++ restatement of the reference's CPU path
              tracer, all host threads) on a bounded pixel sample of the frame.
   traversal  the 4,194,304-ray closest-hit and any-hit batches (Mrays/s).
+  workloads  device Msamples/s and Mrays/s of the other named scenes
+             (Cornell box, instanced materials, forest) at their sizes.
   guided_equal_time  the learned-proposal workload: two 4x3x3 rooms joined by
              a 0.2x2.0 opening, the light in the unseen room, 1280x720, max
              depth 16. A fresh guided session renders GUIDED_SPP passes from
@@ -206,6 +208,35 @@ def guided_equal_time(ref_spp=4096, cpu_pixels=256, cpu_spp=16384):
     return out
 
 
+def other_workloads(forest_spp=4):
+    """Device throughput of the other named scenes at their configured size:
+    Cornell box 256^2 x 16 spp (depth 8), instanced materials 1920x1080 x 64
+    spp (depth 12), forest 3840x2160 (depth 10; `forest_spp` of its 32 passes,
+    to keep the run short). One warm-up pass, then one timed render call
+    (device time from the session's events); scene build time excluded."""
+    from rtcuda import PtSession, abi, scenes
+    out = {}
+    cases = [("cornell_256x256_16spp_depth8", lambda: scenes.cornell_box(), scenes.CORNELL, 16),
+             ("instanced_materials_1920x1080_64spp_depth12", lambda: scenes.instanced_materials(),
+              scenes.INSTANCED_MATERIALS, 64),
+             (f"forest_3840x2160_depth10_{forest_spp}of32spp", lambda: scenes.forest(), scenes.FOREST, forest_spp)]
+    for name, make, cfg, spp in cases:
+        t0 = time.perf_counter()
+        s = make()
+        p = abi.make_params(max_depth=cfg["max_depth"], rr_start=cfg["rr_start"])
+        with PtSession(s, p) as g:
+            build_s = time.perf_counter() - t0
+            g.render_samples(1 << 20, 1)
+            g.render_samples(0, spp)
+            st = g.stats()
+        ms = st["total_ms"]
+        out[name] = {"Msamples_per_s": st["samples"] / ms / 1e3, "ms": round(ms, 2), "spp": spp,
+                     "Mrays_per_s": (st["extension_rays"] + st["shadow_rays"]) / ms / 1e3,
+                     "triangles_effective": s.triangle_count() if hasattr(s, "triangle_count") else None,
+                     "instances": getattr(s, "n_instances", None), "build_and_upload_s": round(build_s, 2)}
+    return out
+
+
 def run_reference(args):
     """Reference arm: the reference's CPU path (f64 restatement) on host cores."""
     rank = int(os.environ.get("RANK", "0"))
@@ -301,6 +332,7 @@ def main():
                          "workload (both for profiler captures)")
     ap.add_argument("--rays", type=int, default=N_RAYS)
     ap.add_argument("--no-guided", action="store_true", help="skip the guided equal-time comparison")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the other scenes' throughput")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -435,6 +467,9 @@ def main():
         guided = None
         if not args.no_guided and world == 1:
             guided = guided_equal_time()
+        workloads = None
+        if not args.no_workloads and world == 1:
+            workloads = other_workloads()
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -450,6 +485,7 @@ def main():
             "traversal": trav,
             "rays_per_step": {"extension": last["extension_rays"], "shadow": last["shadow_rays"]},
             "guided_equal_time": guided,
+            "workloads": workloads,
             "Mrays_per_s": (last["extension_rays"] + last["shadow_rays"]) / (last["total_ms"] / 1e3) / 1e6,
         }
         print(json.dumps(result), flush=True)

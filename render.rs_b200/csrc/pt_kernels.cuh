@@ -387,7 +387,7 @@ __global__ void k_guide_keep(const uint32_t* tb_cnt, float scale, uint32_t cap, 
 // has no parked leaf tests nodes until it parks one or finishes) and a leaf
 // phase (every lane with a parked leaf processes it), so lanes mostly run
 // the same code path.
-template <bool ANY, class Load, class Finish>
+template <bool ANY, bool TRANSMIT = false, class Load, class Finish>
 __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                          TravStack& st, LeafShared& leaf, Load load, Finish finish) {
     PhaseState ps;
@@ -449,7 +449,7 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
         bool done_now = false;
         if (active && ps.pending && !ps.ts.in_inst) done_now = op_leaf<ANY>(S, ps, st, err);
         const bool tri_leaf = active && !done_now && ps.pending && ps.ts.in_inst;
-        if (__any_sync(0xFFFFFFFFu, tri_leaf)) done_now |= leaf_coop<ANY>(S, ps, tri_leaf, leaf);
+        if (__any_sync(0xFFFFFFFFu, tri_leaf)) done_now |= leaf_coop<ANY, TRANSMIT>(S, ps, tri_leaf, leaf);
         if (__any_sync(0xFFFFFFFFu, done_now)) finish(done_now, item, ps.ts);
         if (done_now) active = false;
     }
@@ -863,11 +863,9 @@ template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S, Paths P, PtConsts C) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
     __shared__ LeafShared leaf_sh[BLOCK / 32];
-    __shared__ uint32_t warp_base[BLOCK / 32];
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
     uint32_t n = P.cnt[CNT_SHADOW];
-    uint32_t w = threadIdx.x >> 5;
     unsigned long long rays = 0;
     auto add = [&](uint32_t slot, float vis) {
         float4 c = P.sh_c[slot];
@@ -897,54 +895,23 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
         if (rays) atomicAdd(&P.stats[1], rays);
         return;
     }
-    for (;;) {
-        if (lane_id() == 0) warp_base[w] = atomicAdd(&P.cnt[CNT_FETCH_SH], 32u);
-        __syncwarp();
-        uint32_t base = warp_base[w];
-        __syncwarp();
-        if (base >= n) break;
-        uint32_t j = base + lane_id();
-        if (j >= n) continue;
-        uint32_t slot = P.q_sh[j];
+    // Scenes with presence cutouts: transmittance queries through the pump
+    // (traverse.cuh: one traversal per shadow ray, cutouts attenuate, opaque
+    // surfaces block).
+    uint32_t slot = 0;
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
+        slot = P.q_sh[j];
         float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
-        float3 o = xyz(o4), d = xyz(d4);
-        float remaining = d4.w;
-        float vis = 1.0f;
-        if (!S.any_presence) {
-            TraceHit h;
-            rays++;
-            if (trace<true>(S, o, d, remaining, h, st, P.err)) vis = 0.0f;
-        } else {
-            // transmittance (mod.rs:1254-1306): closest-hit segments, cutouts
-            // attenuate by (1 - presence), opaque surfaces block.
-            for (uint32_t k = 0; k < RT_MAX_PRESENCE_SKIPS; k++) {
-                TraceHit h;
-                rays++;
-                if (!trace<false>(S, o, d, remaining, h, st, P.err)) break;
-                float pr = S.materials[__ldg(&S.inst[h.inst].z)].presence;
-                if (pr >= 1.0f) {
-                    vis = 0.0f;
-                    break;
-                }
-                vis *= 1.0f - pr;
-                if (vis < 1e-4f) {
-                    vis = 0.0f;
-                    break;
-                }
-                o = o + d * h.t + d * RT_RAY_OFFSET;
-                remaining -= h.t + RT_RAY_OFFSET;
-            }
-        }
-        if (vis > 0.0f) {
-            float4 c = P.sh_c[slot];
-            float4 L = P.L[slot];
-            P.L[slot] = make_float4(L.x + c.x * vis, L.y + c.y * vis, L.z + c.z * vis, L.w);
-            if (C.aovs && c.w != 0.0f) {
-                float4 a = P.aux_d[slot];
-                P.aux_d[slot] = make_float4(a.x + c.x * vis, a.y + c.y * vis, a.z + c.z * vis, a.w);
-            }
-        }
-    }
+        o = xyz(o4);
+        d = xyz(d4);
+        tmax = d4.w;
+    };
+    auto finish = [&](bool done, uint32_t, const TravState& ts) {
+        if (!done) return;
+        rays++;
+        if (ts.trans > 0.0f) add(slot, ts.trans);
+    };
+    ray_pump<true, true>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
     if (rays) atomicAdd(&P.stats[1], rays);
 }
 

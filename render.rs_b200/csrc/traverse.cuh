@@ -260,6 +260,7 @@ struct TravState {
     uint32_t steps;
     int inst_sp;
     bool in_inst, found;
+    float trans;       // shadow transmittance (TRANSMIT queries)
 };
 
 // Start a closest-hit / any-hit query; false when the scene is empty.
@@ -276,6 +277,7 @@ __device__ __forceinline__ bool trav_begin(const DevScene& S, TravState& ts, Tra
     ts.inst_sp = 0;
     ts.cur_inst = 0;
     ts.steps = 0;
+    ts.trans = 1.0f;
     st.sp = 0;
     st.base = 0;
     st.overflow = false;
@@ -549,12 +551,24 @@ __device__ __forceinline__ bool op_leaf(const DevScene& S, PhaseState& ps, TravS
 struct LeafShared {
     unsigned long long key[32];  // best (t bits << 32 | triangle) per owner lane
     float2 bary[32];             // barycentrics of that triangle
+    float trans[32];             // TRANSMIT: transmittance of this leaf's hits per owner
     uint16_t item[512];          // pool item -> (owner lane << 4) | index in its leaf
 };
 
+// Shadow transmittance (TRANSMIT): the reference walks a shadow ray's
+// blockers in distance order, multiplying by (1 - presence) per cutout,
+// returning zero at an opaque surface or once the product falls below 1e-4,
+// for at most 16 segments (src/raytracer/pt/mod.rs:1241-1306). The product
+// does not depend on the order, so here one traversal visits every surface
+// the segment crosses (no t_max shrinking, like any-hit) and multiplies the
+// factors, ending the query at an opaque hit or below 1e-4. The answers agree
+// whenever the product falls below 1e-4 within 16 cutouts or fewer than 17
+// are crossed, e.g. for every presence >= 0.44.
+#define RT_TRANSMIT_CUTOFF 1e-4f
+
 // `mine`: this lane's parked leaf is a triangle leaf to test. Returns true
 // when an any-hit query found a hit (the query is over).
-template <bool ANY>
+template <bool ANY, bool TRANSMIT = false>
 __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, bool mine, LeafShared& L) {
     const uint32_t lane = threadIdx.x & 31u;
     TravState& ts = ps.ts;
@@ -574,6 +588,10 @@ __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, boo
     const uint32_t excl = incl - count, total = __shfl_sync(0xFFFFFFFFu, incl, 31);
     for (uint32_t k = 0; k < count; k++) L.item[excl + k] = (uint16_t)((lane << 4) | k);
     L.key[lane] = ~0ull;
+    L.trans[lane] = 1.0f;
+    // TRANSMIT: the presence of the material of this lane's instance.
+    const float pres_own =
+        (TRANSMIT && mine) ? __ldg(&S.materials[__ldg(&S.inst[ts.cur_inst].z)].presence) : 1.0f;
     __syncwarp();
     // This lane's ray, as the owners of pool items read it.
     const float tmax_own = ts.hit.t;
@@ -596,24 +614,60 @@ __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, boo
         r.kx = (int)(kp & 3u);
         r.ky = (int)((kp >> 2) & 3u);
         r.kz = (int)((kp >> 4) & 3u);
+        const float pres = __shfl_sync(0xFFFFFFFFu, pres_own, owner);
         float t = 0.0f, b1 = 0.0f, b2 = 0.0f;
         unsigned long long key = ~0ull;
+        float factor = 1.0f;
         if (has) {
             const unsigned long long best = L.key[owner];
             // Cull with the best hit so far, keeping hits at equal t (they
             // compete on the triangle index).
-            if (best != ~0ull) tmax = fminf(tmax, nextafterf(__uint_as_float((uint32_t)(best >> 32)), INFINITY));
+            if (!TRANSMIT && best != ~0ull)
+                tmax = fminf(tmax, nextafterf(__uint_as_float((uint32_t)(best >> 32)), INFINITY));
             const uint32_t tri = f + (it & 15u);
             const float4* tp = S.tris + 3 * (size_t)tri;
             float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
             if (tri_watertight(r, xyz(a), xyz(b), xyz(c), tmax, t, b1, b2)) {
-                key = ((unsigned long long)__float_as_uint(t) << 32) | tri;
-                atomicMin(&L.key[owner], key);
+                if (TRANSMIT) {
+                    factor = pres >= 1.0f ? 0.0f : 1.0f - pres;
+                } else {
+                    key = ((unsigned long long)__float_as_uint(t) << 32) | tri;
+                    atomicMin(&L.key[owner], key);
+                }
+            }
+        }
+        if (TRANSMIT) {
+            // Pool items of one owner are consecutive lanes: a segmented
+            // product scan (fixed order, so results are reproducible) leaves
+            // each run's product on its last lane.
+            const uint32_t seg = has ? owner : 32u + lane;
+            float prod = factor;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const float v = __shfl_up_sync(0xFFFFFFFFu, prod, off);
+                const uint32_t so = __shfl_up_sync(0xFFFFFFFFu, seg, off);
+                if (lane >= (uint32_t)off && so == seg) prod *= v;
+            }
+            const uint32_t next_seg = __shfl_down_sync(0xFFFFFFFFu, seg, 1);
+            if (has && (lane == 31u || next_seg != seg)) L.trans[owner] *= prod;
+            __syncwarp();
+        } else {
+            __syncwarp();
+            if (key != ~0ull && L.key[owner] == key) L.bary[owner] = make_float2(b1, b2);
+            __syncwarp();
+        }
+    }
+    if (TRANSMIT) {
+        bool over = false;
+        if (mine) {
+            ts.trans *= L.trans[lane];
+            if (!(ts.trans >= RT_TRANSMIT_CUTOFF)) {
+                ts.trans = 0.0f;
+                over = true;
             }
         }
         __syncwarp();
-        if (key != ~0ull && L.key[owner] == key) L.bary[owner] = make_float2(b1, b2);
-        __syncwarp();
+        return over;
     }
     bool hit_now = false;
     if (mine) {
