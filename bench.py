@@ -145,7 +145,7 @@ def cpu_baseline_sample(scene, params, threads=0, target_s=12.0):
     return samples / el / 1e6, f"{len(pixels)} pixels (every {stride}th) x {SPP} spp of the frame", cores, work, el
 
 
-GUIDED_W, GUIDED_H, GUIDED_SPP, GUIDED_DEPTH = 1280, 720, 256, 16
+GUIDED_W, GUIDED_H, GUIDED_SPP, GUIDED_DEPTH = 1280, 720, 1024, 16
 
 # DRAM bytes (read + write) per k_extend launch, averaged over the 32 launches
 # of one render step, from one ncu capture of this command (1 pass):
@@ -160,15 +160,22 @@ def rel_mse(img, ref):
     return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
 
 
-def guided_equal_time(ref_spp=4096, cpu_pixels=256, cpu_spp=16384):
-    """Equal-time relMSE of guided vs plain path tracing on the two-room scene."""
+def guided_equal_time(ref_spp=8192, cpu_pixels=256, cpu_spp=16384):
+    """Equal-time relMSE of guided vs plain path tracing on the two-room scene.
+    The GPU reference is the mean of two independent halves A and B; its own
+    error, mean((A - B)^2 / (ref^2 + 1e-2)) / 4, is reported and subtracted
+    in the `*_corrected` figures (it adds to both estimators' relMSE)."""
     from rtcuda import PtSession, abi, scenes
     s = scenes.two_rooms(GUIDED_W, GUIDED_H)
     plain_p = abi.make_params(max_depth=GUIDED_DEPTH)
     guided_p = abi.make_params(max_depth=GUIDED_DEPTH, guided=True, guide_fraction=0.5)
-    with PtSession(s, plain_p) as g:                       # high-spp GPU reference
-        g.render_samples(1 << 24, ref_spp)
-        ref = g.image()
+    halves = []
+    for h in range(2):                                     # high-spp GPU reference, two halves
+        with PtSession(s, plain_p) as g:
+            g.render_samples((1 << 24) + h * ref_spp, ref_spp // 2)
+            halves.append(g.image())
+    ref = 0.5 * (halves[0] + halves[1])
+    ref_err = float(np.mean((halves[0] - halves[1]) ** 2 / (ref ** 2 + 1e-2))) / 4.0
     with PtSession(s, guided_p) as g:                      # warm-up of the code paths only
         g.render_samples(1 << 23, 2)
     with PtSession(s, guided_p) as g:
@@ -189,7 +196,10 @@ def guided_equal_time(ref_spp=4096, cpu_pixels=256, cpu_spp=16384):
            "plain_ms": round(plain_ms, 2), "plain_ms_per_spp": round(per_spp, 4),
            "gpu_reference_spp": ref_spp}
     e_p, e_g = rel_mse(plain, ref), rel_mse(guided, ref)
-    out.update({"relmse_plain_vs_gpu_ref": e_p, "relmse_guided_vs_gpu_ref": e_g, "ratio_vs_gpu_ref": e_p / e_g})
+    out.update({"relmse_plain_vs_gpu_ref": e_p, "relmse_guided_vs_gpu_ref": e_g, "ratio_vs_gpu_ref": e_p / e_g,
+                "gpu_ref_relmse": ref_err, "relmse_plain_corrected": e_p - ref_err,
+                "relmse_guided_corrected": e_g - ref_err, "ratio_corrected": (e_p - ref_err) / (e_g - ref_err),
+                "guide_steps_per_pass": st["guide_steps"] / GUIDED_SPP})
     try:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle  # test infrastructure: the f64 reference pixels
