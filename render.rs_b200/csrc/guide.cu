@@ -238,9 +238,14 @@ __global__ void __launch_bounds__(FWD_THREADS, 3) k_guide_fwd(GuideDev G, const 
 
 // ---- backward -----------------------------------------------------------------
 // Shared memory: WT0 [48][64] 6144 | WT1 8192 | WT2 8192 | WT3 [64][48] 6144 |
-//                DZ [128][64] 16384 | DZT [128][128] 32768 | HT [64][128] 16384
+//                DZ [128][64] 16384 | DZT [128][128] 32768 | HT [80][128] 20480
+// HT holds the layer input transposed plus one row of ones and zero rows up
+// to K_in + 16: the dW GEMM then also yields column K_in = sum over the batch
+// of dZ, the bias gradient (no per-neuron warp reductions).
+// TMEM: dW (and the bias column) in columns [0, 80), dH in [128, 192).
 constexpr int B_WT0 = 0, B_WT1 = 6144, B_WT2 = B_WT1 + 8192, B_WT3 = B_WT2 + 8192, B_DZ = B_WT3 + 6144,
-              B_DZT = B_DZ + 16384, B_HT = B_DZT + 32768, B_BYTES = B_HT + 16384;
+              B_DZT = B_DZ + 16384, B_HT = B_DZT + 32768, B_BYTES = B_HT + 20480;
+constexpr uint32_t B_TMEM_DH = 128;
 
 __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloat16* __restrict__ X0,
                                                     const __nv_bfloat16* __restrict__ acts,
@@ -254,7 +259,6 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
     extern __shared__ __align__(1024) uint8_t sm[];
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
-    __shared__ float gbias[G_HID];
     __shared__ float red[TILE / 32];
     const int tid = threadIdx.x, warp = tid >> 5;
     for (int l = 0; l < 4; l++) {
@@ -262,7 +266,10 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
         stage_transpose(sm + dst, G.w + w_off(l), l_out(l), l_in(l));
     }
     for (int i = tid; i < 32768 / 16; i += TILE) reinterpret_cast<uint4*>(sm + B_DZT)[i] = make_uint4(0, 0, 0, 0);
-    if (warp == 0) tmem_alloc(&tmem_base, 128);
+    // HT rows 64..79 (layers with K_in = 64): a row of ones, then zeros.
+    for (int k = 64; k < 80; k++)
+        *reinterpret_cast<__nv_bfloat16*>(sm + B_HT + core_offset(k, tid, TILE)) = __float2bfloat16_rn(k == 64 ? 1.f : 0.f);
+    if (warp == 0) tmem_alloc(&tmem_base, 256);
     if (tid == 0) mbar_init(&mbar, 1);
     tc_fence_before();
     __syncthreads();
@@ -307,17 +314,6 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
 #pragma unroll
             for (int k = 0; k < 64; k++)
                 if (k < N_out) *reinterpret_cast<__nv_bfloat16*>(sm + B_DZT + core_offset(k, tid, TILE)) = __float2bfloat16_rn(dz[k]);
-            // Bias gradient: column sums of dZ over the tile.
-            if (tid < G_HID) gbias[tid] = 0.f;
-            __syncthreads();
-#pragma unroll
-            for (int k = 0; k < 64; k++)
-                if (k < N_out) {
-                    float s = dz[k];
-#pragma unroll
-                    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, off);
-                    if ((tid & 31) == 0) atomicAdd(&gbias[k], s);
-                }
             // Layer input H (rows of this tile) -> registers and H^T operand.
             float h[64];
             if (l > 0) {
@@ -349,19 +345,23 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
                     }
                 }
             }
+            // H^T rows 0..K_in-1, then (layer 0) a row of ones and zeros up to
+            // row 63; for K_in = 64 the ones row 64 and zeros were set up front.
 #pragma unroll
-            for (int k = 0; k < 64; k++)
-                if (k < K_in) *reinterpret_cast<__nv_bfloat16*>(sm + B_HT + core_offset(k, tid, TILE)) = __float2bfloat16_rn(h[k]);
+            for (int k = 0; k < 64; k++) {
+                const float hv = k < K_in ? h[k] : (k == K_in ? 1.f : 0.f);
+                *reinterpret_cast<__nv_bfloat16*>(sm + B_HT + core_offset(k, tid, TILE)) = __float2bfloat16_rn(hv);
+            }
             fence_proxy_async_smem();
             __syncthreads();
-            if (tid < N_out) atomicAdd(&gb[b_off(l) + tid], gbias[tid]);
             if (tid == 0) {
                 tc_fence_after();
-                // dW[n][k] = sum_m dZ[m][n] H[m][k]  (M = 128 padded neurons, N = K_in, K = batch)
-                tc_gemm_issue(tb, s0 + B_DZT, s0 + B_HT, K_in, TILE, false);
+                // dW[n][k] = sum_m dZ[m][n] H[m][k]  (M = 128 padded neurons, N = K_in + 16, K = batch);
+                // column K_in is the bias gradient.
+                tc_gemm_issue(tb, s0 + B_DZT, s0 + B_HT, K_in + 16, TILE, false);
                 // dH[m][k] = sum_n dZ[m][n] W[n][k]  (N = K_in, K = N_out)
                 const uint32_t wt = l == 0 ? B_WT0 : l == 1 ? B_WT1 : l == 2 ? B_WT2 : B_WT3;
-                tc_gemm_issue(tb + 64, s0 + B_DZ, s0 + wt, K_in, N_out, false);
+                tc_gemm_issue(tb + B_TMEM_DH, s0 + B_DZ, s0 + wt, K_in, N_out, false);
                 tc_commit(&mbar);
             }
             bool ok = mbar_wait_bounded(&mbar, phase);
@@ -371,19 +371,21 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
                 break;
             }
             tc_fence_after();
-            float v[64];
+            float v[64], vb[16];
 #pragma unroll
             for (int c = 0; c < 4; c++)
                 if (c * 16 < K_in) tmem_ld16(lane_addr + c * 16, v + 16 * c);
+            tmem_ld16(lane_addr + K_in, vb);
             if (tid < N_out) {
                 float* g = gW + w_off(l) + (size_t)tid * K_in;
 #pragma unroll
                 for (int k = 0; k < 64; k++)
                     if (k < K_in) atomicAdd(g + k, v[k]);
+                atomicAdd(&gb[b_off(l) + tid], vb[0]);
             }
 #pragma unroll
             for (int c = 0; c < 4; c++)
-                if (c * 16 < K_in) tmem_ld16(lane_addr + 64 + c * 16, v + 16 * c);
+                if (c * 16 < K_in) tmem_ld16(lane_addr + B_TMEM_DH + c * 16, v + 16 * c);
             if (l > 0) {
 #pragma unroll
                 for (int k = 0; k < 64; k++) dz[k] = h[k] > 0.f ? v[k] : 0.f;
@@ -403,7 +405,7 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
     if (tid == 0) atomicAdd(loss_sum, red[0] + red[1] + red[2] + red[3]);
     if (failed && tid == 0) atomicOr(err, GERR_WAIT);
     if (warp == 0) {
-        tmem_dealloc(tb, 128);
+        tmem_dealloc(tb, 256);
         tmem_relinquish();
     }
 }
