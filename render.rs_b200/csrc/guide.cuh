@@ -214,6 +214,51 @@ __device__ __forceinline__ float3 mixture_sample(const Mixture& m, float u0, flo
     return normalize_ref(a * (sr * c) + b * (sr * s) + mu * wz);
 }
 
+// The renderer's view of a decoded mixture: read in place from its record
+// (global memory, L1-resident after the first touch) instead of copying its
+// 48 floats into per-thread storage, which spilled to local memory and held
+// registers through the whole shade.
+struct MixtureRef {
+    const float4* p;  // 12 float4: 8 x (mu.xyz, kappa), weights (2), A (2)
+};
+
+__device__ __forceinline__ float mixture_pdf(const MixtureRef& m, float3 w) {
+    const float4 a0 = m.p[10], a1 = m.p[11];
+    const float A[G_LOBES] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    float p = 0.f;
+#pragma unroll
+    for (int j = 0; j < G_LOBES; j++) {
+        const float4 l = m.p[j];
+        p += __expf(A[j] + l.w * dot(f3(l.x, l.y, l.z), w));
+    }
+    return p;
+}
+
+__device__ __forceinline__ float3 mixture_sample(const MixtureRef& m, float u0, float u1, float u2) {
+    const float4 w0 = m.p[8], w1 = m.p[9];
+    const float wt[G_LOBES] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    int j = G_LOBES - 1;
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < G_LOBES; k++) {
+        acc += wt[k];
+        if (u0 < acc) {
+            j = k;
+            break;
+        }
+    }
+    const float4 l = m.p[j];
+    const float kappa = l.w;
+    const float3 mu = f3(l.x, l.y, l.z);
+    float wz = 1.f + logf(u1 + (1.f - u1) * __expf(-2.f * kappa)) / kappa;
+    wz = fminf(fmaxf(wz, -1.f), 1.f);
+    float sr = sqrtf(fmaxf(1.f - wz * wz, 0.f)), s, c;
+    sincosf(2.f * RT_PI * u2, &s, &c);
+    float3 t = fabsf(mu.x) > 0.9f ? f3(0, 1, 0) : f3(1, 0, 0);
+    float3 a = normalize_ref(cross(mu, t)), b = cross(mu, a);
+    return normalize_ref(a * (sr * c) + b * (sr * s) + mu * wz);
+}
+
 // Loss -weight * log q(w) for raw outputs o; writes d loss / d o into g (40 used).
 __device__ __forceinline__ float mixture_loss_grad(const float* o, float3 w, float weight, float* g) {
     float mx = -1e30f;

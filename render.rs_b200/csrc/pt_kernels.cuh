@@ -341,7 +341,9 @@ __global__ void k_guide_collect(Paths P, PtConsts C) {
     const float keep = *P.tr_keep;
     const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t slot = (uint32_t)(id / C.max_depth), d = (uint32_t)(id % C.max_depth);
-    bool cand = false;
+    bool cand = false, kept = false;
+    float wt = 0.0f;
+    const float* rec = nullptr;
     if (slot < P.P && d < (__float_as_uint(P.prev[slot].w) >> FL_DEPTH_SHIFT)) {
         const float* r = P.tr_rec + ((size_t)slot * C.max_depth + d) * TR_FLOATS;
         float2 tags = *reinterpret_cast<const float2*>(r + 18);
@@ -351,17 +353,29 @@ __global__ void k_guide_collect(Paths P, PtConsts C) {
             float w = luminance(dl) / fmaxf(luminance(f3(r[12], r[13], r[14])), 1e-8f);
             cand = w > 0.0f && isfinite(w);
             uint32_t h = hash32((slot * C.max_depth + d) ^ hash32(P.tr_tag));
-            if (cand && (float)(h >> 8) * (1.0f / 16777216.0f) < keep) {
-                uint32_t idx = atomicAdd(P.tb_cnt, 1u);
-                if (idx < P.tb_cap) {
-                    float4* o = reinterpret_cast<float4*>(P.tb_rec + (size_t)idx * 16);
-                    const float4* ri = reinterpret_cast<const float4*>(r);
-                    o[0] = ri[0];
-                    o[1] = ri[1];
-                    o[2] = ri[2];
-                    o[3] = make_float4(fminf(w, 50.0f), 0.0f, 0.0f, 0.0f);
-                }
-            }
+            kept = cand && (float)(h >> 8) * (1.0f / 16777216.0f) < keep;
+            wt = w;
+            rec = r;
+        }
+    }
+    // Warp-aggregated appends: one atomic per warp for the kept records and
+    // one for the candidate count.
+    const uint32_t km = __ballot_sync(0xFFFFFFFFu, kept);
+    uint32_t base = 0;
+    if (km) {
+        const uint32_t leader = __ffs(km) - 1;
+        if (lane_id() == leader) base = atomicAdd(P.tb_cnt, (uint32_t)__popc(km));
+        base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    }
+    if (kept) {
+        const uint32_t idx = base + __popc(km & ((1u << lane_id()) - 1u));
+        if (idx < P.tb_cap) {
+            float4* o = reinterpret_cast<float4*>(P.tb_rec + (size_t)idx * 16);
+            const float4* ri = reinterpret_cast<const float4*>(rec);
+            o[0] = ri[0];
+            o[1] = ri[1];
+            o[2] = ri[2];
+            o[3] = make_float4(fminf(wt, 50.0f), 0.0f, 0.0f, 0.0f);
         }
     }
     uint32_t m = __ballot_sync(0xFFFFFFFFu, cand);
@@ -502,7 +516,7 @@ struct NeeOut {
 // its unoccluded contribution (already divided by the pick pmf).
 __device__ __forceinline__ bool nee_light(const DevScene& S, const DevLight& L, float3 p, float3 n, const Frame& fr,
                                           float3 wo_l, float eta, const DevMaterial& m, float pick, Pcg& rng,
-                                          NeeOut& out, const Mixture* mix = nullptr, float alpha = 0.0f) {
+                                          NeeOut& out, const MixtureRef* mix = nullptr, float alpha = 0.0f) {
     float3 Le = f3(L.radiance[0], L.radiance[1], L.radiance[2]);
     // BSDF value with cosine, and the pdf of the direction-sampling strategy
     // it is MIS-weighted against: the BSDF pdf, or under guiding the one-sample
@@ -627,7 +641,10 @@ __device__ __forceinline__ float light_pdf_sa(const DevLight& L, float3 origin, 
     return 0.0f;
 }
 
-__global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, uint32_t qout) {
+#ifndef RT_SHADE_MIN_BLOCKS
+#define RT_SHADE_MIN_BLOCKS 1
+#endif
+__global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, Paths P, PtConsts C, uint32_t qout) {
     uint32_t counts[N_QUEUES];
     uint32_t total = 0;
 #pragma unroll
@@ -743,12 +760,12 @@ __global__ void __launch_bounds__(128) k_shade(DevScene S, Paths P, PtConsts C, 
                     Frame fr(n);
                     float3 wo_l = fr.to_local(wo);
                     // Learned proposal at this vertex (guided mode only).
-                    Mixture mix;
+                    MixtureRef mix{nullptr};
                     bool guided = false;
                     if (C.guided) {
                         uint32_t gi = P.g_idx[slot];
                         if (gi != 0xFFFFFFFFu) {
-                            mixture_load(P.g_raw + (size_t)gi * G_OUT, mix);
+                            mix.p = reinterpret_cast<const float4*>(P.g_raw + (size_t)gi * G_OUT);
                             guided = true;
                         }
                     }
