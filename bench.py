@@ -145,7 +145,7 @@ def cpu_baseline_sample(scene, params, threads=0, target_s=12.0):
     return samples / el / 1e6, f"{len(pixels)} pixels (every {stride}th) x {SPP} spp of the frame", cores, work, el
 
 
-GUIDED_W, GUIDED_H, GUIDED_SPP, GUIDED_DEPTH = 1280, 720, 1024, 16
+GUIDED_W, GUIDED_H, GUIDED_SPP, GUIDED_DEPTH = 1280, 720, 2048, 16
 
 # DRAM bytes (read + write) per k_extend launch, averaged over the 32 launches
 # of one render step, from one ncu capture of this command (1 pass):
@@ -160,7 +160,7 @@ def rel_mse(img, ref):
     return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
 
 
-def guided_equal_time(ref_spp=8192, cpu_pixels=256, cpu_spp=16384):
+def guided_equal_time(ref_spp=16384, cpu_pixels=256, cpu_spp=16384):
     """Equal-time relMSE of guided vs plain path tracing on the two-room scene.
     The GPU reference is the mean of two independent halves A and B; its own
     error, mean((A - B)^2 / (ref^2 + 1e-2)) / 4, is reported and subtracted

@@ -138,7 +138,7 @@ typedef struct rt_params {
     double   guide_fraction;  /* one-sample MIS fraction drawn from the guide */
     uint64_t max_paths;       /* wavefront slab capacity in paths (0 = auto) */
     double   guide_lr;        /* Adam learning rate of the proposal (0 = 1e-2) */
-    uint32_t guide_steps;     /* Adam steps per sample pass when guided (0 = 2) */
+    uint32_t guide_steps;     /* Adam steps per sample pass when guided (0 = 3) */
     uint32_t guide_depth;     /* guide only vertices of depth < this (0 = all) */
 } rt_params;
 

@@ -124,7 +124,7 @@ def make_params(max_depth=8, rr_start=3, firefly_clamp=60.0, aovs=False, guided=
     """Integrator knobs; defaults follow the reference's constants
     (src/raytracer/pt/mod.rs:26-32) except the bounce cap, which the configs set.
     guide_lr / guide_steps: Adam learning rate and steps per sample pass of the
-    learned proposal (0 = 1e-2 and 2); guide_depth: only vertices of depth
+    learned proposal (0 = 1e-2 and 3); guide_depth: only vertices of depth
     below it use the proposal (0 = every depth)."""
     return RtParams(max_depth, rr_start, firefly_clamp, 1 if aovs else 0, 1 if guided else 0,
                     guide_fraction, max_paths, guide_lr, guide_steps, guide_depth)

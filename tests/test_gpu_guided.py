@@ -57,7 +57,7 @@ def test_guided_is_unbiased_and_reduces_variance(reference):
     with PtSession(s, abi.make_params(max_depth=16)) as g:
         g.render_samples(0, spp)
         plain = g.image()
-    assert st["guide_steps"] == 2 * spp and st["guide_records"] > 100  # 2 Adam steps per pass (default)
+    assert st["guide_steps"] == 3 * spp and st["guide_records"] > 100  # 3 Adam steps per pass (default)
     mr, mi = ref.mean((0, 1)), guided.mean((0, 1))
     assert np.all(np.abs(mr - mi) / np.maximum(mr, 0.02) < 0.03), (mr, mi)
     e_plain, e_guided = rel_mse(plain, ref), rel_mse(guided, ref)
