@@ -160,6 +160,24 @@ def rel_mse(img, ref):
     return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
 
 
+def equal_time_plain(scene, params, budget_ms):
+    """Plain render for the same device time as `budget_ms`: whole slabs at a
+    time (the session's own slab size, so no pass runs in an undersized
+    slab) until the summed device time reaches the budget. Returns (image,
+    passes, device ms)."""
+    from rtcuda import PtSession
+    with PtSession(scene, params) as g:
+        g.render_samples(0, 64)
+        st = g.stats()
+        done, ms = 64, st["total_ms"]
+        slab = max(1, -(-64 // max(1, st["slabs"])))
+        while ms < budget_ms:
+            g.render_samples(done, slab)
+            done += slab
+            ms += g.stats()["total_ms"]
+        return g.image(), done, ms
+
+
 def guided_equal_time(ref_spp=16384, cpu_pixels=256, cpu_spp=16384):
     """Equal-time relMSE of guided vs plain path tracing on the two-room scene.
     The GPU reference is the mean of two independent halves A and B; its own
@@ -183,14 +201,8 @@ def guided_equal_time(ref_spp=16384, cpu_pixels=256, cpu_spp=16384):
         st = g.stats()
         guided_ms = st["total_ms"]
         guided = g.image()
-    with PtSession(s, plain_p) as g:
-        g.render_samples(1 << 22, 32)
-        per_spp = g.stats()["total_ms"] / 32
-        g.reset()
-        plain_spp = max(1, int(round(guided_ms / per_spp)))
-        g.render_samples(0, plain_spp)
-        plain_ms = g.stats()["total_ms"]
-        plain = g.image()
+    plain, plain_spp, plain_ms = equal_time_plain(s, plain_p, guided_ms)
+    per_spp = plain_ms / plain_spp
     out = {"scene": f"two_rooms_{GUIDED_W}x{GUIDED_H}_depth{GUIDED_DEPTH}", "guided_spp": GUIDED_SPP,
            "guided_ms": round(guided_ms, 2), "guide_steps": st["guide_steps"], "plain_spp": plain_spp,
            "plain_ms": round(plain_ms, 2), "plain_ms_per_spp": round(per_spp, 4),
@@ -245,6 +257,39 @@ def other_workloads(forest_spp=4):
                      "triangles_effective": s.triangle_count() if hasattr(s, "triangle_count") else None,
                      "instances": getattr(s, "n_instances", None), "build_and_upload_s": round(build_s, 2)}
     return out
+
+
+def guided_forest(width=480, height=270, budget=128, ref_spp=512):
+    """The large-scale workload's guided-vs-plain comparison, reduced: the
+    forest (772,001 instances, 1,200 point lights, depth 10) at
+    `width` x `height`, `budget` guided passes from an untrained network
+    against plain passes in the same device time, relMSE against a GPU
+    reference of `ref_spp` passes (two halves; its own noise is removed in
+    `ratio_corrected`). The full-size comparison against a 4,096-spp f64 crop
+    is hours of CPU time and is not run."""
+    from rtcuda import PtSession, abi, scenes
+    s = scenes.forest(width, height)
+    cfg = scenes.FOREST
+    plain_p = abi.make_params(max_depth=cfg["max_depth"], rr_start=cfg["rr_start"])
+    guided_p = abi.make_params(max_depth=cfg["max_depth"], rr_start=cfg["rr_start"], guided=True)
+    halves = []
+    for h in range(2):
+        with PtSession(s, plain_p) as g:
+            g.render_samples((1 << 24) + h * ref_spp, ref_spp // 2)
+            halves.append(g.image())
+    ref = 0.5 * (halves[0] + halves[1])
+    ref_err = float(np.mean((halves[0] - halves[1]) ** 2 / (ref ** 2 + 1e-2))) / 4.0
+    with PtSession(s, guided_p) as g:
+        g.render_samples(0, budget)
+        guided_ms = g.stats()["total_ms"]
+        guided = g.image()
+    plain, plain_spp, plain_ms = equal_time_plain(s, plain_p, guided_ms)
+    e_p, e_g = rel_mse(plain, ref), rel_mse(guided, ref)
+    return {"scene": f"forest_{width}x{height}_depth{cfg['max_depth']}", "guided_spp": budget,
+            "guided_ms": round(guided_ms, 1), "plain_spp": plain_spp, "plain_ms": round(plain_ms, 1),
+            "gpu_reference_spp": ref_spp, "relmse_plain": e_p, "relmse_guided": e_g, "ratio": e_p / e_g,
+            "gpu_ref_relmse": ref_err,
+            "ratio_corrected": (e_p - ref_err) / (e_g - ref_err) if e_g > ref_err else None}
 
 
 def run_reference(args):
@@ -480,6 +525,9 @@ def main():
         workloads = None
         if not args.no_workloads and world == 1:
             workloads = other_workloads()
+        forest_guided = None
+        if not args.no_guided and not args.no_workloads and world == 1:
+            forest_guided = guided_forest()
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -496,6 +544,7 @@ def main():
             "rays_per_step": {"extension": last["extension_rays"], "shadow": last["shadow_rays"]},
             "guided_equal_time": guided,
             "workloads": workloads,
+            "guided_forest": forest_guided,
             "Mrays_per_s": (last["extension_rays"] + last["shadow_rays"]) / (last["total_ms"] / 1e3) / 1e6,
         }
         print(json.dumps(result), flush=True)
