@@ -374,6 +374,28 @@ def run_guided(args):
     return 0
 
 
+def run_scene(args):
+    """One named scene alone (for profiler captures): `--scene`, `--res WxH`,
+    `args.warmup` passes in a throwaway call, then `args.steps` passes;
+    one JSON line with the session's device-timed stats."""
+    from rtcuda import PtSession, abi, scenes
+    w, h = (int(v) for v in args.res.split("x"))
+    make = {"cornell": (scenes.cornell_box, scenes.CORNELL), "cloud": (scenes.triangle_cloud, scenes.TRIANGLE_CLOUD),
+            "instanced": (scenes.instanced_materials, scenes.INSTANCED_MATERIALS),
+            "two_rooms": (scenes.two_rooms, scenes.TWO_ROOMS), "forest": (scenes.forest, scenes.FOREST)}
+    gen, cfg = make[args.scene]
+    s = gen(w, h)
+    p = abi.make_params(max_depth=cfg["max_depth"], rr_start=cfg["rr_start"])
+    with PtSession(s, p) as g:
+        if args.warmup:
+            g.render_samples(1 << 20, args.warmup)
+        g.render_samples(0, args.steps)
+        st = g.stats()
+    st["Msamples_per_s"] = st["samples"] / st["total_ms"] / 1e3
+    print(json.dumps({"mode": "scene", "scene": args.scene, "res": args.res, **st}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -382,7 +404,9 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--mode", default="full", choices=["full", "traversal", "guided"],
+    ap.add_argument("--scene", default="forest", help="--mode scene: cornell, cloud, instanced, two_rooms, forest")
+    ap.add_argument("--res", default="640x360", help="--mode scene: frame size WxH")
+    ap.add_argument("--mode", default="full", choices=["full", "traversal", "guided", "scene"],
                     help="traversal: only the closest/any-hit ray batches; guided: only the learned-proposal "
                          "workload (both for profiler captures)")
     ap.add_argument("--rays", type=int, default=N_RAYS)
@@ -395,6 +419,8 @@ def main():
         return run_traversal(args)
     if args.mode == "guided":
         return run_guided(args)
+    if args.mode == "scene":
+        return run_scene(args)
 
     import torch
     import torch.distributed as dist
