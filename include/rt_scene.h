@@ -140,6 +140,8 @@ typedef struct rt_params {
     double   guide_lr;        /* Adam learning rate of the proposal (0 = 1e-2) */
     uint32_t guide_steps;     /* Adam steps per sample pass when guided (0 = 3) */
     uint32_t guide_depth;     /* guide only vertices of depth < this (0 = all) */
+    uint32_t bvh_build;       /* 0 = build the BVHs on the GPU, 1 = on the host (same trees) */
+    uint32_t reserved0;       /* 0 */
 } rt_params;
 
 /* Size checks shared by every consumer of the descriptor. */
@@ -149,7 +151,7 @@ static_assert(sizeof(rt_instance_desc) == 104, "rt_instance_desc layout");
 static_assert(sizeof(rt_material_desc) == 264, "rt_material_desc layout");
 static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
 static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
-static_assert(sizeof(rt_params) == 56, "rt_params layout");
+static_assert(sizeof(rt_params) == 64, "rt_params layout");
 }
 #endif
 

@@ -76,6 +76,19 @@ void parallel_for(size_t n, const std::function<void(size_t, size_t)>& fn, size_
     for (auto& th : pool) th.join();
 }
 
+// A box in f32 for the builders: rounded outward (exact for boxes of f32
+// vertices), with -0 folded into +0 so every comparison-based and key-based
+// min / max agrees.
+void f32_box(const Box& b, float* lo, float* hi) {
+    for (int a = 0; a < 3; a++) {
+        float l = (float)b.lo[a], h = (float)b.hi[a];
+        if ((double)l > b.lo[a]) l = std::nextafter(l, -INFINITY);
+        if ((double)h < b.hi[a]) h = std::nextafter(h, INFINITY);
+        lo[a] = l + 0.0f;
+        hi[a] = h + 0.0f;
+    }
+}
+
 struct BinNode {
     Box b;
     uint32_t first = 0, count = 0;  // interior: first = left child index, count = 0
@@ -128,13 +141,7 @@ BinBvh build_binary(const std::vector<Box>& bounds) {
     };
     std::vector<Prim> prims(n);
     for (size_t i = 0; i < n; i++) {
-        for (int a = 0; a < 3; a++) {
-            float l = (float)bounds[i].lo[a], h = (float)bounds[i].hi[a];
-            if ((double)l > bounds[i].lo[a]) l = std::nextafter(l, -INFINITY);
-            if ((double)h < bounds[i].hi[a]) h = std::nextafter(h, INFINITY);
-            prims[i].lo[a] = l;
-            prims[i].hi[a] = h;
-        }
+        f32_box(bounds[i], prims[i].lo, prims[i].hi);
         prims[i].idx = (uint32_t)i;
     }
     t.nodes.resize(2 * n + 1);
@@ -378,9 +385,14 @@ void choose_grid(double lo, double hi, float* p_out, int* e_out) {
     if (!(hi >= lo)) hi = lo;
     double maxabs = std::fmax(std::fabs(lo), std::fabs(hi));
     int e_ulp = -149;
-    if (maxabs > 0) e_ulp = (int)std::floor(std::log2(maxabs)) - 23 + 4;
+    if (maxabs > 0) e_ulp = std::ilogb(maxabs) - 23 + 4;  // floor(log2), exact
     double extent = hi - lo;
-    int e = extent > 0 ? (int)std::ceil(std::log2(extent / 255.0)) : -126;
+    int e = -126;
+    if (extent > 0) {  // ceil(log2(extent / 255)), exact
+        int q;
+        double mant = std::frexp(extent / 255.0, &q);
+        e = mant == 0.5 ? q - 1 : q;
+    }
     e = std::max(std::max(e, e_ulp), -126);
     for (;;) {
         double s = std::ldexp(1.0, e);
@@ -674,7 +686,74 @@ uint32_t lbvh_build(std::vector<LightNode>& nodes, std::vector<uint32_t>& leaf_o
 
 DevMaterial fold_material_public(const rt_material_desc& m) { return fold_material(m); }
 
-bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
+void instance_boxes(const rt_scene_desc* d, const double* mesh_bounds, std::vector<double>* boxes,
+                    std::vector<double>* invs, HostScene* H) {
+    const uint32_t n = d->n_instances;
+    boxes->assign(6ull * n, 0.0);
+    invs->assign(12ull * n, 0.0);
+    parallel_for(n, [&](size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; i++) {
+            const rt_instance_desc& id = d->instances[i];
+            affine_inverse(id.object_to_world, &(*invs)[12ull * i]);
+            const double* lb = mesh_bounds + 6ull * id.mesh_id;
+            Box wb;
+            if (d->meshes[id.mesh_id].n_triangles) {
+                for (int k = 0; k < 8; k++) {
+                    double c[3] = {(k & 1) ? lb[3] : lb[0], (k & 2) ? lb[4] : lb[1], (k & 4) ? lb[5] : lb[2]};
+                    double w[3];
+                    xf_point(id.object_to_world, c, w);
+                    wb.grow_pt(w);
+                }
+            }
+            // Empty meshes get a degenerate far-away box so the TLAS never enters them.
+            if (!(wb.hi[0] >= wb.lo[0])) {
+                double far[3] = {1e30, 1e30, 1e30};
+                wb = Box();
+                wb.grow_pt(far);
+            }
+            for (int a = 0; a < 3; a++) {
+                (*boxes)[6 * i + a] = wb.lo[a];
+                (*boxes)[6 * i + 3 + a] = wb.hi[a];
+            }
+        }
+    }, 4096);
+    Box world;
+    for (uint32_t i = 0; i < n; i++) {
+        const double* b = &(*boxes)[6ull * i];
+        if (b[3] < 1e29) {
+            Box x;
+            for (int a = 0; a < 3; a++) {
+                x.lo[a] = b[a];
+                x.hi[a] = b[3 + a];
+            }
+            world.grow(x);
+        }
+    }
+    for (int a = 0; a < 3; a++) {
+        H->world_lo[a] = world.lo[a] <= world.hi[a] ? world.lo[a] : 0.0;
+        H->world_hi[a] = world.lo[a] <= world.hi[a] ? world.hi[a] : 0.0;
+    }
+}
+
+void prim_records(const std::vector<double>& boxes, float* out) {
+    const size_t n = boxes.size() / 6;
+    parallel_for(n, [&](size_t i0, size_t i1) {
+        for (size_t i = i0; i < i1; i++) {
+            Box b;
+            for (int a = 0; a < 3; a++) {
+                b.lo[a] = boxes[6 * i + a];
+                b.hi[a] = boxes[6 * i + 3 + a];
+            }
+            float* o = out + 8 * i;
+            f32_box(b, o, o + 4);
+            uint32_t idx = (uint32_t)i;
+            memcpy(&o[3], &idx, 4);
+            o[7] = 0.0f;
+        }
+    });
+}
+
+bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, bool build_bvh) {
     HostScene& H = *out;
     if (!d) {
         *err = "null scene descriptor";
@@ -697,13 +776,33 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
         *err = "more than 2^27 unique triangles";
         return false;
     }
-    H.tris.reserve(3 * tri_total);
+    H.n_tris = tri_total;
+    if (build_bvh) H.tris.reserve(3 * tri_total);
+    uint64_t tri_base = 0;
     for (uint32_t m = 0; m < d->n_meshes; m++) {
         const rt_mesh_desc& md = d->meshes[m];
         if (md.n_triangles && (!md.positions || !md.indices)) {
             *err = "mesh " + std::to_string(m) + " has NULL positions or indices";
             return false;
         }
+        MeshInfo& mi = H.meshes[m];
+        mi.n_tris = md.n_triangles;
+        mi.tri_base = (uint32_t)tri_base;
+        mi.blas_root = 0xFFFFFFFFu;
+        mi.idx_base = 0xFFFFFFFFu;
+        tri_base += md.n_triangles;
+        if (md.normals) {
+            mi.idx_base = (uint32_t)H.orig_idx.size();
+            uint32_t vbase = (uint32_t)(H.normals.size() / 3);
+            const size_t o = H.orig_idx.size();
+            H.orig_idx.resize(o + 3ull * md.n_triangles);
+            uint32_t* oi = H.orig_idx.data() + o;
+            parallel_for(3ull * md.n_triangles, [&](size_t k0, size_t k1) {
+                for (size_t k = k0; k < k1; k++) oi[k] = vbase + md.indices[k];
+            });
+            H.normals.insert(H.normals.end(), md.normals, md.normals + 3ull * md.n_vertices);
+        }
+        if (!build_bvh) continue;  // the device builder validates, bounds and builds
         std::vector<Box> tb(md.n_triangles);
         std::atomic<int> bad_index{0}, bad_vertex{0};
         std::mutex bounds_mu;
@@ -740,16 +839,6 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
         }
         BinBvh bin = build_binary(tb);
         H.binary_blas_nodes += bin.nodes.size();
-        MeshInfo& mi = H.meshes[m];
-        mi.n_tris = md.n_triangles;
-        mi.tri_base = (uint32_t)(H.tris.size() / 3);
-        mi.idx_base = 0xFFFFFFFFu;
-        if (md.normals) {
-            mi.idx_base = (uint32_t)H.orig_idx.size();
-            uint32_t vbase = (uint32_t)(H.normals.size() / 3);
-            for (uint64_t k = 0; k < 3ull * md.n_triangles; k++) H.orig_idx.push_back(vbase + md.indices[k]);
-            H.normals.insert(H.normals.end(), md.normals, md.normals + 3ull * md.n_vertices);
-        }
         const size_t tri_off = H.tris.size();
         H.tris.resize(tri_off + 3ull * md.n_triangles);
         float4* dst = H.tris.data() + tri_off;
@@ -769,10 +858,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
                 dst[3 * k + 2] = v[2];
             }
         });
-        if (md.n_triangles == 0) {
-            mi.blas_root = 0xFFFFFFFFu;
-            continue;
-        }
+        if (md.n_triangles == 0) continue;
         Collapser col{bin, H.nodes, mi.tri_base};
         H.nodes.reserve(H.nodes.size() + WIDE_NODE_WORDS * (bin.nodes.size() / 4 + 1));
         mi.blas_root = col.emit(0);
@@ -788,45 +874,30 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err) {
         *err = "instances pointer is NULL";
         return false;
     }
-    std::vector<Box> ib(d->n_instances);
-    std::vector<double> invs(12ull * d->n_instances);
     for (uint32_t i = 0; i < d->n_instances; i++) {
         const rt_instance_desc& id = d->instances[i];
         if (id.mesh_id >= d->n_meshes || id.material_id >= d->n_materials) {
             *err = "instance " + std::to_string(i) + " references a missing mesh or material";
             return false;
         }
-        affine_inverse(id.object_to_world, &invs[12ull * i]);
-        const Box& lb = local_bounds[id.mesh_id];
-        Box wb;
-        if (d->meshes[id.mesh_id].n_triangles) {
-            for (int k = 0; k < 8; k++) {
-                double c[3] = {(k & 1) ? lb.hi[0] : lb.lo[0], (k & 2) ? lb.hi[1] : lb.lo[1],
-                               (k & 4) ? lb.hi[2] : lb.lo[2]};
-                double w[3];
-                xf_point(id.object_to_world, c, w);
-                wb.grow_pt(w);
-            }
-        }
-        ib[i] = wb;
     }
     H.tlas_nodes = 0;
     H.scalars.tlas_root = 0xFFFFFFFFu;
-    if (d->n_instances) {
-        // Empty meshes get a degenerate far-away box so the TLAS never enters them.
-        for (auto& b : ib)
-            if (!(b.hi[0] >= b.lo[0])) {
-                double far[3] = {1e30, 1e30, 1e30};
-                b = Box();
-                b.grow_pt(far);
+    if (build_bvh && d->n_instances) {
+        std::vector<double> mb(6ull * d->n_meshes);
+        for (uint32_t m = 0; m < d->n_meshes; m++)
+            for (int a = 0; a < 3; a++) {
+                mb[6ull * m + a] = local_bounds[m].lo[a];
+                mb[6ull * m + 3 + a] = local_bounds[m].hi[a];
             }
-        Box world;
-        for (const auto& b : ib)
-            if (b.hi[0] < 1e29) world.grow(b);
-        for (int a = 0; a < 3; a++) {
-            H.world_lo[a] = world.lo[a] <= world.hi[a] ? world.lo[a] : 0.0;
-            H.world_hi[a] = world.lo[a] <= world.hi[a] ? world.hi[a] : 0.0;
-        }
+        std::vector<double> boxes, invs;
+        instance_boxes(d, mb.data(), &boxes, &invs, &H);
+        std::vector<Box> ib(d->n_instances);
+        for (uint32_t i = 0; i < d->n_instances; i++)
+            for (int a = 0; a < 3; a++) {
+                ib[i].lo[a] = boxes[6ull * i + a];
+                ib[i].hi[a] = boxes[6ull * i + 3 + a];
+            }
         BinBvh tl = build_binary(ib);
         Collapser col{tl, H.nodes, 0};
         H.scalars.tlas_root = col.emit(0);

@@ -26,13 +26,28 @@ struct HostScene {
     std::vector<uint32_t> inf_lights;
     std::vector<float> inf_power;
     uint64_t blas_nodes = 0, tlas_nodes = 0, binary_blas_nodes = 0;
+    uint64_t n_tris = 0;             // unique triangles over all meshes
     double world_lo[3] = {0, 0, 0}, world_hi[3] = {0, 0, 0};  // union of instance bounds
     DevScene scalars{};              // pointer fields unset; scalar fields filled
 };
 
 // Flatten `desc` into device-ready arrays. Returns false with `err` set on
-// invalid input (index out of range, non-finite vertex, ...).
-bool flatten_scene(const rt_scene_desc* desc, HostScene* out, std::string* err);
+// invalid input (index out of range, non-finite vertex, ...). With
+// build_bvh false the BLASes and the TLAS are left to the device builder
+// (bvh_build.h): nodes, tris, inst_xf and inst stay empty, mesh records get
+// their triangle ranges but no BLAS root, and vertex data is not validated.
+bool flatten_scene(const rt_scene_desc* desc, HostScene* out, std::string* err, bool build_bvh = true);
+
+// World boxes (6 doubles per instance: lo xyz, hi xyz; a far-away point
+// for empty meshes) and world-to-object 3x4 inverses (12 doubles) of the
+// instances, from the meshes' local bounds (6 doubles per mesh); sets the
+// world box in H. Instance ids must be validated.
+void instance_boxes(const rt_scene_desc* d, const double* mesh_bounds, std::vector<double>* boxes,
+                    std::vector<double>* invs, HostScene* H);
+
+// Builder primitive records (8 floats each: lo xyz, index bits, hi xyz, 0)
+// of boxes given as 6 doubles: rounded outward to f32, -0 folded into +0.
+void prim_records(const std::vector<double>& boxes, float* out);
 
 // f32 material constants as the shade kernel reads them.
 DevMaterial fold_material_public(const rt_material_desc& m);

@@ -14,6 +14,7 @@
 #include <string>
 #include <vector>
 
+#include "bvh_build.h"
 #include "flatten.h"
 #include "guide_internal.h"
 #include "pt_kernels.cuh"
@@ -143,7 +144,8 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     auto* s = new rt_session();
     s->params = *params;
     std::string err;
-    if (!flatten_scene(scene, &s->host, &err)) {
+    const bool device_bvh = params->bvh_build == 0;
+    if (!flatten_scene(scene, &s->host, &err, !device_bvh)) {
         delete s;
         return fail(RT_ERR_INVALID, err);
     }
@@ -168,12 +170,28 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     for (auto& e : s->ev) cudaEventCreate(&e);
     HostScene& H = s->host;
     DevScene& S = s->S;
-    S = H.scalars;
     int rc = 0;
-    rc = rc ? rc : s->upload((const uint4**)&S.nodes, H.nodes);
-    rc = rc ? rc : s->upload((const float4**)&S.tris, H.tris);
-    rc = rc ? rc : s->upload((const float4**)&S.inst_xf, H.inst_xf);
-    rc = rc ? rc : s->upload((const uint4**)&S.inst, H.inst);
+    if (device_bvh) {
+        DeviceBvh b;
+        rc = device_build_scene(scene, &H, &b, s->stream, &err);
+        for (void* p : b.allocations) s->allocs.push_back(p);
+        if (rc) {
+            delete s;
+            return fail(rc, err);
+        }
+        s->device_bytes += b.n_nodes * WIDE_NODE_WORDS * 16 + H.n_tris * 48 + (uint64_t)scene->n_instances * 64;
+        S = H.scalars;
+        S.nodes = b.nodes;
+        S.tris = b.tris;
+        S.inst_xf = b.inst_xf;
+        S.inst = b.inst;
+    } else {
+        S = H.scalars;
+        rc = rc ? rc : s->upload((const uint4**)&S.nodes, H.nodes);
+        rc = rc ? rc : s->upload((const float4**)&S.tris, H.tris);
+        rc = rc ? rc : s->upload((const float4**)&S.inst_xf, H.inst_xf);
+        rc = rc ? rc : s->upload((const uint4**)&S.inst, H.inst);
+    }
     rc = rc ? rc : s->upload(&S.meshes, H.meshes);
     rc = rc ? rc : s->upload(&S.orig_idx, H.orig_idx);
     rc = rc ? rc : s->upload(&S.normals, H.normals);
@@ -696,7 +714,7 @@ int rt_get_stats(rt_session* s, rt_stats* out) {
     *out = s->last;
     out->blas_nodes = s->host.blas_nodes;
     out->tlas_nodes = s->host.tlas_nodes;
-    out->triangles = s->host.tris.size() / 3;
+    out->triangles = s->host.n_tris;
     out->device_bytes = s->device_bytes;
     return RT_OK;
 }

@@ -108,6 +108,8 @@ class RtParams(C.Structure):
         ("guide_lr", C.c_double),
         ("guide_steps", C.c_uint32),
         ("guide_depth", C.c_uint32),
+        ("bvh_build", C.c_uint32),
+        ("reserved0", C.c_uint32),
     ]
 
 
@@ -115,16 +117,20 @@ LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK = range(5)
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
 for _t, _n in ((RtMeshDesc, 32), (RtInstanceDesc, 104), (RtMaterialDesc, 264),
-               (RtLightDesc, 120), (RtCameraDesc, 144), (RtParams, 56)):
+               (RtLightDesc, 120), (RtCameraDesc, 144), (RtParams, 64)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
 
 def make_params(max_depth=8, rr_start=3, firefly_clamp=60.0, aovs=False, guided=False,
-                guide_fraction=0.5, max_paths=0, guide_lr=0.0, guide_steps=0, guide_depth=0):
+                guide_fraction=0.5, max_paths=0, guide_lr=0.0, guide_steps=0, guide_depth=0, bvh_build="device"):
     """Integrator knobs; defaults follow the reference's constants
     (src/raytracer/pt/mod.rs:26-32) except the bounce cap, which the configs set.
     guide_lr / guide_steps: Adam learning rate and steps per sample pass of the
     learned proposal (0 = 1e-2 and 3); guide_depth: only vertices of depth
-    below it use the proposal (0 = every depth)."""
+    below it use the proposal (0 = every depth). bvh_build: "device" (default)
+    or "host" builds the same BVHs on the GPU or on the host cores."""
+    if bvh_build not in ("device", "host"):
+        raise ValueError("bvh_build must be 'device' or 'host'")
     return RtParams(max_depth, rr_start, firefly_clamp, 1 if aovs else 0, 1 if guided else 0,
-                    guide_fraction, max_paths, guide_lr, guide_steps, guide_depth)
+                    guide_fraction, max_paths, guide_lr, guide_steps, guide_depth,
+                    0 if bvh_build == "device" else 1, 0)
