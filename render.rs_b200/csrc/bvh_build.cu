@@ -21,6 +21,7 @@
 // bottom-up, indices top-down, then every node quantised independently.
 
 #include "bvh_build.h"
+#include "devmem.h"
 #include "rt_cuda.h"
 
 #include <algorithm>
@@ -950,11 +951,14 @@ struct Fail {
     int code;
 };
 
-// Device allocations of one build; freed when the build returns.
+// Device allocations of one build; returned to the pool when the build
+// returns (after the work queued on the build's stream).
 struct Scratch {
+    cudaStream_t st;
     std::vector<void*> ptrs;
+    explicit Scratch(cudaStream_t s) : st(s) {}
     ~Scratch() {
-        for (void* p : ptrs) cudaFree(p);
+        for (void* p : ptrs) pool_free(p, st);
     }
 };
 
@@ -968,9 +972,9 @@ struct Scratch {
     } while (0)
 
 template <class T>
-int dev_alloc(std::vector<void*>& owner, T** p, size_t count, std::string* err) {
+int dev_alloc(std::vector<void*>& owner, T** p, size_t count, cudaStream_t st, std::string* err) {
     void* v = nullptr;
-    BV_TRY(cudaMalloc(&v, std::max<size_t>(count, 1) * sizeof(T)));
+    BV_TRY(pool_alloc(&v, std::max<size_t>(count, 1) * sizeof(T), st));
     owner.push_back(v);
     *p = (T*)v;
     return RT_OK;
@@ -1004,18 +1008,18 @@ int build_binary_device(Scratch& D, BPrim* P0, BPrim* P1, uint32_t n,
     uint32_t *chunk_job, *chunk_left, *acc_box[2], *acc_bin[2], *counters;
     unsigned long long* acc_cb[2];
     int rc = 0;
-    rc = rc ? rc : dev_alloc(D.ptrs, &nodes, node_cap, err);
+    rc = rc ? rc : dev_alloc(D.ptrs, &nodes, node_cap, st, err);
     for (int b = 0; b < 2; b++) {
-        rc = rc ? rc : dev_alloc(D.ptrs, &jobs[b], J_cap, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &info[b], J_cap, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &acc_box[b], 6ull * J_cap, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &acc_cb[b], 6ull * J_cap, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &acc_bin[b], (size_t)BINS * 7 * J_cap, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &jobs[b], J_cap, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &info[b], J_cap, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &acc_box[b], 6ull * J_cap, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &acc_cb[b], 6ull * J_cap, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &acc_bin[b], (size_t)BINS * 7 * J_cap, st, err);
     }
-    rc = rc ? rc : dev_alloc(D.ptrs, &chunk_job, C_cap, err);
-    rc = rc ? rc : dev_alloc(D.ptrs, &chunk_left, C_cap, err);
-    rc = rc ? rc : dev_alloc(D.ptrs, &small, S_cap, err);
-    rc = rc ? rc : dev_alloc(D.ptrs, &counters, 4, err);  // nodes, next jobs, next chunks, small jobs
+    rc = rc ? rc : dev_alloc(D.ptrs, &chunk_job, C_cap, st, err);
+    rc = rc ? rc : dev_alloc(D.ptrs, &chunk_left, C_cap, st, err);
+    rc = rc ? rc : dev_alloc(D.ptrs, &small, S_cap, st, err);
+    rc = rc ? rc : dev_alloc(D.ptrs, &counters, 4, st, err);  // nodes, next jobs, next chunks, small jobs
     if (rc) return rc;
 
     // Level 0: roots above SMALL are level jobs, the rest subtree jobs.
@@ -1128,8 +1132,8 @@ int wide_structure(Scratch& D, const BNode* nodes, uint32_t n_nodes, uint32_t R,
                    cudaStream_t st, std::string* err) {
     const uint32_t cap = n_nodes + 1;
     uint32_t* counter;
-    int rc = dev_alloc(D.ptrs, &T->W, cap, err);
-    rc = rc ? rc : dev_alloc(D.ptrs, &counter, 1, err);
+    int rc = dev_alloc(D.ptrs, &T->W, cap, st, err);
+    rc = rc ? rc : dev_alloc(D.ptrs, &counter, 1, st, err);
     if (rc) return rc;
     std::vector<WideS> roots(R);
     for (uint32_t r = 0; r < R; r++) {
@@ -1172,7 +1176,7 @@ int wide_write(Scratch& D, WideTree& T, const BNode* nodes, const std::vector<ui
     const uint32_t R = (uint32_t)root_idx.size();
     if (T.n == 0) return RT_OK;
     uint32_t* d_root;
-    int rc = dev_alloc(D.ptrs, &d_root, R, err);
+    int rc = dev_alloc(D.ptrs, &d_root, R, st, err);
     if (rc) return rc;
     BV_TRY(cudaMemcpyAsync(d_root, root_idx.data(), R * 4, cudaMemcpyHostToDevice, st));
     k_wide_root_index<<<blocks_for(R, JB), JB, 0, st>>>(T.W, d_root, R);
@@ -1188,7 +1192,7 @@ int wide_write(Scratch& D, WideTree& T, const BNode* nodes, const std::vector<ui
 }  // namespace
 
 int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cudaStream_t st, std::string* err) {
-    Scratch D;
+    Scratch D(st);
     const uint32_t M = d->n_meshes;
     std::vector<uint32_t> tri_base(M), vbase(M), nverts(M);
     uint64_t N = 0, V = 0;
@@ -1204,7 +1208,7 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
         return RT_ERR_INVALID;
     }
     uint32_t* d_err;
-    int rc = dev_alloc(D.ptrs, &d_err, 1, err);
+    int rc = dev_alloc(D.ptrs, &d_err, 1, st, err);
     if (rc) return rc;
     BV_TRY(cudaMemsetAsync(d_err, 0, 4, st));
 
@@ -1230,13 +1234,13 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
             root_mesh.push_back(m);
         }
     if (N) {
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_pos, 3 * V, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_idx, 3 * N, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_tri_base, M, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_vbase, M, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_nverts, M, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &P0, N, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &P1, N, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_pos, 3 * V, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_idx, 3 * N, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_tri_base, M, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_vbase, M, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_nverts, M, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &P0, N, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &P1, N, st, err);
         if (rc) return rc;
         for (uint32_t m = 0; m < M; m++) {
             const rt_mesh_desc& md = d->meshes[m];
@@ -1318,8 +1322,8 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
             rec[i] = make_uint4(blas_root[id.mesh_id], i, id.material_id, id.mesh_id);
         }
         BPrim* Q1;
-        rc = rc ? rc : dev_alloc(D.ptrs, &Q0, NI, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &Q1, NI, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &Q0, NI, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &Q1, NI, st, err);
         if (rc) return rc;
         BV_TRY(cudaMemcpyAsync(Q0, prims.data(), prims.size() * 4, cudaMemcpyHostToDevice, st));
         uint32_t n_tnodes = 0;
@@ -1335,10 +1339,10 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
     // ---- outputs ------------------------------------------------------------------------
     const uint64_t total = (uint64_t)blas_total + tlas_total;
     out->n_nodes = total;
-    rc = rc ? rc : dev_alloc(out->allocations, &out->nodes, WIDE_NODE_WORDS * total, err);
-    rc = rc ? rc : dev_alloc(out->allocations, &out->tris, 3 * N, err);
-    rc = rc ? rc : dev_alloc(out->allocations, &out->inst_xf, 3ull * NI, err);
-    rc = rc ? rc : dev_alloc(out->allocations, &out->inst, NI, err);
+    rc = rc ? rc : dev_alloc(out->allocations, &out->nodes, WIDE_NODE_WORDS * total, st, err);
+    rc = rc ? rc : dev_alloc(out->allocations, &out->tris, 3 * N, st, err);
+    rc = rc ? rc : dev_alloc(out->allocations, &out->inst_xf, 3ull * NI, st, err);
+    rc = rc ? rc : dev_alloc(out->allocations, &out->inst, NI, st, err);
     if (rc) return rc;
     if (N) {
         std::vector<uint32_t> ridx(roots.size());
@@ -1352,8 +1356,8 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
         if (rc) return rc;
         float4* d_xf;
         uint4* d_rec;
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_xf, 3ull * NI, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_rec, NI, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_xf, 3ull * NI, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_rec, NI, st, err);
         if (rc) return rc;
         BV_TRY(cudaMemcpyAsync(d_xf, xf.data(), xf.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
         BV_TRY(cudaMemcpyAsync(d_rec, rec.data(), rec.size() * sizeof(uint4), cudaMemcpyHostToDevice, st));

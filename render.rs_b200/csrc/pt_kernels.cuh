@@ -415,6 +415,18 @@ __global__ void k_guide_keep(const uint32_t* tb_cnt, float scale, uint32_t cap, 
 #ifndef RT_NODE_PHASE_EXIT
 #define RT_NODE_PHASE_EXIT 14
 #endif
+// A node-phase step pops the next entry and tests it at once when it is a
+// node (RT_FUSED_POP), instead of spending a whole warp step on the pop
+// while other lanes test nodes: closest hit 422 -> 484 Mrays/s, the
+// 1080p cloud frame 119 -> 105 ms. Entering instance leaves inside the node
+// phase (RT_INST_IN_NODE_PHASE, with RT_FUSED_POP) made the forest frame 3-8%
+// slower, so instance leaves wait for the leaf phase.
+#ifndef RT_FUSED_POP
+#define RT_FUSED_POP 1
+#endif
+#ifndef RT_INST_IN_NODE_PHASE
+#define RT_INST_IN_NODE_PHASE 0
+#endif
 template <bool ANY, bool TRANSMIT = false, class Load, class Finish>
 __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                          TravStack& st, LeafShared& leaf, Load load, Finish finish) {
@@ -456,7 +468,7 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
         }
         // Node phase.
         for (;;) {
-            bool want = active && ps.pending == 0;
+            bool want = active && (ps.pending == 0 || (RT_FUSED_POP && RT_INST_IN_NODE_PHASE && !ps.ts.in_inst));
             const uint32_t wm = __ballot_sync(0xFFFFFFFFu, want);
             if (!wm) break;
             if (RT_NODE_PHASE_EXIT > 0 && __popc(wm) <= RT_NODE_PHASE_EXIT &&
@@ -467,6 +479,14 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
                 if (++steps > RT_MAX_TRAV_STEPS) {
                     atomicOr(err, RT_DEVERR_ITER);
                     done_now = true;
+                } else if (RT_FUSED_POP) {
+                    // One step: enter a parked instance leaf, or pop; then
+                    // test the node that is current, if any.
+                    if (RT_INST_IN_NODE_PHASE && ps.pending && !ps.ts.in_inst)
+                        done_now = op_leaf<ANY>(S, ps, st, err);
+                    else if (ps.need_pop)
+                        done_now = !op_pop(ps, st);
+                    if (!done_now && ps.pending == 0 && !ps.need_pop) done_now = op_node<ANY>(S, ps, st, err);
                 } else if (ps.need_pop) {
                     done_now = !op_pop(ps, st);
                 } else {

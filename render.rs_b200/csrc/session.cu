@@ -11,16 +11,53 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
 #include "bvh_build.h"
+#include "devmem.h"
 #include "flatten.h"
 #include "guide_internal.h"
 #include "pt_kernels.cuh"
 #include "rt_cuda.h"
 
 using namespace rt;
+
+namespace rt {
+
+cudaError_t pool_alloc(void** p, size_t bytes, cudaStream_t st) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (!pools[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            e = cudaMemPoolCreate(&pools[dev], &props);
+            if (e != cudaSuccess) {
+                pools[dev] = nullptr;
+                return e;
+            }
+            uint64_t keep = ~0ull;
+            cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        pool = pools[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
+cudaError_t pool_free(void* p, cudaStream_t st) { return cudaFreeAsync(p, st); }
+
+}  // namespace rt
 
 namespace {
 
@@ -40,7 +77,10 @@ int fail(int code, const std::string& msg) {
         }                                                                                      \
     } while (0)
 
-constexpr int TRAV_BLOCK = 128;
+#ifndef RT_TRAV_BLOCK
+#define RT_TRAV_BLOCK 128
+#endif
+constexpr int TRAV_BLOCK = RT_TRAV_BLOCK;
 
 // Adam steps per sample pass of a guided render: 0 selects the default of 3
 // (on the two-room scene at 1280x720 and a 1024-pass budget, equal-time
@@ -89,10 +129,10 @@ struct rt_session {
     int alloc(T** p, size_t count) {
         size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
         void* v = nullptr;
-        cudaError_t e = cudaMalloc(&v, bytes);
+        cudaError_t e = pool_alloc(&v, bytes, stream);
         if (e != cudaSuccess)
             return fail(e == cudaErrorMemoryAllocation ? RT_ERR_OOM : RT_ERR_CUDA,
-                        std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+                        std::string("device allocation (") + std::to_string(bytes) + " B): " + cudaGetErrorString(e));
         allocs.push_back(v);
         device_bytes += bytes;
         *p = (T*)v;
@@ -125,10 +165,13 @@ struct rt_session {
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         for (auto& e : evpool) cudaEventDestroy(e);
-        for (void* p : allocs) cudaFree(p);
+        for (void* p : allocs) pool_free(p, stream);
         if (batch_buf) cudaFree(batch_buf);
         if (guide) rt_guide_destroy(guide);
-        if (stream) cudaStreamDestroy(stream);
+        if (stream) {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
     }
 };
 
