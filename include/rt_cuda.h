@@ -85,9 +85,35 @@ int rt_read_aux(rt_session* s, float* aux12);
 /* Checkpoint / resume of the f64 accumulator and completed-sample count.
  * Written to `path`.tmp then renamed (atomic). A load only succeeds when the
  * image size matches. Replaces save_checkpoint / load_checkpoint
- * (renderer.rs:219-254) with an f64 payload (magic "RCU1"). */
+ * (renderer.rs:219-254) with an f64 payload (magic "RCU1");
+ * rt_checkpoint_save_rckp writes the reference's own f32 format ("RCKP",
+ * width, height, passes done, f32 RGBW per pixel; renderer.rs:222-236), and
+ * rt_checkpoint_load reads either, so a checkpoint of the Metal backend
+ * resumes here and the other way round. */
 int rt_checkpoint_save(rt_session* s, const char* path);
+int rt_checkpoint_save_rckp(rt_session* s, const char* path);
 int rt_checkpoint_load(rt_session* s, const char* path, uint32_t* samples_done);
+/* The RCKP file of an RGBW accumulator held by the caller (f64 in, f32 on disk). */
+int rt_rckp_write(const char* path, uint32_t width, uint32_t height, uint32_t passes_done, const double* rgbw);
+
+/* Accumulation files of distributed renders (src/output/accum.rs): an
+ * OpenEXR image with the f32 channels B, G, R (radiance sums of a sample
+ * range) and count (samples per pixel), layer "accum".
+ *  - rt_accum_exr_write: writes `rgbw` (4 doubles per pixel: RGB sum, count;
+ *    rt_read_accum's layout) as uncompressed scanlines; replaces
+ *    write_accum_exr (accum.rs:14-46).
+ *  - rt_accum_exr_info / rt_accum_exr_read: size, then the sums and counts of
+ *    such a file (scanline or one-level tiled, uncompressed, RLE, ZIPS or
+ *    ZIP, FLOAT or HALF channels); replaces read_accum_exr (accum.rs:48-85).
+ *  - rt_accum_merge: the mean image of any number of files (sum of sums /
+ *    sum of counts, 0 where no samples), 3 floats per pixel; replaces merge
+ *    (accum.rs:88-119), the `render merge` subcommand.
+ * No GPU is involved; errors are RT_ERR_IO (unreadable or not such a file)
+ * and RT_ERR_MISMATCH (resolution). */
+int rt_accum_exr_write(const char* path, uint32_t width, uint32_t height, const double* rgbw);
+int rt_accum_exr_info(const char* path, uint32_t* width, uint32_t* height);
+int rt_accum_exr_read(const char* path, uint32_t width, uint32_t height, double* rgbw);
+int rt_accum_merge(const char* const* paths, uint32_t n_paths, uint32_t width, uint32_t height, float* rgb);
 
 /* Ray batch against the session's scene. `rays` holds 8 floats per ray in
  * two planes: [0, 4n) = (ox, oy, oz, unused), [4n, 8n) = (dx, dy, dz, tmax).

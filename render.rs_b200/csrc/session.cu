@@ -91,6 +91,10 @@ constexpr int SHADE_BLOCK = 128;
 
 }  // namespace
 
+namespace rt {
+std::string& accum_error() { return g_err; }
+}  // namespace rt
+
 struct rt_session {
     HostScene host;
     DevScene S{};
@@ -577,6 +581,14 @@ int rt_checkpoint_save(rt_session* s, const char* path) {
     return RT_OK;
 }
 
+int rt_checkpoint_save_rckp(rt_session* s, const char* path) {
+    if (!s || !path) return fail(RT_ERR_INVALID, "NULL argument");
+    std::vector<double> a(4ull * s->npix);
+    int rc = rt_read_accum(s, a.data());
+    if (rc) return rc;
+    return rt_rckp_write(path, s->S.width, s->S.height, s->samples_done, a.data());
+}
+
 int rt_checkpoint_load(rt_session* s, const char* path, uint32_t* samples_done) {
     if (!s || !path) return fail(RT_ERR_INVALID, "NULL argument");
     FILE* f = fopen(path, "rb");
@@ -584,11 +596,20 @@ int rt_checkpoint_load(rt_session* s, const char* path, uint32_t* samples_done) 
     uint32_t hdr[4];
     std::vector<double> a(4ull * s->npix);
     bool ok = fread(hdr, 4, 4, f) == 4;
-    if (ok && (hdr[0] != 0x31554352u || hdr[1] != s->S.width || hdr[2] != s->S.height)) {
+    // This library's f64 checkpoint ("RCU1") or the Metal backend's f32 one
+    // ("RCKP", src/raytracer/metal/renderer.rs:219-254).
+    const bool rckp = ok && hdr[0] == 0x504B4352u;
+    if (ok && ((hdr[0] != 0x31554352u && !rckp) || hdr[1] != s->S.width || hdr[2] != s->S.height)) {
         fclose(f);
         return fail(RT_ERR_MISMATCH, "checkpoint does not match this session");
     }
-    ok = ok && fread(a.data(), 8, a.size(), f) == a.size();
+    if (rckp) {
+        std::vector<float> a32(a.size());
+        ok = ok && fread(a32.data(), 4, a32.size(), f) == a32.size();
+        for (size_t i = 0; i < a.size(); i++) a[i] = a32[i];
+    } else {
+        ok = ok && fread(a.data(), 8, a.size(), f) == a.size();
+    }
     char extra;
     ok = ok && fread(&extra, 1, 1, f) == 0;
     fclose(f);

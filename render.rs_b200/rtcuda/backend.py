@@ -30,7 +30,8 @@ EXPORTS = ("rt_session_create", "rt_session_destroy", "rt_last_error", "rt_rende
            "rt_read_accum", "rt_read_image", "rt_read_aux", "rt_checkpoint_save", "rt_checkpoint_load",
            "rt_intersect_batch", "rt_intersect_batch_device", "rt_get_stats", "rt_session_stream",
            "rt_bsdf_furnace", "rt_intersect_batch_noalloc", "rt_session_guide", "rt_set_adaptive",
-           "rt_average_spp")
+           "rt_average_spp", "rt_checkpoint_save_rckp", "rt_rckp_write", "rt_accum_exr_write",
+           "rt_accum_exr_info", "rt_accum_exr_read", "rt_accum_merge")
 
 
 class RtError(RuntimeError):
@@ -85,6 +86,12 @@ def lib():
         L.rt_session_guide.argtypes = [vp]
         L.rt_set_adaptive.argtypes = [vp, C.c_double]
         L.rt_average_spp.argtypes = [vp, C.POINTER(C.c_double)]
+        L.rt_checkpoint_save_rckp.argtypes = [vp, C.c_char_p]
+        L.rt_rckp_write.argtypes = [C.c_char_p, u32, u32, u32, vp]
+        L.rt_accum_exr_write.argtypes = [C.c_char_p, u32, u32, vp]
+        L.rt_accum_exr_info.argtypes = [C.c_char_p, C.POINTER(u32), C.POINTER(u32)]
+        L.rt_accum_exr_read.argtypes = [C.c_char_p, u32, u32, vp]
+        L.rt_accum_merge.argtypes = [C.POINTER(C.c_char_p), u32, u32, u32, vp]
         _lib = L
     return _lib
 
@@ -161,6 +168,16 @@ class PtSession:
 
     def checkpoint_save(self, path):
         _check(lib().rt_checkpoint_save(self.h, os.fsencode(path)))
+
+    def checkpoint_save_rckp(self, path):
+        """The Metal backend's f32 checkpoint format (renderer.rs:219-236)."""
+        _check(lib().rt_checkpoint_save_rckp(self.h, os.fsencode(path)))
+
+    def write_accum_exr(self, path):
+        """This session's sums and sample counts as an accumulation EXR
+        (the --sample-range output, src/main.rs:363-403)."""
+        from .accum import write_accum
+        write_accum(path, self.sum_and_weight())
 
     def checkpoint_load(self, path):
         done = C.c_uint32()
