@@ -141,7 +141,8 @@ typedef struct rt_params {
     uint32_t guide_steps;     /* Adam steps per sample pass when guided (0 = 3) */
     uint32_t guide_depth;     /* guide only vertices of depth < this (0 = all) */
     uint32_t bvh_build;       /* 0 = build the BVHs on the GPU, 1 = on the host (same trees) */
-    uint32_t reserved0;       /* 0 */
+    uint32_t guide_train_passes; /* train the proposal during the first this many sample passes,
+                                    then keep it fixed (0 = 512; 0xFFFFFFFF = never stop) */
 } rt_params;
 
 /* Size checks shared by every consumer of the descriptor. */

@@ -80,6 +80,7 @@ struct PtConsts {
     float clamp;
     uint64_t sample0;  // first sample index of the slab
     uint32_t guided;
+    uint32_t train;    // guided and still training: shading writes training vertices
     float alpha;       // one-sample MIS probability of sampling the guide
     GuideDev G;
     // Adaptive sampling (tol > 0): per pixel (luminance sum, luminance^2 sum,
@@ -738,7 +739,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
             // Training: close the previous vertex's record with the radiance
             // gathered so far (its own emission and NEE included).
             auto tr_close = [&]() {
-                if (!C.guided) return;
+                if (!C.train) return;
                 uint32_t d0 = flags >> FL_DEPTH_SHIFT;
                 if (d0 == 0 || d0 > C.max_depth) return;
                 float* r = P.tr_rec + ((size_t)slot * C.max_depth + (d0 - 1)) * TR_FLOATS;
@@ -863,7 +864,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                         float3 wi = fr.to_world(bs.wi);
                         const float3 beta_in = beta;
                         beta = beta * bs.f * (fabsf(bs.wi.z) / pdf_path);
-                        if (C.guided) {
+                        if (C.train) {
                             // Training vertex: closed with the radiance at the next vertex.
                             uint32_t d0 = flags >> FL_DEPTH_SHIFT;
                             if (d0 < C.max_depth) {

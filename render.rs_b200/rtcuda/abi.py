@@ -109,7 +109,7 @@ class RtParams(C.Structure):
         ("guide_steps", C.c_uint32),
         ("guide_depth", C.c_uint32),
         ("bvh_build", C.c_uint32),
-        ("reserved0", C.c_uint32),
+        ("guide_train_passes", C.c_uint32),
     ]
 
 
@@ -122,15 +122,18 @@ for _t, _n in ((RtMeshDesc, 32), (RtInstanceDesc, 104), (RtMaterialDesc, 264),
 
 
 def make_params(max_depth=8, rr_start=3, firefly_clamp=60.0, aovs=False, guided=False,
-                guide_fraction=0.5, max_paths=0, guide_lr=0.0, guide_steps=0, guide_depth=0, bvh_build="device"):
+                guide_fraction=0.5, max_paths=0, guide_lr=0.0, guide_steps=0, guide_depth=0, bvh_build="device",
+                guide_train_passes=0):
     """Integrator knobs; defaults follow the reference's constants
     (src/raytracer/pt/mod.rs:26-32) except the bounce cap, which the configs set.
     guide_lr / guide_steps: Adam learning rate and steps per sample pass of the
     learned proposal (0 = 1e-2 and 3); guide_depth: only vertices of depth
-    below it use the proposal (0 = every depth). bvh_build: "device" (default)
-    or "host" builds the same BVHs on the GPU or on the host cores."""
+    below it use the proposal (0 = every depth); guide_train_passes: sample
+    passes that train the proposal before it is kept fixed (0 = 512,
+    0xFFFFFFFF = never stop). bvh_build: "device" (default) or "host" builds
+    the same BVHs on the GPU or on the host cores."""
     if bvh_build not in ("device", "host"):
         raise ValueError("bvh_build must be 'device' or 'host'")
     return RtParams(max_depth, rr_start, firefly_clamp, 1 if aovs else 0, 1 if guided else 0,
                     guide_fraction, max_paths, guide_lr, guide_steps, guide_depth,
-                    0 if bvh_build == "device" else 1, 0)
+                    0 if bvh_build == "device" else 1, guide_train_passes)
