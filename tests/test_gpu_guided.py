@@ -131,3 +131,22 @@ def test_trained_proposal_gain():
         p_bsdf = (np.maximum(W @ n, 0) / np.pi)[sl].sum() * dw
         print(f"  vertex {p}: P(opening) guide {p_guide:.4f}, cosine BSDF {p_bsdf:.4f}")
         assert p_guide > 3.0 * p_bsdf
+
+
+def test_training_stops_after_budget():
+    # guide_train_passes: the proposal trains on the first N sample passes
+    # (3 Adam steps each), then stays fixed while rendering continues.
+    s = scenes.two_rooms(64, 48)
+    p = abi.make_params(max_depth=16, guided=True, guide_fraction=0.5, guide_train_passes=6)
+    with PtSession(s, p) as g:
+        g.render_samples(0, 4)
+        assert g.stats()["guide_steps"] == 4 * 3
+        g.render_samples(4, 8)
+        assert g.stats()["guide_steps"] == 2 * 3
+        m0, t0 = g.guide().params()
+        g.render_samples(12, 4)
+        assert g.stats()["guide_steps"] == 0
+        m1, t1 = g.guide().params()
+        np.testing.assert_array_equal(m0, m1)
+        np.testing.assert_array_equal(t0, t1)
+        assert np.isfinite(g.image()).all()
