@@ -1,0 +1,918 @@
+"""RIB scene files -> rtcuda scenes (the reference's ``parse_rib`` +
+``SceneBuilder::build``, src/parser/parser.rs and
+src/parser/scene_builder.rs), for the part of RenderMan the CUDA path
+renders: triangle meshes and polygons, quadrics, instancing, legacy and
+PxrSurface materials, point / distant / area lights, the camera.
+
+Same conventions as the reference: requests are an identifier followed by
+values (numbers, strings, or homogeneous [arrays]); ``#`` starts a comment;
+parameter tokens match on their last word ("uniform float roughness");
+the current transform keeps the pre-WorldBegin camera transform, so world
+geometry lands in camera space and the camera sits at the origin looking
+down +z; ``Translate`` / ``Rotate`` / ``Scale`` / ``ConcatTransform``
+post-multiply the current matrix (column vectors); RIB matrices are
+transposed on ingest (scene_builder.rs:1925-1938); ``LightSource``
+positions are taken as written, without the current transform
+(scene_builder.rs:1582-1635).
+
+Deviations (recorded in ``RibScene.warnings`` at load time):
+  * Quadrics (Sphere, Cylinder, Cone, Disk, Torus, Paraboloid,
+    Hyperboloid) and the emitter shapes of PxrSphereLight / PxrDiskLight
+    are tessellated into smooth-normal triangle meshes; the reference
+    intersects them analytically.
+  * SubdivisionMesh renders its control cage; Curves, Points, patches,
+    dome lights, patterns, displacement, media and motion blur are skipped
+    (motion blocks use their first sample).
+"""
+import math
+import os
+
+import numpy as np
+
+from . import abi
+from .scene import Scene, default_material, emitter
+
+# ---- parsing (src/parser/parser.rs) --------------------------------------------------------
+
+
+class RibError(ValueError):
+    pass
+
+
+def _skip_ws(s, i):
+    n = len(s)
+    while i < n:
+        c = s[i]
+        if c in " \t\r\n\f\v":
+            i += 1
+        elif c == "#":
+            j = s.find("\n", i)
+            i = n if j < 0 else j
+        else:
+            break
+    return i
+
+
+def _string(s, i):
+    j = s.find('"', i + 1)
+    if j < 0:
+        raise RibError("unterminated string")
+    return s[i + 1:j], j + 1
+
+
+_NUM_CHARS = set("0123456789+-.eE")
+
+
+def _number(s, i):
+    j = i
+    n = len(s)
+    while j < n and s[j] in _NUM_CHARS:
+        j += 1
+    try:
+        return float(s[i:j]), j
+    except ValueError:
+        raise RibError(f"bad number near {s[i:i + 20]!r}") from None
+
+
+def parse_rib(text):
+    """List of (name, values); values are float, str, list of floats or list
+    of strings."""
+    out = []
+    i = _skip_ws(text, 0)
+    n = len(text)
+    while i < n:
+        j = i
+        while j < n and (text[j].isascii() and text[j].isalpha() or text[j] == "_"):
+            j += 1
+        if j == i:
+            raise RibError(f"failed to parse RIB near: {text[i:i + 60]!r}")
+        name = text[i:j]
+        vals = []
+        i = _skip_ws(text, j)
+        while i < n:
+            c = text[i]
+            if c == '"':
+                v, i = _string(text, i)
+                vals.append(v)
+            elif c == "[":
+                i = _skip_ws(text, i + 1)
+                if i < n and text[i] == '"':
+                    arr = []
+                    while True:
+                        i = _skip_ws(text, i)
+                        if i >= n:
+                            raise RibError("unterminated array")
+                        if text[i] == "]":
+                            i += 1
+                            break
+                        v, i = _string(text, i)
+                        arr.append(v)
+                    vals.append(arr)
+                else:
+                    arr = []
+                    while True:
+                        i = _skip_ws(text, i)
+                        if i >= n:
+                            raise RibError("unterminated array")
+                        if text[i] == "]":
+                            i += 1
+                            break
+                        v, i = _number(text, i)
+                        arr.append(v)
+                    vals.append([float(x) for x in arr])
+            elif c.isdigit() or c in "+-.":
+                v, i = _number(text, i)
+                vals.append(v)
+            else:
+                break
+            i = _skip_ws(text, i)
+        out.append((name, vals))
+    return out
+
+
+def _as_number(v):
+    if isinstance(v, float):
+        return v
+    if isinstance(v, list) and len(v) == 1 and isinstance(v[0], float):
+        return v[0]
+    return None
+
+
+def _as_numbers(v):
+    if isinstance(v, float):
+        return [v]
+    if isinstance(v, list) and all(isinstance(x, float) for x in v):
+        return v
+    return None
+
+
+def _as_str(v):
+    if isinstance(v, str):
+        return v
+    if isinstance(v, list) and len(v) == 1 and isinstance(v[0], str):
+        return v[0]
+    return None
+
+
+class _Params:
+    """Token/value pairs from a value index on (ast.rs:63-112)."""
+
+    def __init__(self, vals, start):
+        self.pairs = []
+        i = start
+        while i + 1 < len(vals):
+            t = _as_str(vals[i])
+            if t is None:
+                break
+            self.pairs.append((t, vals[i + 1]))
+            i += 2
+
+    def get(self, name):
+        for t, v in self.pairs:
+            w = t.split()
+            if w and w[-1] == name:
+                return v
+        return None
+
+    def number(self, name):
+        v = self.get(name)
+        return None if v is None else _as_number(v)
+
+    def numbers(self, name):
+        v = self.get(name)
+        return None if v is None else _as_numbers(v)
+
+    def string(self, name):
+        v = self.get(name)
+        return None if v is None else _as_str(v)
+
+
+def _num(vals, k):
+    return _as_number(vals[k]) if k < len(vals) else None
+
+
+def _str(vals, k):
+    return _as_str(vals[k]) if k < len(vals) else None
+
+
+# ---- matrices (src/math/matrix.rs; column-vector convention) --------------------------------
+
+
+def _translate(x, y, z):
+    m = np.eye(4)
+    m[:3, 3] = (x, y, z)
+    return m
+
+
+def _scale(x, y, z):
+    return np.diag([x, y, z, 1.0])
+
+
+def _rotate(angle, x, y, z):
+    a = np.array([x, y, z], dtype=np.float64)
+    ln = np.linalg.norm(a)
+    if ln > 1e-6:
+        a = a / ln
+    x, y, z = a
+    r = math.radians(angle)
+    c, s = math.cos(r), math.sin(r)
+    t = 1.0 - c
+    m = np.eye(4)
+    m[:3, :3] = [[c + x * x * t, x * y * t - z * s, x * z * t + y * s],
+                 [y * x * t + z * s, c + y * y * t, y * z * t - x * s],
+                 [z * x * t - y * s, z * y * t + x * s, c + z * z * t]]
+    return m
+
+
+def _from_rib(v):
+    return np.array(v, dtype=np.float64).reshape(4, 4).T
+
+
+def _xf_point(m, p):
+    q = m @ np.array([p[0], p[1], p[2], 1.0])
+    return q[:3] / q[3] if abs(q[3] - 1.0) >= 1e-6 else q[:3]
+
+
+def _xf_vec(m, v):
+    return m[:3, :3] @ np.asarray(v, dtype=np.float64)
+
+
+# ---- quadric tessellation ----------------------------------------------------------------------
+
+
+def _grid(fn, nu, nv):
+    """Parametric surface on [0,1]^2 -> (positions, normals, indices); fn
+    maps (u, v) arrays to (points (..,3), normals (..,3))."""
+    u = np.linspace(0.0, 1.0, nu + 1)
+    v = np.linspace(0.0, 1.0, nv + 1)
+    U, V = np.meshgrid(u, v)  # (nv+1, nu+1)
+    P, N = fn(U, V)
+    P = P.reshape(-1, 3)
+    N = N.reshape(-1, 3)
+    nn = np.linalg.norm(N, axis=1, keepdims=True)
+    N = np.where(nn > 1e-12, N / np.maximum(nn, 1e-300), np.array([0.0, 0.0, 1.0]))
+    idx = []
+    w = nu + 1
+    for j in range(nv):
+        for i in range(nu):
+            a, b, c, d = j * w + i, j * w + i + 1, (j + 1) * w + i + 1, (j + 1) * w + i
+            idx += [(a, b, c), (a, c, d)]
+    I = np.array(idx, dtype=np.int64)
+    # Wind every triangle like its vertex normals.
+    g = np.cross(P[I[:, 1]] - P[I[:, 0]], P[I[:, 2]] - P[I[:, 0]])
+    flip = np.einsum("ij,ij->i", g, N[I].sum(axis=1)) < 0
+    I[flip] = I[flip][:, [0, 2, 1]]
+    area = np.linalg.norm(g, axis=1)
+    I = I[area > 0]
+    return P.astype(np.float32), N.astype(np.float32), I.astype(np.uint32)
+
+
+def _segments(thetamax):
+    return max(8, int(math.ceil(64 * abs(thetamax) / 360.0)))
+
+
+def tessellate(kind, a):
+    """Triangle mesh of a RenderMan quadric (RiSpec parameterisations)."""
+    if kind == "Sphere":
+        r, zmin, zmax, tm = a
+        cl = lambda x: max(-1.0, min(1.0, x))
+        p0, p1 = math.asin(cl(zmin / r)), math.asin(cl(zmax / r))
+
+        def f(U, V):
+            th = U * math.radians(tm)
+            ph = p0 + V * (p1 - p0)
+            n = np.stack([np.cos(ph) * np.cos(th), np.cos(ph) * np.sin(th), np.sin(ph)], -1)
+            return r * n, n if r > 0 else -n
+        return _grid(f, _segments(tm), 32)
+    if kind == "Cylinder":
+        r, zmin, zmax, tm = a
+
+        def f(U, V):
+            th = U * math.radians(tm)
+            P = np.stack([r * np.cos(th), r * np.sin(th), zmin + V * (zmax - zmin)], -1)
+            return P, np.stack([np.cos(th), np.sin(th), np.zeros_like(th)], -1)
+        return _grid(f, _segments(tm), 1)
+    if kind == "Cone":
+        h, r, tm = a
+
+        def f(U, V):
+            th = U * math.radians(tm)
+            P = np.stack([r * (1 - V) * np.cos(th), r * (1 - V) * np.sin(th), V * h], -1)
+            return P, np.stack([h * np.cos(th), h * np.sin(th), np.full_like(th, r)], -1)
+        return _grid(f, _segments(tm), 1)
+    if kind == "Disk":
+        h, r, tm = a
+
+        def f(U, V):
+            th = U * math.radians(tm)
+            P = np.stack([r * (1 - V) * np.cos(th), r * (1 - V) * np.sin(th), np.full_like(th, h)], -1)
+            return P, np.stack([np.zeros_like(th), np.zeros_like(th), np.ones_like(th)], -1)
+        return _grid(f, _segments(tm), 1)
+    if kind == "Torus":
+        R, rr, pmin, pmax, tm = a
+
+        def f(U, V):
+            th = U * math.radians(tm)
+            ph = math.radians(pmin) + V * math.radians(pmax - pmin)
+            n = np.stack([np.cos(ph) * np.cos(th), np.cos(ph) * np.sin(th), np.sin(ph)], -1)
+            P = np.stack([(R + rr * np.cos(ph)) * np.cos(th), (R + rr * np.cos(ph)) * np.sin(th), rr * np.sin(ph)], -1)
+            return P, n
+        return _grid(f, _segments(tm), 32)
+    if kind == "Paraboloid":
+        rmax, zmin, zmax, tm = a
+        k = zmax / (rmax * rmax) if rmax != 0 else 0.0
+
+        def f(U, V):
+            th = U * math.radians(tm)
+            z = zmin + V * (zmax - zmin)
+            rad = rmax * np.sqrt(np.maximum(z / zmax, 0.0)) if zmax != 0 else np.zeros_like(z)
+            P = np.stack([rad * np.cos(th), rad * np.sin(th), z], -1)
+            N = np.stack([2 * k * P[..., 0], 2 * k * P[..., 1], -np.ones_like(z)], -1)
+            return P, N
+        return _grid(f, _segments(tm), 16)
+    if kind == "Hyperboloid":
+        p1, p2, tm = np.array(a[0:3]), np.array(a[3:6]), a[6]
+
+        def f(U, V):
+            th = U * math.radians(tm)
+            q = p1[None, None, :] * (1 - V)[..., None] + p2[None, None, :] * V[..., None]
+            c, s = np.cos(th), np.sin(th)
+            P = np.stack([q[..., 0] * c - q[..., 1] * s, q[..., 0] * s + q[..., 1] * c, q[..., 2]], -1)
+            dv = p2 - p1
+            Dv = np.stack([dv[0] * c - dv[1] * s, dv[0] * s + dv[1] * c, np.full_like(th, dv[2])], -1)
+            Dt = np.stack([-P[..., 1], P[..., 0], np.zeros_like(th)], -1)
+            return P, np.cross(Dt, Dv)
+        return _grid(f, _segments(tm), 1)
+    raise RibError(f"unknown quadric {kind}")
+
+
+MAX_ARCHIVE_DEPTH = 16
+
+_QUADRIC_ARGS = {"Sphere": 4, "Cylinder": 4, "Cone": 3, "Disk": 3, "Torus": 5, "Paraboloid": 4, "Hyperboloid": 7}
+
+# ---- materials (src/scene/material.rs, src/scene/pbr.rs) ------------------------------------
+
+
+def _pbr_matte(c):
+    m = default_material()
+    m.update(diffuse_gain=1.0, diffuse_color=tuple(c), specular_ior=1.0)
+    return m
+
+
+def _pbr_plastic(c, rough):
+    m = default_material()
+    m.update(diffuse_gain=0.9, diffuse_color=tuple(c), specular_ior=1.5, specular_roughness=max(rough, 0.02))
+    return m
+
+
+def _pbr_metal(c, rough):
+    m = default_material()
+    m.update(diffuse_gain=0.0, specular_face_color=tuple(c), specular_edge_color=(1.0, 1.0, 1.0),
+             specular_roughness=max(rough, 0.02))
+    return m
+
+
+def _pbr_bxdf(p):
+    """PbrParams::from_bxdf_params (pbr.rs:133-187)."""
+    m = default_material()
+    m.update(diffuse_gain=1.0, diffuse_color=(0.18, 0.18, 0.18), specular_ior=1.5, specular_roughness=0.2)
+    colors = {"diffuseColor": "diffuse_color", "specularFaceColor": "specular_face_color",
+              "specularEdgeColor": "specular_edge_color", "fuzzColor": "fuzz_color",
+              "refractionColor": "refraction_color"}
+    scalars = {"diffuseGain": "diffuse_gain", "diffuseRoughness": "diffuse_roughness",
+               "specularRoughness": "specular_roughness", "specularIor": "specular_ior",
+               "clearcoatGain": "clearcoat_gain", "clearcoatRoughness": "clearcoat_roughness",
+               "fuzzGain": "fuzz_gain", "glassRefractionGain": "glass_gain", "glassIor": "glass_ior",
+               "glassRoughness": "glass_roughness", "presence": "presence"}
+    for tok, key in colors.items():
+        v = p.numbers(tok)
+        if v is not None and len(v) >= 3:
+            m[key] = tuple(v[:3])
+    for tok, key in scalars.items():
+        v = p.number(tok)
+        if v is not None:
+            m[key] = v
+    gg = p.number("glowGain") or 0.0
+    gc = p.numbers("glowColor")
+    gc = tuple(gc[:3]) if gc is not None and len(gc) >= 3 else (1.0, 1.0, 1.0)
+    m["glow"] = tuple(c * gg for c in gc)
+    for key in ("specular_roughness", "glass_roughness", "clearcoat_roughness"):
+        m[key] = min(max(m[key], 0.005), 1.0)
+    return m
+
+
+class _State:
+    def __init__(self):
+        self.color = (1.0, 1.0, 1.0)
+        self.surface = "matte"
+        self.roughness = 0.1
+        self.area_light = None   # (intensity, color)
+        self.bxdf = None         # material dict
+        self.identifier = None
+
+    def copy(self):
+        s = _State()
+        s.__dict__.update(self.__dict__)
+        return s
+
+
+class RibScene(Scene):
+    """An rtcuda Scene built from a RIB file; ``pixel_samples`` and
+    ``warnings`` as the reference's Scene keeps them."""
+
+    def __init__(self, width, height, fov):
+        super().__init__(width, height, fov)
+        self.pixel_samples = (1, 1)
+        self.warnings = []
+
+    @property
+    def spp(self):
+        return self.pixel_samples[0] * self.pixel_samples[1]
+
+
+class _Builder:
+    def __init__(self, base_dir=None):
+        self.width, self.height, self.fov = 640, 480, 45.0
+        self.dof = None
+        self.filter = (abi.FILTER_BOX, 1.0)
+        self.pixel_samples = (1, 1)
+        self.background = (0.0, 0.0, 0.0)
+        self.state = _State()
+        self.attr_stack = []
+        self.xf = [np.eye(4)]
+        self.base_dir = base_dir
+        self.archives = {}
+        self.recording = None
+        self.object_defs = {}
+        self.defining = None
+        self.archive_depth = 0
+        self.object_ids = {}
+        self.next_id = 1
+        self.warned = []
+        self.motion = None
+        # scene contents (materials / lights / meshes / instances)
+        self.meshes, self.instances, self.materials, self.lights = [], [], [], []
+
+    # -- helpers ------------------------------------------------------------------
+    def warn(self, msg):
+        if msg not in self.warned:
+            self.warned.append(msg)
+
+    @property
+    def ctm(self):
+        return self.xf[-1]
+
+    def apply(self, m):
+        self.xf[-1] = self.xf[-1] @ m
+
+    def object_id(self):
+        name = self.state.identifier or f"object_{self.next_id}"
+        if name in self.object_ids:
+            return self.object_ids[name]
+        i = self.next_id
+        self.next_id += 1
+        self.object_ids[name] = i
+        return i
+
+    def make_material(self):
+        """SceneBuilder::make_material (scene_builder.rs:1850-1877)."""
+        st = self.state
+        if st.bxdf is not None:
+            m = dict(st.bxdf)
+        elif st.surface == "plastic":
+            m = _pbr_plastic(st.color, st.roughness)
+        elif st.surface == "metal":
+            m = _pbr_metal(st.color, st.roughness)
+        else:
+            m = _pbr_matte(st.color)
+        m["id"] = self.object_id()
+        return m
+
+    def add_material(self, m):
+        self.materials.append(m)
+        return len(self.materials) - 1
+
+    def add_light(self, type_, intensity, color, p=(0, 0, 0), e1=(0, 0, 0), e2=(0, 0, 0), radius=0.0):
+        self.lights.append(dict(type=type_, intensity=float(intensity), color=tuple(color), p=tuple(p),
+                                e1=tuple(e1), e2=tuple(e2), radius=float(radius)))
+        return len(self.lights) - 1
+
+    def add_mesh(self, P, I, N=None):
+        self.meshes.append((np.asarray(P, np.float32).reshape(-1, 3), np.asarray(I, np.uint32).reshape(-1, 3),
+                            None if N is None else np.asarray(N, np.float32).reshape(-1, 3)))
+        return len(self.meshes) - 1
+
+    def place(self, mesh, mat, xf):
+        self.instances.append((mesh, mat, np.asarray(xf, np.float64)[:3, :].reshape(12)))
+
+    def tessellated_mesh(self, P, I, N=None, emissive=True):
+        """add_tessellated_mesh (scene_builder.rs:1195-1234); quadrics take
+        the plain state material (no area-light emission, :813-909)."""
+        mesh = self.add_mesh(P, I, N)
+        m = self.make_material()
+        if emissive and self.state.area_light is not None:
+            inten, col = self.state.area_light
+            m["emission"] = tuple(c * inten for c in col)
+        mat = self.add_material(m)
+        if self.defining is not None:
+            self.defining[1].append((mesh, self.ctm.copy(), mat))
+        else:
+            self.place(mesh, mat, self.ctm)
+
+    # -- requests -------------------------------------------------------------------
+    def run(self, reqs):
+        for name, vals in reqs:
+            if self.recording is not None:
+                if name == "ArchiveEnd":
+                    self.archives[self.recording[0]] = self.recording[1]
+                    self.recording = None
+                else:
+                    self.recording[1].append((name, vals))
+                continue
+            if self.motion is not None and name != "MotionEnd":
+                self.motion.append((name, vals))
+                continue
+            self.process(name, vals)
+
+    def process(self, name, vals):
+        st = self.state
+        if name in ("version", "WorldEnd", "FrameBegin", "FrameEnd", "WorldBegin", "IfBegin", "ElseIf", "Else",
+                    "IfEnd", "Display", "Clipping", "ClippingPlane", "CropWindow", "FrameAspectRatio",
+                    "PixelVariance", "Exposure", "Quantize", "Hider", "Integrator", "TextureCoordinates",
+                    "ShadingInterpolation", "RelativeDetail", "Declare", "Orientation", "ReverseOrientation",
+                    "Sides", "ShadingRate", "Opacity", "Basis", "CoordinateSystem", "ScopedCoordinateSystem",
+                    "Shutter", "ArchiveEnd"):
+            return
+        if name == "AttributeBegin":
+            self.attr_stack.append(st.copy())
+            self.xf.append(self.ctm.copy())
+        elif name == "AttributeEnd":
+            if self.attr_stack:
+                self.state = self.attr_stack.pop()
+            if len(self.xf) > 1:
+                self.xf.pop()
+        elif name == "TransformBegin":
+            self.xf.append(self.ctm.copy())
+        elif name == "TransformEnd":
+            if len(self.xf) > 1:
+                self.xf.pop()
+        elif name == "MotionBegin":
+            self.motion = []
+        elif name == "MotionEnd":
+            block, self.motion = self.motion or [], None
+            if block:
+                self.warn("motion blur is not rendered: motion blocks use their first sample")
+                self.process(*block[0])
+        elif name == "ArchiveBegin":
+            self.recording = (_str(vals, 0) or "", [])
+        elif name == "ReadArchive":
+            self.read_archive(_str(vals, 0))
+        elif name == "ObjectBegin":
+            h = _str(vals, 0) or (str(_num(vals, 0)) if _num(vals, 0) is not None else "0")
+            self.attr_stack.append(st.copy())
+            self.xf.append(np.eye(4))
+            self.defining = (h, [])
+        elif name == "ObjectEnd":
+            if self.defining is not None:
+                self.object_defs[self.defining[0]] = self.defining[1]
+                self.defining = None
+            if self.attr_stack:
+                self.state = self.attr_stack.pop()
+            if len(self.xf) > 1:
+                self.xf.pop()
+        elif name == "ObjectInstance":
+            h = _str(vals, 0) or (str(_num(vals, 0)) if _num(vals, 0) is not None else "0")
+            entries = self.object_defs.get(h)
+            if entries is None:
+                self.warn(f'ObjectInstance "{h}" has no definition')
+            else:
+                for mesh, local, mat in entries:
+                    self.place(mesh, mat, self.ctm @ local)
+        elif name == "Format":
+            w, h = _num(vals, 0), _num(vals, 1)
+            if w is not None and h is not None:
+                self.width, self.height = int(w), int(h)
+        elif name == "Projection":
+            kind = _str(vals, 0)
+            if kind == "perspective":
+                fov = _Params(vals, 1).number("fov")
+                if fov is not None:
+                    self.fov = fov
+            elif kind is not None:
+                self.warn(f'Projection "{kind}" not rendered; using perspective')
+        elif name == "DepthOfField":
+            a = [_num(vals, k) for k in range(3)]
+            if all(x is not None for x in a):
+                self.dof = tuple(a)
+        elif name == "PixelFilter":
+            f = _str(vals, 0)
+            if f is not None:
+                xw = _num(vals, 1)
+                xw = 2.0 if xw is None else xw
+                yw = _num(vals, 2)
+                yw = xw if yw is None else yw
+                w = (xw + yw) * 0.5
+                kinds = {"triangle": abi.FILTER_TRIANGLE, "gaussian": abi.FILTER_GAUSSIAN, "box": abi.FILTER_BOX}
+                self.filter = (kinds[f], max(w, 1e-3)) if f in kinds else (abi.FILTER_BOX, 1.0)
+        elif name == "ScreenWindow":
+            self.warn("ScreenWindow only affects orthographic cameras; ignored")
+        elif name == "PixelSamples":
+            x, y = _num(vals, 0), _num(vals, 1)
+            if x is not None and y is not None:
+                self.pixel_samples = (max(int(x), 1), max(int(y), 1))
+        elif name in ("Option", "Attribute"):
+            cat = _str(vals, 0)
+            p = _Params(vals, 1)
+            if name == "Attribute" and cat == "identifier":
+                nm = p.string("name")
+                if nm is not None:
+                    st.identifier = nm
+            if name == "Option" and cat == "background":
+                c = p.numbers("color")
+                if c is not None and len(c) >= 3:
+                    self.background = tuple(c[:3])
+        elif name == "Identity":
+            self.xf[-1] = np.eye(4)
+        elif name in ("Transform", "ConcatTransform"):
+            m = _as_numbers(vals[0]) if vals else None
+            if m is not None and len(m) == 16:
+                if name == "Transform":
+                    self.xf[-1] = _from_rib(m)
+                else:
+                    self.apply(_from_rib(m))
+        elif name == "Translate":
+            a = [_num(vals, k) for k in range(3)]
+            if all(x is not None for x in a):
+                self.apply(_translate(*a))
+        elif name == "Rotate":
+            a = [_num(vals, k) for k in range(4)]
+            if all(x is not None for x in a):
+                self.apply(_rotate(*a))
+        elif name == "Scale":
+            a = [_num(vals, k) for k in range(3)]
+            if all(x is not None for x in a):
+                self.apply(_scale(*a))
+        elif name == "Color":
+            c = self.color_from(vals)
+            if c is not None:
+                st.color = c
+        elif name == "Surface":
+            s = _str(vals, 0)
+            if s is not None:
+                st.surface = s
+                r = _Params(vals, 1).number("roughness")
+                st.roughness = 0.1 if r is None else r
+        elif name == "Bxdf":
+            t = _str(vals, 0) or ""
+            if t == "PxrMarschnerHair":
+                self.warn("hair is not rendered on this path; PxrMarschnerHair treated as PxrSurface")
+            elif t != "PxrSurface":
+                self.warn(f'Bxdf "{t}" not implemented; treating as PxrSurface')
+            st.bxdf = _pbr_bxdf(_Params(vals, 2 if len(vals) % 2 == 0 else 1))
+        elif name == "AreaLightSource":
+            p = _Params(vals, 2 if len(vals) % 2 == 0 else 1)
+            inten = p.number("intensity")
+            col = p.numbers("lightcolor")
+            st.area_light = (1.0 if inten is None else inten,
+                             tuple(col[:3]) if col is not None and len(col) >= 3 else (1.0, 1.0, 1.0))
+        elif name == "LightSource":
+            self.light_source(vals)
+        elif name == "Light":
+            self.pxr_light(vals)
+        elif name == "Polygon":
+            self.polygon(vals)
+        elif name == "GeneralPolygon":
+            nl = _as_numbers(vals[0]) if vals else None
+            p = _Params(vals, 1).numbers("P")
+            if nl and p:
+                n0 = int(nl[0])
+                if len(nl) > 1:
+                    self.warn("GeneralPolygon holes are not supported; using the outer loop")
+                self.polygon(["P", p[:3 * n0]])
+        elif name in ("PointsPolygons", "PointsGeneralPolygons", "SubdivisionMesh", "HierarchicalSubdivisionMesh"):
+            self.points_polygons(name, vals)
+        elif name in _QUADRIC_ARGS:
+            a = [_num(vals, k) for k in range(_QUADRIC_ARGS[name])]
+            if all(x is not None for x in a):
+                if self.defining is not None:
+                    self.warn(f"{name} inside ObjectBegin is not instanced; skipping")
+                    return
+                self.warn("quadrics are tessellated into triangle meshes (the reference intersects them exactly)")
+                P, N, I = tessellate(name, a)
+                self.tessellated_mesh(P, I, N, emissive=False)
+        else:
+            self.warn(f"RIB request '{name}' not rendered on this path; skipping")
+
+    def color_from(self, vals):
+        a = [_num(vals, k) for k in range(3)]
+        if all(x is not None for x in a):
+            return tuple(a)
+        v = _as_numbers(vals[0]) if vals else None
+        return tuple(v[:3]) if v is not None and len(v) >= 3 else None
+
+    def read_archive(self, name):
+        """read_archive (scene_builder.rs:1448-1476): inline archives first,
+        then a file beside the scene; a missing or unparsable file warns."""
+        if name is None:
+            return
+        if self.archive_depth >= MAX_ARCHIVE_DEPTH:
+            self.warn(f'ReadArchive "{name}": max depth exceeded; skipping')
+            return
+        if name in self.archives:
+            reqs = self.archives[name]
+        else:
+            path = name if os.path.isabs(name) or self.base_dir is None else os.path.join(self.base_dir, name)
+            try:
+                with open(path, "r", encoding="utf-8", errors="replace") as f:
+                    reqs = parse_rib(f.read())
+            except OSError as e:
+                self.warn(f'ReadArchive "{name}": {e.strerror}')
+                return
+            except RibError as e:
+                self.warn(f'ReadArchive "{name}": parse error: {e}')
+                return
+        self.archive_depth += 1
+        try:
+            self.run(reqs)
+        finally:
+            self.archive_depth -= 1
+
+    def polygon(self, vals):
+        """Polygon (scene_builder.rs:911-950): a fan of triangles; with an
+        area light on the state, a quad is also a sampleable rect light."""
+        p = _Params(vals, 0).numbers("P")
+        if p is None or len(p) < 9:
+            return
+        if self.defining is not None:
+            self.warn("Polygon inside ObjectBegin is not instanced; skipping")
+            return
+        nv = len(p) // 3
+        P = np.array(p[:3 * nv], dtype=np.float64).reshape(nv, 3)
+        m = self.make_material()
+        if self.state.area_light is not None:
+            inten, col = self.state.area_light
+            m["emission"] = tuple(c * inten for c in col)
+            if len(p) == 12:
+                c0 = _xf_point(self.ctm, P[0])
+                e1 = _xf_point(self.ctm, P[1]) - c0
+                e2 = _xf_point(self.ctm, P[3]) - c0
+                m["area_light"] = self.add_light(abi.LIGHT_RECT, inten, col, p=c0, e1=e1, e2=e2)
+        mat = self.add_material(m)
+        I = [(0, i, i + 1) for i in range(1, nv - 1)]
+        self.place(self.add_mesh(P, I), mat, self.ctm)
+
+    def points_polygons(self, name, vals):
+        """points_polygons (scene_builder.rs:982-1051): fan-triangulated
+        polygons with optional per-vertex normals."""
+        if name == "PointsGeneralPolygons":
+            nl = _as_numbers(vals[0]) if vals else None
+            if nl is None:
+                return
+            if any(int(n) != 1 for n in nl):
+                self.warn("PointsGeneralPolygons holes are not supported; using outer loops only")
+            vals = vals[1:]
+        elif name != "PointsPolygons":
+            self.warn(f"{name} renders its control mesh (no subdivision on this path)")
+            # SubdivisionMesh "scheme" [nverts] [verts] ([tags] [nargs] [ints] [floats]) params;
+            # HierarchicalSubdivisionMesh adds [strings] after [floats].
+            ntag = 5 if name == "HierarchicalSubdivisionMesh" else 4
+            tagged = len(vals) > 3 + ntag and isinstance(vals[3], list)
+            vals = vals[1:3] + vals[3 + ntag:] if tagged else vals[1:]
+        nverts = _as_numbers(vals[0]) if len(vals) > 0 else None
+        verts = _as_numbers(vals[1]) if len(vals) > 1 else None
+        if nverts is None or verts is None:
+            return
+        prm = _Params(vals, 2)
+        p = prm.numbers("P")
+        if p is None:
+            self.warn(f"{name} without \"P\"; skipping")
+            return
+        P = np.array(p, dtype=np.float64).reshape(-1, 3)
+        n = prm.numbers("N")
+        N = None
+        if n is not None:
+            if len(n) == len(p):
+                N = np.array(n, dtype=np.float64).reshape(-1, 3)
+            else:
+                self.warn(f"{name} \"N\" is not per-vertex; ignoring normals")
+        tris, cur = [], 0
+        for nv in nverts:
+            nv = int(nv)
+            if cur + nv > len(verts):
+                break
+            poly = verts[cur:cur + nv]
+            for i in range(1, nv - 1):
+                tris.append((int(poly[0]), int(poly[i]), int(poly[i + 1])))
+            cur += nv
+        if not tris:
+            return
+        I = np.array(tris, dtype=np.int64)
+        if I.max() >= len(P):
+            raise RibError(f"{name}: vertex index out of range")
+        self.tessellated_mesh(P, I, N)
+
+    def light_source(self, vals):
+        """parse_light (scene_builder.rs:1582-1635): positions untransformed."""
+        t = _str(vals, 0)
+        p = _Params(vals, 2 if len(vals) % 2 == 0 else 1)
+        inten = p.number("intensity")
+        inten = 1.0 if inten is None else inten
+        if t == "pointlight":
+            f = p.numbers("from")
+            pos = tuple(f[:3]) if f is not None and len(f) >= 3 else (0.0, 0.0, 0.0)
+            if p.string("iesProfile") is not None:
+                self.warn("IES profiles are not rendered on this path; pointlight is isotropic")
+            self.add_light(abi.LIGHT_POINT, inten, (1.0, 1.0, 1.0), p=pos)
+        elif t == "distantlight":
+            f, to = p.numbers("from"), p.numbers("to")
+            f = np.array(f[:3]) if f is not None and len(f) >= 3 else np.array([0.0, 0.0, -10.0])
+            to = np.array(to[:3]) if to is not None and len(to) >= 3 else np.zeros(3)
+            d = to - f
+            ln = np.linalg.norm(d)
+            d = d / ln if ln > 1e-6 else d
+            self.add_light(abi.LIGHT_DISTANT, inten, (1.0, 1.0, 1.0), e1=d)
+        elif t is not None:
+            self.warn(f'LightSource "{t}" not rendered on this path; skipping')
+
+    def pxr_light(self, vals):
+        """build_light (scene_builder.rs:1488-1580)."""
+        t = _str(vals, 0)
+        if t is None:
+            return
+        p = _Params(vals, 2 if len(vals) % 2 == 0 else 1)
+        inten = p.number("intensity")
+        inten = 1.0 if inten is None else inten
+        exposure = p.number("exposure") or 0.0
+        scale = inten * 2.0 ** exposure
+        col = p.numbers("lightColor")
+        col = tuple(col[:3]) if col is not None and len(col) >= 3 else (1.0, 1.0, 1.0)
+        xf = self.ctm
+        origin = _xf_point(xf, (0, 0, 0))
+
+        def emitter_mat(li):
+            return self.add_material(emitter(tuple(c * scale for c in col), area_light=li))
+
+        if t == "PxrRectLight":
+            corner = _xf_point(xf, (-0.5, -0.5, 0))
+            li = self.add_light(abi.LIGHT_RECT, scale, col, p=corner, e1=_xf_vec(xf, (1, 0, 0)),
+                                e2=_xf_vec(xf, (0, 1, 0)))
+            P = np.array([[-0.5, -0.5, 0], [0.5, -0.5, 0], [0.5, 0.5, 0], [-0.5, 0.5, 0]])
+            self.place(self.add_mesh(P, [(0, 1, 2), (0, 2, 3)]), emitter_mat(li), xf)
+        elif t == "PxrSphereLight":
+            radius = float(np.linalg.norm(_xf_vec(xf, (0.5, 0, 0))))
+            li = self.add_light(abi.LIGHT_SPHERE, scale, col, p=origin, radius=radius)
+            P, N, I = tessellate("Sphere", (0.5, -0.5, 0.5, 360.0))
+            self.warn("quadrics are tessellated into triangle meshes (the reference intersects them exactly)")
+            self.place(self.add_mesh(P, I, N), emitter_mat(li), xf)
+        elif t == "PxrDiskLight":
+            li = self.add_light(abi.LIGHT_DISK, scale, col, p=origin, e1=_xf_vec(xf, (0.5, 0, 0)),
+                                e2=_xf_vec(xf, (0, 0.5, 0)))
+            P, N, I = tessellate("Disk", (0.0, 0.5, 360.0))
+            self.warn("quadrics are tessellated into triangle meshes (the reference intersects them exactly)")
+            self.place(self.add_mesh(P, I, N), emitter_mat(li), xf)
+        elif t == "PxrDistantLight":
+            d = _xf_vec(xf, (0, 0, -1))
+            ln = np.linalg.norm(d)
+            d = d / ln if ln > 1e-6 else d
+            ang = p.number("angleExtent")
+            ang = 0.53 if ang is None else ang
+            self.add_light(abi.LIGHT_DISTANT, scale, col, e1=d, radius=math.radians(ang * 0.5))
+        elif t == "PxrDomeLight":
+            self.warn("PxrDomeLight is not rendered on this path; skipping")
+        else:
+            self.warn(f'Light "{t}" not implemented; skipping')
+
+    def scene(self):
+        s = RibScene(self.width, self.height, self.fov)
+        for P, I, N in self.meshes:
+            s.add_mesh(P, I, N)
+        for m in self.materials:
+            s.add_material(m)
+        for l in self.lights:
+            s._light(l["type"], l["intensity"], l["color"], p=l["p"], e1=l["e1"], e2=l["e2"], radius=l["radius"])
+        if self.instances:
+            s.add_instances([i[0] for i in self.instances], [i[1] for i in self.instances],
+                            np.stack([i[2] for i in self.instances]))
+        s.filter, s.filter_width = self.filter
+        if self.dof is not None:
+            fstop, flen, fdist = self.dof
+            if math.isfinite(fstop) and fstop > 0:
+                s.lens_radius, s.focal_distance = flen / (2.0 * fstop), fdist
+        s.background = self.background
+        s.pixel_samples = self.pixel_samples
+        s.warnings = list(self.warned)
+        return s
+
+
+def load_rib_string(text, base_dir=None):
+    """A RibScene from RIB text (ReadArchive paths resolve against base_dir)."""
+    b = _Builder(base_dir)
+    b.run(parse_rib(text))
+    return b.scene()
+
+
+def load_rib(path):
+    """A RibScene from a RIB file (SceneBuilder::with_base_dir(dir of path))."""
+    with open(path, "r", encoding="utf-8", errors="replace") as f:
+        text = f.read()
+    return load_rib_string(text, os.path.dirname(os.path.abspath(path)))

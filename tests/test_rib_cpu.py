@@ -1,0 +1,205 @@
+"""RIB ingest (rtcuda.rib): the reference's tokenizer rules
+(src/parser/parser.rs and its tests) and SceneBuilder semantics
+(src/parser/scene_builder.rs) checked on RIB text written here; the
+reference's own fixture files are parsed too when they are available."""
+import glob
+import math
+import os
+
+import numpy as np
+import pytest
+
+from rtcuda import abi
+from rtcuda.rib import load_rib, load_rib_string, parse_rib, tessellate
+
+
+def test_tokenizer_values():
+    r = parse_rib('Display "out.ppm" "file" "rgb"\nSphere 1.0 -1.0 1.0 360 # comment\n'
+                  'ConcatTransform [1 0 0 0 0 1 0 0 0 0 1 0 -2.5e-1 0 3 1]\n'
+                  'Procedural "DelayedReadArchive" ["big.rib"] [-1 1 -1 1 -1 1]\n'
+                  'SubdivisionMesh "catmull-clark" [4] [0 1 2 3] [] [] [] [] "P" [0 0 0 1 0 0 1 1 0 0 1 0]')
+    assert [n for n, _ in r] == ["Display", "Sphere", "ConcatTransform", "Procedural", "SubdivisionMesh"]
+    assert r[0][1] == ["out.ppm", "file", "rgb"]
+    assert r[1][1] == [1.0, -1.0, 1.0, 360.0]
+    assert len(r[2][1][0]) == 16 and abs(r[2][1][0][12] + 0.25) < 1e-12
+    assert r[3][1][1] == ["big.rib"] and r[3][1][2] == [-1.0, 1.0, -1.0, 1.0, -1.0, 1.0]
+    assert r[4][1][3] == []
+
+
+def test_inline_declarations_match_last_word():
+    s = load_rib_string('Surface "plastic" "uniform float roughness" [0.25] "Ks" 0.6\nPolygon "P" [0 0 5 1 0 5 0 1 5]')
+    m = s.materials[0]
+    assert m["specular_ior"] == 1.5 and m["diffuse_gain"] == 0.9 and m["specular_roughness"] == 0.25
+
+
+CORNELL = """
+Format 64 48 1.0
+PixelSamples 4 2
+Projection "perspective" "fov" [36]
+PixelFilter "triangle" 2 2
+WorldBegin
+  AttributeBegin
+    AreaLightSource "arealight" "ceiling" "intensity" [17] "lightcolor" [1 0.9 0.75]
+    Translate 0 0 1
+    Polygon "P" [-0.25 0.995 3.95  0.25 0.995 3.95  0.25 0.995 4.45  -0.25 0.995 4.45]
+  AttributeEnd
+  AttributeBegin
+    Color 0.73 0.73 0.73
+    Surface "matte"
+    Polygon "P" [-1 -1 3  1 -1 3  1 -1 5  -1 -1 5]
+  AttributeEnd
+  AttributeBegin
+    Color [0.95 0.93 0.88]
+    Surface "metal" "roughness" [0.01]
+    Translate 0.4 -0.65 3.9
+    Sphere 0.35 -0.35 0.35 360
+  AttributeEnd
+  LightSource "pointlight" 1 "from" [0 0.5 4] "intensity" [3]
+WorldEnd
+"""
+
+
+def test_cornell_like_scene():
+    s = load_rib_string(CORNELL)
+    assert (s.width, s.height, s.fov, s.spp) == (64, 48, 36.0, 8)
+    assert s.filter == abi.FILTER_TRIANGLE and s.filter_width == 2.0
+    np.testing.assert_array_equal(s.eye, 0)
+    np.testing.assert_array_equal(s.forward, [0, 0, 1])
+    np.testing.assert_array_equal(s.right, [1, 0, 0])
+    # The area-light quad is a sampleable rect light in world space (after its Translate).
+    rect = [l for l in s.lights if l["type"] == abi.LIGHT_RECT]
+    assert len(rect) == 1
+    np.testing.assert_allclose(rect[0]["p"], (-0.25, 0.995, 4.95))
+    np.testing.assert_allclose(rect[0]["e1"], (0.5, 0, 0))
+    np.testing.assert_allclose(rect[0]["e2"], (0, 0, 0.5))
+    assert rect[0]["intensity"] == 17 and rect[0]["color"] == (1.0, 0.9, 0.75)
+    emat = s.materials[0]
+    np.testing.assert_allclose(emat["emission"], (17, 15.3, 12.75))
+    assert emat["area_light"] == s.lights.index(rect[0])
+    # Legacy surfaces map to PbrParams (pbr.rs:104-131); metal roughness floors at 0.02.
+    assert s.materials[1]["diffuse_color"] == (0.73, 0.73, 0.73) and s.materials[1]["specular_ior"] == 1.0
+    metal = s.materials[2]
+    assert metal["diffuse_gain"] == 0.0 and metal["specular_face_color"] == (0.95, 0.93, 0.88)
+    assert metal["specular_roughness"] == 0.02
+    # Object ids for the id AOV: one per material, from 1.
+    assert [m["id"] for m in s.materials] == [1, 2, 3]
+    # Point light position as written (no current transform applied).
+    pt = [l for l in s.lights if l["type"] == abi.LIGHT_POINT]
+    assert pt[0]["p"] == (0.0, 0.5, 4.0) and pt[0]["intensity"] == 3.0
+    # The sphere: a smooth mesh of radius 0.35 placed by its Translate.
+    inst = s.instance_array()
+    p, i, n = s.meshes[inst["mesh"][2]]
+    np.testing.assert_allclose(np.linalg.norm(p, axis=1), 0.35, rtol=1e-6)
+    np.testing.assert_allclose(np.linalg.norm(n, axis=1), 1.0, rtol=1e-6)
+    np.testing.assert_allclose(inst["xf"][2].reshape(3, 4)[:, 3], (0.4, -0.65, 3.9))
+
+
+def test_transform_order_and_rib_matrices():
+    s = load_rib_string("Translate 1 2 3\nRotate 90 0 1 0\nScale 2 3 4\nPolygon \"P\" [0 0 0 1 0 0 0 1 0]\n"
+                        "Identity\nConcatTransform [1 0 0 0 0 1 0 0 0 0 1 0 5 6 7 1]\nPolygon \"P\" [0 0 0 1 0 0 0 1 0]")
+    xf = s.instance_array()["xf"].reshape(-1, 3, 4)
+    r = np.array([[0, 0, 1], [0, 1, 0], [-1, 0, 0]], dtype=np.float64)
+    want = np.zeros((3, 4))
+    want[:, :3] = r @ np.diag([2, 3, 4])
+    want[:, 3] = (1, 2, 3)
+    np.testing.assert_allclose(xf[0], want, atol=1e-12)
+    np.testing.assert_allclose(xf[1][:, 3], (5, 6, 7))
+
+
+def test_instancing_and_pxr_lights():
+    s = load_rib_string("""
+ObjectBegin "tri"
+  Translate 0 0 1
+  PointsPolygons [3] [0 1 2] "P" [0 0 0 1 0 0 0 1 0]
+ObjectEnd
+Translate 10 0 0
+ObjectInstance "tri"
+Translate 0 5 0
+ObjectInstance "tri"
+AttributeBegin
+  Translate 0 3 0
+  Scale 2 4 1
+  Light "PxrRectLight" "rect" "intensity" [2] "exposure" [1] "lightColor" [1 0.5 0.25]
+AttributeEnd
+Light "PxrDistantLight" "sun" "intensity" [3] "angleExtent" [1.0]
+AttributeBegin
+  Scale 3 3 3
+  Light "PxrSphereLight" "ball" "intensity" [1]
+AttributeEnd
+""")
+    inst = s.instance_array()
+    tri = inst[inst["mesh"] == 0]
+    assert len(tri) == 2
+    np.testing.assert_allclose(tri["xf"].reshape(-1, 3, 4)[:, :, 3], [(10, 0, 1), (10, 5, 1)])
+    rect = s.lights[0]
+    assert rect["type"] == abi.LIGHT_RECT and rect["intensity"] == 4.0 and rect["color"] == (1.0, 0.5, 0.25)
+    np.testing.assert_allclose(rect["p"], (9, 6, 0))  # the CTM also holds the two Translates above
+    np.testing.assert_allclose(rect["e1"], (2, 0, 0))
+    np.testing.assert_allclose(rect["e2"], (0, 4, 0))
+    sun = s.lights[1]
+    assert sun["type"] == abi.LIGHT_DISTANT
+    np.testing.assert_allclose(sun["e1"], (0, 0, -1))
+    assert abs(sun["radius"] - math.radians(0.5)) < 1e-15
+    ball = s.lights[2]
+    assert ball["type"] == abi.LIGHT_SPHERE and abs(ball["radius"] - 1.5) < 1e-12
+    # Emitters of the area lights are linked to their lights for MIS.
+    assert sorted(m["area_light"] for m in s.materials if m["area_light"] >= 0) == [0, 2]
+
+
+def test_pxr_surface_and_identifiers():
+    s = load_rib_string("""
+Attribute "identifier" "name" ["teapot"]
+Bxdf "PxrSurface" "m" "color diffuseColor" [0.2 0.3 0.4] "float specularRoughness" [0.0]
+  "float glassRefractionGain" [1] "float glowGain" [2] "color glowColor" [1 0 0.5] "float presence" [0.5]
+Polygon "P" [0 0 0 1 0 0 0 1 0]
+Polygon "P" [0 0 1 1 0 1 0 1 1]
+Option "background" "color" [0.1 0.2 0.3]
+""")
+    a, b = s.materials
+    assert a["diffuse_color"] == (0.2, 0.3, 0.4) and a["specular_roughness"] == 0.005
+    assert a["glass_gain"] == 1.0 and a["glow"] == (2.0, 0.0, 1.0) and a["presence"] == 0.5
+    assert a["id"] == b["id"] == 1
+    assert s.background == (0.1, 0.2, 0.3)
+
+
+@pytest.mark.parametrize("kind,args", [("Sphere", (1.0, -0.5, 0.8, 270.0)), ("Cylinder", (0.5, -1, 1, 360.0)),
+                                       ("Cone", (2.0, 0.5, 360.0)), ("Disk", (0.3, 1.0, 180.0)),
+                                       ("Torus", (1.0, 0.25, 0.0, 360.0, 360.0)),
+                                       ("Paraboloid", (1.0, 0.1, 2.0, 360.0)),
+                                       ("Hyperboloid", (1.0, 0.0, -1.0, 0.5, 0.5, 1.0, 360.0))])
+def test_quadric_tessellation(kind, args):
+    P, N, I = tessellate(kind, args)
+    assert len(I) > 8 and I.max() < len(P)
+    np.testing.assert_allclose(np.linalg.norm(N, axis=1), 1.0, rtol=1e-5)
+    g = np.cross(P[I[:, 1]] - P[I[:, 0]], P[I[:, 2]] - P[I[:, 0]])
+    assert (np.einsum("ij,ij->i", g, N[I].sum(axis=1)) > 0).all()  # windings follow the normals
+    if kind == "Sphere":
+        np.testing.assert_allclose(np.linalg.norm(P, axis=1), 1.0, rtol=1e-6)
+        assert P[:, 2].min() >= -0.5 - 1e-6 and P[:, 2].max() <= 0.8 + 1e-6
+    if kind == "Torus":
+        rho = np.hypot(np.hypot(P[:, 0], P[:, 1]) - 1.0, P[:, 2])
+        np.testing.assert_allclose(rho, 0.25, rtol=1e-5)
+
+
+def test_archives_and_missing_files(tmp_path):
+    (tmp_path / "part.rib").write_text('Polygon "P" [0 0 0 1 0 0 0 1 0]\n')
+    (tmp_path / "main.rib").write_text('ArchiveBegin "inline"\nPolygon "P" [0 0 1 1 0 1 0 1 1]\nArchiveEnd\n'
+                                       'ReadArchive "part.rib"\nReadArchive "inline"\nReadArchive "nope.rib"\n')
+    s = load_rib(str(tmp_path / "main.rib"))
+    assert len(s.meshes) == 2
+    assert any("nope.rib" in w for w in s.warnings)
+
+
+FIXTURES = "/root/reference/tests/fixtures"
+
+
+@pytest.mark.skipif(not os.path.isdir(FIXTURES), reason="the reference's fixture files are not on this machine")
+def test_reference_fixtures_load():
+    files = sorted(glob.glob(os.path.join(FIXTURES, "*.rib")))
+    assert files
+    for f in files:
+        s = load_rib(f)
+        assert s.width > 0 and s.height > 0, f
+    c = load_rib(os.path.join(FIXTURES, "cornell.rib"))
+    assert (c.width, c.height, c.spp) == (600, 600, 64)
+    assert [l["type"] for l in c.lights] == [abi.LIGHT_RECT]
