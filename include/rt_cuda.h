@@ -200,6 +200,37 @@ int rt_set_adaptive(rt_session* s, double tol);
  * renderer.rs:586-591): the mean of the accumulator's weight channel. */
 int rt_average_spp(rt_session* s, double* out);
 
+/* The AOV film (src/output/film.rs: Film) of a session created with
+ * params.aovs = 1, RT_FILM_FLOATS floats per pixel at the offsets below:
+ * beauty, diffuse, specular (max(beauty - diffuse, 0)), albedo, normal (RGB /
+ * XYZ), depth (mean over the samples that hit), id and its coverage. Decoded
+ * on the device from the accumulator and the AOV sums as render_pt_film
+ * (src/raytracer/metal/renderer.rs:180-217), each pixel by its own sample
+ * count. */
+#define RT_FILM_FLOATS 18
+#define RT_FILM_BEAUTY 0
+#define RT_FILM_DIFFUSE 3
+#define RT_FILM_SPECULAR 6
+#define RT_FILM_ALBEDO 9
+#define RT_FILM_NORMAL 12
+#define RT_FILM_DEPTH 15
+#define RT_FILM_ID 16
+int rt_read_film(rt_session* s, float* film);
+
+/* The denoised beauty (3 floats per pixel) of a session's film (needs
+ * params.aovs = 1) or of a film held by the caller (rt_denoise_film, run on
+ * the current device): the reference's edge-avoiding a-trous filter
+ * (src/output/denoise.rs:28-139; diffuse demodulated by albedo, 5 passes
+ * guided by normal, depth and object id, specular added back). */
+int rt_denoise(rt_session* s, float* rgb);
+int rt_denoise_film(const float* film, uint32_t width, uint32_t height, float* rgb);
+
+/* A film as the reference's multilayer EXR (src/output/multilayer.rs:
+ * channels R G B, diffuse.*, specular.*, albedo.*, N.*, depth.Z, id.x,
+ * id.coverage in name order; layer "rgba"; the id manifest "id:name;..." in
+ * the render_rs/manifest attribute, NULL for none). Host only. */
+int rt_film_exr_write(const char* path, uint32_t width, uint32_t height, const float* film, const char* manifest);
+
 /* The session's learned directional proposal (rt_guide.h) when it renders
  * guided, else NULL. The session owns the handle: callers may pass it to
  * rt_guide_infer / rt_guide_get_params to inspect what the network has

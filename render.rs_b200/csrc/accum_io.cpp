@@ -175,10 +175,10 @@ int exr_read(const char* path, Exr* out, bool header_only) {
             p++;
             break;
         }
-        std::string name((const char*)&d[p]);
+        std::string name((const char*)&d[p], strnlen((const char*)&d[p], d.size() - p));
         p += name.size() + 1;
         if (p >= d.size()) return fail_io(RT_ERR_IO, bad + "truncated header");
-        std::string type((const char*)&d[p]);
+        std::string type((const char*)&d[p], strnlen((const char*)&d[p], d.size() - p));
         p += type.size() + 1;
         if (p + 4 > d.size()) return fail_io(RT_ERR_IO, bad + "truncated header");
         const uint32_t sz = get_u32(&d[p]);
@@ -188,7 +188,7 @@ int exr_read(const char* path, Exr* out, bool header_only) {
         if (name == "channels") {
             size_t q = 0;
             while (q < sz && v[q]) {
-                std::string cn((const char*)v + q);
+                std::string cn((const char*)v + q, strnlen((const char*)v + q, sz - q));
                 q += cn.size() + 1;
                 if (q + 16 > sz) return fail_io(RT_ERR_IO, bad + "bad channel list");
                 if (get_u32(v + q + 8) != 1u || get_u32(v + q + 12) != 1u)
@@ -384,6 +384,78 @@ int rt_rckp_write(const char* path, uint32_t width, uint32_t height, uint32_t pa
     if (!ok || rename(tmp.c_str(), path) != 0) {
         remove(tmp.c_str());
         return fail_io(RT_ERR_IO, std::string("cannot write checkpoint ") + path);
+    }
+    return RT_OK;
+}
+
+int rt_film_exr_write(const char* path, uint32_t width, uint32_t height, const float* film, const char* manifest) {
+    if (!path || !film || !width || !height) return fail_io(RT_ERR_INVALID, "NULL argument or empty image");
+    // (name, film offset) in byte order of the names, as the reference sorts them.
+    static const struct {
+        const char* name;
+        int off;
+    } ch[RT_FILM_FLOATS] = {{"B", RT_FILM_BEAUTY + 2},        {"G", RT_FILM_BEAUTY + 1},
+                            {"N.X", RT_FILM_NORMAL},          {"N.Y", RT_FILM_NORMAL + 1},
+                            {"N.Z", RT_FILM_NORMAL + 2},      {"R", RT_FILM_BEAUTY},
+                            {"albedo.B", RT_FILM_ALBEDO + 2}, {"albedo.G", RT_FILM_ALBEDO + 1},
+                            {"albedo.R", RT_FILM_ALBEDO},     {"depth.Z", RT_FILM_DEPTH},
+                            {"diffuse.B", RT_FILM_DIFFUSE + 2}, {"diffuse.G", RT_FILM_DIFFUSE + 1},
+                            {"diffuse.R", RT_FILM_DIFFUSE},   {"id.coverage", RT_FILM_ID + 1},
+                            {"id.x", RT_FILM_ID},             {"specular.B", RT_FILM_SPECULAR + 2},
+                            {"specular.G", RT_FILM_SPECULAR + 1}, {"specular.R", RT_FILM_SPECULAR}};
+    std::vector<uint8_t> b;
+    put_u32(b, 20000630u);
+    put_u32(b, 2u);
+    std::vector<uint8_t> v;
+    for (const auto& c : ch) {
+        put_str(v, c.name);
+        put_u32(v, 2u);
+        put_u32(v, 0u);
+        put_u32(v, 1u);
+        put_u32(v, 1u);
+    }
+    v.push_back(0);
+    put_attr(b, "channels", "chlist", v);
+    put_attr(b, "compression", "compression", {0});
+    v.clear();
+    for (uint32_t x : {0u, 0u, width - 1, height - 1}) put_u32(v, x);
+    put_attr(b, "dataWindow", "box2i", v);
+    put_attr(b, "displayWindow", "box2i", v);
+    put_attr(b, "lineOrder", "lineOrder", {0});
+    v.assign({'r', 'g', 'b', 'a'});
+    put_attr(b, "name", "string", v);
+    v.clear();
+    put_f32(v, 1.0f);
+    put_attr(b, "pixelAspectRatio", "float", v);
+    if (manifest && *manifest) {
+        v.assign(manifest, manifest + strlen(manifest));
+        put_attr(b, "render_rs/manifest", "string", v);
+    }
+    v.clear();
+    put_f32(v, 0.0f);
+    put_f32(v, 0.0f);
+    put_attr(b, "screenWindowCenter", "v2f", v);
+    v.clear();
+    put_f32(v, 1.0f);
+    put_attr(b, "screenWindowWidth", "float", v);
+    b.push_back(0);
+    const uint64_t line_bytes = 8ull + 4ull * RT_FILM_FLOATS * width;
+    const uint64_t first = b.size() + 8ull * height;
+    for (uint32_t y = 0; y < height; y++) put_u64(b, first + y * line_bytes);
+    for (uint32_t y = 0; y < height; y++) {
+        put_u32(b, y);
+        put_u32(b, 4u * RT_FILM_FLOATS * width);
+        for (const auto& c : ch)
+            for (uint32_t x = 0; x < width; x++) put_f32(b, film[(size_t)RT_FILM_FLOATS * ((size_t)y * width + x) + c.off]);
+    }
+    std::string tmp = std::string(path) + ".tmp";
+    FILE* f = fopen(tmp.c_str(), "wb");
+    if (!f) return fail_io(RT_ERR_IO, "cannot open " + tmp);
+    bool ok = fwrite(b.data(), 1, b.size(), f) == b.size();
+    ok = (fclose(f) == 0) && ok;
+    if (!ok || rename(tmp.c_str(), path) != 0) {
+        remove(tmp.c_str());
+        return fail_io(RT_ERR_IO, std::string("cannot write ") + path);
     }
     return RT_OK;
 }

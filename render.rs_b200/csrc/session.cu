@@ -100,6 +100,8 @@ constexpr int SHADE_BLOCK = 128;
 
 namespace rt {
 std::string& accum_error() { return g_err; }
+int film_decode_device(const double* accum, const float* aux, uint32_t npix, float* film, cudaStream_t st);
+int denoise_device(const float* film, uint32_t w, uint32_t h, float* rgb, cudaStream_t st);
 }  // namespace rt
 
 struct rt_session {
@@ -594,6 +596,38 @@ int rt_checkpoint_save(rt_session* s, const char* path) {
         return fail(RT_ERR_IO, std::string("cannot write checkpoint ") + path);
     }
     return RT_OK;
+}
+
+int rt_read_film(rt_session* s, float* film) {
+    if (!s || !film) return fail(RT_ERR_INVALID, "NULL argument");
+    if (!s->params.aovs) return fail(RT_ERR_INVALID, "the session was created without AOVs (params.aovs = 0)");
+    float* d = nullptr;
+    CUDA_TRY(pool_alloc((void**)&d, 4ull * RT_FILM_FLOATS * s->npix, s->stream));
+    int rc = film_decode_device(s->accum, s->aux, s->npix, d, s->stream);
+    cudaError_t e = rc ? cudaSuccess
+                       : cudaMemcpyAsync(film, d, 4ull * RT_FILM_FLOATS * s->npix, cudaMemcpyDeviceToHost, s->stream);
+    pool_free(d, s->stream);
+    cudaStreamSynchronize(s->stream);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(RT_ERR_CUDA, std::string("film read-back: ") + cudaGetErrorString(e));
+    return RT_OK;
+}
+
+int rt_denoise(rt_session* s, float* rgb) {
+    if (!s || !rgb) return fail(RT_ERR_INVALID, "NULL argument");
+    if (!s->params.aovs) return fail(RT_ERR_INVALID, "the session was created without AOVs (params.aovs = 0)");
+    float *d = nullptr, *o = nullptr;
+    CUDA_TRY(pool_alloc((void**)&d, 4ull * RT_FILM_FLOATS * s->npix, s->stream));
+    cudaError_t e = pool_alloc((void**)&o, 12ull * s->npix, s->stream);
+    int rc = e != cudaSuccess ? fail(RT_ERR_OOM, "denoise buffers") : RT_OK;
+    rc = rc ? rc : film_decode_device(s->accum, s->aux, s->npix, d, s->stream);
+    rc = rc ? rc : denoise_device(d, s->S.width, s->S.height, o, s->stream);
+    if (!rc && cudaMemcpyAsync(rgb, o, 12ull * s->npix, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess)
+        rc = fail(RT_ERR_CUDA, "denoise read-back failed");
+    pool_free(d, s->stream);
+    if (o) pool_free(o, s->stream);
+    cudaStreamSynchronize(s->stream);
+    return rc;
 }
 
 int rt_checkpoint_save_rckp(rt_session* s, const char* path) {

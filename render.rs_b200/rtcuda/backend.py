@@ -31,7 +31,8 @@ EXPORTS = ("rt_session_create", "rt_session_destroy", "rt_last_error", "rt_rende
            "rt_intersect_batch", "rt_intersect_batch_device", "rt_get_stats", "rt_session_stream",
            "rt_bsdf_furnace", "rt_intersect_batch_noalloc", "rt_session_guide", "rt_set_adaptive",
            "rt_average_spp", "rt_checkpoint_save_rckp", "rt_rckp_write", "rt_accum_exr_write",
-           "rt_accum_exr_info", "rt_accum_exr_read", "rt_accum_merge")
+           "rt_accum_exr_info", "rt_accum_exr_read", "rt_accum_merge", "rt_read_film", "rt_denoise",
+           "rt_denoise_film", "rt_film_exr_write")
 
 
 class RtError(RuntimeError):
@@ -92,6 +93,10 @@ def lib():
         L.rt_accum_exr_info.argtypes = [C.c_char_p, C.POINTER(u32), C.POINTER(u32)]
         L.rt_accum_exr_read.argtypes = [C.c_char_p, u32, u32, vp]
         L.rt_accum_merge.argtypes = [C.POINTER(C.c_char_p), u32, u32, u32, vp]
+        L.rt_read_film.argtypes = [vp, vp]
+        L.rt_denoise.argtypes = [vp, vp]
+        L.rt_denoise_film.argtypes = [vp, u32, u32, vp]
+        L.rt_film_exr_write.argtypes = [C.c_char_p, u32, u32, vp, C.c_char_p]
         _lib = L
     return _lib
 
@@ -168,6 +173,22 @@ class PtSession:
 
     def checkpoint_save(self, path):
         _check(lib().rt_checkpoint_save(self.h, os.fsencode(path)))
+
+    def film_array(self):
+        """(H, W, 18) f32 film decoded on the device (RT_FILM_* layout)."""
+        a = np.empty((self.height, self.width, FILM_FLOATS), dtype=np.float32)
+        _check(lib().rt_read_film(self.h, a.ctypes.data))
+        return a
+
+    def film(self):
+        """The AOV film as a dict of layers (src/output/film.rs: Film)."""
+        return film_layers(self.film_array())
+
+    def denoise(self):
+        """output::denoise of this session's film (needs aovs=True), (H, W, 3)."""
+        a = np.empty((self.height, self.width, 3), dtype=np.float32)
+        _check(lib().rt_denoise(self.h, a.ctypes.data))
+        return a
 
     def checkpoint_save_rckp(self, path):
         """The Metal backend's f32 checkpoint format (renderer.rs:219-236)."""
@@ -252,6 +273,43 @@ def render_pt_checkpointed(scene, spp, checkpoint=None, every=4, **kw):
             if checkpoint:
                 s.checkpoint_save(checkpoint)
         return s.image()
+
+
+FILM_FLOATS = 18
+FILM_LAYERS = {"beauty": (0, 3), "diffuse": (3, 3), "specular": (6, 3), "albedo": (9, 3), "normal": (12, 3),
+               "depth": (15, 1), "id": (16, 2)}
+
+
+def film_layers(arr):
+    """Dict of layers from an (H, W, 18) film array."""
+    return {k: arr[..., o:o + n] for k, (o, n) in FILM_LAYERS.items()}
+
+
+def film_array(film):
+    """(H, W, 18) f32 film array from a dict of layers."""
+    h, w = film["beauty"].shape[:2]
+    a = np.zeros((h, w, FILM_FLOATS), dtype=np.float32)
+    for k, (o, n) in FILM_LAYERS.items():
+        a[..., o:o + n] = np.asarray(film[k], dtype=np.float32).reshape(h, w, -1)[..., :n]
+    return a
+
+
+def denoise_film(film):
+    """output::denoise (src/output/denoise.rs:28-139) on the GPU for a film
+    dict or (H, W, 18) array; returns the (H, W, 3) beauty."""
+    a = np.ascontiguousarray(film if isinstance(film, np.ndarray) else film_array(film), dtype=np.float32)
+    h, w = a.shape[:2]
+    out = np.empty((h, w, 3), dtype=np.float32)
+    _check(lib().rt_denoise_film(a.ctypes.data, w, h, out.ctypes.data))
+    return out
+
+
+def write_multilayer_exr(film, path, manifest=None):
+    """write_multilayer_exr (src/output/multilayer.rs): manifest {id: name}."""
+    a = np.ascontiguousarray(film if isinstance(film, np.ndarray) else film_array(film), dtype=np.float32)
+    h, w = a.shape[:2]
+    m = ";".join(f"{k}:{v}" for k, v in sorted(manifest.items())).encode() if manifest else None
+    _check(lib().rt_film_exr_write(os.fsencode(path), w, h, a.ctypes.data, m))
 
 
 def decode_film(beauty, aux, spp):
