@@ -240,16 +240,13 @@ __global__ void k_tri_gather(const BPrim* __restrict__ P0, const float* __restri
     }
 }
 
-// Leaf-order instance records.
-__global__ void k_inst_gather(const BPrim* __restrict__ P0, const float4* __restrict__ xf_in,
-                              const uint4* __restrict__ rec_in, uint32_t n, float4* __restrict__ xf_out,
-                              uint4* __restrict__ rec_out) {
+// Leaf-order TLAS items.
+__global__ void k_item_gather(const BPrim* __restrict__ P0, const uint2* __restrict__ in, uint32_t n,
+                              uint2* __restrict__ out) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     uint32_t i = __float_as_uint(P0[k].a.w);
-    if (i >= n) return;
-    for (int r = 0; r < 3; r++) xf_out[3ull * k + r] = xf_in[3ull * i + r];
-    rec_out[k] = rec_in[i];
+    if (i < n) out[k] = in[i];
 }
 
 // ---- binary build: level passes over nodes of more than SMALL primitives ------------
@@ -837,6 +834,26 @@ __global__ void k_wide_root_index(WideS* W, const uint32_t* root_idx, uint32_t n
     if (s < n) W[s].idx = root_idx[s];
 }
 
+// The children of every BLAS root (boxes and final references) for the
+// TLAS items; needs the preorder indices.
+__global__ void k_root_children(const WideS* __restrict__ W, uint32_t R, const BNode* __restrict__ nodes,
+                                RootChild* __restrict__ out, uint32_t* __restrict__ nk_out) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= R) return;
+    const WideS w = W[r];
+    nk_out[r] = w.nk;
+    for (uint32_t k = 0; k < w.nk && k < 8; k++) {
+        const BNode c = nodes[w.kids[k]];
+        RootChild rc;
+        for (int a = 0; a < 3; a++) {
+            rc.lo[a] = c.lo[a];
+            rc.hi[a] = c.hi[a];
+        }
+        rc.ref = c.count > 0 ? make_leaf_ref(c.first, c.count) : (w.child[k] != NONE ? W[w.child[k]].idx : REF_EMPTY);
+        out[8ull * r + k] = rc;
+    }
+}
+
 // Quantisation grid of one axis (the host's choose_grid): origin p, a
 // multiple of s = 2^e, with every p + q*s (q in 0..255) an exact f32 and
 // p + 255*s >= hi. floor(log2) and ceil(log2) are taken exactly from the
@@ -1170,9 +1187,8 @@ int wide_structure(Scratch& D, const BNode* nodes, uint32_t n_nodes, uint32_t R,
     return RT_OK;
 }
 
-// Preorder indices from the roots' indices, then every node's words.
-int wide_write(Scratch& D, WideTree& T, const BNode* nodes, const std::vector<uint32_t>& root_idx, uint4* out,
-               uint64_t out_nodes, uint32_t* d_err, cudaStream_t st, std::string* err) {
+// Preorder indices from the roots' indices.
+int wide_index(Scratch& D, WideTree& T, const std::vector<uint32_t>& root_idx, cudaStream_t st, std::string* err) {
     const uint32_t R = (uint32_t)root_idx.size();
     if (T.n == 0) return RT_OK;
     uint32_t* d_root;
@@ -1184,6 +1200,14 @@ int wide_write(Scratch& D, WideTree& T, const BNode* nodes, const std::vector<ui
         uint32_t lo = T.level_off[l], hi = T.level_off[l + 1];
         if (hi > lo) k_wide_index<<<blocks_for(hi - lo, JB), JB, 0, st>>>(T.W, lo, hi);
     }
+    BV_TRY(cudaGetLastError());
+    return RT_OK;
+}
+
+// Every node's 6 words (after wide_index).
+int wide_words(WideTree& T, const BNode* nodes, uint4* out, uint64_t out_nodes, uint32_t* d_err, cudaStream_t st,
+               std::string* err) {
+    if (T.n == 0) return RT_OK;
     k_wide_write<<<blocks_for(T.n, JB), JB, 0, st>>>(T.W, T.n, nodes, 0, out, out_nodes, d_err);
     BV_TRY(cudaGetLastError());
     return RT_OK;
@@ -1215,12 +1239,7 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
     // ---- BLAS: every mesh's triangles in one primitive array ----------------------
     uint32_t blas_total = 0;
     std::vector<uint32_t> blas_root(M, 0xFFFFFFFFu);
-    std::vector<double> mesh_bounds(6ull * M);
-    for (uint32_t m = 0; m < M; m++)
-        for (int a = 0; a < 3; a++) {
-            mesh_bounds[6ull * m + a] = INFINITY;
-            mesh_bounds[6ull * m + 3 + a] = -INFINITY;
-        }
+    std::vector<std::vector<RootChild>> root_children(M);
     BNode* bnodes = nullptr;
     WideTree bw;
     BPrim *P0 = nullptr, *P1 = nullptr;
@@ -1283,56 +1302,70 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
         H->binary_blas_nodes = n_bnodes;
         rc = wide_structure(D, bnodes, n_bnodes, (uint32_t)roots.size(), d_err, &bw, st, err);
         if (rc) return rc;
-        std::vector<BNode> rb(roots.size());
-        BV_TRY(cudaMemcpyAsync(rb.data(), bnodes, rb.size() * sizeof(BNode), cudaMemcpyDeviceToHost, st));
-        BV_TRY(cudaStreamSynchronize(st));
+        std::vector<uint32_t> ridx(roots.size());
         for (size_t r = 0; r < roots.size(); r++) {
             const uint32_t m = root_mesh[r];
             blas_root[m] = blas_total;
+            ridx[r] = blas_total;
             blas_total += bw.root_sizes[r];
-            for (int a = 0; a < 3; a++) {
-                mesh_bounds[6ull * m + a] = rb[r].lo[a];
-                mesh_bounds[6ull * m + 3 + a] = rb[r].hi[a];
-            }
         }
+        rc = wide_index(D, bw, ridx, st, err);
+        if (rc) return rc;
+        // The BLAS roots' children become the TLAS items.
+        const uint32_t R = (uint32_t)roots.size();
+        RootChild* d_rc;
+        uint32_t* d_nk;
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_rc, 8ull * R, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_nk, R, st, err);
+        if (rc) return rc;
+        k_root_children<<<blocks_for(R, JB), JB, 0, st>>>(bw.W, R, bnodes, d_rc, d_nk);
+        std::vector<RootChild> hrc(8ull * R);
+        std::vector<uint32_t> hnk(R);
+        BV_TRY(cudaMemcpyAsync(hrc.data(), d_rc, hrc.size() * sizeof(RootChild), cudaMemcpyDeviceToHost, st));
+        BV_TRY(cudaMemcpyAsync(hnk.data(), d_nk, 4ull * R, cudaMemcpyDeviceToHost, st));
+        BV_TRY(cudaStreamSynchronize(st));
+        for (uint32_t r = 0; r < R; r++)
+            root_children[root_mesh[r]].assign(hrc.begin() + 8ull * r, hrc.begin() + 8ull * r + std::min(hnk[r], 8u));
     }
     for (uint32_t m = 0; m < M; m++) H->meshes[m].blas_root = blas_root[m];
     H->blas_nodes = blas_total;
 
-    // ---- TLAS ---------------------------------------------------------------------------
+    // ---- TLAS over instance subtrees ------------------------------------------------------
     const uint32_t NI = d->n_instances;
     BNode* tnodes = nullptr;
     WideTree tw;
     BPrim* Q0 = nullptr;
-    uint32_t tlas_total = 0;
+    uint32_t tlas_total = 0, NIT = 0;
     std::vector<float4> xf;
     std::vector<uint4> rec;
+    std::vector<uint2> items;
     if (NI) {
-        std::vector<double> boxes, invs;
-        instance_boxes(d, mesh_bounds.data(), &boxes, &invs, H);
-        std::vector<float> prims(8ull * NI);
-        prim_records(boxes, prims.data());
-        xf.resize(3ull * NI);
-        rec.resize(NI);
-        for (uint32_t i = 0; i < NI; i++) {
-            const double* v = &invs[12ull * i];
-            for (int r = 0; r < 3; r++)
-                xf[3ull * i + r] = make_float4((float)v[r * 4], (float)v[r * 4 + 1], (float)v[r * 4 + 2], (float)v[r * 4 + 3]);
-            const rt_instance_desc& id = d->instances[i];
-            rec[i] = make_uint4(blas_root[id.mesh_id], i, id.material_id, id.mesh_id);
+        std::vector<double> boxes;
+        tlas_items(d, root_children, &boxes, &items, H);
+        if (items.size() >= (1ull << 27)) {
+            *err = "more than 2^27 instance subtrees";
+            return RT_ERR_INVALID;
         }
-        BPrim* Q1;
-        rc = rc ? rc : dev_alloc(D.ptrs, &Q0, NI, st, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &Q1, NI, st, err);
-        if (rc) return rc;
-        BV_TRY(cudaMemcpyAsync(Q0, prims.data(), prims.size() * 4, cudaMemcpyHostToDevice, st));
-        uint32_t n_tnodes = 0;
-        rc = build_binary_device(D, Q0, Q1, NI, {{0u, NI}}, d_err, &tnodes, &n_tnodes, st, err);
-        if (rc) return rc;
-        rc = wide_structure(D, tnodes, n_tnodes, 1, d_err, &tw, st, err);
-        if (rc) return rc;
-        tlas_total = tw.root_sizes[0];
-        H->scalars.tlas_root = blas_total;
+        NIT = (uint32_t)items.size();
+        instance_records(d, *H, &xf, &rec);
+        if (NIT) {
+            std::vector<float> prims(8ull * NIT);
+            prim_records(boxes, prims.data());
+            BPrim* Q1;
+            rc = rc ? rc : dev_alloc(D.ptrs, &Q0, NIT, st, err);
+            rc = rc ? rc : dev_alloc(D.ptrs, &Q1, NIT, st, err);
+            if (rc) return rc;
+            BV_TRY(cudaMemcpyAsync(Q0, prims.data(), prims.size() * 4, cudaMemcpyHostToDevice, st));
+            uint32_t n_tnodes = 0;
+            rc = build_binary_device(D, Q0, Q1, NIT, {{0u, NIT}}, d_err, &tnodes, &n_tnodes, st, err);
+            if (rc) return rc;
+            rc = wide_structure(D, tnodes, n_tnodes, 1, d_err, &tw, st, err);
+            if (rc) return rc;
+            tlas_total = tw.root_sizes[0];
+            H->scalars.tlas_root = blas_total;
+            rc = wide_index(D, tw, {blas_total}, st, err);
+            if (rc) return rc;
+        }
     }
     H->tlas_nodes = tlas_total;
 
@@ -1343,25 +1376,25 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
     rc = rc ? rc : dev_alloc(out->allocations, &out->tris, 3 * N, st, err);
     rc = rc ? rc : dev_alloc(out->allocations, &out->inst_xf, 3ull * NI, st, err);
     rc = rc ? rc : dev_alloc(out->allocations, &out->inst, NI, st, err);
+    rc = rc ? rc : dev_alloc(out->allocations, &out->items, NIT, st, err);
     if (rc) return rc;
     if (N) {
-        std::vector<uint32_t> ridx(roots.size());
-        for (size_t r = 0; r < roots.size(); r++) ridx[r] = blas_root[root_mesh[r]];
-        rc = wide_write(D, bw, bnodes, ridx, out->nodes, total, d_err, st, err);
+        rc = wide_words(bw, bnodes, out->nodes, total, d_err, st, err);
         if (rc) return rc;
         k_tri_gather<<<blocks_for(N, 256), 256, 0, st>>>(P0, d_pos, d_idx, d_tri_base, d_vbase, M, (uint32_t)N, out->tris);
     }
     if (NI) {
-        rc = wide_write(D, tw, tnodes, {blas_total}, out->nodes, total, d_err, st, err);
+        BV_TRY(cudaMemcpyAsync(out->inst_xf, xf.data(), xf.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
+        BV_TRY(cudaMemcpyAsync(out->inst, rec.data(), rec.size() * sizeof(uint4), cudaMemcpyHostToDevice, st));
+    }
+    if (NIT) {
+        rc = wide_words(tw, tnodes, out->nodes, total, d_err, st, err);
         if (rc) return rc;
-        float4* d_xf;
-        uint4* d_rec;
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_xf, 3ull * NI, st, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_rec, NI, st, err);
+        uint2* d_items;
+        rc = dev_alloc(D.ptrs, &d_items, NIT, st, err);
         if (rc) return rc;
-        BV_TRY(cudaMemcpyAsync(d_xf, xf.data(), xf.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
-        BV_TRY(cudaMemcpyAsync(d_rec, rec.data(), rec.size() * sizeof(uint4), cudaMemcpyHostToDevice, st));
-        k_inst_gather<<<blocks_for(NI, 256), 256, 0, st>>>(Q0, d_xf, d_rec, NI, out->inst_xf, out->inst);
+        BV_TRY(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
+        k_item_gather<<<blocks_for(NIT, 256), 256, 0, st>>>(Q0, d_items, NIT, out->items);
     }
     BV_TRY(cudaGetLastError());
     uint32_t e = 0;

@@ -11,12 +11,14 @@
 
 namespace rt {
 
-// Device arrays of a built scene (cudaMalloc'd; the caller frees them).
+// Device arrays of a built scene (from the device memory pool of devmem.h;
+// the caller returns them).
 struct DeviceBvh {
     uint4* nodes = nullptr;      // 8-wide nodes: every BLAS in mesh order, then the TLAS
     float4* tris = nullptr;      // 3 per triangle, BLAS leaf order
-    float4* inst_xf = nullptr;   // 3 per instance, TLAS leaf order
-    uint4* inst = nullptr;       // 1 per instance, TLAS leaf order
+    float4* inst_xf = nullptr;   // 3 per instance, scene order
+    uint4* inst = nullptr;       // 1 per instance, scene order
+    uint2* items = nullptr;      // TLAS primitives (instance, BLAS root child), leaf order
     uint64_t n_nodes = 0;
     std::vector<void*> allocations;
 };

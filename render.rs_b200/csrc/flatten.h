@@ -14,8 +14,9 @@ namespace rt {
 struct HostScene {
     std::vector<uint4> nodes;        // 8-wide nodes, 6 words each
     std::vector<float4> tris;        // 3 per triangle, leaf order
-    std::vector<float4> inst_xf;     // 3 per instance, TLAS leaf order
-    std::vector<uint4> inst;         // 1 per instance, TLAS leaf order
+    std::vector<float4> inst_xf;     // 3 per instance, scene order
+    std::vector<uint4> inst;         // 1 per instance, scene order
+    std::vector<uint2> items;        // TLAS primitives, leaf order
     std::vector<MeshInfo> meshes;
     std::vector<uint32_t> orig_idx;
     std::vector<float> normals;
@@ -38,12 +39,25 @@ struct HostScene {
 // their triangle ranges but no BLAS root, and vertex data is not validated.
 bool flatten_scene(const rt_scene_desc* desc, HostScene* out, std::string* err, bool build_bvh = true);
 
-// World boxes (6 doubles per instance: lo xyz, hi xyz; a far-away point
-// for empty meshes) and world-to-object 3x4 inverses (12 doubles) of the
-// instances, from the meshes' local bounds (6 doubles per mesh); sets the
-// world box in H. Instance ids must be validated.
-void instance_boxes(const rt_scene_desc* d, const double* mesh_bounds, std::vector<double>* boxes,
-                    std::vector<double>* invs, HostScene* H);
+// One child of a mesh's BLAS root: its exact box and its reference (wide
+// node index or leaf reference).
+struct RootChild {
+    float lo[3], hi[3];
+    uint32_t ref;
+};
+
+// TLAS primitives: every instance contributes one item (instance, BLAS root
+// reference) boxed by the union of its root children's world boxes, or one
+// item per root child (instance, child reference) when that splits its box
+// area well (flatten.cpp: RT_BRAID_RATIO); 6 doubles per item box. Meshes
+// without triangles contribute none. Needs H's mesh records (blas_root);
+// sets the world box in H. Instance ids must be validated.
+void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>>& root_children,
+                std::vector<double>* boxes, std::vector<uint2>* items, HostScene* H);
+
+// World-to-object 3x4 of every instance (f32, 3 float4 each, scene order)
+// and its record (BLAS root, index, material, mesh).
+void instance_records(const rt_scene_desc* d, const HostScene& H, std::vector<float4>* xf, std::vector<uint4>* rec);
 
 // Builder primitive records (8 floats each: lo xyz, index bits, hi xyz, 0)
 // of boxes given as 6 doubles: rounded outward to f32, -0 folded into +0.

@@ -2,11 +2,16 @@
 // (flatten.cpp) and the CUDA kernels (pt_kernels.cu).
 //
 // HBM layout (all arrays 16-byte aligned, read with 128-bit loads):
-//   nodes   : 8-wide BVH nodes, 96 B = 6 x uint4 each. TLAS and every BLAS
-//             share one array; the TLAS root is node 0 when instances exist.
+//   nodes   : 8-wide BVH nodes, 96 B = 6 x uint4 each. Every BLAS (in mesh
+//             order) and then the TLAS share one array.
 //   tris    : 3 x float4 per triangle in BLAS leaf order, meshes concatenated.
 //             (v0.xyz, orig tri id bits) (v1.xyz, -) (v2.xyz, -).
-//   inst_xf : 3 x float4 per instance in TLAS leaf order: world->object 3x4.
+//   items   : uint2 per TLAS primitive in TLAS leaf order: (instance,
+//             reference to one child of the instance's BLAS root). The TLAS
+//             is built over these instance subtrees (their world boxes are
+//             tighter than whole-instance boxes), so a ray enters only the
+//             parts of an instance its path crosses.
+//   inst_xf : 3 x float4 per instance (scene order): world->object 3x4.
 //   inst    : uint4 per instance: (blas root node, original instance id,
 //             material id, mesh id).
 // The reference's equivalents are 32-B binary nodes, u32 index triples into
@@ -103,6 +108,7 @@ struct DevScene {
     const float4* tris;
     const float4* inst_xf;
     const uint4* inst;
+    const uint2* items;          // TLAS primitives (instance, BLAS child ref), leaf order
     const MeshInfo* meshes;
     const uint32_t* orig_idx;    // original index triples (meshes with normals)
     const float* normals;        // per-vertex normals (meshes with normals)

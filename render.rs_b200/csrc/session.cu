@@ -242,12 +242,14 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
         S.tris = b.tris;
         S.inst_xf = b.inst_xf;
         S.inst = b.inst;
+        S.items = b.items;
     } else {
         S = H.scalars;
         rc = rc ? rc : s->upload((const uint4**)&S.nodes, H.nodes);
         rc = rc ? rc : s->upload((const float4**)&S.tris, H.tris);
         rc = rc ? rc : s->upload((const float4**)&S.inst_xf, H.inst_xf);
         rc = rc ? rc : s->upload((const uint4**)&S.inst, H.inst);
+        rc = rc ? rc : s->upload((const uint2**)&S.items, H.items);
     }
     rc = rc ? rc : s->upload(&S.meshes, H.meshes);
     rc = rc ? rc : s->upload(&S.orig_idx, H.orig_idx);

@@ -244,10 +244,6 @@ struct TraceHit {
 #define RT_DEVERR_STACK 1u
 #define RT_DEVERR_ITER 2u
 #define RT_MAX_TRAV_STEPS (1u << 22)
-// Error bits written to the device error word.
-#define RT_DEVERR_STACK 1u
-#define RT_DEVERR_ITER 2u
-#define RT_MAX_TRAV_STEPS (1u << 22)
 
 // Resumable traversal state of one ray (registers), so persistent warps can
 // advance rays a few steps at a time and refill lanes whose ray finished.
@@ -281,120 +277,10 @@ __device__ __forceinline__ bool trav_begin(const DevScene& S, TravState& ts, Tra
     st.sp = 0;
     st.base = 0;
     st.overflow = false;
-    if (S.n_instances == 0) return false;
+    if (S.tlas_root == 0xFFFFFFFFu) return false;
     ray_pre(ts.r, o, d);
     ts.cur = S.tlas_root;
     return true;
-}
-
-// Process the current reference (test a node's 8 children, enter an
-// instance, or test a leaf's triangles), then pick the next one. Returns
-// true when the query is finished (ts.found / ts.hit hold the answer).
-template <bool ANY>
-__device__ __forceinline__ bool trav_step(const DevScene& S, TravState& ts, TravStack& st, uint32_t* err) {
-    if (++ts.steps > RT_MAX_TRAV_STEPS) {
-        atomicOr(err, RT_DEVERR_ITER);
-        return true;
-    }
-    const uint32_t cur = ts.cur;
-    if (!(cur & REF_LEAF)) {
-        NodeHits h;
-        test_node(S.nodes, cur, ts.r, ts.hit.t, h);
-        uint32_t m = h.mask;
-        if (m) {
-            if (ANY) {
-                int k0 = __ffs(m) - 1;
-                uint32_t next = 0;
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    if (k == k0) next = h.ref[k];
-                    else if ((m >> k) & 1u) st.push(h.ref[k], h.tn[k]);
-                }
-                ts.cur = next;
-            } else {
-                // Push far-to-near; continue with the nearest.
-                while (__popc(m) > 1) {
-                    float bt = -1.0f;
-                    int bk = 0;
-#pragma unroll
-                    for (int k = 0; k < 8; k++)
-                        if (((m >> k) & 1u) && h.tn[k] > bt) {
-                            bt = h.tn[k];
-                            bk = k;
-                        }
-                    uint32_t rf = 0;
-#pragma unroll
-                    for (int k = 0; k < 8; k++)
-                        if (k == bk) rf = h.ref[k];
-                    st.push(rf, bt);
-                    m &= ~(1u << bk);
-                }
-                uint32_t next = 0;
-#pragma unroll
-                for (int k = 0; k < 8; k++)
-                    if ((m >> k) & 1u) next = h.ref[k];
-                ts.cur = next;
-            }
-            if (st.overflow) {
-                atomicOr(err, RT_DEVERR_STACK);
-                return true;
-            }
-            return false;
-        }
-    } else if (!ts.in_inst) {
-        // TLAS leaf: a run of instances. Defer all but the first on the
-        // stack (as one-instance leaves), then enter the first.
-        uint32_t first = cur & LEAF_FIRST_MASK;
-        uint32_t count = ((cur >> 27) & 15u) + 1u;
-        for (uint32_t k = count - 1; k >= 1; k--) st.push(make_leaf_ref(first + k, 1), 0.0f);
-        if (st.overflow) {
-            atomicOr(err, RT_DEVERR_STACK);
-            return true;
-        }
-        ts.cur_inst = first;
-        float4 x0 = __ldg(S.inst_xf + 3 * (size_t)first), x1 = __ldg(S.inst_xf + 3 * (size_t)first + 1),
-               x2 = __ldg(S.inst_xf + 3 * (size_t)first + 2);
-        uint32_t root = __ldg(&S.inst[first].x);
-        ray_pre(ts.r, xf_point(x0, x1, x2, ts.o), xf_vec(x0, x1, x2, ts.d));
-        ts.in_inst = true;
-        ts.inst_sp = st.sp;
-        if (root != 0xFFFFFFFFu) {
-            ts.cur = root;
-            return false;
-        }
-    } else {
-        // BLAS leaf: triangles in leaf order.
-        uint32_t first = cur & LEAF_FIRST_MASK;
-        uint32_t count = ((cur >> 27) & 15u) + 1u;
-        for (uint32_t k = 0; k < count; k++) {
-            const float4* tp = S.tris + 3 * (size_t)(first + k);
-            float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-            float t, b1, b2;
-            if (tri_watertight(ts.r, xyz(a), xyz(b), xyz(c), ts.hit.t, t, b1, b2)) {
-                ts.hit.t = t;
-                ts.hit.tri = first + k;
-                ts.hit.inst = ts.cur_inst;
-                ts.hit.b1 = b1;
-                ts.hit.b2 = b2;
-                ts.found = true;
-                if (ANY) return true;
-            }
-        }
-    }
-    // Pop the next entry that can still hold a closer hit; leaving an
-    // instance's BLAS restores the world-space ray.
-    for (;;) {
-        if (ts.in_inst && st.sp == ts.inst_sp) {
-            ts.in_inst = false;
-            ray_pre(ts.r, ts.o, ts.d);
-        }
-        if (st.sp == 0) return true;
-        uint2 e = st.pop();
-        if (__uint_as_float(e.y) < ts.hit.t) {
-            ts.cur = e.x;
-            return false;
-        }
-    }
 }
 
 // ---- phased traversal: node operations and leaf operations ---------------------------
@@ -509,15 +395,20 @@ __device__ __forceinline__ bool op_leaf(const DevScene& S, PhaseState& ps, TravS
             atomicOr(err, RT_DEVERR_STACK);
             return true;
         }
-        ts.cur_inst = first;
-        float4 x0 = __ldg(S.inst_xf + 3 * (size_t)first), x1 = __ldg(S.inst_xf + 3 * (size_t)first + 1),
-               x2 = __ldg(S.inst_xf + 3 * (size_t)first + 2);
-        uint32_t root = __ldg(&S.inst[first].x);
+        // TLAS item: (instance, child of its BLAS root); the child is a
+        // node to descend from or a triangle leaf tested in this leaf phase.
+        const uint2 item = __ldg(S.items + first);
+        const uint32_t inst = item.x, root = item.y;
+        ts.cur_inst = inst;
+        float4 x0 = __ldg(S.inst_xf + 3 * (size_t)inst), x1 = __ldg(S.inst_xf + 3 * (size_t)inst + 1),
+               x2 = __ldg(S.inst_xf + 3 * (size_t)inst + 2);
         ray_pre(ts.r, xf_point(x0, x1, x2, ts.o), xf_vec(x0, x1, x2, ts.d));
         ts.in_inst = true;
         ts.inst_sp = st.sp;
         ts.cur = root;
-        ps.need_pop = root == 0xFFFFFFFFu;
+        ps.need_pop = true;
+        if (root & REF_LEAF) ps.pending = root;
+        else ps.need_pop = false;
         return false;
     }
     for (uint32_t k = 0; k < count; k++) {
@@ -685,20 +576,6 @@ __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, boo
     }
     __syncwarp();
     return ANY && hit_now;
-}
-
-// Closest hit (ANY = false) or any hit (ANY = true, returns at the first
-// hit with t < t_max) of one ray, to completion. World-space ray (o, d),
-// parametric t.
-template <bool ANY>
-__device__ __forceinline__ bool trace(const DevScene& S, float3 o, float3 d, float t_max, TraceHit& hit,
-                                      TravStack& st, uint32_t* err) {
-    TravState ts;
-    if (trav_begin(S, ts, st, o, d, t_max))
-        while (!trav_step<ANY>(S, ts, st, err)) {
-        }
-    hit = ts.hit;
-    return ts.found;
 }
 
 }  // namespace rt
