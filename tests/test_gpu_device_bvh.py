@@ -44,11 +44,12 @@ def _both(scene, rays=None, spp=0, max_depth=6):
     return out
 
 
-def _check(dev, host, exact_prims=True):
+def _check(dev, host, exact_prims=True, t_ulps=0):
     assert (dev["blas"], dev["tlas"], dev["tris"]) == (host["blas"], host["tlas"], host["tris"])
     if "closest" in dev:
         (pd, idd, td), (ph, ih, th) = dev["closest"], host["closest"]
-        np.testing.assert_array_equal(td.view(np.uint32), th.view(np.uint32))
+        d = np.abs(td.view(np.int32).astype(np.int64) - th.view(np.int32).astype(np.int64))
+        assert d.max() <= t_ulps, (int(d.max()), int((d > 0).sum()))
         np.testing.assert_array_equal(pd == MISS, ph == MISS)
         if exact_prims:
             np.testing.assert_array_equal(pd, ph)
@@ -112,8 +113,13 @@ def test_degenerate_and_offset_meshes():
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     rays[1, :, :3] = d
     dev, host = _both(s, rays=rays, spp=2)
-    # Duplicated triangles tie exactly: which copy reports the hit follows leaf order.
-    _check(dev, host, exact_prims=False)
+    # Coincident centroids end in median splits, which group primitives by
+    # their order within the node (the host's swap partition and the
+    # device's stable partition leave different orders): the trees have the
+    # same shape but may group duplicates and coplanar triangles
+    # differently, so the hit copy and, on 0.003% of rays here, the last
+    # bit of t may differ.
+    _check(dev, host, exact_prims=False, t_ulps=1)
     assert (dev["closest"][0] != MISS).mean() > 0.05
 
 
