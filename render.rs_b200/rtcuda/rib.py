@@ -1,6 +1,6 @@
-"""RIB scene files -> rtcuda scenes (the reference's ``parse_rib`` +
-``SceneBuilder::build``, src/parser/parser.rs and
-src/parser/scene_builder.rs), for the part of RenderMan the CUDA path
+"""RIB scene files -> rtcuda scenes (the reference's ``parse_rib_bytes`` +
+``SceneBuilder::build``, src/parser/parser.rs, src/parser/binary.rs and
+src/parser/scene_builder.rs), text or binary RIB, for the part of RenderMan the CUDA path
 renders: triangle meshes and polygons, quadrics, instancing, legacy and
 PxrSurface materials, point / distant / area lights, the camera.
 
@@ -128,6 +128,115 @@ def parse_rib(text):
             i = _skip_ws(text, i)
         out.append((name, vals))
     return out
+
+
+# ---- binary RIB (src/parser/binary.rs: RISpec 3.2 Appendix C.2) ----------------------------
+
+
+def looks_binary(data):
+    """True when bytes >= 0200 appear outside comments (binary.rs:21-33)."""
+    in_comment = False
+    for b in data:
+        if b == 0x23:
+            in_comment = True
+        elif b == 0x0A:
+            in_comment = False
+        elif b >= 0x80 and not in_comment:
+            return True
+    return False
+
+
+def _be_uint(data, pos, n):
+    if pos + n > len(data):
+        raise RibError(f"binary RIB: truncated integer at byte {pos}")
+    return int.from_bytes(data[pos:pos + n], "big"), pos + n
+
+
+def _be_int(data, pos, n):
+    v, pos = _be_uint(data, pos, n)
+    if v >> (8 * n - 1):
+        v -= 1 << (8 * n)
+    return v, pos
+
+
+def _bin_string(data, pos):
+    if pos >= len(data):
+        raise RibError("binary RIB: truncated string")
+    code = data[pos]
+    pos += 1
+    if 0x90 <= code <= 0x9F:
+        n = code - 0x90
+    elif 0xA0 <= code <= 0xA3:
+        n, pos = _be_uint(data, pos, code - 0xA0 + 1)
+    else:
+        raise RibError(f"binary RIB: expected string code, got {code:#o}")
+    if pos + n > len(data):
+        raise RibError("binary RIB: truncated string body")
+    return data[pos:pos + n].decode("utf-8", errors="replace"), pos + n
+
+
+def decode_binary(data):
+    """Binary RIB bytes -> canonical text RIB (binary.rs:86-198): integers
+    0200-0203, fixed point 0204-0217, strings 0220-0243, float 0244, double
+    0245, request use 0246, string-token definitions 0310-0313, request
+    definition 0314, string-token references 0315-0316; other codes >= 0200
+    are skipped."""
+    out = []
+    requests, strings = {}, {}
+    pos, n = 0, len(data)
+    quote = lambda t: '"' + t.replace("\\", "\\\\").replace('"', '\\"').replace("\n", "\\n") + '"'
+    while pos < n:
+        b = data[pos]
+        if b < 0x80:
+            if b == 0x23:
+                j = data.find(b"\n", pos)
+                j = n if j < 0 else j
+                out.append(data[pos:j].decode("latin-1"))
+                pos = j
+            else:
+                out.append(chr(b))
+                pos += 1
+        elif b <= 0x83:
+            v, pos = _be_int(data, pos + 1, b - 0x80 + 1)
+            out.append(f" {v} ")
+        elif b <= 0x8F:
+            q = b - 0x84
+            d, w = q // 4, q % 4
+            raw, pos = _be_int(data, pos + 1, w + 1 + d)
+            out.append(f" {repr(raw / 256.0 ** d)} ")
+        elif b <= 0xA3:
+            t, pos = _bin_string(data, pos)
+            out.append(" " + quote(t) + " ")
+        elif b == 0xA4:
+            raw, pos = _be_uint(data, pos + 1, 4)
+            out.append(f" {str(np.frombuffer(raw.to_bytes(4, 'little'), '<f4')[0])} ")  # shortest f32 form
+        elif b == 0xA5:
+            raw, pos = _be_uint(data, pos + 1, 8)
+            out.append(f" {repr(float(np.frombuffer(raw.to_bytes(8, 'little'), '<f8')[0]))} ")
+        elif b == 0xA6:
+            if pos + 1 >= n:
+                raise RibError("binary RIB: truncated request code")
+            code = data[pos + 1]
+            pos += 2
+            if code not in requests:
+                raise RibError(f"binary RIB: request code {code} used before definition")
+            out.append(f"\n{requests[code]} ")
+        elif 0xC8 <= b <= 0xCB:
+            tok, pos = _be_uint(data, pos + 1, b - 0xC8 + 1)
+            strings[tok], pos = _bin_string(data, pos)
+        elif b == 0xCC:
+            if pos + 1 >= n:
+                raise RibError("binary RIB: truncated request def")
+            code = data[pos + 1]
+            requests[code], pos = _bin_string(data, pos + 2)
+        elif b in (0xCD, 0xCE):
+            tok, pos = _be_uint(data, pos + 1, b - 0xCD + 1)
+            if tok not in strings:
+                raise RibError(f"binary RIB: string token {tok} used before definition")
+            out.append(" " + quote(strings[tok]) + " ")
+        else:
+            pos += 1
+    return "".join(out)
 
 
 def _as_number(v):
@@ -723,8 +832,7 @@ class _Builder:
         else:
             path = name if os.path.isabs(name) or self.base_dir is None else os.path.join(self.base_dir, name)
             try:
-                with open(path, "r", encoding="utf-8", errors="replace") as f:
-                    reqs = parse_rib(f.read())
+                reqs = parse_rib(_read_text(path))
             except OSError as e:
                 self.warn(f'ReadArchive "{name}": {e.strerror}')
                 return
@@ -911,8 +1019,13 @@ def load_rib_string(text, base_dir=None):
     return b.scene()
 
 
+def _read_text(path):
+    """A RIB file's text, decoding binary RIB (parse_rib_bytes)."""
+    with open(path, "rb") as f:
+        data = f.read()
+    return decode_binary(data) if looks_binary(data) else data.decode("utf-8", errors="replace")
+
+
 def load_rib(path):
-    """A RibScene from a RIB file (SceneBuilder::with_base_dir(dir of path))."""
-    with open(path, "r", encoding="utf-8", errors="replace") as f:
-        text = f.read()
-    return load_rib_string(text, os.path.dirname(os.path.abspath(path)))
+    """A RibScene from a RIB file, text or binary (SceneBuilder::with_base_dir(dir of path))."""
+    return load_rib_string(_read_text(path), os.path.dirname(os.path.abspath(path)))

@@ -203,3 +203,78 @@ def test_reference_fixtures_load():
     c = load_rib(os.path.join(FIXTURES, "cornell.rib"))
     assert (c.width, c.height, c.spp) == (600, 600, 64)
     assert [l["type"] for l in c.lights] == [abi.LIGHT_RECT]
+
+
+# ---- binary RIB (src/parser/binary.rs) -------------------------------------------------------
+def _bin_str(t):
+    b = t.encode()
+    return (bytes([0x90 + len(b)]) if len(b) < 16 else bytes([0xA0, len(b)])) + b
+
+
+def _encode_binary(reqs):
+    """A binary RIB encoder written from RISpec 3.2 Appendix C.2: one request
+    definition (0314) per name, then uses (0246); numbers as 32-bit floats
+    (0244) or small integers (0200); strings length-prefixed; arrays kept as
+    ASCII brackets."""
+    import struct
+    out, codes = bytearray(), {}
+    for name, vals in reqs:
+        if name not in codes:
+            codes[name] = len(codes)
+            out += bytes([0xCC, codes[name]]) + _bin_str(name)
+        out += bytes([0xA6, codes[name]])
+        for v in vals:
+            items = v if isinstance(v, list) else [v]
+            if isinstance(v, list):
+                out += b"["
+            for x in items:
+                if isinstance(x, str):
+                    out += _bin_str(x)
+                elif float(x).is_integer() and -128 <= x < 128:
+                    out += bytes([0x80]) + struct.pack(">b", int(x))
+                else:
+                    out += bytes([0xA4]) + struct.pack(">f", x)
+            if isinstance(v, list):
+                out += b"]"
+    return bytes(out)
+
+
+def test_binary_rib_loads_like_text(tmp_path):
+    from rtcuda.rib import looks_binary
+    text = CORNELL.replace("0.995", "0.5").replace("0.73", "0.75").replace("0.65", "0.625")
+    data = _encode_binary(parse_rib(text))
+    assert looks_binary(data) and not looks_binary(text.encode())
+    (tmp_path / "b.rib").write_bytes(data)
+    (tmp_path / "t.rib").write_text(text)
+    a, b = load_rib(str(tmp_path / "t.rib")), load_rib(str(tmp_path / "b.rib"))
+    assert (a.width, a.height, a.fov, a.spp) == (b.width, b.height, b.fov, b.spp)
+    assert a.materials == b.materials and a.lights == b.lights
+    for (pa, ia, na), (pb, ib, nb) in zip(a.meshes, b.meshes):
+        np.testing.assert_array_equal(pa, pb)
+        np.testing.assert_array_equal(ia, ib)
+    np.testing.assert_array_equal(a.instance_array(), b.instance_array())
+
+
+def test_binary_codes_tokens_fixed_point_double():
+    import struct
+    from rtcuda.rib import decode_binary
+    data = (bytes([0xCC, 7]) + _bin_str("Translate")
+            + bytes([0xC8, 5]) + _bin_str("roughness")                          # string token 5
+            + bytes([0xA6, 7]) + bytes([0x85]) + struct.pack(">h", 384)         # fixed point: 384
+            + bytes([0x89]) + struct.pack(">i", -640)[1:]                       # 2 int + 1 fraction bytes: -2.5
+            + bytes([0xA5]) + struct.pack(">d", 0.1)                            # double
+            + b"\n# comment \xff stays\n"
+            + bytes([0xCD, 5]))                                                 # token reference
+    r = parse_rib(decode_binary(data))
+    assert r[0] == ("Translate", [384.0, -2.5, 0.1, "roughness"])
+
+
+def test_binary_decoder_is_total_on_noise():
+    from rtcuda.rib import RibError, decode_binary
+    rng = np.random.default_rng(0x9E3779B9)
+    for _ in range(300):
+        data = bytes(rng.integers(0, 256, size=int(rng.integers(0, 200)), dtype=np.uint8))
+        try:
+            decode_binary(data)
+        except RibError:
+            pass
