@@ -77,7 +77,8 @@ enum {
     RT_LIGHT_DISTANT = 1,  /* e1 = direction light travels; radius = angular radius */
     RT_LIGHT_RECT    = 2,  /* p = corner, e1/e2 = edges */
     RT_LIGHT_SPHERE  = 3,  /* p = centre, radius */
-    RT_LIGHT_DISK    = 4   /* p = centre, e1/e2 span the radius */
+    RT_LIGHT_DISK    = 4,  /* p = centre, e1/e2 span the radius */
+    RT_LIGHT_DOME    = 5   /* constant environment: radiance color * intensity from every direction */
 };
 
 /* Light: `Light { light_type, intensity, color }` (src/scene/light.rs:7-49).

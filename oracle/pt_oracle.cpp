@@ -1276,6 +1276,20 @@ struct Tracer {
                 V3 sp = l.p + l.e1 * (r * std::cos(phi)) + l.e2 * (r * std::sin(phi));
                 return area_contrib(p, n, sp, l, eval, pick);
             }
+            case RT_LIGHT_DOME: {  // mod.rs:1139-1172: constant dome, uniform sphere
+                double u = rng.next_f64(), v = rng.next_f64();
+                double z = 1.0 - 2.0 * u;
+                double r = std::sqrt(std::fmax(1.0 - z * z, 0.0));
+                double phi = 2.0 * PI * v;
+                V3 wi{r * std::cos(phi), r * std::sin(phi), z};
+                double pdf_sa = pick / (4.0 * PI);
+                double bp;
+                V3 f = eval(wi, &bp);
+                if (max_comp(f) <= 0.0) return {0, 0, 0};
+                V3 vis = visibility_toward(p, n, wi);
+                if (max_comp(vis) <= 0.0) return {0, 0, 0};
+                return f * l.radiance() * vis * (power_heuristic(pdf_sa, bp) / pdf_sa);
+            }
             case RT_LIGHT_SPHERE: {
                 V3 tc = l.p - p;
                 double dist2 = length_sq(tc);
@@ -1324,7 +1338,22 @@ struct Tracer {
             Hit hit;
             ext_rays++;
             if (!sc.intersect(ray, &hit, &cext)) {
-                emit(beta * sc.background);
+                // mod.rs:643-656: the first dome light (MIS against its NEE
+                // sampling unless seen from the camera), else the background.
+                int dome = -1;
+                for (size_t k = 0; k < sc.lights.size(); k++)
+                    if (sc.lights[k].type == RT_LIGHT_DOME) {
+                        dome = (int)k;
+                        break;
+                    }
+                if (dome >= 0) {
+                    double w = 1.0;
+                    if (!from_camera)
+                        w = power_heuristic(prev_pdf, sc.ls.pmf(prev_origin, (uint32_t)dome) / (4.0 * PI));
+                    emit(beta * sc.lights[dome].radiance() * w);
+                } else {
+                    emit(beta * sc.background);
+                }
                 break;
             }
             const Pbr& pbr = sc.materials[hit.material_id];

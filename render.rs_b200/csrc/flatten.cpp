@@ -1016,6 +1016,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
     }
     std::vector<LEntry> finite;
     H.light_leaf.assign(d->n_lights, 0xFFFFFFFFu);
+    H.scalars.dome = 0xFFFFFFFFu;
     double inf_total = 0;
     for (uint32_t l = 0; l < d->n_lights; l++) {
         const rt_light_desc& ld = d->lights[l];
@@ -1064,6 +1065,12 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
                 finite.push_back(en);
                 break;
             }
+            case RT_LIGHT_DOME:  // light_sampler.rs:104-118: infinite group, power lum * 4 pi
+                if (H.scalars.dome == 0xFFFFFFFFu) H.scalars.dome = l;
+                H.inf_lights.push_back(l);
+                H.inf_power.push_back((float)(pw * 4.0 * PI));
+                inf_total += pw * 4.0 * PI;
+                break;
             case RT_LIGHT_DISTANT: {
                 double dn = l1 > 1e-6 ? l1 : 1.0;
                 for (int k = 0; k < 3; k++) dl.e1[k] = (float)(ld.e1[k] / dn);

@@ -635,6 +635,22 @@ __device__ __forceinline__ bool nee_light(const DevScene& S, const DevLight& L, 
             shadow_to(sp);
             return true;
         }
+        case 5: {  // constant dome: uniform sphere, pdf 1 / (4 pi) (mod.rs:1139-1172)
+            float u = rng.next_f(), v = rng.next_f();
+            float z = 1.0f - 2.0f * u;
+            float r = sqrtf(fmaxf(1.0f - z * z, 0.0f)), s, c;
+            sincosf(2.0f * RT_PI * v, &s, &c);
+            float3 wi = f3(r * c, r * s, z);
+            float bp;
+            float3 f = eval(wi, bp);
+            if (maxc(f) <= 0.0f) return false;
+            float pdf_sa = pick * (0.25f / RT_PI);
+            out.c = f * Le * (power_heuristic(pdf_sa, bp) / pdf_sa);
+            out.o = p + n * RT_RAY_OFFSET;
+            out.d = wi;
+            out.tmax = 1e8f;
+            return true;
+        }
         case 3: {  // sphere
             float3 tc = lp - p;
             float dist2 = dot(tc, tc);
@@ -752,7 +768,17 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
             };
             if (hr.y == 0xFFFFFFFFu) {
                 tr_close();
-                emit(beta * f3(S.background[0], S.background[1], S.background[2]));
+                if (S.dome != 0xFFFFFFFFu) {
+                    // Miss: the dome light, MIS-weighted against its NEE
+                    // sampling unless seen from the camera (mod.rs:643-655).
+                    const DevLight& D = S.lights[S.dome];
+                    float wgt = 1.0f;
+                    if (!(flags & FL_FROM_CAMERA))
+                        wgt = power_heuristic(beta4.w, light_pmf(S, xyz(prev4), S.dome) * (0.25f / RT_PI));
+                    emit(beta * f3(D.radiance[0], D.radiance[1], D.radiance[2]) * wgt);
+                } else {
+                    emit(beta * f3(S.background[0], S.background[1], S.background[2]));
+                }
             } else {
                 HitGeo hg;
                 hit_geometry(S, o, d, hr, hg);

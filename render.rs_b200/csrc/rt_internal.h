@@ -126,6 +126,7 @@ struct DevScene {
     float inf_total;
     float p_infinite;
     uint32_t any_presence;       // some material has presence < 1
+    uint32_t dome;               // first dome light (misses see it), ~0 for none
     // camera (src/scene/camera.rs:150-179)
     float eye[3], fwd[3], right[3], up[3];
     float half_w, half_h, lens_radius, focal_distance, filter_width;

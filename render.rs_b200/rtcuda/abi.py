@@ -113,7 +113,7 @@ class RtParams(C.Structure):
     ]
 
 
-LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK = range(5)
+LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK, LIGHT_DOME = range(6)
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
 for _t, _n in ((RtMeshDesc, 32), (RtInstanceDesc, 104), (RtMaterialDesc, 264),

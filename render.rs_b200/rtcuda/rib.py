@@ -21,8 +21,9 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     are tessellated into smooth-normal triangle meshes; the reference
     intersects them analytically.
   * SubdivisionMesh renders its control cage; Curves, Points, patches,
-    dome lights, patterns, displacement, media and motion blur are skipped
-    (motion blocks use their first sample).
+    patterns, displacement, media and motion blur are skipped (motion
+    blocks use their first sample); PxrDomeLight is a constant dome (its
+    lightColorMap is not read).
 """
 import math
 import os
@@ -986,7 +987,9 @@ class _Builder:
             ang = 0.53 if ang is None else ang
             self.add_light(abi.LIGHT_DISTANT, scale, col, e1=d, radius=math.radians(ang * 0.5))
         elif t == "PxrDomeLight":
-            self.warn("PxrDomeLight is not rendered on this path; skipping")
+            if p.string("lightColorMap") is not None:
+                self.warn("PxrDomeLight environment maps are not rendered on this path; using a constant dome")
+            self.add_light(abi.LIGHT_DOME, scale, col)
         else:
             self.warn(f'Light "{t}" not implemented; skipping')
 

@@ -169,6 +169,11 @@ class Scene:
     def add_distant_light(self, direction, intensity, color=(1, 1, 1), angular_radius=0.0):
         return self._light(abi.LIGHT_DISTANT, intensity, color, e1=direction, radius=angular_radius)
 
+    def add_dome_light(self, intensity, color=(1, 1, 1)):
+        """Light::dome without an environment map: constant radiance
+        color * intensity from every direction (src/scene/light.rs:142-151)."""
+        return self._light(abi.LIGHT_DOME, intensity, color)
+
     def add_rect_light(self, corner, edge1, edge2, intensity, color=(1, 1, 1)):
         return self._light(abi.LIGHT_RECT, intensity, color, p=corner, e1=edge1, e2=edge2)
 

@@ -149,3 +149,23 @@ def test_white_furnace_per_lobe(name, mat, eta):
     assert abs(g - c) < 1e-3, (name, g, c)
     if name == "lambert":
         assert abs(g - 1.0) < 1e-3
+
+
+def test_constant_dome_furnace_and_oracle():
+    # Lambertian sphere of albedo 0.5 in a unit constant dome: surface pixels
+    # converge to 0.5, missed pixels show the dome; GPU and oracle agree.
+    from rtcuda.scene import Scene, matte
+    s = Scene(32, 32, fov=30.0)
+    s.look_at((0, 0, -4.0), (0, 0, 0))
+    pos, idx, nrm = scenes.icosphere(4)
+    s.add_instance(s.add_mesh(pos, idx, normals=nrm), s.add_material(matte((0.5, 0.5, 0.5))))
+    s.add_dome_light(1.0, (1.0, 1.0, 1.0))
+    p = abi.make_params(max_depth=8)
+    spp = 1024
+    with PtSession(s, p) as g:
+        g.render_samples(0, spp)
+        img = g.image()
+    np.testing.assert_allclose(img[0, 0], 1.0, rtol=1e-6)
+    np.testing.assert_allclose(img[12:20, 12:20].mean((0, 1)), 0.5, rtol=0.01)
+    cpu = oracle.OracleScene(s).render(p, 0, 256)[0].reshape(32, 32, 3) / 256
+    np.testing.assert_allclose(img.mean((0, 1)), cpu.mean((0, 1)), rtol=0.01)

@@ -299,3 +299,22 @@ def test_sample_ranges_add_up(cornell48):
     full = o_s.render(p, 0, 6)[0]
     parts = o_s.render(p, 0, 2)[0] + o_s.render(p, 2, 6)[0]
     assert np.allclose(full, parts, rtol=1e-12, atol=1e-12)
+
+
+def test_constant_dome_furnace():
+    # A convex Lambertian sphere of albedo rho inside a constant dome of
+    # radiance 1: every surface point reflects rho * 1 (no interreflection),
+    # and camera rays that miss see the dome itself (mod.rs:643-656, 1139-1172).
+    from rtcuda import abi, scenes
+    from rtcuda.scene import Scene, matte
+    s = Scene(24, 24, fov=30.0)
+    s.look_at((0, 0, -4.0), (0, 0, 0))
+    pos, idx, nrm = scenes.icosphere(4)
+    s.add_instance(s.add_mesh(pos, idx, normals=nrm), s.add_material(matte((0.5, 0.5, 0.5))))
+    s.add_dome_light(1.0, (1.0, 1.0, 1.0))
+    p = abi.make_params(max_depth=8)
+    spp = 256
+    img = oracle.OracleScene(s).render(p, 0, spp)[0].reshape(24, 24, 3) / spp
+    np.testing.assert_allclose(img[0, 0], 1.0, rtol=1e-12)          # a miss: the dome
+    centre = img[9:15, 9:15].mean((0, 1))
+    np.testing.assert_allclose(centre, 0.5, rtol=0.03)

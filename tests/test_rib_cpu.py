@@ -278,3 +278,11 @@ def test_binary_decoder_is_total_on_noise():
             decode_binary(data)
         except RibError:
             pass
+
+
+def test_pxr_dome_light():
+    s = load_rib_string('Light "PxrDomeLight" "sky" "intensity" [2] "exposure" [1] "lightColor" [0.5 0.5 1]\n'
+                        'Light "PxrDomeLight" "env" "string lightColorMap" ["sky.exr"]')
+    assert [l["type"] for l in s.lights] == [abi.LIGHT_DOME, abi.LIGHT_DOME]
+    assert s.lights[0]["intensity"] == 4.0 and s.lights[0]["color"] == (0.5, 0.5, 1.0)
+    assert any("environment maps" in w for w in s.warnings)
