@@ -125,6 +125,14 @@ typedef struct rt_scene_desc {
     uint32_t n_lights;
     rt_camera_desc camera;
     double background[3];
+    /* Environment map of one dome light (src/scene/envmap.rs): lat-long,
+     * env_width x env_height RGB f32 texels, row-major, row 0 at the zenith
+     * (+y), column u = atan2(x, -z) / 2pi; NULL for none. */
+    const float* env_rgb;
+    uint32_t env_width;
+    uint32_t env_height;
+    uint32_t env_light;       /* index of the RT_LIGHT_DOME light it belongs to */
+    uint32_t env_reserved;    /* 0 */
 } rt_scene_desc;
 
 /* Integrator knobs. The reference hard-codes these as constants
@@ -154,6 +162,7 @@ static_assert(sizeof(rt_material_desc) == 264, "rt_material_desc layout");
 static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
 static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
 static_assert(sizeof(rt_params) == 64, "rt_params layout");
+static_assert(sizeof(rt_scene_desc) == 240, "rt_scene_desc layout");
 }
 #endif
 

@@ -46,6 +46,8 @@ def lib():
         L.oracle_bsdf_furnace.restype = C.c_double
         L.oracle_bsdf_furnace.argtypes = [vp, f64p, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, f64p]
         L.oracle_light_sample.argtypes = [vp, f64p, C.c_double, u32p, f64p]
+        L.oracle_env_eval_pdf.argtypes = [C.c_uint32, C.c_uint32, vp, C.c_uint64, vp, vp, vp]
+        L.oracle_env_sample.argtypes = [C.c_uint32, C.c_uint32, vp, C.c_uint64, vp, vp, vp, vp]
         L.oracle_light_pmf.restype = C.c_double
         L.oracle_light_pmf.argtypes = [vp, f64p, C.c_uint32]
         _lib = L
@@ -174,3 +176,24 @@ def guide_eval(mlp, table16, res, lo, inv_ext, records, grads=True):
                         rec.ctypes.data, n, raw.ctypes.data, g_mlp.ctypes.data if grads else None,
                         g_tab.ctypes.data if grads else None, C.byref(loss))
     return raw, loss.value, g_mlp, g_tab
+
+
+def env_eval_pdf(env, dirs):
+    """envmap.rs eval + pdf for (n, 3) directions on an (H, W, 3) map."""
+    e = np.ascontiguousarray(env, dtype=np.float32)
+    d = np.ascontiguousarray(dirs, dtype=np.float64)
+    rad = np.empty((len(d), 3))
+    pdf = np.empty(len(d))
+    lib().oracle_env_eval_pdf(e.shape[1], e.shape[0], e.ctypes.data, len(d), d.ctypes.data, rad.ctypes.data,
+                               pdf.ctypes.data)
+    return rad, pdf
+
+
+def env_sample(env, uv):
+    """envmap.rs sample for (n, 2) uniforms: (dirs, radiance, pdf)."""
+    e = np.ascontiguousarray(env, dtype=np.float32)
+    u = np.ascontiguousarray(uv, dtype=np.float64)
+    dirs, rad, pdf = np.empty((len(u), 3)), np.empty((len(u), 3)), np.empty(len(u))
+    lib().oracle_env_sample(e.shape[1], e.shape[0], e.ctypes.data, len(u), u.ctypes.data, dirs.ctypes.data,
+                             rad.ctypes.data, pdf.ctypes.data)
+    return dirs, rad, pdf

@@ -468,11 +468,77 @@ struct Hit {
 
 // ---- lights (src/scene/light.rs) and the light BVH (light_sampler.rs) ----
 
+// envmap.rs: lat-long environment map of a dome light with 2D-CDF
+// importance sampling (f64 CDFs, nearest texel).
+struct EnvMap {
+    uint32_t w = 0, h = 0;
+    std::vector<float> rgb;  // 3 per texel, row-major, row 0 at the zenith
+    std::vector<double> marginal, conditional;
+    double total = 0.0;
+    V3 texel(size_t x, size_t y) const {
+        const float* c = &rgb[3 * (std::min<size_t>(y, h - 1) * w + std::min<size_t>(x, w - 1))];
+        return V3{c[0], c[1], c[2]};
+    }
+    void build() {  // envmap.rs:36-55
+        marginal.assign(h + 1, 0.0);
+        conditional.assign((size_t)(w + 1) * h, 0.0);
+        for (uint32_t y = 0; y < h; y++) {
+            const double sin_t = std::sin(PI * (y + 0.5) / h);
+            double acc = 0.0;
+            for (uint32_t x = 0; x < w; x++) {
+                acc += lum(texel(x, y)) * sin_t;
+                conditional[(size_t)y * (w + 1) + x + 1] = acc;
+            }
+            marginal[y + 1] = marginal[y] + acc;
+        }
+        total = std::fmax(marginal[h], 1e-12);
+    }
+    double mean_luminance() const { return total / std::fmax((double)w * h * (2.0 / PI), 1e-12); }  // :62-67
+    void texel_of(V3 dir, size_t* x, size_t* y) const {
+        V3 d = normalize(dir);
+        double u = std::atan2(d.x, -d.z) / (2.0 * PI);
+        u -= std::floor(u);
+        double v = std::fmin(std::fmax(std::acos(std::fmin(std::fmax(d.y, -1.0), 1.0)) / PI, 0.0), 1.0);
+        *x = std::min((size_t)(u * w), (size_t)w - 1);
+        *y = std::min((size_t)(v * h), (size_t)h - 1);
+    }
+    V3 eval(V3 dir) const {  // :83-91
+        size_t x, y;
+        texel_of(dir, &x, &y);
+        return texel(x, y);
+    }
+    double pdf(V3 dir) const {  // :129-144
+        size_t x, y;
+        texel_of(dir, &x, &y);
+        const double sin_t = std::sin(PI * (y + 0.5) / h);
+        if (sin_t < 1e-9) return 0.0;
+        return lum(texel(x, y)) * sin_t * w * h / (total * 2.0 * PI * PI * sin_t);
+    }
+    static size_t find(const double* cdf, size_t n, double target) {  // binary_search, then clamp
+        const double* it = std::lower_bound(cdf, cdf + n + 1, target);
+        size_t i = (size_t)(it - cdf);
+        size_t r = (i <= n && cdf[i] == target) ? i : (i > 0 ? i - 1 : 0);
+        return std::min(r, n - 1);
+    }
+    V3 sample(double u1, double u2, V3* rad, double* pdf_out) const {  // :100-126
+        size_t y = find(marginal.data(), h, u1 * total);
+        double row = std::fmax(marginal[y + 1] - marginal[y], 1e-12);
+        size_t x = find(&conditional[y * (w + 1)], w, u2 * row);
+        double u = (x + 0.5) / w, v = (y + 0.5) / h;
+        double phi = u * 2.0 * PI, theta = v * PI, st = std::sin(theta);
+        V3 dir{st * std::sin(phi), std::cos(theta), -st * std::cos(phi)};
+        *rad = texel(x, y);
+        *pdf_out = pdf(dir);
+        return dir;
+    }
+};
+
 struct Light {
     int type;
     double intensity;
     V3 color, p, e1, e2, normal;
     double radius = 0, area = 0;
+    std::shared_ptr<EnvMap> env;  // dome lights only
     V3 radiance() const { return color * intensity; }  // light.rs:151-153
 };
 
@@ -580,9 +646,12 @@ struct LightSampler {
                     finite.push_back({(uint32_t)i, l.p, l.radius, pw * 4.0 * PI * l.radius * l.radius * PI});
                     break;
                 case RT_LIGHT_DISK: finite.push_back({(uint32_t)i, l.p, length(l.e1), pw * l.area * PI}); break;
-                default:
+                default: {
+                    // light_sampler.rs:104-118: env maps fold in their mean luminance
+                    double base = l.env ? l.env->mean_luminance() * l.intensity : pw;
                     infinite.push_back((uint32_t)i);
-                    infinite_power.push_back(pw * 4.0 * PI);
+                    infinite_power.push_back(base * 4.0 * PI);
+                }
             }
         }
         infinite_total = 0;
@@ -1276,19 +1345,28 @@ struct Tracer {
                 V3 sp = l.p + l.e1 * (r * std::cos(phi)) + l.e2 * (r * std::sin(phi));
                 return area_contrib(p, n, sp, l, eval, pick);
             }
-            case RT_LIGHT_DOME: {  // mod.rs:1139-1172: constant dome, uniform sphere
+            case RT_LIGHT_DOME: {  // mod.rs:1139-1172: the map's importance sampling, or a uniform sphere
                 double u = rng.next_f64(), v = rng.next_f64();
-                double z = 1.0 - 2.0 * u;
-                double r = std::sqrt(std::fmax(1.0 - z * z, 0.0));
-                double phi = 2.0 * PI * v;
-                V3 wi{r * std::cos(phi), r * std::sin(phi), z};
-                double pdf_sa = pick / (4.0 * PI);
+                V3 wi, rad = l.radiance();
+                double pdf_dir = 1.0 / (4.0 * PI);
+                if (l.env) {
+                    V3 tex;
+                    wi = l.env->sample(u, v, &tex, &pdf_dir);
+                    rad = tex * l.radiance();
+                } else {
+                    double z = 1.0 - 2.0 * u;
+                    double r = std::sqrt(std::fmax(1.0 - z * z, 0.0));
+                    double phi = 2.0 * PI * v;
+                    wi = V3{r * std::cos(phi), r * std::sin(phi), z};
+                }
+                if (pdf_dir <= 0.0) return {0, 0, 0};
+                double pdf_sa = pdf_dir * pick;
                 double bp;
                 V3 f = eval(wi, &bp);
                 if (max_comp(f) <= 0.0) return {0, 0, 0};
                 V3 vis = visibility_toward(p, n, wi);
                 if (max_comp(vis) <= 0.0) return {0, 0, 0};
-                return f * l.radiance() * vis * (power_heuristic(pdf_sa, bp) / pdf_sa);
+                return f * rad * vis * (power_heuristic(pdf_sa, bp) / pdf_sa);
             }
             case RT_LIGHT_SPHERE: {
                 V3 tc = l.p - p;
@@ -1347,10 +1425,13 @@ struct Tracer {
                         break;
                     }
                 if (dome >= 0) {
+                    const Light& dl = sc.lights[dome];
+                    V3 dir = normalize(ray.d);
                     double w = 1.0;
                     if (!from_camera)
-                        w = power_heuristic(prev_pdf, sc.ls.pmf(prev_origin, (uint32_t)dome) / (4.0 * PI));
-                    emit(beta * sc.lights[dome].radiance() * w);
+                        w = power_heuristic(prev_pdf, sc.ls.pmf(prev_origin, (uint32_t)dome) *
+                                                          (dl.env ? dl.env->pdf(dir) : 1.0 / (4.0 * PI)));
+                    emit(beta * (dl.env ? dl.env->eval(dir) * dl.radiance() : dl.radiance()) * w);
                 } else {
                     emit(beta * sc.background);
                 }
@@ -1522,6 +1603,14 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
         if (d->materials[i].presence < 1.0) s.any_presence = true;
     }
     for (uint32_t i = 0; i < d->n_lights; i++) s.lights.push_back(make_light(d->lights[i]));
+    if (d->env_rgb && d->env_width && d->env_height && d->env_light < d->n_lights) {
+        auto env = std::make_shared<EnvMap>();
+        env->w = d->env_width;
+        env->h = d->env_height;
+        env->rgb.assign(d->env_rgb, d->env_rgb + 3ull * env->w * env->h);
+        env->build();
+        s.lights[d->env_light].env = env;
+    }
     s.ls.build(s.lights);
     const rt_camera_desc& c = d->camera;
     s.cam.width = c.width;
@@ -1725,5 +1814,44 @@ int oracle_light_sample(const oracle_scene* os, const double* p, double u, uint3
 }
 
 double oracle_light_pmf(const oracle_scene* os, const double* p, uint32_t light) { return os->s.ls.pmf(v3(p), light); }
+
+// Environment map functions (envmap.rs) on a w x h RGB map: per direction
+// eval (3 doubles) and pdf; per (u1, u2) the sampled direction, radiance
+// and pdf.
+void oracle_env_eval_pdf(uint32_t w, uint32_t h, const float* rgb, uint64_t n, const double* dirs, double* rad,
+                         double* pdf) {
+    EnvMap e;
+    e.w = w;
+    e.h = h;
+    e.rgb.assign(rgb, rgb + 3ull * w * h);
+    e.build();
+    for (uint64_t i = 0; i < n; i++) {
+        V3 d{dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]};
+        V3 c = e.eval(d);
+        rad[3 * i] = c.x;
+        rad[3 * i + 1] = c.y;
+        rad[3 * i + 2] = c.z;
+        pdf[i] = e.pdf(d);
+    }
+}
+
+void oracle_env_sample(uint32_t w, uint32_t h, const float* rgb, uint64_t n, const double* uv, double* dirs,
+                       double* rad, double* pdf) {
+    EnvMap e;
+    e.w = w;
+    e.h = h;
+    e.rgb.assign(rgb, rgb + 3ull * w * h);
+    e.build();
+    for (uint64_t i = 0; i < n; i++) {
+        V3 c;
+        V3 d = e.sample(uv[2 * i], uv[2 * i + 1], &c, &pdf[i]);
+        dirs[3 * i] = d.x;
+        dirs[3 * i + 1] = d.y;
+        dirs[3 * i + 2] = d.z;
+        rad[3 * i] = c.x;
+        rad[3 * i + 1] = c.y;
+        rad[3 * i + 2] = c.z;
+    }
+}
 
 }  // extern "C"

@@ -80,6 +80,10 @@ double oracle_bsdf_furnace(const rt_material_desc* m, const double* wo, double e
 int    oracle_light_sample(const oracle_scene* s, const double* p, double u,
                            uint32_t* light, double* pmf);
 double oracle_light_pmf(const oracle_scene* s, const double* p, uint32_t light);
+void   oracle_env_eval_pdf(uint32_t w, uint32_t h, const float* rgb, uint64_t n, const double* dirs, double* rad,
+                           double* pdf);
+void   oracle_env_sample(uint32_t w, uint32_t h, const float* rgb, uint64_t n, const double* uv, double* dirs,
+                         double* rad, double* pdf);
 
 #ifdef __cplusplus
 }

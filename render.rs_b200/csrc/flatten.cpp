@@ -1014,6 +1014,47 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         *err = "lights pointer is NULL";
         return false;
     }
+    // Environment map of a dome light (envmap.rs:36-55): CDFs over the
+    // sin-weighted luminance, accumulated in f64, stored in f32 as the
+    // reference's GPU export does (envmap.rs:64-71).
+    H.scalars.env_light = 0xFFFFFFFFu;
+    H.scalars.env_w = H.scalars.env_h = 0;
+    H.scalars.env_total = 0.0f;
+    double env_mean_lum = 0.0;
+    if (d->env_rgb) {
+        if (!d->env_width || !d->env_height || d->env_light >= d->n_lights ||
+            d->lights[d->env_light].type != RT_LIGHT_DOME) {
+            *err = "environment map without a size or a dome light";
+            return false;
+        }
+        const uint32_t w = d->env_width, h = d->env_height;
+        H.env.resize((size_t)w * h);
+        H.env_marg.assign(h + 1, 0.0f);
+        H.env_cond.assign((size_t)(w + 1) * h, 0.0f);
+        std::vector<double> marg(h + 1, 0.0);
+        for (uint32_t y = 0; y < h; y++) {
+            const double sin_t = std::sin(PI * (y + 0.5) / h);
+            double acc = 0.0;
+            for (uint32_t x = 0; x < w; x++) {
+                const float* c = d->env_rgb + 3 * ((size_t)y * w + x);
+                if (!std::isfinite(c[0]) || !std::isfinite(c[1]) || !std::isfinite(c[2])) {
+                    *err = "environment map has a non-finite texel";
+                    return false;
+                }
+                H.env[(size_t)y * w + x] = make_float4(c[0], c[1], c[2], 0.0f);
+                acc += (0.2126 * c[0] + 0.7152 * c[1] + 0.0722 * c[2]) * sin_t;
+                H.env_cond[(size_t)y * (w + 1) + x + 1] = (float)acc;
+            }
+            marg[y + 1] = marg[y] + acc;
+            H.env_marg[y + 1] = (float)marg[y + 1];
+        }
+        const double total = std::max(marg[h], 1e-12);
+        H.scalars.env_total = (float)total;
+        H.scalars.env_w = w;
+        H.scalars.env_h = h;
+        H.scalars.env_light = d->env_light;
+        env_mean_lum = total / std::max((double)w * h * (2.0 / PI), 1e-12);
+    }
     std::vector<LEntry> finite;
     H.light_leaf.assign(d->n_lights, 0xFFFFFFFFu);
     H.scalars.dome = 0xFFFFFFFFu;
@@ -1065,12 +1106,15 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
                 finite.push_back(en);
                 break;
             }
-            case RT_LIGHT_DOME:  // light_sampler.rs:104-118: infinite group, power lum * 4 pi
+            case RT_LIGHT_DOME: {  // light_sampler.rs:104-118: infinite group
                 if (H.scalars.dome == 0xFFFFFFFFu) H.scalars.dome = l;
+                // power: lum(radiance) * 4 pi, or with a map its mean luminance * intensity * 4 pi
+                const double base = l == H.scalars.env_light ? env_mean_lum * ld.intensity : pw;
                 H.inf_lights.push_back(l);
-                H.inf_power.push_back((float)(pw * 4.0 * PI));
-                inf_total += pw * 4.0 * PI;
+                H.inf_power.push_back((float)(base * 4.0 * PI));
+                inf_total += base * 4.0 * PI;
                 break;
+            }
             case RT_LIGHT_DISTANT: {
                 double dn = l1 > 1e-6 ? l1 : 1.0;
                 for (int k = 0; k < 3; k++) dl.e1[k] = (float)(ld.e1[k] / dn);

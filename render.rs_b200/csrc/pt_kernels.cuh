@@ -635,17 +635,26 @@ __device__ __forceinline__ bool nee_light(const DevScene& S, const DevLight& L, 
             shadow_to(sp);
             return true;
         }
-        case 5: {  // constant dome: uniform sphere, pdf 1 / (4 pi) (mod.rs:1139-1172)
+        case 5: {  // dome (mod.rs:1139-1172): the map's importance sampling, or a uniform sphere
             float u = rng.next_f(), v = rng.next_f();
-            float z = 1.0f - 2.0f * u;
-            float r = sqrtf(fmaxf(1.0f - z * z, 0.0f)), s, c;
-            sincosf(2.0f * RT_PI * v, &s, &c);
-            float3 wi = f3(r * c, r * s, z);
+            float3 wi, rad = Le;
+            float pdf_dir = 0.25f / RT_PI;
+            if ((uint32_t)(&L - S.lights) == S.env_light) {  // this dome carries the map
+                float3 tex;
+                wi = env_sample(S, u, v, &tex, &pdf_dir);
+                rad = tex * Le;
+                if (pdf_dir <= 0.0f) return false;
+            } else {
+                float z = 1.0f - 2.0f * u;
+                float r = sqrtf(fmaxf(1.0f - z * z, 0.0f)), s, c;
+                sincosf(2.0f * RT_PI * v, &s, &c);
+                wi = f3(r * c, r * s, z);
+            }
             float bp;
             float3 f = eval(wi, bp);
             if (maxc(f) <= 0.0f) return false;
-            float pdf_sa = pick * (0.25f / RT_PI);
-            out.c = f * Le * (power_heuristic(pdf_sa, bp) / pdf_sa);
+            float pdf_sa = pick * pdf_dir;
+            out.c = f * rad * (power_heuristic(pdf_sa, bp) / pdf_sa);
             out.o = p + n * RT_RAY_OFFSET;
             out.d = wi;
             out.tmax = 1e8f;
@@ -772,10 +781,14 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                     // Miss: the dome light, MIS-weighted against its NEE
                     // sampling unless seen from the camera (mod.rs:643-655).
                     const DevLight& D = S.lights[S.dome];
+                    const bool mapped = S.dome == S.env_light;
                     float wgt = 1.0f;
                     if (!(flags & FL_FROM_CAMERA))
-                        wgt = power_heuristic(beta4.w, light_pmf(S, xyz(prev4), S.dome) * (0.25f / RT_PI));
-                    emit(beta * f3(D.radiance[0], D.radiance[1], D.radiance[2]) * wgt);
+                        wgt = power_heuristic(beta4.w, light_pmf(S, xyz(prev4), S.dome) *
+                                                           (mapped ? env_pdf(S, d) : 0.25f / RT_PI));
+                    float3 rad = f3(D.radiance[0], D.radiance[1], D.radiance[2]);
+                    if (mapped) rad = env_eval(S, d) * rad;
+                    emit(beta * rad * wgt);
                 } else {
                     emit(beta * f3(S.background[0], S.background[1], S.background[2]));
                 }

@@ -127,6 +127,14 @@ struct DevScene {
     float p_infinite;
     uint32_t any_presence;       // some material has presence < 1
     uint32_t dome;               // first dome light (misses see it), ~0 for none
+    // Environment map of light env_light (src/scene/envmap.rs): lat-long
+    // texels (RGB + pad), row-marginal CDF (env_h + 1), per-row conditional
+    // CDFs (env_w + 1 each) over sin-weighted luminance, their total.
+    const float4* env;
+    const float* env_marg;
+    const float* env_cond;
+    uint32_t env_w, env_h, env_light;
+    float env_total;
     // camera (src/scene/camera.rs:150-179)
     float eye[3], fwd[3], right[3], up[3];
     float half_w, half_h, lens_radius, focal_distance, filter_width;

@@ -260,6 +260,9 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     rc = rc ? rc : s->upload(&S.light_leaf, H.light_leaf);
     rc = rc ? rc : s->upload(&S.inf_lights, H.inf_lights);
     rc = rc ? rc : s->upload(&S.inf_power, H.inf_power);
+    rc = rc ? rc : s->upload((const float4**)&S.env, H.env);
+    rc = rc ? rc : s->upload(&S.env_marg, H.env_marg);
+    rc = rc ? rc : s->upload(&S.env_cond, H.env_cond);
     if (rc) {
         delete s;
         return rc;

@@ -341,6 +341,62 @@ __device__ __forceinline__ float light_pmf(const DevScene& S, float3 p, uint32_t
     return pmf;
 }
 
+// ---- environment map of a dome light (src/scene/envmap.rs:83-160) -----------------
+__device__ __forceinline__ void env_texel_of(const DevScene& S, float3 dir, uint32_t* x, uint32_t* y) {
+    float3 d = normalize_ref(dir);
+    float u = atan2f(d.x, -d.z) * (0.5f / RT_PI);
+    u -= floorf(u);  // rem_euclid(1)
+    float v = fminf(fmaxf(acosf(fminf(fmaxf(d.y, -1.0f), 1.0f)) / RT_PI, 0.0f), 1.0f);
+    *x = min((uint32_t)(u * (float)S.env_w), S.env_w - 1);
+    *y = min((uint32_t)(v * (float)S.env_h), S.env_h - 1);
+}
+
+__device__ __forceinline__ float3 env_eval(const DevScene& S, float3 dir) {
+    uint32_t x, y;
+    env_texel_of(S, dir, &x, &y);
+    return xyz(__ldg(S.env + (size_t)y * S.env_w + x));
+}
+
+// Solid-angle pdf of env_sample: texel weight * w * h / (total * 2 pi^2 sin theta).
+__device__ __forceinline__ float env_pdf(const DevScene& S, float3 dir) {
+    uint32_t x, y;
+    env_texel_of(S, dir, &x, &y);
+    const float sin_t = sinf(RT_PI * ((float)y + 0.5f) / (float)S.env_h);
+    if (sin_t < 1e-9f) return 0.0f;
+    const float4 c = __ldg(S.env + (size_t)y * S.env_w + x);
+    const float tw = (0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z) * sin_t;
+    return tw * (float)S.env_w * (float)S.env_h / (S.env_total * 2.0f * RT_PI * RT_PI * sin_t);
+}
+
+// Index of the CDF interval holding `target` (the reference's binary_search:
+// an exact match gives its own index, otherwise the entry before the
+// insertion point), clamped to [0, n - 1]; cdf has n + 1 entries.
+__device__ __forceinline__ uint32_t env_cdf_find(const float* cdf, uint32_t n, float target) {
+    uint32_t lo = 0, hi = n + 1;  // first index with cdf >= target, in [lo, hi]
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) < target) lo = mid + 1;
+        else hi = mid;
+    }
+    uint32_t i = (lo <= n && __ldg(cdf + lo) == target) ? lo : (lo > 0 ? lo - 1 : 0);
+    return min(i, n - 1);
+}
+
+__device__ __forceinline__ float3 env_sample(const DevScene& S, float u1, float u2, float3* rad, float* pdf) {
+    const uint32_t y = env_cdf_find(S.env_marg, S.env_h, u1 * S.env_total);
+    const float row = fmaxf(__ldg(S.env_marg + y + 1) - __ldg(S.env_marg + y), 1e-12f);
+    const float* cond = S.env_cond + (size_t)y * (S.env_w + 1);
+    const uint32_t x = env_cdf_find(cond, S.env_w, u2 * row);
+    const float u = ((float)x + 0.5f) / (float)S.env_w, v = ((float)y + 0.5f) / (float)S.env_h;
+    float sp, cp, st, ct;
+    sincosf(u * 2.0f * RT_PI, &sp, &cp);
+    sincosf(v * RT_PI, &st, &ct);
+    const float3 dir = f3(st * sp, ct, -st * cp);
+    *rad = xyz(__ldg(S.env + (size_t)y * S.env_w + x));
+    *pdf = env_pdf(S, dir);
+    return dir;
+}
+
 __device__ __forceinline__ float power_heuristic(float a, float b) {
     float a2 = a * a, b2 = b * b;
     return a2 + b2 <= 0.0f ? 0.0f : a2 / (a2 + b2);

@@ -93,6 +93,11 @@ class RtSceneDesc(C.Structure):
         ("n_lights", C.c_uint32),
         ("camera", RtCameraDesc),
         ("background", c_double3),
+        ("env_rgb", C.POINTER(C.c_float)),
+        ("env_width", C.c_uint32),
+        ("env_height", C.c_uint32),
+        ("env_light", C.c_uint32),
+        ("env_reserved", C.c_uint32),
     ]
 
 
@@ -117,7 +122,7 @@ LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK, LIGHT_DOME = r
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
 for _t, _n in ((RtMeshDesc, 32), (RtInstanceDesc, 104), (RtMaterialDesc, 264),
-               (RtLightDesc, 120), (RtCameraDesc, 144), (RtParams, 64)):
+               (RtLightDesc, 120), (RtCameraDesc, 144), (RtParams, 64), (RtSceneDesc, 240)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
 

@@ -22,8 +22,8 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     intersects them analytically.
   * SubdivisionMesh renders its control cage; Curves, Points, patches,
     patterns, displacement, media and motion blur are skipped (motion
-    blocks use their first sample); PxrDomeLight is a constant dome (its
-    lightColorMap is not read).
+    blocks use their first sample); a PxrDomeLight lightColorMap is read
+    when it is a Radiance .hdr (one map per scene).
 """
 import math
 import os
@@ -560,6 +560,7 @@ class _Builder:
         self.next_id = 1
         self.warned = []
         self.motion = None
+        self.env = None
         # scene contents (materials / lights / meshes / instances)
         self.meshes, self.instances, self.materials, self.lights = [], [], [], []
 
@@ -987,9 +988,18 @@ class _Builder:
             ang = 0.53 if ang is None else ang
             self.add_light(abi.LIGHT_DISTANT, scale, col, e1=d, radius=math.radians(ang * 0.5))
         elif t == "PxrDomeLight":
-            if p.string("lightColorMap") is not None:
-                self.warn("PxrDomeLight environment maps are not rendered on this path; using a constant dome")
-            self.add_light(abi.LIGHT_DOME, scale, col)
+            li = self.add_light(abi.LIGHT_DOME, scale, col)
+            f = p.string("lightColorMap")
+            if f is not None:
+                path = f if os.path.isabs(f) or self.base_dir is None else os.path.join(self.base_dir, f)
+                try:
+                    from .envmap import read_hdr
+                    if self.env is None:
+                        self.env = (li, read_hdr(path))
+                    else:
+                        self.warn("only one environment map per scene; later PxrDomeLight maps are constant")
+                except (OSError, ValueError) as e:
+                    self.warn(f"PxrDomeLight map: {e}; using a constant dome")
         else:
             self.warn(f'Light "{t}" not implemented; skipping')
 
@@ -1010,6 +1020,8 @@ class _Builder:
             if math.isfinite(fstop) and fstop > 0:
                 s.lens_radius, s.focal_distance = flen / (2.0 * fstop), fdist
         s.background = self.background
+        if self.env is not None:
+            s.env = (self.env[0], np.ascontiguousarray(self.env[1], dtype=np.float32))
         s.pixel_samples = self.pixel_samples
         s.warnings = list(self.warned)
         return s

@@ -108,6 +108,7 @@ class Scene:
         self.materials = []
         self.lights = []
         self.background = (0.0, 0.0, 0.0)
+        self.env = None           # (dome light index, (H, W, 3) f32 radiance) or None
         # Reference default camera: origin, looking down +z (camera.rs:97-103).
         self.eye = np.zeros(3)
         self.forward = np.array([0.0, 0.0, 1.0])
@@ -169,10 +170,15 @@ class Scene:
     def add_distant_light(self, direction, intensity, color=(1, 1, 1), angular_radius=0.0):
         return self._light(abi.LIGHT_DISTANT, intensity, color, e1=direction, radius=angular_radius)
 
-    def add_dome_light(self, intensity, color=(1, 1, 1)):
-        """Light::dome without an environment map: constant radiance
-        color * intensity from every direction (src/scene/light.rs:142-151)."""
-        return self._light(abi.LIGHT_DOME, intensity, color)
+    def add_dome_light(self, intensity, color=(1, 1, 1), env=None):
+        """Light::dome (src/scene/light.rs:142-151): radiance color *
+        intensity from every direction, times the lat-long environment map
+        `env` ((H, W, 3) float radiance, row 0 at +y) when one is given
+        (one map per scene)."""
+        li = self._light(abi.LIGHT_DOME, intensity, color)
+        if env is not None:
+            self.env = (li, np.ascontiguousarray(env, dtype=np.float32).reshape(np.shape(env)[0], -1, 3))
+        return li
 
     def add_rect_light(self, corner, edge1, edge2, intensity, color=(1, 1, 1)):
         return self._light(abi.LIGHT_RECT, intensity, color, p=corner, e1=edge1, e2=edge2)
@@ -257,6 +263,12 @@ class Scene:
         d.n_materials, d.n_lights = len(self.materials), len(self.lights)
         d.camera = cam
         d.background = abi.c_double3(*self.background)
+        if self.env is not None:
+            li, env = self.env
+            keep.append(env)
+            d.env_rgb = env.ctypes.data_as(C.POINTER(C.c_float))
+            d.env_height, d.env_width = env.shape[0], env.shape[1]
+            d.env_light = li
         self._desc = d
         self._keep = (keep, mesh_arr, mat_arr, light_arr)
         return d

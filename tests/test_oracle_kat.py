@@ -318,3 +318,50 @@ def test_constant_dome_furnace():
     np.testing.assert_allclose(img[0, 0], 1.0, rtol=1e-12)          # a miss: the dome
     centre = img[9:15, 9:15].mean((0, 1))
     np.testing.assert_allclose(centre, 0.5, rtol=0.03)
+
+
+def _patch_map(w=32, h=16):
+    m = np.full((h, w, 3), 0.05, np.float32)
+    m[4:8, 10:16] = 5.0
+    return m
+
+
+def test_envmap_sample_pdf_consistency():
+    # envmap.rs tests (sample_pdf_consistency): the pdf integrates to ~1 over
+    # the sphere, samples land on the bright patch and carry its radiance.
+    env = _patch_map()
+    nt, npp = 128, 256
+    th = (np.arange(nt) + 0.5) / nt * np.pi
+    ph = (np.arange(npp) + 0.5) / npp * 2 * np.pi
+    T, Ph = np.meshgrid(th, ph, indexing="ij")
+    d = np.stack([np.sin(T) * np.sin(Ph), np.cos(T), -np.sin(T) * np.cos(Ph)], -1).reshape(-1, 3)
+    _, pdf = oracle.env_eval_pdf(env, d)
+    integral = float((pdf * np.sin(T).ravel()).sum() * (np.pi / nt) * (2 * np.pi / npp))
+    assert abs(integral - 1.0) < 0.03, integral
+    state = 0x1234
+    uv = []
+    for _ in range(400):
+        state = (state * 6364136223846793005 + 1) % (1 << 64)
+        uv.append((state >> 11) / float(1 << 53))
+    dirs, rad, pdf = oracle.env_sample(env, np.array(uv).reshape(200, 2))
+    assert (pdf > 0).all()
+    rad2, _ = oracle.env_eval_pdf(env, dirs)
+    np.testing.assert_allclose(rad2, rad, atol=1e-9)
+    assert (rad[:, 0] > 1.0).sum() > 150
+
+
+def test_uniform_envmap_equals_constant_dome():
+    # A map of ones under intensity 1 is the constant dome of radiance 1:
+    # same image in expectation (the sampling densities differ).
+    from rtcuda.scene import Scene, matte
+    pos, idx, nrm = scenes.icosphere(3)
+    imgs = []
+    for env in (None, np.ones((8, 16, 3), np.float32)):
+        s = scene.Scene(16, 16, fov=30.0)
+        s.look_at((0, 0, -4.0), (0, 0, 0))
+        s.add_instance(s.add_mesh(pos, idx, normals=nrm), s.add_material(matte((0.5, 0.5, 0.5))))
+        s.add_dome_light(1.0, (1.0, 1.0, 1.0), env=env)
+        p = abi.make_params(max_depth=6)
+        imgs.append(oracle.OracleScene(s).render(p, 0, 512)[0].reshape(16, 16, 3) / 512)
+    np.testing.assert_allclose(imgs[0][0, 0], imgs[1][0, 0], rtol=1e-12)
+    np.testing.assert_allclose(imgs[0][6:10, 6:10].mean(), imgs[1][6:10, 6:10].mean(), rtol=0.03)

@@ -285,4 +285,14 @@ def test_pxr_dome_light():
                         'Light "PxrDomeLight" "env" "string lightColorMap" ["sky.exr"]')
     assert [l["type"] for l in s.lights] == [abi.LIGHT_DOME, abi.LIGHT_DOME]
     assert s.lights[0]["intensity"] == 4.0 and s.lights[0]["color"] == (0.5, 0.5, 1.0)
-    assert any("environment maps" in w for w in s.warnings)
+    assert any("sky.exr" in w for w in s.warnings) and s.env is None  # a map that cannot be read: constant dome
+
+
+def test_pxr_dome_light_reads_hdr_map(tmp_path):
+    from test_envmap_cpu import _encode, _rgbe
+    img = np.full((4, 16, 3), 0.5, np.float32)
+    (tmp_path / "sky.hdr").write_bytes(_encode(_rgbe(img)))
+    (tmp_path / "s.rib").write_text('Light "PxrDomeLight" "sky" "string lightColorMap" ["sky.hdr"]\n')
+    s = load_rib(str(tmp_path / "s.rib"))
+    assert s.env is not None and s.env[0] == 0 and s.env[1].shape == (4, 16, 3)
+    np.testing.assert_allclose(s.env[1], 0.5, atol=1 / 256)  # RGBE has 8-bit mantissas
