@@ -152,7 +152,7 @@ GUIDED_W, GUIDED_H, GUIDED_SPP, GUIDED_DEPTH = 1280, 720, 2048, 16
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #       --clock-control none -k regex:k_extend -s 32 -c 32
 #       python bench.py --steps 1 --warmup 1 --e2e-steps 0 --no-cpu-baseline --no-guided --no-workloads
-EXTEND_DRAM_BYTES_PER_LAUNCH = 140.6e6  # 110.2 MB read + 30.4 MB written
+EXTEND_DRAM_BYTES_PER_LAUNCH = 138.0e6  # 107.8 MB read + 30.2 MB written
 EXTEND_DRAM_SOURCE = "ncu, dram__bytes_read.sum + dram__bytes_write.sum, mean of one step's 32 k_extend launches"
 
 
