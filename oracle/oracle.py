@@ -48,6 +48,7 @@ def lib():
         L.oracle_light_sample.argtypes = [vp, f64p, C.c_double, u32p, f64p]
         L.oracle_env_eval_pdf.argtypes = [C.c_uint32, C.c_uint32, vp, C.c_uint64, vp, vp, vp]
         L.oracle_env_sample.argtypes = [C.c_uint32, C.c_uint32, vp, C.c_uint64, vp, vp, vp, vp]
+        L.oracle_filter_sample.argtypes = [C.c_int, C.c_double, C.c_uint64, vp, vp]
         L.oracle_light_pmf.restype = C.c_double
         L.oracle_light_pmf.argtypes = [vp, f64p, C.c_uint32]
         _lib = L
@@ -197,3 +198,11 @@ def env_sample(env, uv):
     lib().oracle_env_sample(e.shape[1], e.shape[0], e.ctypes.data, len(u), u.ctypes.data, dirs.ctypes.data,
                              rad.ctypes.data, pdf.ctypes.data)
     return dirs, rad, pdf
+
+
+def filter_sample(kind, width, u):
+    """camera.rs:36-61 PixelFilter::sample_1d for each uniform in `u`."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    out = np.empty(len(u))
+    lib().oracle_filter_sample(int(kind), float(width), len(u), u.ctypes.data, out.ctypes.data)
+    return out

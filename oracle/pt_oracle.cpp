@@ -1854,4 +1854,11 @@ void oracle_env_sample(uint32_t w, uint32_t h, const float* rgb, uint64_t n, con
     }
 }
 
+void oracle_filter_sample(int filter, double width, uint64_t n, const double* u, double* out) {
+    Camera c{};
+    c.filter = filter;
+    c.filter_width = width;
+    for (uint64_t i = 0; i < n; i++) out[i] = c.sample_1d(u[i]);
+}
+
 }  // extern "C"

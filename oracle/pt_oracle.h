@@ -84,6 +84,8 @@ void   oracle_env_eval_pdf(uint32_t w, uint32_t h, const float* rgb, uint64_t n,
                            double* pdf);
 void   oracle_env_sample(uint32_t w, uint32_t h, const float* rgb, uint64_t n, const double* uv, double* dirs,
                          double* rad, double* pdf);
+// camera.rs:36-61: one pixel-filter offset per uniform.
+void   oracle_filter_sample(int filter, double width, uint64_t n, const double* u, double* out);
 
 #ifdef __cplusplus
 }

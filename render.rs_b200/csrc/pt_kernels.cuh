@@ -173,9 +173,14 @@ __device__ __forceinline__ float filter_offset(uint32_t kind, float width, float
         return u < 0.5f ? (sqrtf(2.0f * u) - 1.0f) * hw : (1.0f - sqrtf(2.0f * (1.0f - u))) * hw;
     }
     if (kind == 2u) {
+        // The second uniform is fract(u * 2654435761) as camera.rs:55 forms
+        // it in f64. In f32 the product is a whole number for every
+        // u > 2^-8 (its ulp there is >= 256), so u2 would be 0, the cosine 1
+        // and every offset >= 0: a half-Gaussian shifted off the pixel
+        // centre. One f64 multiply per camera ray keeps it centred.
         float u1 = fmaxf(u, 1e-12f);
-        float x = u * 2654435761.0f;
-        float u2 = x - truncf(x);
+        const double x = (double)u * 2654435761.0;
+        float u2 = (float)(x - trunc(x));
         float g = sqrtf(-2.0f * logf(u1)) * cosf(2.0f * RT_PI * u2);
         return fminf(fmaxf(g * (width * 0.25f), -width * 0.5f), width * 0.5f);
     }

@@ -1,5 +1,6 @@
 // rt_internal.h — device data layouts shared by the host flattener
-// (flatten.cpp) and the CUDA kernels (pt_kernels.cu).
+// and device BVH builders (flatten.cpp, bvh_build.cu) and the CUDA kernels
+// (pt_kernels.cuh, traverse.cuh, shade.cuh).
 //
 // HBM layout (all arrays 16-byte aligned, read with 128-bit loads):
 //   nodes   : 8-wide BVH nodes, 96 B = 6 x uint4 each. Every BLAS (in mesh

@@ -365,3 +365,27 @@ def test_uniform_envmap_equals_constant_dome():
         imgs.append(oracle.OracleScene(s).render(p, 0, 512)[0].reshape(16, 16, 3) / 512)
     np.testing.assert_allclose(imgs[0][0, 0], imgs[1][0, 0], rtol=1e-12)
     np.testing.assert_allclose(imgs[0][6:10, 6:10].mean(), imgs[1][6:10, 6:10].mean(), rtol=0.03)
+
+
+@pytest.mark.parametrize("kind,width", [(abi.FILTER_BOX, 1.0), (abi.FILTER_TRIANGLE, 2.0), (abi.FILTER_GAUSSIAN, 2.0)])
+def test_filter_samples_stay_in_support_and_center(kind, width):
+    """camera.rs:213-239: 4096 stratified uniforms; every offset within half
+    the width, mean offset below 0.05."""
+    u = (np.arange(4096) + 0.5) / 4096
+    dx = oracle.filter_sample(kind, width, u)
+    assert np.all(np.abs(dx) <= width * 0.5 + 1e-9)
+    assert abs(dx.mean()) < 0.05, dx.mean()
+
+
+def test_gaussian_second_uniform_needs_f64():
+    """The Gaussian filter's second uniform fract(u * 2654435761)
+    (camera.rs:55) collapses to 0 when the product is rounded to f32, which
+    would fail the centring test above: why the CUDA raygen forms it in f64."""
+    u = ((np.arange(4096) + 0.5) / 4096).astype(np.float32)
+    x32 = u * np.float32(2654435761.0)
+    assert np.mean(x32 - np.trunc(x32) == 0) > 0.99
+    x64 = u.astype(np.float64) * 2654435761.0
+    u2 = x64 - np.trunc(x64)
+    g = np.sqrt(-2.0 * np.log(np.maximum(u.astype(np.float64), 1e-12))) * np.cos(2.0 * np.pi * u2)
+    np.testing.assert_allclose(np.clip(g * 0.5, -1.0, 1.0), oracle.filter_sample(abi.FILTER_GAUSSIAN, 2.0, u),
+                               atol=1e-6)
