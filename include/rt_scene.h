@@ -28,14 +28,16 @@
 extern "C" {
 #endif
 
-/* Triangle mesh: f32 xyz positions, u32 index triples, optional normals.
- * Mirrors `Mesh { positions, indices, normals }` (src/geometry/mesh.rs:20-33). */
+/* Triangle mesh: f32 xyz positions, u32 index triples, optional normals
+ * and texture coordinates.
+ * Mirrors `Mesh { positions, indices, normals, st }` (src/geometry/mesh.rs:20-33). */
 typedef struct rt_mesh_desc {
     const float*    positions;    /* 3 * n_vertices */
     const uint32_t* indices;      /* 3 * n_triangles */
     const float*    normals;      /* 3 * n_vertices, or NULL (geometric normal) */
     uint32_t        n_vertices;
     uint32_t        n_triangles;
+    const float*    st;           /* 2 * n_vertices (s, t), or NULL (st = 0, density 0) */
 } rt_mesh_desc;
 
 /* Placed copy of a mesh. `object_to_world` is the row-major upper 3x4 of
@@ -114,6 +116,58 @@ typedef struct rt_camera_desc {
     double   filter_width;
 } rt_camera_desc;
 
+/* Procedural pattern node (src/texture/pattern.rs:47-67; PatternNode).
+ * Every node outputs RGB; scalar consumers read channel 0. The file-texture
+ * nodes (Texture, Triplanar) are not carried. */
+enum {
+    RT_PATTERN_CHECKER       = 0,  /* color_a / color_b cells over st * scale, footprint-filtered */
+    RT_PATTERN_FRACTAL       = 1,  /* fBm of classic Perlin noise over world P, remapped to [0,1] */
+    RT_PATTERN_MIX           = 2,  /* lerp(in[0], in[1], in[2].r) */
+    RT_PATTERN_COLOR_CORRECT = 3,  /* (in[0] * color_a + color_b) ^ (1 / gamma), then saturation */
+    RT_PATTERN_RAMP          = 4   /* piecewise-linear ramp over s (or t) */
+};
+
+/* Node input (PInput): another node's output or a constant. A node may only
+ * read nodes of lower index (the graph is a DAG in index order). */
+typedef struct rt_pattern_input {
+    int32_t node;       /* index of the node read, or -1 for `value` */
+    int32_t pad_;
+    double  value[3];
+} rt_pattern_input;
+
+typedef struct rt_pattern_desc {
+    int32_t  type;                /* RT_PATTERN_* */
+    uint32_t octaves;             /* fractal */
+    double   color_a[3];          /* checker colour A; colour-correct gain */
+    double   color_b[3];          /* checker colour B; colour-correct offset */
+    double   scale[2];            /* checker s, t scale */
+    double   frequency, gain, lacunarity;  /* fractal */
+    double   gamma, saturation;   /* colour correct */
+    rt_pattern_input in[3];       /* mix: color1, color2, mix; colour correct: in[0] */
+    const double* ramp_positions; /* n_ramp, ascending */
+    const double* ramp_colors;    /* 3 * n_ramp */
+    uint32_t n_ramp;
+    uint32_t use_t;               /* ramp over t instead of s */
+} rt_pattern_desc;
+
+/* PbrParams fields a pattern output drives (BoundField, pattern.rs:238-254). */
+enum {
+    RT_FIELD_DIFFUSE_COLOR = 0, RT_FIELD_DIFFUSE_GAIN = 1, RT_FIELD_DIFFUSE_ROUGHNESS = 2,
+    RT_FIELD_SPECULAR_FACE_COLOR = 3, RT_FIELD_SPECULAR_EDGE_COLOR = 4, RT_FIELD_SPECULAR_ROUGHNESS = 5,
+    RT_FIELD_CLEARCOAT_GAIN = 6, RT_FIELD_FUZZ_GAIN = 7, RT_FIELD_FUZZ_COLOR = 8, RT_FIELD_GLASS_GAIN = 9,
+    RT_FIELD_GLASS_ROUGHNESS = 10, RT_FIELD_REFRACTION_COLOR = 11, RT_FIELD_GLOW = 12, RT_FIELD_PRESENCE = 13
+};
+
+/* Material::pattern_bindings entry (src/scene/material.rs:29-30): the
+ * output of `node` replaces `field` of `material` at every shading point,
+ * in binding order. */
+typedef struct rt_pattern_binding {
+    uint32_t material;
+    uint32_t field;     /* RT_FIELD_* */
+    uint32_t node;
+    uint32_t pad_;
+} rt_pattern_binding;
+
 typedef struct rt_scene_desc {
     const rt_mesh_desc*     meshes;
     const rt_instance_desc* instances;
@@ -133,6 +187,12 @@ typedef struct rt_scene_desc {
     uint32_t env_height;
     uint32_t env_light;       /* index of the RT_LIGHT_DOME light it belongs to */
     uint32_t env_reserved;    /* 0 */
+    /* Pattern graph shared by all materials (Scene::patterns,
+     * src/scene/mod.rs:39-40) and the material bindings into it. */
+    const rt_pattern_desc*    patterns;
+    const rt_pattern_binding* bindings;
+    uint32_t n_patterns;
+    uint32_t n_bindings;
 } rt_scene_desc;
 
 /* Integrator knobs. The reference hard-codes these as constants
@@ -156,13 +216,16 @@ typedef struct rt_params {
 
 /* Size checks shared by every consumer of the descriptor. */
 #ifdef __cplusplus
-static_assert(sizeof(rt_mesh_desc) == 32, "rt_mesh_desc layout");
+static_assert(sizeof(rt_mesh_desc) == 40, "rt_mesh_desc layout");
 static_assert(sizeof(rt_instance_desc) == 104, "rt_instance_desc layout");
 static_assert(sizeof(rt_material_desc) == 264, "rt_material_desc layout");
 static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
 static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
 static_assert(sizeof(rt_params) == 64, "rt_params layout");
-static_assert(sizeof(rt_scene_desc) == 240, "rt_scene_desc layout");
+static_assert(sizeof(rt_pattern_input) == 32, "rt_pattern_input layout");
+static_assert(sizeof(rt_pattern_desc) == 232, "rt_pattern_desc layout");
+static_assert(sizeof(rt_pattern_binding) == 16, "rt_pattern_binding layout");
+static_assert(sizeof(rt_scene_desc) == 264, "rt_scene_desc layout");
 }
 #endif
 

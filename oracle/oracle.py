@@ -49,6 +49,8 @@ def lib():
         L.oracle_env_eval_pdf.argtypes = [C.c_uint32, C.c_uint32, vp, C.c_uint64, vp, vp, vp]
         L.oracle_env_sample.argtypes = [C.c_uint32, C.c_uint32, vp, C.c_uint64, vp, vp, vp, vp]
         L.oracle_filter_sample.argtypes = [C.c_int, C.c_double, C.c_uint64, vp, vp]
+        L.oracle_pattern_eval.argtypes = [vp, C.c_uint32, C.c_uint64, vp, vp]
+        L.oracle_intersect_st.argtypes = [vp, C.c_uint64, vp, vp]
         L.oracle_light_pmf.restype = C.c_double
         L.oracle_light_pmf.argtypes = [vp, f64p, C.c_uint32]
         _lib = L
@@ -115,6 +117,13 @@ class OracleScene:
         b, t = C.c_uint64(), C.c_uint64()
         lib().oracle_scene_stats(self.h, C.byref(b), C.byref(t))
         return b.value, t.value
+
+    def intersect_st(self, origins, directions):
+        """Closest hits of rays: (t or -1, s, t, st density) per ray."""
+        r = np.ascontiguousarray(np.hstack([np.atleast_2d(origins), np.atleast_2d(directions)]), dtype=np.float64)
+        out = np.empty((len(r), 4))
+        lib().oracle_intersect_st(self.h, len(r), r.ctypes.data, out.ctypes.data)
+        return out
 
     def intersect(self, planes, any_hit=False, threads=0):
         planes = np.ascontiguousarray(planes, dtype=np.float32)
@@ -198,6 +207,16 @@ def env_sample(env, uv):
     lib().oracle_env_sample(e.shape[1], e.shape[0], e.ctypes.data, len(u), u.ctypes.data, dirs.ctypes.data,
                              rad.ctypes.data, pdf.ctypes.data)
     return dirs, rad, pdf
+
+
+def pattern_eval(scene, node, ctx):
+    """pattern.rs eval of `node` of `scene`'s pattern graph at points ctx
+    (n, 6) = (s, t, Px, Py, Pz, footprint); returns (n, 3) RGB."""
+    c = np.ascontiguousarray(np.atleast_2d(ctx), dtype=np.float64)
+    out = np.empty((len(c), 3))
+    d = scene.desc()
+    lib().oracle_pattern_eval(C.addressof(d), int(node), len(c), c.ctypes.data, out.ctypes.data)
+    return out
 
 
 def filter_sample(kind, width, u):

@@ -397,6 +397,7 @@ struct Mesh {
     std::vector<float> pos;
     std::vector<uint32_t> idx;
     std::vector<float> nrm;  // empty when absent
+    std::vector<float> st;   // 2 per vertex; empty when absent
     Bvh blas;
     Aabb local_bounds;
 
@@ -451,12 +452,30 @@ struct Mesh {
         V3 v0 = vertex(i0);
         return normalize(cross(vertex(i1) - v0, vertex(i2) - v0));
     }
+
+    // mesh.rs:177-197 interpolated st and st density (sqrt of st area over
+    // local geometric area); false without st.
+    bool st_at(uint32_t tri, double u, double v, double st_out[2], double* density) const {
+        if (st.empty()) return false;
+        uint32_t i0 = idx[3 * tri], i1 = idx[3 * tri + 1], i2 = idx[3 * tri + 2];
+        const float *s0 = &st[2 * i0], *s1 = &st[2 * i1], *s2 = &st[2 * i2];
+        double w = 1.0 - u - v;
+        st_out[0] = (double)s0[0] * w + (double)s1[0] * u + (double)s2[0] * v;
+        st_out[1] = (double)s0[1] * w + (double)s1[1] * u + (double)s2[1] * v;
+        double st_area = 0.5 * std::fabs((double)(s1[0] - s0[0]) * (double)(s2[1] - s0[1]) -
+                                         (double)(s2[0] - s0[0]) * (double)(s1[1] - s0[1]));
+        V3 v0 = vertex(i0);
+        double geo_area = 0.5 * length(cross(vertex(i1) - v0, vertex(i2) - v0));
+        *density = geo_area > 1e-18 ? std::sqrt(st_area / geo_area) : 0.0;
+        return true;
+    }
 };
 
 struct Instance {
     uint32_t mesh_id = 0, material_id = 0;
     M4 transform, inv;
     Aabb world_bounds;
+    double scale = 1.0;  // Matrix4::approx_scale (math/matrix.rs:246-251)
 };
 
 struct Hit {
@@ -464,7 +483,129 @@ struct Hit {
     V3 point, normal;
     uint32_t material_id, inst, prim;
     bool front_face;
+    double st[2] = {0.0, 0.0};
+    double st_density = 0.0;  // st units per world unit (0 without st)
 };
+
+// ---- patterns (src/texture/pattern.rs, src/geometry/displace.rs) -------------
+
+// displace.rs:36-80: classic Perlin gradient noise over a hashed lattice.
+static uint32_t lattice_hash(int64_t x) {
+    uint64_t u = (uint64_t)x * 0x9e3779b97f4a7c15ull;
+    x = (int64_t)u;
+    x ^= x >> 29;  // arithmetic shift, as on the reference's i64
+    u = (uint64_t)x * 0xbf58476d1ce4e5b9ull;
+    x = (int64_t)u;
+    x ^= x >> 32;
+    return (uint32_t)(uint64_t)x;
+}
+static double perlin(double px, double py, double pz) {
+    double cx = std::floor(px), cy = std::floor(py), cz = std::floor(pz);
+    double f[3] = {px - cx, py - cy, pz - cz};
+    int64_t ix = (int64_t)cx, iy = (int64_t)cy, iz = (int64_t)cz;
+    double corner[8];
+    for (int k = 0; k < 8; k++) {
+        int64_t dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+        uint64_t key = (uint64_t)(ix + dx) * 73856093ull ^ (uint64_t)(iy + dy) * 19349663ull ^
+                       (uint64_t)(iz + dz) * 83492791ull;
+        uint32_t h = lattice_hash((int64_t)key) % 12u;
+        // The 12 cube-edge gradients, in the reference's order.
+        double g0 = (h < 8) ? ((h & 1) ? -1.0 : 1.0) : 0.0;
+        double g1 = (h < 4) ? ((h & 2) ? -1.0 : 1.0) : (h < 8 ? 0.0 : ((h & 1) ? -1.0 : 1.0));
+        double g2 = (h < 4) ? 0.0 : (h < 8 ? ((h & 2) ? -1.0 : 1.0) : ((h & 2) ? -1.0 : 1.0));
+        corner[k] = g0 * (f[0] - (double)dx) + g1 * (f[1] - (double)dy) + g2 * (f[2] - (double)dz);
+    }
+    auto fade = [](double t) { return t * t * t * (t * (t * 6.0 - 15.0) + 10.0); };
+    auto lerp = [](double a, double b, double t) { return a + (b - a) * t; };
+    double u = fade(f[0]), v = fade(f[1]), w = fade(f[2]);
+    double y0 = lerp(lerp(corner[0], corner[1], u), lerp(corner[2], corner[3], u), v);
+    double y1 = lerp(lerp(corner[4], corner[5], u), lerp(corner[6], corner[7], u), v);
+    return lerp(y0, y1, w);
+}
+// displace.rs:82-97 (offset 0, as PatternNode::Fractal passes it).
+static double fbm(V3 p, double frequency, uint32_t octaves, double gain, double lacunarity) {
+    double sum = 0.0, amp = 1.0, freq = frequency;
+    for (uint32_t o = 0; o < std::max(octaves, 1u); o++) {
+        sum += amp * perlin(p.x * freq, p.y * freq, p.z * freq);
+        amp *= gain;
+        freq *= lacunarity;
+    }
+    return sum;
+}
+
+struct PatInput {
+    int32_t node;  // -1: constant
+    V3 value;
+};
+struct PatNode {
+    int32_t type;
+    uint32_t octaves;
+    V3 a, b;
+    double scale[2], frequency, gain, lacunarity, gamma, saturation;
+    PatInput in[3];
+    std::vector<double> ramp_pos;
+    std::vector<V3> ramp_col;
+    bool use_t;
+};
+struct ShadeCtx {  // pattern.rs:69-82 (no file textures: st, P and footprint)
+    double st[2];
+    V3 p;
+    double footprint;
+};
+static const V3 MISSING_COLOR{1.0, 0.0, 1.0};
+
+// pattern.rs:126-226 eval_at.
+static V3 pattern_eval(const std::vector<PatNode>& nodes, int64_t index, const ShadeCtx& c, uint32_t depth) {
+    if (depth > 16) return MISSING_COLOR;
+    if (index < 0 || (size_t)index >= nodes.size()) return MISSING_COLOR;
+    const PatNode& n = nodes[(size_t)index];
+    auto input = [&](int k) { return n.in[k].node < 0 ? n.in[k].value : pattern_eval(nodes, n.in[k].node, c, depth + 1); };
+    switch (n.type) {
+        case RT_PATTERN_CHECKER: {
+            double fs = c.st[0] * n.scale[0], ft = c.st[1] * n.scale[1];
+            int64_t cell = (int64_t)(std::floor(fs) + std::floor(ft));
+            cell = ((cell % 2) + 2) % 2;
+            V3 sharp = cell == 0 ? n.a : n.b;
+            V3 mean = (n.a + n.b) * 0.5;
+            double w = std::fmin(c.footprint * std::fmax(std::fabs(n.scale[0]), std::fabs(n.scale[1])), 1.0);
+            return sharp * (1.0 - w) + mean * w;
+        }
+        case RT_PATTERN_FRACTAL: {
+            double v = std::min(std::max(fbm(c.p, n.frequency, n.octaves, n.gain, n.lacunarity) * 0.5 + 0.5, 0.0), 1.0);
+            return {v, v, v};
+        }
+        case RT_PATTERN_MIX: {
+            V3 a = input(0), b = input(1);
+            double m = std::min(std::max(input(2).x, 0.0), 1.0);
+            return a * (1.0 - m) + b * m;
+        }
+        case RT_PATTERN_COLOR_CORRECT: {
+            V3 in = input(0);
+            double g = 1.0 / std::fmax(n.gamma, 1e-6);
+            V3 out{std::pow(std::fmax(in.x * n.a.x + n.b.x, 0.0), g), std::pow(std::fmax(in.y * n.a.y + n.b.y, 0.0), g),
+                   std::pow(std::fmax(in.z * n.a.z + n.b.z, 0.0), g)};
+            if (std::fabs(n.saturation - 1.0) > 1e-9) {
+                double l = 0.2126 * out.x + 0.7152 * out.y + 0.0722 * out.z;
+                V3 grey{l, l, l};
+                out = grey + (out - grey) * n.saturation;
+            }
+            return out;
+        }
+        case RT_PATTERN_RAMP: {
+            double x = std::min(std::max(n.use_t ? c.st[1] : c.st[0], 0.0), 1.0);
+            if (n.ramp_col.empty()) return MISSING_COLOR;
+            if (x <= n.ramp_pos[0]) return n.ramp_col[0];
+            for (size_t i = 1; i < n.ramp_pos.size(); i++)
+                if (x <= n.ramp_pos[i]) {
+                    double span = std::fmax(n.ramp_pos[i] - n.ramp_pos[i - 1], 1e-9);
+                    double a = (x - n.ramp_pos[i - 1]) / span;
+                    return n.ramp_col[i - 1] * (1.0 - a) + n.ramp_col[i] * a;
+                }
+            return n.ramp_col.back();
+        }
+        default: return MISSING_COLOR;
+    }
+}
 
 // ---- lights (src/scene/light.rs) and the light BVH (light_sampler.rs) ----
 
@@ -800,6 +941,26 @@ struct Pbr {
         return {0, 0, 0};
     }
     bool has_specular() const { return lum(specular_f0()) > 1e-6; }  // pbr.rs:100-102
+    // BoundField::apply (pattern.rs:278-296): scalars take channel 0.
+    void apply(uint32_t field, V3 v) {
+        switch (field) {
+            case RT_FIELD_DIFFUSE_COLOR: diffuse_color = v; break;
+            case RT_FIELD_DIFFUSE_GAIN: diffuse_gain = v.x; break;
+            case RT_FIELD_DIFFUSE_ROUGHNESS: diffuse_roughness = v.x; break;
+            case RT_FIELD_SPECULAR_FACE_COLOR: spec_face = v; break;
+            case RT_FIELD_SPECULAR_EDGE_COLOR: spec_edge = v; break;
+            case RT_FIELD_SPECULAR_ROUGHNESS: spec_rough = std::min(std::max(v.x, 0.005), 1.0); break;
+            case RT_FIELD_CLEARCOAT_GAIN: cc_gain = v.x; break;
+            case RT_FIELD_FUZZ_GAIN: fuzz_gain = v.x; break;
+            case RT_FIELD_FUZZ_COLOR: fuzz_color = v; break;
+            case RT_FIELD_GLASS_GAIN: glass_gain = v.x; break;
+            case RT_FIELD_GLASS_ROUGHNESS: glass_rough = std::min(std::max(v.x, 0.005), 1.0); break;
+            case RT_FIELD_REFRACTION_COLOR: refraction_color = v; break;
+            case RT_FIELD_GLOW: glow = v; break;
+            case RT_FIELD_PRESENCE: presence = std::min(std::max(v.x, 0.0), 1.0); break;
+            default: break;
+        }
+    }
     // pbr.rs:188-201
     bool lobe_weights(double w[5]) const {
         double wd = diffuse_gain * lum(diffuse_color);
@@ -1113,6 +1274,19 @@ struct Scene {
     Camera cam;
     V3 background;
     bool any_presence = false;
+    std::vector<PatNode> patterns;
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> bindings;  // per material: (field, node)
+
+    // shade_params (pt/mod.rs:389-439) without file textures: the material
+    // with its pattern outputs substituted, footprint = cone width x st density.
+    Pbr shade_params(const Hit& h, double cone_width) const {
+        const Pbr& base = materials[h.material_id];
+        if (h.material_id >= bindings.size() || bindings[h.material_id].empty()) return base;
+        Pbr p = base;
+        ShadeCtx c{{h.st[0], h.st[1]}, h.point, cone_width * h.st_density};
+        for (const auto& b : bindings[h.material_id]) p.apply(b.first, pattern_eval(patterns, b.second, c, 0));
+        return p;
+    }
 
     // mesh.rs:308-381 Instance::intersect + scene/mod.rs:105-146.
     bool intersect(const Ray& ray, Hit* out, Counters* c) const {
@@ -1165,6 +1339,9 @@ struct Scene {
         out->inst = best.inst;
         out->prim = best.tri;
         out->front_face = front;
+        // mesh.rs:357-360: st and its density, transferred to world scale.
+        double dens;
+        if (m.st_at(best.tri, best.u, best.v, out->st, &dens)) out->st_density = dens / in.scale;
         return true;
     }
 
@@ -1236,6 +1413,8 @@ struct Tracer {
     const rt_params& prm;
     uint64_t ext_rays = 0, shadow_rays = 0;
     Counters cext, cshadow;  // traversal work of extension / shadow rays
+    // Angular size of one pixel, the initial ray-cone spread (pt/mod.rs:73-76).
+    double pixel_spread() const { return std::tan(sc.cam.fov * PI / 180.0 / 2.0) * 2.0 / (double)sc.cam.height; }
 
     // mod.rs:1254-1306 transmittance, restricted to surfaces (no media).
     V3 transmittance(V3 origin, V3 dir, double remaining) {
@@ -1246,7 +1425,7 @@ struct Tracer {
             Ray r = make_ray(origin, dir);
             if (!sc.intersect(r, &h, &cshadow)) return vis;
             if (h.t >= remaining) return vis;
-            double presence = std::min(std::max(sc.materials[h.material_id].presence, 0.0), 1.0);
+            double presence = std::min(std::max(sc.shade_params(h, 0.0).presence, 0.0), 1.0);
             if (presence >= 1.0) return {0, 0, 0};
             vis = vis * (1.0 - presence);
             if (max_comp(vis) < 1e-4) return {0, 0, 0};
@@ -1411,6 +1590,7 @@ struct Tracer {
         V3 prev_origin = ray.o;
         bool from_camera = true;
         int presence_skips = 0;
+        double cone_width = 0.0, cone_spread = pixel_spread();
         uint32_t depth = 0;
         while (depth < prm.max_depth) {
             Hit hit;
@@ -1437,9 +1617,10 @@ struct Tracer {
                 }
                 break;
             }
-            const Pbr& pbr = sc.materials[hit.material_id];
             V3 wo = -normalize(ray.d);
+            cone_width += hit.t * cone_spread;
             travel += hit.t;
+            const Pbr pbr = sc.shade_params(hit, cone_width);
             if (!aux_set) {
                 aux_set = true;
                 V3 a = pbr.diffuse_color * pbr.diffuse_gain + pbr.specular_f0() * (pbr.has_specular() ? 1.0 : 0.0) +
@@ -1499,6 +1680,7 @@ struct Tracer {
             prev_pdf = s.pdf;
             prev_origin = hit.point;
             from_camera = false;
+            cone_spread += std::fmin(1.0 / (1.0 + s.pdf), 0.4);  // pt/mod.rs:965-967
             double off = s.transmitted ? -RAY_OFFSET : RAY_OFFSET;
             ray = make_ray(hit.point + n * off, wi_world);
             depth++;
@@ -1515,6 +1697,31 @@ struct Tracer {
 }  // namespace orc
 
 using namespace orc;
+
+static void load_patterns(const rt_scene_desc* d, std::vector<PatNode>& out) {
+    for (uint32_t i = 0; i < d->n_patterns && d->patterns; i++) {
+        const rt_pattern_desc& pd = d->patterns[i];
+        PatNode n;
+        n.type = pd.type;
+        n.octaves = pd.octaves;
+        n.a = v3(pd.color_a);
+        n.b = v3(pd.color_b);
+        n.scale[0] = pd.scale[0];
+        n.scale[1] = pd.scale[1];
+        n.frequency = pd.frequency;
+        n.gain = pd.gain;
+        n.lacunarity = pd.lacunarity;
+        n.gamma = pd.gamma;
+        n.saturation = pd.saturation;
+        for (int k = 0; k < 3; k++) n.in[k] = {pd.in[k].node, v3(pd.in[k].value)};
+        for (uint32_t r = 0; r < pd.n_ramp && pd.ramp_positions && pd.ramp_colors; r++) {
+            n.ramp_pos.push_back(pd.ramp_positions[r]);
+            n.ramp_col.push_back(v3(pd.ramp_colors + 3 * r));
+        }
+        n.use_t = pd.use_t != 0;
+        out.push_back(n);
+    }
+}
 
 struct oracle_scene {
     Scene s;
@@ -1576,6 +1783,7 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
         m.pos.assign(md.positions, md.positions + 3ull * md.n_vertices);
         m.idx.assign(md.indices, md.indices + 3ull * md.n_triangles);
         if (md.normals) m.nrm.assign(md.normals, md.normals + 3ull * md.n_vertices);
+        if (md.st) m.st.assign(md.st, md.st + 2ull * md.n_vertices);
         m.build();
     }
     s.instances.resize(d->n_instances);
@@ -1589,6 +1797,9 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
         for (int r = 0; r < 3; r++)
             for (int c = 0; c < 4; c++) in.transform.m[r][c] = id.object_to_world[r * 4 + c];
         if (!inverse(in.transform, in.inv)) in.inv = identity();  // mesh.rs:282
+        double lx = length(xf_vec(in.transform, V3{1, 0, 0})), ly = length(xf_vec(in.transform, V3{0, 1, 0})),
+               lz = length(xf_vec(in.transform, V3{0, 0, 1}));
+        in.scale = std::fmax(std::cbrt(lx * ly * lz), 1e-12);
         // mesh.rs:283-297 world bounds from the 8 transformed corners.
         const Aabb& lb = s.meshes[in.mesh_id].local_bounds;
         for (int k = 0; k < 8; k++) {
@@ -1601,6 +1812,15 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
     for (uint32_t i = 0; i < d->n_materials; i++) {
         s.materials.push_back(Pbr::from(d->materials[i]));
         if (d->materials[i].presence < 1.0) s.any_presence = true;
+    }
+    load_patterns(d, s.patterns);
+    s.bindings.resize(d->n_materials);
+    for (uint32_t i = 0; i < d->n_bindings && d->bindings; i++) {
+        const rt_pattern_binding& b = d->bindings[i];
+        if (b.material < d->n_materials) {
+            s.bindings[b.material].push_back({b.field, b.node});
+            if (b.field == RT_FIELD_PRESENCE) s.any_presence = true;
+        }
     }
     for (uint32_t i = 0; i < d->n_lights; i++) s.lights.push_back(make_light(d->lights[i]));
     if (d->env_rgb && d->env_width && d->env_height && d->env_light < d->n_lights) {
@@ -1851,6 +2071,31 @@ void oracle_env_sample(uint32_t w, uint32_t h, const float* rgb, uint64_t n, con
         rad[3 * i] = c.x;
         rad[3 * i + 1] = c.y;
         rad[3 * i + 2] = c.z;
+    }
+}
+
+void oracle_pattern_eval(const rt_scene_desc* d, uint32_t node, uint64_t n, const double* ctx, double* rgb) {
+    std::vector<PatNode> nodes;
+    load_patterns(d, nodes);
+    for (uint64_t i = 0; i < n; i++) {
+        const double* c = ctx + 6 * i;
+        ShadeCtx sc{{c[0], c[1]}, V3{c[2], c[3], c[4]}, c[5]};
+        V3 v = pattern_eval(nodes, node, sc, 0);
+        rgb[3 * i] = v.x;
+        rgb[3 * i + 1] = v.y;
+        rgb[3 * i + 2] = v.z;
+    }
+}
+
+void oracle_intersect_st(const oracle_scene* os, uint64_t n, const double* rays, double* out) {
+    for (uint64_t i = 0; i < n; i++) {
+        const double* r = rays + 6 * i;
+        Hit h;
+        bool hit = os->s.intersect(make_ray(V3{r[0], r[1], r[2]}, V3{r[3], r[4], r[5]}), &h, nullptr);
+        out[4 * i] = hit ? h.t : -1.0;
+        out[4 * i + 1] = hit ? h.st[0] : 0.0;
+        out[4 * i + 2] = hit ? h.st[1] : 0.0;
+        out[4 * i + 3] = hit ? h.st_density : 0.0;
     }
 }
 

@@ -84,6 +84,11 @@ void   oracle_env_eval_pdf(uint32_t w, uint32_t h, const float* rgb, uint64_t n,
                            double* pdf);
 void   oracle_env_sample(uint32_t w, uint32_t h, const float* rgb, uint64_t n, const double* uv, double* dirs,
                          double* rad, double* pdf);
+// pattern.rs:126-226: node `node` of d's pattern graph at n shading points,
+// ctx = (s, t, Px, Py, Pz, footprint) per point; rgb = 3 per point.
+void   oracle_pattern_eval(const rt_scene_desc* d, uint32_t node, uint64_t n, const double* ctx, double* rgb);
+// Closest hit of n rays (o, d: 6 doubles each): (t or -1, s, t, st density).
+void   oracle_intersect_st(const oracle_scene* s, uint64_t n, const double* rays, double* out);
 // camera.rs:36-61: one pixel-filter offset per uniform.
 void   oracle_filter_sample(int filter, double width, uint64_t n, const double* u, double* out);
 

@@ -682,6 +682,161 @@ uint32_t lbvh_build(std::vector<LightNode>& nodes, std::vector<uint32_t>& leaf_o
     return index;
 }
 
+// Pattern graph and bindings (src/texture/pattern.rs, material.rs:29-30,
+// 95-101) in device form. Nodes may read only lower-indexed nodes, so the
+// graph is evaluated in index order; a material's bindings may reach at
+// most RT_MAX_PATTERN_NODES consecutive nodes. Presence bindings would need
+// pattern evaluation inside shadow-ray traversal and are refused.
+bool flatten_patterns(const rt_scene_desc* d, HostScene& H, std::string* err) {
+    if (!d->n_patterns && !d->n_bindings) return true;
+    if ((d->n_patterns && !d->patterns) || (d->n_bindings && !d->bindings)) {
+        *err = "patterns or bindings pointer is NULL";
+        return false;
+    }
+    const uint32_t np = d->n_patterns;
+    H.patterns.resize(np);
+    for (uint32_t i = 0; i < np; i++) {
+        const rt_pattern_desc& pd = d->patterns[i];
+        DevPattern& g = H.patterns[i];
+        memset(&g, 0, sizeof(g));
+        if (pd.type < RT_PATTERN_CHECKER || pd.type > RT_PATTERN_RAMP) {
+            *err = "pattern node " + std::to_string(i) + " has an unknown type";
+            return false;
+        }
+        g.type = (uint32_t)pd.type;
+        for (int k = 0; k < 3; k++) {
+            const bool used = (pd.type == RT_PATTERN_MIX) || (pd.type == RT_PATTERN_COLOR_CORRECT && k == 0);
+            g.in[k] = 0xFFFFFFFFu;
+            if (used && pd.in[k].node >= 0) {
+                if ((uint32_t)pd.in[k].node >= i) {
+                    *err = "pattern node " + std::to_string(i) + " reads node " + std::to_string(pd.in[k].node) +
+                           " (a node may read only nodes of lower index)";
+                    return false;
+                }
+                g.in[k] = (uint32_t)pd.in[k].node;
+            }
+            for (int c = 0; c < 3; c++) g.c[k][c] = (float)pd.in[k].value[c];
+        }
+        switch (pd.type) {
+            case RT_PATTERN_CHECKER:
+                for (int c = 0; c < 3; c++) {
+                    g.c[0][c] = (float)pd.color_a[c];
+                    g.c[1][c] = (float)pd.color_b[c];
+                }
+                g.s0 = (float)pd.scale[0];
+                g.s1 = (float)pd.scale[1];
+                break;
+            case RT_PATTERN_FRACTAL:
+                g.s0 = (float)pd.frequency;
+                g.s1 = (float)pd.gain;
+                g.s2 = (float)pd.lacunarity;
+                g.u0 = std::max(pd.octaves, 1u);
+                if (g.u0 > 32) {
+                    *err = "pattern node " + std::to_string(i) + " asks for more than 32 octaves";
+                    return false;
+                }
+                break;
+            case RT_PATTERN_COLOR_CORRECT:
+                for (int c = 0; c < 3; c++) {
+                    g.c[1][c] = (float)pd.color_a[c];
+                    g.c[2][c] = (float)pd.color_b[c];
+                }
+                g.s0 = (float)pd.gamma;
+                g.s1 = (float)pd.saturation;
+                break;
+            case RT_PATTERN_RAMP:
+                if (pd.n_ramp && (!pd.ramp_positions || !pd.ramp_colors)) {
+                    *err = "pattern node " + std::to_string(i) + " has a ramp without positions or colours";
+                    return false;
+                }
+                g.u0 = (uint32_t)H.ramp.size();
+                g.u1 = pd.n_ramp;
+                g.u2 = pd.use_t ? 1u : 0u;
+                for (uint32_t r = 0; r < pd.n_ramp; r++)
+                    H.ramp.push_back(make_float4((float)pd.ramp_positions[r], (float)pd.ramp_colors[3 * r],
+                                                 (float)pd.ramp_colors[3 * r + 1], (float)pd.ramp_colors[3 * r + 2]));
+                break;
+            default: break;
+        }
+    }
+    std::vector<std::vector<uint2>> per_mat(d->n_materials);
+    for (uint32_t b = 0; b < d->n_bindings; b++) {
+        const rt_pattern_binding& pb = d->bindings[b];
+        if (pb.material >= d->n_materials || pb.node >= np || pb.field > RT_FIELD_PRESENCE) {
+            *err = "pattern binding " + std::to_string(b) + " names a missing material, node or field";
+            return false;
+        }
+        if (pb.field == RT_FIELD_PRESENCE) {
+            *err = "pattern binding " + std::to_string(b) +
+                   ": presence bindings are not supported by the CUDA backend";
+            return false;
+        }
+        per_mat[pb.material].push_back(make_uint2(pb.field, pb.node));
+    }
+    H.mat_pat.assign(d->n_materials, DevMatPat{});
+    for (uint32_t m = 0; m < d->n_materials; m++) {
+        DevMatPat& mp = H.mat_pat[m];
+        if (per_mat[m].empty()) continue;
+        // Nodes reached from the bindings (inputs always point lower).
+        std::vector<uint8_t> reach(np, 0);
+        for (const uint2& b : per_mat[m]) reach[b.y] = 1;
+        uint32_t lo = np, hi = 0;
+        for (uint32_t i = np; i-- > 0;) {
+            if (!reach[i]) continue;
+            lo = std::min(lo, i);
+            hi = std::max(hi, i);
+            for (int k = 0; k < 3; k++)
+                if (H.patterns[i].in[k] != 0xFFFFFFFFu) reach[H.patterns[i].in[k]] = 1;
+        }
+        if (hi - lo >= RT_MAX_PATTERN_NODES) {
+            *err = "material " + std::to_string(m) + " reaches pattern nodes " + std::to_string(lo) + ".." +
+                   std::to_string(hi) + " (at most 16 consecutive nodes per material)";
+            return false;
+        }
+        mp.bind_off = (uint32_t)H.binds.size();
+        mp.bind_n = (uint32_t)per_mat[m].size();
+        mp.node_lo = lo;
+        for (uint32_t i = lo; i <= hi; i++)
+            if (reach[i]) mp.node_mask |= 1u << (i - lo);
+        H.binds.insert(H.binds.end(), per_mat[m].begin(), per_mat[m].end());
+        mp.pbr_index = (uint32_t)H.pbr.size();
+        const rt_material_desc& md = d->materials[m];
+        DevPbr p;
+        p.diffuse_gain = (float)md.diffuse_gain;
+        p.diffuse_roughness = (float)md.diffuse_roughness;
+        p.spec_rough = (float)md.specular_roughness;
+        p.spec_ior = (float)md.specular_ior;
+        p.cc_gain = (float)md.clearcoat_gain;
+        p.cc_rough = (float)md.clearcoat_roughness;
+        p.fuzz_gain = (float)md.fuzz_gain;
+        p.glass_gain = (float)md.glass_gain;
+        p.glass_ior = (float)md.glass_ior;
+        p.glass_rough = (float)md.glass_roughness;
+        p.presence = (float)md.presence;
+        for (int c = 0; c < 3; c++) {
+            p.diffuse_color[c] = (float)md.diffuse_color[c];
+            p.spec_face[c] = (float)md.specular_face_color[c];
+            p.spec_edge[c] = (float)md.specular_edge_color[c];
+            p.fuzz_color[c] = (float)md.fuzz_color[c];
+            p.refraction[c] = (float)md.refraction_color[c];
+            p.glow[c] = (float)md.glow[c];
+            p.emission[c] = (float)md.emission[c];
+        }
+        H.pbr.push_back(p);
+        // The lobe set varies per hit: shade through the general class.
+        H.materials[m].mclass = MAT_MIXED;
+    }
+    // Matrix4::approx_scale (math/matrix.rs:246-251): st density per world unit.
+    H.inst_scale.resize(d->n_instances);
+    for (uint32_t i = 0; i < d->n_instances; i++) {
+        const double* x = d->instances[i].object_to_world;
+        double l[3];
+        for (int c = 0; c < 3; c++) l[c] = std::sqrt(x[c] * x[c] + x[4 + c] * x[4 + c] + x[8 + c] * x[8 + c]);
+        H.inst_scale[i] = (float)std::max(std::cbrt(l[0] * l[1] * l[2]), 1e-12);
+    }
+    return true;
+}
+
 }  // namespace
 
 DevMaterial fold_material_public(const rt_material_desc& m) { return fold_material(m); }
@@ -868,7 +1023,10 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         mi.blas_root = 0xFFFFFFFFu;
         mi.idx_base = 0xFFFFFFFFu;
         tri_base += md.n_triangles;
-        if (md.normals) {
+        mi.attrs = (md.normals ? MESH_NORMALS : 0u) | (md.st ? MESH_ST : 0u);
+        if (mi.attrs) {
+            // Vertex attributes (normals and/or st) share one vertex
+            // numbering; a mesh without one of them stores zeros there.
             mi.idx_base = (uint32_t)H.orig_idx.size();
             uint32_t vbase = (uint32_t)(H.normals.size() / 3);
             const size_t o = H.orig_idx.size();
@@ -877,7 +1035,12 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
             parallel_for(3ull * md.n_triangles, [&](size_t k0, size_t k1) {
                 for (size_t k = k0; k < k1; k++) oi[k] = vbase + md.indices[k];
             });
-            H.normals.insert(H.normals.end(), md.normals, md.normals + 3ull * md.n_vertices);
+            if (md.normals) H.normals.insert(H.normals.end(), md.normals, md.normals + 3ull * md.n_vertices);
+            else H.normals.resize(H.normals.size() + 3ull * md.n_vertices, 0.0f);
+            if (md.st) {
+                H.st.resize(2ull * vbase, 0.0f);
+                H.st.insert(H.st.end(), md.st, md.st + 2ull * md.n_vertices);
+            }
         }
         if (!build_bvh) continue;  // the device builder validates, bounds and builds
         std::vector<Box> tb(md.n_triangles);
@@ -948,6 +1111,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
             root_children[m].push_back(c);
         }
     }
+    if (!H.st.empty()) H.st.resize(2 * (H.normals.size() / 3), 0.0f);
     // ---- instances + TLAS ------------------------------------------------
     if (d->n_instances && !d->instances) {
         *err = "instances pointer is NULL";
@@ -1009,6 +1173,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         H.materials.push_back(fold_material(md));
         if (md.presence < 1.0) H.scalars.any_presence = 1;
     }
+    if (!flatten_patterns(d, H, err)) return false;
     // ---- lights + light BVH --------------------------------------------------
     if (d->n_lights && !d->lights) {
         *err = "lights pointer is NULL";

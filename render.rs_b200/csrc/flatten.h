@@ -20,6 +20,13 @@ struct HostScene {
     std::vector<MeshInfo> meshes;
     std::vector<uint32_t> orig_idx;
     std::vector<float> normals;
+    std::vector<float> st;           // 2 per attribute vertex, empty when no mesh has st
+    std::vector<float> inst_scale;   // per instance when the scene has patterns
+    std::vector<DevPattern> patterns;
+    std::vector<float4> ramp;
+    std::vector<DevMatPat> mat_pat;  // per material when the scene has bindings
+    std::vector<uint2> binds;
+    std::vector<DevPbr> pbr;
     std::vector<DevMaterial> materials;
     std::vector<DevLight> lights;
     std::vector<LightNode> lbvh;

@@ -20,6 +20,7 @@
 #pragma once
 
 #include "guide.cuh"
+#include "pattern.cuh"
 
 namespace rt {
 
@@ -50,6 +51,7 @@ struct Paths {
     float4* aux_a;    // albedo xyz, depth
     float4* aux_n;    // normal xyz, id bits
     float4* aux_d;    // diffuse share xyz, hit flag
+    float2* cone;     // ray cone (width, spread) when the scene has patterns, else null
     uint32_t* q_ext[2];
     uint32_t* q_cls;  // N_QUEUES x P
     uint32_t* q_sh;
@@ -146,7 +148,7 @@ __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3
     float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
     float3 nl;
     MeshInfo mi = S.meshes[info.w];
-    if (mi.idx_base != 0xFFFFFFFFu) {
+    if (mi.attrs & MESH_NORMALS) {
         // Interpolated vertex normals (Mesh::local_normal, mesh.rs:200-220).
         float b1 = __half2float(__ushort_as_half((unsigned short)(hr.w & 0xFFFFu)));
         float b2 = __half2float(__ushort_as_half((unsigned short)(hr.w >> 16)));
@@ -163,6 +165,30 @@ __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3
     g.wo = -normalize_ref(d);
     g.eucl = length(g.p - o);
     g.mat = info.z;
+}
+
+// (s, t) and st density (st units per world unit) at a closest hit:
+// Mesh::st_at (src/geometry/mesh.rs:177-197) with the density carried to
+// world scale by the instance's approx_scale (mesh.rs:357-360); zeros when
+// the mesh has no st.
+__device__ __forceinline__ float3 hit_st(const DevScene& S, uint4 hr) {
+    const uint4 info = __ldg(S.inst + hr.z);
+    const MeshInfo mi = S.meshes[info.w];
+    if (!(mi.attrs & MESH_ST)) return f3(0.0f, 0.0f, 0.0f);
+    const float4* tp = S.tris + 3 * (size_t)hr.y;
+    const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+    const float b1 = __half2float(__ushort_as_half((unsigned short)(hr.w & 0xFFFFu)));
+    const float b2 = __half2float(__ushort_as_half((unsigned short)(hr.w >> 16)));
+    const uint32_t* ix = S.orig_idx + mi.idx_base + 3 * (size_t)__float_as_uint(v0.w);
+    const float2* st = reinterpret_cast<const float2*>(S.st);
+    const float2 s0 = st[ix[0]], s1 = st[ix[1]], s2 = st[ix[2]];
+    const float w = 1.0f - b1 - b2;
+    const float s = s0.x * w + s1.x * b1 + s2.x * b2;
+    const float t = s0.y * w + s1.y * b1 + s2.y * b2;
+    const float st_area = 0.5f * fabsf((s1.x - s0.x) * (s2.y - s0.y) - (s2.x - s0.x) * (s1.y - s0.y));
+    const float geo_area = 0.5f * length(cross(xyz(v1) - xyz(v0), xyz(v2) - xyz(v0)));
+    const float dens = geo_area > 1e-18f ? sqrtf(st_area / geo_area) : 0.0f;
+    return f3(s, t, dens / __ldg(S.inst_scale + info.y));
 }
 
 // ---- raygen: camera rays for all P slots ------------------------------------------
@@ -247,6 +273,8 @@ __global__ void k_raygen(DevScene S, Paths P, PtConsts C) {
     P.beta[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     P.L[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     P.prev[i] = make_float4(o.x, o.y, o.z, __uint_as_float(FL_FROM_CAMERA | FL_SPEC_NONE));
+    // Ray cone: width 0, spread one pixel's angle (kernel_pt.metal:2283-2284).
+    if (P.cone) P.cone[i] = make_float2(0.0f, 2.0f * S.half_h / (float)S.height);
     P.rng[i] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
                           (uint32_t)(rng.inc >> 32));
     if (C.aovs) {
@@ -805,7 +833,23 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                 const bool front = hg.front;
                 const float eucl = hg.eucl;
                 travel += eucl;
-                const DevMaterial& m = S.materials[hg.mat];
+                // Ray cone at this hit and the material's pattern outputs
+                // (pt/mod.rs:687-689; footprint = cone width x st density).
+                float2 cone = make_float2(0.0f, 0.0f);
+                DevMaterial mres;
+                const DevMaterial* mptr = S.materials + hg.mat;
+                if (P.cone) {
+                    cone = P.cone[slot];
+                    cone.x += eucl * cone.y;
+                    const DevMatPat mp = S.mat_pat[hg.mat];
+                    if (mp.bind_n) {
+                        const float3 stv = hit_st(S, hr);
+                        mres = *mptr;
+                        resolve_material(S, mp, stv.x, stv.y, p, cone.x * stv.z, mres);
+                        mptr = &mres;
+                    }
+                }
+                const DevMaterial& m = *mptr;
                 if (C.aovs && !(flags & FL_AUX_SET)) {
                     flags |= FL_AUX_SET;
                     float3 an = dot(nw, wo) >= 0.0f ? nw : -nw;
@@ -927,6 +971,8 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                             flags = (flags & ~FL_SPEC_MASK) | (bs.specular ? FL_SPEC_TRUE : 0u);
                         flags &= ~FL_FROM_CAMERA;
                         beta4.w = pdf_path;
+                        // Widen the cone after rough bounces (pt/mod.rs:965-967).
+                        cone.y += fminf(1.0f / (1.0f + pdf_path), 0.4f);
                         prev4 = make_float4(p.x, p.y, p.z, 0.0f);
                         float off = bs.transmitted ? -RT_RAY_OFFSET : RT_RAY_OFFSET;
                         float3 no = p + n * off;
@@ -946,6 +992,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                         }
                     }
                 }
+                if (P.cone) P.cone[slot] = cone;
             }
             P.beta[slot] = make_float4(beta.x, beta.y, beta.z, beta4.w);
             P.L[slot] = make_float4(Lr.x, Lr.y, Lr.z, travel);

@@ -96,12 +96,56 @@ struct LightNode {
 };
 static_assert(sizeof(LightNode) == 48, "LightNode layout");
 
+// Vertex attributes a mesh carries (MeshInfo::attrs).
+#define MESH_NORMALS 1u
+#define MESH_ST 2u
+
 struct MeshInfo {
-    uint32_t idx_base;     // first index of this mesh in orig_idx (3 per tri), or ~0 if no normals
+    uint32_t idx_base;     // first index of this mesh in orig_idx (3 per tri), or ~0 if no attributes
     uint32_t n_tris;
     uint32_t blas_root;
     uint32_t tri_base;     // first triangle (leaf order) in tris
+    uint32_t attrs;        // MESH_NORMALS | MESH_ST
+    uint32_t pad_[3];
 };
+static_assert(sizeof(MeshInfo) == 32, "MeshInfo layout");
+
+// ---- patterns (src/texture/pattern.rs) ------------------------------------------
+// One node of the shared pattern graph. Inputs are node indices (below the
+// node's own) or ~0 for the constant in c[k].
+struct DevPattern {
+    uint32_t type;           // RT_PATTERN_*
+    uint32_t in[3];
+    float c[3][3];           // input constants; checker colours A, B in c[0], c[1];
+                             // colour-correct gain, offset in c[1], c[2]
+    float s0, s1, s2;        // checker s, t scale | fractal frequency, gain, lacunarity |
+                             // colour-correct gamma, saturation
+    uint32_t u0, u1, u2;     // fractal octaves | ramp first entry, entries, use_t
+    uint32_t pad_;
+};
+static_assert(sizeof(DevPattern) == 80, "DevPattern layout");
+
+// Base PbrParams of a patterned material (f32), re-folded at every hit
+// after the pattern outputs are substituted.
+struct DevPbr {
+    float diffuse_gain, diffuse_color[3], diffuse_roughness;
+    float spec_face[3], spec_edge[3], spec_rough, spec_ior;
+    float cc_gain, cc_rough;
+    float fuzz_gain, fuzz_color[3];
+    float glass_gain, glass_ior, glass_rough;
+    float refraction[3], glow[3], presence, emission[3];
+};
+static_assert(sizeof(DevPbr) == 128, "DevPbr layout");
+
+// Per material: its bindings (binds[bind_off .. bind_off + bind_n) as
+// (field, node)), the nodes they reach (node_lo + bit k of node_mask),
+// and its base parameters (pbr[pbr_index]).
+struct DevMatPat {
+    uint32_t bind_off, bind_n, node_lo, node_mask;
+    uint32_t pbr_index, pad_[3];
+};
+static_assert(sizeof(DevMatPat) == 32, "DevMatPat layout");
+#define RT_MAX_PATTERN_NODES 16
 
 // ---- everything a kernel needs to read the scene ------------------------------
 struct DevScene {
@@ -111,8 +155,16 @@ struct DevScene {
     const uint4* inst;
     const uint2* items;          // TLAS primitives (instance, BLAS child ref), leaf order
     const MeshInfo* meshes;
-    const uint32_t* orig_idx;    // original index triples (meshes with normals)
-    const float* normals;        // per-vertex normals (meshes with normals)
+    const uint32_t* orig_idx;    // original index triples (meshes with normals or st)
+    const float* normals;        // per-vertex normals (meshes with attributes; 0 without normals)
+    const float* st;             // per-vertex (s, t) (same numbering), or null without any st
+    const float* inst_scale;     // Matrix4::approx_scale per instance (scene order), or null
+    // Pattern graph (null when the scene has none).
+    const DevPattern* patterns;
+    const float4* ramp;          // (position, r, g, b) ramp entries
+    const DevMatPat* mat_pat;    // per material
+    const uint2* binds;          // (field, node)
+    const DevPbr* pbr;
     const DevMaterial* materials;
     const DevLight* lights;
     const LightNode* lbvh;

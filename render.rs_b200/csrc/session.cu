@@ -254,6 +254,16 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     rc = rc ? rc : s->upload(&S.meshes, H.meshes);
     rc = rc ? rc : s->upload(&S.orig_idx, H.orig_idx);
     rc = rc ? rc : s->upload(&S.normals, H.normals);
+    // Texture coordinates and the pattern graph: null pointers when absent.
+    if (!H.st.empty()) rc = rc ? rc : s->upload(&S.st, H.st);
+    if (!H.mat_pat.empty()) {
+        rc = rc ? rc : s->upload(&S.inst_scale, H.inst_scale);
+        rc = rc ? rc : s->upload(&S.patterns, H.patterns);
+        rc = rc ? rc : s->upload(&S.ramp, H.ramp);
+        rc = rc ? rc : s->upload(&S.mat_pat, H.mat_pat);
+        rc = rc ? rc : s->upload(&S.binds, H.binds);
+        rc = rc ? rc : s->upload(&S.pbr, H.pbr);
+    }
     rc = rc ? rc : s->upload(&S.materials, H.materials);
     rc = rc ? rc : s->upload(&S.lights, H.lights);
     rc = rc ? rc : s->upload(&S.lbvh, H.lbvh);
@@ -295,6 +305,8 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     rc = rc ? rc : s->alloc(&Pp.aux_a, aov ? P : 1);
     rc = rc ? rc : s->alloc(&Pp.aux_n, aov ? P : 1);
     rc = rc ? rc : s->alloc(&Pp.aux_d, aov ? P : 1);
+    Pp.cone = nullptr;
+    if (S.mat_pat) rc = rc ? rc : s->alloc(&Pp.cone, P);
     rc = rc ? rc : s->alloc(&Pp.q_ext[0], P);
     rc = rc ? rc : s->alloc(&Pp.q_ext[1], P);
     rc = rc ? rc : s->alloc(&Pp.q_cls, P * N_QUEUES);

@@ -15,6 +15,7 @@ class RtMeshDesc(C.Structure):
         ("normals", C.POINTER(C.c_float)),
         ("n_vertices", C.c_uint32),
         ("n_triangles", C.c_uint32),
+        ("st", C.POINTER(C.c_float)),
     ]
 
 
@@ -81,6 +82,46 @@ class RtCameraDesc(C.Structure):
     ]
 
 
+PATTERN_CHECKER, PATTERN_FRACTAL, PATTERN_MIX, PATTERN_COLOR_CORRECT, PATTERN_RAMP = range(5)
+
+# BoundField (src/texture/pattern.rs:238-254), by the RIB parameter names
+# (BoundField::from_param, pattern.rs:258-275).
+PATTERN_FIELDS = {
+    "diffuseColor": 0, "diffuseGain": 1, "diffuseRoughness": 2, "specularFaceColor": 3,
+    "specularEdgeColor": 4, "specularRoughness": 5, "clearcoatGain": 6, "fuzzGain": 7, "fuzzColor": 8,
+    "glassRefractionGain": 9, "glassRoughness": 10, "refractionColor": 11, "glowColor": 12, "presence": 13,
+}
+FIELD_PRESENCE = 13
+
+
+class RtPatternInput(C.Structure):
+    _fields_ = [("node", C.c_int32), ("pad_", C.c_int32), ("value", c_double3)]
+
+
+class RtPatternDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32),
+        ("octaves", C.c_uint32),
+        ("color_a", c_double3),
+        ("color_b", c_double3),
+        ("scale", C.c_double * 2),
+        ("frequency", C.c_double),
+        ("gain", C.c_double),
+        ("lacunarity", C.c_double),
+        ("gamma", C.c_double),
+        ("saturation", C.c_double),
+        ("inputs", RtPatternInput * 3),
+        ("ramp_positions", C.POINTER(C.c_double)),
+        ("ramp_colors", C.POINTER(C.c_double)),
+        ("n_ramp", C.c_uint32),
+        ("use_t", C.c_uint32),
+    ]
+
+
+class RtPatternBinding(C.Structure):
+    _fields_ = [("material", C.c_uint32), ("field", C.c_uint32), ("node", C.c_uint32), ("pad_", C.c_uint32)]
+
+
 class RtSceneDesc(C.Structure):
     _fields_ = [
         ("meshes", C.POINTER(RtMeshDesc)),
@@ -98,6 +139,10 @@ class RtSceneDesc(C.Structure):
         ("env_height", C.c_uint32),
         ("env_light", C.c_uint32),
         ("env_reserved", C.c_uint32),
+        ("patterns", C.POINTER(RtPatternDesc)),
+        ("bindings", C.POINTER(RtPatternBinding)),
+        ("n_patterns", C.c_uint32),
+        ("n_bindings", C.c_uint32),
     ]
 
 
@@ -121,8 +166,9 @@ class RtParams(C.Structure):
 LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK, LIGHT_DOME = range(6)
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
-for _t, _n in ((RtMeshDesc, 32), (RtInstanceDesc, 104), (RtMaterialDesc, 264),
-               (RtLightDesc, 120), (RtCameraDesc, 144), (RtParams, 64), (RtSceneDesc, 240)):
+for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 264), (RtLightDesc, 120),
+               (RtCameraDesc, 144), (RtParams, 64), (RtPatternInput, 32), (RtPatternDesc, 232),
+               (RtPatternBinding, 16), (RtSceneDesc, 264)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
 

@@ -96,6 +96,12 @@ def affine(linear=None, translate=(0, 0, 0)):
     return m.reshape(12)
 
 
+def _rgb(v):
+    if np.ndim(v) == 0:
+        return (float(v),) * 3
+    return tuple(float(x) for x in v)
+
+
 class Scene:
     """Scene under construction. Keeps every array alive for as long as the
     descriptor returned by :meth:`desc` is in use."""
@@ -109,6 +115,9 @@ class Scene:
         self.lights = []
         self.background = (0.0, 0.0, 0.0)
         self.env = None           # (dome light index, (H, W, 3) f32 radiance) or None
+        self.mesh_st = {}         # mesh id -> (n, 2) f32 texture coordinates
+        self.patterns = []        # pattern nodes (dicts, see add_pattern)
+        self.bindings = []        # (material, field id, node)
         # Reference default camera: origin, looking down +z (camera.rs:97-103).
         self.eye = np.zeros(3)
         self.forward = np.array([0.0, 0.0, 1.0])
@@ -119,15 +128,65 @@ class Scene:
         self._desc = None
 
     # -- geometry --------------------------------------------------------
-    def add_mesh(self, positions, indices, normals=None):
+    def add_mesh(self, positions, indices, normals=None, st=None):
+        """Mesh::new(positions, indices, normals, st) (src/geometry/mesh.rs:
+        37-60); `st` is (n_vertices, 2) texture coordinates or None."""
         p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
         i = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
         n = None if normals is None else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
         if i.size and int(i.max()) >= len(p):
             raise ValueError("mesh index out of range")
         self.meshes.append((p, i, n))
+        if st is not None:
+            st = np.ascontiguousarray(st, dtype=np.float32).reshape(-1, 2)
+            if len(st) != len(p):
+                raise ValueError("st needs one (s, t) pair per vertex")
+            self.mesh_st[len(self.meshes) - 1] = st
         self._desc = None
         return len(self.meshes) - 1
+
+    # -- patterns (src/texture/pattern.rs) ---------------------------------
+    # A node input is another node's index (int) or a constant: a float
+    # (grey) or an RGB triple. Nodes may read only nodes added before them.
+    def _pattern(self, **node):
+        self.patterns.append(node)
+        self._desc = None
+        return len(self.patterns) - 1
+
+    def add_checker(self, color_a, color_b, scale=(1.0, 1.0)):
+        """PxrChecker: color_a where floor(s*ss) + floor(t*ts) is even."""
+        return self._pattern(type=abi.PATTERN_CHECKER, color_a=_rgb(color_a), color_b=_rgb(color_b),
+                             scale=tuple(float(v) for v in scale))
+
+    def add_fractal(self, frequency=1.0, octaves=4, gain=0.5, lacunarity=2.0):
+        """PxrFractal: fBm of Perlin noise over world P, remapped to [0, 1]."""
+        return self._pattern(type=abi.PATTERN_FRACTAL, frequency=float(frequency), octaves=int(octaves),
+                             gain=float(gain), lacunarity=float(lacunarity))
+
+    def add_mix(self, color1, color2, mix):
+        """PxrMix: lerp(color1, color2, mix.r)."""
+        return self._pattern(type=abi.PATTERN_MIX, inputs=(color1, color2, mix))
+
+    def add_color_correct(self, input, gain=(1, 1, 1), offset=(0, 0, 0), gamma=1.0, saturation=1.0):
+        """PxrColorCorrect subset: (in * gain + offset) ^ (1 / gamma), then saturation."""
+        return self._pattern(type=abi.PATTERN_COLOR_CORRECT, inputs=(input,), color_a=_rgb(gain),
+                             color_b=_rgb(offset), gamma=float(gamma), saturation=float(saturation))
+
+    def add_ramp(self, positions, colors, use_t=False):
+        """PxrRamp subset: piecewise-linear colours over s (or t)."""
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1)
+        col = np.ascontiguousarray(colors, dtype=np.float64).reshape(-1, 3)
+        if len(pos) != len(col):
+            raise ValueError("ramp needs one colour per position")
+        return self._pattern(type=abi.PATTERN_RAMP, ramp=(pos, col), use_t=bool(use_t))
+
+    def bind_pattern(self, material, field, node):
+        """Material::pattern_bindings: `node`'s output replaces PbrParams
+        field `field` (a RIB parameter name such as "diffuseColor", or an
+        RT_FIELD_* id) at every shading point."""
+        f = abi.PATTERN_FIELDS[field] if isinstance(field, str) else int(field)
+        self.bindings.append((int(material), f, int(node)))
+        self._desc = None
 
     def add_instance(self, mesh_id, material_id, xform=None):
         rec = np.zeros(1, dtype=INSTANCE_DTYPE)
@@ -227,6 +286,10 @@ class Scene:
         mesh_arr = (abi.RtMeshDesc * max(1, len(self.meshes)))()
         for k, (p, i, n) in enumerate(self.meshes):
             keep += [p, i, n]
+            st = self.mesh_st.get(k)
+            if st is not None:
+                keep.append(st)
+                mesh_arr[k].st = st.ctypes.data_as(C.POINTER(C.c_float))
             mesh_arr[k].positions = p.ctypes.data_as(C.POINTER(C.c_float))
             mesh_arr[k].indices = i.ctypes.data_as(C.POINTER(C.c_uint32))
             mesh_arr[k].normals = n.ctypes.data_as(C.POINTER(C.c_float)) if n is not None else None
@@ -269,6 +332,41 @@ class Scene:
             d.env_rgb = env.ctypes.data_as(C.POINTER(C.c_float))
             d.env_height, d.env_width = env.shape[0], env.shape[1]
             d.env_light = li
+        pat_arr = (abi.RtPatternDesc * max(1, len(self.patterns)))()
+        for k, node in enumerate(self.patterns):
+            pd = pat_arr[k]
+            pd.type = node["type"]
+            pd.octaves = node.get("octaves", 0)
+            pd.color_a = abi.c_double3(*node.get("color_a", (0, 0, 0)))
+            pd.color_b = abi.c_double3(*node.get("color_b", (0, 0, 0)))
+            pd.scale = (C.c_double * 2)(*node.get("scale", (1.0, 1.0)))
+            pd.frequency, pd.gain = node.get("frequency", 1.0), node.get("gain", 0.5)
+            pd.lacunarity = node.get("lacunarity", 2.0)
+            pd.gamma, pd.saturation = node.get("gamma", 1.0), node.get("saturation", 1.0)
+            for j, v in enumerate(node.get("inputs", ())):
+                if isinstance(v, (int, np.integer)) and not isinstance(v, bool):
+                    pd.inputs[j].node = int(v)
+                else:
+                    pd.inputs[j].node = -1
+                    pd.inputs[j].value = abi.c_double3(*_rgb(v))
+            for j in range(len(node.get("inputs", ())), 3):
+                pd.inputs[j].node = -1
+            if "ramp" in node:
+                pos, col = node["ramp"]
+                keep += [pos, col]
+                pd.ramp_positions = pos.ctypes.data_as(C.POINTER(C.c_double))
+                pd.ramp_colors = col.ctypes.data_as(C.POINTER(C.c_double))
+                pd.n_ramp = len(pos)
+                pd.use_t = int(node["use_t"])
+        bind_arr = (abi.RtPatternBinding * max(1, len(self.bindings)))()
+        for k, (m, f, n) in enumerate(self.bindings):
+            bind_arr[k].material, bind_arr[k].field, bind_arr[k].node = m, f, n
+        if self.patterns:
+            d.patterns = pat_arr
+            d.n_patterns = len(self.patterns)
+        if self.bindings:
+            d.bindings = bind_arr
+            d.n_bindings = len(self.bindings)
         self._desc = d
-        self._keep = (keep, mesh_arr, mat_arr, light_arr)
+        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr)
         return d

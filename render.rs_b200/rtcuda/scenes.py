@@ -396,3 +396,50 @@ def forest(width=3840, height=2160, n_trees=20, n_placements=386_000, n_lights=1
 
 
 FOREST = dict(spp=32, max_depth=10, rr_start=3)
+
+
+def patterned_room(width=96, height=72):
+    """A small room whose materials are driven by procedural patterns
+    (src/texture/pattern.rs): a checker floor (8 x 8 cells over st, fine
+    enough that the ray-cone footprint blends it far away), a back wall
+    whose diffuse colour mixes a ramp over s with a colour-corrected fBm,
+    fBm-driven specular roughness on a plastic block placed with a 0.5
+    scale (st density doubles in world units), and a ceiling light."""
+    s = Scene(width, height, fov=50.0)
+    s.look_at((0.0, 1.0, -3.2), (0.0, 0.8, 0.0))
+    st_quad = np.array([[0.0, 0.0], [1.0, 0.0], [1.0, 1.0], [0.0, 1.0]])
+
+    def quad_mesh(corner, e1, e2):
+        p, i = quad(corner, e1, e2)
+        return s.add_mesh(p, i, st=st_quad)
+
+    checker = s.add_checker((0.8, 0.8, 0.8), (0.1, 0.1, 0.1), scale=(8.0, 8.0))
+    floor_m = s.add_material(matte((1.0, 1.0, 1.0)))
+    s.bind_pattern(floor_m, "diffuseColor", checker)
+    s.add_instance(quad_mesh((-2, 0, -4), (0, 0, 6), (4, 0, 0)), floor_m)
+
+    ramp = s.add_ramp([0.0, 0.5, 1.0], [[0.9, 0.2, 0.1], [0.2, 0.8, 0.2], [0.1, 0.3, 0.9]])
+    noise = s.add_fractal(frequency=3.0, octaves=4, gain=0.5, lacunarity=2.0)
+    graded = s.add_color_correct(noise, gain=(1.2, 1.0, 0.8), offset=(0.0, 0.05, 0.1), gamma=1.5, saturation=0.6)
+    wall = s.add_mix(ramp, graded, 0.4)
+    wall_m = s.add_material(matte((1.0, 1.0, 1.0)))
+    s.bind_pattern(wall_m, "diffuseColor", wall)
+    s.add_instance(quad_mesh((-2, 0, 2), (4, 0, 0), (0, 3, 0)), wall_m)
+    side = s.add_material(matte((0.6, 0.6, 0.6)))
+    s.add_instance(quad_mesh((-2, 0, -4), (0, 3, 0), (0, 0, 6)), side)
+    s.add_instance(quad_mesh((2, 0, -4), (0, 0, 6), (0, 3, 0)), side)
+    s.add_instance(quad_mesh((-2, 3, -4), (4, 0, 0), (0, 0, 6)), side)
+
+    rough = s.add_fractal(frequency=6.0, octaves=3)
+    block_m = s.add_material(ggx_floor((0.7, 0.5, 0.3), 0.3))
+    s.bind_pattern(block_m, "specularRoughness", rough)
+    s.bind_pattern(block_m, "diffuseColor", s.add_checker((0.9, 0.6, 0.2), (0.2, 0.3, 0.8), scale=(4.0, 4.0)))
+    # The cube with one st square per face (unshared corners).
+    cp, ci = unit_cube()
+    corners = np.concatenate([cp[[t0[0], t0[1], t0[2], t1[2]]] for t0, t1 in zip(ci[0::2], ci[1::2])])
+    idx = np.array([[4 * f, 4 * f + 1, 4 * f + 2, 4 * f, 4 * f + 2, 4 * f + 3] for f in range(6)]).reshape(-1, 3)
+    block = s.add_mesh(corners, idx, st=np.tile(st_quad, (6, 1)))
+    s.add_instance(block, block_m, affine(rot_y(25) * 0.5, (0.4, 0.5, 0.6)))
+
+    s.add_emissive_quad((-0.5, 2.99, -0.5), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0), (12.0, 11.0, 9.0))
+    return s
