@@ -21,9 +21,14 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     are tessellated into smooth-normal triangle meshes; the reference
     intersects them analytically.
   * SubdivisionMesh renders its control cage; Curves, Points, patches,
-    patterns, displacement, media and motion blur are skipped (motion
-    blocks use their first sample); a PxrDomeLight lightColorMap is read
-    when it is a Radiance .hdr (one map per scene).
+    displacement, media and motion blur are skipped (motion blocks use
+    their first sample); a PxrDomeLight lightColorMap is read when it is a
+    Radiance .hdr (one map per scene).
+  * Pattern graphs: PxrChecker, PxrFractal, PxrMix, PxrColorCorrect and
+    PxrRamp nodes and Bxdf "reference" connections are carried; file
+    textures (PxrTexture, triplanar) and presence connections are skipped.
+    Tessellated spheres and cylinders carry the reference's st; the other
+    quadrics have none.
 """
 import math
 import os
@@ -350,9 +355,9 @@ def _xf_vec(m, v):
 # ---- quadric tessellation ----------------------------------------------------------------------
 
 
-def _grid(fn, nu, nv):
-    """Parametric surface on [0,1]^2 -> (positions, normals, indices); fn
-    maps (u, v) arrays to (points (..,3), normals (..,3))."""
+def _grid(fn, nu, nv, with_uv=False):
+    """Parametric surface on [0,1]^2 -> (positions, normals, indices[, uv]);
+    fn maps (u, v) arrays to (points (..,3), normals (..,3))."""
     u = np.linspace(0.0, 1.0, nu + 1)
     v = np.linspace(0.0, 1.0, nv + 1)
     U, V = np.meshgrid(u, v)  # (nv+1, nu+1)
@@ -374,14 +379,28 @@ def _grid(fn, nu, nv):
     I[flip] = I[flip][:, [0, 2, 1]]
     area = np.linalg.norm(g, axis=1)
     I = I[area > 0]
-    return P.astype(np.float32), N.astype(np.float32), I.astype(np.uint32)
+    out = (P.astype(np.float32), N.astype(np.float32), I.astype(np.uint32))
+    return out + (np.stack([U.reshape(-1), V.reshape(-1)], -1),) if with_uv else out
 
 
 def _segments(thetamax):
     return max(8, int(math.ceil(64 * abs(thetamax) / 360.0)))
 
 
-def tessellate(kind, a):
+def quadric_st(kind, a):
+    """(P, N, I, st) of a Sphere or Cylinder with the reference's st
+    (sphere.rs:86-93, cylinder.rs:100-107: s = phi / thetamax, t = (z -
+    zmin) / (zmax - zmin)), taken at the tessellation's grid vertices so
+    the seam column keeps s = 1; None for other quadrics."""
+    if kind not in ("Sphere", "Cylinder"):
+        return None
+    P, N, I, uv = tessellate(kind, a, with_uv=True)
+    zmin, zmax = a[1], a[2]
+    t = np.clip((P[:, 2].astype(np.float64) - zmin) / max(zmax - zmin, 1e-12), 0.0, 1.0)
+    return P, N, I, np.stack([uv[:, 0], t], -1).astype(np.float32)
+
+
+def tessellate(kind, a, with_uv=False):
     """Triangle mesh of a RenderMan quadric (RiSpec parameterisations)."""
     if kind == "Sphere":
         r, zmin, zmax, tm = a
@@ -393,7 +412,7 @@ def tessellate(kind, a):
             ph = p0 + V * (p1 - p0)
             n = np.stack([np.cos(ph) * np.cos(th), np.cos(ph) * np.sin(th), np.sin(ph)], -1)
             return r * n, n if r > 0 else -n
-        return _grid(f, _segments(tm), 32)
+        return _grid(f, _segments(tm), 32, with_uv)
     if kind == "Cylinder":
         r, zmin, zmax, tm = a
 
@@ -401,7 +420,7 @@ def tessellate(kind, a):
             th = U * math.radians(tm)
             P = np.stack([r * np.cos(th), r * np.sin(th), zmin + V * (zmax - zmin)], -1)
             return P, np.stack([np.cos(th), np.sin(th), np.zeros_like(th)], -1)
-        return _grid(f, _segments(tm), 1)
+        return _grid(f, _segments(tm), 1, with_uv)
     if kind == "Cone":
         h, r, tm = a
 
@@ -518,6 +537,7 @@ class _State:
         self.roughness = 0.1
         self.area_light = None   # (intensity, color)
         self.bxdf = None         # material dict
+        self.bxdf_bindings = []  # (field id, pattern node) of the active Bxdf
         self.identifier = None
 
     def copy(self):
@@ -563,6 +583,10 @@ class _Builder:
         self.env = None
         # scene contents (materials / lights / meshes / instances)
         self.meshes, self.instances, self.materials, self.lights = [], [], [], []
+        self.mesh_st = {}                 # mesh index -> (n, 2) st
+        self.patterns = []                # Scene pattern node dicts
+        self.pattern_handles = {}         # handle -> node index
+        self.bindings = []                # (material, field id, node)
 
     # -- helpers ------------------------------------------------------------------
     def warn(self, msg):
@@ -597,9 +621,14 @@ class _Builder:
         else:
             m = _pbr_matte(st.color)
         m["id"] = self.object_id()
+        if st.bxdf is not None and st.bxdf_bindings:
+            m["_bindings"] = list(st.bxdf_bindings)
         return m
 
     def add_material(self, m):
+        m = dict(m)
+        for field, node in m.pop("_bindings", ()):
+            self.bindings.append((len(self.materials), field, node))
         self.materials.append(m)
         return len(self.materials) - 1
 
@@ -608,18 +637,20 @@ class _Builder:
                                 e1=tuple(e1), e2=tuple(e2), radius=float(radius)))
         return len(self.lights) - 1
 
-    def add_mesh(self, P, I, N=None):
+    def add_mesh(self, P, I, N=None, st=None):
         self.meshes.append((np.asarray(P, np.float32).reshape(-1, 3), np.asarray(I, np.uint32).reshape(-1, 3),
                             None if N is None else np.asarray(N, np.float32).reshape(-1, 3)))
+        if st is not None:
+            self.mesh_st[len(self.meshes) - 1] = np.asarray(st, np.float32).reshape(-1, 2)
         return len(self.meshes) - 1
 
     def place(self, mesh, mat, xf):
         self.instances.append((mesh, mat, np.asarray(xf, np.float64)[:3, :].reshape(12)))
 
-    def tessellated_mesh(self, P, I, N=None, emissive=True):
+    def tessellated_mesh(self, P, I, N=None, emissive=True, st=None):
         """add_tessellated_mesh (scene_builder.rs:1195-1234); quadrics take
         the plain state material (no area-light emission, :813-909)."""
-        mesh = self.add_mesh(P, I, N)
+        mesh = self.add_mesh(P, I, N, st)
         m = self.make_material()
         if emissive and self.state.area_light is not None:
             inten, col = self.state.area_light
@@ -779,7 +810,11 @@ class _Builder:
                 self.warn("hair is not rendered on this path; PxrMarschnerHair treated as PxrSurface")
             elif t != "PxrSurface":
                 self.warn(f'Bxdf "{t}" not implemented; treating as PxrSurface')
-            st.bxdf = _pbr_bxdf(_Params(vals, 2 if len(vals) % 2 == 0 else 1))
+            prm = _Params(vals, 2 if len(vals) % 2 == 0 else 1)
+            st.bxdf = _pbr_bxdf(prm)
+            st.bxdf_bindings = self.bxdf_bindings(prm)
+        elif name == "Pattern":
+            self.pattern_request(vals)
         elif name == "AreaLightSource":
             p = _Params(vals, 2 if len(vals) % 2 == 0 else 1)
             inten = p.number("intensity")
@@ -809,8 +844,12 @@ class _Builder:
                     self.warn(f"{name} inside ObjectBegin is not instanced; skipping")
                     return
                 self.warn("quadrics are tessellated into triangle meshes (the reference intersects them exactly)")
-                P, N, I = tessellate(name, a)
-                self.tessellated_mesh(P, I, N, emissive=False)
+                q = quadric_st(name, a)
+                if q is not None:
+                    self.tessellated_mesh(q[0], q[2], q[1], emissive=False, st=q[3])
+                else:
+                    P, N, I = tessellate(name, a)
+                    self.tessellated_mesh(P, I, N, emissive=False)
         else:
             self.warn(f"RIB request '{name}' not rendered on this path; skipping")
 
@@ -919,7 +958,115 @@ class _Builder:
         I = np.array(tris, dtype=np.int64)
         if I.max() >= len(P):
             raise RibError(f"{name}: vertex index out of range")
-        self.tessellated_mesh(P, I, N)
+        stv = prm.numbers("st")
+        ST = None
+        if stv is not None and len(stv) * 3 == len(p) * 2:
+            ST = np.array(stv, dtype=np.float64).reshape(-1, 2)
+        self.tessellated_mesh(P, I, N, st=ST)
+
+    # -- patterns (scene_builder.rs:703-728, 1738-1846) -------------------------------
+    def _ref_target(self, prm, name):
+        """The node a "reference <type> <name>" ["handle:output"] parameter
+        names, or None."""
+        for t, v in prm.pairs:
+            w = t.split()
+            if "reference" in w and w[-1] == name:
+                target = v if isinstance(v, str) else (v[0] if isinstance(v, list) and v and
+                                                       isinstance(v[0], str) else None)
+                if target is not None:
+                    return self.pattern_handles.get(target.split(":")[0])
+        return None
+
+    def pattern_input(self, prm, name, default):
+        node = self._ref_target(prm, name)
+        if node is not None:
+            return node
+        v = prm.numbers(name)
+        if v is not None and len(v) >= 3:
+            return tuple(v[:3])
+        if v is not None and len(v) >= 1:
+            return (v[0],) * 3
+        return tuple(default)
+
+    def pattern_request(self, vals):
+        """pattern_request: one node of the scene's pattern graph, named by
+        its handle; the file-texture nodes are not carried."""
+        ptype = _str(vals, 0) or ""
+        start = 2 if len(vals) % 2 == 0 else 1
+        handle = _str(vals, 1) if start == 2 else None
+        if handle is None:
+            self.warn("Pattern without a handle; skipping")
+            return
+        prm = _Params(vals, start)
+
+        def color(name, default):
+            v = prm.numbers(name)
+            return tuple(v[:3]) if v is not None and len(v) >= 3 else default
+
+        def number(name, default):
+            v = prm.number(name)
+            return default if v is None else v
+
+        if ptype in ("PxrChecker", "checker"):
+            node = dict(type=abi.PATTERN_CHECKER, color_a=color("colorA", (1.0, 1.0, 1.0)),
+                        color_b=color("colorB", (0.0, 0.0, 0.0)),
+                        scale=(number("sScale", 8.0), number("tScale", 8.0)))
+        elif ptype in ("PxrFractal", "fractal", "noise"):
+            node = dict(type=abi.PATTERN_FRACTAL, frequency=number("frequency", 1.0),
+                        octaves=int(number("layers", 4.0)), gain=number("gain", 0.5),
+                        lacunarity=number("lacunarity", 2.0))
+        elif ptype in ("PxrMix", "mix"):
+            node = dict(type=abi.PATTERN_MIX, inputs=(self.pattern_input(prm, "color1", (0.0, 0.0, 0.0)),
+                                                      self.pattern_input(prm, "color2", (1.0, 1.0, 1.0)),
+                                                      self.pattern_input(prm, "mix", (0.0, 0.0, 0.0))))
+        elif ptype in ("PxrColorCorrect", "colorCorrect"):
+            node = dict(type=abi.PATTERN_COLOR_CORRECT,
+                        inputs=(self.pattern_input(prm, "inputRGB", (0.5, 0.5, 0.5)),),
+                        color_a=color("gain", (1.0, 1.0, 1.0)), color_b=color("offset", (0.0, 0.0, 0.0)),
+                        gamma=number("gamma", 1.0), saturation=number("saturation", 1.0))
+        elif ptype in ("PxrRamp", "ramp"):
+            pos = prm.numbers("positions")
+            pos = [0.0, 1.0] if pos is None else list(pos)
+            col = prm.numbers("colors")
+            col = [0.0, 0.0, 0.0, 1.0, 1.0, 1.0] if col is None else list(col)
+            n = min(len(pos), len(col) // 3)
+            if n != len(pos) or n * 3 != len(col):
+                self.warn(f'Pattern "{handle}": ramp positions and colours differ in count; using {n}')
+            node = dict(type=abi.PATTERN_RAMP,
+                        ramp=(np.array(pos[:n], np.float64), np.array(col[:3 * n], np.float64).reshape(-1, 3)),
+                        use_t=prm.string("axis") == "t")
+        elif ptype in ("PxrTexture", "texture", "triplanar"):
+            self.warn(f'Pattern "{ptype}": file textures are not rendered on this path; skipping')
+            return
+        else:
+            self.warn(f'Pattern "{ptype}" not implemented; skipping')
+            return
+        self.pattern_handles[handle] = len(self.patterns)
+        self.patterns.append(node)
+
+    def bxdf_bindings(self, prm):
+        """The Bxdf's "reference <type> <param>" ["handle:output"]
+        connections as (field id, node) pairs."""
+        out = []
+        for t, v in prm.pairs:
+            w = t.split()
+            if "reference" not in w:
+                continue
+            param = w[-1]
+            field = abi.PATTERN_FIELDS.get(param)
+            if field is None:
+                self.warn(f'reference to unsupported Bxdf param "{param}"; ignoring')
+                continue
+            node = self._ref_target(prm, param)
+            if node is None:
+                target = v if isinstance(v, str) else (v[0] if isinstance(v, list) and v else "")
+                self.warn(f'Bxdf references unknown Pattern "{str(target).split(":")[0]}"; ignoring')
+                continue
+            if field == abi.FIELD_PRESENCE:
+                self.warn("presence driven by a pattern is not rendered on this path; ignoring")
+                continue
+            out.append((field, node))
+        return out
 
     def light_source(self, vals):
         """parse_light (scene_builder.rs:1582-1635): positions untransformed."""
@@ -1005,8 +1152,10 @@ class _Builder:
 
     def scene(self):
         s = RibScene(self.width, self.height, self.fov)
-        for P, I, N in self.meshes:
-            s.add_mesh(P, I, N)
+        for k, (P, I, N) in enumerate(self.meshes):
+            s.add_mesh(P, I, N, st=self.mesh_st.get(k))
+        s.patterns = [dict(n) for n in self.patterns]
+        s.bindings = list(self.bindings)
         for m in self.materials:
             s.add_material(m)
         for l in self.lights:

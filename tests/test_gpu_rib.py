@@ -87,7 +87,31 @@ WorldEnd
 """
 
 
-@pytest.mark.parametrize("text", [BOX, PXR], ids=["legacy_box_quadrics", "pxr_lights"])
+PATTERNS = """
+Format 40 30 1.0
+Projection "perspective" "fov" [45]
+WorldBegin
+  LightSource "pointlight" 1 "from" [0.5 1.5 3.5] "intensity" [20]
+  AttributeBegin
+    Pattern "PxrChecker" "check" "colorA" [0.9 0.9 0.9] "colorB" [0.1 0.1 0.1] "sScale" [6] "tScale" [6]
+    Bxdf "PxrSurface" "floor" "reference color diffuseColor" ["check:resultRGB"] "specularIor" [1]
+    PointsPolygons [4] [0 1 2 3] "P" [-2 -1 2  2 -1 2  2 -1 7  -2 -1 7] "st" [0 0  1 0  1 1  0 1]
+  AttributeEnd
+  AttributeBegin
+    Pattern "PxrFractal" "grain" "frequency" [4] "layers" [3]
+    Pattern "PxrRamp" "band" "positions" [0 1] "colors" [0.9 0.2 0.1  0.1 0.3 0.9] "axis" "t"
+    Pattern "PxrMix" "paint" "reference color color1" ["band:resultRGB"] "color2" [0.9 0.9 0.2]
+      "reference float mix" ["grain:resultF"]
+    Bxdf "PxrSurface" "ball" "reference color diffuseColor" ["paint:resultRGB"] "specularIor" [1.5]
+      "reference float specularRoughness" ["grain:resultF"]
+    Translate 0 -0.4 4.5
+    Sphere 0.6 -0.6 0.6 360
+  AttributeEnd
+WorldEnd
+"""
+
+
+@pytest.mark.parametrize("text", [BOX, PXR, PATTERNS], ids=["legacy_box_quadrics", "pxr_lights", "patterns"])
 def test_rib_scene_matches_oracle(text):
     s = load_rib_string(text)
     p = abi.make_params(max_depth=8)

@@ -296,3 +296,58 @@ def test_pxr_dome_light_reads_hdr_map(tmp_path):
     s = load_rib(str(tmp_path / "s.rib"))
     assert s.env is not None and s.env[0] == 0 and s.env[1].shape == (4, 16, 3)
     np.testing.assert_allclose(s.env[1], 0.5, atol=1 / 256)  # RGBE has 8-bit mantissas
+
+
+def test_pattern_graph_binds_to_bxdf():
+    """scene_builder.rs:1993-2023: two Pattern nodes, one Bxdf connection;
+    the checker cell (0, 0) is red, mixed 25% toward green."""
+    import oracle
+    s = load_rib_string('''
+        Format 64 64 1.0
+        WorldBegin
+            Pattern "PxrChecker" "check" "colorA" [1 0 0] "colorB" [0 0 1] "sScale" [4] "tScale" [4]
+            Pattern "PxrMix" "blend" "reference color color1" ["check:resultRGB"] "color2" [0 1 0] "mix" [0.25]
+            Bxdf "PxrSurface" "mat" "reference color diffuseColor" ["blend:resultRGB"] "specularIor" [1]
+            Sphere 1 -1 1 360
+        WorldEnd''')
+    assert len(s.patterns) == 2
+    assert s.bindings == [(len(s.materials) - 1, abi.PATTERN_FIELDS["diffuseColor"], 1)]
+    c = oracle.pattern_eval(s, 1, [[0.1, 0.1, 0.0, 0.0, 0.0, 0.0]])[0]
+    assert abs(c[0] - 0.75) < 1e-9 and abs(c[1] - 0.25) < 1e-9
+
+
+def test_pattern_requests_and_connections():
+    s = load_rib_string('''
+        Pattern "PxrFractal" "n" "frequency" [2] "layers" [3] "gain" [0.4]
+        Pattern "PxrColorCorrect" "cc" "reference color inputRGB" ["n:resultRGB"] "gamma" [2] "saturation" [0.5]
+        Pattern "PxrRamp" "r" "positions" [0 0.5 1] "colors" [0 0 0  1 0 0  1 1 1] "axis" "t"
+        Pattern "PxrTexture" "tex" "filename" "wood.tex"
+        Pattern "PxrChecker" "nohandle_is_fine" 
+        Bxdf "PxrSurface" "m" "reference color diffuseColor" ["cc:resultRGB"] "reference float presence" ["n:resultF"]
+          "reference color specularFaceColor" ["tex:resultRGB"] "reference float bogus" ["n:resultF"]
+        Polygon "P" [0 0 1  1 0 1  1 1 1]''')
+    kinds = [n["type"] for n in s.patterns]
+    assert kinds == [abi.PATTERN_FRACTAL, abi.PATTERN_COLOR_CORRECT, abi.PATTERN_RAMP, abi.PATTERN_CHECKER]
+    assert s.patterns[0]["octaves"] == 3 and s.patterns[0]["gain"] == 0.4
+    assert s.patterns[1]["inputs"] == (0,) and s.patterns[1]["gamma"] == 2.0
+    assert s.patterns[2]["use_t"] and list(s.patterns[2]["ramp"][0]) == [0.0, 0.5, 1.0]
+    assert s.patterns[3]["scale"] == (8.0, 8.0) and s.patterns[3]["color_a"] == (1.0, 1.0, 1.0)
+    assert [b[1:] for b in s.bindings] == [(abi.PATTERN_FIELDS["diffuseColor"], 1)]
+    w = " | ".join(s.warnings)
+    assert "file textures" in w and "presence" in w and "unknown Pattern \"tex\"" in w and "bogus" in w
+
+
+def test_st_primvar_and_quadric_st():
+    s = load_rib_string('PointsPolygons [4] [0 1 2 3] "P" [0 0 1  1 0 1  1 1 1  0 1 1] "st" [0 0  1 0  1 1  0 1]\n'
+                        'PointsPolygons [3] [0 1 2] "P" [0 0 1  1 0 1  1 1 1] "st" [0 0  1 0]\n'
+                        'Sphere 1 -0.5 1 180\nCylinder 1 0 2 360\nTorus 1 0.2 0 360 360')
+    assert sorted(s.mesh_st) == [0, 2, 3]  # wrong-length st ignored; the torus carries none
+    np.testing.assert_array_equal(s.mesh_st[0], [[0, 0], [1, 0], [1, 1], [0, 1]])
+    P, st = s.meshes[2][0], s.mesh_st[2]
+    # sphere.rs:86-93: s = phi / thetamax, t = (z - zmin) / (zmax - zmin).
+    phi = np.degrees(np.arctan2(P[:, 1], P[:, 0])) % 360.0
+    ring = np.hypot(P[:, 0], P[:, 1])
+    inner = (st[:, 0] > 1e-3) & (st[:, 0] < 1 - 1e-3) & (ring > 1e-3)  # phi is undefined at the pole
+    np.testing.assert_allclose(st[inner, 0], phi[inner] / 180.0, atol=1e-4)
+    np.testing.assert_allclose(st[:, 1], (P[:, 2] + 0.5) / 1.5, atol=1e-5)
+    assert st[:, 0].min() == 0.0 and st[:, 0].max() == 1.0
