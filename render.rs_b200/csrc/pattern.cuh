@@ -202,8 +202,10 @@ __device__ __forceinline__ void fold_pbr(const DevPbr& q, DevMaterial& d) {
 
 // Material `mat` at a shading point: base parameters with every bound
 // pattern output substituted in binding order, folded into `d` (which
-// must hold the material's plain record on entry).
-__device__ __forceinline__ void resolve_material(const DevScene& S, const DevMatPat& mp, float s, float t, float3 p,
+// must hold the material's plain record on entry). Kept out of line: only
+// patterned hits call it, and inlined its node table and fold would raise
+// the shade kernel's register count for every scene (128 -> 192).
+__device__ __noinline__ void resolve_material(const DevScene& S, const DevMatPat& mp, float s, float t, float3 p,
                                                  float footprint, DevMaterial& d) {
     float3 v[RT_MAX_PATTERN_NODES];
     for (uint32_t k = 0; k < RT_MAX_PATTERN_NODES; k++) {

@@ -741,6 +741,10 @@ __device__ __forceinline__ float light_pdf_sa(const DevLight& L, float3 origin, 
 #ifndef RT_SHADE_MIN_BLOCKS
 #define RT_SHADE_MIN_BLOCKS 1
 #endif
+// PAT: the scene has patterns (ray cones tracked, patterned materials
+// resolved per hit). The plain instance keeps its material reads on the
+// global material table and the register count of a kernel without them.
+template <bool PAT>
 __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, Paths P, PtConsts C, uint32_t qout) {
     uint32_t counts[N_QUEUES];
     uint32_t total = 0;
@@ -838,7 +842,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                 float2 cone = make_float2(0.0f, 0.0f);
                 DevMaterial mres;
                 const DevMaterial* mptr = S.materials + hg.mat;
-                if (P.cone) {
+                if (PAT) {
                     cone = P.cone[slot];
                     cone.x += eucl * cone.y;
                     const DevMatPat mp = S.mat_pat[hg.mat];
@@ -972,7 +976,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                         flags &= ~FL_FROM_CAMERA;
                         beta4.w = pdf_path;
                         // Widen the cone after rough bounces (pt/mod.rs:965-967).
-                        cone.y += fminf(1.0f / (1.0f + pdf_path), 0.4f);
+                        if (PAT) cone.y += fminf(1.0f / (1.0f + pdf_path), 0.4f);
                         prev4 = make_float4(p.x, p.y, p.z, 0.0f);
                         float off = bs.transmitted ? -RT_RAY_OFFSET : RT_RAY_OFFSET;
                         float3 no = p + n * off;
@@ -992,7 +996,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                         }
                     }
                 }
-                if (P.cone) P.cone[slot] = cone;
+                if (PAT) P.cone[slot] = cone;
             }
             P.beta[slot] = make_float4(beta.x, beta.y, beta.z, beta4.w);
             P.L[slot] = make_float4(Lr.x, Lr.y, Lr.z, travel);

@@ -490,7 +490,8 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
                 P.g_raw = raw;
                 launches += 3;
             }
-            k_shade<<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
+            if (P.cone) k_shade<true><<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
+            else k_shade<false><<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 2], st));
             k_shadow<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 3], st));
