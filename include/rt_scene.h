@@ -116,16 +116,29 @@ typedef struct rt_camera_desc {
     double   filter_width;
 } rt_camera_desc;
 
-/* Procedural pattern node (src/texture/pattern.rs:47-67; PatternNode).
- * Every node outputs RGB; scalar consumers read channel 0. The file-texture
- * nodes (Texture, Triplanar) are not carried. */
+/* Pattern node (src/texture/pattern.rs:47-67; PatternNode). Every node
+ * outputs RGB; scalar consumers read channel 0. */
 enum {
     RT_PATTERN_CHECKER       = 0,  /* color_a / color_b cells over st * scale, footprint-filtered */
     RT_PATTERN_FRACTAL       = 1,  /* fBm of classic Perlin noise over world P, remapped to [0,1] */
     RT_PATTERN_MIX           = 2,  /* lerp(in[0], in[1], in[2].r) */
     RT_PATTERN_COLOR_CORRECT = 3,  /* (in[0] * color_a + color_b) ^ (1 / gamma), then saturation */
-    RT_PATTERN_RAMP          = 4   /* piecewise-linear ramp over s (or t) */
+    RT_PATTERN_RAMP          = 4,  /* piecewise-linear ramp over s (or t) */
+    RT_PATTERN_TEXTURE       = 5,  /* file texture over st * scale (trilinear, or EWA along the footprint) */
+    RT_PATTERN_TRIPLANAR     = 6   /* file texture projected on the three axis planes of P * frequency */
 };
+
+/* Texture wrap modes (src/texture/cache.rs:19-34). */
+enum { RT_WRAP_PERIODIC = 0, RT_WRAP_CLAMP = 1, RT_WRAP_BLACK = 2 };
+
+/* A file texture's base image, linear RGB f32, row-major from the top row
+ * (what the reference's texture cache holds after txmake,
+ * src/texture/tex.rs:71-87); the consumer builds the mip chain. */
+typedef struct rt_texture_desc {
+    const float* rgb;     /* 3 * width * height */
+    uint32_t width;
+    uint32_t height;
+} rt_texture_desc;
 
 /* Node input (PInput): another node's output or a constant. A node may only
  * read nodes of lower index (the graph is a DAG in index order). */
@@ -140,14 +153,16 @@ typedef struct rt_pattern_desc {
     uint32_t octaves;             /* fractal */
     double   color_a[3];          /* checker colour A; colour-correct gain */
     double   color_b[3];          /* checker colour B; colour-correct offset */
-    double   scale[2];            /* checker s, t scale */
-    double   frequency, gain, lacunarity;  /* fractal */
+    double   scale[2];            /* checker, texture s, t scale */
+    double   frequency, gain, lacunarity;  /* fractal; triplanar frequency */
     double   gamma, saturation;   /* colour correct */
     rt_pattern_input in[3];       /* mix: color1, color2, mix; colour correct: in[0] */
     const double* ramp_positions; /* n_ramp, ascending */
     const double* ramp_colors;    /* 3 * n_ramp */
     uint32_t n_ramp;
     uint32_t use_t;               /* ramp over t instead of s */
+    int32_t  texture;             /* texture, triplanar: index into textures, -1 = missing (magenta) */
+    uint32_t wrap;                /* RT_WRAP_* */
 } rt_pattern_desc;
 
 /* PbrParams fields a pattern output drives (BoundField, pattern.rs:238-254). */
@@ -193,6 +208,9 @@ typedef struct rt_scene_desc {
     const rt_pattern_binding* bindings;
     uint32_t n_patterns;
     uint32_t n_bindings;
+    const rt_texture_desc*    textures;
+    uint32_t n_textures;
+    uint32_t tex_reserved;    /* 0 */
 } rt_scene_desc;
 
 /* Integrator knobs. The reference hard-codes these as constants
@@ -223,9 +241,10 @@ static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
 static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
 static_assert(sizeof(rt_params) == 64, "rt_params layout");
 static_assert(sizeof(rt_pattern_input) == 32, "rt_pattern_input layout");
-static_assert(sizeof(rt_pattern_desc) == 232, "rt_pattern_desc layout");
+static_assert(sizeof(rt_pattern_desc) == 240, "rt_pattern_desc layout");
+static_assert(sizeof(rt_texture_desc) == 16, "rt_texture_desc layout");
 static_assert(sizeof(rt_pattern_binding) == 16, "rt_pattern_binding layout");
-static_assert(sizeof(rt_scene_desc) == 264, "rt_scene_desc layout");
+static_assert(sizeof(rt_scene_desc) == 280, "rt_scene_desc layout");
 }
 #endif
 

@@ -51,6 +51,7 @@ def lib():
         L.oracle_filter_sample.argtypes = [C.c_int, C.c_double, C.c_uint64, vp, vp]
         L.oracle_pattern_eval.argtypes = [vp, C.c_uint32, C.c_uint64, vp, vp]
         L.oracle_intersect_st.argtypes = [vp, C.c_uint64, vp, vp]
+        L.oracle_texture_sample.argtypes = [C.c_uint32, C.c_uint32, vp, C.c_int, C.c_uint64, vp, vp]
         L.oracle_light_pmf.restype = C.c_double
         L.oracle_light_pmf.argtypes = [vp, f64p, C.c_uint32]
         _lib = L
@@ -211,11 +212,31 @@ def env_sample(env, uv):
 
 def pattern_eval(scene, node, ctx):
     """pattern.rs eval of `node` of `scene`'s pattern graph at points ctx
-    (n, 6) = (s, t, Px, Py, Pz, footprint); returns (n, 3) RGB."""
-    c = np.ascontiguousarray(np.atleast_2d(ctx), dtype=np.float64)
+    (n, 6) = (s, t, Px, Py, Pz, footprint), or (n, 13) = (s, t, P, N,
+    footprint, dst_major, dst_minor); returns (n, 3) RGB."""
+    c = np.atleast_2d(np.asarray(ctx, dtype=np.float64))
+    if c.shape[1] == 6:
+        c = np.hstack([c[:, :5], np.tile([0.0, 0.0, 1.0], (len(c), 1)), c[:, 5:6], np.zeros((len(c), 4))])
+    c = np.ascontiguousarray(c)
     out = np.empty((len(c), 3))
     d = scene.desc()
     lib().oracle_pattern_eval(C.addressof(d), int(node), len(c), c.ctypes.data, out.ctypes.data)
+    return out
+
+
+def texture_sample(rgb, queries, wrap=0, ewa=False):
+    """texture/cache.rs lookups on the mip chain of `rgb` ((H, W, 3)):
+    queries (n, 3) = (s, t, footprint) for `sample`, or (n, 6) = (s, t,
+    du, dv) for `sample_ewa` (ewa=True); returns (n, 3) f32."""
+    t = np.ascontiguousarray(rgb, dtype=np.float32)
+    q = np.atleast_2d(np.asarray(queries, dtype=np.float64))
+    full = np.zeros((len(q), 7))
+    full[:, :q.shape[1]] = q
+    full[:, 6] = 1.0 if ewa else 0.0
+    full = np.ascontiguousarray(full)
+    out = np.empty((len(q), 3), np.float32)
+    lib().oracle_texture_sample(t.shape[1], t.shape[0], t.ctypes.data, int(wrap), len(q), full.ctypes.data,
+                                out.ctypes.data)
     return out
 
 

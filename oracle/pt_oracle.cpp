@@ -453,6 +453,24 @@ struct Mesh {
         return normalize(cross(vertex(i1) - v0, vertex(i2) - v0));
     }
 
+    // mesh.rs:147-173 local gradients of s and t within the triangle's
+    // plane (dual basis of its edges); false without st or when degenerate.
+    bool st_gradients(uint32_t tri, V3* gs, V3* gt) const {
+        if (st.empty()) return false;
+        uint32_t i0 = idx[3 * tri], i1 = idx[3 * tri + 1], i2 = idx[3 * tri + 2];
+        V3 p0 = vertex(i0);
+        V3 e1 = vertex(i1) - p0, e2 = vertex(i2) - p0;
+        double ds1 = (double)(st[2 * i1] - st[2 * i0]), dt1 = (double)(st[2 * i1 + 1] - st[2 * i0 + 1]);
+        double ds2 = (double)(st[2 * i2] - st[2 * i0]), dt2 = (double)(st[2 * i2 + 1] - st[2 * i0 + 1]);
+        V3 n = cross(e1, e2);
+        double n2 = length_sq(n);
+        if (n2 < 1e-24) return false;
+        V3 dual1 = cross(e2, n) / n2, dual2 = cross(e1, n) / -n2;
+        *gs = dual1 * ds1 + dual2 * ds2;
+        *gt = dual1 * dt1 + dual2 * dt2;
+        return true;
+    }
+
     // mesh.rs:177-197 interpolated st and st density (sqrt of st area over
     // local geometric area); false without st.
     bool st_at(uint32_t tri, double u, double v, double st_out[2], double* density) const {
@@ -485,6 +503,7 @@ struct Hit {
     bool front_face;
     double st[2] = {0.0, 0.0};
     double st_density = 0.0;  // st units per world unit (0 without st)
+    V3 st_grad[2] = {{0, 0, 0}, {0, 0, 0}};  // world-space gradients of s and t
 };
 
 // ---- patterns (src/texture/pattern.rs, src/geometry/displace.rs) -------------
@@ -546,21 +565,191 @@ struct PatNode {
     std::vector<double> ramp_pos;
     std::vector<V3> ramp_col;
     bool use_t;
+    int32_t texture;  // texture / triplanar: index, -1 = missing
+    int wrap;
 };
-struct ShadeCtx {  // pattern.rs:69-82 (no file textures: st, P and footprint)
+struct ShadeCtx {  // pattern.rs:69-82
     double st[2];
-    V3 p;
+    V3 p, n;
     double footprint;
+    double dst_major[2], dst_minor[2];
+};
+
+// A file texture as the reference's cache serves it (texture/cache.rs,
+// texture/tex.rs): the box mip chain down to 1x1 (f32 2x2 averages, odd
+// sizes clamping the second tap), texels read with wrap, bilinear,
+// trilinear and EWA lookups. Sums are f32 where the reference's are.
+struct Texture {
+    struct Mip {
+        uint32_t w, h;
+        std::vector<float> rgb;
+    };
+    std::vector<Mip> mips;
+
+    void build(const float* rgb, uint32_t w, uint32_t h) {  // tex.rs:89-130
+        mips.clear();
+        mips.push_back({w, h, std::vector<float>(rgb, rgb + 3ull * w * h)});
+        while (mips.back().w > 1 || mips.back().h > 1) {
+            const Mip& a = mips.back();
+            Mip b{std::max(a.w / 2, 1u), std::max(a.h / 2, 1u), {}};
+            b.rgb.resize(3ull * b.w * b.h);
+            for (uint32_t y = 0; y < b.h; y++) {
+                uint32_t y0 = std::min(2 * y, a.h - 1), y1 = std::min(2 * y + 1, a.h - 1);
+                for (uint32_t x = 0; x < b.w; x++) {
+                    uint32_t x0 = std::min(2 * x, a.w - 1), x1 = std::min(2 * x + 1, a.w - 1);
+                    for (int c = 0; c < 3; c++) {
+                        float sum = a.rgb[3 * ((size_t)y0 * a.w + x0) + c] + a.rgb[3 * ((size_t)y0 * a.w + x1) + c];
+                        sum = sum + a.rgb[3 * ((size_t)y1 * a.w + x0) + c];
+                        sum = sum + a.rgb[3 * ((size_t)y1 * a.w + x1) + c];
+                        b.rgb[3 * ((size_t)y * b.w + x) + c] = sum * 0.25f;
+                    }
+                }
+            }
+            mips.push_back(std::move(b));
+        }
+    }
+    // cache.rs:186-203
+    void texel(size_t mip, int64_t x, int64_t y, int wrap, float out[3]) const {
+        const Mip& m = mips[mip];
+        const int64_t w = m.w, h = m.h;
+        if (wrap == RT_WRAP_PERIODIC) {
+            x = ((x % w) + w) % w;
+            y = ((y % h) + h) % h;
+        } else if (wrap == RT_WRAP_CLAMP) {
+            x = std::min(std::max(x, (int64_t)0), w - 1);
+            y = std::min(std::max(y, (int64_t)0), h - 1);
+        } else if (x < 0 || x >= w || y < 0 || y >= h) {
+            out[0] = out[1] = out[2] = 0.0f;
+            return;
+        }
+        for (int c = 0; c < 3; c++) out[c] = m.rgb[3 * ((size_t)y * m.w + (size_t)x) + c];
+    }
+    // cache.rs:205-229
+    void bilinear(size_t mip, double s, double t, int wrap, float out[3]) const {
+        const Mip& m = mips[mip];
+        double fx = s * m.w - 0.5, fy = t * m.h - 0.5;
+        double x0 = std::floor(fx), y0 = std::floor(fy);
+        double ax = fx - x0, ay = fy - y0;
+        const int64_t ix = (int64_t)x0, iy = (int64_t)y0;
+        out[0] = out[1] = out[2] = 0.0f;
+        const int64_t dx[4] = {0, 1, 0, 1}, dy[4] = {0, 0, 1, 1};
+        const double wt[4] = {(1.0 - ax) * (1.0 - ay), ax * (1.0 - ay), (1.0 - ax) * ay, ax * ay};
+        for (int k = 0; k < 4; k++) {
+            float px[3];
+            texel(mip, ix + dx[k], iy + dy[k], wrap, px);
+            for (int c = 0; c < 3; c++) out[c] += px[c] * (float)wt[k];
+        }
+    }
+    // cache.rs:230-252
+    void sample(double s, double t, double footprint, int wrap, float out[3]) const {
+        const double base = std::max(mips[0].w, mips[0].h);
+        const double texels = std::fmax(footprint * base, 1e-9);
+        const double mip_f = std::min(std::max(std::log2(texels), 0.0), (double)(mips.size() - 1));
+        const size_t m0 = (size_t)std::floor(mip_f), m1 = std::min(m0 + 1, mips.size() - 1);
+        const double a = mip_f - (double)m0;
+        bilinear(m0, s, t, wrap, out);
+        if (a < 1e-6 || m1 == m0) return;
+        float hi[3];
+        bilinear(m1, s, t, wrap, hi);
+        for (int c = 0; c < 3; c++) out[c] = out[c] * (float)(1.0 - a) + hi[c] * (float)a;
+    }
+    // cache.rs:283-377 (Heckbert's EWA with a Gaussian falloff)
+    void sample_ewa(double s, double t, const double du[2], const double dv[2], int wrap, float out[3]) const {
+        double major = std::sqrt(du[0] * du[0] + du[1] * du[1]), minor = std::sqrt(dv[0] * dv[0] + dv[1] * dv[1]);
+        const double *axm = du, *axn = dv;
+        if (minor > major) {
+            std::swap(major, minor);
+            std::swap(axm, axn);
+        }
+        if (major <= 1e-9) return sample(s, t, 0.0, wrap, out);
+        if (minor < major / 16.0) minor = major / 16.0;
+        const double base = std::max(mips[0].w, mips[0].h);
+        const double level = std::min(std::max(std::log2(std::fmax(minor * base, 1e-9)), 0.0), (double)(mips.size() - 1));
+        const size_t mip = (size_t)std::floor(level);
+        const double mw = mips[mip].w, mh = mips[mip].h;
+        const double px = s * mw - 0.5, py = t * mh - 0.5;
+        const double dux = axm[0] * mw, duy = axm[1] * mh, dvx = axn[0] * mw, dvy = axn[1] * mh;
+        double a = duy * duy + dvy * dvy + 1.0, b = -2.0 * (dux * duy + dvx * dvy), c = dux * dux + dvx * dvx + 1.0;
+        const double f = a * c - 0.25 * b * b;
+        if (f <= 1e-12) return sample(s, t, minor, wrap, out);
+        a /= f;
+        b /= f;
+        c /= f;
+        const double det = -b * b + 4.0 * a * c;
+        if (det <= 0.0) return sample(s, t, minor, wrap, out);
+        const double ur = std::sqrt(4.0 * c * det) / det, vr = std::sqrt(4.0 * a * det) / det;
+        const int64_t x0 = (int64_t)std::floor(px - ur), x1 = (int64_t)std::ceil(px + ur);
+        const int64_t y0 = (int64_t)std::floor(py - vr), y1 = (int64_t)std::ceil(py + vr);
+        if ((x1 - x0) * (y1 - y0) > 4096) return sample(s, t, minor, wrap, out);
+        float sum[3] = {0, 0, 0}, wsum = 0.0f;
+        for (int64_t y = y0; y <= y1; y++) {
+            const double ddy = (double)y - py;
+            for (int64_t x = x0; x <= x1; x++) {
+                const double ddx = (double)x - px;
+                const double r2 = a * ddx * ddx + b * ddx * ddy + c * ddy * ddy;
+                if (r2 < 1.0) {
+                    const float w = (float)std::exp(-2.0 * r2);
+                    float p3[3];
+                    texel(mip, x, y, wrap, p3);
+                    for (int k = 0; k < 3; k++) sum[k] += p3[k] * w;
+                    wsum += w;
+                }
+            }
+        }
+        if (wsum <= 1e-9f) return sample(s, t, minor, wrap, out);
+        for (int k = 0; k < 3; k++) out[k] = sum[k] / wsum;
+    }
 };
 static const V3 MISSING_COLOR{1.0, 0.0, 1.0};
 
 // pattern.rs:126-226 eval_at.
-static V3 pattern_eval(const std::vector<PatNode>& nodes, int64_t index, const ShadeCtx& c, uint32_t depth) {
+// pattern.rs:93-124: a texture lookup with t flipped into image rows; a
+// missing texture reads magenta.
+static V3 sample_tex(const std::vector<Texture>& tex, int32_t id, int wrap, double s, double t, double footprint) {
+    if (id < 0 || (size_t)id >= tex.size()) return MISSING_COLOR;
+    float c[3];
+    tex[(size_t)id].sample(s, 1.0 - t, footprint, wrap, c);
+    return {c[0], c[1], c[2]};
+}
+static V3 sample_tex_ewa(const std::vector<Texture>& tex, int32_t id, int wrap, double s, double t, const double du[2],
+                         const double dv[2]) {
+    if (id < 0 || (size_t)id >= tex.size()) return MISSING_COLOR;
+    const double u[2] = {du[0], -du[1]}, v[2] = {dv[0], -dv[1]};
+    float c[3];
+    tex[(size_t)id].sample_ewa(s, 1.0 - t, u, v, wrap, c);
+    return {c[0], c[1], c[2]};
+}
+
+static V3 pattern_eval(const std::vector<PatNode>& nodes, const std::vector<Texture>& tex, int64_t index,
+                       const ShadeCtx& c, uint32_t depth) {
     if (depth > 16) return MISSING_COLOR;
     if (index < 0 || (size_t)index >= nodes.size()) return MISSING_COLOR;
     const PatNode& n = nodes[(size_t)index];
-    auto input = [&](int k) { return n.in[k].node < 0 ? n.in[k].value : pattern_eval(nodes, n.in[k].node, c, depth + 1); };
+    auto input = [&](int k) {
+        return n.in[k].node < 0 ? n.in[k].value : pattern_eval(nodes, tex, n.in[k].node, c, depth + 1);
+    };
     switch (n.type) {
+        case RT_PATTERN_TEXTURE: {  // pattern.rs:134-149
+            const double s = c.st[0] * n.scale[0], t = c.st[1] * n.scale[1];
+            const double aniso = std::fabs(c.dst_major[0]) + std::fabs(c.dst_major[1]) + std::fabs(c.dst_minor[0]) +
+                                 std::fabs(c.dst_minor[1]);
+            if (aniso > 1e-12) {
+                const double du[2] = {c.dst_major[0] * n.scale[0], c.dst_major[1] * n.scale[1]};
+                const double dv[2] = {c.dst_minor[0] * n.scale[0], c.dst_minor[1] * n.scale[1]};
+                return sample_tex_ewa(tex, n.texture, n.wrap, s, t, du, dv);
+            }
+            return sample_tex(tex, n.texture, n.wrap, s, t,
+                              c.footprint * std::fmax(std::fabs(n.scale[0]), std::fabs(n.scale[1])));
+        }
+        case RT_PATTERN_TRIPLANAR: {  // pattern.rs:200-214
+            const V3 a{std::fabs(c.n.x), std::fabs(c.n.y), std::fabs(c.n.z)};
+            const double total = std::fmax(a.x + a.y + a.z, 1e-9);
+            const double f = n.frequency;
+            const V3 cx = sample_tex(tex, n.texture, n.wrap, c.p.y * f, c.p.z * f, c.footprint);
+            const V3 cy = sample_tex(tex, n.texture, n.wrap, c.p.z * f, c.p.x * f, c.footprint);
+            const V3 cz = sample_tex(tex, n.texture, n.wrap, c.p.x * f, c.p.y * f, c.footprint);
+            return cx * (a.x / total) + cy * (a.y / total) + cz * (a.z / total);
+        }
         case RT_PATTERN_CHECKER: {
             double fs = c.st[0] * n.scale[0], ft = c.st[1] * n.scale[1];
             int64_t cell = (int64_t)(std::floor(fs) + std::floor(ft));
@@ -1276,15 +1465,31 @@ struct Scene {
     bool any_presence = false;
     std::vector<PatNode> patterns;
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> bindings;  // per material: (field, node)
+    std::vector<Texture> textures;
 
-    // shade_params (pt/mod.rs:389-439) without file textures: the material
-    // with its pattern outputs substituted, footprint = cone width x st density.
-    Pbr shade_params(const Hit& h, double cone_width) const {
+    // shade_params (pt/mod.rs:389-439): the material with its pattern
+    // outputs substituted; footprint = cone width x st density, and the ray
+    // cone's ellipse on the surface carried into st by the st gradients.
+    Pbr shade_params(const Hit& h, V3 ray_dir, double cone_width) const {
         const Pbr& base = materials[h.material_id];
         if (h.material_id >= bindings.size() || bindings[h.material_id].empty()) return base;
+        ShadeCtx c{{h.st[0], h.st[1]}, h.point, h.normal, cone_width * h.st_density, {0, 0}, {0, 0}};
+        const V3 gs = h.st_grad[0], gt = h.st_grad[1];
+        if (length_sq(gs) + length_sq(gt) > 1e-18 && cone_width > 0.0) {
+            const V3 n = h.normal, d = normalize(ray_dir);
+            const double cs = std::fmax(std::fabs(dot(d, n)), 1.0 / 16.0);
+            V3 t1 = d - n * dot(d, n);
+            if (length_sq(t1) < 1e-12) t1 = std::fabs(n.x) < 0.9 ? cross(V3{1, 0, 0}, n) : cross(V3{0, 1, 0}, n);
+            t1 = normalize(t1) * (cone_width / cs);
+            const V3 t2 = normalize(cross(n, t1)) * cone_width;
+            c.dst_major[0] = dot(gs, t1);
+            c.dst_major[1] = dot(gt, t1);
+            c.dst_minor[0] = dot(gs, t2);
+            c.dst_minor[1] = dot(gt, t2);
+        }
         Pbr p = base;
-        ShadeCtx c{{h.st[0], h.st[1]}, h.point, cone_width * h.st_density};
-        for (const auto& b : bindings[h.material_id]) p.apply(b.first, pattern_eval(patterns, b.second, c, 0));
+        for (const auto& b : bindings[h.material_id])
+            p.apply(b.first, pattern_eval(patterns, textures, b.second, c, 0));
         return p;
     }
 
@@ -1342,6 +1547,11 @@ struct Scene {
         // mesh.rs:357-360: st and its density, transferred to world scale.
         double dens;
         if (m.st_at(best.tri, best.u, best.v, out->st, &dens)) out->st_density = dens / in.scale;
+        V3 gs, gt;  // mesh.rs:361-371: gradients pulled back through the inverse
+        if (m.st_gradients(best.tri, &gs, &gt)) {
+            out->st_grad[0] = xf_normal(in.inv, gs);
+            out->st_grad[1] = xf_normal(in.inv, gt);
+        }
         return true;
     }
 
@@ -1425,7 +1635,7 @@ struct Tracer {
             Ray r = make_ray(origin, dir);
             if (!sc.intersect(r, &h, &cshadow)) return vis;
             if (h.t >= remaining) return vis;
-            double presence = std::min(std::max(sc.shade_params(h, 0.0).presence, 0.0), 1.0);
+            double presence = std::min(std::max(sc.shade_params(h, dir, 0.0).presence, 0.0), 1.0);
             if (presence >= 1.0) return {0, 0, 0};
             vis = vis * (1.0 - presence);
             if (max_comp(vis) < 1e-4) return {0, 0, 0};
@@ -1620,7 +1830,7 @@ struct Tracer {
             V3 wo = -normalize(ray.d);
             cone_width += hit.t * cone_spread;
             travel += hit.t;
-            const Pbr pbr = sc.shade_params(hit, cone_width);
+            const Pbr pbr = sc.shade_params(hit, ray.d, cone_width);
             if (!aux_set) {
                 aux_set = true;
                 V3 a = pbr.diffuse_color * pbr.diffuse_gain + pbr.specular_f0() * (pbr.has_specular() ? 1.0 : 0.0) +
@@ -1698,6 +1908,11 @@ struct Tracer {
 
 using namespace orc;
 
+static void load_textures(const rt_scene_desc* d, std::vector<Texture>& out) {
+    out.resize(d->textures ? d->n_textures : 0);
+    for (size_t i = 0; i < out.size(); i++) out[i].build(d->textures[i].rgb, d->textures[i].width, d->textures[i].height);
+}
+
 static void load_patterns(const rt_scene_desc* d, std::vector<PatNode>& out) {
     for (uint32_t i = 0; i < d->n_patterns && d->patterns; i++) {
         const rt_pattern_desc& pd = d->patterns[i];
@@ -1719,6 +1934,8 @@ static void load_patterns(const rt_scene_desc* d, std::vector<PatNode>& out) {
             n.ramp_col.push_back(v3(pd.ramp_colors + 3 * r));
         }
         n.use_t = pd.use_t != 0;
+        n.texture = pd.texture;
+        n.wrap = (int)pd.wrap;
         out.push_back(n);
     }
 }
@@ -1814,6 +2031,7 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
         if (d->materials[i].presence < 1.0) s.any_presence = true;
     }
     load_patterns(d, s.patterns);
+    load_textures(d, s.textures);
     s.bindings.resize(d->n_materials);
     for (uint32_t i = 0; i < d->n_bindings && d->bindings; i++) {
         const rt_pattern_binding& b = d->bindings[i];
@@ -2076,11 +2294,13 @@ void oracle_env_sample(uint32_t w, uint32_t h, const float* rgb, uint64_t n, con
 
 void oracle_pattern_eval(const rt_scene_desc* d, uint32_t node, uint64_t n, const double* ctx, double* rgb) {
     std::vector<PatNode> nodes;
+    std::vector<Texture> tex;
     load_patterns(d, nodes);
+    load_textures(d, tex);
     for (uint64_t i = 0; i < n; i++) {
-        const double* c = ctx + 6 * i;
-        ShadeCtx sc{{c[0], c[1]}, V3{c[2], c[3], c[4]}, c[5]};
-        V3 v = pattern_eval(nodes, node, sc, 0);
+        const double* c = ctx + 13 * i;
+        ShadeCtx sc{{c[0], c[1]}, V3{c[2], c[3], c[4]}, V3{c[5], c[6], c[7]}, c[8], {c[9], c[10]}, {c[11], c[12]}};
+        V3 v = pattern_eval(nodes, tex, node, sc, 0);
         rgb[3 * i] = v.x;
         rgb[3 * i + 1] = v.y;
         rgb[3 * i + 2] = v.z;
@@ -2096,6 +2316,21 @@ void oracle_intersect_st(const oracle_scene* os, uint64_t n, const double* rays,
         out[4 * i + 1] = hit ? h.st[0] : 0.0;
         out[4 * i + 2] = hit ? h.st[1] : 0.0;
         out[4 * i + 3] = hit ? h.st_density : 0.0;
+    }
+}
+
+void oracle_texture_sample(uint32_t w, uint32_t h, const float* rgb, int wrap, uint64_t n, const double* q,
+                           float* out) {
+    Texture t;
+    t.build(rgb, w, h);
+    for (uint64_t i = 0; i < n; i++) {
+        const double* c = q + 7 * i;
+        if (c[6] != 0.0) {
+            const double du[2] = {c[2], c[3]}, dv[2] = {c[4], c[5]};
+            t.sample_ewa(c[0], c[1], du, dv, wrap, out + 3 * i);
+        } else {
+            t.sample(c[0], c[1], c[2], wrap, out + 3 * i);
+        }
     }
 }
 

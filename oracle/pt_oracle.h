@@ -85,10 +85,16 @@ void   oracle_env_eval_pdf(uint32_t w, uint32_t h, const float* rgb, uint64_t n,
 void   oracle_env_sample(uint32_t w, uint32_t h, const float* rgb, uint64_t n, const double* uv, double* dirs,
                          double* rad, double* pdf);
 // pattern.rs:126-226: node `node` of d's pattern graph at n shading points,
-// ctx = (s, t, Px, Py, Pz, footprint) per point; rgb = 3 per point.
+// ctx = (s, t, P xyz, N xyz, footprint, dst_major st, dst_minor st) per
+// point (13 doubles); rgb = 3 per point.
 void   oracle_pattern_eval(const rt_scene_desc* d, uint32_t node, uint64_t n, const double* ctx, double* rgb);
 // Closest hit of n rays (o, d: 6 doubles each): (t or -1, s, t, st density).
 void   oracle_intersect_st(const oracle_scene* s, uint64_t n, const double* rays, double* out);
+// texture/cache.rs lookups on the mip chain of one w x h RGB texture: per
+// query 7 doubles (s, t, footprint, -, -, -, 0) for the trilinear `sample`
+// or (s, t, du s, du t, dv s, dv t, 1) for `sample_ewa`; 3 floats out.
+void   oracle_texture_sample(uint32_t w, uint32_t h, const float* rgb, int wrap, uint64_t n, const double* q,
+                             float* out);
 // camera.rs:36-61: one pixel-filter offset per uniform.
 void   oracle_filter_sample(int filter, double width, uint64_t n, const double* u, double* out);
 

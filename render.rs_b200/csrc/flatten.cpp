@@ -689,9 +689,50 @@ uint32_t lbvh_build(std::vector<LightNode>& nodes, std::vector<uint32_t>& leaf_o
 // pattern evaluation inside shadow-ray traversal and are refused.
 bool flatten_patterns(const rt_scene_desc* d, HostScene& H, std::string* err) {
     if (!d->n_patterns && !d->n_bindings) return true;
-    if ((d->n_patterns && !d->patterns) || (d->n_bindings && !d->bindings)) {
-        *err = "patterns or bindings pointer is NULL";
+    if ((d->n_patterns && !d->patterns) || (d->n_bindings && !d->bindings) || (d->n_textures && !d->textures)) {
+        *err = "patterns, bindings or textures pointer is NULL";
         return false;
+    }
+    // Texture mip chains (texture/tex.rs:89-130): 2x2 f32 box averages,
+    // odd sizes clamping the second tap, down to 1x1.
+    for (uint32_t k = 0; k < d->n_textures; k++) {
+        const rt_texture_desc& td = d->textures[k];
+        if (!td.rgb || !td.width || !td.height) {
+            *err = "texture " + std::to_string(k) + " has no pixels";
+            return false;
+        }
+        DevTexture t{(uint32_t)H.tex_mips.size(), 0, (float)std::max(td.width, td.height), 0};
+        std::vector<float> cur(td.rgb, td.rgb + 3ull * td.width * td.height), next;
+        uint32_t w = td.width, h = td.height;
+        for (;;) {
+            if (H.texels.size() + (size_t)w * h >= (1ull << 32)) {
+                *err = "textures hold more than 2^32 texels";
+                return false;
+            }
+            H.tex_mips.push_back(DevMip{(uint32_t)H.texels.size(), w, h, 0});
+            for (size_t p = 0; p < (size_t)w * h; p++)
+                H.texels.push_back(make_float4(cur[3 * p], cur[3 * p + 1], cur[3 * p + 2], 0.0f));
+            t.n_mips++;
+            if (w == 1 && h == 1) break;
+            const uint32_t nw = std::max(w / 2, 1u), nh = std::max(h / 2, 1u);
+            next.assign(3ull * nw * nh, 0.0f);
+            for (uint32_t y = 0; y < nh; y++) {
+                const uint32_t y0 = std::min(2 * y, h - 1), y1 = std::min(2 * y + 1, h - 1);
+                for (uint32_t x = 0; x < nw; x++) {
+                    const uint32_t x0 = std::min(2 * x, w - 1), x1 = std::min(2 * x + 1, w - 1);
+                    for (int c = 0; c < 3; c++) {
+                        float sum = cur[3 * ((size_t)y0 * w + x0) + c] + cur[3 * ((size_t)y0 * w + x1) + c];
+                        sum = sum + cur[3 * ((size_t)y1 * w + x0) + c];
+                        sum = sum + cur[3 * ((size_t)y1 * w + x1) + c];
+                        next[3 * ((size_t)y * nw + x) + c] = sum * 0.25f;
+                    }
+                }
+            }
+            cur.swap(next);
+            w = nw;
+            h = nh;
+        }
+        H.textures.push_back(t);
     }
     const uint32_t np = d->n_patterns;
     H.patterns.resize(np);
@@ -699,7 +740,7 @@ bool flatten_patterns(const rt_scene_desc* d, HostScene& H, std::string* err) {
         const rt_pattern_desc& pd = d->patterns[i];
         DevPattern& g = H.patterns[i];
         memset(&g, 0, sizeof(g));
-        if (pd.type < RT_PATTERN_CHECKER || pd.type > RT_PATTERN_RAMP) {
+        if (pd.type < RT_PATTERN_CHECKER || pd.type > RT_PATTERN_TRIPLANAR) {
             *err = "pattern node " + std::to_string(i) + " has an unknown type";
             return false;
         }
@@ -743,6 +784,23 @@ bool flatten_patterns(const rt_scene_desc* d, HostScene& H, std::string* err) {
                 }
                 g.s0 = (float)pd.gamma;
                 g.s1 = (float)pd.saturation;
+                break;
+            case RT_PATTERN_TEXTURE:
+            case RT_PATTERN_TRIPLANAR:
+                // A texture index outside the table is the reference's
+                // missing texture (magenta), as is -1.
+                g.u0 = (pd.texture >= 0 && (uint32_t)pd.texture < d->n_textures) ? (uint32_t)pd.texture : 0xFFFFFFFFu;
+                if (pd.wrap > RT_WRAP_BLACK) {
+                    *err = "pattern node " + std::to_string(i) + " has an unknown wrap mode";
+                    return false;
+                }
+                g.u1 = pd.wrap;
+                if (pd.type == RT_PATTERN_TEXTURE) {
+                    g.s0 = (float)pd.scale[0];
+                    g.s1 = (float)pd.scale[1];
+                } else {
+                    g.s0 = (float)pd.frequency;
+                }
                 break;
             case RT_PATTERN_RAMP:
                 if (pd.n_ramp && (!pd.ramp_positions || !pd.ramp_colors)) {

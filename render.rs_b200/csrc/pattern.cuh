@@ -59,10 +59,128 @@ __device__ __forceinline__ float perlin(float px, float py, float pz) {
 
 __device__ __forceinline__ float lum3(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
 
+// st at a hit: coordinates, density (st units per world unit) and the
+// world-space gradients of s and t.
+struct HitSt {
+    float s, t, dens;
+    float3 gs, gt;
+};
+
+// ---- file textures (src/texture/cache.rs) -------------------------------------------
+// One texel of a mip level with the wrap mode applied (cache.rs:186-203).
+__device__ __forceinline__ float3 tex_texel(const DevScene& S, const DevMip& m, int64_t x, int64_t y, uint32_t wrap) {
+    const int64_t w = m.w, h = m.h;
+    if (wrap == RT_WRAP_PERIODIC) {
+        x = ((x % w) + w) % w;
+        y = ((y % h) + h) % h;
+    } else if (wrap == RT_WRAP_CLAMP) {
+        x = x < 0 ? 0 : (x >= w ? w - 1 : x);
+        y = y < 0 ? 0 : (y >= h ? h - 1 : y);
+    } else if (x < 0 || x >= w || y < 0 || y >= h) {
+        return f3(0.0f, 0.0f, 0.0f);
+    }
+    const float4 v = __ldg(S.texels + m.offset + (size_t)y * m.w + (size_t)x);
+    return f3(v.x, v.y, v.z);
+}
+
+// Bilinear lookup at (s, t), t = 0 at the top row (cache.rs:205-229).
+__device__ __forceinline__ float3 tex_bilinear(const DevScene& S, const DevMip& m, float s, float t, uint32_t wrap) {
+    const float fx = s * (float)m.w - 0.5f, fy = t * (float)m.h - 0.5f;
+    const float x0 = floorf(fx), y0 = floorf(fy);
+    const float ax = fx - x0, ay = fy - y0;
+    const int64_t ix = (int64_t)x0, iy = (int64_t)y0;
+    return tex_texel(S, m, ix, iy, wrap) * ((1.0f - ax) * (1.0f - ay)) +
+           tex_texel(S, m, ix + 1, iy, wrap) * (ax * (1.0f - ay)) +
+           tex_texel(S, m, ix, iy + 1, wrap) * ((1.0f - ax) * ay) + tex_texel(S, m, ix + 1, iy + 1, wrap) * (ax * ay);
+}
+
+// Trilinear lookup with the mip chosen by the footprint's diameter in st
+// units (cache.rs:230-252).
+__device__ __forceinline__ float3 tex_sample(const DevScene& S, const DevTexture& T, float s, float t, float footprint,
+                                             uint32_t wrap) {
+    const float texels = fmaxf(footprint * T.base, 1e-9f);
+    const float mip_f = fminf(fmaxf(log2f(texels), 0.0f), (float)(T.n_mips - 1));
+    const uint32_t m0 = (uint32_t)floorf(mip_f), m1 = min(m0 + 1, T.n_mips - 1);
+    const float a = mip_f - (float)m0;
+    const float3 lo = tex_bilinear(S, S.tex_mips[T.first_mip + m0], s, t, wrap);
+    if (a < 1e-6f || m1 == m0) return lo;
+    return lo * (1.0f - a) + tex_bilinear(S, S.tex_mips[T.first_mip + m1], s, t, wrap) * a;
+}
+
+// Elliptical weighted average along the footprint axes du (major) and dv
+// (minor) in st units (cache.rs:283-377): the mip from the minor axis
+// (anisotropy capped at 16), Gaussian weights exp(-2 r^2) over the
+// ellipse's texels (at most 4096 of them, else trilinear).
+__device__ __forceinline__ float3 tex_sample_ewa(const DevScene& S, const DevTexture& T, float s, float t, float2 du,
+                                                 float2 dv, uint32_t wrap) {
+    float major = sqrtf(du.x * du.x + du.y * du.y), minor = sqrtf(dv.x * dv.x + dv.y * dv.y);
+    float2 am = du, an = dv;
+    if (minor > major) {
+        const float tmp = major;
+        major = minor;
+        minor = tmp;
+        am = dv;
+        an = du;
+    }
+    if (major <= 1e-9f) return tex_sample(S, T, s, t, 0.0f, wrap);
+    if (minor < major / 16.0f) minor = major / 16.0f;
+    const float level = fminf(fmaxf(log2f(fmaxf(minor * T.base, 1e-9f)), 0.0f), (float)(T.n_mips - 1));
+    const DevMip m = S.tex_mips[T.first_mip + (uint32_t)floorf(level)];
+    const float mw = (float)m.w, mh = (float)m.h;
+    const float px = s * mw - 0.5f, py = t * mh - 0.5f;
+    const float dux = am.x * mw, duy = am.y * mh, dvx = an.x * mw, dvy = an.y * mh;
+    float a = duy * duy + dvy * dvy + 1.0f, b = -2.0f * (dux * duy + dvx * dvy), c = dux * dux + dvx * dvx + 1.0f;
+    const float f = a * c - 0.25f * b * b;
+    if (f <= 1e-12f) return tex_sample(S, T, s, t, minor, wrap);
+    a /= f;
+    b /= f;
+    c /= f;
+    const float det = -b * b + 4.0f * a * c;
+    if (det <= 0.0f) return tex_sample(S, T, s, t, minor, wrap);
+    const float ur = sqrtf(4.0f * c * det) / det, vr = sqrtf(4.0f * a * det) / det;
+    const int64_t x0 = (int64_t)floorf(px - ur), x1 = (int64_t)ceilf(px + ur);
+    const int64_t y0 = (int64_t)floorf(py - vr), y1 = (int64_t)ceilf(py + vr);
+    if ((x1 - x0) * (y1 - y0) > 4096) return tex_sample(S, T, s, t, minor, wrap);
+    float3 sum = f3(0.0f, 0.0f, 0.0f);
+    float wsum = 0.0f;
+    for (int64_t y = y0; y <= y1; y++) {
+        const float ddy = (float)y - py;
+        for (int64_t x = x0; x <= x1; x++) {
+            const float ddx = (float)x - px;
+            const float r2 = a * ddx * ddx + b * ddx * ddy + c * ddy * ddy;
+            if (r2 < 1.0f) {
+                const float w = expf(-2.0f * r2);
+                sum = sum + tex_texel(S, m, x, y, wrap) * w;
+                wsum += w;
+            }
+        }
+    }
+    if (wsum <= 1e-9f) return tex_sample(S, T, s, t, minor, wrap);
+    return sum / wsum;
+}
+
+// pattern.rs:93-124: lookups with t flipped into image rows; a missing
+// texture (~0) reads magenta.
+__device__ __forceinline__ float3 sample_tex(const DevScene& S, uint32_t tex, uint32_t wrap, float s, float t,
+                                             float footprint) {
+    if (tex == 0xFFFFFFFFu) return f3(1.0f, 0.0f, 1.0f);
+    return tex_sample(S, S.textures[tex], s, 1.0f - t, footprint, wrap);
+}
+
+// Everything a node reads at a shading point (pattern.rs:69-82).
+struct PatCtx {
+    float s, t;
+    float3 p, n;
+    float footprint;
+    float2 dst_major, dst_minor;
+};
+
 // One node at a shading point; `v` holds the outputs of nodes node_lo.. so
 // far, `lo` is node_lo.
 __device__ __forceinline__ float3 pattern_node(const DevScene& S, const DevPattern& g, const float3* v, uint32_t lo,
-                                               float s, float t, float3 p, float footprint) {
+                                               const PatCtx& cx) {
+    const float s = cx.s, t = cx.t, footprint = cx.footprint;
+    const float3 p = cx.p;
     auto input = [&](int k) {
         return g.in[k] == 0xFFFFFFFFu ? f3(g.c[k][0], g.c[k][1], g.c[k][2]) : v[g.in[k] - lo];
     };
@@ -116,6 +234,26 @@ __device__ __forceinline__ float3 pattern_node(const DevScene& S, const DevPatte
                 prev = cur;
             }
             return f3(prev.y, prev.z, prev.w);
+        }
+        case RT_PATTERN_TEXTURE: {  // pattern.rs:134-149
+            const float ts = s * g.s0, tt = t * g.s1;
+            const float aniso =
+                fabsf(cx.dst_major.x) + fabsf(cx.dst_major.y) + fabsf(cx.dst_minor.x) + fabsf(cx.dst_minor.y);
+            if (aniso > 1e-12f) {
+                if (g.u0 == 0xFFFFFFFFu) return f3(1.0f, 0.0f, 1.0f);
+                const float2 du = make_float2(cx.dst_major.x * g.s0, -(cx.dst_major.y * g.s1));
+                const float2 dv = make_float2(cx.dst_minor.x * g.s0, -(cx.dst_minor.y * g.s1));
+                return tex_sample_ewa(S, S.textures[g.u0], ts, 1.0f - tt, du, dv, g.u1);
+            }
+            return sample_tex(S, g.u0, g.u1, ts, tt, footprint * fmaxf(fabsf(g.s0), fabsf(g.s1)));
+        }
+        case RT_PATTERN_TRIPLANAR: {  // pattern.rs:200-214
+            const float3 an = f3(fabsf(cx.n.x), fabsf(cx.n.y), fabsf(cx.n.z));
+            const float total = fmaxf(an.x + an.y + an.z, 1e-9f);
+            const float f = g.s0;
+            return sample_tex(S, g.u0, g.u1, p.y * f, p.z * f, footprint) * (an.x / total) +
+                   sample_tex(S, g.u0, g.u1, p.z * f, p.x * f, footprint) * (an.y / total) +
+                   sample_tex(S, g.u0, g.u1, p.x * f, p.y * f, footprint) * (an.z / total);
         }
         default: return f3(1.0f, 0.0f, 1.0f);
     }
@@ -200,18 +338,32 @@ __device__ __forceinline__ void fold_pbr(const DevPbr& q, DevMaterial& d) {
     }
 }
 
-// Material `mat` at a shading point: base parameters with every bound
-// pattern output substituted in binding order, folded into `d` (which
-// must hold the material's plain record on entry). Kept out of line: only
-// patterned hits call it, and inlined its node table and fold would raise
-// the shade kernel's register count for every scene (128 -> 192).
-__device__ __noinline__ void resolve_material(const DevScene& S, const DevMatPat& mp, float s, float t, float3 p,
-                                                 float footprint, DevMaterial& d) {
+// A patterned material at a shading point (shade_params, pt/mod.rs:389-439):
+// the footprint is the cone width times the st density, and the cone's
+// ellipse on the surface (minor axis the cone width, major stretched by
+// 1/|cos| along the projected ray) is carried into st by the gradients;
+// base parameters with every bound pattern output substituted in binding
+// order are folded into `d` (which holds the material's plain record on
+// entry). Kept out of line: only patterned hits call it, and inlined its
+// node table and fold would raise the shade kernel's register count.
+__device__ __noinline__ void resolve_material(const DevScene& S, const DevMatPat& mp, const HitSt& hs, float3 p,
+                                              float3 n, float3 dir, float cone_width, DevMaterial& d) {
+    PatCtx cx{hs.s, hs.t, p, n, cone_width * hs.dens, make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+    if (dot(hs.gs, hs.gs) + dot(hs.gt, hs.gt) > 1e-18f && cone_width > 0.0f) {
+        const float3 dn = normalize_ref(dir);
+        const float cs = fmaxf(fabsf(dot(dn, n)), 1.0f / 16.0f);
+        float3 t1 = dn - n * dot(dn, n);
+        if (dot(t1, t1) < 1e-12f) t1 = fabsf(n.x) < 0.9f ? cross(f3(1.0f, 0.0f, 0.0f), n) : cross(f3(0.0f, 1.0f, 0.0f), n);
+        t1 = normalize_ref(t1) * (cone_width / cs);
+        const float3 t2 = normalize_ref(cross(n, t1)) * cone_width;
+        cx.dst_major = make_float2(dot(hs.gs, t1), dot(hs.gt, t1));
+        cx.dst_minor = make_float2(dot(hs.gs, t2), dot(hs.gt, t2));
+    }
     float3 v[RT_MAX_PATTERN_NODES];
     for (uint32_t k = 0; k < RT_MAX_PATTERN_NODES; k++) {
         if (!((mp.node_mask >> k) & 1u)) continue;
         const DevPattern g = S.patterns[mp.node_lo + k];
-        v[k] = pattern_node(S, g, v, mp.node_lo, s, t, p, footprint);
+        v[k] = pattern_node(S, g, v, mp.node_lo, cx);
     }
     DevPbr q = S.pbr[mp.pbr_index];
     for (uint32_t b = 0; b < mp.bind_n; b++) {

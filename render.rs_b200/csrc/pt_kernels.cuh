@@ -167,28 +167,49 @@ __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3
     g.mat = info.z;
 }
 
-// (s, t) and st density (st units per world unit) at a closest hit:
-// Mesh::st_at (src/geometry/mesh.rs:177-197) with the density carried to
-// world scale by the instance's approx_scale (mesh.rs:357-360); zeros when
-// the mesh has no st.
-__device__ __forceinline__ float3 hit_st(const DevScene& S, uint4 hr) {
+// (s, t), st density (st units per world unit) and the world-space st
+// gradients at a closest hit: Mesh::st_at and st_gradients
+// (src/geometry/mesh.rs:147-197) with the density carried to world scale
+// by the instance's approx_scale and the gradients pulled back through the
+// world-to-object transform (mesh.rs:357-371); zeros when the mesh has no st.
+__device__ __forceinline__ HitSt hit_st(const DevScene& S, uint4 hr, float3 p) {
+    HitSt r{0.0f, 0.0f, 0.0f, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f)};
     const uint4 info = __ldg(S.inst + hr.z);
     const MeshInfo mi = S.meshes[info.w];
-    if (!(mi.attrs & MESH_ST)) return f3(0.0f, 0.0f, 0.0f);
+    if (!(mi.attrs & MESH_ST)) return r;
     const float4* tp = S.tris + 3 * (size_t)hr.y;
     const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
-    const float b1 = __half2float(__ushort_as_half((unsigned short)(hr.w & 0xFFFFu)));
-    const float b2 = __half2float(__ushort_as_half((unsigned short)(hr.w >> 16)));
+    const float4 x0 = __ldg(S.inst_xf + 3 * (size_t)hr.z), x1 = __ldg(S.inst_xf + 3 * (size_t)hr.z + 1),
+                 x2 = __ldg(S.inst_xf + 3 * (size_t)hr.z + 2);
+    const float3 e1 = xyz(v1) - xyz(v0), e2 = xyz(v2) - xyz(v0);
+    const float3 nl = cross(e1, e2);
+    const float n2 = dot(nl, nl);
+    // Barycentrics of the hit point in f32 (the hit record's are half
+    // precision, ~1e-3 of the triangle: too coarse for texture lookups).
+    float b1 = __half2float(__ushort_as_half((unsigned short)(hr.w & 0xFFFFu)));
+    float b2 = __half2float(__ushort_as_half((unsigned short)(hr.w >> 16)));
+    if (n2 > 0.0f) {
+        const float3 q = f3(dot(xyz(x0), p) + x0.w, dot(xyz(x1), p) + x1.w, dot(xyz(x2), p) + x2.w) - xyz(v0);
+        b1 = dot(cross(q, e2), nl) / n2;
+        b2 = dot(cross(e1, q), nl) / n2;
+    }
     const uint32_t* ix = S.orig_idx + mi.idx_base + 3 * (size_t)__float_as_uint(v0.w);
     const float2* st = reinterpret_cast<const float2*>(S.st);
     const float2 s0 = st[ix[0]], s1 = st[ix[1]], s2 = st[ix[2]];
     const float w = 1.0f - b1 - b2;
-    const float s = s0.x * w + s1.x * b1 + s2.x * b2;
-    const float t = s0.y * w + s1.y * b1 + s2.y * b2;
+    r.s = s0.x * w + s1.x * b1 + s2.x * b2;
+    r.t = s0.y * w + s1.y * b1 + s2.y * b2;
     const float st_area = 0.5f * fabsf((s1.x - s0.x) * (s2.y - s0.y) - (s2.x - s0.x) * (s1.y - s0.y));
-    const float geo_area = 0.5f * length(cross(xyz(v1) - xyz(v0), xyz(v2) - xyz(v0)));
-    const float dens = geo_area > 1e-18f ? sqrtf(st_area / geo_area) : 0.0f;
-    return f3(s, t, dens / __ldg(S.inst_scale + info.y));
+    const float geo_area = 0.5f * length(nl);
+    r.dens = (geo_area > 1e-18f ? sqrtf(st_area / geo_area) : 0.0f) / __ldg(S.inst_scale + info.y);
+    if (n2 >= 1e-24f) {
+        const float3 d1 = cross(e2, nl) / n2, d2 = cross(e1, nl) / -n2;
+        const float3 gs = d1 * (s1.x - s0.x) + d2 * (s2.x - s0.x);
+        const float3 gt = d1 * (s1.y - s0.y) + d2 * (s2.y - s0.y);
+        r.gs = xf_normal(x0, x1, x2, gs);
+        r.gt = xf_normal(x0, x1, x2, gt);
+    }
+    return r;
 }
 
 // ---- raygen: camera rays for all P slots ------------------------------------------
@@ -847,9 +868,9 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                     cone.x += eucl * cone.y;
                     const DevMatPat mp = S.mat_pat[hg.mat];
                     if (mp.bind_n) {
-                        const float3 stv = hit_st(S, hr);
+                        const HitSt hs = hit_st(S, hr, p);
                         mres = *mptr;
-                        resolve_material(S, mp, stv.x, stv.y, p, cone.x * stv.z, mres);
+                        resolve_material(S, mp, hs, p, nw, d, cone.x, mres);
                         mptr = &mres;
                     }
                 }

@@ -147,6 +147,18 @@ struct DevMatPat {
 static_assert(sizeof(DevMatPat) == 32, "DevMatPat layout");
 #define RT_MAX_PATTERN_NODES 16
 
+// File textures: every mip level of every texture, RGB texels as float4
+// (w = 0) row-major from the top row, concatenated in `texels`.
+struct DevTexture {
+    uint32_t first_mip, n_mips;
+    float base;              // max(width, height) of the base level
+    uint32_t pad_;
+};
+struct DevMip {
+    uint32_t offset, w, h, pad_;  // first texel in `texels`, size
+};
+static_assert(sizeof(DevTexture) == 16 && sizeof(DevMip) == 16, "texture table layout");
+
 // ---- everything a kernel needs to read the scene ------------------------------
 struct DevScene {
     const uint4* nodes;
@@ -165,6 +177,9 @@ struct DevScene {
     const DevMatPat* mat_pat;    // per material
     const uint2* binds;          // (field, node)
     const DevPbr* pbr;
+    const DevTexture* textures;  // file textures (null when none)
+    const DevMip* tex_mips;
+    const float4* texels;
     const DevMaterial* materials;
     const DevLight* lights;
     const LightNode* lbvh;

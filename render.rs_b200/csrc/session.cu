@@ -263,6 +263,11 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
         rc = rc ? rc : s->upload(&S.mat_pat, H.mat_pat);
         rc = rc ? rc : s->upload(&S.binds, H.binds);
         rc = rc ? rc : s->upload(&S.pbr, H.pbr);
+        if (!H.textures.empty()) {
+            rc = rc ? rc : s->upload(&S.textures, H.textures);
+            rc = rc ? rc : s->upload(&S.tex_mips, H.tex_mips);
+            rc = rc ? rc : s->upload(&S.texels, H.texels);
+        }
     }
     rc = rc ? rc : s->upload(&S.materials, H.materials);
     rc = rc ? rc : s->upload(&S.lights, H.lights);

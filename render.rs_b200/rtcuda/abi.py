@@ -82,7 +82,14 @@ class RtCameraDesc(C.Structure):
     ]
 
 
-PATTERN_CHECKER, PATTERN_FRACTAL, PATTERN_MIX, PATTERN_COLOR_CORRECT, PATTERN_RAMP = range(5)
+(PATTERN_CHECKER, PATTERN_FRACTAL, PATTERN_MIX, PATTERN_COLOR_CORRECT, PATTERN_RAMP, PATTERN_TEXTURE,
+ PATTERN_TRIPLANAR) = range(7)
+WRAP_PERIODIC, WRAP_CLAMP, WRAP_BLACK = range(3)
+WRAP_MODES = {"periodic": WRAP_PERIODIC, "clamp": WRAP_CLAMP, "black": WRAP_BLACK}
+
+
+class RtTextureDesc(C.Structure):
+    _fields_ = [("rgb", C.POINTER(C.c_float)), ("width", C.c_uint32), ("height", C.c_uint32)]
 
 # BoundField (src/texture/pattern.rs:238-254), by the RIB parameter names
 # (BoundField::from_param, pattern.rs:258-275).
@@ -115,6 +122,8 @@ class RtPatternDesc(C.Structure):
         ("ramp_colors", C.POINTER(C.c_double)),
         ("n_ramp", C.c_uint32),
         ("use_t", C.c_uint32),
+        ("texture", C.c_int32),
+        ("wrap", C.c_uint32),
     ]
 
 
@@ -143,6 +152,9 @@ class RtSceneDesc(C.Structure):
         ("bindings", C.POINTER(RtPatternBinding)),
         ("n_patterns", C.c_uint32),
         ("n_bindings", C.c_uint32),
+        ("textures", C.POINTER(RtTextureDesc)),
+        ("n_textures", C.c_uint32),
+        ("tex_reserved", C.c_uint32),
     ]
 
 
@@ -167,8 +179,8 @@ LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK, LIGHT_DOME = r
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
 for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 264), (RtLightDesc, 120),
-               (RtCameraDesc, 144), (RtParams, 64), (RtPatternInput, 32), (RtPatternDesc, 232),
-               (RtPatternBinding, 16), (RtSceneDesc, 264)):
+               (RtCameraDesc, 144), (RtParams, 64), (RtPatternInput, 32), (RtPatternDesc, 240),
+               (RtPatternBinding, 16), (RtTextureDesc, 16), (RtSceneDesc, 280)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
 

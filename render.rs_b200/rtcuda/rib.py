@@ -24,9 +24,12 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     displacement, media and motion blur are skipped (motion blocks use
     their first sample); a PxrDomeLight lightColorMap is read when it is a
     Radiance .hdr (one map per scene).
-  * Pattern graphs: PxrChecker, PxrFractal, PxrMix, PxrColorCorrect and
-    PxrRamp nodes and Bxdf "reference" connections are carried; file
-    textures (PxrTexture, triplanar) and presence connections are skipped.
+  * Pattern graphs: PxrChecker, PxrFractal, PxrMix, PxrColorCorrect,
+    PxrRamp, PxrTexture and triplanar nodes and Bxdf "reference"
+    connections are carried; texture files are read when they are .tex,
+    Radiance .hdr or PNG (others render magenta, as the reference's
+    unreadable files do); UDIM tile sets and presence connections are
+    skipped.
     Tessellated spheres and cylinders carry the reference's st; the other
     quadrics have none.
 """
@@ -587,6 +590,8 @@ class _Builder:
         self.patterns = []                # Scene pattern node dicts
         self.pattern_handles = {}         # handle -> node index
         self.bindings = []                # (material, field id, node)
+        self.textures = []                # (H, W, 3) f32 linear RGB
+        self.texture_ids = {}             # file path -> texture index (-1: unreadable)
 
     # -- helpers ------------------------------------------------------------------
     def warn(self, msg):
@@ -1035,14 +1040,36 @@ class _Builder:
             node = dict(type=abi.PATTERN_RAMP,
                         ramp=(np.array(pos[:n], np.float64), np.array(col[:3 * n], np.float64).reshape(-1, 3)),
                         use_t=prm.string("axis") == "t")
-        elif ptype in ("PxrTexture", "texture", "triplanar"):
-            self.warn(f'Pattern "{ptype}": file textures are not rendered on this path; skipping')
-            return
+        elif ptype in ("PxrTexture", "texture"):
+            node = dict(type=abi.PATTERN_TEXTURE, texture=self.open_texture(prm.string("filename") or ""),
+                        wrap=abi.WRAP_MODES.get(prm.string("wrapMode") or "periodic", abi.WRAP_PERIODIC),
+                        scale=(number("scaleS", 1.0), number("scaleT", 1.0)))
+        elif ptype == "triplanar":
+            node = dict(type=abi.PATTERN_TRIPLANAR, texture=self.open_texture(prm.string("filename") or ""),
+                        wrap=abi.WRAP_MODES.get(prm.string("wrapMode") or "periodic", abi.WRAP_PERIODIC),
+                        frequency=number("frequency", 1.0))
         else:
             self.warn(f'Pattern "{ptype}" not implemented; skipping')
             return
         self.pattern_handles[handle] = len(self.patterns)
         self.patterns.append(node)
+
+    def open_texture(self, name):
+        """A texture file (beside the scene) as a texture index; one that
+        cannot be read is the reference's missing texture (-1, magenta)."""
+        if not name:
+            self.warn("Pattern texture without \"filename\"; rendering magenta")
+            return -1
+        path = name if os.path.isabs(name) or self.base_dir is None else os.path.join(self.base_dir, name)
+        if path not in self.texture_ids:
+            from .textures import TextureError, load_texture
+            try:
+                self.textures.append(load_texture(path))
+                self.texture_ids[path] = len(self.textures) - 1
+            except (OSError, TextureError, ValueError) as e:
+                self.warn(f"texture {name}: {e}; rendering magenta")
+                self.texture_ids[path] = -1
+        return self.texture_ids[path]
 
     def bxdf_bindings(self, prm):
         """The Bxdf's "reference <type> <param>" ["handle:output"]
@@ -1156,6 +1183,7 @@ class _Builder:
             s.add_mesh(P, I, N, st=self.mesh_st.get(k))
         s.patterns = [dict(n) for n in self.patterns]
         s.bindings = list(self.bindings)
+        s.textures = list(self.textures)
         for m in self.materials:
             s.add_material(m)
         for l in self.lights:

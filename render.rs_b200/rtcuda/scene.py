@@ -118,6 +118,7 @@ class Scene:
         self.mesh_st = {}         # mesh id -> (n, 2) f32 texture coordinates
         self.patterns = []        # pattern nodes (dicts, see add_pattern)
         self.bindings = []        # (material, field id, node)
+        self.textures = []        # (H, W, 3) f32 linear RGB base images
         # Reference default camera: origin, looking down +z (camera.rs:97-103).
         self.eye = np.zeros(3)
         self.forward = np.array([0.0, 0.0, 1.0])
@@ -179,6 +180,28 @@ class Scene:
         if len(pos) != len(col):
             raise ValueError("ramp needs one colour per position")
         return self._pattern(type=abi.PATTERN_RAMP, ramp=(pos, col), use_t=bool(use_t))
+
+    def add_texture(self, rgb):
+        """A file texture's base image ((H, W, 3) linear RGB, row 0 at the
+        top); returns its index for add_texture_node / add_triplanar."""
+        a = np.ascontiguousarray(rgb, dtype=np.float32)
+        if a.ndim != 3 or a.shape[2] != 3 or a.shape[0] < 1 or a.shape[1] < 1:
+            raise ValueError("texture must be (H, W, 3)")
+        self.textures.append(a)
+        self._desc = None
+        return len(self.textures) - 1
+
+    def add_texture_node(self, texture, wrap="periodic", scale=(1.0, 1.0)):
+        """PxrTexture: the texture at (s, t) * scale, t up (texture row 0 at
+        t = 1); `texture` -1 is a missing file (magenta)."""
+        return self._pattern(type=abi.PATTERN_TEXTURE, texture=int(texture), wrap=abi.WRAP_MODES[wrap],
+                             scale=tuple(float(v) for v in scale))
+
+    def add_triplanar(self, texture, wrap="periodic", frequency=1.0):
+        """Triplanar projection of a texture over world P * frequency,
+        blended by the normal's axis weights."""
+        return self._pattern(type=abi.PATTERN_TRIPLANAR, texture=int(texture), wrap=abi.WRAP_MODES[wrap],
+                             frequency=float(frequency))
 
     def bind_pattern(self, material, field, node):
         """Material::pattern_bindings: `node`'s output replaces PbrParams
@@ -358,6 +381,8 @@ class Scene:
                 pd.ramp_colors = col.ctypes.data_as(C.POINTER(C.c_double))
                 pd.n_ramp = len(pos)
                 pd.use_t = int(node["use_t"])
+            pd.texture = node.get("texture", -1)
+            pd.wrap = node.get("wrap", 0)
         bind_arr = (abi.RtPatternBinding * max(1, len(self.bindings)))()
         for k, (m, f, n) in enumerate(self.bindings):
             bind_arr[k].material, bind_arr[k].field, bind_arr[k].node = m, f, n
@@ -367,6 +392,14 @@ class Scene:
         if self.bindings:
             d.bindings = bind_arr
             d.n_bindings = len(self.bindings)
+        tex_arr = (abi.RtTextureDesc * max(1, len(self.textures)))()
+        for k, t in enumerate(self.textures):
+            keep.append(t)
+            tex_arr[k].rgb = t.ctypes.data_as(C.POINTER(C.c_float))
+            tex_arr[k].height, tex_arr[k].width = t.shape[0], t.shape[1]
+        if self.textures:
+            d.textures = tex_arr
+            d.n_textures = len(self.textures)
         self._desc = d
-        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr)
+        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr, tex_arr)
         return d

@@ -58,3 +58,51 @@ def test_footprint_filters_a_sub_pixel_checker_to_its_mean():
     fine, flat = _render(_fine_checker_plane(True), p, 16), _render(_fine_checker_plane(False), p, 16)
     assert flat.mean() > 0.05
     np.testing.assert_allclose(fine, flat, rtol=1e-4, atol=1e-5)
+
+
+def _textured_scene(w=64, h=48, bind=True):
+    """A floor with an st-mapped texture (the EWA path: mesh st and a ray
+    cone) and a block with a triplanar projection of the same texture."""
+    s = scene.Scene(w, h, fov=45.0)
+    s.look_at((0.0, 1.3, -2.6), (0.0, 0.2, 1.0))
+    x, y = np.meshgrid(np.arange(64), np.arange(64))
+    cells = ((x // 8 + y // 8) % 2).astype(np.float32)
+    img = np.stack([0.15 + 0.7 * cells, 0.2 + 0.6 * x / 63.0, 0.8 - 0.6 * y / 63.0], -1).astype(np.float32)
+    t = s.add_texture(img)
+    floor_m = s.add_material(scene.matte((0.5, 0.5, 0.5)))
+    block_m = s.add_material(scene.ggx_floor((0.5, 0.5, 0.5), 0.4))
+    if bind:
+        s.bind_pattern(floor_m, "diffuseColor", s.add_texture_node(t, scale=(3.0, 3.0)))
+        s.bind_pattern(block_m, "diffuseColor", s.add_triplanar(t, wrap="periodic", frequency=1.5))
+    plane = s.add_mesh([[-3, 0, -2], [3, 0, -2], [3, 0, 4], [-3, 0, 4]], [[0, 2, 1], [0, 3, 2]],
+                       st=[[0, 0], [1, 0], [1, 1], [0, 1]])
+    s.add_instance(plane, floor_m)
+    from rtcuda.scenes import unit_cube
+    cp, ci = unit_cube()
+    s.add_instance(s.add_mesh(cp, ci), block_m, scene.affine(scene.rot_y(30) * 0.6, (0.5, 0.3, 1.2)))
+    s.add_distant_light((0.4, -1.0, 0.3), 2.5)
+    s.add_point_light((-1.0, 2.0, 0.0), 3.0)
+    return s
+
+
+def test_textures_match_oracle():
+    w, h, spp = 64, 48, 256
+    p = abi.make_params(max_depth=5, aovs=True)
+    s = _textured_scene(w, h)
+    with PtSession(s, p) as g:
+        g.render_samples(0, spp)
+        gpu, gaux = g.image(), g.aux()
+    rgb, aux, _ = oracle.OracleScene(s).render(p, 0, spp, aovs=True)
+    cpu, caux = rgb.reshape(h, w, 3) / spp, aux.reshape(h, w, 12)
+    # First-hit albedo: the texture lookups themselves (no transport noise;
+    # only sub-pixel positions differ between the two samplers).
+    ga, ca = gaux[..., 0:3] / spp, caux[..., 0:3] / spp
+    assert np.abs(ga - ca).mean() < 0.004, np.abs(ga - ca).mean()
+    assert np.abs(ga - ca).max() < 0.08, np.abs(ga - ca).max()
+    flat = _textured_scene(w, h, bind=False)
+    fa = oracle.OracleScene(flat).render(p, 0, 16, aovs=True)[1].reshape(h, w, 12)[..., 0:3] / 16
+    assert np.abs(fa - ca).mean() > 10 * np.abs(ga - ca).mean()
+    np.testing.assert_allclose(gpu.mean((0, 1)), cpu.mean((0, 1)), rtol=0.03)
+    for axis in (0, 1):
+        a, b = gpu.mean(axis).mean(-1), cpu.mean(axis).mean(-1)
+        assert np.all(np.abs(a - b) <= 0.08 * b + 0.015), (axis, np.abs(a - b).max())

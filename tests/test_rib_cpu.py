@@ -327,14 +327,17 @@ def test_pattern_requests_and_connections():
           "reference color specularFaceColor" ["tex:resultRGB"] "reference float bogus" ["n:resultF"]
         Polygon "P" [0 0 1  1 0 1  1 1 1]''')
     kinds = [n["type"] for n in s.patterns]
-    assert kinds == [abi.PATTERN_FRACTAL, abi.PATTERN_COLOR_CORRECT, abi.PATTERN_RAMP, abi.PATTERN_CHECKER]
+    assert kinds == [abi.PATTERN_FRACTAL, abi.PATTERN_COLOR_CORRECT, abi.PATTERN_RAMP, abi.PATTERN_TEXTURE,
+                     abi.PATTERN_CHECKER]
     assert s.patterns[0]["octaves"] == 3 and s.patterns[0]["gain"] == 0.4
     assert s.patterns[1]["inputs"] == (0,) and s.patterns[1]["gamma"] == 2.0
     assert s.patterns[2]["use_t"] and list(s.patterns[2]["ramp"][0]) == [0.0, 0.5, 1.0]
-    assert s.patterns[3]["scale"] == (8.0, 8.0) and s.patterns[3]["color_a"] == (1.0, 1.0, 1.0)
-    assert [b[1:] for b in s.bindings] == [(abi.PATTERN_FIELDS["diffuseColor"], 1)]
+    assert s.patterns[3]["texture"] == -1  # wood.tex cannot be read: magenta
+    assert s.patterns[4]["scale"] == (8.0, 8.0) and s.patterns[4]["color_a"] == (1.0, 1.0, 1.0)
+    assert [b[1:] for b in s.bindings] == [(abi.PATTERN_FIELDS["diffuseColor"], 1),
+                                           (abi.PATTERN_FIELDS["specularFaceColor"], 3)]
     w = " | ".join(s.warnings)
-    assert "file textures" in w and "presence" in w and "unknown Pattern \"tex\"" in w and "bogus" in w
+    assert "wood.tex" in w and "presence" in w and "bogus" in w
 
 
 def test_st_primvar_and_quadric_st():

@@ -1,0 +1,144 @@
+"""File textures on the CPU: the .tex writer/reader against the reference's
+tex.rs tests (src/texture/tex.rs:253-311), the oracle's texture lookups
+against its cache tests (src/texture/cache.rs:393-477), the mip chain the
+CUDA backend builds against the writer's, PNG decoding, and PxrTexture /
+triplanar requests read from RIB."""
+import struct
+import zlib
+
+import numpy as np
+
+import oracle
+from rtcuda import abi, scene, textures
+from rtcuda.rib import load_rib_string
+
+
+def checker(w, h):
+    x, y = np.arange(w)[None, :], np.arange(h)[:, None]
+    v = np.where((x // 8 + y // 8) % 2 == 0, 1.0, 0.25).astype(np.float32)
+    return np.stack([v, v * np.float32(0.5), np.full_like(v, 0.1)], -1)
+
+
+def gradient(w, h):
+    x, y = np.arange(w)[None, :] / (w - 1), np.arange(h)[:, None] / (h - 1)
+    return np.stack(np.broadcast_arrays(x, y, 0.5), -1).astype(np.float32)
+
+
+def test_tex_round_trip_and_mips(tmp_path):
+    img = checker(70, 50)
+    path = tmp_path / "a.tex"
+    textures.write_tex(path, img)
+    data = path.read_bytes()
+    w, h, mips = textures.read_tex_header(data)
+    assert (w, h) == (70, 50)
+    assert [m[:2] for m in mips] == [(70, 50), (35, 25), (17, 12), (8, 6), (4, 3), (2, 1), (1, 1)]
+    assert mips[0][2:4] == (3, 2)
+    assert textures.read_tex_tile(data, 0, 1, 0)[20, 40 - 32, 0] == img[20, 40, 0]
+    top = textures.read_tex_tile(data, len(mips) - 1, 0, 0)[0, 0, 0]
+    assert 0.25 < top < 1.0
+    np.testing.assert_array_equal(textures.read_tex(path), img)
+
+
+def test_edge_tiles_replicate(tmp_path):
+    img = checker(40, 40)
+    path = tmp_path / "e.tex"
+    textures.write_tex(path, img)
+    assert textures.read_tex_tile(path.read_bytes(), 0, 1, 1)[20, 20, 0] == img[39, 39, 0]
+
+
+def test_sample_center_and_wrap():
+    img = gradient(128, 128)
+    c = oracle.texture_sample(img, [[0.5, 0.5, 0.0]])[0]
+    assert abs(c[0] - 0.5) < 0.02 and abs(c[1] - 0.5) < 0.02
+    assert oracle.texture_sample(img, [[1.02, 0.5, 0.0]])[0][0] < 0.1
+    assert np.all(oracle.texture_sample(img, [[1.5, 0.5, 0.0]], wrap=abi.WRAP_BLACK)[0] == 0.0)
+    top = oracle.texture_sample(img, [[0.25, 0.75, 10.0]])[0]
+    assert abs(top[0] - 0.5) < 0.05 and abs(top[2] - 0.5) < 0.01
+
+
+def test_ewa_preserves_detail_across_anisotropy():
+    x = np.arange(256)
+    v = np.where((x // 8) % 2 == 0, 1.0, 0.0).astype(np.float32)
+    img = np.repeat(np.repeat(v[None, :, None], 256, 0), 3, 2)
+    du, dv = (0.0, 64.0 / 256.0), (1.0 / 256.0, 0.0)
+    on, off = oracle.texture_sample(img, [[4.5 / 256, 0.5, *du, *dv], [12.5 / 256, 0.5, *du, *dv]], ewa=True)
+    assert abs(on[0] - off[0]) > 0.5
+    on_t, off_t = oracle.texture_sample(img, [[4.5 / 256, 0.5, 64.0 / 256], [12.5 / 256, 0.5, 64.0 / 256]])
+    assert abs(on_t[0] - off_t[0]) < 0.2
+
+
+def test_oracle_mip_chain_matches_the_tex_writer():
+    img = checker(70, 50) * np.float32(0.7) + gradient(70, 50) * np.float32(0.3)
+    chain = textures.mip_chain(img)
+    for level in (1, 3):
+        m = chain[level]
+        h, w = m.shape[:2]
+        base = 70.0
+        ys, xs = np.meshgrid(np.arange(h), np.arange(w), indexing="ij")
+        q = np.stack([(xs.ravel() + 0.5) / w, (ys.ravel() + 0.5) / h, np.full(xs.size, 2.0 ** level / base)], -1)
+        got = oracle.texture_sample(img, q, wrap=abi.WRAP_CLAMP)
+        np.testing.assert_allclose(got, m.reshape(-1, 3), rtol=0, atol=2e-7)
+    last = oracle.texture_sample(img, [[0.3, 0.6, 1e3]])[0]  # four bilinear taps of the 1x1 level
+    np.testing.assert_allclose(last, chain[-1][0, 0], rtol=0, atol=2e-7)
+
+
+def _png(a, ftype=0):
+    h, w, _ = a.shape
+    rows = []
+    for y in range(h):
+        line = a[y].reshape(-1).astype(np.int32)
+        if ftype == 1:
+            f = line.copy()
+            f[3:] = (line[3:] - line[:-3]) & 0xFF
+        else:
+            f = line
+        rows.append(bytes([ftype]) + f.astype(np.uint8).tobytes())
+
+    def chunk(k, b):
+        return struct.pack(">I", len(b)) + k + b + struct.pack(">I", zlib.crc32(k + b) & 0xFFFFFFFF)
+    return (b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0)) +
+            chunk(b"IDAT", zlib.compress(b"".join(rows))) + chunk(b"IEND", b""))
+
+
+def test_png_decode_and_srgb():
+    a = np.random.default_rng(3).integers(0, 256, (6, 9, 3)).astype(np.uint8)
+    for ftype in (0, 1):
+        np.testing.assert_allclose(textures.decode_png(_png(a, ftype)), a / 255.0, atol=1e-7)
+    lin = textures.srgb_to_linear(np.array([0.0, 0.04045, 0.5, 1.0], np.float32))
+    np.testing.assert_allclose(lin, [0.0, 0.04045 / 12.92, ((0.5 + 0.055) / 1.055) ** 2.4, 1.0], rtol=1e-6)
+
+
+def test_rib_texture_nodes(tmp_path):
+    textures.write_tex(tmp_path / "wood.tex", checker(16, 16))
+    (tmp_path / "paint.png").write_bytes(_png(np.full((2, 2, 3), 255, np.uint8)))
+    s = load_rib_string('''
+        Pattern "PxrTexture" "wood" "string filename" ["wood.tex"] "string wrapMode" ["clamp"] "scaleS" [2]
+        Pattern "triplanar" "tri" "string filename" ["paint.png"] "frequency" [3]
+        Pattern "PxrTexture" "gone" "string filename" ["missing.tex"]
+        Bxdf "PxrSurface" "m" "reference color diffuseColor" ["wood:resultRGB"]
+        Polygon "P" [0 0 1  1 0 1  1 1 1]''', base_dir=str(tmp_path))
+    wood, tri, gone = s.patterns
+    assert wood["type"] == abi.PATTERN_TEXTURE and wood["wrap"] == abi.WRAP_CLAMP and wood["scale"] == (2.0, 1.0)
+    assert tri["type"] == abi.PATTERN_TRIPLANAR and tri["frequency"] == 3.0
+    assert gone["texture"] == -1 and any("missing.tex" in w for w in s.warnings)
+    assert len(s.textures) == 2
+    np.testing.assert_array_equal(s.textures[wood["texture"]], checker(16, 16))
+    np.testing.assert_allclose(s.textures[tri["texture"]], 1.0)
+    # Missing texture: magenta; a texture node reads t up (row 0 at t = 1).
+    c = oracle.pattern_eval(s, 2, [[0.5, 0.5, 0, 0, 0, 0]])[0]
+    np.testing.assert_array_equal(c, [1.0, 0.0, 1.0])
+    top_left = oracle.pattern_eval(s, 0, [[0.01, 0.99, 0, 0, 0, 0]])[0]
+    np.testing.assert_allclose(top_left, checker(16, 16)[0, 0], atol=1e-6)
+
+
+def test_texture_pattern_on_a_quad_in_the_oracle():
+    s = scene.Scene(4, 4)
+    t = s.add_texture(checker(32, 32))
+    n = s.add_texture_node(t, scale=(1.0, 1.0))
+    m = s.add_material(scene.matte((1, 1, 1)))
+    s.bind_pattern(m, "diffuseColor", n)
+    q = s.add_mesh([[0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], [[0, 1, 2], [0, 2, 3]],
+                   st=[[0, 0], [1, 0], [1, 1], [0, 1]])
+    s.add_instance(q, m)
+    ctx = [[0.2, 0.8, 0.2, 0.8, 1.0, 0, 0, -1, 0.0, 0, 0, 0, 0]]
+    np.testing.assert_allclose(oracle.pattern_eval(s, n, ctx)[0], checker(32, 32)[6, 6], atol=1e-6)
