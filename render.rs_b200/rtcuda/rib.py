@@ -30,8 +30,7 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     Radiance .hdr or PNG (others render magenta, as the reference's
     unreadable files do); UDIM tile sets and presence connections are
     skipped.
-    Tessellated spheres and cylinders carry the reference's st; the other
-    quadrics have none.
+    Tessellated quadrics carry the reference's st, hyperboloids excepted.
 """
 import math
 import os
@@ -391,15 +390,22 @@ def _segments(thetamax):
 
 
 def quadric_st(kind, a):
-    """(P, N, I, st) of a Sphere or Cylinder with the reference's st
-    (sphere.rs:86-93, cylinder.rs:100-107: s = phi / thetamax, t = (z -
-    zmin) / (zmax - zmin)), taken at the tessellation's grid vertices so
-    the seam column keeps s = 1; None for other quadrics."""
-    if kind not in ("Sphere", "Cylinder"):
+    """(P, N, I, st) of a tessellated quadric with the reference's st, taken
+    at the grid vertices so the seam column keeps s = 1: s = phi / thetamax
+    for all; t = (z - zmin) / (zmax - zmin) on spheres (sphere.rs:86-93),
+    and on cylinders, cones (z / height), disks ((radius - r) / radius),
+    tori (the tube angle over its range) and paraboloids the grid's own v
+    (cylinder.rs:100-107, cone.rs:129-134, extra.rs:276-285, 365-366,
+    462-464). None for hyperboloids, whose s starts at the azimuth of
+    their first point rather than at the grid's seam."""
+    if kind not in ("Sphere", "Cylinder", "Cone", "Disk", "Torus", "Paraboloid"):
         return None
     P, N, I, uv = tessellate(kind, a, with_uv=True)
-    zmin, zmax = a[1], a[2]
-    t = np.clip((P[:, 2].astype(np.float64) - zmin) / max(zmax - zmin, 1e-12), 0.0, 1.0)
+    if kind == "Sphere":
+        zmin, zmax = a[1], a[2]
+        t = np.clip((P[:, 2].astype(np.float64) - zmin) / max(zmax - zmin, 1e-12), 0.0, 1.0)
+    else:
+        t = uv[:, 1]
     return P, N, I, np.stack([uv[:, 0], t], -1).astype(np.float32)
 
 
@@ -431,7 +437,7 @@ def tessellate(kind, a, with_uv=False):
             th = U * math.radians(tm)
             P = np.stack([r * (1 - V) * np.cos(th), r * (1 - V) * np.sin(th), V * h], -1)
             return P, np.stack([h * np.cos(th), h * np.sin(th), np.full_like(th, r)], -1)
-        return _grid(f, _segments(tm), 1)
+        return _grid(f, _segments(tm), 1, with_uv)
     if kind == "Disk":
         h, r, tm = a
 
@@ -439,7 +445,7 @@ def tessellate(kind, a, with_uv=False):
             th = U * math.radians(tm)
             P = np.stack([r * (1 - V) * np.cos(th), r * (1 - V) * np.sin(th), np.full_like(th, h)], -1)
             return P, np.stack([np.zeros_like(th), np.zeros_like(th), np.ones_like(th)], -1)
-        return _grid(f, _segments(tm), 1)
+        return _grid(f, _segments(tm), 1, with_uv)
     if kind == "Torus":
         R, rr, pmin, pmax, tm = a
 
@@ -449,7 +455,7 @@ def tessellate(kind, a, with_uv=False):
             n = np.stack([np.cos(ph) * np.cos(th), np.cos(ph) * np.sin(th), np.sin(ph)], -1)
             P = np.stack([(R + rr * np.cos(ph)) * np.cos(th), (R + rr * np.cos(ph)) * np.sin(th), rr * np.sin(ph)], -1)
             return P, n
-        return _grid(f, _segments(tm), 32)
+        return _grid(f, _segments(tm), 32, with_uv)
     if kind == "Paraboloid":
         rmax, zmin, zmax, tm = a
         k = zmax / (rmax * rmax) if rmax != 0 else 0.0
@@ -461,7 +467,7 @@ def tessellate(kind, a, with_uv=False):
             P = np.stack([rad * np.cos(th), rad * np.sin(th), z], -1)
             N = np.stack([2 * k * P[..., 0], 2 * k * P[..., 1], -np.ones_like(z)], -1)
             return P, N
-        return _grid(f, _segments(tm), 16)
+        return _grid(f, _segments(tm), 16, with_uv)
     if kind == "Hyperboloid":
         p1, p2, tm = np.array(a[0:3]), np.array(a[3:6]), a[6]
 

@@ -343,14 +343,26 @@ def test_pattern_requests_and_connections():
 def test_st_primvar_and_quadric_st():
     s = load_rib_string('PointsPolygons [4] [0 1 2 3] "P" [0 0 1  1 0 1  1 1 1  0 1 1] "st" [0 0  1 0  1 1  0 1]\n'
                         'PointsPolygons [3] [0 1 2] "P" [0 0 1  1 0 1  1 1 1] "st" [0 0  1 0]\n'
-                        'Sphere 1 -0.5 1 180\nCylinder 1 0 2 360\nTorus 1 0.2 0 360 360')
-    assert sorted(s.mesh_st) == [0, 2, 3]  # wrong-length st ignored; the torus carries none
+                        'Sphere 1 -0.5 1 180\nCylinder 1 0 2 360\nCone 2 0.5 270\nDisk 0.3 0.8 360\n'
+                        'Torus 1 0.2 -90 180 360\nParaboloid 1 0.2 1.5 360\nHyperboloid 1 0 0  0.5 0.5 1  360')
+    # Wrong-length st is ignored; the hyperboloid carries none.
+    assert sorted(s.mesh_st) == [0, 2, 3, 4, 5, 6, 7]
     np.testing.assert_array_equal(s.mesh_st[0], [[0, 0], [1, 0], [1, 1], [0, 1]])
-    P, st = s.meshes[2][0], s.mesh_st[2]
-    # sphere.rs:86-93: s = phi / thetamax, t = (z - zmin) / (zmax - zmin).
-    phi = np.degrees(np.arctan2(P[:, 1], P[:, 0])) % 360.0
-    ring = np.hypot(P[:, 0], P[:, 1])
-    inner = (st[:, 0] > 1e-3) & (st[:, 0] < 1 - 1e-3) & (ring > 1e-3)  # phi is undefined at the pole
-    np.testing.assert_allclose(st[inner, 0], phi[inner] / 180.0, atol=1e-4)
-    np.testing.assert_allclose(st[:, 1], (P[:, 2] + 0.5) / 1.5, atol=1e-5)
-    assert st[:, 0].min() == 0.0 and st[:, 0].max() == 1.0
+
+    def check(mesh, tm, t_of, u_atol=1e-4):
+        P, st = s.meshes[mesh][0].astype(np.float64), s.mesh_st[mesh]
+        ring = np.hypot(P[:, 0], P[:, 1])
+        phi = np.degrees(np.arctan2(P[:, 1], P[:, 0])) % 360.0
+        inner = (st[:, 0] > 1e-3) & (st[:, 0] < 1 - 1e-3) & (ring > 1e-3)  # phi is undefined on the axis
+        np.testing.assert_allclose(st[inner, 0], phi[inner] / tm, atol=u_atol)
+        np.testing.assert_allclose(st[:, 1], t_of(P, ring), atol=2e-5)
+        assert st[:, 0].min() == 0.0 and st[:, 0].max() == 1.0
+
+    # sphere.rs:86-93, cylinder.rs:100-107, cone.rs:129-134, extra.rs:276-285, 365-366, 462-464.
+    check(2, 180.0, lambda P, r: (P[:, 2] + 0.5) / 1.5)
+    check(3, 360.0, lambda P, r: P[:, 2] / 2.0)
+    check(4, 270.0, lambda P, r: P[:, 2] / 2.0)
+    check(5, 360.0, lambda P, r: (0.8 - r) / 0.8)
+    # (the tube angle is taken with a 1e-3 degree margin so the start of the range does not wrap to 360)
+    check(6, 360.0, lambda P, r: ((np.degrees(np.arctan2(P[:, 2], r - 1.0)) + 90.0 + 1e-3) % 360.0 - 1e-3) / 270.0)
+    check(7, 360.0, lambda P, r: (P[:, 2] - 0.2) / 1.3)
