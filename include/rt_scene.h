@@ -183,6 +183,24 @@ typedef struct rt_pattern_binding {
     uint32_t pad_;
 } rt_pattern_binding;
 
+/* IES profile of a point light (src/scene/ies.rs, src/scene/light.rs:
+ * 44-45, 155-167): the LM-63 candela grid, already scaled by the file's
+ * candela multiplier, over ascending vertical angles (0 = the light's
+ * local -y) and horizontal angles, and the rotation taking world
+ * directions to the light's frame (the upper 3x3 of the inverse of the
+ * light's transform at declaration, row-major). The profile reshapes the
+ * light's output, normalised by its sin-weighted mean candela. */
+typedef struct rt_ies_desc {
+    uint32_t light;            /* index of the RT_LIGHT_POINT light */
+    uint32_t n_v;
+    uint32_t n_h;
+    uint32_t pad_;
+    const double* v_angles;    /* n_v, degrees */
+    const double* h_angles;    /* n_h, degrees */
+    const double* candela;     /* n_h x n_v, candela[h * n_v + v] */
+    double world_to_local[9];
+} rt_ies_desc;
+
 typedef struct rt_scene_desc {
     const rt_mesh_desc*     meshes;
     const rt_instance_desc* instances;
@@ -211,6 +229,9 @@ typedef struct rt_scene_desc {
     const rt_texture_desc*    textures;
     uint32_t n_textures;
     uint32_t tex_reserved;    /* 0 */
+    const rt_ies_desc*        ies;
+    uint32_t n_ies;
+    uint32_t ies_reserved;    /* 0 */
 } rt_scene_desc;
 
 /* Integrator knobs. The reference hard-codes these as constants
@@ -244,7 +265,8 @@ static_assert(sizeof(rt_pattern_input) == 32, "rt_pattern_input layout");
 static_assert(sizeof(rt_pattern_desc) == 240, "rt_pattern_desc layout");
 static_assert(sizeof(rt_texture_desc) == 16, "rt_texture_desc layout");
 static_assert(sizeof(rt_pattern_binding) == 16, "rt_pattern_binding layout");
-static_assert(sizeof(rt_scene_desc) == 280, "rt_scene_desc layout");
+static_assert(sizeof(rt_ies_desc) == 112, "rt_ies_desc layout");
+static_assert(sizeof(rt_scene_desc) == 296, "rt_scene_desc layout");
 }
 #endif
 

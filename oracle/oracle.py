@@ -52,6 +52,7 @@ def lib():
         L.oracle_pattern_eval.argtypes = [vp, C.c_uint32, C.c_uint64, vp, vp]
         L.oracle_intersect_st.argtypes = [vp, C.c_uint64, vp, vp]
         L.oracle_texture_sample.argtypes = [C.c_uint32, C.c_uint32, vp, C.c_int, C.c_uint64, vp, vp]
+        L.oracle_ies_eval.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp, C.c_uint64, vp, vp, vp]
         L.oracle_light_pmf.restype = C.c_double
         L.oracle_light_pmf.argtypes = [vp, f64p, C.c_uint32]
         _lib = L
@@ -238,6 +239,17 @@ def texture_sample(rgb, queries, wrap=0, ewa=False):
     lib().oracle_texture_sample(t.shape[1], t.shape[0], t.ctypes.data, int(wrap), len(q), full.ctypes.data,
                                 out.ctypes.data)
     return out
+
+
+def ies_eval(profile, dirs):
+    """ies.rs candela_toward and factor of (v_angles, h_angles, candela[h][v])
+    toward light-local directions (n, 3); returns (candela, factor)."""
+    v, h, c = (np.ascontiguousarray(a, dtype=np.float64) for a in profile)
+    d = np.ascontiguousarray(np.atleast_2d(dirs), dtype=np.float64)
+    cd, f = np.empty(len(d)), np.empty(len(d))
+    lib().oracle_ies_eval(len(v), len(h), v.ctypes.data, h.ctypes.data, c.ctypes.data, len(d), d.ctypes.data,
+                          cd.ctypes.data, f.ctypes.data)
+    return cd, f
 
 
 def filter_sample(kind, width, u):

@@ -863,13 +863,82 @@ struct EnvMap {
     }
 };
 
+// ies.rs: an LM-63 candela grid and its sin-weighted mean candela.
+struct Ies {
+    std::vector<double> v, h;   // angles in degrees, ascending
+    std::vector<double> cd;     // cd[hi * n_v + vi]
+    double average = 1.0;
+    M4 to_local;                // world -> light (upper 3x3 used)
+
+    void finish() {  // ies.rs:67-80
+        double num = 0.0, den = 0.0;
+        for (size_t vi = 0; vi < v.size(); vi++) {
+            double w = std::fmax(std::sin(v[vi] * PI / 180.0), 1e-4), mean = 0.0;
+            for (size_t hi = 0; hi < h.size(); hi++) mean += cd[hi * v.size() + vi];
+            num += mean / (double)h.size() * w;
+            den += w;
+        }
+        average = std::fmax(num / std::fmax(den, 1e-9), 1e-9);
+    }
+    static void axis(const std::vector<double>& a, double x, size_t* i0, size_t* i1, double* t) {  // ies.rs:89-106
+        *t = 0.0;
+        if (x <= a[0]) {
+            *i0 = *i1 = 0;
+            return;
+        }
+        if (x >= a.back()) {
+            *i0 = *i1 = a.size() - 1;
+            return;
+        }
+        for (size_t i = 0; i + 1 < a.size(); i++)
+            if (x <= a[i + 1]) {
+                *i0 = i;
+                *i1 = i + 1;
+                *t = (x - a[i]) / std::fmax(a[i + 1] - a[i], 1e-9);
+                return;
+            }
+        *i0 = *i1 = a.size() - 1;
+    }
+    double candela(V3 dir_local) const {  // ies.rs:108-137
+        V3 d = normalize(dir_local);
+        double theta = std::acos(std::min(std::max(-d.y, -1.0), 1.0)) * 180.0 / PI;
+        double phi = std::atan2(d.z, d.x) * 180.0 / PI;
+        if (phi < 0.0) phi += 360.0;
+        const double hmax = h.back();
+        if (hmax <= 0.0) {
+            phi = 0.0;
+        } else if (hmax <= 90.0) {
+            double q = std::fmod(phi, 180.0);
+            phi = q > 90.0 ? 180.0 - q : q;
+        } else if (hmax <= 180.0) {
+            double q = std::fmod(phi, 360.0);
+            phi = q > 180.0 ? 360.0 - q : q;
+        }
+        size_t v0, v1, h0, h1;
+        double tv, th;
+        axis(v, theta, &v0, &v1, &tv);
+        axis(h, phi, &h0, &h1, &th);
+        const size_t nv = v.size();
+        const double c00 = cd[h0 * nv + v0], c01 = cd[h0 * nv + v1], c10 = cd[h1 * nv + v0], c11 = cd[h1 * nv + v1];
+        return (c00 * (1.0 - tv) + c01 * tv) * (1.0 - th) + (c10 * (1.0 - tv) + c11 * tv) * th;
+    }
+    double factor(V3 dir_local) const { return candela(dir_local) / average; }
+};
+
 struct Light {
     int type;
     double intensity;
     V3 color, p, e1, e2, normal;
     double radius = 0, area = 0;
     std::shared_ptr<EnvMap> env;  // dome lights only
+    std::shared_ptr<Ies> ies;     // point lights only
     V3 radiance() const { return color * intensity; }  // light.rs:151-153
+    // light.rs:155-167: point lights with a profile reshape their output
+    // toward the emission direction -wi.
+    V3 radiance_toward(V3 wi) const {
+        if (!ies) return radiance();
+        return radiance() * ies->factor(xf_vec(ies->to_local, -wi));
+    }
 };
 
 struct LightNode {  // light_sampler.rs:19-31 (f32 storage, 48 B)
@@ -1702,7 +1771,7 @@ struct Tracer {
                 if (max_comp(f) <= 0.0) return {0, 0, 0};
                 V3 vis = visibility_to(p, n, l.p);
                 if (max_comp(vis) <= 0.0) return {0, 0, 0};
-                return f * l.radiance() * vis / (dist2 * pick);
+                return f * l.radiance_toward(wi) * vis / (dist2 * pick);
             }
             case RT_LIGHT_DISTANT: {
                 V3 base = -l.e1;
@@ -2041,6 +2110,19 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
         }
     }
     for (uint32_t i = 0; i < d->n_lights; i++) s.lights.push_back(make_light(d->lights[i]));
+    for (uint32_t k = 0; k < d->n_ies && d->ies; k++) {
+        const rt_ies_desc& e = d->ies[k];
+        if (e.light >= d->n_lights || !e.n_v || !e.n_h) continue;
+        auto ies = std::make_shared<Ies>();
+        ies->v.assign(e.v_angles, e.v_angles + e.n_v);
+        ies->h.assign(e.h_angles, e.h_angles + e.n_h);
+        ies->cd.assign(e.candela, e.candela + (size_t)e.n_v * e.n_h);
+        ies->to_local = identity();
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) ies->to_local.m[r][c] = e.world_to_local[3 * r + c];
+        ies->finish();
+        s.lights[e.light].ies = ies;
+    }
     if (d->env_rgb && d->env_width && d->env_height && d->env_light < d->n_lights) {
         auto env = std::make_shared<EnvMap>();
         env->w = d->env_width;
@@ -2331,6 +2413,20 @@ void oracle_texture_sample(uint32_t w, uint32_t h, const float* rgb, int wrap, u
         } else {
             t.sample(c[0], c[1], c[2], wrap, out + 3 * i);
         }
+    }
+}
+
+void oracle_ies_eval(uint32_t n_v, uint32_t n_h, const double* v, const double* h, const double* candela,
+                     uint64_t n, const double* dirs, double* cd, double* factor) {
+    Ies p;
+    p.v.assign(v, v + n_v);
+    p.h.assign(h, h + n_h);
+    p.cd.assign(candela, candela + (size_t)n_v * n_h);
+    p.finish();
+    for (uint64_t i = 0; i < n; i++) {
+        V3 d{dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]};
+        cd[i] = p.candela(d);
+        factor[i] = p.factor(d);
     }
 }
 

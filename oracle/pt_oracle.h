@@ -95,6 +95,10 @@ void   oracle_intersect_st(const oracle_scene* s, uint64_t n, const double* rays
 // or (s, t, du s, du t, dv s, dv t, 1) for `sample_ewa`; 3 floats out.
 void   oracle_texture_sample(uint32_t w, uint32_t h, const float* rgb, int wrap, uint64_t n, const double* q,
                              float* out);
+// ies.rs:108-142: raw candela and normalised factor of a profile toward n
+// light-local directions (3 doubles each).
+void   oracle_ies_eval(uint32_t n_v, uint32_t n_h, const double* v, const double* h, const double* candela,
+                       uint64_t n, const double* dirs, double* cd, double* factor);
 // camera.rs:36-61: one pixel-filter offset per uniform.
 void   oracle_filter_sample(int filter, double width, uint64_t n, const double* u, double* out);
 

@@ -1287,6 +1287,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         DevLight dl;
         memset(&dl, 0, sizeof(dl));
         dl.type = (uint32_t)ld.type;
+        dl.ies = 0xFFFFFFFFu;
         double rad[3];
         for (int k = 0; k < 3; k++) {
             rad[k] = ld.color[k] * ld.intensity;
@@ -1350,6 +1351,43 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
             default: *err = "light " + std::to_string(l) + " has an unknown type"; return false;
         }
         H.lights.push_back(dl);
+    }
+    // IES profiles of point lights (ies.rs): f32 angles and candela, the
+    // sin-weighted mean candela in f64 as ies.rs:67-80 takes it.
+    if (d->n_ies && !d->ies) {
+        *err = "ies pointer is NULL";
+        return false;
+    }
+    for (uint32_t k = 0; k < d->n_ies; k++) {
+        const rt_ies_desc& e = d->ies[k];
+        if (e.light >= d->n_lights || d->lights[e.light].type != RT_LIGHT_POINT || !e.n_v || !e.n_h ||
+            e.n_v > 4096 || e.n_h > 4096 || !e.v_angles || !e.h_angles || !e.candela) {
+            *err = "IES profile " + std::to_string(k) + " is empty or not on a point light";
+            return false;
+        }
+        if (H.lights[e.light].ies != 0xFFFFFFFFu) {
+            *err = "light " + std::to_string(e.light) + " has two IES profiles";
+            return false;
+        }
+        DevIes g;
+        memset(&g, 0, sizeof(g));
+        g.off = (uint32_t)H.ies_data.size();
+        g.n_v = e.n_v;
+        g.n_h = e.n_h;
+        double num = 0.0, den = 0.0;
+        for (uint32_t vi = 0; vi < e.n_v; vi++) {
+            double w = std::fmax(std::sin(e.v_angles[vi] * PI / 180.0), 1e-4), mean = 0.0;
+            for (uint32_t hi = 0; hi < e.n_h; hi++) mean += e.candela[(size_t)hi * e.n_v + vi];
+            num += mean / (double)e.n_h * w;
+            den += w;
+        }
+        g.average = (float)std::fmax(num / std::fmax(den, 1e-9), 1e-9);
+        for (int j = 0; j < 9; j++) g.m[j] = (float)e.world_to_local[j];
+        for (uint32_t vi = 0; vi < e.n_v; vi++) H.ies_data.push_back((float)e.v_angles[vi]);
+        for (uint32_t hi = 0; hi < e.n_h; hi++) H.ies_data.push_back((float)e.h_angles[hi]);
+        for (size_t c = 0; c < (size_t)e.n_v * e.n_h; c++) H.ies_data.push_back((float)e.candela[c]);
+        H.lights[e.light].ies = (uint32_t)H.ies.size();
+        H.ies.push_back(g);
     }
     double finite_total = 0;
     for (auto& e : finite) finite_total += e.power;

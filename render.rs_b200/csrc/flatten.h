@@ -27,6 +27,8 @@ struct HostScene {
     std::vector<DevMatPat> mat_pat;  // per material when the scene has bindings
     std::vector<uint2> binds;
     std::vector<DevPbr> pbr;
+    std::vector<DevIes> ies;
+    std::vector<float> ies_data;
     std::vector<DevTexture> textures;
     std::vector<DevMip> tex_mips;
     std::vector<float4> texels;

@@ -640,7 +640,10 @@ __device__ __forceinline__ bool nee_light(const DevScene& S, const DevLight& L, 
             float bp;
             float3 f = eval(wi, bp);
             if (maxc(f) <= 0.0f) return false;
-            out.c = f * Le / (dist2 * pick);
+            // Light::radiance_toward (light.rs:155-167): a profile reshapes
+            // the output toward the emission direction -wi.
+            const float prof = L.ies == 0xFFFFFFFFu ? 1.0f : ies_factor(S, S.ies[L.ies], -wi);
+            out.c = f * Le * prof / (dist2 * pick);
             shadow_to(lp);
             return true;
         }

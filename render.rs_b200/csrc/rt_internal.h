@@ -81,9 +81,21 @@ struct DevLight {
     float p[3], area;     // point/centre/corner; rect/disk area
     float e1[3], radius;  // rect/disk edge 1 or distant direction; sphere radius or distant angle
     float e2[3], cos_max; // rect/disk edge 2; distant cone cos
-    float n[3], pad_;     // rect/disk normal
+    float n[3];           // rect/disk normal
+    uint32_t ies;         // point light: its IES profile in DevScene::ies, ~0 for none
 };
 static_assert(sizeof(DevLight) == 80, "DevLight layout");
+
+// IES profile of a point light (src/scene/ies.rs): angles and candela
+// (f32) in DevScene::ies_data from `off`: n_v vertical angles, n_h
+// horizontal angles, then candela[h][v]; the world-to-light rotation.
+struct DevIes {
+    uint32_t off, n_v, n_h;
+    float average;       // sin-weighted mean candela
+    float m[9];          // world -> light, row-major
+    uint32_t pad_[3];
+};
+static_assert(sizeof(DevIes) == 64, "DevIes layout");
 
 // Light BVH node, byte-identical to the reference's LightBvhNode
 // (src/scene/light_sampler.rs:19-31).
@@ -177,6 +189,8 @@ struct DevScene {
     const DevMatPat* mat_pat;    // per material
     const uint2* binds;          // (field, node)
     const DevPbr* pbr;
+    const DevIes* ies;           // IES profiles (null when none)
+    const float* ies_data;
     const DevTexture* textures;  // file textures (null when none)
     const DevMip* tex_mips;
     const float4* texels;

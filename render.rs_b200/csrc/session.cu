@@ -269,6 +269,10 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
             rc = rc ? rc : s->upload(&S.texels, H.texels);
         }
     }
+    if (!H.ies.empty()) {
+        rc = rc ? rc : s->upload(&S.ies, H.ies);
+        rc = rc ? rc : s->upload(&S.ies_data, H.ies_data);
+    }
     rc = rc ? rc : s->upload(&S.materials, H.materials);
     rc = rc ? rc : s->upload(&S.lights, H.lights);
     rc = rc ? rc : s->upload(&S.lbvh, H.lbvh);

@@ -402,4 +402,61 @@ __device__ __forceinline__ float power_heuristic(float a, float b) {
     return a2 + b2 <= 0.0f ? 0.0f : a2 / (a2 + b2);
 }
 
+// ---- IES profiles (src/scene/ies.rs) -----------------------------------------------
+// interp_axis (ies.rs:89-106): bracketing angles and the blend between them.
+__device__ __forceinline__ void ies_axis(const float* a, uint32_t n, float x, uint32_t& i0, uint32_t& i1, float& t) {
+    t = 0.0f;
+    if (x <= a[0]) {
+        i0 = i1 = 0;
+        return;
+    }
+    if (x >= a[n - 1]) {
+        i0 = i1 = n - 1;
+        return;
+    }
+    for (uint32_t i = 0; i + 1 < n; i++) {
+        if (x <= a[i + 1]) {
+            i0 = i;
+            i1 = i + 1;
+            t = (x - a[i]) / fmaxf(a[i + 1] - a[i], 1e-9f);
+            return;
+        }
+    }
+    i0 = i1 = n - 1;
+}
+
+// IesProfile::factor (ies.rs:108-142): candela toward the light-local
+// emission direction (vertical angle from local -y, horizontal angle from
+// local +x toward +z, folded into the profile's symmetry range), bilinear
+// over the grid, divided by the mean candela.
+__device__ __forceinline__ float ies_factor(const DevScene& S, const DevIes& P, float3 emit_world) {
+    const float3 l = f3(P.m[0] * emit_world.x + P.m[1] * emit_world.y + P.m[2] * emit_world.z,
+                        P.m[3] * emit_world.x + P.m[4] * emit_world.y + P.m[5] * emit_world.z,
+                        P.m[6] * emit_world.x + P.m[7] * emit_world.y + P.m[8] * emit_world.z);
+    const float3 d = normalize_ref(l);
+    const float theta = acosf(fminf(fmaxf(-d.y, -1.0f), 1.0f)) * (180.0f / RT_PI);
+    float phi = atan2f(d.z, d.x) * (180.0f / RT_PI);
+    if (phi < 0.0f) phi += 360.0f;
+    const float* va = S.ies_data + P.off;
+    const float* ha = va + P.n_v;
+    const float* cd = ha + P.n_h;
+    const float hmax = ha[P.n_h - 1];
+    if (hmax <= 0.0f) {
+        phi = 0.0f;
+    } else if (hmax <= 90.0f) {
+        const float q = fmodf(phi, 180.0f);
+        phi = q > 90.0f ? 180.0f - q : q;
+    } else if (hmax <= 180.0f) {
+        const float q = fmodf(phi, 360.0f);
+        phi = q > 180.0f ? 360.0f - q : q;
+    }
+    uint32_t v0, v1, h0, h1;
+    float tv, th;
+    ies_axis(va, P.n_v, theta, v0, v1, tv);
+    ies_axis(ha, P.n_h, phi, h0, h1, th);
+    const float c00 = cd[h0 * P.n_v + v0], c01 = cd[h0 * P.n_v + v1], c10 = cd[h1 * P.n_v + v0],
+                c11 = cd[h1 * P.n_v + v1];
+    return ((c00 * (1.0f - tv) + c01 * tv) * (1.0f - th) + (c10 * (1.0f - tv) + c11 * tv) * th) / P.average;
+}
+
 }  // namespace rt

@@ -131,6 +131,14 @@ class RtPatternBinding(C.Structure):
     _fields_ = [("material", C.c_uint32), ("field", C.c_uint32), ("node", C.c_uint32), ("pad_", C.c_uint32)]
 
 
+class RtIesDesc(C.Structure):
+    _fields_ = [
+        ("light", C.c_uint32), ("n_v", C.c_uint32), ("n_h", C.c_uint32), ("pad_", C.c_uint32),
+        ("v_angles", C.POINTER(C.c_double)), ("h_angles", C.POINTER(C.c_double)),
+        ("candela", C.POINTER(C.c_double)), ("world_to_local", C.c_double * 9),
+    ]
+
+
 class RtSceneDesc(C.Structure):
     _fields_ = [
         ("meshes", C.POINTER(RtMeshDesc)),
@@ -155,6 +163,9 @@ class RtSceneDesc(C.Structure):
         ("textures", C.POINTER(RtTextureDesc)),
         ("n_textures", C.c_uint32),
         ("tex_reserved", C.c_uint32),
+        ("ies", C.POINTER(RtIesDesc)),
+        ("n_ies", C.c_uint32),
+        ("ies_reserved", C.c_uint32),
     ]
 
 
@@ -180,7 +191,7 @@ FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
 for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 264), (RtLightDesc, 120),
                (RtCameraDesc, 144), (RtParams, 64), (RtPatternInput, 32), (RtPatternDesc, 240),
-               (RtPatternBinding, 16), (RtTextureDesc, 16), (RtSceneDesc, 280)):
+               (RtPatternBinding, 16), (RtTextureDesc, 16), (RtIesDesc, 112), (RtSceneDesc, 296)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
 

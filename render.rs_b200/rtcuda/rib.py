@@ -597,6 +597,7 @@ class _Builder:
         self.pattern_handles = {}         # handle -> node index
         self.bindings = []                # (material, field id, node)
         self.textures = []                # (H, W, 3) f32 linear RGB
+        self.ies = {}                     # light index -> (v, h, candela, world_to_local)
         self.texture_ids = {}             # file path -> texture index (-1: unreadable)
 
     # -- helpers ------------------------------------------------------------------
@@ -1110,9 +1111,18 @@ class _Builder:
         if t == "pointlight":
             f = p.numbers("from")
             pos = tuple(f[:3]) if f is not None and len(f) >= 3 else (0.0, 0.0, 0.0)
-            if p.string("iesProfile") is not None:
-                self.warn("IES profiles are not rendered on this path; pointlight is isotropic")
-            self.add_light(abi.LIGHT_POINT, inten, (1.0, 1.0, 1.0), p=pos)
+            li = self.add_light(abi.LIGHT_POINT, inten, (1.0, 1.0, 1.0), p=pos)
+            f = p.string("iesProfile")
+            if f is not None:
+                # scene_builder.rs:1599-1614: oriented by the inverse of the
+                # current transform; an unreadable file leaves it isotropic.
+                from .ies import IesError, load_ies
+                path = f if os.path.isabs(f) or self.base_dir is None else os.path.join(self.base_dir, f)
+                try:
+                    prof = load_ies(path)
+                    self.ies[li] = prof + (np.linalg.inv(self.ctm)[:3, :3],)
+                except (OSError, IesError, np.linalg.LinAlgError) as e:
+                    self.warn(f"iesProfile {f}: {e}")
         elif t == "distantlight":
             f, to = p.numbers("from"), p.numbers("to")
             f = np.array(f[:3]) if f is not None and len(f) >= 3 else np.array([0.0, 0.0, -10.0])
@@ -1190,6 +1200,7 @@ class _Builder:
         s.patterns = [dict(n) for n in self.patterns]
         s.bindings = list(self.bindings)
         s.textures = list(self.textures)
+        s.ies = dict(self.ies)
         for m in self.materials:
             s.add_material(m)
         for l in self.lights:

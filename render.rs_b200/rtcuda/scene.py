@@ -119,6 +119,7 @@ class Scene:
         self.patterns = []        # pattern nodes (dicts, see add_pattern)
         self.bindings = []        # (material, field id, node)
         self.textures = []        # (H, W, 3) f32 linear RGB base images
+        self.ies = {}             # point light index -> (v_angles, h_angles, candela[h][v], world_to_local 3x3)
         # Reference default camera: origin, looking down +z (camera.rs:97-103).
         self.eye = np.zeros(3)
         self.forward = np.array([0.0, 0.0, 1.0])
@@ -246,8 +247,18 @@ class Scene:
         self._desc = None
         return len(self.lights) - 1
 
-    def add_point_light(self, position, intensity, color=(1, 1, 1)):
-        return self._light(abi.LIGHT_POINT, intensity, color, p=position)
+    def add_point_light(self, position, intensity, color=(1, 1, 1), ies=None, world_to_local=None):
+        """Light::point; `ies` = (vertical angles, horizontal angles,
+        candela[h][v]) reshapes its output (src/scene/ies.rs), oriented by
+        `world_to_local` (3x3, identity by default: 0 degrees points down -y)."""
+        li = self._light(abi.LIGHT_POINT, intensity, color, p=position)
+        if ies is not None:
+            v, h, c = (np.ascontiguousarray(a, dtype=np.float64) for a in ies)
+            if c.shape != (len(h), len(v)) or len(v) == 0 or len(h) == 0:
+                raise ValueError("ies candela must be (n_h, n_v)")
+            m = np.eye(3) if world_to_local is None else np.asarray(world_to_local, np.float64).reshape(3, 3)
+            self.ies[li] = (v, h, np.ascontiguousarray(c), np.ascontiguousarray(m))
+        return li
 
     def add_distant_light(self, direction, intensity, color=(1, 1, 1), angular_radius=0.0):
         return self._light(abi.LIGHT_DISTANT, intensity, color, e1=direction, radius=angular_radius)
@@ -401,5 +412,17 @@ class Scene:
             d.textures = tex_arr
             d.n_textures = len(self.textures)
         self._desc = d
-        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr, tex_arr)
+        ies_arr = (abi.RtIesDesc * max(1, len(self.ies)))()
+        for k, (li, (v, h, c, m)) in enumerate(sorted(self.ies.items())):
+            keep += [v, h, c]
+            e = ies_arr[k]
+            e.light, e.n_v, e.n_h = li, len(v), len(h)
+            e.v_angles = v.ctypes.data_as(C.POINTER(C.c_double))
+            e.h_angles = h.ctypes.data_as(C.POINTER(C.c_double))
+            e.candela = c.ctypes.data_as(C.POINTER(C.c_double))
+            e.world_to_local = (C.c_double * 9)(*m.reshape(9))
+        if self.ies:
+            d.ies = ies_arr
+            d.n_ies = len(self.ies)
+        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr, tex_arr, ies_arr)
         return d

@@ -106,3 +106,31 @@ def test_textures_match_oracle():
     for axis in (0, 1):
         a, b = gpu.mean(axis).mean(-1), cpu.mean(axis).mean(-1)
         assert np.all(np.abs(a - b) <= 0.08 * b + 0.015), (axis, np.abs(a - b).max())
+
+
+def test_ies_point_light_matches_oracle():
+    """A narrow downlight profile (src/scene/ies.rs) on a point light above a
+    floor, tilted 30 degrees: GPU against the oracle, and unlike the bare light."""
+    from rtcuda.ies import parse_ies
+    from test_ies_cpu import DOWNLIGHT
+    w, h, spp = 48, 36, 64
+
+    def make(profile):
+        s = scene.Scene(w, h, fov=60.0)
+        s.look_at((0.0, 2.5, -2.5), (0.0, 0.0, 0.5))
+        m = s.add_material(scene.matte((0.7, 0.7, 0.7)))
+        s.add_instance(s.add_mesh([[-4, 0, -3], [4, 0, -3], [4, 0, 5], [-4, 0, 5]], [[0, 2, 1], [0, 3, 2]]), m)
+        a = np.radians(30.0)
+        tilt = np.array([[1, 0, 0], [0, np.cos(a), -np.sin(a)], [0, np.sin(a), np.cos(a)]])
+        s.add_point_light((0.0, 1.5, 0.5), 6.0, ies=parse_ies(DOWNLIGHT) if profile else None,
+                          world_to_local=tilt.T)
+        return s
+
+    p = abi.make_params(max_depth=3)
+    s = make(True)
+    gpu = _render(s, p, spp)
+    cpu = oracle.OracleScene(s).render(p, 0, spp)[0].reshape(h, w, 3) / spp
+    bare = oracle.OracleScene(make(False)).render(p, 0, spp)[0].reshape(h, w, 3) / spp
+    np.testing.assert_allclose(gpu.mean((0, 1)), cpu.mean((0, 1)), rtol=0.03)
+    same, other = np.abs(gpu - cpu).mean(), np.abs(gpu - bare).mean()
+    assert same < 0.2 * other, (same, other)
