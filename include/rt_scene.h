@@ -163,6 +163,13 @@ typedef struct rt_pattern_desc {
     uint32_t use_t;               /* ramp over t instead of s */
     int32_t  texture;             /* texture, triplanar: index into textures, -1 = missing (magenta) */
     uint32_t wrap;                /* RT_WRAP_* */
+    /* A UDIM tile set instead of one texture (TextureRef::Udim,
+     * pattern.rs:14-38): tile numbers 1001 + s cell + 10 t cell and the
+     * texture of each; a tile not in the set reads magenta. */
+    const uint32_t* udim_tiles;
+    const int32_t*  udim_textures;
+    uint32_t n_udim;
+    uint32_t udim_reserved;       /* 0 */
 } rt_pattern_desc;
 
 /* PbrParams fields a pattern output drives (BoundField, pattern.rs:238-254). */
@@ -262,7 +269,7 @@ static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
 static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
 static_assert(sizeof(rt_params) == 64, "rt_params layout");
 static_assert(sizeof(rt_pattern_input) == 32, "rt_pattern_input layout");
-static_assert(sizeof(rt_pattern_desc) == 240, "rt_pattern_desc layout");
+static_assert(sizeof(rt_pattern_desc) == 264, "rt_pattern_desc layout");
 static_assert(sizeof(rt_texture_desc) == 16, "rt_texture_desc layout");
 static_assert(sizeof(rt_pattern_binding) == 16, "rt_pattern_binding layout");
 static_assert(sizeof(rt_ies_desc) == 112, "rt_ies_desc layout");

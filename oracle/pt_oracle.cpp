@@ -567,6 +567,7 @@ struct PatNode {
     bool use_t;
     int32_t texture;  // texture / triplanar: index, -1 = missing
     int wrap;
+    std::vector<std::pair<uint32_t, int32_t>> udim;  // (tile, texture) when a UDIM set
 };
 struct ShadeCtx {  // pattern.rs:69-82
     double st[2];
@@ -703,20 +704,38 @@ struct Texture {
 static const V3 MISSING_COLOR{1.0, 0.0, 1.0};
 
 // pattern.rs:126-226 eval_at.
+// TextureRef::resolve (pattern.rs:25-38): the texture of (s, t) and the
+// st within it; a UDIM set picks tile 1001 + s cell + 10 t cell (s cells
+// clamped to 0..9, t cells from 0) at the cell-local st. -1: missing.
+static int32_t tex_resolve(const PatNode& n, double* s, double* t) {
+    if (n.udim.empty()) return n.texture;
+    const double sc = std::min(std::max(std::floor(*s), 0.0), 9.0), tc = std::fmax(std::floor(*t), 0.0);
+    const uint32_t tile = 1001u + (uint32_t)sc + 10u * (uint32_t)tc;
+    for (const auto& e : n.udim)
+        if (e.first == tile) {
+            *s -= sc;
+            *t -= tc;
+            return e.second;
+        }
+    return -1;
+}
+
 // pattern.rs:93-124: a texture lookup with t flipped into image rows; a
 // missing texture reads magenta.
-static V3 sample_tex(const std::vector<Texture>& tex, int32_t id, int wrap, double s, double t, double footprint) {
+static V3 sample_tex(const std::vector<Texture>& tex, const PatNode& n, double s, double t, double footprint) {
+    const int32_t id = tex_resolve(n, &s, &t);
     if (id < 0 || (size_t)id >= tex.size()) return MISSING_COLOR;
     float c[3];
-    tex[(size_t)id].sample(s, 1.0 - t, footprint, wrap, c);
+    tex[(size_t)id].sample(s, 1.0 - t, footprint, n.wrap, c);
     return {c[0], c[1], c[2]};
 }
-static V3 sample_tex_ewa(const std::vector<Texture>& tex, int32_t id, int wrap, double s, double t, const double du[2],
+static V3 sample_tex_ewa(const std::vector<Texture>& tex, const PatNode& n, double s, double t, const double du[2],
                          const double dv[2]) {
+    const int32_t id = tex_resolve(n, &s, &t);
     if (id < 0 || (size_t)id >= tex.size()) return MISSING_COLOR;
     const double u[2] = {du[0], -du[1]}, v[2] = {dv[0], -dv[1]};
     float c[3];
-    tex[(size_t)id].sample_ewa(s, 1.0 - t, u, v, wrap, c);
+    tex[(size_t)id].sample_ewa(s, 1.0 - t, u, v, n.wrap, c);
     return {c[0], c[1], c[2]};
 }
 
@@ -736,18 +755,17 @@ static V3 pattern_eval(const std::vector<PatNode>& nodes, const std::vector<Text
             if (aniso > 1e-12) {
                 const double du[2] = {c.dst_major[0] * n.scale[0], c.dst_major[1] * n.scale[1]};
                 const double dv[2] = {c.dst_minor[0] * n.scale[0], c.dst_minor[1] * n.scale[1]};
-                return sample_tex_ewa(tex, n.texture, n.wrap, s, t, du, dv);
+                return sample_tex_ewa(tex, n, s, t, du, dv);
             }
-            return sample_tex(tex, n.texture, n.wrap, s, t,
-                              c.footprint * std::fmax(std::fabs(n.scale[0]), std::fabs(n.scale[1])));
+            return sample_tex(tex, n, s, t, c.footprint * std::fmax(std::fabs(n.scale[0]), std::fabs(n.scale[1])));
         }
         case RT_PATTERN_TRIPLANAR: {  // pattern.rs:200-214
             const V3 a{std::fabs(c.n.x), std::fabs(c.n.y), std::fabs(c.n.z)};
             const double total = std::fmax(a.x + a.y + a.z, 1e-9);
             const double f = n.frequency;
-            const V3 cx = sample_tex(tex, n.texture, n.wrap, c.p.y * f, c.p.z * f, c.footprint);
-            const V3 cy = sample_tex(tex, n.texture, n.wrap, c.p.z * f, c.p.x * f, c.footprint);
-            const V3 cz = sample_tex(tex, n.texture, n.wrap, c.p.x * f, c.p.y * f, c.footprint);
+            const V3 cx = sample_tex(tex, n, c.p.y * f, c.p.z * f, c.footprint);
+            const V3 cy = sample_tex(tex, n, c.p.z * f, c.p.x * f, c.footprint);
+            const V3 cz = sample_tex(tex, n, c.p.x * f, c.p.y * f, c.footprint);
             return cx * (a.x / total) + cy * (a.y / total) + cz * (a.z / total);
         }
         case RT_PATTERN_CHECKER: {
@@ -2005,6 +2023,8 @@ static void load_patterns(const rt_scene_desc* d, std::vector<PatNode>& out) {
         n.use_t = pd.use_t != 0;
         n.texture = pd.texture;
         n.wrap = (int)pd.wrap;
+        for (uint32_t k = 0; k < pd.n_udim && pd.udim_tiles && pd.udim_textures; k++)
+            n.udim.push_back({pd.udim_tiles[k], pd.udim_textures[k]});
         out.push_back(n);
     }
 }

@@ -795,6 +795,20 @@ bool flatten_patterns(const rt_scene_desc* d, HostScene& H, std::string* err) {
                     return false;
                 }
                 g.u1 = pd.wrap;
+                if (pd.n_udim) {
+                    if (!pd.udim_tiles || !pd.udim_textures) {
+                        *err = "pattern node " + std::to_string(i) + " has a UDIM set without tiles";
+                        return false;
+                    }
+                    g.u2 = pd.n_udim;
+                    g.udim_off = (uint32_t)H.udim.size();
+                    for (uint32_t k = 0; k < pd.n_udim; k++) {
+                        const int32_t t = pd.udim_textures[k];
+                        H.udim.push_back(make_uint2(pd.udim_tiles[k], (t >= 0 && (uint32_t)t < d->n_textures)
+                                                                          ? (uint32_t)t
+                                                                          : 0xFFFFFFFFu));
+                    }
+                }
                 if (pd.type == RT_PATTERN_TEXTURE) {
                     g.s0 = (float)pd.scale[0];
                     g.s1 = (float)pd.scale[1];

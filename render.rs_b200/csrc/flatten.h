@@ -32,6 +32,7 @@ struct HostScene {
     std::vector<DevTexture> textures;
     std::vector<DevMip> tex_mips;
     std::vector<float4> texels;
+    std::vector<uint2> udim;
     std::vector<DevMaterial> materials;
     std::vector<DevLight> lights;
     std::vector<LightNode> lbvh;

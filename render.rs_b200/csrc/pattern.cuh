@@ -159,12 +159,31 @@ __device__ __forceinline__ float3 tex_sample_ewa(const DevScene& S, const DevTex
     return sum / wsum;
 }
 
+// TextureRef::resolve (pattern.rs:25-38): the texture of a node at (s, t),
+// with (s, t) made cell-local for a UDIM set (tile 1001 + s cell + 10 t
+// cell, s cells clamped to 0..9); ~0 when missing or not in the set.
+__device__ __forceinline__ uint32_t tex_resolve(const DevScene& S, const DevPattern& g, float& s, float& t) {
+    if (g.u2 == 0u) return g.u0;
+    const float sc = fminf(fmaxf(floorf(s), 0.0f), 9.0f), tc = fmaxf(floorf(t), 0.0f);
+    const uint32_t tile = 1001u + (uint32_t)sc + 10u * (uint32_t)tc;
+    for (uint32_t k = 0; k < g.u2; k++) {
+        const uint2 e = __ldg(S.udim + g.udim_off + k);
+        if (e.x == tile) {
+            s -= sc;
+            t -= tc;
+            return e.y;
+        }
+    }
+    return 0xFFFFFFFFu;
+}
+
 // pattern.rs:93-124: lookups with t flipped into image rows; a missing
-// texture (~0) reads magenta.
-__device__ __forceinline__ float3 sample_tex(const DevScene& S, uint32_t tex, uint32_t wrap, float s, float t,
+// texture reads magenta.
+__device__ __forceinline__ float3 sample_tex(const DevScene& S, const DevPattern& g, float s, float t,
                                              float footprint) {
+    const uint32_t tex = tex_resolve(S, g, s, t);
     if (tex == 0xFFFFFFFFu) return f3(1.0f, 0.0f, 1.0f);
-    return tex_sample(S, S.textures[tex], s, 1.0f - t, footprint, wrap);
+    return tex_sample(S, S.textures[tex], s, 1.0f - t, footprint, g.u1);
 }
 
 // Everything a node reads at a shading point (pattern.rs:69-82).
@@ -240,20 +259,22 @@ __device__ __forceinline__ float3 pattern_node(const DevScene& S, const DevPatte
             const float aniso =
                 fabsf(cx.dst_major.x) + fabsf(cx.dst_major.y) + fabsf(cx.dst_minor.x) + fabsf(cx.dst_minor.y);
             if (aniso > 1e-12f) {
-                if (g.u0 == 0xFFFFFFFFu) return f3(1.0f, 0.0f, 1.0f);
+                float ls = ts, lt = tt;
+                const uint32_t tex = tex_resolve(S, g, ls, lt);
+                if (tex == 0xFFFFFFFFu) return f3(1.0f, 0.0f, 1.0f);
                 const float2 du = make_float2(cx.dst_major.x * g.s0, -(cx.dst_major.y * g.s1));
                 const float2 dv = make_float2(cx.dst_minor.x * g.s0, -(cx.dst_minor.y * g.s1));
-                return tex_sample_ewa(S, S.textures[g.u0], ts, 1.0f - tt, du, dv, g.u1);
+                return tex_sample_ewa(S, S.textures[tex], ls, 1.0f - lt, du, dv, g.u1);
             }
-            return sample_tex(S, g.u0, g.u1, ts, tt, footprint * fmaxf(fabsf(g.s0), fabsf(g.s1)));
+            return sample_tex(S, g, ts, tt, footprint * fmaxf(fabsf(g.s0), fabsf(g.s1)));
         }
         case RT_PATTERN_TRIPLANAR: {  // pattern.rs:200-214
             const float3 an = f3(fabsf(cx.n.x), fabsf(cx.n.y), fabsf(cx.n.z));
             const float total = fmaxf(an.x + an.y + an.z, 1e-9f);
             const float f = g.s0;
-            return sample_tex(S, g.u0, g.u1, p.y * f, p.z * f, footprint) * (an.x / total) +
-                   sample_tex(S, g.u0, g.u1, p.z * f, p.x * f, footprint) * (an.y / total) +
-                   sample_tex(S, g.u0, g.u1, p.x * f, p.y * f, footprint) * (an.z / total);
+            return sample_tex(S, g, p.y * f, p.z * f, footprint) * (an.x / total) +
+                   sample_tex(S, g, p.z * f, p.x * f, footprint) * (an.y / total) +
+                   sample_tex(S, g, p.x * f, p.y * f, footprint) * (an.z / total);
         }
         default: return f3(1.0f, 0.0f, 1.0f);
     }

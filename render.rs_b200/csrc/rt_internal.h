@@ -132,8 +132,9 @@ struct DevPattern {
                              // colour-correct gain, offset in c[1], c[2]
     float s0, s1, s2;        // checker s, t scale | fractal frequency, gain, lacunarity |
                              // colour-correct gamma, saturation
-    uint32_t u0, u1, u2;     // fractal octaves | ramp first entry, entries, use_t
-    uint32_t pad_;
+    uint32_t u0, u1, u2;     // fractal octaves | ramp first entry, entries, use_t |
+                             // texture index (~0 missing), wrap, UDIM tiles (0: one texture)
+    uint32_t udim_off;       // UDIM set: first (tile, texture) entry in DevScene::udim
 };
 static_assert(sizeof(DevPattern) == 80, "DevPattern layout");
 
@@ -194,6 +195,7 @@ struct DevScene {
     const DevTexture* textures;  // file textures (null when none)
     const DevMip* tex_mips;
     const float4* texels;
+    const uint2* udim;           // UDIM sets: (tile number, texture index or ~0)
     const DevMaterial* materials;
     const DevLight* lights;
     const LightNode* lbvh;

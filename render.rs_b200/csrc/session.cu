@@ -268,6 +268,7 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
             rc = rc ? rc : s->upload(&S.tex_mips, H.tex_mips);
             rc = rc ? rc : s->upload(&S.texels, H.texels);
         }
+        if (!H.udim.empty()) rc = rc ? rc : s->upload(&S.udim, H.udim);
     }
     if (!H.ies.empty()) {
         rc = rc ? rc : s->upload(&S.ies, H.ies);

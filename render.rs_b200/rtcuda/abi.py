@@ -124,6 +124,10 @@ class RtPatternDesc(C.Structure):
         ("use_t", C.c_uint32),
         ("texture", C.c_int32),
         ("wrap", C.c_uint32),
+        ("udim_tiles", C.POINTER(C.c_uint32)),
+        ("udim_textures", C.POINTER(C.c_int32)),
+        ("n_udim", C.c_uint32),
+        ("udim_reserved", C.c_uint32),
     ]
 
 
@@ -190,7 +194,7 @@ LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK, LIGHT_DOME = r
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
 for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 264), (RtLightDesc, 120),
-               (RtCameraDesc, 144), (RtParams, 64), (RtPatternInput, 32), (RtPatternDesc, 240),
+               (RtCameraDesc, 144), (RtParams, 64), (RtPatternInput, 32), (RtPatternDesc, 264),
                (RtPatternBinding, 16), (RtTextureDesc, 16), (RtIesDesc, 112), (RtSceneDesc, 296)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 

@@ -26,9 +26,9 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     Radiance .hdr (one map per scene).
   * Pattern graphs: PxrChecker, PxrFractal, PxrMix, PxrColorCorrect,
     PxrRamp, PxrTexture and triplanar nodes and Bxdf "reference"
-    connections are carried; texture files are read when they are .tex,
-    Radiance .hdr or PNG (others render magenta, as the reference's
-    unreadable files do); UDIM tile sets and presence connections are
+    connections are carried, UDIM tile sets included; texture files are
+    read when they are .tex, Radiance .hdr or PNG (others render magenta,
+    as the reference's unreadable files do); presence connections are
     skipped.
     Tessellated quadrics carry the reference's st, hyperboloids excepted.
 """
@@ -1047,14 +1047,17 @@ class _Builder:
             node = dict(type=abi.PATTERN_RAMP,
                         ramp=(np.array(pos[:n], np.float64), np.array(col[:3 * n], np.float64).reshape(-1, 3)),
                         use_t=prm.string("axis") == "t")
-        elif ptype in ("PxrTexture", "texture"):
-            node = dict(type=abi.PATTERN_TEXTURE, texture=self.open_texture(prm.string("filename") or ""),
-                        wrap=abi.WRAP_MODES.get(prm.string("wrapMode") or "periodic", abi.WRAP_PERIODIC),
-                        scale=(number("scaleS", 1.0), number("scaleT", 1.0)))
-        elif ptype == "triplanar":
-            node = dict(type=abi.PATTERN_TRIPLANAR, texture=self.open_texture(prm.string("filename") or ""),
-                        wrap=abi.WRAP_MODES.get(prm.string("wrapMode") or "periodic", abi.WRAP_PERIODIC),
-                        frequency=number("frequency", 1.0))
+        elif ptype in ("PxrTexture", "texture", "triplanar"):
+            tex = self.open_texture(prm.string("filename") or "")
+            node = dict(type=abi.PATTERN_TEXTURE if ptype != "triplanar" else abi.PATTERN_TRIPLANAR,
+                        texture=tex if isinstance(tex, int) else -1,
+                        wrap=abi.WRAP_MODES.get(prm.string("wrapMode") or "periodic", abi.WRAP_PERIODIC))
+            if isinstance(tex, dict):
+                node["udim"] = tex
+            if ptype == "triplanar":
+                node["frequency"] = number("frequency", 1.0)
+            else:
+                node["scale"] = (number("scaleS", 1.0), number("scaleT", 1.0))
         else:
             self.warn(f'Pattern "{ptype}" not implemented; skipping')
             return
@@ -1062,11 +1065,26 @@ class _Builder:
         self.patterns.append(node)
 
     def open_texture(self, name):
-        """A texture file (beside the scene) as a texture index; one that
-        cannot be read is the reference's missing texture (-1, magenta)."""
+        """open_texture (scene_builder.rs:1703-1736): a texture file (beside
+        the scene) as a texture index, one that cannot be read as -1
+        (magenta); a name holding <UDIM> as {tile: index} over the tiles
+        1001..1100 that exist (-1 when none do)."""
         if not name:
             self.warn("Pattern texture without \"filename\"; rendering magenta")
             return -1
+        if "<UDIM>" in name:
+            tiles = {}
+            for tile in range(1001, 1101):
+                f = name.replace("<UDIM>", str(tile))
+                path = f if os.path.isabs(f) or self.base_dir is None else os.path.join(self.base_dir, f)
+                if os.path.exists(path):
+                    idx = self.open_texture(f)
+                    if idx >= 0:
+                        tiles[tile] = idx
+            if not tiles:
+                self.warn(f'no UDIM tiles found for "{name}"')
+                return -1
+            return tiles
         path = name if os.path.isabs(name) or self.base_dir is None else os.path.join(self.base_dir, name)
         if path not in self.texture_ids:
             from .textures import TextureError, load_texture

@@ -192,11 +192,16 @@ class Scene:
         self._desc = None
         return len(self.textures) - 1
 
-    def add_texture_node(self, texture, wrap="periodic", scale=(1.0, 1.0)):
+    def add_texture_node(self, texture, wrap="periodic", scale=(1.0, 1.0), udim=None):
         """PxrTexture: the texture at (s, t) * scale, t up (texture row 0 at
-        t = 1); `texture` -1 is a missing file (magenta)."""
-        return self._pattern(type=abi.PATTERN_TEXTURE, texture=int(texture), wrap=abi.WRAP_MODES[wrap],
-                             scale=tuple(float(v) for v in scale))
+        t = 1); `texture` -1 is a missing file (magenta). `udim` = {tile
+        number: texture} makes it a UDIM tile set (tile 1001 + s cell + 10 t
+        cell, looked up at the cell-local st)."""
+        node = dict(type=abi.PATTERN_TEXTURE, texture=int(texture), wrap=abi.WRAP_MODES[wrap],
+                    scale=tuple(float(v) for v in scale))
+        if udim:
+            node["udim"] = {int(k): int(v) for k, v in udim.items()}
+        return self._pattern(**node)
 
     def add_triplanar(self, texture, wrap="periodic", frequency=1.0):
         """Triplanar projection of a texture over world P * frequency,
@@ -394,6 +399,13 @@ class Scene:
                 pd.use_t = int(node["use_t"])
             pd.texture = node.get("texture", -1)
             pd.wrap = node.get("wrap", 0)
+            if node.get("udim"):
+                tiles = np.array(sorted(node["udim"]), dtype=np.uint32)
+                texs = np.array([node["udim"][int(t)] for t in tiles], dtype=np.int32)
+                keep += [tiles, texs]
+                pd.udim_tiles = tiles.ctypes.data_as(C.POINTER(C.c_uint32))
+                pd.udim_textures = texs.ctypes.data_as(C.POINTER(C.c_int32))
+                pd.n_udim = len(tiles)
         bind_arr = (abi.RtPatternBinding * max(1, len(self.bindings)))()
         for k, (m, f, n) in enumerate(self.bindings):
             bind_arr[k].material, bind_arr[k].field, bind_arr[k].node = m, f, n

@@ -134,3 +134,25 @@ def test_ies_point_light_matches_oracle():
     np.testing.assert_allclose(gpu.mean((0, 1)), cpu.mean((0, 1)), rtol=0.03)
     same, other = np.abs(gpu - cpu).mean(), np.abs(gpu - bare).mean()
     assert same < 0.2 * other, (same, other)
+
+
+def test_udim_tiles_match_oracle():
+    """A floor whose st spans 2 x 2 UDIM cells, one constant-colour texture
+    per tile: the GPU's first-hit albedo equals the oracle's."""
+    w, h, spp = 32, 24, 64
+    s = scene.Scene(w, h, fov=50.0)
+    s.look_at((0.0, 2.0, -2.0), (0.0, 0.0, 0.3))
+    colors = {1001: (0.9, 0.1, 0.1), 1002: (0.1, 0.9, 0.1), 1011: (0.1, 0.1, 0.9), 1012: (0.9, 0.9, 0.1)}
+    tiles = {t: s.add_texture(np.tile(np.array(c, np.float32), (8, 8, 1))) for t, c in colors.items()}
+    m = s.add_material(scene.matte((0.5, 0.5, 0.5)))
+    s.bind_pattern(m, "diffuseColor", s.add_texture_node(-1, udim=tiles))
+    s.add_instance(s.add_mesh([[-2, 0, -1], [2, 0, -1], [2, 0, 3], [-2, 0, 3]], [[0, 2, 1], [0, 3, 2]],
+                              st=[[0, 0], [2, 0], [2, 2], [0, 2]]), m)
+    s.add_distant_light((0.2, -1.0, 0.1), 2.0)
+    p = abi.make_params(max_depth=2, aovs=True)
+    with PtSession(s, p) as g:
+        g.render_samples(0, spp)
+        ga = g.aux()[..., 0:3] / spp
+    ca = oracle.OracleScene(s).render(p, 0, spp, aovs=True)[1].reshape(h, w, 12)[..., 0:3] / spp
+    assert np.abs(ga - ca).mean() < 0.01, np.abs(ga - ca).mean()
+    assert len(np.unique(np.round(ca.reshape(-1, 3), 1), axis=0)) >= 4

@@ -142,3 +142,32 @@ def test_texture_pattern_on_a_quad_in_the_oracle():
     s.add_instance(q, m)
     ctx = [[0.2, 0.8, 0.2, 0.8, 1.0, 0, 0, -1, 0.0, 0, 0, 0, 0]]
     np.testing.assert_allclose(oracle.pattern_eval(s, n, ctx)[0], checker(32, 32)[6, 6], atol=1e-6)
+
+
+def _udim_scene():
+    """Four constant-colour tiles 1001, 1002, 1011, 1012 as one UDIM set."""
+    s = scene.Scene(4, 4)
+    colors = {1001: (1.0, 0.0, 0.0), 1002: (0.0, 1.0, 0.0), 1011: (0.0, 0.0, 1.0), 1012: (1.0, 1.0, 0.0)}
+    tiles = {t: s.add_texture(np.tile(np.array(c, np.float32), (4, 4, 1))) for t, c in colors.items()}
+    return s, s.add_texture_node(-1, udim=tiles), colors
+
+
+def test_udim_tile_pick():
+    """pattern.rs:350-373: (0.5, 0.5) is tile 1001, (1.3, 1.4) tile 1012,
+    (5.0, 0.0) a tile outside the set (magenta)."""
+    s, node, colors = _udim_scene()
+    c = oracle.pattern_eval(s, node, [[0.5, 0.5, 0, 0, 0, 0], [1.3, 1.4, 0, 0, 0, 0], [5.0, 0.0, 0, 0, 0, 0],
+                                      [1.5, 0.2, 0, 0, 0, 0], [0.2, 1.5, 0, 0, 0, 0]])
+    np.testing.assert_allclose(c, [colors[1001], colors[1012], (1, 0, 1), colors[1002], colors[1011]], atol=1e-6)
+
+
+def test_rib_udim_files(tmp_path):
+    for tile, v in ((1001, 0.25), (1012, 0.75)):
+        textures.write_tex(tmp_path / f"paint.{tile}.tex", np.full((2, 2, 3), v, np.float32))
+    s = load_rib_string('Pattern "PxrTexture" "p" "string filename" ["paint.<UDIM>.tex"]\n'
+                        'Pattern "PxrTexture" "q" "string filename" ["none.<UDIM>.tex"]', base_dir=str(tmp_path))
+    assert sorted(s.patterns[0]["udim"]) == [1001, 1012]
+    assert s.patterns[1]["texture"] == -1 and "udim" not in s.patterns[1]
+    assert any("no UDIM tiles" in w for w in s.warnings)
+    c = oracle.pattern_eval(s, 0, [[0.5, 0.5, 0, 0, 0, 0], [1.5, 1.5, 0, 0, 0, 0]])
+    np.testing.assert_allclose(c[:, 0], [0.25, 0.75], atol=1e-6)
