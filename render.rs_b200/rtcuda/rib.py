@@ -1239,6 +1239,29 @@ class _Builder:
         return s
 
 
+def _rib_value(v):
+    if isinstance(v, str):
+        return '"' + v.replace("\\", "\\\\").replace('"', '\\"') + '"'
+    if isinstance(v, list):
+        if v and all(isinstance(x, str) for x in v):
+            return "[" + " ".join(_rib_value(x) for x in v) + "]"
+        return "[" + " ".join(repr(float(x)) for x in v) + "]"
+    return repr(float(v))  # the shortest text that reads back to the same double
+
+
+def format_rib(requests):
+    """RIB text of a request list (name, values) as parse_rib returns it:
+    what the reference's `catrib` writes for a translated scene."""
+    out, depth = [], 0
+    for name, vals in requests:
+        if name in ("AttributeEnd", "WorldEnd", "TransformEnd"):
+            depth = max(depth - 1, 0)
+        out.append("  " * depth + " ".join([name] + [_rib_value(v) for v in vals]))
+        if name in ("AttributeBegin", "WorldBegin", "TransformBegin"):
+            depth += 1
+    return "\n".join(out) + "\n"
+
+
 def load_rib_string(text, base_dir=None):
     """A RibScene from RIB text (ReadArchive paths resolve against base_dir)."""
     b = _Builder(base_dir)

@@ -428,6 +428,13 @@ def usda_to_requests(text):
     return conv.out, parser.warnings + conv.warnings
 
 
+def usda_to_rib(text):
+    """The RIB text of a .usda stage's translation (`render catrib
+    scene.usda out.rib`)."""
+    from .rib import format_rib
+    return format_rib(usda_to_requests(text)[0])
+
+
 def load_usda_string(text, base_dir=None):
     """A RibScene from .usda text (asset paths resolve against base_dir)."""
     reqs, warnings = usda_to_requests(text)

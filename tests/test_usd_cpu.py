@@ -154,3 +154,24 @@ def DomeLight "Sky" { float inputs:intensity = 0.5 }
     assert np.allclose(np.abs(P), 2.0)
     reqs, _ = usda_to_requests(usda)
     assert ("Rotate", [-90.0, 1.0, 0.0, 0.0]) in reqs[:reqs.index(("WorldBegin", []))]
+
+
+def test_translation_round_trips_through_rib_text():
+    from rtcuda.rib import format_rib, parse_rib
+    from rtcuda.usd import usda_to_rib
+    reqs, _ = usda_to_requests(STAGE)
+    text = usda_to_rib(STAGE)
+    back = parse_rib(text)
+    assert [r[0] for r in back] == [r[0] for r in reqs]
+    for (n0, v0), (n1, v1) in zip(reqs, back):
+        flat0 = [x for v in v0 for x in (v if isinstance(v, list) else [v])]
+        flat1 = [x for v in v1 for x in (v if isinstance(v, list) else [v])]
+        assert len(flat0) == len(flat1), n0
+        for a, b in zip(flat0, flat1):
+            assert a == b
+    # The RIB text builds the same scene as the stage.
+    a, b = load_usda_string(STAGE), load_rib_string(text)
+    np.testing.assert_array_equal(a.instance_array()["xf"], b.instance_array()["xf"])
+    assert a.materials == b.materials and a.fov == b.fov
+    assert format_rib([("Attribute", ["identifier", "name", ['say "hi"']])]) == \
+        'Attribute "identifier" "name" ["say \\"hi\\""]\n'
