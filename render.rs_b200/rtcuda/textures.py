@@ -119,35 +119,40 @@ def read_tex(path):
 
 
 def _unfilter(raw, h, stride, bpp):
-    """PNG scanline filters 0-4 (ISO/IEC 15948 section 9)."""
+    """PNG scanline filters 0-4 (ISO/IEC 15948 section 9). None and Up are
+    whole-row array operations; Sub, Average and Paeth depend on the byte
+    to the left and run per byte on bytearrays."""
     out = np.zeros((h, stride), dtype=np.uint8)
-    prev = np.zeros(stride, dtype=np.int32)
+    prev = bytearray(stride)
     pos = 0
+    if len(raw) < h * (stride + 1):
+        raise TextureError("PNG: truncated image data")
     for y in range(h):
         ftype = raw[pos]
-        line = np.frombuffer(raw, np.uint8, stride, pos + 1).astype(np.int32)
+        line = raw[pos + 1:pos + 1 + stride]
         pos += 1 + stride
         if ftype == 0:
-            cur = line
+            cur = bytearray(line)
         elif ftype == 2:
-            cur = (line + prev) & 0xFF
-        else:
-            cur = np.zeros(stride, dtype=np.int32)
+            cur = bytearray(((np.frombuffer(line, np.uint8).astype(np.uint16) +
+                              np.frombuffer(bytes(prev), np.uint8)) & 0xFF).astype(np.uint8).tobytes())
+        elif ftype in (1, 3, 4):
+            cur = bytearray(line)
             for i in range(stride):
                 a = cur[i - bpp] if i >= bpp else 0
-                b = prev[i]
-                c = prev[i - bpp] if i >= bpp else 0
                 if ftype == 1:
                     p = a
                 elif ftype == 3:
-                    p = (a + b) >> 1
-                elif ftype == 4:
+                    p = (a + prev[i]) >> 1
+                else:
+                    b = prev[i]
+                    c = prev[i - bpp] if i >= bpp else 0
                     pa, pb, pc = abs(b - c), abs(a - c), abs(a + b - 2 * c)
                     p = a if pa <= pb and pa <= pc else (b if pb <= pc else c)
-                else:
-                    raise TextureError(f"PNG: bad filter type {ftype}")
-                cur[i] = (line[i] + p) & 0xFF
-        out[y] = cur
+                cur[i] = (cur[i] + p) & 0xFF
+        else:
+            raise TextureError(f"PNG: bad filter type {ftype}")
+        out[y] = np.frombuffer(bytes(cur), np.uint8)
         prev = cur
     return out
 

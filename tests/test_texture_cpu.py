@@ -82,17 +82,36 @@ def test_oracle_mip_chain_matches_the_tex_writer():
     np.testing.assert_allclose(last, chain[-1][0, 0], rtol=0, atol=2e-7)
 
 
+def _filter_row(line, prev, ftype, bpp=3):
+    """The encoder side of PNG filter `ftype` for one row (ints 0-255)."""
+    out = []
+    for i, x in enumerate(line):
+        a = line[i - bpp] if i >= bpp else 0
+        b = prev[i]
+        c = prev[i - bpp] if i >= bpp else 0
+        if ftype == 0:
+            p = 0
+        elif ftype == 1:
+            p = a
+        elif ftype == 2:
+            p = b
+        elif ftype == 3:
+            p = (a + b) >> 1
+        else:
+            pa, pb, pc = abs(b - c), abs(a - c), abs(a + b - 2 * c)
+            p = a if pa <= pb and pa <= pc else (b if pb <= pc else c)
+        out.append((x - p) & 0xFF)
+    return bytes(out)
+
+
 def _png(a, ftype=0):
     h, w, _ = a.shape
-    rows = []
+    rows, prev = [], [0] * (w * 3)
     for y in range(h):
-        line = a[y].reshape(-1).astype(np.int32)
-        if ftype == 1:
-            f = line.copy()
-            f[3:] = (line[3:] - line[:-3]) & 0xFF
-        else:
-            f = line
-        rows.append(bytes([ftype]) + f.astype(np.uint8).tobytes())
+        line = [int(v) for v in a[y].reshape(-1)]
+        f = ftype if ftype >= 0 else y % 5  # -1: a different filter on every row
+        rows.append(bytes([f]) + _filter_row(line, prev, f))
+        prev = line
 
     def chunk(k, b):
         return struct.pack(">I", len(b)) + k + b + struct.pack(">I", zlib.crc32(k + b) & 0xFFFFFFFF)
@@ -102,7 +121,7 @@ def _png(a, ftype=0):
 
 def test_png_decode_and_srgb():
     a = np.random.default_rng(3).integers(0, 256, (6, 9, 3)).astype(np.uint8)
-    for ftype in (0, 1):
+    for ftype in (0, 1, 2, 3, 4, -1):
         np.testing.assert_allclose(textures.decode_png(_png(a, ftype)), a / 255.0, atol=1e-7)
     lin = textures.srgb_to_linear(np.array([0.0, 0.04045, 0.5, 1.0], np.float32))
     np.testing.assert_allclose(lin, [0.0, 0.04045 / 12.92, ((0.5 + 0.055) / 1.055) ** 2.4, 1.0], rtol=1e-6)
