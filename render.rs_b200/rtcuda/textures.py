@@ -180,7 +180,11 @@ def decode_png(data):
     if chans is None or depth not in (8, 16) or interlace:
         raise TextureError("PNG: only non-interlaced 8/16-bit grey or RGB(A) images are read")
     bpp = chans * depth // 8
-    rows = _unfilter(zlib.decompress(b"".join(idat)), h, w * bpp, bpp)
+    try:
+        raw = zlib.decompress(b"".join(idat))
+    except zlib.error as e:
+        raise TextureError(f"PNG: {e}") from None
+    rows = _unfilter(raw, h, w * bpp, bpp)
     if depth == 16:
         px = rows.reshape(h, w * chans, 2).astype(np.uint32)
         px = ((px[..., 0] << 8) | px[..., 1]).reshape(h, w, chans) / 65535.0

@@ -123,6 +123,13 @@ def test_png_decode_and_srgb():
     a = np.random.default_rng(3).integers(0, 256, (6, 9, 3)).astype(np.uint8)
     for ftype in (0, 1, 2, 3, 4, -1):
         np.testing.assert_allclose(textures.decode_png(_png(a, ftype)), a / 255.0, atol=1e-7)
+    full = _png(a, 4)
+    for broken in (full[:60] + full[-12:], full[:40]):
+        try:
+            textures.decode_png(broken)
+            raise AssertionError("a broken PNG decoded")
+        except textures.TextureError:
+            pass
     lin = textures.srgb_to_linear(np.array([0.0, 0.04045, 0.5, 1.0], np.float32))
     np.testing.assert_allclose(lin, [0.0, 0.04045 / 12.92, ((0.5 + 0.055) / 1.055) ** 2.4, 1.0], rtol=1e-6)
 
