@@ -167,7 +167,9 @@ def decode_png(data):
         n, kind = struct.unpack_from(">I4s", data, pos)
         body = data[pos + 8:pos + 8 + n]
         if kind == b"IHDR":
-            ihdr = struct.unpack(">IIBBBBB", body)
+            if len(body) < 13:
+                raise TextureError("PNG: truncated header")
+            ihdr = struct.unpack(">IIBBBBB", body[:13])
         elif kind == b"IDAT":
             idat.append(body)
         elif kind == b"IEND":

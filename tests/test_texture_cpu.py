@@ -124,7 +124,7 @@ def test_png_decode_and_srgb():
     for ftype in (0, 1, 2, 3, 4, -1):
         np.testing.assert_allclose(textures.decode_png(_png(a, ftype)), a / 255.0, atol=1e-7)
     full = _png(a, 4)
-    for broken in (full[:60] + full[-12:], full[:40]):
+    for broken in (full[:60] + full[-12:], full[:40], full[:20], b"not a png"):
         try:
             textures.decode_png(broken)
             raise AssertionError("a broken PNG decoded")
