@@ -85,11 +85,15 @@ def write_tex(path, img):
 def read_tex_header(data):
     if data[:4] != MAGIC:
         raise TextureError("not a .tex file (bad magic)")
+    if len(data) < 28:
+        raise TextureError("truncated .tex header")
     version, w, h, ch, tile, n = struct.unpack_from("<6I", data, 4)
     if version != 1:
         raise TextureError(f"unsupported .tex version {version}")
-    if ch != 3 or tile != TILE or n > 32:
+    if ch != 3 or tile != TILE or n > 32 or n == 0:
         raise TextureError("unsupported .tex layout")
+    if len(data) < 28 + 24 * n:
+        raise TextureError("truncated .tex header")
     mips = [struct.unpack_from("<4IQ", data, 28 + 24 * k) for k in range(n)]
     return w, h, mips
 

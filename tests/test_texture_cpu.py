@@ -39,6 +39,18 @@ def test_tex_round_trip_and_mips(tmp_path):
     np.testing.assert_array_equal(textures.read_tex(path), img)
 
 
+def test_broken_tex_files_raise(tmp_path):
+    textures.write_tex(tmp_path / "ok.tex", checker(40, 40))
+    data = (tmp_path / "ok.tex").read_bytes()
+    for k, broken in enumerate((data[:20], data[:40], data[:300], b"XTEX" + data[4:])):
+        (tmp_path / f"b{k}.tex").write_bytes(broken)
+        try:
+            textures.read_tex(tmp_path / f"b{k}.tex")
+            raise AssertionError(f"broken file {k} read")
+        except textures.TextureError:
+            pass
+
+
 def test_edge_tiles_replicate(tmp_path):
     img = checker(40, 40)
     path = tmp_path / "e.tex"
