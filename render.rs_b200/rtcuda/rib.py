@@ -21,8 +21,9 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     are tessellated into smooth-normal triangle meshes; the reference
     intersects them analytically.
   * SubdivisionMesh renders its control cage; Curves, Points, patches,
-    displacement, media and motion blur are skipped (motion blocks use
-    their first sample); a PxrDomeLight lightColorMap is read when it is a
+    media and motion blur are skipped (motion blocks use their first
+    sample); Displace "noise" moves polygon-mesh vertices at load time as
+    the reference does; a PxrDomeLight lightColorMap is read when it is a
     Radiance .hdr (one map per scene).
   * Pattern graphs: PxrChecker, PxrFractal, PxrMix, PxrColorCorrect,
     PxrRamp, PxrTexture and triplanar nodes and Bxdf "reference"
@@ -547,6 +548,7 @@ class _State:
         self.area_light = None   # (intensity, color)
         self.bxdf = None         # material dict
         self.bxdf_bindings = []  # (field id, pattern node) of the active Bxdf
+        self.displace = None     # Displace "noise" parameters (dict) for tessellated meshes
         self.identifier = None
 
     def copy(self):
@@ -659,9 +661,14 @@ class _Builder:
     def place(self, mesh, mat, xf):
         self.instances.append((mesh, mat, np.asarray(xf, np.float64)[:3, :].reshape(12)))
 
-    def tessellated_mesh(self, P, I, N=None, emissive=True, st=None):
-        """add_tessellated_mesh (scene_builder.rs:1195-1234); quadrics take
-        the plain state material (no area-light emission, :813-909)."""
+    def tessellated_mesh(self, P, I, N=None, emissive=True, st=None, displace=False):
+        """add_tessellated_mesh (scene_builder.rs:1195-1234): the state's
+        displacement on meshes the reference tessellates (`displace`; not
+        on the quadrics it intersects analytically); quadrics take the
+        plain state material (no area-light emission, :813-909)."""
+        if displace and self.state.displace is not None:
+            from .displace import displace_mesh
+            P, N = displace_mesh(P, I, N, **self.state.displace)
         mesh = self.add_mesh(P, I, N, st)
         m = self.make_material()
         if emissive and self.state.area_light is not None:
@@ -827,6 +834,24 @@ class _Builder:
             st.bxdf_bindings = self.bxdf_bindings(prm)
         elif name == "Pattern":
             self.pattern_request(vals)
+        elif name == "Displace":
+            # scene_builder.rs:776-795: the built-in fBm "noise" displacement.
+            kind = _str(vals, 0) or ""
+            if kind != "noise":
+                self.warn(f'Displace "{kind}": only the built-in "noise" displacement exists; using it')
+            prm = _Params(vals, 2 if len(vals) % 2 == 0 else 1)
+            d = dict(amplitude=0.1, frequency=1.0, octaves=4, gain=0.5, lacunarity=2.0, offset=(0.0, 0.0, 0.0))
+            for key in ("amplitude", "frequency", "gain", "lacunarity"):
+                v = prm.number(key)
+                if v is not None:
+                    d[key] = v
+            v = prm.number("octaves")
+            if v is not None:
+                d["octaves"] = int(v)
+            v = prm.numbers("offset")
+            if v is not None and len(v) >= 3:
+                d["offset"] = tuple(v[:3])
+            st.displace = d
         elif name == "AreaLightSource":
             p = _Params(vals, 2 if len(vals) % 2 == 0 else 1)
             inten = p.number("intensity")
@@ -974,7 +999,7 @@ class _Builder:
         ST = None
         if stv is not None and len(stv) * 3 == len(p) * 2:
             ST = np.array(stv, dtype=np.float64).reshape(-1, 2)
-        self.tessellated_mesh(P, I, N, st=ST)
+        self.tessellated_mesh(P, I, N, st=ST, displace=True)
 
     # -- patterns (scene_builder.rs:703-728, 1738-1846) -------------------------------
     def _ref_target(self, prm, name):
