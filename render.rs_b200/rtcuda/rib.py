@@ -20,8 +20,8 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     Hyperboloid) and the emitter shapes of PxrSphereLight / PxrDiskLight
     are tessellated into smooth-normal triangle meshes; the reference
     intersects them analytically.
-  * SubdivisionMesh renders its control cage; Curves, Points, patches,
-    media and motion blur are skipped (motion blocks use their first
+  * SubdivisionMesh is diced by uniform Catmull-Clark as the reference
+    does; Curves, Points, patches, media and motion blur are skipped (motion blocks use their first
     sample); Displace "noise" moves polygon-mesh vertices at load time as
     the reference does; a PxrDomeLight lightColorMap is read when it is a
     Radiance .hdr (one map per scene).
@@ -549,6 +549,7 @@ class _State:
         self.bxdf = None         # material dict
         self.bxdf_bindings = []  # (field id, pattern node) of the active Bxdf
         self.displace = None     # Displace "noise" parameters (dict) for tessellated meshes
+        self.shading_rate = 1.0  # sets the subdivision level of SubdivisionMesh
         self.identifier = None
 
     def copy(self):
@@ -701,8 +702,13 @@ class _Builder:
                     "IfEnd", "Display", "Clipping", "ClippingPlane", "CropWindow", "FrameAspectRatio",
                     "PixelVariance", "Exposure", "Quantize", "Hider", "Integrator", "TextureCoordinates",
                     "ShadingInterpolation", "RelativeDetail", "Declare", "Orientation", "ReverseOrientation",
-                    "Sides", "ShadingRate", "Opacity", "Basis", "CoordinateSystem", "ScopedCoordinateSystem",
+                    "Sides", "Opacity", "Basis", "CoordinateSystem", "ScopedCoordinateSystem",
                     "Shutter", "ArchiveEnd"):
+            return
+        if name == "ShadingRate":
+            r = _num(vals, 0)
+            if r is not None:
+                st.shading_rate = r
             return
         if name == "AttributeBegin":
             self.attr_stack.append(st.copy())
@@ -872,7 +878,9 @@ class _Builder:
                 if len(nl) > 1:
                     self.warn("GeneralPolygon holes are not supported; using the outer loop")
                 self.polygon(["P", p[:3 * n0]])
-        elif name in ("PointsPolygons", "PointsGeneralPolygons", "SubdivisionMesh", "HierarchicalSubdivisionMesh"):
+        elif name in ("SubdivisionMesh", "HierarchicalSubdivisionMesh"):
+            self.subdivision_mesh(name, vals)
+        elif name in ("PointsPolygons", "PointsGeneralPolygons"):
             self.points_polygons(name, vals)
         elif name in _QUADRIC_ARGS:
             a = [_num(vals, k) for k in range(_QUADRIC_ARGS[name])]
@@ -957,13 +965,6 @@ class _Builder:
             if any(int(n) != 1 for n in nl):
                 self.warn("PointsGeneralPolygons holes are not supported; using outer loops only")
             vals = vals[1:]
-        elif name != "PointsPolygons":
-            self.warn(f"{name} renders its control mesh (no subdivision on this path)")
-            # SubdivisionMesh "scheme" [nverts] [verts] ([tags] [nargs] [ints] [floats]) params;
-            # HierarchicalSubdivisionMesh adds [strings] after [floats].
-            ntag = 5 if name == "HierarchicalSubdivisionMesh" else 4
-            tagged = len(vals) > 3 + ntag and isinstance(vals[3], list)
-            vals = vals[1:3] + vals[3 + ntag:] if tagged else vals[1:]
         nverts = _as_numbers(vals[0]) if len(vals) > 0 else None
         verts = _as_numbers(vals[1]) if len(vals) > 1 else None
         if nverts is None or verts is None:
@@ -1144,6 +1145,68 @@ class _Builder:
                 continue
             out.append((field, node))
         return out
+
+    def subdivision_mesh(self, name, vals):
+        """subdivision_mesh (scene_builder.rs:1236-1322): SubdivisionMesh
+        "scheme" [nverts] [verts] ([tags] [nargs] [ints] [floats]) params,
+        HierarchicalSubdivisionMesh with [strings] after [floats]; uniform
+        Catmull-Clark at the shading rate's level (rtcuda/subdiv.py)."""
+        from .subdiv import levels_for_shading_rate, tessellate as subdivide
+        scheme = _str(vals, 0)
+        if scheme is None:
+            return
+        if scheme != "catmull-clark":
+            self.warn(f'SubdivisionMesh scheme "{scheme}" treated as catmull-clark')
+        nverts = _as_numbers(vals[1]) if len(vals) > 1 else None
+        verts = _as_numbers(vals[2]) if len(vals) > 2 else None
+        if nverts is None or verts is None:
+            return
+        creases, corners, holes, interp = [], [], [], False
+        start = 3
+        if len(vals) > 3 and isinstance(vals[3], list) and all(isinstance(t, str) for t in vals[3]):
+            tags = vals[3]
+            nargs = (_as_numbers(vals[4]) if len(vals) > 4 else None) or []
+            ints = (_as_numbers(vals[5]) if len(vals) > 5 else None) or []
+            floats = (_as_numbers(vals[6]) if len(vals) > 6 else None) or []
+            ic = fc = 0
+            for ti, tag in enumerate(tags):
+                ni = int(nargs[2 * ti]) if 2 * ti < len(nargs) else 0
+                nf = int(nargs[2 * ti + 1]) if 2 * ti + 1 < len(nargs) else 0
+                ti_ints, ti_floats = ints[ic:ic + ni], floats[fc:fc + nf]
+                if tag == "crease":
+                    sharp = ti_floats[0] if ti_floats else 10.0
+                    creases += [(int(a), int(b), sharp) for a, b in zip(ti_ints, ti_ints[1:])]
+                elif tag == "corner":
+                    for i, v in enumerate(ti_ints):
+                        corners.append((int(v), ti_floats[i] if i < len(ti_floats) else
+                                        (ti_floats[0] if ti_floats else 10.0)))
+                elif tag == "hole":
+                    holes += [int(f) for f in ti_ints]
+                elif tag == "interpolateboundary":
+                    interp = True
+                else:
+                    self.warn(f'SubdivisionMesh tag "{tag}" not supported; ignoring')
+                ic += ni
+                fc += nf
+            start = 8 if name == "HierarchicalSubdivisionMesh" else 7
+        p = _Params(vals, start).numbers("P")
+        if p is None:
+            self.warn("SubdivisionMesh without \"P\"; skipping")
+            return
+        faces, cur = [], 0
+        for nv in nverts:
+            nv = int(nv)
+            if cur + nv > len(verts):
+                break
+            faces.append([int(v) for v in verts[cur:cur + nv]])
+            cur += nv
+        P = np.array(p, dtype=np.float64).reshape(-1, 3)
+        if any(v >= len(P) for f in faces for v in f):
+            raise RibError(f"{name}: vertex index out of range")
+        pos, idx, nrm = subdivide(P, faces, levels_for_shading_rate(self.state.shading_rate), creases, corners,
+                                  holes, interp)
+        if len(idx):
+            self.tessellated_mesh(pos, idx, nrm, displace=True)
 
     def light_source(self, vals):
         """parse_light (scene_builder.rs:1582-1635): positions untransformed."""
