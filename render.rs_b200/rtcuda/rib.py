@@ -20,8 +20,9 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     Hyperboloid) and the emitter shapes of PxrSphereLight / PxrDiskLight
     are tessellated into smooth-normal triangle meshes; the reference
     intersects them analytically.
-  * SubdivisionMesh is diced by uniform Catmull-Clark as the reference
-    does; Curves, Points, patches, media and motion blur are skipped (motion blocks use their first
+  * SubdivisionMesh is diced by uniform Catmull-Clark and bilinear /
+    bicubic PatchMesh and Patch by the current Basis, as the reference
+    does; Curves, Points, NuPatch, media and motion blur are skipped (motion blocks use their first
     sample); Displace "noise" moves polygon-mesh vertices at load time as
     the reference does; a PxrDomeLight lightColorMap is read when it is a
     Radiance .hdr (one map per scene).
@@ -549,7 +550,9 @@ class _State:
         self.bxdf = None         # material dict
         self.bxdf_bindings = []  # (field id, pattern node) of the active Bxdf
         self.displace = None     # Displace "noise" parameters (dict) for tessellated meshes
-        self.shading_rate = 1.0  # sets the subdivision level of SubdivisionMesh
+        self.shading_rate = 1.0  # sets the subdivision level of SubdivisionMesh and the patch dicing
+        self.basis_u = ("bezier", None)  # Basis: (name or 16 numbers, step or None) per direction
+        self.basis_v = ("bezier", None)
         self.identifier = None
 
     def copy(self):
@@ -702,8 +705,17 @@ class _Builder:
                     "IfEnd", "Display", "Clipping", "ClippingPlane", "CropWindow", "FrameAspectRatio",
                     "PixelVariance", "Exposure", "Quantize", "Hider", "Integrator", "TextureCoordinates",
                     "ShadingInterpolation", "RelativeDetail", "Declare", "Orientation", "ReverseOrientation",
-                    "Sides", "Opacity", "Basis", "CoordinateSystem", "ScopedCoordinateSystem",
+                    "Sides", "Opacity", "CoordinateSystem", "ScopedCoordinateSystem",
                     "Shutter", "ArchiveEnd"):
+            return
+        if name == "Basis":
+            # Basis <name | 16 numbers> ustep <name | 16 numbers> vstep (scene_builder.rs:576-601).
+            for k, attr in ((0, "basis_u"), (2, "basis_v")):
+                if k < len(vals):
+                    b = vals[k]
+                    step = _num(vals, k + 1)
+                    if isinstance(b, str) or (isinstance(b, list) and len(b) == 16):
+                        setattr(st, attr, (b, step))
             return
         if name == "ShadingRate":
             r = _num(vals, 0)
@@ -880,6 +892,8 @@ class _Builder:
                 self.polygon(["P", p[:3 * n0]])
         elif name in ("SubdivisionMesh", "HierarchicalSubdivisionMesh"):
             self.subdivision_mesh(name, vals)
+        elif name in ("PatchMesh", "Patch"):
+            self.patch_mesh(name, vals)
         elif name in ("PointsPolygons", "PointsGeneralPolygons"):
             self.points_polygons(name, vals)
         elif name in _QUADRIC_ARGS:
@@ -1145,6 +1159,51 @@ class _Builder:
                 continue
             out.append((field, node))
         return out
+
+    def _basis(self, spec):
+        from .patches import BASES
+        b, step = spec
+        if isinstance(b, str):
+            if b not in BASES:
+                return None
+            m, default = BASES[b]
+            return m, int(step) if step is not None else default
+        return np.array(b, np.float64).reshape(4, 4), int(step) if step is not None else 1
+
+    def patch_mesh(self, name, vals):
+        """patch_mesh (scene_builder.rs:1324-1362): PatchMesh "type" nu
+        uwrap nv vwrap params / Patch "type" params, bilinear or bicubic
+        with the current Basis, diced by the shading rate."""
+        from .patches import dice_segments, tessellate_bicubic, tessellate_bilinear
+        ptype = _str(vals, 0)
+        if ptype is None:
+            return
+        if name == "Patch":
+            n = 2 if ptype == "bilinear" else 4
+            nu, uw, nv, vw, start = n, False, n, False, 1
+        else:
+            nu, nv = _num(vals, 1), _num(vals, 3)
+            if nu is None or nv is None:
+                return
+            nu, nv, uw, vw, start = int(nu), int(nv), _str(vals, 2) == "periodic", _str(vals, 4) == "periodic", 5
+        p = _Params(vals, start).numbers("P")
+        if p is None:
+            self.warn(f'{name} without "P"; skipping')
+            return
+        segs = dice_segments(self.state.shading_rate)
+        if ptype == "bilinear":
+            mesh = tessellate_bilinear(p, nu, nv, uw, vw, segs)
+        elif ptype == "bicubic":
+            bu, bv = self._basis(self.state.basis_u), self._basis(self.state.basis_v)
+            mesh = None if bu is None or bv is None else tessellate_bicubic(p, nu, nv, uw, vw, bu, bv, segs)
+        else:
+            self.warn(f'{name} type "{ptype}" not supported')
+            return
+        if mesh is None:
+            self.warn(f"{name}: invalid control grid; skipping")
+            return
+        pos, idx, nrm, st = mesh
+        self.tessellated_mesh(pos, idx, nrm, st=st, displace=True)
 
     def subdivision_mesh(self, name, vals):
         """subdivision_mesh (scene_builder.rs:1236-1322): SubdivisionMesh
