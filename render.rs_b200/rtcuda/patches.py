@@ -98,3 +98,60 @@ def tessellate_bilinear(points, nu, nv, u_wrap, v_wrap, segs):
 def dice_segments(shading_rate):
     """dice_segments (scene_builder.rs:1173-1175)."""
     return int(min(max(16.0 / max(shading_rate, 0.05), 2.0), 64.0))
+
+
+def bspline_basis(knots, n_ctrl, order, t):
+    """The n_ctrl B-spline basis values at t: the knot span holding t (the
+    last one at the end of the range, as patches.rs:236-251 picks it), then
+    the Cox-de Boor recursion up to degree order - 1 within that span. The
+    in-place update runs upward (each N_i,p reads the old N_i,p-1 and
+    N_i+1,p-1); the reference's runs downward and reads N_i+1,p instead,
+    which for knots [0 0 1 1] gives N_0 = t (1 - t) rather than 1 - t."""
+    k = [float(x) for x in knots]
+    degree = order - 1
+    basis = [0.0] * (n_ctrl + degree + 1)
+    hi = min(n_ctrl, max(len(k) - order, 0))
+    span = degree
+    for i in range(degree, hi):
+        if t < k[i + 1] or i == hi - 1:
+            span = i
+            break
+        span = i + 1
+    basis[span] = 1.0
+
+    def knot(i):
+        return k[i] if 0 <= i < len(k) else 0.0
+    for p in range(1, degree + 1):
+        for i in range(max(span - p, 0), span + 1):
+            val = 0.0
+            d1 = knot(i + p) - k[i]
+            if d1 > 1e-12:
+                val += basis[i] * (t - k[i]) / d1
+            d2 = knot(i + p + 1) - knot(i + 1)
+            if d2 > 1e-12:
+                val += basis[i + 1] * (knot(i + p + 1) - t) / d2
+            basis[i] = val
+    return np.array(basis[:n_ctrl])
+
+
+def tessellate_nurbs(nu, uorder, uknot, umin, umax, nv, vorder, vknot, vmin, vmax, points, rational, segs_u,
+                     segs_v):
+    """tessellate_nurbs (patches.rs:271-336): a (segs_u + 1) x (segs_v + 1)
+    grid over [umin, umax] x [vmin, vmax]; rational points are homogeneous
+    (w x, w y, w z, w)."""
+    stride = 4 if rational else 3
+    pts = np.asarray(points, dtype=np.float64)
+    if len(pts) < nu * nv * stride:
+        return None
+    ctrl = pts[:nu * nv * stride].reshape(nv, nu, stride)
+    us = umin + (umax - umin) * np.arange(segs_u + 1) / segs_u
+    vs = vmin + (vmax - vmin) * np.arange(segs_v + 1) / segs_v
+    bu = np.array([bspline_basis(uknot, nu, uorder, u) for u in us])  # (gu, nu)
+    bv = np.array([bspline_basis(vknot, nv, vorder, v) for v in vs])  # (gv, nv)
+    xyz = np.einsum("vj,ui,jic->vuc", bv, bu, ctrl[..., :3])
+    if rational:
+        w = np.einsum("vj,ui,ji->vu", bv, bu, ctrl[..., 3])
+        xyz = np.where(np.abs(w)[..., None] > 1e-12, xyz / np.where(np.abs(w) > 1e-12, w, 1.0)[..., None], xyz)
+    su = (np.arange(segs_u + 1) / segs_u).astype(np.float32)
+    sv = (np.arange(segs_v + 1) / segs_v).astype(np.float32)
+    return _mesh(xyz, segs_u + 1, segs_v + 1, False, False, su, sv)

@@ -22,7 +22,8 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     intersects them analytically.
   * SubdivisionMesh is diced by uniform Catmull-Clark and bilinear /
     bicubic PatchMesh and Patch by the current Basis, as the reference
-    does; Curves, Points, NuPatch, media and motion blur are skipped (motion blocks use their first
+    does, NuPatch NURBS untrimmed; Curves, Points, media and motion blur
+    are skipped (motion blocks use their first
     sample); Displace "noise" moves polygon-mesh vertices at load time as
     the reference does; a PxrDomeLight lightColorMap is read when it is a
     Radiance .hdr (one map per scene).
@@ -894,6 +895,8 @@ class _Builder:
             self.subdivision_mesh(name, vals)
         elif name in ("PatchMesh", "Patch"):
             self.patch_mesh(name, vals)
+        elif name == "NuPatch":
+            self.nu_patch(vals)
         elif name in ("PointsPolygons", "PointsGeneralPolygons"):
             self.points_polygons(name, vals)
         elif name in _QUADRIC_ARGS:
@@ -1201,6 +1204,34 @@ class _Builder:
             return
         if mesh is None:
             self.warn(f"{name}: invalid control grid; skipping")
+            return
+        pos, idx, nrm, st = mesh
+        self.tessellated_mesh(pos, idx, nrm, st=st, displace=True)
+
+    def nu_patch(self, vals):
+        """nu_patch (scene_builder.rs:1364-1411): NuPatch nu uorder [uknot]
+        umin umax nv vorder [vknot] vmin vmax "P" | "Pw"; untrimmed."""
+        from .patches import dice_segments, tessellate_nurbs
+        nums = [_num(vals, k) for k in (0, 1, 3, 4, 5, 6, 8, 9)]
+        knots = [_as_numbers(vals[k]) if k < len(vals) else None for k in (2, 7)]
+        if any(v is None for v in nums) or any(k is None for k in knots):
+            return
+        nu, uorder, umin, umax, nv, vorder, vmin, vmax = nums
+        prm = _Params(vals, 10)
+        pw, p = prm.numbers("Pw"), prm.numbers("P")
+        if pw is None and p is None:
+            self.warn('NuPatch without "P"/"Pw"; skipping')
+            return
+        if prm.get("trimcurve") is not None:
+            self.warn("NuPatch trim curves not supported yet; rendering untrimmed")
+        base = dice_segments(self.state.shading_rate)
+        nu, nv, uorder, vorder = int(nu), int(nv), int(uorder), int(vorder)
+        segs_u = min(max(base * (max(nu - uorder, 0) + 1), 4), 128)
+        segs_v = min(max(base * (max(nv - vorder, 0) + 1), 4), 128)
+        mesh = tessellate_nurbs(nu, uorder, knots[0], umin, umax, nv, vorder, knots[1], vmin, vmax,
+                                pw if pw is not None else p, pw is not None, segs_u, segs_v)
+        if mesh is None:
+            self.warn("NuPatch: invalid control data; skipping")
             return
         pos, idx, nrm, st = mesh
         self.tessellated_mesh(pos, idx, nrm, st=st, displace=True)

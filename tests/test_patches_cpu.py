@@ -2,7 +2,8 @@
 patch tests (src/geometry/patches.rs:338-380) and the RIB requests."""
 import numpy as np
 
-from rtcuda.patches import BASES, basis_weights, dice_segments, tessellate_bicubic, tessellate_bilinear
+from rtcuda.patches import (BASES, basis_weights, bspline_basis, dice_segments, tessellate_bicubic,
+                            tessellate_bilinear, tessellate_nurbs)
 from rtcuda.rib import load_rib_string
 
 
@@ -58,10 +59,42 @@ def test_rib_patch_requests():
                         f'Patch "bilinear" "P" [0 0 0  1 0 0  0 1 0  1 1 0]\n'
                         f'NuPatch 2 2 [0 0 1 1] 0 1 2 2 [0 0 1 1] 0 1 "P" [0 0 0 1 0 0 0 1 0 1 1 0]')
     inst = s.instance_array()
-    assert len(inst) == 2
+    assert len(inst) == 3  # the bicubic mesh, the bilinear patch, the NURBS sheet
     a = s.meshes[inst["mesh"][0]][0]
     ref = tessellate_bicubic(_grid(4, 4).round(3), 4, 4, False, False, BASES["b-spline"], BASES["catmull-rom"],
                              dice_segments(4.0))[0]
     np.testing.assert_allclose(a, ref, atol=1e-6)
-    assert 0 in s.mesh_st and 1 in s.mesh_st
-    assert any("NuPatch" in w for w in s.warnings)
+    assert 0 in s.mesh_st and 1 in s.mesh_st and 2 in s.mesh_st
+    sheet = s.meshes[inst["mesh"][2]][0]
+    np.testing.assert_allclose(sheet[:, 2], 0.0) and np.testing.assert_allclose(sheet[0], [0, 0, 0], atol=1e-7)
+
+
+def test_nurbs_flat_sheet():
+    """patches.rs:380-417: an order-3 clamped sheet over a flat 4 x 3 net."""
+    pts = [c for j in range(3) for i in range(4) for c in (i, j, 0.0)]
+    pos, idx, _, _ = tessellate_nurbs(4, 3, [0, 0, 0, 0.5, 1, 1, 1], 0, 1, 3, 3, [0, 0, 0, 1, 1, 1], 0, 1, pts,
+                                      False, 8, 8)
+    assert np.abs(pos[:, 2]).max() < 1e-5
+    assert pos[:, 0].min() >= -1e-5 and pos[:, 0].max() <= 3.0 + 1e-4
+    assert abs(pos[0, 0]) < 1e-5 and abs(pos[0, 1]) < 1e-5
+    # Clamped at both ends: the far corner too; bases sum to one inside.
+    np.testing.assert_allclose(pos[-1], [3, 2, 0], atol=1e-5)
+    for t in np.linspace(0, 1, 9):
+        assert abs(bspline_basis([0, 0, 0, 0.5, 1, 1, 1], 4, 3, t).sum() - 1.0) < 1e-12
+
+
+def test_bspline_basis_is_the_textbook_one():
+    # Linear: N0 = 1 - t, N1 = t; quadratic Bezier-clamped: Bernstein polynomials.
+    for t in (0.0, 0.3, 0.999):
+        np.testing.assert_allclose(bspline_basis([0, 0, 1, 1], 2, 2, t), [1 - t, t], atol=1e-12)
+        np.testing.assert_allclose(bspline_basis([0, 0, 0, 1, 1, 1], 3, 3, t),
+                                   [(1 - t) ** 2, 2 * t * (1 - t), t * t], atol=1e-12)
+
+
+def test_rational_nurbs_circle_arc():
+    # A quarter circle as a rational quadratic (weights 1, sqrt(2)/2, 1), extruded in z.
+    w = np.sqrt(0.5)
+    row = [(1, 0, 1), (w * 1, w * 1, w), (0, 1, 1)]
+    pts = [c for z in (0.0, 1.0) for (x, y, ww) in row for c in (x, y, z * ww, ww)]
+    pos, _, _, _ = tessellate_nurbs(3, 3, [0, 0, 0, 1, 1, 1], 0, 1, 2, 2, [0, 0, 1, 1], 0, 1, pts, True, 8, 1)
+    np.testing.assert_allclose(np.hypot(pos[:, 0], pos[:, 1]), 1.0, atol=1e-6)
