@@ -884,13 +884,7 @@ class _Builder:
         elif name == "Polygon":
             self.polygon(vals)
         elif name == "GeneralPolygon":
-            nl = _as_numbers(vals[0]) if vals else None
-            p = _Params(vals, 1).numbers("P")
-            if nl and p:
-                n0 = int(nl[0])
-                if len(nl) > 1:
-                    self.warn("GeneralPolygon holes are not supported; using the outer loop")
-                self.polygon(["P", p[:3 * n0]])
+            self.general_polygon(vals)
         elif name in ("SubdivisionMesh", "HierarchicalSubdivisionMesh"):
             self.subdivision_mesh(name, vals)
         elif name in ("PatchMesh", "Patch"):
@@ -1207,6 +1201,35 @@ class _Builder:
             return
         pos, idx, nrm, st = mesh
         self.tessellated_mesh(pos, idx, nrm, st=st, displace=True)
+
+    def general_polygon(self, vals):
+        """general_polygon (scene_builder.rs:1413-1446): GeneralPolygon
+        [loop nverts] "P", ear-clipped with its holes bridged in."""
+        from .displace import smooth_normals
+        from .earclip import triangulate_with_holes
+        nl = _as_numbers(vals[0]) if vals else None
+        p = _Params(vals, 1).numbers("P")
+        if nl is None:
+            return
+        if p is None:
+            self.warn('GeneralPolygon without "P"; skipping')
+            return
+        pts = np.array(p[:len(p) // 3 * 3], dtype=np.float64).reshape(-1, 3)
+        loops, cur = [], 0
+        for n in nl:
+            n = int(n)
+            if cur + n > len(pts):
+                break
+            loops.append(pts[cur:cur + n])
+            cur += n
+        if not loops or len(loops[0]) < 3:
+            return
+        res = triangulate_with_holes(loops)
+        if res is None:
+            self.warn("GeneralPolygon: triangulation failed; skipping")
+            return
+        P = res[0].astype(np.float32)
+        self.tessellated_mesh(P, res[1], smooth_normals(P, res[1]), displace=True)
 
     def nu_patch(self, vals):
         """nu_patch (scene_builder.rs:1364-1411): NuPatch nu uorder [uknot]
