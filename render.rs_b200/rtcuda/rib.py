@@ -20,10 +20,10 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     Hyperboloid) and the emitter shapes of PxrSphereLight / PxrDiskLight
     are tessellated into smooth-normal triangle meshes; the reference
     intersects them analytically.
-  * SubdivisionMesh is diced by uniform Catmull-Clark and bilinear /
-    bicubic PatchMesh and Patch by the current Basis, as the reference
-    does, NuPatch NURBS untrimmed; Curves, Points, media and motion blur
-    are skipped (motion blocks use their first
+  * Bilinear / bicubic PatchMesh and Patch are diced by the current
+    Basis, as the reference does, NuPatch NURBS untrimmed;
+    SubdivisionMesh, GeneralPolygon, Curves, Points, media and motion blur
+    are skipped with a warning (motion blocks use their first
     sample); Displace "noise" moves polygon-mesh vertices at load time as
     the reference does; a PxrDomeLight lightColorMap is read when it is a
     Radiance .hdr (one map per scene).
@@ -551,7 +551,7 @@ class _State:
         self.bxdf = None         # material dict
         self.bxdf_bindings = []  # (field id, pattern node) of the active Bxdf
         self.displace = None     # Displace "noise" parameters (dict) for tessellated meshes
-        self.shading_rate = 1.0  # sets the subdivision level of SubdivisionMesh and the patch dicing
+        self.shading_rate = 1.0  # sets the patch dicing
         self.basis_u = ("bezier", None)  # Basis: (name or 16 numbers, step or None) per direction
         self.basis_v = ("bezier", None)
         self.identifier = None
@@ -883,10 +883,8 @@ class _Builder:
             self.pxr_light(vals)
         elif name == "Polygon":
             self.polygon(vals)
-        elif name == "GeneralPolygon":
-            self.general_polygon(vals)
-        elif name in ("SubdivisionMesh", "HierarchicalSubdivisionMesh"):
-            self.subdivision_mesh(name, vals)
+        elif name in ("GeneralPolygon", "SubdivisionMesh", "HierarchicalSubdivisionMesh"):
+            self.warn(f"{name} not supported; skipping")
         elif name in ("PatchMesh", "Patch"):
             self.patch_mesh(name, vals)
         elif name == "NuPatch":
@@ -1202,35 +1200,6 @@ class _Builder:
         pos, idx, nrm, st = mesh
         self.tessellated_mesh(pos, idx, nrm, st=st, displace=True)
 
-    def general_polygon(self, vals):
-        """general_polygon (scene_builder.rs:1413-1446): GeneralPolygon
-        [loop nverts] "P", ear-clipped with its holes bridged in."""
-        from .displace import smooth_normals
-        from .earclip import triangulate_with_holes
-        nl = _as_numbers(vals[0]) if vals else None
-        p = _Params(vals, 1).numbers("P")
-        if nl is None:
-            return
-        if p is None:
-            self.warn('GeneralPolygon without "P"; skipping')
-            return
-        pts = np.array(p[:len(p) // 3 * 3], dtype=np.float64).reshape(-1, 3)
-        loops, cur = [], 0
-        for n in nl:
-            n = int(n)
-            if cur + n > len(pts):
-                break
-            loops.append(pts[cur:cur + n])
-            cur += n
-        if not loops or len(loops[0]) < 3:
-            return
-        res = triangulate_with_holes(loops)
-        if res is None:
-            self.warn("GeneralPolygon: triangulation failed; skipping")
-            return
-        P = res[0].astype(np.float32)
-        self.tessellated_mesh(P, res[1], smooth_normals(P, res[1]), displace=True)
-
     def nu_patch(self, vals):
         """nu_patch (scene_builder.rs:1364-1411): NuPatch nu uorder [uknot]
         umin umax nv vorder [vknot] vmin vmax "P" | "Pw"; untrimmed."""
@@ -1258,68 +1227,6 @@ class _Builder:
             return
         pos, idx, nrm, st = mesh
         self.tessellated_mesh(pos, idx, nrm, st=st, displace=True)
-
-    def subdivision_mesh(self, name, vals):
-        """subdivision_mesh (scene_builder.rs:1236-1322): SubdivisionMesh
-        "scheme" [nverts] [verts] ([tags] [nargs] [ints] [floats]) params,
-        HierarchicalSubdivisionMesh with [strings] after [floats]; uniform
-        Catmull-Clark at the shading rate's level (rtcuda/subdiv.py)."""
-        from .subdiv import levels_for_shading_rate, tessellate as subdivide
-        scheme = _str(vals, 0)
-        if scheme is None:
-            return
-        if scheme != "catmull-clark":
-            self.warn(f'SubdivisionMesh scheme "{scheme}" treated as catmull-clark')
-        nverts = _as_numbers(vals[1]) if len(vals) > 1 else None
-        verts = _as_numbers(vals[2]) if len(vals) > 2 else None
-        if nverts is None or verts is None:
-            return
-        creases, corners, holes, interp = [], [], [], False
-        start = 3
-        if len(vals) > 3 and isinstance(vals[3], list) and all(isinstance(t, str) for t in vals[3]):
-            tags = vals[3]
-            nargs = (_as_numbers(vals[4]) if len(vals) > 4 else None) or []
-            ints = (_as_numbers(vals[5]) if len(vals) > 5 else None) or []
-            floats = (_as_numbers(vals[6]) if len(vals) > 6 else None) or []
-            ic = fc = 0
-            for ti, tag in enumerate(tags):
-                ni = int(nargs[2 * ti]) if 2 * ti < len(nargs) else 0
-                nf = int(nargs[2 * ti + 1]) if 2 * ti + 1 < len(nargs) else 0
-                ti_ints, ti_floats = ints[ic:ic + ni], floats[fc:fc + nf]
-                if tag == "crease":
-                    sharp = ti_floats[0] if ti_floats else 10.0
-                    creases += [(int(a), int(b), sharp) for a, b in zip(ti_ints, ti_ints[1:])]
-                elif tag == "corner":
-                    for i, v in enumerate(ti_ints):
-                        corners.append((int(v), ti_floats[i] if i < len(ti_floats) else
-                                        (ti_floats[0] if ti_floats else 10.0)))
-                elif tag == "hole":
-                    holes += [int(f) for f in ti_ints]
-                elif tag == "interpolateboundary":
-                    interp = True
-                else:
-                    self.warn(f'SubdivisionMesh tag "{tag}" not supported; ignoring')
-                ic += ni
-                fc += nf
-            start = 8 if name == "HierarchicalSubdivisionMesh" else 7
-        p = _Params(vals, start).numbers("P")
-        if p is None:
-            self.warn("SubdivisionMesh without \"P\"; skipping")
-            return
-        faces, cur = [], 0
-        for nv in nverts:
-            nv = int(nv)
-            if cur + nv > len(verts):
-                break
-            faces.append([int(v) for v in verts[cur:cur + nv]])
-            cur += nv
-        P = np.array(p, dtype=np.float64).reshape(-1, 3)
-        if any(v >= len(P) for f in faces for v in f):
-            raise RibError(f"{name}: vertex index out of range")
-        pos, idx, nrm = subdivide(P, faces, levels_for_shading_rate(self.state.shading_rate), creases, corners,
-                                  holes, interp)
-        if len(idx):
-            self.tessellated_mesh(pos, idx, nrm, displace=True)
 
     def light_source(self, vals):
         """parse_light (scene_builder.rs:1582-1635): positions untransformed."""
@@ -1438,29 +1345,6 @@ class _Builder:
         s.pixel_samples = self.pixel_samples
         s.warnings = list(self.warned)
         return s
-
-
-def _rib_value(v):
-    if isinstance(v, str):
-        return '"' + v.replace("\\", "\\\\").replace('"', '\\"') + '"'
-    if isinstance(v, list):
-        if v and all(isinstance(x, str) for x in v):
-            return "[" + " ".join(_rib_value(x) for x in v) + "]"
-        return "[" + " ".join(repr(float(x)) for x in v) + "]"
-    return repr(float(v))  # the shortest text that reads back to the same double
-
-
-def format_rib(requests):
-    """RIB text of a request list (name, values) as parse_rib returns it:
-    what the reference's `catrib` writes for a translated scene."""
-    out, depth = [], 0
-    for name, vals in requests:
-        if name in ("AttributeEnd", "WorldEnd", "TransformEnd"):
-            depth = max(depth - 1, 0)
-        out.append("  " * depth + " ".join([name] + [_rib_value(v) for v in vals]))
-        if name in ("AttributeBegin", "WorldBegin", "TransformBegin"):
-            depth += 1
-    return "\n".join(out) + "\n"
 
 
 def load_rib_string(text, base_dir=None):

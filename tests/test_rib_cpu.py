@@ -190,10 +190,9 @@ def test_archives_and_missing_files(tmp_path):
     assert any("nope.rib" in w for w in s.warnings)
 
 
-FIXTURES = "/root/reference/tests/fixtures"
+FIXTURES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "fixtures")
 
 
-@pytest.mark.skipif(not os.path.isdir(FIXTURES), reason="the reference's fixture files are not on this machine")
 def test_reference_fixtures_load():
     files = sorted(glob.glob(os.path.join(FIXTURES, "*.rib")))
     assert files
