@@ -14,6 +14,10 @@
  *  - A session owns all of its device memory and one CUDA stream; calls are
  *    synchronous on that stream. One session per host thread (the reference's
  *    PtSession is not Send, renderer.rs:256-259).
+ *  - A session lives on the device that was current when it was created.
+ *    Every call that takes a session makes that device current for its
+ *    duration and restores the caller's current device before returning,
+ *    so sessions on several GPUs can be driven from one thread.
  *  - Output buffers are caller-allocated host memory unless the name says
  *    `_device`.
  *  - Seeding is per (pixel, sample) exactly as Pcg32::for_pixel_sample
@@ -141,9 +145,12 @@ int rt_intersect_batch_device(rt_session* s, const float* rays, uint64_t n, int 
  * error word live in a fixed static device array of RT_NOALLOC_MAX_RAYS rays
  * (about 2.9 MB), reserved on every GPU that loads the library until the
  * process exits; nothing is allocated or freed per call. n beyond
- * RT_NOALLOC_MAX_RAYS is rejected with RT_ERR_INVALID. The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current, so make that first call before any stream capture.
+ * RT_NOALLOC_MAX_RAYS is rejected with RT_ERR_INVALID. The call runs on the
+ * session's device (as every session call does); the first call on a device
+ * looks up the array's device address there (cudaGetSymbolAddress), so make
+ * that first call before any stream capture. Each call copies the host rays
+ * in and the results out and waits for the session's stream before it
+ * returns.
  * All calls share the one array: calls that overlap on the GPU (from several
  * threads or sessions on the same device) race on it and must be serialised
  * by the caller. No counterpart in the reference: its Metal backend has no

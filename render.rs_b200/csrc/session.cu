@@ -11,6 +11,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -77,6 +78,37 @@ int fail(int code, const std::string& msg) {
         }                                                                                      \
     } while (0)
 
+// The text of a device error word (RT_DEVERR_* bits), shared by every
+// entry point that reads one.
+std::string device_error_text(uint32_t e) {
+    std::string t = "device reported";
+    if (e & RT_DEVERR_STACK) t += " traversal stack overflow";
+    if (e & RT_DEVERR_ITER) t += " traversal step limit";
+    if (e & ~(RT_DEVERR_STACK | RT_DEVERR_ITER)) t += " error bits " + std::to_string(e);
+    return t;
+}
+
+// Makes a session's device current for the duration of an entry point and
+// restores the caller's device afterwards, so a session created on one GPU
+// runs there whatever device the calling thread has current.
+struct DeviceScope {
+    int prev = -1;
+    cudaError_t status = cudaSuccess;
+    explicit DeviceScope(int dev) {
+        status = cudaGetDevice(&prev);
+        if (status == cudaSuccess && prev != dev) status = cudaSetDevice(dev);
+        else prev = -1;
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+#define SESSION_DEVICE(s)                                                                      \
+    DeviceScope dev_scope_((s)->device);                                                       \
+    if (dev_scope_.status != cudaSuccess)                                                      \
+        return fail(RT_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(dev_scope_.status))
+
 #ifndef RT_TRAV_BLOCK
 #define RT_TRAV_BLOCK 128
 #endif
@@ -109,6 +141,7 @@ struct rt_session {
     DevScene S{};
     rt_params params{};
     cudaStream_t stream = nullptr;
+    int device = 0;                // the device the session was created on; every call runs there
     int sm_count = 148;
     std::vector<void*> allocs;
     uint64_t device_bytes = 0;
@@ -168,13 +201,12 @@ struct rt_session {
         if (e) {
             cudaMemsetAsync(err, 0, 4, stream);
             cudaStreamSynchronize(stream);
-            return fail(RT_ERR_DEVICE, std::string("device reported ") +
-                                           ((e & RT_DEVERR_STACK) ? "traversal stack overflow " : "") +
-                                           ((e & RT_DEVERR_ITER) ? "traversal step limit " : ""));
+            return fail(RT_ERR_DEVICE, device_error_text(e));
         }
         return RT_OK;
     }
     ~rt_session() {
+        DeviceScope scope(device);
         if (stream) cudaStreamSynchronize(stream);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
@@ -212,6 +244,7 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
         delete s;
         return fail(RT_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(de));
     }
+    s->device = dev;
     cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, dev);
     {
         // Persistent traversal grids: every resident block slot on every SM.
@@ -400,6 +433,7 @@ int rt_set_adaptive(rt_session* s, double tol) {
 
 int rt_average_spp(rt_session* s, double* out) {
     if (!s || !out) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     std::vector<double> a(4ull * s->npix);
     int rc = rt_read_accum(s, a.data());
     if (rc) return rc;
@@ -411,6 +445,7 @@ int rt_average_spp(rt_session* s, double* out) {
 
 int rt_reset(rt_session* s) {
     if (!s) return fail(RT_ERR_INVALID, "session is NULL");
+    SESSION_DEVICE(s);
     CUDA_TRY(cudaMemsetAsync(s->accum, 0, 32ull * s->npix, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->lum_stats, 0, 32ull * s->npix, s->stream));
     if (s->params.aovs) CUDA_TRY(cudaMemsetAsync(s->aux, 0, 48ull * s->npix, s->stream));
@@ -421,6 +456,7 @@ int rt_reset(rt_session* s) {
 
 int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     if (!s) return fail(RT_ERR_INVALID, "session is NULL");
+    SESSION_DEVICE(s);
     if (count == 0) return RT_OK;
     cudaStream_t st = s->stream;
     Paths& P = s->paths;
@@ -583,6 +619,7 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
 
 int rt_read_accum(rt_session* s, double* rgbw) {
     if (!s || !rgbw) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     CUDA_TRY(cudaMemcpyAsync(rgbw, s->accum, 32ull * s->npix, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
     return RT_OK;
@@ -590,6 +627,7 @@ int rt_read_accum(rt_session* s, double* rgbw) {
 
 int rt_read_image(rt_session* s, float* rgb) {
     if (!s || !rgb) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     // Resolve on the device into the shadow-ray origin buffer (free between
     // renders; at least 16 B per pixel), then copy 12 B per pixel.
     float* img = reinterpret_cast<float*>(s->paths.sh_o);
@@ -602,6 +640,7 @@ int rt_read_image(rt_session* s, float* rgb) {
 
 int rt_read_aux(rt_session* s, float* aux12) {
     if (!s || !aux12) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     if (!s->params.aovs) return fail(RT_ERR_INVALID, "session was created with aovs = 0");
     CUDA_TRY(cudaMemcpyAsync(aux12, s->aux, 48ull * s->npix, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));
@@ -610,6 +649,7 @@ int rt_read_aux(rt_session* s, float* aux12) {
 
 int rt_checkpoint_save(rt_session* s, const char* path) {
     if (!s || !path) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     std::vector<double> a(4ull * s->npix);
     int rc = rt_read_accum(s, a.data());
     if (rc) return rc;
@@ -628,6 +668,7 @@ int rt_checkpoint_save(rt_session* s, const char* path) {
 
 int rt_read_film(rt_session* s, float* film) {
     if (!s || !film) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     if (!s->params.aovs) return fail(RT_ERR_INVALID, "the session was created without AOVs (params.aovs = 0)");
     float* d = nullptr;
     CUDA_TRY(pool_alloc((void**)&d, 4ull * RT_FILM_FLOATS * s->npix, s->stream));
@@ -643,6 +684,7 @@ int rt_read_film(rt_session* s, float* film) {
 
 int rt_denoise(rt_session* s, float* rgb) {
     if (!s || !rgb) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     if (!s->params.aovs) return fail(RT_ERR_INVALID, "the session was created without AOVs (params.aovs = 0)");
     float *d = nullptr, *o = nullptr;
     CUDA_TRY(pool_alloc((void**)&d, 4ull * RT_FILM_FLOATS * s->npix, s->stream));
@@ -660,6 +702,7 @@ int rt_denoise(rt_session* s, float* rgb) {
 
 int rt_checkpoint_save_rckp(rt_session* s, const char* path) {
     if (!s || !path) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     std::vector<double> a(4ull * s->npix);
     int rc = rt_read_accum(s, a.data());
     if (rc) return rc;
@@ -668,6 +711,7 @@ int rt_checkpoint_save_rckp(rt_session* s, const char* path) {
 
 int rt_checkpoint_load(rt_session* s, const char* path, uint32_t* samples_done) {
     if (!s || !path) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     FILE* f = fopen(path, "rb");
     if (!f) return fail(RT_ERR_IO, std::string("cannot open ") + path);
     uint32_t hdr[4];
@@ -704,6 +748,7 @@ int rt_checkpoint_load(rt_session* s, const char* path, uint32_t* samples_done) 
 int rt_intersect_batch_device(rt_session* s, const float* rays, uint64_t n, int any_hit, uint32_t* prim,
                               uint32_t* inst, float* t, void* stream) {
     if (!s || (!rays && n) || (!prim && n)) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     if (n >= 0xFFFFFFFFull - 64) return fail(RT_ERR_INVALID, "batch larger than 2^32 rays");
     if (((uintptr_t)rays & 15u) != 0) return fail(RT_ERR_INVALID, "rays must be 16-byte aligned");
     if (n == 0) return RT_OK;
@@ -723,6 +768,7 @@ int rt_intersect_batch_device(rt_session* s, const float* rays, uint64_t n, int 
 int rt_intersect_batch(rt_session* s, const float* rays, uint64_t n, int any_hit, uint32_t* prim, uint32_t* inst,
                        float* t) {
     if (!s || (!rays && n) || (!prim && n)) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     if (n == 0) return RT_OK;
     size_t need = n * (32 + 12);
     if (need > s->batch_cap) {
@@ -754,8 +800,8 @@ int rt_intersect_batch(rt_session* s, const float* rays, uint64_t n, int any_hit
 // buffer it grows with cudaMalloc, plus a work counter and an error word.
 // rt_intersect_batch_noalloc keeps all of that in this file-scope array
 // instead: RT_NOALLOC_MAX_RAYS rays of staging (32 B in, 12 B out each) and
-// two counter words, 2,883,648 bytes in all, held by every GPU that loads the
-// library until the process exits.
+// two counter words (padded to 64), 2,883,840 bytes in all, held by every GPU
+// that loads the library until the process exits.
 namespace {
 constexpr uint64_t NOALLOC_IN = 8ull * RT_NOALLOC_MAX_RAYS;       // floats: two planes of float4
 constexpr uint64_t NOALLOC_OUT = 3ull * RT_NOALLOC_MAX_RAYS;      // prim, inst, t (32-bit each)
@@ -767,19 +813,23 @@ namespace {
 // Device address of g_noalloc_scratch per device. Host code cannot use the
 // array's name as a device address; cudaGetSymbolAddress gives it, once per
 // device, with that device current.
+// Threads that make their first call on a device at the same time may both
+// look the address up; the atomic store makes that benign.
 constexpr int NOALLOC_MAX_DEVICES = 64;
-uint32_t* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+std::atomic<uint32_t*> g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
 
 int noalloc_scratch(uint32_t** out) {
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(RT_ERR_INVALID, "device index beyond the no-alloc table");
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_noalloc_ptr[dev] = (uint32_t*)p;
+    uint32_t* p = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+    if (!p) {
+        void* v = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&v, g_noalloc_scratch));
+        p = (uint32_t*)v;
+        g_noalloc_ptr[dev].store(p, std::memory_order_release);
     }
-    *out = g_noalloc_ptr[dev];
+    *out = p;
     return RT_OK;
 }
 }  // namespace
@@ -787,6 +837,7 @@ int noalloc_scratch(uint32_t** out) {
 extern "C" int rt_intersect_batch_noalloc(rt_session* s, const float* rays, uint64_t n, int any_hit, uint32_t* prim,
                                           uint32_t* inst, float* t) {
     if (!s || (!rays && n) || (!prim && n)) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
     if (n > RT_NOALLOC_MAX_RAYS)
         return fail(RT_ERR_INVALID, "rt_intersect_batch_noalloc: " + std::to_string(n) + " rays exceed its fixed " +
                                         std::to_string(RT_NOALLOC_MAX_RAYS) + "-ray staging area");
@@ -820,7 +871,7 @@ extern "C" int rt_intersect_batch_noalloc(rt_session* s, const float* rays, uint
     if (!any_hit && t) CUDA_TRY(cudaMemcpyAsync(t, d_t, 4 * n, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaMemcpyAsync(&e, d_err, 4, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    if (e) return fail(RT_ERR_DEVICE, "device reported a traversal overrun");
+    if (e) return fail(RT_ERR_DEVICE, device_error_text(e));
     return RT_OK;
 }
 

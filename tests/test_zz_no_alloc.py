@@ -68,3 +68,22 @@ def test_noalloc_rejects_oversized_batch(cloud_session):
     rc, _, _, _ = _noalloc(cloud_session, rays, False)
     assert rc == -1
     assert "exceed" in backend.lib().rt_last_error().decode()
+
+
+def test_noalloc_allocates_nothing(cloud_session):
+    """After one warm-up call, further calls leave the device's free memory
+    and the session's own device bytes unchanged."""
+    import torch
+    g = cloud_session
+    rays = scenes.triangle_cloud_rays(MAX_RAYS, seed=33)
+    rc, _, _, _ = _noalloc(g, rays, False)
+    assert rc == 0, backend.lib().rt_last_error()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    held0 = g.stats()["device_bytes"]
+    for any_hit in (False, True, False, True, False):
+        rc, _, _, _ = _noalloc(g, rays, any_hit)
+        assert rc == 0, backend.lib().rt_last_error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    assert g.stats()["device_bytes"] == held0
