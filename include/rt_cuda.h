@@ -191,6 +191,30 @@ int rt_get_stats(rt_session* s, rt_stats* out);
 int rt_bsdf_furnace(const rt_material_desc* material, const double* wo, double eta, uint64_t n,
                     uint64_t seed, double* out);
 
+/* Diagnostics: the device functions the render kernels use, run on caller
+ * inputs, so tests can compare them one by one with the reference's
+ * functions. Host pointers; each call stages through device memory and
+ * waits for its result.
+ *  - rt_pcg_streams: the first n u32 draws of the generator of (pixel[i],
+ *    sample[i]) for i < m, n per row of `out` (Pcg32::for_pixel_sample and
+ *    next_u32, src/raytracer/pt/sampler.rs:24-42); runs on the current device.
+ *  - rt_light_sample_batch: the light the session's light BVH picks at
+ *    points[3i..3i+3) with the uniform u[i], and its pick probability
+ *    (LightSampler::sample, src/scene/light_sampler.rs:150-211); light
+ *    0xFFFFFFFF and pmf 0 when the scene has no lights.
+ *  - rt_light_pmf_batch: the probability of picking light[i] at points[i]
+ *    (LightSampler::pmf, light_sampler.rs:213-238).
+ *  - rt_transmittance_batch: the shadow kernel's transmittance of rays in
+ *    rt_intersect_batch's layout (direction and distance tmax): the product
+ *    of (1 - presence) over the cutout surfaces crossed before tmax, 0 when
+ *    an opaque surface is crossed or the product falls below 1e-4
+ *    (transmittance, src/raytracer/pt/mod.rs:1254-1306). */
+int rt_pcg_streams(const uint64_t* pixel, const uint64_t* sample, uint32_t m, uint32_t n, uint32_t* out);
+int rt_light_sample_batch(rt_session* s, const float* points, const float* u, uint32_t m,
+                          uint32_t* light, float* pmf);
+int rt_light_pmf_batch(rt_session* s, const float* points, const uint32_t* light, uint32_t m, float* pmf);
+int rt_transmittance_batch(rt_session* s, const float* rays, uint64_t n, float* trans);
+
 /* The session's CUDA stream (a cudaStream_t), for callers that time or
  * order work against it. */
 void* rt_session_stream(rt_session* s);

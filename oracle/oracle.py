@@ -53,6 +53,7 @@ def lib():
         L.oracle_intersect_st.argtypes = [vp, C.c_uint64, vp, vp]
         L.oracle_texture_sample.argtypes = [C.c_uint32, C.c_uint32, vp, C.c_int, C.c_uint64, vp, vp]
         L.oracle_ies_eval.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp, C.c_uint64, vp, vp, vp]
+        L.oracle_transmittance.argtypes = [vp, vp, C.c_uint64, vp, C.c_int]
         L.oracle_light_pmf.restype = C.c_double
         L.oracle_light_pmf.argtypes = [vp, f64p, C.c_uint32]
         _lib = L
@@ -137,6 +138,15 @@ class OracleScene:
         lib().oracle_intersect(self.h, planes.ctypes.data, n, 1 if any_hit else 0, prim.ctypes.data,
                                inst.ctypes.data, t.ctypes.data, C.byref(c), threads)
         return prim, inst, t, c
+
+    def transmittance(self, planes, threads=0):
+        """Shadow-ray transmittance (mod.rs:1254-1306) of rays in the
+        two-plane layout; (n, 3) RGB."""
+        planes = np.ascontiguousarray(planes, dtype=np.float32)
+        n = planes.shape[1]
+        out = np.zeros((n, 3))
+        lib().oracle_transmittance(self.h, planes.ctypes.data, n, out.ctypes.data, threads)
+        return out
 
     def render(self, params, s0, s1, pixels=None, aovs=False, threads=0):
         """Radiance sums over samples [s0, s1) (and AOV sums) for a pixel list;

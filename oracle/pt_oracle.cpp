@@ -2409,6 +2409,27 @@ void oracle_pattern_eval(const rt_scene_desc* d, uint32_t node, uint64_t n, cons
     }
 }
 
+// Shadow-ray transmittance (mod.rs:1254-1306, Tracer::transmittance) of
+// rays in rt_intersect_batch's two-plane layout: from each origin along the
+// normalised direction for the distance tmax; one RGB transmittance each.
+void oracle_transmittance(const oracle_scene* os, const float* planes, uint64_t n, double* out, int threads) {
+    const Scene& s = os->s;
+    rt_params prm{};
+    int nt = threads <= 0 ? (int)std::max(1u, std::thread::hardware_concurrency()) : threads;
+    parallel_for(n, nt, [&](uint64_t b, uint64_t e, int) {
+        Tracer tr{s, prm, 0, 0, Counters{}, Counters{}};
+        for (uint64_t i = b; i < e; i++) {
+            const float* po = planes + 4 * i;
+            const float* pd = planes + 4 * n + 4 * i;
+            V3 o{po[0], po[1], po[2]}, d{pd[0], pd[1], pd[2]};
+            V3 v = tr.transmittance(o, normalize(d), pd[3]);
+            out[3 * i] = v.x;
+            out[3 * i + 1] = v.y;
+            out[3 * i + 2] = v.z;
+        }
+    });
+}
+
 void oracle_intersect_st(const oracle_scene* os, uint64_t n, const double* rays, double* out) {
     for (uint64_t i = 0; i < n; i++) {
         const double* r = rays + 6 * i;

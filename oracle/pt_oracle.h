@@ -89,6 +89,9 @@ void   oracle_env_sample(uint32_t w, uint32_t h, const float* rgb, uint64_t n, c
 // point (13 doubles); rgb = 3 per point.
 void   oracle_pattern_eval(const rt_scene_desc* d, uint32_t node, uint64_t n, const double* ctx, double* rgb);
 // Closest hit of n rays (o, d: 6 doubles each): (t or -1, s, t, st density).
+/* Shadow-ray transmittance (mod.rs:1254-1306) of rays in the two-plane
+ * layout (origin; direction, distance): RGB per ray. */
+void   oracle_transmittance(const oracle_scene* s, const float* planes, uint64_t n, double* out, int threads);
 void   oracle_intersect_st(const oracle_scene* s, uint64_t n, const double* rays, double* out);
 // texture/cache.rs lookups on the mip chain of one w x h RGB texture: per
 // query 7 doubles (s, t, footprint, -, -, -, 0) for the trilinear `sample`

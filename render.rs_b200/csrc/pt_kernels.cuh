@@ -79,6 +79,7 @@ struct Paths {
 
 struct PtConsts {
     uint32_t npix, width, max_depth, rr_start, aovs;
+    uint32_t pres_in_trav;  // cutouts are decided inside k_extend's traversal; k_shade skips none
     float clamp;
     uint64_t sample0;  // first sample index of the slab
     uint32_t guided;
@@ -450,7 +451,8 @@ __global__ void k_guide_keep(const uint32_t* tb_cnt, float scale, uint32_t cap, 
 // from the global work counter as soon as half the warp is idle (one
 // warp-aggregated atomic per refill), so a few long rays no longer hold a
 // warp's other lanes hostage (Aila & Laine 2009, "persistent while-while").
-// load(j, o, d, tmax) reads work item j; finish(done, j, ts) is called by
+// load(j, o, d, tmax, seed) reads work item j (seed: the ray's presence
+// seed, see leaf_coop); finish(done, j, ts) is called by
 // the whole warp whenever some lane finished, with `done` true on those lanes.
 // Within a warp the work alternates between a node phase (every lane that
 // has no parked leaf tests nodes until it parks one or finishes) and a leaf
@@ -482,12 +484,13 @@ __global__ void k_guide_keep(const uint32_t* tb_cnt, float scale, uint32_t cap, 
 #ifndef RT_INST_IN_NODE_PHASE
 #define RT_INST_IN_NODE_PHASE 0
 #endif
-template <bool ANY, bool TRANSMIT = false, class Load, class Finish>
+template <bool ANY, bool TRANSMIT = false, bool PRES = false, class Load, class Finish>
 __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                          TravStack& st, LeafShared& leaf, Load load, Finish finish) {
     PhaseState ps;
     bool active = false, exhausted = false;
     uint32_t item = 0, steps = 0;
+    uint64_t ray_seed = 0;  // PRES: the current ray's presence seed
     const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
     for (;;) {
         uint32_t act = __ballot_sync(0xFFFFFFFFu, active);
@@ -504,8 +507,10 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
                     item = j;
                     float3 o, d;
                     float tmax;
-                    load(j, o, d, tmax);
+                    uint64_t seed = 0;
+                    load(j, o, d, tmax, seed);
                     active = trav_begin(S, ps.ts, st, o, d, tmax);
+                    if (PRES) ray_seed = seed;
                     if (active) {
                         phase_begin(ps);
                         steps = 0;
@@ -556,14 +561,16 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
         bool done_now = false;
         if (active && ps.pending && !ps.ts.in_inst) done_now = op_leaf<ANY>(S, ps, st, err);
         const bool tri_leaf = active && !done_now && ps.pending && ps.ts.in_inst;
-        if (__any_sync(0xFFFFFFFFu, tri_leaf)) done_now |= leaf_coop<ANY, TRANSMIT>(S, ps, tri_leaf, leaf);
+        if (__any_sync(0xFFFFFFFFu, tri_leaf)) done_now |= leaf_coop<ANY, TRANSMIT, PRES>(S, ps, tri_leaf, leaf, ray_seed);
         if (__any_sync(0xFFFFFFFFu, done_now)) finish(done_now, item, ps.ts);
         if (done_now) active = false;
     }
 }
 
 // ---- extend ---------------------------------------------------------------------------
-template <int BLOCK>
+// `pres`: cutout surfaces are passed through inside the traversal
+// (leaf_coop, PRES) instead of by the shade kernel's skip waves.
+template <int BLOCK, bool PRES>
 __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S, Paths P, uint32_t qsel) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
     __shared__ LeafShared leaf_sh[BLOCK / 32];
@@ -573,12 +580,19 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S
     const uint32_t n = P.cnt[CNT_EXT_IN];
     unsigned long long rays = 0;
     uint32_t slot = 0;
-    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
         slot = q[j];
         float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot];
         o = xyz(o4);
         d = xyz(d4);
         tmax = d4.w;
+        if (PRES) {
+            // The path's random state at this bounce, hashed: a seed no
+            // other ray of the render shares.
+            const uint4 rs = P.rng[slot];
+            seed = splitmix(((uint64_t)rs.x | ((uint64_t)rs.y << 32)) ^
+                            (((uint64_t)rs.z | ((uint64_t)rs.w << 32)) * 0x9E3779B97F4A7C15ull));
+        }
     };
     auto finish = [&](bool done, uint32_t, const TravState& ts) {
         uint32_t cls = CLS_MISS;
@@ -595,7 +609,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S
         for (uint32_t c = 0; c < N_QUEUES; c++)
             push_queue(P.q_cls + (size_t)c * P.P, &P.cnt[CNT_CLASS + c], slot, done && cls == c);
     };
-    ray_pump<false>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+    ray_pump<false, false, PRES>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
     if (rays) atomicAdd(&P.stats[0], rays);
 }
 
@@ -887,7 +901,8 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                 }
                 uint32_t skips = (flags & FL_SKIP_MASK) >> FL_SKIP_SHIFT;
                 bool done = false;
-                if (m.presence < 1.0f && rng.next_f() >= m.presence && skips < RT_MAX_PRESENCE_SKIPS) {
+                if (!C.pres_in_trav && m.presence < 1.0f && rng.next_f() >= m.presence &&
+                    skips < RT_MAX_PRESENCE_SKIPS) {
                     // Presence cutout: pass straight through, no bounce.
                     flags = (flags & ~FL_SKIP_MASK) | ((skips + 1) << FL_SKIP_SHIFT);
                     travel += eucl;
@@ -1054,7 +1069,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
     if (!S.any_presence) {
         // Opaque scenes: one any-hit query per shadow ray, through the pump.
         uint32_t slot = 0;
-        auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
+        auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
             slot = P.q_sh[j];
             float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
             o = xyz(o4);
@@ -1074,7 +1089,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
     // (traverse.cuh: one traversal per shadow ray, cutouts attenuate, opaque
     // surfaces block).
     uint32_t slot = 0;
-    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
         slot = P.q_sh[j];
         float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
         o = xyz(o4);
@@ -1170,7 +1185,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_intersect(DevScen
     __shared__ LeafShared leaf_sh[BLOCK / 32];
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
-    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax) {
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
         float4 o4 = __ldg(org + j), d4 = __ldg(dir + j);
         o = xyz(o4);
         d = xyz(d4);
@@ -1194,6 +1209,63 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_intersect(DevScen
         }
     };
     ray_pump<ANY>(S, (uint32_t)n, fetch, err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+}
+
+// ---- diagnostics: the device functions the render kernels use, on caller inputs ----------
+// Transmittance of caller rays through the shadow kernel's query
+// (rt_transmittance_batch): the same pump and cooperative leaves as k_shadow
+// in scenes with presence cutouts.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_transmit_batch(DevScene S, const float4* __restrict__ org,
+                                                          const float4* __restrict__ dir, uint64_t n, float* out,
+                                                          uint32_t* fetch, uint32_t* err) {
+    __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    __shared__ LeafShared leaf_sh[BLOCK / 32];
+    TravStack st;
+    st.init(stack_sh + threadIdx.x, BLOCK);
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
+        float4 o4 = __ldg(org + j), d4 = __ldg(dir + j);
+        o = xyz(o4);
+        d = xyz(d4);
+        tmax = d4.w;
+    };
+    auto finish = [&](bool done, uint32_t i, const TravState& ts) {
+        if (done) out[i] = ts.trans;
+    };
+    ray_pump<true, true>(S, (uint32_t)n, fetch, err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+}
+
+// The first n u32 draws of Pcg32::for_pixel_sample(pixel[i], sample[i]).
+__global__ void k_pcg_streams(const uint64_t* __restrict__ pixel, const uint64_t* __restrict__ sample, uint32_t m,
+                              uint32_t n, uint32_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    Pcg r = pcg_for_pixel_sample(pixel[i], sample[i]);
+    for (uint32_t k = 0; k < n; k++) out[(size_t)i * n + k] = r.next_u32();
+}
+
+// Light-BVH pick (light_sample) at points p with uniforms u; light ~0 when
+// the scene has no lights.
+__global__ void k_light_sample_batch(DevScene S, const float* __restrict__ p, const float* __restrict__ u, uint32_t m,
+                                     uint32_t* __restrict__ light, float* __restrict__ pmf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    uint32_t li = 0xFFFFFFFFu;
+    float pm = 0.0f;
+    if (!light_sample(S, f3(p[3 * i], p[3 * i + 1], p[3 * i + 2]), u[i], li, pm)) {
+        li = 0xFFFFFFFFu;
+        pm = 0.0f;
+    }
+    light[i] = li;
+    pmf[i] = pm;
+}
+
+// Light-BVH pick probability (light_pmf) of light[i] at p[i].
+__global__ void k_light_pmf_batch(DevScene S, const float* __restrict__ p, const uint32_t* __restrict__ light,
+                                  uint32_t m, float* __restrict__ pmf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    pmf[i] = light_pmf(S, f3(p[3 * i], p[3 * i + 1], p[3 * i + 2]), light[i]);
 }
 
 // White-furnace estimator of one material: per thread, `per` BSDF samples

@@ -249,7 +249,7 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     {
         // Persistent traversal grids: every resident block slot on every SM.
         int nb = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<TRAV_BLOCK>, TRAV_BLOCK, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_extend<TRAV_BLOCK, false>, TRAV_BLOCK, 0);
         s->trav_grid = s->sm_count * std::max(nb, 1);
     }
     cudaError_t ce = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
@@ -474,7 +474,12 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     C.lum_stats = s->lum_stats;
     uint64_t guide_records = 0;
     int guide_trainings = 0;
-    uint32_t waves = s->params.max_depth + (s->S.any_presence ? RT_MAX_PRESENCE_SKIPS : 0u);
+    // Cutouts: decided inside the extension traversal, except when AOVs are
+    // kept, whose first-hit values come from the first surface a camera ray
+    // meets even when it passes through it (pt/mod.rs:690-700); then the
+    // shade kernel skips surfaces as the reference does, in extra waves.
+    C.pres_in_trav = (s->S.any_presence && !s->params.aovs) ? 1u : 0u;
+    uint32_t waves = s->params.max_depth + (s->S.any_presence && !C.pres_in_trav ? RT_MAX_PRESENCE_SKIPS : 0u);
     const int trav_grid = s->trav_grid, shade_grid = s->sm_count * 8;
     const uint32_t batch = 1u << 16;  // training records per Adam step
     CUDA_TRY(cudaMemsetAsync(s->stats, 0, 32, st));
@@ -524,7 +529,8 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
         for (uint32_t w = 0; w < waves; w++) {
             uint32_t qin = w & 1u, qout = qin ^ 1u;
             CUDA_TRY(cudaEventRecord(s->evpool[ei], st));
-            k_extend<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
+            if (C.pres_in_trav) k_extend<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
+            else k_extend<TRAV_BLOCK, false><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 1], st));
             if (s->guide) {
                 // Network inputs for this wave's guided vertices, then inference.
@@ -899,6 +905,104 @@ int rt_bsdf_furnace(const rt_material_desc* material, const double* wo, double e
     double total = (double)(per * nt);
     for (int c = 0; c < 4; c++) out[c] = acc[c] / total;
     return RT_OK;
+}
+
+int rt_pcg_streams(const uint64_t* pixel, const uint64_t* sample, uint32_t m, uint32_t n, uint32_t* out) {
+    if ((!pixel || !sample || !out) && m && n) return fail(RT_ERR_INVALID, "NULL argument");
+    if (!m || !n) return RT_OK;
+    if ((uint64_t)m * n > (1ull << 31)) return fail(RT_ERR_INVALID, "rt_pcg_streams: more than 2^31 draws");
+    void* d = nullptr;
+    const size_t bytes = 16ull * m + 4ull * m * n;
+    CUDA_TRY(cudaMalloc(&d, bytes));
+    uint64_t* dp = (uint64_t*)d;
+    uint64_t* ds = dp + m;
+    uint32_t* dout = (uint32_t*)(ds + m);
+    cudaError_t e = cudaMemcpy(dp, pixel, 8ull * m, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ds, sample, 8ull * m, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_pcg_streams<<<(m + 127) / 128, 128>>>(dp, ds, m, n, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, 4ull * m * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(RT_ERR_CUDA, std::string("rt_pcg_streams: ") + cudaGetErrorString(e));
+    return RT_OK;
+}
+
+// Staging for the session diagnostics below: one pool block on the
+// session's stream, freed before returning.
+namespace {
+struct Staging {
+    rt_session* s;
+    void* p = nullptr;
+    explicit Staging(rt_session* s_) : s(s_) {}
+    cudaError_t get(size_t bytes) { return pool_alloc(&p, bytes, s->stream); }
+    ~Staging() {
+        if (p) {
+            pool_free(p, s->stream);
+            cudaStreamSynchronize(s->stream);
+        }
+    }
+};
+}  // namespace
+
+int rt_light_sample_batch(rt_session* s, const float* points, const float* u, uint32_t m, uint32_t* light,
+                          float* pmf) {
+    if (!s || ((!points || !u || !light || !pmf) && m)) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
+    if (!m) return RT_OK;
+    Staging g(s);
+    CUDA_TRY(g.get(24ull * m));
+    float* dp = (float*)g.p;
+    float* du = dp + 3ull * m;
+    uint32_t* dl = (uint32_t*)(du + m);
+    float* dm = (float*)(dl + m);
+    CUDA_TRY(cudaMemcpyAsync(dp, points, 12ull * m, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(du, u, 4ull * m, cudaMemcpyHostToDevice, s->stream));
+    k_light_sample_batch<<<(m + 127) / 128, 128, 0, s->stream>>>(s->S, dp, du, m, dl, dm);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(light, dl, 4ull * m, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(pmf, dm, 4ull * m, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return RT_OK;
+}
+
+int rt_light_pmf_batch(rt_session* s, const float* points, const uint32_t* light, uint32_t m, float* pmf) {
+    if (!s || ((!points || !light || !pmf) && m)) return fail(RT_ERR_INVALID, "NULL argument");
+    SESSION_DEVICE(s);
+    if (!m) return RT_OK;
+    Staging g(s);
+    CUDA_TRY(g.get(20ull * m));
+    float* dp = (float*)g.p;
+    uint32_t* dl = (uint32_t*)(dp + 3ull * m);
+    float* dm = (float*)(dl + m);
+    CUDA_TRY(cudaMemcpyAsync(dp, points, 12ull * m, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemcpyAsync(dl, light, 4ull * m, cudaMemcpyHostToDevice, s->stream));
+    k_light_pmf_batch<<<(m + 127) / 128, 128, 0, s->stream>>>(s->S, dp, dl, m, dm);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(pmf, dm, 4ull * m, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return RT_OK;
+}
+
+int rt_transmittance_batch(rt_session* s, const float* rays, uint64_t n, float* trans) {
+    if (!s || ((!rays || !trans) && n)) return fail(RT_ERR_INVALID, "NULL argument");
+    if (n >= 0xFFFFFFFFull - 64) return fail(RT_ERR_INVALID, "batch larger than 2^32 rays");
+    SESSION_DEVICE(s);
+    if (!n) return RT_OK;
+    Staging g(s);
+    CUDA_TRY(g.get(36ull * n + 16));
+    float* d_rays = (float*)g.p;
+    float* d_out = d_rays + 8 * n;
+    CUDA_TRY(cudaMemcpyAsync(d_rays, rays, 32 * n, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(cudaMemsetAsync(s->fetch, 0, 4, s->stream));
+    const float4* o = (const float4*)d_rays;
+    k_transmit_batch<TRAV_BLOCK><<<s->trav_grid, TRAV_BLOCK, 0, s->stream>>>(s->S, o, o + n, n, d_out, s->fetch,
+                                                                             s->err);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(trans, d_out, 4 * n, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return s->check_device_error();
 }
 
 int rt_get_stats(rt_session* s, rt_stats* out) {

@@ -457,10 +457,36 @@ struct LeafShared {
 // are crossed, e.g. for every presence >= 0.44.
 #define RT_TRANSMIT_CUTOFF 1e-4f
 
-// `mine`: this lane's parked leaf is a triangle leaf to test. Returns true
-// when an any-hit query found a hit (the query is over).
-template <bool ANY, bool TRANSMIT = false>
-__device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, bool mine, LeafShared& L) {
+// Presence cutouts inside a closest-hit query (PRES): the reference
+// (src/raytracer/pt/mod.rs:702-710) meets a hit of presence p < 1 and passes
+// through it with probability 1 - p, tracing on from the hit point, for at
+// most 16 such skips. Here the traversal makes the same decision for every
+// cutout surface it meets and ignores the surfaces it passes through, so the
+// closest hit returned is the first surface that stopped the ray, in one
+// traversal. Each decision is an independent uniform per (ray, surface): a
+// hash of the ray's seed (drawn from the path's random state) and the
+// triangle and instance. The surfaces along the ray are then accepted with
+// probability p each, as in the reference; the 16-skip cap is not kept (with
+// p = 1/2 a ray reaches it with probability 2^-16).
+__device__ __forceinline__ uint32_t fmix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    return h ^ (h >> 16);
+}
+__device__ __forceinline__ bool presence_passes(uint64_t seed, uint32_t tri, uint32_t inst, float presence) {
+    const uint32_t h = fmix32((uint32_t)seed ^ fmix32((uint32_t)(seed >> 32) ^ tri * 0x9E3779B9u) ^
+                              inst * 0x27D4EB2Fu);
+    return (float)(h >> 8) * (1.0f / 16777216.0f) >= presence;
+}
+
+// `mine`: this lane's parked leaf is a triangle leaf to test; `seed_own`:
+// this lane's ray seed (PRES). Returns true when an any-hit query found a
+// hit (the query is over).
+template <bool ANY, bool TRANSMIT = false, bool PRES = false>
+__device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, bool mine, LeafShared& L,
+                                          uint64_t seed_own = 0) {
     const uint32_t lane = threadIdx.x & 31u;
     TravState& ts = ps.ts;
     uint32_t first = 0, count = 0;
@@ -480,9 +506,9 @@ __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, boo
     for (uint32_t k = 0; k < count; k++) L.item[excl + k] = (uint16_t)((lane << 4) | k);
     L.key[lane] = ~0ull;
     L.trans[lane] = 1.0f;
-    // TRANSMIT: the presence of the material of this lane's instance.
+    // TRANSMIT / PRES: the presence of the material of this lane's instance.
     const float pres_own =
-        (TRANSMIT && mine) ? __ldg(&S.materials[__ldg(&S.inst[ts.cur_inst].z)].presence) : 1.0f;
+        ((TRANSMIT || PRES) && mine) ? __ldg(&S.materials[__ldg(&S.inst[ts.cur_inst].z)].presence) : 1.0f;
     __syncwarp();
     // This lane's ray, as the owners of pool items read it.
     const float tmax_own = ts.hit.t;
@@ -506,6 +532,13 @@ __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, boo
         r.ky = (int)((kp >> 2) & 3u);
         r.kz = (int)((kp >> 4) & 3u);
         const float pres = __shfl_sync(0xFFFFFFFFu, pres_own, owner);
+        uint64_t seed = 0;
+        uint32_t inst_o = 0;
+        if (PRES) {
+            seed = ((uint64_t)__shfl_sync(0xFFFFFFFFu, (uint32_t)(seed_own >> 32), owner) << 32) |
+                   __shfl_sync(0xFFFFFFFFu, (uint32_t)seed_own, owner);
+            inst_o = __shfl_sync(0xFFFFFFFFu, ts.cur_inst, owner);
+        }
         float t = 0.0f, b1 = 0.0f, b2 = 0.0f;
         unsigned long long key = ~0ull;
         float factor = 1.0f;
@@ -521,7 +554,7 @@ __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, boo
             if (tri_watertight(r, xyz(a), xyz(b), xyz(c), tmax, t, b1, b2)) {
                 if (TRANSMIT) {
                     factor = pres >= 1.0f ? 0.0f : 1.0f - pres;
-                } else {
+                } else if (!(PRES && pres < 1.0f && presence_passes(seed, tri, inst_o, pres))) {
                     key = ((unsigned long long)__float_as_uint(t) << 32) | tri;
                     atomicMin(&L.key[owner], key);
                 }

@@ -32,7 +32,8 @@ EXPORTS = ("rt_session_create", "rt_session_destroy", "rt_last_error", "rt_rende
            "rt_bsdf_furnace", "rt_intersect_batch_noalloc", "rt_session_guide", "rt_set_adaptive",
            "rt_average_spp", "rt_checkpoint_save_rckp", "rt_rckp_write", "rt_accum_exr_write",
            "rt_accum_exr_info", "rt_accum_exr_read", "rt_accum_merge", "rt_read_film", "rt_denoise",
-           "rt_denoise_film", "rt_film_exr_write")
+           "rt_denoise_film", "rt_film_exr_write", "rt_pcg_streams", "rt_light_sample_batch",
+           "rt_light_pmf_batch", "rt_transmittance_batch")
 
 
 class RtError(RuntimeError):
@@ -97,6 +98,10 @@ def lib():
         L.rt_denoise.argtypes = [vp, vp]
         L.rt_denoise_film.argtypes = [vp, u32, u32, vp]
         L.rt_film_exr_write.argtypes = [C.c_char_p, u32, u32, vp, C.c_char_p]
+        L.rt_pcg_streams.argtypes = [vp, vp, u32, u32, vp]
+        L.rt_light_sample_batch.argtypes = [vp, vp, vp, u32, vp, vp]
+        L.rt_light_pmf_batch.argtypes = [vp, vp, vp, u32, vp]
+        L.rt_transmittance_batch.argtypes = [vp, vp, u64, vp]
         _lib = L
     return _lib
 
@@ -104,6 +109,15 @@ def lib():
 def _check(rc):
     if rc != RT_OK:
         raise RtError(rc, lib().rt_last_error().decode(errors="replace"))
+
+
+def pcg_streams(pixels, samples, n):
+    """(m, n) u32 draws of the device PCG32 of each (pixel, sample) pair."""
+    px = np.ascontiguousarray(pixels, dtype=np.uint64)
+    sm = np.ascontiguousarray(samples, dtype=np.uint64)
+    out = np.empty((len(px), n), np.uint32)
+    _check(lib().rt_pcg_streams(px.ctypes.data, sm.ctypes.data, len(px), n, out.ctypes.data))
+    return out
 
 
 class PtSession:
@@ -221,6 +235,33 @@ class PtSession:
         """Device-pointer ray batch, enqueued without a host sync."""
         _check(lib().rt_intersect_batch_device(self.h, planes_ptr, n, 1 if any_hit else 0, prim_ptr, inst_ptr,
                                                t_ptr, stream))
+
+    def light_sample(self, points, u):
+        """Device light-BVH picks at (m, 3) points with (m,) uniforms:
+        (light indices, pick probabilities)."""
+        p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+        uu = np.ascontiguousarray(u, dtype=np.float32)
+        light = np.empty(len(p), np.uint32)
+        pmf = np.empty(len(p), np.float32)
+        _check(lib().rt_light_sample_batch(self.h, p.ctypes.data, uu.ctypes.data, len(p), light.ctypes.data,
+                                           pmf.ctypes.data))
+        return light, pmf
+
+    def light_pmf(self, points, lights):
+        """Device pick probability of lights[i] at points[i]."""
+        p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 3)
+        li = np.ascontiguousarray(lights, dtype=np.uint32)
+        pmf = np.empty(len(p), np.float32)
+        _check(lib().rt_light_pmf_batch(self.h, p.ctypes.data, li.ctypes.data, len(p), pmf.ctypes.data))
+        return pmf
+
+    def transmittance(self, planes):
+        """Shadow-ray transmittance of rays in the two-plane layout."""
+        planes = np.ascontiguousarray(planes, dtype=np.float32)
+        n = planes.shape[1]
+        out = np.empty(n, np.float32)
+        _check(lib().rt_transmittance_batch(self.h, planes.ctypes.data, n, out.ctypes.data))
+        return out
 
     def stats(self):
         s = RtStats()

@@ -46,13 +46,14 @@ def merge(parts):
 
 # ---------------------------------------------------------------------------
 # C1: Cornell-like box
-def cornell_box(width=256, height=256):
+def cornell_box(width=256, height=256, light_size=0.5, light_radiance=(17.0, 12.0, 4.0)):
     """Closed box [-1,1]^3 open toward +z: floor, ceiling, back (0.73 grey),
     left wall (0.63, 0.065, 0.05), right wall (0.14, 0.45, 0.09) — 5 inward
     quads, 10 triangles. Two boxes (a unit cube mesh instanced twice: 0.6x1.2x0.6
     rotated 17 deg, 0.6^3 rotated -18 deg; grey Oren-Nayar sigma 0). A 0.5x0.5
-    ceiling quad of radiance (17, 12, 4) that is both geometry and a rect light.
-    Pinhole camera at z = +3.9 looking at the origin, 40 deg vertical fov."""
+    ceiling quad of radiance (17, 12, 4) that is both geometry and a rect light
+    (`light_size` and `light_radiance` change it). Pinhole camera at z = +3.9
+    looking at the origin, 40 deg vertical fov."""
     s = Scene(width, height, fov=40.0)
     s.look_at((0.0, 0.0, 3.9), (0.0, 0.0, 0.0))
     white = s.add_material(matte((0.73, 0.73, 0.73), id=1))
@@ -72,7 +73,8 @@ def cornell_box(width=256, height=256):
     short = affine(rot_y(-18.0) @ np.diag([0.6, 0.6, 0.6]), (0.35, -0.699, 0.3))
     s.add_instance(cube, grey, tall)
     s.add_instance(cube, grey, short)
-    s.add_emissive_quad((-0.25, 0.999, -0.25), (0.5, 0.0, 0.0), (0.0, 0.0, 0.5), (17.0, 12.0, 4.0))
+    h = 0.5 * light_size
+    s.add_emissive_quad((-h, 0.999, -h), (light_size, 0.0, 0.0), (0.0, 0.0, light_size), tuple(light_radiance))
     s.materials[-1]["id"] = 5
     return s
 

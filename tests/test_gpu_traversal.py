@@ -141,3 +141,29 @@ def test_empty_batch_and_miss_everything():
         planes[1, :, 3] = np.inf
         p, i, t = g.intersect(planes)
         assert (p == 0xFFFFFFFF).all() and np.isinf(t).all()
+
+
+def test_full_traversal_stress_set():
+    """The traversal-stress configuration at its stated size: 4,194,304
+    seeded rays (origins on the radius-2 sphere, aimed into the cube) into
+    the 1,000,000-triangle cloud, closest hit and any hit, checked ray for
+    ray against the f64 oracle with the near-tie / edge rule above; the
+    mismatch count is reported."""
+    s = scene.Scene(16, 16)
+    s.add_instance(s.add_mesh(*scenes.triangle_cloud_mesh(1_000_000)), s.add_material(scene.matte((0.5,) * 3)))
+    rays = scenes.triangle_cloud_rays(4_194_304)
+    op, oi, ot, _ = oracle.OracleScene(s).intersect(rays)
+    with PtSession(s) as g:
+        gp, gi, gt = g.intersect(rays)
+        ghit, _, _ = g.intersect(rays, any_hit=True)
+    tri_of = _tri_lookup(s)
+    mismatches = _check_closest(s, rays, gp, gi, gt, op, oi, ot, tri_of)
+    print(f"closest hit: {mismatches} near-tie / edge mismatches of {rays.shape[1]}")
+    assert mismatches < 1e-3 * rays.shape[1]
+    ohit = op != 0xFFFFFFFF
+    for k in np.nonzero(ghit.astype(bool) != ohit)[0]:
+        m = None
+        for p_, i_ in ((gp[k], gi[k]), (op[k], oi[k])):
+            if p_ != 0xFFFFFFFF:
+                m = _bary(tri_of(i_, p_), rays[0, k, :3].astype(np.float64), rays[1, k, :3].astype(np.float64))
+        assert m is not None and abs(m) < EDGE, (k, m)
