@@ -1,26 +1,31 @@
-"""Benchmark: the triangle-cloud traversal-stress workload on B200.
+"""Benchmark: the large-scale forest workload on B200.
 
-Workload (one step): the 1,000,000-triangle cloud (seeded centres uniform in
-[-0.5, 0.5]^3, vertices jittered by N(0, 0.01^2)) rendered at 1920x1080 with
-16 samples per pixel, diffuse albedo 0.5, one distant light, max depth 8,
-Russian roulette from depth 3: 33,177,600 camera samples per step.
+Workload (one step): one full frame of the procedural forest -- 20 seeded
+trees (bark + leaf meshes, ~46k triangles each, leaves with a presence
+cutout of 0.5) placed as 772,000 instances on a 1 km^2 fBm terrain, 1,200
+point lights through the light BVH -- rendered at 3840x2160 with 32 samples
+per pixel, max depth 10, Russian roulette from depth 3: 265,420,800 camera
+samples per step, plain (unguided) path tracing.
 
 Printed (one JSON line on rank 0):
   value      Msamples/s of the whole job, scene and path state resident in HBM
              (device time, CUDA events on the session stream, max over ranks);
   e2e        the same metric through the C ABI's render call a user makes
-             (rt_session_create from host arrays + rt_render_samples +
-             rt_read_image to host), host<->device copies included;
-  roofline   the closest-hit (extend) kernel: algorithmic bytes per extension
-             ray (reference binary BVH: 32 B per node visit, 48 B per triangle
-             test, 48 B per instance visit, 48 B ray in/out, counted by the f64
-             oracle on a pixel sample of the same frame) x rays per launch /
-             launch time, against the measured HBM copy bandwidth;
+             (rt_session_create from host arrays, incl. the device BVH build,
+             + rt_render_samples of the 32 passes + rt_read_image to host),
+             host<->device copies included;
+  roofline   the closest-hit (extend) kernel: algorithmic bytes per camera
+             sample of the reference's extension rays (reference binary BVH:
+             32 B per node visit, 48 B per triangle test, 48 B per instance
+             visit, 48 B ray in/out, counted by the f64 oracle on a pixel
+             sample of the same frame) x samples per launch / launch time,
+             against the measured HBM copy bandwidth;
   cpu_baseline  the f64 oracle (C++ restatement of the reference's CPU path
              tracer, all host threads) on a bounded pixel sample of the frame.
-  traversal  the 4,194,304-ray closest-hit and any-hit batches (Mrays/s).
-  workloads  device Msamples/s and Mrays/s of the other named scenes
-             (Cornell box, instanced materials, forest) at their sizes.
+  workloads  the other configurations: the 1M-triangle cloud at 1920x1080 x
+             16 spp and its 4,194,304-ray closest-hit / any-hit batches, the
+             Cornell box 256^2 x 16 spp, instanced materials 1920x1080 x 64
+             spp (device Msamples/s and Mrays/s).
   guided_equal_time  the learned-proposal workload: two 4x3x3 rooms joined by
              a 0.2x2.0 opening, the light in the unseen room, 1280x720, max
              depth 16. A fresh guided session renders GUIDED_SPP passes from
@@ -28,11 +33,13 @@ Printed (one JSON line on rank 0):
              plain session renders as many passes as fit in the same device
              time. Both are scored by relMSE against a high-spp GPU render
              (all pixels) and against the f64 CPU oracle on a strided pixel
-             subset (the 65,536-spp full-frame oracle render is hours of CPU).
+             subset, with a confidence interval over the pixels.
+  guided_forest  the forest's guided-vs-plain comparison at reduced size.
 
 `--impl reference` times the reference arm instead: the reference's CPU path
 (its Rust build is unavailable here, so the f64 C++ restatement of
-src/raytracer/pt/*) on the host cores, on a bounded sample of the workload.
+src/raytracer/pt/*) on the host cores, on a bounded pixel sample of the same
+frame each step.
 """
 import argparse
 import json
@@ -50,9 +57,15 @@ sys.path.insert(0, os.path.join(ROOT, "render.rs_b200"))
 
 METRIC = "Msamples/s at 1 B200; equal-time relMSE guided vs plain PT vs f64 CPU oracle"
 UNIT = "Msamples/s"
-WIDTH, HEIGHT, SPP, MAX_DEPTH = 1920, 1080, 16, 8
+# The headline workload: the forest at its configured size.
+WIDTH, HEIGHT, SPP, MAX_DEPTH = 3840, 2160, 32, 10
+WORKLOAD = "forest_772k_instances_1200_lights_3840x2160_32spp_depth10"
+CONFIG = {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_depth": MAX_DEPTH,
+          "rr_start": 3, "instances": 772_001, "trees": 20, "point_lights": 1200, "presence_cutouts": True,
+          "guided": False, "l2_flush": "256 MB write before every step; scene + path state > L2"}
+# The traversal-stress workload (a `workloads` entry).
+CLOUD_W, CLOUD_H, CLOUD_SPP, CLOUD_DEPTH = 1920, 1080, 16, 8
 N_TRIS, N_RAYS = 1_000_000, 4_194_304
-WORKLOAD = "triangle_cloud_1M_1920x1080_16spp_depth8"
 
 
 def load_peaks():
@@ -116,48 +129,59 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline_sample(scene, params, threads=0, target_s=12.0):
-    """The f64 oracle on a strided pixel sample of the frame, all host threads.
-    Returns Msamples/s, the sample description and per-ray traversal work."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle  # test infrastructure: the CPU baseline and the work counter
-    o_s = oracle.OracleScene(scene)
+def oracle_sample(o_s, scene, params, n_pixels, offset=0, threads=0):
+    """The f64 oracle (all host threads unless `threads`) on `n_pixels`
+    strided pixels of the frame at SPP samples each: (Msamples/s, sample
+    description, cores, per-sample traversal work, seconds)."""
     npix = scene.width * scene.height
-    stride = 64
-    pixels = np.arange(0, npix, stride, dtype=np.uint32)
+    stride = max(1, npix // n_pixels)
+    pixels = np.arange(offset % stride, npix, stride, dtype=np.uint32)[:n_pixels]
     t0 = time.perf_counter()
     _, _, counts = o_s.render(params, 0, SPP, pixels=pixels, threads=threads)
     el = time.perf_counter() - t0
-    # Grow the sample toward target_s of CPU work for a steadier number.
-    if el < target_s / 4:
-        stride = max(1, int(stride * el / target_s * 1.0) or 1)
-        stride = max(stride, 2)
-        pixels = np.arange(1, npix, stride, dtype=np.uint32)
-        t0 = time.perf_counter()
-        _, _, counts = o_s.render(params, 0, SPP, pixels=pixels, threads=threads)
-        el = time.perf_counter() - t0
     samples = len(pixels) * SPP
     cores = threads if threads > 0 else os.cpu_count()
     ext, sh = int(counts[0]), int(counts[1])
-    work = {"ext_rays": ext, "shadow_rays": sh,
-            "ext_bytes_per_ray": (32.0 * counts[2] + 48.0 * counts[3] + 48.0 * counts[4]) / max(ext, 1) + 48.0,
-            "shadow_bytes_per_ray": (32.0 * counts[5] + 48.0 * counts[6] + 48.0 * counts[7]) / max(sh, 1) + 48.0}
-    return samples / el / 1e6, f"{len(pixels)} pixels (every {stride}th) x {SPP} spp of the frame", cores, work, el
+    # Reference binary-BVH bytes (32 B / node visit, 48 B / triangle test,
+    # 48 B / instance visit, 48 B ray in + hit out) of the extension rays,
+    # per camera sample; presence skips re-trace as extension rays there.
+    ext_bytes = 32.0 * counts[2] + 48.0 * counts[3] + 48.0 * counts[4] + 48.0 * ext
+    work = {"ext_rays_per_sample": ext / samples, "shadow_segments_per_sample": sh / samples,
+            "ext_bytes_per_sample": ext_bytes / samples, "ext_bytes_per_ray": ext_bytes / max(ext, 1),
+            "node_visits_per_ext_ray": counts[2] / max(ext, 1), "tri_tests_per_ext_ray": counts[3] / max(ext, 1),
+            "instance_visits_per_ext_ray": counts[4] / max(ext, 1)}
+    return (samples / el / 1e6, f"{len(pixels)} pixels (every {stride}th) x {SPP} spp of the frame", cores, work,
+            el)
 
 
 GUIDED_W, GUIDED_H, GUIDED_SPP, GUIDED_DEPTH = 1280, 720, 2048, 16
 
-# DRAM bytes (read + write) per k_extend launch, averaged over the 32 launches
-# of one render step, from one ncu capture of this command (1 pass):
-#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
-#       --clock-control none -k regex:k_extend -s 32 -c 32
-#       python bench.py --steps 1 --warmup 1 --e2e-steps 0 --no-cpu-baseline --no-guided --no-workloads
-EXTEND_DRAM_BYTES_PER_LAUNCH = 138.0e6  # 107.8 MB read + 30.2 MB written
-EXTEND_DRAM_SOURCE = "ncu, dram__bytes_read.sum + dram__bytes_write.sum, mean of one step's 32 k_extend launches"
+# DRAM bytes (read + write) per k_extend launch on the forest at 3840x2160,
+# scaled from one ncu capture of a smaller frame of the same scene (traffic
+# per launch grows with the rays per launch; profiles/ has the capture).
+# None until measured.
+EXTEND_DRAM_BYTES_PER_LAUNCH = None
+EXTEND_DRAM_SOURCE = "not captured"
 
 
 def rel_mse(img, ref):
     return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def ratio_ci(plain, guided, ref, z=1.96):
+    """relMSE(plain) / relMSE(guided) against `ref` with a confidence
+    interval over the pixels (delta method on the ratio of the per-pixel
+    means; pixels are independent)."""
+    den = ref.reshape(-1, 3) ** 2 + 1e-2
+    a = ((plain.reshape(-1, 3) - ref.reshape(-1, 3)) ** 2 / den).mean(1)
+    b = ((guided.reshape(-1, 3) - ref.reshape(-1, 3)) ** 2 / den).mean(1)
+    n = len(a)
+    ma, mb = a.mean(), b.mean()
+    r = ma / mb
+    cov = np.cov(a, b)
+    var = (cov[0, 0] / mb ** 2 + ma ** 2 * cov[1, 1] / mb ** 4 - 2 * ma * cov[0, 1] / mb ** 3) / n
+    h = z * float(np.sqrt(max(var, 0.0)))
+    return float(r), [float(r - h), float(r + h)]
 
 
 def equal_time_plain(scene, params, budget_ms):
@@ -178,7 +202,7 @@ def equal_time_plain(scene, params, budget_ms):
         return g.image(), done, ms
 
 
-def guided_equal_time(ref_spp=16384, cpu_pixels=256, cpu_spp=16384):
+def guided_equal_time(ref_spp=16384, cpu_pixels=1024, cpu_spp=65536):
     """Equal-time relMSE of guided vs plain path tracing on the two-room scene.
     The GPU reference is the mean of two independent halves A and B; its own
     error, mean((A - B)^2 / (ref^2 + 1e-2)) / 4, is reported and subtracted
@@ -208,6 +232,7 @@ def guided_equal_time(ref_spp=16384, cpu_pixels=256, cpu_spp=16384):
            "plain_ms": round(plain_ms, 2), "plain_ms_per_spp": round(per_spp, 4),
            "gpu_reference_spp": ref_spp}
     e_p, e_g = rel_mse(plain, ref), rel_mse(guided, ref)
+    out["ratio_vs_gpu_ref_ci95"] = ratio_ci(plain, guided, ref)[1]
     out.update({"relmse_plain_vs_gpu_ref": e_p, "relmse_guided_vs_gpu_ref": e_g, "ratio_vs_gpu_ref": e_p / e_g,
                 "gpu_ref_relmse": ref_err, "relmse_plain_corrected": e_p - ref_err,
                 "relmse_guided_corrected": e_g - ref_err, "ratio_corrected": (e_p - ref_err) / (e_g - ref_err),
@@ -223,25 +248,30 @@ def guided_equal_time(ref_spp=16384, cpu_pixels=256, cpu_spp=16384):
         el = time.perf_counter() - t0
         gp, gg = plain.reshape(-1, 3)[pix], guided.reshape(-1, 3)[pix]
         c_p, c_g = rel_mse(gp, cref), rel_mse(gg, cref)
-        out.update({"relmse_plain_vs_f64": c_p, "relmse_guided_vs_f64": c_g, "ratio_vs_f64": c_p / c_g,
+        r, ci = ratio_ci(gp, gg, cref)
+        out.update({"relmse_plain_vs_f64": c_p, "relmse_guided_vs_f64": c_g, "ratio_vs_f64": r,
+                    "ratio_vs_f64_ci95": ci,
                     "f64_reference": f"oracle, {len(pix)} strided pixels x {cpu_spp} spp ({el:.1f} s)"})
     except Exception as exc:  # the oracle is optional on a box without it
         out["f64_reference"] = f"unavailable: {exc}"
     return out
 
 
-def other_workloads(forest_spp=4):
-    """Device throughput of the other named scenes at their configured size:
-    Cornell box 256^2 x 16 spp (depth 8), instanced materials 1920x1080 x 64
-    spp (depth 12), forest 3840x2160 (depth 10; `forest_spp` of its 32 passes,
-    to keep the run short). One warm-up pass, then one timed render call
-    (device time from the session's events); scene build time excluded."""
+def other_workloads(flush, stream):
+    """Device throughput of the other configurations at their configured
+    size: the 1M-triangle cloud at 1920x1080 x 16 spp (depth 8) and its
+    4,194,304-ray closest-hit / any-hit batches (L2 flushed before each
+    batch), the Cornell box 256^2 x 16 spp (depth 8), instanced materials
+    1920x1080 x 64 spp (depth 12). One warm-up pass, then one timed render
+    call (device time from the session's events); scene build excluded."""
+    import torch
     from rtcuda import PtSession, abi, scenes
     out = {}
-    cases = [("cornell_256x256_16spp_depth8", lambda: scenes.cornell_box(), scenes.CORNELL, 16),
+    cases = [("triangle_cloud_1M_1920x1080_16spp_depth8", lambda: scenes.triangle_cloud(CLOUD_W, CLOUD_H, N_TRIS),
+              scenes.TRIANGLE_CLOUD, CLOUD_SPP),
+             ("cornell_256x256_16spp_depth8", lambda: scenes.cornell_box(), scenes.CORNELL, 16),
              ("instanced_materials_1920x1080_64spp_depth12", lambda: scenes.instanced_materials(),
-              scenes.INSTANCED_MATERIALS, 64),
-             (f"forest_3840x2160_depth10_{forest_spp}of32spp", lambda: scenes.forest(), scenes.FOREST, forest_spp)]
+              scenes.INSTANCED_MATERIALS, 64)]
     for name, make, cfg, spp in cases:
         t0 = time.perf_counter()
         s = make()
@@ -251,12 +281,49 @@ def other_workloads(forest_spp=4):
             g.render_samples(1 << 20, 1)
             g.render_samples(0, spp)
             st = g.stats()
-        ms = st["total_ms"]
-        out[name] = {"Msamples_per_s": st["samples"] / ms / 1e3, "ms": round(ms, 2), "spp": spp,
-                     "Mrays_per_s": (st["extension_rays"] + st["shadow_rays"]) / ms / 1e3,
-                     "triangles_effective": s.triangle_count() if hasattr(s, "triangle_count") else None,
-                     "instances": getattr(s, "n_instances", None), "build_and_upload_s": round(build_s, 2)}
+            ms = st["total_ms"]
+            out[name] = {"Msamples_per_s": st["samples"] / ms / 1e3, "ms": round(ms, 2), "spp": spp,
+                         "Mrays_per_s": (st["extension_rays"] + st["shadow_rays"]) / ms / 1e3,
+                         "extend_ms": round(st["extend_ms"], 2), "extension_rays": st["extension_rays"],
+                         "triangles_effective": s.triangle_count(), "instances": s.n_instances,
+                         "build_and_upload_s": round(build_s, 2)}
+            if name.startswith("triangle_cloud"):
+                out[name]["traversal"] = traversal_batches(g, flush)
     return out
+
+
+def traversal_batches(sess, flush, reps=5):
+    """The 4,194,304-ray closest-hit and any-hit batches into the session's
+    scene from HBM (CUDA events on the session stream, L2 flushed before
+    each batch)."""
+    import torch
+    from rtcuda import scenes
+    stream = torch.cuda.ExternalStream(sess.stream())
+    d_rays = torch.from_numpy(scenes.triangle_cloud_rays(N_RAYS)).cuda()
+    prim = torch.empty(N_RAYS, dtype=torch.int32, device="cuda")
+    inst = torch.empty_like(prim)
+    tt = torch.empty(N_RAYS, dtype=torch.float32, device="cuda")
+    trav = {}
+    for any_hit, name in ((0, "closest_hit"), (1, "any_hit")):
+        for _ in range(3):
+            sess.intersect_device(d_rays.data_ptr(), N_RAYS, any_hit, prim.data_ptr(), inst.data_ptr(),
+                                  tt.data_ptr(), sess.stream())
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        tot = 0.0
+        for _ in range(reps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            a.record(stream)
+            sess.intersect_device(d_rays.data_ptr(), N_RAYS, any_hit, prim.data_ptr(), inst.data_ptr(),
+                                  tt.data_ptr(), sess.stream())
+            b.record(stream)
+            torch.cuda.synchronize()
+            tot += a.elapsed_time(b)
+        tms = tot / reps
+        trav[name] = {"ms": round(tms, 3), "Mrays_per_s": N_RAYS / tms / 1e3}
+    return trav
 
 
 def guided_forest(width=480, height=270, budget=128, ref_spp=512):
@@ -293,29 +360,35 @@ def guided_forest(width=480, height=270, budget=128, ref_spp=512):
 
 
 def run_reference(args):
-    """Reference arm: the reference's CPU path (f64 restatement) on host cores."""
+    """Reference arm: the reference's CPU path (its f64 C++ restatement) on
+    the host cores, each step a bounded pixel sample of the same frame."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # the reference arm runs the oracle by design
     from rtcuda import abi, scenes
-    scene = scenes.triangle_cloud(WIDTH, HEIGHT, N_TRIS)
-    params = abi.make_params(max_depth=MAX_DEPTH)
-    vals = []
+    scene = scenes.forest(WIDTH, HEIGHT)
+    params = abi.make_params(max_depth=MAX_DEPTH, rr_start=3)
+    o_s = oracle.OracleScene(scene)
+    vals, sample, cores = [], "", os.cpu_count()
     for i in range(args.warmup + args.steps):
-        v, sample, cores, _, el = cpu_baseline_sample(scene, params, target_s=max(2.0, 60.0 / (args.warmup + args.steps)))
+        v, sample, cores, _, _ = oracle_sample(o_s, scene, params, REF_PIXELS_PER_STEP, offset=i)
         if i >= args.warmup:
             vals.append(v)
     value = statistics.median(vals)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_depth": MAX_DEPTH,
-                       "triangles": N_TRIS},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": dict(CONFIG),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"per step: {sample}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "reference is Rust (no toolchain here): its CPU path restated in C++ f64 (oracle/)"}
     print(json.dumps(line), flush=True)
     return 0
+
+
+REF_PIXELS_PER_STEP = 384   # x 32 spp: a few seconds of the oracle per step on the forest
 
 
 def run_traversal(args):
@@ -399,7 +472,7 @@ def run_scene(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -408,10 +481,10 @@ def main():
     ap.add_argument("--res", default="640x360", help="--mode scene: frame size WxH")
     ap.add_argument("--mode", default="full", choices=["full", "traversal", "guided", "scene"],
                     help="traversal: only the closest/any-hit ray batches; guided: only the learned-proposal "
-                         "workload (both for profiler captures)")
+                         "workload; scene: one named scene (all for profiler captures)")
     ap.add_argument("--rays", type=int, default=N_RAYS)
-    ap.add_argument("--no-guided", action="store_true", help="skip the guided equal-time comparison")
-    ap.add_argument("--no-workloads", action="store_true", help="skip the other scenes' throughput")
+    ap.add_argument("--no-guided", action="store_true", help="skip the guided equal-time comparisons")
+    ap.add_argument("--no-workloads", action="store_true", help="skip the other configurations")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -432,11 +505,11 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = torch.device("cuda", local)
 
-    scene = scenes.triangle_cloud(WIDTH, HEIGHT, N_TRIS)
-    params = abi.make_params(max_depth=MAX_DEPTH)
+    scene = scenes.forest(WIDTH, HEIGHT)
+    params = abi.make_params(max_depth=MAX_DEPTH, rr_start=3)
     sess = PtSession(scene, params)
     stream = torch.cuda.ExternalStream(sess.stream(), device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
@@ -446,12 +519,13 @@ def main():
             dist.barrier(device_ids=[local])
         torch.cuda.synchronize()
 
-    # Weak scaling: every rank renders its own 16 samples of the same frame
-    # (sample range offset by rank, as --sample-range partitions the reference).
+    # Weak scaling: every rank renders its own 32-pass frames of the same
+    # view (sample ranges offset by rank, as --sample-range partitions the
+    # reference's render), so per-GPU work is fixed as ranks are added.
     def step(i):
         with torch.cuda.stream(stream):
             flush.zero_()
-        sess.render_samples((rank * 100000 + i * SPP) % (1 << 31), SPP)
+        sess.render_samples((rank * 1_000_000 + i * SPP) % (1 << 31), SPP)
 
     for i in range(args.warmup):
         step(i)
@@ -459,7 +533,8 @@ def main():
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
-    ext_ms = ext_rays = launches = ext_launches = 0.0
+    ext_ms = launches = ext_launches = samples = 0.0
+    ext_rays = sh_rays = 0
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     barrier()
@@ -469,8 +544,10 @@ def main():
         st = sess.stats()
         ext_ms += st["extend_ms"]
         ext_rays += st["extension_rays"]
+        sh_rays += st["shadow_rays"]
+        samples += st["samples"]
         ext_launches += st["slabs"] * st["waves"]
-        launches += st["kernel_launches"] + 1
+        launches += st["kernel_launches"] + 1   # + the L2 flush
     e1.record(stream)
     barrier()
     clk = clocks.stop()
@@ -482,44 +559,20 @@ def main():
     samples_per_step = WIDTH * HEIGHT * SPP
     value = samples_per_step * args.steps * world / (ms_max / 1e3) / 1e6
     last = sess.stats()
-
-    # Traversal batches (4,194,304 rays) from HBM.
-    rays = scenes.triangle_cloud_rays(N_RAYS)
-    d_rays = torch.from_numpy(rays).to(dev)
-    prim = torch.empty(N_RAYS, dtype=torch.int32, device=dev)
-    inst = torch.empty_like(prim)
-    tt = torch.empty(N_RAYS, dtype=torch.float32, device=dev)
-    trav = {}
-    for any_hit, name in ((0, "closest_hit"), (1, "any_hit")):
-        for _ in range(3):
-            sess.intersect_device(d_rays.data_ptr(), N_RAYS, any_hit, prim.data_ptr(), inst.data_ptr(),
-                                  tt.data_ptr(), sess.stream())
-        torch.cuda.synchronize()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        reps = 5
-        a.record(stream)
-        for _ in range(reps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-            sess.intersect_device(d_rays.data_ptr(), N_RAYS, any_hit, prim.data_ptr(), inst.data_ptr(),
-                                  tt.data_ptr(), sess.stream())
-        b.record(stream)
-        torch.cuda.synchronize()
-        tms = a.elapsed_time(b) / reps
-        trav[name] = {"ms": tms, "Mrays_per_s": N_RAYS / tms / 1e3}
-
-    # End to end through the C ABI: host scene arrays in, host image out, one
-    # session at a time as a caller rendering frame after frame would hold.
     sess.close()
+
+    # End to end through the C ABI: host scene arrays in (the session
+    # uploads them and builds the BVHs on the device), 32 passes, host image
+    # out; one session at a time, as a caller rendering frame after frame.
     e2e_ms = []
-    h2d = sum(p.nbytes + i.nbytes for p, i, _ in scene.meshes) + scene.instance_array().nbytes
+    h2d = sum(p.nbytes + i.nbytes + (n.nbytes if n is not None else 0) for p, i, n in scene.meshes) + \
+        scene.instance_array().nbytes
     d2h = WIDTH * HEIGHT * 3 * 4
     for i in range(args.e2e_steps):
         barrier()
         t0 = time.perf_counter()
         with PtSession(scene, params) as s2:
-            s2.render_samples(rank * 1000 + 7 + i, SPP)
+            s2.render_samples(rank * 1000 + 7 + i * SPP, SPP)
             s2.image()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     et = torch.tensor([max(e2e_ms) if e2e_ms else 0.0], device=dev)
@@ -530,50 +583,48 @@ def main():
     result = None
     if rank == 0:
         peak, peak_kind = load_peaks()
-        cpu = None
-        work = None
+        cpu = roof = None
         if not args.no_cpu_baseline and world == 1:
-            v, sample, cores, work, el = cpu_baseline_sample(scene, params)
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle  # test infrastructure: the CPU baseline and the work counter
+            o_s = oracle.OracleScene(scene)
+            v, sample, cores, work, el = oracle_sample(o_s, scene, params, 2048)
+            o_s.close()
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
                    "seconds": round(el, 2)}
-        roof = None
-        if work:
-            bytes_per_ray = work["ext_bytes_per_ray"]
             launches_ext = max(1.0, ext_launches)
-            achieved = bytes_per_ray * ext_rays / (ext_ms / 1e3) / 1e9
-            roof = {"kernel": "k_extend (closest hit, 8-wide BVH)", "bound": "hbm", "achieved": achieved,
-                    "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": EXTEND_DRAM_BYTES_PER_LAUNCH,
-                    "traffic_source": EXTEND_DRAM_SOURCE, "peak_kind": peak_kind, "bytes_per_ray": bytes_per_ray,
-                    "algorithmic_bytes_per_launch": bytes_per_ray * ext_rays / launches_ext,
-                    "rays_per_launch": ext_rays / launches_ext, "launch_ms": ext_ms / launches_ext,
-                    "launches": int(launches_ext)}
-        guided = None
-        if not args.no_guided and world == 1:
-            guided = guided_equal_time()
+            alg_bytes = work["ext_bytes_per_sample"] * samples
+            achieved = alg_bytes / (ext_ms / 1e3) / 1e9
+            roof = {"kernel": "k_extend (closest hit, 8-wide BVH, cutouts decided in traversal)", "bound": "hbm",
+                    "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": EXTEND_DRAM_BYTES_PER_LAUNCH, "traffic_source": EXTEND_DRAM_SOURCE,
+                    "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg_bytes / launches_ext,
+                    "samples_per_launch": samples / launches_ext, "launch_ms": ext_ms / launches_ext,
+                    "launches": int(launches_ext), "per_sample_work": work,
+                    "gpu_extension_rays_per_sample": ext_rays / max(samples, 1)}
         workloads = None
         if not args.no_workloads and world == 1:
-            workloads = other_workloads()
-        forest_guided = None
-        if not args.no_guided and not args.no_workloads and world == 1:
+            workloads = other_workloads(flush, stream)
+        guided = forest_guided = None
+        if not args.no_guided and world == 1:
+            guided = guided_equal_time()
             forest_guided = guided_forest()
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP,
-                       "max_depth": MAX_DEPTH, "triangles": N_TRIS, "rays": N_RAYS,
-                       "parallelism": f"replica-sample-ranges x{world}", "l2_flush": True,
-                       "accumulator": "f64"},
+            "config": dict(CONFIG, parallelism=f"replica-sample-ranges x{world}", accumulator="f64"),
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h,
                     "ms": max(e2e_ms) if e2e_ms else None, "ms_each": [round(v, 2) for v in e2e_ms]},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
-            "gpu_launches": int(launches + 3 * 0),
-            "traversal": trav,
-            "rays_per_step": {"extension": last["extension_rays"], "shadow": last["shadow_rays"]},
-            "guided_equal_time": guided,
+            "gpu_launches": int(launches),
+            "Mrays_per_s": (ext_rays + sh_rays) / (ms_max / 1e3) / 1e6,
+            "rays_per_step": {"extension": ext_rays // max(args.steps, 1), "shadow": sh_rays // max(args.steps, 1)},
+            "stage_ms_last_step": {"extend": round(last["extend_ms"], 1), "shade": round(last["shade_ms"], 1),
+                                   "shadow": round(last["shadow_ms"], 1), "total": round(last["total_ms"], 1)},
             "workloads": workloads,
+            "guided_equal_time": guided,
             "guided_forest": forest_guided,
-            "Mrays_per_s": (last["extension_rays"] + last["shadow_rays"]) / (last["total_ms"] / 1e3) / 1e6,
         }
         print(json.dumps(result), flush=True)
     if world > 1:

@@ -2063,7 +2063,9 @@ static void parallel_for(uint64_t n, int threads, F&& f) {
         return;
     }
     std::atomic<uint64_t> next{0};
-    const uint64_t chunk = 64;
+    // Chunks of up to 64 items, smaller when there are few items per thread
+    // (a few hundred pixels of an expensive scene still use every thread).
+    const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(64, n / ((uint64_t)threads * 16)));
     std::vector<std::thread> pool;
     for (int t = 0; t < threads; t++)
         pool.emplace_back([&, t] {

@@ -9,13 +9,18 @@
 //                     the 48 raw outputs, or the decoded mixture when rendering
 //   k_guide_bwd       vMF-mixture loss gradient in registers, then per layer
 //                     two tcgen05 GEMMs: dW = dZ^T H (batch is the K dimension)
-//                     and dH = dZ W; dW/db reduced into f32 gradients
-//   k_guide_hash_bwd  scatter-add of d loss / d features into the table gradient
+//                     and dH = dZ W; each CTA sums dW/db of its tiles into its
+//                     own f32 row, k_guide_grad_reduce adds the rows in order
+//   k_guide_hash_bwd  scatter-add of d loss / d features into the table
+//                     gradient, in 2^-24 fixed point (integer sums do not
+//                     depend on the order the atomics land in)
 //   k_guide_adam      Adam on the f32 masters, refreshing the bf16 / fp16 copies
 //                     (lazy on the hash table: entries without gradient skip)
 // Loss: -w * log q(wi | x) with w = lum(f cos Li) / p_sample, the
 // importance-weighted KL objective of neural importance sampling
 // (Müller et al. 2019), estimated from the path tracer's own vertices.
+// Training is deterministic: no gradient is summed by float atomics, so a
+// render with the same seed trains the same network bit for bit.
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -250,11 +255,17 @@ constexpr uint32_t B_TMEM_DH = 128;
 __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloat16* __restrict__ X0,
                                                     const __nv_bfloat16* __restrict__ acts,
                                                     const float* __restrict__ out, const float* __restrict__ rec,
-                                                    uint32_t n, BatchSel B, float* gW, float* gb,
+                                                    uint32_t n, BatchSel B, float* part,
                                                     float* dX0, float* loss_sum, uint32_t* err) {
     uint32_t begin;
     n = batch_slice(B, n, begin);
     rec += 16 * (size_t)begin;
+    // This CTA's row of dW / db partial sums (weights, then biases): its
+    // tiles add into it in tile order; k_guide_grad_reduce adds the rows.
+    float* gW = part + (size_t)blockIdx.x * G_NPARAMS;
+    float* gb = gW + G_NWEIGHTS;
+    for (int i = threadIdx.x; i < G_NPARAMS; i += blockDim.x) gW[i] = 0.f;
+    __syncthreads();
     if ((uint64_t)blockIdx.x * TILE >= n) return;
     extern __shared__ __align__(1024) uint8_t sm[];
     __shared__ uint64_t mbar;
@@ -380,8 +391,8 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
                 float* g = gW + w_off(l) + (size_t)tid * K_in;
 #pragma unroll
                 for (int k = 0; k < 64; k++)
-                    if (k < K_in) atomicAdd(g + k, v[k]);
-                atomicAdd(&gb[b_off(l) + tid], vb[0]);
+                    if (k < K_in) g[k] += v[k];
+                gb[b_off(l) + tid] += vb[0];
             }
 #pragma unroll
             for (int c = 0; c < 4; c++)
@@ -410,9 +421,27 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
     }
 }
 
+// Adds the backward CTAs' partial rows to the MLP gradient, in CTA order.
+__global__ void k_guide_grad_reduce(const float* __restrict__ part, int rows, float* gw) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= G_NPARAMS) return;
+    float s = 0.f;
+    for (int b = 0; b < rows; b++) s += part[(size_t)b * G_NPARAMS + i];
+    gw[i] += s;
+}
+
+// Table gradients are summed as integers in units of 2^-24 (each
+// contribution rounded, clamped to +-2^30): the sum is the same whatever
+// order the scattered atomics arrive in.
+#define G_FIX_SCALE 16777216.0f
+__device__ __forceinline__ unsigned long long to_fix(float v) {
+    return (unsigned long long)__float2ll_rn(fminf(fmaxf(v, -1073741824.0f), 1073741824.0f) * G_FIX_SCALE);
+}
+__device__ __forceinline__ float from_fix(unsigned long long q) { return (float)(long long)q * (1.0f / G_FIX_SCALE); }
+
 // ---- hash-grid backward ---------------------------------------------------------
 __global__ void k_guide_hash_bwd(GuideDev G, const float* __restrict__ rec, const float* __restrict__ dX0, uint32_t n,
-                                 BatchSel B, float* gtable) {
+                                 BatchSel B, unsigned long long* gtable) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, begin;
     n = batch_slice(B, n, begin);
     rec += 16 * (size_t)begin;
@@ -429,12 +458,14 @@ __global__ void k_guide_hash_bwd(GuideDev G, const float* __restrict__ rec, cons
         float tx = fx - ix, ty = fy - iy, tz = fz - iz;
         uint32_t x0 = (uint32_t)ix, y0 = (uint32_t)iy, z0 = (uint32_t)iz;
         float g0 = dx[2 * l], g1 = dx[2 * l + 1];
-        float* T = gtable + (size_t)l * G_T * 2;
+        unsigned long long* T = gtable + (size_t)l * G_T * 2;
         for (int c = 0; c < 8; c++) {
             uint32_t ddx = c & 1, ddy = (c >> 1) & 1, ddz = (c >> 2) & 1;
             float w = (ddx ? tx : 1.f - tx) * (ddy ? ty : 1.f - ty) * (ddz ? tz : 1.f - tz);
             uint32_t idx = grid_index(x0 + ddx, y0 + ddy, z0 + ddz, res1, dense);
-            atomicAdd(reinterpret_cast<float2*>(T) + idx, make_float2(w * g0, w * g1));
+            const float a = w * g0, b = w * g1;
+            if (a != 0.f) atomicAdd(T + 2 * (size_t)idx, to_fix(a));
+            if (b != 0.f) atomicAdd(T + 2 * (size_t)idx + 1, to_fix(b));
         }
     }
 }
@@ -476,22 +507,24 @@ __global__ void k_guide_adam_mlp(AdamArgs A, float* p, float* g, float* m, float
     if (i < n_weights) w16[i] = __float2bfloat16_rn(pi);
 }
 
-__global__ void k_guide_adam_table(AdamArgs A, float* p, float* g, float* m, float* v, __half* t16, uint32_t n) {
+__global__ void k_guide_adam_table(AdamArgs A, float* p, unsigned long long* g, float* m, float* v, __half* t16,
+                                   uint32_t n) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || A.c[2] == 0.f) return;
     const float c1 = A.c[0], c2 = A.c[1];
     // Lazy (sparse) Adam: a table entry no record touched this step keeps its
     // parameter and moments. A batch touches a few percent of the 16M
     // entries, so the step reads the gradient table and updates only those.
-    float gi = g[i];
-    if (gi == 0.f) return;
+    const unsigned long long q = g[i];
+    if (q == 0ull) return;
+    float gi = from_fix(q);
     float mi = A.b1 * m[i] + (1.f - A.b1) * gi;
     float vi = A.b2 * v[i] + (1.f - A.b2) * gi * gi;
     m[i] = mi;
     v[i] = vi;
     float pi = p[i] - A.lr * (mi * c1) / (sqrtf(vi * c2) + A.eps);
     p[i] = pi;
-    g[i] = 0.f;
+    g[i] = 0ull;
     t16[i] = __float2half_rn(pi);
 }
 
@@ -544,7 +577,9 @@ struct rt_guide {
     float* vw = nullptr;
     __nv_bfloat16* w16 = nullptr;
     float* t32 = nullptr;      // table master (levels * T * 2)
-    float* gt = nullptr;
+    unsigned long long* gt = nullptr;  // table gradient, 2^-24 fixed point
+    float* part = nullptr;     // backward CTAs' dW / db partial rows (bwd_rows x G_NPARAMS)
+    int bwd_rows = 0;
     float* mt = nullptr;
     float* vt = nullptr;
     __half* t16 = nullptr;
@@ -624,10 +659,11 @@ static int launch_forward(rt_guide* g, const float* rec, uint32_t n, int mode, c
 static int launch_backward(rt_guide* g, const float* rec, uint32_t n, cudaStream_t st,
                            BatchSel B = BatchSel{nullptr, 0, 1}) {
     uint32_t tiles = (n + TILE - 1) / TILE;
-    int grid = (int)std::min<uint32_t>(tiles, (uint32_t)g->sms * 2);
+    int grid = (int)std::min<uint32_t>(tiles, (uint32_t)g->bwd_rows);
     G_TRY(cudaMemsetAsync(g->loss, 0, 4, st));
-    k_guide_bwd<<<grid, TILE, B_BYTES, st>>>(g->G, g->X0, g->acts, g->out, rec, n, B, g->gw, g->gw + G_NWEIGHTS,
-                                             g->dX0, g->loss, g->err);
+    k_guide_bwd<<<grid, TILE, B_BYTES, st>>>(g->G, g->X0, g->acts, g->out, rec, n, B, g->part, g->dX0, g->loss,
+                                             g->err);
+    k_guide_grad_reduce<<<(G_NPARAMS + 255) / 256, 256, 0, st>>>(g->part, grid, g->gw);
     k_guide_hash_bwd<<<(n + 127) / 128, 128, 0, st>>>(g->G, rec, g->dX0, n, B, g->gt);
     G_TRY(cudaGetLastError());
     return 0;
@@ -708,6 +744,8 @@ int rt_guide_create(const float* lo, const float* hi, uint64_t seed, float lr, r
     rc = rc ? rc : g->alloc(&g->w16, G_NWEIGHTS);
     rc = rc ? rc : g->alloc(&g->t32, tn);
     rc = rc ? rc : g->alloc(&g->gt, tn);
+    g->bwd_rows = g->sms * 2;
+    rc = rc ? rc : g->alloc(&g->part, (size_t)g->bwd_rows * G_NPARAMS);
     rc = rc ? rc : g->alloc(&g->mt, tn);
     rc = rc ? rc : g->alloc(&g->vt, tn);
     rc = rc ? rc : g->alloc(&g->t16, tn);
@@ -751,7 +789,7 @@ int rt_guide_create(const float* lo, const float* hi, uint64_t seed, float lr, r
     cudaMemset(g->gw, 0, G_NPARAMS * 4);
     cudaMemset(g->mw, 0, G_NPARAMS * 4);
     cudaMemset(g->vw, 0, G_NPARAMS * 4);
-    cudaMemset(g->gt, 0, tn * 4);
+    cudaMemset(g->gt, 0, tn * 8);
     cudaMemset(g->mt, 0, tn * 4);
     cudaMemset(g->vt, 0, tn * 4);
     cudaMemset(g->err, 0, 4);
@@ -858,16 +896,20 @@ int rt_guide_grads(rt_guide* g, const float* rec_host, uint32_t n, float* g_mlp,
     G_TRY(cudaMemcpy(rec, rec_host, (size_t)n * 64, cudaMemcpyHostToDevice));
     size_t tn = (size_t)G_LEVELS * G_T * 2;
     cudaMemset(g->gw, 0, G_NPARAMS * 4);
-    cudaMemset(g->gt, 0, tn * 4);
+    cudaMemset(g->gt, 0, tn * 8);
     int rc = launch_forward(g, rec, n, FWD_TRAIN, 0);
     rc = rc ? rc : launch_backward(g, rec, n, 0);
     if (!rc) rc = check_err(g, 0);
     if (!rc && g_mlp) G_TRY(cudaMemcpy(g_mlp, g->gw, G_NPARAMS * 4, cudaMemcpyDeviceToHost));
-    if (!rc && g_table) G_TRY(cudaMemcpy(g_table, g->gt, tn * 4, cudaMemcpyDeviceToHost));
+    if (!rc && g_table) {
+        std::vector<long long> q(tn);
+        G_TRY(cudaMemcpy(q.data(), g->gt, tn * 8, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < tn; i++) g_table[i] = (float)q[i] * (1.0f / G_FIX_SCALE);
+    }
     if (!rc && raw_out) G_TRY(cudaMemcpy(raw_out, g->out, (size_t)n * G_OUT * 4, cudaMemcpyDeviceToHost));
     if (!rc && loss) G_TRY(cudaMemcpy(loss, g->loss, 4, cudaMemcpyDeviceToHost));
     cudaMemset(g->gw, 0, G_NPARAMS * 4);
-    cudaMemset(g->gt, 0, tn * 4);
+    cudaMemset(g->gt, 0, tn * 8);
     cudaFree(rec);
     return rc;
 }

@@ -67,6 +67,7 @@ struct Paths {
     float* tr_rec;         // training vertices: [P][max_depth] x TR_FLOATS
     float* tb_rec;         // training batch, 16 floats per record
     uint32_t* tb_cnt;      // [0] records kept, [1] candidate records
+    uint32_t* tb_blk;      // collection: kept records per block, then their offsets
     float* tr_keep;        // probability of keeping a candidate (device word)
     uint32_t tr_tag, tb_cap;
 };
@@ -389,53 +390,108 @@ __device__ __forceinline__ uint32_t hash32(uint32_t x) {
     return x;
 }
 
-__global__ void k_guide_collect(Paths P, PtConsts C) {
-    // One thread per (slot, depth): the records of a path are consecutive, so
-    // the threads of a warp read neighbouring records of a few paths. A path
-    // opened records 0 .. depth-1 (its final bounce count); threads past that
-    // leave without touching the record buffer.
-    const float keep = *P.tr_keep;
-    const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// Collection of the slab's closed training vertices, one thread per (slot,
+// depth): the records of a path are consecutive, so the threads of a warp
+// read neighbouring records of a few paths. A path opened records
+// 0 .. depth-1 (its final bounce count); threads past that touch nothing.
+// Whether a vertex is a candidate and whether it is kept depend only on the
+// vertex (the keep draw hashes (slot, depth, slab tag)), and the kept records
+// are written in (slot, depth) order -- per-block counts, an exclusive scan
+// of the counts, then each record at its block's offset plus its rank in the
+// block -- so the batches the Adam steps take are the same on every run.
+__device__ __forceinline__ bool collect_vertex(const Paths& P, const PtConsts& C, float keep, uint64_t id, bool& cand,
+                                               float& wt, const float*& rec) {
     const uint32_t slot = (uint32_t)(id / C.max_depth), d = (uint32_t)(id % C.max_depth);
-    bool cand = false, kept = false;
-    float wt = 0.0f;
-    const float* rec = nullptr;
-    if (slot < P.P && d < (__float_as_uint(P.prev[slot].w) >> FL_DEPTH_SHIFT)) {
-        const float* r = P.tr_rec + ((size_t)slot * C.max_depth + d) * TR_FLOATS;
-        float2 tags = *reinterpret_cast<const float2*>(r + 18);
-        if (__float_as_uint(tags.x) == P.tr_tag && __float_as_uint(tags.y) == P.tr_tag) {
-            const float4 Le = P.L[slot];
-            float3 dl = f3(Le.x - r[15], Le.y - r[16], Le.z - r[17]);
-            float w = luminance(dl) / fmaxf(luminance(f3(r[12], r[13], r[14])), 1e-8f);
-            cand = w > 0.0f && isfinite(w);
-            uint32_t h = hash32((slot * C.max_depth + d) ^ hash32(P.tr_tag));
-            kept = cand && (float)(h >> 8) * (1.0f / 16777216.0f) < keep;
-            wt = w;
-            rec = r;
-        }
+    cand = false;
+    wt = 0.0f;
+    rec = nullptr;
+    if (slot >= P.P || d >= (__float_as_uint(P.prev[slot].w) >> FL_DEPTH_SHIFT)) return false;
+    const float* r = P.tr_rec + ((size_t)slot * C.max_depth + d) * TR_FLOATS;
+    float2 tags = *reinterpret_cast<const float2*>(r + 18);
+    if (__float_as_uint(tags.x) != P.tr_tag || __float_as_uint(tags.y) != P.tr_tag) return false;
+    const float4 Le = P.L[slot];
+    float3 dl = f3(Le.x - r[15], Le.y - r[16], Le.z - r[17]);
+    float w = luminance(dl) / fmaxf(luminance(f3(r[12], r[13], r[14])), 1e-8f);
+    cand = w > 0.0f && isfinite(w);
+    uint32_t h = hash32((slot * C.max_depth + d) ^ hash32(P.tr_tag));
+    wt = w;
+    rec = r;
+    return cand && (float)(h >> 8) * (1.0f / 16777216.0f) < keep;
+}
+
+#define COLLECT_BLOCK 256
+
+// Pass 1: kept records per block (P.tb_blk), candidates counted into
+// tb_cnt[1] (an integer sum: the same in any order).
+__global__ void __launch_bounds__(COLLECT_BLOCK) k_guide_collect_count(Paths P, PtConsts C) {
+    __shared__ uint32_t warp_kept[COLLECT_BLOCK / 32];
+    const float keep = *P.tr_keep;
+    const uint64_t id = (uint64_t)blockIdx.x * COLLECT_BLOCK + threadIdx.x;
+    bool cand;
+    float wt;
+    const float* rec;
+    const bool kept = collect_vertex(P, C, keep, id, cand, wt, rec);
+    const uint32_t km = __ballot_sync(0xFFFFFFFFu, kept), cm = __ballot_sync(0xFFFFFFFFu, cand);
+    if (lane_id() == 0) {
+        warp_kept[threadIdx.x >> 5] = __popc(km);
+        if (cm) atomicAdd(P.tb_cnt + 1, (uint32_t)__popc(cm));
     }
-    // Warp-aggregated appends: one atomic per warp for the kept records and
-    // one for the candidate count.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < COLLECT_BLOCK / 32; w++) t += warp_kept[w];
+        P.tb_blk[blockIdx.x] = t;
+    }
+}
+
+// Pass 2: exclusive scan of the nb block counts in place (one block), total
+// kept into tb_cnt[0].
+__global__ void __launch_bounds__(1024) k_guide_collect_scan(uint32_t* blk, uint32_t nb, uint32_t* tb_cnt) {
+    __shared__ uint32_t part[1024];
+    const uint32_t t = threadIdx.x, per = (nb + 1023) / 1024, b0 = t * per, b1 = min(nb, b0 + per);
+    uint32_t sum = 0;
+    for (uint32_t b = b0; b < b1; b++) sum += blk[b];
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {
+        const uint32_t v = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;  // exclusive prefix of this thread's chunk
+    for (uint32_t b = b0; b < b1; b++) {
+        const uint32_t c = blk[b];
+        blk[b] = run;
+        run += c;
+    }
+    if (t == 1023) tb_cnt[0] = part[1023];
+}
+
+// Pass 3: each kept record to its block's offset plus its rank in the block.
+__global__ void __launch_bounds__(COLLECT_BLOCK) k_guide_collect_write(Paths P, PtConsts C) {
+    __shared__ uint32_t warp_off[COLLECT_BLOCK / 32];
+    const float keep = *P.tr_keep;
+    const uint64_t id = (uint64_t)blockIdx.x * COLLECT_BLOCK + threadIdx.x;
+    bool cand;
+    float wt;
+    const float* rec;
+    const bool kept = collect_vertex(P, C, keep, id, cand, wt, rec);
     const uint32_t km = __ballot_sync(0xFFFFFFFFu, kept);
-    uint32_t base = 0;
-    if (km) {
-        const uint32_t leader = __ffs(km) - 1;
-        if (lane_id() == leader) base = atomicAdd(P.tb_cnt, (uint32_t)__popc(km));
-        base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (lane_id() == 0) warp_off[threadIdx.x >> 5] = __popc(km);
+    __syncthreads();
+    if (!kept) return;
+    uint32_t base = P.tb_blk[blockIdx.x];
+    for (uint32_t w = 0; w < (threadIdx.x >> 5); w++) base += warp_off[w];
+    const uint32_t idx = base + __popc(km & ((1u << lane_id()) - 1u));
+    if (idx < P.tb_cap) {
+        float4* o = reinterpret_cast<float4*>(P.tb_rec + (size_t)idx * 16);
+        const float4* ri = reinterpret_cast<const float4*>(rec);
+        o[0] = ri[0];
+        o[1] = ri[1];
+        o[2] = ri[2];
+        o[3] = make_float4(fminf(wt, 50.0f), 0.0f, 0.0f, 0.0f);
     }
-    if (kept) {
-        const uint32_t idx = base + __popc(km & ((1u << lane_id()) - 1u));
-        if (idx < P.tb_cap) {
-            float4* o = reinterpret_cast<float4*>(P.tb_rec + (size_t)idx * 16);
-            const float4* ri = reinterpret_cast<const float4*>(rec);
-            o[0] = ri[0];
-            o[1] = ri[1];
-            o[2] = ri[2];
-            o[3] = make_float4(fminf(wt, 50.0f), 0.0f, 0.0f, 0.0f);
-        }
-    }
-    uint32_t m = __ballot_sync(0xFFFFFFFFu, cand);
-    if (lane_id() == 0 && m) atomicAdd(P.tb_cnt + 1, (uint32_t)__popc(m));
 }
 
 // Keep probability for this slab's collection: aim the expected batch at 95%

@@ -375,6 +375,7 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     rc = rc ? rc : s->alloc(&Pp.tr_rec, tr_floats);
     rc = rc ? rc : s->alloc(&Pp.tb_rec, guided ? (size_t)Pp.tb_cap * 16 : 1);
     rc = rc ? rc : s->alloc(&Pp.tb_cnt, 4);
+    rc = rc ? rc : s->alloc(&Pp.tb_blk, guided ? (P * params->max_depth + COLLECT_BLOCK - 1) / COLLECT_BLOCK : 1);
     rc = rc ? rc : s->alloc(&keep, 1);
     if (!rc) {
         const float one = 1.0f;
@@ -566,11 +567,14 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
             Paths Pc = P;
             Pc.tb_cap = steps * batch;
             const uint64_t collect_threads = (uint64_t)P.P * C.max_depth;
-            k_guide_collect<<<(unsigned)((collect_threads + 255) / 256), 256, 0, st>>>(Pc, C);
+            const uint32_t nb = (uint32_t)((collect_threads + COLLECT_BLOCK - 1) / COLLECT_BLOCK);
+            k_guide_collect_count<<<nb, COLLECT_BLOCK, 0, st>>>(Pc, C);
+            k_guide_collect_scan<<<1, 1024, 0, st>>>(Pc.tb_blk, nb, Pc.tb_cnt);
+            k_guide_collect_write<<<nb, COLLECT_BLOCK, 0, st>>>(Pc, C);
             int grc = guide_train_slices(s->guide, P.tb_rec, P.tb_cnt, batch, steps, st);
             if (grc) return fail(grc, rt_guide_last_error());
             guide_trainings += (int)steps;
-            launches += 3 + 7 * (uint64_t)steps;
+            launches += 4 + 8 * (uint64_t)steps;
             s->guide_prev_k = k;
             s->guide_trained_passes += k;
             last_records_slab = steps * batch;

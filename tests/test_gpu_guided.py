@@ -150,3 +150,24 @@ def test_training_stops_after_budget():
         np.testing.assert_array_equal(m0, m1)
         np.testing.assert_array_equal(t0, t1)
         assert np.isfinite(g.image()).all()
+
+
+def test_guided_same_seed_bitwise():
+    """Training is deterministic (gradients summed in a fixed order or as
+    integers, training batches compacted in vertex order), so two guided
+    renders of the same samples train the same network and give the same
+    image bit for bit, over several slabs with training between them."""
+    s = scenes.two_rooms(160, 90)
+    p = abi.make_params(max_depth=16, guided=True)
+    imgs, mlps, tables = [], [], []
+    for _ in range(2):
+        with PtSession(s, p) as g:
+            g.render_samples(0, 12)   # slabs of 1, 2, 4 and 5 passes, each followed by Adam steps
+            imgs.append(g.image())
+            m, t = g.guide().params()
+            mlps.append(m)
+            tables.append(t)
+            assert g.stats()["guide_steps"] > 0
+    assert np.array_equal(mlps[0], mlps[1])
+    assert np.array_equal(tables[0], tables[1])
+    assert np.array_equal(imgs[0], imgs[1])
