@@ -14,12 +14,12 @@ Printed (one JSON line on rank 0):
              (rt_session_create from host arrays, incl. the device BVH build,
              + rt_render_samples of the 32 passes + rt_read_image to host),
              host<->device copies included;
-  roofline   the closest-hit (extend) kernel: algorithmic bytes per camera
-             sample of the reference's extension rays (reference binary BVH:
-             32 B per node visit, 48 B per triangle test, 48 B per instance
-             visit, 48 B ray in/out, counted by the f64 oracle on a pixel
-             sample of the same frame) x samples per launch / launch time,
-             against the measured HBM copy bandwidth;
+  roofline   the closest-hit (extend) kernel: algorithmic bytes per
+             extension ray (reference binary BVH: 32 B per node visit, 48 B
+             per triangle test, 48 B per instance visit, 48 B ray in/out,
+             counted by the f64 oracle on a pixel sample of the same frame)
+             x extension rays per launch / launch time, against the measured
+             HBM copy bandwidth;
   cpu_baseline  the f64 oracle (C++ restatement of the reference's CPU path
              tracer, all host threads) on a bounded pixel sample of the frame.
   workloads  the other configurations: the 1M-triangle cloud at 1920x1080 x
@@ -593,15 +593,23 @@ def main():
             cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
                    "seconds": round(el, 2)}
             launches_ext = max(1.0, ext_launches)
-            alg_bytes = work["ext_bytes_per_sample"] * samples
+            # Bytes per extension ray (the reference's binary BVH, counted by
+            # the oracle) x the extension rays a launch traces.
+            alg_bytes = work["ext_bytes_per_ray"] * ext_rays
             achieved = alg_bytes / (ext_ms / 1e3) / 1e9
+            # The same work counted per camera sample: a GPU ray passes the
+            # cutouts it does not stop at inside one traversal, where the
+            # reference traces a new ray after each, so it covers the work of
+            # several reference rays.
+            per_sample = work["ext_bytes_per_sample"] * samples / (ext_ms / 1e3) / 1e9
             roof = {"kernel": "k_extend (closest hit, 8-wide BVH, cutouts decided in traversal)", "bound": "hbm",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                     "traffic": EXTEND_DRAM_BYTES_PER_LAUNCH, "traffic_source": EXTEND_DRAM_SOURCE,
                     "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg_bytes / launches_ext,
-                    "samples_per_launch": samples / launches_ext, "launch_ms": ext_ms / launches_ext,
-                    "launches": int(launches_ext), "per_sample_work": work,
-                    "gpu_extension_rays_per_sample": ext_rays / max(samples, 1)}
+                    "rays_per_launch": ext_rays / launches_ext, "launch_ms": ext_ms / launches_ext,
+                    "launches": int(launches_ext), "reference_work": work,
+                    "gpu_extension_rays_per_sample": ext_rays / max(samples, 1),
+                    "achieved_per_sample_normalised": per_sample}
         workloads = None
         if not args.no_workloads and world == 1:
             workloads = other_workloads(flush, stream)

@@ -70,6 +70,15 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count);
 /* Zero the accumulators (beauty and AOVs). */
 int rt_reset(rt_session* s);
 
+/* Limits of the device's bounded loops for the following calls, as
+ * rt_params.max_trav_steps and wait_polls (0 = the defaults, 2^22 traversal
+ * steps per ray and 2^24 polls per tensor-core pipeline wait). A loop that
+ * reaches its limit ends, sets the session's device error word, and the call
+ * returns RT_ERR_DEVICE; the session stays usable (rt_reset, then render
+ * again). The reference's counterpart is the GPU watchdog retry of
+ * PtSession::render_samples (src/raytracer/metal/renderer.rs:406-437). */
+int rt_set_limits(rt_session* s, uint32_t max_trav_steps, uint32_t wait_polls);
+
 /* Copy the f64 accumulator: 4 doubles per pixel (r, g, b sums, sample
  * weight), row-major from the top-left pixel. Replaces
  * PtSession::sum_and_weight (renderer.rs:476-490). */

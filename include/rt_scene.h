@@ -258,6 +258,10 @@ typedef struct rt_params {
     uint32_t bvh_build;       /* 0 = build the BVHs on the GPU, 1 = on the host (same trees) */
     uint32_t guide_train_passes; /* train the proposal during the first this many sample passes,
                                     then keep it fixed (0 = 512; 0xFFFFFFFF = never stop) */
+    uint32_t max_trav_steps;  /* traversal steps one ray may take before the kernel gives it up
+                                 and reports RT_ERR_DEVICE (0 = 2^22) */
+    uint32_t wait_polls;      /* polls of a tensor-core pipeline wait in the learned proposal's
+                                 kernels before they report RT_ERR_DEVICE (0 = 2^24) */
 } rt_params;
 
 /* Size checks shared by every consumer of the descriptor. */
@@ -267,7 +271,7 @@ static_assert(sizeof(rt_instance_desc) == 104, "rt_instance_desc layout");
 static_assert(sizeof(rt_material_desc) == 264, "rt_material_desc layout");
 static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
 static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
-static_assert(sizeof(rt_params) == 64, "rt_params layout");
+static_assert(sizeof(rt_params) == 72, "rt_params layout");
 static_assert(sizeof(rt_pattern_input) == 32, "rt_pattern_input layout");
 static_assert(sizeof(rt_pattern_desc) == 264, "rt_pattern_desc layout");
 static_assert(sizeof(rt_texture_desc) == 16, "rt_texture_desc layout");

@@ -186,7 +186,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 3) k_guide_fwd(GuideDev G, const 
                 tc_gemm_issue(acc, s0 + act, s0 + w_sm, N, K, false);
                 tc_commit(&mbar[grp]);
             }
-            if (!mbar_wait_bounded(&mbar[grp], phase)) group_failed[grp] = 1;
+            if (!mbar_wait_or_drain(&mbar[grp], phase, G.wait_polls)) group_failed[grp] = 1;
             phase ^= 1u;
             group_sync(grp);
             if (group_failed[grp]) {
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(TILE) k_guide_bwd(GuideDev G, const __nv_bfloa
                 tc_gemm_issue(tb + B_TMEM_DH, s0 + B_DZ, s0 + wt, K_in, N_out, false);
                 tc_commit(&mbar);
             }
-            bool ok = mbar_wait_bounded(&mbar, phase);
+            bool ok = mbar_wait_or_drain(&mbar, phase, G.wait_polls);
             phase ^= 1u;
             if (__syncthreads_or(!ok)) {
                 failed = true;
@@ -622,6 +622,9 @@ struct rt_guide {
             cap = std::max(n, 1u << 16);
             rc = rc ? rc : alloc(&X0, (size_t)cap * G_IN);
             rc = rc ? rc : alloc(&out, (size_t)cap * G_OUT);
+            // Zeroed, so rows a failed forward pass did not write hold an
+            // empty mixture rather than stale bits.
+            if (!rc && cudaMemset(out, 0, (size_t)cap * G_OUT * 4) != cudaSuccess) rc = gfail(-2, "cudaMemset");
         }
         if (train && n > train_cap) {
             release(acts);
@@ -706,6 +709,7 @@ int guide_reserve(rt_guide* g, uint32_t n) { return g->ensure(n, false); }
 const float* guide_loss_ptr(rt_guide* g) { return g->loss; }
 const uint32_t* guide_err_ptr(rt_guide* g) { return g->err; }
 GuideDev guide_dev(rt_guide* g) { return g->G; }
+void guide_set_wait_polls(rt_guide* g, uint32_t polls) { g->G.wait_polls = polls ? polls : (1u << 24); }
 
 }  // namespace rt
 
@@ -795,6 +799,7 @@ int rt_guide_create(const float* lo, const float* hi, uint64_t seed, float lr, r
     cudaMemset(g->err, 0, 4);
     cudaMemset(g->step, 0, 4);
     g->G.table = reinterpret_cast<const __half2*>(g->t16);
+    g->G.wait_polls = 1u << 24;
     g->G.w = g->w16;
     g->G.b = g->w32 + G_NWEIGHTS;
     // Level resolutions: geometric from 16 to 2048.

@@ -57,6 +57,7 @@ struct GuideDev {
     const float* b;           // biases
     float res[G_LEVELS];      // grid resolution per level
     float lo[3], inv_ext[3];  // scene bounds -> [0,1]^3
+    uint32_t wait_polls;      // polls of a tensor-core pipeline wait before it reports an error
 };
 
 // Table slot of a grid vertex. Vertices are stored in 2x2x2 blocks of 8

@@ -23,5 +23,8 @@ int guide_reserve(rt_guide* g, uint32_t n);
 const float* guide_loss_ptr(rt_guide* g);
 const uint32_t* guide_err_ptr(rt_guide* g);
 GuideDev guide_dev(rt_guide* g);
+// Polls of a tensor-core pipeline wait before the network's kernels report
+// an error (0 = the default of 2^24).
+void guide_set_wait_polls(rt_guide* g, uint32_t polls);
 
 }  // namespace rt

@@ -592,7 +592,7 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
                 break;
             bool done_now = false;
             if (want) {
-                if (++steps > RT_MAX_TRAV_STEPS) {
+                if (++steps > S.max_steps) {
                     atomicOr(err, RT_DEVERR_ITER);
                     done_now = true;
                 } else if (RT_FUSED_POP) {

@@ -210,6 +210,7 @@ struct DevScene {
     float inf_total;
     float p_infinite;
     uint32_t any_presence;       // some material has presence < 1
+    uint32_t max_steps;          // traversal steps per ray before the query is given up (error bit)
     uint32_t dome;               // first dome light (misses see it), ~0 for none
     // Environment map of light env_light (src/scene/envmap.rs): lat-long
     // texels (RGB + pad), row-marginal CDF (env_h + 1), per-row conditional

@@ -284,6 +284,7 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
         rc = rc ? rc : s->upload((const uint4**)&S.inst, H.inst);
         rc = rc ? rc : s->upload((const uint2**)&S.items, H.items);
     }
+    S.max_steps = params->max_trav_steps ? params->max_trav_steps : RT_MAX_TRAV_STEPS;
     rc = rc ? rc : s->upload(&S.meshes, H.meshes);
     rc = rc ? rc : s->upload(&S.orig_idx, H.orig_idx);
     rc = rc ? rc : s->upload(&S.normals, H.normals);
@@ -396,6 +397,8 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
         const float lr = params->guide_lr > 0.0 ? (float)params->guide_lr : 1e-2f;
         if (rt_guide_create(lo, hi, 0x5eed, lr, &s->guide) != 0 || guide_reserve(s->guide, (uint32_t)P) != 0)
             rc = fail(RT_ERR_CUDA, rt_guide_last_error());
+        else
+            guide_set_wait_polls(s->guide, params->wait_polls);
     }
     if (rc) {
         delete s;
@@ -441,6 +444,15 @@ int rt_average_spp(rt_session* s, double* out) {
     double sum = 0.0;
     for (size_t p = 0; p < s->npix; p++) sum += a[4 * p + 3];
     *out = sum / (double)s->npix;
+    return RT_OK;
+}
+
+int rt_set_limits(rt_session* s, uint32_t max_trav_steps, uint32_t wait_polls) {
+    if (!s) return fail(RT_ERR_INVALID, "session is NULL");
+    s->params.max_trav_steps = max_trav_steps;
+    s->params.wait_polls = wait_polls;
+    s->S.max_steps = max_trav_steps ? max_trav_steps : RT_MAX_TRAV_STEPS;
+    if (s->guide) guide_set_wait_polls(s->guide, wait_polls);
     return RT_OK;
 }
 
@@ -617,7 +629,11 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
         uint32_t gerr = 0, nrec = 0;
         float loss = 0.f;
         CUDA_TRY(cudaMemcpy(&gerr, guide_err_ptr(s->guide), 4, cudaMemcpyDeviceToHost));
-        if (gerr) return fail(RT_ERR_DEVICE, "guide network: tensor-core pipeline wait timed out");
+        if (gerr) {
+            cudaMemsetAsync((void*)guide_err_ptr(s->guide), 0, 4, st);
+            cudaStreamSynchronize(st);
+            return fail(RT_ERR_DEVICE, "guide network: tensor-core pipeline wait timed out");
+        }
         CUDA_TRY(cudaMemcpy(&nrec, P.tb_cnt, 4, cudaMemcpyDeviceToHost));
         CUDA_TRY(cudaMemcpy(&loss, guide_loss_ptr(s->guide), 4, cudaMemcpyDeviceToHost));
         s->last.guide_records = std::min(nrec, last_records_slab);

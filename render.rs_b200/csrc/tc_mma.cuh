@@ -84,11 +84,38 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t phase) {
         : "memory");
     return ok != 0;
 }
+// Non-blocking test of a barrier phase.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* mbar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(mbar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
 // Bounded wait: returns false (and the caller records an error) if the
-// barrier phase has not completed after `limit` polls.
+// barrier phase has not completed after `limit` polls. Polls block for a
+// while (try_wait) unless the limit is tiny (at most 64), where they return
+// at once (test_wait) so that such a limit really runs out.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* mbar, uint32_t phase, uint32_t limit = (1u << 24)) {
+    if (limit <= 64) {
+        for (uint32_t i = 0; i < limit; i++)
+            if (mbar_test_wait(mbar, phase)) return true;
+        return false;
+    }
     for (uint32_t i = 0; i < limit; i++)
         if (mbar_try_wait(mbar, phase)) return true;
+    return false;
+}
+// A pipeline wait with a settable limit. When it runs out the caller
+// reports an error, but the MMAs it already issued are still drained first
+// (a second wait with the default limit), so no tensor-core work writes the
+// TMEM the caller then frees. Returns false when the first wait ran out.
+__device__ __forceinline__ bool mbar_wait_or_drain(uint64_t* mbar, uint32_t phase, uint32_t limit) {
+    if (mbar_wait_bounded(mbar, phase, limit)) return true;
+    mbar_wait_bounded(mbar, phase);
     return false;
 }
 

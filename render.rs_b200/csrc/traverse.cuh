@@ -243,7 +243,7 @@ struct TraceHit {
 // Error bits written to the device error word.
 #define RT_DEVERR_STACK 1u
 #define RT_DEVERR_ITER 2u
-#define RT_MAX_TRAV_STEPS (1u << 22)
+#define RT_MAX_TRAV_STEPS (1u << 22)   // default of DevScene::max_steps (rt_params.max_trav_steps)
 
 // Resumable traversal state of one ray (registers), so persistent warps can
 // advance rays a few steps at a time and refill lanes whose ray finished.

@@ -187,6 +187,8 @@ class RtParams(C.Structure):
         ("guide_depth", C.c_uint32),
         ("bvh_build", C.c_uint32),
         ("guide_train_passes", C.c_uint32),
+        ("max_trav_steps", C.c_uint32),
+        ("wait_polls", C.c_uint32),
     ]
 
 
@@ -194,14 +196,14 @@ LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK, LIGHT_DOME = r
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
 for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 264), (RtLightDesc, 120),
-               (RtCameraDesc, 144), (RtParams, 64), (RtPatternInput, 32), (RtPatternDesc, 264),
+               (RtCameraDesc, 144), (RtParams, 72), (RtPatternInput, 32), (RtPatternDesc, 264),
                (RtPatternBinding, 16), (RtTextureDesc, 16), (RtIesDesc, 112), (RtSceneDesc, 296)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
 
 def make_params(max_depth=8, rr_start=3, firefly_clamp=60.0, aovs=False, guided=False,
                 guide_fraction=0.5, max_paths=0, guide_lr=0.0, guide_steps=0, guide_depth=0, bvh_build="device",
-                guide_train_passes=0):
+                guide_train_passes=0, max_trav_steps=0, wait_polls=0):
     """Integrator knobs; defaults follow the reference's constants
     (src/raytracer/pt/mod.rs:26-32) except the bounce cap, which the configs set.
     guide_lr / guide_steps: Adam learning rate and steps per sample pass of the
@@ -209,9 +211,12 @@ def make_params(max_depth=8, rr_start=3, firefly_clamp=60.0, aovs=False, guided=
     below it use the proposal (0 = every depth); guide_train_passes: sample
     passes that train the proposal before it is kept fixed (0 = 512,
     0xFFFFFFFF = never stop). bvh_build: "device" (default) or "host" builds
-    the same BVHs on the GPU or on the host cores."""
+    the same BVHs on the GPU or on the host cores. max_trav_steps / wait_polls:
+    limits of the device's bounded loops (0 = 2^22 traversal steps per ray and
+    2^24 polls per tensor-core pipeline wait); a loop that reaches its limit
+    ends and the call returns RT_ERR_DEVICE."""
     if bvh_build not in ("device", "host"):
         raise ValueError("bvh_build must be 'device' or 'host'")
     return RtParams(max_depth, rr_start, firefly_clamp, 1 if aovs else 0, 1 if guided else 0,
                     guide_fraction, max_paths, guide_lr, guide_steps, guide_depth,
-                    0 if bvh_build == "device" else 1, guide_train_passes)
+                    0 if bvh_build == "device" else 1, guide_train_passes, max_trav_steps, wait_polls)

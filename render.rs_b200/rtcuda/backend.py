@@ -33,7 +33,7 @@ EXPORTS = ("rt_session_create", "rt_session_destroy", "rt_last_error", "rt_rende
            "rt_average_spp", "rt_checkpoint_save_rckp", "rt_rckp_write", "rt_accum_exr_write",
            "rt_accum_exr_info", "rt_accum_exr_read", "rt_accum_merge", "rt_read_film", "rt_denoise",
            "rt_denoise_film", "rt_film_exr_write", "rt_pcg_streams", "rt_light_sample_batch",
-           "rt_light_pmf_batch", "rt_transmittance_batch")
+           "rt_light_pmf_batch", "rt_transmittance_batch", "rt_set_limits")
 
 
 class RtError(RuntimeError):
@@ -102,6 +102,7 @@ def lib():
         L.rt_light_sample_batch.argtypes = [vp, vp, vp, u32, vp, vp]
         L.rt_light_pmf_batch.argtypes = [vp, vp, vp, u32, vp]
         L.rt_transmittance_batch.argtypes = [vp, vp, u64, vp]
+        L.rt_set_limits.argtypes = [vp, u32, u32]
         _lib = L
     return _lib
 
@@ -235,6 +236,10 @@ class PtSession:
         """Device-pointer ray batch, enqueued without a host sync."""
         _check(lib().rt_intersect_batch_device(self.h, planes_ptr, n, 1 if any_hit else 0, prim_ptr, inst_ptr,
                                                t_ptr, stream))
+
+    def set_limits(self, max_trav_steps=0, wait_polls=0):
+        """Limits of the device's bounded loops (0 = defaults)."""
+        _check(lib().rt_set_limits(self.h, max_trav_steps, wait_polls))
 
     def light_sample(self, points, u):
         """Device light-BVH picks at (m, 3) points with (m,) uniforms:
