@@ -208,6 +208,40 @@ typedef struct rt_ies_desc {
     double world_to_local[9];
 } rt_ies_desc;
 
+/* Analytic RiSpec quadrics, the reference's legacy primitives
+ * (src/geometry/sphere.rs, cylinder.rs, cone.rs, extra.rs): each is
+ * intersected in its own object space (the ray transformed by the inverse
+ * of object_to_world, its direction normalised there), its hit distance is
+ * the world distance from the ray origin, and the scene tests them all
+ * before the meshes, as Scene::intersect's scan of `objects` does
+ * (src/scene/mod.rs:105-146). params by type (angles in degrees):
+ *   SPHERE       radius, zmin, zmax, thetamax
+ *   CYLINDER     radius, zmin, zmax, thetamax
+ *   CONE         height, radius, thetamax
+ *   TORUS        major radius, minor radius, phimin, phimax, thetamax
+ *   DISK         height, radius, thetamax
+ *   PARABOLOID   rmax, zmin, zmax, thetamax
+ *   HYPERBOLOID  p1 (x, y, z), p2 (x, y, z), thetamax */
+enum {
+    RT_QUADRIC_SPHERE = 0,
+    RT_QUADRIC_CYLINDER = 1,
+    RT_QUADRIC_CONE = 2,
+    RT_QUADRIC_TORUS = 3,
+    RT_QUADRIC_DISK = 4,
+    RT_QUADRIC_PARABOLOID = 5,
+    RT_QUADRIC_HYPERBOLOID = 6
+};
+/* Ray-batch results name a quadric hit by this bit in the instance id, the
+ * quadric's index in the low bits (its primitive id is 0). */
+#define RT_HIT_QUADRIC 0x80000000u
+
+typedef struct rt_quadric_desc {
+    double   object_to_world[12];  /* row-major 3x4 */
+    double   params[8];
+    uint32_t type;                 /* RT_QUADRIC_* */
+    uint32_t material_id;
+} rt_quadric_desc;
+
 typedef struct rt_scene_desc {
     const rt_mesh_desc*     meshes;
     const rt_instance_desc* instances;
@@ -239,6 +273,9 @@ typedef struct rt_scene_desc {
     const rt_ies_desc*        ies;
     uint32_t n_ies;
     uint32_t ies_reserved;    /* 0 */
+    const rt_quadric_desc*    quadrics;
+    uint32_t n_quadrics;
+    uint32_t quadric_reserved; /* 0 */
 } rt_scene_desc;
 
 /* Integrator knobs. The reference hard-codes these as constants
@@ -277,7 +314,8 @@ static_assert(sizeof(rt_pattern_desc) == 264, "rt_pattern_desc layout");
 static_assert(sizeof(rt_texture_desc) == 16, "rt_texture_desc layout");
 static_assert(sizeof(rt_pattern_binding) == 16, "rt_pattern_binding layout");
 static_assert(sizeof(rt_ies_desc) == 112, "rt_ies_desc layout");
-static_assert(sizeof(rt_scene_desc) == 296, "rt_scene_desc layout");
+static_assert(sizeof(rt_quadric_desc) == 168, "rt_quadric_desc layout");
+static_assert(sizeof(rt_scene_desc) == 312, "rt_scene_desc layout");
 }
 #endif
 

@@ -54,6 +54,8 @@ def lib():
         L.oracle_texture_sample.argtypes = [C.c_uint32, C.c_uint32, vp, C.c_int, C.c_uint64, vp, vp]
         L.oracle_ies_eval.argtypes = [C.c_uint32, C.c_uint32, vp, vp, vp, C.c_uint64, vp, vp, vp]
         L.oracle_transmittance.argtypes = [vp, vp, C.c_uint64, vp, C.c_int]
+        L.oracle_quadric_intersect.argtypes = [vp, C.c_uint64, vp, vp]
+        L.oracle_solve_quartic.argtypes = [vp, vp]
         L.oracle_light_pmf.restype = C.c_double
         L.oracle_light_pmf.argtypes = [vp, f64p, C.c_uint32]
         _lib = L
@@ -63,6 +65,22 @@ def lib():
 def _f64(a):
     a = np.ascontiguousarray(a, dtype=np.float64)
     return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def quadric_intersect(desc, origins, directions):
+    """One rt_quadric_desc against rays: (n, 10) = t (-1 on a miss), point,
+    normal, u, v, st density."""
+    r = np.ascontiguousarray(np.hstack([np.atleast_2d(origins), np.atleast_2d(directions)]), dtype=np.float64)
+    out = np.empty((len(r), 10))
+    lib().oracle_quadric_intersect(C.byref(desc), len(r), r.ctypes.data, out.ctypes.data)
+    return out
+
+
+def solve_quartic(coef):
+    c = np.ascontiguousarray(coef, dtype=np.float64)
+    roots = np.zeros(4)
+    n = lib().oracle_solve_quartic(c.ctypes.data, roots.ctypes.data)
+    return roots[:n]
 
 
 def pcg_stream(pixel, sample, n):

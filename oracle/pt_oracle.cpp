@@ -496,6 +496,398 @@ struct Instance {
     double scale = 1.0;  // Matrix4::approx_scale (math/matrix.rs:246-251)
 };
 
+// ---- analytic quadrics (src/geometry/sphere.rs, cylinder.rs, cone.rs, extra.rs) ----
+// The reference's legacy RiSpec primitives: the ray goes to object space
+// with its direction normalised there, the local root is tested against the
+// shape's cuts, and t is the world distance of the hit point from the ray
+// origin. Each function returns the local hit point and local normal.
+struct QuadricHit {
+    V3 p, n;          // object space
+    double u, v;      // RiSpec parameterisation
+    double dpdu, dpdv;
+    bool front_set;   // the shape decides the front face from the world normal (sphere)
+};
+
+// extra.rs:44-54 (phi in [0, 360) from x, y; accepted when <= thetamax).
+static bool q_theta_ok(double x, double y, double thetamax) {
+    if (thetamax >= 360.0) return true;
+    double phi = std::atan2(y, x) * 180.0 / PI;
+    if (phi < 0.0) phi += 360.0;
+    return phi <= thetamax;
+}
+// extra.rs:35-42.
+static double q_phi_u(double x, double y, double thetamax) {
+    double phi = std::atan2(y, x) * 180.0 / PI;
+    if (phi < 0.0) phi += 360.0;
+    return std::min(std::max(phi / std::fmax(thetamax, 1e-9), 0.0), 1.0);
+}
+
+// Real roots of a3 t^3 + a2 t^2 + a1 t + a0, ascending: Cardano with the
+// trigonometric form for three real roots (extra.rs:195-241 solves it the
+// same way).
+static std::vector<double> q_cubic(double a3, double a2, double a1, double a0) {
+    if (std::fabs(a3) < 1e-12) {
+        if (std::fabs(a2) < 1e-12) {
+            if (std::fabs(a1) < 1e-12) return {};
+            return {-a0 / a1};
+        }
+        double disc = a1 * a1 - 4.0 * a2 * a0;
+        if (disc < 0.0) return {};
+        double r = std::sqrt(disc);
+        std::vector<double> v{(-a1 - r) / (2.0 * a2), (-a1 + r) / (2.0 * a2)};
+        std::sort(v.begin(), v.end());
+        return v;
+    }
+    const double a = a2 / a3, b = a1 / a3, c = a0 / a3;
+    const double p = b - a * a / 3.0, q = 2.0 * a * a * a / 27.0 - a * b / 3.0 + c, shift = -a / 3.0;
+    const double disc = q * q / 4.0 + p * p * p / 27.0;
+    std::vector<double> out;
+    if (disc > 0.0) {
+        double r = std::sqrt(disc);
+        out.push_back(std::cbrt(-q / 2.0 + r) + std::cbrt(-q / 2.0 - r) + shift);
+    } else {
+        double m = 2.0 * std::sqrt(std::fmax(-p / 3.0, 0.0));
+        if (m < 1e-30) {
+            out.push_back(shift);
+        } else {
+            double th = std::acos(std::min(std::max(3.0 * q / (p * m), -1.0), 1.0)) / 3.0;
+            for (int k = 0; k < 3; k++) out.push_back(m * std::cos(th - 2.0 * PI * k / 3.0) + shift);
+        }
+    }
+    std::sort(out.begin(), out.end());
+    return out;
+}
+
+// Real roots of a4 t^4 + ... + a0, ascending (extra.rs:112-193): Ferrari's
+// reduction to the resolvent cubic (biquadratic when the depressed quartic
+// has no linear term), each root polished by Newton on the original
+// polynomial, spurious roots and duplicates dropped.
+static std::vector<double> q_quartic(double a4, double a3, double a2, double a1, double a0) {
+    if (std::fabs(a4) < 1e-12) return q_cubic(a3, a2, a1, a0);
+    const double b = a3 / a4, c = a2 / a4, d = a1 / a4, e = a0 / a4;
+    const double p = c - 3.0 * b * b / 8.0;
+    const double q = d - b * c / 2.0 + b * b * b / 8.0;
+    const double r = e - b * d / 4.0 + b * b * c / 16.0 - 3.0 * b * b * b * b / 256.0;
+    const double shift = -b / 4.0;
+    auto f = [&](double t) { return (((a4 * t + a3) * t + a2) * t + a1) * t + a0; };
+    auto df = [&](double t) { return ((4.0 * a4 * t + 3.0 * a3) * t + 2.0 * a2) * t + a1; };
+    auto polish = [&](double t) {
+        for (int it = 0; it < 8; it++) {
+            double g = df(t);
+            if (std::fabs(g) < 1e-30) break;
+            double step = f(t) / g;
+            t -= step;
+            if (std::fabs(step) < 1e-12 * std::fmax(std::fabs(t), 1.0)) break;
+        }
+        return t;
+    };
+    std::vector<double> roots;
+    if (std::fabs(q) < 1e-12) {
+        double disc = p * p - 4.0 * r;
+        if (disc >= 0.0) {
+            double sq = std::sqrt(disc);
+            for (double y2 : {(-p - sq) / 2.0, (-p + sq) / 2.0})
+                if (y2 >= 0.0) {
+                    double y = std::sqrt(y2);
+                    roots.push_back(polish(y + shift));
+                    roots.push_back(polish(-y + shift));
+                }
+        }
+    } else {
+        double z = NAN;
+        for (double zz : q_cubic(1.0, 2.0 * p, p * p - 4.0 * r, -q * q))
+            if (zz > 1e-12 && !(zz <= z)) z = zz;   // the largest positive root
+        if (std::isfinite(z)) {
+            double m = std::sqrt(z), n = q / (2.0 * m);
+            for (int sgn : {1, -1}) {
+                double bq = sgn * m, cq = (p + z) / 2.0 - sgn * n;
+                double disc = bq * bq - 4.0 * cq;
+                if (disc >= 0.0) {
+                    double sq = std::sqrt(disc);
+                    roots.push_back(polish((-bq - sq) / 2.0 + shift));
+                    roots.push_back(polish((-bq + sq) / 2.0 + shift));
+                }
+            }
+        }
+    }
+    std::vector<double> keep;
+    for (double t : roots)
+        if (std::isfinite(t) && std::fabs(f(t)) < 1e-6 * (1.0 + std::pow(std::fabs(t), 4) * std::fabs(a4)))
+            keep.push_back(t);
+    std::sort(keep.begin(), keep.end());
+    std::vector<double> out;
+    for (double t : keep)
+        if (out.empty() || std::fabs(t - out.back()) >= 1e-9) out.push_back(t);
+    return out;
+}
+
+struct Quadric {
+    uint32_t type = 0, material_id = 0;
+    double prm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    M4 transform, inv;
+    double scale = 1.0;  // Matrix4::approx_scale
+
+    // Local intersection; false on a miss.
+    bool local_hit(V3 lo, V3 ld, QuadricHit* h) const {
+        h->front_set = false;
+        switch (type) {
+            case RT_QUADRIC_SPHERE: return sphere(lo, ld, h);
+            case RT_QUADRIC_CYLINDER: return cylinder(lo, ld, h);
+            case RT_QUADRIC_CONE: return cone(lo, ld, h);
+            case RT_QUADRIC_TORUS: return torus(lo, ld, h);
+            case RT_QUADRIC_DISK: return disk(lo, ld, h);
+            case RT_QUADRIC_PARABOLOID: return paraboloid(lo, ld, h);
+            case RT_QUADRIC_HYPERBOLOID: return hyperboloid(lo, ld, h);
+        }
+        return false;
+    }
+    // sphere.rs:39-103: near root, else far root; the z cut and the theta
+    // cut reject without trying the other root.
+    bool sphere(V3 o, V3 d, QuadricHit* h) const {
+        const double radius = prm[0], zmin = prm[1], zmax = prm[2], thetamax = prm[3];
+        double a = dot(d, d), b = 2.0 * dot(o, d), c = dot(o, o) - radius * radius;
+        double disc = b * b - 4.0 * a * c;
+        if (disc < 0.0) return false;
+        double sq = std::sqrt(disc), t1 = (-b - sq) / (2.0 * a), t2 = (-b + sq) / (2.0 * a);
+        double t = t1 > EPSILON ? t1 : t2;
+        if (!(t > EPSILON)) return false;
+        V3 p = o + d * t;
+        if (p.z < zmin || p.z > zmax) return false;
+        if (thetamax < 360.0 && !q_theta_ok(p.x, p.y, thetamax)) return false;
+        h->p = p;
+        h->n = normalize(p);
+        h->u = q_phi_u(p.x, p.y, thetamax);
+        double zr = std::fmax(zmax - zmin, 1e-12);
+        h->v = std::min(std::max((p.z - zmin) / zr, 0.0), 1.0);
+        double ring = std::fmax(std::sqrt(p.x * p.x + p.y * p.y), 1e-6 * std::fmax(radius, 1e-12));
+        h->dpdu = ring * thetamax * PI / 180.0;
+        h->dpdv = zr * radius / ring;
+        h->front_set = true;
+        return true;
+    }
+    // cylinder.rs:37-120: a z-cut miss on the near root retries the far root.
+    bool cylinder(V3 o, V3 d, QuadricHit* h) const {
+        const double radius = prm[0], zmin = prm[1], zmax = prm[2], thetamax = prm[3];
+        double a = d.x * d.x + d.y * d.y, b = 2.0 * (o.x * d.x + o.y * d.y), c = o.x * o.x + o.y * o.y - radius * radius;
+        if (std::fabs(a) < EPSILON) return false;
+        double disc = b * b - 4.0 * a * c;
+        if (disc < 0.0) return false;
+        double sq = std::sqrt(disc), t1 = (-b - sq) / (2.0 * a), t2 = (-b + sq) / (2.0 * a);
+        double t = t1 > EPSILON ? t1 : t2;
+        if (t <= EPSILON) return false;
+        V3 p = o + d * t;
+        if (p.z < zmin || p.z > zmax) {
+            if (t == t1 && t2 > EPSILON) {
+                t = t2;
+                p = o + d * t;
+                if (p.z < zmin || p.z > zmax) return false;
+            } else {
+                return false;
+            }
+        }
+        if (thetamax < 360.0 && !q_theta_ok(p.x, p.y, thetamax)) return false;
+        h->p = p;
+        h->n = normalize(V3{p.x, p.y, 0.0});
+        h->u = q_phi_u(p.x, p.y, thetamax);
+        double zr = std::fmax(zmax - zmin, 1e-12);
+        h->v = std::min(std::max((p.z - zmin) / zr, 0.0), 1.0);
+        h->dpdu = std::fmax(radius, 1e-12) * thetamax * PI / 180.0;
+        h->dpdv = zr;
+        return true;
+    }
+    // cone.rs:36-142: the cone x^2 + y^2 = k z^2, k = (radius / height)^2,
+    // apex at the origin, 0 <= z <= height.
+    bool cone_finish(V3 p, QuadricHit* h) const {
+        const double height = prm[0], radius = prm[1], thetamax = prm[2];
+        double r = std::sqrt(p.x * p.x + p.y * p.y);
+        double k = radius / height;
+        h->p = p;
+        h->n = normalize(V3{p.x / r, p.y / r, -k});
+        h->u = q_phi_u(p.x, p.y, thetamax);
+        h->v = std::min(std::max(p.z / std::fmax(height, 1e-12), 0.0), 1.0);
+        h->dpdu = std::fmax(r, 1e-6 * std::fmax(radius, 1e-12)) * thetamax * PI / 180.0;
+        h->dpdv = std::sqrt(height * height + radius * radius);
+        return true;
+    }
+    bool cone(V3 o, V3 d, QuadricHit* h) const {
+        const double height = prm[0], radius = prm[1], thetamax = prm[2];
+        double k = (radius / height) * (radius / height);
+        double a = d.x * d.x + d.y * d.y - k * d.z * d.z;
+        double b = 2.0 * (o.x * d.x + o.y * d.y - k * o.z * d.z);
+        double c = o.x * o.x + o.y * o.y - k * o.z * o.z;
+        if (std::fabs(a) < EPSILON) {
+            if (std::fabs(b) < EPSILON) return false;
+            double t = -c / b;
+            if (t > EPSILON) {
+                V3 p = o + d * t;
+                if (p.z >= 0.0 && p.z <= height) return cone_finish(p, h);
+            }
+            return false;
+        }
+        double disc = b * b - 4.0 * a * c;
+        if (disc < 0.0) return false;
+        double sq = std::sqrt(disc);
+        for (double t : {(-b - sq) / (2.0 * a), (-b + sq) / (2.0 * a)}) {
+            if (!(t > EPSILON)) continue;
+            V3 p = o + d * t;
+            if (!(p.z >= 0.0 && p.z <= height)) continue;
+            if (thetamax < 360.0 && !q_theta_ok(p.x, p.y, thetamax)) continue;
+            return cone_finish(p, h);
+        }
+        return false;
+    }
+    // extra.rs:92-109 (the tube angle phi in [phimin, phimin + 360)).
+    bool torus_phi(V3 p, double* vphi) const {
+        const double R = prm[0], phimin = prm[2];
+        double rxy = std::sqrt(p.x * p.x + p.y * p.y);
+        double phi = std::atan2(p.z, rxy - R) * 180.0 / PI;
+        while (phi < phimin) phi += 360.0;
+        while (phi >= phimin + 360.0) phi -= 360.0;
+        *vphi = phi;
+        return true;
+    }
+    // extra.rs:243-303: roots ascending, the first past EPSILON inside both cuts.
+    bool torus(V3 o, V3 d, QuadricHit* h) const {
+        const double R = prm[0], r = prm[1], phimin = prm[2], phimax = prm[3], thetamax = prm[4];
+        double g = dot(d, d), hh = 2.0 * dot(o, d), i = dot(o, o) + R * R - r * r;
+        double j = d.x * d.x + d.y * d.y, k = 2.0 * (o.x * d.x + o.y * d.y), l = o.x * o.x + o.y * o.y;
+        double fr = 4.0 * R * R;
+        for (double t : q_quartic(g * g, 2.0 * g * hh, hh * hh + 2.0 * g * i - fr * j, 2.0 * hh * i - fr * k,
+                                  i * i - fr * l)) {
+            if (t <= EPSILON) continue;
+            V3 p = o + d * t;
+            double vphi;
+            torus_phi(p, &vphi);
+            if (phimax - phimin < 360.0 && !(vphi <= phimax)) continue;
+            if (!q_theta_ok(p.x, p.y, thetamax)) continue;
+            double rxy = std::fmax(std::sqrt(p.x * p.x + p.y * p.y), 1e-12);
+            double sc = 1.0 - R / rxy;
+            h->p = p;
+            h->n = normalize(V3{p.x * sc, p.y * sc, p.z});
+            h->u = q_phi_u(p.x, p.y, thetamax);
+            double vr = std::fmax(phimax - phimin, 1e-9);
+            h->v = std::min(std::max((vphi - phimin) / vr, 0.0), 1.0);
+            h->dpdu = rxy * thetamax * PI / 180.0;
+            h->dpdv = std::fmax(r, 1e-12) * vr * PI / 180.0;
+            return true;
+        }
+        return false;
+    }
+    // extra.rs:347-381.
+    bool disk(V3 o, V3 d, QuadricHit* h) const {
+        const double height = prm[0], radius = prm[1], thetamax = prm[2];
+        if (std::fabs(d.z) < EPSILON) return false;
+        double t = (height - o.z) / d.z;
+        if (t <= EPSILON) return false;
+        V3 p = o + d * t;
+        if (p.x * p.x + p.y * p.y > radius * radius) return false;
+        if (!q_theta_ok(p.x, p.y, thetamax)) return false;
+        double rh = std::sqrt(p.x * p.x + p.y * p.y);
+        h->p = p;
+        h->n = V3{0, 0, 1};
+        h->u = q_phi_u(p.x, p.y, thetamax);
+        h->v = std::min(std::max((radius - rh) / std::fmax(radius, 1e-12), 0.0), 1.0);
+        h->dpdu = std::fmax(rh, 1e-6 * std::fmax(radius, 1e-12)) * thetamax * PI / 180.0;
+        h->dpdv = radius;
+        return true;
+    }
+    // extra.rs:425-484: candidates in order, the first inside both cuts.
+    bool paraboloid(V3 o, V3 d, QuadricHit* h) const {
+        const double rmax = prm[0], zmin = prm[1], zmax = prm[2], thetamax = prm[3];
+        if (std::fabs(zmax) < EPSILON) return false;
+        double k = rmax * rmax / zmax;
+        double a = d.x * d.x + d.y * d.y, b = 2.0 * (o.x * d.x + o.y * d.y) - k * d.z;
+        double c = o.x * o.x + o.y * o.y - k * o.z;
+        double cand[2];
+        int nc = 0;
+        if (std::fabs(a) < EPSILON) {
+            if (std::fabs(b) < EPSILON) return false;
+            cand[nc++] = -c / b;
+        } else {
+            double disc = b * b - 4.0 * a * c;
+            if (disc < 0.0) return false;
+            double sq = std::sqrt(disc);
+            cand[nc++] = (-b - sq) / (2.0 * a);
+            cand[nc++] = (-b + sq) / (2.0 * a);
+        }
+        for (int i = 0; i < nc; i++) {
+            double t = cand[i];
+            if (t <= EPSILON) continue;
+            V3 p = o + d * t;
+            if (p.z < zmin || p.z > zmax) continue;
+            if (!q_theta_ok(p.x, p.y, thetamax)) continue;
+            h->p = p;
+            h->n = normalize(V3{2.0 * p.x, 2.0 * p.y, -k});
+            h->u = q_phi_u(p.x, p.y, thetamax);
+            double zr = std::fmax(zmax - zmin, 1e-12);
+            h->v = std::min(std::max((p.z - zmin) / zr, 0.0), 1.0);
+            double ring = std::fmax(std::sqrt(p.x * p.x + p.y * p.y), 1e-6 * std::fmax(rmax, 1e-12));
+            h->dpdu = ring * thetamax * PI / 180.0;
+            h->dpdv = zr;
+            return true;
+        }
+        return false;
+    }
+    // extra.rs:526-632: a flat annulus when p1 and p2 share z, else the
+    // hyperboloid of revolution swept by the line p1 -> p2.
+    bool hyperboloid(V3 o, V3 d, QuadricHit* h) const {
+        const double p1[3] = {prm[0], prm[1], prm[2]}, p2[3] = {prm[3], prm[4], prm[5]};
+        const double thetamax = prm[6];
+        const double zlo = std::fmin(p1[2], p2[2]), zhi = std::fmax(p1[2], p2[2]);
+        if (std::fabs(p2[2] - p1[2]) < EPSILON) {
+            if (std::fabs(d.z) < EPSILON) return false;
+            double t = (p1[2] - o.z) / d.z;
+            if (t <= EPSILON) return false;
+            V3 p = o + d * t;
+            double r2 = p.x * p.x + p.y * p.y;
+            double ra = p1[0] * p1[0] + p1[1] * p1[1], rb = p2[0] * p2[0] + p2[1] * p2[1];
+            if (r2 < std::fmin(ra, rb) || r2 > std::fmax(ra, rb)) return false;
+            if (!q_theta_ok(p.x, p.y, thetamax)) return false;
+            h->p = p;
+            h->n = V3{0, 0, 1};
+            h->u = h->v = 0.0;
+            h->dpdu = h->dpdv = 0.0;   // no st on the flat case (extra.rs:560-567)
+            return true;
+        }
+        const double dz = p2[2] - p1[2], iu = 1.0 / dz;
+        const double sx = (p2[0] - p1[0]) * iu, sy = (p2[1] - p1[1]) * iu;
+        const double cx = p1[0] - p1[2] * sx, cy = p1[1] - p1[2] * sy;
+        const double pa = sx * sx + sy * sy, pb = 2.0 * (cx * sx + cy * sy), pc = cx * cx + cy * cy;
+        double a = d.x * d.x + d.y * d.y - pa * d.z * d.z;
+        double b = 2.0 * (o.x * d.x + o.y * d.y - pa * o.z * d.z) - pb * d.z;
+        double c = o.x * o.x + o.y * o.y - pa * o.z * o.z - pb * o.z - pc;
+        double cand[2];
+        int nc = 0;
+        if (std::fabs(a) < EPSILON) {
+            if (std::fabs(b) < EPSILON) return false;
+            cand[nc++] = -c / b;
+        } else {
+            double disc = b * b - 4.0 * a * c;
+            if (disc < 0.0) return false;
+            double sq = std::sqrt(disc);
+            cand[nc++] = (-b - sq) / (2.0 * a);
+            cand[nc++] = (-b + sq) / (2.0 * a);
+        }
+        for (int i = 0; i < nc; i++) {
+            double t = cand[i];
+            if (t <= EPSILON) continue;
+            V3 p = o + d * t;
+            if (p.z < zlo || p.z > zhi) continue;
+            if (!q_theta_ok(p.x, p.y, thetamax)) continue;
+            h->p = p;
+            h->n = normalize(V3{2.0 * p.x, 2.0 * p.y, -(2.0 * pa * p.z + pb)});
+            h->u = q_phi_u(p.x, p.y, thetamax);
+            h->v = std::min(std::max((p.z - p1[2]) / dz, 0.0), 1.0);
+            double ring = std::fmax(std::sqrt(p.x * p.x + p.y * p.y), 1e-12);
+            h->dpdu = ring * thetamax * PI / 180.0;
+            double sw[3] = {p2[0] - p1[0], p2[1] - p1[1], p2[2] - p1[2]};
+            h->dpdv = std::fmax(std::sqrt(sw[0] * sw[0] + sw[1] * sw[1] + sw[2] * sw[2]), 1e-12);
+            return true;
+        }
+        return false;
+    }
+};
+
 struct Hit {
     double t;        // euclidean distance from the ray origin
     V3 point, normal;
@@ -1543,6 +1935,7 @@ struct Camera {
 struct Scene {
     std::vector<Mesh> meshes;
     std::vector<Instance> instances;
+    std::vector<Quadric> quadrics;
     std::vector<Pbr> materials;
     std::vector<Light> lights;
     LightSampler ls;
@@ -1580,11 +1973,44 @@ struct Scene {
         return p;
     }
 
+    // scene/mod.rs:105-146, the scan of `objects`: the closest quadric hit
+    // (world distance) below t_limit.
+    bool quadric_closest(const Ray& ray, double t_limit, Hit* out) const {
+        bool any = false;
+        double best = t_limit;
+        for (size_t k = 0; k < quadrics.size(); k++) {
+            const Quadric& q = quadrics[k];
+            QuadricHit qh;
+            V3 lo = xf_point(q.inv, ray.o), ld = normalize(xf_vec(q.inv, ray.d));
+            if (!q.local_hit(lo, ld, &qh)) continue;
+            V3 wp = xf_point(q.transform, qh.p);
+            double t = length(wp - ray.o);
+            if (!(t < best)) continue;
+            best = t;
+            any = true;
+            V3 wn = normalize(xf_normal(q.inv, qh.n));
+            out->t = t;
+            out->point = wp;
+            out->normal = wn;
+            out->material_id = q.material_id;
+            out->inst = RT_HIT_QUADRIC | (uint32_t)k;
+            out->prim = 0;
+            out->front_face = qh.front_set ? dot(ray.d, wn) < 0.0 : true;
+            out->st[0] = qh.u;
+            out->st[1] = qh.v;
+            out->st_density = (qh.dpdu > 0.0 || qh.dpdv > 0.0)
+                                  ? 1.0 / std::sqrt(std::fmax(qh.dpdu * qh.dpdv, 1e-24)) / q.scale : 0.0;
+            out->st_grad[0] = out->st_grad[1] = V3{0, 0, 0};
+        }
+        return any;
+    }
+
     // mesh.rs:308-381 Instance::intersect + scene/mod.rs:105-146.
     bool intersect(const Ray& ray, Hit* out, Counters* c) const {
-        if (instances.empty()) return false;
+        bool have_q = !quadrics.empty() && quadric_closest(ray, INF, out);
+        if (instances.empty()) return have_q;
         double dir_len = std::fmax(length(ray.d), 1e-300);
-        double t_budget = INF / dir_len;
+        double t_budget = (have_q ? out->t : INF) / dir_len;
         struct Best {
             uint32_t inst, tri;
             double u, v;
@@ -1615,7 +2041,8 @@ struct Scene {
         };
         uint32_t winner;
         double tw;
-        if (!tlas.traverse(ray.o, ray.d, t_budget, inst_isect, &winner, &tw, c)) return false;
+        if (!tlas.traverse(ray.o, ray.d, t_budget, inst_isect, &winner, &tw, c)) return have_q;
+        if (have_q && !(length(ray.d * tw) < out->t)) return true;
         const Instance& in = instances[best.inst];
         const Mesh& m = meshes[in.mesh_id];
         V3 ln = m.local_normal(best.tri, best.u, best.v);
@@ -1644,6 +2071,31 @@ struct Scene {
 
     bool intersect_param(V3 o, V3 d, double t_max, uint32_t* inst, uint32_t* prim, double* t_out,
                          Counters* c) const {
+        Ray ray{o, d};
+        const double dl = std::fmax(length(d), 1e-300);
+        if (!quadrics.empty()) {
+            Hit qh;
+            if (quadric_closest(ray, t_max * dl, &qh)) {
+                t_max = qh.t / dl;
+                *inst = qh.inst;
+                *prim = 0;
+                *t_out = t_max;
+                if (instances.empty()) return true;
+                uint32_t ii, pp;
+                double tt;
+                if (intersect_param_meshes(o, d, t_max, &ii, &pp, &tt, c) && tt * dl < qh.t) {
+                    *inst = ii;
+                    *prim = pp;
+                    *t_out = tt;
+                }
+                return true;
+            }
+        }
+        return intersect_param_meshes(o, d, t_max, inst, prim, t_out, c);
+    }
+
+    bool intersect_param_meshes(V3 o, V3 d, double t_max, uint32_t* inst, uint32_t* prim, double* t_out,
+                                Counters* c) const {
         if (instances.empty()) return false;
         Ray ray{o, d};
         uint32_t bi = 0, bt = 0;
@@ -1676,6 +2128,10 @@ struct Scene {
 
     // mesh.rs:384-407 Instance::occludes under Bvh::any_hit on the TLAS.
     bool occluded_param(V3 o, V3 d, double t_limit, Counters* c) const {
+        if (!quadrics.empty()) {
+            Hit qh;
+            if (quadric_closest(Ray{o, d}, t_limit * std::fmax(length(d), 1e-300), &qh)) return true;
+        }
         if (instances.empty()) return false;
         auto inst_hit = [&](uint32_t ii, double lim) -> bool {
             const Instance& in = instances[ii];
@@ -2117,6 +2573,21 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
         ib[i] = in.world_bounds;
     }
     s.tlas.build(ib);  // scene/mod.rs:82-86
+    for (uint32_t k = 0; k < d->n_quadrics && d->quadrics; k++) {
+        const rt_quadric_desc& qd = d->quadrics[k];
+        Quadric q;
+        q.type = qd.type;
+        q.material_id = qd.material_id;
+        for (int j = 0; j < 8; j++) q.prm[j] = qd.params[j];
+        q.transform = identity();
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 4; c++) q.transform.m[r][c] = qd.object_to_world[r * 4 + c];
+        if (!inverse(q.transform, q.inv)) q.inv = identity();
+        double lx = length(xf_vec(q.transform, V3{1, 0, 0})), ly = length(xf_vec(q.transform, V3{0, 1, 0})),
+               lz = length(xf_vec(q.transform, V3{0, 0, 1}));
+        q.scale = std::fmax(std::cbrt(lx * ly * lz), 1e-12);
+        s.quadrics.push_back(q);
+    }
     for (uint32_t i = 0; i < d->n_materials; i++) {
         s.materials.push_back(Pbr::from(d->materials[i]));
         if (d->materials[i].presence < 1.0) s.any_presence = true;
@@ -2409,6 +2880,52 @@ void oracle_pattern_eval(const rt_scene_desc* d, uint32_t node, uint64_t n, cons
         rgb[3 * i + 1] = v.y;
         rgb[3 * i + 2] = v.z;
     }
+}
+
+// One quadric against world rays (origin, direction: 6 doubles each): per
+// ray t (world distance, -1 on a miss), hit point, world normal, u, v, st
+// density, front face (10 doubles).
+void oracle_quadric_intersect(const rt_quadric_desc* qd, uint64_t n, const double* rays, double* out) {
+    Quadric q;
+    q.type = qd->type;
+    q.material_id = qd->material_id;
+    for (int j = 0; j < 8; j++) q.prm[j] = qd->params[j];
+    q.transform = identity();
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 4; c++) q.transform.m[r][c] = qd->object_to_world[r * 4 + c];
+    if (!inverse(q.transform, q.inv)) q.inv = identity();
+    double lx = length(xf_vec(q.transform, V3{1, 0, 0})), ly = length(xf_vec(q.transform, V3{0, 1, 0})),
+           lz = length(xf_vec(q.transform, V3{0, 0, 1}));
+    q.scale = std::fmax(std::cbrt(lx * ly * lz), 1e-12);
+    Scene one;
+    one.quadrics.push_back(q);
+    for (uint64_t i = 0; i < n; i++) {
+        const double* r = rays + 6 * i;
+        double* o = out + 10 * i;
+        Hit h;
+        if (!one.quadric_closest(Ray{V3{r[0], r[1], r[2]}, V3{r[3], r[4], r[5]}}, INF, &h)) {
+            for (int k = 0; k < 10; k++) o[k] = k == 0 ? -1.0 : 0.0;
+            continue;
+        }
+        o[0] = h.t;
+        o[1] = h.point.x;
+        o[2] = h.point.y;
+        o[3] = h.point.z;
+        o[4] = h.normal.x;
+        o[5] = h.normal.y;
+        o[6] = h.normal.z;
+        o[7] = h.st[0];
+        o[8] = h.st[1];
+        o[9] = h.st_density;
+        (void)h.front_face;
+    }
+}
+
+// Real roots of a quartic (extra.rs:112-193), ascending; returns the count.
+int oracle_solve_quartic(const double* coef, double* roots) {
+    std::vector<double> r = q_quartic(coef[0], coef[1], coef[2], coef[3], coef[4]);
+    for (size_t k = 0; k < r.size() && k < 4; k++) roots[k] = r[k];
+    return (int)std::min<size_t>(r.size(), 4);
 }
 
 // Shadow-ray transmittance (mod.rs:1254-1306, Tracer::transmittance) of

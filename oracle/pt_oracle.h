@@ -89,6 +89,11 @@ void   oracle_env_sample(uint32_t w, uint32_t h, const float* rgb, uint64_t n, c
 // point (13 doubles); rgb = 3 per point.
 void   oracle_pattern_eval(const rt_scene_desc* d, uint32_t node, uint64_t n, const double* ctx, double* rgb);
 // Closest hit of n rays (o, d: 6 doubles each): (t or -1, s, t, st density).
+/* One analytic quadric against n world rays (6 doubles: origin, direction):
+ * 10 doubles per ray (t or -1, point, normal, u, v, st density). */
+void   oracle_quadric_intersect(const rt_quadric_desc* q, uint64_t n, const double* rays, double* out);
+/* Real roots of coef[0] t^4 + ... + coef[4], ascending; returns the count. */
+int    oracle_solve_quartic(const double* coef, double* roots);
 /* Shadow-ray transmittance (mod.rs:1254-1306) of rays in the two-plane
  * layout (origin; direction, distance): RGB per ray. */
 void   oracle_transmittance(const oracle_scene* s, const float* planes, uint64_t n, double* out, int threads);

@@ -1057,6 +1057,85 @@ void prim_records(const std::vector<double>& boxes, float* out) {
     });
 }
 
+// Analytic quadrics (rt_quadric_desc): f32 transforms both ways (the
+// inverse in f64, identity when singular as Matrix4::inverse().unwrap_or),
+// Matrix4::approx_scale, and the union of the world boxes of the shapes'
+// local bounds (the learned proposal's position bounds include it).
+bool flatten_quadrics(const rt_scene_desc* d, HostScene& H, std::string* err) {
+    H.scalars.n_quadrics = 0;
+    if (!d->n_quadrics) return true;
+    if (!d->quadrics) {
+        *err = "quadrics pointer is NULL";
+        return false;
+    }
+    for (uint32_t k = 0; k < d->n_quadrics; k++) {
+        const rt_quadric_desc& q = d->quadrics[k];
+        if (q.type > RT_QUADRIC_HYPERBOLOID) {
+            *err = "quadric " + std::to_string(k) + " has an unknown type";
+            return false;
+        }
+        if (q.material_id >= d->n_materials) {
+            *err = "quadric " + std::to_string(k) + " names a missing material";
+            return false;
+        }
+        for (int j = 0; j < 12; j++)
+            if (!std::isfinite(q.object_to_world[j])) {
+                *err = "quadric " + std::to_string(k) + " has a non-finite transform";
+                return false;
+            }
+        DevQuadric dq{};
+        double inv[12];
+        affine_inverse(q.object_to_world, inv);
+        for (int r = 0; r < 3; r++) {
+            dq.w2o[r] = make_float4((float)inv[r * 4], (float)inv[r * 4 + 1], (float)inv[r * 4 + 2], (float)inv[r * 4 + 3]);
+            const double* m = q.object_to_world + r * 4;
+            dq.o2w[r] = make_float4((float)m[0], (float)m[1], (float)m[2], (float)m[3]);
+        }
+        for (int j = 0; j < 8; j++) dq.prm[j] = (float)q.params[j];
+        dq.type = q.type;
+        dq.material = q.material_id;
+        double len[3];
+        for (int c = 0; c < 3; c++) {
+            const double* m = q.object_to_world;
+            len[c] = std::sqrt(m[c] * m[c] + m[4 + c] * m[4 + c] + m[8 + c] * m[8 + c]);
+        }
+        dq.scale = (float)std::fmax(std::cbrt(len[0] * len[1] * len[2]), 1e-12);
+        H.quadrics.push_back(dq);
+        // Local bounds of the shape, then the world box of its corners.
+        const double* p = q.params;
+        double lo[3], hi[3];
+        auto box = [&](double rx, double z0, double z1) {
+            lo[0] = lo[1] = -rx;
+            hi[0] = hi[1] = rx;
+            lo[2] = std::fmin(z0, z1);
+            hi[2] = std::fmax(z0, z1);
+        };
+        switch (q.type) {
+            case RT_QUADRIC_SPHERE: box(p[0], std::fmax(p[1], -p[0]), std::fmin(p[2], p[0])); break;
+            case RT_QUADRIC_CYLINDER: box(p[0], p[1], p[2]); break;
+            case RT_QUADRIC_CONE: box(p[1], 0.0, p[0]); break;
+            case RT_QUADRIC_TORUS: box(p[0] + p[1], -p[1], p[1]); break;
+            case RT_QUADRIC_DISK: box(p[1], p[0], p[0]); break;
+            case RT_QUADRIC_PARABOLOID: box(p[0], p[1], p[2]); break;
+            default:
+                box(std::sqrt(std::fmax(p[0] * p[0] + p[1] * p[1], p[3] * p[3] + p[4] * p[4])), p[2], p[5]);
+                break;
+        }
+        for (int c = 0; c < 8; c++) {
+            const double pt[3] = {(c & 1) ? hi[0] : lo[0], (c & 2) ? hi[1] : lo[1], (c & 4) ? hi[2] : lo[2]};
+            double w[3];
+            xf_point(q.object_to_world, pt, w);
+            for (int a = 0; a < 3; a++) {
+                if (!std::isfinite(w[a])) continue;
+                H.quad_lo[a] = std::fmin(H.quad_lo[a], w[a]);
+                H.quad_hi[a] = std::fmax(H.quad_hi[a], w[a]);
+            }
+        }
+    }
+    H.scalars.n_quadrics = d->n_quadrics;
+    return true;
+}
+
 bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, bool build_bvh) {
     HostScene& H = *out;
     if (!d) {
@@ -1246,6 +1325,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         if (md.presence < 1.0) H.scalars.any_presence = 1;
     }
     if (!flatten_patterns(d, H, err)) return false;
+    if (!flatten_quadrics(d, H, err)) return false;
     // ---- lights + light BVH --------------------------------------------------
     if (d->n_lights && !d->lights) {
         *err = "lights pointer is NULL";

@@ -41,9 +41,11 @@ struct HostScene {
     std::vector<float> inf_power;
     std::vector<float4> env;         // environment map texels (RGB, 0)
     std::vector<float> env_marg, env_cond;
+    std::vector<DevQuadric> quadrics;
     uint64_t blas_nodes = 0, tlas_nodes = 0, binary_blas_nodes = 0;
     uint64_t n_tris = 0;             // unique triangles over all meshes
     double world_lo[3] = {0, 0, 0}, world_hi[3] = {0, 0, 0};  // union of instance bounds
+    double quad_lo[3] = {1e300, 1e300, 1e300}, quad_hi[3] = {-1e300, -1e300, -1e300};  // union of quadric bounds
     DevScene scalars{};              // pointer fields unset; scalar fields filled
 };
 

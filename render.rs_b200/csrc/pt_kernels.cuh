@@ -21,6 +21,7 @@
 
 #include "guide.cuh"
 #include "pattern.cuh"
+#include "quadric.cuh"
 
 namespace rt {
 
@@ -142,6 +143,16 @@ struct HitGeo {
 __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3 d, uint4 hr, HitGeo& g) {
     float t = __uint_as_float(hr.x);
     g.p = o + d * t;
+    g.wo = -normalize_ref(d);
+    g.eucl = length(g.p - o);
+    if (hr.y & RT_TRI_QUADRIC) {
+        // Quadric: normal and front face as the shape reports them
+        // (not flipped; shading flips toward wo as for every hit).
+        const uint32_t k = hr.y & ~RT_TRI_QUADRIC;
+        quadric_surface(S, k, g.p, d, g.nw, g.front, nullptr);
+        g.mat = S.quadrics[k].material;
+        return;
+    }
     uint32_t il = hr.z;
     float4 x0 = __ldg(S.inst_xf + 3 * (size_t)il), x1 = __ldg(S.inst_xf + 3 * (size_t)il + 1),
            x2 = __ldg(S.inst_xf + 3 * (size_t)il + 2);
@@ -164,8 +175,6 @@ __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3
     float3 nw = normalize_ref(xf_normal(x0, x1, x2, nl));
     g.front = dot(nw, d) < 0.0f;
     g.nw = g.front ? nw : -nw;
-    g.wo = -normalize_ref(d);
-    g.eucl = length(g.p - o);
     g.mat = info.z;
 }
 
@@ -176,6 +185,18 @@ __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3
 // world-to-object transform (mesh.rs:357-371); zeros when the mesh has no st.
 __device__ __forceinline__ HitSt hit_st(const DevScene& S, uint4 hr, float3 p) {
     HitSt r{0.0f, 0.0f, 0.0f, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f)};
+    if (hr.y & RT_TRI_QUADRIC) {
+        // The quadric's RiSpec (u, v) and density; no st gradients (the
+        // reference's quadrics set none).
+        float st[3];
+        float3 nw;
+        bool front;
+        quadric_surface(S, hr.y & ~RT_TRI_QUADRIC, p, f3(0.0f, 0.0f, 1.0f), nw, front, st);
+        r.s = st[0];
+        r.t = st[1];
+        r.dens = st[2];
+        return r;
+    }
     const uint4 info = __ldg(S.inst + hr.z);
     const MeshInfo mi = S.meshes[info.w];
     if (!(mi.attrs & MESH_ST)) return r;
@@ -626,7 +647,7 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
 // ---- extend ---------------------------------------------------------------------------
 // `pres`: cutout surfaces are passed through inside the traversal
 // (leaf_coop, PRES) instead of by the shade kernel's skip waves.
-template <int BLOCK, bool PRES>
+template <int BLOCK, bool PRES, bool QUAD = false>
 __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S, Paths P, uint32_t qsel) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
     __shared__ LeafShared leaf_sh[BLOCK / 32];
@@ -636,6 +657,8 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S
     const uint32_t n = P.cnt[CNT_EXT_IN];
     unsigned long long rays = 0;
     uint32_t slot = 0;
+    uint32_t qk = 0xFFFFFFFFu;  // closest quadric of this lane's ray (scene/mod.rs:105-146), ~0 for none
+    float qt = 0.0f;            // its parametric distance
     auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
         slot = q[j];
         float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot];
@@ -649,6 +672,15 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S
             seed = splitmix(((uint64_t)rs.x | ((uint64_t)rs.y << 32)) ^
                             (((uint64_t)rs.z | ((uint64_t)rs.w << 32)) * 0x9E3779B97F4A7C15ull));
         }
+        qk = 0xFFFFFFFFu;
+        if (QUAD) {
+            // Quadrics first; the BVH then only looks for closer surfaces.
+            const float dl = fmaxf(length(d), 1e-30f);
+            float tw;
+            qk = PRES ? quadrics_closest_stopping(S, o, d / dl, tmax * dl, seed, tw)
+                      : quadrics_closest(S, o, d / dl, tmax * dl, tw);
+            if (qk != 0xFFFFFFFFu) tmax = qt = tw / dl;
+        }
     };
     auto finish = [&](bool done, uint32_t, const TravState& ts) {
         uint32_t cls = CLS_MISS;
@@ -656,9 +688,15 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S
             const TraceHit& h = ts.hit;
             uint32_t uv = (uint32_t)__half_as_ushort(__float2half_rn(h.b1)) |
                           ((uint32_t)__half_as_ushort(__float2half_rn(h.b2)) << 16);
-            uint32_t tri = ts.found ? h.tri : 0xFFFFFFFFu;
-            P.hit[slot] = make_uint4(__float_as_uint(h.t), tri, h.inst, uv);
-            if (ts.found) cls = __ldg(&S.materials[__ldg(&S.inst[h.inst].z)].mclass);
+            if (ts.found) {
+                P.hit[slot] = make_uint4(__float_as_uint(h.t), h.tri, h.inst, uv);
+                cls = __ldg(&S.materials[__ldg(&S.inst[h.inst].z)].mclass);
+            } else if (qk != 0xFFFFFFFFu) {
+                P.hit[slot] = make_uint4(__float_as_uint(qt), RT_TRI_QUADRIC | qk, 0xFFFFFFFFu, 0u);
+                cls = __ldg(&S.materials[S.quadrics[qk].material].mclass);
+            } else {
+                P.hit[slot] = make_uint4(__float_as_uint(h.t), 0xFFFFFFFFu, h.inst, uv);
+            }
             rays++;
         }
         // Bucket by material class: one atomic per (warp, class).
@@ -1105,7 +1143,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
 }
 
 // ---- shadow -------------------------------------------------------------------------------
-template <int BLOCK>
+template <int BLOCK, bool QUAD = false>
 __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S, Paths P, PtConsts C) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
     __shared__ LeafShared leaf_sh[BLOCK / 32];
@@ -1125,17 +1163,25 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
     if (!S.any_presence) {
         // Opaque scenes: one any-hit query per shadow ray, through the pump.
         uint32_t slot = 0;
+        bool qblock = false;  // a quadric blocks this lane's shadow ray
         auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
             slot = P.q_sh[j];
             float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
             o = xyz(o4);
             d = xyz(d4);
             tmax = d4.w;
+            qblock = false;
+            if (QUAD) {
+                const float dl = fmaxf(length(d), 1e-30f);
+                float tw;
+                qblock = quadrics_closest(S, o, d / dl, tmax * dl, tw) != 0xFFFFFFFFu;
+                if (qblock) tmax = -1.0f;  // nothing left for the BVH to find
+            }
         };
         auto finish = [&](bool done, uint32_t, const TravState& ts) {
             if (!done) return;
             rays++;
-            if (!ts.found) add(slot, 1.0f);
+            if (!ts.found && !qblock) add(slot, 1.0f);
         };
         ray_pump<true>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
         if (rays) atomicAdd(&P.stats[1], rays);
@@ -1145,17 +1191,25 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
     // (traverse.cuh: one traversal per shadow ray, cutouts attenuate, opaque
     // surfaces block).
     uint32_t slot = 0;
+    float qvis = 1.0f;  // transmittance of this lane's shadow ray through the quadrics
     auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
         slot = P.q_sh[j];
         float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
         o = xyz(o4);
         d = xyz(d4);
         tmax = d4.w;
+        qvis = 1.0f;
+        if (QUAD) {
+            const float dl = fmaxf(length(d), 1e-30f);
+            qvis = quadrics_transmittance(S, o, d / dl, tmax * dl);
+            if (qvis == 0.0f) tmax = -1.0f;  // nothing left for the BVH to find
+        }
     };
     auto finish = [&](bool done, uint32_t, const TravState& ts) {
         if (!done) return;
         rays++;
-        if (ts.trans > 0.0f) add(slot, ts.trans);
+        const float vis = ts.trans * qvis;
+        if (vis > 0.0f) add(slot, vis);
     };
     ray_pump<true, true>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
     if (rays) atomicAdd(&P.stats[1], rays);
@@ -1233,7 +1287,7 @@ __global__ void k_resolve(const double* __restrict__ accum, float* __restrict__ 
 }
 
 // ---- ray batch (rt_intersect_batch) ------------------------------------------------------
-template <int BLOCK, bool ANY>
+template <int BLOCK, bool ANY, bool QUAD = false>
 __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_intersect(DevScene S, const float4* __restrict__ org,
                                                      const float4* __restrict__ dir, uint64_t n, uint32_t* prim,
                                                      uint32_t* inst, float* tout, uint32_t* fetch, uint32_t* err) {
@@ -1241,16 +1295,25 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_intersect(DevScen
     __shared__ LeafShared leaf_sh[BLOCK / 32];
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
+    uint32_t qk = 0xFFFFFFFFu;  // closest (or blocking) quadric of this lane's ray
+    float qt = 0.0f;
     auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
         float4 o4 = __ldg(org + j), d4 = __ldg(dir + j);
         o = xyz(o4);
         d = xyz(d4);
         tmax = d4.w;
+        qk = 0xFFFFFFFFu;
+        if (QUAD) {
+            const float dl = fmaxf(length(d), 1e-30f);
+            float tw;
+            qk = quadrics_closest(S, o, d / dl, tmax * dl, tw);
+            if (qk != 0xFFFFFFFFu) tmax = qt = ANY ? -1.0f : tw / dl;
+        }
     };
     auto finish = [&](bool done, uint32_t i, const TravState& ts) {
         if (!done) return;
         if (ANY) {
-            prim[i] = ts.found ? 1u : 0u;
+            prim[i] = (ts.found || qk != 0xFFFFFFFFu) ? 1u : 0u;
         } else {
             uint32_t p = 0xFFFFFFFFu, ii = 0xFFFFFFFFu;
             float t = INFINITY;
@@ -1258,6 +1321,10 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_intersect(DevScen
                 p = __float_as_uint(__ldg(&S.tris[3 * (size_t)ts.hit.tri].w));
                 ii = __ldg(&S.inst[ts.hit.inst].y);
                 t = ts.hit.t;
+            } else if (qk != 0xFFFFFFFFu) {
+                p = 0u;
+                ii = RT_HIT_QUADRIC | qk;
+                t = qt;
             }
             prim[i] = p;
             if (inst) inst[i] = ii;
@@ -1271,7 +1338,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_intersect(DevScen
 // Transmittance of caller rays through the shadow kernel's query
 // (rt_transmittance_batch): the same pump and cooperative leaves as k_shadow
 // in scenes with presence cutouts.
-template <int BLOCK>
+template <int BLOCK, bool QUAD = false>
 __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_transmit_batch(DevScene S, const float4* __restrict__ org,
                                                           const float4* __restrict__ dir, uint64_t n, float* out,
                                                           uint32_t* fetch, uint32_t* err) {
@@ -1279,14 +1346,21 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_transmit_batch(De
     __shared__ LeafShared leaf_sh[BLOCK / 32];
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
+    float qvis = 1.0f;
     auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
         float4 o4 = __ldg(org + j), d4 = __ldg(dir + j);
         o = xyz(o4);
         d = xyz(d4);
         tmax = d4.w;
+        qvis = 1.0f;
+        if (QUAD) {
+            const float dl = fmaxf(length(d), 1e-30f);
+            qvis = quadrics_transmittance(S, o, d / dl, tmax * dl);
+            if (qvis == 0.0f) tmax = -1.0f;  // nothing left for the BVH to find
+        }
     };
     auto finish = [&](bool done, uint32_t i, const TravState& ts) {
-        if (done) out[i] = ts.trans;
+        if (done) out[i] = ts.trans * qvis;
     };
     ray_pump<true, true>(S, (uint32_t)n, fetch, err, st, leaf_sh[threadIdx.x >> 5], load, finish);
 }

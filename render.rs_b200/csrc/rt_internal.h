@@ -173,6 +173,20 @@ struct DevMip {
 static_assert(sizeof(DevTexture) == 16 && sizeof(DevMip) == 16, "texture table layout");
 
 // ---- everything a kernel needs to read the scene ------------------------------
+// Analytic quadric (rt_quadric_desc) in f32: both transforms, the
+// parameters, and Matrix4::approx_scale of object_to_world.
+struct DevQuadric {
+    float4 w2o[3];      // world -> object rows (3x4)
+    float4 o2w[3];      // object -> world rows (3x4)
+    float prm[8];
+    uint32_t type, material;
+    float scale, pad_;
+};
+static_assert(sizeof(DevQuadric) == 144, "DevQuadric layout");
+// Closest-hit records name a quadric hit by this bit in the triangle field
+// (leaf-order triangle indices stay below it); the low bits are its index.
+#define RT_TRI_QUADRIC 0x80000000u
+
 struct DevScene {
     const uint4* nodes;
     const float4* tris;
@@ -209,6 +223,8 @@ struct DevScene {
     uint32_t n_inf;
     float inf_total;
     float p_infinite;
+    const DevQuadric* quadrics;  // analytic quadrics, tested before the BVH (null when none)
+    uint32_t n_quadrics;
     uint32_t any_presence;       // some material has presence < 1
     uint32_t max_steps;          // traversal steps per ray before the query is given up (error bit)
     uint32_t dome;               // first dome light (misses see it), ~0 for none

@@ -221,6 +221,21 @@ struct rt_session {
     }
 };
 
+// The ray-batch kernel variant for the query and the scene (with the
+// quadric tests only when the scene has quadrics).
+static void launch_intersect(rt_session* s, int any_hit, int grid, cudaStream_t st, const float4* o, const float4* d,
+                             uint64_t n, uint32_t* prim, uint32_t* inst, float* t, uint32_t* fetch, uint32_t* err) {
+    const bool quad = s->S.n_quadrics > 0;
+    if (any_hit && quad)
+        k_intersect<TRAV_BLOCK, true, true><<<grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, prim, inst, t, fetch, err);
+    else if (any_hit)
+        k_intersect<TRAV_BLOCK, true><<<grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, prim, inst, t, fetch, err);
+    else if (quad)
+        k_intersect<TRAV_BLOCK, false, true><<<grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, prim, inst, t, fetch, err);
+    else
+        k_intersect<TRAV_BLOCK, false><<<grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, prim, inst, t, fetch, err);
+}
+
 extern "C" {
 
 const char* rt_last_error(void) { return g_err.c_str(); }
@@ -308,6 +323,7 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
         rc = rc ? rc : s->upload(&S.ies, H.ies);
         rc = rc ? rc : s->upload(&S.ies_data, H.ies_data);
     }
+    if (!H.quadrics.empty()) rc = rc ? rc : s->upload(&S.quadrics, H.quadrics);
     rc = rc ? rc : s->upload(&S.materials, H.materials);
     rc = rc ? rc : s->upload(&S.lights, H.lights);
     rc = rc ? rc : s->upload(&S.lbvh, H.lbvh);
@@ -390,9 +406,15 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     if (!rc && guided) {
         float lo[3], hi[3];
         for (int a = 0; a < 3; a++) {
-            double pad = 1e-3 * (s->host.world_hi[a] - s->host.world_lo[a]) + 1e-6;
-            lo[a] = (float)(s->host.world_lo[a] - pad);
-            hi[a] = (float)(s->host.world_hi[a] + pad);
+            double wlo = s->host.world_lo[a], whi = s->host.world_hi[a];
+            if (s->host.quad_lo[a] <= s->host.quad_hi[a]) {
+                const bool meshes = scene->n_instances > 0;
+                wlo = meshes ? std::min(wlo, s->host.quad_lo[a]) : s->host.quad_lo[a];
+                whi = meshes ? std::max(whi, s->host.quad_hi[a]) : s->host.quad_hi[a];
+            }
+            double pad = 1e-3 * (whi - wlo) + 1e-6;
+            lo[a] = (float)(wlo - pad);
+            hi[a] = (float)(whi + pad);
         }
         const float lr = params->guide_lr > 0.0 ? (float)params->guide_lr : 1e-2f;
         if (rt_guide_create(lo, hi, 0x5eed, lr, &s->guide) != 0 || guide_reserve(s->guide, (uint32_t)P) != 0)
@@ -542,7 +564,12 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
         for (uint32_t w = 0; w < waves; w++) {
             uint32_t qin = w & 1u, qout = qin ^ 1u;
             CUDA_TRY(cudaEventRecord(s->evpool[ei], st));
-            if (C.pres_in_trav) k_extend<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
+            // Scenes with analytic quadrics run the variants that test them
+            // (the others keep their registers for the BVH walk).
+            const bool quad = s->S.n_quadrics > 0;
+            if (C.pres_in_trav && quad) k_extend<TRAV_BLOCK, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
+            else if (C.pres_in_trav) k_extend<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
+            else if (quad) k_extend<TRAV_BLOCK, false, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
             else k_extend<TRAV_BLOCK, false><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 1], st));
             if (s->guide) {
@@ -558,7 +585,8 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
             if (P.cone) k_shade<true><<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
             else k_shade<false><<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 2], st));
-            k_shadow<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            if (quad) k_shadow<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            else k_shadow<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 3], st));
             k_wave_prep<<<1, 32, 0, st>>>(P.cnt);
             launches += 4;
@@ -783,10 +811,7 @@ int rt_intersect_batch_device(rt_session* s, const float* rays, uint64_t n, int 
     const float4* o = (const float4*)rays;
     const float4* d = o + n;
     int grid = s->trav_grid;
-    if (any_hit)
-        k_intersect<TRAV_BLOCK, true><<<grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, prim, inst, t, s->fetch, s->err);
-    else
-        k_intersect<TRAV_BLOCK, false><<<grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, prim, inst, t, s->fetch, s->err);
+    launch_intersect(s, any_hit, grid, st, o, d, n, prim, inst, t, s->fetch, s->err);
     CUDA_TRY(cudaGetLastError());
     return RT_OK;
 }
@@ -884,12 +909,7 @@ extern "C" int rt_intersect_batch_noalloc(rt_session* s, const float* rays, uint
     CUDA_TRY(cudaMemsetAsync(d_err, 0, 4, st));
     const float4* o = (const float4*)d_rays;
     const float4* d = o + n;
-    if (any_hit)
-        k_intersect<TRAV_BLOCK, true><<<s->trav_grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, d_prim, d_inst, d_t,
-                                                                           d_fetch, d_err);
-    else
-        k_intersect<TRAV_BLOCK, false><<<s->trav_grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, d_prim, d_inst, d_t,
-                                                                            d_fetch, d_err);
+    launch_intersect(s, any_hit, s->trav_grid, st, o, d, n, d_prim, d_inst, d_t, d_fetch, d_err);
     CUDA_TRY(cudaGetLastError());
     uint32_t e = 0;
     CUDA_TRY(cudaMemcpyAsync(prim, d_prim, 4 * n, cudaMemcpyDeviceToHost, st));
@@ -1017,8 +1037,12 @@ int rt_transmittance_batch(rt_session* s, const float* rays, uint64_t n, float* 
     CUDA_TRY(cudaMemcpyAsync(d_rays, rays, 32 * n, cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->fetch, 0, 4, s->stream));
     const float4* o = (const float4*)d_rays;
-    k_transmit_batch<TRAV_BLOCK><<<s->trav_grid, TRAV_BLOCK, 0, s->stream>>>(s->S, o, o + n, n, d_out, s->fetch,
-                                                                             s->err);
+    if (s->S.n_quadrics)
+        k_transmit_batch<TRAV_BLOCK, true><<<s->trav_grid, TRAV_BLOCK, 0, s->stream>>>(s->S, o, o + n, n, d_out,
+                                                                                       s->fetch, s->err);
+    else
+        k_transmit_batch<TRAV_BLOCK><<<s->trav_grid, TRAV_BLOCK, 0, s->stream>>>(s->S, o, o + n, n, d_out, s->fetch,
+                                                                                 s->err);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(trans, d_out, 4 * n, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(cudaStreamSynchronize(s->stream));

@@ -143,6 +143,15 @@ class RtIesDesc(C.Structure):
     ]
 
 
+QUADRIC_SPHERE, QUADRIC_CYLINDER, QUADRIC_CONE, QUADRIC_TORUS, QUADRIC_DISK, QUADRIC_PARABOLOID, \
+    QUADRIC_HYPERBOLOID = range(7)
+
+
+class RtQuadricDesc(C.Structure):
+    _fields_ = [("object_to_world", C.c_double * 12), ("params", C.c_double * 8), ("type", C.c_uint32),
+                ("material_id", C.c_uint32)]
+
+
 class RtSceneDesc(C.Structure):
     _fields_ = [
         ("meshes", C.POINTER(RtMeshDesc)),
@@ -170,6 +179,9 @@ class RtSceneDesc(C.Structure):
         ("ies", C.POINTER(RtIesDesc)),
         ("n_ies", C.c_uint32),
         ("ies_reserved", C.c_uint32),
+        ("quadrics", C.POINTER(RtQuadricDesc)),
+        ("n_quadrics", C.c_uint32),
+        ("quadric_reserved", C.c_uint32),
     ]
 
 
@@ -197,7 +209,8 @@ FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
 for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 264), (RtLightDesc, 120),
                (RtCameraDesc, 144), (RtParams, 72), (RtPatternInput, 32), (RtPatternDesc, 264),
-               (RtPatternBinding, 16), (RtTextureDesc, 16), (RtIesDesc, 112), (RtSceneDesc, 296)):
+               (RtPatternBinding, 16), (RtTextureDesc, 16), (RtIesDesc, 112), (RtQuadricDesc, 168),
+               (RtSceneDesc, 312)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
 

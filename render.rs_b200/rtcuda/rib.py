@@ -18,8 +18,8 @@ positions are taken as written, without the current transform
 Deviations (recorded in ``RibScene.warnings`` at load time):
   * Quadrics (Sphere, Cylinder, Cone, Disk, Torus, Paraboloid,
     Hyperboloid) and the emitter shapes of PxrSphereLight / PxrDiskLight
-    are tessellated into smooth-normal triangle meshes; the reference
-    intersects them analytically.
+    are analytic quadrics, as the reference's objects; inside ObjectBegin
+    they are skipped, as the reference does.
   * Bilinear / bicubic PatchMesh and Patch are diced by the current
     Basis, as the reference does, NuPatch NURBS untrimmed;
     SubdivisionMesh, GeneralPolygon, Curves, Points, media and motion blur
@@ -357,139 +357,15 @@ def _xf_vec(m, v):
     return m[:3, :3] @ np.asarray(v, dtype=np.float64)
 
 
-# ---- quadric tessellation ----------------------------------------------------------------------
-
-
-def _grid(fn, nu, nv, with_uv=False):
-    """Parametric surface on [0,1]^2 -> (positions, normals, indices[, uv]);
-    fn maps (u, v) arrays to (points (..,3), normals (..,3))."""
-    u = np.linspace(0.0, 1.0, nu + 1)
-    v = np.linspace(0.0, 1.0, nv + 1)
-    U, V = np.meshgrid(u, v)  # (nv+1, nu+1)
-    P, N = fn(U, V)
-    P = P.reshape(-1, 3)
-    N = N.reshape(-1, 3)
-    nn = np.linalg.norm(N, axis=1, keepdims=True)
-    N = np.where(nn > 1e-12, N / np.maximum(nn, 1e-300), np.array([0.0, 0.0, 1.0]))
-    idx = []
-    w = nu + 1
-    for j in range(nv):
-        for i in range(nu):
-            a, b, c, d = j * w + i, j * w + i + 1, (j + 1) * w + i + 1, (j + 1) * w + i
-            idx += [(a, b, c), (a, c, d)]
-    I = np.array(idx, dtype=np.int64)
-    # Wind every triangle like its vertex normals.
-    g = np.cross(P[I[:, 1]] - P[I[:, 0]], P[I[:, 2]] - P[I[:, 0]])
-    flip = np.einsum("ij,ij->i", g, N[I].sum(axis=1)) < 0
-    I[flip] = I[flip][:, [0, 2, 1]]
-    area = np.linalg.norm(g, axis=1)
-    I = I[area > 0]
-    out = (P.astype(np.float32), N.astype(np.float32), I.astype(np.uint32))
-    return out + (np.stack([U.reshape(-1), V.reshape(-1)], -1),) if with_uv else out
-
-
-def _segments(thetamax):
-    return max(8, int(math.ceil(64 * abs(thetamax) / 360.0)))
-
-
-def quadric_st(kind, a):
-    """(P, N, I, st) of a tessellated quadric with the reference's st, taken
-    at the grid vertices so the seam column keeps s = 1: s = phi / thetamax
-    for all; t = (z - zmin) / (zmax - zmin) on spheres (sphere.rs:86-93),
-    and on cylinders, cones (z / height), disks ((radius - r) / radius),
-    tori (the tube angle over its range) and paraboloids the grid's own v
-    (cylinder.rs:100-107, cone.rs:129-134, extra.rs:276-285, 365-366,
-    462-464). None for hyperboloids, whose s starts at the azimuth of
-    their first point rather than at the grid's seam."""
-    if kind not in ("Sphere", "Cylinder", "Cone", "Disk", "Torus", "Paraboloid"):
-        return None
-    P, N, I, uv = tessellate(kind, a, with_uv=True)
-    if kind == "Sphere":
-        zmin, zmax = a[1], a[2]
-        t = np.clip((P[:, 2].astype(np.float64) - zmin) / max(zmax - zmin, 1e-12), 0.0, 1.0)
-    else:
-        t = uv[:, 1]
-    return P, N, I, np.stack([uv[:, 0], t], -1).astype(np.float32)
-
-
-def tessellate(kind, a, with_uv=False):
-    """Triangle mesh of a RenderMan quadric (RiSpec parameterisations)."""
-    if kind == "Sphere":
-        r, zmin, zmax, tm = a
-        cl = lambda x: max(-1.0, min(1.0, x))
-        p0, p1 = math.asin(cl(zmin / r)), math.asin(cl(zmax / r))
-
-        def f(U, V):
-            th = U * math.radians(tm)
-            ph = p0 + V * (p1 - p0)
-            n = np.stack([np.cos(ph) * np.cos(th), np.cos(ph) * np.sin(th), np.sin(ph)], -1)
-            return r * n, n if r > 0 else -n
-        return _grid(f, _segments(tm), 32, with_uv)
-    if kind == "Cylinder":
-        r, zmin, zmax, tm = a
-
-        def f(U, V):
-            th = U * math.radians(tm)
-            P = np.stack([r * np.cos(th), r * np.sin(th), zmin + V * (zmax - zmin)], -1)
-            return P, np.stack([np.cos(th), np.sin(th), np.zeros_like(th)], -1)
-        return _grid(f, _segments(tm), 1, with_uv)
-    if kind == "Cone":
-        h, r, tm = a
-
-        def f(U, V):
-            th = U * math.radians(tm)
-            P = np.stack([r * (1 - V) * np.cos(th), r * (1 - V) * np.sin(th), V * h], -1)
-            return P, np.stack([h * np.cos(th), h * np.sin(th), np.full_like(th, r)], -1)
-        return _grid(f, _segments(tm), 1, with_uv)
-    if kind == "Disk":
-        h, r, tm = a
-
-        def f(U, V):
-            th = U * math.radians(tm)
-            P = np.stack([r * (1 - V) * np.cos(th), r * (1 - V) * np.sin(th), np.full_like(th, h)], -1)
-            return P, np.stack([np.zeros_like(th), np.zeros_like(th), np.ones_like(th)], -1)
-        return _grid(f, _segments(tm), 1, with_uv)
-    if kind == "Torus":
-        R, rr, pmin, pmax, tm = a
-
-        def f(U, V):
-            th = U * math.radians(tm)
-            ph = math.radians(pmin) + V * math.radians(pmax - pmin)
-            n = np.stack([np.cos(ph) * np.cos(th), np.cos(ph) * np.sin(th), np.sin(ph)], -1)
-            P = np.stack([(R + rr * np.cos(ph)) * np.cos(th), (R + rr * np.cos(ph)) * np.sin(th), rr * np.sin(ph)], -1)
-            return P, n
-        return _grid(f, _segments(tm), 32, with_uv)
-    if kind == "Paraboloid":
-        rmax, zmin, zmax, tm = a
-        k = zmax / (rmax * rmax) if rmax != 0 else 0.0
-
-        def f(U, V):
-            th = U * math.radians(tm)
-            z = zmin + V * (zmax - zmin)
-            rad = rmax * np.sqrt(np.maximum(z / zmax, 0.0)) if zmax != 0 else np.zeros_like(z)
-            P = np.stack([rad * np.cos(th), rad * np.sin(th), z], -1)
-            N = np.stack([2 * k * P[..., 0], 2 * k * P[..., 1], -np.ones_like(z)], -1)
-            return P, N
-        return _grid(f, _segments(tm), 16, with_uv)
-    if kind == "Hyperboloid":
-        p1, p2, tm = np.array(a[0:3]), np.array(a[3:6]), a[6]
-
-        def f(U, V):
-            th = U * math.radians(tm)
-            q = p1[None, None, :] * (1 - V)[..., None] + p2[None, None, :] * V[..., None]
-            c, s = np.cos(th), np.sin(th)
-            P = np.stack([q[..., 0] * c - q[..., 1] * s, q[..., 0] * s + q[..., 1] * c, q[..., 2]], -1)
-            dv = p2 - p1
-            Dv = np.stack([dv[0] * c - dv[1] * s, dv[0] * s + dv[1] * c, np.full_like(th, dv[2])], -1)
-            Dt = np.stack([-P[..., 1], P[..., 0], np.zeros_like(th)], -1)
-            return P, np.cross(Dt, Dv)
-        return _grid(f, _segments(tm), 1)
-    raise RibError(f"unknown quadric {kind}")
-
-
 MAX_ARCHIVE_DEPTH = 16
 
+# ---- quadrics --------------------------------------------------------------------------------
+# Arguments per request (scene_builder.rs:813-909); each becomes an analytic
+# quadric (rt_quadric_desc) with the same parameters.
 _QUADRIC_ARGS = {"Sphere": 4, "Cylinder": 4, "Cone": 3, "Disk": 3, "Torus": 5, "Paraboloid": 4, "Hyperboloid": 7}
+_QUADRIC_KIND = {"Sphere": abi.QUADRIC_SPHERE, "Cylinder": abi.QUADRIC_CYLINDER, "Cone": abi.QUADRIC_CONE,
+                 "Disk": abi.QUADRIC_DISK, "Torus": abi.QUADRIC_TORUS, "Paraboloid": abi.QUADRIC_PARABOLOID,
+                 "Hyperboloid": abi.QUADRIC_HYPERBOLOID}
 
 # ---- materials (src/scene/material.rs, src/scene/pbr.rs) ------------------------------------
 
@@ -600,6 +476,7 @@ class _Builder:
         # scene contents (materials / lights / meshes / instances)
         self.meshes, self.instances, self.materials, self.lights = [], [], [], []
         self.mesh_st = {}                 # mesh index -> (n, 2) st
+        self.quadrics = []                # (kind, params, material, object_to_world 3x4)
         self.patterns = []                # Scene pattern node dicts
         self.pattern_handles = {}         # handle -> node index
         self.bindings = []                # (material, field id, node)
@@ -665,6 +542,9 @@ class _Builder:
 
     def place(self, mesh, mat, xf):
         self.instances.append((mesh, mat, np.asarray(xf, np.float64)[:3, :].reshape(12)))
+
+    def add_quadric(self, kind, params, mat, xf):
+        self.quadrics.append((kind, [float(v) for v in params], mat, np.asarray(xf, np.float64)[:3, :].reshape(12)))
 
     def tessellated_mesh(self, P, I, N=None, emissive=True, st=None, displace=False):
         """add_tessellated_mesh (scene_builder.rs:1195-1234): the state's
@@ -897,13 +777,9 @@ class _Builder:
                 if self.defining is not None:
                     self.warn(f"{name} inside ObjectBegin is not instanced; skipping")
                     return
-                self.warn("quadrics are tessellated into triangle meshes (the reference intersects them exactly)")
-                q = quadric_st(name, a)
-                if q is not None:
-                    self.tessellated_mesh(q[0], q[2], q[1], emissive=False, st=q[3])
-                else:
-                    P, N, I = tessellate(name, a)
-                    self.tessellated_mesh(P, I, N, emissive=False)
+                # An analytic quadric with the current transform and the
+                # plain state material (scene_builder.rs:813-909).
+                self.add_quadric(_QUADRIC_KIND[name], a, self.add_material(self.make_material()), self.ctm)
         else:
             self.warn(f"RIB request '{name}' not rendered on this path; skipping")
 
@@ -1287,15 +1163,11 @@ class _Builder:
         elif t == "PxrSphereLight":
             radius = float(np.linalg.norm(_xf_vec(xf, (0.5, 0, 0))))
             li = self.add_light(abi.LIGHT_SPHERE, scale, col, p=origin, radius=radius)
-            P, N, I = tessellate("Sphere", (0.5, -0.5, 0.5, 360.0))
-            self.warn("quadrics are tessellated into triangle meshes (the reference intersects them exactly)")
-            self.place(self.add_mesh(P, I, N), emitter_mat(li), xf)
+            self.add_quadric(abi.QUADRIC_SPHERE, (0.5, -0.5, 0.5, 360.0), emitter_mat(li), xf)
         elif t == "PxrDiskLight":
             li = self.add_light(abi.LIGHT_DISK, scale, col, p=origin, e1=_xf_vec(xf, (0.5, 0, 0)),
                                 e2=_xf_vec(xf, (0, 0.5, 0)))
-            P, N, I = tessellate("Disk", (0.0, 0.5, 360.0))
-            self.warn("quadrics are tessellated into triangle meshes (the reference intersects them exactly)")
-            self.place(self.add_mesh(P, I, N), emitter_mat(li), xf)
+            self.add_quadric(abi.QUADRIC_DISK, (0.0, 0.5, 360.0), emitter_mat(li), xf)
         elif t == "PxrDistantLight":
             d = _xf_vec(xf, (0, 0, -1))
             ln = np.linalg.norm(d)
@@ -1334,6 +1206,8 @@ class _Builder:
         if self.instances:
             s.add_instances([i[0] for i in self.instances], [i[1] for i in self.instances],
                             np.stack([i[2] for i in self.instances]))
+        for kind, params, mat, xf in self.quadrics:
+            s.add_quadric(kind, params, mat, xf)
         s.filter, s.filter_width = self.filter
         if self.dof is not None:
             fstop, flen, fdist = self.dof

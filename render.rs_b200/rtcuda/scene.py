@@ -120,6 +120,7 @@ class Scene:
         self.bindings = []        # (material, field id, node)
         self.textures = []        # (H, W, 3) f32 linear RGB base images
         self.ies = {}             # point light index -> (v_angles, h_angles, candela[h][v], world_to_local 3x3)
+        self.quadrics = []        # (type, params (<= 8), object_to_world 3x4, material)
         # Reference default camera: origin, looking down +z (camera.rs:97-103).
         self.eye = np.zeros(3)
         self.forward = np.array([0.0, 0.0, 1.0])
@@ -251,6 +252,17 @@ class Scene:
                                 p=tuple(p), e1=tuple(e1), e2=tuple(e2), radius=float(radius)))
         self._desc = None
         return len(self.lights) - 1
+
+    def add_quadric(self, kind, params, material, object_to_world=None):
+        """An analytic RiSpec quadric (rt_quadric_desc): `kind` one of
+        abi.QUADRIC_*, `params` as rt_scene.h lists them per kind."""
+        xf = affine() if object_to_world is None else np.asarray(object_to_world, np.float64).reshape(3, 4)
+        pr = [float(v) for v in params]
+        if len(pr) > 8:
+            raise ValueError("at most 8 quadric parameters")
+        self.quadrics.append((int(kind), pr + [0.0] * (8 - len(pr)), xf.copy(), int(material)))
+        self._desc = None
+        return len(self.quadrics) - 1
 
     def add_point_light(self, position, intensity, color=(1, 1, 1), ies=None, world_to_local=None):
         """Light::point; `ies` = (vertical angles, horizontal angles,
@@ -436,5 +448,14 @@ class Scene:
         if self.ies:
             d.ies = ies_arr
             d.n_ies = len(self.ies)
-        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr, tex_arr, ies_arr)
+        quad_arr = (abi.RtQuadricDesc * max(1, len(self.quadrics)))()
+        for k, (kind, pr, xf, mat) in enumerate(self.quadrics):
+            q = quad_arr[k]
+            q.object_to_world = (C.c_double * 12)(*xf.reshape(12))
+            q.params = (C.c_double * 8)(*pr)
+            q.type, q.material_id = kind, mat
+        if self.quadrics:
+            d.quadrics = quad_arr
+            d.n_quadrics = len(self.quadrics)
+        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr, tex_arr, ies_arr, quad_arr)
         return d

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 def test_descriptor_layouts_match_headers():
     sizes = {"rt_mesh_desc": 40, "rt_instance_desc": 104, "rt_material_desc": 264, "rt_light_desc": 120,
              "rt_camera_desc": 144, "rt_params": 72, "rt_pattern_desc": 264, "rt_pattern_binding": 16,
-             "rt_texture_desc": 16, "rt_ies_desc": 112, "rt_scene_desc": 296}
+             "rt_texture_desc": 16, "rt_ies_desc": 112, "rt_quadric_desc": 168, "rt_scene_desc": 312}
     text = open(os.path.join(ROOT, "include", "rt_scene.h")).read()
     for name, size in sizes.items():
         assert f"sizeof({name}) == {size}" in text

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from rtcuda import abi
-from rtcuda.rib import load_rib, load_rib_string, parse_rib, tessellate
+from rtcuda.rib import load_rib, load_rib_string, parse_rib
 
 
 def test_tokenizer_values():
@@ -86,12 +86,10 @@ def test_cornell_like_scene():
     # Point light position as written (no current transform applied).
     pt = [l for l in s.lights if l["type"] == abi.LIGHT_POINT]
     assert pt[0]["p"] == (0.0, 0.5, 4.0) and pt[0]["intensity"] == 3.0
-    # The sphere: a smooth mesh of radius 0.35 placed by its Translate.
-    inst = s.instance_array()
-    p, i, n = s.meshes[inst["mesh"][2]]
-    np.testing.assert_allclose(np.linalg.norm(p, axis=1), 0.35, rtol=1e-6)
-    np.testing.assert_allclose(np.linalg.norm(n, axis=1), 1.0, rtol=1e-6)
-    np.testing.assert_allclose(inst["xf"][2].reshape(3, 4)[:, 3], (0.4, -0.65, 3.9))
+    # The sphere: an analytic quadric of radius 0.35 placed by its Translate.
+    kind, params, xf, mat = s.quadrics[0]
+    assert kind == abi.QUADRIC_SPHERE and params[:4] == [0.35, -0.35, 0.35, 360.0]
+    np.testing.assert_allclose(np.asarray(xf).reshape(3, 4)[:, 3], (0.4, -0.65, 3.9))
 
 
 def test_transform_order_and_rib_matrices():
@@ -162,23 +160,23 @@ Option "background" "color" [0.1 0.2 0.3]
     assert s.background == (0.1, 0.2, 0.3)
 
 
-@pytest.mark.parametrize("kind,args", [("Sphere", (1.0, -0.5, 0.8, 270.0)), ("Cylinder", (0.5, -1, 1, 360.0)),
-                                       ("Cone", (2.0, 0.5, 360.0)), ("Disk", (0.3, 1.0, 180.0)),
-                                       ("Torus", (1.0, 0.25, 0.0, 360.0, 360.0)),
-                                       ("Paraboloid", (1.0, 0.1, 2.0, 360.0)),
-                                       ("Hyperboloid", (1.0, 0.0, -1.0, 0.5, 0.5, 1.0, 360.0))])
-def test_quadric_tessellation(kind, args):
-    P, N, I = tessellate(kind, args)
-    assert len(I) > 8 and I.max() < len(P)
-    np.testing.assert_allclose(np.linalg.norm(N, axis=1), 1.0, rtol=1e-5)
-    g = np.cross(P[I[:, 1]] - P[I[:, 0]], P[I[:, 2]] - P[I[:, 0]])
-    assert (np.einsum("ij,ij->i", g, N[I].sum(axis=1)) > 0).all()  # windings follow the normals
-    if kind == "Sphere":
-        np.testing.assert_allclose(np.linalg.norm(P, axis=1), 1.0, rtol=1e-6)
-        assert P[:, 2].min() >= -0.5 - 1e-6 and P[:, 2].max() <= 0.8 + 1e-6
-    if kind == "Torus":
-        rho = np.hypot(np.hypot(P[:, 0], P[:, 1]) - 1.0, P[:, 2])
-        np.testing.assert_allclose(rho, 0.25, rtol=1e-5)
+def test_quadric_requests_are_analytic():
+    """Each quadric request becomes an analytic quadric with the request's
+    arguments, the current transform and the plain state material
+    (scene_builder.rs:813-909); inside an object definition it is skipped."""
+    s = load_rib_string('Translate 0 0 5\nSphere 1 -0.5 0.8 270\nCylinder 0.5 -1 1 360\nCone 2 0.5 360\n'
+                        'Disk 0.3 1 180\nTorus 1 0.25 0 360 360\nParaboloid 1 0.1 2 360\n'
+                        'Hyperboloid 1 0 -1  0.5 0.5 1  360\n'
+                        'ObjectBegin 1\nSphere 1 -1 1 360\nObjectEnd\n')
+    kinds = [q[0] for q in s.quadrics]
+    assert kinds == [abi.QUADRIC_SPHERE, abi.QUADRIC_CYLINDER, abi.QUADRIC_CONE, abi.QUADRIC_DISK,
+                     abi.QUADRIC_TORUS, abi.QUADRIC_PARABOLOID, abi.QUADRIC_HYPERBOLOID]
+    assert s.quadrics[4][1][:5] == [1.0, 0.25, 0.0, 360.0, 360.0]
+    assert s.quadrics[6][1][:7] == [1.0, 0.0, -1.0, 0.5, 0.5, 1.0, 360.0]
+    for q in s.quadrics:
+        np.testing.assert_allclose(np.asarray(q[2]).reshape(3, 4)[:, 3], (0, 0, 5))
+        assert s.materials[q[3]]["emission"] == (0.0, 0.0, 0.0)
+    assert any("ObjectBegin" in w for w in s.warnings)
 
 
 def test_archives_and_missing_files(tmp_path):
@@ -339,29 +337,9 @@ def test_pattern_requests_and_connections():
     assert "wood.tex" in w and "presence" in w and "bogus" in w
 
 
-def test_st_primvar_and_quadric_st():
+def test_st_primvar():
     s = load_rib_string('PointsPolygons [4] [0 1 2 3] "P" [0 0 1  1 0 1  1 1 1  0 1 1] "st" [0 0  1 0  1 1  0 1]\n'
-                        'PointsPolygons [3] [0 1 2] "P" [0 0 1  1 0 1  1 1 1] "st" [0 0  1 0]\n'
-                        'Sphere 1 -0.5 1 180\nCylinder 1 0 2 360\nCone 2 0.5 270\nDisk 0.3 0.8 360\n'
-                        'Torus 1 0.2 -90 180 360\nParaboloid 1 0.2 1.5 360\nHyperboloid 1 0 0  0.5 0.5 1  360')
-    # Wrong-length st is ignored; the hyperboloid carries none.
-    assert sorted(s.mesh_st) == [0, 2, 3, 4, 5, 6, 7]
+                        'PointsPolygons [3] [0 1 2] "P" [0 0 1  1 0 1  1 1 1] "st" [0 0  1 0]\n')
+    # Wrong-length st is ignored.
+    assert sorted(s.mesh_st) == [0]
     np.testing.assert_array_equal(s.mesh_st[0], [[0, 0], [1, 0], [1, 1], [0, 1]])
-
-    def check(mesh, tm, t_of, u_atol=1e-4):
-        P, st = s.meshes[mesh][0].astype(np.float64), s.mesh_st[mesh]
-        ring = np.hypot(P[:, 0], P[:, 1])
-        phi = np.degrees(np.arctan2(P[:, 1], P[:, 0])) % 360.0
-        inner = (st[:, 0] > 1e-3) & (st[:, 0] < 1 - 1e-3) & (ring > 1e-3)  # phi is undefined on the axis
-        np.testing.assert_allclose(st[inner, 0], phi[inner] / tm, atol=u_atol)
-        np.testing.assert_allclose(st[:, 1], t_of(P, ring), atol=2e-5)
-        assert st[:, 0].min() == 0.0 and st[:, 0].max() == 1.0
-
-    # sphere.rs:86-93, cylinder.rs:100-107, cone.rs:129-134, extra.rs:276-285, 365-366, 462-464.
-    check(2, 180.0, lambda P, r: (P[:, 2] + 0.5) / 1.5)
-    check(3, 360.0, lambda P, r: P[:, 2] / 2.0)
-    check(4, 270.0, lambda P, r: P[:, 2] / 2.0)
-    check(5, 360.0, lambda P, r: (0.8 - r) / 0.8)
-    # (the tube angle is taken with a 1e-3 degree margin so the start of the range does not wrap to 360)
-    check(6, 360.0, lambda P, r: ((np.degrees(np.arctan2(P[:, 2], r - 1.0)) + 90.0 + 1e-3) % 360.0 - 1e-3) / 270.0)
-    check(7, 360.0, lambda P, r: (P[:, 2] - 0.2) / 1.3)
