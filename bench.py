@@ -156,12 +156,18 @@ def oracle_sample(o_s, scene, params, n_pixels, offset=0, threads=0):
 
 GUIDED_W, GUIDED_H, GUIDED_SPP, GUIDED_DEPTH = 1280, 720, 2048, 16
 
-# DRAM bytes (read + write) per k_extend launch on the forest at 3840x2160,
-# scaled from one ncu capture of a smaller frame of the same scene (traffic
-# per launch grows with the rays per launch; profiles/ has the capture).
-# None until measured.
-EXTEND_DRAM_BYTES_PER_LAUNCH = None
-EXTEND_DRAM_SOURCE = "not captured"
+# DRAM bytes (read + write) per extension ray of k_extend on the forest, from
+# one ncu capture of all 10 k_extend launches of a 1280x720 pass of the same
+# scene (849.6 MB for 1,985,150 extension rays; 1 metric pass):
+#   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum,lts__t_bytes.sum
+#       --clock-control none -k regex:"k_extend" -s 10 -c 10
+#       python bench.py --mode scene --scene forest --res 1280x720 --steps 1 --warmup 1
+# A 3840x2160 launch is scaled from it by its rays; per-ray traffic falls as
+# the frame grows (582 B per ray over the first waves at 640x360), so the
+# scaled figure is an upper bound.
+EXTEND_DRAM_BYTES_PER_RAY = 849.6e6 / 1_985_150
+EXTEND_DRAM_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the 10 k_extend launches of a "
+                      "1280x720 forest pass (428 B per extension ray), scaled by the rays per launch")
 
 
 def rel_mse(img, ref):
@@ -255,6 +261,66 @@ def guided_equal_time(ref_spp=16384, cpu_pixels=1024, cpu_spp=65536):
     except Exception as exc:  # the oracle is optional on a box without it
         out["f64_reference"] = f"unavailable: {exc}"
     return out
+
+
+def load_tensor_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)["bf16_tflops"], "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+GUIDE_FWD_FLOP = 2 * (48 * 64 + 64 * 64 + 64 * 64 + 64 * 48)   # MLP 48-64-64-64-48 per record
+
+
+def guide_network_rate(n_infer=1 << 20, n_train=1 << 16, reps=20):
+    """The learned proposal's tcgen05 MLP alone, device-resident records:
+    inference of 2^20 records (hash-grid encode + forward) and training
+    steps of 2^16 records (encode, forward, backward, gradient reduction,
+    hash-grid backward, Adam), CUDA events on one stream. FLOP/s count the
+    MLP's algorithmic FLOPs (forward 28,672 per record; a training step
+    forward + backward = 3x) against the measured dense bf16 peak."""
+    import ctypes
+    import torch
+    from rtcuda import guide as G
+    peak, kind = load_tensor_peak()
+    g = G.Guide((-1, -1, -1), (1, 1, 1), seed=3, lr=1e-2)
+    L = G._g()
+    rng = np.random.default_rng(1)
+    rec = np.zeros((n_infer, 16), np.float32)
+    rec[:, 0:3] = rng.uniform(-1, 1, (n_infer, 3))
+    for a, b in ((3, 6), (6, 9), (9, 12)):
+        v = rng.normal(size=(n_infer, 3))
+        rec[:, a:b] = v / np.linalg.norm(v, axis=1, keepdims=True)
+    rec[:, 12] = rng.uniform(0.0, 2.0, n_infer)
+    d_rec = torch.from_numpy(rec).cuda()
+    d_out = torch.empty((n_infer, 48), dtype=torch.float32, device="cuda")
+    st = torch.cuda.Stream()
+    sp = ctypes.c_void_p(st.cuda_stream)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        for _ in range(reps):
+            fn()
+        b.record(st)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    infer_ms = timed(lambda: G._check(L.rt_guide_infer_device(g.h, d_rec.data_ptr(), n_infer, d_out.data_ptr(), sp)))
+    train_ms = timed(lambda: G._check(L.rt_guide_train_step_device(g.h, d_rec.data_ptr(), n_train, None, sp)))
+    g.close()
+    inf_tf = n_infer * GUIDE_FWD_FLOP / (infer_ms * 1e-3) / 1e12
+    tr_tf = 3 * n_train * GUIDE_FWD_FLOP / (train_ms * 1e-3) / 1e12
+    return {"inference_records": n_infer, "inference_ms": round(infer_ms, 4), "inference_tflops": inf_tf,
+            "inference_frac": inf_tf / peak, "train_records": n_train, "train_step_ms": round(train_ms, 4),
+            "train_tflops": tr_tf, "train_frac": tr_tf / peak, "peak_tflops": peak, "peak_kind": kind,
+            "flop_per_record_forward": GUIDE_FWD_FLOP}
 
 
 def other_workloads(flush, stream):
@@ -604,7 +670,8 @@ def main():
             per_sample = work["ext_bytes_per_sample"] * samples / (ext_ms / 1e3) / 1e9
             roof = {"kernel": "k_extend (closest hit, 8-wide BVH, cutouts decided in traversal)", "bound": "hbm",
                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": EXTEND_DRAM_BYTES_PER_LAUNCH, "traffic_source": EXTEND_DRAM_SOURCE,
+                    "traffic": EXTEND_DRAM_BYTES_PER_RAY * ext_rays / launches_ext,
+                    "traffic_source": EXTEND_DRAM_SOURCE,
                     "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg_bytes / launches_ext,
                     "rays_per_launch": ext_rays / launches_ext, "launch_ms": ext_ms / launches_ext,
                     "launches": int(launches_ext), "reference_work": work,
@@ -613,8 +680,9 @@ def main():
         workloads = None
         if not args.no_workloads and world == 1:
             workloads = other_workloads(flush, stream)
-        guided = forest_guided = None
+        guided = forest_guided = network = None
         if not args.no_guided and world == 1:
+            network = guide_network_rate()
             guided = guided_equal_time()
             forest_guided = guided_forest()
         result = {
@@ -633,6 +701,7 @@ def main():
             "workloads": workloads,
             "guided_equal_time": guided,
             "guided_forest": forest_guided,
+            "guide_network": network,
         }
         print(json.dumps(result), flush=True)
     if world > 1:
