@@ -208,7 +208,7 @@ def equal_time_plain(scene, params, budget_ms):
         return g.image(), done, ms
 
 
-def guided_equal_time(ref_spp=16384, cpu_pixels=1024, cpu_spp=65536):
+def guided_equal_time(ref_spp=16384, cpu_pixels=4096, cpu_spp=65536):
     """Equal-time relMSE of guided vs plain path tracing on the two-room scene.
     The GPU reference is the mean of two independent halves A and B; its own
     error, mean((A - B)^2 / (ref^2 + 1e-2)) / 4, is reported and subtracted
