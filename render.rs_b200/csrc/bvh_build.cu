@@ -841,17 +841,26 @@ __global__ void k_root_children(const WideS* __restrict__ W, uint32_t R, const B
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= R) return;
     const WideS w = W[r];
-    nk_out[r] = w.nk;
-    for (uint32_t k = 0; k < w.nk && k < 8; k++) {
-        const BNode c = nodes[w.kids[k]];
+    uint32_t n = 0;
+    auto put = [&](const BNode& c, uint32_t child) {
         RootChild rc;
         for (int a = 0; a < 3; a++) {
             rc.lo[a] = c.lo[a];
             rc.hi[a] = c.hi[a];
         }
-        rc.ref = c.count > 0 ? make_leaf_ref(c.first, c.count) : (w.child[k] != NONE ? W[w.child[k]].idx : REF_EMPTY);
-        out[8ull * r + k] = rc;
+        rc.ref = c.count > 0 ? make_leaf_ref(c.first, c.count) : (child != NONE ? W[child].idx : REF_EMPTY);
+        out[(size_t)RT_TOP_MAX * r + n++] = rc;
+    };
+    for (uint32_t k = 0; k < w.nk && k < 8; k++) {
+        const BNode c = nodes[w.kids[k]];
+        if (RT_BRAID_LEVELS >= 2 && c.count == 0 && w.child[k] != NONE) {
+            const WideS cw = W[w.child[k]];
+            for (uint32_t kk = 0; kk < cw.nk && kk < 8; kk++) put(nodes[cw.kids[kk]], cw.child[kk]);
+            continue;
+        }
+        put(c, w.child[k]);
     }
+    nk_out[r] = n;
 }
 
 // Quantisation grid of one axis (the host's choose_grid): origin p, a
@@ -1315,17 +1324,18 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
         const uint32_t R = (uint32_t)roots.size();
         RootChild* d_rc;
         uint32_t* d_nk;
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_rc, 8ull * R, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_rc, (size_t)RT_TOP_MAX * R, st, err);
         rc = rc ? rc : dev_alloc(D.ptrs, &d_nk, R, st, err);
         if (rc) return rc;
         k_root_children<<<blocks_for(R, JB), JB, 0, st>>>(bw.W, R, bnodes, d_rc, d_nk);
-        std::vector<RootChild> hrc(8ull * R);
+        std::vector<RootChild> hrc((size_t)RT_TOP_MAX * R);
         std::vector<uint32_t> hnk(R);
         BV_TRY(cudaMemcpyAsync(hrc.data(), d_rc, hrc.size() * sizeof(RootChild), cudaMemcpyDeviceToHost, st));
         BV_TRY(cudaMemcpyAsync(hnk.data(), d_nk, 4ull * R, cudaMemcpyDeviceToHost, st));
         BV_TRY(cudaStreamSynchronize(st));
         for (uint32_t r = 0; r < R; r++)
-            root_children[root_mesh[r]].assign(hrc.begin() + 8ull * r, hrc.begin() + 8ull * r + std::min(hnk[r], 8u));
+            root_children[root_mesh[r]].assign(hrc.begin() + (size_t)RT_TOP_MAX * r,
+                                               hrc.begin() + (size_t)RT_TOP_MAX * r + std::min(hnk[r], RT_TOP_MAX));
     }
     for (uint32_t m = 0; m < M; m++) H->meshes[m].blas_root = blas_root[m];
     H->blas_nodes = blas_total;

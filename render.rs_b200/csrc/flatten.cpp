@@ -967,7 +967,7 @@ void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>
         double total_area = 0.0;
         Box all;
         parallel_for(n, [&](size_t i0, size_t i1) {
-            Box cb[8], local;
+            Box cb[RT_TOP_MAX], local;
             double a = 0.0;
             for (size_t i = i0; i < i1; i++) {
                 Box u;
@@ -984,7 +984,7 @@ void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>
     }
     std::vector<uint64_t> off(n + 1, 0);
     parallel_for(n, [&](size_t i0, size_t i1) {
-        Box cb[8];
+        Box cb[RT_TOP_MAX];
         for (size_t i = i0; i < i1; i++) {
             Box u;
             off[i + 1] = child_boxes((uint32_t)i, cb, &u);
@@ -997,7 +997,7 @@ void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>
     std::mutex mu;
     Box world;
     parallel_for(n, [&](size_t i0, size_t i1) {
-        Box local, cb[8];
+        Box local, cb[RT_TOP_MAX];
         for (size_t i = i0; i < i1; i++) {
             Box u;
             const uint32_t k_items = child_boxes((uint32_t)i, cb, &u);
@@ -1256,8 +1256,21 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         }
         const auto& root = col.wide[0];
         for (uint32_t k = 0; k < root.nk; k++) {
+            const BinNode& kn = bin.nodes[root.kids[k]];
+            if (RT_BRAID_LEVELS >= 2 && kn.count == 0) {
+                // The child's own children (the wide nodes were emitted in
+                // preorder, one `wide` entry per node index).
+                const auto& cw = col.wide[root.refs[k] - root.idx];
+                for (uint32_t kk = 0; kk < cw.nk; kk++) {
+                    RootChild c;
+                    f32_box(bin.nodes[cw.kids[kk]].b, c.lo, c.hi);
+                    c.ref = cw.refs[kk];
+                    root_children[m].push_back(c);
+                }
+                continue;
+            }
             RootChild c;
-            f32_box(bin.nodes[root.kids[k]].b, c.lo, c.hi);
+            f32_box(kn.b, c.lo, c.hi);
             c.ref = root.refs[k];
             root_children[m].push_back(c);
         }

@@ -62,6 +62,13 @@ struct RootChild {
     float lo[3], hi[3];
     uint32_t ref;
 };
+// Depth of the BLAS frontier that splits a dense scene's instances into TLAS
+// items: 1 = the root's children (at most 8 per instance), 2 = their
+// children (at most 64).
+#ifndef RT_BRAID_LEVELS
+#define RT_BRAID_LEVELS 1
+#endif
+constexpr uint32_t RT_TOP_MAX = RT_BRAID_LEVELS >= 2 ? 64u : 8u;
 
 // TLAS primitives: every instance contributes one item (instance, BLAS root
 // reference) boxed by the union of its root children's world boxes, or one
