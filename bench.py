@@ -63,6 +63,11 @@ WORKLOAD = "forest_772k_instances_1200_lights_3840x2160_32spp_depth10"
 CONFIG = {"workload": WORKLOAD, "width": WIDTH, "height": HEIGHT, "spp": SPP, "max_depth": MAX_DEPTH,
           "rr_start": 3, "instances": 772_001, "trees": 20, "point_lights": 1200, "presence_cutouts": True,
           "guided": False, "l2_flush": "256 MB write before every step; scene + path state > L2"}
+def config_for(world):
+    """The `config` both arms print (the driver compares them)."""
+    return dict(CONFIG, parallelism=f"replica-sample-ranges x{world}", accumulator="f64")
+
+
 # The traversal-stress workload (a `workloads` entry).
 CLOUD_W, CLOUD_H, CLOUD_SPP, CLOUD_DEPTH = 1920, 1080, 16, 8
 N_TRIS, N_RAYS = 1_000_000, 4_194_304
@@ -437,15 +442,18 @@ def run_reference(args):
     scene = scenes.forest(WIDTH, HEIGHT)
     params = abi.make_params(max_depth=MAX_DEPTH, rr_start=3)
     o_s = oracle.OracleScene(scene)
-    vals, sample, cores = [], "", os.cpu_count()
+    vals, secs, sample, cores = [], [], "", os.cpu_count()
     for i in range(args.warmup + args.steps):
-        v, sample, cores, _, _ = oracle_sample(o_s, scene, params, REF_PIXELS_PER_STEP, offset=i)
+        v, sample, cores, _, el = oracle_sample(o_s, scene, params, REF_PIXELS_PER_STEP, offset=i)
         if i >= args.warmup:
             vals.append(v)
+            secs.append(el)
     value = statistics.median(vals)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": dict(CONFIG),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(secs),
+            "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_for(int(os.environ.get("WORLD_SIZE", str(args.gpus)))),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"per step: {sample}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -689,7 +697,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(CONFIG, parallelism=f"replica-sample-ranges x{world}", accumulator="f64"),
+            "config": config_for(world),
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": d2h,
                     "ms": max(e2e_ms) if e2e_ms else None, "ms_each": [round(v, 2) for v in e2e_ms]},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,

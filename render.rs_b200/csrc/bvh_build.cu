@@ -834,33 +834,39 @@ __global__ void k_wide_root_index(WideS* W, const uint32_t* root_idx, uint32_t n
     if (s < n) W[s].idx = root_idx[s];
 }
 
-// The children of every BLAS root (boxes and final references) for the
-// TLAS items; needs the preorder indices.
+// The children of every BLAS root (boxes and final references) and the
+// second-level frontier (each inner child replaced by its children) for the
+// TLAS items, in the host builder's order; needs the preorder indices.
 __global__ void k_root_children(const WideS* __restrict__ W, uint32_t R, const BNode* __restrict__ nodes,
-                                RootChild* __restrict__ out, uint32_t* __restrict__ nk_out) {
+                                RootChild* __restrict__ out1, uint32_t* __restrict__ nk1,
+                                RootChild* __restrict__ out2, uint32_t* __restrict__ nk2) {
     const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= R) return;
     const WideS w = W[r];
-    uint32_t n = 0;
-    auto put = [&](const BNode& c, uint32_t child) {
+    auto child_of = [&](const BNode& c, uint32_t child) {
         RootChild rc;
         for (int a = 0; a < 3; a++) {
             rc.lo[a] = c.lo[a];
             rc.hi[a] = c.hi[a];
         }
         rc.ref = c.count > 0 ? make_leaf_ref(c.first, c.count) : (child != NONE ? W[child].idx : REF_EMPTY);
-        out[(size_t)RT_TOP_MAX * r + n++] = rc;
+        return rc;
     };
+    uint32_t n1 = 0, n2 = 0;
     for (uint32_t k = 0; k < w.nk && k < 8; k++) {
         const BNode c = nodes[w.kids[k]];
-        if (RT_BRAID_LEVELS >= 2 && c.count == 0 && w.child[k] != NONE) {
+        const RootChild rc = child_of(c, w.child[k]);
+        out1[8ull * r + n1++] = rc;
+        if (c.count == 0 && w.child[k] != NONE) {
             const WideS cw = W[w.child[k]];
-            for (uint32_t kk = 0; kk < cw.nk && kk < 8; kk++) put(nodes[cw.kids[kk]], cw.child[kk]);
-            continue;
+            for (uint32_t kk = 0; kk < cw.nk && kk < 8; kk++)
+                out2[(size_t)RT_TOP_MAX * r + n2++] = child_of(nodes[cw.kids[kk]], cw.child[kk]);
+        } else {
+            out2[(size_t)RT_TOP_MAX * r + n2++] = rc;
         }
-        put(c, w.child[k]);
     }
-    nk_out[r] = n;
+    nk1[r] = n1;
+    nk2[r] = n2;
 }
 
 // Quantisation grid of one axis (the host's choose_grid): origin p, a
@@ -1248,7 +1254,7 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
     // ---- BLAS: every mesh's triangles in one primitive array ----------------------
     uint32_t blas_total = 0;
     std::vector<uint32_t> blas_root(M, 0xFFFFFFFFu);
-    std::vector<std::vector<RootChild>> root_children(M);
+    std::vector<std::vector<RootChild>> root_children(M), grand_children(M);
     BNode* bnodes = nullptr;
     WideTree bw;
     BPrim *P0 = nullptr, *P1 = nullptr;
@@ -1320,22 +1326,28 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
         }
         rc = wide_index(D, bw, ridx, st, err);
         if (rc) return rc;
-        // The BLAS roots' children become the TLAS items.
+        // The BLAS roots' children (and their children) become the TLAS items.
         const uint32_t R = (uint32_t)roots.size();
-        RootChild* d_rc;
-        uint32_t* d_nk;
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_rc, (size_t)RT_TOP_MAX * R, st, err);
-        rc = rc ? rc : dev_alloc(D.ptrs, &d_nk, R, st, err);
+        RootChild *d_rc1, *d_rc2;
+        uint32_t *d_nk1, *d_nk2;
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_rc1, 8ull * R, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_rc2, (size_t)RT_TOP_MAX * R, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_nk1, R, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_nk2, R, st, err);
         if (rc) return rc;
-        k_root_children<<<blocks_for(R, JB), JB, 0, st>>>(bw.W, R, bnodes, d_rc, d_nk);
-        std::vector<RootChild> hrc((size_t)RT_TOP_MAX * R);
-        std::vector<uint32_t> hnk(R);
-        BV_TRY(cudaMemcpyAsync(hrc.data(), d_rc, hrc.size() * sizeof(RootChild), cudaMemcpyDeviceToHost, st));
-        BV_TRY(cudaMemcpyAsync(hnk.data(), d_nk, 4ull * R, cudaMemcpyDeviceToHost, st));
+        k_root_children<<<blocks_for(R, JB), JB, 0, st>>>(bw.W, R, bnodes, d_rc1, d_nk1, d_rc2, d_nk2);
+        std::vector<RootChild> hrc1(8ull * R), hrc2((size_t)RT_TOP_MAX * R);
+        std::vector<uint32_t> hnk1(R), hnk2(R);
+        BV_TRY(cudaMemcpyAsync(hrc1.data(), d_rc1, hrc1.size() * sizeof(RootChild), cudaMemcpyDeviceToHost, st));
+        BV_TRY(cudaMemcpyAsync(hrc2.data(), d_rc2, hrc2.size() * sizeof(RootChild), cudaMemcpyDeviceToHost, st));
+        BV_TRY(cudaMemcpyAsync(hnk1.data(), d_nk1, 4ull * R, cudaMemcpyDeviceToHost, st));
+        BV_TRY(cudaMemcpyAsync(hnk2.data(), d_nk2, 4ull * R, cudaMemcpyDeviceToHost, st));
         BV_TRY(cudaStreamSynchronize(st));
-        for (uint32_t r = 0; r < R; r++)
-            root_children[root_mesh[r]].assign(hrc.begin() + (size_t)RT_TOP_MAX * r,
-                                               hrc.begin() + (size_t)RT_TOP_MAX * r + std::min(hnk[r], RT_TOP_MAX));
+        for (uint32_t r = 0; r < R; r++) {
+            root_children[root_mesh[r]].assign(hrc1.begin() + 8ull * r, hrc1.begin() + 8ull * r + std::min(hnk1[r], 8u));
+            grand_children[root_mesh[r]].assign(hrc2.begin() + (size_t)RT_TOP_MAX * r,
+                                                hrc2.begin() + (size_t)RT_TOP_MAX * r + std::min(hnk2[r], RT_TOP_MAX));
+        }
     }
     for (uint32_t m = 0; m < M; m++) H->meshes[m].blas_root = blas_root[m];
     H->blas_nodes = blas_total;
@@ -1351,7 +1363,7 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
     std::vector<uint2> items;
     if (NI) {
         std::vector<double> boxes;
-        tlas_items(d, root_children, &boxes, &items, H);
+        tlas_items(d, root_children, grand_children, &boxes, &items, H);
         if (items.size() >= (1ull << 27)) {
             *err = "more than 2^27 instance subtrees";
             return RT_ERR_INVALID;

@@ -936,30 +936,45 @@ DevMaterial fold_material_public(const rt_material_desc& m) { return fold_materi
 #define RT_BRAID_DENSE 32.0
 #endif
 
+// World box of a local box under an affine 3x4: centre mapped, half
+// extents through |M| (the exact box of the 8 transformed corners).
+static Box world_box(const double* m, const float* lo, const float* hi) {
+    Box wb;
+    for (int r = 0; r < 3; r++) {
+        double c = m[r * 4 + 3], e = 0.0;
+        for (int k = 0; k < 3; k++) {
+            const double ck = 0.5 * ((double)lo[k] + (double)hi[k]), hk = 0.5 * ((double)hi[k] - (double)lo[k]);
+            c += m[r * 4 + k] * ck;
+            e += std::fabs(m[r * 4 + k]) * hk;
+        }
+        wb.lo[r] = c - e;
+        wb.hi[r] = c + e;
+    }
+    return wb;
+}
+
 void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>>& root_children,
-                std::vector<double>* boxes, std::vector<uint2>* items, HostScene* H) {
+                const std::vector<std::vector<RootChild>>& grand_children, std::vector<double>* boxes,
+                std::vector<uint2>* items, HostScene* H) {
     const uint32_t n = d->n_instances;
-    double ratio = RT_BRAID_RATIO;
-    // World boxes of one instance's root children, their union, and whether to split.
-    auto child_boxes = [&](uint32_t i, Box* cb, Box* u) -> uint32_t {
+    bool dense = false;
+    // World boxes of one instance's frontier (`list` per mesh), their union,
+    // and how many items it becomes: every child in a dense scene, else the
+    // children when their summed area is below RT_BRAID_RATIO x the union's.
+    auto child_boxes = [&](uint32_t i, const std::vector<std::vector<RootChild>>& list, bool split_all, Box* cb,
+                           Box* u) -> uint32_t {
         const rt_instance_desc& id = d->instances[i];
         if (!d->meshes[id.mesh_id].n_triangles) return 0;
-        const auto& rc = root_children[id.mesh_id];
+        const auto& rc = list[id.mesh_id];
         double sum = 0.0;
         for (size_t k = 0; k < rc.size(); k++) {
-            const RootChild& c = rc[k];
-            Box wb;
-            for (int q = 0; q < 8; q++) {
-                double p[3] = {(q & 1) ? c.hi[0] : c.lo[0], (q & 2) ? c.hi[1] : c.lo[1], (q & 4) ? c.hi[2] : c.lo[2]};
-                double w[3];
-                xf_point(id.object_to_world, p, w);
-                wb.grow_pt(w);
-            }
-            cb[k] = wb;
+            const Box wb = world_box(id.object_to_world, rc[k].lo, rc[k].hi);
+            if (cb) cb[k] = wb;
             u->grow(wb);
             sum += wb.area();
         }
-        return rc.size() > 1 && sum < ratio * u->area() ? (uint32_t)rc.size() : 1u;
+        if (rc.size() <= 1) return 1u;
+        return split_all || sum < RT_BRAID_RATIO * u->area() ? (uint32_t)rc.size() : 1u;
     };
     // Density: the instances' union boxes against the world box.
     {
@@ -967,11 +982,11 @@ void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>
         double total_area = 0.0;
         Box all;
         parallel_for(n, [&](size_t i0, size_t i1) {
-            Box cb[RT_TOP_MAX], local;
+            Box local;
             double a = 0.0;
             for (size_t i = i0; i < i1; i++) {
                 Box u;
-                if (child_boxes((uint32_t)i, cb, &u)) {
+                if (child_boxes((uint32_t)i, root_children, false, nullptr, &u)) {
                     a += u.area();
                     local.grow(u);
                 }
@@ -980,14 +995,24 @@ void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>
             total_area += a;
             all.grow(local);
         }, 4096);
-        if (all.area() > 0.0 && total_area > RT_BRAID_DENSE * all.area()) ratio = INFINITY;
+        dense = all.area() > 0.0 && total_area > RT_BRAID_DENSE * all.area();
     }
+    // A dense scene splits every instance into its BLAS's second-level
+    // frontier; others split an instance into its root's children when
+    // they overlap little.
+    const auto& list = dense ? grand_children : root_children;
     std::vector<uint64_t> off(n + 1, 0);
     parallel_for(n, [&](size_t i0, size_t i1) {
         Box cb[RT_TOP_MAX];
         for (size_t i = i0; i < i1; i++) {
+            const rt_instance_desc& id = d->instances[i];
+            if (dense) {
+                const size_t k = list[id.mesh_id].size();
+                off[i + 1] = d->meshes[id.mesh_id].n_triangles ? (k > 1 ? k : 1) : 0;
+                continue;
+            }
             Box u;
-            off[i + 1] = child_boxes((uint32_t)i, cb, &u);
+            off[i + 1] = child_boxes((uint32_t)i, list, false, cb, &u);
         }
     }, 4096);
     for (uint32_t i = 0; i < n; i++) off[i + 1] += off[i];
@@ -1000,9 +1025,9 @@ void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>
         Box local, cb[RT_TOP_MAX];
         for (size_t i = i0; i < i1; i++) {
             Box u;
-            const uint32_t k_items = child_boxes((uint32_t)i, cb, &u);
+            const uint32_t k_items = child_boxes((uint32_t)i, list, dense, cb, &u);
             const rt_instance_desc& id = d->instances[i];
-            const auto& rc = root_children[id.mesh_id];
+            const auto& rc = list[id.mesh_id];
             for (uint32_t k = 0; k < k_items; k++) {
                 const uint64_t j = off[i] + k;
                 const Box& b = k_items == 1 ? u : cb[k];
@@ -1151,7 +1176,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         return false;
     }
     // ---- BLAS per mesh -------------------------------------------------
-    std::vector<std::vector<RootChild>> root_children(d->n_meshes);
+    std::vector<std::vector<RootChild>> root_children(d->n_meshes), grand_children(d->n_meshes);
     H.meshes.resize(d->n_meshes);
     uint64_t tri_total = 0;
     for (uint32_t m = 0; m < d->n_meshes; m++) tri_total += d->meshes[m].n_triangles;
@@ -1254,25 +1279,27 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
             *err = "internal: quantised BLAS boxes not conservative";
             return false;
         }
+        // The root's children, and the second-level frontier (each inner
+        // child replaced by its own children; the wide nodes were emitted in
+        // preorder, one `wide` entry per node index).
         const auto& root = col.wide[0];
         for (uint32_t k = 0; k < root.nk; k++) {
             const BinNode& kn = bin.nodes[root.kids[k]];
-            if (RT_BRAID_LEVELS >= 2 && kn.count == 0) {
-                // The child's own children (the wide nodes were emitted in
-                // preorder, one `wide` entry per node index).
-                const auto& cw = col.wide[root.refs[k] - root.idx];
-                for (uint32_t kk = 0; kk < cw.nk; kk++) {
-                    RootChild c;
-                    f32_box(bin.nodes[cw.kids[kk]].b, c.lo, c.hi);
-                    c.ref = cw.refs[kk];
-                    root_children[m].push_back(c);
-                }
-                continue;
-            }
             RootChild c;
             f32_box(kn.b, c.lo, c.hi);
             c.ref = root.refs[k];
             root_children[m].push_back(c);
+            if (kn.count == 0) {
+                const auto& cw = col.wide[root.refs[k] - root.idx];
+                for (uint32_t kk = 0; kk < cw.nk; kk++) {
+                    RootChild g;
+                    f32_box(bin.nodes[cw.kids[kk]].b, g.lo, g.hi);
+                    g.ref = cw.refs[kk];
+                    grand_children[m].push_back(g);
+                }
+            } else {
+                grand_children[m].push_back(c);
+            }
         }
     }
     if (!H.st.empty()) H.st.resize(2 * (H.normals.size() / 3), 0.0f);
@@ -1293,7 +1320,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
     if (build_bvh && d->n_instances) {
         std::vector<double> boxes;
         std::vector<uint2> items;
-        tlas_items(d, root_children, &boxes, &items, &H);
+        tlas_items(d, root_children, grand_children, &boxes, &items, &H);
         if (items.size() >= (1ull << 27)) {
             *err = "more than 2^27 instance subtrees";
             return false;

@@ -62,22 +62,22 @@ struct RootChild {
     float lo[3], hi[3];
     uint32_t ref;
 };
-// Depth of the BLAS frontier that splits a dense scene's instances into TLAS
-// items: 1 = the root's children (at most 8 per instance), 2 = their
-// children (at most 64).
-#ifndef RT_BRAID_LEVELS
-#define RT_BRAID_LEVELS 1
-#endif
-constexpr uint32_t RT_TOP_MAX = RT_BRAID_LEVELS >= 2 ? 64u : 8u;
+// Largest BLAS frontier an instance is split into: a dense scene's
+// instances become the second-level frontier (at most 8 x 8 subtrees).
+constexpr uint32_t RT_TOP_MAX = 64u;
 
 // TLAS primitives: every instance contributes one item (instance, BLAS root
 // reference) boxed by the union of its root children's world boxes, or one
 // item per root child (instance, child reference) when that splits its box
-// area well (flatten.cpp: RT_BRAID_RATIO); 6 doubles per item box. Meshes
-// without triangles contribute none. Needs H's mesh records (blas_root);
-// sets the world box in H. Instance ids must be validated.
+// area well (flatten.cpp: RT_BRAID_RATIO); in a dense scene (instance boxes
+// adding up to more than RT_BRAID_DENSE world boxes) one item per node of
+// the BLAS's second-level frontier (`grand_children`: each inner root child
+// replaced by its children). 6 doubles per item box. Meshes without
+// triangles contribute none. Needs H's mesh records (blas_root); sets the
+// world box in H. Instance ids must be validated.
 void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>>& root_children,
-                std::vector<double>* boxes, std::vector<uint2>* items, HostScene* H);
+                const std::vector<std::vector<RootChild>>& grand_children, std::vector<double>* boxes,
+                std::vector<uint2>* items, HostScene* H);
 
 // World-to-object 3x4 of every instance (f32, 3 float4 each, scene order)
 // and its record (BLAS root, index, material, mesh).
