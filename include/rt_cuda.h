@@ -156,10 +156,9 @@ int rt_intersect_batch_device(rt_session* s, const float* rays, uint64_t n, int 
  * process exits; nothing is allocated or freed per call. n beyond
  * RT_NOALLOC_MAX_RAYS is rejected with RT_ERR_INVALID. The call runs on the
  * session's device (as every session call does); the first call on a device
- * looks up the array's device address there (cudaGetSymbolAddress), so make
- * that first call before any stream capture. Each call copies the host rays
- * in and the results out and waits for the session's stream before it
- * returns.
+ * looks up the array's device address there (cudaGetSymbolAddress). The call
+ * is synchronous: it copies the host rays in and the results out on the
+ * session's stream and waits for that stream before it returns.
  * All calls share the one array: calls that overlap on the GPU (from several
  * threads or sessions on the same device) race on it and must be serialised
  * by the caller. No counterpart in the reference: its Metal backend has no
