@@ -72,6 +72,13 @@ typedef struct rt_material_desc {
     double  emission[3];             /* emitted radiance */
     int32_t area_light;              /* index into lights, or -1 */
     uint32_t id;                     /* object id for the id AOV */
+    /* Subsurface random walk (PbrParams::subsurface_*, pbr.rs:43-47):
+     * probability of entering the walk, surface colour, mean free path. */
+    double  subsurface_gain;
+    double  subsurface_color[3];
+    double  subsurface_dmfp[3];
+    int32_t interior;                /* medium inside this geometry (Material::interior), or -1 */
+    uint32_t material_reserved;      /* 0 */
 } rt_material_desc;
 
 enum {
@@ -242,6 +249,23 @@ typedef struct rt_quadric_desc {
     uint32_t material_id;
 } rt_quadric_desc;
 
+/* Participating medium: `Medium` (src/scene/medium.rs:28-43). Homogeneous
+ * when density is RT_DENSITY_NONE; RT_DENSITY_FBM scales the coefficients
+ * by clamp((fbm(p) * 0.5 + 0.5 - (1 - coverage)) * sharpness, 0, 1)
+ * (medium.rs:56-65, fBm of src/geometry/displace.rs:82-97 with amplitude 1
+ * and offset 0). */
+enum { RT_DENSITY_NONE = 0, RT_DENSITY_FBM = 1 };
+typedef struct rt_medium_desc {
+    double   sigma_a[3];
+    double   sigma_s[3];
+    double   g;               /* Henyey-Greenstein anisotropy */
+    double   emission[3];
+    double   max_distance;    /* extent along any ray (atmospheres are slabs) */
+    uint32_t density;         /* RT_DENSITY_* */
+    uint32_t octaves;
+    double   frequency, gain, lacunarity, coverage, sharpness;
+} rt_medium_desc;
+
 typedef struct rt_scene_desc {
     const rt_mesh_desc*     meshes;
     const rt_instance_desc* instances;
@@ -276,6 +300,11 @@ typedef struct rt_scene_desc {
     const rt_quadric_desc*    quadrics;
     uint32_t n_quadrics;
     uint32_t quadric_reserved; /* 0 */
+    /* Participating media (Scene::media) and the global one (Scene::atmosphere,
+     * -1 for none); materials name theirs by rt_material_desc::interior. */
+    const rt_medium_desc*     media;
+    uint32_t n_media;
+    int32_t  atmosphere;
 } rt_scene_desc;
 
 /* Integrator knobs. The reference hard-codes these as constants
@@ -305,7 +334,8 @@ typedef struct rt_params {
 #ifdef __cplusplus
 static_assert(sizeof(rt_mesh_desc) == 40, "rt_mesh_desc layout");
 static_assert(sizeof(rt_instance_desc) == 104, "rt_instance_desc layout");
-static_assert(sizeof(rt_material_desc) == 264, "rt_material_desc layout");
+static_assert(sizeof(rt_material_desc) == 328, "rt_material_desc layout");
+static_assert(sizeof(rt_medium_desc) == 136, "rt_medium_desc layout");
 static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
 static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
 static_assert(sizeof(rt_params) == 72, "rt_params layout");
@@ -315,7 +345,7 @@ static_assert(sizeof(rt_texture_desc) == 16, "rt_texture_desc layout");
 static_assert(sizeof(rt_pattern_binding) == 16, "rt_pattern_binding layout");
 static_assert(sizeof(rt_ies_desc) == 112, "rt_ies_desc layout");
 static_assert(sizeof(rt_quadric_desc) == 168, "rt_quadric_desc layout");
-static_assert(sizeof(rt_scene_desc) == 312, "rt_scene_desc layout");
+static_assert(sizeof(rt_scene_desc) == 328, "rt_scene_desc layout");
 }
 #endif
 

@@ -58,6 +58,13 @@ def lib():
         L.oracle_solve_quartic.argtypes = [vp, vp]
         L.oracle_light_pmf.restype = C.c_double
         L.oracle_light_pmf.argtypes = [vp, f64p, C.c_uint32]
+        L.oracle_medium_sample.restype = C.c_uint64
+        L.oracle_medium_sample.argtypes = [vp, vp, vp, C.c_double, vp, C.c_uint64, C.c_uint64, C.c_uint64, vp, vp]
+        L.oracle_medium_transmittance.argtypes = [vp, vp, vp, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, vp]
+        L.oracle_medium_density.argtypes = [vp, C.c_uint64, vp, vp]
+        L.oracle_hg_phase.argtypes = [C.c_double, C.c_uint64, vp, vp]
+        L.oracle_hg_sample.argtypes = [C.c_double, vp, C.c_uint64, vp, vp]
+        L.oracle_sss_medium.argtypes = [vp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -65,6 +72,70 @@ def lib():
 def _f64(a):
     a = np.ascontiguousarray(a, dtype=np.float64)
     return a, a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _medium_desc(med):
+    from rtcuda import abi
+    d = abi.RtMediumDesc()
+    for key, val in med.items():
+        setattr(d, key, abi.c_double3(*val) if isinstance(val, tuple) else val)
+    return d
+
+
+def medium_sample(med, o, d, t_max, beta, pixel, sample, n):
+    """n draws of volume.rs sample_distance from one PCG32 stream: (pass
+    weight sum, scatter weight sum, scatters)."""
+    md = _medium_desc(med)
+    o, _ = _f64(o)
+    d, _ = _f64(d)
+    b, _ = _f64(beta)
+    ps, ss = np.zeros(3), np.zeros(3)
+    k = lib().oracle_medium_sample(C.byref(md), o.ctypes.data, d.ctypes.data, float(t_max), b.ctypes.data,
+                                   int(pixel), int(sample), int(n), ps.ctypes.data, ss.ctypes.data)
+    return ps, ss, int(k)
+
+
+def medium_transmittance(med, o, d, dist, pixel, sample, n):
+    """Mean of n volume.rs transmittance estimates (RGB)."""
+    md = _medium_desc(med)
+    o, _ = _f64(o)
+    d, _ = _f64(d)
+    out = np.zeros(3)
+    lib().oracle_medium_transmittance(C.byref(md), o.ctypes.data, d.ctypes.data, float(dist), int(pixel),
+                                      int(sample), int(n), out.ctypes.data)
+    return out
+
+
+def medium_density(med, points):
+    md = _medium_desc(med)
+    p, _ = _f64(np.reshape(points, (-1, 3)))
+    out = np.zeros(len(p))
+    lib().oracle_medium_density(C.byref(md), len(p), p.ctypes.data, out.ctypes.data)
+    return out
+
+
+def hg_phase(g, cos_theta):
+    c, _ = _f64(np.ravel(cos_theta))
+    out = np.zeros(len(c))
+    lib().oracle_hg_phase(float(g), len(c), c.ctypes.data, out.ctypes.data)
+    return out
+
+
+def hg_sample(g, wo, u):
+    """(wi xyz, pdf) per uniform pair."""
+    w, _ = _f64(wo)
+    uu, _ = _f64(np.reshape(u, (-1, 2)))
+    out = np.zeros((len(uu), 4))
+    lib().oracle_hg_sample(float(g), w.ctypes.data, len(uu), uu.ctypes.data, out.ctypes.data)
+    return out
+
+
+def sss_medium(color, dmfp):
+    c, _ = _f64(color)
+    m, _ = _f64(dmfp)
+    sa, ss = np.zeros(3), np.zeros(3)
+    lib().oracle_sss_medium(c.ctypes.data, m.ctypes.data, sa.ctypes.data, ss.ctypes.data)
+    return sa, ss
 
 
 def quadric_intersect(desc, origins, directions):

@@ -944,6 +944,203 @@ static double fbm(V3 p, double frequency, uint32_t octaves, double gain, double 
     return sum;
 }
 
+// ---- participating media (src/scene/medium.rs, src/raytracer/pt/volume.rs) ----
+
+struct Medium {  // medium.rs:28-43
+    V3 sigma_a, sigma_s, emission;
+    double g = 0.0, max_distance = INF;
+    bool fbm_density = false;
+    uint32_t octaves = 5;
+    double frequency = 0.3, gain = 0.55, lacunarity = 2.0, coverage = 0.5, sharpness = 4.0;
+    V3 sigma_t() const { return sigma_a + sigma_s; }
+    double majorant() const { return max_comp(sigma_t()); }  // medium.rs:50-55
+    double density_at(V3 p) const {                           // medium.rs:57-66
+        if (!fbm_density) return 1.0;
+        double n = fbm(p, frequency, octaves, gain, lacunarity) * 0.5 + 0.5;
+        return std::min(std::max((n - (1.0 - coverage)) * sharpness, 0.0), 1.0);
+    }
+};
+
+// medium.rs:73-76
+static double hg_phase(double g, double cos_theta) {
+    double denom = 1.0 + g * g + 2.0 * g * cos_theta;
+    return (1.0 - g * g) / (4.0 * PI * denom * std::sqrt(std::fmax(denom, 1e-9)));
+}
+
+// medium.rs:80-103: direction around the propagation direction -wo; pdf = phase.
+static V3 hg_sample(double g, V3 wo, double u1, double u2, double* pdf) {
+    double cos_theta;
+    if (std::fabs(g) < 1e-3) {
+        cos_theta = 1.0 - 2.0 * u1;
+    } else {
+        double sq = (1.0 - g * g) / (1.0 + g - 2.0 * g * u1);
+        cos_theta = -(1.0 + g * g - sq * sq) / (2.0 * g);
+    }
+    double sin_theta = std::sqrt(std::fmax(1.0 - cos_theta * cos_theta, 0.0));
+    double phi = 2.0 * PI * u2;
+    V3 w = -wo;
+    V3 a = std::fabs(w.x) > 0.9 ? V3{0, 1, 0} : V3{1, 0, 0};
+    V3 t = normalize(cross(w, a));
+    V3 b = cross(w, t);
+    V3 wi = normalize(t * (sin_theta * std::cos(phi)) + b * (sin_theta * std::sin(phi)) + w * cos_theta);
+    *pdf = hg_phase(g, dot(wo, wi) * -1.0);
+    return wi;
+}
+
+static V3 exp3(V3 v, double t) { return {std::exp(-v.x * t), std::exp(-v.y * t), std::exp(-v.z * t)}; }
+
+// volume.rs:11-20: scatter at t (scatter = true) or pass the segment; the
+// weight folds transmittance, sigma_s and the sampling pdf.
+struct MediumEvent {
+    bool scatter = false;
+    double t = 0.0;
+    V3 weight{1, 1, 1};
+};
+
+template <class R>
+static MediumEvent sample_homogeneous(const Medium& m, double t_max, V3 beta, R& rng) {  // volume.rs:62-105
+    MediumEvent ev;
+    V3 st = m.sigma_t();
+    if ((st.x + st.y + st.z) / 3.0 <= 1e-9) return ev;
+    V3 b{std::fmax(beta.x, 0.0), std::fmax(beta.y, 0.0), std::fmax(beta.z, 0.0)};  // volume.rs:51-59
+    double total = b.x + b.y + b.z;
+    double w[3] = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0};
+    if (total > 1e-12) {
+        w[0] = b.x / total;
+        w[1] = b.y / total;
+        w[2] = b.z / total;
+    }
+    double u = rng.next_f64();
+    int c = u < w[0] ? 0 : (u < w[0] + w[1] ? 1 : 2);
+    double sigma_c = std::fmax(axis_of(st, c), 1e-9);
+    double t = -std::log(std::fmax(1.0 - rng.next_f64(), 1e-12)) / sigma_c;
+    if (t < t_max) {
+        V3 tr = exp3(st, t);
+        double pdf = w[0] * st.x * tr.x + w[1] * st.y * tr.y + w[2] * st.z * tr.z;
+        if (pdf <= 1e-300) {
+            ev.weight = {0, 0, 0};
+            return ev;
+        }
+        ev.scatter = true;
+        ev.t = t;
+        ev.weight = m.sigma_s * tr / pdf;
+        return ev;
+    }
+    V3 tr = exp3(st, t_max);
+    double pdf = w[0] * tr.x + w[1] * tr.y + w[2] * tr.z;
+    ev.weight = pdf <= 1e-300 ? V3{0, 0, 0} : tr / pdf;
+    return ev;
+}
+
+// volume.rs:109-156: weighted delta tracking against the channel-max majorant.
+template <class R>
+static MediumEvent sample_delta_tracked(const Medium& m, V3 o, V3 d, double t_max, R& rng) {
+    MediumEvent ev;
+    double maj = m.majorant();
+    if (maj <= 1e-9) return ev;
+    V3 st = m.sigma_t();
+    double t = 0.0;
+    V3 weight{1, 1, 1};
+    for (int i = 0; i < 10000; i++) {
+        t -= std::log(std::fmax(1.0 - rng.next_f64(), 1e-12)) / maj;
+        if (t >= t_max) {
+            ev.weight = weight;
+            return ev;
+        }
+        double rho = m.density_at(o + d * t);
+        V3 sh = st * rho;
+        double p_real = std::min(std::max((sh.x + sh.y + sh.z) / 3.0 / maj, 0.0), 1.0);
+        if (rng.next_f64() < p_real) {
+            ev.scatter = true;
+            ev.t = t;
+            ev.weight = weight * (m.sigma_s * rho) / (maj * p_real);
+            return ev;
+        }
+        double p_null = std::fmax(1.0 - p_real, 1e-9);
+        weight = weight * V3{(1.0 - sh.x / maj) / p_null, (1.0 - sh.y / maj) / p_null, (1.0 - sh.z / maj) / p_null};
+        if (max_comp(weight) < 1e-6) {
+            ev.weight = {0, 0, 0};
+            return ev;
+        }
+    }
+    ev.weight = weight;
+    return ev;
+}
+
+// volume.rs:35-49 (o, d: the ray; d normalised as Ray::new keeps it).
+template <class R>
+static MediumEvent sample_distance(const Medium& m, V3 o, V3 d, double t_max, V3 beta, R& rng) {
+    t_max = std::fmin(t_max, m.max_distance);
+    if (!m.fbm_density) return sample_homogeneous(m, t_max, beta, rng);
+    return sample_delta_tracked(m, o, d, t_max, rng);
+}
+
+// volume.rs:160-193: closed form, or ratio tracking.
+template <class R>
+static V3 medium_transmittance(const Medium& m, V3 o, V3 d, double dist, R& rng) {
+    dist = std::fmin(dist, m.max_distance);
+    V3 st = m.sigma_t();
+    if (!m.fbm_density) return exp3(st, dist);
+    double maj = m.majorant();
+    if (maj <= 1e-9) return {1, 1, 1};
+    double t = 0.0;
+    V3 tr{1, 1, 1};
+    for (int i = 0; i < 10000; i++) {
+        t -= std::log(std::fmax(1.0 - rng.next_f64(), 1e-12)) / maj;
+        if (t >= dist) break;
+        double rho = m.density_at(o + d * t);
+        tr = tr * V3{1.0 - st.x * rho / maj, 1.0 - st.y * rho / maj, 1.0 - st.z * rho / maj};
+        if (max_comp(tr) < 1e-5) return {0, 0, 0};
+    }
+    return tr;
+}
+
+// volume.rs:199-235: equiangular sampling toward a point light and its pdf.
+static double equiangular_pdf(V3 o, V3 d, double t_max, V3 lp, double t) {
+    double delta = dot(lp - o, d);
+    double h = std::fmax(length(lp - (o + d * delta)), 1e-6);
+    double ta = std::atan(-delta / h), tb = std::atan((t_max - delta) / h);
+    double span = std::fmax(tb - ta, 1e-9);
+    return h / (span * (h * h + (t - delta) * (t - delta)));
+}
+static double equiangular_sample(V3 o, V3 d, double t_max, V3 lp, double u, double* pdf) {
+    double delta = dot(lp - o, d);
+    double h = std::fmax(length(lp - (o + d * delta)), 1e-6);
+    double ta = std::atan(-delta / h), tb = std::atan((t_max - delta) / h);
+    double span = std::fmax(tb - ta, 1e-9);
+    double t = delta + h * std::tan(ta + u * span);
+    t = std::min(std::max(t, 0.0), t_max);
+    *pdf = h / (span * (h * h + (t - delta) * (t - delta)));
+    return t;
+}
+
+// volume.rs:240-249
+static double distance_pdf_approx(const Medium& m, double t, double t_max) {
+    V3 st = m.sigma_t();
+    double s = std::fmax((st.x + st.y + st.z) / 3.0, 1e-9);
+    return t < t_max ? s * std::exp(-s * t) : std::exp(-s * t_max);
+}
+
+// volume.rs:259-288: the random-walk medium of a PxrSurface subsurface
+// colour and mean free path (Kulla-Conty albedo inversion, Christensen-Burley
+// scaling).
+static Medium sss_medium(V3 color, V3 dmfp) {
+    auto alpha_fit = [](double a) {
+        a = std::min(std::max(a, 0.0), 1.0);
+        return 1.0 - std::exp(-a * (11.43 - 15.38 * a + 13.91 * a * a));
+    };
+    auto s_fit = [](double a) { return 1.85 - a + 7.0 * std::pow(std::fabs(a - 0.8), 3); };
+    auto cl = [](double v) { return std::min(std::max(v, 0.0), 1.0); };
+    V3 a{cl(color.x), cl(color.y), cl(color.z)};
+    V3 st{s_fit(a.x) / std::fmax(dmfp.x, 1e-5), s_fit(a.y) / std::fmax(dmfp.y, 1e-5), s_fit(a.z) / std::fmax(dmfp.z, 1e-5)};
+    V3 alpha{alpha_fit(a.x), alpha_fit(a.y), alpha_fit(a.z)};
+    Medium m;
+    m.sigma_s = alpha * st;
+    m.sigma_a = st - m.sigma_s;
+    m.emission = {0, 0, 0};
+    return m;
+}
+
 struct PatInput {
     int32_t node;  // -1: constant
     V3 value;
@@ -1570,10 +1767,13 @@ struct Pbr {
     double glass_gain, glass_ior, glass_rough;
     V3 refraction_color, glow;
     double presence;
+    double subsurface_gain = 0.0;
+    V3 subsurface_color, subsurface_dmfp;
     // Material fields
     V3 emission;
     int32_t area_light;
     uint32_t id;
+    int32_t interior = -1;  // Material::interior (material.rs:35-37), -1 for none
 
     static Pbr from(const rt_material_desc& m) {
         Pbr p;
@@ -1597,6 +1797,10 @@ struct Pbr {
         p.emission = v3(m.emission);
         p.area_light = m.area_light;
         p.id = m.id;
+        p.subsurface_gain = m.subsurface_gain;
+        p.subsurface_color = v3(m.subsurface_color);
+        p.subsurface_dmfp = v3(m.subsurface_dmfp);
+        p.interior = m.interior;
         return p;
     }
     // pbr.rs:86-96
@@ -1946,6 +2150,16 @@ struct Scene {
     std::vector<PatNode> patterns;
     std::vector<std::vector<std::pair<uint32_t, uint32_t>>> bindings;  // per material: (field, node)
     std::vector<Texture> textures;
+    std::vector<Medium> media;  // Scene::media
+    int32_t atmosphere = -1;     // Scene::atmosphere
+
+    // A volume hull (pt/mod.rs:662-667, 1280-1284): an interior medium, no
+    // lobes, no emission -- the surface only bounds the medium.
+    bool is_hull(uint32_t material_id) const {
+        const Pbr& m = materials[material_id];
+        double w[5];
+        return m.interior >= 0 && !m.lobe_weights(w) && max_comp(m.emission + m.glow) <= 0.0;
+    }
 
     // shade_params (pt/mod.rs:389-439): the material with its pattern
     // outputs substituted; footprint = cone width x st density, and the ray
@@ -2161,6 +2375,22 @@ static double power_heuristic(double a, double b) {  // mod.rs:992-996
     return a2 + b2 <= 0.0 ? 0.0 : a2 / (a2 + b2);
 }
 
+// mod.rs:34-67: nested media, the top is the medium the ray travels in and
+// the atmosphere the implicit bottom.
+struct MedStack {
+    uint32_t s[8];
+    int depth = 0;
+    int32_t atmosphere;
+    explicit MedStack(int32_t a) : atmosphere(a) {}
+    int32_t current() const { return depth > 0 ? (int32_t)s[depth - 1] : atmosphere; }
+    void push(uint32_t m) {
+        if (depth < 8) s[depth++] = m;
+    }
+    void pop() {
+        if (depth > 0) depth--;
+    }
+};
+
 struct Tracer {
     const Scene& sc;
     const rt_params& prm;
@@ -2169,15 +2399,33 @@ struct Tracer {
     // Angular size of one pixel, the initial ray-cone spread (pt/mod.rs:73-76).
     double pixel_spread() const { return std::tan(sc.cam.fov * PI / 180.0 / 2.0) * 2.0 / (double)sc.cam.height; }
 
-    // mod.rs:1254-1306 transmittance, restricted to surfaces (no media).
-    V3 transmittance(V3 origin, V3 dir, double remaining) {
+    // mod.rs:1244-1306 transmittance: opaque surfaces block, cutouts
+    // attenuate, volume hulls push and pop the medium (the shadow ray starts
+    // in the shading point's medium), and every segment takes its medium's
+    // transmittance.
+    V3 transmittance(V3 origin, V3 dir, double remaining, int32_t medium, Pcg32& rng) {
+        MedStack ms(sc.atmosphere);
+        if (medium >= 0 && medium != sc.atmosphere) ms.push((uint32_t)medium);
         V3 vis{1, 1, 1};
         for (int k = 0; k < MAX_PRESENCE_SKIPS; k++) {
             shadow_rays++;
             Hit h;
             Ray r = make_ray(origin, dir);
-            if (!sc.intersect(r, &h, &cshadow)) return vis;
-            if (h.t >= remaining) return vis;
+            const bool found = sc.intersect(r, &h, &cshadow);
+            const double seg = std::fmin(found ? h.t : remaining, remaining);
+            const int32_t cur = ms.current();
+            if (cur >= 0) {
+                vis = vis * medium_transmittance(sc.media[cur], origin, dir, seg, rng);
+                if (max_comp(vis) < 1e-4) return {0, 0, 0};
+            }
+            if (!found || h.t >= remaining) return vis;
+            if (sc.is_hull(h.material_id)) {
+                if (h.front_face) ms.push((uint32_t)sc.materials[h.material_id].interior);
+                else ms.pop();
+                origin = h.point + dir * RAY_OFFSET;
+                remaining -= h.t + RAY_OFFSET;
+                continue;
+            }
             double presence = std::min(std::max(sc.shade_params(h, dir, 0.0).presence, 0.0), 1.0);
             if (presence >= 1.0) return {0, 0, 0};
             vis = vis * (1.0 - presence);
@@ -2188,12 +2436,14 @@ struct Tracer {
         return vis;
     }
     // mod.rs:1212-1237
-    V3 visibility_to(V3 p, V3 n, V3 target) {
+    V3 visibility_to(V3 p, V3 n, V3 target, int32_t medium, Pcg32& rng) {
         V3 dir = target - p;
         double dist = length(dir);
-        return transmittance(p + n * RAY_OFFSET, normalize(dir), dist - 1e-3);
+        return transmittance(p + n * RAY_OFFSET, normalize(dir), dist - 1e-3, medium, rng);
     }
-    V3 visibility_toward(V3 p, V3 n, V3 wi) { return transmittance(p + n * RAY_OFFSET, wi, 1e8); }
+    V3 visibility_toward(V3 p, V3 n, V3 wi, int32_t medium, Pcg32& rng) {
+        return transmittance(p + n * RAY_OFFSET, wi, 1e8, medium, rng);
+    }
 
     // mod.rs:1000-1023 (rect/disk/sphere).
     static double light_pdf_sa(const Light& l, V3 origin, const Hit& h) {
@@ -2216,7 +2466,7 @@ struct Tracer {
 
     // mod.rs:1177-1209
     template <class E>
-    V3 area_contrib(V3 p, V3 n, V3 sp, const Light& l, E& eval, double pick) {
+    V3 area_contrib(V3 p, V3 n, V3 sp, const Light& l, E& eval, double pick, int32_t medium, Pcg32& rng) {
         V3 to = sp - p;
         double dist2 = std::fmax(length_sq(to), 1e-12);
         V3 wi = normalize(to);
@@ -2225,7 +2475,7 @@ struct Tracer {
         double bpdf;
         V3 f = eval(wi, &bpdf);
         if (max_comp(f) <= 0.0) return {0, 0, 0};
-        V3 vis = visibility_to(p, n, sp);
+        V3 vis = visibility_to(p, n, sp, medium, rng);
         if (max_comp(vis) <= 0.0) return {0, 0, 0};
         double pdf_sa = pick * dist2 / (cos_l * l.area);
         double w = power_heuristic(pdf_sa, bpdf);
@@ -2234,7 +2484,7 @@ struct Tracer {
 
     // mod.rs:1032-1174 (point, distant, rect, disk, sphere).
     template <class E>
-    V3 sample_light(const Light& l, V3 p, V3 n, E& eval, double pick, Pcg32& rng) {
+    V3 sample_light(const Light& l, V3 p, V3 n, E& eval, double pick, int32_t medium, Pcg32& rng) {
         switch (l.type) {
             case RT_LIGHT_POINT: {
                 V3 to = l.p - p;
@@ -2243,7 +2493,7 @@ struct Tracer {
                 double bp;
                 V3 f = eval(wi, &bp);
                 if (max_comp(f) <= 0.0) return {0, 0, 0};
-                V3 vis = visibility_to(p, n, l.p);
+                V3 vis = visibility_to(p, n, l.p, medium, rng);
                 if (max_comp(vis) <= 0.0) return {0, 0, 0};
                 return f * l.radiance_toward(wi) * vis / (dist2 * pick);
             }
@@ -2262,20 +2512,20 @@ struct Tracer {
                 double bp;
                 V3 f = eval(wi, &bp);
                 if (max_comp(f) <= 0.0) return {0, 0, 0};
-                V3 vis = visibility_toward(p, n, wi);
+                V3 vis = visibility_toward(p, n, wi, medium, rng);
                 if (max_comp(vis) <= 0.0) return {0, 0, 0};
                 return f * l.radiance() * vis / pick;
             }
             case RT_LIGHT_RECT: {
                 double u = rng.next_f64(), v = rng.next_f64();
                 V3 sp = l.p + l.e1 * u + l.e2 * v;
-                return area_contrib(p, n, sp, l, eval, pick);
+                return area_contrib(p, n, sp, l, eval, pick, medium, rng);
             }
             case RT_LIGHT_DISK: {
                 double u = rng.next_f64(), v = rng.next_f64();
                 double r = std::sqrt(u), phi = 2.0 * PI * v;
                 V3 sp = l.p + l.e1 * (r * std::cos(phi)) + l.e2 * (r * std::sin(phi));
-                return area_contrib(p, n, sp, l, eval, pick);
+                return area_contrib(p, n, sp, l, eval, pick, medium, rng);
             }
             case RT_LIGHT_DOME: {  // mod.rs:1139-1172: the map's importance sampling, or a uniform sphere
                 double u = rng.next_f64(), v = rng.next_f64();
@@ -2296,7 +2546,7 @@ struct Tracer {
                 double bp;
                 V3 f = eval(wi, &bp);
                 if (max_comp(f) <= 0.0) return {0, 0, 0};
-                V3 vis = visibility_toward(p, n, wi);
+                V3 vis = visibility_toward(p, n, wi, medium, rng);
                 if (max_comp(vis) <= 0.0) return {0, 0, 0};
                 return f * rad * vis * (power_heuristic(pdf_sa, bp) / pdf_sa);
             }
@@ -2318,7 +2568,7 @@ struct Tracer {
                 double dist = std::sqrt(dist2) * cos_t -
                               std::sqrt(std::fmax(l.radius * l.radius - dist2 * sin_t * sin_t, 0.0));
                 V3 target = p + wi * dist;
-                V3 vis = visibility_to(p, n, target);
+                V3 vis = visibility_to(p, n, target, medium, rng);
                 if (max_comp(vis) <= 0.0) return {0, 0, 0};
                 double pdf_sa = pick / std::fmax(2.0 * PI * (1.0 - cos_max), 1e-12);
                 double w = power_heuristic(pdf_sa, bp);
@@ -2328,7 +2578,7 @@ struct Tracer {
         return {0, 0, 0};
     }
 
-    // mod.rs:449-990 trace_full, surface transport only.
+    // mod.rs:449-990 trace_full (hair excluded).
     V3 trace(Ray ray, Pcg32& rng, Aux& aux) {
         V3 L{0, 0, 0};
         int first_specular = -1;  // -1 None, 0 false, 1 true
@@ -2344,11 +2594,108 @@ struct Tracer {
         bool from_camera = true;
         int presence_skips = 0;
         double cone_width = 0.0, cone_spread = pixel_spread();
+        MedStack med_stack(sc.atmosphere);
+        // Multiple scattering needs a deeper budget (mod.rs:483-484).
+        const uint32_t max_bounces = sc.media.empty() ? prm.max_depth : 64u;
         uint32_t depth = 0;
-        while (depth < prm.max_depth) {
+        auto roulette = [&]() {
+            if (depth >= prm.rr_start) {
+                double q = std::fmin(max_comp(beta), 0.95);
+                if (q <= 0.0 || rng.next_f64() > q) return false;
+                beta = beta / q;
+            }
+            return true;
+        };
+        while (depth < max_bounces) {
             Hit hit;
             ext_rays++;
-            if (!sc.intersect(ray, &hit, &cext)) {
+            const bool found = sc.intersect(ray, &hit, &cext);
+            // Medium interaction along this segment, before any surface
+            // (mod.rs:490-640).
+            const int32_t medium = med_stack.current();
+            if (medium >= 0) {
+                const Medium& med = sc.media[medium];
+                const double t_limit = found ? hit.t : 1e8;
+                // One light pick per segment, shared by equiangular and
+                // collision NEE so their MIS weights cancel the pick pmf.
+                uint32_t pli = 0;
+                double ppmf = 0.0;
+                const V3 mid = ray.o + ray.d * std::fmin(std::fmin(t_limit, med.max_distance) * 0.5, 50.0);
+                const bool seg_pick = sc.ls.sample(mid, rng.next_f64(), &pli, &ppmf);
+                const bool point = seg_pick && sc.lights[pli].type == RT_LIGHT_POINT;
+                const double t_seg = std::fmin(t_limit, med.max_distance);
+                if (point && t_seg > 1e-6) {
+                    // Equiangular single-scatter NEE toward the point light.
+                    const V3 lp = sc.lights[pli].p;
+                    double pdf_eq;
+                    const double t_eq = equiangular_sample(ray.o, ray.d, t_seg, lp, rng.next_f64(), &pdf_eq);
+                    if (pdf_eq > 1e-12) {
+                        const V3 p = ray.o + ray.d * t_eq;
+                        const double rho = med.density_at(p);
+                        if (rho > 0.0) {
+                            const V3 tr = medium_transmittance(med, ray.o, ray.d, t_eq, rng);
+                            const V3 sig_s = med.sigma_s * rho;
+                            const V3 to_l = lp - p;
+                            const double dist2 = std::fmax(length_sq(to_l), 1e-12);
+                            const V3 wi = normalize(to_l), wo = -normalize(ray.d);
+                            const double ph = hg_phase(med.g, -dot(wo, wi));
+                            const V3 vis = transmittance(p, wi, std::sqrt(dist2) - 1e-3, medium, rng);
+                            if (max_comp(vis) > 0.0) {
+                                const double pdf_d = distance_pdf_approx(med, t_eq, t_seg);
+                                const double w_eq = pdf_eq / (pdf_eq + pdf_d);
+                                emit(beta * (sig_s * tr * vis * sc.lights[pli].radiance_toward(wi) *
+                                             (ph * w_eq / (dist2 * pdf_eq * ppmf))));
+                            }
+                        }
+                    }
+                }
+                const MediumEvent ev = sample_distance(med, ray.o, ray.d, t_limit, beta, rng);
+                beta = beta * ev.weight;
+                if (ev.scatter) {
+                    const V3 p = ray.o + ray.d * ev.t;
+                    if (!aux_set) {
+                        aux_set = true;
+                        const V3 st = med.sigma_t();
+                        aux.albedo = {med.sigma_s.x / std::fmax(st.x, 1e-9), med.sigma_s.y / std::fmax(st.y, 1e-9),
+                                      med.sigma_s.z / std::fmax(st.z, 1e-9)};
+                        aux.normal = -normalize(ray.d);
+                        aux.depth = travel + ev.t;
+                        aux.id = 0;
+                    }
+                    if (first_specular < 0) first_specular = 0;
+                    if (max_comp(med.emission) > 0.0) emit(beta * med.emission);
+                    const V3 wo = -normalize(ray.d);
+                    const double g = med.g;
+                    if (seg_pick) {
+                        double w_dist = 1.0;
+                        if (point) {
+                            const double pdf_d = distance_pdf_approx(med, ev.t, t_seg);
+                            const double pdf_e = equiangular_pdf(ray.o, ray.d, t_seg, sc.lights[pli].p, ev.t);
+                            w_dist = pdf_d / (pdf_d + pdf_e);
+                        }
+                        auto eval = [&](V3 wi, double* pdf) -> V3 {
+                            const double ph = hg_phase(g, -dot(wo, wi));
+                            *pdf = ph;
+                            return {ph, ph, ph};
+                        };
+                        const V3 c = sample_light(sc.lights[pli], p, V3{0, 0, 0}, eval, ppmf, medium, rng);
+                        emit(beta * c * w_dist);
+                    }
+                    const double u1 = rng.next_f64(), u2 = rng.next_f64();
+                    double pdf;
+                    const V3 wi = hg_sample(g, wo, u1, u2, &pdf);
+                    prev_pdf = pdf;
+                    prev_origin = p;
+                    from_camera = false;
+                    cone_spread += 0.4;
+                    ray = make_ray(p, wi);
+                    depth++;
+                    if (!roulette()) break;
+                    continue;
+                }
+                if (max_comp(beta) <= 0.0) break;
+            }
+            if (!found) {
                 // mod.rs:643-656: the first dome light (MIS against its NEE
                 // sampling unless seen from the camera), else the background.
                 int dome = -1;
@@ -2370,6 +2717,15 @@ struct Tracer {
                 }
                 break;
             }
+            // Volume hull: the crossing only toggles the medium (mod.rs:662-680).
+            if (sc.is_hull(hit.material_id) && presence_skips < MAX_PRESENCE_SKIPS) {
+                presence_skips++;
+                travel += hit.t;
+                if (hit.front_face) med_stack.push((uint32_t)sc.materials[hit.material_id].interior);
+                else med_stack.pop();
+                ray = make_ray(hit.point + normalize(ray.d) * RAY_OFFSET, ray.d);
+                continue;
+            }
             V3 wo = -normalize(ray.d);
             cone_width += hit.t * cone_spread;
             travel += hit.t;
@@ -2377,7 +2733,7 @@ struct Tracer {
             if (!aux_set) {
                 aux_set = true;
                 V3 a = pbr.diffuse_color * pbr.diffuse_gain + pbr.specular_f0() * (pbr.has_specular() ? 1.0 : 0.0) +
-                       pbr.refraction_color * pbr.glass_gain;
+                       pbr.subsurface_color * pbr.subsurface_gain + pbr.refraction_color * pbr.glass_gain;
                 aux.albedo = {std::fmin(a.x, 1.0), std::fmin(a.y, 1.0), std::fmin(a.z, 1.0)};
                 aux.normal = dot(hit.normal, wo) >= 0.0 ? hit.normal : -hit.normal;
                 aux.depth = travel;
@@ -2404,6 +2760,69 @@ struct Tracer {
                 }
                 emit(beta * emission * weight);
             }
+            // Subsurface scattering (mod.rs:794-892): with probability
+            // subsurfaceGain an isotropic random walk inside the object through
+            // the Burley-fit homogeneous medium, leaving diffusely where the
+            // walk first reaches a surface.
+            if (pbr.subsurface_gain > 0.0 &&
+                rng.next_f64() < std::min(std::max(pbr.subsurface_gain, 0.0), 1.0)) {
+                if (first_specular < 0) first_specular = 0;
+                const Medium sss = sss_medium(pbr.subsurface_color, pbr.subsurface_dmfp);
+                const Frame entry(-n);
+                const double e1 = rng.next_f64(), e2 = rng.next_f64();
+                const double er = std::sqrt(e1), ephi = 2.0 * PI * e2;
+                Ray walk = make_ray(hit.point - n * RAY_OFFSET,
+                                    entry.to_world(V3{er * std::cos(ephi), er * std::sin(ephi), std::sqrt(std::fmax(1.0 - e1, 0.0))}));
+                bool exited = false;
+                for (int step = 0; step < 256; step++) {
+                    Hit wh;
+                    ext_rays++;
+                    if (!sc.intersect(walk, &wh, &cext)) break;  // escaped through a crack
+                    const MediumEvent ev = sample_distance(sss, walk.o, walk.d, wh.t, beta, rng);
+                    beta = beta * ev.weight;
+                    if (ev.scatter) {
+                        const V3 p = walk.o + walk.d * ev.t;
+                        const double u = rng.next_f64(), v = rng.next_f64();
+                        const double z = 1.0 - 2.0 * u, rr = std::sqrt(std::fmax(1.0 - z * z, 0.0)), ph = 2.0 * PI * v;
+                        walk = make_ray(p, V3{rr * std::cos(ph), rr * std::sin(ph), z});
+                        const double q = std::fmin(max_comp(beta), 0.95);
+                        if (q <= 0.0 || (step > 8 && rng.next_f64() > q)) break;
+                        if (step > 8) beta = beta / q;
+                        continue;
+                    }
+                    const V3 out_n = dot(wh.normal, walk.d) > 0.0 ? wh.normal : -wh.normal;
+                    const Frame xf(out_n);
+                    const V3 exit_p = walk.o + walk.d * wh.t;
+                    uint32_t xli;
+                    double xpmf;
+                    if (sc.ls.sample(exit_p, rng.next_f64(), &xli, &xpmf)) {
+                        auto eval = [&](V3 wi, double* pdf) -> V3 {
+                            const V3 wl = xf.to_local(wi);
+                            if (wl.z <= 0.0) {
+                                *pdf = 0.0;
+                                return {0, 0, 0};
+                            }
+                            *pdf = wl.z / PI;
+                            return V3{1, 1, 1} * (wl.z / PI);
+                        };
+                        emit(beta * sample_light(sc.lights[xli], exit_p, out_n, eval, xpmf, medium, rng));
+                    }
+                    const double x1 = rng.next_f64(), x2 = rng.next_f64();
+                    const double xr = std::sqrt(x1), xphi = 2.0 * PI * x2;
+                    const V3 local{xr * std::cos(xphi), xr * std::sin(xphi), std::sqrt(std::fmax(1.0 - x1, 0.0))};
+                    prev_pdf = std::fmax(local.z, 1e-9) / PI;
+                    prev_origin = exit_p;
+                    from_camera = false;
+                    cone_spread += 0.4;
+                    ray = make_ray(exit_p + out_n * RAY_OFFSET, xf.to_world(local));
+                    exited = true;
+                    break;
+                }
+                if (!exited) break;
+                depth++;
+                if (!roulette()) break;
+                continue;
+            }
             Frame frame(n);
             V3 wo_l = frame.to_local(wo);
             double lw[5];
@@ -2421,7 +2840,7 @@ struct Tracer {
                 uint32_t li;
                 double pmf;
                 if (sc.ls.sample(hit.point, rng.next_f64(), &li, &pmf)) {
-                    V3 c = sample_light(sc.lights[li], hit.point, n, eval, pmf, rng);
+                    V3 c = sample_light(sc.lights[li], hit.point, n, eval, pmf, medium, rng);
                     emit(beta * c);
                 }
             }
@@ -2434,14 +2853,14 @@ struct Tracer {
             prev_origin = hit.point;
             from_camera = false;
             cone_spread += std::fmin(1.0 / (1.0 + s.pdf), 0.4);  // pt/mod.rs:965-967
+            if (s.transmitted && pbr.interior >= 0) {  // mod.rs:969-975
+                if (entering) med_stack.push((uint32_t)pbr.interior);
+                else med_stack.pop();
+            }
             double off = s.transmitted ? -RAY_OFFSET : RAY_OFFSET;
             ray = make_ray(hit.point + n * off, wi_world);
             depth++;
-            if (depth >= prm.rr_start) {
-                double q = std::fmin(max_comp(beta), 0.95);
-                if (q <= 0.0 || rng.next_f64() > q) break;
-                beta = beta / q;
-            }
+            if (!roulette()) break;
         }
         return L;
     }
@@ -2536,6 +2955,23 @@ static void parallel_for(uint64_t n, int threads, F&& f) {
 
 extern "C" {
 
+static Medium medium_from(const rt_medium_desc& md) {
+    Medium m;
+    m.sigma_a = v3(md.sigma_a);
+    m.sigma_s = v3(md.sigma_s);
+    m.emission = v3(md.emission);
+    m.g = md.g;
+    m.max_distance = md.max_distance;
+    m.fbm_density = md.density == RT_DENSITY_FBM;
+    m.octaves = md.octaves;
+    m.frequency = md.frequency;
+    m.gain = md.gain;
+    m.lacunarity = md.lacunarity;
+    m.coverage = md.coverage;
+    m.sharpness = md.sharpness;
+    return m;
+}
+
 oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
     if (!d) return nullptr;
     auto* os = new oracle_scene();
@@ -2588,8 +3024,11 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
         q.scale = std::fmax(std::cbrt(lx * ly * lz), 1e-12);
         s.quadrics.push_back(q);
     }
+    for (uint32_t k = 0; k < d->n_media && d->media; k++) s.media.push_back(medium_from(d->media[k]));
+    s.atmosphere = (d->atmosphere >= 0 && (uint32_t)d->atmosphere < s.media.size()) ? d->atmosphere : -1;
     for (uint32_t i = 0; i < d->n_materials; i++) {
         s.materials.push_back(Pbr::from(d->materials[i]));
+        if (s.materials.back().interior >= (int32_t)s.media.size()) s.materials.back().interior = -1;
         if (d->materials[i].presence < 1.0) s.any_presence = true;
     }
     load_patterns(d, s.patterns);
@@ -2941,7 +3380,8 @@ void oracle_transmittance(const oracle_scene* os, const float* planes, uint64_t 
             const float* po = planes + 4 * i;
             const float* pd = planes + 4 * n + 4 * i;
             V3 o{po[0], po[1], po[2]}, d{pd[0], pd[1], pd[2]};
-            V3 v = tr.transmittance(o, normalize(d), pd[3]);
+            Pcg32 rng = Pcg32::for_pixel_sample(i, 0);
+            V3 v = tr.transmittance(o, normalize(d), pd[3], s.atmosphere, rng);
             out[3 * i] = v.x;
             out[3 * i + 1] = v.y;
             out[3 * i + 2] = v.z;
@@ -2998,3 +3438,57 @@ void oracle_filter_sample(int filter, double width, uint64_t n, const double* u,
 }
 
 }  // extern "C"
+
+uint64_t oracle_medium_sample(const rt_medium_desc* md, const double* o, const double* d, double t_max,
+                              const double* beta, uint64_t pixel, uint64_t sample, uint64_t n, double* pass_sum,
+                              double* scat_sum) {
+    const Medium m = medium_from(*md);
+    Pcg32 rng = Pcg32::for_pixel_sample(pixel, sample);
+    V3 ps{0, 0, 0}, ss{0, 0, 0};
+    uint64_t scatters = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        MediumEvent ev = sample_distance(m, v3(o), v3(d), t_max, v3(beta), rng);
+        if (ev.scatter) {
+            ss = ss + ev.weight;
+            scatters++;
+        } else {
+            ps = ps + ev.weight;
+        }
+    }
+    pass_sum[0] = ps.x, pass_sum[1] = ps.y, pass_sum[2] = ps.z;
+    scat_sum[0] = ss.x, scat_sum[1] = ss.y, scat_sum[2] = ss.z;
+    return scatters;
+}
+
+void oracle_medium_transmittance(const rt_medium_desc* md, const double* o, const double* d, double dist,
+                                 uint64_t pixel, uint64_t sample, uint64_t n, double* mean) {
+    const Medium m = medium_from(*md);
+    Pcg32 rng = Pcg32::for_pixel_sample(pixel, sample);
+    V3 sum{0, 0, 0};
+    for (uint64_t i = 0; i < n; i++) sum = sum + medium_transmittance(m, v3(o), v3(d), dist, rng);
+    mean[0] = sum.x / (double)n, mean[1] = sum.y / (double)n, mean[2] = sum.z / (double)n;
+}
+
+void oracle_medium_density(const rt_medium_desc* md, uint64_t n, const double* p, double* out) {
+    const Medium m = medium_from(*md);
+    for (uint64_t i = 0; i < n; i++) out[i] = m.density_at(v3(p + 3 * i));
+}
+
+void oracle_hg_phase(double g, uint64_t n, const double* c, double* out) {
+    for (uint64_t i = 0; i < n; i++) out[i] = hg_phase(g, c[i]);
+}
+
+void oracle_hg_sample(double g, const double* wo, uint64_t n, const double* u, double* out) {
+    for (uint64_t i = 0; i < n; i++) {
+        double pdf;
+        V3 wi = hg_sample(g, v3(wo), u[2 * i], u[2 * i + 1], &pdf);
+        out[4 * i] = wi.x, out[4 * i + 1] = wi.y, out[4 * i + 2] = wi.z, out[4 * i + 3] = pdf;
+    }
+}
+
+void oracle_sss_medium(const double* color, const double* dmfp, double* sigma_a, double* sigma_s) {
+    Medium m = sss_medium(v3(color), v3(dmfp));
+    sigma_a[0] = m.sigma_a.x, sigma_a[1] = m.sigma_a.y, sigma_a[2] = m.sigma_a.z;
+    sigma_s[0] = m.sigma_s.x, sigma_s[1] = m.sigma_s.y, sigma_s[2] = m.sigma_s.z;
+}
+

@@ -109,6 +109,25 @@ void   oracle_ies_eval(uint32_t n_v, uint32_t n_h, const double* v, const double
                        uint64_t n, const double* dirs, double* cd, double* factor);
 // camera.rs:36-61: one pixel-filter offset per uniform.
 void   oracle_filter_sample(int filter, double width, uint64_t n, const double* u, double* out);
+/* Media (src/scene/medium.rs, src/raytracer/pt/volume.rs), for the
+ * reference's own unit tests. n draws of sample_distance along the ray
+ * (o, d) over [0, t_max] with throughput beta from the PCG32 stream of
+ * (pixel, sample): sums of the pass weights and of the scatter weights
+ * (3 doubles each); returns the number of scatters. */
+uint64_t oracle_medium_sample(const rt_medium_desc* m, const double* o, const double* d, double t_max,
+                              const double* beta, uint64_t pixel, uint64_t sample, uint64_t n, double* pass_sum,
+                              double* scat_sum);
+/* Mean over n estimates of the segment transmittance (3 doubles). */
+void   oracle_medium_transmittance(const rt_medium_desc* m, const double* o, const double* d, double dist,
+                                   uint64_t pixel, uint64_t sample, uint64_t n, double* mean);
+/* Density multiplier at n points (3 doubles each). */
+void   oracle_medium_density(const rt_medium_desc* m, uint64_t n, const double* p, double* out);
+/* Henyey-Greenstein: phase at n cosines, or n sampled directions around
+ * -wo from uniform pairs (u: 2 per draw; out: wi xyz, pdf). */
+void   oracle_hg_phase(double g, uint64_t n, const double* cos_theta, double* out);
+void   oracle_hg_sample(double g, const double* wo, uint64_t n, const double* u, double* out);
+/* sss_medium (volume.rs:259-288): sigma_a, sigma_s (3 doubles each). */
+void   oracle_sss_medium(const double* color, const double* dmfp, double* sigma_a, double* sigma_s);
 
 #ifdef __cplusplus
 }

@@ -49,6 +49,31 @@ class RtMaterialDesc(C.Structure):
         ("emission", c_double3),
         ("area_light", C.c_int32),
         ("id", C.c_uint32),
+        ("subsurface_gain", C.c_double),
+        ("subsurface_color", c_double3),
+        ("subsurface_dmfp", c_double3),
+        ("interior", C.c_int32),
+        ("material_reserved", C.c_uint32),
+    ]
+
+
+DENSITY_NONE, DENSITY_FBM = 0, 1
+
+
+class RtMediumDesc(C.Structure):
+    _fields_ = [
+        ("sigma_a", c_double3),
+        ("sigma_s", c_double3),
+        ("g", C.c_double),
+        ("emission", c_double3),
+        ("max_distance", C.c_double),
+        ("density", C.c_uint32),
+        ("octaves", C.c_uint32),
+        ("frequency", C.c_double),
+        ("gain", C.c_double),
+        ("lacunarity", C.c_double),
+        ("coverage", C.c_double),
+        ("sharpness", C.c_double),
     ]
 
 
@@ -182,6 +207,9 @@ class RtSceneDesc(C.Structure):
         ("quadrics", C.POINTER(RtQuadricDesc)),
         ("n_quadrics", C.c_uint32),
         ("quadric_reserved", C.c_uint32),
+        ("media", C.POINTER(RtMediumDesc)),
+        ("n_media", C.c_uint32),
+        ("atmosphere", C.c_int32),
     ]
 
 
@@ -207,10 +235,10 @@ class RtParams(C.Structure):
 LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK, LIGHT_DOME = range(6)
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
-for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 264), (RtLightDesc, 120),
+for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 328), (RtLightDesc, 120),
                (RtCameraDesc, 144), (RtParams, 72), (RtPatternInput, 32), (RtPatternDesc, 264),
                (RtPatternBinding, 16), (RtTextureDesc, 16), (RtIesDesc, 112), (RtQuadricDesc, 168),
-               (RtSceneDesc, 312)):
+               (RtSceneDesc, 328), (RtMediumDesc, 136)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
 

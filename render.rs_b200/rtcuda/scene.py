@@ -32,7 +32,8 @@ def default_material():
                 clearcoat_roughness=0.1, fuzz_gain=0.0, fuzz_color=(1.0, 1.0, 1.0),
                 glass_gain=0.0, glass_ior=1.5, glass_roughness=0.05,
                 refraction_color=(1.0, 1.0, 1.0), glow=(0.0, 0.0, 0.0), presence=1.0,
-                emission=(0.0, 0.0, 0.0), area_light=-1, id=0)
+                emission=(0.0, 0.0, 0.0), area_light=-1, id=0, subsurface_gain=0.0,
+                subsurface_color=(0.8, 0.6, 0.4), subsurface_dmfp=(0.1, 0.1, 0.1), interior=-1)
 
 
 def matte(color, sigma=0.0, **kw):
@@ -82,6 +83,28 @@ def emitter(radiance, area_light=-1, **kw):
     return m
 
 
+def volume_hull(**kw):
+    """A material that reflects and emits nothing: with an interior medium,
+    its surface only bounds the medium (pt/mod.rs:662-680)."""
+    m = default_material()
+    m.update(diffuse_gain=0.0, specular_ior=1.0)
+    m.update(kw)
+    return m
+
+
+def medium(sigma_a, sigma_s, g=0.0, emission=(0.0, 0.0, 0.0), max_distance=np.inf, fbm=None):
+    """Medium (src/scene/medium.rs:28-43); `fbm` = dict(frequency, octaves,
+    gain, lacunarity, coverage, sharpness) makes it heterogeneous with the
+    reference's defaults for missing keys (scene_builder.rs:336-347)."""
+    d = dict(sigma_a=_rgb(sigma_a), sigma_s=_rgb(sigma_s), g=float(g), emission=_rgb(emission),
+             max_distance=float(max_distance), density=abi.DENSITY_NONE, octaves=0, frequency=0.3,
+             gain=0.55, lacunarity=2.0, coverage=0.5, sharpness=4.0)
+    if fbm is not None:
+        d.update(density=abi.DENSITY_FBM, octaves=5)
+        d.update({k: (int(v) if k == "octaves" else float(v)) for k, v in fbm.items()})
+    return d
+
+
 def rot_y(deg):
     a = np.deg2rad(deg)
     c, s = np.cos(a), np.sin(a)
@@ -121,6 +144,8 @@ class Scene:
         self.textures = []        # (H, W, 3) f32 linear RGB base images
         self.ies = {}             # point light index -> (v_angles, h_angles, candela[h][v], world_to_local 3x3)
         self.quadrics = []        # (type, params (<= 8), object_to_world 3x4, material)
+        self.media = []           # medium dicts (see medium())
+        self.atmosphere = -1      # index into media of the global medium, -1 for none
         # Reference default camera: origin, looking down +z (camera.rs:97-103).
         self.eye = np.zeros(3)
         self.forward = np.array([0.0, 0.0, 1.0])
@@ -263,6 +288,15 @@ class Scene:
         self.quadrics.append((int(kind), pr + [0.0] * (8 - len(pr)), xf.copy(), int(material)))
         self._desc = None
         return len(self.quadrics) - 1
+
+    def add_medium(self, med, atmosphere=False):
+        """A participating medium (see medium()); materials reference it by
+        their `interior` index, or it becomes the scene's atmosphere."""
+        self.media.append(dict(med))
+        if atmosphere:
+            self.atmosphere = len(self.media) - 1
+        self._desc = None
+        return len(self.media) - 1
 
     def add_point_light(self, position, intensity, color=(1, 1, 1), ies=None, world_to_local=None):
         """Light::point; `ies` = (vertical angles, horizontal angles,
@@ -457,5 +491,13 @@ class Scene:
         if self.quadrics:
             d.quadrics = quad_arr
             d.n_quadrics = len(self.quadrics)
-        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr, tex_arr, ies_arr, quad_arr)
+        med_arr = (abi.RtMediumDesc * max(1, len(self.media)))()
+        for k, m in enumerate(self.media):
+            for key, val in m.items():
+                setattr(med_arr[k], key, abi.c_double3(*val) if isinstance(val, tuple) else val)
+        if self.media:
+            d.media = med_arr
+            d.n_media = len(self.media)
+        d.atmosphere = self.atmosphere
+        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr, tex_arr, ies_arr, quad_arr, med_arr)
         return d
