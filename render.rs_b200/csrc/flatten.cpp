@@ -616,11 +616,27 @@ DevMaterial fold_material(const rt_material_desc& m) {
         d.refr[k] = (float)m.refraction_color[k];
         d.emission[k] = (float)(m.emission[k] + m.glow[k]);
         alb[k] = m.diffuse_color[k] * m.diffuse_gain + f0[k] * (has_spec ? 1.0 : 0.0) +
-                 m.refraction_color[k] * m.glass_gain;
+                 m.subsurface_color[k] * m.subsurface_gain + m.refraction_color[k] * m.glass_gain;
         d.albedo[k] = (float)std::fmin(alb[k], 1.0);
     }
     d.area_light = m.area_light;
     d.id = m.id;
+    // Interior medium (validated by the caller) and volume hulls
+    // (pt/mod.rs:662-667): no lobes and no emission; a hull is never a
+    // cutout, the reference testing it before presence.
+    d.interior = m.interior >= 0 ? (uint32_t)m.interior : 0xFFFFFFFFu;
+    const bool emits = std::max({m.emission[0] + m.glow[0], m.emission[1] + m.glow[1], m.emission[2] + m.glow[2]}) > 0.0;
+    d.hull = (m.interior >= 0 && !lobes && !emits) ? 1.0f : 0.0f;
+    if (d.hull != 0.0f) d.presence = 1.0f;
+    // Subsurface walk: probability and the Burley-fit medium (volume.rs:259-288).
+    d.sss_gain = (float)std::min(std::max(m.subsurface_gain, 0.0), 1.0);
+    for (int k = 0; k < 3; k++) {
+        const double a = std::min(std::max(m.subsurface_color[k], 0.0), 1.0);
+        const double st = (1.85 - a + 7.0 * std::pow(std::fabs(a - 0.8), 3)) / std::max(m.subsurface_dmfp[k], 1e-5);
+        const double alpha = 1.0 - std::exp(-a * (11.43 - 15.38 * a + 13.91 * a * a));
+        d.sss_st[k] = (float)st;
+        d.sss_ss[k] = (float)(alpha * st);
+    }
     if (!lobes) d.mclass = MAT_EMITTER;
     else if (wd > 0 && ws == 0 && wc == 0 && wf == 0 && wg == 0) d.mclass = MAT_DIFFUSE;
     else if (ws > 0 && wd == 0 && wc == 0 && wf == 0 && wg == 0) d.mclass = MAT_CONDUCTOR;
@@ -893,7 +909,9 @@ bool flatten_patterns(const rt_scene_desc* d, HostScene& H, std::string* err) {
             p.refraction[c] = (float)md.refraction_color[c];
             p.glow[c] = (float)md.glow[c];
             p.emission[c] = (float)md.emission[c];
+            p.sss_albedo[c] = (float)(md.subsurface_color[c] * md.subsurface_gain);
         }
+        p.pad_ = 0.0f;
         H.pbr.push_back(p);
         // The lobe set varies per hit: shade through the general class.
         H.materials[m].mclass = MAT_MIXED;
@@ -1354,15 +1372,72 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         *err = "materials pointer is NULL";
         return false;
     }
+    // ---- participating media (medium.rs:28-66) ------------------------------
+    // Indices are read only when the scene has media: an interior or
+    // atmosphere of -1 means none, anything else must name a medium.
+    if (d->n_media && !d->media) {
+        *err = "media pointer is NULL";
+        return false;
+    }
+    if (d->n_media > RT_MAX_MEDIA) {
+        *err = "at most " + std::to_string(RT_MAX_MEDIA) + " media";
+        return false;
+    }
+    H.scalars.n_media = d->n_media;
+    H.scalars.atmosphere = 0xFFFFFFFFu;
+    if (d->n_media) {
+        if (d->atmosphere >= (int32_t)d->n_media || d->atmosphere < -1) {
+            *err = "the atmosphere names a missing medium";
+            return false;
+        }
+        if (d->atmosphere >= 0) H.scalars.atmosphere = (uint32_t)d->atmosphere;
+    }
+    for (uint32_t k = 0; k < d->n_media; k++) {
+        const rt_medium_desc& md = d->media[k];
+        DevMedium m{};
+        double maj = 0.0;
+        for (int c = 0; c < 3; c++) {
+            if (!(md.sigma_a[c] >= 0.0) || !(md.sigma_s[c] >= 0.0) || !std::isfinite(md.sigma_a[c] + md.sigma_s[c])) {
+                *err = "medium " + std::to_string(k) + " has a negative or non-finite coefficient";
+                return false;
+            }
+            m.sigma_a[c] = (float)md.sigma_a[c];
+            m.sigma_s[c] = (float)md.sigma_s[c];
+            m.emission[c] = (float)md.emission[c];
+            maj = std::max(maj, md.sigma_a[c] + md.sigma_s[c]);
+        }
+        if (md.density > RT_DENSITY_FBM || !(md.max_distance >= 0.0)) {
+            *err = "medium " + std::to_string(k) + " has an unknown density or a negative extent";
+            return false;
+        }
+        m.g = (float)md.g;
+        m.max_distance = (float)std::min(md.max_distance, 3.0e38);
+        m.majorant = (float)maj;
+        m.frequency = (float)md.frequency;
+        m.gain = (float)md.gain;
+        m.lacunarity = (float)md.lacunarity;
+        m.coverage = (float)md.coverage;
+        m.sharpness = (float)md.sharpness;
+        m.octaves = md.octaves;
+        m.density = md.density;
+        H.media.push_back(m);
+    }
     H.scalars.any_presence = 0;
+    H.scalars.any_sss = 0;
     for (uint32_t m = 0; m < d->n_materials; m++) {
-        const rt_material_desc& md = d->materials[m];
+        rt_material_desc md = d->materials[m];
         if (md.area_light >= (int32_t)d->n_lights) {
             *err = "material " + std::to_string(m) + " names a missing area light";
             return false;
         }
+        if (!d->n_media) md.interior = -1;
+        if (md.interior >= (int32_t)d->n_media || md.interior < -1) {
+            *err = "material " + std::to_string(m) + " names a missing medium";
+            return false;
+        }
         H.materials.push_back(fold_material(md));
-        if (md.presence < 1.0) H.scalars.any_presence = 1;
+        if (H.materials.back().presence < 1.0f) H.scalars.any_presence = 1;
+        if (H.materials.back().sss_gain > 0.0f) H.scalars.any_sss = 1;
     }
     if (!flatten_patterns(d, H, err)) return false;
     if (!flatten_quadrics(d, H, err)) return false;

@@ -308,7 +308,8 @@ __device__ __forceinline__ void apply_field(DevPbr& q, uint32_t field, float3 v)
 
 // The host's fold_material in f32: lobe weights (pbr.rs:188-201), F0
 // (pbr.rs:86-96), under-layer scale (bxdf.rs:137-143), Oren-Nayar A/B, GGX
-// alphas, the first-hit albedo. Keeps d's area light, id and class.
+// alphas, the first-hit albedo. Keeps d's area light, id, class, interior
+// medium and subsurface walk.
 __device__ __forceinline__ void fold_pbr(const DevPbr& q, DevMaterial& d) {
     const float3 face = f3(q.spec_face[0], q.spec_face[1], q.spec_face[2]);
     float3 f0 = f3(0.0f, 0.0f, 0.0f);
@@ -353,7 +354,7 @@ __device__ __forceinline__ void fold_pbr(const DevPbr& q, DevMaterial& d) {
         d.kfuzz[k] = q.fuzz_color[k] * q.fuzz_gain * (1.0f / RT_PI);
         d.refr[k] = q.refraction[k];
         d.emission[k] = q.emission[k] + q.glow[k];
-        d.albedo[k] = fminf(q.diffuse_color[k] * q.diffuse_gain + (has_spec ? f0a[k] : 0.0f) +
+        d.albedo[k] = fminf(q.diffuse_color[k] * q.diffuse_gain + (has_spec ? f0a[k] : 0.0f) + q.sss_albedo[k] +
                                 q.refraction[k] * q.glass_gain,
                             1.0f);
     }

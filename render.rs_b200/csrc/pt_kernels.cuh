@@ -22,6 +22,7 @@
 #include "guide.cuh"
 #include "pattern.cuh"
 #include "quadric.cuh"
+#include "media.cuh"
 
 namespace rt {
 
@@ -35,8 +36,17 @@ enum : uint32_t {
     CNT_CLASS = 3,                  // N_QUEUES words
     CNT_FETCH_EXT = CNT_CLASS + N_QUEUES,
     CNT_FETCH_SH = CNT_FETCH_EXT + 1,
+    CNT_SSS = CNT_FETCH_SH + 1,     // subsurface walks queued this wave
     CNT_WORDS = 16
 };
+
+// Shadow-queue entries of scenes with media: the slot, bit 30 set when its
+// surface / collision / walk-exit shadow ray (sh_*) is pending, bit 31 when
+// its equiangular one (sh2_*) is; one entry per slot, so one thread adds
+// both contributions in a fixed order.
+#define SH_PRIMARY (1u << 30)
+#define SH_EQUI (1u << 31)
+#define SH_SLOT_MASK (SH_PRIMARY - 1u)
 
 struct Paths {
     float4* ray_o;    // origin xyz, w = roulette gain (see k_shade)
@@ -53,6 +63,11 @@ struct Paths {
     float4* aux_n;    // normal xyz, id bits
     float4* aux_d;    // diffuse share xyz, hit flag
     float2* cone;     // ray cone (width, spread) when the scene has patterns, else null
+    uint2* med;       // nested-media stack (media.cuh) when the scene has media, else null
+    float4* sh2_o;    // equiangular shadow ray toward a point light (scenes with media):
+    float4* sh2_d;    //   origin xyz + medium bits, direction xyz + distance,
+    float4* sh2_c;    //   contribution xyz + diffuse-AOV flag
+    uint32_t* q_sss;  // subsurface walks queued this wave (scenes with a walk), else null
     uint32_t* q_ext[2];
     uint32_t* q_cls;  // N_QUEUES x P
     uint32_t* q_sh;
@@ -104,6 +119,7 @@ struct PtConsts {
 #define FL_SPEC_MASK (3u << FL_SPEC_SHIFT)
 #define FL_AUX_SET (1u << 8)
 #define FL_INACTIVE (1u << 9)   // adaptive sampling: the pixel had converged, no path was spawned
+#define FL_SH2 (1u << 10)       // an equiangular shadow ray waits for the subsurface walk's queue entry
 #define FL_DEPTH_SHIFT 16
 
 #define RT_RAY_OFFSET 1e-4f
@@ -317,6 +333,7 @@ __global__ void k_raygen(DevScene S, Paths P, PtConsts C) {
     P.beta[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     P.L[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     P.prev[i] = make_float4(o.x, o.y, o.z, __uint_as_float(FL_FROM_CAMERA | FL_SPEC_NONE));
+    if (P.med) P.med[i] = make_uint2(0u, 0u);  // camera rays start in the atmosphere
     // Ray cone: width 0, spread one pixel's angle (kernel_pt.metal:2283-2284).
     if (P.cone) P.cone[i] = make_float2(0.0f, 2.0f * S.half_h / (float)S.height);
     P.rng[i] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
@@ -714,24 +731,14 @@ struct NeeOut {
 };
 
 // NEE for one light (mod.rs:1032-1209): returns true with a shadow ray and
-// its unoccluded contribution (already divided by the pick pmf).
-__device__ __forceinline__ bool nee_light(const DevScene& S, const DevLight& L, float3 p, float3 n, const Frame& fr,
-                                          float3 wo_l, float eta, const DevMaterial& m, float pick, Pcg& rng,
-                                          NeeOut& out, const MixtureRef* mix = nullptr, float alpha = 0.0f) {
+// its unoccluded contribution (already divided by the pick pmf). eval(wi,
+// pdf) gives the scattering value toward wi with any cosine applied and the
+// pdf of the direction-sampling strategy it is MIS-weighted against; n only
+// offsets the shadow ray's origin (zero at a medium collision).
+template <class Eval>
+__device__ __forceinline__ bool nee_light_eval(const DevScene& S, const DevLight& L, float3 p, float3 n, Eval eval,
+                                               float pick, Pcg& rng, NeeOut& out) {
     float3 Le = f3(L.radiance[0], L.radiance[1], L.radiance[2]);
-    // BSDF value with cosine, and the pdf of the direction-sampling strategy
-    // it is MIS-weighted against: the BSDF pdf, or under guiding the one-sample
-    // mixture alpha * q + (1 - alpha) * p_bsdf.
-    auto eval = [&](float3 wi, float& pdf) -> float3 {
-        float3 wl = fr.to_local(wi);
-        if (wl.z <= 0.0f) {
-            pdf = 0.0f;
-            return f3(0, 0, 0);
-        }
-        float3 f = bsdf_eval(m, wo_l, wl, eta, pdf) * wl.z;
-        if (mix) pdf = alpha * mixture_pdf(*mix, wi) + (1.0f - alpha) * pdf;
-        return f;
-    };
     auto shadow_to = [&](float3 target) {
         float3 dir = target - p;
         float dist = length(dir);
@@ -851,6 +858,25 @@ __device__ __forceinline__ bool nee_light(const DevScene& S, const DevLight& L, 
     return false;
 }
 
+// NEE from a surface: the BSDF value with cosine, MIS-weighted against the
+// BSDF pdf, or under guiding the one-sample mixture alpha * q + (1 - alpha)
+// * p_bsdf.
+__device__ __forceinline__ bool nee_light(const DevScene& S, const DevLight& L, float3 p, float3 n, const Frame& fr,
+                                          float3 wo_l, float eta, const DevMaterial& m, float pick, Pcg& rng,
+                                          NeeOut& out, const MixtureRef* mix = nullptr, float alpha = 0.0f) {
+    auto eval = [&](float3 wi, float& pdf) -> float3 {
+        float3 wl = fr.to_local(wi);
+        if (wl.z <= 0.0f) {
+            pdf = 0.0f;
+            return f3(0, 0, 0);
+        }
+        float3 f = bsdf_eval(m, wo_l, wl, eta, pdf) * wl.z;
+        if (mix) pdf = alpha * mixture_pdf(*mix, wi) + (1.0f - alpha) * pdf;
+        return f;
+    };
+    return nee_light_eval(S, L, p, n, eval, pick, rng, out);
+}
+
 // mod.rs:1000-1023 solid-angle pdf of an area light toward a hit.
 __device__ __forceinline__ float light_pdf_sa(const DevLight& L, float3 origin, float3 hp) {
     if (L.type == 2 || L.type == 4) {
@@ -876,7 +902,9 @@ __device__ __forceinline__ float light_pdf_sa(const DevLight& L, float3 origin, 
 // PAT: the scene has patterns (ray cones tracked, patterned materials
 // resolved per hit). The plain instance keeps its material reads on the
 // global material table and the register count of a kernel without them.
-template <bool PAT>
+// MED: the scene has participating media (medium segments, hull crossings,
+// nested-media stacks, equiangular shadow rays).
+template <bool PAT, bool MED = false>
 __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, Paths P, PtConsts C, uint32_t qout) {
     uint32_t counts[N_QUEUES];
     uint32_t total = 0;
@@ -907,7 +935,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
             }
             slot = P.q_cls[(size_t)c * P.P + off];
         }
-        bool extend = false, shadow = false;
+        bool extend = false, shadow = false, shadow2 = false, walk = false;
         if (active) {
             float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot];
             uint4 hr = P.hit[slot];
@@ -944,7 +972,131 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                     r[19] = __uint_as_float(P.tr_tag);
                 }
             };
-            if (hr.y == 0xFFFFFFFFu) {
+            uint2 mstk = make_uint2(0u, 0u);
+            uint32_t cur_med = RT_MEDIUM_NONE;
+            bool consumed = false;  // the medium segment ended this step (collision or absorbed path)
+            if (MED) {
+                mstk = P.med[slot];
+                cur_med = mstack_top(mstk, S.atmosphere);
+            }
+            if (MED && cur_med != RT_MEDIUM_NONE) {
+                // Medium interaction along this segment, before any surface
+                // (pt/mod.rs:490-640). One light pick per segment serves both
+                // the equiangular and the collision NEE, so their MIS weights
+                // cancel its pmf.
+                const DevMedium& med = S.media[cur_med];
+                const float3 dn = normalize_ref(d);
+                const float t_limit = hr.y != 0xFFFFFFFFu ? __uint_as_float(hr.x) * length(d) : 1e8f;
+                const float t_seg = fminf(t_limit, med.max_distance);
+                uint32_t pli = 0;
+                float ppmf = 0.0f;
+                const bool seg_pick = light_sample(S, o + dn * fminf(t_seg * 0.5f, 50.0f), rng.next_f(), pli, ppmf);
+                const bool point = seg_pick && S.lights[pli].type == 0;
+                const float3 lp = point ? f3(S.lights[pli].p[0], S.lights[pli].p[1], S.lights[pli].p[2]) : f3(0, 0, 0);
+                if (point && t_seg > 1e-6f) {
+                    // Equiangular single-scatter NEE toward the point light
+                    // (Kulla-Fajardo); its shadow ray goes out as sh2.
+                    const DevLight& Lp = S.lights[pli];
+                    float pdf_eq;
+                    const float t_eq = equiangular_sample(o, dn, t_seg, lp, rng.next_f(), pdf_eq);
+                    if (pdf_eq > 1e-12f) {
+                        const float3 pe = o + dn * t_eq;
+                        const float rho = med_density(med, pe);
+                        if (rho > 0.0f) {
+                            const float3 tr = med_transmittance(med, o, dn, t_eq, rng);
+                            const float3 to_l = lp - pe;
+                            const float dist2 = fmaxf(dot(to_l, to_l), 1e-12f);
+                            const float3 wi = normalize_ref(to_l);
+                            const float ph = hg_phase(med.g, dot(dn, wi));
+                            const float prof = Lp.ies == 0xFFFFFFFFu ? 1.0f : ies_factor(S, S.ies[Lp.ies], -wi);
+                            const float pdf_d = distance_pdf_approx(med, t_eq, t_seg);
+                            const float w_eq = pdf_eq / (pdf_eq + pdf_d);
+                            const float3 c = beta * (med_sigma_s(med) * rho) * tr *
+                                             f3(Lp.radiance[0], Lp.radiance[1], Lp.radiance[2]) *
+                                             (prof * ph * w_eq / (dist2 * pdf_eq * ppmf));
+                            if (maxc(c) > 0.0f) {
+                                P.sh2_o[slot] = make_float4(pe.x, pe.y, pe.z, __uint_as_float(cur_med));
+                                P.sh2_d[slot] = make_float4(wi.x, wi.y, wi.z, sqrtf(dist2) - 1e-3f);
+                                P.sh2_c[slot] = make_float4(c.x, c.y, c.z, spec_true ? 0.0f : 1.0f);
+                                shadow2 = true;
+                            }
+                        }
+                    }
+                }
+                const MedEvent ev = med_sample(med, o, dn, t_limit, beta, rng);
+                beta = beta * ev.w;
+                if (ev.scatter) {
+                    consumed = true;
+                    const float3 pm = o + dn * ev.t;
+                    if (C.aovs && !(flags & FL_AUX_SET)) {
+                        flags |= FL_AUX_SET;
+                        const float3 stt = med_sigma_t(med);
+                        P.aux_a[slot] = make_float4(med.sigma_s[0] / fmaxf(stt.x, 1e-9f), med.sigma_s[1] / fmaxf(stt.y, 1e-9f),
+                                                    med.sigma_s[2] / fmaxf(stt.z, 1e-9f), travel + ev.t);
+                        P.aux_n[slot] = make_float4(-dn.x, -dn.y, -dn.z, __uint_as_float(0u));
+                        auxd.w = 1.0f;
+                    }
+                    if ((flags & FL_SPEC_MASK) == FL_SPEC_NONE) flags &= ~FL_SPEC_MASK;
+                    const float3 em = f3(med.emission[0], med.emission[1], med.emission[2]);
+                    if (maxc(em) > 0.0f) emit(beta * em);
+                    const float3 wo = -dn;
+                    const float g = med.g;
+                    if (seg_pick) {
+                        // Collision NEE; point lights carry the MIS weight that
+                        // pairs it with the equiangular strategy.
+                        float w_dist = 1.0f;
+                        if (point) {
+                            const float pdf_d = distance_pdf_approx(med, ev.t, t_seg);
+                            w_dist = pdf_d / (pdf_d + equiangular_pdf(o, dn, t_seg, lp, ev.t));
+                        }
+                        auto eval = [&](float3 wi, float& pdf) -> float3 {
+                            const float ph = hg_phase(g, -dot(wo, wi));
+                            pdf = ph;
+                            return f3(ph, ph, ph);
+                        };
+                        NeeOut ne;
+                        if (nee_light_eval(S, S.lights[pli], pm, f3(0.0f, 0.0f, 0.0f), eval, ppmf, rng, ne)) {
+                            const float3 c = beta * ne.c * w_dist;
+                            if (maxc(c) > 0.0f) {
+                                P.sh_o[slot] = make_float4(ne.o.x, ne.o.y, ne.o.z, __uint_as_float(cur_med));
+                                P.sh_d[slot] = make_float4(ne.d.x, ne.d.y, ne.d.z, ne.tmax);
+                                P.sh_c[slot] = make_float4(c.x, c.y, c.z, spec_true ? 0.0f : 1.0f);
+                                shadow = true;
+                            }
+                        }
+                    }
+                    // Continue along a phase-function sample (phase / pdf = 1).
+                    const float u1 = rng.next_f(), u2 = rng.next_f();
+                    float pdf;
+                    const float3 wi = hg_sample(g, wo, u1, u2, pdf);
+                    beta4.w = pdf;
+                    prev4 = make_float4(pm.x, pm.y, pm.z, 0.0f);
+                    flags &= ~FL_FROM_CAMERA;
+                    if (PAT) {
+                        float2 cn = P.cone[slot];
+                        cn.y += 0.4f;
+                        P.cone[slot] = cn;
+                    }
+                    const uint32_t depth = (flags >> FL_DEPTH_SHIFT) + 1;
+                    flags = (flags & 0xFFFFu) | (depth << FL_DEPTH_SHIFT);
+                    bool alive = true;
+                    if (depth >= C.rr_start) {
+                        const float q = fminf(maxc(beta) * o4.w, 0.95f);
+                        if (q <= 0.0f || rng.next_f() > q) alive = false;
+                        else beta = beta / q;
+                    }
+                    if (alive && depth < C.max_depth) {
+                        P.ray_o[slot] = make_float4(pm.x, pm.y, pm.z, o4.w);
+                        P.ray_d[slot] = make_float4(wi.x, wi.y, wi.z, INFINITY);
+                        extend = true;
+                    }
+                } else if (maxc(beta) <= 0.0f) {
+                    consumed = true;  // absorbed on the way
+                }
+            }
+            if (consumed) {
+                // handled above
+            } else if (hr.y == 0xFFFFFFFFu) {
                 tr_close();
                 if (S.dome != 0xFFFFFFFFu) {
                     // Miss: the dome light, MIS-weighted against its NEE
@@ -968,6 +1120,10 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                 float3 nw = hg.nw;
                 const bool front = hg.front;
                 const float eucl = hg.eucl;
+                // Volume hull: the crossing only toggles the medium
+                // (pt/mod.rs:662-680): no AOV, no cone growth, no bounce.
+                const bool hull_skip = MED && S.materials[hg.mat].hull != 0.0f &&
+                                       ((flags & FL_SKIP_MASK) >> FL_SKIP_SHIFT) < RT_MAX_PRESENCE_SKIPS;
                 travel += eucl;
                 // Ray cone at this hit and the material's pattern outputs
                 // (pt/mod.rs:687-689; footprint = cone width x st density).
@@ -976,7 +1132,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                 const DevMaterial* mptr = S.materials + hg.mat;
                 if (PAT) {
                     cone = P.cone[slot];
-                    cone.x += eucl * cone.y;
+                    if (!hull_skip) cone.x += eucl * cone.y;
                     const DevMatPat mp = S.mat_pat[hg.mat];
                     if (mp.bind_n) {
                         const HitSt hs = hit_st(S, hr, p);
@@ -986,7 +1142,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                     }
                 }
                 const DevMaterial& m = *mptr;
-                if (C.aovs && !(flags & FL_AUX_SET)) {
+                if (C.aovs && !(flags & FL_AUX_SET) && !hull_skip) {
                     flags |= FL_AUX_SET;
                     float3 an = dot(nw, wo) >= 0.0f ? nw : -nw;
                     P.aux_a[slot] = make_float4(m.albedo[0], m.albedo[1], m.albedo[2], travel);
@@ -995,7 +1151,17 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                 }
                 uint32_t skips = (flags & FL_SKIP_MASK) >> FL_SKIP_SHIFT;
                 bool done = false;
-                if (!C.pres_in_trav && m.presence < 1.0f && rng.next_f() >= m.presence &&
+                if (hull_skip) {
+                    flags = (flags & ~FL_SKIP_MASK) | ((skips + 1) << FL_SKIP_SHIFT);
+                    if (front) mstack_push(mstk, S.materials[hg.mat].interior);
+                    else mstack_pop(mstk);
+                    const float3 no = p + normalize_ref(d) * RT_RAY_OFFSET;
+                    P.ray_o[slot] = make_float4(no.x, no.y, no.z, o4.w);
+                    P.ray_d[slot] = make_float4(d.x, d.y, d.z, INFINITY);
+                    extend = true;
+                    done = true;
+                }
+                if (!done && !C.pres_in_trav && m.presence < 1.0f && rng.next_f() >= m.presence &&
                     skips < RT_MAX_PRESENCE_SKIPS) {
                     // Presence cutout: pass straight through, no bounce.
                     flags = (flags & ~FL_SKIP_MASK) | ((skips + 1) << FL_SKIP_SHIFT);
@@ -1021,116 +1187,142 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                         }
                         emit(beta * em * wgt);
                     }
-                    Frame fr(n);
-                    float3 wo_l = fr.to_local(wo);
-                    // Learned proposal at this vertex (guided mode only).
-                    MixtureRef mix{nullptr};
-                    bool guided = false;
-                    if (C.guided) {
-                        uint32_t gi = P.g_idx[slot];
-                        if (gi != 0xFFFFFFFFu) {
-                            mix.p = reinterpret_cast<const float4*>(P.g_raw + (size_t)gi * G_OUT);
-                            guided = true;
-                        }
+                    // Subsurface scattering (pt/mod.rs:794-892): with probability
+                    // sss_gain the path enters a random walk inside the object
+                    // (k_sss), starting from a cosine direction around -n.
+                    if (m.sss_gain > 0.0f && rng.next_f() < m.sss_gain) {
+                        if ((flags & FL_SPEC_MASK) == FL_SPEC_NONE) flags &= ~FL_SPEC_MASK;
+                        const Frame ef(-n);
+                        const float e1 = rng.next_f(), e2 = rng.next_f();
+                        const float er = sqrtf(e1);
+                        float es, ec;
+                        sincosf(2.0f * RT_PI * e2, &es, &ec);
+                        const float3 wd = normalize_ref(ef.to_world(f3(er * ec, er * es, sqrtf(fmaxf(1.0f - e1, 0.0f)))));
+                        const float3 wp = p - n * RT_RAY_OFFSET;
+                        P.ray_o[slot] = make_float4(wp.x, wp.y, wp.z, o4.w);
+                        P.ray_d[slot] = make_float4(wd.x, wd.y, wd.z, INFINITY);
+                        P.hit[slot] = make_uint4(hg.mat, 0u, 0u, 0u);
+                        walk = true;
                     }
-                    if (S.n_lights > 0 && m.has_lobes != 0.0f) {
-                        uint32_t li;
-                        float pmf;
-                        if (light_sample(S, p, rng.next_f(), li, pmf)) {
-                            NeeOut ne;
-                            if (nee_light(S, S.lights[li], p, n, fr, wo_l, eta, m, pmf, rng, ne,
-                                          guided ? &mix : nullptr, C.alpha)) {
-                                float3 c = beta * ne.c;
-                                if (maxc(c) > 0.0f) {
-                                    P.sh_o[slot] = make_float4(ne.o.x, ne.o.y, ne.o.z, 0.0f);
-                                    P.sh_d[slot] = make_float4(ne.d.x, ne.d.y, ne.d.z, ne.tmax);
-                                    P.sh_c[slot] = make_float4(c.x, c.y, c.z, spec_true ? 0.0f : 1.0f);
-                                    shadow = true;
+                    if (!walk) {
+                        Frame fr(n);
+                        float3 wo_l = fr.to_local(wo);
+                        // Learned proposal at this vertex (guided mode only).
+                        MixtureRef mix{nullptr};
+                        bool guided = false;
+                        if (C.guided) {
+                            uint32_t gi = P.g_idx[slot];
+                            if (gi != 0xFFFFFFFFu) {
+                                mix.p = reinterpret_cast<const float4*>(P.g_raw + (size_t)gi * G_OUT);
+                                guided = true;
+                            }
+                        }
+                        if (S.n_lights > 0 && m.has_lobes != 0.0f) {
+                            uint32_t li;
+                            float pmf;
+                            if (light_sample(S, p, rng.next_f(), li, pmf)) {
+                                NeeOut ne;
+                                if (nee_light(S, S.lights[li], p, n, fr, wo_l, eta, m, pmf, rng, ne,
+                                              guided ? &mix : nullptr, C.alpha)) {
+                                    float3 c = beta * ne.c;
+                                    if (maxc(c) > 0.0f) {
+                                        P.sh_o[slot] = make_float4(ne.o.x, ne.o.y, ne.o.z, MED ? __uint_as_float(cur_med) : 0.0f);
+                                        P.sh_d[slot] = make_float4(ne.d.x, ne.d.y, ne.d.z, ne.tmax);
+                                        P.sh_c[slot] = make_float4(c.x, c.y, c.z, spec_true ? 0.0f : 1.0f);
+                                        shadow = true;
+                                    }
                                 }
                             }
                         }
-                    }
-                    BsdfSample bs;
-                    bool sampled;
-                    float pdf_path = 0.0f;
-                    if (guided) {
-                        // One-sample MIS: the guide with probability alpha, else the
-                        // BSDF; the path pdf is the mixture of both full pdfs.
-                        if (rng.next_f() < C.alpha) {
-                            float u0 = rng.next_f(), u1 = rng.next_f(), u2 = rng.next_f();
-                            bs.wi = fr.to_local(mixture_sample(mix, u0, u1, u2));
-                            bs.f = bsdf_eval(m, wo_l, bs.wi, eta, bs.pdf);
-                            bs.transmitted = bs.wi.z < 0.0f;
-                            bs.specular = false;
-                            sampled = maxc(bs.f) > 0.0f;
+                        BsdfSample bs;
+                        bool sampled;
+                        float pdf_path = 0.0f;
+                        if (guided) {
+                            // One-sample MIS: the guide with probability alpha, else the
+                            // BSDF; the path pdf is the mixture of both full pdfs.
+                            if (rng.next_f() < C.alpha) {
+                                float u0 = rng.next_f(), u1 = rng.next_f(), u2 = rng.next_f();
+                                bs.wi = fr.to_local(mixture_sample(mix, u0, u1, u2));
+                                bs.f = bsdf_eval(m, wo_l, bs.wi, eta, bs.pdf);
+                                bs.transmitted = bs.wi.z < 0.0f;
+                                bs.specular = false;
+                                sampled = maxc(bs.f) > 0.0f;
+                            } else {
+                                sampled = bsdf_sample(m, wo_l, eta, rng, bs);
+                            }
+                            if (sampled) {
+                                pdf_path = C.alpha * mixture_pdf(mix, fr.to_world(bs.wi)) + (1.0f - C.alpha) * bs.pdf;
+                                sampled = pdf_path > 0.0f;
+                            }
                         } else {
                             sampled = bsdf_sample(m, wo_l, eta, rng, bs);
+                            pdf_path = bs.pdf;
                         }
+                        // Roulette gain: Russian roulette acts on the throughput the
+                        // path would carry had every bounce been BSDF-sampled,
+                        // beta * prod(pdf_path / p_bsdf). Guiding concentrates paths
+                        // on directions of high incident radiance and gives them a
+                        // low beta for it; roulette on beta alone would kill those
+                        // paths at the next bounce and cancel the gain. Without
+                        // guiding the gain stays exactly 1 (the reference's rule,
+                        // pt/mod.rs:980-987).
+                        float rr_gain = o4.w;
+                        if (guided && sampled)
+                            rr_gain = fminf(fmaxf(rr_gain * (pdf_path / fmaxf(bs.pdf, 1e-20f)), 1e-20f), 1e20f);
                         if (sampled) {
-                            pdf_path = C.alpha * mixture_pdf(mix, fr.to_world(bs.wi)) + (1.0f - C.alpha) * bs.pdf;
-                            sampled = pdf_path > 0.0f;
-                        }
-                    } else {
-                        sampled = bsdf_sample(m, wo_l, eta, rng, bs);
-                        pdf_path = bs.pdf;
-                    }
-                    // Roulette gain: Russian roulette acts on the throughput the
-                    // path would carry had every bounce been BSDF-sampled,
-                    // beta * prod(pdf_path / p_bsdf). Guiding concentrates paths
-                    // on directions of high incident radiance and gives them a
-                    // low beta for it; roulette on beta alone would kill those
-                    // paths at the next bounce and cancel the gain. Without
-                    // guiding the gain stays exactly 1 (the reference's rule,
-                    // pt/mod.rs:980-987).
-                    float rr_gain = o4.w;
-                    if (guided && sampled)
-                        rr_gain = fminf(fmaxf(rr_gain * (pdf_path / fmaxf(bs.pdf, 1e-20f)), 1e-20f), 1e20f);
-                    if (sampled) {
-                        float3 wi = fr.to_world(bs.wi);
-                        const float3 beta_in = beta;
-                        beta = beta * bs.f * (fabsf(bs.wi.z) / pdf_path);
-                        if (C.train) {
-                            // Training vertex: closed with the radiance at the next vertex.
-                            uint32_t d0 = flags >> FL_DEPTH_SHIFT;
-                            if (d0 < C.max_depth) {
-                                float* r = P.tr_rec + ((size_t)slot * C.max_depth + d0) * TR_FLOATS;
-                                float3 wn = normalize_ref(wi);
-                                r[0] = p.x; r[1] = p.y; r[2] = p.z;
-                                r[3] = n.x; r[4] = n.y; r[5] = n.z;
-                                r[6] = wo.x; r[7] = wo.y; r[8] = wo.z;
-                                r[9] = wn.x; r[10] = wn.y; r[11] = wn.z;
-                                r[12] = beta_in.x; r[13] = beta_in.y; r[14] = beta_in.z;
-                                r[18] = __uint_as_float(P.tr_tag);
-                                r[19] = 0.0f;
+                            float3 wi = fr.to_world(bs.wi);
+                            const float3 beta_in = beta;
+                            if (MED && bs.transmitted && m.interior != RT_MEDIUM_NONE) {  // pt/mod.rs:969-975
+                                if (front) mstack_push(mstk, m.interior);
+                                else mstack_pop(mstk);
+                            }
+                            beta = beta * bs.f * (fabsf(bs.wi.z) / pdf_path);
+                            if (C.train) {
+                                // Training vertex: closed with the radiance at the next vertex.
+                                uint32_t d0 = flags >> FL_DEPTH_SHIFT;
+                                if (d0 < C.max_depth) {
+                                    float* r = P.tr_rec + ((size_t)slot * C.max_depth + d0) * TR_FLOATS;
+                                    float3 wn = normalize_ref(wi);
+                                    r[0] = p.x; r[1] = p.y; r[2] = p.z;
+                                    r[3] = n.x; r[4] = n.y; r[5] = n.z;
+                                    r[6] = wo.x; r[7] = wo.y; r[8] = wo.z;
+                                    r[9] = wn.x; r[10] = wn.y; r[11] = wn.z;
+                                    r[12] = beta_in.x; r[13] = beta_in.y; r[14] = beta_in.z;
+                                    r[18] = __uint_as_float(P.tr_tag);
+                                    r[19] = 0.0f;
+                                }
+                            }
+                            if ((flags & FL_SPEC_MASK) == FL_SPEC_NONE)
+                                flags = (flags & ~FL_SPEC_MASK) | (bs.specular ? FL_SPEC_TRUE : 0u);
+                            flags &= ~FL_FROM_CAMERA;
+                            beta4.w = pdf_path;
+                            // Widen the cone after rough bounces (pt/mod.rs:965-967).
+                            if (PAT) cone.y += fminf(1.0f / (1.0f + pdf_path), 0.4f);
+                            prev4 = make_float4(p.x, p.y, p.z, 0.0f);
+                            float off = bs.transmitted ? -RT_RAY_OFFSET : RT_RAY_OFFSET;
+                            float3 no = p + n * off;
+                            float3 nd = normalize_ref(wi);
+                            uint32_t depth = (flags >> FL_DEPTH_SHIFT) + 1;
+                            flags = (flags & 0xFFFFu) | (depth << FL_DEPTH_SHIFT);
+                            bool alive = true;
+                            if (depth >= C.rr_start) {
+                                float q = fminf(maxc(beta) * rr_gain, 0.95f);
+                                if (q <= 0.0f || rng.next_f() > q) alive = false;
+                                else beta = beta / q;
+                            }
+                            if (alive && depth < C.max_depth) {
+                                P.ray_o[slot] = make_float4(no.x, no.y, no.z, rr_gain);
+                                P.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, INFINITY);
+                                extend = true;
                             }
                         }
-                        if ((flags & FL_SPEC_MASK) == FL_SPEC_NONE)
-                            flags = (flags & ~FL_SPEC_MASK) | (bs.specular ? FL_SPEC_TRUE : 0u);
-                        flags &= ~FL_FROM_CAMERA;
-                        beta4.w = pdf_path;
-                        // Widen the cone after rough bounces (pt/mod.rs:965-967).
-                        if (PAT) cone.y += fminf(1.0f / (1.0f + pdf_path), 0.4f);
-                        prev4 = make_float4(p.x, p.y, p.z, 0.0f);
-                        float off = bs.transmitted ? -RT_RAY_OFFSET : RT_RAY_OFFSET;
-                        float3 no = p + n * off;
-                        float3 nd = normalize_ref(wi);
-                        uint32_t depth = (flags >> FL_DEPTH_SHIFT) + 1;
-                        flags = (flags & 0xFFFFu) | (depth << FL_DEPTH_SHIFT);
-                        bool alive = true;
-                        if (depth >= C.rr_start) {
-                            float q = fminf(maxc(beta) * rr_gain, 0.95f);
-                            if (q <= 0.0f || rng.next_f() > q) alive = false;
-                            else beta = beta / q;
-                        }
-                        if (alive && depth < C.max_depth) {
-                            P.ray_o[slot] = make_float4(no.x, no.y, no.z, rr_gain);
-                            P.ray_d[slot] = make_float4(nd.x, nd.y, nd.z, INFINITY);
-                            extend = true;
-                        }
-                    }
+                    }  // !walk
                 }
                 if (PAT) P.cone[slot] = cone;
             }
+            if (MED) P.med[slot] = mstk;
+            // A walk queues its equiangular shadow ray with its own (k_sss).
+            if (walk && shadow2) flags |= FL_SH2;
             P.beta[slot] = make_float4(beta.x, beta.y, beta.z, beta4.w);
             P.L[slot] = make_float4(Lr.x, Lr.y, Lr.z, travel);
             P.prev[slot] = make_float4(prev4.x, prev4.y, prev4.z, __uint_as_float(flags));
@@ -1138,7 +1330,12 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
             if (C.aovs) P.aux_d[slot] = auxd;
         }
         push_queue(P.q_ext[qout], &P.cnt[CNT_EXT_OUT], slot, extend);
-        push_queue(P.q_sh, &P.cnt[CNT_SHADOW], slot, shadow);
+        if (MED)
+            push_queue(P.q_sh, &P.cnt[CNT_SHADOW], slot | (shadow ? SH_PRIMARY : 0u) | (shadow2 ? SH_EQUI : 0u),
+                       (shadow || shadow2) && !walk);
+        else
+            push_queue(P.q_sh, &P.cnt[CNT_SHADOW], slot, shadow);
+        if (P.q_sss) push_queue(P.q_sss, &P.cnt[CNT_SSS], slot, walk);
     }
 }
 
@@ -1216,6 +1413,217 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
 }
 
 // Between waves: the next extend queue becomes the current one.
+// ---- subsurface walks ------------------------------------------------------------------
+// One thread per walk queued by k_shade (pt/mod.rs:794-892): isotropic
+// scattering through the material's homogeneous Burley-fit medium, one
+// closest-hit query per step (trace_closest), roulette after step 8, at most
+// 256 steps. The walk leaves diffusely where it first reaches a surface:
+// NEE there for a white Lambert lobe, then a cosine direction becomes the
+// path's next ray. Walks that escape or run out of steps end the path.
+template <int BLOCK, bool MED>
+__global__ void __launch_bounds__(BLOCK) k_sss(DevScene S, Paths P, PtConsts C, uint32_t qout) {
+    __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    TravStack st;
+    st.init(stack_sh + threadIdx.x, BLOCK);
+    const uint32_t n = P.cnt[CNT_SSS];
+    unsigned long long rays = 0;
+    const uint32_t stride = gridDim.x * BLOCK;
+    for (uint32_t j0 = blockIdx.x * BLOCK; j0 < n; j0 += stride) {
+        const uint32_t j = j0 + threadIdx.x;
+        uint32_t slot = 0;
+        bool extend = false, shadow = false, shadow2 = false;
+        if (j < n) {
+            slot = P.q_sss[j];
+            const float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot];
+            const float4 beta4 = P.beta[slot];
+            float4 prev4 = P.prev[slot];
+            const uint4 rs = P.rng[slot];
+            Pcg rng;
+            rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
+            rng.inc = (uint64_t)rs.z | ((uint64_t)rs.w << 32);
+            uint32_t flags = __float_as_uint(prev4.w);
+            float3 beta = xyz(beta4);
+            float pdf_prev = beta4.w;
+            const DevMaterial& m = S.materials[P.hit[slot].x];
+            const float3 sst = f3(m.sss_st[0], m.sss_st[1], m.sss_st[2]);
+            const float3 sss = f3(m.sss_ss[0], m.sss_ss[1], m.sss_ss[2]);
+            const uint32_t cur_med = MED ? mstack_top(P.med[slot], S.atmosphere) : RT_MEDIUM_NONE;
+            float3 wo = xyz(o4), wd = xyz(d4);
+            bool exited = false;
+            for (int step = 0; step < 256; step++) {
+                uint4 hr;
+                rays++;
+                if (!trace_closest(S, st, wo, wd, INFINITY, P.err, hr)) break;  // escaped through a crack
+                const MedEvent ev = homog_sample(sst, sss, __uint_as_float(hr.x), beta, rng);
+                beta = beta * ev.w;
+                if (ev.scatter) {
+                    wo = wo + wd * ev.t;
+                    const float u = rng.next_f(), v = rng.next_f();
+                    const float z = 1.0f - 2.0f * u, r = sqrtf(fmaxf(1.0f - z * z, 0.0f));
+                    float sp, cp;
+                    sincosf(2.0f * RT_PI * v, &sp, &cp);
+                    wd = f3(r * cp, r * sp, z);
+                    const float q = fminf(maxc(beta), 0.95f);
+                    if (q <= 0.0f || (step > 8 && rng.next_f() > q)) break;
+                    if (step > 8) beta = beta / q;
+                    continue;
+                }
+                // Exit on the outside: normal along the walk's direction.
+                HitGeo hg;
+                hit_geometry(S, wo, wd, hr, hg);
+                const float3 out_n = dot(hg.nw, wd) > 0.0f ? hg.nw : -hg.nw;
+                const Frame xf(out_n);
+                const float3 xp = hg.p;
+                uint32_t li;
+                float pmf;
+                if (light_sample(S, xp, rng.next_f(), li, pmf)) {
+                    auto eval = [&](float3 wi, float& pdf) -> float3 {
+                        const float3 wl = xf.to_local(wi);
+                        pdf = wl.z > 0.0f ? wl.z * (1.0f / RT_PI) : 0.0f;
+                        return f3(pdf, pdf, pdf);
+                    };
+                    NeeOut ne;
+                    if (nee_light_eval(S, S.lights[li], xp, out_n, eval, pmf, rng, ne)) {
+                        const float3 c = beta * ne.c;
+                        if (maxc(c) > 0.0f) {
+                            const bool spec_true = (flags & FL_SPEC_MASK) == FL_SPEC_TRUE;
+                            P.sh_o[slot] = make_float4(ne.o.x, ne.o.y, ne.o.z, MED ? __uint_as_float(cur_med) : 0.0f);
+                            P.sh_d[slot] = make_float4(ne.d.x, ne.d.y, ne.d.z, ne.tmax);
+                            P.sh_c[slot] = make_float4(c.x, c.y, c.z, spec_true ? 0.0f : 1.0f);
+                            shadow = true;
+                        }
+                    }
+                }
+                const float x1 = rng.next_f(), x2 = rng.next_f();
+                const float xr = sqrtf(x1);
+                float xs, xc;
+                sincosf(2.0f * RT_PI * x2, &xs, &xc);
+                const float3 local = f3(xr * xc, xr * xs, sqrtf(fmaxf(1.0f - x1, 0.0f)));
+                const float3 wi = normalize_ref(xf.to_world(local));
+                pdf_prev = fmaxf(local.z, 1e-9f) * (1.0f / RT_PI);
+                prev4 = make_float4(xp.x, xp.y, xp.z, 0.0f);
+                flags &= ~FL_FROM_CAMERA;
+                if (P.cone) {
+                    float2 cn = P.cone[slot];
+                    cn.y += 0.4f;
+                    P.cone[slot] = cn;
+                }
+                wo = xp + out_n * RT_RAY_OFFSET;
+                wd = wi;
+                exited = true;
+                break;
+            }
+            if (exited) {
+                const uint32_t depth = (flags >> FL_DEPTH_SHIFT) + 1;
+                flags = (flags & 0xFFFFu) | (depth << FL_DEPTH_SHIFT);
+                bool alive = true;
+                if (depth >= C.rr_start) {
+                    const float q = fminf(maxc(beta) * o4.w, 0.95f);
+                    if (q <= 0.0f || rng.next_f() > q) alive = false;
+                    else beta = beta / q;
+                }
+                if (alive && depth < C.max_depth) {
+                    P.ray_o[slot] = make_float4(wo.x, wo.y, wo.z, o4.w);
+                    P.ray_d[slot] = make_float4(wd.x, wd.y, wd.z, INFINITY);
+                    extend = true;
+                }
+            }
+            shadow2 = MED && (flags & FL_SH2);
+            flags &= ~FL_SH2;
+            P.beta[slot] = make_float4(beta.x, beta.y, beta.z, pdf_prev);
+            P.prev[slot] = make_float4(prev4.x, prev4.y, prev4.z, __uint_as_float(flags));
+            P.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), rs.z, rs.w);
+        }
+        push_queue(P.q_ext[qout], &P.cnt[CNT_EXT_OUT], slot, extend);
+        if (MED)
+            push_queue(P.q_sh, &P.cnt[CNT_SHADOW], slot | (shadow ? SH_PRIMARY : 0u) | (shadow2 ? SH_EQUI : 0u),
+                       shadow || shadow2);
+        else
+            push_queue(P.q_sh, &P.cnt[CNT_SHADOW], slot, shadow);
+    }
+    if (rays) atomicAdd(&P.stats[0], rays);
+}
+
+// ---- shadow rays through media -------------------------------------------------------
+// Transmittance of one shadow ray (pt/mod.rs:1244-1306): segment by segment
+// to the closest hit, each segment taking its medium's transmittance
+// (closed form, or ratio tracking from rng); volume hulls push and pop the
+// medium (the ray starts in `medium`, the atmosphere below it), cutouts
+// attenuate by 1 - presence, anything else blocks; at most 16 segments.
+__device__ __forceinline__ float3 shadow_walk(const DevScene& S, TravStack& st, float3 o, float3 d, float remaining,
+                                              uint32_t medium, Pcg& rng, uint32_t* err, unsigned long long& rays) {
+    uint2 ms = make_uint2(0u, 0u);
+    if (medium != RT_MEDIUM_NONE && medium != S.atmosphere) mstack_push(ms, medium);
+    float3 vis = f3(1.0f, 1.0f, 1.0f);
+    for (int k = 0; k < RT_MAX_PRESENCE_SKIPS; k++) {
+        rays++;
+        uint4 hr;
+        const bool found = remaining > 0.0f && trace_closest(S, st, o, d, remaining, err, hr);
+        const float t = found ? __uint_as_float(hr.x) : remaining;
+        const uint32_t cur = mstack_top(ms, S.atmosphere);
+        if (cur != RT_MEDIUM_NONE) {
+            vis = vis * med_transmittance(S.media[cur], o, d, fmaxf(t, 0.0f), rng);
+            if (maxc(vis) < 1e-4f) return f3(0.0f, 0.0f, 0.0f);
+        }
+        if (!found) return vis;
+        const uint32_t mat = (hr.y & RT_TRI_QUADRIC) ? S.quadrics[hr.y & ~RT_TRI_QUADRIC].material
+                                                     : __ldg(&S.inst[hr.z].z);
+        const DevMaterial& m = S.materials[mat];
+        if (m.hull != 0.0f) {
+            HitGeo hg;
+            hit_geometry(S, o, d, hr, hg);
+            if (hg.front) mstack_push(ms, m.interior);
+            else mstack_pop(ms);
+        } else {
+            if (m.presence >= 1.0f) return f3(0.0f, 0.0f, 0.0f);
+            vis = vis * (1.0f - m.presence);
+            if (maxc(vis) < 1e-4f) return f3(0.0f, 0.0f, 0.0f);
+        }
+        o = o + d * (t + RT_RAY_OFFSET);
+        remaining -= t + RT_RAY_OFFSET;
+    }
+    return vis;
+}
+
+// Scenes with media: one thread per queued slot walks its shadow rays (the
+// surface / collision / walk-exit one, then the equiangular one) and adds
+// both contributions in that order. Ratio tracking draws from a stream
+// derived from the path's state, so the image stays reproducible.
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_shadow_media(DevScene S, Paths P, PtConsts C) {
+    __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
+    TravStack st;
+    st.init(stack_sh + threadIdx.x, BLOCK);
+    const uint32_t n = P.cnt[CNT_SHADOW];
+    unsigned long long rays = 0;
+    for (uint32_t j = blockIdx.x * BLOCK + threadIdx.x; j < n; j += gridDim.x * BLOCK) {
+        const uint32_t e = P.q_sh[j];
+        const uint32_t slot = e & SH_SLOT_MASK;
+        const uint4 rs = P.rng[slot];
+        Pcg rng;
+        rng.state = splitmix(((uint64_t)rs.x | ((uint64_t)rs.y << 32)) ^ 0xD1B54A32D192ED03ull);
+        rng.inc = (splitmix((uint64_t)rs.z | ((uint64_t)rs.w << 32)) << 1) | 1ull;
+        float3 add = f3(0.0f, 0.0f, 0.0f), add_aux = f3(0.0f, 0.0f, 0.0f);
+        for (int r = 0; r < 2; r++) {
+            if (!(e & (r == 0 ? SH_PRIMARY : SH_EQUI))) continue;
+            const float4 o4 = r == 0 ? P.sh_o[slot] : P.sh2_o[slot];
+            const float4 d4 = r == 0 ? P.sh_d[slot] : P.sh2_d[slot];
+            const float4 c4 = r == 0 ? P.sh_c[slot] : P.sh2_c[slot];
+            const float3 vis = shadow_walk(S, st, xyz(o4), xyz(d4), d4.w, __float_as_uint(o4.w), rng, P.err, rays);
+            const float3 c = xyz(c4) * vis;
+            add = add + c;
+            if (c4.w != 0.0f) add_aux = add_aux + c;
+        }
+        const float4 L = P.L[slot];
+        P.L[slot] = make_float4(L.x + add.x, L.y + add.y, L.z + add.z, L.w);
+        if (C.aovs) {
+            const float4 a = P.aux_d[slot];
+            P.aux_d[slot] = make_float4(a.x + add_aux.x, a.y + add_aux.y, a.z + add_aux.z, a.w);
+        }
+    }
+    if (rays) atomicAdd(&P.stats[1], rays);
+}
+
 __global__ void k_wave_prep(uint32_t* cnt) {
     uint32_t t = threadIdx.x;
     if (t == 0) {
@@ -1224,6 +1632,7 @@ __global__ void k_wave_prep(uint32_t* cnt) {
         cnt[CNT_SHADOW] = 0;
         cnt[CNT_FETCH_EXT] = 0;
         cnt[CNT_FETCH_SH] = 0;
+        cnt[CNT_SSS] = 0;
     }
     if (t < N_QUEUES) cnt[CNT_CLASS + t] = 0;
 }

@@ -70,9 +70,25 @@ struct DevMaterial {
     int32_t area_light;
     uint32_t id;
     uint32_t mclass;
-    uint32_t pad_;
+    uint32_t interior;                       // medium inside (Material::interior), ~0 for none
+    // Subsurface random walk: probability, and the Burley-fit homogeneous
+    // medium (volume.rs sss_medium) as extinction and scattering.
+    float sss_gain, sss_st[3];
+    float sss_ss[3], hull;                   // hull: 1 when the surface only bounds `interior`
 };
-static_assert(sizeof(DevMaterial) == 160, "DevMaterial layout");
+static_assert(sizeof(DevMaterial) == 192, "DevMaterial layout");
+
+// ---- participating media (src/scene/medium.rs) ---------------------------------
+struct DevMedium {
+    float sigma_a[3], g;
+    float sigma_s[3], max_distance;
+    float emission[3], majorant;             // channel-max extinction
+    float frequency, gain, lacunarity, coverage;
+    float sharpness;
+    uint32_t octaves, density, pad_;         // density: RT_DENSITY_*
+};
+static_assert(sizeof(DevMedium) == 80, "DevMedium layout");
+#define RT_MAX_MEDIA 127u   // medium indices fit the 7-bit entries of a path's medium stack
 
 // ---- lights -----------------------------------------------------------------
 struct DevLight {
@@ -147,8 +163,9 @@ struct DevPbr {
     float fuzz_gain, fuzz_color[3];
     float glass_gain, glass_ior, glass_rough;
     float refraction[3], glow[3], presence, emission[3];
+    float sss_albedo[3], pad_;   // subsurface colour x gain, the first-hit albedo's share
 };
-static_assert(sizeof(DevPbr) == 128, "DevPbr layout");
+static_assert(sizeof(DevPbr) == 144, "DevPbr layout");
 
 // Per material: its bindings (binds[bind_off .. bind_off + bind_n) as
 // (field, node)), the nodes they reach (node_lo + bit k of node_mask),
@@ -228,6 +245,10 @@ struct DevScene {
     uint32_t any_presence;       // some material has presence < 1
     uint32_t max_steps;          // traversal steps per ray before the query is given up (error bit)
     uint32_t dome;               // first dome light (misses see it), ~0 for none
+    const DevMedium* media;      // participating media (null when none)
+    uint32_t n_media;
+    uint32_t atmosphere;         // global medium, ~0 for none
+    uint32_t any_sss;            // some material has a subsurface walk
     // Environment map of light env_light (src/scene/envmap.rs): lat-long
     // texels (RGB + pad), row-marginal CDF (env_h + 1), per-row conditional
     // CDFs (env_w + 1 each) over sin-weighted luminance, their total.

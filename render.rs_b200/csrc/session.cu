@@ -324,6 +324,7 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
         rc = rc ? rc : s->upload(&S.ies_data, H.ies_data);
     }
     if (!H.quadrics.empty()) rc = rc ? rc : s->upload(&S.quadrics, H.quadrics);
+    if (!H.media.empty()) rc = rc ? rc : s->upload(&S.media, H.media);
     rc = rc ? rc : s->upload(&S.materials, H.materials);
     rc = rc ? rc : s->upload(&S.lights, H.lights);
     rc = rc ? rc : s->upload(&S.lbvh, H.lbvh);
@@ -343,6 +344,10 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     // passes up to about 4M paths (16 passes at most), with guide_steps
     // network updates per sample pass.
     const bool guided = params->guided != 0;
+    if (guided && S.n_media) {
+        delete s;
+        return fail(RT_ERR_INVALID, "the learned proposal does not guide scenes with participating media");
+    }
     uint64_t guided_k = std::max<uint64_t>(1, std::min<uint64_t>(16, (4ull << 20) / s->npix));
     // Plain renders: slabs of up to 32M paths and 16 passes. A wave lasts as
     // long as its longest rays, so more passes per slab spread those tails
@@ -372,6 +377,18 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     rc = rc ? rc : s->alloc(&Pp.aux_d, aov ? P : 1);
     Pp.cone = nullptr;
     if (S.mat_pat) rc = rc ? rc : s->alloc(&Pp.cone, P);
+    // Media: nested-medium stacks and the equiangular shadow slot; walks:
+    // their queue.
+    Pp.med = nullptr;
+    Pp.sh2_o = Pp.sh2_d = Pp.sh2_c = nullptr;
+    Pp.q_sss = nullptr;
+    if (S.n_media) {
+        rc = rc ? rc : s->alloc(&Pp.med, P);
+        rc = rc ? rc : s->alloc(&Pp.sh2_o, P);
+        rc = rc ? rc : s->alloc(&Pp.sh2_d, P);
+        rc = rc ? rc : s->alloc(&Pp.sh2_c, P);
+    }
+    if (S.any_sss) rc = rc ? rc : s->alloc(&Pp.q_sss, P);
     rc = rc ? rc : s->alloc(&Pp.q_ext[0], P);
     rc = rc ? rc : s->alloc(&Pp.q_ext[1], P);
     rc = rc ? rc : s->alloc(&Pp.q_cls, P * N_QUEUES);
@@ -503,7 +520,9 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     PtConsts C;
     C.npix = s->npix;
     C.width = s->S.width;
-    C.max_depth = s->params.max_depth;
+    // Multiple scattering needs a deeper budget: 64 bounces in scenes with
+    // media (pt/mod.rs:483-484, gpu_scene.rs:671).
+    C.max_depth = s->S.n_media ? 64u : s->params.max_depth;
     C.rr_start = s->params.rr_start;
     C.aovs = s->params.aovs;
     C.clamp = (float)s->params.firefly_clamp;
@@ -519,7 +538,10 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     // meets even when it passes through it (pt/mod.rs:690-700); then the
     // shade kernel skips surfaces as the reference does, in extra waves.
     C.pres_in_trav = (s->S.any_presence && !s->params.aovs) ? 1u : 0u;
-    uint32_t waves = s->params.max_depth + (s->S.any_presence && !C.pres_in_trav ? RT_MAX_PRESENCE_SKIPS : 0u);
+    // Waves: one per bounce, plus the surfaces a path may pass without a
+    // bounce (cutouts skipped in shade waves, volume-hull crossings).
+    const bool skip_waves = (s->S.any_presence && !C.pres_in_trav) || s->S.n_media;
+    uint32_t waves = C.max_depth + (skip_waves ? RT_MAX_PRESENCE_SKIPS : 0u);
     const int trav_grid = s->trav_grid, shade_grid = s->sm_count * 8;
     const uint32_t batch = 1u << 16;  // training records per Adam step
     CUDA_TRY(cudaMemsetAsync(s->stats, 0, 32, st));
@@ -587,10 +609,20 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
                 P.g_raw = raw;
                 launches += 3;
             }
-            if (P.cone) k_shade<true><<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
+            const bool med = s->S.n_media > 0;
+            if (P.cone && med) k_shade<true, true><<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
+            else if (P.cone) k_shade<true><<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
+            else if (med) k_shade<false, true><<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
             else k_shade<false><<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
+            if (s->S.any_sss) {
+                // Subsurface walks started by this wave's shading.
+                if (med) k_sss<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C, qout);
+                else k_sss<TRAV_BLOCK, false><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C, qout);
+                launches++;
+            }
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 2], st));
-            if (quad) k_shadow<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            if (med) k_shadow_media<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            else if (quad) k_shadow<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             else k_shadow<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 3], st));
             k_wave_prep<<<1, 32, 0, st>>>(P.cnt);

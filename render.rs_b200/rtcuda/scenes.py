@@ -11,11 +11,14 @@ down for tests; the defaults are the full workloads.
   two_rooms              two 4x3x3 rooms joined by a 0.2x2.0 opening, light in the unseen room
   forest                 20 trees x ~45k triangles, 772,000 instances on a 512x512 fBm terrain,
                          1,200 point lights
+  media_cornell          the Cornell box with participating media (fog, an fBm cloud in a
+                         volume hull, glass with an absorbing interior) and a subsurface sphere
 """
 import numpy as np
 
-from .scene import (Scene, affine, emitter, ggx_conductor, ggx_floor, matte, rot_y,
-                    rough_dielectric)
+from . import abi
+from .scene import (Scene, affine, emitter, ggx_conductor, ggx_floor, matte, medium, rot_y,
+                    rough_dielectric, volume_hull)
 
 
 # ---------------------------------------------------------------------------
@@ -445,3 +448,42 @@ def patterned_room(width=96, height=72):
 
     s.add_emissive_quad((-0.5, 2.99, -0.5), (1.0, 0.0, 0.0), (0.0, 0.0, 1.0), (12.0, 11.0, 9.0))
     return s
+
+
+# ---------------------------------------------------------------------------
+# Participating media and subsurface scattering
+def media_cornell(width=64, height=64, fog=True, cloud=True, glass=True, sss=True, point_light=True):
+    """The Cornell box (cornell_box) with the reference's media and
+    subsurface features, each switchable:
+      fog    an atmosphere of thin forward-scattering haze (sigma_s 0.12-0.16,
+             sigma_a 0.01, g 0.5, 8 units deep);
+      cloud  a volume-hull sphere (r 0.3, mid-air) holding an fBm cloud
+             (sigma_s 4, g 0.6, frequency 2, 3 octaves, coverage 0.6);
+      glass  a rough-glass sphere (r 0.25, on the floor) with an absorbing
+             amber interior;
+      sss    a sphere (r 0.22, on the floor) whose paths take the subsurface
+             walk (gain 1, colour (0.9, 0.5, 0.3), mean free path 0.2/0.1/0.05);
+      point_light  a warm point light under the ceiling (equiangular NEE).
+    Scenes with media render with 64 bounces (the reference's rule)."""
+    s = cornell_box(width, height)
+    if point_light:
+        s.add_point_light((0.45, 0.7, 0.4), 0.8, (1.0, 0.85, 0.6))
+    if fog:
+        s.add_medium(medium((0.01, 0.01, 0.01), (0.12, 0.14, 0.16), g=0.5, max_distance=8.0), atmosphere=True)
+    sphere = [1.0, -1.0, 1.0, 360.0]
+    if cloud:
+        ci = s.add_medium(medium((0.05, 0.05, 0.05), (4.0, 4.0, 4.0), g=0.6,
+                                 fbm=dict(frequency=2.0, octaves=3, gain=0.5, lacunarity=2.0, coverage=0.6,
+                                          sharpness=3.0)))
+        hull = s.add_material(volume_hull(interior=ci, id=6))
+        s.add_quadric(abi.QUADRIC_SPHERE, sphere, hull, affine(np.eye(3) * 0.3, (-0.05, 0.35, 0.0)))
+    if glass:
+        gi = s.add_medium(medium((0.9, 0.35, 0.08), (0.0, 0.0, 0.0)))
+        gm = s.add_material(rough_dielectric(1.5, 0.05, interior=gi, id=7))
+        s.add_quadric(abi.QUADRIC_SPHERE, sphere, gm, affine(np.eye(3) * 0.25, (-0.55, -0.75, 0.55)))
+    if sss:
+        sm = s.add_material(matte((0.8, 0.8, 0.8), subsurface_gain=1.0, subsurface_color=(0.9, 0.5, 0.3),
+                                  subsurface_dmfp=(0.2, 0.1, 0.05), id=8))
+        s.add_quadric(abi.QUADRIC_SPHERE, sphere, sm, affine(np.eye(3) * 0.22, (0.05, -0.78, 0.7)))
+    return s
+
