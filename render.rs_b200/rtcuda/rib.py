@@ -22,9 +22,10 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     they are skipped, as the reference does.
   * Bilinear / bicubic PatchMesh and Patch are diced by the current
     Basis, as the reference does, NuPatch NURBS untrimmed;
-    SubdivisionMesh, GeneralPolygon, Curves, Points, media and motion blur
+    SubdivisionMesh, GeneralPolygon, Curves, Points and motion blur
     are skipped with a warning (motion blocks use their first
-    sample); Displace "noise" moves polygon-mesh vertices at load time as
+    sample); Interior and Atmosphere media (homogeneous or fBm) and
+    PxrSurface subsurface parameters are carried; Displace "noise" moves polygon-mesh vertices at load time as
     the reference does; a PxrDomeLight lightColorMap is read when it is a
     Radiance .hdr (one map per scene).
   * Pattern graphs: PxrChecker, PxrFractal, PxrMix, PxrColorCorrect,
@@ -41,7 +42,7 @@ import os
 import numpy as np
 
 from . import abi
-from .scene import Scene, default_material, emitter
+from .scene import Scene, default_material, emitter, medium
 
 # ---- parsing (src/parser/parser.rs) --------------------------------------------------------
 
@@ -409,6 +410,17 @@ def _pbr_bxdf(p):
         v = p.number(tok)
         if v is not None:
             m[key] = v
+    # Subsurface walk (pbr.rs:174-183): a scalar mean free path applies to
+    # all three channels.
+    v = p.number("subsurfaceGain")
+    if v is not None:
+        m["subsurface_gain"] = v
+    v = p.numbers("subsurfaceColor")
+    if v is not None and len(v) >= 3:
+        m["subsurface_color"] = tuple(v[:3])
+    v = p.numbers("subsurfaceDmfp")
+    if v:
+        m["subsurface_dmfp"] = tuple(v[:3]) if len(v) >= 3 else (v[0],) * 3
     gg = p.number("glowGain") or 0.0
     gc = p.numbers("glowColor")
     gc = tuple(gc[:3]) if gc is not None and len(gc) >= 3 else (1.0, 1.0, 1.0)
@@ -431,6 +443,7 @@ class _State:
         self.basis_u = ("bezier", None)  # Basis: (name or 16 numbers, step or None) per direction
         self.basis_v = ("bezier", None)
         self.identifier = None
+        self.interior = -1       # Interior medium bound to subsequent geometry
 
     def copy(self):
         s = _State()
@@ -483,6 +496,8 @@ class _Builder:
         self.textures = []                # (H, W, 3) f32 linear RGB
         self.ies = {}                     # light index -> (v, h, candela, world_to_local)
         self.texture_ids = {}             # file path -> texture index (-1: unreadable)
+        self.media = []                   # Scene medium dicts
+        self.atmosphere = -1              # index into media, -1 for none
 
     # -- helpers ------------------------------------------------------------------
     def warn(self, msg):
@@ -517,6 +532,7 @@ class _Builder:
         else:
             m = _pbr_matte(st.color)
         m["id"] = self.object_id()
+        m["interior"] = st.interior
         if st.bxdf is not None and st.bxdf_bindings:
             m["_bindings"] = list(st.bxdf_bindings)
         return m
@@ -733,6 +749,11 @@ class _Builder:
             st.bxdf_bindings = self.bxdf_bindings(prm)
         elif name == "Pattern":
             self.pattern_request(vals)
+        elif name in ("Interior", "Atmosphere"):
+            self.medium_request(name, vals)
+        elif name == "Exterior":
+            self.warn("Exterior is subsumed by nested Interior tracking (rays exiting an object return "
+                      "to the enclosing medium); ignoring")
         elif name == "Displace":
             # scene_builder.rs:776-795: the built-in fBm "noise" displacement.
             kind = _str(vals, 0) or ""
@@ -782,6 +803,37 @@ class _Builder:
                 self.add_quadric(_QUADRIC_KIND[name], a, self.add_material(self.make_material()), self.ctm)
         else:
             self.warn(f"RIB request '{name}' not rendered on this path; skipping")
+
+    def medium_request(self, name, vals):
+        """Interior / Atmosphere (scene_builder.rs:324-373): sigma_a, sigma_s,
+        g, emission, maxdistance, and density "fbm" with frequency, octaves,
+        gain, lacunarity, coverage and sharpness. Atmospheres are slabs of
+        1200 units by default."""
+        p = _Params(vals, 1)
+
+        def get3(key, default):
+            v = p.numbers(key)
+            return tuple(v[:3]) if v is not None and len(v) >= 3 else default
+
+        dens = p.string("density")
+        fbm = None
+        if dens in ("fbm", "noise"):
+            fbm = {}
+            for key, default in (("frequency", 0.3), ("octaves", 5.0), ("gain", 0.55), ("lacunarity", 2.0),
+                                 ("coverage", 0.5), ("sharpness", 4.0)):
+                v = p.number(key)
+                fbm[key] = default if v is None else v
+        elif dens is not None:
+            self.warn(f'Interior density "{dens}" not implemented; homogeneous')
+        ext = p.number("maxdistance")
+        med = medium(get3("sigma_a", (0.1, 0.1, 0.1)), get3("sigma_s", (0.5, 0.5, 0.5)),
+                     g=p.number("g") or 0.0, emission=get3("emission", (0.0, 0.0, 0.0)),
+                     max_distance=(1200.0 if name == "Atmosphere" else math.inf) if ext is None else ext, fbm=fbm)
+        self.media.append(med)
+        if name == "Atmosphere":
+            self.atmosphere = len(self.media) - 1
+        else:
+            self.state.interior = len(self.media) - 1
 
     def color_from(self, vals):
         a = [_num(vals, k) for k in range(3)]
@@ -1208,6 +1260,9 @@ class _Builder:
                             np.stack([i[2] for i in self.instances]))
         for kind, params, mat, xf in self.quadrics:
             s.add_quadric(kind, params, mat, xf)
+        for med in self.media:
+            s.add_medium(med)
+        s.atmosphere = self.atmosphere
         s.filter, s.filter_width = self.filter
         if self.dof is not None:
             fstop, flen, fdist = self.dof

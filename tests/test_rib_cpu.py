@@ -343,3 +343,44 @@ def test_st_primvar():
     # Wrong-length st is ignored.
     assert sorted(s.mesh_st) == [0]
     np.testing.assert_array_equal(s.mesh_st[0], [[0, 0], [1, 0], [1, 1], [0, 1]])
+
+
+def test_media_requests_and_subsurface():
+    """Interior / Atmosphere (scene_builder.rs:324-373) and the PxrSurface
+    subsurface parameters (pbr.rs:174-183)."""
+    s = load_rib_string("""
+Format 8 8 1
+Atmosphere "haze" "sigma_a" [0.1 0.2 0.3] "sigma_s" [0.5 0.5 0.5] "g" [0.3]
+WorldBegin
+  AttributeBegin
+    Interior "cloud" "sigma_s" [4 4 4] "density" ["fbm"] "frequency" [0.2] "octaves" [3] "coverage" [0.7]
+    Bxdf "PxrSurface" "hull" "diffuseGain" [0] "specularIor" [1]
+    Sphere 1 -1 1 360
+  AttributeEnd
+  Bxdf "PxrSurface" "skin" "subsurfaceGain" [0.8] "subsurfaceColor" [0.9 0.4 0.3] "subsurfaceDmfp" [0.05]
+  Polygon "P" [-1 -1 5  1 -1 5  1 1 5  -1 1 5]
+WorldEnd
+""")
+    assert len(s.media) == 2 and s.atmosphere == 0
+    haze, cloud = s.media
+    assert haze["sigma_a"] == (0.1, 0.2, 0.3) and haze["g"] == 0.3 and haze["max_distance"] == 1200.0
+    assert haze["density"] == abi.DENSITY_NONE
+    assert cloud["density"] == abi.DENSITY_FBM and cloud["octaves"] == 3 and cloud["frequency"] == 0.2
+    assert cloud["coverage"] == 0.7 and cloud["gain"] == 0.55 and cloud["max_distance"] == float("inf")
+    assert cloud["sigma_a"] == (0.1, 0.1, 0.1)  # the request's defaults
+    hull = s.materials[s.quadrics[0][3]]
+    assert hull["interior"] == 1 and hull["diffuse_gain"] == 0.0
+    skin = s.materials[-1]
+    assert skin["interior"] == -1  # AttributeEnd restored the state
+    assert skin["subsurface_gain"] == 0.8 and skin["subsurface_dmfp"] == (0.05, 0.05, 0.05)
+    assert skin["subsurface_color"] == (0.9, 0.4, 0.3)
+
+
+def test_clouds_fixture_media():
+    s = load_rib(os.path.join(FIXTURES, "clouds.rib"))
+    assert len(s.media) == 3 and s.atmosphere == 0
+    assert [m["density"] for m in s.media] == [abi.DENSITY_NONE, abi.DENSITY_FBM, abi.DENSITY_FBM]
+    assert s.media[0]["max_distance"] == 900.0
+    hulls = [q for q in s.quadrics if s.materials[q[3]]["interior"] >= 0]
+    assert len(hulls) == 9
+
