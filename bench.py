@@ -333,7 +333,9 @@ def other_workloads(flush, stream):
     size: the 1M-triangle cloud at 1920x1080 x 16 spp (depth 8) and its
     4,194,304-ray closest-hit / any-hit batches (L2 flushed before each
     batch), the Cornell box 256^2 x 16 spp (depth 8), instanced materials
-    1920x1080 x 64 spp (depth 12). One warm-up pass, then one timed render
+    1920x1080 x 64 spp (depth 12), the media Cornell box 512^2 x 16 spp (fog,
+    an fBm cloud, absorbing glass, a subsurface sphere; 64 bounces, the
+    reference's depth with media). One warm-up pass, then one timed render
     call (device time from the session's events); scene build excluded."""
     import torch
     from rtcuda import PtSession, abi, scenes
@@ -342,7 +344,9 @@ def other_workloads(flush, stream):
               scenes.TRIANGLE_CLOUD, CLOUD_SPP),
              ("cornell_256x256_16spp_depth8", lambda: scenes.cornell_box(), scenes.CORNELL, 16),
              ("instanced_materials_1920x1080_64spp_depth12", lambda: scenes.instanced_materials(),
-              scenes.INSTANCED_MATERIALS, 64)]
+              scenes.INSTANCED_MATERIALS, 64),
+             ("media_cornell_512x512_16spp_depth64", lambda: scenes.media_cornell(512, 512),
+              dict(max_depth=8, rr_start=3), 16)]
     for name, make, cfg, spp in cases:
         t0 = time.perf_counter()
         s = make()
@@ -529,7 +533,8 @@ def run_scene(args):
     w, h = (int(v) for v in args.res.split("x"))
     make = {"cornell": (scenes.cornell_box, scenes.CORNELL), "cloud": (scenes.triangle_cloud, scenes.TRIANGLE_CLOUD),
             "instanced": (scenes.instanced_materials, scenes.INSTANCED_MATERIALS),
-            "two_rooms": (scenes.two_rooms, scenes.TWO_ROOMS), "forest": (scenes.forest, scenes.FOREST)}
+            "two_rooms": (scenes.two_rooms, scenes.TWO_ROOMS), "forest": (scenes.forest, scenes.FOREST),
+            "media": (scenes.media_cornell, dict(max_depth=8, rr_start=3))}
     gen, cfg = make[args.scene]
     s = gen(w, h)
     p = abi.make_params(max_depth=cfg["max_depth"], rr_start=cfg["rr_start"])
@@ -551,7 +556,8 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--scene", default="forest", help="--mode scene: cornell, cloud, instanced, two_rooms, forest")
+    ap.add_argument("--scene", default="forest",
+                    help="--mode scene: cornell, cloud, instanced, two_rooms, forest, media")
     ap.add_argument("--res", default="640x360", help="--mode scene: frame size WxH")
     ap.add_argument("--mode", default="full", choices=["full", "traversal", "guided", "scene"],
                     help="traversal: only the closest/any-hit ray batches; guided: only the learned-proposal "
