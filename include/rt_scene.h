@@ -40,14 +40,28 @@ typedef struct rt_mesh_desc {
     const float*    st;           /* 2 * n_vertices (s, t), or NULL (st = 0, density 0) */
 } rt_mesh_desc;
 
-/* Placed copy of a mesh. `object_to_world` is the row-major upper 3x4 of
- * the reference's `Instance::transform` (mesh.rs:237); the bottom row is
- * (0,0,0,1). The inverse is computed by the consumer in f64. */
+/* Placed copy of a mesh or a curve set. `object_to_world` is the row-major
+ * upper 3x4 of the reference's `Instance::transform` (mesh.rs:237); the
+ * bottom row is (0,0,0,1). The inverse is computed by the consumer in f64.
+ * mesh_id below n_meshes names a mesh, n_meshes + k the curve set k
+ * (`Instance::new_curves`, mesh.rs:256-264). */
 typedef struct rt_instance_desc {
     double   object_to_world[12];
     uint32_t mesh_id;
     uint32_t material_id;
 } rt_instance_desc;
+
+/* Curve set: `CurveSet` (src/geometry/curves.rs:15-26), rounded-cone
+ * segments (a swept sphere whose radius goes linearly from the start's to
+ * the end's; equal ends make a point particle a sphere). */
+typedef struct rt_curves_desc {
+    const float* p0;          /* 4 per segment: start xyz, radius */
+    const float* p1;          /* 4 per segment: end xyz, radius */
+    const float* v0;          /* curve parameter at the start (0 root, 1 tip) */
+    const float* v1;          /* and at the end */
+    uint32_t n_segments;
+    uint32_t reserved;        /* 0 */
+} rt_curves_desc;
 
 /* Material: `PbrParams` fields in scope (src/scene/pbr.rs:10-51) plus
  * `Material::{emission, area_light, id}` (src/scene/material.rs:21-39). */
@@ -78,7 +92,11 @@ typedef struct rt_material_desc {
     double  subsurface_color[3];
     double  subsurface_dmfp[3];
     int32_t interior;                /* medium inside this geometry (Material::interior), or -1 */
-    uint32_t material_reserved;      /* 0 */
+    uint32_t hair;                   /* 1: Marschner hair on curve hits (Material::hair, pt/hair.rs) */
+    double  hair_sigma_a[3];         /* HairParams::sigma_a, absorption per fiber diameter */
+    double  hair_beta_m;             /* longitudinal roughness (clamped to [0.01, 1]) */
+    double  hair_beta_n;             /* azimuthal roughness (clamped to [0.01, 1]) */
+    double  hair_eta;                /* fiber index of refraction */
 } rt_material_desc;
 
 enum {
@@ -305,6 +323,10 @@ typedef struct rt_scene_desc {
     const rt_medium_desc*     media;
     uint32_t n_media;
     int32_t  atmosphere;
+    /* Curve sets (Scene::curve_sets), placed by instances (mesh_id >= n_meshes). */
+    const rt_curves_desc*     curves;
+    uint32_t n_curves;
+    uint32_t curves_reserved; /* 0 */
 } rt_scene_desc;
 
 /* Integrator knobs. The reference hard-codes these as constants
@@ -334,7 +356,8 @@ typedef struct rt_params {
 #ifdef __cplusplus
 static_assert(sizeof(rt_mesh_desc) == 40, "rt_mesh_desc layout");
 static_assert(sizeof(rt_instance_desc) == 104, "rt_instance_desc layout");
-static_assert(sizeof(rt_material_desc) == 328, "rt_material_desc layout");
+static_assert(sizeof(rt_material_desc) == 376, "rt_material_desc layout");
+static_assert(sizeof(rt_curves_desc) == 40, "rt_curves_desc layout");
 static_assert(sizeof(rt_medium_desc) == 136, "rt_medium_desc layout");
 static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
 static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
@@ -345,7 +368,7 @@ static_assert(sizeof(rt_texture_desc) == 16, "rt_texture_desc layout");
 static_assert(sizeof(rt_pattern_binding) == 16, "rt_pattern_binding layout");
 static_assert(sizeof(rt_ies_desc) == 112, "rt_ies_desc layout");
 static_assert(sizeof(rt_quadric_desc) == 168, "rt_quadric_desc layout");
-static_assert(sizeof(rt_scene_desc) == 328, "rt_scene_desc layout");
+static_assert(sizeof(rt_scene_desc) == 344, "rt_scene_desc layout");
 }
 #endif
 

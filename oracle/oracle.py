@@ -65,6 +65,11 @@ def lib():
         L.oracle_hg_phase.argtypes = [C.c_double, C.c_uint64, vp, vp]
         L.oracle_hg_sample.argtypes = [C.c_double, vp, C.c_uint64, vp, vp]
         L.oracle_sss_medium.argtypes = [vp, vp, vp, vp]
+        L.oracle_hair_eval.argtypes = [vp, C.c_uint64, vp, vp, vp]
+        L.oracle_hair_sample.argtypes = [vp, vp, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, vp]
+        L.oracle_fiber_h.restype = C.c_double
+        L.oracle_fiber_h.argtypes = [vp, vp, vp]
+        L.oracle_curve_segment.argtypes = [vp, vp, C.c_double, C.c_double, C.c_uint64, vp, vp]
         _lib = L
     return _lib
 
@@ -136,6 +141,52 @@ def sss_medium(color, dmfp):
     sa, ss = np.zeros(3), np.zeros(3)
     lib().oracle_sss_medium(c.ctypes.data, m.ctypes.data, sa.ctypes.data, ss.ctypes.data)
     return sa, ss
+
+
+def _hair_params(sigma_a, beta_m, beta_n, eta):
+    p, _ = _f64(list(np.broadcast_to(np.asarray(sigma_a, float), 3)) + [beta_m, beta_n, eta])
+    return p
+
+
+def hair_eval(params, wo, wi, h):
+    """hair::f and hair::pdf for rows of (wo, wi, h); params = (sigma_a,
+    beta_m, beta_n, eta)."""
+    p = _hair_params(*params)
+    wo, wi = np.atleast_2d(wo), np.atleast_2d(wi)
+    n = max(len(wo), len(wi))
+    q, _ = _f64(np.concatenate([np.broadcast_to(wo, (n, 3)), np.broadcast_to(wi, (n, 3)),
+                                np.broadcast_to(np.reshape(h, (-1, 1)), (n, 1))], axis=1))
+    f, pdf = np.zeros((n, 3)), np.zeros(n)
+    lib().oracle_hair_eval(p.ctypes.data, n, q.ctypes.data, f.ctypes.data, pdf.ctypes.data)
+    return f, pdf
+
+
+def hair_sample(params, wo, h, pixel, sample, n):
+    """n draws of hair::sample: (wi, f, pdf), pdf 0 for failed draws."""
+    p = _hair_params(*params)
+    w, _ = _f64(wo)
+    out = np.zeros((n, 7))
+    lib().oracle_hair_sample(p.ctypes.data, w.ctypes.data, float(h), int(pixel), int(sample), int(n), out.ctypes.data)
+    return out[:, :3], out[:, 3:6], out[:, 6]
+
+
+def fiber_h(tangent, normal, wo):
+    t, _ = _f64(tangent)
+    n, _ = _f64(normal)
+    w, _ = _f64(wo)
+    return lib().oracle_fiber_h(t.ctypes.data, n.ctypes.data, w.ctypes.data)
+
+
+def curve_segment(p0, p1, v0, v1, origins, directions):
+    """One rounded-cone segment against rays: rows of (t or -1, normal,
+    tangent, v)."""
+    a, _ = _f64(p0)
+    b, _ = _f64(p1)
+    r, _ = _f64(np.concatenate([np.atleast_2d(origins), np.atleast_2d(directions)], axis=1))
+    out = np.zeros((len(r), 8))
+    lib().oracle_curve_segment(a.ctypes.data, b.ctypes.data, float(v0), float(v1), len(r), r.ctypes.data,
+                               out.ctypes.data)
+    return out
 
 
 def quadric_intersect(desc, origins, directions):

@@ -489,8 +489,106 @@ struct Mesh {
     }
 };
 
+// ---- curve sets (src/geometry/curves.rs) ------------------------------------
+// Rounded-cone segments: a sphere swept from p0 to p1 with its radius going
+// linearly from r0 to r1 (curves.rs:15-26).
+struct CurveSet {
+    std::vector<float> p0, p1;  // xyz + radius per segment
+    std::vector<float> v0, v1;  // curve parameter at each end
+    Bvh blas;
+    Aabb local_bounds;
+
+    size_t segments() const { return v0.size(); }
+    void build() {  // curves.rs:29-62: boxes of the two end spheres
+        std::vector<Aabb> bounds(segments());
+        for (size_t k = 0; k < segments(); k++) {
+            Aabb b;
+            for (const float* e : {&p0[4 * k], &p1[4 * k]}) {
+                const double r = e[3];
+                b.grow_point(V3{(double)e[0] - r, (double)e[1] - r, (double)e[2] - r});
+                b.grow_point(V3{(double)e[0] + r, (double)e[1] + r, (double)e[2] + r});
+            }
+            bounds[k] = b;
+            local_bounds.grow(b);
+        }
+        blas.build(bounds);
+    }
+
+    // curves.rs:171-188
+    static bool sphere_hit(const Ray& r, V3 c, double radius, double t_max, double* t_out, V3* n_out) {
+        V3 oc = r.o - c;
+        double a = dot(r.d, r.d), b = dot(oc, r.d), cc = dot(oc, oc) - radius * radius;
+        double disc = b * b - a * cc;
+        if (disc < 0.0) return false;
+        double sq = std::sqrt(disc);
+        double t = (-b - sq) / a;
+        if (t <= 1e-9) t = (-b + sq) / a;
+        if (t <= 1e-9 || t >= t_max) return false;
+        *t_out = t;
+        *n_out = normalize(r.o + r.d * t - c);
+        return true;
+    }
+
+    // curves.rs:107-169: Quilez's rounded cone, parametric t along the
+    // (unnormalised) local ray, outward normal.
+    static bool rounded_cone(const Ray& r, V3 pa, double ra, V3 pb, double rb, double t_max, double* t_out,
+                             V3* n_out) {
+        V3 ba = pb - pa, oa = r.o - pa;
+        double rr = ra - rb;
+        double m0 = dot(ba, ba), m1 = dot(ba, oa), m2 = dot(ba, r.d), m3 = dot(r.d, oa), m5 = dot(oa, oa);
+        double dd = dot(r.d, r.d);
+        if (m0 < 1e-24) return sphere_hit(r, pa, std::fmax(ra, rb), t_max, t_out, n_out);
+        double d2 = m0 - rr * rr;
+        double k2 = d2 * dd - m2 * m2;
+        double k1 = d2 * m3 - m1 * m2 + m2 * rr * ra;
+        double k0 = d2 * m5 - m1 * m1 + m1 * rr * ra * 2.0 - m0 * ra * ra;
+        if (std::fabs(k2) > 1e-24) {
+            double h = k1 * k1 - k0 * k2;
+            if (h >= 0.0) {
+                double t = (-k1 - std::sqrt(h)) / k2;
+                double y = m1 + t * m2;
+                if (t > 1e-9 && t < t_max && y > 0.0 && y < d2) {
+                    *t_out = t;
+                    *n_out = normalize((oa + r.d * t) * d2 - ba * y);
+                    return true;
+                }
+            }
+        }
+        // Caps: the start sphere owns y <= 0, the end sphere y >= d2.
+        bool any = false;
+        double tb = t_max, t;
+        V3 n;
+        if (sphere_hit(r, pa, ra, t_max, &t, &n) && m1 + t * m2 <= 0.0) {
+            any = true;
+            tb = t;
+            *t_out = t;
+            *n_out = n;
+        }
+        if (sphere_hit(r, pb, rb, tb, &t, &n) && m1 + t * m2 >= d2) {
+            any = true;
+            *t_out = t;
+            *n_out = n;
+        }
+        return any;
+    }
+
+    // curves.rs:67-101: hit t, outward normal, tangent, curve parameter v.
+    bool intersect_segment(const Ray& r, uint32_t k, double t_max, double* t, V3* n, V3* tang, double* v) const {
+        const float *a = &p0[4 * k], *b = &p1[4 * k];
+        V3 pa{a[0], a[1], a[2]}, pb{b[0], b[1], b[2]};
+        if (!rounded_cone(r, pa, a[3], pb, b[3], t_max, t, n)) return false;
+        V3 axis = pb - pa;
+        double len2 = length_sq(axis);
+        double along = len2 > 1e-24 ? std::min(std::max(dot(r.o + r.d * *t - pa, axis) / len2, 0.0), 1.0) : 0.5;
+        *v = (double)v0[k] + (double)(v1[k] - v0[k]) * along;
+        *tang = len2 > 1e-24 ? normalize(axis) : V3{0, 0, 1};
+        return true;
+    }
+};
+
 struct Instance {
     uint32_t mesh_id = 0, material_id = 0;
+    bool curves = false;  // GeomKind::Curves: mesh_id indexes the curve sets
     M4 transform, inv;
     Aabb world_bounds;
     double scale = 1.0;  // Matrix4::approx_scale (math/matrix.rs:246-251)
@@ -896,6 +994,7 @@ struct Hit {
     double st[2] = {0.0, 0.0};
     double st_density = 0.0;  // st units per world unit (0 without st)
     V3 st_grad[2] = {{0, 0, 0}, {0, 0, 0}};  // world-space gradients of s and t
+    V3 tangent{0, 0, 0};                        // curve tangent (zero for surfaces)
 };
 
 // ---- patterns (src/texture/pattern.rs, src/geometry/displace.rs) -------------
@@ -1769,11 +1868,14 @@ struct Pbr {
     double presence;
     double subsurface_gain = 0.0;
     V3 subsurface_color, subsurface_dmfp;
+    V3 hair_sigma_a;
+    double hair_beta_m = 0.3, hair_beta_n = 0.3, hair_eta = 1.55;
     // Material fields
     V3 emission;
     int32_t area_light;
     uint32_t id;
     int32_t interior = -1;  // Material::interior (material.rs:35-37), -1 for none
+    bool hair = false;      // Material::hair (Marschner on curve hits)
 
     static Pbr from(const rt_material_desc& m) {
         Pbr p;
@@ -1801,6 +1903,11 @@ struct Pbr {
         p.subsurface_color = v3(m.subsurface_color);
         p.subsurface_dmfp = v3(m.subsurface_dmfp);
         p.interior = m.interior;
+        p.hair = m.hair != 0;
+        p.hair_sigma_a = v3(m.hair_sigma_a);
+        p.hair_beta_m = m.hair_beta_m;
+        p.hair_beta_n = m.hair_beta_n;
+        p.hair_eta = m.hair_eta;
         return p;
     }
     // pbr.rs:86-96
@@ -2092,6 +2199,210 @@ static bool sample_bsdf(const Pbr& p, V3 wo, double eta, Pcg32& rng, BsdfSample*
     return true;
 }
 
+// ---- hair (src/raytracer/pt/hair.rs) --------------------------------------
+// Marschner / d'Eon / pbrt-v3 hair: R, TT, TRT lobes and a residual, in the
+// fiber frame (x along the fiber); f is per solid angle with no cosine.
+static const int HAIR_PMAX = 3;
+
+struct HairParams {  // hair.rs:24-55
+    V3 sigma_a;
+    double beta_m = 0.3, beta_n = 0.3, eta = 1.55;
+    double v[HAIR_PMAX + 1] = {0, 0, 0, 0};
+    double s = 0.0;
+    void init(V3 sa, double bm, double bn, double e) {
+        sigma_a = sa;
+        beta_m = std::min(std::max(bm, 0.01), 1.0);
+        beta_n = std::min(std::max(bn, 0.01), 1.0);
+        eta = e;
+        double v0 = 0.726 * beta_m + 0.812 * beta_m * beta_m + 3.7 * std::pow(beta_m, 20);
+        v0 *= v0;
+        v[0] = v0;
+        v[1] = 0.25 * v0;
+        v[2] = 4.0 * v0;
+        v[3] = 4.0 * v0;
+        s = 0.626657069 * (0.265 * beta_n + 1.194 * beta_n * beta_n + 5.372 * std::pow(beta_n, 22));
+    }
+};
+
+static double hair_i0(double x) {  // hair.rs:104-118 (series to 10 terms)
+    double val = 0.0, x2i = 1.0, ifact = 1.0, i4 = 1.0;
+    for (int i = 0; i < 10; i++) {
+        if (i > 1) ifact *= i;
+        val += x2i / (i4 * ifact * ifact);
+        x2i *= x * x;
+        i4 *= 4.0;
+    }
+    return val;
+}
+static double hair_log_i0(double x) {  // hair.rs:120-126
+    if (x > 12.0) return x + 0.5 * (-std::log(2.0 * PI * x) + 1.0 / (8.0 * x));
+    return std::log(hair_i0(x));
+}
+// hair.rs:129-137: energy-conserving longitudinal lobe.
+static double hair_mp(double cos_ti, double cos_to, double sin_ti, double sin_to, double v) {
+    double a = cos_ti * cos_to / v, b = sin_ti * sin_to / v;
+    if (v <= 0.1) return std::exp(hair_log_i0(a) - b - 1.0 / v + 0.6931 + std::log(1.0 / (2.0 * v)));
+    return std::exp(-b) * hair_i0(a) / (std::sinh(1.0 / v) * 2.0 * v);
+}
+static double hair_fr(double cos_i, double eta_i, double eta_t) {  // hair.rs:139-157
+    cos_i = std::min(std::max(cos_i, -1.0), 1.0);
+    if (cos_i <= 0.0) {
+        std::swap(eta_i, eta_t);
+        cos_i = -cos_i;
+    }
+    double sin_i = std::sqrt(std::fmax(1.0 - cos_i * cos_i, 0.0));
+    double sin_t = eta_i / eta_t * sin_i;
+    if (sin_t >= 1.0) return 1.0;
+    double cos_t = std::sqrt(std::fmax(1.0 - sin_t * sin_t, 0.0));
+    double rpa = (eta_t * cos_i - eta_i * cos_t) / (eta_t * cos_i + eta_i * cos_t);
+    double rpe = (eta_i * cos_i - eta_t * cos_t) / (eta_i * cos_i + eta_t * cos_t);
+    return (rpa * rpa + rpe * rpe) / 2.0;
+}
+// hair.rs:160-183: attenuation per lobe, then the residual's geometric series.
+static void hair_ap(double cos_to, double eta, double h, V3 t, V3 out[HAIR_PMAX + 1]) {
+    double cos_gamma_o = std::sqrt(std::fmax(1.0 - h * h, 0.0));
+    double f = hair_fr(cos_to * cos_gamma_o, 1.0, eta);
+    out[0] = V3{f, f, f};
+    out[1] = t * ((1.0 - f) * (1.0 - f));
+    for (int p = 2; p < HAIR_PMAX; p++) out[p] = out[p - 1] * t * f;
+    V3 last = out[HAIR_PMAX - 1];
+    out[HAIR_PMAX] = V3{last.x * f * t.x / std::fmax(1.0 - t.x * f, 1e-6), last.y * f * t.y / std::fmax(1.0 - t.y * f, 1e-6),
+                        last.z * f * t.z / std::fmax(1.0 - t.z * f, 1e-6)};
+}
+static double hair_logistic(double x, double s) {  // hair.rs:185-189
+    x = std::fabs(x);
+    double e = std::exp(-x / s);
+    return e / (s * (1.0 + e) * (1.0 + e));
+}
+static double hair_logistic_cdf(double x, double s) { return 1.0 / (1.0 + std::exp(-x / s)); }
+static double hair_trimmed_logistic(double x, double s, double a, double b) {
+    return hair_logistic(x, s) / (hair_logistic_cdf(b, s) - hair_logistic_cdf(a, s));
+}
+static double hair_sample_trimmed_logistic(double u, double s, double a, double b) {  // hair.rs:199-203
+    double k = hair_logistic_cdf(b, s) - hair_logistic_cdf(a, s);
+    double x = -s * std::log(1.0 / std::min(std::max(u * k + hair_logistic_cdf(a, s), 1e-9), 1.0 - 1e-9) - 1.0);
+    return std::min(std::max(x, a), b);
+}
+static double hair_phi(int p, double gamma_o, double gamma_t) { return 2.0 * p * gamma_t - 2.0 * gamma_o + p * PI; }
+static double hair_np(double phi, int p, double s, double gamma_o, double gamma_t) {  // hair.rs:211-220
+    double dphi = phi - hair_phi(p, gamma_o, gamma_t);
+    while (dphi > PI) dphi -= 2.0 * PI;
+    while (dphi < -PI) dphi += 2.0 * PI;
+    return hair_trimmed_logistic(dphi, s, -PI, PI);
+}
+struct HairGeom {  // hair.rs:224-258
+    double sin_to, cos_to, phi_o, gamma_o, gamma_t;
+    V3 t;
+};
+static HairGeom hair_geom(const HairParams& hp, V3 wo, double h) {
+    HairGeom g;
+    g.sin_to = std::min(std::max(wo.x, -1.0), 1.0);
+    g.cos_to = std::sqrt(std::fmax(1.0 - g.sin_to * g.sin_to, 0.0));
+    g.phi_o = std::atan2(wo.z, wo.y);
+    g.gamma_o = std::asin(std::min(std::max(h, -1.0), 1.0));
+    double sin_tt = g.sin_to / hp.eta;
+    double cos_tt = std::sqrt(std::fmax(1.0 - sin_tt * sin_tt, 0.0));
+    double etap = std::sqrt(std::fmax(hp.eta * hp.eta - g.sin_to * g.sin_to, 0.0)) / std::fmax(g.cos_to, 1e-9);
+    double sin_gt = std::min(std::max(h / etap, -1.0), 1.0);
+    double cos_gt = std::sqrt(std::fmax(1.0 - sin_gt * sin_gt, 0.0));
+    g.gamma_t = std::asin(sin_gt);
+    double l = 2.0 * cos_gt / std::fmax(cos_tt, 1e-9);
+    g.t = exp3(hp.sigma_a, l);
+    return g;
+}
+static V3 hair_f(const HairParams& hp, V3 wo, V3 wi, double h) {  // hair.rs:262-281
+    HairGeom g = hair_geom(hp, wo, h);
+    double sin_ti = std::min(std::max(wi.x, -1.0), 1.0);
+    double cos_ti = std::sqrt(std::fmax(1.0 - sin_ti * sin_ti, 0.0));
+    double phi = std::atan2(wi.z, wi.y) - g.phi_o;
+    V3 a[HAIR_PMAX + 1];
+    hair_ap(g.cos_to, hp.eta, h, g.t, a);
+    V3 out{0, 0, 0};
+    for (int p = 0; p <= HAIR_PMAX; p++) {
+        double m = hair_mp(cos_ti, g.cos_to, sin_ti, g.sin_to, hp.v[p]);
+        double n = p < HAIR_PMAX ? hair_np(phi, p, hp.s, g.gamma_o, g.gamma_t) : 1.0 / (2.0 * PI);
+        out = out + a[p] * (m * n);
+    }
+    return out;
+}
+static void hair_ap_pdf(const HairParams& hp, const HairGeom& g, double h, double w[HAIR_PMAX + 1]) {  // :284-302
+    V3 a[HAIR_PMAX + 1];
+    hair_ap(g.cos_to, hp.eta, h, g.t, a);
+    double total = 0.0;
+    for (int p = 0; p <= HAIR_PMAX; p++) total += (w[p] = lum(a[p]));
+    if (total > 1e-12) {
+        for (int p = 0; p <= HAIR_PMAX; p++) w[p] /= total;
+    } else {
+        for (int p = 0; p <= HAIR_PMAX; p++) w[p] = p == 0 ? 1.0 : 0.0;
+    }
+}
+static double hair_pdf(const HairParams& hp, V3 wo, V3 wi, double h) {  // hair.rs:305-324
+    HairGeom g = hair_geom(hp, wo, h);
+    double sin_ti = std::min(std::max(wi.x, -1.0), 1.0);
+    double cos_ti = std::sqrt(std::fmax(1.0 - sin_ti * sin_ti, 0.0));
+    double phi = std::atan2(wi.z, wi.y) - g.phi_o;
+    double w[HAIR_PMAX + 1];
+    hair_ap_pdf(hp, g, h, w);
+    double out = 0.0;
+    for (int p = 0; p <= HAIR_PMAX; p++) {
+        double m = hair_mp(cos_ti, g.cos_to, sin_ti, g.sin_to, hp.v[p]);
+        double n = p < HAIR_PMAX ? hair_np(phi, p, hp.s, g.gamma_o, g.gamma_t) : 1.0 / (2.0 * PI);
+        out += w[p] * m * n;
+    }
+    return std::fmax(out, 0.0);
+}
+// hair.rs:327-374: lobe by attenuation energy, d'Eon's longitudinal
+// inverse, trimmed-logistic azimuth; false when the pdf vanishes.
+template <class R>
+static bool hair_sample(const HairParams& hp, V3 wo, double h, R& rng, V3* wi_out, V3* f_out, double* pdf_out) {
+    HairGeom g = hair_geom(hp, wo, h);
+    double w[HAIR_PMAX + 1];
+    hair_ap_pdf(hp, g, h, w);
+    double u = rng.next_f64();
+    int p = HAIR_PMAX;
+    for (int i = 0; i <= HAIR_PMAX; i++) {
+        if (u < w[i]) {
+            p = i;
+            break;
+        }
+        u -= w[i];
+    }
+    double v = hp.v[p];
+    double u1 = std::fmax(rng.next_f64(), 1e-9);
+    double u2 = rng.next_f64();
+    double cos_theta = 1.0 + v * std::log(u1 + (1.0 - u1) * std::exp(-2.0 / v));
+    double sin_theta = std::sqrt(std::fmax(1.0 - cos_theta * cos_theta, 0.0));
+    double cos_phi_l = std::cos(2.0 * PI * u2);
+    double sin_ti = -cos_theta * g.sin_to + sin_theta * cos_phi_l * g.cos_to;
+    double cos_ti = std::sqrt(std::fmax(1.0 - sin_ti * sin_ti, 0.0));
+    double u3 = rng.next_f64();
+    double dphi = p < HAIR_PMAX ? hair_phi(p, g.gamma_o, g.gamma_t) + hair_sample_trimmed_logistic(u3, hp.s, -PI, PI)
+                                : 2.0 * PI * u3;
+    double phi_i = g.phi_o + dphi;
+    V3 wi{sin_ti, cos_ti * std::cos(phi_i), cos_ti * std::sin(phi_i)};
+    double pdf = hair_pdf(hp, wo, wi, h);
+    if (pdf <= 1e-12) return false;
+    *wi_out = wi;
+    *f_out = hair_f(hp, wo, wi, h);
+    *pdf_out = pdf;
+    return true;
+}
+struct FiberFrame {  // hair.rs:378-411
+    V3 x, y, z;
+    double h;
+    FiberFrame(V3 tangent, V3 n, V3 wo) {
+        x = normalize(tangent);
+        V3 zz = wo - x * dot(wo, x);
+        if (length_sq(zz) < 1e-12) zz = n - x * dot(n, x);
+        z = normalize(zz);
+        y = normalize(cross(z, x));
+        V3 n_perp = normalize(n - x * dot(n, x));
+        h = std::min(std::max(dot(n_perp, y), -1.0), 1.0);
+    }
+    V3 to_local(V3 w) const { return {dot(w, x), dot(w, y), dot(w, z)}; }
+    V3 to_world(V3 w) const { return x * w.x + y * w.y + z * w.z; }
+};
+
 // ---- scene ------------------------------------------------------------------
 
 struct Camera {
@@ -2138,6 +2449,7 @@ struct Camera {
 
 struct Scene {
     std::vector<Mesh> meshes;
+    std::vector<CurveSet> curve_sets;
     std::vector<Instance> instances;
     std::vector<Quadric> quadrics;
     std::vector<Pbr> materials;
@@ -2158,7 +2470,7 @@ struct Scene {
     bool is_hull(uint32_t material_id) const {
         const Pbr& m = materials[material_id];
         double w[5];
-        return m.interior >= 0 && !m.lobe_weights(w) && max_comp(m.emission + m.glow) <= 0.0;
+        return m.interior >= 0 && !m.hair && !m.lobe_weights(w) && max_comp(m.emission + m.glow) <= 0.0;
     }
 
     // shade_params (pt/mod.rs:389-439): the material with its pattern
@@ -2185,6 +2497,20 @@ struct Scene {
         for (const auto& b : bindings[h.material_id])
             p.apply(b.first, pattern_eval(patterns, textures, b.second, c, 0));
         return p;
+    }
+
+    const Bvh& blas_of(const Instance& in) const {
+        return in.curves ? curve_sets[in.mesh_id].blas : meshes[in.mesh_id].blas;
+    }
+    // One primitive of an instance against the local ray (mesh.rs:311-333):
+    // a triangle (u, v its barycentrics) or a curve segment.
+    bool prim_isect(const Instance& in, const Ray& lr, uint32_t p, double t_max, double* t, double* u,
+                    double* v) const {
+        if (in.curves) {
+            V3 n, tg;
+            return curve_sets[in.mesh_id].intersect_segment(lr, p, t_max, t, &n, &tg, v);
+        }
+        return meshes[in.mesh_id].intersect_triangle(lr, p, t_max, t, u, v);
     }
 
     // scene/mod.rs:105-146, the scan of `objects`: the closest quadric hit
@@ -2233,14 +2559,13 @@ struct Scene {
             const Instance& in = instances[ii];
             if (c) c->insts++;
             Ray lr{xf_point(in.inv, ray.o), xf_vec(in.inv, ray.d)};
-            const Mesh& m = meshes[in.mesh_id];
             double hu = 0, hv = 0;
             uint32_t tri;
             double t;
             auto tri_isect = [&](uint32_t tr, double tmax, double* to) -> bool {
                 if (c) c->tris++;
-                double tt, uu, vv;
-                if (m.intersect_triangle(lr, tr, tmax, &tt, &uu, &vv)) {
+                double tt, uu = 0, vv = 0;
+                if (prim_isect(in, lr, tr, tmax, &tt, &uu, &vv)) {
                     hu = uu;
                     hv = vv;
                     *to = tt;
@@ -2248,7 +2573,7 @@ struct Scene {
                 }
                 return false;
             };
-            if (!m.blas.traverse(lr.o, lr.d, t_max, tri_isect, &tri, &t, c)) return false;
+            if (!blas_of(in).traverse(lr.o, lr.d, t_max, tri_isect, &tri, &t, c)) return false;
             best = {ii, tri, hu, hv};
             *t_out = t;
             return true;
@@ -2258,6 +2583,31 @@ struct Scene {
         if (!tlas.traverse(ray.o, ray.d, t_budget, inst_isect, &winner, &tw, c)) return have_q;
         if (have_q && !(length(ray.d * tw) < out->t)) return true;
         const Instance& in = instances[best.inst];
+        if (in.curves) {
+            // mesh.rs:323-344: the segment's normal and tangent, st = (0.5, v).
+            const CurveSet& cs = curve_sets[in.mesh_id];
+            Ray lr{xf_point(in.inv, ray.o), xf_vec(in.inv, ray.d)};
+            double t, v;
+            V3 n, tg;
+            cs.intersect_segment(lr, best.tri, INF, &t, &n, &tg, &v);
+            V3 wn = normalize(xf_normal(in.inv, n));
+            V3 point = ray.o + ray.d * tw;
+            bool front = dot(wn, ray.d) < 0.0;
+            if (!front) wn = -wn;
+            out->t = length(point - ray.o);
+            out->point = point;
+            out->normal = normalize(wn);
+            out->material_id = in.material_id;
+            out->inst = best.inst;
+            out->prim = best.tri;
+            out->front_face = front;
+            out->st[0] = 0.5;
+            out->st[1] = v;
+            out->st_density = 0.0;
+            out->st_grad[0] = out->st_grad[1] = V3{0, 0, 0};
+            out->tangent = normalize(xf_vec(in.transform, tg));
+            return true;
+        }
         const Mesh& m = meshes[in.mesh_id];
         V3 ln = m.local_normal(best.tri, best.u, best.v);
         V3 wn = normalize(xf_normal(in.inv, ln));
@@ -2317,15 +2667,14 @@ struct Scene {
             const Instance& in = instances[ii];
             if (c) c->insts++;
             Ray lr{xf_point(in.inv, ray.o), xf_vec(in.inv, ray.d)};
-            const Mesh& m = meshes[in.mesh_id];
             uint32_t tri;
             double t;
             auto tri_isect = [&](uint32_t tr, double tm, double* tt) -> bool {
                 if (c) c->tris++;
                 double uu, vv;
-                return m.intersect_triangle(lr, tr, tm, tt, &uu, &vv);
+                return prim_isect(in, lr, tr, tm, tt, &uu, &vv);
             };
-            if (!m.blas.traverse(lr.o, lr.d, tmax, tri_isect, &tri, &t, c)) return false;
+            if (!blas_of(in).traverse(lr.o, lr.d, tmax, tri_isect, &tri, &t, c)) return false;
             bi = ii;
             bt = tri;
             *to = t;
@@ -2351,11 +2700,10 @@ struct Scene {
             const Instance& in = instances[ii];
             if (c) c->insts++;
             Ray lr{xf_point(in.inv, o), xf_vec(in.inv, d)};
-            const Mesh& m = meshes[in.mesh_id];
-            return m.blas.any_hit(lr.o, lr.d, lim, [&](uint32_t tr, double l2) -> bool {
+            return blas_of(in).any_hit(lr.o, lr.d, lim, [&](uint32_t tr, double l2) -> bool {
                 if (c) c->tris++;
                 double t, u, v;
-                return m.intersect_triangle(lr, tr, l2, &t, &u, &v);
+                return prim_isect(in, lr, tr, l2, &t, &u, &v);
             }, c);
         };
         return tlas.any_hit(o, d, t_limit, inst_hit, c);
@@ -2578,7 +2926,7 @@ struct Tracer {
         return {0, 0, 0};
     }
 
-    // mod.rs:449-990 trace_full (hair excluded).
+    // mod.rs:449-990 trace_full.
     V3 trace(Ray ray, Pcg32& rng, Aux& aux) {
         V3 L{0, 0, 0};
         int first_specular = -1;  // -1 None, 0 false, 1 true
@@ -2764,7 +3112,42 @@ struct Tracer {
             // subsurfaceGain an isotropic random walk inside the object through
             // the Burley-fit homogeneous medium, leaving diffusely where the
             // walk first reaches a surface.
-            if (pbr.subsurface_gain > 0.0 &&
+            // Hair fibers scatter over the whole sphere with their own BSDF
+            // (mod.rs:737-781), on curve hits only.
+            if (pbr.hair && length_sq(hit.tangent) > 0.5) {
+                HairParams hp;
+                hp.init(pbr.hair_sigma_a, pbr.hair_beta_m, pbr.hair_beta_n, pbr.hair_eta);
+                const FiberFrame ff(hit.tangent, hit.normal, wo);
+                const V3 wo_f = ff.to_local(wo);
+                const double hh = ff.h;
+                if (!sc.lights.empty()) {
+                    auto eval = [&](V3 wi, double* pdf) -> V3 {
+                        const V3 wf = ff.to_local(wi);
+                        *pdf = hair_pdf(hp, wo_f, wf, hh);
+                        return hair_f(hp, wo_f, wf, hh);
+                    };
+                    uint32_t li;
+                    double pmf;
+                    if (sc.ls.sample(hit.point, rng.next_f64(), &li, &pmf))
+                        emit(beta * sample_light(sc.lights[li], hit.point, n, eval, pmf, medium, rng));
+                }
+                V3 wi_f, fv;
+                double pv;
+                if (!hair_sample(hp, wo_f, hh, rng, &wi_f, &fv, &pv)) break;
+                const V3 wi = ff.to_world(wi_f);
+                beta = beta * fv / pv;  // f is per solid angle: no cosine
+                if (first_specular < 0) first_specular = 0;
+                prev_pdf = pv;
+                prev_origin = hit.point;
+                from_camera = false;
+                cone_spread += 0.4;
+                const V3 side = dot(wi, hit.normal) >= 0.0 ? hit.normal : -hit.normal;
+                ray = make_ray(hit.point + side * RAY_OFFSET, wi);
+                depth++;
+                if (!roulette()) break;
+                continue;
+            }
+            if (pbr.subsurface_gain > 0.0 && !pbr.hair &&
                 rng.next_f64() < std::min(std::max(pbr.subsurface_gain, 0.0), 1.0)) {
                 if (first_specular < 0) first_specular = 0;
                 const Medium sss = sss_medium(pbr.subsurface_color, pbr.subsurface_dmfp);
@@ -2986,12 +3369,23 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
         if (md.st) m.st.assign(md.st, md.st + 2ull * md.n_vertices);
         m.build();
     }
+    s.curve_sets.resize(d->curves ? d->n_curves : 0);
+    for (uint32_t k = 0; k < s.curve_sets.size(); k++) {
+        const rt_curves_desc& cd = d->curves[k];
+        CurveSet& cs = s.curve_sets[k];
+        cs.p0.assign(cd.p0, cd.p0 + 4ull * cd.n_segments);
+        cs.p1.assign(cd.p1, cd.p1 + 4ull * cd.n_segments);
+        cs.v0.assign(cd.v0, cd.v0 + cd.n_segments);
+        cs.v1.assign(cd.v1, cd.v1 + cd.n_segments);
+        cs.build();
+    }
     s.instances.resize(d->n_instances);
     std::vector<Aabb> ib(d->n_instances);
     for (uint32_t i = 0; i < d->n_instances; i++) {
         const rt_instance_desc& id = d->instances[i];
         Instance& in = s.instances[i];
-        in.mesh_id = id.mesh_id;
+        in.curves = id.mesh_id >= d->n_meshes;
+        in.mesh_id = in.curves ? id.mesh_id - d->n_meshes : id.mesh_id;
         in.material_id = id.material_id;
         in.transform = identity();
         for (int r = 0; r < 3; r++)
@@ -3001,7 +3395,7 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
                lz = length(xf_vec(in.transform, V3{0, 0, 1}));
         in.scale = std::fmax(std::cbrt(lx * ly * lz), 1e-12);
         // mesh.rs:283-297 world bounds from the 8 transformed corners.
-        const Aabb& lb = s.meshes[in.mesh_id].local_bounds;
+        const Aabb& lb = in.curves ? s.curve_sets[in.mesh_id].local_bounds : s.meshes[in.mesh_id].local_bounds;
         for (int k = 0; k < 8; k++) {
             V3 corner{(k & 1) ? lb.mx.x : lb.mn.x, (k & 2) ? lb.mx.y : lb.mn.y, (k & 4) ? lb.mx.z : lb.mn.z};
             in.world_bounds.grow_point(xf_point(in.transform, corner));
@@ -3490,5 +3884,60 @@ void oracle_sss_medium(const double* color, const double* dmfp, double* sigma_a,
     Medium m = sss_medium(v3(color), v3(dmfp));
     sigma_a[0] = m.sigma_a.x, sigma_a[1] = m.sigma_a.y, sigma_a[2] = m.sigma_a.z;
     sigma_s[0] = m.sigma_s.x, sigma_s[1] = m.sigma_s.y, sigma_s[2] = m.sigma_s.z;
+}
+
+static HairParams hair_params(const double* p) {
+    HairParams hp;
+    hp.init(v3(p), p[3], p[4], p[5]);
+    return hp;
+}
+
+void oracle_hair_eval(const double* params, uint64_t n, const double* q, double* f, double* pdf) {
+    const HairParams hp = hair_params(params);
+    for (uint64_t i = 0; i < n; i++) {
+        const double* r = q + 7 * i;
+        V3 v = hair_f(hp, v3(r), v3(r + 3), r[6]);
+        f[3 * i] = v.x, f[3 * i + 1] = v.y, f[3 * i + 2] = v.z;
+        pdf[i] = hair_pdf(hp, v3(r), v3(r + 3), r[6]);
+    }
+}
+
+void oracle_hair_sample(const double* params, const double* wo, double h, uint64_t pixel, uint64_t sample,
+                        uint64_t n, double* out) {
+    const HairParams hp = hair_params(params);
+    Pcg32 rng = Pcg32::for_pixel_sample(pixel, sample);
+    for (uint64_t i = 0; i < n; i++) {
+        V3 wi{0, 0, 0}, fv{0, 0, 0};
+        double pdf = 0.0;
+        if (!hair_sample(hp, v3(wo), h, rng, &wi, &fv, &pdf)) pdf = 0.0;
+        double* o = out + 7 * i;
+        o[0] = wi.x, o[1] = wi.y, o[2] = wi.z, o[3] = fv.x, o[4] = fv.y, o[5] = fv.z, o[6] = pdf;
+    }
+}
+
+double oracle_fiber_h(const double* tangent, const double* normal, const double* wo) {
+    return FiberFrame(v3(tangent), v3(normal), v3(wo)).h;
+}
+
+void oracle_curve_segment(const double* p0, const double* p1, double v0, double v1, uint64_t n, const double* rays,
+                          double* out) {
+    CurveSet cs;
+    for (int k = 0; k < 4; k++) {
+        cs.p0.push_back((float)p0[k]);
+        cs.p1.push_back((float)p1[k]);
+    }
+    cs.v0.push_back((float)v0);
+    cs.v1.push_back((float)v1);
+    for (uint64_t i = 0; i < n; i++) {
+        Ray r{v3(rays + 6 * i), v3(rays + 6 * i + 3)};
+        double t, v;
+        V3 nn, tg;
+        double* o = out + 8 * i;
+        if (cs.intersect_segment(r, 0, INF, &t, &nn, &tg, &v)) {
+            o[0] = t, o[1] = nn.x, o[2] = nn.y, o[3] = nn.z, o[4] = tg.x, o[5] = tg.y, o[6] = tg.z, o[7] = v;
+        } else {
+            for (int k = 0; k < 8; k++) o[k] = k == 0 ? -1.0 : 0.0;
+        }
+    }
 }
 

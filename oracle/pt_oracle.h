@@ -128,6 +128,19 @@ void   oracle_hg_phase(double g, uint64_t n, const double* cos_theta, double* ou
 void   oracle_hg_sample(double g, const double* wo, uint64_t n, const double* u, double* out);
 /* sss_medium (volume.rs:259-288): sigma_a, sigma_s (3 doubles each). */
 void   oracle_sss_medium(const double* color, const double* dmfp, double* sigma_a, double* sigma_s);
+/* Hair (src/raytracer/pt/hair.rs), params = sigma_a xyz, beta_m, beta_n,
+ * eta. Per query (wo xyz, wi xyz, h): f rgb and pdf. */
+void   oracle_hair_eval(const double* params, uint64_t n, const double* q, double* f, double* pdf);
+/* n draws of hair::sample for (wo, h) from the PCG32 stream of (pixel,
+ * sample): wi xyz, f rgb, pdf (pdf 0 when the draw failed). */
+void   oracle_hair_sample(const double* params, const double* wo, double h, uint64_t pixel, uint64_t sample,
+                          uint64_t n, double* out);
+/* FiberFrame (hair.rs:378-401): h of (tangent, normal, wo). */
+double oracle_fiber_h(const double* tangent, const double* normal, const double* wo);
+/* One rounded-cone segment (curves.rs:67-169; p0, p1 = xyz radius) against
+ * n rays (origin, direction; 6 doubles): t or -1, normal xyz, tangent xyz, v. */
+void   oracle_curve_segment(const double* p0, const double* p1, double v0, double v1, uint64_t n,
+                            const double* rays, double* out);
 
 #ifdef __cplusplus
 }

@@ -53,7 +53,22 @@ class RtMaterialDesc(C.Structure):
         ("subsurface_color", c_double3),
         ("subsurface_dmfp", c_double3),
         ("interior", C.c_int32),
-        ("material_reserved", C.c_uint32),
+        ("hair", C.c_uint32),
+        ("hair_sigma_a", c_double3),
+        ("hair_beta_m", C.c_double),
+        ("hair_beta_n", C.c_double),
+        ("hair_eta", C.c_double),
+    ]
+
+
+class RtCurvesDesc(C.Structure):
+    _fields_ = [
+        ("p0", C.POINTER(C.c_float)),
+        ("p1", C.POINTER(C.c_float)),
+        ("v0", C.POINTER(C.c_float)),
+        ("v1", C.POINTER(C.c_float)),
+        ("n_segments", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 
@@ -210,6 +225,9 @@ class RtSceneDesc(C.Structure):
         ("media", C.POINTER(RtMediumDesc)),
         ("n_media", C.c_uint32),
         ("atmosphere", C.c_int32),
+        ("curves", C.POINTER(RtCurvesDesc)),
+        ("n_curves", C.c_uint32),
+        ("curves_reserved", C.c_uint32),
     ]
 
 
@@ -235,10 +253,10 @@ class RtParams(C.Structure):
 LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK, LIGHT_DOME = range(6)
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 
-for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 328), (RtLightDesc, 120),
+for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 376), (RtLightDesc, 120),
                (RtCameraDesc, 144), (RtParams, 72), (RtPatternInput, 32), (RtPatternDesc, 264),
                (RtPatternBinding, 16), (RtTextureDesc, 16), (RtIesDesc, 112), (RtQuadricDesc, 168),
-               (RtSceneDesc, 328), (RtMediumDesc, 136)):
+               (RtSceneDesc, 344), (RtMediumDesc, 136), (RtCurvesDesc, 40)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
 

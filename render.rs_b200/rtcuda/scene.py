@@ -16,6 +16,9 @@ INSTANCE_DTYPE = np.dtype([("xf", "<f8", (12,)), ("mesh", "<u4"), ("mat", "<u4")
 assert INSTANCE_DTYPE.itemsize == C.sizeof(abi.RtInstanceDesc)
 
 IDENTITY_3x4 = np.array([1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0], dtype=np.float64)
+# Curve-set handles (add_curves) as instances hold them; the descriptor maps
+# them to n_meshes + k, as rt_instance_desc numbers curve sets.
+CURVE_BASE = 1 << 30
 
 
 def _normalize(v):
@@ -33,7 +36,8 @@ def default_material():
                 glass_gain=0.0, glass_ior=1.5, glass_roughness=0.05,
                 refraction_color=(1.0, 1.0, 1.0), glow=(0.0, 0.0, 0.0), presence=1.0,
                 emission=(0.0, 0.0, 0.0), area_light=-1, id=0, subsurface_gain=0.0,
-                subsurface_color=(0.8, 0.6, 0.4), subsurface_dmfp=(0.1, 0.1, 0.1), interior=-1)
+                subsurface_color=(0.8, 0.6, 0.4), subsurface_dmfp=(0.1, 0.1, 0.1), interior=-1, hair=0,
+                hair_sigma_a=(0.0, 0.0, 0.0), hair_beta_m=0.3, hair_beta_n=0.3, hair_eta=1.55)
 
 
 def matte(color, sigma=0.0, **kw):
@@ -79,6 +83,24 @@ def emitter(radiance, area_light=-1, **kw):
     """Black, non-reflecting emitter (no lobes)."""
     m = default_material()
     m.update(diffuse_gain=0.0, specular_ior=1.0, emission=tuple(radiance), area_light=area_light)
+    m.update(kw)
+    return m
+
+
+def marschner_hair(color=None, absorption=None, roughness=0.3, azimuthal_roughness=0.3, ior=1.55, **kw):
+    """Bxdf "PxrMarschnerHair" (HairParams::from_bxdf_params, hair.rs:82-100):
+    absorption given directly or from the fiber colour (pbrt's
+    SigmaAFromReflectance); off curves the material is the brown matte the
+    reference falls back to (scene_builder.rs:1850-1860)."""
+    bn = min(max(azimuthal_roughness, 0.01), 1.0)
+    if absorption is None:
+        c = np.clip(np.asarray((0.35, 0.2, 0.06) if color is None else color, float), 1e-4, 0.999)
+        den = 5.969 - 0.215 * bn + 2.532 * bn ** 2 - 10.73 * bn ** 3 + 5.574 * bn ** 4 + 0.245 * bn ** 5
+        absorption = (np.log(c) / den) ** 2
+    sa = _rgb(absorption)
+    m = matte((0.35, 0.22, 0.12))
+    m.update(hair=1, hair_sigma_a=sa, hair_beta_m=float(roughness), hair_beta_n=float(azimuthal_roughness),
+             hair_eta=float(ior))
     m.update(kw)
     return m
 
@@ -145,6 +167,7 @@ class Scene:
         self.ies = {}             # point light index -> (v_angles, h_angles, candela[h][v], world_to_local 3x3)
         self.quadrics = []        # (type, params (<= 8), object_to_world 3x4, material)
         self.media = []           # medium dicts (see medium())
+        self.curves = []          # (p0 (n, 4) f32 xyz radius, p1, v0 (n,) f32, v1)
         self.atmosphere = -1      # index into media of the global medium, -1 for none
         # Reference default camera: origin, looking down +z (camera.rs:97-103).
         self.eye = np.zeros(3)
@@ -242,6 +265,20 @@ class Scene:
         f = abi.PATTERN_FIELDS[field] if isinstance(field, str) else int(field)
         self.bindings.append((int(material), f, int(node)))
         self._desc = None
+
+    def add_curves(self, p0, p1, v0, v1):
+        """A curve set (src/geometry/curves.rs:15-26): rounded-cone segments
+        from p0 to p1 (rows xyz + radius) with curve parameters v0, v1.
+        Returns a handle that add_instance places like a mesh id."""
+        p0 = np.ascontiguousarray(np.reshape(p0, (-1, 4)), dtype=np.float32)
+        p1 = np.ascontiguousarray(np.reshape(p1, (-1, 4)), dtype=np.float32)
+        v0 = np.ascontiguousarray(np.ravel(v0), dtype=np.float32)
+        v1 = np.ascontiguousarray(np.ravel(v1), dtype=np.float32)
+        if not (len(p0) == len(p1) == len(v0) == len(v1)):
+            raise ValueError("curve arrays of different lengths")
+        self.curves.append((p0, p1, v0, v1))
+        self._desc = None
+        return CURVE_BASE + len(self.curves) - 1
 
     def add_instance(self, mesh_id, material_id, xform=None):
         rec = np.zeros(1, dtype=INSTANCE_DTYPE)
@@ -355,7 +392,8 @@ class Scene:
         """Effective (instanced) triangles."""
         inst = self.instance_array()
         per_mesh = np.array([len(m[1]) for m in self.meshes], dtype=np.int64)
-        return int(per_mesh[inst["mesh"]].sum()) if len(inst) else 0
+        mesh = inst["mesh"][inst["mesh"] < CURVE_BASE] if len(inst) else inst["mesh"]
+        return int(per_mesh[mesh].sum()) if len(mesh) else 0
 
     def instance_array(self):
         if self._inst_chunks:
@@ -381,6 +419,10 @@ class Scene:
             mesh_arr[k].n_vertices = len(p)
             mesh_arr[k].n_triangles = len(i)
         inst = np.ascontiguousarray(self.instance_array())
+        if len(inst) and (inst["mesh"] >= CURVE_BASE).any():
+            inst = inst.copy()
+            cm = inst["mesh"] >= CURVE_BASE
+            inst["mesh"][cm] = inst["mesh"][cm] - CURVE_BASE + len(self.meshes)
         keep.append(inst)
         mat_arr = (abi.RtMaterialDesc * max(1, len(self.materials)))()
         for k, m in enumerate(self.materials):
@@ -499,5 +541,16 @@ class Scene:
             d.media = med_arr
             d.n_media = len(self.media)
         d.atmosphere = self.atmosphere
-        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr, tex_arr, ies_arr, quad_arr, med_arr)
+        cur_arr = (abi.RtCurvesDesc * max(1, len(self.curves)))()
+        for k, (p0, p1, v0, v1) in enumerate(self.curves):
+            keep += [p0, p1, v0, v1]
+            c = cur_arr[k]
+            c.p0, c.p1 = (a.ctypes.data_as(C.POINTER(C.c_float)) for a in (p0, p1))
+            c.v0, c.v1 = (a.ctypes.data_as(C.POINTER(C.c_float)) for a in (v0, v1))
+            c.n_segments = len(v0)
+        if self.curves:
+            d.curves = cur_arr
+            d.n_curves = len(self.curves)
+        self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr, tex_arr, ies_arr, quad_arr, med_arr,
+                      cur_arr)
         return d
