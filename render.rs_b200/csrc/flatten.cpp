@@ -626,10 +626,11 @@ DevMaterial fold_material(const rt_material_desc& m) {
     // cutout, the reference testing it before presence.
     d.interior = m.interior >= 0 ? (uint32_t)m.interior : 0xFFFFFFFFu;
     const bool emits = std::max({m.emission[0] + m.glow[0], m.emission[1] + m.glow[1], m.emission[2] + m.glow[2]}) > 0.0;
-    d.hull = (m.interior >= 0 && !lobes && !emits) ? 1.0f : 0.0f;
+    d.hull = (m.interior >= 0 && !m.hair && !lobes && !emits) ? 1.0f : 0.0f;
     if (d.hull != 0.0f) d.presence = 1.0f;
     // Subsurface walk: probability and the Burley-fit medium (volume.rs:259-288).
-    d.sss_gain = (float)std::min(std::max(m.subsurface_gain, 0.0), 1.0);
+    d.sss_gain = m.hair ? 0.0f : (float)std::min(std::max(m.subsurface_gain, 0.0), 1.0);
+    d.hair = 0xFFFFFFFFu;  // set by the caller with the hair table
     for (int k = 0; k < 3; k++) {
         const double a = std::min(std::max(m.subsurface_color[k], 0.0), 1.0);
         const double st = (1.85 - a + 7.0 * std::pow(std::fabs(a - 0.8), 3)) / std::max(m.subsurface_dmfp[k], 1e-5);
@@ -982,7 +983,7 @@ void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>
     auto child_boxes = [&](uint32_t i, const std::vector<std::vector<RootChild>>& list, bool split_all, Box* cb,
                            Box* u) -> uint32_t {
         const rt_instance_desc& id = d->instances[i];
-        if (!d->meshes[id.mesh_id].n_triangles) return 0;
+        if (!H->meshes[id.mesh_id].n_tris) return 0;
         const auto& rc = list[id.mesh_id];
         double sum = 0.0;
         for (size_t k = 0; k < rc.size(); k++) {
@@ -1193,17 +1194,64 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         *err = "meshes pointer is NULL";
         return false;
     }
-    // ---- BLAS per mesh -------------------------------------------------
-    std::vector<std::vector<RootChild>> root_children(d->n_meshes), grand_children(d->n_meshes);
-    H.meshes.resize(d->n_meshes);
+    if (d->n_curves && !d->curves) {
+        *err = "curves pointer is NULL";
+        return false;
+    }
+    // ---- BLAS per mesh, then per curve set (geometry n_meshes + k) ------------
+    const uint32_t n_geom = d->n_meshes + d->n_curves;
+    std::vector<std::vector<RootChild>> root_children(n_geom), grand_children(n_geom);
+    H.meshes.resize(n_geom);
     uint64_t tri_total = 0;
     for (uint32_t m = 0; m < d->n_meshes; m++) tri_total += d->meshes[m].n_triangles;
+    for (uint32_t k = 0; k < d->n_curves; k++) tri_total += d->curves[k].n_segments;
     if (tri_total >= (1ull << 27)) {
         *err = "more than 2^27 unique triangles";
         return false;
     }
     H.n_tris = tri_total;
     if (build_bvh) H.tris.reserve(3 * tri_total);
+    if (d->n_curves && !build_bvh) {
+        *err = "internal: curve sets are built by the host BVH builder";
+        return false;
+    }
+    // A geometry's collapsed BLAS (its primitives already in `tris` in the
+    // leaf order of `bin`), its root's children and second-level frontier.
+    auto emit_blas = [&](uint32_t g, const BinBvh& bin) -> bool {
+        MeshInfo& mi = H.meshes[g];
+        Collapser col{bin, H.nodes, mi.tri_base};
+        H.nodes.reserve(H.nodes.size() + WIDE_NODE_WORDS * (bin.nodes.size() / 4 + 1));
+        mi.blas_root = col.emit(0);
+        col.finish();
+        H.blas_nodes += col.emitted;
+        if (col.decode_errors) {
+            *err = "internal: quantised BLAS boxes not conservative";
+            return false;
+        }
+        // The root's children, and the second-level frontier (each inner
+        // child replaced by its own children; the wide nodes were emitted in
+        // preorder, one `wide` entry per node index).
+        const auto& root = col.wide[0];
+        for (uint32_t k = 0; k < root.nk; k++) {
+            const BinNode& kn = bin.nodes[root.kids[k]];
+            RootChild c;
+            f32_box(kn.b, c.lo, c.hi);
+            c.ref = root.refs[k];
+            root_children[g].push_back(c);
+            if (kn.count == 0) {
+                const auto& cw = col.wide[root.refs[k] - root.idx];
+                for (uint32_t kk = 0; kk < cw.nk; kk++) {
+                    RootChild gc;
+                    f32_box(bin.nodes[cw.kids[kk]].b, gc.lo, gc.hi);
+                    gc.ref = cw.refs[kk];
+                    grand_children[g].push_back(gc);
+                }
+            } else {
+                grand_children[g].push_back(c);
+            }
+        }
+        return true;
+    };
     uint64_t tri_base = 0;
     for (uint32_t m = 0; m < d->n_meshes; m++) {
         const rt_mesh_desc& md = d->meshes[m];
@@ -1288,37 +1336,56 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
             }
         });
         if (md.n_triangles == 0) continue;
-        Collapser col{bin, H.nodes, mi.tri_base};
-        H.nodes.reserve(H.nodes.size() + WIDE_NODE_WORDS * (bin.nodes.size() / 4 + 1));
-        mi.blas_root = col.emit(0);
-        col.finish();
-        H.blas_nodes += col.emitted;
-        if (col.decode_errors) {
-            *err = "internal: quantised BLAS boxes not conservative";
+        if (!emit_blas(m, bin)) return false;
+    }
+    // Curve sets (curves.rs:29-62): BLASes over the boxes of each segment's
+    // two end spheres; segments stored in the triangles' records.
+    for (uint32_t k = 0; k < d->n_curves; k++) {
+        const rt_curves_desc& cd = d->curves[k];
+        const uint32_t g = d->n_meshes + k;
+        if (cd.n_segments && (!cd.p0 || !cd.p1 || !cd.v0 || !cd.v1)) {
+            *err = "curve set " + std::to_string(k) + " has NULL arrays";
             return false;
         }
-        // The root's children, and the second-level frontier (each inner
-        // child replaced by its own children; the wide nodes were emitted in
-        // preorder, one `wide` entry per node index).
-        const auto& root = col.wide[0];
-        for (uint32_t k = 0; k < root.nk; k++) {
-            const BinNode& kn = bin.nodes[root.kids[k]];
-            RootChild c;
-            f32_box(kn.b, c.lo, c.hi);
-            c.ref = root.refs[k];
-            root_children[m].push_back(c);
-            if (kn.count == 0) {
-                const auto& cw = col.wide[root.refs[k] - root.idx];
-                for (uint32_t kk = 0; kk < cw.nk; kk++) {
-                    RootChild g;
-                    f32_box(bin.nodes[cw.kids[kk]].b, g.lo, g.hi);
-                    g.ref = cw.refs[kk];
-                    grand_children[m].push_back(g);
+        MeshInfo& mi = H.meshes[g];
+        mi.n_tris = cd.n_segments;
+        mi.tri_base = (uint32_t)tri_base;
+        mi.blas_root = 0xFFFFFFFFu;
+        mi.idx_base = 0xFFFFFFFFu;
+        mi.attrs = MESH_CURVES;
+        tri_base += cd.n_segments;
+        std::vector<Box> sb(cd.n_segments);
+        for (uint32_t t = 0; t < cd.n_segments; t++) {
+            Box b;
+            for (const float* e : {cd.p0 + 4ull * t, cd.p1 + 4ull * t}) {
+                if (!std::isfinite(e[0] + e[1] + e[2] + e[3]) || e[3] < 0.0f) {
+                    *err = "curve set " + std::to_string(k) + " has a non-finite point or a negative radius";
+                    return false;
                 }
-            } else {
-                grand_children[m].push_back(c);
+                const double r = e[3];
+                const double lo[3] = {(double)e[0] - r, (double)e[1] - r, (double)e[2] - r};
+                const double hi[3] = {(double)e[0] + r, (double)e[1] + r, (double)e[2] + r};
+                b.grow_pt(lo);
+                b.grow_pt(hi);
             }
+            sb[t] = b;
         }
+        BinBvh bin = build_binary(sb);
+        H.binary_blas_nodes += bin.nodes.size();
+        for (uint32_t j = 0; j < cd.n_segments; j++) {
+            const uint32_t t = bin.order[j];
+            const float* a = cd.p0 + 4ull * t;
+            const float* b = cd.p1 + 4ull * t;
+            float4 r0 = make_float4(a[0], a[1], a[2], 0.0f), r1 = make_float4(b[0], b[1], b[2], a[3]);
+            float4 r2 = make_float4(b[3], cd.v0[t], cd.v1[t], 0.0f);
+            const uint32_t mark = RT_SEG_MARK;
+            memcpy(&r0.w, &t, 4);
+            memcpy(&r2.w, &mark, 4);
+            H.tris.push_back(r0);
+            H.tris.push_back(r1);
+            H.tris.push_back(r2);
+        }
+        if (cd.n_segments && !emit_blas(g, bin)) return false;
     }
     if (!H.st.empty()) H.st.resize(2 * (H.normals.size() / 3), 0.0f);
     // ---- instances + TLAS ------------------------------------------------
@@ -1328,7 +1395,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
     }
     for (uint32_t i = 0; i < d->n_instances; i++) {
         const rt_instance_desc& id = d->instances[i];
-        if (id.mesh_id >= d->n_meshes || id.material_id >= d->n_materials) {
+        if (id.mesh_id >= n_geom || id.material_id >= d->n_materials) {
             *err = "instance " + std::to_string(i) + " references a missing mesh or material";
             return false;
         }
@@ -1367,6 +1434,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         }
     }
     H.scalars.n_instances = d->n_instances;
+    H.scalars.any_curves = d->n_curves ? 1u : 0u;
     // ---- materials ---------------------------------------------------------
     if (d->n_materials && !d->materials) {
         *err = "materials pointer is NULL";
@@ -1436,6 +1504,22 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
             return false;
         }
         H.materials.push_back(fold_material(md));
+        if (md.hair) {
+            // HairParams::new (hair.rs:40-55): clamped roughnesses, the
+            // longitudinal variance per lobe, the azimuthal logistic scale.
+            DevHair hp{};
+            const double bm = std::min(std::max(md.hair_beta_m, 0.01), 1.0);
+            const double bn = std::min(std::max(md.hair_beta_n, 0.01), 1.0);
+            double v0 = 0.726 * bm + 0.812 * bm * bm + 3.7 * std::pow(bm, 20);
+            v0 *= v0;
+            const double v[4] = {v0, 0.25 * v0, 4.0 * v0, 4.0 * v0};
+            for (int k = 0; k < 4; k++) hp.v[k] = (float)v[k];
+            for (int c = 0; c < 3; c++) hp.sigma_a[c] = (float)md.hair_sigma_a[c];
+            hp.eta = (float)md.hair_eta;
+            hp.s = (float)(0.626657069 * (0.265 * bn + 1.194 * bn * bn + 5.372 * std::pow(bn, 22)));
+            H.materials.back().hair = (uint32_t)H.hair.size();
+            H.hair.push_back(hp);
+        }
         if (H.materials.back().presence < 1.0f) H.scalars.any_presence = 1;
         if (H.materials.back().sss_gain > 0.0f) H.scalars.any_sss = 1;
     }

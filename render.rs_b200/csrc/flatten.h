@@ -43,6 +43,7 @@ struct HostScene {
     std::vector<float> env_marg, env_cond;
     std::vector<DevQuadric> quadrics;
     std::vector<DevMedium> media;
+    std::vector<DevHair> hair;
     uint64_t blas_nodes = 0, tlas_nodes = 0, binary_blas_nodes = 0;
     uint64_t n_tris = 0;             // unique triangles over all meshes
     double world_lo[3] = {0, 0, 0}, world_hi[3] = {0, 0, 0};  // union of instance bounds

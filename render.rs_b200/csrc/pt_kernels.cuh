@@ -23,6 +23,7 @@
 #include "pattern.cuh"
 #include "quadric.cuh"
 #include "media.cuh"
+#include "hair.cuh"
 
 namespace rt {
 
@@ -154,6 +155,7 @@ struct HitGeo {
     float eucl;
     uint32_t mat;
     bool front;
+    bool curve;  // a curve-set segment (hair shading applies)
 };
 
 __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3 d, uint4 hr, HitGeo& g) {
@@ -161,6 +163,7 @@ __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3
     g.p = o + d * t;
     g.wo = -normalize_ref(d);
     g.eucl = length(g.p - o);
+    g.curve = false;
     if (hr.y & RT_TRI_QUADRIC) {
         // Quadric: normal and front face as the shape reports them
         // (not flipped; shading flips toward wo as for every hit).
@@ -177,7 +180,14 @@ __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3
     float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
     float3 nl;
     MeshInfo mi = S.meshes[info.w];
-    if (mi.attrs & MESH_NORMALS) {
+    if (mi.attrs & MESH_CURVES) {
+        // Curve segment (mesh.rs:323-344): the rounded cone's outward
+        // normal at the hit, flipped against the ray as meshes are.
+        float tt;
+        nl = f3(0.0f, 0.0f, 1.0f);
+        seg_intersect(xf_point(x0, x1, x2, o), xf_vec(x0, x1, x2, d), v0, v1, v2, INFINITY, tt, &nl);
+        g.curve = true;
+    } else if (mi.attrs & MESH_NORMALS) {
         // Interpolated vertex normals (Mesh::local_normal, mesh.rs:200-220).
         float b1 = __half2float(__ushort_as_half((unsigned short)(hr.w & 0xFFFFu)));
         float b2 = __half2float(__ushort_as_half((unsigned short)(hr.w >> 16)));
@@ -192,6 +202,21 @@ __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3
     g.front = dot(nw, d) < 0.0f;
     g.nw = g.front ? nw : -nw;
     g.mat = info.z;
+}
+
+// World tangent of a curve hit (mesh.rs:342): the segment's axis (0, 0, 1
+// for a point particle) through the instance's object-to-world transform,
+// which is the inverse of the stored world-to-object rows: the adjugate's
+// columns are their pairwise cross products.
+__device__ __forceinline__ float3 curve_tangent(const DevScene& S, uint4 hr) {
+    const float4* tp = S.tris + 3 * (size_t)hr.y;
+    const float3 axis = xyz(__ldg(tp + 1)) - xyz(__ldg(tp));
+    const float3 a = dot(axis, axis) > 1e-24f ? axis : f3(0.0f, 0.0f, 1.0f);
+    const float4 x0 = __ldg(S.inst_xf + 3 * (size_t)hr.z), x1 = __ldg(S.inst_xf + 3 * (size_t)hr.z + 1),
+                 x2 = __ldg(S.inst_xf + 3 * (size_t)hr.z + 2);
+    const float3 r0 = xyz(x0), r1 = xyz(x1), r2 = xyz(x2);
+    const float3 w = cross(r1, r2) * a.x + cross(r2, r0) * a.y + cross(r0, r1) * a.z;
+    return normalize_ref(dot(r0, cross(r1, r2)) < 0.0f ? -w : w);
 }
 
 // (s, t), st density (st units per world unit) and the world-space st
@@ -215,6 +240,21 @@ __device__ __forceinline__ HitSt hit_st(const DevScene& S, uint4 hr, float3 p) {
     }
     const uint4 info = __ldg(S.inst + hr.z);
     const MeshInfo mi = S.meshes[info.w];
+    if (mi.attrs & MESH_CURVES) {
+        // st = (0.5, v) with v the curve parameter along the segment, no
+        // density (mesh.rs:323-344).
+        const float4* tp = S.tris + 3 * (size_t)hr.y;
+        const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        const float4 x0 = __ldg(S.inst_xf + 3 * (size_t)hr.z), x1 = __ldg(S.inst_xf + 3 * (size_t)hr.z + 1),
+                     x2 = __ldg(S.inst_xf + 3 * (size_t)hr.z + 2);
+        const float3 axis = xyz(b) - xyz(a);
+        const float len2 = dot(axis, axis);
+        const float along =
+            len2 > 1e-24f ? fminf(fmaxf(dot(xf_point(x0, x1, x2, p) - xyz(a), axis) / len2, 0.0f), 1.0f) : 0.5f;
+        r.s = 0.5f;
+        r.t = c.y + (c.z - c.y) * along;
+        return r;
+    }
     if (!(mi.attrs & MESH_ST)) return r;
     const float4* tp = S.tris + 3 * (size_t)hr.y;
     const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
@@ -578,7 +618,7 @@ __global__ void k_guide_keep(const uint32_t* tb_cnt, float scale, uint32_t cap, 
 #ifndef RT_INST_IN_NODE_PHASE
 #define RT_INST_IN_NODE_PHASE 0
 #endif
-template <bool ANY, bool TRANSMIT = false, bool PRES = false, class Load, class Finish>
+template <bool ANY, bool TRANSMIT = false, bool PRES = false, bool CURV = false, class Load, class Finish>
 __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                          TravStack& st, LeafShared& leaf, Load load, Finish finish) {
     PhaseState ps;
@@ -655,7 +695,7 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
         bool done_now = false;
         if (active && ps.pending && !ps.ts.in_inst) done_now = op_leaf<ANY>(S, ps, st, err);
         const bool tri_leaf = active && !done_now && ps.pending && ps.ts.in_inst;
-        if (__any_sync(0xFFFFFFFFu, tri_leaf)) done_now |= leaf_coop<ANY, TRANSMIT, PRES>(S, ps, tri_leaf, leaf, ray_seed);
+        if (__any_sync(0xFFFFFFFFu, tri_leaf)) done_now |= leaf_coop<ANY, TRANSMIT, PRES, CURV>(S, ps, tri_leaf, leaf, ray_seed);
         if (__any_sync(0xFFFFFFFFu, done_now)) finish(done_now, item, ps.ts);
         if (done_now) active = false;
     }
@@ -720,7 +760,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S
         for (uint32_t c = 0; c < N_QUEUES; c++)
             push_queue(P.q_cls + (size_t)c * P.P, &P.cnt[CNT_CLASS + c], slot, done && cls == c);
     };
-    ray_pump<false, false, PRES>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+    ray_pump<false, false, PRES, QUAD>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
     if (rays) atomicAdd(&P.stats[0], rays);
 }
 
@@ -875,6 +915,32 @@ __device__ __forceinline__ bool nee_light(const DevScene& S, const DevLight& L, 
         return f;
     };
     return nee_light_eval(S, L, p, n, eval, pick, rng, out);
+}
+
+// Hair at a curve hit (pt/mod.rs:737-781): NEE through the hair lobes
+// (n, the viewer-facing normal, offsets the shadow ray), then a
+// hair-sampled direction with its weight f / pdf (no cosine: f is per solid
+// angle). Returns false when sampling fails and the path ends. Out of line:
+// only hair hits call it, and the shade kernel keeps its registers.
+__device__ __noinline__ bool shade_hair(const DevScene& S, const DevHair& hp, uint4 hr, float3 p, float3 n, float3 wo,
+                                        Pcg& rng, NeeOut& ne, bool& nee_ok, float3& wi, float3& weight, float& pdf) {
+    const FiberFrame ff(curve_tangent(S, hr), n, wo);
+    HairEval g;
+    hair_prepare(hp, ff.to_local(wo), ff.h, g);
+    nee_ok = false;
+    if (S.n_lights > 0) {
+        uint32_t li;
+        float pmf;
+        if (light_sample(S, p, rng.next_f(), li, pmf)) {
+            auto eval = [&](float3 w, float& pd) -> float3 { return hair_f_pdf(hp, g, ff.to_local(w), pd); };
+            nee_ok = nee_light_eval(S, S.lights[li], p, n, eval, pmf, rng, ne);
+        }
+    }
+    float3 wf, f;
+    if (!hair_sample(hp, g, rng, wf, f, pdf)) return false;
+    wi = normalize_ref(ff.to_world(wf));
+    weight = f / pdf;
+    return true;
 }
 
 // mod.rs:1000-1023 solid-angle pdf of an area light toward a hit.
@@ -1187,10 +1253,52 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                         }
                         emit(beta * em * wgt);
                     }
+                    // Hair fibers scatter over the whole sphere with their own
+                    // BSDF (pt/mod.rs:737-781), on curve hits only.
+                    const bool fiber = hg.curve && m.hair != 0xFFFFFFFFu;
+                    if (fiber) {
+                        NeeOut ne;
+                        bool nee_ok;
+                        float3 wi, wgt;
+                        float pv;
+                        const bool ok = shade_hair(S, S.hair[m.hair], hr, p, n, wo, rng, ne, nee_ok, wi, wgt, pv);
+                        if (nee_ok) {
+                            const float3 c = beta * ne.c;
+                            if (maxc(c) > 0.0f) {
+                                P.sh_o[slot] = make_float4(ne.o.x, ne.o.y, ne.o.z, MED ? __uint_as_float(cur_med) : 0.0f);
+                                P.sh_d[slot] = make_float4(ne.d.x, ne.d.y, ne.d.z, ne.tmax);
+                                P.sh_c[slot] = make_float4(c.x, c.y, c.z, spec_true ? 0.0f : 1.0f);
+                                shadow = true;
+                            }
+                        }
+                        if (ok) {
+                            beta = beta * wgt;
+                            if ((flags & FL_SPEC_MASK) == FL_SPEC_NONE) flags &= ~FL_SPEC_MASK;
+                            flags &= ~FL_FROM_CAMERA;
+                            beta4.w = pv;
+                            prev4 = make_float4(p.x, p.y, p.z, 0.0f);
+                            if (PAT) cone.y += 0.4f;
+                            const float3 side = dot(wi, nw) >= 0.0f ? nw : -nw;
+                            const float3 no = p + side * RT_RAY_OFFSET;
+                            const uint32_t depth = (flags >> FL_DEPTH_SHIFT) + 1;
+                            flags = (flags & 0xFFFFu) | (depth << FL_DEPTH_SHIFT);
+                            bool alive = true;
+                            if (depth >= C.rr_start) {
+                                const float q = fminf(maxc(beta) * o4.w, 0.95f);
+                                if (q <= 0.0f || rng.next_f() > q) alive = false;
+                                else beta = beta / q;
+                            }
+                            if (alive && depth < C.max_depth) {
+                                P.ray_o[slot] = make_float4(no.x, no.y, no.z, o4.w);
+                                P.ray_d[slot] = make_float4(wi.x, wi.y, wi.z, INFINITY);
+                                extend = true;
+                            }
+                        }
+                    }
                     // Subsurface scattering (pt/mod.rs:794-892): with probability
                     // sss_gain the path enters a random walk inside the object
                     // (k_sss), starting from a cosine direction around -n.
-                    if (m.sss_gain > 0.0f && rng.next_f() < m.sss_gain) {
+                    if (!fiber && m.sss_gain > 0.0f && rng.next_f() < m.sss_gain) {
                         if ((flags & FL_SPEC_MASK) == FL_SPEC_NONE) flags &= ~FL_SPEC_MASK;
                         const Frame ef(-n);
                         const float e1 = rng.next_f(), e2 = rng.next_f();
@@ -1204,7 +1312,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                         P.hit[slot] = make_uint4(hg.mat, 0u, 0u, 0u);
                         walk = true;
                     }
-                    if (!walk) {
+                    if (!walk && !fiber) {
                         Frame fr(n);
                         float3 wo_l = fr.to_local(wo);
                         // Learned proposal at this vertex (guided mode only).
@@ -1380,7 +1488,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
             rays++;
             if (!ts.found && !qblock) add(slot, 1.0f);
         };
-        ray_pump<true>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+        ray_pump<true, false, false, QUAD>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
         if (rays) atomicAdd(&P.stats[1], rays);
         return;
     }
@@ -1408,7 +1516,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
         const float vis = ts.trans * qvis;
         if (vis > 0.0f) add(slot, vis);
     };
-    ray_pump<true, true>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+    ray_pump<true, true, false, QUAD>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
     if (rays) atomicAdd(&P.stats[1], rays);
 }
 
@@ -1740,7 +1848,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_intersect(DevScen
             if (tout) tout[i] = t;
         }
     };
-    ray_pump<ANY>(S, (uint32_t)n, fetch, err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+    ray_pump<ANY, false, false, QUAD>(S, (uint32_t)n, fetch, err, st, leaf_sh[threadIdx.x >> 5], load, finish);
 }
 
 // ---- diagnostics: the device functions the render kernels use, on caller inputs ----------
@@ -1771,7 +1879,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_transmit_batch(De
     auto finish = [&](bool done, uint32_t i, const TravState& ts) {
         if (done) out[i] = ts.trans * qvis;
     };
-    ray_pump<true, true>(S, (uint32_t)n, fetch, err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+    ray_pump<true, true, false, QUAD>(S, (uint32_t)n, fetch, err, st, leaf_sh[threadIdx.x >> 5], load, finish);
 }
 
 // The first n u32 draws of Pcg32::for_pixel_sample(pixel[i], sample[i]).

@@ -75,8 +75,19 @@ struct DevMaterial {
     // medium (volume.rs sss_medium) as extinction and scattering.
     float sss_gain, sss_st[3];
     float sss_ss[3], hull;                   // hull: 1 when the surface only bounds `interior`
+    uint32_t hair;                           // Marschner parameters in DevScene::hair, ~0 for none
+    uint32_t pad2_[3];
 };
-static_assert(sizeof(DevMaterial) == 192, "DevMaterial layout");
+static_assert(sizeof(DevMaterial) == 208, "DevMaterial layout");
+
+// Marschner hair (src/raytracer/pt/hair.rs HairParams): absorption, IOR,
+// the longitudinal variances per lobe and the azimuthal logistic scale.
+struct DevHair {
+    float sigma_a[3], eta;
+    float v[4];
+    float s, pad_[3];
+};
+static_assert(sizeof(DevHair) == 48, "DevHair layout");
 
 // ---- participating media (src/scene/medium.rs) ---------------------------------
 struct DevMedium {
@@ -127,6 +138,12 @@ static_assert(sizeof(LightNode) == 48, "LightNode layout");
 // Vertex attributes a mesh carries (MeshInfo::attrs).
 #define MESH_NORMALS 1u
 #define MESH_ST 2u
+#define MESH_CURVES 4u   // a curve set: its "triangles" are rounded-cone segments
+
+// A curve segment takes a triangle's 3 float4 in `tris`: (p0 xyz, segment
+// id bits) (p1 xyz, r0) (r1, v0, v1, RT_SEG_MARK bits). Triangles keep 0 in
+// that last word, so a leaf test tells them apart by it.
+#define RT_SEG_MARK 0x7FC5E6u
 
 struct MeshInfo {
     uint32_t idx_base;     // first index of this mesh in orig_idx (3 per tri), or ~0 if no attributes
@@ -249,6 +266,8 @@ struct DevScene {
     uint32_t n_media;
     uint32_t atmosphere;         // global medium, ~0 for none
     uint32_t any_sss;            // some material has a subsurface walk
+    const DevHair* hair;         // hair parameters (null when no material has them)
+    uint32_t any_curves;         // the scene has curve sets
     // Environment map of light env_light (src/scene/envmap.rs): lat-long
     // texels (RGB + pad), row-marginal CDF (env_h + 1), per-row conditional
     // CDFs (env_w + 1 each) over sin-weighted luminance, their total.

@@ -221,11 +221,14 @@ struct rt_session {
     }
 };
 
-// The ray-batch kernel variant for the query and the scene (with the
-// quadric tests only when the scene has quadrics).
+// Scenes with analytic quadrics or curve sets run the kernel variants that
+// test them (the others keep their registers for the BVH walk).
+static bool extra_geometry(const rt_session* s) { return s->S.n_quadrics > 0 || s->S.any_curves; }
+
+// The ray-batch kernel variant for the query and the scene.
 static void launch_intersect(rt_session* s, int any_hit, int grid, cudaStream_t st, const float4* o, const float4* d,
                              uint64_t n, uint32_t* prim, uint32_t* inst, float* t, uint32_t* fetch, uint32_t* err) {
-    const bool quad = s->S.n_quadrics > 0;
+    const bool quad = extra_geometry(s);
     if (any_hit && quad)
         k_intersect<TRAV_BLOCK, true, true><<<grid, TRAV_BLOCK, 0, st>>>(s->S, o, d, n, prim, inst, t, fetch, err);
     else if (any_hit)
@@ -248,7 +251,9 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     auto* s = new rt_session();
     s->params = *params;
     std::string err;
-    const bool device_bvh = params->bvh_build == 0;
+    // The device builder covers triangle meshes; scenes with curve sets are
+    // built on the host (the same SAH rules and wide layout).
+    const bool device_bvh = params->bvh_build == 0 && !(scene && scene->n_curves);
     if (!flatten_scene(scene, &s->host, &err, !device_bvh)) {
         delete s;
         return fail(RT_ERR_INVALID, err);
@@ -325,6 +330,7 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     }
     if (!H.quadrics.empty()) rc = rc ? rc : s->upload(&S.quadrics, H.quadrics);
     if (!H.media.empty()) rc = rc ? rc : s->upload(&S.media, H.media);
+    if (!H.hair.empty()) rc = rc ? rc : s->upload(&S.hair, H.hair);
     rc = rc ? rc : s->upload(&S.materials, H.materials);
     rc = rc ? rc : s->upload(&S.lights, H.lights);
     rc = rc ? rc : s->upload(&S.lbvh, H.lbvh);
@@ -591,9 +597,7 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
         for (uint32_t w = 0; w < waves; w++) {
             uint32_t qin = w & 1u, qout = qin ^ 1u;
             CUDA_TRY(cudaEventRecord(s->evpool[ei], st));
-            // Scenes with analytic quadrics run the variants that test them
-            // (the others keep their registers for the BVH walk).
-            const bool quad = s->S.n_quadrics > 0;
+            const bool quad = extra_geometry(s);
             if (C.pres_in_trav && quad) k_extend<TRAV_BLOCK, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
             else if (C.pres_in_trav) k_extend<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
             else if (quad) k_extend<TRAV_BLOCK, false, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
@@ -1074,7 +1078,7 @@ int rt_transmittance_batch(rt_session* s, const float* rays, uint64_t n, float* 
     CUDA_TRY(cudaMemcpyAsync(d_rays, rays, 32 * n, cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(cudaMemsetAsync(s->fetch, 0, 4, s->stream));
     const float4* o = (const float4*)d_rays;
-    if (s->S.n_quadrics)
+    if (extra_geometry(s))
         k_transmit_batch<TRAV_BLOCK, true><<<s->trav_grid, TRAV_BLOCK, 0, s->stream>>>(s->S, o, o + n, n, d_out,
                                                                                        s->fetch, s->err);
     else

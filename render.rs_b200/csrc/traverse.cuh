@@ -133,6 +133,89 @@ __device__ __forceinline__ bool tri_watertight(const RayPre& r, float3 v0, float
     return true;
 }
 
+// ---- curve segments (src/geometry/curves.rs:107-188) ---------------------------------
+// Rounded cone after Quilez: a sphere swept from pa (radius ra) to pb
+// (radius rb). The ray is first advanced to its closest approach to pa
+// (t0), so the quadratic's terms are on the scale of the segment rather
+// than of the ray's length and keep their precision in f32; t is
+// parametric along d (not normalised). Writes the outward normal when n is
+// given.
+__device__ __forceinline__ bool seg_sphere(float3 o, float3 d, float dd, float3 c, float r, float t_lo, float t_hi,
+                                           float& t) {
+    const float3 oc = o - c;
+    const float b = dot(oc, d), cc = dot(oc, oc) - r * r;
+    const float disc = b * b - dd * cc;
+    if (disc < 0.0f) return false;
+    const float sq = sqrtf(disc);
+    float tt = (-b - sq) / dd;
+    if (tt <= t_lo) tt = (-b + sq) / dd;
+    if (tt <= t_lo || tt >= t_hi) return false;
+    t = tt;
+    return true;
+}
+__device__ __forceinline__ bool seg_intersect(float3 o, float3 d, float4 a, float4 b, float4 c, float t_max, float& t_out,
+                                              float3* n_out = nullptr) {
+    const float3 pa = xyz(a), pb = xyz(b);
+    const float ra = b.w, rb = c.x;
+    const float dd = dot(d, d);
+    const float t0 = dot(pa - o, d) / dd;
+    const float3 os = o + d * t0;  // the ray's closest approach to pa
+    const float lo = -t0, hi = t_max - t0;
+    const float3 ba = pb - pa, oa = os - pa;
+    const float m0 = dot(ba, ba);
+    float ts;
+    float3 n;
+    if (m0 < 1e-24f) {
+        // A point particle: the sphere of the larger radius.
+        if (!seg_sphere(os, d, dd, pa, fmaxf(ra, rb), lo, hi, ts)) return false;
+        n = os + d * ts - pa;
+    } else {
+        const float rr = ra - rb;
+        const float m1 = dot(ba, oa), m2 = dot(ba, d), m3 = dot(d, oa), m5 = dot(oa, oa);
+        const float d2 = m0 - rr * rr;
+        const float k2 = d2 * dd - m2 * m2;
+        const float k1 = d2 * m3 - m1 * m2 + m2 * rr * ra;
+        const float k0 = d2 * m5 - m1 * m1 + m1 * rr * ra * 2.0f - m0 * ra * ra;
+        bool body = false;
+        if (fabsf(k2) > 1e-24f) {
+            const float h = k1 * k1 - k0 * k2;
+            if (h >= 0.0f) {
+                const float tb = (-k1 - sqrtf(h)) / k2;
+                const float y = m1 + tb * m2;
+                if (tb > lo && tb < hi && y > 0.0f && y < d2) {
+                    ts = tb;
+                    n = (oa + d * tb) * d2 - ba * y;
+                    body = true;
+                }
+            }
+        }
+        if (!body) {
+            // Caps: the start sphere owns y <= 0, the end sphere y >= d2.
+            bool any = false;
+            float tc;
+            float lim = hi;
+            if (seg_sphere(os, d, dd, pa, ra, lo, lim, tc) && m1 + tc * m2 <= 0.0f) {
+                any = true;
+                ts = tc;
+                lim = tc;
+                n = os + d * tc - pa;
+            }
+            if (seg_sphere(os, d, dd, pb, rb, lo, lim, tc) && m1 + tc * m2 >= d2) {
+                any = true;
+                ts = tc;
+                n = os + d * tc - pb;
+            }
+            if (!any) return false;
+        }
+    }
+    const float t = t0 + ts;
+    if (!(t > 0.0f && t < t_max)) return false;
+    t_out = t;
+    if (n_out) *n_out = normalize_ref(n);
+    return true;
+}
+__device__ __forceinline__ bool is_segment(float4 c) { return __float_as_uint(c.w) == RT_SEG_MARK; }
+
 // ---- 8-wide node: decode and test all children --------------------------------------
 __device__ __forceinline__ float q8(uint32_t word, int byte) {
     // Exact u8 -> f32 through the 2^23 mantissa trick.
@@ -414,8 +497,10 @@ __device__ __forceinline__ bool op_leaf(const DevScene& S, PhaseState& ps, TravS
     for (uint32_t k = 0; k < count; k++) {
         const float4* tp = S.tris + 3 * (size_t)(first + k);
         float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-        float t, b1, b2;
-        if (tri_watertight(ts.r, xyz(a), xyz(b), xyz(c), ts.hit.t, t, b1, b2)) {
+        float t, b1 = 0.0f, b2 = 0.0f;
+        const bool hit = (S.any_curves && is_segment(c)) ? seg_intersect(ts.r.o, ts.r.d, a, b, c, ts.hit.t, t)
+                                                         : tri_watertight(ts.r, xyz(a), xyz(b), xyz(c), ts.hit.t, t, b1, b2);
+        if (hit) {
             ts.hit.t = t;
             ts.hit.tri = first + k;
             ts.hit.inst = ts.cur_inst;
@@ -484,7 +569,8 @@ __device__ __forceinline__ bool presence_passes(uint64_t seed, uint32_t tri, uin
 // `mine`: this lane's parked leaf is a triangle leaf to test; `seed_own`:
 // this lane's ray seed (PRES). Returns true when an any-hit query found a
 // hit (the query is over).
-template <bool ANY, bool TRANSMIT = false, bool PRES = false>
+// CURV: the scene has curve sets, whose leaves hold segments (seg_intersect).
+template <bool ANY, bool TRANSMIT = false, bool PRES = false, bool CURV = false>
 __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, bool mine, LeafShared& L,
                                           uint64_t seed_own = 0) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -531,6 +617,11 @@ __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, boo
         r.kx = (int)(kp & 3u);
         r.ky = (int)((kp >> 2) & 3u);
         r.kz = (int)((kp >> 4) & 3u);
+        if (CURV) {
+            r.d.x = __shfl_sync(0xFFFFFFFFu, ts.r.d.x, owner);
+            r.d.y = __shfl_sync(0xFFFFFFFFu, ts.r.d.y, owner);
+            r.d.z = __shfl_sync(0xFFFFFFFFu, ts.r.d.z, owner);
+        }
         const float pres = __shfl_sync(0xFFFFFFFFu, pres_own, owner);
         uint64_t seed = 0;
         uint32_t inst_o = 0;
@@ -551,7 +642,9 @@ __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, boo
             const uint32_t tri = f + (it & 15u);
             const float4* tp = S.tris + 3 * (size_t)tri;
             float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-            if (tri_watertight(r, xyz(a), xyz(b), xyz(c), tmax, t, b1, b2)) {
+            const bool hit = (CURV && is_segment(c)) ? seg_intersect(r.o, r.d, a, b, c, tmax, t)
+                                                     : tri_watertight(r, xyz(a), xyz(b), xyz(c), tmax, t, b1, b2);
+            if (hit) {
                 if (TRANSMIT) {
                     factor = pres >= 1.0f ? 0.0f : 1.0f - pres;
                 } else if (!(PRES && pres < 1.0f && presence_passes(seed, tri, inst_o, pres))) {

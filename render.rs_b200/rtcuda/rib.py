@@ -22,9 +22,10 @@ Deviations (recorded in ``RibScene.warnings`` at load time):
     they are skipped, as the reference does.
   * Bilinear / bicubic PatchMesh and Patch are diced by the current
     Basis, as the reference does, NuPatch NURBS untrimmed;
-    SubdivisionMesh, GeneralPolygon, Curves, Points and motion blur
-    are skipped with a warning (motion blocks use their first
-    sample); Interior and Atmosphere media (homogeneous or fBm) and
+    SubdivisionMesh, GeneralPolygon and motion blur are skipped with a
+    warning (motion blocks use their first sample); Curves and Points
+    become curve sets (rounded-cone segments) and PxrMarschnerHair their
+    hair material; Interior and Atmosphere media (homogeneous or fBm) and
     PxrSurface subsurface parameters are carried; Displace "noise" moves polygon-mesh vertices at load time as
     the reference does; a PxrDomeLight lightColorMap is read when it is a
     Radiance .hdr (one map per scene).
@@ -42,7 +43,7 @@ import os
 import numpy as np
 
 from . import abi
-from .scene import Scene, default_material, emitter, medium
+from .scene import Scene, default_material, emitter, marschner_hair, medium
 
 # ---- parsing (src/parser/parser.rs) --------------------------------------------------------
 
@@ -308,6 +309,40 @@ class _Params:
         return None if v is None else _as_str(v)
 
 
+def _or(v, default):
+    return default if v is None else v
+
+
+def dice_curve(ctrl, cubic, w_root, w_tip, segs):
+    """dice_curve (curves.rs:193-247): sample the curve (each cubic span of
+    the basis at `segs` steps, the last span including its end; linear
+    curves at their control points), then one rounded-cone segment per
+    pair of samples with the half-width going linearly root to tip and v
+    = sample index / (samples - 1). Returns (p0, p1, v0, v1) or None."""
+    from .patches import basis_weights
+    ctrl = np.asarray(ctrl, np.float64)
+    if cubic is None:
+        pts = ctrl
+    else:
+        m, step = cubic
+        n = len(ctrl)
+        if n < 4:
+            return None
+        spans = (n - 4) // step + 1
+        pts = []
+        for sp in range(spans):
+            g = ctrl[sp * step:sp * step + 4]
+            count = segs + 1 if sp == spans - 1 else segs
+            pts.append(basis_weights(m, np.arange(count) / segs) @ g)
+        pts = np.concatenate(pts)
+    if len(pts) < 2:
+        return None
+    v = np.arange(len(pts)) / (len(pts) - 1)
+    r = (w_root + (w_tip - w_root) * v) * 0.5
+    p = np.concatenate([pts, r[:, None]], axis=1)
+    return p[:-1], p[1:], v[:-1], v[1:]
+
+
 def _num(vals, k):
     return _as_number(vals[k]) if k < len(vals) else None
 
@@ -444,6 +479,7 @@ class _State:
         self.basis_v = ("bezier", None)
         self.identifier = None
         self.interior = -1       # Interior medium bound to subsequent geometry
+        self.hair = None         # Bxdf "PxrMarschnerHair" parameters (dict)
 
     def copy(self):
         s = _State()
@@ -498,6 +534,7 @@ class _Builder:
         self.texture_ids = {}             # file path -> texture index (-1: unreadable)
         self.media = []                   # Scene medium dicts
         self.atmosphere = -1              # index into media, -1 for none
+        self.curve_sets = []              # (p0, p1, v0, v1, material, object_to_world 4x4)
 
     # -- helpers ------------------------------------------------------------------
     def warn(self, msg):
@@ -523,6 +560,12 @@ class _Builder:
     def make_material(self):
         """SceneBuilder::make_material (scene_builder.rs:1850-1877)."""
         st = self.state
+        if st.hair is not None:
+            # A plain brown matte off curves, Marschner hair on them.
+            m = marschner_hair(**st.hair)
+            m["id"] = self.object_id()
+            m["interior"] = st.interior
+            return m
         if st.bxdf is not None:
             m = dict(st.bxdf)
         elif st.surface == "plastic":
@@ -740,15 +783,29 @@ class _Builder:
                 st.roughness = 0.1 if r is None else r
         elif name == "Bxdf":
             t = _str(vals, 0) or ""
-            if t == "PxrMarschnerHair":
-                self.warn("hair is not rendered on this path; PxrMarschnerHair treated as PxrSurface")
-            elif t != "PxrSurface":
-                self.warn(f'Bxdf "{t}" not implemented; treating as PxrSurface')
             prm = _Params(vals, 2 if len(vals) % 2 == 0 else 1)
+            if t == "PxrMarschnerHair":
+                # HairParams::from_bxdf_params (hair.rs:82-100).
+                a = prm.numbers("absorption")
+                c = prm.numbers("color")
+                st.hair = dict(roughness=_or(prm.number("roughness"), 0.3),
+                               azimuthal_roughness=_or(prm.number("azimuthalRoughness"), 0.3),
+                               ior=_or(prm.number("ior"), 1.55),
+                               absorption=None if not a else (tuple(a[:3]) if len(a) >= 3 else (a[0],) * 3),
+                               color=tuple(c[:3]) if c is not None and len(c) >= 3 else None)
+                st.bxdf, st.bxdf_bindings = None, []
+                return
+            st.hair = None
+            if t != "PxrSurface":
+                self.warn(f'Bxdf "{t}" not implemented; treating as PxrSurface')
             st.bxdf = _pbr_bxdf(prm)
             st.bxdf_bindings = self.bxdf_bindings(prm)
         elif name == "Pattern":
             self.pattern_request(vals)
+        elif name == "Curves":
+            self.curves_request(vals)
+        elif name == "Points":
+            self.points_request(vals)
         elif name in ("Interior", "Atmosphere"):
             self.medium_request(name, vals)
         elif name == "Exterior":
@@ -803,6 +860,73 @@ class _Builder:
                 self.add_quadric(_QUADRIC_KIND[name], a, self.add_material(self.make_material()), self.ctm)
         else:
             self.warn(f"RIB request '{name}' not rendered on this path; skipping")
+
+    def curves_request(self, vals):
+        """curves_request (scene_builder.rs:1050-1119): Curves "cubic" |
+        "linear" [nvertices] "nonperiodic" "P" [...] with "width" (root to
+        tip) or "constantwidth"; cubic curves by the v Basis, diced into
+        clamp(8 / shading rate, 2, 24) segments per span."""
+        if self.defining is not None:
+            self.warn("Curves inside ObjectBegin is not instanced; skipping")
+            return
+        kind = _str(vals, 0) or "cubic"
+        nverts = _as_numbers(vals[1]) if len(vals) > 1 else None
+        if nverts is None:
+            self.warn("Curves without [nvertices]; skipping")
+            return
+        if (_str(vals, 2) or "nonperiodic") == "periodic":
+            self.warn('Curves "periodic" not supported; treating as nonperiodic')
+        prm = _Params(vals, 3)
+        P = prm.numbers("P")
+        if P is None:
+            self.warn('Curves without "P"; skipping')
+            return
+        w = prm.numbers("width")
+        if w:
+            w_root, w_tip = w[0], w[-1]
+        else:
+            w_root = w_tip = _or(prm.number("constantwidth"), 0.01)
+        cubic = None
+        if kind != "linear":
+            cubic = self._basis(self.state.basis_v)
+        segs = min(max(int(8.0 / max(self.state.shading_rate, 0.1)), 2), 24)
+        P = np.asarray(P, np.float64)
+        parts, cursor = [], 0
+        for nv in nverts:
+            nv = int(nv)
+            if (cursor + nv) * 3 > len(P):
+                break
+            parts.append(dice_curve(P[3 * cursor:3 * (cursor + nv)].reshape(-1, 3), cubic, w_root, w_tip, segs))
+            cursor += nv
+        parts = [q for q in parts if q is not None]
+        if parts:
+            self.add_curve_set(*(np.concatenate([q[k] for q in parts]) for k in range(4)))
+
+    def points_request(self, vals):
+        """points_request (scene_builder.rs:1122-1154): particles as
+        zero-length segments (spheres) of diameter "width" (per point) or
+        "constantwidth" (0.05)."""
+        if self.defining is not None:
+            self.warn("Points inside ObjectBegin is not instanced; skipping")
+            return
+        prm = _Params(vals, 0)
+        P = prm.numbers("P")
+        if P is None:
+            self.warn('Points without "P"; skipping')
+            return
+        P = np.asarray(P, np.float64).reshape(-1, 3)
+        widths = prm.numbers("width")
+        cw = _or(prm.number("constantwidth"), 0.05)
+        w = np.array([widths[i] if widths is not None and i < len(widths) else cw for i in range(len(P))])
+        e = np.concatenate([P, (w * 0.5)[:, None]], axis=1)
+        half = np.full(len(P), 0.5)
+        self.add_curve_set(e, e, half, half)
+
+    def add_curve_set(self, p0, p1, v0, v1):
+        """add_curve_set (scene_builder.rs:1157-1170): the state material and
+        the current placement."""
+        mat = self.add_material(self.make_material())
+        self.curve_sets.append((p0, p1, v0, v1, mat, self.ctm.copy()))
 
     def medium_request(self, name, vals):
         """Interior / Atmosphere (scene_builder.rs:324-373): sigma_a, sigma_s,
@@ -1260,6 +1384,8 @@ class _Builder:
                             np.stack([i[2] for i in self.instances]))
         for kind, params, mat, xf in self.quadrics:
             s.add_quadric(kind, params, mat, xf)
+        for p0, p1, v0, v1, mat, xf in self.curve_sets:
+            s.add_instance(s.add_curves(p0, p1, v0, v1), mat, np.asarray(xf, np.float64)[:3, :].reshape(12))
         for med in self.media:
             s.add_medium(med)
         s.atmosphere = self.atmosphere

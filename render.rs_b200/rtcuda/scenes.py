@@ -13,11 +13,12 @@ down for tests; the defaults are the full workloads.
                          1,200 point lights
   media_cornell          the Cornell box with participating media (fog, an fBm cloud in a
                          volume hull, glass with an absorbing interior) and a subsurface sphere
+  furball                a sphere groomed with cubic b-spline strands of Marschner hair
 """
 import numpy as np
 
 from . import abi
-from .scene import (Scene, affine, emitter, ggx_conductor, ggx_floor, matte, medium, rot_y,
+from .scene import (Scene, affine, emitter, ggx_conductor, ggx_floor, marschner_hair, matte, medium, rot_y,
                     rough_dielectric, volume_hull)
 
 
@@ -485,5 +486,39 @@ def media_cornell(width=64, height=64, fog=True, cloud=True, glass=True, sss=Tru
         sm = s.add_material(matte((0.8, 0.8, 0.8), subsurface_gain=1.0, subsurface_color=(0.9, 0.5, 0.3),
                                   subsurface_dmfp=(0.2, 0.1, 0.05), id=8))
         s.add_quadric(abi.QUADRIC_SPHERE, sphere, sm, affine(np.eye(3) * 0.22, (0.05, -0.78, 0.7)))
+    return s
+
+
+# ---------------------------------------------------------------------------
+# Curves and hair
+def furball(width=128, height=64, n_strands=20_000, seed=5):
+    """A unit sphere of skin (an analytic quadric) groomed with `n_strands`
+    cubic b-spline strands of 6 control points (3 spans x 8 segments each,
+    dice_curve), 0.35 long, swept sideways, 0.012 wide at the root and
+    0.002 at the tip, shaded with Marschner hair (colour (0.32, 0.14,
+    0.05), roughness 0.35 / 0.32); a constant blue dome and a warm rect
+    key light. The layout of the reference's furball scene with a seeded
+    groom of its own."""
+    from .patches import BASES
+    from .rib import dice_curve
+    s = Scene(width, height, fov=26.0)
+    s.look_at((0.0, 1.3, 0.0), (0.0, 1.3, 9.5))
+    s.add_dome_light(0.6, (0.6, 0.7, 1.0))
+    s.add_rect_light((-4.5, 6.0, 2.5), (3.0, 0.0, 0.0), (0.0, 0.0, 3.0), 6.0, (1.0, 0.9, 0.8))
+    centre = np.array([0.0, 1.32, 9.5])
+    skin = s.add_material(matte((0.30, 0.17, 0.08)))
+    s.add_quadric(abi.QUADRIC_SPHERE, [1.0, -1.0, 1.0, 360.0], skin, affine(np.eye(3), centre))
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n_strands, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    side = np.cross(d, [0.3, 1.0, 0.1])
+    side /= np.linalg.norm(side, axis=1, keepdims=True)
+    sj = np.arange(6) / 5 * 0.35
+    ctrl = (d[:, None, :] * (1.0 + sj[None, :, None]) + side[:, None, :] * (0.32 * sj * sj)[None, :, None]
+            + np.array([0.0, -0.1, 0.0]) * (sj * sj)[None, :, None])
+    parts = [dice_curve(c, (BASES["b-spline"][0], 1), 0.012, 0.002, 8) for c in ctrl]
+    p0, p1, v0, v1 = (np.concatenate([q[k] for q in parts]) for k in range(4))
+    coat = s.add_material(marschner_hair(color=(0.32, 0.14, 0.05), roughness=0.35, azimuthal_roughness=0.32))
+    s.add_instance(s.add_curves(p0, p1, v0, v1), coat, affine(np.eye(3), centre))
     return s
 

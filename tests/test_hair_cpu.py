@@ -125,3 +125,41 @@ def test_hair_render_is_lit():
     s = _hair_scene()
     img = oracle.OracleScene(s).render(abi.make_params(max_depth=8), 0, 16)[0] / 16
     assert np.isfinite(img).all() and img.mean() > 0.01
+
+
+def test_dice_bezier_curve():
+    """curves.rs:292-320: one cubic Bezier span diced into 8 segments."""
+    from rtcuda.patches import BASES
+    from rtcuda.rib import dice_curve
+    p0, p1, v0, v1 = dice_curve([[0, 0, 0], [0, 1, 0], [1, 2, 0], [2, 2, 0]], (BASES["bezier"][0], 3), 0.1, 0.02, 8)
+    assert len(p0) == 8
+    assert abs(p0[0][0]) < 1e-6 and abs(p0[0][1]) < 1e-6
+    assert abs(p1[7][0] - 2.0) < 1e-6 and abs(p1[7][1] - 2.0) < 1e-6
+    assert p0[0][3] > p1[7][3] and abs(p0[0][3] - 0.05) < 1e-6
+    assert v0[0] == 0.0 and v1[7] == 1.0
+
+
+def test_rib_curves_points_and_hair():
+    """Curves / Points requests (scene_builder.rs:1050-1170) with a
+    PxrMarschnerHair material (hair.rs:82-100)."""
+    from rtcuda.rib import load_rib_string
+    s = load_rib_string("""
+Format 8 8 1
+WorldBegin
+  Bxdf "PxrMarschnerHair" "h" "roughness" [0.25] "azimuthalRoughness" [0.4] "color" [0.5 0.3 0.1]
+  Curves "cubic" [4 4] "nonperiodic" "P" [0 0 0 0 1 0 1 2 0 2 2 0  0 0 1 0 1 1 1 2 1 2 2 1] "width" [0.1 0.02]
+  Bxdf "PxrSurface" "s" "diffuseColor" [0.5 0.5 0.5]
+  Curves "linear" [3] "nonperiodic" "P" [0 0 0 1 0 0 2 0 0] "constantwidth" [0.04]
+  Points "P" [0 0 5 1 0 5] "width" [0.2 0.4]
+WorldEnd
+""")
+    assert len(s.curves) == 3
+    p0, p1, v0, v1 = s.curves[0]
+    assert len(p0) == 2 * 8  # two cubic Bezier curves, 8 segments each at shading rate 1
+    hair = s.materials[s.instance_array()["mat"][0]]
+    assert hair["hair"] == 1 and hair["hair_beta_m"] == 0.25 and hair["hair_beta_n"] == 0.4
+    lin = s.curves[1]
+    assert len(lin[0]) == 2 and abs(lin[0][0][3] - 0.02) < 1e-7
+    pts = s.curves[2]
+    assert np.array_equal(pts[0], pts[1]) and abs(pts[0][1][3] - 0.2) < 1e-7 and (pts[2] == 0.5).all()
+    assert s.materials[s.instance_array()["mat"][1]]["hair"] == 0
