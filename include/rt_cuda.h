@@ -190,6 +190,16 @@ typedef struct rt_stats {
 
 int rt_get_stats(rt_session* s, rt_stats* out);
 
+/* Diagnostics of the hair BSDF (src/raytracer/pt/hair.rs f, pdf, sample)
+ * as the shade kernel evaluates it in f32. params = sigma_a xyz, beta_m,
+ * beta_n, eta. rt_hair_eval: per query (wo xyz, wi xyz, h) in the fiber
+ * frame, f (3 floats) and pdf. rt_hair_sample: n consecutive samples for
+ * one (wo, h) from the PCG32 stream of (pixel, sample): wi xyz, f rgb, pdf
+ * (pdf 0 where sampling failed). */
+int rt_hair_eval(const double* params, uint64_t n, const float* q, float* f, float* pdf);
+int rt_hair_sample(const double* params, const double* wo, double h, uint64_t pixel, uint64_t sample, uint64_t n,
+                   float* out);
+
 /* Diagnostic: white-furnace estimate of one material on the GPU, using the
  * shade kernel's f32 BSDF sampling. `wo` is in the local frame (z = shading
  * normal), eta = transmitted / incident IOR. out[0] = mean of

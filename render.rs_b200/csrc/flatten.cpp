@@ -646,6 +646,22 @@ DevMaterial fold_material(const rt_material_desc& m) {
     return d;
 }
 
+// HairParams::new (hair.rs:40-55): clamped roughnesses, the longitudinal
+// variance per lobe, the azimuthal logistic scale.
+DevHair hair_dev(const rt_material_desc& md) {
+    DevHair hp{};
+    const double bm = std::min(std::max(md.hair_beta_m, 0.01), 1.0);
+    const double bn = std::min(std::max(md.hair_beta_n, 0.01), 1.0);
+    double v0 = 0.726 * bm + 0.812 * bm * bm + 3.7 * std::pow(bm, 20);
+    v0 *= v0;
+    const double v[4] = {v0, 0.25 * v0, 4.0 * v0, 4.0 * v0};
+    for (int k = 0; k < 4; k++) hp.v[k] = (float)v[k];
+    for (int c = 0; c < 3; c++) hp.sigma_a[c] = (float)md.hair_sigma_a[c];
+    hp.eta = (float)md.hair_eta;
+    hp.s = (float)(0.626657069 * (0.265 * bn + 1.194 * bn * bn + 5.372 * std::pow(bn, 22)));
+    return hp;
+}
+
 // Light BVH (light_sampler.rs:242-312): median split on the widest axis of
 // the light-extent box, stable sort by centre along that axis.
 struct LEntry {
@@ -931,6 +947,7 @@ bool flatten_patterns(const rt_scene_desc* d, HostScene& H, std::string* err) {
 }  // namespace
 
 DevMaterial fold_material_public(const rt_material_desc& m) { return fold_material(m); }
+DevHair hair_dev_public(const rt_material_desc& m) { return hair_dev(m); }
 
 // An instance is split into its BLAS root's children (one TLAS item each)
 // when their world boxes' summed surface area is below RT_BRAID_RATIO times
@@ -1505,20 +1522,8 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         }
         H.materials.push_back(fold_material(md));
         if (md.hair) {
-            // HairParams::new (hair.rs:40-55): clamped roughnesses, the
-            // longitudinal variance per lobe, the azimuthal logistic scale.
-            DevHair hp{};
-            const double bm = std::min(std::max(md.hair_beta_m, 0.01), 1.0);
-            const double bn = std::min(std::max(md.hair_beta_n, 0.01), 1.0);
-            double v0 = 0.726 * bm + 0.812 * bm * bm + 3.7 * std::pow(bm, 20);
-            v0 *= v0;
-            const double v[4] = {v0, 0.25 * v0, 4.0 * v0, 4.0 * v0};
-            for (int k = 0; k < 4; k++) hp.v[k] = (float)v[k];
-            for (int c = 0; c < 3; c++) hp.sigma_a[c] = (float)md.hair_sigma_a[c];
-            hp.eta = (float)md.hair_eta;
-            hp.s = (float)(0.626657069 * (0.265 * bn + 1.194 * bn * bn + 5.372 * std::pow(bn, 22)));
             H.materials.back().hair = (uint32_t)H.hair.size();
-            H.hair.push_back(hp);
+            H.hair.push_back(hair_dev(md));
         }
         if (H.materials.back().presence < 1.0f) H.scalars.any_presence = 1;
         if (H.materials.back().sss_gain > 0.0f) H.scalars.any_sss = 1;

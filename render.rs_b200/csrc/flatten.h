@@ -91,5 +91,7 @@ void prim_records(const std::vector<double>& boxes, float* out);
 
 // f32 material constants as the shade kernel reads them.
 DevMaterial fold_material_public(const rt_material_desc& m);
+// f32 hair parameters of a hair material.
+DevHair hair_dev_public(const rt_material_desc& m);
 
 }  // namespace rt

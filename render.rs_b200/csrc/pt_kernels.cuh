@@ -1882,6 +1882,39 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_transmit_batch(De
     ray_pump<true, true, false, QUAD>(S, (uint32_t)n, fetch, err, st, leaf_sh[threadIdx.x >> 5], load, finish);
 }
 
+// Hair BSDF value and pdf for n (wo, wi, h) queries, 7 floats each.
+__global__ void k_hair_eval_batch(DevHair hp, const float* __restrict__ q, uint32_t n, float* __restrict__ f,
+                                  float* __restrict__ pdf) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* r = q + 7ull * i;
+    HairEval g;
+    hair_prepare(hp, f3(r[0], r[1], r[2]), r[6], g);
+    float pd;
+    const float3 v = hair_f_pdf(hp, g, f3(r[3], r[4], r[5]), pd);
+    f[3ull * i] = v.x;
+    f[3ull * i + 1] = v.y;
+    f[3ull * i + 2] = v.z;
+    pdf[i] = pd;
+}
+
+// n consecutive hair samples for one (wo, h) from the stream of (pixel,
+// sample): wi, f, pdf (pdf 0 where sampling failed). One thread.
+__global__ void k_hair_sample_batch(DevHair hp, float3 wo, float h, uint64_t pixel, uint64_t sample, uint32_t n,
+                                    float* __restrict__ out) {
+    if (blockIdx.x || threadIdx.x) return;
+    Pcg rng = pcg_for_pixel_sample(pixel, sample);
+    HairEval g;
+    hair_prepare(hp, wo, h, g);
+    for (uint32_t i = 0; i < n; i++) {
+        float3 wi = f3(0.0f, 0.0f, 0.0f), f = f3(0.0f, 0.0f, 0.0f);
+        float pdf = 0.0f;
+        if (!hair_sample(hp, g, rng, wi, f, pdf)) pdf = 0.0f;
+        float* o = out + 7ull * i;
+        o[0] = wi.x, o[1] = wi.y, o[2] = wi.z, o[3] = f.x, o[4] = f.y, o[5] = f.z, o[6] = pdf;
+    }
+}
+
 // The first n u32 draws of Pcg32::for_pixel_sample(pixel[i], sample[i]).
 __global__ void k_pcg_streams(const uint64_t* __restrict__ pixel, const uint64_t* __restrict__ sample, uint32_t m,
                               uint32_t n, uint32_t* __restrict__ out) {

@@ -988,6 +988,53 @@ int rt_bsdf_furnace(const rt_material_desc* material, const double* wo, double e
     return RT_OK;
 }
 
+// HairParams::new (hair.rs:40-55) in f32, as flatten_scene folds a hair material.
+static DevHair hair_params(const double* p) {
+    rt_material_desc md{};
+    md.hair = 1;
+    for (int c = 0; c < 3; c++) md.hair_sigma_a[c] = p[c];
+    md.hair_beta_m = p[3];
+    md.hair_beta_n = p[4];
+    md.hair_eta = p[5];
+    return hair_dev_public(md);
+}
+
+int rt_hair_eval(const double* params, uint64_t n, const float* q, float* f, float* pdf) {
+    if ((!params || !q || !f || !pdf) && n) return fail(RT_ERR_INVALID, "NULL argument");
+    if (!n) return RT_OK;
+    if (n > (1ull << 26)) return fail(RT_ERR_INVALID, "rt_hair_eval: more than 2^26 queries");
+    const DevHair hp = hair_params(params);
+    float* d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, 4ull * 11 * n));
+    cudaError_t e = cudaMemcpy(d, q, 4ull * 7 * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_hair_eval_batch<<<(uint32_t)((n + 127) / 128), 128>>>(hp, d, (uint32_t)n, d + 7 * n, d + 10 * n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(f, d + 7 * n, 12ull * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(pdf, d + 10 * n, 4ull * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(RT_ERR_CUDA, std::string("rt_hair_eval: ") + cudaGetErrorString(e));
+    return RT_OK;
+}
+
+int rt_hair_sample(const double* params, const double* wo, double h, uint64_t pixel, uint64_t sample, uint64_t n,
+                   float* out) {
+    if ((!params || !wo || !out) && n) return fail(RT_ERR_INVALID, "NULL argument");
+    if (!n) return RT_OK;
+    if (n > (1ull << 24)) return fail(RT_ERR_INVALID, "rt_hair_sample: more than 2^24 samples");
+    const DevHair hp = hair_params(params);
+    float* d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, 28ull * n));
+    k_hair_sample_batch<<<1, 32>>>(hp, make_float3((float)wo[0], (float)wo[1], (float)wo[2]), (float)h, pixel, sample,
+                                   (uint32_t)n, d);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, 28ull * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(RT_ERR_CUDA, std::string("rt_hair_sample: ") + cudaGetErrorString(e));
+    return RT_OK;
+}
+
 int rt_pcg_streams(const uint64_t* pixel, const uint64_t* sample, uint32_t m, uint32_t n, uint32_t* out) {
     if ((!pixel || !sample || !out) && m && n) return fail(RT_ERR_INVALID, "NULL argument");
     if (!m || !n) return RT_OK;

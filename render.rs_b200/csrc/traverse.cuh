@@ -140,6 +140,16 @@ __device__ __forceinline__ bool tri_watertight(const RayPre& r, float3 v0, float
 // than of the ray's length and keep their precision in f32; t is
 // parametric along d (not normalised). Writes the outward normal when n is
 // given.
+// Roots closer than RT_SEG_EPS to the ray's origin count as behind it (the
+// reference's bound is t > 1e-9 in f64, curves.rs:146, 182). The gap
+// matters for thin segments: there the reference's surface normal is
+// shorter than Vec3::normalize's 1e-6 threshold and stays unnormalised, so
+// rays leaving a hair hit start on the surface itself (the 1e-4 offset
+// along that normal vanishes); an f32 hit point is off the surface by about
+// an ulp of its coordinates, and without the gap the ray would meet its own
+// segment again at t ~ 1e-6 where the reference's f64 ray passes on.
+// Offset origins (unit normals) sit 1e-4 away and are not affected.
+#define RT_SEG_EPS 2e-5f
 __device__ __forceinline__ bool seg_sphere(float3 o, float3 d, float dd, float3 c, float r, float t_lo, float t_hi,
                                            float& t) {
     const float3 oc = o - c;
@@ -160,7 +170,7 @@ __device__ __forceinline__ bool seg_intersect(float3 o, float3 d, float4 a, floa
     const float dd = dot(d, d);
     const float t0 = dot(pa - o, d) / dd;
     const float3 os = o + d * t0;  // the ray's closest approach to pa
-    const float lo = -t0, hi = t_max - t0;
+    const float lo = RT_SEG_EPS - t0, hi = t_max - t0;
     const float3 ba = pb - pa, oa = os - pa;
     const float m0 = dot(ba, ba);
     float ts;
@@ -209,7 +219,7 @@ __device__ __forceinline__ bool seg_intersect(float3 o, float3 d, float4 a, floa
         }
     }
     const float t = t0 + ts;
-    if (!(t > 0.0f && t < t_max)) return false;
+    if (!(t > RT_SEG_EPS && t < t_max)) return false;
     t_out = t;
     if (n_out) *n_out = normalize_ref(n);
     return true;

@@ -29,7 +29,7 @@ ERRORS = {-1: "invalid argument", -2: "CUDA error", -3: "out of device memory", 
 EXPORTS = ("rt_session_create", "rt_session_destroy", "rt_last_error", "rt_render_samples", "rt_reset",
            "rt_read_accum", "rt_read_image", "rt_read_aux", "rt_checkpoint_save", "rt_checkpoint_load",
            "rt_intersect_batch", "rt_intersect_batch_device", "rt_get_stats", "rt_session_stream",
-           "rt_bsdf_furnace", "rt_intersect_batch_noalloc", "rt_session_guide", "rt_set_adaptive",
+           "rt_bsdf_furnace", "rt_hair_eval", "rt_hair_sample", "rt_intersect_batch_noalloc", "rt_session_guide", "rt_set_adaptive",
            "rt_average_spp", "rt_checkpoint_save_rckp", "rt_rckp_write", "rt_accum_exr_write",
            "rt_accum_exr_info", "rt_accum_exr_read", "rt_accum_merge", "rt_read_film", "rt_denoise",
            "rt_denoise_film", "rt_film_exr_write", "rt_pcg_streams", "rt_light_sample_batch",
@@ -99,6 +99,8 @@ def lib():
         L.rt_denoise_film.argtypes = [vp, u32, u32, vp]
         L.rt_film_exr_write.argtypes = [C.c_char_p, u32, u32, vp, C.c_char_p]
         L.rt_pcg_streams.argtypes = [vp, vp, u32, u32, vp]
+        L.rt_hair_eval.argtypes = [vp, C.c_uint64, vp, vp, vp]
+        L.rt_hair_sample.argtypes = [vp, vp, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, vp]
         L.rt_light_sample_batch.argtypes = [vp, vp, vp, u32, vp, vp]
         L.rt_light_pmf_batch.argtypes = [vp, vp, vp, u32, vp]
         L.rt_transmittance_batch.argtypes = [vp, vp, u64, vp]
@@ -119,6 +121,35 @@ def pcg_streams(pixels, samples, n):
     out = np.empty((len(px), n), np.uint32)
     _check(lib().rt_pcg_streams(px.ctypes.data, sm.ctypes.data, len(px), n, out.ctypes.data))
     return out
+
+
+def _hair_params(params):
+    sa, bm, bn, eta = params
+    return np.ascontiguousarray(list(np.broadcast_to(np.asarray(sa, float), 3)) + [bm, bn, eta], dtype=np.float64)
+
+
+def hair_eval(params, wo, wi, h):
+    """Device hair::f and hair::pdf (rt_hair_eval) for rows of (wo, wi, h)
+    in the fiber frame; params = (sigma_a, beta_m, beta_n, eta)."""
+    p = _hair_params(params)
+    wo, wi = np.atleast_2d(wo), np.atleast_2d(wi)
+    n = max(len(wo), len(wi))
+    q = np.ascontiguousarray(np.concatenate([np.broadcast_to(wo, (n, 3)), np.broadcast_to(wi, (n, 3)),
+                                             np.broadcast_to(np.reshape(h, (-1, 1)), (n, 1))], axis=1),
+                             dtype=np.float32)
+    f, pdf = np.empty((n, 3), np.float32), np.empty(n, np.float32)
+    _check(lib().rt_hair_eval(p.ctypes.data, n, q.ctypes.data, f.ctypes.data, pdf.ctypes.data))
+    return f, pdf
+
+
+def hair_sample(params, wo, h, pixel, sample, n):
+    """n device hair samples (rt_hair_sample): (wi, f, pdf)."""
+    p = _hair_params(params)
+    w = np.ascontiguousarray(wo, dtype=np.float64)
+    out = np.empty((n, 7), np.float32)
+    _check(lib().rt_hair_sample(p.ctypes.data, w.ctypes.data, C.c_double(h), C.c_uint64(pixel), C.c_uint64(sample),
+                                C.c_uint64(n), out.ctypes.data))
+    return out[:, :3], out[:, 3:6], out[:, 6]
 
 
 class PtSession:

@@ -19,6 +19,45 @@ from rtcuda import PtSession, abi, scenes
 pytestmark = pytest.mark.gpu
 
 
+HAIR = ((0.4, 0.9, 1.8), 0.35, 0.32, 1.55)
+
+
+def test_hair_bsdf_eval_matches_oracle():
+    """Device hair f and pdf (f32) against the oracle's f64 on random
+    fiber-frame queries."""
+    from rtcuda import backend
+    rng = np.random.default_rng(3)
+    n = 20_000
+    wo = rng.normal(size=(n, 3))
+    wo /= np.linalg.norm(wo, axis=1, keepdims=True)
+    wi = rng.normal(size=(n, 3))
+    wi /= np.linalg.norm(wi, axis=1, keepdims=True)
+    h = rng.uniform(-1, 1, n)
+    fg, pg = backend.hair_eval(HAIR, wo, wi, h)
+    fo, po = np.zeros((n, 3)), np.zeros(n)
+    for k in range(0, n, 2000):
+        fo[k:k + 2000], po[k:k + 2000] = oracle.hair_eval(HAIR, wo[k:k + 2000], wi[k:k + 2000], h[k:k + 2000])
+    scale_f, scale_p = np.maximum(np.abs(fo), 1e-3), np.maximum(po, 1e-3)
+    assert np.quantile(np.abs(fg - fo) / scale_f, 0.999) < 1e-3
+    assert np.quantile(np.abs(pg - po) / scale_p, 0.999) < 1e-3
+
+
+def test_hair_sampling_matches_oracle():
+    """Device hair::sample from the same PCG32 stream as the oracle's:
+    the same directions (up to f32), and E[f / pdf] equal."""
+    from rtcuda import backend
+    for sin_to, h in ((0.3, -0.4), (-0.6, 0.8), (0.05, 0.0)):
+        wo = np.array([sin_to, np.sqrt(1 - sin_to ** 2), 0.0])
+        wg, fg, pg = backend.hair_sample(HAIR, wo, h, 11, 5, 40_000)
+        wo_, fo, po = oracle.hair_sample(HAIR, wo, h, 11, 5, 40_000)
+        same = np.linalg.norm(wg - wo_, axis=1) < 1e-3
+        assert same.mean() > 0.99, same.mean()
+        lum = lambda f: 0.2126 * f[:, 0] + 0.7152 * f[:, 1] + 0.0722 * f[:, 2]
+        eg = np.where(pg > 0, lum(fg) / np.maximum(pg, 1e-30), 0).mean()
+        eo = np.where(po > 0, lum(fo) / np.maximum(po, 1e-30), 0).mean()
+        assert abs(eg - eo) < 0.01 * eo, (eg, eo)
+
+
 @pytest.fixture(scope="module")
 def fur():
     s = scenes.furball(64, 32, 20_000)
