@@ -335,7 +335,9 @@ def other_workloads(flush, stream):
     batch), the Cornell box 256^2 x 16 spp (depth 8), instanced materials
     1920x1080 x 64 spp (depth 12), the media Cornell box 512^2 x 16 spp (fog,
     an fBm cloud, absorbing glass, a subsurface sphere; 64 bounces, the
-    reference's depth with media). One warm-up pass, then one timed render
+    reference's depth with media), the furball 960x480 x 16 spp (20,000
+    b-spline strands of Marschner hair, 480,000 segments). One warm-up
+    pass, then one timed render
     call (device time from the session's events); scene build excluded."""
     import torch
     from rtcuda import PtSession, abi, scenes
@@ -346,6 +348,8 @@ def other_workloads(flush, stream):
              ("instanced_materials_1920x1080_64spp_depth12", lambda: scenes.instanced_materials(),
               scenes.INSTANCED_MATERIALS, 64),
              ("media_cornell_512x512_16spp_depth64", lambda: scenes.media_cornell(512, 512),
+              dict(max_depth=8, rr_start=3), 16),
+             ("furball_20k_strands_960x480_16spp_depth8", lambda: scenes.furball(960, 480, 20_000),
               dict(max_depth=8, rr_start=3), 16)]
     for name, make, cfg, spp in cases:
         t0 = time.perf_counter()
@@ -534,7 +538,8 @@ def run_scene(args):
     make = {"cornell": (scenes.cornell_box, scenes.CORNELL), "cloud": (scenes.triangle_cloud, scenes.TRIANGLE_CLOUD),
             "instanced": (scenes.instanced_materials, scenes.INSTANCED_MATERIALS),
             "two_rooms": (scenes.two_rooms, scenes.TWO_ROOMS), "forest": (scenes.forest, scenes.FOREST),
-            "media": (scenes.media_cornell, dict(max_depth=8, rr_start=3))}
+            "media": (scenes.media_cornell, dict(max_depth=8, rr_start=3)),
+            "furball": (scenes.furball, dict(max_depth=8, rr_start=3))}
     gen, cfg = make[args.scene]
     s = gen(w, h)
     p = abi.make_params(max_depth=cfg["max_depth"], rr_start=cfg["rr_start"])
@@ -557,7 +562,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--scene", default="forest",
-                    help="--mode scene: cornell, cloud, instanced, two_rooms, forest, media")
+                    help="--mode scene: cornell, cloud, instanced, two_rooms, forest, media, furball")
     ap.add_argument("--res", default="640x360", help="--mode scene: frame size WxH")
     ap.add_argument("--mode", default="full", choices=["full", "traversal", "guided", "scene"],
                     help="traversal: only the closest/any-hit ray batches; guided: only the learned-proposal "
