@@ -869,6 +869,117 @@ __global__ void k_root_children(const WideS* __restrict__ W, uint32_t R, const B
     nk2[r] = n2;
 }
 
+// ---- TLAS items on the device (flatten.cpp tlas_items, the same numbers) ----------------
+// A mesh's BLAS frontiers for the items: its root's children (off1, n1) and
+// its second-level frontier (off2, n2) in one RootChild table.
+struct MeshFrontier {
+    uint32_t off1, n1, off2, n2;
+    uint32_t blas_root, n_tris, pad_[2];
+};
+// world_box in f64 with every product and sum rounded on its own, as the
+// host computes it (no contraction into fused multiply-adds), so both
+// builders make the same boxes and the same trees.
+__device__ __forceinline__ void world_box_d(const double* m, const RootChild& rc, double* lo, double* hi) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        double c = m[r * 4 + 3], e = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const double ck = __dmul_rn(0.5, __dadd_rn((double)rc.lo[k], (double)rc.hi[k]));
+            const double hk = __dmul_rn(0.5, __dsub_rn((double)rc.hi[k], (double)rc.lo[k]));
+            c = __dadd_rn(c, __dmul_rn(m[r * 4 + k], ck));
+            e = __dadd_rn(e, __dmul_rn(fabs(m[r * 4 + k]), hk));
+        }
+        lo[r] = __dsub_rn(c, e);
+        hi[r] = __dadd_rn(c, e);
+    }
+}
+__device__ __forceinline__ double area_d(const double* lo, const double* hi) {
+    const double d0 = __dsub_rn(hi[0], lo[0]), d1 = __dsub_rn(hi[1], lo[1]), d2 = __dsub_rn(hi[2], lo[2]);
+    if (d0 < 0 || d1 < 0 || d2 < 0) return 0.0;
+    return __dmul_rn(2.0, __dadd_rn(__dadd_rn(__dmul_rn(d0, d1), __dmul_rn(d1, d2)), __dmul_rn(d2, d0)));
+}
+__device__ __forceinline__ void grow_d(double* lo, double* hi, const double* blo, const double* bhi) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        lo[a] = blo[a] < lo[a] ? blo[a] : lo[a];
+        hi[a] = bhi[a] > hi[a] ? bhi[a] : hi[a];
+    }
+}
+// An instance's frontier (the root's children, or the second level) under
+// its transform: the union of the children's world boxes and how many items
+// it becomes (flatten.cpp child_boxes); boxes of the children into cb when
+// given.
+__device__ uint32_t child_boxes_d(const rt_instance_desc& id, const MeshFrontier& f, const RootChild* fr, bool second,
+                                  bool split_all, double* ulo, double* uhi, double* cb) {
+    for (int a = 0; a < 3; a++) {
+        ulo[a] = HUGE_VAL;
+        uhi[a] = -HUGE_VAL;
+    }
+    if (!f.n_tris) return 0;
+    const uint32_t n = second ? f.n2 : f.n1, off = second ? f.off2 : f.off1;
+    double sum = 0.0;
+    for (uint32_t k = 0; k < n; k++) {
+        double lo[3], hi[3];
+        world_box_d(id.object_to_world, fr[off + k], lo, hi);
+        if (cb)
+            for (int a = 0; a < 3; a++) {
+                cb[6 * k + a] = lo[a];
+                cb[6 * k + 3 + a] = hi[a];
+            }
+        grow_d(ulo, uhi, lo, hi);
+        sum = __dadd_rn(sum, area_d(lo, hi));
+    }
+    if (n <= 1) return 1u;
+    return split_all || sum < __dmul_rn(RT_BRAID_RATIO, area_d(ulo, uhi)) ? n : 1u;
+}
+// Pass 1: per instance the union of its root children's world boxes and
+// the number of items it becomes in a scene that is not dense.
+__global__ void k_items_density(const rt_instance_desc* __restrict__ inst, uint32_t n, const MeshFrontier* __restrict__ mf,
+                                const RootChild* __restrict__ fr, double* __restrict__ ubox, uint32_t* __restrict__ cnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const rt_instance_desc id = inst[i];
+    double lo[3], hi[3];
+    cnt[i] = child_boxes_d(id, mf[id.mesh_id], fr, false, false, lo, hi, nullptr);
+    for (int a = 0; a < 3; a++) {
+        ubox[6ull * i + a] = lo[a];
+        ubox[6ull * i + 3 + a] = hi[a];
+    }
+}
+// f32_box (flatten.cpp): rounded outward, -0 folded into +0.
+__device__ __forceinline__ float f32_down(double x) { return __double2float_rd(x) + 0.0f; }
+__device__ __forceinline__ float f32_up(double x) { return __double2float_ru(x) + 0.0f; }
+// Pass 2: each instance's items at its offset: builder records (f32 box,
+// item index) and (instance, BLAS reference); the union of the item boxes
+// per instance for the world box.
+__global__ void k_items_write(const rt_instance_desc* __restrict__ inst, uint32_t n, const MeshFrontier* __restrict__ mf,
+                              const RootChild* __restrict__ fr, bool dense, const uint64_t* __restrict__ off,
+                              BPrim* __restrict__ prims, uint2* __restrict__ items, double* __restrict__ ubox) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const rt_instance_desc id = inst[i];
+    const MeshFrontier f = mf[id.mesh_id];
+    double cb[6 * RT_TOP_MAX], lo[3], hi[3];
+    const uint32_t k_items = child_boxes_d(id, f, fr, dense, dense, lo, hi, cb);
+    for (uint32_t k = 0; k < k_items; k++) {
+        const uint64_t j = off[i] + k;
+        const double* b = cb + 6 * k;
+        const double blo[3] = {k_items == 1 ? lo[0] : b[0], k_items == 1 ? lo[1] : b[1], k_items == 1 ? lo[2] : b[2]};
+        const double bhi[3] = {k_items == 1 ? hi[0] : b[3], k_items == 1 ? hi[1] : b[4], k_items == 1 ? hi[2] : b[5]};
+        BPrim p;
+        p.a = make_float4(f32_down(blo[0]), f32_down(blo[1]), f32_down(blo[2]), __uint_as_float((uint32_t)j));
+        p.b = make_float4(f32_up(bhi[0]), f32_up(bhi[1]), f32_up(bhi[2]), 0.0f);
+        prims[j] = p;
+        const uint32_t ref = k_items == 1 ? f.blas_root : fr[(dense ? f.off2 : f.off1) + k].ref;
+        items[j] = make_uint2(i, ref);
+    }
+    for (int a = 0; a < 3; a++) {
+        ubox[6ull * i + a] = k_items ? lo[a] : HUGE_VAL;
+        ubox[6ull * i + 3 + a] = k_items ? hi[a] : -HUGE_VAL;
+    }
+}
+
 // Quantisation grid of one axis (the host's choose_grid): origin p, a
 // multiple of s = 2^e, with every p + q*s (q in 0..255) an exact f32 and
 // p + 255*s >= hi. floor(log2) and ceil(log2) are taken exactly from the
@@ -1360,24 +1471,97 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
     uint32_t tlas_total = 0, NIT = 0;
     std::vector<float4> xf;
     std::vector<uint4> rec;
-    std::vector<uint2> items;
+    uint2* d_items = nullptr;
     if (NI) {
-        std::vector<double> boxes;
-        tlas_items(d, root_children, grand_children, &boxes, &items, H);
-        if (items.size() >= (1ull << 27)) {
+        // TLAS items on the device: the host's tlas_items rules and numbers
+        // (flatten.cpp), with the density decision and the offsets on the host.
+        std::vector<MeshFrontier> mf(M);
+        std::vector<RootChild> fr;
+        for (uint32_t m = 0; m < M; m++) {
+            MeshFrontier& f = mf[m];
+            f.off1 = (uint32_t)fr.size();
+            f.n1 = (uint32_t)root_children[m].size();
+            fr.insert(fr.end(), root_children[m].begin(), root_children[m].end());
+            f.off2 = (uint32_t)fr.size();
+            f.n2 = (uint32_t)grand_children[m].size();
+            fr.insert(fr.end(), grand_children[m].begin(), grand_children[m].end());
+            f.blas_root = blas_root[m];
+            f.n_tris = H->meshes[m].n_tris;
+        }
+        rt_instance_desc* d_inst;
+        MeshFrontier* d_mf;
+        RootChild* d_fr;
+        double* d_ubox;
+        uint32_t* d_cnt;
+        uint64_t* d_off;
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_inst, NI, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_mf, M, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_fr, std::max<size_t>(fr.size(), 1), st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_ubox, 6ull * NI, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_cnt, NI, st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_off, NI, st, err);
+        if (rc) return rc;
+        BV_TRY(cudaMemcpyAsync(d_inst, d->instances, sizeof(rt_instance_desc) * NI, cudaMemcpyHostToDevice, st));
+        BV_TRY(cudaMemcpyAsync(d_mf, mf.data(), sizeof(MeshFrontier) * M, cudaMemcpyHostToDevice, st));
+        if (!fr.empty()) BV_TRY(cudaMemcpyAsync(d_fr, fr.data(), sizeof(RootChild) * fr.size(), cudaMemcpyHostToDevice, st));
+        k_items_density<<<blocks_for(NI, JB), JB, 0, st>>>(d_inst, NI, d_mf, d_fr, d_ubox, d_cnt);
+        std::vector<double> ubox(6ull * NI);
+        std::vector<uint32_t> cnt(NI);
+        BV_TRY(cudaMemcpyAsync(ubox.data(), d_ubox, 48ull * NI, cudaMemcpyDeviceToHost, st));
+        BV_TRY(cudaMemcpyAsync(cnt.data(), d_cnt, 4ull * NI, cudaMemcpyDeviceToHost, st));
+        BV_TRY(cudaStreamSynchronize(st));
+        // Density: the instances' union boxes against their union.
+        double total_area = 0.0, alo[3] = {HUGE_VAL, HUGE_VAL, HUGE_VAL}, ahi[3] = {-HUGE_VAL, -HUGE_VAL, -HUGE_VAL};
+        auto area = [](const double* lo, const double* hi) {
+            const double d0 = hi[0] - lo[0], d1 = hi[1] - lo[1], d2 = hi[2] - lo[2];
+            if (d0 < 0 || d1 < 0 || d2 < 0) return 0.0;
+            return 2.0 * (d0 * d1 + d1 * d2 + d2 * d0);
+        };
+        for (uint32_t i = 0; i < NI; i++) {
+            if (!cnt[i]) continue;
+            const double* u = ubox.data() + 6ull * i;
+            total_area += area(u, u + 3);
+            for (int a = 0; a < 3; a++) {
+                alo[a] = u[a] < alo[a] ? u[a] : alo[a];
+                ahi[a] = u[3 + a] > ahi[a] ? u[3 + a] : ahi[a];
+            }
+        }
+        const double wa = area(alo, ahi);
+        const bool dense = wa > 0.0 && total_area > RT_BRAID_DENSE * wa;
+        std::vector<uint64_t> off(NI);
+        uint64_t total = 0;
+        for (uint32_t i = 0; i < NI; i++) {
+            off[i] = total;
+            const MeshFrontier& f = mf[d->instances[i].mesh_id];
+            total += dense ? (f.n_tris ? std::max<uint32_t>(f.n2, 1u) : 0u) : cnt[i];
+        }
+        if (total >= (1ull << 27)) {
             *err = "more than 2^27 instance subtrees";
             return RT_ERR_INVALID;
         }
-        NIT = (uint32_t)items.size();
+        NIT = (uint32_t)total;
         instance_records(d, *H, &xf, &rec);
+        BPrim* Q1 = nullptr;
+        rc = rc ? rc : dev_alloc(D.ptrs, &Q0, std::max<uint32_t>(NIT, 1), st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &Q1, std::max<uint32_t>(NIT, 1), st, err);
+        rc = rc ? rc : dev_alloc(D.ptrs, &d_items, std::max<uint32_t>(NIT, 1), st, err);
+        if (rc) return rc;
+        BV_TRY(cudaMemcpyAsync(d_off, off.data(), 8ull * NI, cudaMemcpyHostToDevice, st));
+        k_items_write<<<blocks_for(NI, JB), JB, 0, st>>>(d_inst, NI, d_mf, d_fr, dense, d_off, Q0, d_items, d_ubox);
+        BV_TRY(cudaMemcpyAsync(ubox.data(), d_ubox, 48ull * NI, cudaMemcpyDeviceToHost, st));
+        BV_TRY(cudaStreamSynchronize(st));
+        double wlo[3] = {HUGE_VAL, HUGE_VAL, HUGE_VAL}, whi[3] = {-HUGE_VAL, -HUGE_VAL, -HUGE_VAL};
+        for (uint32_t i = 0; i < NI; i++)
+            for (int a = 0; a < 3; a++) {
+                const double* u = ubox.data() + 6ull * i;
+                wlo[a] = u[a] < wlo[a] ? u[a] : wlo[a];
+                whi[a] = u[3 + a] > whi[a] ? u[3 + a] : whi[a];
+            }
+        for (int a = 0; a < 3; a++) {
+            H->world_lo[a] = wlo[a] <= whi[a] ? wlo[a] : 0.0;
+            H->world_hi[a] = wlo[a] <= whi[a] ? whi[a] : 0.0;
+        }
         if (NIT) {
-            std::vector<float> prims(8ull * NIT);
-            prim_records(boxes, prims.data());
-            BPrim* Q1;
-            rc = rc ? rc : dev_alloc(D.ptrs, &Q0, NIT, st, err);
-            rc = rc ? rc : dev_alloc(D.ptrs, &Q1, NIT, st, err);
-            if (rc) return rc;
-            BV_TRY(cudaMemcpyAsync(Q0, prims.data(), prims.size() * 4, cudaMemcpyHostToDevice, st));
             uint32_t n_tnodes = 0;
             rc = build_binary_device(D, Q0, Q1, NIT, {{0u, NIT}}, d_err, &tnodes, &n_tnodes, st, err);
             if (rc) return rc;
@@ -1412,10 +1596,6 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
     if (NIT) {
         rc = wide_words(tw, tnodes, out->nodes, total, d_err, st, err);
         if (rc) return rc;
-        uint2* d_items;
-        rc = dev_alloc(D.ptrs, &d_items, NIT, st, err);
-        if (rc) return rc;
-        BV_TRY(cudaMemcpyAsync(d_items, items.data(), items.size() * sizeof(uint2), cudaMemcpyHostToDevice, st));
         k_item_gather<<<blocks_for(NIT, 256), 256, 0, st>>>(Q0, d_items, NIT, out->items);
     }
     BV_TRY(cudaGetLastError());

@@ -959,18 +959,13 @@ DevHair hair_dev_public(const rt_material_desc& m) { return hair_dev(m); }
 // (B200): the 1280x720 forest frame 239 -> 211 ms at 1.75 (-6% at 0 with
 // union boxes alone, -16% at 1.9); at 2.2 and above the 1M-triangle cloud's
 // single instance splits and its frame slows by 40%, the instanced scene by
-// 18%.
-#ifndef RT_BRAID_RATIO
-#define RT_BRAID_RATIO 1.75
-#endif
+// 18%. (RT_BRAID_RATIO in flatten.h.)
 // In a dense scene, where the instances' boxes add up to more than
 // RT_BRAID_DENSE times the world box's area (the forest: 385; the instanced
 // scene: 5; one instance: 1), every instance with several root children is
 // split: a ray there crosses hundreds of instance boxes, and the children's
-// boxes overlap far less (forest frame 211 -> 182 ms).
-#ifndef RT_BRAID_DENSE
-#define RT_BRAID_DENSE 32.0
-#endif
+// boxes overlap far less (forest frame 211 -> 182 ms). (RT_BRAID_DENSE in
+// flatten.h.)
 
 // World box of a local box under an affine 3x4: centre mapped, half
 // extents through |M| (the exact box of the 8 transformed corners).

@@ -67,6 +67,14 @@ struct RootChild {
 // Largest BLAS frontier an instance is split into: a dense scene's
 // instances become the second-level frontier (at most 8 x 8 subtrees).
 constexpr uint32_t RT_TOP_MAX = 64u;
+// The instance-splitting rules of tlas_items (flatten.cpp explains them);
+// the device builder's item kernels apply the same.
+#ifndef RT_BRAID_RATIO
+#define RT_BRAID_RATIO 1.75
+#endif
+#ifndef RT_BRAID_DENSE
+#define RT_BRAID_DENSE 32.0
+#endif
 
 // TLAS primitives: every instance contributes one item (instance, BLAS root
 // reference) boxed by the union of its root children's world boxes, or one

@@ -73,6 +73,27 @@ def test_instanced_scene_matches_host_build():
     _check(dev, host)
 
 
+def test_dense_instanced_scene_matches_host_build():
+    """2,500 rotated, scaled copies of an icosphere crowded into a small box:
+    a dense scene (the instances' boxes add up to well over 32 world boxes),
+    so every instance becomes its BLAS's second-level frontier; the device
+    makes those items (world boxes from the centre and |M| extents) exactly
+    as the host does."""
+    rng = np.random.default_rng(9)
+    s = Scene(64, 48, fov=40.0)
+    s.look_at((0.0, 0.0, 4.0), (0.0, 0.0, 0.0))
+    mesh = s.add_mesh(*scenes.icosphere(3))
+    mat = s.add_material(matte((0.6, 0.6, 0.6)))
+    rot = scenes.random_rotations(rng, 2500)
+    for k in range(2500):
+        lin = rot[k] * rng.uniform(0.3, 0.5) * np.diag(rng.uniform(0.6, 1.4, 3))
+        s.add_instance(mesh, mat, scenes.affine(lin, rng.uniform(-0.8, 0.8, 3)))
+    s.add_point_light((0.0, 3.0, 3.0), 20.0)
+    dev, host = _both(s, _rays(32768, 5), spp=2)
+    _check(dev, host)
+    assert dev["tlas"] > 0
+
+
 @pytest.mark.parametrize("n", [1, 4, 5, 16, 17, 256, 257, 2048, 2049, 5000])
 def test_mesh_sizes_around_builder_thresholds(n):
     # Leaf limits (4, 16), the subtree threshold (256) and the chunk size (2048).
