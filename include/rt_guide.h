@@ -52,6 +52,13 @@ int rt_guide_train_step_device(rt_guide* g, const float* records, uint32_t n, fl
 int rt_guide_infer(rt_guide* g, const float* records, uint32_t n, float* raw_out);
 int rt_guide_infer_device(rt_guide* g, const float* records, uint32_t n, float* raw_out, void* stream);
 
+/* The decoded mixture the renderer samples from, for n records (host
+ * pointers), 48 floats per record: lobe j's (mu.xyz, kappa) at [4j, 4j+4),
+ * its weight at [32 + j] and at [40 + j] the log of its weighted density at
+ * mu.w = 0, A_j = log w_j + log(kappa_j / (2 pi (1 - e^{-2 kappa_j}))) -
+ * kappa_j, so that q(w) = sum_j exp(A_j + kappa_j mu_j.w). */
+int rt_guide_infer_mixture(rt_guide* g, const float* records, uint32_t n, float* mixture_out);
+
 /* Gradients of the summed loss without updating (host pointers):
  * g_mlp: RT_GUIDE_MLP_PARAMS floats (weights row-major [out][in] per layer,
  * then biases); g_table: RT_GUIDE_LEVELS * RT_GUIDE_TABLE_ENTRIES * 2 floats

@@ -69,6 +69,13 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
     __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
     return *reinterpret_cast<uint32_t*>(&v);
 }
+// The same with ReLU folded into the conversion (a in the low half, as
+// above): rounding keeps the sign, so this equals pack_bf16(max(a, 0), max(b, 0)).
+__device__ __forceinline__ uint32_t pack_bf16_relu(float a, float b) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+    return r;
+}
 
 // Copy a row-major [R][K] bf16 matrix into the core-matrix layout.
 __device__ void stage_matrix(uint8_t* dst, const __nv_bfloat16* src, int R, int K) {
@@ -102,31 +109,44 @@ __device__ __forceinline__ void encode_record(const GuideDev& G, const float* r,
 
 // Encoding runs as its own kernel at full occupancy: its cost is the 128
 // scattered table reads per record, which need many threads in flight (inside
-// the 128-thread forward CTAs they ran 1.7x slower than here).
+// the 128-thread forward CTAs they ran 1.7x slower than here). The grid is
+// sized for the record capacity but at most ENCODE_CTAS_PER_SM per SM, and
+// strides over the records: a launch whose count (read on the device) is
+// small then ends in a few microseconds instead of retiring one CTA per 256
+// records of capacity.
+constexpr uint32_t ENCODE_CTAS_PER_SM = 8;
 __global__ void __launch_bounds__(256) k_guide_encode(GuideDev G, const float* __restrict__ rec, uint32_t n,
                                                       BatchSel B, __nv_bfloat16* X0) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, begin;
+    uint32_t begin;
     n = batch_slice(B, n, begin);
     rec += 16 * (size_t)begin;
-    if (i >= n) return;
-    float feat[G_IN];
-    encode_record(G, rec + 16 * (size_t)i, feat);
-    uint4* out = reinterpret_cast<uint4*>(X0 + (size_t)i * G_IN);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float feat[G_IN];
+        encode_record(G, rec + 16 * (size_t)i, feat);
+        uint4* out = reinterpret_cast<uint4*>(X0 + (size_t)i * G_IN);
 #pragma unroll
-    for (int c = 0; c < G_IN / 8; c++)
-        out[c] = make_uint4(pack_bf16(feat[8 * c], feat[8 * c + 1]), pack_bf16(feat[8 * c + 2], feat[8 * c + 3]),
-                            pack_bf16(feat[8 * c + 4], feat[8 * c + 5]), pack_bf16(feat[8 * c + 6], feat[8 * c + 7]));
+        for (int c = 0; c < G_IN / 8; c++)
+            out[c] = make_uint4(pack_bf16(feat[8 * c], feat[8 * c + 1]), pack_bf16(feat[8 * c + 2], feat[8 * c + 3]),
+                                pack_bf16(feat[8 * c + 4], feat[8 * c + 5]),
+                                pack_bf16(feat[8 * c + 6], feat[8 * c + 7]));
+    }
 }
 
 // ---- forward ------------------------------------------------------------------
-// Each CTA runs FWD_GROUPS independent 128-row tile pipelines (one per 128
-// threads) that share the weights in shared memory; a pipeline's layers are
-// latency-bound (MMA -> commit -> TMEM load -> epilogue), so several tiles in
-// flight per SM hide each other's waits. A tile keeps one activation buffer:
-// X (K = 48), then H1, H2, H3 (K = 64) overwrite it in turn, which is safe
-// because a layer's MMA has finished reading its input when the epilogue runs.
+// One persistent CTA per SM runs FWD_GROUPS independent 128-row tile
+// pipelines (one per 128 threads, one warpgroup) that share the weights in
+// shared memory; a pipeline's layers are latency-bound (MMA -> commit -> TMEM
+// load -> epilogue), so six tiles in flight per SM hide each other's waits.
+// (Three CTAs of two pipelines each held the same work, but the weights three
+// times, and in some launches ran one CTA per SM at a time.) A tile keeps
+// one activation buffer: X (K = 48), then H1, H2, H3 (K = 64) overwrite it in
+// turn, which is safe because a layer's MMA has finished reading its input
+// when the epilogue runs.
 // Shared memory: W0 6144 | W1 8192 | W2 8192 | W3 6144 | ACT 16384 per group.
-constexpr int FWD_GROUPS = 2, FWD_THREADS = FWD_GROUPS * TILE;
+// TMEM: 64 columns per group, allocated as the next power of two.
+constexpr int FWD_GROUPS = 6, FWD_THREADS = FWD_GROUPS * TILE;
+constexpr uint32_t FWD_TMEM_COLS = 512;
+static_assert(64 * FWD_GROUPS <= FWD_TMEM_COLS && FWD_GROUPS <= 7, "forward: TMEM columns and named barriers");
 constexpr int F_W0 = 0, F_W1 = 6144, F_W2 = F_W1 + 8192, F_W3 = F_W2 + 8192, F_ACT = F_W3 + 6144,
               F_BYTES = F_ACT + FWD_GROUPS * 16384;
 
@@ -136,7 +156,7 @@ constexpr int F_W0 = 0, F_W1 = 6144, F_W2 = F_W1 + 8192, F_W3 = F_W2 + 8192, F_A
 enum { FWD_RAW = 0, FWD_TRAIN = 1, FWD_RENDER = 2 };
 
 template <int MODE>
-__global__ void __launch_bounds__(FWD_THREADS, 3) k_guide_fwd(GuideDev G, const __nv_bfloat16* __restrict__ X0,
+__global__ void __launch_bounds__(FWD_THREADS, 1) k_guide_fwd(GuideDev G, const __nv_bfloat16* __restrict__ X0,
                                                               uint32_t n, BatchSel B, __nv_bfloat16* acts,
                                                               float* out, uint32_t* err) {
     constexpr bool TRAIN = MODE == FWD_TRAIN;
@@ -147,14 +167,14 @@ __global__ void __launch_bounds__(FWD_THREADS, 3) k_guide_fwd(GuideDev G, const 
     __shared__ uint64_t mbar[FWD_GROUPS];
     __shared__ uint32_t tmem_base;
     __shared__ uint32_t group_failed[FWD_GROUPS];
-    __shared__ float bias[G_NBIAS];
+    __shared__ __align__(16) float bias[G_NBIAS];
     const int tid = threadIdx.x, warp = tid >> 5, grp = tid / TILE, gt = tid % TILE;
     stage_matrix(sm + F_W0, G.w + w_off(0), G_HID, G_IN);
     stage_matrix(sm + F_W1, G.w + w_off(1), G_HID, G_HID);
     stage_matrix(sm + F_W2, G.w + w_off(2), G_HID, G_HID);
     stage_matrix(sm + F_W3, G.w + w_off(3), G_OUT, G_HID);
     for (int i = tid; i < G_NBIAS; i += FWD_THREADS) bias[i] = G.b[i];
-    if (warp == 0) tmem_alloc(&tmem_base, 64 * FWD_GROUPS);
+    if (warp == 0) tmem_alloc(&tmem_base, FWD_TMEM_COLS);
     if (tid < FWD_GROUPS) {
         mbar_init(&mbar[tid], 1);
         group_failed[tid] = 0;
@@ -194,36 +214,53 @@ __global__ void __launch_bounds__(FWD_THREADS, 3) k_guide_fwd(GuideDev G, const 
                 break;
             }
             tc_fence_after();
-            uint32_t r[64];
-#pragma unroll
-            for (int c = 0; c < 4; c++)
-                if (c * 16 < N) tmem_ld16_nowait(lane_addr + c * 16, r + 16 * c);
-            tmem_ld_wait();
-            float v[64];
-#pragma unroll
-            for (int k = 0; k < 64; k++) v[k] = __uint_as_float(r[k]);
             if (l < 3) {
+                // Hidden layer: bias, ReLU, bf16 into the activation buffer,
+                // 32 columns at a time (fewer live registers).
 #pragma unroll
-                for (int k = 0; k < 64; k++) v[k] = fmaxf(v[k] + bias[b_off(l) + k], 0.f);
+                for (int h = 0; h < 2; h++) {
+                    uint32_t r[32];
+                    tmem_ld16_nowait(lane_addr + 32 * h, r);
+                    tmem_ld16_nowait(lane_addr + 32 * h + 16, r + 16);
+                    tmem_ld_wait();
 #pragma unroll
-                for (int c = 0; c < 8; c++) {
-                    uint4 q = make_uint4(pack_bf16(v[8 * c], v[8 * c + 1]), pack_bf16(v[8 * c + 2], v[8 * c + 3]),
-                                         pack_bf16(v[8 * c + 4], v[8 * c + 5]), pack_bf16(v[8 * c + 6], v[8 * c + 7]));
-                    *reinterpret_cast<uint4*>(sm + act + core_offset(gt, 8 * c, G_HID)) = q;
-                    if (TRAIN && valid)
-                        reinterpret_cast<uint4*>(acts + ((size_t)row * 3 + l) * G_HID)[c] = q;
+                    for (int c = 0; c < 4; c++) {
+                        const int k = 32 * h + 8 * c;
+                        const float4 ba = *reinterpret_cast<const float4*>(&bias[b_off(l) + k]);
+                        const float4 bb = *reinterpret_cast<const float4*>(&bias[b_off(l) + k + 4]);
+                        const float* f = reinterpret_cast<const float*>(r + 8 * c);
+                        const uint4 q = make_uint4(pack_bf16_relu(f[0] + ba.x, f[1] + ba.y),
+                                                   pack_bf16_relu(f[2] + ba.z, f[3] + ba.w),
+                                                   pack_bf16_relu(f[4] + bb.x, f[5] + bb.y),
+                                                   pack_bf16_relu(f[6] + bb.z, f[7] + bb.w));
+                        *reinterpret_cast<uint4*>(sm + act + core_offset(gt, k, G_HID)) = q;
+                        if (TRAIN && valid)
+                            reinterpret_cast<uint4*>(acts + ((size_t)row * 3 + l) * G_HID)[k / 8] = q;
+                    }
                 }
-            } else if (valid) {
+            } else {
+                uint32_t r[G_OUT];
 #pragma unroll
-                for (int k = 0; k < G_OUT; k++) v[k] += bias[b_off(3) + k];
-                if (MODE == FWD_RENDER) {
-                    Mixture mx;
-                    mixture_decode(v, mx);
-                    mixture_store(mx, out + (size_t)row * G_OUT);
-                } else {
-                    float4* o = reinterpret_cast<float4*>(out + (size_t)row * G_OUT);
+                for (int c = 0; c < G_OUT / 16; c++) tmem_ld16_nowait(lane_addr + c * 16, r + 16 * c);
+                tmem_ld_wait();
+                if (valid) {
+                    float v[G_OUT];
 #pragma unroll
-                    for (int c = 0; c < G_OUT / 4; c++) o[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+                    for (int k = 0; k < G_OUT; k += 4) {
+                        const float4 b4 = *reinterpret_cast<const float4*>(&bias[b_off(3) + k]);
+                        v[k] = __uint_as_float(r[k]) + b4.x;
+                        v[k + 1] = __uint_as_float(r[k + 1]) + b4.y;
+                        v[k + 2] = __uint_as_float(r[k + 2]) + b4.z;
+                        v[k + 3] = __uint_as_float(r[k + 3]) + b4.w;
+                    }
+                    if (MODE == FWD_RENDER) {
+                        mixture_decode_store(v, out + (size_t)row * G_OUT);
+                    } else {
+                        float4* o = reinterpret_cast<float4*>(out + (size_t)row * G_OUT);
+#pragma unroll
+                        for (int c = 0; c < G_OUT / 4; c++)
+                            o[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+                    }
                 }
             }
             tc_fence_before();
@@ -236,7 +273,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 3) k_guide_fwd(GuideDev G, const 
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        tmem_dealloc(tmem_base, 64 * FWD_GROUPS);
+        tmem_dealloc(tmem_base, FWD_TMEM_COLS);
         tmem_relinquish();
     }
 }
@@ -646,9 +683,10 @@ static int launch_forward(rt_guide* g, const float* rec, uint32_t n, int mode, c
     if (n == 0) return 0;
     int rc = g->ensure(n, mode == FWD_TRAIN);
     if (rc) return rc;
-    k_guide_encode<<<(n + 255) / 256, 256, 0, st>>>(g->G, rec, n, B, g->X0);
+    const uint32_t enc_grid = std::min<uint32_t>((n + 255) / 256, (uint32_t)g->sms * ENCODE_CTAS_PER_SM);
+    k_guide_encode<<<enc_grid, 256, 0, st>>>(g->G, rec, n, B, g->X0);
     uint32_t tiles = (n + TILE - 1) / TILE;
-    int grid = (int)std::min<uint32_t>((tiles + FWD_GROUPS - 1) / FWD_GROUPS, (uint32_t)g->sms * 3);
+    int grid = (int)std::min<uint32_t>((tiles + FWD_GROUPS - 1) / FWD_GROUPS, (uint32_t)g->sms);
     if (mode == FWD_TRAIN)
         k_guide_fwd<FWD_TRAIN><<<grid, FWD_THREADS, F_BYTES, st>>>(g->G, g->X0, n, B, g->acts, g->out, g->err);
     else if (mode == FWD_RENDER)
@@ -941,6 +979,18 @@ int rt_guide_infer(rt_guide* g, const float* rec_host, uint32_t n, float* raw_ho
     int rc = launch_forward(g, rec, n, FWD_RAW, 0);
     if (!rc) rc = check_err(g, 0);
     if (!rc) G_TRY(cudaMemcpy(raw_host, g->out, (size_t)n * G_OUT * 4, cudaMemcpyDeviceToHost));
+    cudaFree(rec);
+    return rc;
+}
+
+int rt_guide_infer_mixture(rt_guide* g, const float* rec_host, uint32_t n, float* mix_host) {
+    if (!g || !rec_host || !mix_host || n == 0) return gfail(-1, "bad argument");
+    float* rec = nullptr;
+    G_TRY(cudaMalloc(&rec, (size_t)n * 64));
+    G_TRY(cudaMemcpy(rec, rec_host, (size_t)n * 64, cudaMemcpyHostToDevice));
+    int rc = launch_forward(g, rec, n, FWD_RENDER, 0);
+    if (!rc) rc = check_err(g, 0);
+    if (!rc) G_TRY(cudaMemcpy(mix_host, g->out, (size_t)n * G_OUT * 4, cudaMemcpyDeviceToHost));
     cudaFree(rec);
     return rc;
 }

@@ -116,103 +116,50 @@ __device__ __forceinline__ float3 guide_normalize_pos(const GuideDev& G, float3 
 // [32 + j] and at [40 + j] the log of its weighted density at mu.w = 0,
 // A_j = log w_j + log(kappa_j / (2 pi (1 - e^{-2 kappa_j}))) - kappa_j, so that
 // q(w) = sum_j exp(A_j + kappa_j mu_j.w).
-struct Mixture {
-    float3 mu[G_LOBES];
-    float kappa[G_LOBES];
-    float w[G_LOBES];
-    float A[G_LOBES];
-};
-
-__device__ __forceinline__ void mixture_decode(const float* o, Mixture& m) {
+//
+// Raw outputs -> the decoded record (48 floats, layout above), stored as
+// it is computed so few values stay live. The logarithms are taken where
+// they are cheap: log w_j = (o_j - max) - log(sum of e^(o_i - max)), one
+// logarithm for the whole softmax, and log kappa_j is the clamped output
+// itself. log(1 - e^{-2 kappa}) uses the fast intrinsics: 1 - e^{-2 kappa}
+// >= 1 - e^{-2 e^-4} = 0.036, so its absolute error stays near 1e-6, a
+// relative 1e-6 on the density. Means are normalised with rsqrt (relative
+// error below 2^-22).
+__device__ __forceinline__ void mixture_decode_store(const float* o, float* dst) {
+    float4* d4 = reinterpret_cast<float4*>(dst);
     float mx = -1e30f;
 #pragma unroll
     for (int j = 0; j < G_LOBES; j++) mx = fmaxf(mx, o[5 * j + 4]);
-    float sw = 0.f;
+    float e[G_LOBES], k[G_LOBES], sw = 0.f;
 #pragma unroll
     for (int j = 0; j < G_LOBES; j++) {
-        float3 v = f3(o[5 * j], o[5 * j + 1], o[5 * j + 2]);
-        float len = length(v);
-        m.mu[j] = len > 1e-8f ? v / len : f3(0.f, 0.f, 1.f);
-        m.kappa[j] = __expf(fminf(fmaxf(o[5 * j + 3], -4.f), 9.f));
-        m.w[j] = __expf(o[5 * j + 4] - mx);
-        sw += m.w[j];
+        const float3 v = f3(o[5 * j], o[5 * j + 1], o[5 * j + 2]);
+        const float len2 = dot(v, v);
+        const float3 mu = len2 > 1e-16f ? v * rsqrtf(len2) : f3(0.f, 0.f, 1.f);
+        k[j] = __expf(fminf(fmaxf(o[5 * j + 3], -4.f), 9.f));
+        d4[j] = make_float4(mu.x, mu.y, mu.z, k[j]);
+        e[j] = __expf(o[5 * j + 4] - mx);
+        sw += e[j];
     }
+    const float inv_sw = __frcp_rn(sw), log_sw = __logf(sw);
+    const float log_2pi = 1.8378770664093453f;
+    float A[G_LOBES];
 #pragma unroll
     for (int j = 0; j < G_LOBES; j++) {
-        m.w[j] /= sw;
-        const float k = m.kappa[j];
-        m.A[j] = logf(fmaxf(m.w[j], 1e-30f)) + logf(k) - logf(2.f * RT_PI) - log1pf(-__expf(-2.f * k)) - k;
+        e[j] *= inv_sw;
+        const float log_k = fminf(fmaxf(o[5 * j + 3], -4.f), 9.f);
+        A[j] = (o[5 * j + 4] - mx) - log_sw + log_k - log_2pi - __logf(1.f - __expf(-2.f * k[j])) - k[j];
     }
-}
-
-// Decoded record <-> Mixture.
-__device__ __forceinline__ void mixture_store(const Mixture& m, float* dst) {
-    float4* d4 = reinterpret_cast<float4*>(dst);
-#pragma unroll
-    for (int j = 0; j < G_LOBES; j++) d4[j] = make_float4(m.mu[j].x, m.mu[j].y, m.mu[j].z, m.kappa[j]);
-    d4[8] = make_float4(m.w[0], m.w[1], m.w[2], m.w[3]);
-    d4[9] = make_float4(m.w[4], m.w[5], m.w[6], m.w[7]);
-    d4[10] = make_float4(m.A[0], m.A[1], m.A[2], m.A[3]);
-    d4[11] = make_float4(m.A[4], m.A[5], m.A[6], m.A[7]);
-}
-
-__device__ __forceinline__ void mixture_load(const float* src, Mixture& m) {
-    const float4* s4 = reinterpret_cast<const float4*>(src);
-#pragma unroll
-    for (int j = 0; j < G_LOBES; j++) {
-        float4 v = s4[j];
-        m.mu[j] = f3(v.x, v.y, v.z);
-        m.kappa[j] = v.w;
-    }
-    float4 a = s4[8], b = s4[9], c = s4[10], d = s4[11];
-    m.w[0] = a.x; m.w[1] = a.y; m.w[2] = a.z; m.w[3] = a.w;
-    m.w[4] = b.x; m.w[5] = b.y; m.w[6] = b.z; m.w[7] = b.w;
-    m.A[0] = c.x; m.A[1] = c.y; m.A[2] = c.z; m.A[3] = c.w;
-    m.A[4] = d.x; m.A[5] = d.y; m.A[6] = d.z; m.A[7] = d.w;
+    d4[8] = make_float4(e[0], e[1], e[2], e[3]);
+    d4[9] = make_float4(e[4], e[5], e[6], e[7]);
+    d4[10] = make_float4(A[0], A[1], A[2], A[3]);
+    d4[11] = make_float4(A[4], A[5], A[6], A[7]);
 }
 
 // log of the vMF density kappa / (2 pi (1 - e^{-2 kappa})) exp(kappa (mu.w - 1)).
 __device__ __forceinline__ float vmf_log_pdf(float3 mu, float kappa, float3 w) {
     float norm = logf(kappa) - logf(2.f * RT_PI) - log1pf(-__expf(-2.f * kappa));
     return norm + kappa * (dot(mu, w) - 1.f);
-}
-
-__device__ __forceinline__ float mixture_pdf(const Mixture& m, float3 w) {
-    float p = 0.f;
-#pragma unroll
-    for (int j = 0; j < G_LOBES; j++) p += __expf(m.A[j] + m.kappa[j] * dot(m.mu[j], w));
-    return p;
-}
-
-// Sample: pick a lobe by weight, then a direction around its mean
-// (W. Jakob, "Numerically stable sampling of the von Mises-Fisher
-// distribution on S^2", 2012).
-__device__ __forceinline__ float3 mixture_sample(const Mixture& m, float u0, float u1, float u2) {
-    int j = G_LOBES - 1;
-    float acc = 0.f;
-#pragma unroll
-    for (int k = 0; k < G_LOBES; k++) {
-        acc += m.w[k];
-        if (u0 < acc) {
-            j = k;
-            break;
-        }
-    }
-    float kappa = 0.f;
-    float3 mu = f3(0, 0, 1);
-#pragma unroll
-    for (int k = 0; k < G_LOBES; k++)
-        if (k == j) {
-            kappa = m.kappa[k];
-            mu = m.mu[k];
-        }
-    float wz = 1.f + logf(u1 + (1.f - u1) * __expf(-2.f * kappa)) / kappa;
-    wz = fminf(fmaxf(wz, -1.f), 1.f);
-    float sr = sqrtf(fmaxf(1.f - wz * wz, 0.f)), s, c;
-    sincosf(2.f * RT_PI * u2, &s, &c);
-    float3 t = fabsf(mu.x) > 0.9f ? f3(0, 1, 0) : f3(1, 0, 0);
-    float3 a = normalize_ref(cross(mu, t)), b = cross(mu, a);
-    return normalize_ref(a * (sr * c) + b * (sr * s) + mu * wz);
 }
 
 // The renderer's view of a decoded mixture: read in place from its record
@@ -235,6 +182,9 @@ __device__ __forceinline__ float mixture_pdf(const MixtureRef& m, float3 w) {
     return p;
 }
 
+// Sample: pick a lobe by weight, then a direction around its mean
+// (W. Jakob, "Numerically stable sampling of the von Mises-Fisher
+// distribution on S^2", 2012).
 __device__ __forceinline__ float3 mixture_sample(const MixtureRef& m, float u0, float u1, float u2) {
     const float4 w0 = m.p[8], w1 = m.p[9];
     const float wt[G_LOBES] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};

@@ -145,14 +145,15 @@ __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.
 // Barrier over the 128 threads of tile group `grp` (named barrier 1 + grp;
 // immediate ids, so the kernel reserves only the barriers it uses).
 __device__ __forceinline__ void group_sync(uint32_t grp) {
-    if (grp == 0)
-        asm volatile("bar.sync 1, 128;" ::: "memory");
-    else if (grp == 1)
-        asm volatile("bar.sync 2, 128;" ::: "memory");
-    else if (grp == 2)
-        asm volatile("bar.sync 3, 128;" ::: "memory");
-    else
-        asm volatile("bar.sync 4, 128;" ::: "memory");
+    switch (grp) {
+        case 0: asm volatile("bar.sync 1, 128;" ::: "memory"); break;
+        case 1: asm volatile("bar.sync 2, 128;" ::: "memory"); break;
+        case 2: asm volatile("bar.sync 3, 128;" ::: "memory"); break;
+        case 3: asm volatile("bar.sync 4, 128;" ::: "memory"); break;
+        case 4: asm volatile("bar.sync 5, 128;" ::: "memory"); break;
+        case 5: asm volatile("bar.sync 6, 128;" ::: "memory"); break;
+        default: asm volatile("bar.sync 7, 128;" ::: "memory"); break;
+    }
 }
 
 // Issue D = A * B^T for a 128-row tile (thread 0 of the CTA issues).

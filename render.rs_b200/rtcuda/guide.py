@@ -13,7 +13,8 @@ OUTPUTS = 48
 
 # Every entry point declared in include/rt_guide.h.
 EXPORTS = ("rt_guide_create", "rt_guide_destroy", "rt_guide_last_error", "rt_guide_train_step",
-           "rt_guide_train_step_device", "rt_guide_infer", "rt_guide_infer_device", "rt_guide_grads",
+           "rt_guide_train_step_device", "rt_guide_infer", "rt_guide_infer_device", "rt_guide_infer_mixture",
+           "rt_guide_grads",
            "rt_guide_get_params", "rt_guide_set_params", "rt_guide_info", "rt_tc_gemm_selftest")
 
 
@@ -28,6 +29,7 @@ def _g():
         L.rt_guide_train_step_device.argtypes = [vp, vp, u32, vp, vp]
         L.rt_guide_infer.argtypes = [vp, vp, u32, vp]
         L.rt_guide_infer_device.argtypes = [vp, vp, u32, vp, vp]
+        L.rt_guide_infer_mixture.argtypes = [vp, vp, u32, vp]
         L.rt_guide_grads.argtypes = [vp, vp, u32, vp, vp, vp, vp]
         L.rt_guide_get_params.argtypes = [vp, vp, vp]
         L.rt_guide_set_params.argtypes = [vp, vp, vp]
@@ -92,6 +94,14 @@ class Guide:
         r = np.ascontiguousarray(records, dtype=np.float32)
         out = np.zeros((len(r), OUTPUTS), dtype=np.float32)
         _check(_g().rt_guide_infer(self.h, r.ctypes.data, len(r), out.ctypes.data))
+        return out
+
+    def infer_mixture(self, records):
+        """The decoded mixture the renderer samples from (48 floats per
+        record: 8 x (mu, kappa), 8 weights, 8 log-density offsets A)."""
+        r = np.ascontiguousarray(records, dtype=np.float32)
+        out = np.zeros((len(r), OUTPUTS), dtype=np.float32)
+        _check(_g().rt_guide_infer_mixture(self.h, r.ctypes.data, len(r), out.ctypes.data))
         return out
 
     def grads(self, records, table=True):

@@ -77,6 +77,48 @@ def test_forward_matches_oracle(guide):
     assert diff.max() < 2e-2, diff.max()
 
 
+def _decode_f64(raw):
+    """The renderer's mixture from raw outputs, in f64: normalised means,
+    kappa = exp(clamp(., -4, 9)), softmax weights and the log-density offsets
+    A_j = log w_j + log(kappa_j / (2 pi (1 - e^{-2 kappa_j}))) - kappa_j."""
+    o = raw[:, :40].astype(np.float64).reshape(-1, 8, 5)
+    v = o[..., :3]
+    n = np.linalg.norm(v, axis=2, keepdims=True)
+    mu = np.where(n > 1e-8, v / np.maximum(n, 1e-300), np.array([0.0, 0.0, 1.0]))
+    lk = np.clip(o[..., 3], -4, 9)
+    k = np.exp(lk)
+    z = o[..., 4] - o[..., 4].max(axis=1, keepdims=True)
+    logw = z - np.log(np.exp(z).sum(axis=1, keepdims=True))
+    A = logw + lk - np.log(2 * np.pi) - np.log(-np.expm1(-2 * k)) - k
+    return mu, k, np.exp(logw), A
+
+
+def test_decoded_mixture_matches_raw_outputs():
+    """The forward pass's decoded mixture (what the renderer samples from and
+    evaluates) against an f64 decode of the same network's raw outputs, over
+    outputs spread across the whole kappa range and sharp weight logits."""
+    g = Guide((-1, -1, -1), (1, 1, 1), seed=4)
+    m, t = g.params()
+    rng = np.random.default_rng(12)
+    m = m * 3.0
+    m[-48:] = rng.normal(scale=4.0, size=48)       # output biases: kappa from clamp to clamp
+    g.set_params(mlp=m, table16=np.float16(rng.normal(scale=0.5, size=t.size)).view(np.uint16))
+    rec = _records(4096, 7)
+    raw = g.infer(rec)
+    mix = g.infer_mixture(rec)
+    g.close()
+    mu, k, w, A = _decode_f64(raw)
+    lobes = mix[:, :32].reshape(-1, 8, 4)
+    assert np.abs(lobes[..., :3] - mu).max() < 1e-6
+    assert (np.abs(lobes[..., 3] - k) <= 2e-6 * k).all()
+    assert np.abs(mix[:, 32:40] - w).max() < 1e-6
+    # A sums terms up to e^9 in f32 (-kappa, and logits far below the
+    # largest): its rounding, and kappa's relative 1e-6, grow with |A| and kappa.
+    err = np.abs(mix[:, 40:48] - A)
+    assert (err <= 2e-5 + 1e-6 * (np.abs(A) + k)).all(), err.max()
+    assert k.min() < 0.02 and k.max() > 8000 and w.min() < 1e-3
+
+
 def test_gradients_match_oracle(guide):
     rec = _records(512, 2)
     m, t = guide.params()
