@@ -195,17 +195,17 @@ def ratio_ci(plain, guided, ref, z=1.96):
     return float(r), [float(r - h), float(r + h)]
 
 
-def equal_time_plain(scene, params, budget_ms):
-    """Plain render for the same device time as `budget_ms`: whole slabs at a
-    time (the session's own slab size, so no pass runs in an undersized
-    slab) until the summed device time reaches the budget. Returns (image,
-    passes, device ms)."""
+def equal_time_plain(scene, params, budget_ms, first=64):
+    """Plain render for the same device time as `budget_ms`: `first` passes,
+    then whole slabs at a time (the session's own slab size, so no pass runs
+    in an undersized slab) until the summed device time reaches the budget.
+    Returns (image, passes, device ms)."""
     from rtcuda import PtSession
     with PtSession(scene, params) as g:
-        g.render_samples(0, 64)
+        g.render_samples(0, first)
         st = g.stats()
-        done, ms = 64, st["total_ms"]
-        slab = max(1, -(-64 // max(1, st["slabs"])))
+        done, ms = first, st["total_ms"]
+        slab = max(1, -(-first // max(1, st["slabs"])))
         while ms < budget_ms:
             g.render_samples(done, slab)
             done += slab
@@ -411,8 +411,9 @@ def guided_forest(width=480, height=270, budget=128, ref_spp=512):
     `width` x `height`, `budget` guided passes from an untrained network
     against plain passes in the same device time, relMSE against a GPU
     reference of `ref_spp` passes (two halves; its own noise is removed in
-    `ratio_corrected`). The full-size comparison against a 4,096-spp f64 crop
-    is hours of CPU time and is not run."""
+    `ratio_corrected`). The comparison against a 4,096-spp f64 crop is hours
+    of CPU time and is not run; `--mode guided-forest --res 3840x2160` runs
+    this one at the full frame size."""
     from rtcuda import PtSession, abi, scenes
     s = scenes.forest(width, height)
     cfg = scenes.FOREST
@@ -429,12 +430,15 @@ def guided_forest(width=480, height=270, budget=128, ref_spp=512):
         g.render_samples(0, budget)
         guided_ms = g.stats()["total_ms"]
         guided = g.image()
-    plain, plain_spp, plain_ms = equal_time_plain(s, plain_p, guided_ms)
+    plain, plain_spp, plain_ms = equal_time_plain(s, plain_p, guided_ms, first=min(64, max(1, budget // 8)))
     e_p, e_g = rel_mse(plain, ref), rel_mse(guided, ref)
     return {"scene": f"forest_{width}x{height}_depth{cfg['max_depth']}", "guided_spp": budget,
             "guided_ms": round(guided_ms, 1), "plain_spp": plain_spp, "plain_ms": round(plain_ms, 1),
             "gpu_reference_spp": ref_spp, "relmse_plain": e_p, "relmse_guided": e_g, "ratio": e_p / e_g,
-            "gpu_ref_relmse": ref_err,
+            "ratio_ci95": ratio_ci(plain, guided, ref)[1],
+            # Plain's last slab overshoots the guided time a little; relMSE
+            # falls as 1/time, so this scales plain's error to the guided time.
+            "ratio_time_scaled": e_p * plain_ms / guided_ms / e_g, "gpu_ref_relmse": ref_err,
             "ratio_corrected": (e_p - ref_err) / (e_g - ref_err) if e_g > ref_err else None}
 
 
@@ -564,9 +568,12 @@ def main():
     ap.add_argument("--scene", default="forest",
                     help="--mode scene: cornell, cloud, instanced, two_rooms, forest, media, furball")
     ap.add_argument("--res", default="640x360", help="--mode scene: frame size WxH")
-    ap.add_argument("--mode", default="full", choices=["full", "traversal", "guided", "scene"],
+    ap.add_argument("--mode", default="full", choices=["full", "traversal", "guided", "scene", "guided-forest"],
                     help="traversal: only the closest/any-hit ray batches; guided: only the learned-proposal "
-                         "workload; scene: one named scene (all for profiler captures)")
+                         "workload; scene: one named scene (all for profiler captures); guided-forest: the "
+                         "forest's equal-time guided-vs-plain comparison at --res with --steps guided passes "
+                         "and a --ref-spp GPU reference")
+    ap.add_argument("--ref-spp", type=int, default=512, help="--mode guided-forest: passes of the GPU reference")
     ap.add_argument("--rays", type=int, default=N_RAYS)
     ap.add_argument("--no-guided", action="store_true", help="skip the guided equal-time comparisons")
     ap.add_argument("--no-workloads", action="store_true", help="skip the other configurations")
@@ -579,6 +586,10 @@ def main():
         return run_guided(args)
     if args.mode == "scene":
         return run_scene(args)
+    if args.mode == "guided-forest":
+        w, h = (int(v) for v in args.res.split("x"))
+        print(json.dumps({"mode": "guided-forest", **guided_forest(w, h, args.steps, args.ref_spp)}), flush=True)
+        return 0
 
     import torch
     import torch.distributed as dist
