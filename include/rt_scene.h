@@ -51,6 +51,25 @@ typedef struct rt_instance_desc {
     uint32_t material_id;
 } rt_instance_desc;
 
+/* Motion blur: shutter-close endpoints (the reference's
+ * `Instance::transform1`, mesh.rs:230-235, `Mesh::positions1`,
+ * mesh.rs:29-31). Rays draw a shutter time t in [0, 1) per sample when a
+ * scene has any endpoint or camera motion (pt/mod.rs:339-356); a moving
+ * instance is placed by the component-wise lerp of its two transforms at t
+ * (`Instance::transforms_at`, mesh.rs:295-304), a deforming mesh by the
+ * lerp of its two vertex positions (`Mesh::vertex_at`, mesh.rs:96-111). */
+typedef struct rt_instance_motion {
+    uint32_t instance;            /* index into rt_scene_desc::instances */
+    uint32_t reserved;            /* 0 */
+    double   object_to_world1[12]; /* row-major upper 3x4 at shutter close */
+} rt_instance_motion;
+
+typedef struct rt_mesh_motion {
+    uint32_t     mesh;            /* index into rt_scene_desc::meshes */
+    uint32_t     reserved;        /* 0 */
+    const float* positions1;      /* 3 * n_vertices at shutter close (same topology) */
+} rt_mesh_motion;
+
 /* Curve set: `CurveSet` (src/geometry/curves.rs:15-26), rounded-cone
  * segments (a swept sphere whose radius goes linearly from the start's to
  * the end's; equal ends make a point particle a sphere). */
@@ -327,6 +346,16 @@ typedef struct rt_scene_desc {
     const rt_curves_desc*     curves;
     uint32_t n_curves;
     uint32_t curves_reserved; /* 0 */
+    /* Motion blur (all NULL / 0 in a static scene): moving instances,
+     * deforming meshes (each named at most once), and camera motion, the
+     * row-major upper 3x4 of `Camera::motion_inv` (camera.rs:85-146): camera
+     * rays at time t are transformed by lerp(I, camera_motion_inv, t), their
+     * direction renormalised. Analytic quadrics do not move. */
+    const rt_instance_motion* instance_motion;
+    uint32_t n_instance_motion;
+    uint32_t n_mesh_motion;
+    const rt_mesh_motion*     mesh_motion;
+    const double*             camera_motion_inv;
 } rt_scene_desc;
 
 /* Integrator knobs. The reference hard-codes these as constants
@@ -358,6 +387,8 @@ static_assert(sizeof(rt_mesh_desc) == 40, "rt_mesh_desc layout");
 static_assert(sizeof(rt_instance_desc) == 104, "rt_instance_desc layout");
 static_assert(sizeof(rt_material_desc) == 376, "rt_material_desc layout");
 static_assert(sizeof(rt_curves_desc) == 40, "rt_curves_desc layout");
+static_assert(sizeof(rt_instance_motion) == 104, "rt_instance_motion layout");
+static_assert(sizeof(rt_mesh_motion) == 16, "rt_mesh_motion layout");
 static_assert(sizeof(rt_medium_desc) == 136, "rt_medium_desc layout");
 static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
 static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
@@ -368,7 +399,7 @@ static_assert(sizeof(rt_texture_desc) == 16, "rt_texture_desc layout");
 static_assert(sizeof(rt_pattern_binding) == 16, "rt_pattern_binding layout");
 static_assert(sizeof(rt_ies_desc) == 112, "rt_ies_desc layout");
 static_assert(sizeof(rt_quadric_desc) == 168, "rt_quadric_desc layout");
-static_assert(sizeof(rt_scene_desc) == 344, "rt_scene_desc layout");
+static_assert(sizeof(rt_scene_desc) == 376, "rt_scene_desc layout");
 }
 #endif
 

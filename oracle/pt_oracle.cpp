@@ -69,6 +69,13 @@ static M4 identity() {
     for (int i = 0; i < 4; i++) r.m[i][i] = 1.0;
     return r;
 }
+// matrix.rs:228-240 component-wise interpolation toward b.
+static M4 lerp(const M4& a, const M4& b, double t) {
+    M4 r;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) r.m[i][j] = a.m[i][j] + (b.m[i][j] - a.m[i][j]) * t;
+    return r;
+}
 // matrix.rs: inverse via cofactors; None when |det| < EPSILON.
 static bool inverse(const M4& a, M4& out) {
     const double(*m)[4] = a.m;
@@ -198,11 +205,14 @@ struct Aabb {
     }
 };
 
+// `time`: the shutter time in [0, 1) the ray samples (0 in static scenes);
+// every ray of a path carries the camera ray's (`Ray::with_time`).
 struct Ray {
     V3 o, d;
+    double time = 0.0;
 };
 // raytracer/ray.rs:13-19 — Ray::new normalises the direction.
-static inline Ray make_ray(V3 o, V3 d) { return {o, normalize(d)}; }
+static inline Ray make_ray(V3 o, V3 d, double time = 0.0) { return {o, normalize(d), time}; }
 
 struct Counters {
     uint64_t pops = 0, tris = 0, insts = 0;
@@ -398,12 +408,19 @@ struct Mesh {
     std::vector<uint32_t> idx;
     std::vector<float> nrm;  // empty when absent
     std::vector<float> st;   // 2 per vertex; empty when absent
+    std::vector<float> pos1; // positions at shutter close (deformation blur); empty when static
     Bvh blas;
     Aabb local_bounds;
 
     V3 vertex(uint32_t i) const { return {(double)pos[3 * i], (double)pos[3 * i + 1], (double)pos[3 * i + 2]}; }
+    // mesh.rs:96-111 vertex at shutter time (lerped toward the endpoint).
+    V3 vertex_at(uint32_t i, double time) const {
+        if (pos1.empty() || !(time > 0.0)) return vertex(i);
+        V3 a = vertex(i), b{(double)pos1[3 * i], (double)pos1[3 * i + 1], (double)pos1[3 * i + 2]};
+        return {a.x + (b.x - a.x) * time, a.y + (b.y - a.y) * time, a.z + (b.z - a.z) * time};
+    }
 
-    void build() {  // mesh.rs:45-86
+    void build() {  // mesh.rs:45-86: triangle boxes cover both endpoints when deforming
         size_t n = idx.size() / 3;
         std::vector<Aabb> bounds(n);
         for (size_t t = 0; t < n; t++) {
@@ -411,18 +428,21 @@ struct Mesh {
             b.grow_point(vertex(idx[3 * t]));
             b.grow_point(vertex(idx[3 * t + 1]));
             b.grow_point(vertex(idx[3 * t + 2]));
+            if (!pos1.empty())
+                for (int k = 0; k < 3; k++) b.grow_point(vertex_at(idx[3 * t + k], 1.0));
             bounds[t] = b;
             local_bounds.grow(b);
         }
         blas.build(bounds);
     }
 
-    // mesh.rs:117-142 Möller–Trumbore (parametric t along the local ray).
+    // mesh.rs:117-142 Möller–Trumbore (parametric t along the local ray),
+    // against the triangle at the ray's shutter time.
     bool intersect_triangle(const Ray& r, uint32_t tri, double t_max, double* t_out, double* u_out,
                             double* v_out) const {
-        V3 v0 = vertex(idx[3 * tri]);
-        V3 e1 = vertex(idx[3 * tri + 1]) - v0;
-        V3 e2 = vertex(idx[3 * tri + 2]) - v0;
+        V3 v0 = vertex_at(idx[3 * tri], r.time);
+        V3 e1 = vertex_at(idx[3 * tri + 1], r.time) - v0;
+        V3 e2 = vertex_at(idx[3 * tri + 2], r.time) - v0;
         V3 p = cross(r.d, e2);
         double det = dot(e1, p);
         if (std::fabs(det) < 1e-14) return false;
@@ -441,16 +461,18 @@ struct Mesh {
         return true;
     }
 
-    // mesh.rs:200-220 interpolated or geometric local normal.
-    V3 local_normal(uint32_t tri, double u, double v) const {
+    // mesh.rs:200-220 interpolated or geometric local normal; a deforming
+    // mesh takes the geometric normal at the shutter time (vertex normals
+    // are authored for the rest pose).
+    V3 local_normal(uint32_t tri, double u, double v, double time = 0.0) const {
         uint32_t i0 = idx[3 * tri], i1 = idx[3 * tri + 1], i2 = idx[3 * tri + 2];
-        if (!nrm.empty()) {
+        if (!nrm.empty() && pos1.empty()) {
             auto n = [&](uint32_t i) { return V3{nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]}; };
             double w = 1.0 - u - v;
             return normalize(n(i0) * w + n(i1) * u + n(i2) * v);
         }
-        V3 v0 = vertex(i0);
-        return normalize(cross(vertex(i1) - v0, vertex(i2) - v0));
+        V3 v0 = vertex_at(i0, time);
+        return normalize(cross(vertex_at(i1, time) - v0, vertex_at(i2, time) - v0));
     }
 
     // mesh.rs:147-173 local gradients of s and t within the triangle's
@@ -590,8 +612,19 @@ struct Instance {
     uint32_t mesh_id = 0, material_id = 0;
     bool curves = false;  // GeomKind::Curves: mesh_id indexes the curve sets
     M4 transform, inv;
+    bool moving = false;  // transform1 holds the shutter-close endpoint
+    M4 transform1;
     Aabb world_bounds;
     double scale = 1.0;  // Matrix4::approx_scale (math/matrix.rs:246-251)
+
+    // mesh.rs:295-304 Instance::transforms_at: the inverse at shutter time
+    // (the lerped transform inverted, identity when singular).
+    M4 inv_at(double time) const {
+        if (!moving || !(time > 0.0)) return inv;
+        M4 r;
+        if (!inverse(lerp(transform, transform1, time), r)) r = identity();
+        return r;
+    }
 };
 
 // ---- analytic quadrics (src/geometry/sphere.rs, cylinder.rs, cone.rs, extra.rs) ----
@@ -2412,6 +2445,16 @@ struct Camera {
     double lens_radius, focal_distance;
     int filter;
     double filter_width;
+    bool moving = false;  // camera.rs:87-92 motion_inv present
+    M4 motion_inv;
+
+    // camera.rs:134-146 Camera::apply_motion: lerp(I, motion_inv, t) applied
+    // to the ray, direction renormalised.
+    Ray apply_motion(Ray r) const {
+        if (!moving || !(r.time > 0.0)) return r;
+        const M4 m = lerp(identity(), motion_inv, r.time);
+        return {xf_point(m, r.o), normalize(xf_vec(m, r.d)), r.time};
+    }
 
     double sample_1d(double u) const {  // camera.rs:36-61
         switch (filter) {
@@ -2464,6 +2507,7 @@ struct Scene {
     std::vector<Texture> textures;
     std::vector<Medium> media;  // Scene::media
     int32_t atmosphere = -1;     // Scene::atmosphere
+    bool has_motion = false;     // scene/mod.rs:42-44: rays draw a shutter time
 
     // A volume hull (pt/mod.rs:662-667, 1280-1284): an interior medium, no
     // lobes, no emission -- the surface only bounds the medium.
@@ -2558,7 +2602,8 @@ struct Scene {
         auto inst_isect = [&](uint32_t ii, double t_max, double* t_out) -> bool {
             const Instance& in = instances[ii];
             if (c) c->insts++;
-            Ray lr{xf_point(in.inv, ray.o), xf_vec(in.inv, ray.d)};
+            const M4 iv = in.inv_at(ray.time);
+            Ray lr{xf_point(iv, ray.o), xf_vec(iv, ray.d), ray.time};
             double hu = 0, hv = 0;
             uint32_t tri;
             double t;
@@ -2583,14 +2628,15 @@ struct Scene {
         if (!tlas.traverse(ray.o, ray.d, t_budget, inst_isect, &winner, &tw, c)) return have_q;
         if (have_q && !(length(ray.d * tw) < out->t)) return true;
         const Instance& in = instances[best.inst];
+        const M4 iv = in.inv_at(ray.time);  // mesh.rs:315: normals through the inverse at shutter time
         if (in.curves) {
             // mesh.rs:323-344: the segment's normal and tangent, st = (0.5, v).
             const CurveSet& cs = curve_sets[in.mesh_id];
-            Ray lr{xf_point(in.inv, ray.o), xf_vec(in.inv, ray.d)};
+            Ray lr{xf_point(iv, ray.o), xf_vec(iv, ray.d), ray.time};
             double t, v;
             V3 n, tg;
             cs.intersect_segment(lr, best.tri, INF, &t, &n, &tg, &v);
-            V3 wn = normalize(xf_normal(in.inv, n));
+            V3 wn = normalize(xf_normal(iv, n));
             V3 point = ray.o + ray.d * tw;
             bool front = dot(wn, ray.d) < 0.0;
             if (!front) wn = -wn;
@@ -2609,8 +2655,8 @@ struct Scene {
             return true;
         }
         const Mesh& m = meshes[in.mesh_id];
-        V3 ln = m.local_normal(best.tri, best.u, best.v);
-        V3 wn = normalize(xf_normal(in.inv, ln));
+        V3 ln = m.local_normal(best.tri, best.u, best.v, ray.time);
+        V3 wn = normalize(xf_normal(iv, ln));
         // mesh.rs:427-439 to_intersection.
         V3 point = ray.o + ray.d * tw;
         bool front = dot(wn, ray.d) < 0.0;
@@ -2744,6 +2790,7 @@ struct Tracer {
     const rt_params& prm;
     uint64_t ext_rays = 0, shadow_rays = 0;
     Counters cext, cshadow;  // traversal work of extension / shadow rays
+    double time_ = 0.0;      // the current path's shutter time: every ray it traces carries it
     // Angular size of one pixel, the initial ray-cone spread (pt/mod.rs:73-76).
     double pixel_spread() const { return std::tan(sc.cam.fov * PI / 180.0 / 2.0) * 2.0 / (double)sc.cam.height; }
 
@@ -2758,7 +2805,7 @@ struct Tracer {
         for (int k = 0; k < MAX_PRESENCE_SKIPS; k++) {
             shadow_rays++;
             Hit h;
-            Ray r = make_ray(origin, dir);
+            Ray r = make_ray(origin, dir, time_);
             const bool found = sc.intersect(r, &h, &cshadow);
             const double seg = std::fmin(found ? h.t : remaining, remaining);
             const int32_t cur = ms.current();
@@ -2928,6 +2975,7 @@ struct Tracer {
 
     // mod.rs:449-990 trace_full.
     V3 trace(Ray ray, Pcg32& rng, Aux& aux) {
+        time_ = ray.time;
         V3 L{0, 0, 0};
         int first_specular = -1;  // -1 None, 0 false, 1 true
         bool aux_set = false;
@@ -3036,7 +3084,7 @@ struct Tracer {
                     prev_origin = p;
                     from_camera = false;
                     cone_spread += 0.4;
-                    ray = make_ray(p, wi);
+                    ray = make_ray(p, wi, time_);
                     depth++;
                     if (!roulette()) break;
                     continue;
@@ -3071,7 +3119,7 @@ struct Tracer {
                 travel += hit.t;
                 if (hit.front_face) med_stack.push((uint32_t)sc.materials[hit.material_id].interior);
                 else med_stack.pop();
-                ray = make_ray(hit.point + normalize(ray.d) * RAY_OFFSET, ray.d);
+                ray = make_ray(hit.point + normalize(ray.d) * RAY_OFFSET, ray.d, time_);
                 continue;
             }
             V3 wo = -normalize(ray.d);
@@ -3091,7 +3139,7 @@ struct Tracer {
             if (presence < 1.0 && rng.next_f64() >= presence && presence_skips < MAX_PRESENCE_SKIPS) {
                 presence_skips++;
                 travel += hit.t;
-                ray = make_ray(hit.point + normalize(ray.d) * RAY_OFFSET, ray.d);
+                ray = make_ray(hit.point + normalize(ray.d) * RAY_OFFSET, ray.d, time_);
                 continue;
             }
             bool entering = hit.front_face;
@@ -3142,7 +3190,7 @@ struct Tracer {
                 from_camera = false;
                 cone_spread += 0.4;
                 const V3 side = dot(wi, hit.normal) >= 0.0 ? hit.normal : -hit.normal;
-                ray = make_ray(hit.point + side * RAY_OFFSET, wi);
+                ray = make_ray(hit.point + side * RAY_OFFSET, wi, time_);
                 depth++;
                 if (!roulette()) break;
                 continue;
@@ -3155,7 +3203,7 @@ struct Tracer {
                 const double e1 = rng.next_f64(), e2 = rng.next_f64();
                 const double er = std::sqrt(e1), ephi = 2.0 * PI * e2;
                 Ray walk = make_ray(hit.point - n * RAY_OFFSET,
-                                    entry.to_world(V3{er * std::cos(ephi), er * std::sin(ephi), std::sqrt(std::fmax(1.0 - e1, 0.0))}));
+                                    entry.to_world(V3{er * std::cos(ephi), er * std::sin(ephi), std::sqrt(std::fmax(1.0 - e1, 0.0))}), time_);
                 bool exited = false;
                 for (int step = 0; step < 256; step++) {
                     Hit wh;
@@ -3167,7 +3215,7 @@ struct Tracer {
                         const V3 p = walk.o + walk.d * ev.t;
                         const double u = rng.next_f64(), v = rng.next_f64();
                         const double z = 1.0 - 2.0 * u, rr = std::sqrt(std::fmax(1.0 - z * z, 0.0)), ph = 2.0 * PI * v;
-                        walk = make_ray(p, V3{rr * std::cos(ph), rr * std::sin(ph), z});
+                        walk = make_ray(p, V3{rr * std::cos(ph), rr * std::sin(ph), z}, time_);
                         const double q = std::fmin(max_comp(beta), 0.95);
                         if (q <= 0.0 || (step > 8 && rng.next_f64() > q)) break;
                         if (step > 8) beta = beta / q;
@@ -3197,7 +3245,7 @@ struct Tracer {
                     prev_origin = exit_p;
                     from_camera = false;
                     cone_spread += 0.4;
-                    ray = make_ray(exit_p + out_n * RAY_OFFSET, xf.to_world(local));
+                    ray = make_ray(exit_p + out_n * RAY_OFFSET, xf.to_world(local), time_);
                     exited = true;
                     break;
                 }
@@ -3241,7 +3289,7 @@ struct Tracer {
                 else med_stack.pop();
             }
             double off = s.transmitted ? -RAY_OFFSET : RAY_OFFSET;
-            ray = make_ray(hit.point + n * off, wi_world);
+            ray = make_ray(hit.point + n * off, wi_world, time_);
             depth++;
             if (!roulette()) break;
         }
@@ -3367,7 +3415,11 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
         m.idx.assign(md.indices, md.indices + 3ull * md.n_triangles);
         if (md.normals) m.nrm.assign(md.normals, md.normals + 3ull * md.n_vertices);
         if (md.st) m.st.assign(md.st, md.st + 2ull * md.n_vertices);
+        for (uint32_t k = 0; k < d->n_mesh_motion && d->mesh_motion; k++)
+            if (d->mesh_motion[k].mesh == i && d->mesh_motion[k].positions1)
+                m.pos1.assign(d->mesh_motion[k].positions1, d->mesh_motion[k].positions1 + 3ull * md.n_vertices);
         m.build();
+        s.has_motion |= !m.pos1.empty();
     }
     s.curve_sets.resize(d->curves ? d->n_curves : 0);
     for (uint32_t k = 0; k < s.curve_sets.size(); k++) {
@@ -3394,11 +3446,29 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
         double lx = length(xf_vec(in.transform, V3{1, 0, 0})), ly = length(xf_vec(in.transform, V3{0, 1, 0})),
                lz = length(xf_vec(in.transform, V3{0, 0, 1}));
         in.scale = std::fmax(std::cbrt(lx * ly * lz), 1e-12);
-        // mesh.rs:283-297 world bounds from the 8 transformed corners.
+        ib[i] = Aabb{};
+    }
+    for (uint32_t k = 0; k < d->n_instance_motion && d->instance_motion; k++) {
+        const rt_instance_motion& im = d->instance_motion[k];
+        if (im.instance >= d->n_instances) continue;
+        Instance& in = s.instances[im.instance];
+        in.moving = true;
+        in.transform1 = identity();
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 4; c++) in.transform1.m[r][c] = im.object_to_world1[r * 4 + c];
+        s.has_motion = true;
+    }
+    for (uint32_t i = 0; i < d->n_instances; i++) {
+        Instance& in = s.instances[i];
+        // mesh.rs:276-290 world bounds from the 8 transformed corners, at
+        // both shutter endpoints when moving.
         const Aabb& lb = in.curves ? s.curve_sets[in.mesh_id].local_bounds : s.meshes[in.mesh_id].local_bounds;
-        for (int k = 0; k < 8; k++) {
-            V3 corner{(k & 1) ? lb.mx.x : lb.mn.x, (k & 2) ? lb.mx.y : lb.mn.y, (k & 4) ? lb.mx.z : lb.mn.z};
-            in.world_bounds.grow_point(xf_point(in.transform, corner));
+        for (const M4* xf : {&in.transform, in.moving ? &in.transform1 : nullptr}) {
+            if (!xf) continue;
+            for (int k = 0; k < 8; k++) {
+                V3 corner{(k & 1) ? lb.mx.x : lb.mn.x, (k & 2) ? lb.mx.y : lb.mn.y, (k & 4) ? lb.mx.z : lb.mn.z};
+                in.world_bounds.grow_point(xf_point(*xf, corner));
+            }
         }
         ib[i] = in.world_bounds;
     }
@@ -3470,6 +3540,13 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
     s.cam.focal_distance = c.focal_distance;
     s.cam.filter = c.filter;
     s.cam.filter_width = c.filter_width;
+    if (d->camera_motion_inv) {
+        s.cam.moving = true;
+        s.cam.motion_inv = identity();
+        for (int r = 0; r < 3; r++)
+            for (int k = 0; k < 4; k++) s.cam.motion_inv.m[r][k] = d->camera_motion_inv[r * 4 + k];
+        s.has_motion = true;  // scene_builder.rs:239-241
+    }
     s.background = v3(d->background);
     return os;
 }
@@ -3552,6 +3629,10 @@ int oracle_render(const oracle_scene* os, const rt_params* p, const uint32_t* pi
                     lv = rng.next_f64();
                 }
                 Ray ray = s.cam.generate(px, py, lu, lv);
+                if (s.has_motion) {  // mod.rs:350-353 shutter time, camera motion
+                    ray.time = rng.next_f64();
+                    ray = s.cam.apply_motion(ray);
+                }
                 Aux aux;
                 V3 l = tr.trace(ray, rng, aux);
                 double lm = lum(l);

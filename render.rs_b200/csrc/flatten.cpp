@@ -989,6 +989,11 @@ void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>
                 std::vector<uint2>* items, HostScene* H) {
     const uint32_t n = d->n_instances;
     bool dense = false;
+    // Shutter-close transforms of moving instances (mesh.rs:276-290: their
+    // world boxes cover both endpoints; a corner moves on a segment under
+    // the lerped transform, so the union of the two boxes bounds it).
+    std::vector<const double*> xf1(n, nullptr);
+    for (uint32_t k = 0; k < d->n_instance_motion; k++) xf1[d->instance_motion[k].instance] = d->instance_motion[k].object_to_world1;
     // World boxes of one instance's frontier (`list` per mesh), their union,
     // and how many items it becomes: every child in a dense scene, else the
     // children when their summed area is below RT_BRAID_RATIO x the union's.
@@ -999,7 +1004,8 @@ void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>
         const auto& rc = list[id.mesh_id];
         double sum = 0.0;
         for (size_t k = 0; k < rc.size(); k++) {
-            const Box wb = world_box(id.object_to_world, rc[k].lo, rc[k].hi);
+            Box wb = world_box(id.object_to_world, rc[k].lo, rc[k].hi);
+            if (xf1[i]) wb.grow(world_box(xf1[i], rc[k].lo, rc[k].hi));
             if (cb) cb[k] = wb;
             u->grow(wb);
             sum += wb.area();
@@ -1210,6 +1216,55 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         *err = "curves pointer is NULL";
         return false;
     }
+    // ---- motion blur endpoints (mesh.rs:29-31, 230-235) -------------------------
+    std::vector<const float*> pos1(d->n_meshes, nullptr);
+    if (d->n_mesh_motion && !d->mesh_motion) {
+        *err = "mesh_motion pointer is NULL";
+        return false;
+    }
+    if (d->n_instance_motion && !d->instance_motion) {
+        *err = "instance_motion pointer is NULL";
+        return false;
+    }
+    for (uint32_t k = 0; k < d->n_mesh_motion; k++) {
+        const rt_mesh_motion& mm = d->mesh_motion[k];
+        if (mm.mesh >= d->n_meshes || !mm.positions1 || pos1[mm.mesh]) {
+            *err = "mesh motion " + std::to_string(k) + " names a missing or repeated mesh, or has no positions";
+            return false;
+        }
+        const rt_mesh_desc& md = d->meshes[mm.mesh];
+        for (size_t v = 0; v < 3ull * md.n_vertices; v++)
+            if (!std::isfinite(mm.positions1[v])) {
+                *err = "mesh motion " + std::to_string(k) + " has a non-finite position";
+                return false;
+            }
+        pos1[mm.mesh] = mm.positions1;
+    }
+    std::vector<const double*> xf1(d->n_instances, nullptr);
+    for (uint32_t k = 0; k < d->n_instance_motion; k++) {
+        const rt_instance_motion& im = d->instance_motion[k];
+        if (im.instance >= d->n_instances || xf1[im.instance]) {
+            *err = "instance motion " + std::to_string(k) + " names a missing or repeated instance";
+            return false;
+        }
+        for (int j = 0; j < 12; j++)
+            if (!std::isfinite(im.object_to_world1[j])) {
+                *err = "instance motion " + std::to_string(k) + " has a non-finite transform";
+                return false;
+            }
+        xf1[im.instance] = im.object_to_world1;
+    }
+    if (d->camera_motion_inv)
+        for (int j = 0; j < 12; j++)
+            if (!std::isfinite(d->camera_motion_inv[j])) {
+                *err = "camera motion has a non-finite entry";
+                return false;
+            }
+    const bool motion = d->n_mesh_motion || d->n_instance_motion || d->camera_motion_inv;
+    if ((d->n_mesh_motion || d->n_instance_motion) && !build_bvh) {
+        *err = "internal: scenes with moving geometry are built by the host BVH builder";
+        return false;
+    }
     // ---- BLAS per mesh, then per curve set (geometry n_meshes + k) ------------
     const uint32_t n_geom = d->n_meshes + d->n_curves;
     std::vector<std::vector<RootChild>> root_children(n_geom), grand_children(n_geom);
@@ -1314,6 +1369,10 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
                         continue;
                     }
                     b.grow_pt(p);
+                    if (pos1[m]) {  // mesh.rs:62-77: the box covers both endpoints
+                        const double q[3] = {pos1[m][3ull * vi], pos1[m][3ull * vi + 1], pos1[m][3ull * vi + 2]};
+                        b.grow_pt(q);
+                    }
                 }
                 tb[t] = b;
             }
@@ -1331,6 +1390,9 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
         const size_t tri_off = H.tris.size();
         H.tris.resize(tri_off + 3ull * md.n_triangles);
         float4* dst = H.tris.data() + tri_off;
+        const float* p1 = pos1[m];
+        if (p1) H.tris1.resize(tri_off + 3ull * md.n_triangles);  // entries of static meshes stay unused
+        float4* dst1 = p1 ? H.tris1.data() + tri_off : nullptr;
         parallel_for(md.n_triangles, [&](size_t k0, size_t k1) {
             for (size_t k = k0; k < k1; k++) {
                 uint32_t t = bin.order[k];
@@ -1339,9 +1401,14 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
                     uint32_t vi = md.indices[3ull * t + c];
                     v[c] = make_float4(md.positions[3ull * vi], md.positions[3ull * vi + 1],
                                        md.positions[3ull * vi + 2], 0.0f);
+                    if (p1) dst1[3 * k + c] = make_float4(p1[3ull * vi], p1[3ull * vi + 1], p1[3ull * vi + 2], 0.0f);
                 }
                 uint32_t tid = t;
                 memcpy(&v[0].w, &tid, 4);
+                if (p1) {
+                    const uint32_t mark = RT_DEFORM_MARK;
+                    memcpy(&v[1].w, &mark, 4);
+                }
                 dst[3 * k] = v[0];
                 dst[3 * k + 1] = v[1];
                 dst[3 * k + 2] = v[2];
@@ -1447,6 +1514,29 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
     }
     H.scalars.n_instances = d->n_instances;
     H.scalars.any_curves = d->n_curves ? 1u : 0u;
+    // ---- motion blur tables ---------------------------------------------------
+    if (!H.tris1.empty()) H.tris1.resize(H.tris.size(), make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+    H.inst_motion.clear();
+    H.inst_mot.clear();
+    if (d->n_instance_motion) {
+        H.inst_mot.assign(d->n_instances, 0xFFFFFFFFu);
+        for (uint32_t i = 0; i < d->n_instances; i++) {
+            if (!xf1[i]) continue;
+            DevInstMotion im;
+            for (int r = 0; r < 3; r++) {
+                const double* a = d->instances[i].object_to_world + 4 * r;
+                const double* b = xf1[i] + 4 * r;
+                im.o2w0[r] = make_float4((float)a[0], (float)a[1], (float)a[2], (float)a[3]);
+                im.o2w1[r] = make_float4((float)b[0], (float)b[1], (float)b[2], (float)b[3]);
+            }
+            H.inst_mot[i] = (uint32_t)H.inst_motion.size();
+            H.inst_motion.push_back(im);
+        }
+    }
+    H.scalars.motion = motion ? 1u : 0u;
+    H.scalars.cam_moving = d->camera_motion_inv ? 1u : 0u;
+    for (int k = 0; k < 12; k++)
+        H.scalars.cam_mot[k] = d->camera_motion_inv ? (float)d->camera_motion_inv[k] : 0.0f;
     // ---- materials ---------------------------------------------------------
     if (d->n_materials && !d->materials) {
         *err = "materials pointer is NULL";

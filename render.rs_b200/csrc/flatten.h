@@ -14,6 +14,9 @@ namespace rt {
 struct HostScene {
     std::vector<uint4> nodes;        // 8-wide nodes, 6 words each
     std::vector<float4> tris;        // 3 per triangle, leaf order
+    std::vector<float4> tris1;       // deformation blur: triangles at shutter close (same index), or empty
+    std::vector<DevInstMotion> inst_motion;  // transform motion blur: moving instances
+    std::vector<uint32_t> inst_mot;  // per instance: its inst_motion entry or ~0 (empty without motion)
     std::vector<float4> inst_xf;     // 3 per instance, scene order
     std::vector<uint4> inst;         // 1 per instance, scene order
     std::vector<uint2> items;        // TLAS primitives, leaf order

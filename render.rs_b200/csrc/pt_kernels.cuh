@@ -50,6 +50,7 @@ enum : uint32_t {
 #define SH_SLOT_MASK (SH_PRIMARY - 1u)
 
 struct Paths {
+    float* time;      // shutter time of the path (scenes with motion blur; else unused)
     float4* ray_o;    // origin xyz, w = roulette gain (see k_shade)
     float4* ray_d;    // direction xyz, w = tmax
     uint4* hit;       // t bits, tri (leaf order), inst (leaf order), b1|b2 half2
@@ -158,7 +159,10 @@ struct HitGeo {
     bool curve;  // a curve-set segment (hair shading applies)
 };
 
-__device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3 d, uint4 hr, HitGeo& g) {
+// `time`: the path's shutter time (motion blur): moving instances and
+// deforming meshes are taken at it (Instance::intersect, mesh.rs:308-381).
+__device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3 d, uint4 hr, HitGeo& g,
+                                             float time = 0.0f) {
     float t = __uint_as_float(hr.x);
     g.p = o + d * t;
     g.wo = -normalize_ref(d);
@@ -173,11 +177,10 @@ __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3
         return;
     }
     uint32_t il = hr.z;
-    float4 x0 = __ldg(S.inst_xf + 3 * (size_t)il), x1 = __ldg(S.inst_xf + 3 * (size_t)il + 1),
-           x2 = __ldg(S.inst_xf + 3 * (size_t)il + 2);
+    float4 x0, x1, x2, v0, v1, v2;
+    inst_rows<true>(S, il, time, x0, x1, x2);
     uint4 info = __ldg(S.inst + il);
-    const float4* tp = S.tris + 3 * (size_t)hr.y;
-    float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+    tri_at<true>(S, hr.y, time, v0, v1, v2);
     float3 nl;
     MeshInfo mi = S.meshes[info.w];
     if (mi.attrs & MESH_CURVES) {
@@ -187,8 +190,9 @@ __device__ __forceinline__ void hit_geometry(const DevScene& S, float3 o, float3
         nl = f3(0.0f, 0.0f, 1.0f);
         seg_intersect(xf_point(x0, x1, x2, o), xf_vec(x0, x1, x2, d), v0, v1, v2, INFINITY, tt, &nl);
         g.curve = true;
-    } else if (mi.attrs & MESH_NORMALS) {
-        // Interpolated vertex normals (Mesh::local_normal, mesh.rs:200-220).
+    } else if ((mi.attrs & MESH_NORMALS) && __float_as_uint(v1.w) != RT_DEFORM_MARK) {
+        // Interpolated vertex normals (Mesh::local_normal, mesh.rs:200-220);
+        // a deforming mesh takes the geometric normal at the shutter time.
         float b1 = __half2float(__ushort_as_half((unsigned short)(hr.w & 0xFFFFu)));
         float b2 = __half2float(__ushort_as_half((unsigned short)(hr.w >> 16)));
         uint32_t ot = __float_as_uint(v0.w);
@@ -224,7 +228,11 @@ __device__ __forceinline__ float3 curve_tangent(const DevScene& S, uint4 hr) {
 // (src/geometry/mesh.rs:147-197) with the density carried to world scale
 // by the instance's approx_scale and the gradients pulled back through the
 // world-to-object transform (mesh.rs:357-371); zeros when the mesh has no st.
-__device__ __forceinline__ HitSt hit_st(const DevScene& S, uint4 hr, float3 p) {
+// With motion blur the hit's barycentrics come from the instance and the
+// triangle at the path's shutter `time` (the reference's hit uv), while the
+// density and the gradients keep the rest pose and the shutter-open
+// transform, as Mesh::st_at / st_gradients and Instance::inverse do.
+__device__ __forceinline__ HitSt hit_st(const DevScene& S, uint4 hr, float3 p, float time = 0.0f) {
     HitSt r{0.0f, 0.0f, 0.0f, f3(0.0f, 0.0f, 0.0f), f3(0.0f, 0.0f, 0.0f)};
     if (hr.y & RT_TRI_QUADRIC) {
         // The quadric's RiSpec (u, v) and density; no st gradients (the
@@ -245,8 +253,8 @@ __device__ __forceinline__ HitSt hit_st(const DevScene& S, uint4 hr, float3 p) {
         // density (mesh.rs:323-344).
         const float4* tp = S.tris + 3 * (size_t)hr.y;
         const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-        const float4 x0 = __ldg(S.inst_xf + 3 * (size_t)hr.z), x1 = __ldg(S.inst_xf + 3 * (size_t)hr.z + 1),
-                     x2 = __ldg(S.inst_xf + 3 * (size_t)hr.z + 2);
+        float4 x0, x1, x2;
+        inst_rows<true>(S, hr.z, time, x0, x1, x2);
         const float3 axis = xyz(b) - xyz(a);
         const float len2 = dot(axis, axis);
         const float along =
@@ -267,7 +275,19 @@ __device__ __forceinline__ HitSt hit_st(const DevScene& S, uint4 hr, float3 p) {
     // precision, ~1e-3 of the triangle: too coarse for texture lookups).
     float b1 = __half2float(__ushort_as_half((unsigned short)(hr.w & 0xFFFFu)));
     float b2 = __half2float(__ushort_as_half((unsigned short)(hr.w >> 16)));
-    if (n2 > 0.0f) {
+    if (time > 0.0f && S.motion) {
+        // The hit's triangle and instance at the shutter time.
+        float4 y0, y1, y2, w0, w1, w2;
+        inst_rows<true>(S, hr.z, time, y0, y1, y2);
+        tri_at<true>(S, hr.y, time, w0, w1, w2);
+        const float3 f1 = xyz(w1) - xyz(w0), f2 = xyz(w2) - xyz(w0), fn = cross(f1, f2);
+        const float m2 = dot(fn, fn);
+        if (m2 > 0.0f) {
+            const float3 q = xf_point(y0, y1, y2, p) - xyz(w0);
+            b1 = dot(cross(q, f2), fn) / m2;
+            b2 = dot(cross(f1, q), fn) / m2;
+        }
+    } else if (n2 > 0.0f) {
         const float3 q = f3(dot(xyz(x0), p) + x0.w, dot(xyz(x1), p) + x1.w, dot(xyz(x2), p) + x2.w) - xyz(v0);
         b1 = dot(cross(q, e2), nl) / n2;
         b2 = dot(cross(e1, q), nl) / n2;
@@ -368,6 +388,25 @@ __global__ void k_raygen(DevScene S, Paths P, PtConsts C) {
     } else {
         d = normalize_ref(dir);
     }
+    if (S.motion) {
+        // Shutter time after the filter and lens draws (pt/mod.rs:350-353,
+        // kernel_pt.metal:2422-2434); camera motion moves the ray by
+        // lerp(I, motion_inv, t), its direction renormalised.
+        const float tm = rng.next_f();
+        P.time[i] = tm;
+        if (S.cam_moving && tm > 0.0f) {
+            const float* M = S.cam_mot;
+            float4 r[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                r[k] = make_float4((k == 0 ? 1.0f : 0.0f) + (M[4 * k] - (k == 0 ? 1.0f : 0.0f)) * tm,
+                                   (k == 1 ? 1.0f : 0.0f) + (M[4 * k + 1] - (k == 1 ? 1.0f : 0.0f)) * tm,
+                                   (k == 2 ? 1.0f : 0.0f) + (M[4 * k + 2] - (k == 2 ? 1.0f : 0.0f)) * tm,
+                                   M[4 * k + 3] * tm);
+            o = xf_point(r[0], r[1], r[2], o);
+            d = normalize_ref(xf_vec(r[0], r[1], r[2], d));
+        }
+    }
     P.ray_o[i] = make_float4(o.x, o.y, o.z, 1.0f);
     P.ray_d[i] = make_float4(d.x, d.y, d.z, INFINITY);
     P.beta[i] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -425,7 +464,8 @@ __global__ void __launch_bounds__(128) k_guide_gather(DevScene S, Paths P, uint3
             if (want && guide_depth) want = (__float_as_uint(P.prev[slot].w) >> FL_DEPTH_SHIFT) < guide_depth;
             if (want) {
                 HitGeo hg;
-                hit_geometry(S, xyz(P.ray_o[slot]), xyz(P.ray_d[slot]), P.hit[slot], hg);
+                hit_geometry(S, xyz(P.ray_o[slot]), xyz(P.ray_d[slot]), P.hit[slot], hg,
+                             S.motion ? P.time[slot] : 0.0f);
                 float3 n = dot(hg.nw, hg.wo) >= 0.0f ? hg.nw : -hg.nw;
                 rec[0] = hg.p.x; rec[1] = hg.p.y; rec[2] = hg.p.z;
                 rec[3] = n.x; rec[4] = n.y; rec[5] = n.z;
@@ -585,8 +625,9 @@ __global__ void k_guide_keep(const uint32_t* tb_cnt, float scale, uint32_t cap, 
 // from the global work counter as soon as half the warp is idle (one
 // warp-aggregated atomic per refill), so a few long rays no longer hold a
 // warp's other lanes hostage (Aila & Laine 2009, "persistent while-while").
-// load(j, o, d, tmax, seed) reads work item j (seed: the ray's presence
-// seed, see leaf_coop); finish(done, j, ts) is called by
+// load(j, o, d, tmax, seed, time) reads work item j (seed: the ray's
+// presence seed, see leaf_coop; time: its shutter time, read with MOT);
+// finish(done, j, ts) is called by
 // the whole warp whenever some lane finished, with `done` true on those lanes.
 // Within a warp the work alternates between a node phase (every lane that
 // has no parked leaf tests nodes until it parks one or finishes) and a leaf
@@ -618,7 +659,8 @@ __global__ void k_guide_keep(const uint32_t* tb_cnt, float scale, uint32_t cap, 
 #ifndef RT_INST_IN_NODE_PHASE
 #define RT_INST_IN_NODE_PHASE 0
 #endif
-template <bool ANY, bool TRANSMIT = false, bool PRES = false, bool CURV = false, class Load, class Finish>
+template <bool ANY, bool TRANSMIT = false, bool PRES = false, bool CURV = false, bool MOT = false, class Load,
+          class Finish>
 __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t* fetch, uint32_t* err,
                                          TravStack& st, LeafShared& leaf, Load load, Finish finish) {
     PhaseState ps;
@@ -640,10 +682,10 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
                 if (base < n && j < n) {
                     item = j;
                     float3 o, d;
-                    float tmax;
+                    float tmax, time = 0.0f;
                     uint64_t seed = 0;
-                    load(j, o, d, tmax, seed);
-                    active = trav_begin(S, ps.ts, st, o, d, tmax);
+                    load(j, o, d, tmax, seed, time);
+                    active = trav_begin(S, ps.ts, st, o, d, tmax, MOT ? time : 0.0f);
                     if (PRES) ray_seed = seed;
                     if (active) {
                         phase_begin(ps);
@@ -677,7 +719,7 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
                     // One step: enter a parked instance leaf, or pop; then
                     // test the node that is current, if any.
                     if (RT_INST_IN_NODE_PHASE && ps.pending && !ps.ts.in_inst)
-                        done_now = op_leaf<ANY>(S, ps, st, err);
+                        done_now = op_leaf<ANY, MOT>(S, ps, st, err);
                     else if (ps.need_pop)
                         done_now = !op_pop(ps, st);
                     if (!done_now && ps.pending == 0 && !ps.need_pop) done_now = op_node<ANY>(S, ps, st, err);
@@ -693,9 +735,10 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
         // Leaf phase: instance leaves (TLAS) per lane, then the warp's
         // triangle leaves together (leaf_coop).
         bool done_now = false;
-        if (active && ps.pending && !ps.ts.in_inst) done_now = op_leaf<ANY>(S, ps, st, err);
+        if (active && ps.pending && !ps.ts.in_inst) done_now = op_leaf<ANY, MOT>(S, ps, st, err);
         const bool tri_leaf = active && !done_now && ps.pending && ps.ts.in_inst;
-        if (__any_sync(0xFFFFFFFFu, tri_leaf)) done_now |= leaf_coop<ANY, TRANSMIT, PRES, CURV>(S, ps, tri_leaf, leaf, ray_seed);
+        if (__any_sync(0xFFFFFFFFu, tri_leaf))
+            done_now |= leaf_coop<ANY, TRANSMIT, PRES, CURV, MOT>(S, ps, tri_leaf, leaf, ray_seed);
         if (__any_sync(0xFFFFFFFFu, done_now)) finish(done_now, item, ps.ts);
         if (done_now) active = false;
     }
@@ -704,7 +747,9 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
 // ---- extend ---------------------------------------------------------------------------
 // `pres`: cutout surfaces are passed through inside the traversal
 // (leaf_coop, PRES) instead of by the shade kernel's skip waves.
-template <int BLOCK, bool PRES, bool QUAD = false>
+// QUAD: the scene has quadrics or curve sets; MOT: motion blur (rays carry
+// their path's shutter time; launched with QUAD).
+template <int BLOCK, bool PRES, bool QUAD = false, bool MOT = false>
 __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S, Paths P, uint32_t qsel) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
     __shared__ LeafShared leaf_sh[BLOCK / 32];
@@ -716,12 +761,13 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S
     uint32_t slot = 0;
     uint32_t qk = 0xFFFFFFFFu;  // closest quadric of this lane's ray (scene/mod.rs:105-146), ~0 for none
     float qt = 0.0f;            // its parametric distance
-    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed, float& time) {
         slot = q[j];
         float4 o4 = P.ray_o[slot], d4 = P.ray_d[slot];
         o = xyz(o4);
         d = xyz(d4);
         tmax = d4.w;
+        if (MOT) time = P.time[slot];
         if (PRES) {
             // The path's random state at this bounce, hashed: a seed no
             // other ray of the render shares.
@@ -760,7 +806,8 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_extend(DevScene S
         for (uint32_t c = 0; c < N_QUEUES; c++)
             push_queue(P.q_cls + (size_t)c * P.P, &P.cnt[CNT_CLASS + c], slot, done && cls == c);
     };
-    ray_pump<false, false, PRES, QUAD>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+    ray_pump<false, false, PRES, QUAD, MOT>(S, n, &P.cnt[CNT_FETCH_EXT], P.err, st, leaf_sh[threadIdx.x >> 5], load,
+                                            finish);
     if (rays) atomicAdd(&P.stats[0], rays);
 }
 
@@ -1181,7 +1228,8 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                 }
             } else {
                 HitGeo hg;
-                hit_geometry(S, o, d, hr, hg);
+                const float tm = S.motion ? P.time[slot] : 0.0f;
+                hit_geometry(S, o, d, hr, hg, tm);
                 const float3 p = hg.p, wo = hg.wo;
                 float3 nw = hg.nw;
                 const bool front = hg.front;
@@ -1201,7 +1249,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
                     if (!hull_skip) cone.x += eucl * cone.y;
                     const DevMatPat mp = S.mat_pat[hg.mat];
                     if (mp.bind_n) {
-                        const HitSt hs = hit_st(S, hr, p);
+                        const HitSt hs = hit_st(S, hr, p, tm);
                         mres = *mptr;
                         resolve_material(S, mp, hs, p, nw, d, cone.x, mres);
                         mptr = &mres;
@@ -1448,7 +1496,7 @@ __global__ void __launch_bounds__(128, RT_SHADE_MIN_BLOCKS) k_shade(DevScene S, 
 }
 
 // ---- shadow -------------------------------------------------------------------------------
-template <int BLOCK, bool QUAD = false>
+template <int BLOCK, bool QUAD = false, bool MOT = false>
 __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S, Paths P, PtConsts C) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
     __shared__ LeafShared leaf_sh[BLOCK / 32];
@@ -1469,12 +1517,13 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
         // Opaque scenes: one any-hit query per shadow ray, through the pump.
         uint32_t slot = 0;
         bool qblock = false;  // a quadric blocks this lane's shadow ray
-        auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
+        auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed, float& time) {
             slot = P.q_sh[j];
             float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
             o = xyz(o4);
             d = xyz(d4);
             tmax = d4.w;
+            if (MOT) time = P.time[slot];
             qblock = false;
             if (QUAD) {
                 const float dl = fmaxf(length(d), 1e-30f);
@@ -1488,7 +1537,8 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
             rays++;
             if (!ts.found && !qblock) add(slot, 1.0f);
         };
-        ray_pump<true, false, false, QUAD>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+        ray_pump<true, false, false, QUAD, MOT>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load,
+                                                finish);
         if (rays) atomicAdd(&P.stats[1], rays);
         return;
     }
@@ -1497,12 +1547,13 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
     // surfaces block).
     uint32_t slot = 0;
     float qvis = 1.0f;  // transmittance of this lane's shadow ray through the quadrics
-    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed, float& time) {
         slot = P.q_sh[j];
         float4 o4 = P.sh_o[slot], d4 = P.sh_d[slot];
         o = xyz(o4);
         d = xyz(d4);
         tmax = d4.w;
+        if (MOT) time = P.time[slot];
         qvis = 1.0f;
         if (QUAD) {
             const float dl = fmaxf(length(d), 1e-30f);
@@ -1516,7 +1567,8 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
         const float vis = ts.trans * qvis;
         if (vis > 0.0f) add(slot, vis);
     };
-    ray_pump<true, true, false, QUAD>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load, finish);
+    ray_pump<true, true, false, QUAD, MOT>(S, n, &P.cnt[CNT_FETCH_SH], P.err, st, leaf_sh[threadIdx.x >> 5], load,
+                                           finish);
     if (rays) atomicAdd(&P.stats[1], rays);
 }
 
@@ -1556,12 +1608,13 @@ __global__ void __launch_bounds__(BLOCK) k_sss(DevScene S, Paths P, PtConsts C, 
             const float3 sst = f3(m.sss_st[0], m.sss_st[1], m.sss_st[2]);
             const float3 sss = f3(m.sss_ss[0], m.sss_ss[1], m.sss_ss[2]);
             const uint32_t cur_med = MED ? mstack_top(P.med[slot], S.atmosphere) : RT_MEDIUM_NONE;
+            const float tm = S.motion ? P.time[slot] : 0.0f;
             float3 wo = xyz(o4), wd = xyz(d4);
             bool exited = false;
             for (int step = 0; step < 256; step++) {
                 uint4 hr;
                 rays++;
-                if (!trace_closest(S, st, wo, wd, INFINITY, P.err, hr)) break;  // escaped through a crack
+                if (!trace_closest(S, st, wo, wd, INFINITY, P.err, hr, tm)) break;  // escaped through a crack
                 const MedEvent ev = homog_sample(sst, sss, __uint_as_float(hr.x), beta, rng);
                 beta = beta * ev.w;
                 if (ev.scatter) {
@@ -1578,7 +1631,7 @@ __global__ void __launch_bounds__(BLOCK) k_sss(DevScene S, Paths P, PtConsts C, 
                 }
                 // Exit on the outside: normal along the walk's direction.
                 HitGeo hg;
-                hit_geometry(S, wo, wd, hr, hg);
+                hit_geometry(S, wo, wd, hr, hg, tm);
                 const float3 out_n = dot(hg.nw, wd) > 0.0f ? hg.nw : -hg.nw;
                 const Frame xf(out_n);
                 const float3 xp = hg.p;
@@ -1659,14 +1712,15 @@ __global__ void __launch_bounds__(BLOCK) k_sss(DevScene S, Paths P, PtConsts C, 
 // medium (the ray starts in `medium`, the atmosphere below it), cutouts
 // attenuate by 1 - presence, anything else blocks; at most 16 segments.
 __device__ __forceinline__ float3 shadow_walk(const DevScene& S, TravStack& st, float3 o, float3 d, float remaining,
-                                              uint32_t medium, Pcg& rng, uint32_t* err, unsigned long long& rays) {
+                                              uint32_t medium, Pcg& rng, uint32_t* err, unsigned long long& rays,
+                                              float time) {
     uint2 ms = make_uint2(0u, 0u);
     if (medium != RT_MEDIUM_NONE && medium != S.atmosphere) mstack_push(ms, medium);
     float3 vis = f3(1.0f, 1.0f, 1.0f);
     for (int k = 0; k < RT_MAX_PRESENCE_SKIPS; k++) {
         rays++;
         uint4 hr;
-        const bool found = remaining > 0.0f && trace_closest(S, st, o, d, remaining, err, hr);
+        const bool found = remaining > 0.0f && trace_closest(S, st, o, d, remaining, err, hr, time);
         const float t = found ? __uint_as_float(hr.x) : remaining;
         const uint32_t cur = mstack_top(ms, S.atmosphere);
         if (cur != RT_MEDIUM_NONE) {
@@ -1679,7 +1733,7 @@ __device__ __forceinline__ float3 shadow_walk(const DevScene& S, TravStack& st, 
         const DevMaterial& m = S.materials[mat];
         if (m.hull != 0.0f) {
             HitGeo hg;
-            hit_geometry(S, o, d, hr, hg);
+            hit_geometry(S, o, d, hr, hg, time);
             if (hg.front) mstack_push(ms, m.interior);
             else mstack_pop(ms);
         } else {
@@ -1717,7 +1771,8 @@ __global__ void __launch_bounds__(BLOCK) k_shadow_media(DevScene S, Paths P, PtC
             const float4 o4 = r == 0 ? P.sh_o[slot] : P.sh2_o[slot];
             const float4 d4 = r == 0 ? P.sh_d[slot] : P.sh2_d[slot];
             const float4 c4 = r == 0 ? P.sh_c[slot] : P.sh2_c[slot];
-            const float3 vis = shadow_walk(S, st, xyz(o4), xyz(d4), d4.w, __float_as_uint(o4.w), rng, P.err, rays);
+            const float3 vis = shadow_walk(S, st, xyz(o4), xyz(d4), d4.w, __float_as_uint(o4.w), rng, P.err, rays,
+                                           S.motion ? P.time[slot] : 0.0f);
             const float3 c = xyz(c4) * vis;
             add = add + c;
             if (c4.w != 0.0f) add_aux = add_aux + c;
@@ -1814,7 +1869,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_intersect(DevScen
     st.init(stack_sh + threadIdx.x, BLOCK);
     uint32_t qk = 0xFFFFFFFFu;  // closest (or blocking) quadric of this lane's ray
     float qt = 0.0f;
-    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed, float&) {
         float4 o4 = __ldg(org + j), d4 = __ldg(dir + j);
         o = xyz(o4);
         d = xyz(d4);
@@ -1864,7 +1919,7 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_transmit_batch(De
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
     float qvis = 1.0f;
-    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed) {
+    auto load = [&](uint32_t j, float3& o, float3& d, float& tmax, uint64_t& seed, float&) {
         float4 o4 = __ldg(org + j), d4 = __ldg(dir + j);
         o = xyz(o4);
         d = xyz(d4);

@@ -221,6 +221,19 @@ static_assert(sizeof(DevQuadric) == 144, "DevQuadric layout");
 // (leaf-order triangle indices stay below it); the low bits are its index.
 #define RT_TRI_QUADRIC 0x80000000u
 
+// Transform motion blur (Instance::transform1, src/geometry/mesh.rs:230-304):
+// a moving instance's object-to-world rows at shutter open and close (f32);
+// a ray at shutter time t > 0 enters it through the inverse of their
+// component-wise lerp.
+struct DevInstMotion {
+    float4 o2w0[3], o2w1[3];
+};
+static_assert(sizeof(DevInstMotion) == 96, "DevInstMotion layout");
+// Deformation blur (Mesh::positions1, mesh.rs:29-31, 96-111): the second
+// record of a deforming mesh's triangle carries this mark in w, and the
+// scene's second triangle array holds the triangle at shutter close.
+#define RT_DEFORM_MARK 0x7FC5E7u
+
 struct DevScene {
     const uint4* nodes;
     const float4* tris;
@@ -276,6 +289,17 @@ struct DevScene {
     const float* env_cond;
     uint32_t env_w, env_h, env_light;
     float env_total;
+    // Motion blur (null / 0 in a static scene): rays draw a shutter time
+    // (pt/mod.rs:339-356); moving instances, by index (inst_mot: ~0 for a
+    // static instance); triangles at shutter close (leaf order, entries of
+    // static meshes unused); camera motion, the 3x4 rows of
+    // Camera::motion_inv (camera.rs:134-146).
+    const DevInstMotion* inst_motion;
+    const uint32_t* inst_mot;
+    const float4* tris1;
+    uint32_t motion;
+    uint32_t cam_moving;
+    float cam_mot[12];
     // camera (src/scene/camera.rs:150-179)
     float eye[3], fwd[3], right[3], up[3];
     float half_w, half_h, lens_radius, focal_distance, filter_width;

@@ -223,6 +223,9 @@ struct rt_session {
 
 // Scenes with analytic quadrics or curve sets run the kernel variants that
 // test them (the others keep their registers for the BVH walk).
+// Quadrics or curve sets: the traversal kernels' extra-geometry variants
+// (quadrics first, segment leaves); scenes with motion blur run them too,
+// with rays placed at their shutter time.
 static bool extra_geometry(const rt_session* s) { return s->S.n_quadrics > 0 || s->S.any_curves; }
 
 // The ray-batch kernel variant for the query and the scene.
@@ -251,9 +254,11 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     auto* s = new rt_session();
     s->params = *params;
     std::string err;
-    // The device builder covers triangle meshes; scenes with curve sets are
-    // built on the host (the same SAH rules and wide layout).
-    const bool device_bvh = params->bvh_build == 0 && !(scene && scene->n_curves);
+    // The device builder covers static triangle meshes; scenes with curve
+    // sets or motion blur are built on the host (the same SAH rules and wide
+    // layout).
+    const bool device_bvh = params->bvh_build == 0 &&
+                            !(scene && (scene->n_curves || scene->n_mesh_motion || scene->n_instance_motion));
     if (!flatten_scene(scene, &s->host, &err, !device_bvh)) {
         delete s;
         return fail(RT_ERR_INVALID, err);
@@ -331,6 +336,11 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     if (!H.quadrics.empty()) rc = rc ? rc : s->upload(&S.quadrics, H.quadrics);
     if (!H.media.empty()) rc = rc ? rc : s->upload(&S.media, H.media);
     if (!H.hair.empty()) rc = rc ? rc : s->upload(&S.hair, H.hair);
+    if (!H.tris1.empty()) rc = rc ? rc : s->upload((const float4**)&S.tris1, H.tris1);
+    if (!H.inst_motion.empty()) {
+        rc = rc ? rc : s->upload(&S.inst_motion, H.inst_motion);
+        rc = rc ? rc : s->upload(&S.inst_mot, H.inst_mot);
+    }
     rc = rc ? rc : s->upload(&S.materials, H.materials);
     rc = rc ? rc : s->upload(&S.lights, H.lights);
     rc = rc ? rc : s->upload(&S.lbvh, H.lbvh);
@@ -383,6 +393,8 @@ int rt_session_create(const rt_scene_desc* scene, const rt_params* params, rt_se
     rc = rc ? rc : s->alloc(&Pp.aux_d, aov ? P : 1);
     Pp.cone = nullptr;
     if (S.mat_pat) rc = rc ? rc : s->alloc(&Pp.cone, P);
+    Pp.time = nullptr;
+    if (S.motion) rc = rc ? rc : s->alloc(&Pp.time, P);
     // Media: nested-medium stacks and the equiangular shadow slot; walks:
     // their queue.
     Pp.med = nullptr;
@@ -597,8 +609,10 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
         for (uint32_t w = 0; w < waves; w++) {
             uint32_t qin = w & 1u, qout = qin ^ 1u;
             CUDA_TRY(cudaEventRecord(s->evpool[ei], st));
-            const bool quad = extra_geometry(s);
-            if (C.pres_in_trav && quad) k_extend<TRAV_BLOCK, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
+            const bool quad = extra_geometry(s), mot = s->S.motion != 0;
+            if (C.pres_in_trav && mot) k_extend<TRAV_BLOCK, true, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
+            else if (mot) k_extend<TRAV_BLOCK, false, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
+            else if (C.pres_in_trav && quad) k_extend<TRAV_BLOCK, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
             else if (C.pres_in_trav) k_extend<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
             else if (quad) k_extend<TRAV_BLOCK, false, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
             else k_extend<TRAV_BLOCK, false><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, qin);
@@ -626,6 +640,7 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
             }
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 2], st));
             if (med) k_shadow_media<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            else if (mot) k_shadow<TRAV_BLOCK, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             else if (quad) k_shadow<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             else k_shadow<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 3], st));

@@ -61,6 +61,69 @@ __device__ __forceinline__ float3 xf_normal(const float4& r0, const float4& r1, 
               r0.z * n.x + r1.z * n.y + r2.z * n.z);
 }
 
+// ---- motion blur ----------------------------------------------------------------
+// World-to-object rows of instance `inst` for a ray at shutter time `time`
+// (Instance::transforms_at, src/geometry/mesh.rs:295-304): a moving
+// instance at t > 0 is placed by the component-wise lerp of its two
+// object-to-world transforms, inverted here in f32 (adjugate over the
+// determinant; identity when |det| < 1e-6, as Matrix4::inverse gives None).
+// MOT false compiles the static path alone.
+template <bool MOT>
+__device__ __forceinline__ void inst_rows(const DevScene& S, uint32_t inst, float time, float4& x0, float4& x1,
+                                          float4& x2) {
+    if (MOT && S.inst_mot && time > 0.0f) {
+        const uint32_t k = __ldg(S.inst_mot + inst);
+        if (k != 0xFFFFFFFFu) {
+            const DevInstMotion& M = S.inst_motion[k];
+            float4 m[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const float4 a = __ldg(&M.o2w0[r]), b = __ldg(&M.o2w1[r]);
+                m[r] = make_float4(a.x + (b.x - a.x) * time, a.y + (b.y - a.y) * time, a.z + (b.z - a.z) * time,
+                                   a.w + (b.w - a.w) * time);
+            }
+            const float3 a0 = xyz(m[0]), a1 = xyz(m[1]), a2 = xyz(m[2]);
+            const float3 c0 = cross(a1, a2), c1 = cross(a2, a0), c2 = cross(a0, a1);
+            const float det = dot(a0, c0);
+            if (!(fabsf(det) >= 1e-6f)) {
+                x0 = make_float4(1.0f, 0.0f, 0.0f, 0.0f);
+                x1 = make_float4(0.0f, 1.0f, 0.0f, 0.0f);
+                x2 = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+                return;
+            }
+            const float id = 1.0f / det;
+            const float3 r0 = f3(c0.x, c1.x, c2.x) * id, r1 = f3(c0.y, c1.y, c2.y) * id,
+                         r2 = f3(c0.z, c1.z, c2.z) * id;
+            const float3 tr = f3(m[0].w, m[1].w, m[2].w);
+            x0 = make_float4(r0.x, r0.y, r0.z, -dot(r0, tr));
+            x1 = make_float4(r1.x, r1.y, r1.z, -dot(r1, tr));
+            x2 = make_float4(r2.x, r2.y, r2.z, -dot(r2, tr));
+            return;
+        }
+    }
+    x0 = __ldg(S.inst_xf + 3 * (size_t)inst);
+    x1 = __ldg(S.inst_xf + 3 * (size_t)inst + 1);
+    x2 = __ldg(S.inst_xf + 3 * (size_t)inst + 2);
+}
+
+// Triangle `tri` (leaf order) at shutter time `time` (Mesh::vertex_at,
+// mesh.rs:96-111): a deforming mesh's vertices lerp toward their
+// shutter-close positions; the record's w fields are kept.
+template <bool MOT>
+__device__ __forceinline__ void tri_at(const DevScene& S, uint32_t tri, float time, float4& a, float4& b, float4& c) {
+    const float4* tp = S.tris + 3 * (size_t)tri;
+    a = __ldg(tp);
+    b = __ldg(tp + 1);
+    c = __ldg(tp + 2);
+    if (MOT && time > 0.0f && __float_as_uint(b.w) == RT_DEFORM_MARK) {
+        const float4* tq = S.tris1 + 3 * (size_t)tri;
+        const float4 a1 = __ldg(tq), b1 = __ldg(tq + 1), c1 = __ldg(tq + 2);
+        a = make_float4(a.x + (a1.x - a.x) * time, a.y + (a1.y - a.y) * time, a.z + (a1.z - a.z) * time, a.w);
+        b = make_float4(b.x + (b1.x - b.x) * time, b.y + (b1.y - b.y) * time, b.z + (b1.z - b.z) * time, b.w);
+        c = make_float4(c.x + (c1.x - c.x) * time, c.y + (c1.y - c.y) * time, c.z + (c1.z - c.z) * time, c.w);
+    }
+}
+
 // ---- per-ray precomputation ------------------------------------------------------
 struct RayPre {
     float3 o, d, inv;
@@ -350,11 +413,13 @@ struct TravState {
     int inst_sp;
     bool in_inst, found;
     float trans;       // shadow transmittance (TRANSMIT queries)
+    float time;        // shutter time of the ray (motion blur; 0 in static scenes)
 };
 
 // Start a closest-hit / any-hit query; false when the scene is empty.
 __device__ __forceinline__ bool trav_begin(const DevScene& S, TravState& ts, TravStack& st, float3 o, float3 d,
-                                           float t_max) {
+                                           float t_max, float time = 0.0f) {
+    ts.time = time;
     ts.hit.t = t_max;
     ts.hit.tri = 0xFFFFFFFFu;
     ts.hit.inst = 0xFFFFFFFFu;
@@ -475,7 +540,8 @@ __device__ __forceinline__ bool op_node(const DevScene& S, PhaseState& ps, TravS
 }
 
 // Returns true when the query is over (any-hit found, or a fatal condition).
-template <bool ANY>
+// MOT: instances and triangles are placed at the ray's shutter time.
+template <bool ANY, bool MOT = false>
 __device__ __forceinline__ bool op_leaf(const DevScene& S, PhaseState& ps, TravStack& st, uint32_t* err) {
     TravState& ts = ps.ts;
     const uint32_t leaf = ps.pending;
@@ -493,8 +559,8 @@ __device__ __forceinline__ bool op_leaf(const DevScene& S, PhaseState& ps, TravS
         const uint2 item = __ldg(S.items + first);
         const uint32_t inst = item.x, root = item.y;
         ts.cur_inst = inst;
-        float4 x0 = __ldg(S.inst_xf + 3 * (size_t)inst), x1 = __ldg(S.inst_xf + 3 * (size_t)inst + 1),
-               x2 = __ldg(S.inst_xf + 3 * (size_t)inst + 2);
+        float4 x0, x1, x2;
+        inst_rows<MOT>(S, inst, ts.time, x0, x1, x2);
         ray_pre(ts.r, xf_point(x0, x1, x2, ts.o), xf_vec(x0, x1, x2, ts.d));
         ts.in_inst = true;
         ts.inst_sp = st.sp;
@@ -505,8 +571,8 @@ __device__ __forceinline__ bool op_leaf(const DevScene& S, PhaseState& ps, TravS
         return false;
     }
     for (uint32_t k = 0; k < count; k++) {
-        const float4* tp = S.tris + 3 * (size_t)(first + k);
-        float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float4 a, b, c;
+        tri_at<MOT>(S, first + k, ts.time, a, b, c);
         float t, b1 = 0.0f, b2 = 0.0f;
         const bool hit = (S.any_curves && is_segment(c)) ? seg_intersect(ts.r.o, ts.r.d, a, b, c, ts.hit.t, t)
                                                          : tri_watertight(ts.r, xyz(a), xyz(b), xyz(c), ts.hit.t, t, b1, b2);
@@ -580,7 +646,8 @@ __device__ __forceinline__ bool presence_passes(uint64_t seed, uint32_t tri, uin
 // this lane's ray seed (PRES). Returns true when an any-hit query found a
 // hit (the query is over).
 // CURV: the scene has curve sets, whose leaves hold segments (seg_intersect).
-template <bool ANY, bool TRANSMIT = false, bool PRES = false, bool CURV = false>
+// MOT: triangles are placed at the owner ray's shutter time.
+template <bool ANY, bool TRANSMIT = false, bool PRES = false, bool CURV = false, bool MOT = false>
 __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, bool mine, LeafShared& L,
                                           uint64_t seed_own = 0) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -633,6 +700,7 @@ __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, boo
             r.d.z = __shfl_sync(0xFFFFFFFFu, ts.r.d.z, owner);
         }
         const float pres = __shfl_sync(0xFFFFFFFFu, pres_own, owner);
+        const float tm = MOT ? __shfl_sync(0xFFFFFFFFu, ts.time, owner) : 0.0f;
         uint64_t seed = 0;
         uint32_t inst_o = 0;
         if (PRES) {
@@ -650,8 +718,8 @@ __device__ __forceinline__ bool leaf_coop(const DevScene& S, PhaseState& ps, boo
             if (!TRANSMIT && best != ~0ull)
                 tmax = fminf(tmax, nextafterf(__uint_as_float((uint32_t)(best >> 32)), INFINITY));
             const uint32_t tri = f + (it & 15u);
-            const float4* tp = S.tris + 3 * (size_t)tri;
-            float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+            float4 a, b, c;
+            tri_at<MOT>(S, tri, tm, a, b, c);
             const bool hit = (CURV && is_segment(c)) ? seg_intersect(r.o, r.d, a, b, c, tmax, t)
                                                      : tri_watertight(r, xyz(a), xyz(b), xyz(c), tmax, t, b1, b2);
             if (hit) {

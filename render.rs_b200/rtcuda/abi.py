@@ -27,6 +27,22 @@ class RtInstanceDesc(C.Structure):
     ]
 
 
+class RtInstanceMotion(C.Structure):
+    _fields_ = [
+        ("instance", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("object_to_world1", C.c_double * 12),
+    ]
+
+
+class RtMeshMotion(C.Structure):
+    _fields_ = [
+        ("mesh", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("positions1", C.POINTER(C.c_float)),
+    ]
+
+
 class RtMaterialDesc(C.Structure):
     _fields_ = [
         ("diffuse_gain", C.c_double),
@@ -228,6 +244,11 @@ class RtSceneDesc(C.Structure):
         ("curves", C.POINTER(RtCurvesDesc)),
         ("n_curves", C.c_uint32),
         ("curves_reserved", C.c_uint32),
+        ("instance_motion", C.POINTER(RtInstanceMotion)),
+        ("n_instance_motion", C.c_uint32),
+        ("n_mesh_motion", C.c_uint32),
+        ("mesh_motion", C.POINTER(RtMeshMotion)),
+        ("camera_motion_inv", C.POINTER(C.c_double)),
     ]
 
 
@@ -256,7 +277,8 @@ FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
 for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 376), (RtLightDesc, 120),
                (RtCameraDesc, 144), (RtParams, 72), (RtPatternInput, 32), (RtPatternDesc, 264),
                (RtPatternBinding, 16), (RtTextureDesc, 16), (RtIesDesc, 112), (RtQuadricDesc, 168),
-               (RtSceneDesc, 344), (RtMediumDesc, 136), (RtCurvesDesc, 40)):
+               (RtSceneDesc, 376), (RtMediumDesc, 136), (RtCurvesDesc, 40), (RtInstanceMotion, 104),
+               (RtMeshMotion, 16)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 
 

@@ -480,6 +480,8 @@ class _State:
         self.identifier = None
         self.interior = -1       # Interior medium bound to subsequent geometry
         self.hair = None         # Bxdf "PxrMarschnerHair" parameters (dict)
+        self.motion_t0 = None    # transform-motion endpoints of a closed MotionBegin block (4x4)
+        self.motion_t1 = None
 
     def copy(self):
         s = _State()
@@ -521,6 +523,9 @@ class _Builder:
         self.next_id = 1
         self.warned = []
         self.motion = None
+        self.pending_deform_p = None      # shutter-close "P" of a PointsPolygons motion block
+        self.camera_motion_inv = None     # Camera::motion_inv (4x4) from a pre-World motion block
+        self.mesh_p1 = {}                 # mesh index -> (n, 3) positions at shutter close
         self.env = None
         # scene contents (materials / lights / meshes / instances)
         self.meshes, self.instances, self.materials, self.lights = [], [], [], []
@@ -599,21 +604,72 @@ class _Builder:
             self.mesh_st[len(self.meshes) - 1] = np.asarray(st, np.float32).reshape(-1, 2)
         return len(self.meshes) - 1
 
-    def place(self, mesh, mat, xf):
-        self.instances.append((mesh, mat, np.asarray(xf, np.float64)[:3, :].reshape(12)))
+    def place(self, mesh, mat, xf, moving=True):
+        """An instance of `mesh`; with `moving`, at the open MotionBegin
+        block's endpoints (the reference's legacy objects, Polygon and the
+        light geometry, stay put)."""
+        xf1 = self.motion_endpoint(xf) if moving else None
+        self.instances.append((mesh, mat, np.asarray(xf, np.float64)[:3, :].reshape(12),
+                               None if xf1 is None else xf1[:3, :].reshape(12)))
+
+    def motion_endpoint(self, current):
+        """motion_endpoint (scene_builder.rs:1684-1691): the shutter-close
+        transform of geometry placed at `current`: the block's T1 with the
+        transforms composed after the block."""
+        t0, t1 = self.state.motion_t0, self.state.motion_t1
+        if t0 is None or t1 is None:
+            return None
+        try:
+            post = np.linalg.inv(t0) @ current
+        except np.linalg.LinAlgError:
+            return None
+        return t1 @ post
+
+    def finish_motion_block(self, block):
+        """finish_motion_block (scene_builder.rs:1637-1682): a block of
+        transforms records the shutter-open and -close transforms (the
+        current transform stays the open one); a block of PointsPolygons
+        samples makes a deforming mesh (the last sample's "P" at shutter
+        close); anything else uses its first sample."""
+        name0 = block[0][0]
+        if all(n in ("Translate", "Rotate", "Scale", "ConcatTransform", "Transform", "Identity") for n, _ in block):
+            base = self.ctm.copy()
+            self.process(*block[0])
+            t0 = self.ctm.copy()
+            if len(block) > 1:
+                self.xf[-1] = base
+                self.process(*block[-1])
+                t1 = self.ctm.copy()
+                self.xf[-1] = t0
+                self.state.motion_t0, self.state.motion_t1 = t0, t1
+            return
+        if all(n == name0 for n, _ in block) and name0 in ("PointsPolygons", "PointsGeneralPolygons"):
+            if len(block) > 1:
+                self.pending_deform_p = _Params(block[-1][1], 2).numbers("P")
+            self.process(*block[0])
+            self.pending_deform_p = None
+            return
+        self.warn(f'MotionBegin over "{name0}" not supported (transforms and PointsPolygons deformation only); '
+                  "using the first sample")
+        self.process(*block[0])
 
     def add_quadric(self, kind, params, mat, xf):
         self.quadrics.append((kind, [float(v) for v in params], mat, np.asarray(xf, np.float64)[:3, :].reshape(12)))
 
-    def tessellated_mesh(self, P, I, N=None, emissive=True, st=None, displace=False):
+    def tessellated_mesh(self, P, I, N=None, emissive=True, st=None, displace=False, P1=None):
         """add_tessellated_mesh (scene_builder.rs:1195-1234): the state's
         displacement on meshes the reference tessellates (`displace`; not
         on the quadrics it intersects analytically); quadrics take the
-        plain state material (no area-light emission, :813-909)."""
+        plain state material (no area-light emission, :813-909). `P1`: the
+        positions at shutter close of a deforming mesh (displacement
+        rebuilds the mesh without them, as displace_mesh does)."""
         if displace and self.state.displace is not None:
             from .displace import displace_mesh
             P, N = displace_mesh(P, I, N, **self.state.displace)
+            P1 = None
         mesh = self.add_mesh(P, I, N, st)
+        if P1 is not None:
+            self.mesh_p1[mesh] = np.asarray(P1, np.float32).reshape(-1, 3)
         m = self.make_material()
         if emissive and self.state.area_light is not None:
             inten, col = self.state.area_light
@@ -641,6 +697,15 @@ class _Builder:
 
     def process(self, name, vals):
         st = self.state
+        if name == "WorldBegin" and st.motion_t0 is not None and st.motion_t1 is not None:
+            # A motion block over the pre-World transforms animates the
+            # camera (scene_builder.rs:271-285): rays use the inverse of the
+            # delta t1 t0^-1; the motion state does not reach world geometry.
+            try:
+                self.camera_motion_inv = np.linalg.inv(st.motion_t1 @ np.linalg.inv(st.motion_t0))
+            except np.linalg.LinAlgError:
+                pass
+            st.motion_t0 = st.motion_t1 = None
         if name in ("version", "WorldEnd", "FrameBegin", "FrameEnd", "WorldBegin", "IfBegin", "ElseIf", "Else",
                     "IfEnd", "Display", "Clipping", "ClippingPlane", "CropWindow", "FrameAspectRatio",
                     "PixelVariance", "Exposure", "Quantize", "Hider", "Integrator", "TextureCoordinates",
@@ -680,8 +745,7 @@ class _Builder:
         elif name == "MotionEnd":
             block, self.motion = self.motion or [], None
             if block:
-                self.warn("motion blur is not rendered: motion blocks use their first sample")
-                self.process(*block[0])
+                self.finish_motion_block(block)
         elif name == "ArchiveBegin":
             self.recording = (_str(vals, 0) or "", [])
         elif name == "ReadArchive":
@@ -926,7 +990,7 @@ class _Builder:
         """add_curve_set (scene_builder.rs:1157-1170): the state material and
         the current placement."""
         mat = self.add_material(self.make_material())
-        self.curve_sets.append((p0, p1, v0, v1, mat, self.ctm.copy()))
+        self.curve_sets.append((p0, p1, v0, v1, mat, self.ctm.copy(), self.motion_endpoint(self.ctm)))
 
     def medium_request(self, name, vals):
         """Interior / Atmosphere (scene_builder.rs:324-373): sigma_a, sigma_s,
@@ -1014,7 +1078,7 @@ class _Builder:
                 m["area_light"] = self.add_light(abi.LIGHT_RECT, inten, col, p=c0, e1=e1, e2=e2)
         mat = self.add_material(m)
         I = [(0, i, i + 1) for i in range(1, nv - 1)]
-        self.place(self.add_mesh(P, I), mat, self.ctm)
+        self.place(self.add_mesh(P, I), mat, self.ctm, moving=False)
 
     def points_polygons(self, name, vals):
         """points_polygons (scene_builder.rs:982-1051): fan-triangulated
@@ -1061,7 +1125,9 @@ class _Builder:
         ST = None
         if stv is not None and len(stv) * 3 == len(p) * 2:
             ST = np.array(stv, dtype=np.float64).reshape(-1, 2)
-        self.tessellated_mesh(P, I, N, st=ST, displace=True)
+        p1, self.pending_deform_p = self.pending_deform_p, None
+        P1 = np.array(p1, dtype=np.float64).reshape(-1, 3) if p1 is not None and len(p1) == len(p) else None
+        self.tessellated_mesh(P, I, N, st=ST, displace=True, P1=P1)
 
     # -- patterns (scene_builder.rs:703-728, 1738-1846) -------------------------------
     def _ref_target(self, prm, name):
@@ -1335,7 +1401,7 @@ class _Builder:
             li = self.add_light(abi.LIGHT_RECT, scale, col, p=corner, e1=_xf_vec(xf, (1, 0, 0)),
                                 e2=_xf_vec(xf, (0, 1, 0)))
             P = np.array([[-0.5, -0.5, 0], [0.5, -0.5, 0], [0.5, 0.5, 0], [-0.5, 0.5, 0]])
-            self.place(self.add_mesh(P, [(0, 1, 2), (0, 2, 3)]), emitter_mat(li), xf)
+            self.place(self.add_mesh(P, [(0, 1, 2), (0, 2, 3)]), emitter_mat(li), xf, moving=False)
         elif t == "PxrSphereLight":
             radius = float(np.linalg.norm(_xf_vec(xf, (0.5, 0, 0))))
             li = self.add_light(abi.LIGHT_SPHERE, scale, col, p=origin, radius=radius)
@@ -1370,7 +1436,7 @@ class _Builder:
     def scene(self):
         s = RibScene(self.width, self.height, self.fov)
         for k, (P, I, N) in enumerate(self.meshes):
-            s.add_mesh(P, I, N, st=self.mesh_st.get(k))
+            s.add_mesh(P, I, N, st=self.mesh_st.get(k), positions1=self.mesh_p1.get(k))
         s.patterns = [dict(n) for n in self.patterns]
         s.bindings = list(self.bindings)
         s.textures = list(self.textures)
@@ -1382,10 +1448,16 @@ class _Builder:
         if self.instances:
             s.add_instances([i[0] for i in self.instances], [i[1] for i in self.instances],
                             np.stack([i[2] for i in self.instances]))
+            for k, inst in enumerate(self.instances):
+                if inst[3] is not None:
+                    s.instance_motion[k] = np.asarray(inst[3], np.float64)
         for kind, params, mat, xf in self.quadrics:
             s.add_quadric(kind, params, mat, xf)
-        for p0, p1, v0, v1, mat, xf in self.curve_sets:
-            s.add_instance(s.add_curves(p0, p1, v0, v1), mat, np.asarray(xf, np.float64)[:3, :].reshape(12))
+        for p0, p1, v0, v1, mat, xf, xf1 in self.curve_sets:
+            s.add_instance(s.add_curves(p0, p1, v0, v1), mat, np.asarray(xf, np.float64)[:3, :].reshape(12),
+                           None if xf1 is None else np.asarray(xf1, np.float64)[:3, :].reshape(12))
+        if self.camera_motion_inv is not None:
+            s.camera_motion_inv = np.asarray(self.camera_motion_inv, np.float64)[:3, :].reshape(12)
         for med in self.media:
             s.add_medium(med)
         s.atmosphere = self.atmosphere

@@ -168,6 +168,9 @@ class Scene:
         self.quadrics = []        # (type, params (<= 8), object_to_world 3x4, material)
         self.media = []           # medium dicts (see medium())
         self.curves = []          # (p0 (n, 4) f32 xyz radius, p1, v0 (n,) f32, v1)
+        self.instance_motion = {} # instance -> object_to_world at shutter close (12 f64)
+        self.mesh_motion = {}     # mesh id -> (n_vertices, 3) f32 positions at shutter close
+        self.camera_motion_inv = None  # 12 f64: Camera::motion_inv (row-major 3x4), or None
         self.atmosphere = -1      # index into media of the global medium, -1 for none
         # Reference default camera: origin, looking down +z (camera.rs:97-103).
         self.eye = np.zeros(3)
@@ -179,15 +182,22 @@ class Scene:
         self._desc = None
 
     # -- geometry --------------------------------------------------------
-    def add_mesh(self, positions, indices, normals=None, st=None):
+    def add_mesh(self, positions, indices, normals=None, st=None, positions1=None):
         """Mesh::new(positions, indices, normals, st) (src/geometry/mesh.rs:
-        37-60); `st` is (n_vertices, 2) texture coordinates or None."""
+        37-60); `st` is (n_vertices, 2) texture coordinates or None;
+        `positions1` the vertex positions at shutter close (deformation
+        blur, `Mesh::with_motion`, mesh.rs:46-86) or None."""
         p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
         i = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
         n = None if normals is None else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
         if i.size and int(i.max()) >= len(p):
             raise ValueError("mesh index out of range")
         self.meshes.append((p, i, n))
+        if positions1 is not None:
+            p1 = np.ascontiguousarray(positions1, dtype=np.float32).reshape(-1, 3)
+            if p1.shape != p.shape:
+                raise ValueError("positions1 needs one position per vertex")
+            self.mesh_motion[len(self.meshes) - 1] = p1
         if st is not None:
             st = np.ascontiguousarray(st, dtype=np.float32).reshape(-1, 2)
             if len(st) != len(p):
@@ -280,14 +290,24 @@ class Scene:
         self._desc = None
         return CURVE_BASE + len(self.curves) - 1
 
-    def add_instance(self, mesh_id, material_id, xform=None):
+    def add_instance(self, mesh_id, material_id, xform=None, xform1=None):
+        """Instance of a mesh or curve set; `xform1` is its object-to-world
+        transform at shutter close (transform motion blur,
+        `Instance::with_motion`, mesh.rs:244-253) or None."""
         rec = np.zeros(1, dtype=INSTANCE_DTYPE)
         rec["xf"][0] = IDENTITY_3x4 if xform is None else np.asarray(xform, dtype=np.float64).reshape(12)
         rec["mesh"][0] = mesh_id
         rec["mat"][0] = material_id
         self._inst_chunks.append(rec)
         self._desc = None
+        if xform1 is not None:
+            self.instance_motion[self.n_instances - 1] = np.asarray(xform1, dtype=np.float64).reshape(12).copy()
         return self.n_instances - 1
+
+    @property
+    def has_motion(self):
+        """scene_builder.rs:239-241: rays draw a shutter time."""
+        return bool(self.instance_motion or self.mesh_motion or self.camera_motion_inv is not None)
 
     def add_instances(self, mesh_ids, material_ids, xforms):
         """Vectorised instance placement: xforms (n, 12) row-major 3x4."""
@@ -551,6 +571,25 @@ class Scene:
         if self.curves:
             d.curves = cur_arr
             d.n_curves = len(self.curves)
+        im_arr = (abi.RtInstanceMotion * max(1, len(self.instance_motion)))()
+        for k, (ii, xf1) in enumerate(sorted(self.instance_motion.items())):
+            im_arr[k].instance = ii
+            im_arr[k].object_to_world1 = (C.c_double * 12)(*xf1)
+        if self.instance_motion:
+            d.instance_motion = im_arr
+            d.n_instance_motion = len(self.instance_motion)
+        mm_arr = (abi.RtMeshMotion * max(1, len(self.mesh_motion)))()
+        for k, (mi, p1) in enumerate(sorted(self.mesh_motion.items())):
+            keep.append(p1)
+            mm_arr[k].mesh = mi
+            mm_arr[k].positions1 = p1.ctypes.data_as(C.POINTER(C.c_float))
+        if self.mesh_motion:
+            d.mesh_motion = mm_arr
+            d.n_mesh_motion = len(self.mesh_motion)
+        cam_mot = None
+        if self.camera_motion_inv is not None:
+            cam_mot = (C.c_double * 12)(*np.asarray(self.camera_motion_inv, dtype=np.float64).reshape(12))
+            d.camera_motion_inv = cam_mot
         self._keep = (keep, mesh_arr, mat_arr, light_arr, pat_arr, bind_arr, tex_arr, ies_arr, quad_arr, med_arr,
-                      cur_arr)
+                      cur_arr, im_arr, mm_arr, cam_mot)
         return d

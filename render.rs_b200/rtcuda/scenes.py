@@ -522,3 +522,27 @@ def furball(width=128, height=64, n_strands=20_000, seed=5):
     s.add_instance(s.add_curves(p0, p1, v0, v1), coat, affine(np.eye(3), centre))
     return s
 
+
+
+def motion_cornell(width=64, height=64, transform=True, deform=True, camera=True):
+    """The Cornell box with motion blur (src/geometry/mesh.rs:230-304,
+    camera.rs:85-146): the tall box slides 0.5 toward +x and turns a further
+    20 deg over the shutter (transform motion), a glossy sheet with vertex
+    normals bends (its far edge rises 0.4 at shutter close: deformation, so
+    its shading takes the geometric normal), and the camera drifts 0.15
+    along +x (camera motion, as the inverse delta the reference stores).
+    Each part can be left static."""
+    s = cornell_box(width, height)
+    tall = 3   # instance of the tall box (walls, left, right, tall, short, light)
+    if transform:
+        s.instance_motion[tall] = affine(rot_y(37.0) @ np.diag([0.6, 1.2, 0.6]), (0.15, -0.399, -0.3))
+    p, i = quad((-0.2, -0.2, 0.4), (0.6, 0.0, 0.0), (0.0, 0.0, 0.5))
+    p = np.asarray(p, np.float32)
+    p1 = p.copy()
+    p1[np.isclose(p[:, 2], 0.9), 1] += 0.4
+    nrm = np.tile(np.array([[0.0, 1.0, 0.0]], np.float32), (len(p), 1))
+    sheet = s.add_mesh(p, i, normals=nrm, positions1=p1 if deform else None)
+    s.add_instance(sheet, s.add_material(ggx_floor((0.8, 0.7, 0.3), 0.35)))
+    if camera:
+        s.camera_motion_inv = affine(np.eye(3), (-0.15, 0.0, 0.0))
+    return s
