@@ -718,8 +718,8 @@ uint32_t lbvh_build(std::vector<LightNode>& nodes, std::vector<uint32_t>& leaf_o
 // Pattern graph and bindings (src/texture/pattern.rs, material.rs:29-30,
 // 95-101) in device form. Nodes may read only lower-indexed nodes, so the
 // graph is evaluated in index order; a material's bindings may reach at
-// most RT_MAX_PATTERN_NODES consecutive nodes. Presence bindings would need
-// pattern evaluation inside shadow-ray traversal and are refused.
+// most RT_MAX_PATTERN_NODES consecutive nodes. A presence binding makes the
+// scene's cutouts pattern-driven (DevScene::presence_pat).
 bool flatten_patterns(const rt_scene_desc* d, HostScene& H, std::string* err) {
     if (!d->n_patterns && !d->n_bindings) return true;
     if ((d->n_patterns && !d->patterns) || (d->n_bindings && !d->bindings) || (d->n_textures && !d->textures)) {
@@ -872,9 +872,10 @@ bool flatten_patterns(const rt_scene_desc* d, HostScene& H, std::string* err) {
             return false;
         }
         if (pb.field == RT_FIELD_PRESENCE) {
-            *err = "pattern binding " + std::to_string(b) +
-                   ": presence bindings are not supported by the CUDA backend";
-            return false;
+            // Pattern-driven cutouts (texture alpha): decided where the
+            // pattern is evaluated, at shading and per shadow-ray blocker.
+            H.scalars.presence_pat = 1;
+            H.scalars.any_presence = 1;
         }
         per_mat[pb.material].push_back(make_uint2(pb.field, pb.node));
     }

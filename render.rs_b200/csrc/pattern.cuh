@@ -280,8 +280,8 @@ __device__ __forceinline__ float3 pattern_node(const DevScene& S, const DevPatte
     }
 }
 
-// BoundField::apply: scalars take channel 0; roughnesses clamp to
-// [0.005, 1] (presence bindings are refused when the scene is built).
+// BoundField::apply (texture/pattern.rs:270-290): scalars take channel 0;
+// roughnesses clamp to [0.005, 1], presence to [0, 1].
 __device__ __forceinline__ void apply_field(DevPbr& q, uint32_t field, float3 v) {
     auto set3 = [&](float* dst) {
         dst[0] = v.x;
@@ -302,6 +302,7 @@ __device__ __forceinline__ void apply_field(DevPbr& q, uint32_t field, float3 v)
         case RT_FIELD_GLASS_ROUGHNESS: q.glass_rough = fminf(fmaxf(v.x, 0.005f), 1.0f); break;
         case RT_FIELD_REFRACTION_COLOR: set3(q.refraction); break;
         case RT_FIELD_GLOW: set3(q.glow); break;
+        case RT_FIELD_PRESENCE: q.presence = fminf(fmaxf(v.x, 0.0f), 1.0f); break;
         default: break;
     }
 }

@@ -1737,8 +1737,20 @@ __device__ __forceinline__ float3 shadow_walk(const DevScene& S, TravStack& st, 
             if (hg.front) mstack_push(ms, m.interior);
             else mstack_pop(ms);
         } else {
-            if (m.presence >= 1.0f) return f3(0.0f, 0.0f, 0.0f);
-            vis = vis * (1.0f - m.presence);
+            float presence = m.presence;
+            if (S.presence_pat && S.mat_pat[mat].bind_n) {
+                // Pattern-driven cutout: the blocker's material with its
+                // patterns at the hit, footprint 0 (pt/mod.rs:1290,
+                // kernel_pt.metal:1369).
+                HitGeo hg;
+                hit_geometry(S, o, d, hr, hg, time);
+                const HitSt hs = hit_st(S, hr, hg.p, time);
+                DevMaterial mres = m;
+                resolve_material(S, S.mat_pat[mat], hs, hg.p, hg.nw, d, 0.0f, mres);
+                presence = mres.presence;
+            }
+            if (presence >= 1.0f) return f3(0.0f, 0.0f, 0.0f);
+            vis = vis * (1.0f - presence);
             if (maxc(vis) < 1e-4f) return f3(0.0f, 0.0f, 0.0f);
         }
         o = o + d * (t + RT_RAY_OFFSET);
@@ -1751,28 +1763,30 @@ __device__ __forceinline__ float3 shadow_walk(const DevScene& S, TravStack& st, 
 // surface / collision / walk-exit one, then the equiangular one) and adds
 // both contributions in that order. Ratio tracking draws from a stream
 // derived from the path's state, so the image stays reproducible.
-template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_shadow_media(DevScene S, Paths P, PtConsts C) {
+// Without MED (scenes whose cutouts are pattern-driven, no media) each
+// queue entry is a plain slot with one shadow ray and no medium.
+template <int BLOCK, bool MED = true>
+__global__ void __launch_bounds__(BLOCK) k_shadow_walk(DevScene S, Paths P, PtConsts C) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
     TravStack st;
     st.init(stack_sh + threadIdx.x, BLOCK);
     const uint32_t n = P.cnt[CNT_SHADOW];
     unsigned long long rays = 0;
     for (uint32_t j = blockIdx.x * BLOCK + threadIdx.x; j < n; j += gridDim.x * BLOCK) {
-        const uint32_t e = P.q_sh[j];
+        const uint32_t e = MED ? P.q_sh[j] : (P.q_sh[j] | SH_PRIMARY);
         const uint32_t slot = e & SH_SLOT_MASK;
         const uint4 rs = P.rng[slot];
         Pcg rng;
         rng.state = splitmix(((uint64_t)rs.x | ((uint64_t)rs.y << 32)) ^ 0xD1B54A32D192ED03ull);
         rng.inc = (splitmix((uint64_t)rs.z | ((uint64_t)rs.w << 32)) << 1) | 1ull;
         float3 add = f3(0.0f, 0.0f, 0.0f), add_aux = f3(0.0f, 0.0f, 0.0f);
-        for (int r = 0; r < 2; r++) {
+        for (int r = 0; r < (MED ? 2 : 1); r++) {
             if (!(e & (r == 0 ? SH_PRIMARY : SH_EQUI))) continue;
             const float4 o4 = r == 0 ? P.sh_o[slot] : P.sh2_o[slot];
             const float4 d4 = r == 0 ? P.sh_d[slot] : P.sh2_d[slot];
             const float4 c4 = r == 0 ? P.sh_c[slot] : P.sh2_c[slot];
-            const float3 vis = shadow_walk(S, st, xyz(o4), xyz(d4), d4.w, __float_as_uint(o4.w), rng, P.err, rays,
-                                           S.motion ? P.time[slot] : 0.0f);
+            const float3 vis = shadow_walk(S, st, xyz(o4), xyz(d4), d4.w, MED ? __float_as_uint(o4.w) : RT_MEDIUM_NONE,
+                                           rng, P.err, rays, S.motion ? P.time[slot] : 0.0f);
             const float3 c = xyz(c4) * vis;
             add = add + c;
             if (c4.w != 0.0f) add_aux = add_aux + c;

@@ -273,6 +273,7 @@ struct DevScene {
     const DevQuadric* quadrics;  // analytic quadrics, tested before the BVH (null when none)
     uint32_t n_quadrics;
     uint32_t any_presence;       // some material has presence < 1
+    uint32_t presence_pat;       // some material's presence is bound to a pattern (texture cutouts)
     uint32_t max_steps;          // traversal steps per ray before the query is given up (error bit)
     uint32_t dome;               // first dome light (misses see it), ~0 for none
     const DevMedium* media;      // participating media (null when none)

@@ -555,7 +555,9 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     // kept, whose first-hit values come from the first surface a camera ray
     // meets even when it passes through it (pt/mod.rs:690-700); then the
     // shade kernel skips surfaces as the reference does, in extra waves.
-    C.pres_in_trav = (s->S.any_presence && !s->params.aovs) ? 1u : 0u;
+    // Cutouts decided in the extension traversal, unless AOVs want the first
+    // surface met or the cutouts are pattern-driven (decided in shading).
+    C.pres_in_trav = (s->S.any_presence && !s->params.aovs && !s->S.presence_pat) ? 1u : 0u;
     // Waves: one per bounce, plus the surfaces a path may pass without a
     // bounce (cutouts skipped in shade waves, volume-hull crossings).
     const bool skip_waves = (s->S.any_presence && !C.pres_in_trav) || s->S.n_media;
@@ -639,7 +641,8 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
                 launches++;
             }
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 2], st));
-            if (med) k_shadow_media<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            if (med) k_shadow_walk<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            else if (s->S.presence_pat) k_shadow_walk<TRAV_BLOCK, false><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             else if (mot) k_shadow<TRAV_BLOCK, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             else if (quad) k_shadow<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             else k_shadow<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);

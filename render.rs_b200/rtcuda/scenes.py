@@ -546,3 +546,28 @@ def motion_cornell(width=64, height=64, transform=True, deform=True, camera=True
     if camera:
         s.camera_motion_inv = affine(np.eye(3), (-0.15, 0.0, 0.0))
     return s
+
+
+def pattern_cutouts(width=64, height=48):
+    """Cutouts driven by patterns (a presence binding, the reference's
+    texture-alpha leaves): a screen whose presence is a 6 x 6 checker of 1
+    and 0 (square holes), a second one whose presence is fBm noise (graded
+    partial cover), both between a ceiling light and the floor so that
+    their shadows and the views through them depend on the pattern at every
+    blocker."""
+    s = Scene(width, height, fov=50.0)
+    s.look_at((0.0, 1.2, -3.0), (0.0, 0.6, 0.0))
+    st_quad = np.array([[0.0, 0.0], [1.0, 0.0], [1.0, 1.0], [0.0, 1.0]])
+    white = s.add_material(matte((0.75, 0.75, 0.75)))
+    s.add_instance(s.add_mesh(*quad((-2, 0, -3), (0, 0, 5), (4, 0, 0))), white)
+    s.add_instance(s.add_mesh(*quad((-2, 0, 2), (4, 0, 0), (0, 3, 0))), white)
+    holes = s.add_material(matte((0.8, 0.3, 0.2)))
+    s.bind_pattern(holes, "presence", s.add_checker((1, 1, 1), (0, 0, 0), scale=(6.0, 6.0)))
+    p, i = quad((-1.2, 0.9, -0.6), (1.1, 0.0, 0.0), (0.0, 0.3, 1.2))
+    s.add_instance(s.add_mesh(p, i, st=st_quad), holes)
+    veil = s.add_material(ggx_floor((0.2, 0.5, 0.8), 0.3))
+    s.bind_pattern(veil, "presence", s.add_fractal(frequency=4.0, octaves=3))
+    p, i = quad((0.2, 0.4, -0.4), (0.9, 0.0, 0.0), (0.0, 0.9, 0.6))
+    s.add_instance(s.add_mesh(p, i, st=st_quad), veil)
+    s.add_rect_light((-0.6, 2.6, -0.6), (1.2, 0.0, 0.0), (0.0, 0.0, 1.2), 8.0)
+    return s

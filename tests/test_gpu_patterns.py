@@ -1,12 +1,15 @@
 """Procedural patterns on the GPU (csrc/pattern.cuh) against the f64
 oracle's restatement of src/texture/pattern.rs and shade_params
 (pt/mod.rs:389-439): the same scene through both, statistical parity as
-in the other render tests, and the ray-cone footprint filtering a checker
-finer than a pixel to its mean colour."""
+in the other render tests, the ray-cone footprint filtering a checker
+finer than a pixel to its mean colour, and cutouts whose presence is a
+pattern (decided in shading and at every shadow-ray blocker,
+pt/mod.rs:1244-1306, kernel_pt.metal:1336-1378)."""
 import numpy as np
 import pytest
 
 import oracle
+from mc_parity import compare, render_quad
 from rtcuda import PtSession, abi, scene, scenes
 
 pytestmark = pytest.mark.gpu
@@ -156,3 +159,25 @@ def test_udim_tiles_match_oracle():
     ca = oracle.OracleScene(s).render(p, 0, spp, aovs=True)[1].reshape(h, w, 12)[..., 0:3] / spp
     assert np.abs(ga - ca).mean() < 0.01, np.abs(ga - ca).mean()
     assert len(np.unique(np.round(ca.reshape(-1, 3), 1), axis=0)) >= 4
+
+
+def test_pattern_cutouts_match_oracle():
+    s = scenes.pattern_cutouts(48, 36)
+    g, o, r, pr, st = render_quad(s, abi.make_params(max_depth=6), 32, 1024)
+    res = compare(g, o, r, paired=pr)
+    assert res["ok"], res
+
+
+def test_pattern_cutouts_change_the_image():
+    """The same screens without their presence patterns (solid) render
+    differently: light and view pass through the holes."""
+    s = scenes.pattern_cutouts(48, 36)
+    with PtSession(s, abi.make_params(max_depth=6)) as g:
+        g.render_samples(0, 256)
+        img = g.image()
+    flat = scenes.pattern_cutouts(48, 36)
+    flat.bindings = [b for b in flat.bindings if b[1] != abi.FIELD_PRESENCE]
+    with PtSession(flat, abi.make_params(max_depth=6)) as g:
+        g.render_samples(0, 256)
+        solid = g.image()
+    assert abs(img.mean() - solid.mean()) > 0.02 * solid.mean()
