@@ -141,6 +141,8 @@ typedef struct rt_light_desc {
 } rt_light_desc;
 
 enum { RT_FILTER_BOX = 0, RT_FILTER_TRIANGLE = 1, RT_FILTER_GAUSSIAN = 2 };
+/* Camera::projection (camera.rs:5-9). */
+enum { RT_PROJECTION_PERSPECTIVE = 0, RT_PROJECTION_ORTHOGRAPHIC = 1 };
 
 /* Pinhole / thin-lens camera (src/scene/camera.rs:67-92, 150-179).
  * right/up/forward are used as given (Camera::set_transform computes
@@ -156,8 +158,10 @@ typedef struct rt_camera_desc {
     double   lens_radius;           /* 0 = pinhole */
     double   focal_distance;
     int32_t  filter;                /* RT_FILTER_* */
-    int32_t  pad_;
+    int32_t  projection;            /* RT_PROJECTION_*; orthographic rays start on the screen window */
     double   filter_width;
+    double   ortho_half[2];         /* half-extents of the orthographic window (Camera::ortho_half;
+                                       the reference's default is (aspect, 1)) */
 } rt_camera_desc;
 
 /* Pattern node (src/texture/pattern.rs:47-67; PatternNode). Every node
@@ -391,7 +395,7 @@ static_assert(sizeof(rt_instance_motion) == 104, "rt_instance_motion layout");
 static_assert(sizeof(rt_mesh_motion) == 16, "rt_mesh_motion layout");
 static_assert(sizeof(rt_medium_desc) == 136, "rt_medium_desc layout");
 static_assert(sizeof(rt_light_desc) == 120, "rt_light_desc layout");
-static_assert(sizeof(rt_camera_desc) == 144, "rt_camera_desc layout");
+static_assert(sizeof(rt_camera_desc) == 160, "rt_camera_desc layout");
 static_assert(sizeof(rt_params) == 72, "rt_params layout");
 static_assert(sizeof(rt_pattern_input) == 32, "rt_pattern_input layout");
 static_assert(sizeof(rt_pattern_desc) == 264, "rt_pattern_desc layout");
@@ -399,7 +403,7 @@ static_assert(sizeof(rt_texture_desc) == 16, "rt_texture_desc layout");
 static_assert(sizeof(rt_pattern_binding) == 16, "rt_pattern_binding layout");
 static_assert(sizeof(rt_ies_desc) == 112, "rt_ies_desc layout");
 static_assert(sizeof(rt_quadric_desc) == 168, "rt_quadric_desc layout");
-static_assert(sizeof(rt_scene_desc) == 376, "rt_scene_desc layout");
+static_assert(sizeof(rt_scene_desc) == 392, "rt_scene_desc layout");
 }
 #endif
 

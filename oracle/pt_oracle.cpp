@@ -2445,6 +2445,8 @@ struct Camera {
     double lens_radius, focal_distance;
     int filter;
     double filter_width;
+    int projection = RT_PROJECTION_PERSPECTIVE;  // camera.rs:5-9
+    double ortho_half[2] = {1.0, 1.0};           // camera.rs:82-83
     bool moving = false;  // camera.rs:87-92 motion_inv present
     M4 motion_inv;
 
@@ -2473,10 +2475,13 @@ struct Camera {
             default: return (u - 0.5) * filter_width;
         }
     }
-    // camera.rs:150-179 (perspective).
+    // camera.rs:150-179: orthographic rays start on the screen window and
+    // ignore the lens; perspective rays through the thin lens.
     Ray generate(double px, double py, double lu, double lv) const {
         double u = (px / (double)width) * 2.0 - 1.0;
         double v = 1.0 - (py / (double)height) * 2.0;
+        if (projection == RT_PROJECTION_ORTHOGRAPHIC)
+            return make_ray(eye + right * (u * ortho_half[0]) + up * (v * ortho_half[1]), forward);
         double aspect = (double)width / (double)height;
         double half_h = std::tan(fov * PI / 180.0 / 2.0);
         double half_w = aspect * half_h;
@@ -3540,6 +3545,9 @@ oracle_scene* oracle_scene_create(const rt_scene_desc* d) {
     s.cam.focal_distance = c.focal_distance;
     s.cam.filter = c.filter;
     s.cam.filter_width = c.filter_width;
+    s.cam.projection = c.projection;
+    s.cam.ortho_half[0] = c.ortho_half[0];
+    s.cam.ortho_half[1] = c.ortho_half[1];
     if (d->camera_motion_inv) {
         s.cam.moving = true;
         s.cam.motion_inv = identity();

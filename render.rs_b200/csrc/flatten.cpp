@@ -1803,6 +1803,13 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
     H.scalars.focal_distance = (float)c.focal_distance;
     H.scalars.filter = (uint32_t)c.filter;
     H.scalars.filter_width = (float)c.filter_width;
+    if (c.projection != RT_PROJECTION_PERSPECTIVE && c.projection != RT_PROJECTION_ORTHOGRAPHIC) {
+        *err = "unknown camera projection";
+        return false;
+    }
+    H.scalars.projection = (uint32_t)c.projection;
+    H.scalars.ortho_hw = (float)c.ortho_half[0];
+    H.scalars.ortho_hh = (float)c.ortho_half[1];
     H.scalars.width = c.width;
     H.scalars.height = c.height;
     return true;

@@ -377,7 +377,17 @@ __global__ void k_raygen(DevScene S, Paths P, PtConsts C) {
     float3 upv = f3(S.up[0], S.up[1], S.up[2]);
     float3 dir = fwd + rgt * (uu * S.half_w) + upv * (vv * S.half_h);
     float3 o = eye, d;
-    if (S.lens_radius > 0.0f) {
+    if (S.projection == RT_PROJECTION_ORTHOGRAPHIC) {
+        // Rays start on the screen window, parallel to forward (camera.rs:
+        // 154-159). The lens samples are still drawn when the lens is open,
+        // as pt::camera_ray draws them before generating the ray.
+        if (S.lens_radius > 0.0f) {
+            rng.next_f();
+            rng.next_f();
+        }
+        o = eye + rgt * (uu * S.ortho_hw) + upv * (vv * S.ortho_hh);
+        d = normalize_ref(fwd);
+    } else if (S.lens_radius > 0.0f) {
         float lu = rng.next_f(), lv = rng.next_f();
         float r = S.lens_radius * sqrtf(lu), sp, cp;
         sincosf(2.0f * RT_PI * lv, &sp, &cp);

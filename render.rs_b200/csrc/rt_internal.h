@@ -305,6 +305,8 @@ struct DevScene {
     float eye[3], fwd[3], right[3], up[3];
     float half_w, half_h, lens_radius, focal_distance, filter_width;
     uint32_t filter, width, height;
+    uint32_t projection;         // RT_PROJECTION_*
+    float ortho_hw, ortho_hh;    // orthographic window half-extents
     float background[3];
 };
 

@@ -133,8 +133,9 @@ class RtCameraDesc(C.Structure):
         ("lens_radius", C.c_double),
         ("focal_distance", C.c_double),
         ("filter", C.c_int32),
-        ("pad_", C.c_int32),
+        ("projection", C.c_int32),
         ("filter_width", C.c_double),
+        ("ortho_half", C.c_double * 2),
     ]
 
 
@@ -273,11 +274,12 @@ class RtParams(C.Structure):
 
 LIGHT_POINT, LIGHT_DISTANT, LIGHT_RECT, LIGHT_SPHERE, LIGHT_DISK, LIGHT_DOME = range(6)
 FILTER_BOX, FILTER_TRIANGLE, FILTER_GAUSSIAN = range(3)
+PROJECTION_PERSPECTIVE, PROJECTION_ORTHOGRAPHIC = range(2)
 
 for _t, _n in ((RtMeshDesc, 40), (RtInstanceDesc, 104), (RtMaterialDesc, 376), (RtLightDesc, 120),
-               (RtCameraDesc, 144), (RtParams, 72), (RtPatternInput, 32), (RtPatternDesc, 264),
+               (RtCameraDesc, 160), (RtParams, 72), (RtPatternInput, 32), (RtPatternDesc, 264),
                (RtPatternBinding, 16), (RtTextureDesc, 16), (RtIesDesc, 112), (RtQuadricDesc, 168),
-               (RtSceneDesc, 376), (RtMediumDesc, 136), (RtCurvesDesc, 40), (RtInstanceMotion, 104),
+               (RtSceneDesc, 392), (RtMediumDesc, 136), (RtCurvesDesc, 40), (RtInstanceMotion, 104),
                (RtMeshMotion, 16)):
     assert C.sizeof(_t) == _n, (_t.__name__, C.sizeof(_t), _n)
 

@@ -507,6 +507,8 @@ class _Builder:
     def __init__(self, base_dir=None):
         self.width, self.height, self.fov = 640, 480, 45.0
         self.dof = None
+        self.projection = abi.PROJECTION_PERSPECTIVE
+        self.screen_window = None
         self.filter = (abi.FILTER_BOX, 1.0)
         self.pixel_samples = (1, 1)
         self.background = (0.0, 0.0, 0.0)
@@ -778,11 +780,14 @@ class _Builder:
         elif name == "Projection":
             kind = _str(vals, 0)
             if kind == "perspective":
+                self.projection = abi.PROJECTION_PERSPECTIVE
                 fov = _Params(vals, 1).number("fov")
                 if fov is not None:
                     self.fov = fov
+            elif kind == "orthographic":
+                self.projection = abi.PROJECTION_ORTHOGRAPHIC
             elif kind is not None:
-                self.warn(f'Projection "{kind}" not rendered; using perspective')
+                self.warn(f'Projection "{kind}" not implemented; using perspective')
         elif name == "DepthOfField":
             a = [_num(vals, k) for k in range(3)]
             if all(x is not None for x in a):
@@ -798,7 +803,10 @@ class _Builder:
                 kinds = {"triangle": abi.FILTER_TRIANGLE, "gaussian": abi.FILTER_GAUSSIAN, "box": abi.FILTER_BOX}
                 self.filter = (kinds[f], max(w, 1e-3)) if f in kinds else (abi.FILTER_BOX, 1.0)
         elif name == "ScreenWindow":
-            self.warn("ScreenWindow only affects orthographic cameras; ignored")
+            # The orthographic window's half-extents (scene_builder.rs:529-534, 223-225).
+            a = [_num(vals, k) for k in range(4)]
+            if all(x is not None for x in a):
+                self.screen_window = tuple(a)
         elif name == "PixelSamples":
             x, y = _num(vals, 0), _num(vals, 1)
             if x is not None and y is not None:
@@ -1462,6 +1470,10 @@ class _Builder:
             s.add_medium(med)
         s.atmosphere = self.atmosphere
         s.filter, s.filter_width = self.filter
+        s.projection = self.projection
+        if self.screen_window is not None:
+            l, r, b, t = self.screen_window
+            s.ortho_half = (abs(r - l) * 0.5, abs(t - b) * 0.5)
         if self.dof is not None:
             fstop, flen, fdist = self.dof
             if math.isfinite(fstop) and fstop > 0:

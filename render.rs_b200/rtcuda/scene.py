@@ -179,6 +179,10 @@ class Scene:
         self.right = np.cross(self.up, self.forward)
         self.lens_radius, self.focal_distance = 0.0, 1.0
         self.filter, self.filter_width = abi.FILTER_BOX, 1.0
+        # Camera::projection and ortho_half (camera.rs:80-83, 114): the
+        # orthographic window defaults to (aspect, 1).
+        self.projection = abi.PROJECTION_PERSPECTIVE
+        self.ortho_half = (self.width / max(self.height, 1), 1.0)
         self._desc = None
 
     # -- geometry --------------------------------------------------------
@@ -463,7 +467,8 @@ class Scene:
         cam = abi.RtCameraDesc(self.width, self.height, self.fov, abi.c_double3(*self.eye),
                                abi.c_double3(*self.forward), abi.c_double3(*self.up),
                                abi.c_double3(*self.right), self.lens_radius, self.focal_distance,
-                               self.filter, 0, self.filter_width)
+                               self.filter, self.projection, self.filter_width,
+                               (C.c_double * 2)(*self.ortho_half))
         d = abi.RtSceneDesc()
         d.meshes = mesh_arr
         d.instances = inst.ctypes.data_as(C.POINTER(abi.RtInstanceDesc))

@@ -33,8 +33,8 @@ def test_library_exports_every_declared_symbol():
 
 def test_descriptor_layouts_match_headers():
     sizes = {"rt_mesh_desc": 40, "rt_instance_desc": 104, "rt_material_desc": 376, "rt_light_desc": 120,
-             "rt_camera_desc": 144, "rt_params": 72, "rt_pattern_desc": 264, "rt_pattern_binding": 16,
-             "rt_texture_desc": 16, "rt_ies_desc": 112, "rt_quadric_desc": 168, "rt_scene_desc": 376, "rt_medium_desc": 136,
+             "rt_camera_desc": 160, "rt_params": 72, "rt_pattern_desc": 264, "rt_pattern_binding": 16,
+             "rt_texture_desc": 16, "rt_ies_desc": 112, "rt_quadric_desc": 168, "rt_scene_desc": 392, "rt_medium_desc": 136,
              "rt_curves_desc": 40, "rt_instance_motion": 104, "rt_mesh_motion": 16}
     text = open(os.path.join(ROOT, "include", "rt_scene.h")).read()
     for name, size in sizes.items():

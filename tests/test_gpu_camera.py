@@ -40,3 +40,16 @@ def test_camera_models_match_oracle(filt, width, lens, pinhole_box):
         assert np.all(np.abs(a - b) <= 0.08 * b + 0.015), (axis, np.abs(a - b).max())
     same, other = np.abs(img - cpu).mean(), np.abs(img - pinhole_box).mean()
     assert same < 0.8 * other, (same, other)
+
+
+def test_orthographic_camera_matches_oracle():
+    """Orthographic rays (camera.rs:154-159) from a window of half-extents
+    (1.2, 1.2) over the Cornell box: image parity with the oracle
+    (tests/mc_parity.py)."""
+    from mc_parity import compare, render_quad
+    s = scenes.cornell_box(40, 40)
+    s.projection = abi.PROJECTION_ORTHOGRAPHIC
+    s.ortho_half = (1.2, 1.2)
+    g, o, r, pr, _ = render_quad(s, abi.make_params(max_depth=6), 32, 1024)
+    res = compare(g, o, r, paired=pr)
+    assert res["ok"], res
