@@ -336,9 +336,11 @@ def other_workloads(flush, stream):
     1920x1080 x 64 spp (depth 12), the media Cornell box 512^2 x 16 spp (fog,
     an fBm cloud, absorbing glass, a subsurface sphere; 64 bounces, the
     reference's depth with media), the furball 960x480 x 16 spp (20,000
-    b-spline strands of Marschner hair, 480,000 segments). One warm-up
-    pass, then one timed render
-    call (device time from the session's events); scene build excluded."""
+    b-spline strands of Marschner hair, 480,000 segments), the Cornell box
+    with motion blur (a moving box, a deforming sheet and camera motion) and
+    with all of it static, 512^2 x 16 spp, and the pattern-cutout screens
+    512x384 x 16 spp. One warm-up pass, then one timed render call (device
+    time from the session's events); scene build excluded."""
     import torch
     from rtcuda import PtSession, abi, scenes
     out = {}
@@ -350,7 +352,12 @@ def other_workloads(flush, stream):
              ("media_cornell_512x512_16spp_depth64", lambda: scenes.media_cornell(512, 512),
               dict(max_depth=8, rr_start=3), 16),
              ("furball_20k_strands_960x480_16spp_depth8", lambda: scenes.furball(960, 480, 20_000),
-              dict(max_depth=8, rr_start=3), 16)]
+              dict(max_depth=8, rr_start=3), 16),
+             ("motion_cornell_512x512_16spp_depth8", lambda: scenes.motion_cornell(512, 512), scenes.CORNELL, 16),
+             ("motion_cornell_static_512x512_16spp_depth8",
+              lambda: scenes.motion_cornell(512, 512, transform=False, deform=False, camera=False), scenes.CORNELL,
+              16),
+             ("pattern_cutouts_512x384_16spp_depth8", lambda: scenes.pattern_cutouts(512, 384), scenes.CORNELL, 16)]
     for name, make, cfg, spp in cases:
         t0 = time.perf_counter()
         s = make()
