@@ -1528,6 +1528,7 @@ int device_build_scene(const rt_scene_desc* d, HostScene* H, DeviceBvh* out, cud
         }
         const double wa = area(alo, ahi);
         const bool dense = wa > 0.0 && total_area > RT_BRAID_DENSE * wa;
+        H->scalars.refill_at = dense ? RT_REFILL_DENSE : RT_REFILL_SPARSE;
         std::vector<uint64_t> off(NI);
         uint64_t total = 0;
         for (uint32_t i = 0; i < NI; i++) {

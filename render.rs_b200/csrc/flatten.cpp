@@ -1034,6 +1034,7 @@ void tlas_items(const rt_scene_desc* d, const std::vector<std::vector<RootChild>
             all.grow(local);
         }, 4096);
         dense = all.area() > 0.0 && total_area > RT_BRAID_DENSE * all.area();
+        H->scalars.refill_at = dense ? RT_REFILL_DENSE : RT_REFILL_SPARSE;
     }
     // A dense scene splits every instance into its BLAS's second-level
     // frontier; others split an instance into its root's children when
@@ -1482,6 +1483,7 @@ bool flatten_scene(const rt_scene_desc* d, HostScene* out, std::string* err, boo
     }
     H.tlas_nodes = 0;
     H.scalars.tlas_root = 0xFFFFFFFFu;
+    H.scalars.refill_at = RT_REFILL_SPARSE;
     if (build_bvh && d->n_instances) {
         std::vector<double> boxes;
         std::vector<uint2> items;

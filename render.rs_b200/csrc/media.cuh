@@ -215,8 +215,9 @@ __device__ __forceinline__ void mstack_pop(uint2& s) {
 // One ray walked to its closest hit by a single thread (quadrics first, then
 // the BVH below the closest quadric), for the sequential loops of subsurface
 // walks and medium-aware shadow rays. d must be unit length: t is the
-// distance; `time` is the path's shutter time. Returns the hit record in the
-// layout k_extend writes.
+// distance; `time` is the path's shutter time (read with MOT, scenes with
+// motion blur). Returns the hit record in the layout k_extend writes.
+template <bool MOT = false>
 __device__ __forceinline__ bool trace_closest(const DevScene& S, TravStack& st, float3 o, float3 d, float tmax,
                                               uint32_t* err, uint4& hr, float time = 0.0f) {
     float tq = tmax;
@@ -224,7 +225,7 @@ __device__ __forceinline__ bool trace_closest(const DevScene& S, TravStack& st, 
     if (qk != 0xFFFFFFFFu) tmax = tq;
     PhaseState ps;
     bool found = false;
-    if (trav_begin(S, ps.ts, st, o, d, tmax, time)) {
+    if (trav_begin(S, ps.ts, st, o, d, tmax, MOT ? time : 0.0f)) {
         phase_begin(ps);
         for (;;) {
             if (++ps.ts.steps > S.max_steps) {
@@ -232,7 +233,7 @@ __device__ __forceinline__ bool trace_closest(const DevScene& S, TravStack& st, 
                 break;
             }
             if (ps.pending) {
-                if (op_leaf<false, true>(S, ps, st, err)) break;
+                if (op_leaf<false, MOT>(S, ps, st, err)) break;
             } else if (ps.need_pop) {
                 if (!op_pop(ps, st)) break;
             } else if (op_node<false>(S, ps, st, err)) {

@@ -647,13 +647,12 @@ __global__ void k_guide_keep(const uint32_t* tb_cnt, float scale, uint32_t cap, 
 // steps (and some lane has a parked leaf): the other lanes would idle while
 // the last few walk down to their leaves, so they take their leaf phase now
 // and the stragglers continue in the next node phase. Idle lanes are refilled
-// once at most RT_REFILL_AT lanes hold a ray. On the 1M-triangle cloud
-// (B200), against running every node phase to the end with refills at 16:
-// closest hit 286 -> 422 Mrays/s, any hit 420 -> 678, a 1920x1080 16-spp
-// frame 154 -> 119 ms; thresholds 12-16 were within 2% of each other.
-#ifndef RT_REFILL_AT
-#define RT_REFILL_AT 20
-#endif
+// once at most S.refill_at lanes hold a ray (RT_REFILL_SPARSE, or
+// RT_REFILL_DENSE in scenes of densely overlapping instances: rt_internal.h).
+// On the 1M-triangle cloud (B200), against running every node phase to the
+// end with refills at 16: closest hit 286 -> 422 Mrays/s, any hit 420 -> 678,
+// a 1920x1080 16-spp frame 154 -> 119 ms; thresholds 12-16 were within 2% of
+// each other.
 #ifndef RT_NODE_PHASE_EXIT
 #define RT_NODE_PHASE_EXIT 14
 #endif
@@ -680,7 +679,7 @@ __device__ __forceinline__ void ray_pump(const DevScene& S, uint32_t n, uint32_t
     const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
     for (;;) {
         uint32_t act = __ballot_sync(0xFFFFFFFFu, active);
-        if (!exhausted && __popc(act) <= RT_REFILL_AT) {
+        if (!exhausted && __popc(act) <= S.refill_at) {
             uint32_t idle = ~act;
             uint32_t leader = __ffs(idle) - 1, base = 0;
             if (lane == leader) base = atomicAdd(fetch, __popc(idle));
@@ -1590,7 +1589,8 @@ __global__ void __launch_bounds__(BLOCK, RT_TRAV_MIN_BLOCKS) k_shadow(DevScene S
 // 256 steps. The walk leaves diffusely where it first reaches a surface:
 // NEE there for a white Lambert lobe, then a cosine direction becomes the
 // path's next ray. Walks that escape or run out of steps end the path.
-template <int BLOCK, bool MED>
+// MOT: the scene has motion blur (walks take the path's shutter time).
+template <int BLOCK, bool MED, bool MOT = false>
 __global__ void __launch_bounds__(BLOCK) k_sss(DevScene S, Paths P, PtConsts C, uint32_t qout) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
     TravStack st;
@@ -1618,13 +1618,13 @@ __global__ void __launch_bounds__(BLOCK) k_sss(DevScene S, Paths P, PtConsts C, 
             const float3 sst = f3(m.sss_st[0], m.sss_st[1], m.sss_st[2]);
             const float3 sss = f3(m.sss_ss[0], m.sss_ss[1], m.sss_ss[2]);
             const uint32_t cur_med = MED ? mstack_top(P.med[slot], S.atmosphere) : RT_MEDIUM_NONE;
-            const float tm = S.motion ? P.time[slot] : 0.0f;
+            const float tm = MOT ? P.time[slot] : 0.0f;
             float3 wo = xyz(o4), wd = xyz(d4);
             bool exited = false;
             for (int step = 0; step < 256; step++) {
                 uint4 hr;
                 rays++;
-                if (!trace_closest(S, st, wo, wd, INFINITY, P.err, hr, tm)) break;  // escaped through a crack
+                if (!trace_closest<MOT>(S, st, wo, wd, INFINITY, P.err, hr, tm)) break;  // escaped through a crack
                 const MedEvent ev = homog_sample(sst, sss, __uint_as_float(hr.x), beta, rng);
                 beta = beta * ev.w;
                 if (ev.scatter) {
@@ -1721,6 +1721,8 @@ __global__ void __launch_bounds__(BLOCK) k_sss(DevScene S, Paths P, PtConsts C, 
 // (closed form, or ratio tracking from rng); volume hulls push and pop the
 // medium (the ray starts in `medium`, the atmosphere below it), cutouts
 // attenuate by 1 - presence, anything else blocks; at most 16 segments.
+// EXTRA: motion blur (the ray's shutter time) and pattern-driven presence.
+template <bool EXTRA>
 __device__ __forceinline__ float3 shadow_walk(const DevScene& S, TravStack& st, float3 o, float3 d, float remaining,
                                               uint32_t medium, Pcg& rng, uint32_t* err, unsigned long long& rays,
                                               float time) {
@@ -1730,7 +1732,7 @@ __device__ __forceinline__ float3 shadow_walk(const DevScene& S, TravStack& st, 
     for (int k = 0; k < RT_MAX_PRESENCE_SKIPS; k++) {
         rays++;
         uint4 hr;
-        const bool found = remaining > 0.0f && trace_closest(S, st, o, d, remaining, err, hr, time);
+        const bool found = remaining > 0.0f && trace_closest<EXTRA>(S, st, o, d, remaining, err, hr, time);
         const float t = found ? __uint_as_float(hr.x) : remaining;
         const uint32_t cur = mstack_top(ms, S.atmosphere);
         if (cur != RT_MEDIUM_NONE) {
@@ -1748,7 +1750,7 @@ __device__ __forceinline__ float3 shadow_walk(const DevScene& S, TravStack& st, 
             else mstack_pop(ms);
         } else {
             float presence = m.presence;
-            if (S.presence_pat && S.mat_pat[mat].bind_n) {
+            if (EXTRA && S.presence_pat && S.mat_pat[mat].bind_n) {
                 // Pattern-driven cutout: the blocker's material with its
                 // patterns at the hit, footprint 0 (pt/mod.rs:1290,
                 // kernel_pt.metal:1369).
@@ -1774,8 +1776,10 @@ __device__ __forceinline__ float3 shadow_walk(const DevScene& S, TravStack& st, 
 // both contributions in that order. Ratio tracking draws from a stream
 // derived from the path's state, so the image stays reproducible.
 // Without MED (scenes whose cutouts are pattern-driven, no media) each
-// queue entry is a plain slot with one shadow ray and no medium.
-template <int BLOCK, bool MED = true>
+// queue entry is a plain slot with one shadow ray and no medium. EXTRA:
+// motion blur or pattern-driven presence (kept out of the common variant,
+// whose registers they would raise).
+template <int BLOCK, bool MED = true, bool EXTRA = false>
 __global__ void __launch_bounds__(BLOCK) k_shadow_walk(DevScene S, Paths P, PtConsts C) {
     __shared__ uint2 stack_sh[RT_SH_STACK * BLOCK];
     TravStack st;
@@ -1795,8 +1799,9 @@ __global__ void __launch_bounds__(BLOCK) k_shadow_walk(DevScene S, Paths P, PtCo
             const float4 o4 = r == 0 ? P.sh_o[slot] : P.sh2_o[slot];
             const float4 d4 = r == 0 ? P.sh_d[slot] : P.sh2_d[slot];
             const float4 c4 = r == 0 ? P.sh_c[slot] : P.sh2_c[slot];
-            const float3 vis = shadow_walk(S, st, xyz(o4), xyz(d4), d4.w, MED ? __float_as_uint(o4.w) : RT_MEDIUM_NONE,
-                                           rng, P.err, rays, S.motion ? P.time[slot] : 0.0f);
+            const float3 vis = shadow_walk<EXTRA>(S, st, xyz(o4), xyz(d4), d4.w,
+                                                  MED ? __float_as_uint(o4.w) : RT_MEDIUM_NONE, rng, P.err, rays,
+                                                  EXTRA && S.motion ? P.time[slot] : 0.0f);
             const float3 c = xyz(c4) * vis;
             add = add + c;
             if (c4.w != 0.0f) add_aux = add_aux + c;

@@ -234,6 +234,15 @@ static_assert(sizeof(DevInstMotion) == 96, "DevInstMotion layout");
 // scene's second triangle array holds the triangle at shutter close.
 #define RT_DEFORM_MARK 0x7FC5E7u
 
+// Ray pump refill thresholds (lanes of a warp still holding a ray when the
+// idle ones are refilled). Measured on B200 (one 1280x720 pass of the
+// 772k-instance forest, the 1920x1080 cloud at 8 spp): refilling at 20, 26,
+// 28, 30, 32 lanes took the forest 173, 164, 162, 163, 171 ms and the cloud
+// 50.5, 52.3, 54.3, 58.1, 60.5 ms. The forest's long rays through
+// overlapping instances leave lanes idle unevenly, so scenes whose
+// instances overlap densely (the TLAS builders' dense rule) refill earlier.
+constexpr uint32_t RT_REFILL_SPARSE = 20, RT_REFILL_DENSE = 28;
+
 struct DevScene {
     const uint4* nodes;
     const float4* tris;
@@ -275,6 +284,7 @@ struct DevScene {
     uint32_t any_presence;       // some material has presence < 1
     uint32_t presence_pat;       // some material's presence is bound to a pattern (texture cutouts)
     uint32_t max_steps;          // traversal steps per ray before the query is given up (error bit)
+    uint32_t refill_at;          // ray pump: refill idle lanes once at most this many hold a ray
     uint32_t dome;               // first dome light (misses see it), ~0 for none
     const DevMedium* media;      // participating media (null when none)
     uint32_t n_media;

@@ -636,13 +636,19 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
             else k_shade<false><<<shade_grid, SHADE_BLOCK, 0, st>>>(s->S, P, C, qout);
             if (s->S.any_sss) {
                 // Subsurface walks started by this wave's shading.
-                if (med) k_sss<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C, qout);
+                const bool mt = s->S.motion != 0;
+                if (med && mt) k_sss<TRAV_BLOCK, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C, qout);
+                else if (med) k_sss<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C, qout);
+                else if (mt) k_sss<TRAV_BLOCK, false, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C, qout);
                 else k_sss<TRAV_BLOCK, false><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C, qout);
                 launches++;
             }
             CUDA_TRY(cudaEventRecord(s->evpool[ei + 2], st));
-            if (med) k_shadow_walk<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
-            else if (s->S.presence_pat) k_shadow_walk<TRAV_BLOCK, false><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            const bool walk_extra = s->S.motion || s->S.presence_pat;
+            if (med && walk_extra) k_shadow_walk<TRAV_BLOCK, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            else if (med) k_shadow_walk<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
+            else if (s->S.presence_pat)
+                k_shadow_walk<TRAV_BLOCK, false, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             else if (mot) k_shadow<TRAV_BLOCK, true, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             else if (quad) k_shadow<TRAV_BLOCK, true><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
             else k_shadow<TRAV_BLOCK><<<trav_grid, TRAV_BLOCK, 0, st>>>(s->S, P, C);
