@@ -3,8 +3,9 @@
 // Kernels (one training iteration = encode -> forward -> backward -> hash
 // backward -> Adam; inference = encode -> forward):
 //   k_guide_encode    hash-grid features (+ normal, wo) -> X0 rows, bf16
-//   k_guide_fwd       tcgen05 MLP forward, 128-row tiles in two independent
-//                     pipelines per CTA, weights resident in shared memory,
+//   k_guide_fwd       tcgen05 MLP forward, 128-row tiles in six independent
+//                     pipelines of one persistent CTA per SM, weights resident
+//                     in shared memory,
 //                     accumulators in TMEM; stores activations (training) and
 //                     the 48 raw outputs, or the decoded mixture when rendering
 //   k_guide_bwd       vMF-mixture loss gradient in registers, then per layer
@@ -162,7 +163,7 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) k_guide_fwd(GuideDev G, const 
     constexpr bool TRAIN = MODE == FWD_TRAIN;
     uint32_t begin;
     n = batch_slice(B, n, begin);
-    if ((uint64_t)blockIdx.x * FWD_GROUPS * TILE >= n) return;  // no tile for this CTA: skip the weight staging
+    if ((uint64_t)blockIdx.x * TILE >= n) return;  // no tile for this CTA: skip the weight staging
     extern __shared__ __align__(1024) uint8_t sm[];
     __shared__ uint64_t mbar[FWD_GROUPS];
     __shared__ uint32_t tmem_base;
@@ -188,7 +189,10 @@ __global__ void __launch_bounds__(FWD_THREADS, 1) k_guide_fwd(GuideDev G, const 
     const uint32_t s0 = smem_u32(sm);
     const uint32_t act = F_ACT + 16384u * grp;
     uint32_t phase = 0;
-    for (uint32_t tile = blockIdx.x * FWD_GROUPS + grp; tile * TILE < n; tile += gridDim.x * FWD_GROUPS) {
+    // Tiles go to the CTAs first, then to their pipelines (tile = grp x grid +
+    // CTA), so a launch of fewer tiles than pipelines still spreads over
+    // every SM.
+    for (uint32_t tile = grp * gridDim.x + blockIdx.x; tile * TILE < n; tile += gridDim.x * FWD_GROUPS) {
         uint32_t row = tile * TILE + gt;
         bool valid = row < n;
         const uint4* xr = reinterpret_cast<const uint4*>(X0 + (size_t)row * G_IN);
@@ -686,7 +690,7 @@ static int launch_forward(rt_guide* g, const float* rec, uint32_t n, int mode, c
     const uint32_t enc_grid = std::min<uint32_t>((n + 255) / 256, (uint32_t)g->sms * ENCODE_CTAS_PER_SM);
     k_guide_encode<<<enc_grid, 256, 0, st>>>(g->G, rec, n, B, g->X0);
     uint32_t tiles = (n + TILE - 1) / TILE;
-    int grid = (int)std::min<uint32_t>((tiles + FWD_GROUPS - 1) / FWD_GROUPS, (uint32_t)g->sms);
+    int grid = (int)std::min<uint32_t>(tiles, (uint32_t)g->sms);
     if (mode == FWD_TRAIN)
         k_guide_fwd<FWD_TRAIN><<<grid, FWD_THREADS, F_BYTES, st>>>(g->G, g->X0, n, B, g->acts, g->out, g->err);
     else if (mode == FWD_RENDER)
