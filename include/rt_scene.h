@@ -144,7 +144,8 @@ enum { RT_FILTER_BOX = 0, RT_FILTER_TRIANGLE = 1, RT_FILTER_GAUSSIAN = 2 };
 /* Camera::projection (camera.rs:5-9). */
 enum { RT_PROJECTION_PERSPECTIVE = 0, RT_PROJECTION_ORTHOGRAPHIC = 1 };
 
-/* Pinhole / thin-lens camera (src/scene/camera.rs:67-92, 150-179).
+/* Pinhole / thin-lens or orthographic camera (src/scene/camera.rs:67-92,
+ * 150-179).
  * right/up/forward are used as given (Camera::set_transform computes
  * right = forward x up, up = right x forward). */
 typedef struct rt_camera_desc {
