@@ -549,7 +549,6 @@ int rt_render_samples(rt_session* s, uint32_t sample_start, uint32_t count) {
     if (s->guide) C.G = guide_dev(s->guide);
     C.adaptive_tol = s->adaptive_tol;
     C.lum_stats = s->lum_stats;
-    uint64_t guide_records = 0;
     int guide_trainings = 0;
     // Cutouts: decided inside the extension traversal, except when AOVs are
     // kept, whose first-hit values come from the first surface a camera ray
