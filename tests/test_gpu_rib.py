@@ -171,7 +171,7 @@ def test_quadric_ray_batch_matches_oracle():
 
 
 @pytest.mark.parametrize("name,size,spp", [("cornell.rib", (60, 60), 64), ("quadric_zoo.rib", (96, 54), 64),
-                                           ("clouds.rib", (64, 32), 32)])
+                                           ("clouds.rib", (64, 32), 32), ("pan.rib", (64, 32), 32)])
 def test_reference_fixture_renders_match_oracle(name, size, spp):
     """The reference's own scene files through the CUDA path, at reduced
     resolution, against the f64 oracle at the stated tolerance (relMSE in
