@@ -930,6 +930,13 @@ class _Builder:
                 # An analytic quadric with the current transform and the
                 # plain state material (scene_builder.rs:813-909).
                 self.add_quadric(_QUADRIC_KIND[name], a, self.add_material(self.make_material()), self.ctm)
+        elif name == "Procedural" and _str(vals, 0) == "DelayedReadArchive":
+            # Loaded at once, as the reference does (scene_builder.rs:384-399).
+            args = vals[1] if len(vals) > 1 else None
+            f = args[0] if isinstance(args, list) and args and isinstance(args[0], str) else (
+                args if isinstance(args, str) else None)
+            self.warn('Procedural "DelayedReadArchive" loads eagerly (no lazy loading)')
+            self.read_archive(f)
         else:
             self.warn(f"RIB request '{name}' not rendered on this path; skipping")
 
@@ -1274,9 +1281,6 @@ class _Builder:
             if node is None:
                 target = v if isinstance(v, str) else (v[0] if isinstance(v, list) and v else "")
                 self.warn(f'Bxdf references unknown Pattern "{str(target).split(":")[0]}"; ignoring')
-                continue
-            if field == abi.FIELD_PRESENCE:
-                self.warn("presence driven by a pattern is not rendered on this path; ignoring")
                 continue
             out.append((field, node))
         return out

@@ -186,3 +186,34 @@ def test_reference_fixture_renders_match_oracle(name, size, spp):
     res = compare(g, o, r, paired=pr)
     assert res["ok"], res
     assert np.asarray(g).mean() > 0.005
+
+
+def test_rib_presence_pattern_parity():
+    """A RIB scene whose leaf card's presence is a checker pattern
+    ("reference float presence"): pattern-driven cutouts through the RIB
+    route, against the oracle at the stated tolerance."""
+    from mc_parity import compare, render_quad
+    from rtcuda.rib import load_rib_string
+    s = load_rib_string("""
+Format 48 32 1
+Projection "perspective" "fov" [45]
+WorldBegin
+  Light "PxrDomeLight" "sky" "intensity" [0.5]
+  AttributeBegin
+    Translate 0 3 3
+    Rotate 90 1 0 0
+    Light "PxrRectLight" "key" "intensity" [6]
+  AttributeEnd
+  AttributeBegin
+    Pattern "PxrChecker" "holes" "colorA" [1 1 1] "colorB" [0 0 0]
+    Bxdf "PxrSurface" "leaf" "diffuseColor" [0.3 0.7 0.2] "reference float presence" ["holes:resultR"]
+    PointsPolygons [4] [0 1 2 3] "P" [-1 -0.6 3  1 -0.6 3  1 0.6 3.3  -1 0.6 3.3] "st" [0 0 6 0 6 6 0 6]
+  AttributeEnd
+  Bxdf "PxrSurface" "wall" "diffuseColor" [0.8 0.8 0.8]
+  PointsPolygons [4] [0 1 2 3] "P" [-3 -2 5  3 -2 5  3 2 5  -3 2 5]
+WorldEnd
+""")
+    assert [b[1] for b in s.bindings] == [abi.FIELD_PRESENCE]
+    g, o, r, pr, _ = render_quad(s, abi.make_params(max_depth=6), 32, 1024)
+    res = compare(g, o, r, paired=pr)
+    assert res["ok"], res

@@ -202,6 +202,25 @@ def test_reference_fixtures_load():
     assert [l["type"] for l in c.lights] == [abi.LIGHT_RECT]
 
 
+def test_rib_presence_binding_and_delayed_archive():
+    """A Bxdf "reference float presence" connection becomes a presence
+    binding (pattern-driven cutouts), and Procedural "DelayedReadArchive"
+    reads its archive at once (scene_builder.rs:384-399)."""
+    s = load_rib_string("""
+        ArchiveBegin "leaf"
+            PointsPolygons [4] [0 1 2 3] "P" [-1 -1 3  1 -1 3  1 1 3  -1 1 3] "st" [0 0 1 0 1 1 0 1]
+        ArchiveEnd
+        WorldBegin
+            Pattern "PxrChecker" "chk" "colorA" [1 1 1] "colorB" [0 0 0]
+            Bxdf "PxrSurface" "leafy" "diffuseColor" [0.2 0.6 0.2] "reference float presence" ["chk:resultR"]
+            Procedural "DelayedReadArchive" ["leaf"] [-1 1 -1 1 2 4]
+        WorldEnd
+    """)
+    assert s.n_instances == 1
+    assert [(f, n) for _, f, n in s.bindings] == [(abi.FIELD_PRESENCE, 0)]
+    assert not any("presence" in w for w in s.warnings)
+
+
 def test_pan_fixture_motion_blocks():
     """The reference's motion-blur demo (pan.rib): transform blocks on three
     placed objects, a deforming PointsPolygons block, thin-lens depth of
@@ -345,9 +364,10 @@ def test_pattern_requests_and_connections():
     assert s.patterns[3]["texture"] == -1  # wood.tex cannot be read: magenta
     assert s.patterns[4]["scale"] == (8.0, 8.0) and s.patterns[4]["color_a"] == (1.0, 1.0, 1.0)
     assert [b[1:] for b in s.bindings] == [(abi.PATTERN_FIELDS["diffuseColor"], 1),
+                                           (abi.PATTERN_FIELDS["presence"], 0),
                                            (abi.PATTERN_FIELDS["specularFaceColor"], 3)]
     w = " | ".join(s.warnings)
-    assert "wood.tex" in w and "presence" in w and "bogus" in w
+    assert "wood.tex" in w and "bogus" in w
 
 
 def test_st_primvar():
